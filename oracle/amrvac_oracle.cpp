@@ -1,0 +1,1616 @@
+// CPU oracle: FP64 restatement of MPI-AMRVAC's per-block finite-volume update.
+//
+// TEST INFRASTRUCTURE ONLY (see amrvac_oracle.h).  Every routine follows the
+// reference Fortran operation by operation (same expression order, no FMA
+// contraction: compiled with -ffp-contract=off), so that per-cell results
+// agree with the reference to rounding.  Each function cites the reference
+// file:line it restates (paths relative to the reference repository root).
+//
+// All routines are templates on the scalar type R: R=double is the oracle,
+// R=Counted counts +,-,*,/,sqrt,exp (FMA never occurs here) to give the
+// algorithmic flop count per zone update.
+
+#include "amrvac_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+
+// ---------------------------------------------------------------- scalars
+static thread_local long long g_ops = 0;
+
+struct Counted {
+  double v;
+  Counted() : v(0) {}
+  Counted(double x) : v(x) {}
+  explicit operator double() const { return v; }
+};
+inline Counted operator+(Counted a, Counted b) { ++g_ops; return Counted(a.v + b.v); }
+inline Counted operator-(Counted a, Counted b) { ++g_ops; return Counted(a.v - b.v); }
+inline Counted operator*(Counted a, Counted b) { ++g_ops; return Counted(a.v * b.v); }
+inline Counted operator/(Counted a, Counted b) { ++g_ops; return Counted(a.v / b.v); }
+inline Counted operator-(Counted a) { return Counted(-a.v); }
+inline Counted &operator+=(Counted &a, Counted b) { a = a + b; return a; }
+inline Counted &operator-=(Counted &a, Counted b) { a = a - b; return a; }
+inline Counted &operator*=(Counted &a, Counted b) { a = a * b; return a; }
+inline bool operator<(Counted a, Counted b) { return a.v < b.v; }
+inline bool operator>(Counted a, Counted b) { return a.v > b.v; }
+inline bool operator<=(Counted a, Counted b) { return a.v <= b.v; }
+inline bool operator>=(Counted a, Counted b) { return a.v >= b.v; }
+inline bool operator==(Counted a, Counted b) { return a.v == b.v; }
+inline bool operator!=(Counted a, Counted b) { return a.v != b.v; }
+
+inline double val(double x) { return x; }
+inline double val(Counted x) { return x.v; }
+inline double rsqrt_(double x) { return std::sqrt(x); }
+inline Counted rsqrt_(Counted x) { ++g_ops; return Counted(std::sqrt(x.v)); }
+inline double rexp_(double x) { return std::exp(x); }
+inline Counted rexp_(Counted x) { ++g_ops; return Counted(std::exp(x.v)); }
+template <class R> inline R rabs(R x) { return R(std::fabs(val(x))); }
+template <class R> inline R rmax(R a, R b) { return (b > a) ? b : a; }
+template <class R> inline R rmin(R a, R b) { return (b < a) ? b : a; }
+// Fortran sign(a,b): |a| with the sign of b (signed zero honoured).
+template <class R> inline R rsign(double a, R b) { return R(std::copysign(a, val(b))); }
+
+// Fortran parameters (src/mod_constants.t).
+constexpr double zero = 0.0, one = 1.0, two = 2.0, half = 0.5, quarter = 0.25;
+constexpr double third = 1.0 / 3.0;
+constexpr double smalldouble = 1.0e-12, bigdouble = 1.0e99;
+
+// ---------------------------------------------------------------- layout
+struct Box {
+  int lo[3], hi[3];
+};
+inline Box shift(Box b, int d, int s) { b.lo[d] += s; b.hi[d] += s; return b; }
+
+template <class F> inline void forbox(const Box &b, F &&f) {
+  for (int k = b.lo[2]; k <= b.hi[2]; ++k)
+    for (int j = b.lo[1]; j <= b.hi[1]; ++j)
+      for (int i = b.lo[0]; i <= b.hi[0]; ++i) f(i, j, k);
+}
+
+struct Geo {
+  int ndim, ng, n[3], nx[3];
+  size_t cells;
+  int idx(int i, int j, int k) const { return i + n[0] * (j + n[1] * k); }
+  Box ixG() const { Box b; for (int d = 0; d < 3; ++d) { b.lo[d] = 0; b.hi[d] = n[d] - 1; } return b; }
+  Box ixM() const {
+    Box b;
+    for (int d = 0; d < 3; ++d) {
+      if (d < ndim) { b.lo[d] = ng; b.hi[d] = ng + nx[d] - 1; }
+      else { b.lo[d] = 0; b.hi[d] = 0; }
+    }
+    return b;
+  }
+  int off(int d) const { return d == 0 ? 1 : (d == 1 ? n[0] : n[0] * n[1]); }
+};
+
+inline Geo make_geo(const orc_cfg &c) {
+  Geo g;
+  g.ndim = c.ndim;
+  g.ng = c.nghost;
+  for (int d = 0; d < 3; ++d) {
+    g.nx[d] = d < c.ndim ? c.block_nx[d] : 1;
+    g.n[d] = d < c.ndim ? c.block_nx[d] + 2 * c.nghost : 1;
+  }
+  g.cells = (size_t)g.n[0] * g.n[1] * g.n[2];
+  return g;
+}
+
+// Variable indices, 0-based, in the reference order
+// (src/hd/mod_hd_phys.t:210-226, src/mhd/mod_mhd_phys.t:478-503).
+struct Ix {
+  int rho, mom[3], e, mag[3], psi, nw, ndir;
+  bool mhd, glm;
+};
+inline Ix make_ix(const orc_cfg &c) {
+  Ix x;
+  x.ndir = c.ndir;
+  x.mhd = c.physics == 1;
+  x.glm = x.mhd && c.divb == ORC_DIVB_GLM && c.ndim > 1;
+  x.rho = 0;
+  for (int d = 0; d < 3; ++d) x.mom[d] = d < c.ndir ? 1 + d : -1;
+  x.e = c.ndir + 1;
+  for (int d = 0; d < 3; ++d) x.mag[d] = (x.mhd && d < c.ndir) ? c.ndir + 2 + d : -1;
+  x.psi = x.glm ? 2 * c.ndir + 2 : -1;
+  x.nw = x.mhd ? (2 * c.ndir + 2 + (x.glm ? 1 : 0)) : c.ndir + 2;
+  return x;
+}
+
+// Flux types (src/mhd/mod_mhd_phys.t:566-589): 0 default, 1 tvdlf, 2 special, 3 hll.
+enum { FT_DEFAULT = 0, FT_TVDLF = 1, FT_SPECIAL = 2 };
+inline int flux_type(const orc_cfg &c, const Ix &x, int idims /*0-based*/, int iw) {
+  if (!x.mhd || c.ndim <= 1) return FT_DEFAULT;
+  if (x.glm) {
+    if (iw == x.psi) return FT_SPECIAL;
+    if (iw == x.mag[idims]) return FT_SPECIAL;
+    return FT_DEFAULT;
+  }
+  if (iw == x.mag[idims]) return FT_TVDLF;
+  return FT_DEFAULT;
+}
+
+// Block array w(ixG^S,1:nv), column-major.
+template <class R> struct Arr {
+  const Geo *g = nullptr;
+  int nv = 0;
+  std::vector<R> d;
+  Arr() {}
+  Arr(const Geo &geo, int nvars) : g(&geo), nv(nvars), d(geo.cells * nvars) {}
+  R &operator()(int i, int j, int k, int v) { return d[g->idx(i, j, k) + g->cells * (size_t)v]; }
+  const R &operator()(int i, int j, int k, int v) const { return d[g->idx(i, j, k) + g->cells * (size_t)v]; }
+};
+
+struct State {
+  orc_cfg c;
+  Geo g;
+  Ix x;
+  double gamma_1, inv_gamma_1, small_e;
+};
+
+inline State make_state(const orc_cfg &c) {
+  State s;
+  s.c = c;
+  s.g = make_geo(c);
+  s.x = make_ix(c);
+  s.gamma_1 = c.gamma - 1.0;
+  s.inv_gamma_1 = 1.0 / s.gamma_1;
+  // hd_check_params (src/hd/mod_hd_phys.t:541) / mhd_check_params (1213-1214)
+  s.small_e = c.physics == 1 ? c.small_pressure * s.inv_gamma_1 : c.small_pressure / (c.gamma - 1.0);
+  return s;
+}
+
+// Accessor for one cell's variables inside an Arr.
+#define W(a, v) a(i, j, k, v)
+
+// ---------------------------------------------------------------- physics
+// hd_to_conserved (src/hd/mod_hd_phys.t:677-700)
+// mhd_to_conserved_origin (src/mhd/mod_mhd_phys.t:1562-1579)
+template <class R> void to_conserved(const State &s, const Box &b, Arr<R> &w) {
+  const Ix &x = s.x;
+  forbox(b, [&](int i, int j, int k) {
+    R v2 = W(w, x.mom[0]) * W(w, x.mom[0]);
+    for (int c = 1; c < x.ndir; ++c) v2 = v2 + W(w, x.mom[c]) * W(w, x.mom[c]);
+    if (x.mhd) {
+      R b2 = W(w, x.mag[0]) * W(w, x.mag[0]);
+      for (int c = 1; c < x.ndir; ++c) b2 = b2 + W(w, x.mag[c]) * W(w, x.mag[c]);
+      W(w, x.e) = W(w, x.e) * s.inv_gamma_1 + half * (v2 * W(w, x.rho) + b2);
+    } else {
+      W(w, x.e) = W(w, x.e) * s.inv_gamma_1 + half * v2 * W(w, x.rho);
+    }
+    for (int c = 0; c < x.ndir; ++c) W(w, x.mom[c]) = W(w, x.rho) * W(w, x.mom[c]);
+  });
+}
+
+template <class R> int handle_small_values(const State &s, bool primitive, Arr<R> &w, const Box &b);
+
+// hd_to_primitive (src/hd/mod_hd_phys.t:703-734)
+// mhd_to_primitive_origin (src/mhd/mod_mhd_phys.t:1741-1765)
+template <class R> int to_primitive(const State &s, const Box &b, Arr<R> &w) {
+  int st = 0;
+  if (s.c.fix_small_values) st |= handle_small_values(s, false, w, b);
+  const Ix &x = s.x;
+  forbox(b, [&](int i, int j, int k) {
+    R inv_rho = R(1.0) / W(w, x.rho);
+    for (int c = 0; c < x.ndir; ++c) W(w, x.mom[c]) = W(w, x.mom[c]) * inv_rho;
+    R v2 = W(w, x.mom[0]) * W(w, x.mom[0]);
+    for (int c = 1; c < x.ndir; ++c) v2 = v2 + W(w, x.mom[c]) * W(w, x.mom[c]);
+    if (x.mhd) {
+      R b2 = W(w, x.mag[0]) * W(w, x.mag[0]);
+      for (int c = 1; c < x.ndir; ++c) b2 = b2 + W(w, x.mag[c]) * W(w, x.mag[c]);
+      W(w, x.e) = R(s.gamma_1) * (W(w, x.e) - half * (W(w, x.rho) * v2 + b2));
+    } else {
+      W(w, x.e) = R(s.c.gamma - 1.0) * (W(w, x.e) - half * W(w, x.rho) * v2);
+    }
+  });
+  return st;
+}
+
+// hd_check_w (src/hd/mod_hd_phys.t:648-674), mhd_check_w_origin (1452-1473),
+// handle_small_values replace/error (src/hd/mod_hd_phys.t:1420-1516,
+// src/mhd/mod_mhd_phys.t:2191-2253, src/mod_small_values.t:25-87).
+template <class R> int handle_small_values(const State &s, bool primitive, Arr<R> &w, const Box &b) {
+  const Ix &x = s.x;
+  const orc_cfg &c = s.c;
+  int st = 0;
+  forbox(b, [&](int i, int j, int k) {
+    bool frho = W(w, x.rho) < R(c.small_density);
+    bool fe;
+    R m2 = W(w, x.mom[0]) * W(w, x.mom[0]);
+    for (int q = 1; q < x.ndir; ++q) m2 = m2 + W(w, x.mom[q]) * W(w, x.mom[q]);
+    if (primitive) {
+      fe = W(w, x.e) < R(c.small_pressure);
+    } else if (x.mhd) {
+      R b2 = W(w, x.mag[0]) * W(w, x.mag[0]);
+      for (int q = 1; q < x.ndir; ++q) b2 = b2 + W(w, x.mag[q]) * W(w, x.mag[q]);
+      fe = W(w, x.e) - half * (m2 / W(w, x.rho) + b2) < R(s.small_e);
+    } else {
+      R tmp = R(c.gamma - 1.0) * (W(w, x.e) - half * m2 / W(w, x.rho));
+      fe = tmp < R(c.small_pressure);
+    }
+    if (!frho && !fe) return;
+    if (c.small_values_method == 1) {  // replace
+      if (frho) {
+        W(w, x.rho) = R(c.small_density);
+        for (int q = 0; q < x.ndir; ++q) W(w, x.mom[q]) = R(0.0);
+      }
+      auto kin_mag = [&]() {
+        R mm = W(w, x.mom[0]) * W(w, x.mom[0]);
+        for (int q = 1; q < x.ndir; ++q) mm = mm + W(w, x.mom[q]) * W(w, x.mom[q]);
+        if (x.mhd) {
+          R bb = W(w, x.mag[0]) * W(w, x.mag[0]);
+          for (int q = 1; q < x.ndir; ++q) bb = bb + W(w, x.mag[q]) * W(w, x.mag[q]);
+          return half * (mm / W(w, x.rho) + bb);
+        }
+        return half * mm / W(w, x.rho);
+      };
+      if (!x.mhd && frho) {
+        if (primitive) W(w, x.e) = R(c.small_pressure);
+        else W(w, x.e) = R(s.small_e) + kin_mag();
+      }
+      if (fe) {
+        if (primitive) W(w, x.e) = R(c.small_pressure);
+        else W(w, x.e) = R(s.small_e) + kin_mag();
+      }
+    } else {
+      st |= ORC_ST_SMALL_VALUE;
+    }
+  });
+  return st;
+}
+
+// hd_get_flux (src/hd/mod_hd_phys.t:1097-1146),
+// mhd_get_flux (src/mhd/mod_mhd_phys.t:3810-3889)
+template <class R>
+void get_flux(const State &s, const Arr<R> &wC, const Arr<R> &w, const Box &b, int idim,
+              double cmax_global, Arr<R> &f) {
+  const Ix &x = s.x;
+  const int mn = x.mom[idim];
+  forbox(b, [&](int i, int j, int k) {
+    if (!x.mhd) {
+      W(f, x.rho) = W(w, mn) * W(w, x.rho);
+      for (int c = 0; c < x.ndir; ++c) W(f, x.mom[c]) = W(w, mn) * W(wC, x.mom[c]);
+      W(f, mn) = W(f, mn) + W(w, x.e);
+      W(f, x.e) = W(w, mn) * (W(wC, x.e) + W(w, x.e));
+      return;
+    }
+    const int bn = x.mag[idim];
+    W(f, x.rho) = W(w, mn) * W(w, x.rho);
+    for (int c = 0; c < x.ndir; ++c)
+      W(f, x.mom[c]) = W(wC, mn) * W(w, x.mom[c]) - W(w, bn) * W(w, x.mag[c]);
+    R b2 = W(w, x.mag[0]) * W(w, x.mag[0]);
+    for (int c = 1; c < x.ndir; ++c) b2 = b2 + W(w, x.mag[c]) * W(w, x.mag[c]);
+    R ptotal = W(w, x.e) + half * b2;
+    W(f, mn) = W(f, mn) + ptotal;
+    R bv = W(w, x.mag[0]) * W(w, x.mom[0]);
+    for (int c = 1; c < x.ndir; ++c) bv = bv + W(w, x.mag[c]) * W(w, x.mom[c]);
+    W(f, x.e) = W(w, mn) * (W(wC, x.e) + ptotal) - W(w, bn) * bv;
+    for (int c = 0; c < x.ndir; ++c)
+      W(f, x.mag[c]) = W(w, mn) * W(w, x.mag[c]) - W(w, bn) * W(w, x.mom[c]);
+    if (x.glm) {
+      W(f, bn) = W(w, x.psi);
+      W(f, x.psi) = R(cmax_global * cmax_global) * W(w, bn);
+    }
+  });
+}
+
+// mhd_get_csound_prim (src/mhd/mod_mhd_phys.t:3329-3379), one cell.
+template <class R>
+R csound_prim(const State &s, const Arr<R> &w, int i, int j, int k, int idim) {
+  const Ix &x = s.x;
+  R inv_rho = R(1.0) / W(w, x.rho);
+  R cs = R(s.c.gamma) * W(w, x.e) * inv_rho;
+  R b2 = W(w, x.mag[0]) * W(w, x.mag[0]);
+  for (int c = 1; c < x.ndir; ++c) b2 = b2 + W(w, x.mag[c]) * W(w, x.mag[c]);
+  R cfast2 = b2 * inv_rho + cs;
+  R bn = W(w, x.mag[idim]);
+  R av = cfast2 * cfast2 - R(4.0) * cs * (bn * bn) * inv_rho;
+  if (av < R(zero)) av = R(zero);
+  return rsqrt_(half * (cfast2 + rsqrt_(av)));
+}
+
+// hd_get_pthermal + hd_get_csound2 on a conserved state (src/hd/mod_hd_phys.t:1003-1065)
+template <class R>
+R hd_csound2_cons(const State &s, const Arr<R> &w, int i, int j, int k, int &st) {
+  const Ix &x = s.x;
+  R m2 = W(w, x.mom[0]) * W(w, x.mom[0]);
+  for (int c = 1; c < x.ndir; ++c) m2 = m2 + W(w, x.mom[c]) * W(w, x.mom[c]);
+  R ke = R(0.5) * m2 / W(w, x.rho);
+  R pth = R(s.c.gamma - 1.0) * (W(w, x.e) - ke);
+  if (s.c.fix_small_values) {
+    if (pth < R(s.c.small_pressure)) pth = R(s.c.small_pressure);
+  } else if (s.c.check_small_values) {
+    if (pth < R(s.c.small_pressure)) st |= ORC_ST_SMALL_VALUE;
+  }
+  return R(s.c.gamma) * pth / W(w, x.rho);
+}
+
+// hd_get_cbounds (src/hd/mod_hd_phys.t:891-1001),
+// mhd_get_cbounds (src/mhd/mod_mhd_phys.t:3037-3127).  cmin==nullptr: tvdlf form.
+template <class R>
+int get_cbounds(const State &s, const Arr<R> &wLC, const Arr<R> &wRC, const Arr<R> &wLp,
+                const Arr<R> &wRp, const Box &b, int idim, Arr<R> &cmax, Arr<R> *cmin) {
+  const Ix &x = s.x;
+  const int mn = x.mom[idim];
+  int st = 0;
+  const double gam = s.c.gamma;
+  Arr<R> wmean;
+  if (s.c.boundspeed == ORC_BS_CMAXMEAN) wmean = Arr<R>(s.g, x.nw);
+  forbox(b, [&](int i, int j, int k) {
+    switch (s.c.boundspeed) {
+      case ORC_BS_EINFELDT: {
+        R csL, csR;
+        if (x.mhd) {
+          csL = csound_prim(s, wLp, i, j, k, idim);
+          csR = csound_prim(s, wRp, i, j, k, idim);
+        }
+        R tmp1 = rsqrt_(W(wLp, x.rho));
+        R tmp2 = rsqrt_(W(wRp, x.rho));
+        R tmp3 = R(1.0) / (tmp1 + tmp2);
+        R umean = (W(wLp, mn) * tmp1 + W(wRp, mn) * tmp2) * tmp3;
+        R dv = W(wRp, mn) - W(wLp, mn);
+        R dmean;
+        if (x.mhd) {
+          dmean = rsqrt_((tmp1 * (csL * csL) + tmp2 * (csR * csR)) * tmp3 +
+                         half * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
+        } else {
+          csL = R(gam) * W(wLp, x.e) / W(wLp, x.rho);
+          csR = R(gam) * W(wRp, x.e) / W(wRp, x.rho);
+          dmean = (tmp1 * csL + tmp2 * csR) * tmp3 + R(0.5) * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv);
+          dmean = rsqrt_(dmean);
+        }
+        if (cmin) {
+          (*cmin)(i, j, k, 0) = umean - dmean;
+          cmax(i, j, k, 0) = umean + dmean;
+        } else {
+          cmax(i, j, k, 0) = rabs(umean) + dmean;
+        }
+        break;
+      }
+      case ORC_BS_CMAXMEAN: {
+        if (x.mhd) {
+          for (int iw = 0; iw < x.nw; ++iw) W(wmean, iw) = R(0.5) * (W(wLp, iw) + W(wRp, iw));
+          R csR = csound_prim(s, wmean, i, j, k, idim);
+          if (cmin) {
+            cmax(i, j, k, 0) = rmax(W(wmean, mn) + csR, R(zero));
+            (*cmin)(i, j, k, 0) = rmin(W(wmean, mn) - csR, R(zero));
+          } else {
+            cmax(i, j, k, 0) = rabs(W(wmean, mn)) + csR;
+          }
+        } else {
+          for (int iw = 0; iw < x.nw; ++iw) W(wmean, iw) = R(0.5) * (W(wLC, iw) + W(wRC, iw));
+          R tmp1 = W(wmean, mn) / W(wmean, x.rho);
+          R csR = rsqrt_(hd_csound2_cons(s, wmean, i, j, k, st));
+          if (cmin) {
+            cmax(i, j, k, 0) = rmax(tmp1 + csR, R(zero));
+            (*cmin)(i, j, k, 0) = rmin(tmp1 - csR, R(zero));
+          } else {
+            cmax(i, j, k, 0) = rabs(tmp1) + csR;
+          }
+        }
+        break;
+      }
+      default: {  // cmaxleftright
+        R csL, csR;
+        if (x.mhd) {
+          csL = csound_prim(s, wLp, i, j, k, idim);
+          csR = csound_prim(s, wRp, i, j, k, idim);
+          csL = rmax(csL, csR);
+        } else {
+          csL = R(gam) * W(wLp, x.e) / W(wLp, x.rho);
+          csR = R(gam) * W(wRp, x.e) / W(wRp, x.rho);
+          csL = rmax(rsqrt_(csL), rsqrt_(csR));
+        }
+        if (cmin) {
+          (*cmin)(i, j, k, 0) = rmin(W(wLp, mn), W(wRp, mn)) - csL;
+          cmax(i, j, k, 0) = rmax(W(wLp, mn), W(wRp, mn)) + csL;
+        } else {
+          cmax(i, j, k, 0) = rmax(W(wLp, mn), W(wRp, mn)) + csL;
+        }
+        break;
+      }
+    }
+  });
+  return st;
+}
+
+// dwlimiter2 (src/limiter/mod_limiter.t:128-334) on the box ixC; results on
+// ixC contracted by one at its lower end in direction idims.
+template <class R>
+void dwlimiter2(const State &s, const Arr<R> &dwC, const Box &ixC, int idims, double dxlevel,
+                Arr<R> &ldw, Arr<R> &rdw) {
+  const double qsmall = 1.0e-12, qsmall2 = 2.0e-12;
+  const double eps = std::sqrt(2.220446049250313e-16);
+  const double c_mcbeta = 1.4, cadalfa = 0.5, cadbeta = 2.0, cadgamma = 1.6;
+  const double cadepsilon = 1.0e-14, invcadepsilon = 1.0e14;
+  Box ixO = ixC;
+  ixO.lo[idims] += 1;
+  const int o = s.g.off(idims);
+  const int lim = s.c.limiter;
+  R rdelinv(0.0);
+  if (lim == ORC_LIM_CADA3) {
+    R r = R(s.c.cada3_radius) * R(dxlevel);
+    rdelinv = R(one) / (r * r);
+  }
+  forbox(ixO, [&](int i, int j, int k) {
+    const int p = s.g.idx(i, j, k);
+    R a = dwC.d[p];      // dwC(ixO)
+    R bb = dwC.d[p - o]; // dwC(hxO)
+    R l, r;
+    switch (lim) {
+      case ORC_LIM_MINMOD: {
+        R t = rsign(one, a);
+        t = t * rmax(R(zero), rmin(rabs(a), t * bb));
+        l = r = t;
+        break;
+      }
+      case ORC_LIM_WOODWARD: {
+        R t = rsign(one, a);
+        t = R(2.0) * t * rmax(R(zero), rmin(rmin(rabs(a), t * bb), t * R(quarter) * (bb + a)));
+        l = r = t;
+        break;
+      }
+      case ORC_LIM_MCBETA: {
+        R t = rsign(one, a);
+        t = t * rmax(R(zero), rmin(rmin(R(c_mcbeta) * rabs(a), R(c_mcbeta) * t * bb), t * R(half) * (bb + a)));
+        l = r = t;
+        break;
+      }
+      case ORC_LIM_SUPERBEE: {
+        R t = rsign(one, a);
+        t = t * rmax(rmax(R(zero), rmin(R(2.0) * rabs(a), t * bb)), rmin(rabs(a), R(2.0) * t * bb));
+        l = r = t;
+        break;
+      }
+      case ORC_LIM_VANLEER: {
+        R t = R(2.0) * rmax(bb * a, R(zero)) / (a + bb + R(qsmall));
+        l = r = t;
+        break;
+      }
+      case ORC_LIM_ALBADA: {
+        R t = (bb * (a * a + R(qsmall)) + a * (bb * bb + R(qsmall))) / (a * a + bb * bb + R(qsmall2));
+        l = r = t;
+        break;
+      }
+      case ORC_LIM_KOREN: {
+        R t = rsign(one, a);
+        R t2 = rmin(R(2.0) * rabs(a), R(2.0) * t * bb);
+        l = t * rmax(R(zero), rmin(t2, (bb * t + R(2.0) * rabs(a)) * R(third)));
+        r = t * rmax(R(zero), rmin(t2, (R(2.0) * bb * t + rabs(a)) * R(third)));
+        break;
+      }
+      case ORC_LIM_CADA: {
+        R t = bb / (a + rsign(eps, a));
+        R t2 = (R(2.0) + t) * R(third);
+        l = rmax(R(zero), rmin(t2, rmax(-(R(cadalfa) * t), rmin(rmin(R(cadbeta) * t, t2), R(cadgamma))))) * a;
+        t = a / (bb + rsign(eps, bb));
+        t2 = (R(2.0) + t) * R(third);
+        r = rmax(R(zero), rmin(t2, rmax(-(R(cadalfa) * t), rmin(rmin(R(cadbeta) * t, t2), R(cadgamma))))) * bb;
+        break;
+      }
+      default: {  // cada3
+        R tmpeta = (a * a + bb * bb) * rdelinv;
+        auto phi = [&](R t) {
+          R A = (R(two) + t) * R(third);
+          R res;
+          if (tmpeta <= R(one - cadepsilon)) {
+            res = A;
+          } else if (tmpeta >= R(one + cadepsilon)) {
+            res = rmax(R(zero), rmin(A, rmax(-(R(cadalfa) * t), rmin(rmin(R(cadbeta) * t, A), R(cadgamma)))));
+          } else {
+            R t2 = (tmpeta - R(one)) * R(invcadepsilon);
+            res = R(half) * ((R(one) - t2) * A +
+                             (R(one) + t2) * rmax(R(zero), rmin(A, rmax(-(R(cadalfa) * t), rmin(rmin(R(cadbeta) * t, A), R(cadgamma))))));
+          }
+          return res;
+        };
+        l = phi(bb / (a + rsign(eps, a))) * a;
+        r = phi(a / (bb + rsign(eps, bb))) * bb;
+        break;
+      }
+    }
+    ldw.d[p] = l;
+    rdw.d[p] = r;
+  });
+}
+
+// reconstruct_LR default (limiter) branch (src/mod_finite_volume.t:1110-1228)
+template <class R>
+int reconstruct_LR(const State &s, const Box &ixL, const Box &ixR, int idims, const Arr<R> &w,
+                   Arr<R> &wLC, Arr<R> &wRC, Arr<R> &wLp, Arr<R> &wRp, double dxdim) {
+  const Ix &x = s.x;
+  const Geo &g = s.g;
+  const int o = g.off(idims);
+  Box jxR = shift(ixR, idims, 1);
+  Box ixC;
+  for (int d = 0; d < 3; ++d) { ixC.hi[d] = jxR.hi[d]; ixC.lo[d] = ixL.lo[d]; }
+  ixC.lo[idims] -= 1;
+  Arr<R> dwC(g, 1), ldw(g, 1), rdw(g, 1);
+  for (int iw = 0; iw < x.nw; ++iw) {
+    forbox(ixC, [&](int i, int j, int k) {
+      const int p = g.idx(i, j, k);
+      dwC.d[p] = w.d[p + o + g.cells * (size_t)iw] - w.d[p + g.cells * (size_t)iw];
+    });
+    dwlimiter2(s, dwC, ixC, idims, dxdim, ldw, rdw);
+    forbox(ixL, [&](int i, int j, int k) {
+      wLp(i, j, k, iw) = wLp(i, j, k, iw) + R(half) * ldw.d[g.idx(i, j, k)];
+    });
+    forbox(ixR, [&](int i, int j, int k) {
+      wRp(i, j, k, iw) = wRp(i, j, k, iw) - R(half) * rdw.d[g.idx(i, j, k) + o];
+    });
+  }
+  int st = 0;
+  if (s.c.fix_small_values) {
+    st |= handle_small_values(s, true, wLp, ixL);
+    st |= handle_small_values(s, true, wRp, ixR);
+  }
+  for (int iw = 0; iw < x.nw; ++iw) {
+    forbox(ixL, [&](int i, int j, int k) { wLC(i, j, k, iw) = wLp(i, j, k, iw); });
+    forbox(ixR, [&](int i, int j, int k) { wRC(i, j, k, iw) = wRp(i, j, k, iw); });
+  }
+  to_conserved(s, ixL, wLC);
+  to_conserved(s, ixR, wRC);
+  return st;
+}
+
+// mhd_modify_wLR GLM branch (src/mhd/mod_mhd_phys.t:6326-6377)
+template <class R>
+void modify_wLR(const State &s, const Box &b, Arr<R> &wLC, Arr<R> &wRC, Arr<R> &wLp, Arr<R> &wRp,
+                int idir, double cmax_global) {
+  const Ix &x = s.x;
+  const int bn = x.mag[idir], ps = x.psi, e = x.e;
+  const R cg(cmax_global);
+  forbox(b, [&](int i, int j, int k) {
+    R dB = W(wRp, bn) - W(wLp, bn);
+    R dPsi = W(wRp, ps) - W(wLp, ps);
+    W(wLp, bn) = R(half) * (W(wRp, bn) + W(wLp, bn) - dPsi / cg);
+    W(wLp, ps) = R(half) * (W(wRp, ps) + W(wLp, ps) - dB * cg);
+    W(wRp, bn) = W(wLp, bn);
+    W(wRp, ps) = W(wLp, ps);
+    W(wRC, e) = W(wRC, e) - R(half) * (W(wRC, bn) * W(wRC, bn));
+    W(wLC, e) = W(wLC, e) - R(half) * (W(wLC, bn) * W(wLC, bn));
+    W(wRC, bn) = W(wLp, bn);
+    W(wRC, ps) = W(wLp, ps);
+    W(wLC, bn) = W(wLp, bn);
+    W(wLC, ps) = W(wLp, ps);
+    W(wRC, e) = W(wRC, e) + R(half) * (W(wRC, bn) * W(wRC, bn));
+    W(wLC, e) = W(wLC, e) + R(half) * (W(wLC, bn) * W(wLC, bn));
+  });
+}
+
+struct FaceBufs;
+
+// get_Riemann_flux_hll (src/mod_finite_volume.t:381-437)
+template <class R>
+void riemann_hll(const State &s, const Box &b, int idims, const Arr<R> &wLC, const Arr<R> &wRC,
+                 const Arr<R> &fLC, const Arr<R> &fRC, const Arr<R> &cmaxC, const Arr<R> &cminC,
+                 Arr<R> &fC) {
+  const Ix &x = s.x;
+  for (int iw = 0; iw < x.nw; ++iw) {
+    if (flux_type(s.c, x, idims, iw) == FT_TVDLF) {
+      forbox(b, [&](int i, int j, int k) {
+        W(fC, iw) = -(R(s.c.tvdlfeps) * R(half) * rmax(cmaxC(i, j, k, 0), rabs(cminC(i, j, k, 0)))) *
+                    (W(wRC, iw) - W(wLC, iw));
+      });
+      continue;
+    }
+    forbox(b, [&](int i, int j, int k) {
+      R cmin = cminC(i, j, k, 0), cmax = cmaxC(i, j, k, 0);
+      if (cmin >= R(zero)) W(fC, iw) = W(fLC, iw);
+      else if (cmax <= R(zero)) W(fC, iw) = W(fRC, iw);
+      else
+        W(fC, iw) = (cmax * W(fLC, iw) - cmin * W(fRC, iw) + cmin * cmax * (W(wRC, iw) - W(wLC, iw))) /
+                    (cmax - cmin);
+    });
+  }
+}
+
+// get_Riemann_flux_tvdlf (src/mod_finite_volume.t:348-379)
+template <class R>
+void riemann_tvdlf(const State &s, const Box &b, int idims, const Arr<R> &wLC, const Arr<R> &wRC,
+                   const Arr<R> &fLC, const Arr<R> &fRC, const Arr<R> &cmaxC, Arr<R> &fC) {
+  const Ix &x = s.x;
+  for (int iw = 0; iw < x.nw; ++iw) {
+    forbox(b, [&](int i, int j, int k) {
+      R fac = -(R(0.5) * R(s.c.tvdlfeps) * cmaxC(i, j, k, 0));
+      W(fC, iw) = R(0.5) * (W(fLC, iw) + W(fRC, iw));
+      W(fC, iw) = W(fC, iw) + fac * (W(wRC, iw) - W(wLC, iw));
+    });
+  }
+}
+
+// get_Riemann_flux_hllc (src/mod_finite_volume.t:439-504) with hd_get_lCD and
+// hd_get_wCD (src/hd/mod_hd_hllc.t:56-257).  HD only.
+template <class R>
+void riemann_hllc(const State &s, const Box &b, int idims, const Arr<R> &wLC, const Arr<R> &wRC,
+                  Arr<R> &fLC, const Arr<R> &fRC, const Arr<R> &cmaxC, const Arr<R> &cminC,
+                  Arr<R> &fC) {
+  const Ix &x = s.x;
+  const int nw = x.nw, mn = x.mom[idims];
+  forbox(b, [&](int i, int j, int k) {
+    R cmin = cminC(i, j, k, 0), cmax = cmaxC(i, j, k, 0);
+    int patchf = 1;
+    if (cmin >= R(zero)) patchf = -2;
+    else if (cmax <= R(zero)) patchf = 2;
+    R whll[8], Fhll[8], fCD[8];
+    R lambdaCD(0.0);
+    if (patchf == 1) {
+      for (int iw = 0; iw < nw; ++iw) {
+        Fhll[iw] = (cmax * W(fLC, iw) - cmin * W(fRC, iw) + cmin * cmax * (W(wRC, iw) - W(wLC, iw))) /
+                   (cmax - cmin);
+        whll[iw] = (cmax * W(wRC, iw) - cmin * W(wLC, iw) + W(fLC, iw) - W(fRC, iw)) / (cmax - cmin);
+      }
+      lambdaCD = whll[mn] / whll[x.rho];
+      bool cond = true;
+      if (cmin < R(zero) && lambdaCD > R(zero) && lambdaCD < cmax) patchf = -1;
+      else if (cmax > R(zero) && lambdaCD < R(zero) && lambdaCD > cmin) patchf = 1;
+      else if (lambdaCD >= cmax || lambdaCD <= cmin) { lambdaCD = R(zero); patchf = 3; }
+      if (patchf == 3) cond = false;
+      if (cond && lambdaCD == R(zero)) patchf = (-cmin >= cmax) ? 1 : -1;
+    }
+    if (patchf == 1 || patchf == -1) {
+      R cspeed, vSub;
+      const Arr<R> *wSub, *fSub;
+      if (patchf == 1) { cspeed = cmax; vSub = W(wRC, mn) / W(wRC, x.rho); wSub = &wRC; fSub = &fRC; }
+      else { cspeed = cmin; vSub = W(wLC, mn) / W(wLC, x.rho); wSub = &wLC; fSub = &fLC; }
+      R csmls = R(one) / (cspeed - lambdaCD);
+      R wCD[8];
+      wCD[x.rho] = (*wSub)(i, j, k, x.rho) * (cspeed - vSub) * csmls;
+      for (int c = 0; c < x.ndir; ++c) {
+        if (c != idims)
+          wCD[x.mom[c]] = (cspeed * (*wSub)(i, j, k, x.mom[c]) - (*fSub)(i, j, k, x.mom[c])) * csmls;
+        else
+          wCD[x.mom[c]] = wCD[x.rho] * lambdaCD;
+      }
+      R pCD = (*wSub)(i, j, k, x.rho) * (cspeed - vSub) * (lambdaCD - vSub) + (*fSub)(i, j, k, mn) -
+              (*wSub)(i, j, k, mn) * vSub;
+      wCD[x.e] = (cspeed * (*wSub)(i, j, k, x.e) - (*fSub)(i, j, k, x.e) + lambdaCD * pCD) * csmls;
+      for (int iw = 0; iw < nw; ++iw)
+        fCD[iw] = (*fSub)(i, j, k, iw) + cspeed * (wCD[iw] - (*wSub)(i, j, k, iw));
+    }
+    for (int iw = 0; iw < nw; ++iw) {
+      R out = W(fLC, iw);
+      if (patchf == -2) out = W(fLC, iw);
+      else if (patchf == 1 || patchf == -1) out = fCD[iw];
+      else if (patchf == 2) out = W(fRC, iw);
+      else if (patchf == 3) out = Fhll[iw];
+      W(fC, iw) = out;
+    }
+  });
+}
+
+// get_Riemann_flux_hlld (src/mod_finite_volume.t:507-729), no B0/equi split.
+template <class R>
+void riemann_hlld(const State &s, const Box &b, int idims, const Arr<R> &wLC, const Arr<R> &wRC,
+                  const Arr<R> &wLp, const Arr<R> &wRp, const Arr<R> &fLC, const Arr<R> &fRC,
+                  const Arr<R> &cmaxC, const Arr<R> &cminC, Arr<R> &fC) {
+  const Ix &x = s.x;
+  const int nw = x.nw, ndir = x.ndir;
+  const int ip1 = idims;                 // 0-based
+  int ip2 = (idims + 1) % ndir;          // mod(ip1+1,ndir) (1-based) -> 0-based
+  int ip3 = (idims + 2) % ndir;
+  const int rho = x.rho, e = x.e;
+  forbox(b, [&](int i, int j, int k) {
+    R sR = cmaxC(i, j, k, 0), sL = cminC(i, j, k, 0);
+    R BR[3], BL[3];
+    for (int c = 0; c < ndir; ++c) { BR[c] = W(wRC, x.mag[c]); BL[c] = W(wLC, x.mag[c]); }
+    R Bx = (sR * BR[ip1] - sL * BL[ip1]) / (sR - sL);
+    R w1R[10], w1L[10], w2R[10], w2L[10];
+    for (int q = 0; q < 10; ++q) { w1R[q] = w1L[q] = w2R[q] = w2L[q] = R(0.0); }
+    R bR2 = BR[0] * BR[0], bL2 = BL[0] * BL[0];
+    for (int c = 1; c < ndir; ++c) { bR2 = bR2 + BR[c] * BR[c]; bL2 = bL2 + BL[c] * BL[c]; }
+    R ptR = W(wRp, x.e) + R(0.5) * bR2;
+    R ptL = W(wLp, x.e) + R(0.5) * bL2;
+    const int m1 = x.mom[ip1];
+    R suR = (sR - W(wRp, m1)) * W(wRC, rho);
+    R suL = (sL - W(wLp, m1)) * W(wLC, rho);
+    R sm = (suR * W(wRp, m1) - suL * W(wLp, m1) - ptR + ptL) / (suR - suL);
+    w1R[m1] = sm; w1L[m1] = sm; w2R[m1] = sm; w2L[m1] = sm;
+    w1R[x.mag[ip1]] = Bx; w1L[x.mag[ip1]] = Bx;
+    w1R[rho] = suR / (sR - sm);
+    w1L[rho] = suL / (sL - sm);
+    R r1R = suR * (sR - sm) - Bx * Bx;
+    if (r1R != R(0.0)) r1R = R(1.0) / r1R;
+    R r1L = suL * (sL - sm) - Bx * Bx;
+    if (r1L != R(0.0)) r1L = R(1.0) / r1L;
+    const int m2 = x.mom[ip2], b2 = x.mag[ip2];
+    w1R[m2] = W(wRp, m2) - Bx * BR[ip2] * (sm - W(wRp, m1)) * r1R;
+    w1L[m2] = W(wLp, m2) - Bx * BL[ip2] * (sm - W(wLp, m1)) * r1L;
+    w1R[b2] = (suR * (sR - W(wRp, m1)) - Bx * Bx) * r1R;
+    w1L[b2] = (suL * (sL - W(wLp, m1)) - Bx * Bx) * r1L;
+    if (ndir == 3) {
+      const int m3 = x.mom[ip3], b3 = x.mag[ip3];
+      w1R[m3] = W(wRp, m3) - Bx * BR[ip3] * (sm - W(wRp, m1)) * r1R;
+      w1L[m3] = W(wLp, m3) - Bx * BL[ip3] * (sm - W(wLp, m1)) * r1L;
+      w1R[b3] = BR[ip3] * w1R[b2];
+      w1L[b3] = BL[ip3] * w1L[b2];
+    }
+    w1R[b2] = BR[ip2] * w1R[b2];
+    w1L[b2] = BL[ip2] * w1L[b2];
+    // energy (p_ == e_)
+    w1R[e] = suR * (sm - W(wRp, m1)) + ptR;
+    w1L[e] = w1R[e];
+    {
+      R vbR = W(wRp, x.mom[0]) * W(wRC, x.mag[0]);
+      R vbL = W(wLp, x.mom[0]) * W(wLC, x.mag[0]);
+      R v1bR = w1R[x.mom[0]] * w1R[x.mag[0]];
+      R v1bL = w1L[x.mom[0]] * w1L[x.mag[0]];
+      for (int c = 1; c < ndir; ++c) {
+        vbR = vbR + W(wRp, x.mom[c]) * W(wRC, x.mag[c]);
+        vbL = vbL + W(wLp, x.mom[c]) * W(wLC, x.mag[c]);
+        v1bR = v1bR + w1R[x.mom[c]] * w1R[x.mag[c]];
+        v1bL = v1bL + w1L[x.mom[c]] * w1L[x.mag[c]];
+      }
+      R pR = w1R[e], pL = w1L[e];
+      w1R[e] = ((sR - W(wRp, m1)) * W(wRC, e) - ptR * W(wRp, m1) + pR * sm + Bx * (vbR - v1bR)) / (sR - sm);
+      w1L[e] = ((sL - W(wLp, m1)) * W(wLC, e) - ptL * W(wLp, m1) + pL * sm + Bx * (vbL - v1bL)) / (sL - sm);
+    }
+    w2R[rho] = w1R[rho]; w2L[rho] = w1L[rho];
+    w2R[x.mag[ip1]] = w1R[x.mag[ip1]]; w2L[x.mag[ip1]] = w1L[x.mag[ip1]];
+    r1R = rsqrt_(w1R[rho]);
+    r1L = rsqrt_(w1L[rho]);
+    R tmp = R(1.0) / (r1R + r1L);
+    R signBx = rsign(1.0, Bx);
+    R s1R = sm + rabs(Bx) / r1R;
+    R s1L = sm - rabs(Bx) / r1L;
+    w2R[m2] = (r1L * w1L[m2] + r1R * w1R[m2] + (w1R[b2] - w1L[b2]) * signBx) * tmp;
+    w2L[m2] = w2R[m2];
+    w2R[b2] = (r1L * w1R[b2] + r1R * w1L[b2] + r1L * r1R * (w1R[m2] - w1L[m2]) * signBx) * tmp;
+    w2L[b2] = w2R[b2];
+    if (ndir == 3) {
+      const int m3 = x.mom[ip3], b3 = x.mag[ip3];
+      w2R[m3] = (r1L * w1L[m3] + r1R * w1R[m3] + (w1R[b3] - w1L[b3]) * signBx) * tmp;
+      w2L[m3] = w2R[m3];
+      w2R[b3] = (r1L * w1R[b3] + r1R * w1L[b3] + r1L * r1R * (w1R[m3] - w1L[m3]) * signBx) * tmp;
+      w2L[b3] = w2R[b3];
+    }
+    {
+      R a1R = w1R[x.mom[0]] * w1R[x.mag[0]], a2R = w2R[x.mom[0]] * w2R[x.mag[0]];
+      R a1L = w1L[x.mom[0]] * w1L[x.mag[0]], a2L = w2L[x.mom[0]] * w2L[x.mag[0]];
+      for (int c = 1; c < ndir; ++c) {
+        a1R = a1R + w1R[x.mom[c]] * w1R[x.mag[c]];
+        a2R = a2R + w2R[x.mom[c]] * w2R[x.mag[c]];
+        a1L = a1L + w1L[x.mom[c]] * w1L[x.mag[c]];
+        a2L = a2L + w2L[x.mom[c]] * w2L[x.mag[c]];
+      }
+      w2R[e] = w1R[e] + r1R * (a1R - a2R) * signBx;
+      w2L[e] = w1L[e] - r1L * (a1L - a2L) * signBx;
+    }
+    for (int c = 0; c < ndir; ++c) {
+      const int m = x.mom[c];
+      w1R[m] = w1R[m] * w1R[rho];
+      w1L[m] = w1L[m] * w1L[rho];
+      w2R[m] = w2R[m] * w2R[rho];
+      w2L[m] = w2L[m] * w2L[rho];
+    }
+    for (int iw = 0; iw < nw; ++iw) {
+      int ft = flux_type(s.c, x, idims, iw);
+      if (ft == FT_SPECIAL) {
+        W(fC, iw) = W(fLC, iw);
+      } else {
+        R out = W(fC, iw);
+        if (sL > R(0.0)) out = W(fLC, iw);
+        else if (s1L >= R(0.0)) out = W(fLC, iw) + sL * (w1L[iw] - W(wLC, iw));
+        else if (sm >= R(0.0)) out = W(fLC, iw) + sL * (w1L[iw] - W(wLC, iw)) + s1L * (w2L[iw] - w1L[iw]);
+        else if (s1R >= R(0.0)) out = W(fRC, iw) + sR * (w1R[iw] - W(wRC, iw)) + s1R * (w2R[iw] - w1R[iw]);
+        else if (sR >= R(0.0)) out = W(fRC, iw) + sR * (w1R[iw] - W(wRC, iw));
+        else if (sR < R(0.0)) out = W(fRC, iw);
+        W(fC, iw) = out;
+      }
+    }
+  });
+}
+
+// gradient, Cartesian nth=1 (src/mod_geometry.t:329-394)
+template <class R>
+void gradient(const State &s, const Arr<R> &q, int iq, const Box &ixO, int idir, double dxlevel,
+              std::vector<R> &gradq) {
+  const int o = s.g.off(idir);
+  forbox(ixO, [&](int i, int j, int k) {
+    const int p = s.g.idx(i, j, k);
+    const size_t vo = s.g.cells * (size_t)iq;
+    R gq = (q.d[vo + p + o] - q.d[vo + p - o]) * R(half);
+    gradq[p] = gq / R(dxlevel);
+  });
+}
+
+// divvector on the magnetic field, slab_uniform, nth = 1 or 2
+// (src/mod_geometry.t:582-651), as called by get_divb
+// (src/physics/mod_functions_bfield.t:14-46).
+template <class R>
+void divb_central(const State &s, const Arr<R> &w, const Box &ixO, const double *dxlevel, int nth,
+                  std::vector<R> &divq) {
+  const Ix &x = s.x;
+  R invdx[3];
+  for (int d = 0; d < s.c.ndim; ++d) invdx[d] = R(1.0) / R(dxlevel[d]);
+  forbox(ixO, [&](int i, int j, int k) { divq[s.g.idx(i, j, k)] = R(0.0); });
+  for (int d = 0; d < s.c.ndim; ++d) {
+    const int o = s.g.off(d);
+    const size_t vo = s.g.cells * (size_t)x.mag[d];
+    forbox(ixO, [&](int i, int j, int k) {
+      const int p = s.g.idx(i, j, k);
+      if (nth == 1) {
+        divq[p] = divq[p] + R(half) * (w.d[vo + p + o] - w.d[vo + p - o]) * invdx[d];
+      } else {
+        divq[p] = divq[p] + (-w.d[vo + p + 2 * o] + R(8.0) * w.d[vo + p + o] - R(8.0) * w.d[vo + p - o] +
+                             w.d[vo + p - 2 * o]) /
+                                (R(12.0) * R(dxlevel[d]));
+      }
+    });
+  }
+}
+
+// add_source_glm (src/mhd/mod_mhd_phys.t:5472-5531)
+template <class R>
+void add_source_glm(const State &s, double qdt, const Box &ixI, const Box &ixO, const Arr<R> &wCT,
+                    Arr<R> &w, const double *dxlevel, double cmax_global) {
+  const Ix &x = s.x;
+  const orc_cfg &c = s.c;
+  double mindx = dxlevel[0];
+  for (int d = 1; d < c.ndim; ++d) mindx = std::min(mindx, dxlevel[d]);
+  if (c.glm_alpha < 0) {
+    forbox(ixO, [&](int i, int j, int k) { W(w, x.psi) = R(std::fabs(c.glm_alpha)) * W(wCT, x.psi); });
+  } else {
+    R fac = rexp_(-(R(qdt) * R(cmax_global) * R(c.glm_alpha)) / R(mindx));
+    forbox(ixO, [&](int i, int j, int k) { W(w, x.psi) = fac * W(w, x.psi); });
+  }
+  if (c.glm_extended) {
+    std::vector<R> grad(s.g.cells), divb(s.g.cells);
+    for (int d = 0; d < c.ndim; ++d) {
+      gradient(s, wCT, x.psi, ixO, d, dxlevel[d], grad);
+      forbox(ixO, [&](int i, int j, int k) {
+        W(w, x.e) = W(w, x.e) - R(qdt) * W(wCT, x.mag[d]) * grad[s.g.idx(i, j, k)];
+      });
+    }
+    divb_central(s, wCT, ixO, dxlevel, 1, divb);
+    for (int d = 0; d < x.ndir; ++d) {
+      forbox(ixO, [&](int i, int j, int k) {
+        W(w, x.mom[d]) = W(w, x.mom[d]) - R(qdt) * W(wCT, x.mag[d]) * divb[s.g.idx(i, j, k)];
+      });
+    }
+  }
+  (void)ixI;
+}
+
+// add_source_linde (src/mhd/mod_mhd_phys.t:5599-5665), uniform grid (no level jumps).
+template <class R>
+void add_source_linde(const State &s, double qdt, const Box &ixO, const Arr<R> &wCT, Arr<R> &w,
+                      const double *dxlevel) {
+  const Ix &x = s.x;
+  const orc_cfg &c = s.c;
+  Box ixp = ixO;
+  for (int d = 0; d < c.ndim; ++d) { ixp.lo[d] -= 1; ixp.hi[d] += 1; }
+  std::vector<R> divb(s.g.cells), grad(s.g.cells);
+  divb_central(s, wCT, ixp, dxlevel, 1, divb);
+  R inv2(0.0);
+  {
+    R acc = R(1.0) / (R(dxlevel[0]) * R(dxlevel[0]));
+    for (int d = 1; d < c.ndim; ++d) acc = acc + R(1.0) / (R(dxlevel[d]) * R(dxlevel[d]));
+    inv2 = acc;
+  }
+  for (int d = 0; d < c.ndim; ++d) {
+    const int o = s.g.off(d);
+    forbox(ixO, [&](int i, int j, int k) {
+      const int p = s.g.idx(i, j, k);
+      R gq = (divb[p + o] - divb[p - o]) * R(half);
+      gq = gq / R(dxlevel[d]);
+      gq = gq * R(c.divbdiff) / inv2;
+      W(w, x.mag[d]) = W(w, x.mag[d]) + gq;
+      W(w, x.e) = W(w, x.e) + W(wCT, x.mag[d]) * gq;
+    });
+  }
+  (void)qdt;
+}
+
+// finite_volume (src/mod_finite_volume.t:116-339), slab_uniform, no local dt.
+template <class R>
+int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, double dtfactor,
+                  const double *dxs, double cmax_global) {
+  const Ix &x = s.x;
+  const orc_cfg &c = s.c;
+  const Geo &g = s.g;
+  const int nw = x.nw, ndim = c.ndim;
+  Box ixI = g.ixG(), ixO = g.ixM();
+  int st = 0;
+  Arr<R> wprim = wCT;
+  st |= to_primitive(s, ixI, wprim);
+  Arr<R> wLp(g, nw), wRp(g, nw), wLC(g, nw), wRC(g, nw), fLC(g, nw), fRC(g, nw);
+  Arr<R> cmaxC(g, 1), cminC(g, 1);
+  std::vector<Arr<R>> fC;
+  for (int d = 0; d < ndim; ++d) fC.emplace_back(g, nw);
+  for (int idims = 0; idims < ndim; ++idims) {
+    const int o = g.off(idims);
+    Box kxC = ixI;
+    kxC.hi[idims] -= 1;
+    wLp.d = wprim.d;
+    wRp.d = wprim.d;
+    for (int iw = 0; iw < nw; ++iw)
+      forbox(kxC, [&](int i, int j, int k) {
+        const size_t p = g.idx(i, j, k) + g.cells * (size_t)iw;
+        wRp.d[p] = wprim.d[p + o];
+      });
+    Box ixC = ixO;
+    ixC.lo[idims] -= 1;
+    Box ixCR = ixC;
+    st |= reconstruct_LR(s, ixCR, ixCR, idims, wprim, wLC, wRC, wLp, wRp, dxs[idims]);
+    if (x.glm) modify_wLR(s, ixCR, wLC, wRC, wLp, wRp, idims, cmax_global);
+    get_flux(s, wLC, wLp, ixC, idims, cmax_global, fLC);
+    get_flux(s, wRC, wRp, ixC, idims, cmax_global, fRC);
+    if (c.flux_scheme == ORC_FS_TVDLF) {
+      st |= get_cbounds(s, wLC, wRC, wLp, wRp, ixC, idims, cmaxC, (Arr<R> *)nullptr);
+      riemann_tvdlf(s, ixC, idims, wLC, wRC, fLC, fRC, cmaxC, fC[idims]);
+    } else {
+      st |= get_cbounds(s, wLC, wRC, wLp, wRp, ixC, idims, cmaxC, &cminC);
+      switch (c.flux_scheme) {
+        case ORC_FS_HLL: riemann_hll(s, ixC, idims, wLC, wRC, fLC, fRC, cmaxC, cminC, fC[idims]); break;
+        case ORC_FS_HLLC: riemann_hllc(s, ixC, idims, wLC, wRC, fLC, fRC, cmaxC, cminC, fC[idims]); break;
+        default: riemann_hlld(s, ixC, idims, wLC, wRC, wLp, wRp, fLC, fRC, cmaxC, cminC, fC[idims]); break;
+      }
+    }
+  }
+  // conservative update (src/mod_finite_volume.t:269-284)
+  for (int idims = 0; idims < ndim; ++idims) {
+    const int o = g.off(idims);
+    R dxinv = -R(qdt) / R(dxs[idims]);
+    Box hb = ixO;
+    hb.lo[idims] -= 1;
+    for (int iw = 0; iw < nw; ++iw) {
+      forbox(hb, [&](int i, int j, int k) { fC[idims](i, j, k, iw) = dxinv * fC[idims](i, j, k, iw); });
+      forbox(ixO, [&](int i, int j, int k) {
+        const size_t p = g.idx(i, j, k) + g.cells * (size_t)iw;
+        wnew.d[p] = wnew.d[p] + fC[idims].d[p] - fC[idims].d[p - o];
+      });
+    }
+  }
+  if (c.fix_small_values) {
+    int s2 = handle_small_values(s, false, wnew, ixO);
+    st |= s2;
+    if (s2 & ORC_ST_SMALL_VALUE) wnew.d = wCT.d;
+  }
+  // addsource2 -> mhd_add_source divB part (src/mod_source.t:130-160)
+  if (x.mhd && ndim > 1) {
+    double qsrc = qdt * double(ndim) / double(ndim);
+    if (c.divb == ORC_DIVB_GLM) add_source_glm(s, qsrc, ixI, ixO, wCT, wnew, dxs, cmax_global);
+    else if (c.divb == ORC_DIVB_LINDE) add_source_linde(s, qsrc, ixO, wCT, wnew, dxs);
+  }
+  (void)dtfactor;
+  return st;
+}
+
+// getdt_courant (src/mod_dt.t:160-287) with hd_get_cmax (src/hd/mod_hd_phys.t:787-811)
+// and mhd_get_cmax_origin (src/mhd/mod_mhd_phys.t:2482-2550).
+template <class R>
+int getdt_block(const State &s, const Arr<R> &w, const double *dx, double *dtnew, double *cmax_mype) {
+  const Ix &x = s.x;
+  const orc_cfg &c = s.c;
+  const Geo &g = s.g;
+  Box ixI = g.ixG(), ixO = g.ixM();
+  Arr<R> wprim = w;
+  int st = to_primitive(s, ixI, wprim);
+  std::vector<R> cmax(g.cells), cmaxtot(g.cells);
+  R courantmax(0.0), courantmaxtot(0.0);
+  double dtn = bigdouble;
+  R dxinv[3];
+  for (int d = 0; d < c.ndim; ++d) dxinv[d] = R(one) / R(dx[d]);
+  for (int idims = 0; idims < c.ndim; ++idims) {
+    forbox(ixO, [&](int i, int j, int k) {
+      const int mn = x.mom[idims];
+      R cm;
+      if (x.mhd) {
+        R inv_rho = R(1.0) / W(wprim, x.rho);
+        R cs = R(c.gamma) * W(wprim, x.e) * inv_rho;
+        R b2 = W(wprim, x.mag[0]) * W(wprim, x.mag[0]);
+        for (int q = 1; q < x.ndir; ++q) b2 = b2 + W(wprim, x.mag[q]) * W(wprim, x.mag[q]);
+        R cfast2 = b2 * inv_rho + cs;
+        R bn = W(wprim, x.mag[idims]);
+        R av = cfast2 * cfast2 - R(4.0) * cs * (bn * bn) * inv_rho;
+        if (av < R(zero)) av = R(zero);
+        cm = rsqrt_(R(half) * (cfast2 + rsqrt_(av)));
+        cm = rabs(W(wprim, mn)) + cm;
+      } else {
+        cm = rabs(W(wprim, mn)) + rsqrt_(R(c.gamma) * W(wprim, x.e) / W(wprim, x.rho));
+      }
+      cmax[g.idx(i, j, k)] = cm;
+    });
+    R cmx(0.0);
+    bool first = true;
+    forbox(ixO, [&](int i, int j, int k) {
+      R v = cmax[g.idx(i, j, k)];
+      if (first || v > cmx) { cmx = v; first = false; }
+    });
+    if (val(cmx) > *cmax_mype) *cmax_mype = val(cmx);
+    if (c.type_courant == ORC_COURANT_MAXSUM) {
+      forbox(ixO, [&](int i, int j, int k) {
+        const int p = g.idx(i, j, k);
+        if (idims == 0) cmaxtot[p] = cmax[p] * dxinv[idims];
+        else cmaxtot[p] = cmaxtot[p] + cmax[p] * dxinv[idims];
+      });
+    } else {
+      R m(0.0);
+      bool f2 = true;
+      forbox(ixO, [&](int i, int j, int k) {
+        R v = cmax[g.idx(i, j, k)] * dxinv[idims];
+        if (f2 || v > m) { m = v; f2 = false; }
+      });
+      courantmax = rmax(courantmax, m);
+      if (c.type_courant == ORC_COURANT_SUMMAX) courantmaxtot = courantmaxtot + courantmax;
+    }
+  }
+  if (c.type_courant == ORC_COURANT_MAXSUM) {
+    R m(0.0);
+    bool f = true;
+    forbox(ixO, [&](int i, int j, int k) {
+      R v = cmaxtot[g.idx(i, j, k)];
+      if (f || v > m) { m = v; f = false; }
+    });
+    if (val(m) > smalldouble) dtn = std::min(dtn, val(R(c.courantpar) / m));
+  } else if (c.type_courant == ORC_COURANT_SUMMAX) {
+    if (val(courantmaxtot) > smalldouble) dtn = std::min(dtn, val(R(c.courantpar) / courantmaxtot));
+  } else {
+    if (val(courantmax) > smalldouble) dtn = std::min(dtn, val(R(c.courantpar) / courantmax));
+  }
+  *dtnew = dtn;
+  return st;
+}
+
+// ---------------------------------------------------------------- grid
+struct Grid {
+  State s;
+  int nb[3];
+  int nblocks;
+  double dx[3], xmin[3], xmax[3];
+  int bc[6];
+  std::vector<int> nbr;  // [ib][27] neighbour block or -1 (physical boundary)
+  std::vector<double> reg[3];
+  size_t bsize;
+};
+
+inline int dir_index(int di, int dj, int dk) { return (di + 1) + 3 * ((dj + 1) + 3 * (dk + 1)); }
+
+}  // namespace orc
+
+using namespace orc;
+
+struct orc_grid : public Grid {};
+
+extern "C" {
+
+int orc_cfg_finalize(orc_cfg *cfg) {
+  Ix x = make_ix(*cfg);
+  cfg->nw = x.nw;
+  if (cfg->ssprk_order == 0) cfg->ssprk_order = 3;
+  return x.nw;
+}
+
+static Arr<double> wrap_in(const Geo &g, int nw, const double *src) {
+  Arr<double> a(g, nw);
+  std::memcpy(a.d.data(), src, sizeof(double) * a.d.size());
+  return a;
+}
+
+int orc_finite_volume(const orc_cfg *cfg, const double *wct, double *wnew, double qdt, double dtfactor,
+                      const double *dx, double cmax_global) {
+  State s = make_state(*cfg);
+  Arr<double> a = wrap_in(s.g, s.x.nw, wct), b = wrap_in(s.g, s.x.nw, wnew);
+  int st = finite_volume(s, a, b, qdt, dtfactor, dx, cmax_global);
+  std::memcpy(wnew, b.d.data(), sizeof(double) * b.d.size());
+  return st;
+}
+
+int orc_getdt_block(const orc_cfg *cfg, const double *w, const double *dx, double *dtnew,
+                    double *cmax_max) {
+  State s = make_state(*cfg);
+  Arr<double> a = wrap_in(s.g, s.x.nw, w);
+  return getdt_block(s, a, dx, dtnew, cmax_max);
+}
+
+void orc_to_primitive(const orc_cfg *cfg, double *w) {
+  State s = make_state(*cfg);
+  Arr<double> a = wrap_in(s.g, s.x.nw, w);
+  to_primitive(s, s.g.ixG(), a);
+  std::memcpy(w, a.d.data(), sizeof(double) * a.d.size());
+}
+
+void orc_to_conserved(const orc_cfg *cfg, double *w) {
+  State s = make_state(*cfg);
+  Arr<double> a = wrap_in(s.g, s.x.nw, w);
+  to_conserved(s, s.g.ixG(), a);
+  std::memcpy(w, a.d.data(), sizeof(double) * a.d.size());
+}
+
+// Points API: a 1-D "block" of n cells, state-major input.
+static State point_state(const orc_cfg *cfg, int n) {
+  orc_cfg c = *cfg;
+  c.block_nx[0] = n; c.block_nx[1] = 1; c.block_nx[2] = 1;
+  c.nghost = 0;
+  State s = make_state(c);
+  s.g.ndim = 1;
+  s.g.ng = 0;
+  s.g.n[0] = n; s.g.n[1] = 1; s.g.n[2] = 1;
+  s.g.nx[0] = n; s.g.nx[1] = 1; s.g.nx[2] = 1;
+  s.g.cells = n;
+  return s;
+}
+static void load_points(const State &s, int n, const double *src, Arr<double> &a) {
+  for (int p = 0; p < n; ++p)
+    for (int iw = 0; iw < s.x.nw; ++iw) a(p, 0, 0, iw) = src[(size_t)p * s.x.nw + iw];
+}
+static Box line_box(int n) { Box b; b.lo[0] = 0; b.hi[0] = n - 1; b.lo[1] = b.hi[1] = b.lo[2] = b.hi[2] = 0; return b; }
+
+void orc_get_flux_points(const orc_cfg *cfg, int n, const double *wc, const double *wp, int idim,
+                         double cmax_global, double *f) {
+  State s = point_state(cfg, n);
+  Arr<double> C(s.g, s.x.nw), P(s.g, s.x.nw), F(s.g, s.x.nw);
+  load_points(s, n, wc, C);
+  load_points(s, n, wp, P);
+  get_flux(s, C, P, line_box(n), idim - 1, cmax_global, F);
+  for (int p = 0; p < n; ++p)
+    for (int iw = 0; iw < s.x.nw; ++iw) f[(size_t)p * s.x.nw + iw] = F(p, 0, 0, iw);
+}
+
+void orc_get_cbounds_points(const orc_cfg *cfg, int n, const double *wlc, const double *wrc,
+                            const double *wlp, const double *wrp, int idim, double *cmax, double *cmin) {
+  State s = point_state(cfg, n);
+  Arr<double> LC(s.g, s.x.nw), RC(s.g, s.x.nw), LP(s.g, s.x.nw), RP(s.g, s.x.nw), CX(s.g, 1), CN(s.g, 1);
+  load_points(s, n, wlc, LC); load_points(s, n, wrc, RC);
+  load_points(s, n, wlp, LP); load_points(s, n, wrp, RP);
+  get_cbounds(s, LC, RC, LP, RP, line_box(n), idim - 1, CX, cmin ? &CN : (Arr<double> *)nullptr);
+  for (int p = 0; p < n; ++p) {
+    cmax[p] = CX(p, 0, 0, 0);
+    if (cmin) cmin[p] = CN(p, 0, 0, 0);
+  }
+}
+
+void orc_riemann_points(const orc_cfg *cfg, int n, const double *wlp_in, const double *wrp_in, int idim,
+                        double cmax_global, double *f) {
+  State s = point_state(cfg, n);
+  const int d = idim - 1;
+  Arr<double> LP(s.g, s.x.nw), RP(s.g, s.x.nw), LC(s.g, s.x.nw), RC(s.g, s.x.nw), FL(s.g, s.x.nw),
+      FR(s.g, s.x.nw), FC(s.g, s.x.nw), CX(s.g, 1), CN(s.g, 1);
+  load_points(s, n, wlp_in, LP);
+  load_points(s, n, wrp_in, RP);
+  Box b = line_box(n);
+  LC.d = LP.d; RC.d = RP.d;
+  to_conserved(s, b, LC);
+  to_conserved(s, b, RC);
+  if (s.x.mhd && cfg->divb == ORC_DIVB_GLM && cfg->ndim > 1) modify_wLR(s, b, LC, RC, LP, RP, d, cmax_global);
+  get_flux(s, LC, LP, b, d, cmax_global, FL);
+  get_flux(s, RC, RP, b, d, cmax_global, FR);
+  if (cfg->flux_scheme == ORC_FS_TVDLF) {
+    get_cbounds(s, LC, RC, LP, RP, b, d, CX, (Arr<double> *)nullptr);
+    riemann_tvdlf(s, b, d, LC, RC, FL, FR, CX, FC);
+  } else {
+    get_cbounds(s, LC, RC, LP, RP, b, d, CX, &CN);
+    if (cfg->flux_scheme == ORC_FS_HLL) riemann_hll(s, b, d, LC, RC, FL, FR, CX, CN, FC);
+    else if (cfg->flux_scheme == ORC_FS_HLLC) riemann_hllc(s, b, d, LC, RC, FL, FR, CX, CN, FC);
+    else riemann_hlld(s, b, d, LC, RC, LP, RP, FL, FR, CX, CN, FC);
+  }
+  for (int p = 0; p < n; ++p)
+    for (int iw = 0; iw < s.x.nw; ++iw) f[(size_t)p * s.x.nw + iw] = FC(p, 0, 0, iw);
+}
+
+void orc_limiter_line(const orc_cfg *cfg, int n, const double *dwc, double dxlevel, double *ldw,
+                      double *rdw) {
+  orc_cfg c = *cfg;
+  c.ndim = 1;
+  State s = point_state(&c, n);
+  Arr<double> D(s.g, 1), L(s.g, 1), R(s.g, 1);
+  for (int p = 0; p < n; ++p) { D.d[p] = dwc[p]; L.d[p] = ldw[p]; R.d[p] = rdw[p]; }
+  dwlimiter2(s, D, line_box(n), 0, dxlevel, L, R);
+  for (int p = 0; p < n; ++p) { ldw[p] = L.d[p]; rdw[p] = R.d[p]; }
+}
+
+// ---------------------------------------------------------------- grid API
+orc_grid *orc_grid_create(const orc_cfg *cfg, const int *domain_nx, const double *xprobmin,
+                          const double *xprobmax, const int *bc) {
+  orc_grid *g = new orc_grid();
+  g->s = make_state(*cfg);
+  g->nblocks = 1;
+  for (int d = 0; d < 3; ++d) {
+    if (d < cfg->ndim) {
+      g->nb[d] = domain_nx[d] / cfg->block_nx[d];
+      g->dx[d] = (xprobmax[d] - xprobmin[d]) / double(domain_nx[d]);
+      g->xmin[d] = xprobmin[d];
+      g->xmax[d] = xprobmax[d];
+    } else {
+      g->nb[d] = 1; g->dx[d] = 1.0; g->xmin[d] = 0; g->xmax[d] = 1;
+    }
+    g->nblocks *= g->nb[d];
+  }
+  for (int q = 0; q < 6; ++q) g->bc[q] = q < 2 * cfg->ndim ? bc[q] : ORC_BC_PERIODIC;
+  g->bsize = g->s.g.cells * (size_t)g->s.x.nw;
+  for (int r = 0; r < 3; ++r) g->reg[r].assign(g->bsize * g->nblocks, 0.0);
+  g->nbr.assign((size_t)g->nblocks * 27, -1);
+  for (int ib = 0; ib < g->nblocks; ++ib) {
+    int ig[3] = {ib % g->nb[0], (ib / g->nb[0]) % g->nb[1], ib / (g->nb[0] * g->nb[1])};
+    for (int dk = -1; dk <= 1; ++dk)
+      for (int dj = -1; dj <= 1; ++dj)
+        for (int di = -1; di <= 1; ++di) {
+          int dd[3] = {di, dj, dk};
+          int jg[3];
+          bool ok = true;
+          for (int d = 0; d < 3; ++d) {
+            if (d >= cfg->ndim) { if (dd[d] != 0) ok = false; jg[d] = 0; continue; }
+            jg[d] = ig[d] + dd[d];
+            if (jg[d] < 0 || jg[d] >= g->nb[d]) {
+              int side = jg[d] < 0 ? 0 : 1;
+              if (g->bc[2 * d + side] == ORC_BC_PERIODIC) jg[d] = (jg[d] + g->nb[d]) % g->nb[d];
+              else ok = false;
+            }
+          }
+          if (ok) g->nbr[(size_t)ib * 27 + dir_index(di, dj, dk)] = jg[0] + g->nb[0] * (jg[1] + g->nb[1] * jg[2]);
+        }
+  }
+  return g;
+}
+
+void orc_grid_destroy(orc_grid *g) { delete g; }
+int orc_grid_nblocks(const orc_grid *g) { return g->nblocks; }
+void orc_grid_block_index(const orc_grid *g, int ib, int *ig) {
+  ig[0] = ib % g->nb[0];
+  ig[1] = (ib / g->nb[0]) % g->nb[1];
+  ig[2] = ib / (g->nb[0] * g->nb[1]);
+}
+void orc_grid_dx(const orc_grid *g, double *dx) { for (int d = 0; d < g->s.c.ndim; ++d) dx[d] = g->dx[d]; }
+
+// Block geometry (src/amr/mod_amr_solution_node.t:158-164)
+double orc_grid_x(const orc_grid *g, int ib, int idim, int i) {
+  int ig[3];
+  orc_grid_block_index(g, ib, ig);
+  const int d = idim;
+  double dg = g->s.c.block_nx[d] * g->dx[d];
+  double rxmin = g->xmin[d] + double(ig[d]) * dg;
+  return rxmin + (double(i + 1 - g->s.c.nghost) - half) * g->dx[d];
+}
+
+void orc_grid_set_block(orc_grid *g, int ib, const double *w) {
+  std::memcpy(&g->reg[0][g->bsize * ib], w, sizeof(double) * g->bsize);
+}
+void orc_grid_get_block(const orc_grid *g, int ib, double *w) {
+  std::memcpy(w, &g->reg[0][g->bsize * ib], sizeof(double) * g->bsize);
+}
+
+// ixS_srl_/ixR_srl_ (src/mod_ghostcells_update.t:150-162), 0-based inclusive,
+// indexed by i+1 for i in {-1,0,1}.
+void orc_srl_maps(int nghost, int block_nx, int *s_min, int *s_max, int *r_min, int *r_max) {
+  // Fortran 1-based: ixMmin = nghost+1, ixMmax = nghost+block_nx, ixGmax = block_nx+2*nghost
+  int ixMmin = nghost + 1, ixMmax = nghost + block_nx, ixGmax = block_nx + 2 * nghost;
+  int smin[3] = {ixMmin, ixMmin, ixMmax + 1 - nghost};
+  int smax[3] = {ixMmin - 1 + nghost, ixMmax, ixMmax};
+  int rmin[3] = {1, ixMmin, ixMmax + 1};
+  int rmax[3] = {nghost, ixMmax, ixGmax};
+  for (int q = 0; q < 3; ++q) {
+    s_min[q] = smin[q] - 1; s_max[q] = smax[q] - 1;
+    r_min[q] = rmin[q] - 1; r_max[q] = rmax[q] - 1;
+  }
+}
+
+static void getbc_reg(Grid &G, std::vector<double> &reg) {
+  const State &s = G.s;
+  const Geo &g = s.g;
+  const int ndim = s.c.ndim, nw = s.x.nw;
+  int smin[3], smax[3], rmin[3], rmax[3];
+  int sminA[3][3], smaxA[3][3], rminA[3][3], rmaxA[3][3];
+  for (int d = 0; d < 3; ++d) {
+    if (d < ndim) {
+      orc_srl_maps(s.c.nghost, s.c.block_nx[d], smin, smax, rmin, rmax);
+      for (int q = 0; q < 3; ++q) { sminA[d][q] = smin[q]; smaxA[d][q] = smax[q]; rminA[d][q] = rmin[q]; rmaxA[d][q] = rmax[q]; }
+    } else {
+      for (int q = 0; q < 3; ++q) { sminA[d][q] = smaxA[d][q] = rminA[d][q] = rmaxA[d][q] = 0; }
+    }
+  }
+  // same-resolution fill: bc_fill_srl (src/mod_ghostcells_update.t:812-852)
+  for (int ib = 0; ib < G.nblocks; ++ib) {
+    for (int dk = (ndim > 2 ? -1 : 0); dk <= (ndim > 2 ? 1 : 0); ++dk)
+      for (int dj = (ndim > 1 ? -1 : 0); dj <= (ndim > 1 ? 1 : 0); ++dj)
+        for (int di = -1; di <= 1; ++di) {
+          if (di == 0 && dj == 0 && dk == 0) continue;
+          int nb = G.nbr[(size_t)ib * 27 + dir_index(di, dj, dk)];
+          if (nb < 0) continue;
+          int dd[3] = {di, dj, dk};
+          Box S, Rb;
+          for (int d = 0; d < 3; ++d) {
+            S.lo[d] = sminA[d][dd[d] + 1]; S.hi[d] = smaxA[d][dd[d] + 1];
+            Rb.lo[d] = rminA[d][-dd[d] + 1]; Rb.hi[d] = rmaxA[d][-dd[d] + 1];
+          }
+          double *src = &reg[G.bsize * ib], *dst = &reg[G.bsize * nb];
+          for (int iw = 0; iw < nw; ++iw)
+            for (int k = 0; k <= S.hi[2] - S.lo[2]; ++k)
+              for (int j = 0; j <= S.hi[1] - S.lo[1]; ++j)
+                for (int i = 0; i <= S.hi[0] - S.lo[0]; ++i)
+                  dst[g.idx(Rb.lo[0] + i, Rb.lo[1] + j, Rb.lo[2] + k) + g.cells * (size_t)iw] =
+                      src[g.idx(S.lo[0] + i, S.lo[1] + j, S.lo[2] + k) + g.cells * (size_t)iw];
+        }
+  }
+  // physical boundaries: fill_boundary_after_gc (src/mod_ghostcells_update.t:580-615)
+  // with bc_phys cont/symm/asymm (src/mod_boundary_conditions.t:12-265)
+  const int ng = s.c.nghost;
+  for (int ib = 0; ib < G.nblocks; ++ib) {
+    double *w = &reg[G.bsize * ib];
+    auto nbt = [&](int di, int dj, int dk) { return G.nbr[(size_t)ib * 27 + dir_index(di, dj, dk)] < 0; };
+    for (int idims = 0; idims < ndim; ++idims) {
+      int kmin[3] = {0, 0, 0}, kmax[3] = {0, 0, 0};
+      if (ndim >= 2) { kmin[1] = (idims < 1 && nbt(0, -1, 0)) ? 1 : 0; kmax[1] = (idims < 1 && nbt(0, 1, 0)) ? 1 : 0; }
+      if (ndim >= 3) { kmin[2] = (idims < 2 && nbt(0, 0, -1)) ? 1 : 0; kmax[2] = (idims < 2 && nbt(0, 0, 1)) ? 1 : 0; }
+      Box B;
+      for (int d = 0; d < 3; ++d) { B.lo[d] = kmin[d] * ng; B.hi[d] = g.n[d] - 1 - kmax[d] * ng; }
+      if (ndim < 3) { B.lo[2] = B.hi[2] = 0; }
+      if (ndim < 2) { B.lo[1] = B.hi[1] = 0; }
+      for (int iside = 0; iside < 2; ++iside) {
+        int dd[3] = {0, 0, 0};
+        dd[idims] = iside == 0 ? -1 : 1;
+        if (!nbt(dd[0], dd[1], dd[2])) continue;
+        int type = G.bc[2 * idims + iside];
+        Box O = B;
+        if (iside == 1) O.lo[idims] = B.hi[idims] + 1 - ng;
+        else O.hi[idims] = B.lo[idims] - 1 + ng;
+        const int o = g.off(idims);
+        for (int iw = 0; iw < nw; ++iw) {
+          double sgn = 1.0;
+          if (type == ORC_BC_ASYMM) sgn = -1.0;
+          forbox(O, [&](int i, int j, int k) {
+            int p = g.idx(i, j, k);
+            int c[3] = {i, j, k};
+            int q;
+            if (type == ORC_BC_CONT) {
+              int src = iside == 1 ? O.lo[idims] - 1 : O.hi[idims] + 1;
+              q = p + (src - c[idims]) * o;
+              w[p + g.cells * (size_t)iw] = w[q + g.cells * (size_t)iw];
+            } else {
+              // mirror: ghost ixOmin+m <- ixOmin-1-m (max side), ixOmax-m <- ixOmax+1+m (min side)
+              int src = iside == 1 ? 2 * O.lo[idims] - 1 - c[idims] : 2 * O.hi[idims] + 1 - c[idims];
+              q = p + (src - c[idims]) * o;
+              w[p + g.cells * (size_t)iw] = sgn * w[q + g.cells * (size_t)iw];
+            }
+          });
+        }
+      }
+    }
+  }
+}
+
+void orc_grid_getbc(orc_grid *g) { getbc_reg(*g, g->reg[0]); }
+
+int orc_grid_getdt(orc_grid *g, double *dt, double *cmax_global) {
+  const size_t bs = g->bsize;
+  double dtmin = bigdouble, cmx = 0.0;
+  int st = 0;
+  for (int ib = 0; ib < g->nblocks; ++ib) {
+    Arr<double> a = wrap_in(g->s.g, g->s.x.nw, &g->reg[0][bs * ib]);
+    double dtn;
+    st |= getdt_block(g->s, a, g->dx, &dtn, &cmx);
+    dtmin = std::min(dtmin, dtn);
+  }
+  *dt = dtmin;
+  *cmax_global = cmx;
+  return st;
+}
+
+int orc_grid_advect1(orc_grid *g, int ra, int rb, double qdt, double dtfactor, double cmax_global,
+                     int nthreads) {
+  const size_t bs = g->bsize;
+  int st = 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic) reduction(| : st)
+#endif
+  for (int ib = 0; ib < g->nblocks; ++ib) {
+    Arr<double> a = wrap_in(g->s.g, g->s.x.nw, &g->reg[ra][bs * ib]);
+    Arr<double> b = wrap_in(g->s.g, g->s.x.nw, &g->reg[rb][bs * ib]);
+    st |= finite_volume(g->s, a, b, qdt, dtfactor, g->dx, cmax_global);
+    std::memcpy(&g->reg[rb][bs * ib], b.d.data(), sizeof(double) * bs);
+  }
+  getbc_reg(*g, g->reg[rb]);
+  return st;
+}
+
+void orc_grid_copy_reg(orc_grid *g, int dst, int src) { g->reg[dst] = g->reg[src]; }
+
+void orc_grid_combine_reg(orc_grid *g, int dst, double a, int ra, double b, int rb) {
+  std::vector<double> &D = g->reg[dst];
+  const std::vector<double> &A = g->reg[ra], &B = g->reg[rb];
+  for (size_t p = 0; p < D.size(); ++p) D[p] = a * A[p] + b * B[p];
+}
+
+// advect threestep/ssprk3 (src/mod_advance.t:56-73, 249-267), coefficients
+// src/io/mod_input_output.t:941-964.
+int orc_grid_advance(orc_grid *g, double dt, double cmax_global, int nthreads) {
+  double b11, b22, b33, a21, a31;
+  if (g->s.c.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
+  else { b11 = 1.0; b22 = 1.0 / 4.0; b33 = 2.0 / 3.0; a21 = 3.0 / 4.0; a31 = 1.0 / 3.0; }
+  double a22 = 1.0 - a21, a33 = 1.0 - a31;
+  int st = 0;
+  orc_grid_copy_reg(g, 1, 0);
+  st |= orc_grid_advect1(g, 0, 1, b11 * dt, b11, cmax_global, nthreads);
+  orc_grid_combine_reg(g, 2, a21, 0, a22, 1);
+  st |= orc_grid_advect1(g, 1, 2, b22 * dt, b22, cmax_global, nthreads);
+  orc_grid_combine_reg(g, 0, a31, 0, a33, 2);
+  st |= orc_grid_advect1(g, 2, 0, b33 * dt, b33, cmax_global, nthreads);
+  return st;
+}
+
+void orc_grid_volume_average(const orc_grid *g, int power, double *mean) {
+  const Geo &geo = g->s.g;
+  const int nw = g->s.x.nw;
+  double dvol = 1.0;
+  for (int d = 0; d < g->s.c.ndim; ++d) dvol *= g->dx[d];
+  std::vector<double> wsum(nw + 1, 0.0);
+  Box O = geo.ixM();
+  for (int ib = 0; ib < g->nblocks; ++ib) {
+    const double *w = &g->reg[0][g->bsize * ib];
+    double vs = 0;
+    forbox(O, [&](int i, int j, int k) { vs += dvol; });
+    wsum[nw] += vs;
+    for (int iw = 0; iw < nw; ++iw) {
+      double acc = 0;
+      forbox(O, [&](int i, int j, int k) {
+        double v = w[geo.idx(i, j, k) + geo.cells * (size_t)iw];
+        acc += dvol * (power == 1 ? v : v * v);
+      });
+      wsum[iw] += acc;
+    }
+  }
+  for (int iw = 0; iw < nw; ++iw) mean[iw] = wsum[iw] / wsum[nw];
+}
+
+// ---------------------------------------------------------------- field loop
+// tests/mhd/field_loop_2.5D/mod_usr.t: A0=1e-3, R0=0.3, v0=(2,1), vector-potential init.
+static double fmodulo(double a, double p) { return a - std::floor(a / p) * p; }
+
+static void fl_bfield(const orc_grid *g, int ib, double t, std::vector<double> &bx, std::vector<double> &by) {
+  const Geo &geo = g->s.g;
+  const double A0 = 1.0e-3, R0 = 0.3, v[2] = {2.0, 1.0};
+  std::vector<double> Az(geo.cells, 0.0);
+  for (int j = 0; j < geo.n[1]; ++j)
+    for (int i = 0; i < geo.n[0]; ++i) {
+      double x1 = orc_grid_x(g, ib, 0, i) - v[0] * t - g->xmin[0];
+      x1 = g->xmin[0] + fmodulo(x1, g->xmax[0] - g->xmin[0]);
+      double x2 = orc_grid_x(g, ib, 1, j) - v[1] * t - g->xmin[1];
+      x2 = g->xmin[1] + fmodulo(x2, g->xmax[1] - g->xmin[1]);
+      double r2 = x1 * x1 + x2 * x2;
+      Az[geo.idx(i, j, 0)] = r2 < R0 * R0 ? A0 * (R0 - std::sqrt(r2)) : 0.0;
+    }
+  bx.assign(geo.cells, 0.0);
+  by.assign(geo.cells, 0.0);
+  Box O = geo.ixM();
+  const int oy = geo.off(1), ox = geo.off(0);
+  forbox(O, [&](int i, int j, int k) {
+    int p = geo.idx(i, j, k);
+    bx[p] = ((Az[p + oy] - Az[p - oy]) * half) / g->dx[1];
+    double gy = ((Az[p + ox] - Az[p - ox]) * half) / g->dx[0];
+    by[p] = -gy;
+  });
+}
+
+int orc_run_field_loop(const orc_cfg *cfg_in, double courantpar, double time_max, double dtsave, int nrow_max,
+                       double *rows, int nthreads) {
+  orc_cfg cfg = *cfg_in;
+  cfg.courantpar = courantpar;
+  orc_cfg_finalize(&cfg);
+  const int dom[3] = {128, 64, 1};
+  const double xmn[3] = {-1.0, -0.5, 0}, xmx[3] = {1.0, 0.5, 1};
+  const int bc[6] = {0, 0, 0, 0, 0, 0};
+  orc_grid *g = orc_grid_create(&cfg, dom, xmn, xmx, bc);
+  const Geo &geo = g->s.g;
+  const Ix &x = g->s.x;
+  const int nw = x.nw;
+  Box O = geo.ixM();
+  for (int ib = 0; ib < g->nblocks; ++ib) {
+    double *w = &g->reg[0][g->bsize * ib];
+    std::vector<double> bx, by;
+    fl_bfield(g, ib, 0.0, bx, by);
+    Arr<double> a(geo, nw);
+    forbox(O, [&](int i, int j, int k) {
+      a(i, j, k, x.rho) = 1.0;
+      a(i, j, k, x.mom[0]) = 2.0;
+      a(i, j, k, x.mom[1]) = 1.0;
+      a(i, j, k, x.e) = 1.0;
+      int p = geo.idx(i, j, k);
+      a(i, j, k, x.mag[0]) = bx[p];
+      a(i, j, k, x.mag[1]) = by[p];
+    });
+    to_conserved(g->s, O, a);
+    std::memcpy(w, a.d.data(), sizeof(double) * g->bsize);
+  }
+  orc_grid_getbc(g);
+  double t = 0.0, tsavelast = 0.0;
+  const double dtmin = 1.0e-10;
+  int it = 0, nrow = 0, st = 0;
+  const int ncol = 1 + 2 * (nw + 3);
+  double dvol = g->dx[0] * g->dx[1];
+  for (;;) {
+    // setdt (src/mod_dt.t:10-155)
+    double dt, cmax_global;
+    st |= orc_grid_getdt(g, &dt, &cmax_global);
+    if (dt < dtmin) st |= ORC_ST_DT_TOO_SMALL;
+    bool final_exit = false;
+    if (time_max - t <= dtmin) final_exit = true;
+    dt = std::min(dt, time_max - t);
+    {
+      double dtmax = std::ceil(t / dtsave) * dtsave;
+      double other = (t > 0) ? std::ceil(t / bigdouble) * bigdouble : 0.0;
+      dtmax = std::min(dtmax, other) - t;
+      if (dtmax > smalldouble) dt = std::min(dt, dtmax);
+      else dt = std::min(dt, dtsave);
+    }
+    // timetosave (src/amrvac.t:407-439) + usr_modify_output + printlog_regression_test
+    if (t >= tsavelast + dtsave - smalldouble) {
+      tsavelast = t;
+      if (nrow < nrow_max) {
+        double *row = rows + (size_t)nrow * ncol;
+        std::vector<double> s1(nw + 3, 0.0), s2(nw + 3, 0.0);
+        double vol = 0;
+        for (int ib = 0; ib < g->nblocks; ++ib) {
+          Arr<double> a = wrap_in(geo, nw, &g->reg[0][g->bsize * ib]);
+          std::vector<double> d2(geo.cells), d4(geo.cells), bx, by;
+          divb_central(g->s, a, O, g->dx, 1, d2);
+          divb_central(g->s, a, O, g->dx, 2, d4);
+          fl_bfield(g, ib, t, bx, by);
+          forbox(O, [&](int i, int j, int k) {
+            int p = geo.idx(i, j, k);
+            vol += dvol;
+            for (int iw = 0; iw < nw; ++iw) {
+              double v = a(i, j, k, iw);
+              s1[iw] += dvol * v;
+              s2[iw] += dvol * v * v;
+            }
+            double e1 = a(i, j, k, x.mag[0]) - bx[p], e2 = a(i, j, k, x.mag[1]) - by[p];
+            double ex[3] = {d2[p], d4[p], std::sqrt(e1 * e1 + e2 * e2)};
+            for (int q = 0; q < 3; ++q) {
+              s1[nw + q] += dvol * ex[q];
+              s2[nw + q] += dvol * ex[q] * ex[q];
+            }
+          });
+        }
+        row[0] = t;
+        for (int q = 0; q < nw + 3; ++q) {
+          row[1 + q] = s1[q] / vol;
+          row[1 + nw + 3 + q] = s2[q] / vol;
+        }
+      }
+      ++nrow;
+    }
+    if (t >= time_max || final_exit) break;
+    st |= orc_grid_advance(g, dt, cmax_global, nthreads);
+    if (st & ORC_ST_SMALL_VALUE) break;
+    ++it;
+    t = t + dt;
+  }
+  orc_grid_destroy(g);
+  if (st & ORC_ST_SMALL_VALUE) return -st;
+  return nrow;
+}
+
+// ---------------------------------------------------------------- op counts
+double orc_count_flops_stage(const orc_cfg *cfg, const double *wct, const double *wnew, double qdt,
+                             const double *dx, double cmax_global) {
+  State s = make_state(*cfg);
+  Arr<Counted> a(s.g, s.x.nw), b(s.g, s.x.nw);
+  for (size_t p = 0; p < a.d.size(); ++p) { a.d[p] = Counted(wct[p]); b.d[p] = Counted(wnew[p]); }
+  g_ops = 0;
+  finite_volume(s, a, b, qdt, 1.0, dx, cmax_global);
+  double cells = 1;
+  for (int d = 0; d < cfg->ndim; ++d) cells *= cfg->block_nx[d];
+  return double(g_ops) / cells;
+}
+
+double orc_count_flops_getdt(const orc_cfg *cfg, const double *w, const double *dx) {
+  State s = make_state(*cfg);
+  Arr<Counted> a(s.g, s.x.nw);
+  for (size_t p = 0; p < a.d.size(); ++p) a.d[p] = Counted(w[p]);
+  g_ops = 0;
+  double dtn, cm = 0;
+  getdt_block(s, a, dx, &dtn, &cm);
+  double cells = 1;
+  for (int d = 0; d < cfg->ndim; ++d) cells *= cfg->block_nx[d];
+  return double(g_ops) / cells;
+}
+
+}  // extern "C"

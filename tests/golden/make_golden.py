@@ -1,0 +1,33 @@
+"""Copy the reference's golden regression logs for the finite-volume path.
+
+Run once in a checkout that has the reference repository next to it:
+
+    python tests/golden/make_golden.py /path/to/amrvac
+
+The logs are the reference's own correct_output fixtures for the only
+uniform-grid (refine_max_level=1) regression tests on the HLL/HLLD path:
+tests/mhd/field_loop_2.5D/correct_output/fl_2d_3step_{hlld,hll}_cada.log.
+They are copied verbatim so the parity tests can run where the reference
+repository is absent.
+"""
+import os
+import shutil
+import sys
+
+LOGS = [
+    "tests/mhd/field_loop_2.5D/correct_output/fl_2d_3step_hlld_cada.log",
+    "tests/mhd/field_loop_2.5D/correct_output/fl_2d_3step_hll_cada.log",
+]
+
+
+def main(ref_root: str) -> None:
+    here = os.path.dirname(os.path.abspath(__file__))
+    for rel in LOGS:
+        src = os.path.join(ref_root, rel)
+        dst = os.path.join(here, os.path.basename(rel))
+        shutil.copyfile(src, dst)
+        print("wrote", dst)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
