@@ -1,0 +1,121 @@
+"""ctypes binding of libamrvac_gpu.so (C ABI in include/amrvac_gpu.h).
+
+The shared library is built in-tree by ``python -m amrvac_b200.build``.  There
+is no fallback: if the library is missing or cannot be loaded, importing the
+product API raises, and a context cannot be created without a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libamrvac_gpu.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "amrvac_gpu.h")
+
+MAX_NW = 16
+
+E_ARG, E_UNSUPPORTED, E_CUDA, E_STATE = -1, -2, -3, -4
+ST_SMALL_VALUE, ST_NAN, ST_DT_TOO_SMALL = 1, 2, 4
+
+FS = {"tvdlf": 1, "hll": 2, "hllc": 3, "hlld": 4}
+LIMITER = {"minmod": 1, "woodward": 2, "mcbeta": 3, "superbee": 4, "vanleer": 5,
+           "albada": 6, "koren": 7, "cada": 8, "cada3": 9}
+BOUNDSPEED = {"Einfeldt": 1, "cmaxmean": 2, "cmaxleftright": 3}
+DIVB = {"none": 0, "glm": 1, "linde": 4}
+COURANT = {"maxsum": 1, "summax": 2, "minimum": 3}
+BC = {"periodic": 0, "cont": 1, "symm": 2, "asymm": 3}
+TIME_STEPPER = {"onestep": 1, "twostep": 2, "threestep": 3}
+
+
+class AmrvacCfg(ctypes.Structure):
+    """Mirror of ``amrvac_cfg`` (field order and types must match the header)."""
+
+    _fields_ = [
+        ("ndim", ctypes.c_int), ("ndir", ctypes.c_int), ("physics", ctypes.c_int),
+        ("block_nx", ctypes.c_int * 3), ("nghostcells", ctypes.c_int),
+        ("gamma", ctypes.c_double),
+        ("flux_scheme", ctypes.c_int), ("limiter", ctypes.c_int),
+        ("typeboundspeed", ctypes.c_int), ("typedivbfix", ctypes.c_int),
+        ("mhd_glm_alpha", ctypes.c_double), ("mhd_glm_extended", ctypes.c_int),
+        ("divbdiff", ctypes.c_double), ("courantpar", ctypes.c_double),
+        ("type_courant", ctypes.c_int), ("cada3_radius", ctypes.c_double),
+        ("tvdlfeps", ctypes.c_double), ("fix_small_values", ctypes.c_int),
+        ("check_small_values", ctypes.c_int), ("small_values_method", ctypes.c_int),
+        ("small_density", ctypes.c_double), ("small_pressure", ctypes.c_double),
+        ("time_stepper", ctypes.c_int), ("ssprk_order", ctypes.c_int),
+        ("dtmin", ctypes.c_double),
+        ("typeboundary", (ctypes.c_int * MAX_NW) * 6),
+        ("zchunk", ctypes.c_int),
+    ]
+
+
+# (name, restype, argtypes) for every function declared in the header.
+_P = ctypes.POINTER
+_d, _i, _u32, _i64, _vp = ctypes.c_double, ctypes.c_int, ctypes.c_uint32, ctypes.c_int64, ctypes.c_void_p
+_dp, _ip = _P(ctypes.c_double), _P(ctypes.c_int)
+_cfgp = _P(AmrvacCfg)
+SIGNATURES = [
+    ("amrvac_gpu_default_cfg", None, [_cfgp]),
+    ("amrvac_gpu_nw", _i, [_cfgp]),
+    ("amrvac_gpu_create", _i, [_cfgp, _P(_vp)]),
+    ("amrvac_gpu_destroy", _i, [_vp]),
+    ("amrvac_gpu_set_blocks", _i, [_vp, _i, _dp, _ip]),
+    ("amrvac_gpu_set_uniform_grid", _i, [_vp, _ip, _dp, _dp]),
+    ("amrvac_gpu_nblocks", _i, [_vp]),
+    ("amrvac_gpu_upload", _i, [_vp, _i, _i, _i, _dp]),
+    ("amrvac_gpu_download", _i, [_vp, _i, _i, _i, _dp]),
+    ("amrvac_gpu_getdt", _i, [_vp, _i, _dp, _dp]),
+    ("amrvac_gpu_advect1", _i, [_vp, _i, _i, _i, _d, _d, _d, _d]),
+    ("amrvac_gpu_set_cmax_global", _i, [_vp, _d]),
+    ("amrvac_gpu_set_time", _i, [_vp, _d, _d, _d]),
+    ("amrvac_gpu_step", _i, [_vp]),
+    ("amrvac_gpu_run", _i, [_vp, _i]),
+    ("amrvac_gpu_get_time", _i, [_vp, _dp, _dp, _dp]),
+    ("amrvac_gpu_run_timed", _i, [_vp, _i, _dp, _dp, _dp]),
+    ("amrvac_gpu_fp64_peak", _i, [_dp]),
+    ("amrvac_gpu_status", _i, [_vp, _P(_u32)]),
+    ("amrvac_gpu_clear_status", _i, [_vp]),
+    ("amrvac_gpu_synchronize", _i, [_vp]),
+    ("amrvac_gpu_stream", _i, [_vp, _P(_vp)]),
+    ("amrvac_gpu_register_ptr", _i, [_vp, _i, _P(_dp)]),
+    ("amrvac_gpu_launch_count", _i64, [_vp]),
+    ("amrvac_gpu_last_error", ctypes.c_char_p, []),
+    ("amrvac_gpu_get_flux_points", _i, [_vp, _i, _dp, _dp, _i, _d, _dp]),
+    ("amrvac_gpu_get_cbounds_points", _i, [_vp, _i, _dp, _dp, _dp, _dp, _i, _dp, _dp]),
+    ("amrvac_gpu_riemann_points", _i, [_vp, _i, _dp, _dp, _i, _d, _dp]),
+    ("amrvac_gpu_srl_maps", _i, [_i, _i, _ip, _ip, _ip, _ip]),
+]
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the in-tree library; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} not found: build it with `python -m amrvac_b200.build` "
+                "(nvcc, sm_100a). There is no CPU fallback.")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class AmrvacError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        msg = load().amrvac_gpu_last_error().decode(errors="replace")
+        super().__init__(f"{where} failed with code {code}: {msg}")
+        self.code = code
+
+
+def check(code: int, where: str) -> int:
+    """Raise on configuration errors (negative codes); return status bits."""
+    if code < 0:
+        raise AmrvacError(code, where)
+    return code

@@ -1,0 +1,197 @@
+// Pool transfer kernels (host Fortran block arrays <-> device pool), ghost
+// fill on download, and the device-side time-step bookkeeping of setdt.
+#include <cuda_runtime.h>
+
+#include "aux.cuh"
+#include "stage.cuh"
+
+namespace amrvac {
+
+// ---------------------------------------------------------------- upload
+// Fortran w(ixG^S,1:nw) blocks (ghosts included) -> pool interior.
+__global__ void unpack_kernel(const double *__restrict__ src, double *__restrict__ pool, int first,
+                              int n, int nw, int ndim, int ng) {
+  const int nx = BN, ny = ndim >= 2 ? BN : 1, nz = ndim >= 3 ? BN : 1;
+  const int gx = BN + 2 * ng, gy = ndim >= 2 ? BN + 2 * ng : 1, gz = ndim >= 3 ? BN + 2 * ng : 1;
+  const size_t per_block = (size_t)nx * ny * nz;
+  const size_t total = per_block * nw * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    size_t r = e;
+    const int i = r % nx; r /= nx;
+    const int j = r % ny; r /= ny;
+    const int k = r % nz; r /= nz;
+    const int v = r % nw; r /= nw;
+    const int b = (int)r;
+    const int oi = i + ng, oj = ndim >= 2 ? j + ng : 0, ok = ndim >= 3 ? k + ng : 0;
+    const size_t s = ((((size_t)b * nw + v) * gz + ok) * gy + oj) * gx + oi;
+    pool[(size_t)(first + b) * nw * per_block + e - (size_t)b * nw * per_block] = src[s];
+  }
+}
+
+// ---------------------------------------------------------------- download
+// Pool -> Fortran blocks with ghost cells filled like getbc: same-resolution
+// copies through the ixS_srl_/ixR_srl_ maps (src/mod_ghostcells_update.t:
+// 150-162, 812-852) and physical cont/symm/asymm boundaries
+// (src/mod_boundary_conditions.t:12-265, applied per dimension).
+__global__ void pack_kernel(const double *__restrict__ pool, double *__restrict__ dst, int first, int n,
+                            int nw, int ndim, int ng, const int *__restrict__ nbr, SrlMaps maps,
+                            BcSpec bc) {
+  const int gx = BN + 2 * ng, gy = ndim >= 2 ? BN + 2 * ng : 1, gz = ndim >= 3 ? BN + 2 * ng : 1;
+  const size_t per_block_g = (size_t)gx * gy * gz;
+  const size_t per_block = (size_t)BN * (ndim >= 2 ? BN : 1) * (ndim >= 3 ? BN : 1);
+  const size_t total = per_block_g * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    size_t r = e;
+    int g[3];
+    g[0] = r % gx; r /= gx;
+    g[1] = r % gy; r /= gy;
+    g[2] = r % gz; r /= gz;
+    const int lb = (int)r;
+    const int b = first + lb;
+    int dir[3] = {0, 0, 0};
+    uint32_t flip = 0;
+    for (int d = 0; d < ndim; ++d) {
+      int q = -1;
+      for (int s = 0; s < 3; ++s)
+        if (g[d] >= maps.rmin[d][s] && g[d] <= maps.rmax[d][s]) q = s - 1;
+      if (q == 0) continue;
+      int fd[3] = {0, 0, 0};
+      fd[d] = q;
+      const int nf = nbr[b * 27 + (fd[0] + 1) + 3 * (fd[1] + 1) + 9 * (fd[2] + 1)];
+      if (nf < 0) {
+        const int side = q < 0 ? 0 : 1;
+        if (bc.kind[2 * d + side] == 1) {  // cont
+          g[d] = q < 0 ? ng : ng + BN - 1;
+        } else {  // symm / asymm mirror
+          g[d] = q < 0 ? 2 * ng - 1 - g[d] : 2 * (ng + BN) - 1 - g[d];
+          flip ^= bc.flip[2 * d + side];
+        }
+      } else {
+        dir[d] = q;
+      }
+    }
+    int src = b;
+    if (dir[0] | dir[1] | dir[2]) {
+      src = nbr[b * 27 + (dir[0] + 1) + 3 * (dir[1] + 1) + 9 * (dir[2] + 1)];
+      for (int d = 0; d < ndim; ++d) {
+        if (!dir[d]) continue;
+        // receiver region ixR_srl_(dir) <- sender region ixS_srl_(-dir)
+        g[d] = maps.smin[d][-dir[d] + 1] + (g[d] - maps.rmin[d][dir[d] + 1]);
+      }
+    }
+    const int i = g[0] - ng, j = ndim >= 2 ? g[1] - ng : 0, k = ndim >= 3 ? g[2] - ng : 0;
+    const size_t sbase = (size_t)src * nw * per_block + ((size_t)k * (ndim >= 2 ? BN : 1) + j) * BN + i;
+    const size_t gcell = e - (size_t)lb * per_block_g;
+    for (int v = 0; v < nw; ++v) {
+      double x = pool[sbase + (size_t)v * per_block];
+      if ((flip >> v) & 1u) x = -x;
+      dst[((size_t)lb * nw + v) * per_block_g + gcell] = x;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- setdt tail
+// After getdt_kernel: dt = courantpar / max (src/mod_dt.t:233-235), the
+// dtmin check (55-60), final_dt_reduction (69-79) and the output-interval cap
+// (88-99).  scal: [0]=dt [1]=cmax_global [2]=global_time [3]=time_max
+// [4]=dtsave [5]=dtmin [6]=courantpar [7]=final_exit flag.
+__global__ void setdt_finalize_kernel(unsigned long long *red, double *scal, uint32_t *status) {
+  const double smalldouble = 1.0e-12, bigdouble = 1.0e99;
+  const double x = __longlong_as_double((long long)red[0]);
+  const double cm = __longlong_as_double((long long)red[1]);
+  red[0] = 0ull;
+  red[1] = 0ull;
+  double dt = bigdouble;
+  if (x > smalldouble) dt = fmin(dt, scal[6] / x);
+  if (dt < scal[5]) atomicOr(status, ST_DT_TOO_SMALL);
+  const double t = scal[2], tmax = scal[3], dtsave = scal[4];
+  if (tmax - t <= scal[5]) scal[7] = 1.0;
+  dt = fmin(dt, tmax - t);
+  if (dtsave > 0.0) {
+    double dtmax = ceil(t / dtsave) * dtsave;
+    const double other = t > 0.0 ? ceil(t / bigdouble) * bigdouble : 0.0;
+    dtmax = fmin(dtmax, other) - t;
+    if (dtmax > smalldouble) dt = fmin(dt, dtmax);
+    else dt = fmin(dt, dtsave);
+  }
+  scal[0] = dt;
+  scal[1] = cm;
+}
+
+__global__ void advance_time_kernel(double *scal) { scal[2] = scal[2] + scal[0]; }
+
+__global__ void restore_blocks_kernel(const double *__restrict__ wct, double *__restrict__ wnew,
+                                      const uint32_t *__restrict__ block_status, size_t per_block) {
+  const int b = blockIdx.x;
+  if (!(block_status[b] & ST_SMALL_VALUE)) return;
+  for (size_t e = threadIdx.x; e < per_block; e += blockDim.x)
+    wnew[(size_t)b * per_block + e] = wct[(size_t)b * per_block + e];
+}
+
+// Independent FMA chains in registers: measures the FP64 pipe throughput.
+__global__ void fp64_fma_kernel(double *out, int iters, double a, double b) {
+  double x0 = threadIdx.x * 1e-9, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5,
+         x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+    x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+    x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+  }
+  const double s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+  if (s == 1.2345678) out[0] = s;  // keeps the chains live
+}
+
+cudaError_t measure_fp64_peak(double *tflops) {
+  int dev, nsm;
+  cudaError_t e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  double *out;
+  if ((e = cudaMalloc(&out, sizeof(double))) != cudaSuccess) return e;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int iters = 1 << 14, threads = 512, blocks = nsm * 4;
+  fp64_fma_kernel<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+  cudaEventRecord(a);
+  const int reps = 5;
+  for (int r = 0; r < reps; ++r) fp64_fma_kernel<<<blocks, threads>>>(out, iters, 0.999999, 1e-7);
+  cudaEventRecord(b);
+  e = cudaEventSynchronize(b);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  if (e != cudaSuccess) return e;
+  const double flops = 2.0 * 8.0 * iters * (double)threads * blocks * reps;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(const double *src, double *pool, int first, int n, int nw, int ndim, int ng,
+                          cudaStream_t s) {
+  unpack_kernel<<<592, 256, 0, s>>>(src, pool, first, n, nw, ndim, ng);
+  return cudaGetLastError();
+}
+cudaError_t launch_pack(const double *pool, double *dst, int first, int n, int nw, int ndim, int ng,
+                        const int *nbr, const SrlMaps &maps, const BcSpec &bc, cudaStream_t s) {
+  pack_kernel<<<592, 256, 0, s>>>(pool, dst, first, n, nw, ndim, ng, nbr, maps, bc);
+  return cudaGetLastError();
+}
+cudaError_t launch_setdt_finalize(unsigned long long *red, double *scal, uint32_t *status, cudaStream_t s) {
+  setdt_finalize_kernel<<<1, 1, 0, s>>>(red, scal, status);
+  return cudaGetLastError();
+}
+cudaError_t launch_advance_time(double *scal, cudaStream_t s) {
+  advance_time_kernel<<<1, 1, 0, s>>>(scal);
+  return cudaGetLastError();
+}
+cudaError_t launch_restore_blocks(const double *wct, double *wnew, const uint32_t *block_status, int nblocks,
+                                  size_t per_block, cudaStream_t s) {
+  restore_blocks_kernel<<<nblocks, 256, 0, s>>>(wct, wnew, block_status, per_block);
+  return cudaGetLastError();
+}
+
+}  // namespace amrvac

@@ -1,0 +1,764 @@
+// C ABI of the B200 finite-volume block update (declared in include/amrvac_gpu.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/amrvac_gpu.h"
+#include "aux.cuh"
+#include "kernels.cuh"
+
+using namespace amrvac;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+  g_err = std::string(where) + ": " + cudaGetErrorString(e);
+  return AMRVAC_E_CUDA;
+}
+
+#define CK(call)                                   \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+int nw_of(const amrvac_cfg *c) {
+  if (c->physics == 1) {
+    const bool glm = c->typedivbfix == AMRVAC_DIVB_GLM && c->ndim > 1;
+    return 2 * c->ndir + 2 + (glm ? 1 : 0);
+  }
+  return c->ndir + 2;
+}
+
+// init_bc same-resolution maps (src/mod_ghostcells_update.t:150-162), 0-based.
+void srl_maps_1d(int ng, int nx, int *smin, int *smax, int *rmin, int *rmax) {
+  const int ixMmin = ng + 1, ixMmax = ng + nx, ixGmax = nx + 2 * ng;
+  const int s_min[3] = {ixMmin, ixMmin, ixMmax + 1 - ng};
+  const int s_max[3] = {ixMmin - 1 + ng, ixMmax, ixMmax};
+  const int r_min[3] = {1, ixMmin, ixMmax + 1};
+  const int r_max[3] = {ng, ixMmax, ixGmax};
+  for (int q = 0; q < 3; ++q) {
+    smin[q] = s_min[q] - 1; smax[q] = s_max[q] - 1;
+    rmin[q] = r_min[q] - 1; rmax[q] = r_max[q] - 1;
+  }
+}
+
+}  // namespace
+
+struct amrvac_ctx {
+  amrvac_cfg cfg;
+  int nw = 0;
+  PhysParams P;
+  KernelSet ks;
+  BcSpec bc;
+  SrlMaps maps;
+  cudaStream_t stream = nullptr;
+  int nblocks = 0;
+  size_t per_block = 0;  // doubles per block per variable
+  double *pool[3] = {nullptr, nullptr, nullptr};
+  int *d_nbr = nullptr;
+  double *d_dx = nullptr;
+  double *d_scal = nullptr;              // see setdt_finalize_kernel
+  unsigned long long *d_red = nullptr;   // getdt reduction accumulators
+  uint32_t *d_status = nullptr;
+  uint32_t *d_block_status = nullptr;
+  double *d_stage = nullptr;             // upload/download staging
+  size_t stage_doubles = 0;
+  cudaGraphExec_t graph = nullptr;
+  int64_t launches = 0;
+  int64_t graph_nodes = 0;
+  int zchunk = 16;
+};
+
+namespace {
+
+int check_ctx(amrvac_ctx *c, bool need_blocks) {
+  if (!c) return fail(AMRVAC_E_ARG, "null context");
+  if (need_blocks && c->nblocks == 0) return fail(AMRVAC_E_STATE, "no blocks set (amrvac_gpu_set_blocks)");
+  return 0;
+}
+
+StageArgs stage_args(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a, double b,
+                     double dtfactor) {
+  StageArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.uin = c->pool[reg_ct];
+  A.ubase = c->pool[reg_base];
+  A.uout = c->pool[reg_new];
+  A.a_base = a;
+  A.b_in = b;
+  A.dtfactor = dtfactor;
+  A.dt_dev = c->d_scal + 0;
+  A.cmax_dev = c->d_scal + 1;
+  A.nbr = c->d_nbr;
+  A.dxb = c->d_dx;
+  A.nblocks = c->nblocks;
+  A.zchunk = c->zchunk;
+  for (int s = 0; s < 6; ++s) {
+    A.bc_kind[s] = c->bc.kind[s];
+    A.bc_flip[s] = c->bc.flip[s];
+  }
+  A.status = c->d_status;
+  A.block_status = c->d_block_status;
+  A.P = c->P;
+  return A;
+}
+
+int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a, double b, double dtfactor) {
+  StageArgs A = stage_args(c, reg_ct, reg_new, reg_base, a, b, dtfactor);
+  const int nctas = c->cfg.ndim == 3 ? c->nblocks * (16 / c->zchunk) : c->nblocks;
+  if (c->P.fix_small_values && c->P.small_values_method == 0)
+    CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * c->nblocks, c->stream));
+  CK(c->ks.stage(A, nctas, c->stream));
+  ++c->launches;
+  if (c->P.fix_small_values && c->P.small_values_method == 0) {
+    CK(launch_restore_blocks(c->pool[reg_ct], c->pool[reg_new], c->d_block_status, c->nblocks,
+                             c->per_block * c->nw, c->stream));
+    ++c->launches;
+  }
+  return 0;
+}
+
+int launch_getdt(amrvac_ctx *c, int reg) {
+  GetdtArgs G;
+  G.u = c->pool[reg];
+  G.dxb = c->d_dx;
+  G.nblocks = c->nblocks;
+  G.type_courant = c->cfg.type_courant;
+  G.red = c->d_red;
+  G.P = c->P;
+  CK(c->ks.getdt(G, c->stream));
+  ++c->launches;
+  return 0;
+}
+
+// The configured RK stages (src/mod_advance.t:56-567) on registers 0..2.
+int launch_rk(amrvac_ctx *c) {
+  const amrvac_cfg &k = c->cfg;
+  int r = 0;
+  if (k.time_stepper == AMRVAC_TS_ONESTEP) {
+    CK(cudaMemcpyAsync(c->pool[1], c->pool[0], sizeof(double) * c->per_block * c->nw * c->nblocks,
+                       cudaMemcpyDeviceToDevice, c->stream));
+    r = launch_stage(c, 1, 0, 0, 0.0, 1.0, 1.0);
+  } else if (k.time_stepper == AMRVAC_TS_TWOSTEP) {
+    if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0))) return r;
+    r = launch_stage(c, 1, 0, 0, 0.5, 0.5, 0.5);
+  } else {
+    double b11, b22, b33, a21, a31;
+    if (k.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
+    else { b11 = 1.0; b22 = 1.0 / 4.0; b33 = 2.0 / 3.0; a21 = 3.0 / 4.0; a31 = 1.0 / 3.0; }
+    const double a22 = 1.0 - a21, a33 = 1.0 - a31;
+    if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, b11))) return r;
+    if ((r = launch_stage(c, 1, 2, 0, a21, a22, b22))) return r;
+    r = launch_stage(c, 2, 0, 0, a31, a33, b33);
+  }
+  return r;
+}
+
+int launch_step(amrvac_ctx *c) {
+  int r;
+  if ((r = launch_getdt(c, 0))) return r;
+  CK(launch_setdt_finalize(c->d_red, c->d_scal, c->d_status, c->stream));
+  ++c->launches;
+  if ((r = launch_rk(c))) return r;
+  CK(launch_advance_time(c->d_scal, c->stream));
+  ++c->launches;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *amrvac_gpu_last_error(void) { return g_err.c_str(); }
+
+void amrvac_gpu_default_cfg(amrvac_cfg *c) {
+  std::memset(c, 0, sizeof(*c));
+  c->ndim = 2;
+  c->ndir = 2;
+  c->physics = 0;
+  c->block_nx[0] = c->block_nx[1] = c->block_nx[2] = 16;
+  c->nghostcells = 2;
+  c->gamma = 5.0 / 3.0;
+  c->flux_scheme = AMRVAC_FS_TVDLF;
+  c->limiter = AMRVAC_LIM_MINMOD;
+  c->typeboundspeed = AMRVAC_BS_EINFELDT;
+  c->typedivbfix = AMRVAC_DIVB_LINDE;
+  c->mhd_glm_alpha = 0.5;
+  c->mhd_glm_extended = 1;
+  c->divbdiff = 0.8;
+  c->courantpar = 0.8;
+  c->type_courant = AMRVAC_COURANT_MAXSUM;
+  c->cada3_radius = 0.1;
+  c->tvdlfeps = 1.0;
+  c->fix_small_values = 0;
+  c->check_small_values = 1;
+  c->small_values_method = 0;
+  c->time_stepper = AMRVAC_TS_THREESTEP;
+  c->ssprk_order = 3;
+  c->dtmin = 1.0e-10;
+  c->zchunk = 0;
+}
+
+int amrvac_gpu_nw(const amrvac_cfg *cfg) { return cfg ? nw_of(cfg) : AMRVAC_E_ARG; }
+
+int amrvac_gpu_srl_maps(int nghost, int block_nx, int *s_min, int *s_max, int *r_min, int *r_max) {
+  if (!s_min || !s_max || !r_min || !r_max || nghost < 1 || block_nx < nghost) return AMRVAC_E_ARG;
+  srl_maps_1d(nghost, block_nx, s_min, s_max, r_min, r_max);
+  return 0;
+}
+
+int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
+  if (!cfg || !out) return fail(AMRVAC_E_ARG, "null argument");
+  *out = nullptr;
+  const amrvac_cfg &k = *cfg;
+  if (k.ndim < 2 || k.ndim > 3) return fail(AMRVAC_E_UNSUPPORTED, "ndim must be 2 or 3");
+  if (k.ndir < k.ndim || k.ndir > 3) return fail(AMRVAC_E_UNSUPPORTED, "ndir must be in [ndim, 3]");
+  for (int d = 0; d < k.ndim; ++d)
+    if (k.block_nx[d] != 16) return fail(AMRVAC_E_UNSUPPORTED, "block_nx must be 16");
+  if (k.nghostcells < 2) return fail(AMRVAC_E_UNSUPPORTED, "nghostcells must be >= 2");
+  if (k.physics != 0 && k.physics != 1) return fail(AMRVAC_E_ARG, "physics must be 0 (hd) or 1 (mhd)");
+  if (k.limiter < 1 || k.limiter > 9) return fail(AMRVAC_E_UNSUPPORTED, "limiter not supported");
+  if (k.typeboundspeed < 1 || k.typeboundspeed > 3) return fail(AMRVAC_E_ARG, "bad typeboundspeed");
+  if (k.type_courant < 1 || k.type_courant > 3) return fail(AMRVAC_E_ARG, "bad type_courant");
+  if (k.time_stepper < 1 || k.time_stepper > 3) return fail(AMRVAC_E_UNSUPPORTED, "time_stepper not supported");
+  if (k.physics == 0 && k.ndir != k.ndim) return fail(AMRVAC_E_UNSUPPORTED, "hd requires ndir == ndim");
+  if (k.physics == 1) {
+    if (k.flux_scheme == AMRVAC_FS_HLLC) return fail(AMRVAC_E_UNSUPPORTED, "mhd hllc not supported");
+    if (k.typedivbfix != AMRVAC_DIVB_NONE && k.typedivbfix != AMRVAC_DIVB_GLM && k.typedivbfix != AMRVAC_DIVB_LINDE)
+      return fail(AMRVAC_E_UNSUPPORTED, "typedivbfix must be none, glm or linde");
+    if (k.ndim == 3 && k.typedivbfix == AMRVAC_DIVB_LINDE)
+      return fail(AMRVAC_E_UNSUPPORTED, "3-D Linde divB source not supported (use glm)");
+  } else if (k.flux_scheme == AMRVAC_FS_HLLD) {
+    return fail(AMRVAC_E_UNSUPPORTED, "hlld needs mhd");
+  }
+  const int nw = nw_of(cfg);
+  if (nw > AMRVAC_MAX_NW) return fail(AMRVAC_E_UNSUPPORTED, "too many variables");
+  amrvac_ctx *c = new amrvac_ctx();
+  c->cfg = k;
+  c->nw = nw;
+  KernelKey key{k.physics == 1, k.ndim, k.ndir, k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM,
+                k.flux_scheme};
+  bool found = lookup_hd(key, &c->ks) || lookup_mhd2(key, &c->ks) || lookup_mhd3(key, &c->ks);
+  if (!found) {
+    delete c;
+    return fail(AMRVAC_E_UNSUPPORTED, "no kernel for this physics/ndim/ndir/solver combination");
+  }
+  cudaError_t e0;
+  PhysParams &P = c->P;
+  P.gamma = k.gamma;
+  P.gamma_1 = k.gamma - 1.0;
+  P.inv_gamma_1 = 1.0 / (k.gamma - 1.0);
+  P.small_density = k.small_density;
+  P.small_pressure = k.small_pressure;
+  P.small_e = k.physics == 1 ? k.small_pressure * P.inv_gamma_1 : k.small_pressure / (k.gamma - 1.0);
+  P.tvdlfeps = k.tvdlfeps;
+  P.cada3_radius = k.cada3_radius;
+  P.glm_alpha = k.mhd_glm_alpha;
+  P.divbdiff = k.divbdiff;
+  P.courantpar = k.courantpar;
+  P.limiter = k.limiter;
+  P.boundspeed = k.typeboundspeed;
+  P.divb = k.physics == 1 ? k.typedivbfix : 0;
+  P.glm_extended = k.mhd_glm_extended;
+  P.fix_small_values = k.fix_small_values;
+  P.check_small_values = k.check_small_values;
+  P.small_values_method = k.small_values_method;
+  // physical boundaries: per side all variables periodic, all cont, or all symm/asymm
+  for (int s = 0; s < 6; ++s) {
+    c->bc.kind[s] = 0;
+    c->bc.flip[s] = 0;
+    if (s >= 2 * k.ndim) continue;
+    int per = 0, cont = 0, mir = 0;
+    for (int v = 0; v < nw; ++v) {
+      const int t = k.typeboundary[s][v];
+      if (t == AMRVAC_BC_PERIODIC) ++per;
+      else if (t == AMRVAC_BC_CONT) ++cont;
+      else if (t == AMRVAC_BC_SYMM || t == AMRVAC_BC_ASYMM) {
+        ++mir;
+        if (t == AMRVAC_BC_ASYMM) c->bc.flip[s] |= 1u << v;
+      } else {
+        delete c;
+        return fail(AMRVAC_E_UNSUPPORTED, "typeboundary must be periodic, cont, symm or asymm");
+      }
+    }
+    if (per == nw) c->bc.kind[s] = BCK_PERIODIC;
+    else if (cont == nw) c->bc.kind[s] = BCK_CONT;
+    else if (mir == nw) c->bc.kind[s] = BCK_MIRROR;
+    else {
+      delete c;
+      return fail(AMRVAC_E_UNSUPPORTED, "mixed boundary kinds on one side");
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    if (d < k.ndim) {
+      srl_maps_1d(k.nghostcells, 16, c->maps.smin[d], c->maps.smax[d], c->maps.rmin[d], c->maps.rmax[d]);
+    } else {
+      for (int q = 0; q < 3; ++q) c->maps.smin[d][q] = c->maps.smax[d][q] = c->maps.rmin[d][q] = c->maps.rmax[d][q] = 0;
+    }
+  }
+  if ((e0 = c->ks.prepare()) != cudaSuccess) {
+    delete c;
+    return cuda_fail(e0, "cudaFuncSetAttribute");
+  }
+  c->zchunk = (k.zchunk == 8 || k.zchunk == 4 || k.zchunk == 16) ? k.zchunk : 16;
+  c->per_block = 1;
+  for (int d = 0; d < k.ndim; ++d) c->per_block *= 16;
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    delete c;
+    return cuda_fail(e, "cudaStreamCreate");
+  }
+  // scalars: dt, cmax_global, time, time_max, dtsave, dtmin, courantpar, final flag
+  const double sc[8] = {0.0, 0.0, 0.0, 1.0e99, 0.0, k.dtmin, k.courantpar, 0.0};
+  if ((e = cudaMalloc(&c->d_scal, sizeof(sc))) != cudaSuccess ||
+      (e = cudaMemcpy(c->d_scal, sc, sizeof(sc), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMalloc(&c->d_red, 2 * sizeof(unsigned long long))) != cudaSuccess ||
+      (e = cudaMemset(c->d_red, 0, 2 * sizeof(unsigned long long))) != cudaSuccess ||
+      (e = cudaMalloc(&c->d_status, sizeof(uint32_t))) != cudaSuccess ||
+      (e = cudaMemset(c->d_status, 0, sizeof(uint32_t))) != cudaSuccess) {
+    amrvac_gpu_destroy(c);
+    return cuda_fail(e, "context allocation");
+  }
+  *out = c;
+  return 0;
+}
+
+int amrvac_gpu_destroy(amrvac_ctx *c) {
+  if (!c) return AMRVAC_E_ARG;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  for (int r = 0; r < 3; ++r) cudaFree(c->pool[r]);
+  cudaFree(c->d_nbr);
+  cudaFree(c->d_dx);
+  cudaFree(c->d_scal);
+  cudaFree(c->d_red);
+  cudaFree(c->d_status);
+  cudaFree(c->d_block_status);
+  cudaFree(c->d_stage);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const int *neighbor) {
+  if (int r = check_ctx(c, false)) return r;
+  if (nblocks <= 0 || !dx || !neighbor) return fail(AMRVAC_E_ARG, "bad block description");
+  const int nd = c->cfg.ndim;
+  int ndir3 = 1;
+  for (int d = 0; d < nd; ++d) ndir3 *= 3;
+  std::vector<int> nbr((size_t)nblocks * 27, -1);
+  std::vector<double> dxb((size_t)nblocks * 3, 1.0);
+  for (int b = 0; b < nblocks; ++b) {
+    for (int q = 0; q < ndir3; ++q) {
+      const int di = q % 3 - 1, dj = nd >= 2 ? (q / 3) % 3 - 1 : 0, dk = nd >= 3 ? q / 9 - 1 : 0;
+      const int v = neighbor[(size_t)b * ndir3 + q];
+      if (v >= nblocks || v < -1) return fail(AMRVAC_E_ARG, "neighbor id out of range");
+      nbr[(size_t)b * 27 + (di + 1) + 3 * (dj + 1) + 9 * (dk + 1)] = v;
+    }
+    nbr[(size_t)b * 27 + 13] = b;
+    for (int d = 0; d < nd; ++d) {
+      const double h = dx[(size_t)b * nd + d];
+      if (!(h > 0.0)) return fail(AMRVAC_E_ARG, "dx must be positive");
+      dxb[(size_t)b * 3 + d] = h;
+    }
+  }
+  // a physical side needs a boundary kind, a sibling side must not be marked
+  for (int b = 0; b < nblocks; ++b)
+    for (int d = 0; d < nd; ++d)
+      for (int s = 0; s < 2; ++s) {
+        int o[3] = {0, 0, 0};
+        o[d] = s ? 1 : -1;
+        const int v = nbr[(size_t)b * 27 + (o[0] + 1) + 3 * (o[1] + 1) + 9 * (o[2] + 1)];
+        if (v < 0 && c->bc.kind[2 * d + s] == BCK_PERIODIC)
+          return fail(AMRVAC_E_ARG, "physical boundary on a side declared periodic");
+      }
+  cudaStreamSynchronize(c->stream);
+  for (int r = 0; r < 3; ++r) { cudaFree(c->pool[r]); c->pool[r] = nullptr; }
+  cudaFree(c->d_nbr); cudaFree(c->d_dx); cudaFree(c->d_block_status);
+  c->d_nbr = nullptr; c->d_dx = nullptr; c->d_block_status = nullptr;
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+  c->nblocks = nblocks;
+  const size_t bytes = sizeof(double) * c->per_block * c->nw * nblocks;
+  for (int r = 0; r < 3; ++r) {
+    CK(cudaMalloc(&c->pool[r], bytes));
+    CK(cudaMemsetAsync(c->pool[r], 0, bytes, c->stream));
+  }
+  CK(cudaMalloc(&c->d_nbr, sizeof(int) * nbr.size()));
+  CK(cudaMalloc(&c->d_dx, sizeof(double) * dxb.size()));
+  CK(cudaMalloc(&c->d_block_status, sizeof(uint32_t) * nblocks));
+  CK(cudaMemcpyAsync(c->d_nbr, nbr.data(), sizeof(int) * nbr.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_dx, dxb.data(), sizeof(double) * dxb.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * nblocks, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int amrvac_gpu_set_uniform_grid(amrvac_ctx *c, const int *domain_nx, const double *xprobmin,
+                                const double *xprobmax) {
+  if (int r = check_ctx(c, false)) return r;
+  if (!domain_nx || !xprobmin || !xprobmax) return fail(AMRVAC_E_ARG, "null argument");
+  const int nd = c->cfg.ndim;
+  int nb[3] = {1, 1, 1};
+  double h[3] = {1, 1, 1};
+  int total = 1;
+  for (int d = 0; d < nd; ++d) {
+    if (domain_nx[d] <= 0 || domain_nx[d] % 16) return fail(AMRVAC_E_ARG, "domain_nx must be a multiple of block_nx");
+    nb[d] = domain_nx[d] / 16;
+    h[d] = (xprobmax[d] - xprobmin[d]) / double(domain_nx[d]);
+    total *= nb[d];
+  }
+  int ndir3 = 1;
+  for (int d = 0; d < nd; ++d) ndir3 *= 3;
+  std::vector<int> nbr((size_t)total * ndir3);
+  std::vector<double> dx((size_t)total * nd);
+  for (int b = 0; b < total; ++b) {
+    const int ig[3] = {b % nb[0], (b / nb[0]) % nb[1], b / (nb[0] * nb[1])};
+    for (int q = 0; q < ndir3; ++q) {
+      const int o[3] = {q % 3 - 1, nd >= 2 ? (q / 3) % 3 - 1 : 0, nd >= 3 ? q / 9 - 1 : 0};
+      int jg[3] = {0, 0, 0};
+      bool ok = true;
+      for (int d = 0; d < nd; ++d) {
+        jg[d] = ig[d] + o[d];
+        if (jg[d] < 0 || jg[d] >= nb[d]) {
+          const int side = jg[d] < 0 ? 0 : 1;
+          if (c->bc.kind[2 * d + side] == BCK_PERIODIC) jg[d] = (jg[d] + nb[d]) % nb[d];
+          else ok = false;
+        }
+      }
+      nbr[(size_t)b * ndir3 + q] = ok ? jg[0] + nb[0] * (jg[1] + nb[1] * jg[2]) : -1;
+    }
+    for (int d = 0; d < nd; ++d) dx[(size_t)b * nd + d] = h[d];
+  }
+  return amrvac_gpu_set_blocks(c, total, dx.data(), nbr.data());
+}
+
+int amrvac_gpu_nblocks(const amrvac_ctx *c) { return c ? c->nblocks : AMRVAC_E_ARG; }
+
+static int ensure_stage(amrvac_ctx *c, size_t doubles) {
+  if (c->stage_doubles >= doubles) return 0;
+  cudaStreamSynchronize(c->stream);
+  cudaFree(c->d_stage);
+  c->d_stage = nullptr;
+  c->stage_doubles = 0;
+  CK(cudaMalloc(&c->d_stage, sizeof(double) * doubles));
+  c->stage_doubles = doubles;
+  return 0;
+}
+
+static size_t ghosted_per_block(const amrvac_ctx *c) {
+  size_t g = 1;
+  for (int d = 0; d < c->cfg.ndim; ++d) g *= (size_t)(16 + 2 * c->cfg.nghostcells);
+  return g * c->nw;
+}
+
+int amrvac_gpu_upload(amrvac_ctx *c, int reg, int first, int n, const double *w) {
+  if (int r = check_ctx(c, true)) return r;
+  if (reg < 0 || reg > 2 || !w || first < 0 || n <= 0 || first + n > c->nblocks)
+    return fail(AMRVAC_E_ARG, "bad upload range");
+  const size_t gpb = ghosted_per_block(c);
+  const int chunk = (int)std::max<size_t>(1, (size_t)(256u << 20) / (gpb * sizeof(double)));
+  for (int b0 = 0; b0 < n; b0 += chunk) {
+    const int m = std::min(chunk, n - b0);
+    if (int r = ensure_stage(c, gpb * m)) return r;
+    CK(cudaMemcpyAsync(c->d_stage, w + (size_t)b0 * gpb, sizeof(double) * gpb * m, cudaMemcpyHostToDevice,
+                       c->stream));
+    CK(launch_unpack(c->d_stage, c->pool[reg], first + b0, m, c->nw, c->cfg.ndim, c->cfg.nghostcells, c->stream));
+    ++c->launches;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int amrvac_gpu_download(amrvac_ctx *c, int reg, int first, int n, double *w) {
+  if (int r = check_ctx(c, true)) return r;
+  if (reg < 0 || reg > 2 || !w || first < 0 || n <= 0 || first + n > c->nblocks)
+    return fail(AMRVAC_E_ARG, "bad download range");
+  const size_t gpb = ghosted_per_block(c);
+  const int chunk = (int)std::max<size_t>(1, (size_t)(256u << 20) / (gpb * sizeof(double)));
+  for (int b0 = 0; b0 < n; b0 += chunk) {
+    const int m = std::min(chunk, n - b0);
+    if (int r = ensure_stage(c, gpb * m)) return r;
+    CK(launch_pack(c->pool[reg], c->d_stage, first + b0, m, c->nw, c->cfg.ndim, c->cfg.nghostcells, c->d_nbr,
+                   c->maps, c->bc, c->stream));
+    ++c->launches;
+    CK(cudaMemcpyAsync(w + (size_t)b0 * gpb, c->d_stage, sizeof(double) * gpb * m, cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return 0;
+}
+
+int amrvac_gpu_getdt(amrvac_ctx *c, int reg, double *dt, double *cmax_global) {
+  if (int r = check_ctx(c, true)) return r;
+  if (reg < 0 || reg > 2) return fail(AMRVAC_E_ARG, "bad register");
+  if (int r = launch_getdt(c, reg)) return r;
+  unsigned long long red[2];
+  CK(cudaMemcpyAsync(red, c->d_red, sizeof(red), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemsetAsync(c->d_red, 0, sizeof(red), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double x, cm;
+  std::memcpy(&x, &red[0], sizeof(double));
+  std::memcpy(&cm, &red[1], sizeof(double));
+  double d = 1.0e99;
+  if (x > 1.0e-12) d = std::min(d, c->cfg.courantpar / x);
+  if (dt) *dt = d;
+  if (cmax_global) *cmax_global = cm;
+  CK(cudaMemcpyAsync(c->d_scal + 1, &cm, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return d < c->cfg.dtmin ? (int)AMRVAC_ST_DT_TOO_SMALL : 0;
+}
+
+int amrvac_gpu_set_cmax_global(amrvac_ctx *c, double cmax_global) {
+  if (int r = check_ctx(c, false)) return r;
+  CK(cudaMemcpyAsync(c->d_scal + 1, &cmax_global, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int amrvac_gpu_advect1(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a_base, double b_in,
+                       double dtfactor, double dt) {
+  if (int r = check_ctx(c, true)) return r;
+  if (reg_ct < 0 || reg_ct > 2 || reg_new < 0 || reg_new > 2 || reg_base < 0 || reg_base > 2)
+    return fail(AMRVAC_E_ARG, "bad register");
+  if (reg_ct == reg_new) return fail(AMRVAC_E_ARG, "reg_ct and reg_new must differ");
+  if (a_base == 0.0 && b_in != 1.0) return fail(AMRVAC_E_ARG, "a_base == 0 requires b_in == 1");
+  CK(cudaMemcpyAsync(c->d_scal + 0, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int r = launch_stage(c, reg_ct, reg_new, reg_base, a_base, b_in, dtfactor);
+  CK(cudaStreamSynchronize(c->stream));
+  return r;
+}
+
+int amrvac_gpu_set_time(amrvac_ctx *c, double t, double time_max, double dtsave) {
+  if (int r = check_ctx(c, false)) return r;
+  const double v[3] = {t, time_max, dtsave};
+  CK(cudaMemcpyAsync(c->d_scal + 2, v, sizeof(v), cudaMemcpyHostToDevice, c->stream));
+  const double z = 0.0;
+  CK(cudaMemcpyAsync(c->d_scal + 7, &z, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int amrvac_gpu_step(amrvac_ctx *c) {
+  if (int r = check_ctx(c, true)) return r;
+  return launch_step(c);
+}
+
+int amrvac_gpu_run(amrvac_ctx *c, int nsteps) {
+  if (int r = check_ctx(c, true)) return r;
+  if (nsteps <= 0) return 0;
+  if (!c->graph) {
+    cudaGraph_t g;
+    const int64_t before = c->launches;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int r = launch_step(c);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (r) { if (e == cudaSuccess) cudaGraphDestroy(g); return r; }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    c->graph_nodes = c->launches - before;
+    c->launches = before;
+    e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { c->graph = nullptr; return cuda_fail(e, "cudaGraphInstantiate"); }
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    CK(cudaGraphLaunch(c->graph, c->stream));
+    c->launches += c->graph_nodes;
+  }
+  return 0;
+}
+
+int amrvac_gpu_run_timed(amrvac_ctx *c, int nsteps, double *total_ms, double *stage_ms, double *getdt_ms) {
+  if (int r = check_ctx(c, true)) return r;
+  if (nsteps <= 0) return fail(AMRVAC_E_ARG, "nsteps must be positive");
+  const int nst = c->cfg.time_stepper;  // stages per step
+  const int per = 3 + nst;              // events per step
+  std::vector<cudaEvent_t> ev((size_t)nsteps * per + 1);
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  int r = 0;
+  size_t q = 0;
+  CK(cudaEventRecord(ev[q++], c->stream));
+  for (int s = 0; s < nsteps && !r; ++s) {
+    r = launch_getdt(c, 0);
+    if (r) break;
+    CK(cudaEventRecord(ev[q++], c->stream));  // after getdt
+    CK(launch_setdt_finalize(c->d_red, c->d_scal, c->d_status, c->stream));
+    ++c->launches;
+    CK(cudaEventRecord(ev[q++], c->stream));  // before stage 1
+    const amrvac_cfg &k = c->cfg;
+    if (k.time_stepper == AMRVAC_TS_ONESTEP) {
+      CK(cudaMemcpyAsync(c->pool[1], c->pool[0], sizeof(double) * c->per_block * c->nw * c->nblocks,
+                         cudaMemcpyDeviceToDevice, c->stream));
+      r = launch_stage(c, 1, 0, 0, 0.0, 1.0, 1.0);
+      CK(cudaEventRecord(ev[q++], c->stream));
+    } else if (k.time_stepper == AMRVAC_TS_TWOSTEP) {
+      r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);
+      CK(cudaEventRecord(ev[q++], c->stream));
+      if (!r) r = launch_stage(c, 1, 0, 0, 0.5, 0.5, 0.5);
+      CK(cudaEventRecord(ev[q++], c->stream));
+    } else {
+      double b11, b22, b33, a21, a31;
+      if (k.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
+      else { b11 = 1.0; b22 = 1.0 / 4.0; b33 = 2.0 / 3.0; a21 = 3.0 / 4.0; a31 = 1.0 / 3.0; }
+      r = launch_stage(c, 0, 1, 0, 0.0, 1.0, b11);
+      CK(cudaEventRecord(ev[q++], c->stream));
+      if (!r) r = launch_stage(c, 1, 2, 0, a21, 1.0 - a21, b22);
+      CK(cudaEventRecord(ev[q++], c->stream));
+      if (!r) r = launch_stage(c, 2, 0, 0, a31, 1.0 - a31, b33);
+      CK(cudaEventRecord(ev[q++], c->stream));
+    }
+    CK(launch_advance_time(c->d_scal, c->stream));
+    ++c->launches;
+    CK(cudaEventRecord(ev[q++], c->stream));  // end of step
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  double tot = 0, st = 0, gd = 0;
+  float ms;
+  if (!r) {
+    CK(cudaEventElapsedTime(&ms, ev[0], ev[q - 1]));
+    tot = ms;
+    size_t base = 1;
+    cudaEvent_t prev_end = ev[0];
+    for (int s = 0; s < nsteps; ++s) {
+      CK(cudaEventElapsedTime(&ms, prev_end, ev[base]));  // getdt
+      gd += ms;
+      for (int k2 = 0; k2 < nst; ++k2) {
+        CK(cudaEventElapsedTime(&ms, ev[base + 1 + k2], ev[base + 2 + k2]));
+        st += ms;
+      }
+      prev_end = ev[base + 2 + nst];
+      base += per;
+    }
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (r) return r;
+  if (total_ms) *total_ms = tot;
+  if (stage_ms) *stage_ms = st;
+  if (getdt_ms) *getdt_ms = gd;
+  return 0;
+}
+
+int amrvac_gpu_fp64_peak(double *tflops) {
+  if (!tflops) return fail(AMRVAC_E_ARG, "null pointer");
+  CK(measure_fp64_peak(tflops));
+  return 0;
+}
+
+int amrvac_gpu_get_time(amrvac_ctx *c, double *dt, double *cmax_global, double *global_time) {
+  if (int r = check_ctx(c, false)) return r;
+  double s[3];
+  CK(cudaMemcpyAsync(s, c->d_scal, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (dt) *dt = s[0];
+  if (cmax_global) *cmax_global = s[1];
+  if (global_time) *global_time = s[2];
+  return 0;
+}
+
+int amrvac_gpu_status(amrvac_ctx *c, uint32_t *flags) {
+  if (int r = check_ctx(c, false)) return r;
+  if (!flags) return fail(AMRVAC_E_ARG, "null flags");
+  CK(cudaMemcpyAsync(flags, c->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int amrvac_gpu_clear_status(amrvac_ctx *c) {
+  if (int r = check_ctx(c, false)) return r;
+  CK(cudaMemsetAsync(c->d_status, 0, sizeof(uint32_t), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int amrvac_gpu_synchronize(amrvac_ctx *c) {
+  if (int r = check_ctx(c, false)) return r;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int amrvac_gpu_stream(amrvac_ctx *c, void **stream) {
+  if (int r = check_ctx(c, false)) return r;
+  if (!stream) return fail(AMRVAC_E_ARG, "null stream pointer");
+  *stream = (void *)c->stream;
+  return 0;
+}
+
+int amrvac_gpu_register_ptr(amrvac_ctx *c, int reg, double **dptr) {
+  if (int r = check_ctx(c, true)) return r;
+  if (reg < 0 || reg > 2 || !dptr) return fail(AMRVAC_E_ARG, "bad register");
+  *dptr = c->pool[reg];
+  return 0;
+}
+
+int64_t amrvac_gpu_launch_count(const amrvac_ctx *c) { return c ? c->launches : -1; }
+
+// ---------------------------------------------------------------- points
+static int run_points(amrvac_ctx *c, int n, int idim, const double *a, const double *b, const double *cc,
+                      const double *d, double *out, size_t out_per, double *out2, double cg, int kind) {
+  if (int r = check_ctx(c, false)) return r;
+  if (n <= 0 || !a || !out) return fail(AMRVAC_E_ARG, "bad points arguments");
+  const size_t sz = (size_t)n * c->nw;
+  double *dev = nullptr;
+  const size_t total = sz * 4 + (size_t)n * out_per + (size_t)n;
+  CK(cudaMalloc(&dev, sizeof(double) * total));
+  double *da = dev, *db = dev + sz, *dc = dev + 2 * sz, *dd = dev + 3 * sz, *dout = dev + 4 * sz,
+         *dout2 = dout + (size_t)n * out_per;
+  auto up = [&](double *dst, const double *src) -> cudaError_t {
+    return src ? cudaMemcpyAsync(dst, src, sizeof(double) * sz, cudaMemcpyHostToDevice, c->stream) : cudaSuccess;
+  };
+  PointArgs A;
+  A.n = n; A.a = da; A.b = db; A.c = dc; A.d = dd; A.out = dout; A.out2 = out2 ? dout2 : nullptr;
+  A.cg = cg; A.P = c->P;
+  cudaError_t e = up(da, a);
+  if (e == cudaSuccess) e = up(db, b);
+  if (e == cudaSuccess) e = up(dc, cc);
+  if (e == cudaSuccess) e = up(dd, d);
+  if (e == cudaSuccess) {
+    if (kind == 0) e = c->ks.riemann_points(A, idim, c->stream);
+    else if (kind == 1) e = c->ks.flux_points(A, idim, c->stream);
+    else e = c->ks.cbounds_points(A, idim, c->stream);
+    ++c->launches;
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, sizeof(double) * n * out_per, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && out2) e = cudaMemcpyAsync(out2, dout2, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(dev);
+  if (e != cudaSuccess) return cuda_fail(e, "points kernel");
+  return 0;
+}
+
+int amrvac_gpu_riemann_points(amrvac_ctx *c, int n, const double *wlp, const double *wrp, int idim,
+                              double cmax_global, double *f) {
+  if (!c) return fail(AMRVAC_E_ARG, "null context");
+  if (idim < 1 || idim > c->cfg.ndim) return fail(AMRVAC_E_ARG, "idim out of range");
+  return run_points(c, n, idim, wlp, wrp, nullptr, nullptr, f, c->nw, nullptr, cmax_global, 0);
+}
+
+int amrvac_gpu_get_flux_points(amrvac_ctx *c, int n, const double *wc, const double *wp, int idim,
+                               double cmax_global, double *f) {
+  if (!c) return fail(AMRVAC_E_ARG, "null context");
+  if (idim < 1 || idim > c->cfg.ndir) return fail(AMRVAC_E_ARG, "idim out of range");
+  return run_points(c, n, idim, wc, wp, nullptr, nullptr, f, c->nw, nullptr, cmax_global, 1);
+}
+
+int amrvac_gpu_get_cbounds_points(amrvac_ctx *c, int n, const double *wlc, const double *wrc,
+                                  const double *wlp, const double *wrp, int idim, double *cmax,
+                                  double *cmin) {
+  if (!c) return fail(AMRVAC_E_ARG, "null context");
+  if (idim < 1 || idim > c->cfg.ndir) return fail(AMRVAC_E_ARG, "idim out of range");
+  return run_points(c, n, idim, wlc, wrc, wlp, wrp, cmax, 1, cmin, 0.0, 2);
+}
+
+}  // extern "C"

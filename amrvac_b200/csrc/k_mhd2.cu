@@ -1,0 +1,29 @@
+// Stage / getdt / point kernels for ideal MHD in 2-D (ndir 2 or 3, i.e. 2.5D).
+#include "kernels.cuh"
+
+namespace amrvac {
+
+bool lookup_mhd2(const KernelKey &k, KernelSet *out) {
+  if (!k.mhd || k.ndim != 2) return false;
+#define AMRVAC_M2(NDIR, GLM, S)                                 \
+  if (k.ndir == NDIR && k.glm == GLM && k.solver == S) {        \
+    *out = Launch<true, NDIR, GLM, 2, S>::set();                \
+    return true;                                                \
+  }
+  AMRVAC_M2(2, false, SOLVER_TVDLF)
+  AMRVAC_M2(2, false, SOLVER_HLL)
+  AMRVAC_M2(2, false, SOLVER_HLLD)
+  AMRVAC_M2(2, true, SOLVER_TVDLF)
+  AMRVAC_M2(2, true, SOLVER_HLL)
+  AMRVAC_M2(2, true, SOLVER_HLLD)
+  AMRVAC_M2(3, false, SOLVER_TVDLF)
+  AMRVAC_M2(3, false, SOLVER_HLL)
+  AMRVAC_M2(3, false, SOLVER_HLLD)
+  AMRVAC_M2(3, true, SOLVER_TVDLF)
+  AMRVAC_M2(3, true, SOLVER_HLL)
+  AMRVAC_M2(3, true, SOLVER_HLLD)
+#undef AMRVAC_M2
+  return false;
+}
+
+}  // namespace amrvac

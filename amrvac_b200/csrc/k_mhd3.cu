@@ -1,0 +1,23 @@
+// Stage / getdt / point kernels for ideal MHD in 3-D.
+#include "kernels.cuh"
+
+namespace amrvac {
+
+bool lookup_mhd3(const KernelKey &k, KernelSet *out) {
+  if (!k.mhd || k.ndim != 3 || k.ndir != 3) return false;
+#define AMRVAC_M3(GLM, S)                                       \
+  if (k.glm == GLM && k.solver == S) {                          \
+    *out = Launch<true, 3, GLM, 3, S>::set();                   \
+    return true;                                                \
+  }
+  AMRVAC_M3(false, SOLVER_TVDLF)
+  AMRVAC_M3(false, SOLVER_HLL)
+  AMRVAC_M3(false, SOLVER_HLLD)
+  AMRVAC_M3(true, SOLVER_TVDLF)
+  AMRVAC_M3(true, SOLVER_HLL)
+  AMRVAC_M3(true, SOLVER_HLLD)
+#undef AMRVAC_M3
+  return false;
+}
+
+}  // namespace amrvac

@@ -1,0 +1,248 @@
+// Kernel launchers shared by the per-physics translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "stage.cuh"
+
+namespace amrvac {
+
+// ---------------------------------------------------------------- getdt
+// getdt_courant (src/mod_dt.t:160-287) per block, reduced over all blocks.
+// red[0] <- max over blocks of the block's courant sum (maxsum: max_cells
+// sum_d cmax_d/dx_d; summax / minimum per the reference), red[1] <- max cmax.
+struct GetdtArgs {
+  const double *u;
+  const double *dxb;
+  int nblocks;
+  int type_courant;
+  unsigned long long *red;
+  PhysParams P;
+};
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Non-negative doubles order like their bit patterns.
+__device__ __forceinline__ void atomic_max_pos(unsigned long long *a, double v) {
+  if (v > 0.0) atomicMax(a, (unsigned long long)__double_as_longlong(v));
+}
+
+template <bool MHD, int NDIR, bool GLM, int NDIM>
+__global__ void __launch_bounds__(256) getdt_kernel(const GetdtArgs A) {
+  using V = Vars<MHD, NDIR, GLM>;
+  constexpr int NW = V::NW;
+  constexpr int NZ = NDIM == 3 ? BN : 1;
+  const int b = blockIdx.x;
+  const int t = threadIdx.x;
+  const int i = t & (BN - 1), j = t >> 4;
+  double dxinv[3];
+#pragma unroll
+  for (int d = 0; d < NDIM; ++d) dxinv[d] = 1.0 / A.dxb[b * 3 + d];
+  double mtot = 0.0, mcm = 0.0, mdim[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < NZ; ++k) {
+    double w[NW];
+#pragma unroll
+    for (int v = 0; v < NW; ++v) w[v] = __ldg(A.u + cell_offset<NDIM>(b, NW, v, i, j, k));
+    to_primitive<MHD, NDIR, GLM>(w, A.P);
+    double tot = 0.0;
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+      double cm;
+      if constexpr (MHD) {
+        double cf;
+        if (d == 0) cf = fast_speed<NDIR, V::B0 + 0>(w, A.P);
+        else if (d == 1) cf = fast_speed<NDIR, V::B0 + (NDIR > 1 ? 1 : 0)>(w, A.P);
+        else cf = fast_speed<NDIR, V::B0 + (NDIR > 2 ? 2 : 0)>(w, A.P);
+        cm = fabs(w[V::M0 + d]) + cf;
+      } else {
+        cm = fabs(w[V::M0 + d]) + sqrt(A.P.gamma * w[V::E] / w[V::RHO]);
+      }
+      const double c = cm * dxinv[d];
+      tot = d == 0 ? c : tot + c;
+      mdim[d] = fmax(mdim[d], c);
+      mcm = fmax(mcm, cm);
+    }
+    mtot = fmax(mtot, tot);
+  }
+  __shared__ double red[4][8];
+  const int lane = t & 31, wid = t >> 5;
+  double r0 = warp_max(mtot), r1 = warp_max(mcm);
+  double r2[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) r2[d] = warp_max(mdim[d]);
+  if (lane == 0) {
+    red[0][wid] = r0; red[1][wid] = r1;
+    red[2][wid] = r2[0]; red[3][wid] = r2[1];
+  }
+  __shared__ double red3[8];
+  if (lane == 0) red3[wid] = r2[2];
+  __syncthreads();
+  if (t == 0) {
+    double a0 = 0, a1 = 0, d0 = 0, d1 = 0, d2 = 0;
+    for (int q = 0; q < 8; ++q) {
+      a0 = fmax(a0, red[0][q]); a1 = fmax(a1, red[1][q]);
+      d0 = fmax(d0, red[2][q]); d1 = fmax(d1, red[3][q]); d2 = fmax(d2, red3[q]);
+    }
+    double x;
+    if (A.type_courant == 1) {
+      x = a0;
+    } else {
+      double dd[3] = {d0, d1, d2};
+      double courantmax = 0.0, tot = 0.0;
+      for (int d = 0; d < NDIM; ++d) {
+        courantmax = fmax(courantmax, dd[d]);
+        tot = tot + courantmax;
+      }
+      x = A.type_courant == 2 ? tot : courantmax;
+    }
+    atomic_max_pos(A.red + 0, x);
+    atomic_max_pos(A.red + 1, a1);
+  }
+}
+
+// ---------------------------------------------------------------- points
+struct PointArgs {
+  int n;
+  const double *a, *b, *c, *d;  // inputs (state-major [n][nw])
+  double *out, *out2;
+  double cg;
+  PhysParams P;
+};
+
+template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int D>
+__global__ void riemann_points_kernel(const PointArgs A) {
+  using V = Vars<MHD, NDIR, GLM>;
+  constexpr int NW = V::NW;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.n) return;
+  double wL[NW], wR[NW], F[NW];
+#pragma unroll
+  for (int v = 0; v < NW; ++v) { wL[v] = A.a[(size_t)p * NW + v]; wR[v] = A.b[(size_t)p * NW + v]; }
+  face_from_states<MHD, NDIR, GLM, NDIM, SOLVER, D>(wL, wR, A.P, A.cg, F);
+#pragma unroll
+  for (int v = 0; v < NW; ++v) A.out[(size_t)p * NW + v] = F[v];
+}
+
+template <bool MHD, int NDIR, bool GLM, int D>
+__global__ void flux_points_kernel(const PointArgs A) {
+  using V = Vars<MHD, NDIR, GLM>;
+  constexpr int NW = V::NW;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.n) return;
+  double wc[NW], w[NW], f[NW];
+#pragma unroll
+  for (int v = 0; v < NW; ++v) { wc[v] = A.a[(size_t)p * NW + v]; w[v] = A.b[(size_t)p * NW + v]; }
+  phys_flux<MHD, NDIR, GLM, D>(wc, w, A.cg, f);
+#pragma unroll
+  for (int v = 0; v < NW; ++v) A.out[(size_t)p * NW + v] = f[v];
+}
+
+template <bool MHD, int NDIR, bool GLM, int D>
+__global__ void cbounds_points_kernel(const PointArgs A) {
+  using V = Vars<MHD, NDIR, GLM>;
+  constexpr int NW = V::NW;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.n) return;
+  double lc[NW], rc[NW], lp[NW], rp[NW];
+#pragma unroll
+  for (int v = 0; v < NW; ++v) {
+    lc[v] = A.a[(size_t)p * NW + v]; rc[v] = A.b[(size_t)p * NW + v];
+    lp[v] = A.c[(size_t)p * NW + v]; rp[v] = A.d[(size_t)p * NW + v];
+  }
+  double cmax, cmin = 0.0;
+  if (A.out2) cbounds<MHD, NDIR, GLM, D, true>(lc, rc, lp, rp, A.P, cmax, cmin);
+  else cbounds<MHD, NDIR, GLM, D, false>(lc, rc, lp, rp, A.P, cmax, cmin);
+  A.out[p] = cmax;
+  if (A.out2) A.out2[p] = cmin;
+}
+
+// ---------------------------------------------------------------- dispatch
+struct KernelSet {
+  cudaError_t (*prepare)() = nullptr;
+  cudaError_t (*stage)(const StageArgs &, int nctas, cudaStream_t) = nullptr;
+  cudaError_t (*getdt)(const GetdtArgs &, cudaStream_t) = nullptr;
+  cudaError_t (*riemann_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
+  cudaError_t (*flux_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
+  cudaError_t (*cbounds_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
+  size_t stage_smem = 0;
+};
+
+template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER>
+struct Launch {
+  using V = Vars<MHD, NDIR, GLM>;
+  static constexpr size_t SMEM = Tile<V::NW, NDIM>::BYTES;
+  static cudaError_t prepare() {
+    return cudaFuncSetAttribute(fv_stage_kernel<MHD, NDIR, GLM, NDIM, SOLVER>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+  }
+  static cudaError_t stage(const StageArgs &A, int nctas, cudaStream_t s) {
+    fv_stage_kernel<MHD, NDIR, GLM, NDIM, SOLVER><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
+    return cudaGetLastError();
+  }
+  static cudaError_t getdt(const GetdtArgs &A, cudaStream_t s) {
+    getdt_kernel<MHD, NDIR, GLM, NDIM><<<A.nblocks, 256, 0, s>>>(A);
+    return cudaGetLastError();
+  }
+  template <int D>
+  static void rp(const PointArgs &A, cudaStream_t s) {
+    riemann_points_kernel<MHD, NDIR, GLM, NDIM, SOLVER, D><<<(A.n + 127) / 128, 128, 0, s>>>(A);
+  }
+  static cudaError_t riemann_points(const PointArgs &A, int idim, cudaStream_t s) {
+    if (idim == 1) rp<0>(A, s);
+    else if (idim == 2 && NDIM >= 2) rp<NDIM >= 2 ? 1 : 0>(A, s);
+    else if (idim == 3 && NDIM >= 3) rp<NDIM >= 3 ? 2 : 0>(A, s);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+  }
+  template <int D>
+  static void fp(const PointArgs &A, cudaStream_t s) {
+    flux_points_kernel<MHD, NDIR, GLM, D><<<(A.n + 127) / 128, 128, 0, s>>>(A);
+  }
+  static cudaError_t flux_points(const PointArgs &A, int idim, cudaStream_t s) {
+    if (idim == 1) fp<0>(A, s);
+    else if (idim == 2 && NDIR >= 2) fp<NDIR >= 2 ? 1 : 0>(A, s);
+    else if (idim == 3 && NDIR >= 3) fp<NDIR >= 3 ? 2 : 0>(A, s);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+  }
+  template <int D>
+  static void cp(const PointArgs &A, cudaStream_t s) {
+    cbounds_points_kernel<MHD, NDIR, GLM, D><<<(A.n + 127) / 128, 128, 0, s>>>(A);
+  }
+  static cudaError_t cbounds_points(const PointArgs &A, int idim, cudaStream_t s) {
+    if (idim == 1) cp<0>(A, s);
+    else if (idim == 2 && NDIR >= 2) cp<NDIR >= 2 ? 1 : 0>(A, s);
+    else if (idim == 3 && NDIR >= 3) cp<NDIR >= 3 ? 2 : 0>(A, s);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+  }
+  static KernelSet set() {
+    KernelSet k;
+    k.prepare = &prepare;
+    k.stage = &stage;
+    k.getdt = &getdt;
+    k.riemann_points = &riemann_points;
+    k.flux_points = &flux_points;
+    k.cbounds_points = &cbounds_points;
+    k.stage_smem = SMEM;
+    return k;
+  }
+};
+
+// Lookup key for one physics / dimension / solver combination.
+struct KernelKey {
+  bool mhd;
+  int ndim, ndir;
+  bool glm;
+  int solver;
+};
+
+bool lookup_hd(const KernelKey &k, KernelSet *out);
+bool lookup_mhd2(const KernelKey &k, KernelSet *out);
+bool lookup_mhd3(const KernelKey &k, KernelSet *out);
+
+}  // namespace amrvac

@@ -1,0 +1,325 @@
+// Device physics for the finite-volume face update (HD and ideal MHD).
+//
+// Each routine restates one reference routine for a single face or cell; the
+// expression order follows the reference so that the FP64 path agrees with it
+// to rounding (the only reordering is FMA contraction by the compiler).
+// Reference files (relative to the MPI-AMRVAC repository root):
+//   hd:   src/hd/mod_hd_phys.t, src/hd/mod_hd_hllc.t
+//   mhd:  src/mhd/mod_mhd_phys.t
+//   fv:   src/mod_finite_volume.t, src/limiter/mod_limiter.t
+#pragma once
+
+#include <cstdint>
+
+namespace amrvac {
+
+// Limiter ids as in src/limiter/mod_limiter.t:14-24.
+enum : int { LIM_MINMOD = 1, LIM_WOODWARD = 2, LIM_MCBETA = 3, LIM_SUPERBEE = 4,
+             LIM_VANLEER = 5, LIM_ALBADA = 6, LIM_KOREN = 7, LIM_CADA = 8, LIM_CADA3 = 9 };
+enum : int { BS_EINFELDT = 1, BS_CMAXMEAN = 2, BS_CMAXLEFTRIGHT = 3 };
+enum : int { SOLVER_TVDLF = 1, SOLVER_HLL = 2, SOLVER_HLLC = 3, SOLVER_HLLD = 4 };
+enum : int { DIVB_NONE = 0, DIVB_GLM = 1, DIVB_LINDE = 4 };
+// Runtime status bits (atomicOr into the context's status word).
+enum : uint32_t { ST_SMALL_VALUE = 1u, ST_NAN = 2u, ST_DT_TOO_SMALL = 4u, ST_BOUNDS = 8u };
+
+// Physics constants shared by all kernels of one context.
+struct PhysParams {
+  double gamma, gamma_1, inv_gamma_1;
+  double small_density, small_pressure, small_e;
+  double tvdlfeps, cada3_radius, glm_alpha, divbdiff, courantpar;
+  int limiter, boundspeed, divb, glm_extended;
+  int fix_small_values, check_small_values, small_values_method;
+};
+
+// Variable layout in the reference order: rho, m(1:ndir), e, [b(1:ndir), psi].
+template <bool MHD, int NDIR, bool GLM>
+struct Vars {
+  static constexpr int RHO = 0;
+  static constexpr int M0 = 1;
+  static constexpr int E = NDIR + 1;
+  static constexpr int B0 = NDIR + 2;
+  static constexpr int PSI = 2 * NDIR + 2;
+  static constexpr int NW = MHD ? (2 * NDIR + 2 + (GLM ? 1 : 0)) : (NDIR + 2);
+};
+
+__device__ __forceinline__ double fsign(double a, double b) { return copysign(a, b); }
+
+// ------------------------------------------------------------------ conversions
+// hd_to_primitive (mod_hd_phys.t:703-734) / mhd_to_primitive_origin (mod_mhd_phys.t:1741-1765)
+template <bool MHD, int NDIR, bool GLM>
+__device__ __forceinline__ void to_primitive(double *w, const PhysParams &P) {
+  using V = Vars<MHD, NDIR, GLM>;
+  const double inv_rho = 1.0 / w[V::RHO];
+#pragma unroll
+  for (int c = 0; c < NDIR; ++c) w[V::M0 + c] = w[V::M0 + c] * inv_rho;
+  double v2 = w[V::M0] * w[V::M0];
+#pragma unroll
+  for (int c = 1; c < NDIR; ++c) v2 = v2 + w[V::M0 + c] * w[V::M0 + c];
+  if constexpr (MHD) {
+    double b2 = w[V::B0] * w[V::B0];
+#pragma unroll
+    for (int c = 1; c < NDIR; ++c) b2 = b2 + w[V::B0 + c] * w[V::B0 + c];
+    w[V::E] = P.gamma_1 * (w[V::E] - 0.5 * (w[V::RHO] * v2 + b2));
+  } else {
+    w[V::E] = P.gamma_1 * (w[V::E] - 0.5 * w[V::RHO] * v2);
+  }
+}
+
+// hd_to_conserved (mod_hd_phys.t:677-700) / mhd_to_conserved_origin (mod_mhd_phys.t:1562-1579)
+template <bool MHD, int NDIR, bool GLM>
+__device__ __forceinline__ void to_conserved(double *w, const PhysParams &P) {
+  using V = Vars<MHD, NDIR, GLM>;
+  double v2 = w[V::M0] * w[V::M0];
+#pragma unroll
+  for (int c = 1; c < NDIR; ++c) v2 = v2 + w[V::M0 + c] * w[V::M0 + c];
+  if constexpr (MHD) {
+    double b2 = w[V::B0] * w[V::B0];
+#pragma unroll
+    for (int c = 1; c < NDIR; ++c) b2 = b2 + w[V::B0 + c] * w[V::B0 + c];
+    w[V::E] = w[V::E] * P.inv_gamma_1 + 0.5 * (v2 * w[V::RHO] + b2);
+  } else {
+    w[V::E] = w[V::E] * P.inv_gamma_1 + 0.5 * v2 * w[V::RHO];
+  }
+#pragma unroll
+  for (int c = 0; c < NDIR; ++c) w[V::M0 + c] = w[V::RHO] * w[V::M0 + c];
+}
+
+// Small-value check and "replace" fix on one state (hd_check_w mod_hd_phys.t:648-674,
+// mhd_check_w_origin mod_mhd_phys.t:1452-1473, replace branches mod_hd_phys.t:1436-1466
+// and mod_mhd_phys.t:2208-2222).  Returns true if the state was flagged.
+template <bool MHD, int NDIR, bool GLM>
+__device__ __forceinline__ bool small_values(double *w, bool primitive, const PhysParams &P) {
+  using V = Vars<MHD, NDIR, GLM>;
+  const bool frho = w[V::RHO] < P.small_density;
+  double m2 = w[V::M0] * w[V::M0];
+#pragma unroll
+  for (int c = 1; c < NDIR; ++c) m2 = m2 + w[V::M0 + c] * w[V::M0 + c];
+  double b2 = 0.0;
+  if constexpr (MHD) {
+    b2 = w[V::B0] * w[V::B0];
+#pragma unroll
+    for (int c = 1; c < NDIR; ++c) b2 = b2 + w[V::B0 + c] * w[V::B0 + c];
+  }
+  bool fe;
+  if (primitive) fe = w[V::E] < P.small_pressure;
+  else if (MHD) fe = w[V::E] - 0.5 * (m2 / w[V::RHO] + b2) < P.small_e;
+  else fe = P.gamma_1 * (w[V::E] - 0.5 * m2 / w[V::RHO]) < P.small_pressure;
+  if (!(frho || fe)) return false;
+  if (P.small_values_method == 1) {
+    if (frho) {
+      w[V::RHO] = P.small_density;
+#pragma unroll
+      for (int c = 0; c < NDIR; ++c) w[V::M0 + c] = 0.0;
+    }
+    if ((!MHD && frho) || fe) {
+      if (primitive) {
+        w[V::E] = P.small_pressure;
+      } else {
+        double mm = w[V::M0] * w[V::M0];
+#pragma unroll
+        for (int c = 1; c < NDIR; ++c) mm = mm + w[V::M0 + c] * w[V::M0 + c];
+        w[V::E] = MHD ? P.small_e + 0.5 * (mm / w[V::RHO] + b2) : P.small_e + 0.5 * mm / w[V::RHO];
+      }
+    }
+  }
+  return true;
+}
+
+// ------------------------------------------------------------------ fluxes
+// hd_get_flux (mod_hd_phys.t:1097-1146) / mhd_get_flux (mod_mhd_phys.t:3810-3889).
+// wc: conserved, w: primitive state at the face; D: face normal (0-based).
+template <bool MHD, int NDIR, bool GLM, int D>
+__device__ __forceinline__ void phys_flux(const double *wc, const double *w, double cg,
+                                          double *f) {
+  using V = Vars<MHD, NDIR, GLM>;
+  constexpr int MN = V::M0 + D;
+  if constexpr (!MHD) {
+    f[V::RHO] = w[MN] * w[V::RHO];
+#pragma unroll
+    for (int c = 0; c < NDIR; ++c) f[V::M0 + c] = w[MN] * wc[V::M0 + c];
+    f[MN] = f[MN] + w[V::E];
+    f[V::E] = w[MN] * (wc[V::E] + w[V::E]);
+  } else {
+    constexpr int BN = V::B0 + D;
+    f[V::RHO] = w[MN] * w[V::RHO];
+#pragma unroll
+    for (int c = 0; c < NDIR; ++c) f[V::M0 + c] = wc[MN] * w[V::M0 + c] - w[BN] * w[V::B0 + c];
+    double b2 = w[V::B0] * w[V::B0];
+#pragma unroll
+    for (int c = 1; c < NDIR; ++c) b2 = b2 + w[V::B0 + c] * w[V::B0 + c];
+    const double ptotal = w[V::E] + 0.5 * b2;
+    f[MN] = f[MN] + ptotal;
+    double bv = w[V::B0] * w[V::M0];
+#pragma unroll
+    for (int c = 1; c < NDIR; ++c) bv = bv + w[V::B0 + c] * w[V::M0 + c];
+    f[V::E] = w[MN] * (wc[V::E] + ptotal) - w[BN] * bv;
+#pragma unroll
+    for (int c = 0; c < NDIR; ++c) f[V::B0 + c] = w[MN] * w[V::B0 + c] - w[BN] * w[V::M0 + c];
+    if constexpr (GLM) {
+      f[BN] = w[V::PSI];
+      f[V::PSI] = (cg * cg) * w[BN];
+    }
+  }
+}
+
+// mhd_get_csound_prim (mod_mhd_phys.t:3329-3379): fast magnetosonic speed.
+template <int NDIR, int BN>
+__device__ __forceinline__ double fast_speed(const double *w, const PhysParams &P) {
+  constexpr int RHO = 0, E = NDIR + 1, B0 = NDIR + 2;
+  const double inv_rho = 1.0 / w[RHO];
+  const double cs = P.gamma * w[E] * inv_rho;
+  double b2 = w[B0] * w[B0];
+#pragma unroll
+  for (int c = 1; c < NDIR; ++c) b2 = b2 + w[B0 + c] * w[B0 + c];
+  const double cfast2 = b2 * inv_rho + cs;
+  double av = cfast2 * cfast2 - 4.0 * cs * (w[BN] * w[BN]) * inv_rho;
+  if (av < 0.0) av = 0.0;
+  return sqrt(0.5 * (cfast2 + sqrt(av)));
+}
+
+// hd_get_cbounds (mod_hd_phys.t:891-1001) / mhd_get_cbounds (mod_mhd_phys.t:3037-3127).
+// WITH_MIN=false gives the tvdlf form (cmax only).  Returns a status bit.
+template <bool MHD, int NDIR, bool GLM, int D, bool WITH_MIN>
+__device__ __forceinline__ uint32_t cbounds(const double *wLC, const double *wRC, const double *wLp,
+                                            const double *wRp, const PhysParams &P, double &cmax,
+                                            double &cmin) {
+  using V = Vars<MHD, NDIR, GLM>;
+  constexpr int MN = V::M0 + D;
+  uint32_t st = 0;
+  if (P.boundspeed == BS_EINFELDT) {
+    const double tmp1 = sqrt(wLp[V::RHO]);
+    const double tmp2 = sqrt(wRp[V::RHO]);
+    const double tmp3 = 1.0 / (tmp1 + tmp2);
+    const double umean = (wLp[MN] * tmp1 + wRp[MN] * tmp2) * tmp3;
+    const double dv = wRp[MN] - wLp[MN];
+    double dmean;
+    if constexpr (MHD) {
+      const double csL = fast_speed<NDIR, V::B0 + D>(wLp, P);
+      const double csR = fast_speed<NDIR, V::B0 + D>(wRp, P);
+      dmean = sqrt((tmp1 * (csL * csL) + tmp2 * (csR * csR)) * tmp3 +
+                   0.5 * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
+    } else {
+      const double csL = P.gamma * wLp[V::E] / wLp[V::RHO];
+      const double csR = P.gamma * wRp[V::E] / wRp[V::RHO];
+      dmean = sqrt((tmp1 * csL + tmp2 * csR) * tmp3 + 0.5 * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
+    }
+    if (WITH_MIN) {
+      cmin = umean - dmean;
+      cmax = umean + dmean;
+    } else {
+      cmax = fabs(umean) + dmean;
+    }
+  } else if (P.boundspeed == BS_CMAXMEAN) {
+    if constexpr (MHD) {
+      double wm[V::NW];
+#pragma unroll
+      for (int v = 0; v < V::NW; ++v) wm[v] = 0.5 * (wLp[v] + wRp[v]);
+      const double cs = fast_speed<NDIR, V::B0 + D>(wm, P);
+      if (WITH_MIN) {
+        cmax = fmax(wm[MN] + cs, 0.0);
+        cmin = fmin(wm[MN] - cs, 0.0);
+      } else {
+        cmax = fabs(wm[MN]) + cs;
+      }
+    } else {
+      double wm[V::NW];
+#pragma unroll
+      for (int v = 0; v < V::NW; ++v) wm[v] = 0.5 * (wLC[v] + wRC[v]);
+      const double tmp1 = wm[MN] / wm[V::RHO];
+      double m2 = wm[V::M0] * wm[V::M0];
+#pragma unroll
+      for (int c = 1; c < NDIR; ++c) m2 = m2 + wm[V::M0 + c] * wm[V::M0 + c];
+      double pth = P.gamma_1 * (wm[V::E] - 0.5 * m2 / wm[V::RHO]);
+      if (P.fix_small_values) {
+        if (pth < P.small_pressure) pth = P.small_pressure;
+      } else if (P.check_small_values) {
+        if (pth < P.small_pressure) st |= ST_SMALL_VALUE;
+      }
+      const double cs = sqrt(P.gamma * pth / wm[V::RHO]);
+      if (WITH_MIN) {
+        cmax = fmax(tmp1 + cs, 0.0);
+        cmin = fmin(tmp1 - cs, 0.0);
+      } else {
+        cmax = fabs(tmp1) + cs;
+      }
+    }
+  } else {  // cmaxleftright
+    double cs;
+    if constexpr (MHD) {
+      cs = fmax(fast_speed<NDIR, V::B0 + D>(wLp, P), fast_speed<NDIR, V::B0 + D>(wRp, P));
+    } else {
+      const double csL = P.gamma * wLp[V::E] / wLp[V::RHO];
+      const double csR = P.gamma * wRp[V::E] / wRp[V::RHO];
+      cs = fmax(sqrt(csL), sqrt(csR));
+    }
+    if (WITH_MIN) cmin = fmin(wLp[MN], wRp[MN]) - cs;
+    cmax = fmax(wLp[MN], wRp[MN]) + cs;
+  }
+  return st;
+}
+
+// ------------------------------------------------------------------ limiters
+// dwlimiter2 (mod_limiter.t:128-334) for one cell: a = dwC(ix) (forward
+// difference), b = dwC(ix-1) (backward difference).  LEFT selects ldw, else rdw.
+template <bool LEFT>
+__device__ __forceinline__ double limited_slope(int lim, double a, double b, double rdelinv) {
+  constexpr double qsmall = 1.0e-12, qsmall2 = 2.0e-12;
+  constexpr double eps = 1.4901161193847656e-08;  // sqrt(epsilon(1d0)) = 2**-26
+  constexpr double c_mcbeta = 1.4, cadalfa = 0.5, cadbeta = 2.0, cadgamma = 1.6;
+  constexpr double cadepsilon = 1.0e-14, invcadepsilon = 1.0e14;
+  constexpr double third = 1.0 / 3.0;
+  switch (lim) {
+    case LIM_MINMOD: {
+      const double t = fsign(1.0, a);
+      return t * fmax(0.0, fmin(fabs(a), t * b));
+    }
+    case LIM_VANLEER:
+      return 2.0 * fmax(b * a, 0.0) / (a + b + qsmall);
+    case LIM_CADA3: {
+      const double tmpeta = (a * a + b * b) * rdelinv;
+      const double t = LEFT ? b / (a + fsign(eps, a)) : a / (b + fsign(eps, b));
+      const double A = (2.0 + t) * third;
+      double phi;
+      if (tmpeta <= 1.0 - cadepsilon) {
+        phi = A;
+      } else {
+        const double lim2 = fmax(0.0, fmin(A, fmax(-(cadalfa * t), fmin(fmin(cadbeta * t, A), cadgamma))));
+        if (tmpeta >= 1.0 + cadepsilon) {
+          phi = lim2;
+        } else {
+          const double t2 = (tmpeta - 1.0) * invcadepsilon;
+          phi = 0.5 * ((1.0 - t2) * A + (1.0 + t2) * lim2);
+        }
+      }
+      return phi * (LEFT ? a : b);
+    }
+    case LIM_WOODWARD: {
+      const double t = fsign(1.0, a);
+      return 2.0 * t * fmax(0.0, fmin(fmin(fabs(a), t * b), t * 0.25 * (b + a)));
+    }
+    case LIM_MCBETA: {
+      const double t = fsign(1.0, a);
+      return t * fmax(0.0, fmin(fmin(c_mcbeta * fabs(a), c_mcbeta * t * b), t * 0.5 * (b + a)));
+    }
+    case LIM_SUPERBEE: {
+      const double t = fsign(1.0, a);
+      return t * fmax(fmax(0.0, fmin(2.0 * fabs(a), t * b)), fmin(fabs(a), 2.0 * t * b));
+    }
+    case LIM_ALBADA:
+      return (b * (a * a + qsmall) + a * (b * b + qsmall)) / (a * a + b * b + qsmall2);
+    case LIM_KOREN: {
+      const double t = fsign(1.0, a);
+      const double t2 = fmin(2.0 * fabs(a), 2.0 * t * b);
+      if (LEFT) return t * fmax(0.0, fmin(t2, (b * t + 2.0 * fabs(a)) * third));
+      return t * fmax(0.0, fmin(t2, (2.0 * b * t + fabs(a)) * third));
+    }
+    default: {  // cada
+      const double t = LEFT ? b / (a + fsign(eps, a)) : a / (b + fsign(eps, b));
+      const double t2 = (2.0 + t) * third;
+      return fmax(0.0, fmin(t2, fmax(-(cadalfa * t), fmin(fmin(cadbeta * t, t2), cadgamma)))) *
+             (LEFT ? a : b);
+    }
+  }
+}
+
+}  // namespace amrvac

@@ -1,0 +1,247 @@
+// Approximate Riemann solvers for one face (FP64).
+//
+// Restates get_Riemann_flux_{tvdlf,hll,hllc,hlld} (src/mod_finite_volume.t:348-729)
+// and the HD HLLC helpers hd_get_lCD / hd_get_wCD (src/hd/mod_hd_hllc.t:56-257)
+// for a single interface, with the reference's flux_type rules
+// (src/mhd/mod_mhd_phys.t:566-589): with GLM the normal B and psi fluxes are
+// "special" (taken from the left flux); without GLM the normal B uses the
+// diffusive tvdlf form.
+#pragma once
+
+#include "physics.cuh"
+
+namespace amrvac {
+
+template <bool MHD, int NDIM, bool GLM>
+struct FluxTypes {
+  static constexpr bool bn_special = MHD && NDIM > 1 && GLM;
+  static constexpr bool bn_tvdlf = MHD && NDIM > 1 && !GLM;
+};
+
+// get_Riemann_flux_tvdlf (mod_finite_volume.t:348-379)
+template <int NW>
+__device__ __forceinline__ void riemann_tvdlf(const double *wLC, const double *wRC, const double *fL,
+                                              const double *fR, double cmax, double tvdlfeps,
+                                              double *F) {
+  const double fac = -(0.5 * tvdlfeps * cmax);
+#pragma unroll
+  for (int v = 0; v < NW; ++v) {
+    double f = 0.5 * (fL[v] + fR[v]);
+    F[v] = f + fac * (wRC[v] - wLC[v]);
+  }
+}
+
+// get_Riemann_flux_hll (mod_finite_volume.t:381-437)
+template <bool MHD, int NDIR, bool GLM, int NDIM, int D>
+__device__ __forceinline__ void riemann_hll(const double *wLC, const double *wRC, const double *fL,
+                                            const double *fR, double cmax, double cmin,
+                                            double tvdlfeps, double *F) {
+  using V = Vars<MHD, NDIR, GLM>;
+  using FT = FluxTypes<MHD, NDIM, GLM>;
+#pragma unroll
+  for (int v = 0; v < V::NW; ++v) {
+    if (FT::bn_tvdlf && v == V::B0 + D) {
+      F[v] = -(tvdlfeps * 0.5 * fmax(cmax, fabs(cmin))) * (wRC[v] - wLC[v]);
+    } else if (cmin >= 0.0) {
+      F[v] = fL[v];
+    } else if (cmax <= 0.0) {
+      F[v] = fR[v];
+    } else {
+      F[v] = (cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v])) / (cmax - cmin);
+    }
+  }
+}
+
+// get_Riemann_flux_hllc (mod_finite_volume.t:439-504) + hd_get_lCD / hd_get_wCD
+// (mod_hd_hllc.t:56-257); HD only, no hllcd diffusion, flathllc=.false.
+template <int NDIR, int D>
+__device__ __forceinline__ void riemann_hllc_hd(const double *wLC, const double *wRC, const double *fL,
+                                                const double *fR, double cmax, double cmin,
+                                                double *F) {
+  using V = Vars<false, NDIR, false>;
+  constexpr int NW = V::NW, MN = V::M0 + D;
+  int patchf = 1;
+  if (cmin >= 0.0) patchf = -2;
+  else if (cmax <= 0.0) patchf = 2;
+  if (patchf == -2) {
+#pragma unroll
+    for (int v = 0; v < NW; ++v) F[v] = fL[v];
+    return;
+  }
+  if (patchf == 2) {
+#pragma unroll
+    for (int v = 0; v < NW; ++v) F[v] = fR[v];
+    return;
+  }
+  double whll[NW], Fhll[NW];
+#pragma unroll
+  for (int v = 0; v < NW; ++v) {
+    Fhll[v] = (cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v])) / (cmax - cmin);
+    whll[v] = (cmax * wRC[v] - cmin * wLC[v] + fL[v] - fR[v]) / (cmax - cmin);
+  }
+  double lambdaCD = whll[MN] / whll[V::RHO];
+  bool cond = true;
+  if (cmin < 0.0 && lambdaCD > 0.0 && lambdaCD < cmax) {
+    patchf = -1;
+  } else if (cmax > 0.0 && lambdaCD < 0.0 && lambdaCD > cmin) {
+    patchf = 1;
+  } else if (lambdaCD >= cmax || lambdaCD <= cmin) {
+    lambdaCD = 0.0;
+    patchf = 3;
+    cond = false;
+  }
+  if (cond && lambdaCD == 0.0) patchf = (-cmin >= cmax) ? 1 : -1;
+  if (patchf == 3) {
+#pragma unroll
+    for (int v = 0; v < NW; ++v) F[v] = Fhll[v];
+    return;
+  }
+  const bool right = (patchf == 1);
+  const double *wSub = right ? wRC : wLC;
+  const double *fSub = right ? fR : fL;
+  const double cspeed = right ? cmax : cmin;
+  const double vSub = wSub[MN] / wSub[V::RHO];
+  const double csmls = 1.0 / (cspeed - lambdaCD);
+  double wCD[NW];
+  wCD[V::RHO] = wSub[V::RHO] * (cspeed - vSub) * csmls;
+#pragma unroll
+  for (int c = 0; c < NDIR; ++c) {
+    if (c != D) wCD[V::M0 + c] = (cspeed * wSub[V::M0 + c] - fSub[V::M0 + c]) * csmls;
+    else wCD[V::M0 + c] = wCD[V::RHO] * lambdaCD;
+  }
+  const double pCD = wSub[V::RHO] * (cspeed - vSub) * (lambdaCD - vSub) + fSub[MN] - wSub[MN] * vSub;
+  wCD[V::E] = (cspeed * wSub[V::E] - fSub[V::E] + lambdaCD * pCD) * csmls;
+#pragma unroll
+  for (int v = 0; v < NW; ++v) F[v] = fSub[v] + cspeed * (wCD[v] - wSub[v]);
+}
+
+// get_Riemann_flux_hlld (mod_finite_volume.t:507-729), no B0 / equilibrium split.
+template <int NDIR, bool GLM, int NDIM, int D>
+__device__ __forceinline__ void riemann_hlld(const double *wLC, const double *wRC, const double *wLp,
+                                             const double *wRp, const double *fL, const double *fR,
+                                             double sR, double sL, double *F) {
+  using V = Vars<true, NDIR, GLM>;
+  using FT = FluxTypes<true, NDIM, GLM>;
+  constexpr int NW = V::NW, RHO = V::RHO, E = V::E, M0 = V::M0, B0 = V::B0;
+  constexpr int ip1 = D, ip2 = (D + 1) % NDIR, ip3 = (D + 2) % NDIR;
+  constexpr int m1 = M0 + ip1, m2 = M0 + ip2, m3 = M0 + ip3;
+  constexpr int b1 = B0 + ip1, b2 = B0 + ip2, b3 = B0 + ip3;
+  const double Bx = (sR * wRC[b1] - sL * wLC[b1]) / (sR - sL);
+  double bR2 = wRC[B0] * wRC[B0], bL2 = wLC[B0] * wLC[B0];
+#pragma unroll
+  for (int c = 1; c < NDIR; ++c) {
+    bR2 = bR2 + wRC[B0 + c] * wRC[B0 + c];
+    bL2 = bL2 + wLC[B0 + c] * wLC[B0 + c];
+  }
+  const double ptR = wRp[E] + 0.5 * bR2;
+  const double ptL = wLp[E] + 0.5 * bL2;
+  const double vR = wRp[m1], vL = wLp[m1];
+  const double suR = (sR - vR) * wRC[RHO];
+  const double suL = (sL - vL) * wLC[RHO];
+  const double sm = (suR * vR - suL * vL - ptR + ptL) / (suR - suL);
+  // star states w1 (velocities in the momentum slots until the final conversion)
+  double w1R[NW], w1L[NW], w2R[NW], w2L[NW];
+  w1R[m1] = sm; w1L[m1] = sm; w2R[m1] = sm; w2L[m1] = sm;
+  w1R[b1] = Bx; w1L[b1] = Bx;
+  w1R[RHO] = suR / (sR - sm);
+  w1L[RHO] = suL / (sL - sm);
+  double r1R = suR * (sR - sm) - Bx * Bx;
+  if (r1R != 0.0) r1R = 1.0 / r1R;
+  double r1L = suL * (sL - sm) - Bx * Bx;
+  if (r1L != 0.0) r1L = 1.0 / r1L;
+  w1R[m2] = wRp[m2] - Bx * wRC[b2] * (sm - vR) * r1R;
+  w1L[m2] = wLp[m2] - Bx * wLC[b2] * (sm - vL) * r1L;
+  double pb2R = (suR * (sR - vR) - Bx * Bx) * r1R;
+  double pb2L = (suL * (sL - vL) - Bx * Bx) * r1L;
+  if constexpr (NDIR == 3) {
+    w1R[m3] = wRp[m3] - Bx * wRC[b3] * (sm - vR) * r1R;
+    w1L[m3] = wLp[m3] - Bx * wLC[b3] * (sm - vL) * r1L;
+    w1R[b3] = wRC[b3] * pb2R;
+    w1L[b3] = wLC[b3] * pb2L;
+  }
+  w1R[b2] = wRC[b2] * pb2R;
+  w1L[b2] = wLC[b2] * pb2L;
+  const double pts = suR * (sm - vR) + ptR;  // w1R(p_) = w1L(p_)
+  {
+    double vbR = wRp[M0] * wRC[B0], vbL = wLp[M0] * wLC[B0];
+    double v1bR = w1R[M0] * w1R[B0], v1bL = w1L[M0] * w1L[B0];
+#pragma unroll
+    for (int c = 1; c < NDIR; ++c) {
+      vbR = vbR + wRp[M0 + c] * wRC[B0 + c];
+      vbL = vbL + wLp[M0 + c] * wLC[B0 + c];
+      v1bR = v1bR + w1R[M0 + c] * w1R[B0 + c];
+      v1bL = v1bL + w1L[M0 + c] * w1L[B0 + c];
+    }
+    w1R[E] = ((sR - vR) * wRC[E] - ptR * vR + pts * sm + Bx * (vbR - v1bR)) / (sR - sm);
+    w1L[E] = ((sL - vL) * wLC[E] - ptL * vL + pts * sm + Bx * (vbL - v1bL)) / (sL - sm);
+  }
+  w2R[RHO] = w1R[RHO]; w2L[RHO] = w1L[RHO];
+  w2R[b1] = Bx; w2L[b1] = Bx;
+  const double sqR = sqrt(w1R[RHO]);
+  const double sqL = sqrt(w1L[RHO]);
+  const double tmp = 1.0 / (sqR + sqL);
+  const double signBx = copysign(1.0, Bx);
+  const double s1R = sm + fabs(Bx) / sqR;
+  const double s1L = sm - fabs(Bx) / sqL;
+  w2R[m2] = (sqL * w1L[m2] + sqR * w1R[m2] + (w1R[b2] - w1L[b2]) * signBx) * tmp;
+  w2L[m2] = w2R[m2];
+  w2R[b2] = (sqL * w1R[b2] + sqR * w1L[b2] + sqL * sqR * (w1R[m2] - w1L[m2]) * signBx) * tmp;
+  w2L[b2] = w2R[b2];
+  if constexpr (NDIR == 3) {
+    w2R[m3] = (sqL * w1L[m3] + sqR * w1R[m3] + (w1R[b3] - w1L[b3]) * signBx) * tmp;
+    w2L[m3] = w2R[m3];
+    w2R[b3] = (sqL * w1R[b3] + sqR * w1L[b3] + sqL * sqR * (w1R[m3] - w1L[m3]) * signBx) * tmp;
+    w2L[b3] = w2R[b3];
+  }
+  {
+    double a1R = w1R[M0] * w1R[B0], a2R = w2R[M0] * w2R[B0];
+    double a1L = w1L[M0] * w1L[B0], a2L = w2L[M0] * w2L[B0];
+#pragma unroll
+    for (int c = 1; c < NDIR; ++c) {
+      a1R = a1R + w1R[M0 + c] * w1R[B0 + c];
+      a2R = a2R + w2R[M0 + c] * w2R[B0 + c];
+      a1L = a1L + w1L[M0 + c] * w1L[B0 + c];
+      a2L = a2L + w2L[M0 + c] * w2L[B0 + c];
+    }
+    w2R[E] = w1R[E] + sqR * (a1R - a2R) * signBx;
+    w2L[E] = w1L[E] - sqL * (a1L - a2L) * signBx;
+  }
+#pragma unroll
+  for (int c = 0; c < NDIR; ++c) {
+    w1R[M0 + c] = w1R[M0 + c] * w1R[RHO];
+    w1L[M0 + c] = w1L[M0 + c] * w1L[RHO];
+    w2R[M0 + c] = w2R[M0 + c] * w2R[RHO];
+    w2L[M0 + c] = w2L[M0 + c] * w2L[RHO];
+  }
+  if constexpr (GLM) {
+    // psi star values are never used (flux_special); keep them defined.
+    w1R[V::PSI] = w1L[V::PSI] = w2R[V::PSI] = w2L[V::PSI] = 0.0;
+  }
+  // region selection (Miyoshi eq. 66)
+  int region;
+  if (sL > 0.0) region = 0;
+  else if (s1L >= 0.0) region = 1;
+  else if (sm >= 0.0) region = 2;
+  else if (s1R >= 0.0) region = 3;
+  else if (sR >= 0.0) region = 4;
+  else region = 5;  // sR < 0 (a NaN speed also lands here)
+#pragma unroll
+  for (int v = 0; v < NW; ++v) {
+    if (FT::bn_special && (v == b1 || v == V::PSI)) {
+      F[v] = fL[v];
+      continue;
+    }
+    double out;
+    switch (region) {
+      case 0: out = fL[v]; break;
+      case 1: out = fL[v] + sL * (w1L[v] - wLC[v]); break;
+      case 2: out = fL[v] + sL * (w1L[v] - wLC[v]) + s1L * (w2L[v] - w1L[v]); break;
+      case 3: out = fR[v] + sR * (w1R[v] - wRC[v]) + s1R * (w2R[v] - w1R[v]); break;
+      case 4: out = fR[v] + sR * (w1R[v] - wRC[v]); break;
+      default: out = fR[v]; break;
+    }
+    F[v] = out;
+  }
+}
+
+}  // namespace amrvac

@@ -1,0 +1,352 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 finite-volume block update (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload ot128|ot256|kh256]
+
+A step is one full SSP-RK3 time step of the whole grid: setdt (CFL reduction
+on the device), three fused finite-volume stages, time update.  The default
+workload is 3-D ideal MHD Orszag-Tang at 128^3 (512 blocks of 16^3), HLLD,
+cada3, GLM, FP64, periodic.  `value` is zone-updates/s (interior cells x full
+steps / s) with the state resident in HBM, timed with CUDA events on the
+library's stream; N>1 runs independent replicas, one per GPU (weak scaling),
+with the max time over ranks.
+
+--impl reference times the reference algorithm's CPU implementation (the C++
+restatement in oracle/, all host threads) on a bounded sample of the same
+workload (a 1/8 sub-box with the same per-cell work), rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s on 1 B200, plain FP64 vs mixed/batched at fixed L1 err; adj/fwd"
+UNIT = "zone-updates/s"
+
+WORKLOADS = {
+    "ot128": dict(desc="3D ideal MHD Orszag-Tang 128^3, 512 blocks of 16^3, HLLD + cada3 + GLM, SSP-RK3, FP64, "
+                       "periodic", physics="mhd", n=128, ndim=3),
+    "ot256": dict(desc="3D ideal MHD Orszag-Tang 256^3, 4096 blocks of 16^3, HLLD + cada3 + GLM, SSP-RK3, FP64, "
+                       "periodic", physics="mhd", n=256, ndim=3),
+    "kh256": dict(desc="2D Euler Kelvin-Helmholtz 256^2, 256 blocks of 16^2, HLLC + vanleer, SSP-RK3, FP64, "
+                       "periodic", physics="hd", n=256, ndim=2),
+}
+
+# Algorithmic FP64 operations (+,-,*,/,sqrt,exp each 1) per cell for one
+# stage and for one getdt, counted by the oracle's counting scalar on the same
+# physics (tests/test_flop_counts.py recomputes and checks these numbers).
+ALG_FLOPS = {
+    "ot128": dict(stage=2047.0, getdt=86.5),
+    "ot256": dict(stage=2047.0, getdt=86.5),
+    "kh256": dict(stage=416.7, getdt=21.0),
+}
+# Per-launch DRAM traffic of the stage kernel from one ncu capture, bytes per
+# interior cell (profiles/fv_stage_*.md); None until captured.
+NCU_TRAFFIC_PER_CELL = {"ot128": None, "ot256": None, "kh256": None}
+
+
+def _cfg_kwargs(wl: str):
+    w = WORKLOADS[wl]
+    if w["physics"] == "mhd":
+        return dict(physics="mhd", ndim=3, ndir=3, flux_scheme="hlld", limiter="cada3", typedivbfix="glm",
+                    courantpar=0.8)
+    return dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hllc", limiter="vanleer", courantpar=0.8)
+
+
+def _initial_blocks(wl: str, n: int | None = None):
+    from tests import _problems as P
+    w = WORKLOADS[wl]
+    n = n or w["n"]
+    if w["physics"] == "mhd":
+        prim, geo = P.orszag_tang_3d(n=n)
+        cons = P.prim_to_cons(prim, "mhd", 3, 5.0 / 3.0)
+        return P.to_blocks(cons, 3), geo
+    prim, geo = P.kh_2d(n=n)
+    cons = P.prim_to_cons(prim, "hd", 2, 1.4)
+    return P.to_blocks(cons, 2), geo
+
+
+def _measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons of one GPU through NVML."""
+
+    def __init__(self, device_index: int):
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            import torch
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            try:
+                self.h = pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid) if not uuid.startswith("GPU") else uuid)
+            except Exception:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        nv = self.nv
+        names = {
+            "hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
+            "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+            "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+            "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4),
+        }
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for k, bit in names.items():
+                    if r & bit:
+                        self.reasons.add(k)
+            except Exception:
+                pass
+            self._stop.wait(0.05)
+
+    def __enter__(self):
+        if self.nv is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def _dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def _allmax(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline_sample(wl: str, nthreads: int, steps: int = 1):
+    """Time the oracle (C++ restatement, OpenMP) on a 1/8 sub-box of the workload."""
+    import oracle as O
+    w = WORKLOADS[wl]
+    n = w["n"] // 2
+    blocks, geo = _initial_blocks(wl, n=n)
+    kw = _cfg_kwargs(wl)
+    if w["physics"] == "mhd":
+        c = O.make_cfg(physics="mhd", ndim=3, ndir=3, flux_scheme="hlld", limiter="cada3", divb="glm",
+                       courantpar=0.8)
+    else:
+        c = O.make_cfg(physics="hd", ndim=2, gamma=1.4, flux_scheme="hllc", limiter="vanleer", courantpar=0.8)
+    del kw
+    g = O.Grid(c, geo["domain_nx"], geo["xprobmin"], geo["xprobmax"], ["periodic"] * (2 * w["ndim"]))
+    for ib in range(g.nblocks):
+        g.set_block(ib, blocks[ib])
+    g.getbc()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt, cg = g.getdt()
+        g.advance(dt, cg, nthreads)
+    el = time.perf_counter() - t0
+    cells = n ** w["ndim"]
+    return cells * steps / el, f"{steps} SSP-RK3 step(s) of the same physics on a {n}^{w['ndim']} periodic sub-box"
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_baseline_sample(args.workload, nthreads, 1)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, sample = cpu_baseline_sample(args.workload, nthreads, 1)
+        vals.append(v)
+    el = time.perf_counter() - t0
+    value = float(np.mean(vals))
+    w = WORKLOADS[args.workload]
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": w["desc"], "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    from amrvac_b200 import Context, make_cfg
+    from amrvac_b200.api import fp64_peak_tflops
+    wl = args.workload
+    w = WORKLOADS[wl]
+    blocks, geo = _initial_blocks(wl)
+    cfg = make_cfg(**_cfg_kwargs(wl))
+    ctx = Context(cfg)
+    ctx.set_uniform_grid(geo["domain_nx"], geo["xprobmin"], geo["xprobmax"])
+    ctx.upload(blocks)
+    cells = w["n"] ** w["ndim"]
+    nw = ctx.nw
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    # warm-up (also instantiates kernels / first-touch)
+    ctx.run_timed(max(args.warmup, 3))
+    if ctx.status():
+        raise SystemExit(f"bench.py: runtime status {ctx.status()} during warm-up")
+    # ---------------- timed region: K steps, per-kernel CUDA events on the library stream
+    _barrier(ws)
+    torch.cuda.synchronize()
+    l0 = ctx.launch_count()
+    with ClockSampler(local) as clk:
+        total_ms, stage_ms, getdt_ms = ctx.run_timed(args.steps)
+    torch.cuda.synchronize()
+    _barrier(ws)
+    launches = ctx.launch_count() - l0
+    st = ctx.status()
+    tmax = _allmax(total_ms, ws)
+    value = ws * cells * args.steps / (tmax * 1e-3)
+    nstage = 3 * args.steps
+    stage_avg_s = stage_ms * 1e-3 / nstage
+    peaks, peak_kind = _measured_peaks()
+    # algorithmic bytes of one stage launch: read wCT, read the RK base
+    # (stages 2 and 3), write wnew -> (2 + 3 + 3) / 3 * 8 * nw per cell on average
+    bytes_per_cell = (2 + 3 + 3) / 3.0 * 8 * nw
+    achieved_gbs = bytes_per_cell * cells / stage_avg_s / 1e9
+    traffic = NCU_TRAFFIC_PER_CELL.get(wl)
+    roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved_gbs / peaks["hbm_gbs"], "peak_source": peak_kind,
+                "traffic": None if traffic is None else traffic * cells,
+                "kernel": "fv_stage_kernel", "algorithmic_bytes_per_cell": bytes_per_cell,
+                "avg_launch_ms": stage_avg_s * 1e3, "launches": nstage}
+    fp64_peak = fp64_peak_tflops()
+    fl = ALG_FLOPS.get(wl, {}).get("stage")
+    roof64 = None
+    if fl:
+        ach = fl * cells / stage_avg_s / 1e12
+        roof64 = {"bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach / fp64_peak,
+                  "peak_source": "measured in-run (FP64 FMA chains)", "alg_flops_per_cell_stage": fl}
+    # ---------------- e2e through the public API with host buffers
+    e2e = None
+    try:
+        pinned = torch.empty(blocks.shape, dtype=torch.float64).pin_memory()
+        host = pinned.numpy()
+        host[...] = blocks
+        s = torch.cuda.ExternalStream(ctx.stream_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(s)
+        ctx.upload(host)
+        ctx.set_time(0.0, 1.0e99, 0.0)
+        for _ in range(args.steps):
+            ctx.step()
+            ctx.get_time()          # per-step D2H: dt, cmax_global, time
+            ctx.status()            # per-step D2H: status word
+        ctx.L.amrvac_gpu_download(ctx.h, 0, 0, ctx.nblocks, host.ctypes.data_as(
+            __import__("ctypes").POINTER(__import__("ctypes").c_double)))
+        e1.record(s)
+        e1.synchronize()
+        e2e_ms = _allmax(e0.elapsed_time(e1), ws)
+        state_bytes = blocks.nbytes
+        e2e = {"value": ws * cells * args.steps / (e2e_ms * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": (state_bytes + 32 * args.steps) / args.steps,
+               "d2h_bytes_per_step": (state_bytes + 28 * args.steps) / args.steps,
+               "what": "C-ABI from pinned host Fortran block arrays: upload of the initial state, K steps each "
+                       "with a host round trip (set_time in, dt/cmax/time/status out), download of the final "
+                       "state with ghost cells; state transfers amortised over K"}
+    except Exception as ex:  # report, do not hide
+        e2e = {"value": None, "unit": UNIT, "error": str(ex)}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        nthreads = os.cpu_count() or 1
+        v, sample = cpu_baseline_sample(wl, nthreads, 1)
+        cpu = {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample}
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tmax / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["desc"], "cells": cells, "blocks": ctx.nblocks, "nw": nw,
+                       "parallelism": "replicas" if ws > 1 else "single GPU",
+                       "l2": "no flush: working set %.0f MB (3 registers) > 126 MB L2" % (
+                           3 * cells * nw * 8 / 1e6),
+                       "stage_weighted_cell_updates_per_s": 3 * value},
+            "roofline": roofline, "roofline_fp64": roof64, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk.summary(), "status": st,
+            "kernel_ms": {"stage_total": stage_ms, "getdt_total": getdt_ms, "step_total": total_ms},
+        }
+        print(json.dumps(out))
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ot128", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local = _dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,208 @@
+/*
+ * amrvac_gpu.h — C ABI of the B200 finite-volume block update for MPI-AMRVAC.
+ *
+ * The library replaces the per-block loops of the reference's hot path:
+ *   - advect1's OpenMP block loop calling advect1_grid -> finite_volume
+ *     (src/mod_advance.t:611-666, src/mod_finite_volume.t:116-339),
+ *   - setdt's block loop calling getdt_courant (src/mod_dt.t:10-155, 160-287),
+ *   - getbc's same-resolution fill and physical cont/symm/asymm boundaries
+ *     (src/mod_ghostcells_update.t:350-615, 812-852),
+ *   - the SSP-RK stage algebra of advect (src/mod_advance.t:249-267).
+ * Physics follows the reference plugin interface (src/physics/mod_physics.t:
+ * phys_to_primitive/phys_to_conserved, phys_get_flux, phys_get_cbounds,
+ * phys_modify_wLR, phys_add_source, phys_handle_small_values).
+ *
+ * Conventions
+ *   - All entry points return int: 0 = OK, negative = configuration / usage
+ *     error (AMRVAC_E_*), positive = runtime status bits (AMRVAC_ST_*).
+ *   - Host arrays are the Fortran block arrays w(ixG^S,1:nw) (column-major,
+ *     x fastest, variable slowest, ghost cells included), one block after
+ *     another.  They are borrowed only for the duration of the call.
+ *   - The library owns all device memory.  One CUDA stream per context.
+ *     Calls on one context are not reentrant; call from one host thread.
+ *   - Block ids are 0-based.  neighbor[] holds, per block, 3^ndim entries
+ *     ordered with the x offset fastest ((di+1) + 3(dj+1) + 9(dk+1)); -1
+ *     marks a physical boundary (the reference's neighbor_type==1).
+ */
+#ifndef AMRVAC_GPU_H
+#define AMRVAC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* configuration errors */
+#define AMRVAC_E_ARG          (-1)  /* bad argument / null pointer */
+#define AMRVAC_E_UNSUPPORTED  (-2)  /* option outside this library's scope */
+#define AMRVAC_E_CUDA         (-3)  /* CUDA runtime error (see amrvac_gpu_last_error) */
+#define AMRVAC_E_STATE        (-4)  /* call order (e.g. no blocks set) */
+/* runtime status bits (OR-ed, sticky until amrvac_gpu_clear_status) */
+#define AMRVAC_ST_SMALL_VALUE  1u   /* small density/pressure (the reference's crash) */
+#define AMRVAC_ST_NAN          2u
+#define AMRVAC_ST_DT_TOO_SMALL 4u   /* dt < dtmin (src/mod_dt.t:55-60) */
+
+/* flux_scheme (src/mod_finite_volume.t method ids are private; names match) */
+#define AMRVAC_FS_TVDLF 1
+#define AMRVAC_FS_HLL   2
+#define AMRVAC_FS_HLLC  3
+#define AMRVAC_FS_HLLD  4
+/* limiter ids: src/limiter/mod_limiter.t:14-24 */
+#define AMRVAC_LIM_MINMOD   1
+#define AMRVAC_LIM_WOODWARD 2
+#define AMRVAC_LIM_MCBETA   3
+#define AMRVAC_LIM_SUPERBEE 4
+#define AMRVAC_LIM_VANLEER  5
+#define AMRVAC_LIM_ALBADA   6
+#define AMRVAC_LIM_KOREN    7
+#define AMRVAC_LIM_CADA     8
+#define AMRVAC_LIM_CADA3    9
+/* typeboundspeed: src/io/mod_input_output.t:1632-1641 */
+#define AMRVAC_BS_EINFELDT      1
+#define AMRVAC_BS_CMAXMEAN      2
+#define AMRVAC_BS_CMAXLEFTRIGHT 3
+/* typedivbfix: src/mhd/mod_mhd_phys.t divb_* ids */
+#define AMRVAC_DIVB_NONE  0
+#define AMRVAC_DIVB_GLM   1
+#define AMRVAC_DIVB_LINDE 4
+/* typecourant: mod_global_parameters type_maxsum/type_summax/type_minimum */
+#define AMRVAC_COURANT_MAXSUM  1
+#define AMRVAC_COURANT_SUMMAX  2
+#define AMRVAC_COURANT_MINIMUM 3
+/* typeboundary per side and variable: subset of mod_boundary_conditions bc_* */
+#define AMRVAC_BC_PERIODIC 0
+#define AMRVAC_BC_CONT     1
+#define AMRVAC_BC_SYMM     2
+#define AMRVAC_BC_ASYMM    3
+/* time_stepper / time_integrator (src/mod_advance.t:56-567) */
+#define AMRVAC_TS_ONESTEP   1   /* Forward_Euler */
+#define AMRVAC_TS_TWOSTEP   2   /* ssprk2 (Heun) */
+#define AMRVAC_TS_THREESTEP 3   /* ssprk3, ssprk_order 3 or 2 */
+
+#define AMRVAC_MAX_NW 16
+
+/* Mirrors the par-file namelist variables the path reads (methodlist,
+ * boundlist, meshlist, paramlist, hd_list / mhd_list). */
+typedef struct amrvac_cfg {
+  int ndim;                 /* 2 or 3 (1-D: see amrvac_gpu_create) */
+  int ndir;                 /* vector components (2.5D: ndim=2, ndir=3) */
+  int physics;              /* 0 = hd, 1 = mhd */
+  int block_nx[3];          /* block_nx^D; this build requires 16 */
+  int nghostcells;          /* ghost width of the host arrays (2) */
+  double gamma;             /* hd_gamma / mhd_gamma */
+  int flux_scheme;          /* AMRVAC_FS_* (one for all levels) */
+  int limiter;              /* AMRVAC_LIM_* */
+  int typeboundspeed;       /* AMRVAC_BS_* */
+  int typedivbfix;          /* AMRVAC_DIVB_* (mhd) */
+  double mhd_glm_alpha;     /* 0.5 */
+  int mhd_glm_extended;     /* 1 */
+  double divbdiff;          /* 0.8 (Linde) */
+  double courantpar;        /* 0.8 */
+  int type_courant;         /* AMRVAC_COURANT_* */
+  double cada3_radius;      /* 0.1 */
+  double tvdlfeps;          /* 1.0 */
+  int fix_small_values;     /* 0 */
+  int check_small_values;   /* 1 */
+  int small_values_method;  /* 0 = error, 1 = replace */
+  double small_density, small_pressure;
+  int time_stepper;         /* AMRVAC_TS_* */
+  int ssprk_order;          /* 3 */
+  double dtmin;             /* 1e-10 */
+  int typeboundary[6][AMRVAC_MAX_NW]; /* [min1,max1,min2,max2,min3,max3][iw] */
+  int zchunk;               /* tuning: z-planes per CTA in 3-D (0 = auto) */
+} amrvac_cfg;
+
+typedef struct amrvac_ctx amrvac_ctx;
+
+/* Fill *cfg with the reference defaults (src/io/mod_input_output.t:284-480). */
+void amrvac_gpu_default_cfg(amrvac_cfg *cfg);
+/* Number of conserved variables (nwflux) implied by cfg. */
+int amrvac_gpu_nw(const amrvac_cfg *cfg);
+
+/* Create a context on the current CUDA device.  Refuses unsupported options
+ * (AMRVAC_E_UNSUPPORTED): block_nx != 16, 1-D, mhd hllc, 3-D Linde, ndir=1 mhd. */
+int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **ctx);
+int amrvac_gpu_destroy(amrvac_ctx *ctx);
+
+/* Define the block set (replaces the host's ps(:) list for the path).
+ * dx: [nblocks][ndim] cell sizes (rnode(rpdx^D_,igrid)); neighbor as above. */
+int amrvac_gpu_set_blocks(amrvac_ctx *ctx, int nblocks, const double *dx, const int *neighbor);
+/* Convenience: uniform level-1 grid, blocks ordered x fastest; periodicity
+ * from cfg->typeboundary. */
+int amrvac_gpu_set_uniform_grid(amrvac_ctx *ctx, const int *domain_nx, const double *xprobmin,
+                                const double *xprobmax);
+int amrvac_gpu_nblocks(const amrvac_ctx *ctx);
+
+/* Copy n blocks starting at `first` between host Fortran arrays and register
+ * reg (0 = ps, 1 = ps1, 2 = ps2).  Upload reads interior cells only; download
+ * fills ghost cells as getbc would (same-resolution copy + physical BC). */
+int amrvac_gpu_upload(amrvac_ctx *ctx, int reg, int first, int n, const double *w);
+int amrvac_gpu_download(amrvac_ctx *ctx, int reg, int first, int n, double *w);
+
+/* getdt_courant over all blocks of register reg: CFL dt (before any output /
+ * time_max clipping) and cmax_global.  Synchronous. */
+int amrvac_gpu_getdt(amrvac_ctx *ctx, int reg, double *dt, double *cmax_global);
+
+/* One explicit stage (advect1 on all blocks):
+ *   w[reg_new] = a_base*w[reg_base] + b_in*w[reg_ct]  (a_base==0: = w[reg_ct])
+ *   then finite_volume(qdt=dtfactor*dt) with wCT = w[reg_ct] and sources.
+ * Uses cmax_global from the last getdt / set_cmax_global.  Asynchronous. */
+int amrvac_gpu_advect1(amrvac_ctx *ctx, int reg_ct, int reg_new, int reg_base, double a_base,
+                       double b_in, double dtfactor, double dt);
+int amrvac_gpu_set_cmax_global(amrvac_ctx *ctx, double cmax_global);
+
+/* Time control for amrvac_gpu_step: current time, time_max (final_dt_reduction)
+ * and one output interval dtsave (0 = none), as in setdt (src/mod_dt.t:69-99). */
+int amrvac_gpu_set_time(amrvac_ctx *ctx, double global_time, double time_max, double dtsave);
+/* One full time step on register 0: setdt on the device, the configured RK
+ * stages, global_time += dt.  Asynchronous; no host round trip. */
+int amrvac_gpu_step(amrvac_ctx *ctx);
+/* nsteps steps, captured once into a CUDA graph and replayed. */
+int amrvac_gpu_run(amrvac_ctx *ctx, int nsteps);
+/* nsteps steps launched directly (no graph) with CUDA events recorded on the
+ * context stream around every kernel; returns the whole elapsed time and the
+ * summed durations of the stage kernels and of the getdt kernels (ms).
+ * Synchronises.  Used for live per-kernel timing inside a benchmark. */
+int amrvac_gpu_run_timed(amrvac_ctx *ctx, int nsteps, double *total_ms, double *stage_ms, double *getdt_ms);
+/* Measured FP64 FMA throughput of the current device (TFLOP/s, 2 flops per
+ * FMA) from an in-register FMA-chain kernel; the FP64 roofline denominator. */
+int amrvac_gpu_fp64_peak(double *tflops);
+/* Read back the last step's dt, cmax_global and global_time (synchronises). */
+int amrvac_gpu_get_time(amrvac_ctx *ctx, double *dt, double *cmax_global, double *global_time);
+
+/* Status word (OR of AMRVAC_ST_*), sticky.  Synchronises. */
+int amrvac_gpu_status(amrvac_ctx *ctx, uint32_t *flags);
+int amrvac_gpu_clear_status(amrvac_ctx *ctx);
+int amrvac_gpu_synchronize(amrvac_ctx *ctx);
+/* The context's cudaStream_t (as void*), for event timing by the caller. */
+int amrvac_gpu_stream(amrvac_ctx *ctx, void **stream);
+/* Device pointer of register reg (layout pool[block][var][z][y][x], 16^ndim). */
+int amrvac_gpu_register_ptr(amrvac_ctx *ctx, int reg, double **dptr);
+/* Number of kernel launches issued by this context since creation. */
+int64_t amrvac_gpu_launch_count(const amrvac_ctx *ctx);
+/* Text of the last error on this thread (empty if none). */
+const char *amrvac_gpu_last_error(void);
+
+/* Per-routine entry points over n independent faces / states (host arrays,
+ * state-major [n][nw]); used to test phys_get_flux (mhd 3810-3889 / hd
+ * 1097-1146), phys_get_cbounds (mhd 3037-3127 / hd 891-1001) and the
+ * Riemann solvers (src/mod_finite_volume.t:348-729) one routine at a time.
+ * idim is 1-based as in the reference. */
+int amrvac_gpu_get_flux_points(amrvac_ctx *ctx, int n, const double *wc, const double *wp, int idim,
+                               double cmax_global, double *f);
+int amrvac_gpu_get_cbounds_points(amrvac_ctx *ctx, int n, const double *wlc, const double *wrc,
+                                  const double *wlp, const double *wrp, int idim, double *cmax,
+                                  double *cmin);
+int amrvac_gpu_riemann_points(amrvac_ctx *ctx, int n, const double *wlp, const double *wrp, int idim,
+                              double cmax_global, double *f);
+
+/* Same-resolution ghost-fill index maps ixS_srl_ / ixR_srl_ of init_bc
+ * (src/mod_ghostcells_update.t:150-162), 0-based inclusive, for i=-1,0,1
+ * at index i+1. */
+int amrvac_gpu_srl_maps(int nghost, int block_nx, int *s_min, int *s_max, int *r_min, int *r_max);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AMRVAC_GPU_H */

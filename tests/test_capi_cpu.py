@@ -1,0 +1,130 @@
+"""CPU-only checks of the C ABI library and the host layer (no GPU calls)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from amrvac_b200 import build, _lib
+    build.build()
+    return _lib.load()
+
+
+def test_library_exports_every_declared_symbol(lib):
+    """Every function declared in include/amrvac_gpu.h is exported by the .so."""
+    with open(os.path.join(ROOT, "include", "amrvac_gpu.h")) as f:
+        text = f.read()
+    names = set(re.findall(r"\b(amrvac_gpu_\w+)\s*\(", text))
+    assert len(names) >= 25
+    for n in sorted(names):
+        assert hasattr(lib, n), n
+    from amrvac_b200 import _lib
+    assert {s[0] for s in _lib.SIGNATURES} == names
+
+
+def test_default_cfg_matches_reference_defaults(lib):
+    from amrvac_b200 import _lib
+    c = _lib.AmrvacCfg()
+    lib.amrvac_gpu_default_cfg(ctypes.byref(c))
+    assert c.courantpar == 0.8 and c.cada3_radius == 0.1 and c.tvdlfeps == 1.0
+    assert c.nghostcells == 2 and list(c.block_nx) == [16, 16, 16]
+    assert c.typeboundspeed == 1 and c.mhd_glm_alpha == 0.5 and c.divbdiff == 0.8
+    assert c.dtmin == 1e-10 and c.limiter == 1
+
+
+@pytest.mark.parametrize("ng,nx", [(2, 16), (3, 16), (2, 8), (4, 16)])
+def test_srl_maps_match_oracle(lib, oracle_lib, ng, nx):
+    from amrvac_b200 import srl_maps
+    ours = srl_maps(ng, nx)
+    ref = oracle_lib.srl_maps(ng, nx)
+    for a, b in zip(ours, ref):
+        assert np.array_equal(a, b)
+
+
+def test_nw(lib):
+    from amrvac_b200 import make_cfg
+    assert lib.amrvac_gpu_nw(ctypes.byref(make_cfg(physics="hd", ndim=2))) == 4
+    assert lib.amrvac_gpu_nw(ctypes.byref(make_cfg(physics="mhd", ndim=3, typedivbfix="glm"))) == 9
+    assert lib.amrvac_gpu_nw(ctypes.byref(make_cfg(physics="mhd", ndim=2, ndir=3, typedivbfix="linde"))) == 8
+
+
+def test_unsupported_configurations_are_refused_without_gpu(lib):
+    """Config errors come back as negative codes before any CUDA call."""
+    from amrvac_b200 import make_cfg, _lib
+    h = ctypes.c_void_p()
+    bad = [make_cfg(physics="mhd", ndim=3, flux_scheme="hllc"),
+           make_cfg(physics="mhd", ndim=3, typedivbfix="linde", flux_scheme="hll"),
+           make_cfg(physics="hd", ndim=2, flux_scheme="hlld")]
+    c = make_cfg(physics="hd", ndim=2)
+    c.block_nx[0] = 8
+    bad.append(c)
+    for cfg in bad:
+        r = lib.amrvac_gpu_create(ctypes.byref(cfg), ctypes.byref(h))
+        assert r == _lib.E_UNSUPPORTED, lib.amrvac_gpu_last_error()
+
+
+def test_par_namelist_parser():
+    from amrvac_b200 import parse_namelists
+    text = """
+ &methodlist
+        time_stepper  = 'threestep'
+        flux_scheme =    20*'hlld'
+        limiter=  20*'cada3'
+        typeboundspeed  = 'cmaxmean'
+ /
+ &meshlist
+        domain_nx1    = 128
+        xprobmin1     = -1.d0
+        w_refine_weight(1)=0.5d0
+ /
+ &paramlist
+        courantpar = 0.9
+ /
+"""
+    nl = parse_namelists(text)
+    assert nl["methodlist"]["flux_scheme"] == ["hlld"] * 20
+    assert nl["methodlist"]["time_stepper"] == "threestep"
+    assert nl["meshlist"]["domain_nx1"] == 128
+    assert nl["meshlist"]["xprobmin1"] == -1.0
+    assert nl["meshlist"]["w_refine_weight"] == {1: 0.5}
+    assert nl["paramlist"]["courantpar"] == 0.9
+
+
+def test_config_from_par(tmp_path):
+    from amrvac_b200 import config_from_par
+    p = tmp_path / "kh.par"
+    p.write_text("""
+ &stoplist
+    time_max = 1.0
+ /
+ &methodlist
+    time_stepper = 'threestep'
+    flux_scheme = 20*'hllc'
+    limiter = 20*'vanleer'
+ /
+ &boundlist
+    typeboundary_min1 = 4*'periodic'
+    typeboundary_max1 = 4*'periodic'
+    typeboundary_min2 = 4*'periodic'
+    typeboundary_max2 = 4*'periodic'
+ /
+ &meshlist
+    domain_nx1 = 256
+    domain_nx2 = 256
+    xprobmin2 = -0.5
+    xprobmax2 = 0.5
+ /
+ &hd_list
+    hd_gamma = 1.4
+ /
+""")
+    rc = config_from_par([str(p)])
+    assert rc.physics == "hd" and rc.domain_nx == [256, 256]
+    assert rc.cfg.flux_scheme == 3 and rc.cfg.limiter == 5 and rc.cfg.gamma == 1.4
+    assert rc.cfg.time_stepper == 3 and rc.xprobmin == [0.0, -0.5]

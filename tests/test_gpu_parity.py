@@ -1,0 +1,325 @@
+"""GPU parity against the CPU oracle (restatement of the reference Fortran).
+
+Bars (north star): plain FP64 path <= 1e-12 relative per cell on identical
+inputs (FMA contraction is the only reordering); ghost-cell index maps and
+ghost fill bit-exact; conservation to rounding on periodic domains.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from tests import _problems as P
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+def _cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+CASES = {
+    "hd2_hllc_vanleer": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hllc", limiter="vanleer"),
+    "hd2_hll_minmod": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll", limiter="minmod"),
+    "hd2_tvdlf_koren_cmaxmean": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="tvdlf", limiter="koren",
+                                     typeboundspeed="cmaxmean"),
+    "hd2_hllc_woodward_cmaxlr": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hllc", limiter="woodward",
+                                     typeboundspeed="cmaxleftright"),
+    "hd3_hllc_mcbeta": dict(physics="hd", ndim=3, gamma=1.4, flux_scheme="hllc", limiter="mcbeta"),
+    "hd3_hll_cada3": dict(physics="hd", ndim=3, gamma=1.4, flux_scheme="hll", limiter="cada3"),
+    "mhd3_hlld_cada3_glm": dict(physics="mhd", ndim=3, flux_scheme="hlld", limiter="cada3", typedivbfix="glm"),
+    "mhd3_hll_vanleer_glm": dict(physics="mhd", ndim=3, flux_scheme="hll", limiter="vanleer", typedivbfix="glm"),
+    "mhd3_hlld_superbee_none": dict(physics="mhd", ndim=3, flux_scheme="hlld", limiter="superbee",
+                                    typedivbfix="none"),
+    "mhd25_hlld_cada3_glm": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hlld", limiter="cada3",
+                                 typedivbfix="glm"),
+    "mhd25_hll_cada3_linde_cmaxmean": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hll", limiter="cada3",
+                                           typedivbfix="linde", typeboundspeed="cmaxmean"),
+    "mhd2_tvdlf_albada_linde": dict(physics="mhd", ndim=2, ndir=2, flux_scheme="tvdlf", limiter="albada",
+                                    typedivbfix="linde"),
+    "mhd25_hlld_cada_glm_lr": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hlld", limiter="cada",
+                                   typedivbfix="glm", typeboundspeed="cmaxleftright", mhd_glm_extended=False),
+}
+
+
+def _oracle_cfg(O, kw, bc_names):
+    k = dict(kw)
+    div = k.pop("typedivbfix", "none")
+    ext = k.pop("mhd_glm_extended", True)
+    return O.make_cfg(divb=div, glm_extended=ext, **k)
+
+
+def _setup(oracle_lib, name, n=32, bc=None, seed=P.SEED):
+    from amrvac_b200 import Context, make_cfg
+    O = oracle_lib
+    kw = CASES[name]
+    ndim = kw["ndim"]
+    ndir = kw.get("ndir", ndim)
+    bc = bc or ["periodic"] * (2 * ndim)
+    gcfg = make_cfg(typeboundary=bc, **kw)
+    ocfg = _oracle_cfg(O, kw, bc)
+    glm = kw.get("typedivbfix") == "glm"
+    prim = P.random_smooth(kw["physics"], ndim, ndir, n, seed=seed, glm=glm)
+    cons = P.prim_to_cons(prim, kw["physics"], ndir, ocfg.gamma)
+    blocks = P.to_blocks(cons, ndim)
+    dom = [n] * ndim
+    og = O.Grid(ocfg, dom, [0.0] * ndim, [1.0] * ndim, [b if isinstance(b, str) else b[0] for b in bc])
+    for ib in range(og.nblocks):
+        og.set_block(ib, blocks[ib])
+    og.getbc()
+    ctx = Context(gcfg)
+    ctx.set_uniform_grid(dom, [0.0] * ndim, [1.0] * ndim)
+    assert ctx.nblocks == og.nblocks
+    ctx.upload(blocks)
+    return O, ocfg, og, ctx
+
+
+def _maxrel(a, b):
+    """max over cells of |a-b| / (|b| + 1e-3*max|b_v|) per variable."""
+    out = 0.0
+    for v in range(a.shape[1]):
+        scale = np.abs(b[:, v]).max() + 1e-300
+        r = np.abs(a[:, v] - b[:, v]) / (np.abs(b[:, v]) + 1e-3 * scale)
+        out = max(out, float(r.max()))
+    return out
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_ghost_fill_bit_exact(oracle_lib, name):
+    _cuda()
+    O, ocfg, og, ctx = _setup(oracle_lib, name)
+    ref = np.array([og.get_block(ib) for ib in range(og.nblocks)])
+    got = ctx.download()
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("bc", [["cont"] * 4, ["cont", "cont", "periodic", "periodic"], ["symm"] * 4,
+                                ["periodic", "periodic", "symm", "cont"]])
+def test_ghost_fill_physical_boundaries(oracle_lib, bc):
+    """Download fills ghosts like getbc with cont/symm sides, bit-exact."""
+    _cuda()
+    O, ocfg, og, ctx = _setup(oracle_lib, "hd2_hll_minmod", n=48, bc=bc)
+    ref = np.array([og.get_block(ib) for ib in range(og.nblocks)])
+    assert np.array_equal(ctx.download(), ref)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_stage_matches_oracle(oracle_lib, name):
+    """One advect1 stage (ps -> ps1, dtfactor 1) on identical block inputs."""
+    _cuda()
+    O, ocfg, og, ctx = _setup(oracle_lib, name)
+    dt, cg = og.getdt()
+    dt *= 0.5
+    ctx.set_cmax_global(cg)
+    st = ctx.advect1("ps", "ps1", 1.0, dt)
+    assert st == 0
+    got = P.interior(ctx.download("ps1"), ocfg.ndim)
+    ref = []
+    dx = og.dx()
+    for ib in range(og.nblocks):
+        w = og.get_block(ib)
+        wn = w.copy()
+        O.finite_volume(ocfg, w, wn, dt, dx, cg)
+        ref.append(wn)
+    ref = P.interior(np.array(ref), ocfg.ndim)
+    err = _maxrel(got, ref)
+    assert err <= RTOL, f"{name}: max rel err {err:.3e}"
+    assert ctx.status() == 0
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_full_step_matches_oracle(oracle_lib, name):
+    """setdt + all SSP-RK3 stages on the device vs the oracle's advance."""
+    _cuda()
+    O, ocfg, og, ctx = _setup(oracle_lib, name)
+    dt_ref, cg_ref = og.getdt()
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.step()
+    dt, cg, t = ctx.get_time()
+    assert abs(dt - dt_ref) <= 1e-13 * dt_ref
+    assert abs(cg - cg_ref) <= 1e-13 * cg_ref
+    assert t == dt
+    og.advance(dt_ref, cg_ref)
+    got = P.interior(ctx.download("ps"), ocfg.ndim)
+    ref = P.interior(np.array([og.get_block(ib) for ib in range(og.nblocks)]), ocfg.ndim)
+    err = _maxrel(got, ref)
+    assert err <= RTOL, f"{name}: max rel err {err:.3e}"
+
+
+@pytest.mark.parametrize("name", ["hd2_hllc_vanleer", "mhd3_hlld_cada3_glm", "mhd25_hll_cada3_linde_cmaxmean"])
+def test_ten_steps_graph_replay(oracle_lib, name):
+    """run(10): one captured step replayed 10 times == 10 oracle steps."""
+    _cuda()
+    O, ocfg, og, ctx = _setup(oracle_lib, name)
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.run(10)
+    for _ in range(10):
+        dt, cg = og.getdt()
+        og.advance(dt, cg)
+    got = P.interior(ctx.download("ps"), ocfg.ndim)
+    ref = P.interior(np.array([og.get_block(ib) for ib in range(og.nblocks)]), ocfg.ndim)
+    assert _maxrel(got, ref) <= 1e-10
+
+
+@pytest.mark.parametrize("name", ["hd2_hllc_vanleer", "hd3_hllc_mcbeta"])
+def test_conservation_periodic(oracle_lib, name):
+    _cuda()
+    O, ocfg, og, ctx = _setup(oracle_lib, name)
+    before = P.interior(ctx.download(), ocfg.ndim).sum(axis=(0, 2, 3, 4))
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.run(5)
+    after = P.interior(ctx.download(), ocfg.ndim).sum(axis=(0, 2, 3, 4))
+    scale = np.abs(P.interior(ctx.download(), ocfg.ndim)).sum(axis=(0, 2, 3, 4))
+    assert np.all(np.abs(after - before) <= 1e-13 * scale)
+
+
+def test_mass_conservation_mhd_glm(oracle_lib):
+    _cuda()
+    O, ocfg, og, ctx = _setup(oracle_lib, "mhd3_hlld_cada3_glm")
+    m0 = P.interior(ctx.download(), 3)[:, 0].sum()
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.run(3)
+    m1 = P.interior(ctx.download(), 3)[:, 0].sum()
+    assert abs(m1 - m0) <= 1e-13 * abs(m0)
+
+
+def test_stage_with_cont_boundaries(oracle_lib):
+    _cuda()
+    bc = ["cont", "cont", "cont", "cont"]
+    O, ocfg, og, ctx = _setup(oracle_lib, "hd2_hllc_vanleer", n=48, bc=bc)
+    dt, cg = og.getdt()
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.step()
+    og.advance(og.getdt()[0], 0.0)
+    got = P.interior(ctx.download(), 2)
+    ref = P.interior(np.array([og.get_block(ib) for ib in range(og.nblocks)]), 2)
+    assert _maxrel(got, ref) <= RTOL
+
+
+def test_stage_with_mirror_boundaries(oracle_lib):
+    """symm on all sides: ghost values mirrored; stage parity with the oracle."""
+    _cuda()
+    bc = ["symm"] * 4
+    O, ocfg, og, ctx = _setup(oracle_lib, "hd2_hll_minmod", n=32, bc=bc)
+    ref_g = np.array([og.get_block(ib) for ib in range(og.nblocks)])
+    assert np.array_equal(ctx.download(), ref_g)
+    dt, cg = og.getdt()
+    ctx.advect1("ps", "ps1", 1.0, dt)
+    got = P.interior(ctx.download("ps1"), 2)
+    ref = []
+    for ib in range(og.nblocks):
+        w = og.get_block(ib)
+        wn = w.copy()
+        O.finite_volume(ocfg, w, wn, dt, og.dx(), 0.0)
+        ref.append(wn)
+    assert _maxrel(got, P.interior(np.array(ref), 2)) <= RTOL
+
+
+# ---------------------------------------------------------------- per routine
+def _rand_states(rng, n, physics, ndir, glm):
+    nw = (2 * ndir + 2 + (1 if glm else 0)) if physics == "mhd" else ndir + 2
+    w = np.zeros((n, nw))
+    w[:, 0] = rng.uniform(0.2, 3.0, n)
+    w[:, 1:1 + ndir] = rng.uniform(-2, 2, (n, ndir))
+    w[:, ndir + 1] = rng.uniform(0.1, 5.0, n)
+    if physics == "mhd":
+        w[:, ndir + 2:2 * ndir + 2] = rng.uniform(-1.5, 1.5, (n, ndir))
+        if glm:
+            w[:, -1] = rng.uniform(-0.2, 0.2, n)
+    return w
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_riemann_points(oracle_lib, name):
+    """Riemann flux per face from L/R primitive states (no reconstruction)."""
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    O = oracle_lib
+    kw = CASES[name]
+    ndim, ndir = kw["ndim"], kw.get("ndir", kw["ndim"])
+    glm = kw.get("typedivbfix") == "glm"
+    ctx = Context(make_cfg(**kw))
+    ocfg = _oracle_cfg(O, kw, None)
+    rng = np.random.default_rng(7)
+    n = 4096
+    wl = _rand_states(rng, n, kw["physics"], ndir, glm)
+    wr = _rand_states(rng, n, kw["physics"], ndir, glm)
+    # one third of faces nearly continuous (exercises the smooth branches)
+    wr[: n // 3] = wl[: n // 3] * (1 + 1e-3 * rng.standard_normal((n // 3, wl.shape[1])))
+    for idim in range(1, ndim + 1):
+        got = ctx.riemann_points(wl, wr, idim, cmax_global=2.5)
+        ref = np.zeros_like(wl)
+        lib = O.lib()
+        lib.orc_riemann_points(ctypes.byref(ocfg), n, O._dp(np.ascontiguousarray(wl)),
+                               O._dp(np.ascontiguousarray(wr)), idim, 2.5, O._dp(ref))
+        scale = np.abs(ref).max(axis=0) + 1e-300
+        err = (np.abs(got - ref) / (np.abs(ref) + 1e-6 * scale)).max()
+        assert err <= 1e-11, f"{name} idim={idim}: {err:.3e}"
+
+
+@pytest.mark.parametrize("physics,ndir,glm", [("hd", 2, False), ("hd", 3, False), ("mhd", 3, True),
+                                              ("mhd", 3, False), ("mhd", 2, False)])
+def test_flux_and_cbounds_points(oracle_lib, physics, ndir, glm):
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    O = oracle_lib
+    ndim = min(ndir, 3) if physics == "hd" else 2
+    for bs in ("Einfeldt", "cmaxmean", "cmaxleftright"):
+        kw = dict(physics=physics, ndim=ndim if physics == "mhd" else ndir, ndir=ndir, flux_scheme="hll",
+                  typeboundspeed=bs, typedivbfix=("glm" if glm else "none") if physics == "mhd" else None)
+        if physics == "hd":
+            kw.pop("typedivbfix")
+        ctx = Context(make_cfg(**kw))
+        okw = dict(kw)
+        okw.pop("typedivbfix", None)
+        ocfg = O.make_cfg(divb=("glm" if glm else "none"), **okw)
+        rng = np.random.default_rng(11)
+        n = 2048
+        wlp = _rand_states(rng, n, physics, ndir, glm)
+        wrp = _rand_states(rng, n, physics, ndir, glm)
+        conv = O.lib().orc_to_conserved
+        wlc = wlp.copy()
+        wrc = wrp.copy()
+        for idim in range(1, ndir + 1):
+            f = ctx.get_flux_points(wlc, wlp, idim, 1.7)
+            fr = np.zeros_like(f)
+            O.lib().orc_get_flux_points(ctypes.byref(ocfg), n, O._dp(wlc), O._dp(wlp), idim, 1.7, O._dp(fr))
+            assert np.allclose(f, fr, rtol=1e-13, atol=1e-13)
+        for idim in range(1, ndim + 1):
+            cmax, cmin = ctx.get_cbounds_points(wlc, wrc, wlp, wrp, idim)
+            rmax = np.zeros(n)
+            rmin = np.zeros(n)
+            O.lib().orc_get_cbounds_points(ctypes.byref(ocfg), n, O._dp(wlc), O._dp(wrc), O._dp(wlp), O._dp(wrp),
+                                           idim, O._dp(rmax), O._dp(rmin))
+            assert np.allclose(cmax, rmax, rtol=1e-13, atol=1e-13)
+            assert np.allclose(cmin, rmin, rtol=1e-13, atol=1e-13)
+        del conv
+
+
+# ---------------------------------------------------------------- failure detection
+def test_small_value_error_sets_status_and_restores(oracle_lib):
+    """fix_small_values with method 'error': a planted negative density sets
+    the SMALL_VALUE status and the block is restored to wCT
+    (src/mod_finite_volume.t:326-333)."""
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    n = 32
+    prim = P.random_smooth("hd", 2, 2, n)
+    prim[0, 0, 5, 5] = -1.0
+    cons = P.prim_to_cons(prim, "hd", 2, 1.4)
+    blocks = P.to_blocks(cons, 2)
+    ctx = Context(make_cfg(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll", fix_small_values=True,
+                           small_density=1e-8, small_pressure=1e-8))
+    ctx.set_uniform_grid([n, n], [0, 0], [1, 1])
+    ctx.upload(blocks)
+    st = ctx.advect1("ps", "ps1", 1.0, 1e-4)
+    assert ctx.status() & 1
+    out = P.interior(ctx.download("ps1"), 2)
+    assert np.array_equal(out[0], P.interior(blocks, 2)[0])
+    ctx.clear_status()
+    assert ctx.status() == 0
+    del st
