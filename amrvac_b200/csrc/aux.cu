@@ -75,6 +75,10 @@ __global__ void pack_kernel(const double *__restrict__ pool, double *__restrict_
     int src = b;
     if (dir[0] | dir[1] | dir[2]) {
       src = nbr[b * 27 + (dir[0] + 1) + 3 * (dir[1] + 1) + 9 * (dir[2] + 1)];
+      if (src < 0) {  // inconsistent neighbour table: never read out of bounds
+        for (int v = 0; v < nw; ++v) dst[((size_t)lb * nw + v) * per_block_g + (e - (size_t)lb * per_block_g)] = 0.0;
+        continue;
+      }
       for (int d = 0; d < ndim; ++d) {
         if (!dir[d]) continue;
         // receiver region ixR_srl_(dir) <- sender region ixS_srl_(-dir)

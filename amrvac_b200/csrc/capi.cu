@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -250,7 +251,8 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   c->cfg = k;
   c->nw = nw;
   KernelKey key{k.physics == 1, k.ndim, k.ndir, k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM,
-                k.flux_scheme};
+                k.flux_scheme, k.limiter, k.typeboundspeed};
+  if (std::getenv("AMRVAC_GENERIC_KERNELS")) { key.limiter = 0; key.boundspeed = 0; }
   bool found = lookup_hd(key, &c->ks) || lookup_mhd2(key, &c->ks) || lookup_mhd3(key, &c->ks);
   if (!found) {
     delete c;
@@ -385,6 +387,22 @@ int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const in
         if (v < 0 && c->bc.kind[2 * d + s] == BCK_PERIODIC)
           return fail(AMRVAC_E_ARG, "physical boundary on a side declared periodic");
       }
+  // every direction whose face components all lead to siblings must exist
+  for (int b = 0; b < nblocks; ++b)
+    for (int q = 0; q < 27; ++q) {
+      const int o[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
+      bool inner = true, any = false;
+      for (int d = 0; d < 3; ++d) {
+        if (!o[d]) continue;
+        if (d >= nd) { inner = false; break; }
+        any = true;
+        int f[3] = {0, 0, 0};
+        f[d] = o[d];
+        if (nbr[(size_t)b * 27 + (f[0] + 1) + 3 * (f[1] + 1) + 9 * (f[2] + 1)] < 0) inner = false;
+      }
+      if (any && inner && nbr[(size_t)b * 27 + q] < 0)
+        return fail(AMRVAC_E_ARG, "missing edge/corner neighbour between two sibling faces");
+    }
   cudaStreamSynchronize(c->stream);
   for (int r = 0; r < 3; ++r) { cudaFree(c->pool[r]); c->pool[r] = nullptr; }
   cudaFree(c->d_nbr); cudaFree(c->d_dx); cudaFree(c->d_block_status);

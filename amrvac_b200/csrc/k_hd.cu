@@ -5,6 +5,11 @@ namespace amrvac {
 
 bool lookup_hd(const KernelKey &k, KernelSet *out) {
   if (k.mhd || k.ndir != k.ndim) return false;
+  // compile-time limiter / bound speed for the 2-D Kelvin-Helmholtz configuration
+  if (k.ndim == 2 && k.solver == SOLVER_HLLC && k.limiter == LIM_VANLEER && k.boundspeed == BS_EINFELDT) {
+    *out = Launch<false, 2, false, 2, SOLVER_HLLC, LIM_VANLEER, BS_EINFELDT>::set();
+    return true;
+  }
 #define AMRVAC_HD(ND, S)                                        \
   if (k.ndim == ND && k.solver == S) {                          \
     *out = Launch<false, ND, false, ND, S>::set();              \

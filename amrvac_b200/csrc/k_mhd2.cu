@@ -5,6 +5,11 @@ namespace amrvac {
 
 bool lookup_mhd2(const KernelKey &k, KernelSet *out) {
   if (!k.mhd || k.ndim != 2) return false;
+  // compile-time limiter / bound speed for the field-loop regression schemes
+  if (k.ndir == 3 && k.glm && k.solver == SOLVER_HLLD && k.limiter == LIM_CADA3 && k.boundspeed == BS_EINFELDT) {
+    *out = Launch<true, 3, true, 2, SOLVER_HLLD, LIM_CADA3, BS_EINFELDT>::set();
+    return true;
+  }
 #define AMRVAC_M2(NDIR, GLM, S)                                 \
   if (k.ndir == NDIR && k.glm == GLM && k.solver == S) {        \
     *out = Launch<true, NDIR, GLM, 2, S>::set();                \

@@ -5,6 +5,11 @@ namespace amrvac {
 
 bool lookup_mhd3(const KernelKey &k, KernelSet *out) {
   if (!k.mhd || k.ndim != 3 || k.ndir != 3) return false;
+  // compile-time limiter / bound speed for the 3-D Orszag-Tang configuration
+  if (k.glm && k.solver == SOLVER_HLLD && k.limiter == LIM_CADA3 && k.boundspeed == BS_EINFELDT) {
+    *out = Launch<true, 3, true, 3, SOLVER_HLLD, LIM_CADA3, BS_EINFELDT>::set();
+    return true;
+  }
 #define AMRVAC_M3(GLM, S)                                       \
   if (k.glm == GLM && k.solver == S) {                          \
     *out = Launch<true, 3, GLM, 3, S>::set();                   \

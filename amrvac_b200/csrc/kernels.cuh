@@ -121,10 +121,14 @@ __global__ void riemann_points_kernel(const PointArgs A) {
   if (p >= A.n) return;
   double wL[NW], wR[NW], F[NW];
 #pragma unroll
-  for (int v = 0; v < NW; ++v) { wL[v] = A.a[(size_t)p * NW + v]; wR[v] = A.b[(size_t)p * NW + v]; }
-  face_from_states<MHD, NDIR, GLM, NDIM, SOLVER, D>(wL, wR, A.P, A.cg, F);
+  for (int v = 0; v < NW; ++v) {
+    const int ov = orig_index<MHD, NDIR, D>(v);
+    wL[v] = A.a[(size_t)p * NW + ov];
+    wR[v] = A.b[(size_t)p * NW + ov];
+  }
+  face_from_states<MHD, NDIR, GLM, NDIM, SOLVER, 0>(wL, wR, A.P, A.cg, F);
 #pragma unroll
-  for (int v = 0; v < NW; ++v) A.out[(size_t)p * NW + v] = F[v];
+  for (int v = 0; v < NW; ++v) A.out[(size_t)p * NW + orig_index<MHD, NDIR, D>(v)] = F[v];
 }
 
 template <bool MHD, int NDIR, bool GLM, int D>
@@ -171,16 +175,16 @@ struct KernelSet {
   size_t stage_smem = 0;
 };
 
-template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER>
+template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM = 0, int BS = 0>
 struct Launch {
   using V = Vars<MHD, NDIR, GLM>;
   static constexpr size_t SMEM = Tile<V::NW, NDIM>::BYTES;
   static cudaError_t prepare() {
-    return cudaFuncSetAttribute(fv_stage_kernel<MHD, NDIR, GLM, NDIM, SOLVER>,
+    return cudaFuncSetAttribute(fv_stage_kernel<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   }
   static cudaError_t stage(const StageArgs &A, int nctas, cudaStream_t s) {
-    fv_stage_kernel<MHD, NDIR, GLM, NDIM, SOLVER><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
+    fv_stage_kernel<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
     return cudaGetLastError();
   }
   static cudaError_t getdt(const GetdtArgs &A, cudaStream_t s) {
@@ -239,6 +243,8 @@ struct KernelKey {
   int ndim, ndir;
   bool glm;
   int solver;
+  int limiter;     // used to pick a compile-time specialised stage kernel
+  int boundspeed;
 };
 
 bool lookup_hd(const KernelKey &k, KernelSet *out);

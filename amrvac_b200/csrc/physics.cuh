@@ -179,14 +179,15 @@ __device__ __forceinline__ double fast_speed(const double *w, const PhysParams &
 
 // hd_get_cbounds (mod_hd_phys.t:891-1001) / mhd_get_cbounds (mod_mhd_phys.t:3037-3127).
 // WITH_MIN=false gives the tvdlf form (cmax only).  Returns a status bit.
-template <bool MHD, int NDIR, bool GLM, int D, bool WITH_MIN>
+template <bool MHD, int NDIR, bool GLM, int D, bool WITH_MIN, int BS = 0>
 __device__ __forceinline__ uint32_t cbounds(const double *wLC, const double *wRC, const double *wLp,
                                             const double *wRp, const PhysParams &P, double &cmax,
                                             double &cmin) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int MN = V::M0 + D;
   uint32_t st = 0;
-  if (P.boundspeed == BS_EINFELDT) {
+  const int bsel = BS ? BS : P.boundspeed;
+  if (bsel == BS_EINFELDT) {
     const double tmp1 = sqrt(wLp[V::RHO]);
     const double tmp2 = sqrt(wRp[V::RHO]);
     const double tmp3 = 1.0 / (tmp1 + tmp2);
@@ -209,7 +210,7 @@ __device__ __forceinline__ uint32_t cbounds(const double *wLC, const double *wRC
     } else {
       cmax = fabs(umean) + dmean;
     }
-  } else if (P.boundspeed == BS_CMAXMEAN) {
+  } else if (bsel == BS_CMAXMEAN) {
     if constexpr (MHD) {
       double wm[V::NW];
 #pragma unroll
@@ -262,7 +263,7 @@ __device__ __forceinline__ uint32_t cbounds(const double *wLC, const double *wRC
 // dwlimiter2 (mod_limiter.t:128-334) for one cell: a = dwC(ix) (forward
 // difference), b = dwC(ix-1) (backward difference).  LEFT selects ldw, else rdw.
 template <bool LEFT>
-__device__ __forceinline__ double limited_slope(int lim, double a, double b, double rdelinv) {
+__device__ __forceinline__ double slope_impl(int lim, double a, double b, double rdelinv) {
   constexpr double qsmall = 1.0e-12, qsmall2 = 2.0e-12;
   constexpr double eps = 1.4901161193847656e-08;  // sqrt(epsilon(1d0)) = 2**-26
   constexpr double c_mcbeta = 1.4, cadalfa = 0.5, cadbeta = 2.0, cadgamma = 1.6;
@@ -320,6 +321,23 @@ __device__ __forceinline__ double limited_slope(int lim, double a, double b, dou
              (LEFT ? a : b);
     }
   }
+}
+
+// LIM != 0 fixes the limiter at compile time (the switch folds away);
+// LIM == 0 selects it at run time from lim_rt.
+template <bool LEFT, int LIM>
+__device__ __forceinline__ double limited_slope(int lim_rt, double a, double b, double rdelinv) {
+  return slope_impl<LEFT>(LIM ? LIM : lim_rt, a, b, rdelinv);
+}
+
+// Index in the reference variable order of entry v of a state whose vector
+// components are cyclically rotated so that direction D comes first
+// (rotated component c holds original component (c + D) mod ndir).
+template <bool MHD, int NDIR, int D>
+__host__ __device__ constexpr int orig_index(int v) {
+  return (v >= 1 && v <= NDIR) ? 1 + (v - 1 + D) % NDIR
+         : (MHD && v >= NDIR + 2 && v <= 2 * NDIR + 1) ? NDIR + 2 + (v - NDIR - 2 + D) % NDIR
+                                                         : v;
 }
 
 }  // namespace amrvac

@@ -89,8 +89,15 @@ __device__ __forceinline__ int resolve_cell(const StageArgs &A, int b, int &i, i
   int blk = b;
   if (dir[0] | dir[1] | dir[2]) {
     blk = A.nbr[b * 27 + dir_index(dir[0], dir[1], dir[2])];
+    if (blk >= 0) {
 #pragma unroll
-    for (int d = 0; d < NDIM; ++d) c[d] -= dir[d] * BN;
+      for (int d = 0; d < NDIM; ++d) c[d] -= dir[d] * BN;
+    } else {  // inconsistent neighbour table: stay in bounds and flag it
+      blk = b;
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) c[d] = min(max(c[d], 0), BN - 1);
+      atomicOr(A.status, ST_BOUNDS);
+    }
   }
   i = c[0]; j = c[1]; k = c[2];
   return blk;
@@ -127,9 +134,10 @@ __device__ __forceinline__ uint32_t load_prim(const StageArgs &A, int b, int i, 
 // Interface flux from reconstructed primitive left/right states: small-value
 // fix, to_conserved, GLM modify_wLR, physical fluxes, cbounds, Riemann solver
 // (src/mod_finite_volume.t:1217-1222, 200-245).  wLp/wRp are modified.
-template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int D>
+template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int BS>
 __device__ __forceinline__ uint32_t face_from_states(double *wLp, double *wRp, const PhysParams &P,
                                                      double cg, double *F) {
+  constexpr int D = 0;  // states arrive rotated: the face normal is component 0
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
   uint32_t st = 0;
@@ -162,10 +170,10 @@ __device__ __forceinline__ uint32_t face_from_states(double *wLp, double *wRp, c
   phys_flux<MHD, NDIR, GLM, D>(wRC, wRp, cg, fR);
   double cmax, cmin = 0.0;
   if constexpr (SOLVER == SOLVER_TVDLF) {
-    st |= cbounds<MHD, NDIR, GLM, D, false>(wLC, wRC, wLp, wRp, P, cmax, cmin);
+    st |= cbounds<MHD, NDIR, GLM, D, false, BS>(wLC, wRC, wLp, wRp, P, cmax, cmin);
     riemann_tvdlf<NW>(wLC, wRC, fL, fR, cmax, P.tvdlfeps, F);
   } else {
-    st |= cbounds<MHD, NDIR, GLM, D, true>(wLC, wRC, wLp, wRp, P, cmax, cmin);
+    st |= cbounds<MHD, NDIR, GLM, D, true, BS>(wLC, wRC, wLp, wRp, P, cmax, cmin);
     if constexpr (SOLVER == SOLVER_HLL) {
       riemann_hll<MHD, NDIR, GLM, NDIM, D>(wLC, wRC, fL, fR, cmax, cmin, P.tvdlfeps, F);
     } else if constexpr (SOLVER == SOLVER_HLLC) {
@@ -179,9 +187,12 @@ __device__ __forceinline__ uint32_t face_from_states(double *wLp, double *wRp, c
   return st;
 }
 
-// One face: primitives of the 4-cell stencil (cells L-1, L, R, R+1 along D)
-// are read through `ld(o, v)` with o in {-2,-1,0,1} relative to the right cell.
-template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int D, class LD>
+// One face normal to direction D: primitives of the 4-cell stencil (cells
+// L-1, L, R, R+1) are read through `ld(o, v)` with o in {-2,-1,0,1} relative
+// to the right cell and v in the reference variable order.  The states are
+// rotated so that one direction-generic face routine serves x, y and z; the
+// flux F is returned in the reference order.
+template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS, int D, class LD>
 __device__ __forceinline__ uint32_t face_flux(const LD &ld, const PhysParams &P, double cg,
                                               double rdelinv, double *F) {
   using V = Vars<MHD, NDIR, GLM>;
@@ -189,12 +200,17 @@ __device__ __forceinline__ uint32_t face_flux(const LD &ld, const PhysParams &P,
   double wLp[NW], wRp[NW];
 #pragma unroll
   for (int v = 0; v < NW; ++v) {
-    const double q0 = ld(-2, v), q1 = ld(-1, v), q2 = ld(0, v), q3 = ld(1, v);
+    const int ov = orig_index<MHD, NDIR, D>(v);
+    const double q0 = ld(-2, ov), q1 = ld(-1, ov), q2 = ld(0, ov), q3 = ld(1, ov);
     const double d0 = q1 - q0, d1 = q2 - q1, d2 = q3 - q2;
-    wLp[v] = q1 + 0.5 * limited_slope<true>(P.limiter, d1, d0, rdelinv);
-    wRp[v] = q2 - 0.5 * limited_slope<false>(P.limiter, d2, d1, rdelinv);
+    wLp[v] = q1 + 0.5 * limited_slope<true, LIM>(P.limiter, d1, d0, rdelinv);
+    wRp[v] = q2 - 0.5 * limited_slope<false, LIM>(P.limiter, d2, d1, rdelinv);
   }
-  return face_from_states<MHD, NDIR, GLM, NDIM, SOLVER, D>(wLp, wRp, P, cg, F);
+  double Fr[NW];
+  const uint32_t st = face_from_states<MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, cg, Fr);
+#pragma unroll
+  for (int v = 0; v < NW; ++v) F[orig_index<MHD, NDIR, D>(v)] = Fr[v];
+  return st;
 }
 
 // Shared-memory tile (sizes in doubles).
@@ -237,7 +253,7 @@ struct TileView {
   }
 };
 
-template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER>
+template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS>
 __global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageArgs A) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
@@ -316,7 +332,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageA
       auto ld = [&](int o, int v) -> double {
         return tv.ring[(((k + 1 + o) & 3) * NW + v) * (BN * BN) + cj * BN + ci];
       };
-      st |= face_flux<MHD, NDIR, GLM, NDIM, SOLVER, 2>(ld, P, cg, rdel[2], Fs);
+      st |= face_flux<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, 2>(ld, P, cg, rdel[2], Fs);
 #pragma unroll
       for (int v = 0; v < NW; ++v) Fs[v] = dxinv[2] * Fs[v];
     }
@@ -330,6 +346,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageA
     load_center(k0 + 1);
     __syncthreads();
     if (cell_thread) zface(k0 - 1, fz_prev);
+    __syncthreads();  // the first iteration overwrites ring slot (k0-2)&3
   }
 
   for (int k = k0; k < k1; ++k) {
@@ -353,7 +370,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageA
       const int fj = t / (BN + 1), fi = t - fj * (BN + 1);
       auto ld = [&](int o, int v) -> double { return tv.at(slot, v, fi + o, fj); };
       double F[NW];
-      st |= face_flux<MHD, NDIR, GLM, NDIM, SOLVER, 0>(ld, P, cg, rdel[0], F);
+      st |= face_flux<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, 0>(ld, P, cg, rdel[0], F);
 #pragma unroll
       for (int v = 0; v < NW; ++v) tv.fb[v * ((BN + 1) * BN) + t] = dxinv[0] * F[v];
     }
@@ -372,7 +389,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageA
       const int fj = t >> 4, fi = t & (BN - 1);
       auto ld = [&](int o, int v) -> double { return tv.at(slot, v, fi, fj + o); };
       double F[NW];
-      st |= face_flux<MHD, NDIR, GLM, NDIM, SOLVER, 1>(ld, P, cg, rdel[1], F);
+      st |= face_flux<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, 1>(ld, P, cg, rdel[1], F);
 #pragma unroll
       for (int v = 0; v < NW; ++v) tv.fb[v * ((BN + 1) * BN) + t] = dxinv[1] * F[v];
     }

@@ -256,8 +256,14 @@ def test_riemann_points(oracle_lib, name):
         lib = O.lib()
         lib.orc_riemann_points(ctypes.byref(ocfg), n, O._dp(np.ascontiguousarray(wl)),
                                O._dp(np.ascontiguousarray(wr)), idim, 2.5, O._dp(ref))
-        scale = np.abs(ref).max(axis=0) + 1e-300
-        err = (np.abs(got - ref) / (np.abs(ref) + 1e-6 * scale)).max()
+        # far-apart random states can leave the solver's validity range (e.g. a
+        # negative HLLD star density): both sides must then give NaN together
+        bad = ~np.isfinite(ref)
+        assert np.array_equal(bad, ~np.isfinite(got)), f"{name} idim={idim}: NaN pattern differs"
+        ok = ~bad.any(axis=1)
+        assert ok.mean() > 0.5
+        scale = np.abs(ref[ok]).max(axis=0) + 1e-300
+        err = (np.abs(got[ok] - ref[ok]) / (np.abs(ref[ok]) + 1e-6 * scale)).max()
         assert err <= 1e-11, f"{name} idim={idim}: {err:.3e}"
 
 
