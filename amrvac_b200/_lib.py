@@ -10,7 +10,8 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libamrvac_gpu.so")
+# AMRVAC_GPU_LIB selects another build of the same library (e.g. a tuning variant).
+LIB_PATH = os.environ.get("AMRVAC_GPU_LIB", os.path.join(HERE, "libamrvac_gpu.so"))
 HEADER = os.path.join(os.path.dirname(HERE), "include", "amrvac_gpu.h")
 
 MAX_NW = 16

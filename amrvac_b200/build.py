@@ -16,13 +16,14 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-BUILD = os.path.join(HERE, "_build")
-LIB = os.path.join(HERE, "libamrvac_gpu.so")
+BUILD = os.environ.get("AMRVAC_BUILD_DIR", os.path.join(HERE, "_build"))
+LIB = os.environ.get("AMRVAC_LIB_OUT", os.path.join(HERE, "libamrvac_gpu.so"))
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
          "--expt-relaxed-constexpr", "-I", INCLUDE]
+EXTRA = os.environ.get("AMRVAC_NVCC_EXTRA", "").split()
 UNITS = ["capi.cu", "aux.cu", "k_hd.cu", "k_mhd2.cu", "k_mhd3.cu"]
 
 
@@ -34,14 +35,14 @@ def _digest() -> str:
                 with open(os.path.join(d, name), "rb") as f:
                     h.update(name.encode())
                     h.update(f.read())
-    h.update(" ".join(ARCH + FLAGS).encode())
+    h.update(" ".join(ARCH + FLAGS + EXTRA).encode())
     return h.hexdigest()
 
 
 def _compile(unit: str, verbose: bool) -> str:
     src = os.path.join(CSRC, unit)
     obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
-    cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
+    cmd = [NVCC, *ARCH, *FLAGS, *EXTRA, "-c", src, "-o", obj]
     if verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -31,7 +31,12 @@
 namespace amrvac {
 
 constexpr int BN = 16;               // cells per block edge
-constexpr int STAGE_THREADS = 288;   // 9 warps: 17*16 faces + 16 spare
+#ifndef AMRVAC_STAGE_THREADS
+#define AMRVAC_STAGE_THREADS 288
+#endif
+// 288 = 9 warps: one thread per face of a 17x16 face plane.  With 256 threads
+// the 16 extra faces of an x/y phase take a second (partial) round.
+constexpr int STAGE_THREADS = AMRVAC_STAGE_THREADS;
 
 enum : int { BCK_PERIODIC = 0, BCK_CONT = 1, BCK_MIRROR = 2 };
 
@@ -253,10 +258,20 @@ struct TileView {
   }
 };
 
+// Runtime form of orig_index for a face phase D (the v loop is unrolled, so
+// only D is a run-time value: a few integer operations per variable).
+template <bool MHD, int NDIR>
+__device__ __forceinline__ int orig_index_rt(int v, int D) {
+  if (v >= 1 && v <= NDIR) return 1 + (v - 1 + D) % NDIR;
+  if (MHD && v >= NDIR + 2 && v <= 2 * NDIR + 1) return NDIR + 2 + (v - NDIR - 2 + D) % NDIR;
+  return v;
+}
+
 template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS>
 __global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageArgs A) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
+  constexpr int FB = (BN + 1) * BN;  // face-buffer stride per variable
   extern __shared__ double smem[];
   TileView<NW, NDIM> tv(smem);
   const int t = threadIdx.x;
@@ -283,23 +298,33 @@ __global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageA
   const int ci = t & (BN - 1), cj = t >> 4;  // cell role for t < 256
   const bool cell_thread = t < BN * BN;
   const bool need_corners = MHD && !GLM && P.divb == DIVB_LINDE;
+  double fz_prev[NDIM == 3 ? NW : 1];
+#pragma unroll
+  for (int v = 0; v < (NDIM == 3 ? NW : 1); ++v) fz_prev[v] = 0.0;
 
-  auto load_center = [&](int kk) {
+  // 3-D: iteration k stages plane k+2; iterations k0-4 .. k0-1 only stage the
+  // planes k0-2 .. k0+1 (and, at k0-1, compute the z-face k0-1/2);
+  // iterations k0 .. k1-1 update plane k.
+  const int kstart = NDIM == 3 ? k0 - 4 : 0;
+#pragma unroll 1
+  for (int k = kstart; k < k1; ++k) {
+    const bool update = k >= k0;
+    const int slot = NDIM == 3 ? (k & 3) : 0;
+    // ---- stage plane k+2 (3-D) / the block (2-D) as primitives
     if (cell_thread) {
       double w[NW];
+      const int kk = NDIM == 3 ? k + 2 : 0;
       st |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, ci, cj, kk, w);
-      const int slot = NDIM == 3 ? (kk & 3) : 0;
+      const int s2 = NDIM == 3 ? (kk & 3) : 0;
 #pragma unroll
-      for (int v = 0; v < NW; ++v) tv.center(slot, v, ci, cj) = w[v];
+      for (int v = 0; v < NW; ++v) tv.center(s2, v, ci, cj) = w[v];
     }
-  };
-  auto load_halo = [&](int kk) {
-    // x strips: 64 cells, y strips: 64 cells, corners: 16 cells
-    const int ncell = need_corners ? 144 : 128;
-    for (int h = t; h < ncell; h += STAGE_THREADS) {
-      int i, j;
+    // ---- x/y halo strips (and corners for Linde) of plane k
+    const int nhalo = update ? (need_corners ? 144 : 128) : 0;
+    if (t < nhalo) {
+      const int h = t;
+      int i, j, stride;
       double *dst;
-      int stride;
       if (h < 64) {
         j = h >> 2;
         const int c = h & 3;
@@ -320,43 +345,13 @@ __global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageA
         stride = 16;
       }
       double w[NW];
-      st |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, i, j, kk, w);
+      st |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, i, j, k, w);
 #pragma unroll
       for (int v = 0; v < NW; ++v) dst[v * stride] = w[v];
     }
-  };
-
-  // z-face k+1/2 for the column of this cell thread, from ring planes k-1..k+2
-  auto zface = [&](int k, double *Fs) {
-    if constexpr (NDIM == 3) {
-      auto ld = [&](int o, int v) -> double {
-        return tv.ring[(((k + 1 + o) & 3) * NW + v) * (BN * BN) + cj * BN + ci];
-      };
-      st |= face_flux<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, 2>(ld, P, cg, rdel[2], Fs);
-#pragma unroll
-      for (int v = 0; v < NW; ++v) Fs[v] = dxinv[2] * Fs[v];
-    }
-  };
-
-  double fz_prev[NDIM == 3 ? NW : 1];
-  if constexpr (NDIM == 3) {
-    load_center(k0 - 2);
-    load_center(k0 - 1);
-    load_center(k0);
-    load_center(k0 + 1);
-    __syncthreads();
-    if (cell_thread) zface(k0 - 1, fz_prev);
-    __syncthreads();  // the first iteration overwrites ring slot (k0-2)&3
-  }
-
-  for (int k = k0; k < k1; ++k) {
-    const int slot = NDIM == 3 ? (k & 3) : 0;
-    if constexpr (NDIM == 3) load_center(k + 2);
-    else load_center(0);
-    load_halo(k);
-    // RK combination wnew0 = a*base + b*in (src/mod_advance.t:254-266)
+    // ---- RK combination wnew0 = a*base + b*in (src/mod_advance.t:254-266)
     double acc[NW];
-    if (cell_thread) {
+    if (update && cell_thread) {
 #pragma unroll
       for (int v = 0; v < NW; ++v) {
         const size_t o = cell_offset<NDIM>(b, NW, v, ci, cj, k);
@@ -365,58 +360,64 @@ __global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageA
       }
     }
     __syncthreads();
-    // ---- x faces: face (fi - 1/2) of row fj, fi in [0,16]
-    if (t < (BN + 1) * BN) {
-      const int fj = t / (BN + 1), fi = t - fj * (BN + 1);
-      auto ld = [&](int o, int v) -> double { return tv.at(slot, v, fi + o, fj); };
-      double F[NW];
-      st |= face_flux<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, 0>(ld, P, cg, rdel[0], F);
-#pragma unroll
-      for (int v = 0; v < NW; ++v) tv.fb[v * ((BN + 1) * BN) + t] = dxinv[0] * F[v];
-    }
-    __syncthreads();
-    if (cell_thread) {
-      const int f = cj * (BN + 1) + ci;
-#pragma unroll
-      for (int v = 0; v < NW; ++v) {
-        const double *fb = tv.fb + v * ((BN + 1) * BN);
-        acc[v] = acc[v] + fb[f + 1] - fb[f];
-      }
-    }
-    __syncthreads();
-    // ---- y faces: face (fj - 1/2) of column fi, fj in [0,16]
-    if (t < (BN + 1) * BN) {
-      const int fj = t >> 4, fi = t & (BN - 1);
-      auto ld = [&](int o, int v) -> double { return tv.at(slot, v, fi, fj + o); };
-      double F[NW];
-      st |= face_flux<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, 1>(ld, P, cg, rdel[1], F);
-#pragma unroll
-      for (int v = 0; v < NW; ++v) tv.fb[v * ((BN + 1) * BN) + t] = dxinv[1] * F[v];
-    }
-    __syncthreads();
-    if (cell_thread) {
-      const int f = cj * BN + ci;
-#pragma unroll
-      for (int v = 0; v < NW; ++v) {
-        const double *fb = tv.fb + v * ((BN + 1) * BN);
-        acc[v] = acc[v] + fb[f + BN] - fb[f];
-      }
-      // ---- z face k+1/2 (registers)
-      if constexpr (NDIM == 3) {
-        double fz[NW];
-        zface(k, fz);
+    // ---- face phases x, y (plane k) and z (face k+1/2 of every column); one
+    // copy of the face code serves all three through the state rotation.
+    const int dlo = update ? 0 : (NDIM == 3 && k == k0 - 1 ? 2 : NDIM);
+#pragma unroll 1
+    for (int D = dlo; D < NDIM; ++D) {
+      const int nface = D < 2 ? FB : BN * BN;
+#pragma unroll 1
+      for (int f = t; f < nface; f += STAGE_THREADS) {
+        int fi, fj;
+        if (D == 0) { fj = f / (BN + 1); fi = f - fj * (BN + 1); }
+        else { fj = f >> 4; fi = f & (BN - 1); }
+        const double rd = D == 0 ? rdel[0] : (D == 1 ? rdel[1] : rdel[2]);
+        double wLp[NW], wRp[NW];
 #pragma unroll
         for (int v = 0; v < NW; ++v) {
-          acc[v] = acc[v] + fz[v] - fz_prev[v];
-          fz_prev[v] = fz[v];
+          const int ov = orig_index_rt<MHD, NDIR>(v, D);
+          double q[4];
+#pragma unroll
+          for (int o = 0; o < 4; ++o) {
+            if (D == 0) q[o] = tv.at(slot, ov, fi + o - 2, fj);
+            else if (D == 1) q[o] = tv.at(slot, ov, fi, fj + o - 2);
+            else q[o] = tv.ring[(((k + o - 1) & 3) * NW + ov) * (BN * BN) + f];
+          }
+          const double d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
+          wLp[v] = q[1] + 0.5 * limited_slope<true, LIM>(P.limiter, d1, d0, rd);
+          wRp[v] = q[2] - 0.5 * limited_slope<false, LIM>(P.limiter, d2, d1, rd);
+        }
+        double Fr[NW];
+        st |= face_from_states<MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, cg, Fr);
+        const double sc = D == 0 ? dxinv[0] : (D == 1 ? dxinv[1] : dxinv[2]);
+#pragma unroll
+        for (int v = 0; v < NW; ++v) tv.fb[orig_index_rt<MHD, NDIR>(v, D) * FB + f] = sc * Fr[v];
+      }
+      __syncthreads();
+      if (cell_thread) {
+        if (D == 0) {
+          const int f = cj * (BN + 1) + ci;
+#pragma unroll
+          for (int v = 0; v < NW; ++v) acc[v] = acc[v] + tv.fb[v * FB + f + 1] - tv.fb[v * FB + f];
+        } else if (D == 1) {
+          const int f = cj * BN + ci;
+#pragma unroll
+          for (int v = 0; v < NW; ++v) acc[v] = acc[v] + tv.fb[v * FB + f + BN] - tv.fb[v * FB + f];
+        } else if constexpr (NDIM == 3) {
+#pragma unroll
+          for (int v = 0; v < NW; ++v) {
+            const double fz = tv.fb[v * FB + t];
+            if (update) acc[v] = acc[v] + fz - fz_prev[v];
+            fz_prev[v] = fz;
+          }
         }
       }
+      __syncthreads();
+    }
+    if (update && cell_thread) {
       // ---- small values on wnew (src/mod_finite_volume.t:326-333)
       if (P.fix_small_values) {
-        if (small_values<MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) {
-          st |= ST_SMALL_VALUE;
-          atomicOr(A.block_status + b, ST_SMALL_VALUE);
-        }
+        if (small_values<MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
       }
       // ---- unsplit divB sources (addsource2 -> mhd_add_source)
       if constexpr (MHD) {
@@ -477,12 +478,19 @@ __global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageA
           }
         }
       }
+      if (!isfinite(acc[V::RHO]) || !isfinite(acc[V::E])) st |= ST_NAN;
 #pragma unroll
       for (int v = 0; v < NW; ++v) A.uout[cell_offset<NDIM>(b, NW, v, ci, cj, k)] = acc[v];
     }
-    __syncthreads();
+    // the next iteration overwrites ring slot (k-1)&3 and the halo strips,
+    // which the sources above read
+    if (NDIM == 3) __syncthreads();
   }
-  if (st) atomicOr(A.status, st);
+  if (st) {
+    atomicOr(A.status, st);
+    // the reference restores the whole block to wCT on a small-value crash
+    if (st & ST_SMALL_VALUE) atomicOr(A.block_status + b, ST_SMALL_VALUE);
+  }
 }
 
 }  // namespace amrvac
