@@ -44,12 +44,36 @@ struct Vars {
 
 __device__ __forceinline__ double fsign(double a, double b) { return copysign(a, b); }
 
+#ifdef AMRVAC_NR_DIV
+// Reciprocal and quotient by Newton-Raphson iteration from a single-precision
+// seed (Markstein, "IA-64 and Elementary Functions", 2000, ch. 8): each step
+// r <- r + r(1 - y r) squares the relative error (2^-23 -> 2^-46 -> 2^-92); the
+// quotient gets one residual correction q <- q + r(x - y q).  Branch-free;
+// valid for |y| within the single-precision normal range (the path's
+// denominators are densities, wave speeds and limiter slopes >= 2^-26).
+__device__ __forceinline__ double rcp_(double y) {
+  double r = (double)__frcp_rn(__double2float_rn(y));
+  double e = fma(-y, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-y, r, 1.0);
+  return fma(r, e, r);
+}
+__device__ __forceinline__ double div_(double x, double y) {
+  const double r = rcp_(y);
+  const double q = x * r;
+  return fma(fma(-y, q, x), r, q);
+}
+#else
+__device__ __forceinline__ double rcp_(double y) { return 1.0 / y; }
+__device__ __forceinline__ double div_(double x, double y) { return x / y; }
+#endif
+
 // ------------------------------------------------------------------ conversions
 // hd_to_primitive (mod_hd_phys.t:703-734) / mhd_to_primitive_origin (mod_mhd_phys.t:1741-1765)
 template <bool MHD, int NDIR, bool GLM>
 __device__ __forceinline__ void to_primitive(double *w, const PhysParams &P) {
   using V = Vars<MHD, NDIR, GLM>;
-  const double inv_rho = 1.0 / w[V::RHO];
+  const double inv_rho = rcp_(w[V::RHO]);
 #pragma unroll
   for (int c = 0; c < NDIR; ++c) w[V::M0 + c] = w[V::M0 + c] * inv_rho;
   double v2 = w[V::M0] * w[V::M0];
@@ -166,7 +190,7 @@ __device__ __forceinline__ void phys_flux(const double *wc, const double *w, dou
 template <int NDIR, int BN>
 __device__ __forceinline__ double fast_speed(const double *w, const PhysParams &P) {
   constexpr int RHO = 0, E = NDIR + 1, B0 = NDIR + 2;
-  const double inv_rho = 1.0 / w[RHO];
+  const double inv_rho = rcp_(w[RHO]);
   const double cs = P.gamma * w[E] * inv_rho;
   double b2 = w[B0] * w[B0];
 #pragma unroll
@@ -190,7 +214,7 @@ __device__ __forceinline__ uint32_t cbounds(const double *wLC, const double *wRC
   if (bsel == BS_EINFELDT) {
     const double tmp1 = sqrt(wLp[V::RHO]);
     const double tmp2 = sqrt(wRp[V::RHO]);
-    const double tmp3 = 1.0 / (tmp1 + tmp2);
+    const double tmp3 = rcp_(tmp1 + tmp2);
     const double umean = (wLp[MN] * tmp1 + wRp[MN] * tmp2) * tmp3;
     const double dv = wRp[MN] - wLp[MN];
     double dmean;
@@ -275,23 +299,17 @@ __device__ __forceinline__ double slope_impl(int lim, double a, double b, double
       return t * fmax(0.0, fmin(fabs(a), t * b));
     }
     case LIM_VANLEER:
-      return 2.0 * fmax(b * a, 0.0) / (a + b + qsmall);
+      return div_(2.0 * fmax(b * a, 0.0), a + b + qsmall);
     case LIM_CADA3: {
+      // branch-free: both the asymptotic and the limited form are evaluated
+      // and the reference's three-way choice is made with selects
       const double tmpeta = (a * a + b * b) * rdelinv;
-      const double t = LEFT ? b / (a + fsign(eps, a)) : a / (b + fsign(eps, b));
+      const double t = LEFT ? div_(b, a + fsign(eps, a)) : div_(a, b + fsign(eps, b));
       const double A = (2.0 + t) * third;
-      double phi;
-      if (tmpeta <= 1.0 - cadepsilon) {
-        phi = A;
-      } else {
-        const double lim2 = fmax(0.0, fmin(A, fmax(-(cadalfa * t), fmin(fmin(cadbeta * t, A), cadgamma))));
-        if (tmpeta >= 1.0 + cadepsilon) {
-          phi = lim2;
-        } else {
-          const double t2 = (tmpeta - 1.0) * invcadepsilon;
-          phi = 0.5 * ((1.0 - t2) * A + (1.0 + t2) * lim2);
-        }
-      }
+      const double lim2 = fmax(0.0, fmin(A, fmax(-(cadalfa * t), fmin(fmin(cadbeta * t, A), cadgamma))));
+      const double t2 = (tmpeta - 1.0) * invcadepsilon;
+      const double blend = 0.5 * ((1.0 - t2) * A + (1.0 + t2) * lim2);
+      const double phi = tmpeta <= 1.0 - cadepsilon ? A : (tmpeta >= 1.0 + cadepsilon ? lim2 : blend);
       return phi * (LEFT ? a : b);
     }
     case LIM_WOODWARD: {

@@ -47,7 +47,7 @@ __device__ __forceinline__ void riemann_hll(const double *wLC, const double *wRC
     } else if (cmax <= 0.0) {
       F[v] = fR[v];
     } else {
-      F[v] = (cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v])) / (cmax - cmin);
+      F[v] = div_(cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v]), cmax - cmin);
     }
   }
 }
@@ -126,7 +126,7 @@ __device__ __forceinline__ void riemann_hlld(const double *wLC, const double *wR
   constexpr int ip1 = D, ip2 = (D + 1) % NDIR, ip3 = (D + 2) % NDIR;
   constexpr int m1 = M0 + ip1, m2 = M0 + ip2, m3 = M0 + ip3;
   constexpr int b1 = B0 + ip1, b2 = B0 + ip2, b3 = B0 + ip3;
-  const double Bx = (sR * wRC[b1] - sL * wLC[b1]) / (sR - sL);
+  const double Bx = div_(sR * wRC[b1] - sL * wLC[b1], sR - sL);
   double bR2 = wRC[B0] * wRC[B0], bL2 = wLC[B0] * wLC[B0];
 #pragma unroll
   for (int c = 1; c < NDIR; ++c) {
@@ -138,17 +138,17 @@ __device__ __forceinline__ void riemann_hlld(const double *wLC, const double *wR
   const double vR = wRp[m1], vL = wLp[m1];
   const double suR = (sR - vR) * wRC[RHO];
   const double suL = (sL - vL) * wLC[RHO];
-  const double sm = (suR * vR - suL * vL - ptR + ptL) / (suR - suL);
+  const double sm = div_(suR * vR - suL * vL - ptR + ptL, suR - suL);
   // star states w1 (velocities in the momentum slots until the final conversion)
   double w1R[NW], w1L[NW], w2R[NW], w2L[NW];
   w1R[m1] = sm; w1L[m1] = sm; w2R[m1] = sm; w2L[m1] = sm;
   w1R[b1] = Bx; w1L[b1] = Bx;
-  w1R[RHO] = suR / (sR - sm);
-  w1L[RHO] = suL / (sL - sm);
+  w1R[RHO] = div_(suR, sR - sm);
+  w1L[RHO] = div_(suL, sL - sm);
   double r1R = suR * (sR - sm) - Bx * Bx;
-  if (r1R != 0.0) r1R = 1.0 / r1R;
+  if (r1R != 0.0) r1R = rcp_(r1R);
   double r1L = suL * (sL - sm) - Bx * Bx;
-  if (r1L != 0.0) r1L = 1.0 / r1L;
+  if (r1L != 0.0) r1L = rcp_(r1L);
   w1R[m2] = wRp[m2] - Bx * wRC[b2] * (sm - vR) * r1R;
   w1L[m2] = wLp[m2] - Bx * wLC[b2] * (sm - vL) * r1L;
   double pb2R = (suR * (sR - vR) - Bx * Bx) * r1R;
@@ -172,17 +172,17 @@ __device__ __forceinline__ void riemann_hlld(const double *wLC, const double *wR
       v1bR = v1bR + w1R[M0 + c] * w1R[B0 + c];
       v1bL = v1bL + w1L[M0 + c] * w1L[B0 + c];
     }
-    w1R[E] = ((sR - vR) * wRC[E] - ptR * vR + pts * sm + Bx * (vbR - v1bR)) / (sR - sm);
-    w1L[E] = ((sL - vL) * wLC[E] - ptL * vL + pts * sm + Bx * (vbL - v1bL)) / (sL - sm);
+    w1R[E] = div_((sR - vR) * wRC[E] - ptR * vR + pts * sm + Bx * (vbR - v1bR), sR - sm);
+    w1L[E] = div_((sL - vL) * wLC[E] - ptL * vL + pts * sm + Bx * (vbL - v1bL), sL - sm);
   }
   w2R[RHO] = w1R[RHO]; w2L[RHO] = w1L[RHO];
   w2R[b1] = Bx; w2L[b1] = Bx;
   const double sqR = sqrt(w1R[RHO]);
   const double sqL = sqrt(w1L[RHO]);
-  const double tmp = 1.0 / (sqR + sqL);
+  const double tmp = rcp_(sqR + sqL);
   const double signBx = copysign(1.0, Bx);
-  const double s1R = sm + fabs(Bx) / sqR;
-  const double s1L = sm - fabs(Bx) / sqL;
+  const double s1R = sm + div_(fabs(Bx), sqR);
+  const double s1L = sm - div_(fabs(Bx), sqL);
   w2R[m2] = (sqL * w1L[m2] + sqR * w1R[m2] + (w1R[b2] - w1L[b2]) * signBx) * tmp;
   w2L[m2] = w2R[m2];
   w2R[b2] = (sqL * w1R[b2] + sqR * w1L[b2] + sqL * sqR * (w1R[m2] - w1L[m2]) * signBx) * tmp;
@@ -217,7 +217,8 @@ __device__ __forceinline__ void riemann_hlld(const double *wLC, const double *wR
     // psi star values are never used (flux_special); keep them defined.
     w1R[V::PSI] = w1L[V::PSI] = w2R[V::PSI] = w2L[V::PSI] = 0.0;
   }
-  // region selection (Miyoshi eq. 66)
+  // region selection (Miyoshi eq. 66), branch-free: the candidate fluxes of
+  // the chosen side are formed for every variable and the region picks one
   int region;
   if (sL > 0.0) region = 0;
   else if (s1L >= 0.0) region = 1;
@@ -225,22 +226,24 @@ __device__ __forceinline__ void riemann_hlld(const double *wLC, const double *wR
   else if (s1R >= 0.0) region = 3;
   else if (sR >= 0.0) region = 4;
   else region = 5;  // sR < 0 (a NaN speed also lands here)
+  const bool left = region <= 2;
+  const bool one_star = region == 1 || region == 4;
+  const bool two_star = region == 2 || region == 3;
+  const double c1 = left ? sL : sR;
+  const double c2 = left ? s1L : s1R;
 #pragma unroll
   for (int v = 0; v < NW; ++v) {
     if (FT::bn_special && (v == b1 || v == V::PSI)) {
       F[v] = fL[v];
       continue;
     }
-    double out;
-    switch (region) {
-      case 0: out = fL[v]; break;
-      case 1: out = fL[v] + sL * (w1L[v] - wLC[v]); break;
-      case 2: out = fL[v] + sL * (w1L[v] - wLC[v]) + s1L * (w2L[v] - w1L[v]); break;
-      case 3: out = fR[v] + sR * (w1R[v] - wRC[v]) + s1R * (w2R[v] - w1R[v]); break;
-      case 4: out = fR[v] + sR * (w1R[v] - wRC[v]); break;
-      default: out = fR[v]; break;
-    }
-    F[v] = out;
+    const double fs = left ? fL[v] : fR[v];
+    const double ws = left ? wLC[v] : wRC[v];
+    const double w1 = left ? w1L[v] : w1R[v];
+    const double w2 = left ? w2L[v] : w2R[v];
+    const double t1 = fs + c1 * (w1 - ws);
+    const double t2 = t1 + c2 * (w2 - w1);
+    F[v] = two_star ? t2 : (one_star ? t1 : fs);
   }
 }
 

@@ -34,6 +34,9 @@ constexpr int BN = 16;               // cells per block edge
 #ifndef AMRVAC_STAGE_THREADS
 #define AMRVAC_STAGE_THREADS 288
 #endif
+#ifndef AMRVAC_STAGE_MINB
+#define AMRVAC_STAGE_MINB 1
+#endif
 // 288 = 9 warps: one thread per face of a 17x16 face plane.  With 256 threads
 // the 16 extra faces of an x/y phase take a second (partial) round.
 constexpr int STAGE_THREADS = AMRVAC_STAGE_THREADS;
@@ -253,6 +256,19 @@ struct TileView {
     if (ii) return hy[(v * 4 + halo_slot(j)) * BN + i];
     return hc[(v * 4 + halo_slot(j)) * 4 + halo_slot(i)];
   }
+  // Offset (in doubles from the tile start) of variable 0 at in-plane (i, j)
+  // of the plane in `slot`, and the stride between variables there; branch-free.
+  __device__ __forceinline__ void addr(int slot, int i, int j, int &base, int &stride) const {
+    using T = Tile<NW, NDIM>;
+    const bool ii = (unsigned)i < (unsigned)BN, jj = (unsigned)j < (unsigned)BN;
+    const int hi = halo_slot(i), hj = halo_slot(j);
+    const int oc = slot * NW * (BN * BN) + j * BN + i;
+    const int ox = T::RING + j * 4 + hi;
+    const int oy = T::RING + T::HX + hj * BN + i;
+    const int oz = T::RING + T::HX + T::HY + hj * 4 + hi;
+    base = ii ? (jj ? oc : oy) : (jj ? ox : oz);
+    stride = ii ? (jj ? BN * BN : 4 * BN) : (jj ? 4 * BN : 16);
+  }
   __device__ __forceinline__ double &center(int slot, int v, int i, int j) {
     return ring[(slot * NW + v) * (BN * BN) + j * BN + i];
   }
@@ -268,7 +284,7 @@ __device__ __forceinline__ int orig_index_rt(int v, int D) {
 }
 
 template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS>
-__global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageArgs A) {
+__global__ void __launch_bounds__(STAGE_THREADS, AMRVAC_STAGE_MINB) fv_stage_kernel(const StageArgs A) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
   constexpr int FB = (BN + 1) * BN;  // face-buffer stride per variable
@@ -373,16 +389,24 @@ __global__ void __launch_bounds__(STAGE_THREADS, 1) fv_stage_kernel(const StageA
         else { fj = f >> 4; fi = f & (BN - 1); }
         const double rd = D == 0 ? rdel[0] : (D == 1 ? rdel[1] : rdel[2]);
         double wLp[NW], wRp[NW];
+        // shared-memory offsets of the 4 stencil cells (variable 0) and the
+        // per-variable strides, computed once per face
+        int base[4], strd[4];
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+          if (D == 2) {
+            base[o] = ((k + o - 1) & 3) * NW * (BN * BN) + f;
+            strd[o] = BN * BN;
+          } else {
+            tv.addr(slot, D == 0 ? fi + o - 2 : fi, D == 0 ? fj : fj + o - 2, base[o], strd[o]);
+          }
+        }
 #pragma unroll
         for (int v = 0; v < NW; ++v) {
           const int ov = orig_index_rt<MHD, NDIR>(v, D);
           double q[4];
 #pragma unroll
-          for (int o = 0; o < 4; ++o) {
-            if (D == 0) q[o] = tv.at(slot, ov, fi + o - 2, fj);
-            else if (D == 1) q[o] = tv.at(slot, ov, fi, fj + o - 2);
-            else q[o] = tv.ring[(((k + o - 1) & 3) * NW + ov) * (BN * BN) + f];
-          }
+          for (int o = 0; o < 4; ++o) q[o] = smem[base[o] + ov * strd[o]];
           const double d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
           wLp[v] = q[1] + 0.5 * limited_slope<true, LIM>(P.limiter, d1, d0, rd);
           wRp[v] = q[2] - 0.5 * limited_slope<false, LIM>(P.limiter, d2, d1, rd);
