@@ -27,6 +27,7 @@ DIVB = {"none": 0, "glm": 1, "linde": 4}
 COURANT = {"maxsum": 1, "summax": 2, "minimum": 3}
 BC = {"periodic": 0, "cont": 1, "symm": 2, "asymm": 3}
 TIME_STEPPER = {"onestep": 1, "twostep": 2, "threestep": 3}
+PRECISION = {"fp64": 0, "mixed": 1}
 
 
 class AmrvacCfg(ctypes.Structure):
@@ -48,6 +49,7 @@ class AmrvacCfg(ctypes.Structure):
         ("dtmin", ctypes.c_double),
         ("typeboundary", (ctypes.c_int * MAX_NW) * 6),
         ("zchunk", ctypes.c_int),
+        ("precision", ctypes.c_int),
     ]
 
 
@@ -75,6 +77,8 @@ SIGNATURES = [
     ("amrvac_gpu_get_time", _i, [_vp, _dp, _dp, _dp]),
     ("amrvac_gpu_run_timed", _i, [_vp, _i, _dp, _dp, _dp]),
     ("amrvac_gpu_fp64_peak", _i, [_dp]),
+    ("amrvac_gpu_autotune", _i, [_vp, _i, _ip, _dp]),
+    ("amrvac_gpu_set_zchunk", _i, [_vp, _i]),
     ("amrvac_gpu_status", _i, [_vp, _P(_u32)]),
     ("amrvac_gpu_clear_status", _i, [_vp]),
     ("amrvac_gpu_synchronize", _i, [_vp]),

@@ -121,6 +121,14 @@ class Context:
                    "run_timed")
         return a.value, b.value, c.value
 
+    def autotune(self, reps: int = 3, cache: bool = True):
+        """Pick the z-chunk of the 3-D stage kernel by timing (see tuning.py)."""
+        from . import tuning
+        return tuning.autotune(self, reps=reps, cache=cache)
+
+    def set_zchunk(self, zchunk: int):
+        _lib.check(self.L.amrvac_gpu_set_zchunk(self.h, zchunk), "set_zchunk")
+
     def get_time(self):
         dt, cm, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         _lib.check(self.L.amrvac_gpu_get_time(self.h, ctypes.byref(dt), ctypes.byref(cm), ctypes.byref(t)),

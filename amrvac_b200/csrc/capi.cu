@@ -211,6 +211,7 @@ void amrvac_gpu_default_cfg(amrvac_cfg *c) {
   c->ssprk_order = 3;
   c->dtmin = 1.0e-10;
   c->zchunk = 0;
+  c->precision = 0;
 }
 
 int amrvac_gpu_nw(const amrvac_cfg *cfg) { return cfg ? nw_of(cfg) : AMRVAC_E_ARG; }
@@ -251,12 +252,14 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   c->cfg = k;
   c->nw = nw;
   KernelKey key{k.physics == 1, k.ndim, k.ndir, k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM,
-                k.flux_scheme, k.limiter, k.typeboundspeed};
+                k.flux_scheme, k.limiter, k.typeboundspeed, k.precision == 1};
+  if (k.precision != 0 && k.precision != 1) return fail(AMRVAC_E_ARG, "precision must be 0 (fp64) or 1 (mixed)");
   if (std::getenv("AMRVAC_GENERIC_KERNELS")) { key.limiter = 0; key.boundspeed = 0; }
   bool found = lookup_hd(key, &c->ks) || lookup_mhd2(key, &c->ks) || lookup_mhd3(key, &c->ks);
   if (!found) {
     delete c;
-    return fail(AMRVAC_E_UNSUPPORTED, "no kernel for this physics/ndim/ndir/solver combination");
+    return fail(AMRVAC_E_UNSUPPORTED, key.mixed ? "no mixed-precision kernel for this scheme"
+                                                : "no kernel for this physics/ndim/ndir/solver combination");
   }
   cudaError_t e0;
   PhysParams &P = c->P;
@@ -665,6 +668,50 @@ int amrvac_gpu_run_timed(amrvac_ctx *c, int nsteps, double *total_ms, double *st
   if (total_ms) *total_ms = tot;
   if (stage_ms) *stage_ms = st;
   if (getdt_ms) *getdt_ms = gd;
+  return 0;
+}
+
+int amrvac_gpu_set_zchunk(amrvac_ctx *c, int zchunk) {
+  if (int r = check_ctx(c, false)) return r;
+  if (zchunk != 16 && zchunk != 8 && zchunk != 4) return fail(AMRVAC_E_ARG, "zchunk must be 16, 8 or 4");
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+  c->zchunk = zchunk;
+  return 0;
+}
+
+int amrvac_gpu_autotune(amrvac_ctx *c, int reps, int *best_zchunk, double *best_ms) {
+  if (int r = check_ctx(c, true)) return r;
+  if (reps <= 0) reps = 3;
+  if (c->cfg.ndim != 3) {
+    if (best_zchunk) *best_zchunk = 16;
+    if (best_ms) *best_ms = 0.0;
+    return 0;
+  }
+  const int cand[3] = {16, 8, 4};
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  int best = c->zchunk;
+  float bms = 1e30f;
+  for (int q = 0; q < 3; ++q) {
+    c->zchunk = cand[q];
+    int r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);  // warm
+    CK(cudaEventRecord(a, c->stream));
+    for (int i = 0; i < reps && !r; ++i) r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);
+    CK(cudaEventRecord(b, c->stream));
+    CK(cudaEventSynchronize(b));
+    if (r) { cudaEventDestroy(a); cudaEventDestroy(b); return r; }
+    float ms;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    ms /= reps;
+    if (ms < bms) { bms = ms; best = cand[q]; }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  c->zchunk = best;
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+  if (best_zchunk) *best_zchunk = best;
+  if (best_ms) *best_ms = bms;
   return 0;
 }
 

@@ -5,6 +5,15 @@ namespace amrvac {
 
 bool lookup_mhd2(const KernelKey &k, KernelSet *out) {
   if (!k.mhd || k.ndim != 2) return false;
+  if (k.mixed) {
+    if (k.ndir == 3 && k.glm && k.solver == SOLVER_HLLD && k.limiter == LIM_CADA3 && k.boundspeed == BS_EINFELDT) {
+      *out = Launch<true, 3, true, 2, SOLVER_HLLD, LIM_CADA3, BS_EINFELDT, float>::set();
+      return true;
+    }
+    if (k.ndir == 3 && k.glm && k.solver == SOLVER_HLLD) { *out = Launch<true, 3, true, 2, SOLVER_HLLD, 0, 0, float>::set(); return true; }
+    if (k.ndir == 3 && !k.glm && k.solver == SOLVER_HLL) { *out = Launch<true, 3, false, 2, SOLVER_HLL, 0, 0, float>::set(); return true; }
+    return false;
+  }
   // compile-time limiter / bound speed for the field-loop regression schemes
   if (k.ndir == 3 && k.glm && k.solver == SOLVER_HLLD && k.limiter == LIM_CADA3 && k.boundspeed == BS_EINFELDT) {
     *out = Launch<true, 3, true, 2, SOLVER_HLLD, LIM_CADA3, BS_EINFELDT>::set();

@@ -54,9 +54,9 @@ __global__ void __launch_bounds__(256) getdt_kernel(const GetdtArgs A) {
       double cm;
       if constexpr (MHD) {
         double cf;
-        if (d == 0) cf = fast_speed<NDIR, V::B0 + 0>(w, A.P);
-        else if (d == 1) cf = fast_speed<NDIR, V::B0 + (NDIR > 1 ? 1 : 0)>(w, A.P);
-        else cf = fast_speed<NDIR, V::B0 + (NDIR > 2 ? 2 : 0)>(w, A.P);
+        if (d == 0) cf = fast_speed<double, NDIR, V::B0 + 0>(w, A.P);
+        else if (d == 1) cf = fast_speed<double, NDIR, V::B0 + (NDIR > 1 ? 1 : 0)>(w, A.P);
+        else cf = fast_speed<double, NDIR, V::B0 + (NDIR > 2 ? 2 : 0)>(w, A.P);
         cm = fabs(w[V::M0 + d]) + cf;
       } else {
         cm = fabs(w[V::M0 + d]) + sqrt(A.P.gamma * w[V::E] / w[V::RHO]);
@@ -126,7 +126,7 @@ __global__ void riemann_points_kernel(const PointArgs A) {
     wL[v] = A.a[(size_t)p * NW + ov];
     wR[v] = A.b[(size_t)p * NW + ov];
   }
-  face_from_states<MHD, NDIR, GLM, NDIM, SOLVER, 0>(wL, wR, A.P, A.cg, F);
+  face_from_states<double, MHD, NDIR, GLM, NDIM, SOLVER, 0>(wL, wR, A.P, A.cg, F);
 #pragma unroll
   for (int v = 0; v < NW; ++v) A.out[(size_t)p * NW + orig_index<MHD, NDIR, D>(v)] = F[v];
 }
@@ -140,7 +140,7 @@ __global__ void flux_points_kernel(const PointArgs A) {
   double wc[NW], w[NW], f[NW];
 #pragma unroll
   for (int v = 0; v < NW; ++v) { wc[v] = A.a[(size_t)p * NW + v]; w[v] = A.b[(size_t)p * NW + v]; }
-  phys_flux<MHD, NDIR, GLM, D>(wc, w, A.cg, f);
+  phys_flux<double, MHD, NDIR, GLM, D>(wc, w, A.cg, f);
 #pragma unroll
   for (int v = 0; v < NW; ++v) A.out[(size_t)p * NW + v] = f[v];
 }
@@ -158,8 +158,8 @@ __global__ void cbounds_points_kernel(const PointArgs A) {
     lp[v] = A.c[(size_t)p * NW + v]; rp[v] = A.d[(size_t)p * NW + v];
   }
   double cmax, cmin = 0.0;
-  if (A.out2) cbounds<MHD, NDIR, GLM, D, true>(lc, rc, lp, rp, A.P, cmax, cmin);
-  else cbounds<MHD, NDIR, GLM, D, false>(lc, rc, lp, rp, A.P, cmax, cmin);
+  if (A.out2) cbounds<double, MHD, NDIR, GLM, D, true>(lc, rc, lp, rp, A.P, cmax, cmin);
+  else cbounds<double, MHD, NDIR, GLM, D, false>(lc, rc, lp, rp, A.P, cmax, cmin);
   A.out[p] = cmax;
   if (A.out2) A.out2[p] = cmin;
 }
@@ -175,16 +175,16 @@ struct KernelSet {
   size_t stage_smem = 0;
 };
 
-template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM = 0, int BS = 0>
+template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM = 0, int BS = 0, class TF = double>
 struct Launch {
   using V = Vars<MHD, NDIR, GLM>;
-  static constexpr size_t SMEM = Tile<V::NW, NDIM>::BYTES;
+  static constexpr size_t SMEM = Tile<TF, V::NW, NDIM>::BYTES;
   static cudaError_t prepare() {
-    return cudaFuncSetAttribute(fv_stage_kernel<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>,
+    return cudaFuncSetAttribute(fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
   }
   static cudaError_t stage(const StageArgs &A, int nctas, cudaStream_t s) {
-    fv_stage_kernel<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
+    fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
     return cudaGetLastError();
   }
   static cudaError_t getdt(const GetdtArgs &A, cudaStream_t s) {
@@ -245,6 +245,7 @@ struct KernelKey {
   int solver;
   int limiter;     // used to pick a compile-time specialised stage kernel
   int boundspeed;
+  bool mixed;      // FP32 face arithmetic (mixed form)
 };
 
 bool lookup_hd(const KernelKey &k, KernelSet *out);

@@ -43,7 +43,14 @@ struct Vars {
 };
 
 __device__ __forceinline__ double fsign(double a, double b) { return copysign(a, b); }
+__device__ __forceinline__ float fsign(float a, float b) { return copysignf(a, b); }
+// single-precision division / reciprocal of the mixed form: IEEE (correctly rounded)
+__device__ __forceinline__ float rcp_(float y) { return 1.0f / y; }
+__device__ __forceinline__ float div_(float x, float y) { return x / y; }
 
+#ifndef AMRVAC_IEEE_DIV
+#define AMRVAC_NR_DIV 1
+#endif
 #ifdef AMRVAC_NR_DIV
 // Reciprocal and quotient by Newton-Raphson iteration from a single-precision
 // seed (Markstein, "IA-64 and Elementary Functions", 2000, ch. 8): each step
@@ -90,19 +97,19 @@ __device__ __forceinline__ void to_primitive(double *w, const PhysParams &P) {
 }
 
 // hd_to_conserved (mod_hd_phys.t:677-700) / mhd_to_conserved_origin (mod_mhd_phys.t:1562-1579)
-template <bool MHD, int NDIR, bool GLM>
-__device__ __forceinline__ void to_conserved(double *w, const PhysParams &P) {
+template <class T, bool MHD, int NDIR, bool GLM>
+__device__ __forceinline__ void to_conserved(T *w, const PhysParams &P) {
   using V = Vars<MHD, NDIR, GLM>;
-  double v2 = w[V::M0] * w[V::M0];
+  T v2 = w[V::M0] * w[V::M0];
 #pragma unroll
   for (int c = 1; c < NDIR; ++c) v2 = v2 + w[V::M0 + c] * w[V::M0 + c];
   if constexpr (MHD) {
-    double b2 = w[V::B0] * w[V::B0];
+    T b2 = w[V::B0] * w[V::B0];
 #pragma unroll
     for (int c = 1; c < NDIR; ++c) b2 = b2 + w[V::B0 + c] * w[V::B0 + c];
-    w[V::E] = w[V::E] * P.inv_gamma_1 + 0.5 * (v2 * w[V::RHO] + b2);
+    w[V::E] = w[V::E] * T(P.inv_gamma_1) + T(0.5) * (v2 * w[V::RHO] + b2);
   } else {
-    w[V::E] = w[V::E] * P.inv_gamma_1 + 0.5 * v2 * w[V::RHO];
+    w[V::E] = w[V::E] * T(P.inv_gamma_1) + T(0.5) * v2 * w[V::RHO];
   }
 #pragma unroll
   for (int c = 0; c < NDIR; ++c) w[V::M0 + c] = w[V::RHO] * w[V::M0 + c];
@@ -111,38 +118,38 @@ __device__ __forceinline__ void to_conserved(double *w, const PhysParams &P) {
 // Small-value check and "replace" fix on one state (hd_check_w mod_hd_phys.t:648-674,
 // mhd_check_w_origin mod_mhd_phys.t:1452-1473, replace branches mod_hd_phys.t:1436-1466
 // and mod_mhd_phys.t:2208-2222).  Returns true if the state was flagged.
-template <bool MHD, int NDIR, bool GLM>
-__device__ __forceinline__ bool small_values(double *w, bool primitive, const PhysParams &P) {
+template <class T, bool MHD, int NDIR, bool GLM>
+__device__ __forceinline__ bool small_values(T *w, bool primitive, const PhysParams &P) {
   using V = Vars<MHD, NDIR, GLM>;
-  const bool frho = w[V::RHO] < P.small_density;
-  double m2 = w[V::M0] * w[V::M0];
+  const bool frho = w[V::RHO] < T(P.small_density);
+  T m2 = w[V::M0] * w[V::M0];
 #pragma unroll
   for (int c = 1; c < NDIR; ++c) m2 = m2 + w[V::M0 + c] * w[V::M0 + c];
-  double b2 = 0.0;
+  T b2 = T(0.0);
   if constexpr (MHD) {
     b2 = w[V::B0] * w[V::B0];
 #pragma unroll
     for (int c = 1; c < NDIR; ++c) b2 = b2 + w[V::B0 + c] * w[V::B0 + c];
   }
   bool fe;
-  if (primitive) fe = w[V::E] < P.small_pressure;
-  else if (MHD) fe = w[V::E] - 0.5 * (m2 / w[V::RHO] + b2) < P.small_e;
-  else fe = P.gamma_1 * (w[V::E] - 0.5 * m2 / w[V::RHO]) < P.small_pressure;
+  if (primitive) fe = w[V::E] < T(P.small_pressure);
+  else if (MHD) fe = w[V::E] - T(0.5) * (m2 / w[V::RHO] + b2) < T(P.small_e);
+  else fe = T(P.gamma_1) * (w[V::E] - T(0.5) * m2 / w[V::RHO]) < T(P.small_pressure);
   if (!(frho || fe)) return false;
   if (P.small_values_method == 1) {
     if (frho) {
-      w[V::RHO] = P.small_density;
+      w[V::RHO] = T(P.small_density);
 #pragma unroll
-      for (int c = 0; c < NDIR; ++c) w[V::M0 + c] = 0.0;
+      for (int c = 0; c < NDIR; ++c) w[V::M0 + c] = T(0.0);
     }
     if ((!MHD && frho) || fe) {
       if (primitive) {
-        w[V::E] = P.small_pressure;
+        w[V::E] = T(P.small_pressure);
       } else {
-        double mm = w[V::M0] * w[V::M0];
+        T mm = w[V::M0] * w[V::M0];
 #pragma unroll
         for (int c = 1; c < NDIR; ++c) mm = mm + w[V::M0 + c] * w[V::M0 + c];
-        w[V::E] = MHD ? P.small_e + 0.5 * (mm / w[V::RHO] + b2) : P.small_e + 0.5 * mm / w[V::RHO];
+        w[V::E] = MHD ? T(P.small_e) + T(0.5) * (mm / w[V::RHO] + b2) : T(P.small_e) + T(0.5) * mm / w[V::RHO];
       }
     }
   }
@@ -152,9 +159,9 @@ __device__ __forceinline__ bool small_values(double *w, bool primitive, const Ph
 // ------------------------------------------------------------------ fluxes
 // hd_get_flux (mod_hd_phys.t:1097-1146) / mhd_get_flux (mod_mhd_phys.t:3810-3889).
 // wc: conserved, w: primitive state at the face; D: face normal (0-based).
-template <bool MHD, int NDIR, bool GLM, int D>
-__device__ __forceinline__ void phys_flux(const double *wc, const double *w, double cg,
-                                          double *f) {
+template <class T, bool MHD, int NDIR, bool GLM, int D>
+__device__ __forceinline__ void phys_flux(const T *wc, const T *w, T cg,
+                                          T *f) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int MN = V::M0 + D;
   if constexpr (!MHD) {
@@ -168,12 +175,12 @@ __device__ __forceinline__ void phys_flux(const double *wc, const double *w, dou
     f[V::RHO] = w[MN] * w[V::RHO];
 #pragma unroll
     for (int c = 0; c < NDIR; ++c) f[V::M0 + c] = wc[MN] * w[V::M0 + c] - w[BN] * w[V::B0 + c];
-    double b2 = w[V::B0] * w[V::B0];
+    T b2 = w[V::B0] * w[V::B0];
 #pragma unroll
     for (int c = 1; c < NDIR; ++c) b2 = b2 + w[V::B0 + c] * w[V::B0 + c];
-    const double ptotal = w[V::E] + 0.5 * b2;
+    const T ptotal = w[V::E] + T(0.5) * b2;
     f[MN] = f[MN] + ptotal;
-    double bv = w[V::B0] * w[V::M0];
+    T bv = w[V::B0] * w[V::M0];
 #pragma unroll
     for (int c = 1; c < NDIR; ++c) bv = bv + w[V::B0 + c] * w[V::M0 + c];
     f[V::E] = w[MN] * (wc[V::E] + ptotal) - w[BN] * bv;
@@ -187,46 +194,46 @@ __device__ __forceinline__ void phys_flux(const double *wc, const double *w, dou
 }
 
 // mhd_get_csound_prim (mod_mhd_phys.t:3329-3379): fast magnetosonic speed.
-template <int NDIR, int BN>
-__device__ __forceinline__ double fast_speed(const double *w, const PhysParams &P) {
+template <class T, int NDIR, int BN>
+__device__ __forceinline__ T fast_speed(const T *w, const PhysParams &P) {
   constexpr int RHO = 0, E = NDIR + 1, B0 = NDIR + 2;
-  const double inv_rho = rcp_(w[RHO]);
-  const double cs = P.gamma * w[E] * inv_rho;
-  double b2 = w[B0] * w[B0];
+  const T inv_rho = rcp_(w[RHO]);
+  const T cs = T(P.gamma) * w[E] * inv_rho;
+  T b2 = w[B0] * w[B0];
 #pragma unroll
   for (int c = 1; c < NDIR; ++c) b2 = b2 + w[B0 + c] * w[B0 + c];
-  const double cfast2 = b2 * inv_rho + cs;
-  double av = cfast2 * cfast2 - 4.0 * cs * (w[BN] * w[BN]) * inv_rho;
-  if (av < 0.0) av = 0.0;
-  return sqrt(0.5 * (cfast2 + sqrt(av)));
+  const T cfast2 = b2 * inv_rho + cs;
+  T av = cfast2 * cfast2 - T(4.0) * cs * (w[BN] * w[BN]) * inv_rho;
+  if (av < T(0.0)) av = T(0.0);
+  return sqrt(T(0.5) * (cfast2 + sqrt(av)));
 }
 
 // hd_get_cbounds (mod_hd_phys.t:891-1001) / mhd_get_cbounds (mod_mhd_phys.t:3037-3127).
 // WITH_MIN=false gives the tvdlf form (cmax only).  Returns a status bit.
-template <bool MHD, int NDIR, bool GLM, int D, bool WITH_MIN, int BS = 0>
-__device__ __forceinline__ uint32_t cbounds(const double *wLC, const double *wRC, const double *wLp,
-                                            const double *wRp, const PhysParams &P, double &cmax,
-                                            double &cmin) {
+template <class T, bool MHD, int NDIR, bool GLM, int D, bool WITH_MIN, int BS = 0>
+__device__ __forceinline__ uint32_t cbounds(const T *wLC, const T *wRC, const T *wLp,
+                                            const T *wRp, const PhysParams &P, T &cmax,
+                                            T &cmin) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int MN = V::M0 + D;
   uint32_t st = 0;
   const int bsel = BS ? BS : P.boundspeed;
   if (bsel == BS_EINFELDT) {
-    const double tmp1 = sqrt(wLp[V::RHO]);
-    const double tmp2 = sqrt(wRp[V::RHO]);
-    const double tmp3 = rcp_(tmp1 + tmp2);
-    const double umean = (wLp[MN] * tmp1 + wRp[MN] * tmp2) * tmp3;
-    const double dv = wRp[MN] - wLp[MN];
-    double dmean;
+    const T tmp1 = sqrt(wLp[V::RHO]);
+    const T tmp2 = sqrt(wRp[V::RHO]);
+    const T tmp3 = rcp_(tmp1 + tmp2);
+    const T umean = (wLp[MN] * tmp1 + wRp[MN] * tmp2) * tmp3;
+    const T dv = wRp[MN] - wLp[MN];
+    T dmean;
     if constexpr (MHD) {
-      const double csL = fast_speed<NDIR, V::B0 + D>(wLp, P);
-      const double csR = fast_speed<NDIR, V::B0 + D>(wRp, P);
+      const T csL = fast_speed<T, NDIR, V::B0 + D>(wLp, P);
+      const T csR = fast_speed<T, NDIR, V::B0 + D>(wRp, P);
       dmean = sqrt((tmp1 * (csL * csL) + tmp2 * (csR * csR)) * tmp3 +
-                   0.5 * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
+                   T(0.5) * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
     } else {
-      const double csL = P.gamma * wLp[V::E] / wLp[V::RHO];
-      const double csR = P.gamma * wRp[V::E] / wRp[V::RHO];
-      dmean = sqrt((tmp1 * csL + tmp2 * csR) * tmp3 + 0.5 * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
+      const T csL = T(P.gamma) * wLp[V::E] / wLp[V::RHO];
+      const T csR = T(P.gamma) * wRp[V::E] / wRp[V::RHO];
+      dmean = sqrt((tmp1 * csL + tmp2 * csR) * tmp3 + T(0.5) * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
     }
     if (WITH_MIN) {
       cmin = umean - dmean;
@@ -236,45 +243,45 @@ __device__ __forceinline__ uint32_t cbounds(const double *wLC, const double *wRC
     }
   } else if (bsel == BS_CMAXMEAN) {
     if constexpr (MHD) {
-      double wm[V::NW];
+      T wm[V::NW];
 #pragma unroll
-      for (int v = 0; v < V::NW; ++v) wm[v] = 0.5 * (wLp[v] + wRp[v]);
-      const double cs = fast_speed<NDIR, V::B0 + D>(wm, P);
+      for (int v = 0; v < V::NW; ++v) wm[v] = T(0.5) * (wLp[v] + wRp[v]);
+      const T cs = fast_speed<T, NDIR, V::B0 + D>(wm, P);
       if (WITH_MIN) {
-        cmax = fmax(wm[MN] + cs, 0.0);
-        cmin = fmin(wm[MN] - cs, 0.0);
+        cmax = fmax(wm[MN] + cs, T(0.0));
+        cmin = fmin(wm[MN] - cs, T(0.0));
       } else {
         cmax = fabs(wm[MN]) + cs;
       }
     } else {
-      double wm[V::NW];
+      T wm[V::NW];
 #pragma unroll
-      for (int v = 0; v < V::NW; ++v) wm[v] = 0.5 * (wLC[v] + wRC[v]);
-      const double tmp1 = wm[MN] / wm[V::RHO];
-      double m2 = wm[V::M0] * wm[V::M0];
+      for (int v = 0; v < V::NW; ++v) wm[v] = T(0.5) * (wLC[v] + wRC[v]);
+      const T tmp1 = wm[MN] / wm[V::RHO];
+      T m2 = wm[V::M0] * wm[V::M0];
 #pragma unroll
       for (int c = 1; c < NDIR; ++c) m2 = m2 + wm[V::M0 + c] * wm[V::M0 + c];
-      double pth = P.gamma_1 * (wm[V::E] - 0.5 * m2 / wm[V::RHO]);
+      T pth = T(P.gamma_1) * (wm[V::E] - T(0.5) * m2 / wm[V::RHO]);
       if (P.fix_small_values) {
-        if (pth < P.small_pressure) pth = P.small_pressure;
+        if (pth < T(P.small_pressure)) pth = T(P.small_pressure);
       } else if (P.check_small_values) {
-        if (pth < P.small_pressure) st |= ST_SMALL_VALUE;
+        if (pth < T(P.small_pressure)) st |= ST_SMALL_VALUE;
       }
-      const double cs = sqrt(P.gamma * pth / wm[V::RHO]);
+      const T cs = sqrt(P.gamma * pth / wm[V::RHO]);
       if (WITH_MIN) {
-        cmax = fmax(tmp1 + cs, 0.0);
-        cmin = fmin(tmp1 - cs, 0.0);
+        cmax = fmax(tmp1 + cs, T(0.0));
+        cmin = fmin(tmp1 - cs, T(0.0));
       } else {
         cmax = fabs(tmp1) + cs;
       }
     }
   } else {  // cmaxleftright
-    double cs;
+    T cs;
     if constexpr (MHD) {
-      cs = fmax(fast_speed<NDIR, V::B0 + D>(wLp, P), fast_speed<NDIR, V::B0 + D>(wRp, P));
+      cs = fmax(fast_speed<T, NDIR, V::B0 + D>(wLp, P), fast_speed<T, NDIR, V::B0 + D>(wRp, P));
     } else {
-      const double csL = P.gamma * wLp[V::E] / wLp[V::RHO];
-      const double csR = P.gamma * wRp[V::E] / wRp[V::RHO];
+      const T csL = T(P.gamma) * wLp[V::E] / wLp[V::RHO];
+      const T csR = T(P.gamma) * wRp[V::E] / wRp[V::RHO];
       cs = fmax(sqrt(csL), sqrt(csR));
     }
     if (WITH_MIN) cmin = fmin(wLp[MN], wRp[MN]) - cs;
@@ -286,56 +293,56 @@ __device__ __forceinline__ uint32_t cbounds(const double *wLC, const double *wRC
 // ------------------------------------------------------------------ limiters
 // dwlimiter2 (mod_limiter.t:128-334) for one cell: a = dwC(ix) (forward
 // difference), b = dwC(ix-1) (backward difference).  LEFT selects ldw, else rdw.
-template <bool LEFT>
-__device__ __forceinline__ double slope_impl(int lim, double a, double b, double rdelinv) {
-  constexpr double qsmall = 1.0e-12, qsmall2 = 2.0e-12;
-  constexpr double eps = 1.4901161193847656e-08;  // sqrt(epsilon(1d0)) = 2**-26
-  constexpr double c_mcbeta = 1.4, cadalfa = 0.5, cadbeta = 2.0, cadgamma = 1.6;
-  constexpr double cadepsilon = 1.0e-14, invcadepsilon = 1.0e14;
-  constexpr double third = 1.0 / 3.0;
+template <class T, bool LEFT>
+__device__ __forceinline__ T slope_impl(int lim, T a, T b, T rdelinv) {
+  constexpr T qsmall = T(1.0e-12), qsmall2 = T(2.0e-12);
+  constexpr T eps = T(1.4901161193847656e-08);  // sqrt(epsilon(1d0)) = 2**-26
+  constexpr T c_mcbeta = T(1.4), cadalfa = T(0.5), cadbeta = T(2.0), cadgamma = T(1.6);
+  constexpr T cadepsilon = T(1.0e-14), invcadepsilon = T(1.0e14);
+  constexpr T third = T(1.0) / T(3.0);
   switch (lim) {
     case LIM_MINMOD: {
-      const double t = fsign(1.0, a);
-      return t * fmax(0.0, fmin(fabs(a), t * b));
+      const T t = fsign(T(1.0), a);
+      return t * fmax(T(0.0), fmin(fabs(a), t * b));
     }
     case LIM_VANLEER:
-      return div_(2.0 * fmax(b * a, 0.0), a + b + qsmall);
+      return div_(T(2.0) * fmax(b * a, T(0.0)), a + b + qsmall);
     case LIM_CADA3: {
       // branch-free: both the asymptotic and the limited form are evaluated
       // and the reference's three-way choice is made with selects
-      const double tmpeta = (a * a + b * b) * rdelinv;
-      const double t = LEFT ? div_(b, a + fsign(eps, a)) : div_(a, b + fsign(eps, b));
-      const double A = (2.0 + t) * third;
-      const double lim2 = fmax(0.0, fmin(A, fmax(-(cadalfa * t), fmin(fmin(cadbeta * t, A), cadgamma))));
-      const double t2 = (tmpeta - 1.0) * invcadepsilon;
-      const double blend = 0.5 * ((1.0 - t2) * A + (1.0 + t2) * lim2);
-      const double phi = tmpeta <= 1.0 - cadepsilon ? A : (tmpeta >= 1.0 + cadepsilon ? lim2 : blend);
+      const T tmpeta = (a * a + b * b) * rdelinv;
+      const T t = LEFT ? div_(b, a + fsign(eps, a)) : div_(a, b + fsign(eps, b));
+      const T A = (T(2.0) + t) * third;
+      const T lim2 = fmax(T(0.0), fmin(A, fmax(-(cadalfa * t), fmin(fmin(cadbeta * t, A), cadgamma))));
+      const T t2 = (tmpeta - T(1.0)) * invcadepsilon;
+      const T blend = T(0.5) * ((T(1.0) - t2) * A + (T(1.0) + t2) * lim2);
+      const T phi = tmpeta <= T(1.0) - cadepsilon ? A : (tmpeta >= T(1.0) + cadepsilon ? lim2 : blend);
       return phi * (LEFT ? a : b);
     }
     case LIM_WOODWARD: {
-      const double t = fsign(1.0, a);
-      return 2.0 * t * fmax(0.0, fmin(fmin(fabs(a), t * b), t * 0.25 * (b + a)));
+      const T t = fsign(T(1.0), a);
+      return T(2.0) * t * fmax(T(0.0), fmin(fmin(fabs(a), t * b), t * T(0.25) * (b + a)));
     }
     case LIM_MCBETA: {
-      const double t = fsign(1.0, a);
-      return t * fmax(0.0, fmin(fmin(c_mcbeta * fabs(a), c_mcbeta * t * b), t * 0.5 * (b + a)));
+      const T t = fsign(T(1.0), a);
+      return t * fmax(T(0.0), fmin(fmin(c_mcbeta * fabs(a), c_mcbeta * t * b), t * T(0.5) * (b + a)));
     }
     case LIM_SUPERBEE: {
-      const double t = fsign(1.0, a);
-      return t * fmax(fmax(0.0, fmin(2.0 * fabs(a), t * b)), fmin(fabs(a), 2.0 * t * b));
+      const T t = fsign(T(1.0), a);
+      return t * fmax(fmax(T(0.0), fmin(T(2.0) * fabs(a), t * b)), fmin(fabs(a), T(2.0) * t * b));
     }
     case LIM_ALBADA:
       return (b * (a * a + qsmall) + a * (b * b + qsmall)) / (a * a + b * b + qsmall2);
     case LIM_KOREN: {
-      const double t = fsign(1.0, a);
-      const double t2 = fmin(2.0 * fabs(a), 2.0 * t * b);
-      if (LEFT) return t * fmax(0.0, fmin(t2, (b * t + 2.0 * fabs(a)) * third));
-      return t * fmax(0.0, fmin(t2, (2.0 * b * t + fabs(a)) * third));
+      const T t = fsign(T(1.0), a);
+      const T t2 = fmin(T(2.0) * fabs(a), T(2.0) * t * b);
+      if (LEFT) return t * fmax(T(0.0), fmin(t2, (b * t + T(2.0) * fabs(a)) * third));
+      return t * fmax(T(0.0), fmin(t2, (T(2.0) * b * t + fabs(a)) * third));
     }
     default: {  // cada
-      const double t = LEFT ? b / (a + fsign(eps, a)) : a / (b + fsign(eps, b));
-      const double t2 = (2.0 + t) * third;
-      return fmax(0.0, fmin(t2, fmax(-(cadalfa * t), fmin(fmin(cadbeta * t, t2), cadgamma)))) *
+      const T t = LEFT ? b / (a + fsign(eps, a)) : a / (b + fsign(eps, b));
+      const T t2 = (T(2.0) + t) * third;
+      return fmax(T(0.0), fmin(t2, fmax(-(cadalfa * t), fmin(fmin(cadbeta * t, t2), cadgamma)))) *
              (LEFT ? a : b);
     }
   }
@@ -343,9 +350,9 @@ __device__ __forceinline__ double slope_impl(int lim, double a, double b, double
 
 // LIM != 0 fixes the limiter at compile time (the switch folds away);
 // LIM == 0 selects it at run time from lim_rt.
-template <bool LEFT, int LIM>
-__device__ __forceinline__ double limited_slope(int lim_rt, double a, double b, double rdelinv) {
-  return slope_impl<LEFT>(LIM ? LIM : lim_rt, a, b, rdelinv);
+template <class T, bool LEFT, int LIM>
+__device__ __forceinline__ T limited_slope(int lim_rt, T a, T b, T rdelinv) {
+  return slope_impl<T, LEFT>(LIM ? LIM : lim_rt, a, b, rdelinv);
 }
 
 // Index in the reference variable order of entry v of a state whose vector

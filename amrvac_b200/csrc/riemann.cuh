@@ -19,32 +19,32 @@ struct FluxTypes {
 };
 
 // get_Riemann_flux_tvdlf (mod_finite_volume.t:348-379)
-template <int NW>
-__device__ __forceinline__ void riemann_tvdlf(const double *wLC, const double *wRC, const double *fL,
-                                              const double *fR, double cmax, double tvdlfeps,
-                                              double *F) {
-  const double fac = -(0.5 * tvdlfeps * cmax);
+template <class T, int NW>
+__device__ __forceinline__ void riemann_tvdlf(const T *wLC, const T *wRC, const T *fL,
+                                              const T *fR, T cmax, T tvdlfeps,
+                                              T *F) {
+  const T fac = -(T(0.5) * tvdlfeps * cmax);
 #pragma unroll
   for (int v = 0; v < NW; ++v) {
-    double f = 0.5 * (fL[v] + fR[v]);
+    T f = T(0.5) * (fL[v] + fR[v]);
     F[v] = f + fac * (wRC[v] - wLC[v]);
   }
 }
 
 // get_Riemann_flux_hll (mod_finite_volume.t:381-437)
-template <bool MHD, int NDIR, bool GLM, int NDIM, int D>
-__device__ __forceinline__ void riemann_hll(const double *wLC, const double *wRC, const double *fL,
-                                            const double *fR, double cmax, double cmin,
-                                            double tvdlfeps, double *F) {
+template <class T, bool MHD, int NDIR, bool GLM, int NDIM, int D>
+__device__ __forceinline__ void riemann_hll(const T *wLC, const T *wRC, const T *fL,
+                                            const T *fR, T cmax, T cmin,
+                                            T tvdlfeps, T *F) {
   using V = Vars<MHD, NDIR, GLM>;
   using FT = FluxTypes<MHD, NDIM, GLM>;
 #pragma unroll
   for (int v = 0; v < V::NW; ++v) {
     if (FT::bn_tvdlf && v == V::B0 + D) {
-      F[v] = -(tvdlfeps * 0.5 * fmax(cmax, fabs(cmin))) * (wRC[v] - wLC[v]);
-    } else if (cmin >= 0.0) {
+      F[v] = -(tvdlfeps * T(0.5) * fmax(cmax, fabs(cmin))) * (wRC[v] - wLC[v]);
+    } else if (cmin >= T(0.0)) {
       F[v] = fL[v];
-    } else if (cmax <= 0.0) {
+    } else if (cmax <= T(0.0)) {
       F[v] = fR[v];
     } else {
       F[v] = div_(cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v]), cmax - cmin);
@@ -54,15 +54,15 @@ __device__ __forceinline__ void riemann_hll(const double *wLC, const double *wRC
 
 // get_Riemann_flux_hllc (mod_finite_volume.t:439-504) + hd_get_lCD / hd_get_wCD
 // (mod_hd_hllc.t:56-257); HD only, no hllcd diffusion, flathllc=.false.
-template <int NDIR, int D>
-__device__ __forceinline__ void riemann_hllc_hd(const double *wLC, const double *wRC, const double *fL,
-                                                const double *fR, double cmax, double cmin,
-                                                double *F) {
+template <class T, int NDIR, int D>
+__device__ __forceinline__ void riemann_hllc_hd(const T *wLC, const T *wRC, const T *fL,
+                                                const T *fR, T cmax, T cmin,
+                                                T *F) {
   using V = Vars<false, NDIR, false>;
   constexpr int NW = V::NW, MN = V::M0 + D;
   int patchf = 1;
-  if (cmin >= 0.0) patchf = -2;
-  else if (cmax <= 0.0) patchf = 2;
+  if (cmin >= T(0.0)) patchf = -2;
+  else if (cmax <= T(0.0)) patchf = 2;
   if (patchf == -2) {
 #pragma unroll
     for (int v = 0; v < NW; ++v) F[v] = fL[v];
@@ -73,86 +73,86 @@ __device__ __forceinline__ void riemann_hllc_hd(const double *wLC, const double 
     for (int v = 0; v < NW; ++v) F[v] = fR[v];
     return;
   }
-  double whll[NW], Fhll[NW];
+  T whll[NW], Fhll[NW];
 #pragma unroll
   for (int v = 0; v < NW; ++v) {
     Fhll[v] = (cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v])) / (cmax - cmin);
     whll[v] = (cmax * wRC[v] - cmin * wLC[v] + fL[v] - fR[v]) / (cmax - cmin);
   }
-  double lambdaCD = whll[MN] / whll[V::RHO];
+  T lambdaCD = whll[MN] / whll[V::RHO];
   bool cond = true;
-  if (cmin < 0.0 && lambdaCD > 0.0 && lambdaCD < cmax) {
+  if (cmin < T(0.0) && lambdaCD > T(0.0) && lambdaCD < cmax) {
     patchf = -1;
-  } else if (cmax > 0.0 && lambdaCD < 0.0 && lambdaCD > cmin) {
+  } else if (cmax > T(0.0) && lambdaCD < T(0.0) && lambdaCD > cmin) {
     patchf = 1;
   } else if (lambdaCD >= cmax || lambdaCD <= cmin) {
-    lambdaCD = 0.0;
+    lambdaCD = T(0.0);
     patchf = 3;
     cond = false;
   }
-  if (cond && lambdaCD == 0.0) patchf = (-cmin >= cmax) ? 1 : -1;
+  if (cond && lambdaCD == T(0.0)) patchf = (-cmin >= cmax) ? 1 : -1;
   if (patchf == 3) {
 #pragma unroll
     for (int v = 0; v < NW; ++v) F[v] = Fhll[v];
     return;
   }
   const bool right = (patchf == 1);
-  const double *wSub = right ? wRC : wLC;
-  const double *fSub = right ? fR : fL;
-  const double cspeed = right ? cmax : cmin;
-  const double vSub = wSub[MN] / wSub[V::RHO];
-  const double csmls = 1.0 / (cspeed - lambdaCD);
-  double wCD[NW];
+  const T *wSub = right ? wRC : wLC;
+  const T *fSub = right ? fR : fL;
+  const T cspeed = right ? cmax : cmin;
+  const T vSub = wSub[MN] / wSub[V::RHO];
+  const T csmls = T(1.0) / (cspeed - lambdaCD);
+  T wCD[NW];
   wCD[V::RHO] = wSub[V::RHO] * (cspeed - vSub) * csmls;
 #pragma unroll
   for (int c = 0; c < NDIR; ++c) {
     if (c != D) wCD[V::M0 + c] = (cspeed * wSub[V::M0 + c] - fSub[V::M0 + c]) * csmls;
     else wCD[V::M0 + c] = wCD[V::RHO] * lambdaCD;
   }
-  const double pCD = wSub[V::RHO] * (cspeed - vSub) * (lambdaCD - vSub) + fSub[MN] - wSub[MN] * vSub;
+  const T pCD = wSub[V::RHO] * (cspeed - vSub) * (lambdaCD - vSub) + fSub[MN] - wSub[MN] * vSub;
   wCD[V::E] = (cspeed * wSub[V::E] - fSub[V::E] + lambdaCD * pCD) * csmls;
 #pragma unroll
   for (int v = 0; v < NW; ++v) F[v] = fSub[v] + cspeed * (wCD[v] - wSub[v]);
 }
 
 // get_Riemann_flux_hlld (mod_finite_volume.t:507-729), no B0 / equilibrium split.
-template <int NDIR, bool GLM, int NDIM, int D>
-__device__ __forceinline__ void riemann_hlld(const double *wLC, const double *wRC, const double *wLp,
-                                             const double *wRp, const double *fL, const double *fR,
-                                             double sR, double sL, double *F) {
+template <class T, int NDIR, bool GLM, int NDIM, int D>
+__device__ __forceinline__ void riemann_hlld(const T *wLC, const T *wRC, const T *wLp,
+                                             const T *wRp, const T *fL, const T *fR,
+                                             T sR, T sL, T *F) {
   using V = Vars<true, NDIR, GLM>;
   using FT = FluxTypes<true, NDIM, GLM>;
   constexpr int NW = V::NW, RHO = V::RHO, E = V::E, M0 = V::M0, B0 = V::B0;
   constexpr int ip1 = D, ip2 = (D + 1) % NDIR, ip3 = (D + 2) % NDIR;
   constexpr int m1 = M0 + ip1, m2 = M0 + ip2, m3 = M0 + ip3;
   constexpr int b1 = B0 + ip1, b2 = B0 + ip2, b3 = B0 + ip3;
-  const double Bx = div_(sR * wRC[b1] - sL * wLC[b1], sR - sL);
-  double bR2 = wRC[B0] * wRC[B0], bL2 = wLC[B0] * wLC[B0];
+  const T Bx = div_(sR * wRC[b1] - sL * wLC[b1], sR - sL);
+  T bR2 = wRC[B0] * wRC[B0], bL2 = wLC[B0] * wLC[B0];
 #pragma unroll
   for (int c = 1; c < NDIR; ++c) {
     bR2 = bR2 + wRC[B0 + c] * wRC[B0 + c];
     bL2 = bL2 + wLC[B0 + c] * wLC[B0 + c];
   }
-  const double ptR = wRp[E] + 0.5 * bR2;
-  const double ptL = wLp[E] + 0.5 * bL2;
-  const double vR = wRp[m1], vL = wLp[m1];
-  const double suR = (sR - vR) * wRC[RHO];
-  const double suL = (sL - vL) * wLC[RHO];
-  const double sm = div_(suR * vR - suL * vL - ptR + ptL, suR - suL);
+  const T ptR = wRp[E] + T(0.5) * bR2;
+  const T ptL = wLp[E] + T(0.5) * bL2;
+  const T vR = wRp[m1], vL = wLp[m1];
+  const T suR = (sR - vR) * wRC[RHO];
+  const T suL = (sL - vL) * wLC[RHO];
+  const T sm = div_(suR * vR - suL * vL - ptR + ptL, suR - suL);
   // star states w1 (velocities in the momentum slots until the final conversion)
-  double w1R[NW], w1L[NW], w2R[NW], w2L[NW];
+  T w1R[NW], w1L[NW], w2R[NW], w2L[NW];
   w1R[m1] = sm; w1L[m1] = sm; w2R[m1] = sm; w2L[m1] = sm;
   w1R[b1] = Bx; w1L[b1] = Bx;
   w1R[RHO] = div_(suR, sR - sm);
   w1L[RHO] = div_(suL, sL - sm);
-  double r1R = suR * (sR - sm) - Bx * Bx;
-  if (r1R != 0.0) r1R = rcp_(r1R);
-  double r1L = suL * (sL - sm) - Bx * Bx;
-  if (r1L != 0.0) r1L = rcp_(r1L);
+  T r1R = suR * (sR - sm) - Bx * Bx;
+  if (r1R != T(0.0)) r1R = rcp_(r1R);
+  T r1L = suL * (sL - sm) - Bx * Bx;
+  if (r1L != T(0.0)) r1L = rcp_(r1L);
   w1R[m2] = wRp[m2] - Bx * wRC[b2] * (sm - vR) * r1R;
   w1L[m2] = wLp[m2] - Bx * wLC[b2] * (sm - vL) * r1L;
-  double pb2R = (suR * (sR - vR) - Bx * Bx) * r1R;
-  double pb2L = (suL * (sL - vL) - Bx * Bx) * r1L;
+  T pb2R = (suR * (sR - vR) - Bx * Bx) * r1R;
+  T pb2L = (suL * (sL - vL) - Bx * Bx) * r1L;
   if constexpr (NDIR == 3) {
     w1R[m3] = wRp[m3] - Bx * wRC[b3] * (sm - vR) * r1R;
     w1L[m3] = wLp[m3] - Bx * wLC[b3] * (sm - vL) * r1L;
@@ -161,10 +161,10 @@ __device__ __forceinline__ void riemann_hlld(const double *wLC, const double *wR
   }
   w1R[b2] = wRC[b2] * pb2R;
   w1L[b2] = wLC[b2] * pb2L;
-  const double pts = suR * (sm - vR) + ptR;  // w1R(p_) = w1L(p_)
+  const T pts = suR * (sm - vR) + ptR;  // w1R(p_) = w1L(p_)
   {
-    double vbR = wRp[M0] * wRC[B0], vbL = wLp[M0] * wLC[B0];
-    double v1bR = w1R[M0] * w1R[B0], v1bL = w1L[M0] * w1L[B0];
+    T vbR = wRp[M0] * wRC[B0], vbL = wLp[M0] * wLC[B0];
+    T v1bR = w1R[M0] * w1R[B0], v1bL = w1L[M0] * w1L[B0];
 #pragma unroll
     for (int c = 1; c < NDIR; ++c) {
       vbR = vbR + wRp[M0 + c] * wRC[B0 + c];
@@ -177,12 +177,12 @@ __device__ __forceinline__ void riemann_hlld(const double *wLC, const double *wR
   }
   w2R[RHO] = w1R[RHO]; w2L[RHO] = w1L[RHO];
   w2R[b1] = Bx; w2L[b1] = Bx;
-  const double sqR = sqrt(w1R[RHO]);
-  const double sqL = sqrt(w1L[RHO]);
-  const double tmp = rcp_(sqR + sqL);
-  const double signBx = copysign(1.0, Bx);
-  const double s1R = sm + div_(fabs(Bx), sqR);
-  const double s1L = sm - div_(fabs(Bx), sqL);
+  const T sqR = sqrt(w1R[RHO]);
+  const T sqL = sqrt(w1L[RHO]);
+  const T tmp = rcp_(sqR + sqL);
+  const T signBx = copysign(T(1.0), Bx);
+  const T s1R = sm + div_(fabs(Bx), sqR);
+  const T s1L = sm - div_(fabs(Bx), sqL);
   w2R[m2] = (sqL * w1L[m2] + sqR * w1R[m2] + (w1R[b2] - w1L[b2]) * signBx) * tmp;
   w2L[m2] = w2R[m2];
   w2R[b2] = (sqL * w1R[b2] + sqR * w1L[b2] + sqL * sqR * (w1R[m2] - w1L[m2]) * signBx) * tmp;
@@ -194,8 +194,8 @@ __device__ __forceinline__ void riemann_hlld(const double *wLC, const double *wR
     w2L[b3] = w2R[b3];
   }
   {
-    double a1R = w1R[M0] * w1R[B0], a2R = w2R[M0] * w2R[B0];
-    double a1L = w1L[M0] * w1L[B0], a2L = w2L[M0] * w2L[B0];
+    T a1R = w1R[M0] * w1R[B0], a2R = w2R[M0] * w2R[B0];
+    T a1L = w1L[M0] * w1L[B0], a2L = w2L[M0] * w2L[B0];
 #pragma unroll
     for (int c = 1; c < NDIR; ++c) {
       a1R = a1R + w1R[M0 + c] * w1R[B0 + c];
@@ -215,34 +215,34 @@ __device__ __forceinline__ void riemann_hlld(const double *wLC, const double *wR
   }
   if constexpr (GLM) {
     // psi star values are never used (flux_special); keep them defined.
-    w1R[V::PSI] = w1L[V::PSI] = w2R[V::PSI] = w2L[V::PSI] = 0.0;
+    w1R[V::PSI] = w1L[V::PSI] = w2R[V::PSI] = w2L[V::PSI] = T(0.0);
   }
   // region selection (Miyoshi eq. 66), branch-free: the candidate fluxes of
   // the chosen side are formed for every variable and the region picks one
   int region;
-  if (sL > 0.0) region = 0;
-  else if (s1L >= 0.0) region = 1;
-  else if (sm >= 0.0) region = 2;
-  else if (s1R >= 0.0) region = 3;
-  else if (sR >= 0.0) region = 4;
+  if (sL > T(0.0)) region = 0;
+  else if (s1L >= T(0.0)) region = 1;
+  else if (sm >= T(0.0)) region = 2;
+  else if (s1R >= T(0.0)) region = 3;
+  else if (sR >= T(0.0)) region = 4;
   else region = 5;  // sR < 0 (a NaN speed also lands here)
   const bool left = region <= 2;
   const bool one_star = region == 1 || region == 4;
   const bool two_star = region == 2 || region == 3;
-  const double c1 = left ? sL : sR;
-  const double c2 = left ? s1L : s1R;
+  const T c1 = left ? sL : sR;
+  const T c2 = left ? s1L : s1R;
 #pragma unroll
   for (int v = 0; v < NW; ++v) {
     if (FT::bn_special && (v == b1 || v == V::PSI)) {
       F[v] = fL[v];
       continue;
     }
-    const double fs = left ? fL[v] : fR[v];
-    const double ws = left ? wLC[v] : wRC[v];
-    const double w1 = left ? w1L[v] : w1R[v];
-    const double w2 = left ? w2L[v] : w2R[v];
-    const double t1 = fs + c1 * (w1 - ws);
-    const double t2 = t1 + c2 * (w2 - w1);
+    const T fs = left ? fL[v] : fR[v];
+    const T ws = left ? wLC[v] : wRC[v];
+    const T w1 = left ? w1L[v] : w1R[v];
+    const T w2 = left ? w2L[v] : w2R[v];
+    const T t1 = fs + c1 * (w1 - ws);
+    const T t2 = t1 + c2 * (w2 - w1);
     F[v] = two_star ? t2 : (one_star ? t1 : fs);
   }
 }

@@ -32,13 +32,19 @@ namespace amrvac {
 
 constexpr int BN = 16;               // cells per block edge
 #ifndef AMRVAC_STAGE_THREADS
-#define AMRVAC_STAGE_THREADS 288
+#define AMRVAC_STAGE_THREADS 256
 #endif
 #ifndef AMRVAC_STAGE_MINB
-#define AMRVAC_STAGE_MINB 1
+#define AMRVAC_STAGE_MINB 2
 #endif
-// 288 = 9 warps: one thread per face of a 17x16 face plane.  With 256 threads
-// the 16 extra faces of an x/y phase take a second (partial) round.
+#ifndef AMRVAC_STAGE_MINB_MIXED
+#define AMRVAC_STAGE_MINB_MIXED 3
+#endif
+// 256 threads x 2 CTAs per SM (128 registers per thread, shared memory
+// 104 KB per CTA for nw = 9): the two CTAs hide each other's barrier and
+// dependency stalls; the 16 extra faces of an x/y phase (17x16 faces per
+// plane) take a second, partial round.  (288 threads x 1 CTA, one face per
+// thread, measured 17-25 % slower on 3-D MHD.)
 constexpr int STAGE_THREADS = AMRVAC_STAGE_THREADS;
 
 enum : int { BCK_PERIODIC = 0, BCK_CONT = 1, BCK_MIRROR = 2 };
@@ -133,7 +139,7 @@ __device__ __forceinline__ uint32_t load_prim(const StageArgs &A, int b, int i, 
   }
   uint32_t st = 0;
   if (A.P.fix_small_values) {
-    if (small_values<MHD, NDIR, GLM>(w, false, A.P) && A.P.small_values_method != 1) st |= ST_SMALL_VALUE;
+    if (small_values<double, MHD, NDIR, GLM>(w, false, A.P) && A.P.small_values_method != 1) st |= ST_SMALL_VALUE;
   }
   to_primitive<MHD, NDIR, GLM>(w, A.P);
   return st;
@@ -142,87 +148,60 @@ __device__ __forceinline__ uint32_t load_prim(const StageArgs &A, int b, int i, 
 // Interface flux from reconstructed primitive left/right states: small-value
 // fix, to_conserved, GLM modify_wLR, physical fluxes, cbounds, Riemann solver
 // (src/mod_finite_volume.t:1217-1222, 200-245).  wLp/wRp are modified.
-template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int BS>
-__device__ __forceinline__ uint32_t face_from_states(double *wLp, double *wRp, const PhysParams &P,
-                                                     double cg, double *F) {
+template <class T, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int BS>
+__device__ __forceinline__ uint32_t face_from_states(T *wLp, T *wRp, const PhysParams &P, T cg, T *F) {
   constexpr int D = 0;  // states arrive rotated: the face normal is component 0
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
   uint32_t st = 0;
   if (P.fix_small_values) {
-    bool fl = small_values<MHD, NDIR, GLM>(wLp, true, P);
-    bool fr = small_values<MHD, NDIR, GLM>(wRp, true, P);
+    bool fl = small_values<T, MHD, NDIR, GLM>(wLp, true, P);
+    bool fr = small_values<T, MHD, NDIR, GLM>(wRp, true, P);
     if ((fl || fr) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
   }
-  double wLC[NW], wRC[NW];
+  T wLC[NW], wRC[NW];
 #pragma unroll
   for (int v = 0; v < NW; ++v) { wLC[v] = wLp[v]; wRC[v] = wRp[v]; }
-  to_conserved<MHD, NDIR, GLM>(wLC, P);
-  to_conserved<MHD, NDIR, GLM>(wRC, P);
+  to_conserved<T, MHD, NDIR, GLM>(wLC, P);
+  to_conserved<T, MHD, NDIR, GLM>(wRC, P);
   if constexpr (MHD && GLM) {
     // mhd_modify_wLR (src/mhd/mod_mhd_phys.t:6352-6372)
     constexpr int BNI = V::B0 + D, PS = V::PSI, E = V::E;
-    const double dB = wRp[BNI] - wLp[BNI];
-    const double dPsi = wRp[PS] - wLp[PS];
-    const double nb = 0.5 * (wRp[BNI] + wLp[BNI] - dPsi / cg);
-    const double np = 0.5 * (wRp[PS] + wLp[PS] - dB * cg);
+    const T dB = wRp[BNI] - wLp[BNI];
+    const T dPsi = wRp[PS] - wLp[PS];
+    const T nb = T(0.5) * (wRp[BNI] + wLp[BNI] - dPsi / cg);
+    const T np = T(0.5) * (wRp[PS] + wLp[PS] - dB * cg);
     wLp[BNI] = nb; wLp[PS] = np; wRp[BNI] = nb; wRp[PS] = np;
-    wRC[E] = wRC[E] - 0.5 * (wRC[BNI] * wRC[BNI]);
-    wLC[E] = wLC[E] - 0.5 * (wLC[BNI] * wLC[BNI]);
+    wRC[E] = wRC[E] - T(0.5) * (wRC[BNI] * wRC[BNI]);
+    wLC[E] = wLC[E] - T(0.5) * (wLC[BNI] * wLC[BNI]);
     wRC[BNI] = nb; wRC[PS] = np; wLC[BNI] = nb; wLC[PS] = np;
-    wRC[E] = wRC[E] + 0.5 * (nb * nb);
-    wLC[E] = wLC[E] + 0.5 * (nb * nb);
+    wRC[E] = wRC[E] + T(0.5) * (nb * nb);
+    wLC[E] = wLC[E] + T(0.5) * (nb * nb);
   }
-  double fL[NW], fR[NW];
-  phys_flux<MHD, NDIR, GLM, D>(wLC, wLp, cg, fL);
-  phys_flux<MHD, NDIR, GLM, D>(wRC, wRp, cg, fR);
-  double cmax, cmin = 0.0;
+  T fL[NW], fR[NW];
+  phys_flux<T, MHD, NDIR, GLM, D>(wLC, wLp, cg, fL);
+  phys_flux<T, MHD, NDIR, GLM, D>(wRC, wRp, cg, fR);
+  T cmax, cmin = T(0.0);
   if constexpr (SOLVER == SOLVER_TVDLF) {
-    st |= cbounds<MHD, NDIR, GLM, D, false, BS>(wLC, wRC, wLp, wRp, P, cmax, cmin);
-    riemann_tvdlf<NW>(wLC, wRC, fL, fR, cmax, P.tvdlfeps, F);
+    st |= cbounds<T, MHD, NDIR, GLM, D, false, BS>(wLC, wRC, wLp, wRp, P, cmax, cmin);
+    riemann_tvdlf<T, NW>(wLC, wRC, fL, fR, cmax, T(P.tvdlfeps), F);
   } else {
-    st |= cbounds<MHD, NDIR, GLM, D, true, BS>(wLC, wRC, wLp, wRp, P, cmax, cmin);
+    st |= cbounds<T, MHD, NDIR, GLM, D, true, BS>(wLC, wRC, wLp, wRp, P, cmax, cmin);
     if constexpr (SOLVER == SOLVER_HLL) {
-      riemann_hll<MHD, NDIR, GLM, NDIM, D>(wLC, wRC, fL, fR, cmax, cmin, P.tvdlfeps, F);
+      riemann_hll<T, MHD, NDIR, GLM, NDIM, D>(wLC, wRC, fL, fR, cmax, cmin, T(P.tvdlfeps), F);
     } else if constexpr (SOLVER == SOLVER_HLLC) {
       static_assert(!MHD, "HLLC is implemented for HD only");
-      riemann_hllc_hd<NDIR, D>(wLC, wRC, fL, fR, cmax, cmin, F);
+      riemann_hllc_hd<T, NDIR, D>(wLC, wRC, fL, fR, cmax, cmin, F);
     } else {
       static_assert(MHD, "HLLD needs MHD");
-      riemann_hlld<NDIR, GLM, NDIM, D>(wLC, wRC, wLp, wRp, fL, fR, cmax, cmin, F);
+      riemann_hlld<T, NDIR, GLM, NDIM, D>(wLC, wRC, wLp, wRp, fL, fR, cmax, cmin, F);
     }
   }
   return st;
 }
 
-// One face normal to direction D: primitives of the 4-cell stencil (cells
-// L-1, L, R, R+1) are read through `ld(o, v)` with o in {-2,-1,0,1} relative
-// to the right cell and v in the reference variable order.  The states are
-// rotated so that one direction-generic face routine serves x, y and z; the
-// flux F is returned in the reference order.
-template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS, int D, class LD>
-__device__ __forceinline__ uint32_t face_flux(const LD &ld, const PhysParams &P, double cg,
-                                              double rdelinv, double *F) {
-  using V = Vars<MHD, NDIR, GLM>;
-  constexpr int NW = V::NW;
-  double wLp[NW], wRp[NW];
-#pragma unroll
-  for (int v = 0; v < NW; ++v) {
-    const int ov = orig_index<MHD, NDIR, D>(v);
-    const double q0 = ld(-2, ov), q1 = ld(-1, ov), q2 = ld(0, ov), q3 = ld(1, ov);
-    const double d0 = q1 - q0, d1 = q2 - q1, d2 = q3 - q2;
-    wLp[v] = q1 + 0.5 * limited_slope<true, LIM>(P.limiter, d1, d0, rdelinv);
-    wRp[v] = q2 - 0.5 * limited_slope<false, LIM>(P.limiter, d2, d1, rdelinv);
-  }
-  double Fr[NW];
-  const uint32_t st = face_from_states<MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, cg, Fr);
-#pragma unroll
-  for (int v = 0; v < NW; ++v) F[orig_index<MHD, NDIR, D>(v)] = Fr[v];
-  return st;
-}
-
 // Shared-memory tile (sizes in doubles).
-template <int NW, int NDIM>
+template <class TF, int NW, int NDIM>
 struct Tile {
   static constexpr int NSLOT = NDIM == 3 ? 4 : 1;
   static constexpr int PLANE = BN * BN;
@@ -232,16 +211,16 @@ struct Tile {
   static constexpr int HC = NW * 16;                     // [v][r][c] corners
   static constexpr int FB = NW * (BN + 1) * BN;          // [v][face]
   static constexpr int TOTAL = RING + HX + HY + HC + FB;
-  static constexpr size_t BYTES = sizeof(double) * TOTAL;
+  static constexpr size_t BYTES = sizeof(TF) * TOTAL;
 };
 
 __device__ __forceinline__ int halo_slot(int c) { return c < 0 ? c + 2 : c - (BN - 2); }
 
-template <int NW, int NDIM>
+template <class TF, int NW, int NDIM>
 struct TileView {
-  double *ring, *hx, *hy, *hc, *fb;
-  __device__ TileView(double *s) {
-    using T = Tile<NW, NDIM>;
+  TF *ring, *hx, *hy, *hc, *fb;
+  __device__ TileView(TF *s) {
+    using T = Tile<TF, NW, NDIM>;
     ring = s;
     hx = ring + T::RING;
     hy = hx + T::HX;
@@ -249,7 +228,7 @@ struct TileView {
     fb = hc + T::HC;
   }
   // primitive v at in-plane (i, j) in [-2, 17]^2 of the plane held in `slot`
-  __device__ __forceinline__ double at(int slot, int v, int i, int j) const {
+  __device__ __forceinline__ TF at(int slot, int v, int i, int j) const {
     const bool ii = (unsigned)i < (unsigned)BN, jj = (unsigned)j < (unsigned)BN;
     if (ii && jj) return ring[(slot * NW + v) * (BN * BN) + j * BN + i];
     if (jj) return hx[(v * BN + j) * 4 + halo_slot(i)];
@@ -259,7 +238,7 @@ struct TileView {
   // Offset (in doubles from the tile start) of variable 0 at in-plane (i, j)
   // of the plane in `slot`, and the stride between variables there; branch-free.
   __device__ __forceinline__ void addr(int slot, int i, int j, int &base, int &stride) const {
-    using T = Tile<NW, NDIM>;
+    using T = Tile<TF, NW, NDIM>;
     const bool ii = (unsigned)i < (unsigned)BN, jj = (unsigned)j < (unsigned)BN;
     const int hi = halo_slot(i), hj = halo_slot(j);
     const int oc = slot * NW * (BN * BN) + j * BN + i;
@@ -269,7 +248,7 @@ struct TileView {
     base = ii ? (jj ? oc : oy) : (jj ? ox : oz);
     stride = ii ? (jj ? BN * BN : 4 * BN) : (jj ? 4 * BN : 16);
   }
-  __device__ __forceinline__ double &center(int slot, int v, int i, int j) {
+  __device__ __forceinline__ TF &center(int slot, int v, int i, int j) {
     return ring[(slot * NW + v) * (BN * BN) + j * BN + i];
   }
 };
@@ -283,13 +262,20 @@ __device__ __forceinline__ int orig_index_rt(int v, int D) {
   return v;
 }
 
-template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS>
-__global__ void __launch_bounds__(STAGE_THREADS, AMRVAC_STAGE_MINB) fv_stage_kernel(const StageArgs A) {
+// TF: arithmetic type of the face computation — double (plain FP64 path) or
+// float (mixed form: reconstruction, wave speeds, fluxes and Riemann solver in
+// FP32; conserved state, pressure recovery, RK algebra, flux-divergence
+// accumulation, sources and the small-value fix of wnew in FP64).
+template <class TF, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS>
+__global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_MINB : AMRVAC_STAGE_MINB_MIXED)
+    fv_stage_kernel(const StageArgs A) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
   constexpr int FB = (BN + 1) * BN;  // face-buffer stride per variable
-  extern __shared__ double smem[];
-  TileView<NW, NDIM> tv(smem);
+  constexpr bool FP64 = sizeof(TF) == 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TF *smem = reinterpret_cast<TF *>(smem_raw);
+  TileView<TF, NW, NDIM> tv(smem);
   const int t = threadIdx.x;
   const int nchunk = NDIM == 3 ? BN / A.zchunk : 1;
   const int b = blockIdx.x / nchunk;
@@ -333,14 +319,14 @@ __global__ void __launch_bounds__(STAGE_THREADS, AMRVAC_STAGE_MINB) fv_stage_ker
       st |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, ci, cj, kk, w);
       const int s2 = NDIM == 3 ? (kk & 3) : 0;
 #pragma unroll
-      for (int v = 0; v < NW; ++v) tv.center(s2, v, ci, cj) = w[v];
+      for (int v = 0; v < NW; ++v) tv.center(s2, v, ci, cj) = TF(w[v]);
     }
     // ---- x/y halo strips (and corners for Linde) of plane k
     const int nhalo = update ? (need_corners ? 144 : 128) : 0;
     if (t < nhalo) {
       const int h = t;
       int i, j, stride;
-      double *dst;
+      TF *dst;
       if (h < 64) {
         j = h >> 2;
         const int c = h & 3;
@@ -363,7 +349,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, AMRVAC_STAGE_MINB) fv_stage_ker
       double w[NW];
       st |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, i, j, k, w);
 #pragma unroll
-      for (int v = 0; v < NW; ++v) dst[v * stride] = w[v];
+      for (int v = 0; v < NW; ++v) dst[v * stride] = TF(w[v]);
     }
     // ---- RK combination wnew0 = a*base + b*in (src/mod_advance.t:254-266)
     double acc[NW];
@@ -387,8 +373,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, AMRVAC_STAGE_MINB) fv_stage_ker
         int fi, fj;
         if (D == 0) { fj = f / (BN + 1); fi = f - fj * (BN + 1); }
         else { fj = f >> 4; fi = f & (BN - 1); }
-        const double rd = D == 0 ? rdel[0] : (D == 1 ? rdel[1] : rdel[2]);
-        double wLp[NW], wRp[NW];
+        const TF rd = TF(D == 0 ? rdel[0] : (D == 1 ? rdel[1] : rdel[2]));
+        TF wLp[NW], wRp[NW];
         // shared-memory offsets of the 4 stencil cells (variable 0) and the
         // per-variable strides, computed once per face
         int base[4], strd[4];
@@ -404,33 +390,46 @@ __global__ void __launch_bounds__(STAGE_THREADS, AMRVAC_STAGE_MINB) fv_stage_ker
 #pragma unroll
         for (int v = 0; v < NW; ++v) {
           const int ov = orig_index_rt<MHD, NDIR>(v, D);
-          double q[4];
+          TF q[4];
 #pragma unroll
           for (int o = 0; o < 4; ++o) q[o] = smem[base[o] + ov * strd[o]];
-          const double d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
-          wLp[v] = q[1] + 0.5 * limited_slope<true, LIM>(P.limiter, d1, d0, rd);
-          wRp[v] = q[2] - 0.5 * limited_slope<false, LIM>(P.limiter, d2, d1, rd);
+          const TF d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
+          wLp[v] = q[1] + TF(0.5) * limited_slope<TF, true, LIM>(P.limiter, d1, d0, rd);
+          wRp[v] = q[2] - TF(0.5) * limited_slope<TF, false, LIM>(P.limiter, d2, d1, rd);
         }
-        double Fr[NW];
-        st |= face_from_states<MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, cg, Fr);
+        TF Fr[NW];
+        st |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, TF(cg), Fr);
+        // FP64: the scaled flux fC = -qdt/dx * f as in the reference; mixed:
+        // the FP32 flux, scaled in FP64 by the accumulating cell thread
         const double sc = D == 0 ? dxinv[0] : (D == 1 ? dxinv[1] : dxinv[2]);
 #pragma unroll
-        for (int v = 0; v < NW; ++v) tv.fb[orig_index_rt<MHD, NDIR>(v, D) * FB + f] = sc * Fr[v];
+        for (int v = 0; v < NW; ++v) {
+          const int ov = orig_index_rt<MHD, NDIR>(v, D);
+          if constexpr (FP64) tv.fb[ov * FB + f] = sc * Fr[v];
+          else tv.fb[ov * FB + f] = Fr[v];
+        }
       }
       __syncthreads();
       if (cell_thread) {
+        const double sc = FP64 ? 1.0 : (D == 0 ? dxinv[0] : (D == 1 ? dxinv[1] : dxinv[2]));
         if (D == 0) {
           const int f = cj * (BN + 1) + ci;
 #pragma unroll
-          for (int v = 0; v < NW; ++v) acc[v] = acc[v] + tv.fb[v * FB + f + 1] - tv.fb[v * FB + f];
+          for (int v = 0; v < NW; ++v) {
+            if constexpr (FP64) acc[v] = acc[v] + tv.fb[v * FB + f + 1] - tv.fb[v * FB + f];
+            else acc[v] = acc[v] + sc * double(tv.fb[v * FB + f + 1]) - sc * double(tv.fb[v * FB + f]);
+          }
         } else if (D == 1) {
           const int f = cj * BN + ci;
 #pragma unroll
-          for (int v = 0; v < NW; ++v) acc[v] = acc[v] + tv.fb[v * FB + f + BN] - tv.fb[v * FB + f];
+          for (int v = 0; v < NW; ++v) {
+            if constexpr (FP64) acc[v] = acc[v] + tv.fb[v * FB + f + BN] - tv.fb[v * FB + f];
+            else acc[v] = acc[v] + sc * double(tv.fb[v * FB + f + BN]) - sc * double(tv.fb[v * FB + f]);
+          }
         } else if constexpr (NDIM == 3) {
 #pragma unroll
           for (int v = 0; v < NW; ++v) {
-            const double fz = tv.fb[v * FB + t];
+            const double fz = FP64 ? double(tv.fb[v * FB + t]) : sc * double(tv.fb[v * FB + t]);
             if (update) acc[v] = acc[v] + fz - fz_prev[v];
             fz_prev[v] = fz;
           }
@@ -441,7 +440,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, AMRVAC_STAGE_MINB) fv_stage_ker
     if (update && cell_thread) {
       // ---- small values on wnew (src/mod_finite_volume.t:326-333)
       if (P.fix_small_values) {
-        if (small_values<MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
+        if (small_values<double, MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
       }
       // ---- unsplit divB sources (addsource2 -> mhd_add_source)
       if constexpr (MHD) {
@@ -459,14 +458,14 @@ __global__ void __launch_bounds__(STAGE_THREADS, AMRVAC_STAGE_MINB) fv_stage_ker
             }
             if (P.glm_extended) {
               auto nbv = [&](int d, int s, int v) -> double {  // wCT at cell +/- e_d
-                if (d == 0) return tv.at(slot, v, ci + s, cj);
-                if (d == 1) return tv.at(slot, v, ci, cj + s);
-                return tv.ring[((((k + s) & 3)) * NW + v) * (BN * BN) + cj * BN + ci];
+                if (d == 0) return double(tv.at(slot, v, ci + s, cj));
+                if (d == 1) return double(tv.at(slot, v, ci, cj + s));
+                return double(tv.ring[((((k + s) & 3)) * NW + v) * (BN * BN) + cj * BN + ci]);
               };
 #pragma unroll
               for (int d = 0; d < NDIM; ++d) {
                 const double g = ((nbv(d, 1, V::PSI) - nbv(d, -1, V::PSI)) * 0.5) / dx[d];
-                acc[V::E] = acc[V::E] - qsrc * tv.at(slot, V::B0 + d, ci, cj) * g;
+                acc[V::E] = acc[V::E] - qsrc * double(tv.at(slot, V::B0 + d, ci, cj)) * g;
               }
               double divb = 0.0;
 #pragma unroll
@@ -474,14 +473,14 @@ __global__ void __launch_bounds__(STAGE_THREADS, AMRVAC_STAGE_MINB) fv_stage_ker
                 divb = divb + 0.5 * (nbv(d, 1, V::B0 + d) - nbv(d, -1, V::B0 + d)) * (1.0 / dx[d]);
 #pragma unroll
               for (int c = 0; c < NDIR; ++c)
-                acc[V::M0 + c] = acc[V::M0 + c] - qsrc * tv.at(slot, V::B0 + c, ci, cj) * divb;
+                acc[V::M0 + c] = acc[V::M0 + c] - qsrc * double(tv.at(slot, V::B0 + c, ci, cj)) * divb;
             }
           } else if (P.divb == DIVB_LINDE) {
             if constexpr (NDIM == 2) {
               // add_source_linde (src/mhd/mod_mhd_phys.t:5599-5665), uniform grid
               auto divb_at = [&](int i, int j) -> double {
-                double d = 0.5 * (tv.at(slot, V::B0, i + 1, j) - tv.at(slot, V::B0, i - 1, j)) * (1.0 / dx[0]);
-                d = d + 0.5 * (tv.at(slot, V::B0 + 1, i, j + 1) - tv.at(slot, V::B0 + 1, i, j - 1)) * (1.0 / dx[1]);
+                double d = 0.5 * (double(tv.at(slot, V::B0, i + 1, j)) - double(tv.at(slot, V::B0, i - 1, j))) * (1.0 / dx[0]);
+                d = d + 0.5 * (double(tv.at(slot, V::B0 + 1, i, j + 1)) - double(tv.at(slot, V::B0 + 1, i, j - 1))) * (1.0 / dx[1]);
                 return d;
               };
               const double inv2 = 1.0 / (dx[0] * dx[0]) + 1.0 / (dx[1] * dx[1]);
@@ -493,12 +492,12 @@ __global__ void __launch_bounds__(STAGE_THREADS, AMRVAC_STAGE_MINB) fv_stage_ker
                 g = g / dx[d];
                 g = g * P.divbdiff / inv2;
                 acc[V::B0 + d] = acc[V::B0 + d] + g;
-                acc[V::E] = acc[V::E] + tv.at(slot, V::B0 + d, ci, cj) * g;
+                acc[V::E] = acc[V::E] + double(tv.at(slot, V::B0 + d, ci, cj)) * g;
               }
             }
           }
           if (P.fix_small_values) {
-            if (small_values<MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
+            if (small_values<double, MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
           }
         }
       }

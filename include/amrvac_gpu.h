@@ -111,6 +111,9 @@ typedef struct amrvac_cfg {
   double dtmin;             /* 1e-10 */
   int typeboundary[6][AMRVAC_MAX_NW]; /* [min1,max1,min2,max2,min3,max3][iw] */
   int zchunk;               /* tuning: z-planes per CTA in 3-D (0 = auto) */
+  int precision;            /* 0 = plain FP64; 1 = mixed: FP32 reconstruction, wave
+                               speeds, fluxes, Riemann solver; FP64 conserved state,
+                               pressure recovery, accumulation, sources, small values */
 } amrvac_cfg;
 
 typedef struct amrvac_ctx amrvac_ctx;
@@ -168,6 +171,13 @@ int amrvac_gpu_run_timed(amrvac_ctx *ctx, int nsteps, double *total_ms, double *
 /* Measured FP64 FMA throughput of the current device (TFLOP/s, 2 flops per
  * FMA) from an in-register FMA-chain kernel; the FP64 roofline denominator. */
 int amrvac_gpu_fp64_peak(double *tflops);
+/* Tile autotuner: times one stage (ps -> ps1, the state in ps is left
+ * unchanged) for each candidate z-chunk of the 3-D stage kernel (16, 8, 4
+ * planes per CTA), keeps the fastest for this context and returns it.
+ * Call after the state has been uploaded.  2-D: returns 16, no timing. */
+int amrvac_gpu_autotune(amrvac_ctx *ctx, int reps, int *best_zchunk, double *best_ms);
+/* Set the z-chunk directly (16, 8 or 4), e.g. from a cached tuning result. */
+int amrvac_gpu_set_zchunk(amrvac_ctx *ctx, int zchunk);
 /* Read back the last step's dt, cmax_global and global_time (synchronises). */
 int amrvac_gpu_get_time(amrvac_ctx *ctx, double *dt, double *cmax_global, double *global_time);
 
