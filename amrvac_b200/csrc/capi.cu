@@ -688,6 +688,10 @@ int amrvac_gpu_autotune(amrvac_ctx *c, int reps, int *best_zchunk, double *best_
     return 0;
   }
   const int cand[3] = {16, 8, 4};
+  // dt and cmax_global of the current state (GLM needs cmax_global > 0)
+  if (int r = launch_getdt(c, 0)) return r;
+  CK(launch_setdt_finalize(c->d_red, c->d_scal, c->d_status, c->stream));
+  ++c->launches;
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
