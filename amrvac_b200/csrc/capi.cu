@@ -80,7 +80,8 @@ struct amrvac_ctx {
   cudaGraphExec_t graph = nullptr;
   int64_t launches = 0;
   int64_t graph_nodes = 0;
-  int zchunk = 16;
+  int zchunk = 0;          // 0: persistent plane ranges; 16/8/4: one z-chunk per CTA
+  int wave_ctas = 1;       // resident stage CTAs on the device (one wave)
 };
 
 namespace {
@@ -119,7 +120,10 @@ StageArgs stage_args(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, doubl
 
 int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a, double b, double dtfactor) {
   StageArgs A = stage_args(c, reg_ct, reg_new, reg_base, a, b, dtfactor);
-  const int nctas = c->cfg.ndim == 3 ? c->nblocks * (16 / c->zchunk) : c->nblocks;
+  const long planes = (long)c->nblocks * (c->cfg.ndim == 3 ? 16 : 1);
+  int nctas;
+  if (c->zchunk > 0) nctas = c->cfg.ndim == 3 ? c->nblocks * (16 / c->zchunk) : c->nblocks;
+  else nctas = (int)std::min<long>(planes, c->wave_ctas);
   if (c->P.fix_small_values && c->P.small_values_method == 0)
     CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * c->nblocks, c->stream));
   CK(c->ks.stage(A, nctas, c->stream));
@@ -318,7 +322,13 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
     delete c;
     return cuda_fail(e0, "cudaFuncSetAttribute");
   }
-  c->zchunk = (k.zchunk == 8 || k.zchunk == 4 || k.zchunk == 16) ? k.zchunk : 16;
+  c->zchunk = (k.zchunk == 8 || k.zchunk == 4 || k.zchunk == 16) ? k.zchunk : 0;
+  {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    c->wave_ctas = nsm * c->ks.ctas_per_sm();
+  }
   c->per_block = 1;
   for (int d = 0; d < k.ndim; ++d) c->per_block *= 16;
   cudaError_t e;
@@ -673,7 +683,8 @@ int amrvac_gpu_run_timed(amrvac_ctx *c, int nsteps, double *total_ms, double *st
 
 int amrvac_gpu_set_zchunk(amrvac_ctx *c, int zchunk) {
   if (int r = check_ctx(c, false)) return r;
-  if (zchunk != 16 && zchunk != 8 && zchunk != 4) return fail(AMRVAC_E_ARG, "zchunk must be 16, 8 or 4");
+  if (zchunk != 16 && zchunk != 8 && zchunk != 4 && zchunk != 0)
+    return fail(AMRVAC_E_ARG, "zchunk must be 0 (persistent plane ranges), 16, 8 or 4");
   if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
   c->zchunk = zchunk;
   return 0;
@@ -682,12 +693,8 @@ int amrvac_gpu_set_zchunk(amrvac_ctx *c, int zchunk) {
 int amrvac_gpu_autotune(amrvac_ctx *c, int reps, int *best_zchunk, double *best_ms) {
   if (int r = check_ctx(c, true)) return r;
   if (reps <= 0) reps = 3;
-  if (c->cfg.ndim != 3) {
-    if (best_zchunk) *best_zchunk = 16;
-    if (best_ms) *best_ms = 0.0;
-    return 0;
-  }
-  const int cand[3] = {16, 8, 4};
+  const int ncand = c->cfg.ndim == 3 ? 4 : 2;
+  const int cand[4] = {0, 16, 8, 4};
   // dt and cmax_global of the current state (GLM needs cmax_global > 0)
   if (int r = launch_getdt(c, 0)) return r;
   CK(launch_setdt_finalize(c->d_red, c->d_scal, c->d_status, c->stream));
@@ -697,7 +704,7 @@ int amrvac_gpu_autotune(amrvac_ctx *c, int reps, int *best_zchunk, double *best_
   CK(cudaEventCreate(&b));
   int best = c->zchunk;
   float bms = 1e30f;
-  for (int q = 0; q < 3; ++q) {
+  for (int q = 0; q < ncand; ++q) {
     c->zchunk = cand[q];
     int r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);  // warm
     CK(cudaEventRecord(a, c->stream));

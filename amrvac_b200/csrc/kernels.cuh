@@ -167,6 +167,7 @@ __global__ void cbounds_points_kernel(const PointArgs A) {
 // ---------------------------------------------------------------- dispatch
 struct KernelSet {
   cudaError_t (*prepare)() = nullptr;
+  int (*ctas_per_sm)() = nullptr;
   cudaError_t (*stage)(const StageArgs &, int nctas, cudaStream_t) = nullptr;
   cudaError_t (*getdt)(const GetdtArgs &, cudaStream_t) = nullptr;
   cudaError_t (*riemann_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
@@ -186,6 +187,13 @@ struct Launch {
   static cudaError_t stage(const StageArgs &A, int nctas, cudaStream_t s) {
     fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
     return cudaGetLastError();
+  }
+  static int ctas_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>,
+                                                      STAGE_THREADS, SMEM) != cudaSuccess)
+      return 1;
+    return n > 0 ? n : 1;
   }
   static cudaError_t getdt(const GetdtArgs &A, cudaStream_t s) {
     getdt_kernel<MHD, NDIR, GLM, NDIM><<<A.nblocks, 256, 0, s>>>(A);
@@ -227,6 +235,7 @@ struct Launch {
   static KernelSet set() {
     KernelSet k;
     k.prepare = &prepare;
+    k.ctas_per_sm = &ctas_per_sm;
     k.stage = &stage;
     k.getdt = &getdt;
     k.riemann_points = &riemann_points;

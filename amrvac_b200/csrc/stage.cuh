@@ -277,17 +277,40 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
   TF *smem = reinterpret_cast<TF *>(smem_raw);
   TileView<TF, NW, NDIM> tv(smem);
   const int t = threadIdx.x;
-  const int nchunk = NDIM == 3 ? BN / A.zchunk : 1;
-  const int b = blockIdx.x / nchunk;
-  const int chunk = blockIdx.x - b * nchunk;
-  const int k0 = NDIM == 3 ? chunk * A.zchunk : 0;
-  const int k1 = NDIM == 3 ? k0 + A.zchunk : 1;
-  if (b >= A.nblocks) return;
+  // Work: global z-planes g = block*PL + k (PL = 16 in 3-D, 1 in 2-D).
+  // zchunk > 0: one z-chunk of one block per CTA.  zchunk == 0: persistent
+  // plane ranges — the grid is one wave of CTAs, each marching a contiguous
+  // range of planes across block boundaries and re-staging halo planes only
+  // where a new block starts.
+  constexpr int PL = NDIM == 3 ? BN : 1;
+  long g, gend;
+  if (A.zchunk > 0) {
+    const int nchunk = NDIM == 3 ? BN / A.zchunk : 1;
+    const int b0 = blockIdx.x / nchunk;
+    if (b0 >= A.nblocks) return;
+    g = (long)b0 * PL + (NDIM == 3 ? (blockIdx.x - b0 * nchunk) * A.zchunk : 0);
+    gend = g + (NDIM == 3 ? A.zchunk : 1);
+  } else {
+    const long total = (long)A.nblocks * PL;
+    g = (long)blockIdx.x * total / gridDim.x;
+    gend = (long)(blockIdx.x + 1) * total / gridDim.x;
+  }
 
   const PhysParams &P = A.P;
   const double dt = *A.dt_dev;
   const double qdt = A.dtfactor * dt;
   const double cg = GLM ? *A.cmax_dev : 0.0;
+  uint32_t st = 0;
+  const int ci = t & (BN - 1), cj = t >> 4;  // cell role for t < 256
+  const bool cell_thread = t < BN * BN;
+  const bool need_corners = MHD && !GLM && P.divb == DIVB_LINDE;
+#pragma unroll 1
+  while (g < gend) {
+  const int b = (int)(g / PL);
+  const int k0 = (int)(g - (long)b * PL);
+  const int k1 = (int)(k0 + ((gend - g) < (PL - k0) ? (gend - g) : (PL - k0)));
+  g += k1 - k0;
+  uint32_t stb = 0;  // status of this block's update
   double dx[3], dxinv[3], rdel[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -296,10 +319,6 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
     const double r = P.cada3_radius * dx[d];
     rdel[d] = 1.0 / (r * r);
   }
-  uint32_t st = 0;
-  const int ci = t & (BN - 1), cj = t >> 4;  // cell role for t < 256
-  const bool cell_thread = t < BN * BN;
-  const bool need_corners = MHD && !GLM && P.divb == DIVB_LINDE;
   double fz_prev[NDIM == 3 ? NW : 1];
 #pragma unroll
   for (int v = 0; v < (NDIM == 3 ? NW : 1); ++v) fz_prev[v] = 0.0;
@@ -316,7 +335,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
     if (cell_thread) {
       double w[NW];
       const int kk = NDIM == 3 ? k + 2 : 0;
-      st |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, ci, cj, kk, w);
+      stb |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, ci, cj, kk, w);
       const int s2 = NDIM == 3 ? (kk & 3) : 0;
 #pragma unroll
       for (int v = 0; v < NW; ++v) tv.center(s2, v, ci, cj) = TF(w[v]);
@@ -347,7 +366,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
         stride = 16;
       }
       double w[NW];
-      st |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, i, j, k, w);
+      stb |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, i, j, k, w);
 #pragma unroll
       for (int v = 0; v < NW; ++v) dst[v * stride] = TF(w[v]);
     }
@@ -398,7 +417,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
           wRp[v] = q[2] - TF(0.5) * limited_slope<TF, false, LIM>(P.limiter, d2, d1, rd);
         }
         TF Fr[NW];
-        st |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, TF(cg), Fr);
+        stb |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, TF(cg), Fr);
         // FP64: the scaled flux fC = -qdt/dx * f as in the reference; mixed:
         // the FP32 flux, scaled in FP64 by the accumulating cell thread
         const double sc = D == 0 ? dxinv[0] : (D == 1 ? dxinv[1] : dxinv[2]);
@@ -440,7 +459,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
     if (update && cell_thread) {
       // ---- small values on wnew (src/mod_finite_volume.t:326-333)
       if (P.fix_small_values) {
-        if (small_values<double, MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
+        if (small_values<double, MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) stb |= ST_SMALL_VALUE;
       }
       // ---- unsplit divB sources (addsource2 -> mhd_add_source)
       if constexpr (MHD) {
@@ -497,23 +516,23 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
             }
           }
           if (P.fix_small_values) {
-            if (small_values<double, MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
+            if (small_values<double, MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) stb |= ST_SMALL_VALUE;
           }
         }
       }
-      if (!isfinite(acc[V::RHO]) || !isfinite(acc[V::E])) st |= ST_NAN;
+      if (!isfinite(acc[V::RHO]) || !isfinite(acc[V::E])) stb |= ST_NAN;
 #pragma unroll
       for (int v = 0; v < NW; ++v) A.uout[cell_offset<NDIM>(b, NW, v, ci, cj, k)] = acc[v];
     }
-    // the next iteration overwrites ring slot (k-1)&3 and the halo strips,
-    // which the sources above read
-    if (NDIM == 3) __syncthreads();
+    // the next iteration (or the next block) overwrites ring slot (k-1)&3
+    // and the halo strips, which the sources above read
+    __syncthreads();
   }
-  if (st) {
-    atomicOr(A.status, st);
-    // the reference restores the whole block to wCT on a small-value crash
-    if (st & ST_SMALL_VALUE) atomicOr(A.block_status + b, ST_SMALL_VALUE);
-  }
+  // the reference restores the whole block to wCT on a small-value crash
+  if (stb & ST_SMALL_VALUE) atomicOr(A.block_status + b, ST_SMALL_VALUE);
+  st |= stb;
+  }  // while (g < gend)
+  if (st) atomicOr(A.status, st);
 }
 
 }  // namespace amrvac

@@ -110,7 +110,8 @@ typedef struct amrvac_cfg {
   int ssprk_order;          /* 3 */
   double dtmin;             /* 1e-10 */
   int typeboundary[6][AMRVAC_MAX_NW]; /* [min1,max1,min2,max2,min3,max3][iw] */
-  int zchunk;               /* tuning: z-planes per CTA in 3-D (0 = auto) */
+  int zchunk;               /* work distribution: 0 = persistent plane ranges
+                               (default), 16/8/4 = z-planes per CTA in 3-D */
   int precision;            /* 0 = plain FP64; 1 = mixed: FP32 reconstruction, wave
                                speeds, fluxes, Riemann solver; FP64 conserved state,
                                pressure recovery, accumulation, sources, small values */
@@ -171,12 +172,13 @@ int amrvac_gpu_run_timed(amrvac_ctx *ctx, int nsteps, double *total_ms, double *
 /* Measured FP64 FMA throughput of the current device (TFLOP/s, 2 flops per
  * FMA) from an in-register FMA-chain kernel; the FP64 roofline denominator. */
 int amrvac_gpu_fp64_peak(double *tflops);
-/* Tile autotuner: times one stage (ps -> ps1, the state in ps is left
- * unchanged) for each candidate z-chunk of the 3-D stage kernel (16, 8, 4
- * planes per CTA), keeps the fastest for this context and returns it.
- * Call after the state has been uploaded.  2-D: returns 16, no timing. */
+/* Work-distribution autotuner: times one stage (ps -> ps1, the state in ps is
+ * left unchanged) for each candidate — 0: persistent CTAs (one wave), each
+ * marching a contiguous range of z-planes across blocks; 16, 8, 4: one
+ * z-chunk of that many planes per CTA (3-D only) — keeps the fastest for this
+ * context and returns it.  Call after the state has been uploaded. */
 int amrvac_gpu_autotune(amrvac_ctx *ctx, int reps, int *best_zchunk, double *best_ms);
-/* Set the z-chunk directly (16, 8 or 4), e.g. from a cached tuning result. */
+/* Set the work distribution directly (0, 16, 8 or 4), e.g. from a cache. */
 int amrvac_gpu_set_zchunk(amrvac_ctx *ctx, int zchunk);
 /* Read back the last step's dt, cmax_global and global_time (synchronises). */
 int amrvac_gpu_get_time(amrvac_ctx *ctx, double *dt, double *cmax_global, double *global_time);

@@ -332,3 +332,32 @@ def test_small_value_error_sets_status_and_restores(oracle_lib):
     ctx.clear_status()
     assert ctx.status() == 0
     del st
+
+
+@pytest.mark.parametrize("zchunk", [0, 16, 8, 4])
+def test_work_distributions(oracle_lib, zchunk):
+    """Persistent plane ranges (0) and fixed z-chunks give the same step.
+
+    48^3 = 27 blocks x 16 planes = 432 planes over one wave of CTAs: the
+    persistent ranges start and end inside blocks."""
+    _cuda()
+    O, ocfg, og, ctx = _setup(oracle_lib, "mhd3_hlld_cada3_glm", n=48)
+    ctx.set_zchunk(zchunk)
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.step()
+    dt, cg = og.getdt()
+    og.advance(dt, cg)
+    got = P.interior(ctx.download("ps"), 3)
+    ref = P.interior(np.array([og.get_block(ib) for ib in range(og.nblocks)]), 3)
+    assert _maxrel(got, ref) <= RTOL
+    assert ctx.status() == 0
+
+
+def test_autotune_leaves_state(oracle_lib):
+    _cuda()
+    O, ocfg, og, ctx = _setup(oracle_lib, "mhd3_hlld_cada3_glm", n=32)
+    before = ctx.download()
+    z, ms = ctx.autotune(reps=2, cache=False)
+    assert z in (0, 16, 8, 4) and ms > 0
+    assert np.array_equal(ctx.download(), before)
+    assert ctx.status() == 0
