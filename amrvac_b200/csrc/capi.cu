@@ -185,6 +185,11 @@ int launch_step(amrvac_ctx *c) {
 
 }  // namespace
 
+namespace amrvac {
+// Sets this thread's last-error text for entry points defined in other units.
+int record_error(int code, const std::string &msg) { return fail(code, msg); }
+}  // namespace amrvac
+
 extern "C" {
 
 const char *amrvac_gpu_last_error(void) { return g_err.c_str(); }

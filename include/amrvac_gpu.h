@@ -209,6 +209,26 @@ int amrvac_gpu_get_cbounds_points(amrvac_ctx *ctx, int n, const double *wlc, con
 int amrvac_gpu_riemann_points(amrvac_ctx *ctx, int n, const double *wlp, const double *wrp, int idim,
                               double cmax_global, double *f);
 
+/* CFL reduction without any device allocation (no counterpart in the
+ * reference).  For callers that must not call cudaMalloc/cudaFree: host codes
+ * whose device memory is owned by another runtime (OpenACC / CUDA Fortran
+ * data regions, a framework's caching allocator) and so cannot create an
+ * amrvac_ctx.  Computes what amrvac_gpu_getdt computes — dt from courantpar
+ * and cmax_global — over nblocks blocks that the caller holds on the current
+ * device in the register layout w_dev[block][var][z][y][x] (16^ndim cells,
+ * interior only), with dx the host array [nblocks][3].  Uses only
+ * cfg->physics, ndim, ndir, block_nx, gamma, typedivbfix, courantpar,
+ * type_courant and dtmin.  Runs on `stream` (a cudaStream_t; NULL = the
+ * default stream) and synchronises it.
+ * Scratch: a fixed device array inside the library (1.25 MiB per GPU, held
+ * until exit); nblocks above AMRVAC_NOALLOC_MAX_BLOCKS is refused with
+ * AMRVAC_E_ARG.  The first call on a device looks up that array's address, so
+ * make it before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race.  Returns AMRVAC_ST_DT_TOO_SMALL if dt < dtmin. */
+#define AMRVAC_NOALLOC_MAX_BLOCKS 32768
+int amrvac_gpu_getdt_noalloc(const amrvac_cfg *cfg, const double *w_dev, int nblocks, const double *dx,
+                             void *stream, double *dt, double *cmax_global);
+
 /* Same-resolution ghost-fill index maps ixS_srl_ / ixR_srl_ of init_bc
  * (src/mod_ghostcells_update.t:150-162), 0-based inclusive, for i=-1,0,1
  * at index i+1. */
