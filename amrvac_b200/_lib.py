@@ -53,6 +53,17 @@ class AmrvacCfg(ctypes.Structure):
     ]
 
 
+class AmrvacEnsInstance(ctypes.Structure):
+    """Mirror of ``amrvac_ens_instance``."""
+
+    _fields_ = [
+        ("ndim", ctypes.c_int), ("domain_nx", ctypes.c_int * 2),
+        ("xprobmin", ctypes.c_double * 2), ("xprobmax", ctypes.c_double * 2),
+        ("flux_scheme", ctypes.c_int), ("limiter", ctypes.c_int),
+        ("time_max", ctypes.c_double),
+    ]
+
+
 # (name, restype, argtypes) for every function declared in the header.
 _P = ctypes.POINTER
 _d, _i, _u32, _i64, _vp = ctypes.c_double, ctypes.c_int, ctypes.c_uint32, ctypes.c_int64, ctypes.c_void_p
@@ -91,6 +102,21 @@ SIGNATURES = [
     ("amrvac_gpu_get_cbounds_points", _i, [_vp, _i, _dp, _dp, _dp, _dp, _i, _dp, _dp]),
     ("amrvac_gpu_riemann_points", _i, [_vp, _i, _dp, _dp, _i, _d, _dp]),
     ("amrvac_gpu_srl_maps", _i, [_i, _i, _ip, _ip, _ip, _ip]),
+    ("amrvac_ens_create", _i, [_cfgp, _i, _P(AmrvacEnsInstance), _P(_vp)]),
+    ("amrvac_ens_destroy", _i, [_vp]),
+    ("amrvac_ens_nblocks", _i, [_vp, _i]),
+    ("amrvac_ens_upload", _i, [_vp, _i, _dp]),
+    ("amrvac_ens_download", _i, [_vp, _i, _dp]),
+    ("amrvac_ens_reset_time", _i, [_vp]),
+    ("amrvac_ens_step", _i, [_vp]),
+    ("amrvac_ens_run", _i, [_vp, _i, _i, _ip, _ip]),
+    ("amrvac_ens_state", _i, [_vp, _dp, _dp, _ip, _ip]),
+    ("amrvac_ens_status", _i, [_vp, _P(_u32), _P(_u32)]),
+    ("amrvac_ens_set_grid", _i, [_vp, _i]),
+    ("amrvac_ens_grid", _i, [_vp, _ip, _ip]),
+    ("amrvac_ens_autotune", _i, [_vp, _i, _ip, _dp]),
+    ("amrvac_ens_stream", _i, [_vp, _P(_vp)]),
+    ("amrvac_ens_launch_count", _i64, [_vp]),
 ]
 
 _lib = None

@@ -1,0 +1,971 @@
+// Batched ensembles: many independent hydrodynamics runs — 1-D and 2-D, of
+// uneven sizes, each with its own Riemann solver, limiter, time step and end
+// time — advanced together, one persistent kernel launch per RK stage for all
+// of them.  Each instance is one standalone run of the reference's time loop
+// (src/amrvac.t:241-343: setdt, exit check, advance) on a uniform level-1
+// grid of 16^d blocks; instances never exchange data.
+//
+// Device organisation.  Blocks of each dimensionality live in their own pool
+// (1-D: nw = 3, 2-D: nw = 4), interior cells only, [block][var][y][x], three
+// registers.  The unit of work is a tile of 16 rows x 16 cells: one 2-D block,
+// or sixteen 1-D blocks packed as rows (grouped by scheme so a tile's rows
+// usually share solver and limiter).  The tile list holds the 2-D tiles first,
+// then the 1-D tiles; persistent CTAs stride over it.  Instances that have
+// finished are dropped from the list by the host between graph chunks, and
+// skipped by a flag test in the meantime.
+//
+// Per-instance state on the device: dt, time, time_max, dx, solver, limiter,
+// done flag, step count and the getdt reduction word.  One step is
+//   getdt (per-instance max of the maxsum courant number) -> finalize (dt per
+//   instance, dtmin check, final_dt_reduction, exit test) -> RK stages ->
+//   advance time,
+// captured into a CUDA graph of several steps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/amrvac_gpu.h"
+#include "aux.cuh"
+#include "kernels.cuh"
+
+namespace amrvac {
+int record_error(int code, const std::string &msg);  // capi.cu
+
+constexpr int ENS_ROWS = 16;  // rows per tile
+
+struct EnsArgs {
+  StageArgs sa[2];           // per pool (index ndim-1): uin/ubase/uout, nbr, bc, status, P
+  const int *inst[2];        // instance of every block, per pool
+  const int *tiles;          // [tile][16] block ids (2-D tile: entry 0; 1-D tile: one per row, -1 empty)
+  const int *ntiles;         // device: [0] 2-D tiles, [1] all tiles
+  double a_base, b_in, dtfactor;
+  const double *dt;          // [ninst]
+  const double *dx;          // [ninst][2]
+  const int *solver;         // [ninst] SOLVER_*
+  const int *limiter;        // [ninst] LIM_*
+  const int *done;           // [ninst]
+  unsigned long long *red;   // [ninst] getdt accumulators
+};
+
+struct EnsRow {
+  int blk, inst, solver, limiter;
+  double sc[2];   // -qdt/dx per direction
+  double rd[2];   // cada3 1/(radius*dx)^2 per direction
+  double dxinv[2];
+};
+
+// Fill the per-row table of a tile (threads 0..15); returns, for all
+// threads, whether any row of the tile is active.
+template <int ND>
+__device__ __forceinline__ bool ens_rows(const EnsArgs &A, int tile, bool for_getdt, EnsRow *rows) {
+  const int t = threadIdx.x;
+  bool act = false;
+  if (t < ENS_ROWS) {
+    const int b = A.tiles[tile * ENS_ROWS + (ND == 2 ? 0 : t)];
+    int in = b >= 0 ? A.inst[ND - 1][b] : -1;
+    if (in >= 0 && A.done[in]) in = -1;
+    EnsRow &R = rows[t];
+    R.blk = b;
+    R.inst = in;
+    if (in >= 0) {
+      R.solver = A.solver[in];
+      R.limiter = A.limiter[in];
+      const double qdt = for_getdt ? 0.0 : A.dtfactor * A.dt[in];
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        const double dx = A.dx[in * 2 + d];
+        R.sc[d] = -qdt / dx;
+        const double r = A.sa[0].P.cada3_radius * dx;
+        R.rd[d] = 1.0 / (r * r);
+        R.dxinv[d] = 1.0 / dx;
+      }
+    }
+    act = in >= 0;
+  }
+  return __syncthreads_or(act) != 0;
+}
+
+template <class TF, int ND, int SOLVER>
+__device__ __forceinline__ uint32_t ens_face(TF *wLp, TF *wRp, const PhysParams &P, TF *F) {
+  return face_from_states<TF, false, ND, false, ND, SOLVER, 0>(wLp, wRp, P, TF(0), F);
+}
+
+// One RK stage on one tile.
+template <class TF, int ND>
+__device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, int tile, TF *smem, EnsRow *rows) {
+  using V = Vars<false, ND, false>;
+  constexpr int NW = V::NW;
+  constexpr int FB = (BN + 1) * BN;
+  constexpr bool FP64 = sizeof(TF) == 8;
+  const StageArgs &S = A.sa[ND - 1];
+  const PhysParams &P = S.P;
+  const int t = threadIdx.x;
+  const int ci = t & (BN - 1), cj = t >> 4;
+  uint32_t st = 0;
+  if (!ens_rows<ND>(A, tile, false, rows)) {
+    __syncthreads();
+    return 0;
+  }
+  TileView<TF, NW, 2> tv(smem);
+  const EnsRow &R = rows[ND == 2 ? 0 : cj];
+  const bool active = R.inst >= 0;
+  const int cjj = ND == 2 ? cj : 0;  // y index inside the block
+  // ---- stage the cells of the tile as primitives
+  if (active) {
+    double w[NW];
+    st |= load_prim<false, ND, false, ND>(S, R.blk, ci, cjj, 0, w);
+#pragma unroll
+    for (int v = 0; v < NW; ++v) tv.center(0, v, ci, cj) = TF(w[v]);
+  }
+  // ---- halo strips: x (both kinds of tile), y (2-D tiles)
+  if (t < (ND == 2 ? 128 : 64)) {
+    const int h = t;
+    int i, j, row, stride;
+    TF *dst;
+    if (h < 64) {
+      j = h >> 2;
+      const int c = h & 3;
+      i = c < 2 ? c - 2 : c + BN - 2;
+      dst = tv.hx + j * 4 + c;
+      stride = BN * 4;
+      row = ND == 2 ? 0 : j;
+    } else {
+      const int r = (h - 64) >> 4;
+      i = (h - 64) & (BN - 1);
+      j = r < 2 ? r - 2 : r + BN - 2;
+      dst = tv.hy + r * BN + i;
+      stride = 4 * BN;
+      row = 0;
+    }
+    const EnsRow &H = rows[row];
+    if (H.inst >= 0) {
+      double w[NW];
+      st |= load_prim<false, ND, false, ND>(S, H.blk, i, ND == 2 ? j : 0, 0, w);
+#pragma unroll
+      for (int v = 0; v < NW; ++v) dst[v * stride] = TF(w[v]);
+    }
+  }
+  // ---- RK combination wnew0 = a*base + b*in (src/mod_advance.t:254-266)
+  double acc[NW];
+  if (active) {
+#pragma unroll
+    for (int v = 0; v < NW; ++v) {
+      const size_t o = cell_offset<ND>(R.blk, NW, v, ci, cjj, 0);
+      const double win = S.uin[o];
+      acc[v] = (A.a_base == 0.0) ? win : A.a_base * S.ubase[o] + A.b_in * win;
+    }
+  }
+  __syncthreads();
+  // ---- face phases
+#pragma unroll 1
+  for (int D = 0; D < ND; ++D) {
+#pragma unroll 1
+    for (int f = t; f < FB; f += STAGE_THREADS) {
+      int fi, fj;
+      if (D == 0) { fj = f / (BN + 1); fi = f - fj * (BN + 1); }
+      else { fj = f >> 4; fi = f & (BN - 1); }
+      const EnsRow &Rf = rows[ND == 2 ? 0 : fj];
+      if (Rf.inst < 0) continue;
+      const TF rd = TF(Rf.rd[D]);
+      const int lim = Rf.limiter;
+      TF wLp[NW], wRp[NW];
+      int base[4], strd[4];
+#pragma unroll
+      for (int o = 0; o < 4; ++o)
+        tv.addr(0, D == 0 ? fi + o - 2 : fi, D == 0 ? fj : fj + o - 2, base[o], strd[o]);
+#pragma unroll
+      for (int v = 0; v < NW; ++v) {
+        const int ov = orig_index_rt<false, ND>(v, D);
+        TF q[4];
+#pragma unroll
+        for (int o = 0; o < 4; ++o) q[o] = smem[base[o] + ov * strd[o]];
+        const TF d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
+        wLp[v] = q[1] + TF(0.5) * limited_slope<TF, true, 0>(lim, d1, d0, rd);
+        wRp[v] = q[2] - TF(0.5) * limited_slope<TF, false, 0>(lim, d2, d1, rd);
+      }
+      TF Fr[NW];
+      if (Rf.solver == SOLVER_HLLC) st |= ens_face<TF, ND, SOLVER_HLLC>(wLp, wRp, P, Fr);
+      else if (Rf.solver == SOLVER_HLL) st |= ens_face<TF, ND, SOLVER_HLL>(wLp, wRp, P, Fr);
+      else st |= ens_face<TF, ND, SOLVER_TVDLF>(wLp, wRp, P, Fr);
+      const double sc = Rf.sc[D];
+#pragma unroll
+      for (int v = 0; v < NW; ++v) {
+        const int ov = orig_index_rt<false, ND>(v, D);
+        if constexpr (FP64) tv.fb[ov * FB + f] = sc * Fr[v];
+        else tv.fb[ov * FB + f] = Fr[v];
+      }
+    }
+    __syncthreads();
+    if (active) {
+      const double sc = FP64 ? 1.0 : R.sc[D];
+      const int f = D == 0 ? cj * (BN + 1) + ci : cj * BN + ci;
+      const int step = D == 0 ? 1 : BN;
+#pragma unroll
+      for (int v = 0; v < NW; ++v) {
+        if constexpr (FP64) acc[v] = acc[v] + tv.fb[v * FB + f + step] - tv.fb[v * FB + f];
+        else acc[v] = acc[v] + sc * double(tv.fb[v * FB + f + step]) - sc * double(tv.fb[v * FB + f]);
+      }
+    }
+    __syncthreads();
+  }
+  if (active) {
+    if (P.fix_small_values) {
+      if (small_values<double, false, ND, false>(acc, false, P) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
+    }
+    if (!isfinite(acc[V::RHO]) || !isfinite(acc[V::E])) st |= ST_NAN;
+#pragma unroll
+    for (int v = 0; v < NW; ++v) S.uout[cell_offset<ND>(R.blk, NW, v, ci, cjj, 0)] = acc[v];
+  }
+  return st;
+}
+
+template <class TF>
+__global__ void __launch_bounds__(STAGE_THREADS, 2) ens_stage_kernel(const EnsArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TF *smem = reinterpret_cast<TF *>(smem_raw);
+  __shared__ EnsRow rows[ENS_ROWS];
+  const int n2 = A.ntiles[0], nt = A.ntiles[1];
+  uint32_t st = 0;
+#pragma unroll 1
+  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+    if (tile < n2) st |= ens_stage_tile<TF, 2>(A, tile, smem, rows);
+    else st |= ens_stage_tile<TF, 1>(A, tile, smem, rows);
+    __syncthreads();  // the next tile rewrites rows[] and the shared tile
+  }
+  if (st) atomicOr(A.sa[0].status, st);
+}
+
+// getdt_courant (src/mod_dt.t:160-287), maxsum, per instance: the max over
+// the instance's cells of sum_d (|v_d| + c_s) / dx_d.
+template <int ND>
+__device__ __forceinline__ void ens_getdt_tile(const EnsArgs &A, int tile, EnsRow *rows, double *wred) {
+  using V = Vars<false, ND, false>;
+  constexpr int NW = V::NW;
+  const StageArgs &S = A.sa[ND - 1];
+  const int t = threadIdx.x;
+  const int ci = t & (BN - 1), cj = t >> 4;
+  if (!ens_rows<ND>(A, tile, true, rows)) {
+    __syncthreads();
+    return;
+  }
+  const EnsRow &R = rows[ND == 2 ? 0 : cj];
+  double x = 0.0;
+  if (R.inst >= 0) {
+    double w[NW];
+#pragma unroll
+    for (int v = 0; v < NW; ++v) w[v] = __ldg(S.uin + cell_offset<ND>(R.blk, NW, v, ci, ND == 2 ? cj : 0, 0));
+    to_primitive<false, ND, false>(w, S.P);
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const double cm = fabs(w[V::M0 + d]) + sqrt(S.P.gamma * w[V::E] / w[V::RHO]);
+      const double c = cm * R.dxinv[d];
+      x = d == 0 ? c : x + c;
+    }
+  }
+  // rows are half-warps: reduce over the 16 lanes of a row
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+  if constexpr (ND == 1) {
+    if (ci == 0 && R.inst >= 0) atomic_max_pos(A.red + R.inst, x);
+  } else {
+    if (ci == 0) wred[cj] = x;
+    __syncthreads();
+    if (t == 0 && R.inst >= 0) {
+      double m = 0.0;
+      for (int q = 0; q < ENS_ROWS; ++q) m = fmax(m, wred[q]);
+      atomic_max_pos(A.red + R.inst, m);
+    }
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(STAGE_THREADS) ens_getdt_kernel(const EnsArgs A) {
+  __shared__ EnsRow rows[ENS_ROWS];
+  __shared__ double wred[ENS_ROWS];
+  const int n2 = A.ntiles[0], nt = A.ntiles[1];
+#pragma unroll 1
+  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
+    if (tile < n2) ens_getdt_tile<2>(A, tile, rows, wred);
+    else ens_getdt_tile<1>(A, tile, rows, wred);
+  }
+}
+
+struct EnsTime {
+  int ninst;
+  unsigned long long *red;
+  double *dt, *time;
+  const double *time_max;
+  int *done, *steps;
+  uint32_t *inst_status, *status;
+  double courantpar, dtmin;
+};
+
+// setdt per instance (src/mod_dt.t:30-79) and the exit test of the time loop
+// (src/amrvac.t:306: global_time >= time_max or final_dt_exit).
+__global__ void ens_finalize_kernel(const EnsTime T) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T.ninst) return;
+  const double x = __longlong_as_double((long long)T.red[i]);
+  T.red[i] = 0ull;
+  if (T.done[i]) { T.dt[i] = 0.0; return; }
+  double d = 1.0e99;
+  if (x > 1.0e-12) d = fmin(d, T.courantpar / x);
+  const double t = T.time[i], tmax = T.time_max[i];
+  if (d < T.dtmin) {  // crash: this instance stops
+    T.inst_status[i] |= ST_DT_TOO_SMALL;
+    atomicOr(T.status, ST_DT_TOO_SMALL);
+    T.done[i] = 1;
+    T.dt[i] = 0.0;
+    return;
+  }
+  if (tmax - t <= T.dtmin || t >= tmax) {
+    T.done[i] = 1;
+    T.dt[i] = 0.0;
+    return;
+  }
+  T.dt[i] = fmin(d, tmax - t);
+}
+
+__global__ void ens_advance_kernel(const EnsTime T) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T.ninst || T.done[i]) return;
+  T.time[i] = T.time[i] + T.dt[i];
+  T.steps[i] += 1;
+}
+
+}  // namespace amrvac
+
+using namespace amrvac;
+
+struct amrvac_ens {
+  amrvac_cfg cfg;
+  PhysParams P;
+  BcSpec bc;
+  SrlMaps maps;
+  bool mixed = false;
+  int ninst = 0;
+  std::vector<amrvac_ens_instance> inst;
+  std::vector<int> pool_of, first, nblk;     // per instance: pool (0: 1-D, 1: 2-D), first block, blocks
+  std::vector<int> h_tiles2, h_tiles1;       // 2-D tiles (one block each), 1-D tiles (16 rows)
+  std::vector<std::vector<int>> tiles1_of;   // 1-D tile indices per instance (for compaction)
+  int nb[2] = {0, 0};
+  double *pool[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  int *d_nbr[2] = {nullptr, nullptr};
+  int *d_inst[2] = {nullptr, nullptr};
+  int *d_tiles = nullptr, *d_ntiles = nullptr;
+  int ntiles_active[2] = {0, 0};
+  double *d_dt = nullptr, *d_time = nullptr, *d_tmax = nullptr, *d_dx = nullptr;
+  int *d_solver = nullptr, *d_limiter = nullptr, *d_done = nullptr, *d_steps = nullptr;
+  unsigned long long *d_red = nullptr;
+  uint32_t *d_status = nullptr, *d_inst_status = nullptr;
+  double *d_stage = nullptr;
+  size_t stage_doubles = 0;
+  int *h_pin = nullptr;                      // pinned: ntiles + tile list for compaction uploads
+  size_t h_pin_ints = 0;
+  std::vector<int> h_done;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  int grid = 0;          // CTAs per stage / getdt launch
+  int wave = 1;          // resident stage CTAs
+  int64_t launches = 0;
+};
+
+namespace {
+
+int efail(int code, const std::string &m) { return record_error(code, "ens: " + m); }
+int ecuda(cudaError_t e, const char *where) {
+  return record_error(AMRVAC_E_CUDA, std::string("ens: ") + where + ": " + cudaGetErrorString(e));
+}
+#define ECK(call)                                   \
+  do {                                              \
+    cudaError_t e_ = (call);                        \
+    if (e_ != cudaSuccess) return ecuda(e_, #call); \
+  } while (0)
+
+size_t ens_smem(bool mixed) {
+  return mixed ? Tile<float, 4, 2>::BYTES : Tile<double, 4, 2>::BYTES;
+}
+
+EnsArgs ens_args(amrvac_ens *e, int reg_ct, int reg_new, int reg_base, double a, double b, double dtfactor) {
+  EnsArgs A;
+  std::memset(&A, 0, sizeof(A));
+  for (int p = 0; p < 2; ++p) {
+    StageArgs &S = A.sa[p];
+    S.uin = e->pool[p][reg_ct];
+    S.ubase = e->pool[p][reg_base];
+    S.uout = e->pool[p][reg_new];
+    S.nbr = e->d_nbr[p];
+    S.nblocks = e->nb[p];
+    for (int s = 0; s < 6; ++s) { S.bc_kind[s] = e->bc.kind[s]; S.bc_flip[s] = 0; }
+    S.status = e->d_status;
+    S.P = e->P;
+    A.inst[p] = e->d_inst[p];
+  }
+  A.tiles = e->d_tiles;
+  A.ntiles = e->d_ntiles;
+  A.a_base = a;
+  A.b_in = b;
+  A.dtfactor = dtfactor;
+  A.dt = e->d_dt;
+  A.dx = e->d_dx;
+  A.solver = e->d_solver;
+  A.limiter = e->d_limiter;
+  A.done = e->d_done;
+  A.red = e->d_red;
+  return A;
+}
+
+EnsTime ens_time(amrvac_ens *e) {
+  EnsTime T;
+  T.ninst = e->ninst;
+  T.red = e->d_red;
+  T.dt = e->d_dt;
+  T.time = e->d_time;
+  T.time_max = e->d_tmax;
+  T.done = e->d_done;
+  T.steps = e->d_steps;
+  T.inst_status = e->d_inst_status;
+  T.status = e->d_status;
+  T.courantpar = e->cfg.courantpar;
+  T.dtmin = e->cfg.dtmin;
+  return T;
+}
+
+int ens_launch_stage(amrvac_ens *e, int reg_ct, int reg_new, int reg_base, double a, double b, double dtf) {
+  const EnsArgs A = ens_args(e, reg_ct, reg_new, reg_base, a, b, dtf);
+  if (e->mixed) ens_stage_kernel<float><<<e->grid, STAGE_THREADS, ens_smem(true), e->stream>>>(A);
+  else ens_stage_kernel<double><<<e->grid, STAGE_THREADS, ens_smem(false), e->stream>>>(A);
+  ECK(cudaGetLastError());
+  ++e->launches;
+  return 0;
+}
+
+int ens_launch_step(amrvac_ens *e) {
+  const EnsArgs G = ens_args(e, 0, 0, 0, 0.0, 1.0, 1.0);
+  ens_getdt_kernel<<<e->grid, STAGE_THREADS, 0, e->stream>>>(G);
+  ECK(cudaGetLastError());
+  const EnsTime T = ens_time(e);
+  const int nb = (e->ninst + 127) / 128;
+  ens_finalize_kernel<<<nb, 128, 0, e->stream>>>(T);
+  ECK(cudaGetLastError());
+  e->launches += 2;
+  const amrvac_cfg &k = e->cfg;
+  int r = 0;
+  if (k.time_stepper == AMRVAC_TS_ONESTEP) {
+    for (int p = 0; p < 2; ++p)
+      if (e->nb[p])
+        ECK(cudaMemcpyAsync(e->pool[p][1], e->pool[p][0], sizeof(double) * (size_t)e->nb[p] * (p ? 4 * 256 : 3 * 16),
+                            cudaMemcpyDeviceToDevice, e->stream));
+    r = ens_launch_stage(e, 1, 0, 0, 0.0, 1.0, 1.0);
+  } else if (k.time_stepper == AMRVAC_TS_TWOSTEP) {
+    if ((r = ens_launch_stage(e, 0, 1, 0, 0.0, 1.0, 1.0))) return r;
+    r = ens_launch_stage(e, 1, 0, 0, 0.5, 0.5, 0.5);
+  } else {
+    double b11, b22, b33, a21, a31;
+    if (k.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
+    else { b11 = 1.0; b22 = 1.0 / 4.0; b33 = 2.0 / 3.0; a21 = 3.0 / 4.0; a31 = 1.0 / 3.0; }
+    if ((r = ens_launch_stage(e, 0, 1, 0, 0.0, 1.0, b11))) return r;
+    if ((r = ens_launch_stage(e, 1, 2, 0, a21, 1.0 - a21, b22))) return r;
+    r = ens_launch_stage(e, 2, 0, 0, a31, 1.0 - a31, b33);
+  }
+  if (r) return r;
+  ens_advance_kernel<<<nb, 128, 0, e->stream>>>(T);
+  ECK(cudaGetLastError());
+  ++e->launches;
+  return 0;
+}
+
+// Upload the tile list of the instances not yet done (done == nullptr: all).
+int ens_upload_tiles(amrvac_ens *e, const std::vector<int> *done) {
+  std::vector<int> t2, t1;
+  t2.reserve(e->h_tiles2.size());
+  for (int i = 0; i < e->ninst; ++i) {
+    if (done && (*done)[i]) continue;
+    if (e->pool_of[i] == 1)
+      for (int b = 0; b < e->nblk[i]; ++b) t2.push_back(e->first[i] + b);
+  }
+  std::vector<char> keep(e->h_tiles1.size() / ENS_ROWS, 0);
+  for (int i = 0; i < e->ninst; ++i)
+    if (e->pool_of[i] == 0 && !(done && (*done)[i]))
+      for (int q : e->tiles1_of[i]) keep[q] = 1;
+  const size_t n2 = t2.size();
+  size_t n1 = 0;
+  for (char c : keep) n1 += c;
+  const size_t total = n2 + n1;
+  if (total + 1 > e->h_pin_ints / ENS_ROWS) return efail(AMRVAC_E_STATE, "tile staging too small");
+  // pinned staging: [0..15] ntiles, then the tiles; the previous upload from it has completed
+  // (the caller synchronised the stream)
+  int *h = e->h_pin;
+  h[0] = (int)n2;
+  h[1] = (int)total;
+  int *dst = h + ENS_ROWS;
+  for (size_t q = 0; q < n2; ++q) {
+    dst[q * ENS_ROWS] = t2[q];
+    for (int r = 1; r < ENS_ROWS; ++r) dst[q * ENS_ROWS + r] = -1;
+  }
+  size_t w = n2;
+  for (size_t q = 0; q < keep.size(); ++q) {
+    if (!keep[q]) continue;
+    std::memcpy(dst + w * ENS_ROWS, e->h_tiles1.data() + q * ENS_ROWS, sizeof(int) * ENS_ROWS);
+    ++w;
+  }
+  ECK(cudaMemcpyAsync(e->d_ntiles, h, sizeof(int) * 2, cudaMemcpyHostToDevice, e->stream));
+  if (total)
+    ECK(cudaMemcpyAsync(e->d_tiles, dst, sizeof(int) * total * ENS_ROWS, cudaMemcpyHostToDevice, e->stream));
+  ECK(cudaStreamSynchronize(e->stream));
+  e->ntiles_active[0] = (int)n2;
+  e->ntiles_active[1] = (int)total;
+  return 0;
+}
+
+int ens_ensure_stage(amrvac_ens *e, size_t doubles) {
+  if (e->stage_doubles >= doubles) return 0;
+  cudaStreamSynchronize(e->stream);
+  cudaFree(e->d_stage);
+  e->d_stage = nullptr;
+  e->stage_doubles = 0;
+  ECK(cudaMalloc(&e->d_stage, sizeof(double) * doubles));
+  e->stage_doubles = doubles;
+  return 0;
+}
+
+void free_all(amrvac_ens *e) {
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  for (int p = 0; p < 2; ++p) {
+    for (int r = 0; r < 3; ++r) cudaFree(e->pool[p][r]);
+    cudaFree(e->d_nbr[p]);
+    cudaFree(e->d_inst[p]);
+  }
+  cudaFree(e->d_tiles); cudaFree(e->d_ntiles);
+  cudaFree(e->d_dt); cudaFree(e->d_time); cudaFree(e->d_tmax); cudaFree(e->d_dx);
+  cudaFree(e->d_solver); cudaFree(e->d_limiter); cudaFree(e->d_done); cudaFree(e->d_steps);
+  cudaFree(e->d_red); cudaFree(e->d_status); cudaFree(e->d_inst_status); cudaFree(e->d_stage);
+  if (e->h_pin) cudaFreeHost(e->h_pin);
+  if (e->stream) cudaStreamDestroy(e->stream);
+}
+
+int check_ens(amrvac_ens *e) { return e ? 0 : efail(AMRVAC_E_ARG, "null ensemble"); }
+
+int check_inst(amrvac_ens *e, int i) {
+  if (int r = check_ens(e)) return r;
+  if (i < 0 || i >= e->ninst) return efail(AMRVAC_E_ARG, "instance out of range");
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int amrvac_ens_create(const amrvac_cfg *cfg, int ninst, const amrvac_ens_instance *in, amrvac_ens **out) {
+  if (!cfg || !in || !out) return efail(AMRVAC_E_ARG, "null argument");
+  *out = nullptr;
+  if (ninst <= 0) return efail(AMRVAC_E_ARG, "ninst must be positive");
+  const amrvac_cfg &k = *cfg;
+  if (k.physics != 0) return efail(AMRVAC_E_UNSUPPORTED, "ensembles are hydrodynamics (physics 0) only");
+  if (k.nghostcells < 2) return efail(AMRVAC_E_UNSUPPORTED, "nghostcells must be >= 2");
+  if (k.type_courant != AMRVAC_COURANT_MAXSUM) return efail(AMRVAC_E_UNSUPPORTED, "ensembles use typecourant maxsum");
+  if (k.typeboundspeed < 1 || k.typeboundspeed > 3) return efail(AMRVAC_E_ARG, "bad typeboundspeed");
+  if (k.time_stepper < 1 || k.time_stepper > 3) return efail(AMRVAC_E_UNSUPPORTED, "time_stepper not supported");
+  if (k.precision != 0 && k.precision != 1) return efail(AMRVAC_E_ARG, "precision must be 0 or 1");
+  for (int s = 0; s < 4; ++s)
+    for (int v = 0; v < 4; ++v) {
+      const int b = k.typeboundary[s][v];
+      if (b != k.typeboundary[s][0] || (b != AMRVAC_BC_PERIODIC && b != AMRVAC_BC_CONT))
+        return efail(AMRVAC_E_UNSUPPORTED, "ensemble boundaries: periodic or cont, the same for all variables");
+    }
+  for (int i = 0; i < ninst; ++i) {
+    const amrvac_ens_instance &q = in[i];
+    if (q.ndim != 1 && q.ndim != 2) return efail(AMRVAC_E_UNSUPPORTED, "instance ndim must be 1 or 2");
+    for (int d = 0; d < q.ndim; ++d) {
+      if (q.domain_nx[d] <= 0 || q.domain_nx[d] % 16) return efail(AMRVAC_E_ARG, "domain_nx must be a positive multiple of 16");
+      if (!(q.xprobmax[d] > q.xprobmin[d])) return efail(AMRVAC_E_ARG, "xprobmax must exceed xprobmin");
+    }
+    if (q.flux_scheme != AMRVAC_FS_TVDLF && q.flux_scheme != AMRVAC_FS_HLL && q.flux_scheme != AMRVAC_FS_HLLC)
+      return efail(AMRVAC_E_UNSUPPORTED, "instance flux_scheme must be tvdlf, hll or hllc");
+    if (q.limiter < 1 || q.limiter > 9) return efail(AMRVAC_E_UNSUPPORTED, "limiter not supported");
+  }
+  amrvac_ens *e = new amrvac_ens();
+  e->cfg = k;
+  e->mixed = k.precision == 1;
+  e->ninst = ninst;
+  e->inst.assign(in, in + ninst);
+  PhysParams &P = e->P;
+  std::memset(&P, 0, sizeof(P));
+  P.gamma = k.gamma;
+  P.gamma_1 = k.gamma - 1.0;
+  P.inv_gamma_1 = 1.0 / (k.gamma - 1.0);
+  P.small_density = k.small_density;
+  P.small_pressure = k.small_pressure;
+  P.small_e = k.small_pressure / (k.gamma - 1.0);
+  P.tvdlfeps = k.tvdlfeps;
+  P.cada3_radius = k.cada3_radius;
+  P.courantpar = k.courantpar;
+  P.limiter = 0;
+  P.boundspeed = k.typeboundspeed;
+  P.fix_small_values = k.fix_small_values;
+  P.check_small_values = k.check_small_values;
+  P.small_values_method = k.small_values_method;
+  for (int s = 0; s < 6; ++s) {
+    e->bc.kind[s] = s < 4 && k.typeboundary[s][0] == AMRVAC_BC_CONT ? BCK_CONT : BCK_PERIODIC;
+    e->bc.flip[s] = 0;
+  }
+  for (int d = 0; d < 3; ++d) {
+    if (d < 2) amrvac_gpu_srl_maps(k.nghostcells, 16, e->maps.smin[d], e->maps.smax[d], e->maps.rmin[d], e->maps.rmax[d]);
+    else for (int q = 0; q < 3; ++q) e->maps.smin[d][q] = e->maps.smax[d][q] = e->maps.rmin[d][q] = e->maps.rmax[d][q] = 0;
+  }
+  // ---- blocks and neighbour tables
+  std::vector<int> nbr[2], binst[2];
+  std::vector<double> dxv(2 * (size_t)ninst, 1.0);
+  e->pool_of.resize(ninst);
+  e->first.resize(ninst);
+  e->nblk.resize(ninst);
+  for (int i = 0; i < ninst; ++i) {
+    const amrvac_ens_instance &q = in[i];
+    const int p = q.ndim - 1;
+    const int nbx = q.domain_nx[0] / 16, nby = q.ndim == 2 ? q.domain_nx[1] / 16 : 1;
+    e->pool_of[i] = p;
+    e->first[i] = e->nb[p];
+    e->nblk[i] = nbx * nby;
+    for (int d = 0; d < q.ndim; ++d) dxv[2 * i + d] = (q.xprobmax[d] - q.xprobmin[d]) / q.domain_nx[d];
+    for (int jb = 0; jb < nby; ++jb)
+      for (int ib = 0; ib < nbx; ++ib) {
+        for (int dk = -1; dk <= 1; ++dk)
+          for (int dj = -1; dj <= 1; ++dj)
+            for (int di = -1; di <= 1; ++di) {
+              int v = -1;
+              if (dk == 0 && (q.ndim == 2 || dj == 0)) {
+                int x = ib + di, y = jb + dj;
+                bool ok = true;
+                if (x < 0 || x >= nbx) {
+                  if (e->bc.kind[x < 0 ? 0 : 1] == BCK_PERIODIC) x = (x + nbx) % nbx;
+                  else ok = false;
+                }
+                if (y < 0 || y >= nby) {
+                  if (q.ndim == 2 && e->bc.kind[y < 0 ? 2 : 3] == BCK_PERIODIC) y = (y + nby) % nby;
+                  else ok = false;
+                }
+                if (ok) v = e->first[i] + x + nbx * y;
+              }
+              nbr[p].push_back(v);
+            }
+        binst[p].push_back(i);
+      }
+    e->nb[p] += e->nblk[i];
+  }
+  // ---- tiles: 2-D blocks one per tile; 1-D blocks packed 16 per tile, grouped by scheme
+  for (int i = 0; i < ninst; ++i)
+    if (e->pool_of[i] == 1)
+      for (int b = 0; b < e->nblk[i]; ++b) e->h_tiles2.push_back(e->first[i] + b);
+  std::vector<int> order;
+  for (int i = 0; i < ninst; ++i)
+    if (e->pool_of[i] == 0) order.push_back(i);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const int ka = in[a].flux_scheme * 16 + in[a].limiter, kb = in[b].flux_scheme * 16 + in[b].limiter;
+    return ka < kb;
+  });
+  e->tiles1_of.assign(ninst, {});
+  int row = 0;
+  for (int i : order)
+    for (int b = 0; b < e->nblk[i]; ++b) {
+      if (row == 0) e->h_tiles1.insert(e->h_tiles1.end(), ENS_ROWS, -1);
+      const int tq = (int)(e->h_tiles1.size() / ENS_ROWS) - 1;
+      e->h_tiles1[(size_t)tq * ENS_ROWS + row] = e->first[i] + b;
+      if (e->tiles1_of[i].empty() || e->tiles1_of[i].back() != tq) e->tiles1_of[i].push_back(tq);
+      row = (row + 1) % ENS_ROWS;
+    }
+  const size_t ntiles = e->h_tiles2.size() + e->h_tiles1.size() / ENS_ROWS;
+  // ---- device memory
+  cudaError_t ce;
+#define EALLOC(ptr, bytes)                                           \
+  if ((ce = cudaMalloc(&(ptr), (bytes))) != cudaSuccess) {           \
+    free_all(e);                                                     \
+    delete e;                                                        \
+    return ecuda(ce, "cudaMalloc");                                  \
+  }
+  if ((ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    delete e;
+    return ecuda(ce, "cudaStreamCreate");
+  }
+  for (int p = 0; p < 2; ++p) {
+    if (!e->nb[p]) continue;
+    const size_t per = p ? 4 * 256 : 3 * 16;
+    for (int r = 0; r < 3; ++r) EALLOC(e->pool[p][r], sizeof(double) * per * e->nb[p]);
+    EALLOC(e->d_nbr[p], sizeof(int) * nbr[p].size());
+    EALLOC(e->d_inst[p], sizeof(int) * binst[p].size());
+  }
+  EALLOC(e->d_tiles, sizeof(int) * ENS_ROWS * std::max<size_t>(ntiles, 1));
+  EALLOC(e->d_ntiles, sizeof(int) * 2);
+  EALLOC(e->d_dt, sizeof(double) * ninst);
+  EALLOC(e->d_time, sizeof(double) * ninst);
+  EALLOC(e->d_tmax, sizeof(double) * ninst);
+  EALLOC(e->d_dx, sizeof(double) * 2 * ninst);
+  EALLOC(e->d_solver, sizeof(int) * ninst);
+  EALLOC(e->d_limiter, sizeof(int) * ninst);
+  EALLOC(e->d_done, sizeof(int) * ninst);
+  EALLOC(e->d_steps, sizeof(int) * ninst);
+  EALLOC(e->d_red, sizeof(unsigned long long) * ninst);
+  EALLOC(e->d_status, sizeof(uint32_t));
+  EALLOC(e->d_inst_status, sizeof(uint32_t) * ninst);
+#undef EALLOC
+  e->h_pin_ints = (ntiles + 1) * ENS_ROWS;
+  if ((ce = cudaMallocHost(&e->h_pin, sizeof(int) * e->h_pin_ints)) != cudaSuccess) {
+    free_all(e);
+    delete e;
+    return ecuda(ce, "cudaMallocHost");
+  }
+  std::vector<double> tmax(ninst);
+  std::vector<int> solver(ninst), lim(ninst);
+  for (int i = 0; i < ninst; ++i) {
+    tmax[i] = in[i].time_max;
+    solver[i] = in[i].flux_scheme;  // AMRVAC_FS_* equal SOLVER_*
+    lim[i] = in[i].limiter;
+  }
+  auto fail_free = [&](cudaError_t c2, const char *w) {
+    free_all(e);
+    delete e;
+    return ecuda(c2, w);
+  };
+  for (int p = 0; p < 2; ++p) {
+    if (!e->nb[p]) continue;
+    if ((ce = cudaMemcpy(e->d_nbr[p], nbr[p].data(), sizeof(int) * nbr[p].size(), cudaMemcpyHostToDevice)) ||
+        (ce = cudaMemcpy(e->d_inst[p], binst[p].data(), sizeof(int) * binst[p].size(), cudaMemcpyHostToDevice)))
+      return fail_free(ce, "cudaMemcpy(tables)");
+  }
+  if ((ce = cudaMemcpy(e->d_tmax, tmax.data(), sizeof(double) * ninst, cudaMemcpyHostToDevice)) ||
+      (ce = cudaMemcpy(e->d_dx, dxv.data(), sizeof(double) * 2 * ninst, cudaMemcpyHostToDevice)) ||
+      (ce = cudaMemcpy(e->d_solver, solver.data(), sizeof(int) * ninst, cudaMemcpyHostToDevice)) ||
+      (ce = cudaMemcpy(e->d_limiter, lim.data(), sizeof(int) * ninst, cudaMemcpyHostToDevice)) ||
+      (ce = cudaMemset(e->d_red, 0, sizeof(unsigned long long) * ninst)) ||
+      (ce = cudaMemset(e->d_status, 0, sizeof(uint32_t))))
+    return fail_free(ce, "cudaMemcpy(instances)");
+  for (int p = 0; p < 2; ++p)
+    for (int r = 0; r < 3; ++r)
+      if (e->pool[p][r] && (ce = cudaMemset(e->pool[p][r], 0, sizeof(double) * (p ? 4 * 256 : 3 * 16) * e->nb[p])))
+        return fail_free(ce, "cudaMemset(pool)");
+  if (e->mixed) ce = cudaFuncSetAttribute(ens_stage_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ens_smem(true));
+  else ce = cudaFuncSetAttribute(ens_stage_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ens_smem(false));
+  if (ce) return fail_free(ce, "cudaFuncSetAttribute");
+  int per_sm = 1, dev = 0, nsm = 148;
+  if (e->mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_stage_kernel<float>, STAGE_THREADS, ens_smem(true));
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_stage_kernel<double>, STAGE_THREADS, ens_smem(false));
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  e->wave = std::max(1, per_sm) * nsm;
+  e->grid = e->wave;
+  *out = e;
+  if (int r = amrvac_ens_reset_time(e)) {
+    *out = nullptr;
+    free_all(e);
+    delete e;
+    return r;
+  }
+  return 0;
+}
+
+int amrvac_ens_destroy(amrvac_ens *e) {
+  if (!e) return 0;
+  cudaStreamSynchronize(e->stream);
+  free_all(e);
+  delete e;
+  return 0;
+}
+
+int amrvac_ens_nblocks(const amrvac_ens *e, int inst) {
+  if (!e || inst < 0 || inst >= e->ninst) return AMRVAC_E_ARG;
+  return e->nblk[inst];
+}
+
+int amrvac_ens_reset_time(amrvac_ens *e) {
+  if (int r = check_ens(e)) return r;
+  ECK(cudaMemsetAsync(e->d_time, 0, sizeof(double) * e->ninst, e->stream));
+  ECK(cudaMemsetAsync(e->d_dt, 0, sizeof(double) * e->ninst, e->stream));
+  ECK(cudaMemsetAsync(e->d_done, 0, sizeof(int) * e->ninst, e->stream));
+  ECK(cudaMemsetAsync(e->d_steps, 0, sizeof(int) * e->ninst, e->stream));
+  ECK(cudaMemsetAsync(e->d_inst_status, 0, sizeof(uint32_t) * e->ninst, e->stream));
+  ECK(cudaMemsetAsync(e->d_red, 0, sizeof(unsigned long long) * e->ninst, e->stream));
+  ECK(cudaStreamSynchronize(e->stream));
+  return ens_upload_tiles(e, nullptr);
+}
+
+int amrvac_ens_upload(amrvac_ens *e, int inst, const double *w) {
+  if (int r = check_inst(e, inst)) return r;
+  if (!w) return efail(AMRVAC_E_ARG, "null array");
+  const int p = e->pool_of[inst], nw = p ? 4 : 3, ndim = p + 1;
+  const size_t g = (size_t)(16 + 2 * e->cfg.nghostcells) * (p ? 16 + 2 * e->cfg.nghostcells : 1);
+  const size_t doubles = g * nw * e->nblk[inst];
+  if (int r = ens_ensure_stage(e, doubles)) return r;
+  ECK(cudaMemcpyAsync(e->d_stage, w, sizeof(double) * doubles, cudaMemcpyHostToDevice, e->stream));
+  ECK(launch_unpack(e->d_stage, e->pool[p][0], e->first[inst], e->nblk[inst], nw, ndim, e->cfg.nghostcells,
+                    e->stream));
+  ++e->launches;
+  ECK(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+int amrvac_ens_download(amrvac_ens *e, int inst, double *w) {
+  if (int r = check_inst(e, inst)) return r;
+  if (!w) return efail(AMRVAC_E_ARG, "null array");
+  const int p = e->pool_of[inst], nw = p ? 4 : 3, ndim = p + 1;
+  const size_t g = (size_t)(16 + 2 * e->cfg.nghostcells) * (p ? 16 + 2 * e->cfg.nghostcells : 1);
+  const size_t doubles = g * nw * e->nblk[inst];
+  if (int r = ens_ensure_stage(e, doubles)) return r;
+  ECK(launch_pack(e->pool[p][0], e->d_stage, e->first[inst], e->nblk[inst], nw, ndim, e->cfg.nghostcells,
+                  e->d_nbr[p], e->maps, e->bc, e->stream));
+  ++e->launches;
+  ECK(cudaMemcpyAsync(w, e->d_stage, sizeof(double) * doubles, cudaMemcpyDeviceToHost, e->stream));
+  ECK(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+int amrvac_ens_step(amrvac_ens *e) {
+  if (int r = check_ens(e)) return r;
+  return ens_launch_step(e);
+}
+
+int amrvac_ens_run(amrvac_ens *e, int max_steps, int chunk, int *steps_taken, int *nactive) {
+  if (int r = check_ens(e)) return r;
+  if (max_steps <= 0) return efail(AMRVAC_E_ARG, "max_steps must be positive");
+  if (chunk <= 0) chunk = 16;
+  if (e->graph && e->graph_steps != chunk) {
+    cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+  }
+  if (!e->graph) {
+    cudaGraph_t g;
+    const int64_t before = e->launches;
+    ECK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    int r = 0;
+    for (int s = 0; s < chunk && !r; ++s) r = ens_launch_step(e);
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    e->launches = before;
+    if (r) { if (ce == cudaSuccess) cudaGraphDestroy(g); return r; }
+    if (ce != cudaSuccess) return ecuda(ce, "cudaStreamEndCapture");
+    ce = cudaGraphInstantiate(&e->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) { e->graph = nullptr; return ecuda(ce, "cudaGraphInstantiate"); }
+    e->graph_steps = chunk;
+  }
+  const int per_step = 3 + e->cfg.time_stepper;
+  int taken = 0, act = e->ninst;
+  e->h_done.assign(e->ninst, 0);
+  int ndone_prev = 0;
+  while (taken < max_steps) {
+    ECK(cudaGraphLaunch(e->graph, e->stream));
+    e->launches += (int64_t)chunk * per_step;
+    taken += chunk;
+    ECK(cudaMemcpyAsync(e->h_done.data(), e->d_done, sizeof(int) * e->ninst, cudaMemcpyDeviceToHost, e->stream));
+    ECK(cudaStreamSynchronize(e->stream));
+    const int ndone = (int)std::count_if(e->h_done.begin(), e->h_done.end(), [](int d) { return d != 0; });
+    act = e->ninst - ndone;
+    if (act == 0) break;
+    if (ndone != ndone_prev) {  // drop the finished instances' tiles
+      if (int r = ens_upload_tiles(e, &e->h_done)) return r;
+      ndone_prev = ndone;
+    }
+  }
+  if (steps_taken) *steps_taken = taken;
+  if (nactive) *nactive = act;
+  return 0;
+}
+
+int amrvac_ens_state(amrvac_ens *e, double *t, double *dt, int *steps, int *done) {
+  if (int r = check_ens(e)) return r;
+  if (t) ECK(cudaMemcpyAsync(t, e->d_time, sizeof(double) * e->ninst, cudaMemcpyDeviceToHost, e->stream));
+  if (dt) ECK(cudaMemcpyAsync(dt, e->d_dt, sizeof(double) * e->ninst, cudaMemcpyDeviceToHost, e->stream));
+  if (steps) ECK(cudaMemcpyAsync(steps, e->d_steps, sizeof(int) * e->ninst, cudaMemcpyDeviceToHost, e->stream));
+  if (done) ECK(cudaMemcpyAsync(done, e->d_done, sizeof(int) * e->ninst, cudaMemcpyDeviceToHost, e->stream));
+  ECK(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+int amrvac_ens_status(amrvac_ens *e, uint32_t *flags, uint32_t *inst_flags) {
+  if (int r = check_ens(e)) return r;
+  if (flags) ECK(cudaMemcpyAsync(flags, e->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream));
+  if (inst_flags)
+    ECK(cudaMemcpyAsync(inst_flags, e->d_inst_status, sizeof(uint32_t) * e->ninst, cudaMemcpyDeviceToHost, e->stream));
+  ECK(cudaStreamSynchronize(e->stream));
+  return 0;
+}
+
+int amrvac_ens_set_grid(amrvac_ens *e, int ctas) {
+  if (int r = check_ens(e)) return r;
+  if (ctas < 0) return efail(AMRVAC_E_ARG, "ctas must be >= 0");
+  const int g = ctas == 0 ? e->wave : ctas;
+  if (g != e->grid && e->graph) {
+    cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+  }
+  e->grid = g;
+  return 0;
+}
+
+int amrvac_ens_grid(const amrvac_ens *e, int *ctas, int *wave) {
+  if (!e) return AMRVAC_E_ARG;
+  if (ctas) *ctas = e->grid;
+  if (wave) *wave = e->wave;
+  return 0;
+}
+
+// Times one forward-Euler-like stage (register 0 -> 1, the state in 0 is
+// untouched) for each candidate grid size and keeps the fastest.
+int amrvac_ens_autotune(amrvac_ens *e, int reps, int *best_ctas, double *best_ms) {
+  if (int r = check_ens(e)) return r;
+  if (reps <= 0) reps = 5;
+  // dt of the current state, as the stages read it
+  const EnsArgs G = ens_args(e, 0, 0, 0, 0.0, 1.0, 1.0);
+  ens_getdt_kernel<<<e->grid, STAGE_THREADS, 0, e->stream>>>(G);
+  const EnsTime T = ens_time(e);
+  std::vector<int> done_save(e->ninst);
+  ECK(cudaMemcpyAsync(done_save.data(), e->d_done, sizeof(int) * e->ninst, cudaMemcpyDeviceToHost, e->stream));
+  ens_finalize_kernel<<<(e->ninst + 127) / 128, 128, 0, e->stream>>>(T);
+  ECK(cudaGetLastError());
+  ECK(cudaStreamSynchronize(e->stream));
+  const int cands[4] = {e->wave, 2 * e->wave, 4 * e->wave, e->wave / 2};
+  cudaEvent_t a, b;
+  ECK(cudaEventCreate(&a));
+  ECK(cudaEventCreate(&b));
+  double best = 1e30;
+  int bestg = e->wave;
+  const int saved = e->grid;
+  for (int c : cands) {
+    if (c <= 0) continue;
+    e->grid = c;
+    int r = ens_launch_stage(e, 0, 1, 0, 0.0, 1.0, 1.0);  // warm-up
+    if (r) { e->grid = saved; return r; }
+    ECK(cudaEventRecord(a, e->stream));
+    for (int q = 0; q < reps && !r; ++q) r = ens_launch_stage(e, 0, 1, 0, 0.0, 1.0, 1.0);
+    ECK(cudaEventRecord(b, e->stream));
+    ECK(cudaEventSynchronize(b));
+    if (r) { e->grid = saved; return r; }
+    float ms = 0;
+    ECK(cudaEventElapsedTime(&ms, a, b));
+    if (ms / reps < best) { best = ms / reps; bestg = c; }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  // the probe must not change the instances' clocks: restore done flags and dt
+  ECK(cudaMemcpyAsync(e->d_done, done_save.data(), sizeof(int) * e->ninst, cudaMemcpyHostToDevice, e->stream));
+  ECK(cudaMemsetAsync(e->d_dt, 0, sizeof(double) * e->ninst, e->stream));
+  ECK(cudaStreamSynchronize(e->stream));
+  if (int r = amrvac_ens_set_grid(e, bestg)) return r;
+  if (best_ctas) *best_ctas = bestg;
+  if (best_ms) *best_ms = best;
+  return 0;
+}
+
+int amrvac_ens_stream(amrvac_ens *e, void **stream) {
+  if (int r = check_ens(e)) return r;
+  if (!stream) return efail(AMRVAC_E_ARG, "null argument");
+  *stream = e->stream;
+  return 0;
+}
+
+int64_t amrvac_ens_launch_count(const amrvac_ens *e) { return e ? e->launches : -1; }
+
+}  // extern "C"

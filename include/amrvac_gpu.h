@@ -229,6 +229,58 @@ int amrvac_gpu_riemann_points(amrvac_ctx *ctx, int n, const double *wlp, const d
 int amrvac_gpu_getdt_noalloc(const amrvac_cfg *cfg, const double *w_dev, int nblocks, const double *dx,
                              void *stream, double *dt, double *cmax_global);
 
+/* ---- Batched ensembles (no counterpart in the reference) ------------------
+ * Many independent hydrodynamics runs advanced together: 1-D and 2-D
+ * instances of uneven sizes, each a uniform level-1 grid of 16^d blocks with
+ * its own Riemann solver, limiter, end time and CFL time step, all advanced by
+ * one persistent kernel launch per RK stage.  Each instance follows the
+ * reference's time loop (src/amrvac.t:241-343): setdt (maxsum, dtmin check,
+ * final_dt_reduction, src/mod_dt.t:10-99), exit when time_max is reached,
+ * advance.  Shared by all instances (from amrvac_cfg): gamma, typeboundspeed,
+ * courantpar, cada3_radius, tvdlfeps, small values, time_stepper,
+ * ssprk_order, dtmin, typeboundary (periodic or cont per side) and
+ * precision.  Block arrays are the reference's w(ixG^S,1:nw) per block with
+ * nw = ndim + 2 (rho, m(1:ndim), e), blocks x-fastest within an instance. */
+typedef struct amrvac_ens amrvac_ens;
+typedef struct amrvac_ens_instance {
+  int ndim;              /* 1 or 2 */
+  int domain_nx[2];      /* cells per direction, multiples of 16 */
+  double xprobmin[2], xprobmax[2];
+  int flux_scheme;       /* AMRVAC_FS_TVDLF, _HLL or _HLLC */
+  int limiter;           /* AMRVAC_LIM_* */
+  double time_max;
+} amrvac_ens_instance;
+int amrvac_ens_create(const amrvac_cfg *cfg, int ninst, const amrvac_ens_instance *inst, amrvac_ens **out);
+int amrvac_ens_destroy(amrvac_ens *ens);
+/* Number of blocks of instance i. */
+int amrvac_ens_nblocks(const amrvac_ens *ens, int inst);
+/* Instance state in / out (ghosted block arrays; ghosts are ignored on upload
+ * and filled as getbc would on download).  Synchronous. */
+int amrvac_ens_upload(amrvac_ens *ens, int inst, const double *w);
+int amrvac_ens_download(amrvac_ens *ens, int inst, double *w);
+/* time = 0, steps = 0, all instances active. */
+int amrvac_ens_reset_time(amrvac_ens *ens);
+/* One step of every active instance (asynchronous). */
+int amrvac_ens_step(amrvac_ens *ens);
+/* Steps in CUDA-graph chunks of `chunk` steps until every instance has
+ * reached its time_max or max_steps steps were issued; finished instances are
+ * dropped from the work list between chunks.  Returns the steps issued and the
+ * number of instances still running. */
+int amrvac_ens_run(amrvac_ens *ens, int max_steps, int chunk, int *steps_taken, int *nactive);
+/* Per-instance time, last dt, steps taken, done flag (arrays of ninst; any may
+ * be NULL).  Synchronises. */
+int amrvac_ens_state(amrvac_ens *ens, double *t, double *dt, int *steps, int *done);
+/* Sticky status (OR of AMRVAC_ST_*) and per-instance status (may be NULL). */
+int amrvac_ens_status(amrvac_ens *ens, uint32_t *flags, uint32_t *inst_flags);
+/* CTAs of each stage launch (0 = one resident wave), and the current value. */
+int amrvac_ens_set_grid(amrvac_ens *ens, int ctas);
+int amrvac_ens_grid(const amrvac_ens *ens, int *ctas, int *wave);
+/* Times one stage for candidate grid sizes on the current state (left
+ * unchanged) and keeps the fastest. */
+int amrvac_ens_autotune(amrvac_ens *ens, int reps, int *best_ctas, double *best_ms);
+int amrvac_ens_stream(amrvac_ens *ens, void **stream);
+int64_t amrvac_ens_launch_count(const amrvac_ens *ens);
+
 /* Same-resolution ghost-fill index maps ixS_srl_ / ixR_srl_ of init_bc
  * (src/mod_ghostcells_update.t:150-162), 0-based inclusive, for i=-1,0,1
  * at index i+1. */

@@ -1,0 +1,209 @@
+"""Batched ensembles on the GPU against the oracle.
+
+Each instance of an ensemble is an independent standalone run, so the oracle
+check is per instance: the same seeded Riemann problem run by the oracle's
+grid with the reference's time loop (getdt, final_dt_reduction to time_max,
+advance).  Bars: FP64 <= 1e-12 relative per cell (as the single-grid path),
+time and step counts identical; an instance's result does not depend on the
+other instances of the batch (bit-exact); 1-D runs converge to the exact
+Riemann solution; the mixed form stays within the stated L1 error of FP64.
+"""
+import numpy as np
+import pytest
+
+from tests import _problems as P
+from tests import _riemann as R
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+GAMMA = 1.4
+
+
+def _cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _maxrel(a, b):
+    out = 0.0
+    for v in range(a.shape[1]):
+        scale = np.abs(b[:, v]).max() + 1e-300
+        r = np.abs(a[:, v] - b[:, v]) / (np.abs(b[:, v]) + 1e-3 * scale)
+        out = max(out, float(r.max()))
+    return out
+
+
+def _cfg(precision="fp64", **kw):
+    from amrvac_b200 import make_cfg
+    return make_cfg(physics="hd", ndim=2, gamma=GAMMA, courantpar=0.8, typeboundary=["cont"] * 4,
+                    precision=precision, **kw)
+
+
+def _ensemble(specs, precision="fp64", **kw):
+    from amrvac_b200 import Ensemble
+    ens = Ensemble(_cfg(precision, **kw), [R.instance(s) for s in specs])
+    for i, s in enumerate(specs):
+        ens.upload(i, R.initial_blocks(s, GAMMA))
+    return ens
+
+
+def _oracle_run(oracle_lib, spec, nsteps=None, **kw):
+    """The instance run by the oracle: nsteps steps, or to time_max."""
+    O = oracle_lib
+    nd = spec["ndim"]
+    c = O.make_cfg(physics="hd", ndim=nd, gamma=GAMMA, flux_scheme=spec["flux_scheme"], limiter=spec["limiter"],
+                   courantpar=0.8, **kw)
+    g = O.Grid(c, list(spec["shape"]), [0.0] * nd, [1.0] * nd, ["cont"] * (2 * nd))
+    blocks = R.initial_blocks(spec, GAMMA)
+    for ib in range(g.nblocks):
+        g.set_block(ib, blocks[ib])
+    g.getbc()
+    t, n, tmax = 0.0, 0, spec["time_max"]
+    while nsteps is None or n < nsteps:
+        dt, _ = g.getdt()
+        if tmax - t <= 1e-10 or t >= tmax:
+            break
+        dt = min(dt, tmax - t)
+        g.advance(dt)
+        t += dt
+        n += 1
+    return np.array([g.get_block(ib) for ib in range(g.nblocks)]), t, n
+
+
+def _mixed_specs(seed):
+    specs = R.ensemble_specs(8, seed=seed, n1=(32, 160), n2=(32, 64), time_max=0.05)
+    extra = [
+        dict(specs[0], flux_scheme="tvdlf", limiter="koren"),
+        dict(specs[1], flux_scheme="hll", limiter="cada3", shape=(48, 32)),
+        dict(specs[2], flux_scheme="hllc", limiter="woodward", shape=(16,)),
+    ]
+    return specs + extra
+
+
+def test_ensemble_steps_match_oracle(oracle_lib):
+    """A few steps of a mixed 1-D/2-D ensemble, instance by instance."""
+    _cuda()
+    specs = _mixed_specs(7)
+    ens = _ensemble(specs)
+    nst = 4
+    for _ in range(nst):
+        ens.step()
+    t, dt, steps, done = ens.state()
+    for i, s in enumerate(specs):
+        ref, tref, nref = _oracle_run(oracle_lib, s, nsteps=nst)
+        got = ens.download(i)
+        nd = s["ndim"]
+        err = _maxrel(P.interior(got, nd), P.interior(ref, nd))
+        assert err <= RTOL, (i, s["flux_scheme"], s["limiter"], err)
+        assert steps[i] == nref and abs(t[i] - tref) <= 1e-14 * tref, (i, t[i], tref)
+        assert np.array_equal(got, ref) or err <= RTOL
+    flags, per = ens.status()
+    assert flags == 0 and not per.any()
+
+
+def test_ensemble_runs_to_time_max_like_oracle(oracle_lib):
+    """The graph-chunked run to each instance's own time_max."""
+    _cuda()
+    specs = _mixed_specs(11)
+    for k, s in enumerate(specs):
+        s["time_max"] = 0.01 + 0.004 * k  # uneven end times: instances finish in different chunks
+    ens = _ensemble(specs)
+    taken, active = ens.run(max_steps=100000, chunk=8)
+    assert active == 0
+    t, dt, steps, done = ens.state()
+    assert done.all()
+    for i, s in enumerate(specs):
+        ref, tref, nref = _oracle_run(oracle_lib, s)
+        nd = s["ndim"]
+        assert steps[i] == nref, (i, steps[i], nref)
+        assert abs(t[i] - s["time_max"]) <= 1e-14
+        # tens to hundreds of steps through shocks: FMA reordering accumulates
+        # (the per-step bar of 1e-12 is checked by test_ensemble_steps_match_oracle)
+        err = _maxrel(P.interior(ens.download(i), nd), P.interior(ref, nd))
+        assert err <= 1e-9, (i, err)
+
+
+def test_ensemble_result_independent_of_batch(oracle_lib):
+    """An instance advanced inside a large batch equals the same instance alone, bit for bit."""
+    _cuda()
+    specs = R.ensemble_specs(40, seed=5, n1=(32, 512), n2=(32, 96), time_max=0.02)
+    big = _ensemble(specs)
+    big.run(max_steps=100000, chunk=16)
+    for i in (0, 1, 6, 13, 38):
+        alone = _ensemble([specs[i]])
+        alone.run(max_steps=100000, chunk=16)
+        assert np.array_equal(big.download(i), alone.download(0)), i
+        assert big.state()[2][i] == alone.state()[2][0]
+
+
+def test_finished_instances_stay_fixed():
+    _cuda()
+    specs = R.ensemble_specs(6, seed=3, n1=(32, 64), n2=(32, 32), time_max=0.03)
+    specs[0]["time_max"] = 0.005
+    ens = _ensemble(specs)
+    while ens.state()[3][0] == 0:
+        ens.step()
+    w0 = ens.download(0)
+    t0 = ens.state()[0][0]
+    ens.run(max_steps=100000, chunk=4)
+    assert np.array_equal(ens.download(0), w0)
+    assert ens.state()[0][0] == t0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_sod_1d_converges_to_exact(precision):
+    """The reference's analytic 1-D check: RMSE of density against the exact solution."""
+    _cuda()
+    combos = [("hll", "minmod"), ("hll", "vanleer"), ("hllc", "minmod"), ("hllc", "vanleer")]
+    specs = []
+    for n in (128, 256, 512):
+        for fs, lim in combos:
+            specs.append(dict(ndim=1, shape=(n,), rl=1.0, ul=0.0, pl=1.0, rr=0.125, ur=0.0, pr=0.1, x0=0.5,
+                              theta=0.0, flux_scheme=fs, limiter=lim, time_max=0.2))
+    ens = _ensemble(specs, precision=precision)
+    ens.run(max_steps=100000, chunk=16)
+    rmse = {}
+    for i, s in enumerate(specs):
+        n = s["shape"][0]
+        rho = P.interior(ens.download(i), 1)[:, 0].reshape(-1)
+        x = (np.arange(n) + 0.5) / n
+        ex = R.exact_riemann(1.0, 0.0, 1.0, 0.125, 0.0, 0.1, GAMMA, (x - 0.5) / 0.2)
+        rmse[(n, s["flux_scheme"], s["limiter"])] = float(np.sqrt(np.mean((rho - ex[0]) ** 2)))
+    for fs, lim in combos:
+        e = [rmse[(n, fs, lim)] for n in (128, 256, 512)]
+        assert e[1] < 0.02 and e[0] > e[1] > e[2], (fs, lim, e)
+
+
+def test_mixed_form_l1_error():
+    """Mixed form (FP32 faces) against the FP64 ensemble: L1 density error per instance."""
+    _cuda()
+    specs = R.ensemble_specs(24, seed=9, n1=(64, 1024), n2=(32, 128), time_max=0.05)
+    a = _ensemble(specs)
+    b = _ensemble(specs, precision="mixed")
+    a.run(max_steps=100000, chunk=16)
+    b.run(max_steps=100000, chunk=16)
+    ta, _, sa, _ = a.state()
+    tb, _, sb, _ = b.state()
+    assert np.allclose(ta, tb, rtol=0, atol=1e-14)
+    worst = 0.0
+    for i, s in enumerate(specs):
+        nd = s["ndim"]
+        ra = P.interior(a.download(i), nd)[:, 0]
+        rb = P.interior(b.download(i), nd)[:, 0]
+        worst = max(worst, float(np.abs(rb - ra).sum() / np.abs(ra).sum()))
+    assert worst <= 1e-5, worst
+
+
+def test_autotune_keeps_state():
+    _cuda()
+    specs = R.ensemble_specs(10, seed=2, n1=(64, 256), n2=(32, 64), time_max=0.02)
+    ens = _ensemble(specs)
+    before = [ens.download(i) for i in range(len(specs))]
+    ctas, ms = ens.autotune(reps=2)
+    assert ctas > 0 and ms > 0
+    t, dt, steps, done = ens.state()
+    assert not done.any() and not steps.any() and not t.any()
+    for i in range(len(specs)):
+        assert np.array_equal(ens.download(i), before[i])
