@@ -50,6 +50,7 @@ struct EnsArgs {
   const int *limiter;        // [ninst] LIM_*
   const int *done;           // [ninst]
   unsigned long long *red;   // [ninst] getdt accumulators
+  uint32_t *inst_status;     // [ninst] sticky status per instance
 };
 
 struct EnsRow {
@@ -217,7 +218,10 @@ __device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, int tile, T
     if (P.fix_small_values) {
       if (small_values<double, false, ND, false>(acc, false, P) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
     }
-    if (!isfinite(acc[V::RHO]) || !isfinite(acc[V::E])) st |= ST_NAN;
+    if (!isfinite(acc[V::RHO]) || !isfinite(acc[V::E])) {
+      st |= ST_NAN;
+      atomicOr(A.inst_status + R.inst, ST_NAN);
+    }
 #pragma unroll
     for (int v = 0; v < NW; ++v) S.uout[cell_offset<ND>(R.blk, NW, v, ci, cjj, 0)] = acc[v];
   }
@@ -313,6 +317,14 @@ __global__ void ens_finalize_kernel(const EnsTime T) {
   const double x = __longlong_as_double((long long)T.red[i]);
   T.red[i] = 0ull;
   if (T.done[i]) { T.dt[i] = 0.0; return; }
+  // An instance whose last step produced a non-finite density or energy (or
+  // a small-value error) stops here with that status; the others go on.
+  if (T.inst_status[i] & (ST_SMALL_VALUE | ST_NAN)) {
+    atomicOr(T.status, T.inst_status[i]);
+    T.done[i] = 1;
+    T.dt[i] = 0.0;
+    return;
+  }
   double d = 1.0e99;
   if (x > 1.0e-12) d = fmin(d, T.courantpar / x);
   const double t = T.time[i], tmax = T.time_max[i];
@@ -418,6 +430,7 @@ EnsArgs ens_args(amrvac_ens *e, int reg_ct, int reg_new, int reg_base, double a,
   A.limiter = e->d_limiter;
   A.done = e->d_done;
   A.red = e->d_red;
+  A.inst_status = e->d_inst_status;
   return A;
 }
 

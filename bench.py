@@ -41,7 +41,19 @@ WORKLOADS = {
                        "periodic", physics="mhd", n=256, ndim=3),
     "kh256": dict(desc="2D Euler Kelvin-Helmholtz 256^2, 256 blocks of 16^2, HLLC + vanleer, SSP-RK3, FP64, "
                        "periodic", physics="hd", n=256, ndim=2),
+    "ens512": dict(desc="Batched ensemble: 512 independent Euler Riemann problems (256 1-D of 64-4096 cells, "
+                        "256 2-D of 32^2-512^2 in 16^2 blocks), HLL/HLLC x minmod/vanleer per instance, SSP-RK3 "
+                        "to t=0.2 with per-instance CFL dt (0.8), cont boundaries, one persistent launch per stage",
+                   physics="hd", ensemble=512),
 }
+
+# Signal-speed estimate of the ensemble workload (typeboundspeed).  With the
+# default Einfeldt estimate (Roe averages only, Toro eq. 10.52) 34 of the 512
+# seeded instances turn non-finite within ten steps (strongly diverging states
+# whose rarefaction head it does not bound: negative pressure under a square
+# root), in the oracle as on the GPU; cmaxleftright bounds both heads and
+# every instance reaches t = 0.2.
+ENS_BOUNDSPEED = "cmaxleftright"
 
 # Algorithmic FP64 operations (+,-,*,/,sqrt,exp each 1) per cell for one
 # stage and for one getdt, counted by the oracle's counting scalar on the same
@@ -205,12 +217,23 @@ def run_reference(args, ws, rank):
     if rank != 0:
         return
     nthreads = os.cpu_count() or 1
+    if "ensemble" in WORKLOADS[args.workload]:
+        from tests import _riemann as R
+        specs = R.ensemble_specs(WORKLOADS[args.workload]["ensemble"])
+        init = [R.initial_blocks(sp, 1.4) for sp in specs]
+
+        def sample_fn():  # a few seconds of whole instances per step
+            v, _, smp = _ens_cpu_sample(specs, init, budget_s=3.0)
+            return v, smp
+    else:
+        def sample_fn():
+            return cpu_baseline_sample(args.workload, nthreads, 1)
     for _ in range(args.warmup):
-        cpu_baseline_sample(args.workload, nthreads, 1)
+        sample_fn()
     vals = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        v, sample = cpu_baseline_sample(args.workload, nthreads, 1)
+        v, sample = sample_fn()
         vals.append(v)
     el = time.perf_counter() - t0
     value = float(np.mean(vals))
@@ -223,6 +246,184 @@ def run_reference(args, ws, rank):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def _ens_build(specs, precision, boundspeed=ENS_BOUNDSPEED):
+    from amrvac_b200 import Ensemble, make_cfg
+    from tests import _riemann as R
+    cfg = make_cfg(physics="hd", ndim=2, gamma=1.4, courantpar=0.8, typeboundary=["cont"] * 4, precision=precision,
+                   typeboundspeed=boundspeed)
+    return Ensemble(cfg, [R.instance(s) for s in specs])
+
+
+def _ens_cpu_sample(specs, init, budget_s=15.0):
+    """Oracle (C++ restatement), one instance per host thread, on whole instances
+    taken smallest first until about budget_s of CPU work; zone-updates/s."""
+    import concurrent.futures as cf
+    import oracle as O
+    O.build()
+    nthreads = os.cpu_count() or 1
+    order = sorted(range(len(specs)), key=lambda i: int(np.prod(specs[i]["shape"])))
+
+    def one(i):
+        s = specs[i]
+        nd = s["ndim"]
+        c = O.make_cfg(physics="hd", ndim=nd, gamma=1.4, flux_scheme=s["flux_scheme"], limiter=s["limiter"],
+                       courantpar=0.8, typeboundspeed=ENS_BOUNDSPEED)
+        g = O.Grid(c, list(s["shape"]), [0.0] * nd, [1.0] * nd, ["cont"] * (2 * nd))
+        for ib in range(g.nblocks):
+            g.set_block(ib, init[i][ib])
+        g.getbc()
+        t, n = 0.0, 0
+        while True:
+            dt, _ = g.getdt()
+            if s["time_max"] - t <= 1e-10:
+                break
+            g.advance(min(dt, s["time_max"] - t), 0.0, 1)
+            t += min(dt, s["time_max"] - t)
+            n += 1
+        return int(np.prod(s["shape"])) * n
+
+    done_zu, used = 0, []
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=nthreads) as ex:
+        futs = []
+        for i in order:
+            futs.append(ex.submit(one, i))
+            used.append(i)
+            if len(futs) >= nthreads:
+                done_zu += futs.pop(0).result()
+            if time.perf_counter() - t0 > budget_s:
+                break
+        for f in futs:
+            done_zu += f.result()
+    el = time.perf_counter() - t0
+    return done_zu / el, nthreads, (f"{len(used)} whole instances of the ensemble (smallest first) run to t=0.2 "
+                                    f"by the oracle, one instance per host thread")
+
+
+def run_ensemble(args, ws, rank, local):
+    """Batched-ensemble workload: a step is one full run of all instances to t=0.2."""
+    import torch
+    from tests import _riemann as R
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    w = WORKLOADS[args.workload]
+    specs = R.ensemble_specs(w["ensemble"])
+    init = [R.initial_blocks(sp, 1.4) for sp in specs]
+    nw = np.array([sp["ndim"] + 2 for sp in specs], np.float64)
+    cells = np.array([int(np.prod(sp["shape"])) for sp in specs], np.float64)
+    runs = max(1, min(args.steps, 2))
+    peaks, peak_kind = _measured_peaks()
+
+    def load(ens):
+        for i in range(len(specs)):
+            ens.upload(i, init[i])
+        ens.reset_time()
+
+    def timed_run(ens, clocks=None):
+        s = torch.cuda.ExternalStream(ens.stream_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        l0 = ens.launch_count()
+        e0.record(s)
+        taken, active = ens.run(max_steps=args.it_max or (1 << 30), chunk=16)
+        e1.record(s)
+        e1.synchronize()
+        _, _, steps, done = ens.state()
+        return e0.elapsed_time(e1), steps.astype(np.float64), active, ens.launch_count() - l0, taken
+
+    out = {}
+    finals = {}
+    for prec in ("fp64", "mixed"):
+        ens = _ens_build(specs, prec)
+        load(ens)
+        grid, tune_ms = ens.autotune(reps=3)
+        for _ in range(args.warmup):  # partial runs: kernels, graph, first touch
+            load(ens)
+            ens.run(max_steps=min(64, args.it_max or 64), chunk=16)
+        ms_all, zu = [], 0.0
+        clk = ClockSampler(local) if prec == "fp64" else None
+        if clk:
+            clk.__enter__()
+        for _ in range(runs):
+            load(ens)
+            _barrier(ws)
+            ms, steps, active, launches, taken = timed_run(ens)
+            ms_all.append(_allmax(ms, ws))
+            zu = float((cells * steps).sum())
+            if active and not args.it_max:
+                raise SystemExit(f"bench.py: {active} instances did not finish")
+        if clk:
+            clk.__exit__()
+        flags, per = ens.status()
+        finals[prec] = [ens.download(i) for i in range(len(specs))]
+        ms = float(np.mean(ms_all))
+        alg_bytes = float((cells * steps * 72.0 * nw).sum())  # 72*nw B per zone-update: 3 stages + getdt
+        out[prec] = dict(ms=ms, value=ws * zu / (ms * 1e-3), steps=steps, grid=grid, tune_ms=tune_ms,
+                         launches=launches, chunk_steps=taken, status=flags,
+                         hbm_gbs=alg_bytes / (ms * 1e-3) / 1e9, clocks=clk.summary() if clk else None)
+        if prec == "fp64":
+            # e2e: pinned host arrays in, run, host arrays out
+            pins = [torch.empty(b.shape, dtype=torch.float64).pin_memory() for b in init]
+            for p_, b in zip(pins, init):
+                p_.numpy()[...] = b
+            s = torch.cuda.ExternalStream(ens.stream_ptr())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(s)
+            for i, p_ in enumerate(pins):
+                ens.upload(i, p_.numpy())
+            ens.reset_time()
+            ens.run(max_steps=args.it_max or (1 << 30), chunk=16)
+            res = [ens.download(i) for i in range(len(specs))]
+            e1.record(s)
+            e1.synchronize()
+            e2e_ms = _allmax(e0.elapsed_time(e1), ws)
+            nbytes = float(sum(b.nbytes for b in init))
+            out["e2e"] = {"value": ws * zu / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                          "d2h_bytes_per_step": float(sum(r.nbytes for r in res)),
+                          "what": "C-ABI: upload of every instance from pinned host block arrays, the run to "
+                                  "t=0.2, download of every instance with ghost cells"}
+        ens.close()
+    l1 = []
+    for i, sp in enumerate(specs):
+        a = _interior(finals["fp64"][i], sp["ndim"])[:, 0]
+        b = _interior(finals["mixed"][i], sp["ndim"])[:, 0]
+        l1.append(float(np.abs(b - a).sum() / np.abs(a).sum()))
+    f = out["fp64"]
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, cores, sample = _ens_cpu_sample(specs, init)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": f["value"], "unit": UNIT, "n_gpus": ws, "steps": runs,
+            "warmup": args.warmup, "ms_per_step": f["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["desc"],
+                       "step": ("one full run of every instance to t=0.2" if not args.it_max else
+                                f"every instance for at most {args.it_max} steps (it_max)"),
+                       "typeboundspeed": ENS_BOUNDSPEED,
+                       "instances": len(specs), "cells": float(cells.sum()),
+                       "zone_updates_per_run": float((cells * f["steps"]).sum()),
+                       "max_steps_of_an_instance": int(f["steps"].max()), "graph_chunk_steps": 16,
+                       "grid_ctas": f["grid"], "autotuned_stage_ms": f["tune_ms"],
+                       "parallelism": "replicas" if ws > 1 else "single GPU",
+                       "l2": "no flush: working set %.0f MB (3 registers) > 126 MB L2" % (
+                           3 * float((cells * nw).sum()) * 8 / 1e6)},
+            "roofline": {"bound": "hbm", "achieved": f["hbm_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": f["hbm_gbs"] / peaks["hbm_gbs"], "peak_source": peak_kind, "traffic": None,
+                         "kernel": "whole run (ens_getdt + 3 x ens_stage per step)",
+                         "algorithmic_bytes_per_zone_update": "72*nw (nw = 3 in 1-D, 4 in 2-D)"},
+            "cpu_baseline": cpu, "e2e": out["e2e"],
+            "mixed": {"value": out["mixed"]["value"], "unit": UNIT, "ms_per_step": out["mixed"]["ms"],
+                      "speedup_vs_fp64": f["ms"] / out["mixed"]["ms"], "grid_ctas": out["mixed"]["grid"],
+                      "l1_rel_err_density_vs_fp64": {"max": max(l1), "median": float(np.median(l1))},
+                      "status": out["mixed"]["status"]},
+            "gpu_launches": int(f["launches"]), "clocks": f["clocks"], "status": f["status"],
+        }))
 
 
 def run_ours(args, ws, rank, local):
@@ -368,12 +569,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ot128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--it-max", type=int, default=None,
+                    help="ensemble workloads: stop every instance after this many steps (the reference's it_max)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = _dist_init()
     try:
         if args.impl == "reference":
             run_reference(args, ws, rank)
+        elif "ensemble" in WORKLOADS[args.workload]:
+            run_ensemble(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

@@ -7,6 +7,10 @@
   density), here on [0, 1] with the interface at 0.5 and t = 0.2.
 * Invalid ensembles are refused by the C ABI before any CUDA call.
 * The seeded ensemble inputs follow the stated distributions.
+* Instance 20 of the seeded 512-instance ensemble is a strongly diverging
+  Riemann problem whose rarefaction head the Einfeldt estimate (Roe averages,
+  Toro eq. 10.52, src/hd/mod_hd_phys.t:911-932) does not bound: the oracle's
+  state turns non-finite in the first step; with cmaxleftright it runs.
 """
 import ctypes
 
@@ -110,3 +114,32 @@ def test_ensemble_specs_follow_the_distributions():
     assert {(s["flux_scheme"], s["limiter"]) for s in specs} == {("hll", "minmod"), ("hll", "vanleer"),
                                                                   ("hllc", "minmod"), ("hllc", "vanleer")}
     assert R.ensemble_specs(512) == specs  # seeded
+
+
+def _oracle_steps(oracle_lib, spec, boundspeed, nsteps):
+    O = oracle_lib
+    nd = spec["ndim"]
+    c = O.make_cfg(physics="hd", ndim=nd, gamma=1.4, flux_scheme=spec["flux_scheme"], limiter=spec["limiter"],
+                   courantpar=0.8, typeboundspeed=boundspeed)
+    g = O.Grid(c, list(spec["shape"]), [0.0] * nd, [1.0] * nd, ["cont"] * (2 * nd))
+    b = R.initial_blocks(spec, 1.4)
+    for ib in range(g.nblocks):
+        g.set_block(ib, b[ib])
+    g.getbc()
+    pmin = []
+    for _ in range(nsteps):
+        dt, _ = g.getdt()
+        g.advance(dt)
+        w = np.concatenate([g.get_block(ib)[:, 0, 0, 2:18] for ib in range(g.nblocks)], axis=1)
+        p = 0.4 * (w[2] - 0.5 * w[1] ** 2 / w[0])
+        pmin.append(float(np.min(p)) if np.all(np.isfinite(p)) else float("nan"))
+    return pmin
+
+
+def test_einfeldt_crash_instance_in_the_oracle(oracle_lib):
+    spec = R.ensemble_specs(512)[20]
+    assert spec["ndim"] == 1
+    pe = _oracle_steps(oracle_lib, spec, "Einfeldt", 1)
+    assert not (pe[0] >= 0.0)  # negative pressure or NaN
+    pl = _oracle_steps(oracle_lib, spec, "cmaxleftright", 20)
+    assert all(p > 0.0 for p in pl)

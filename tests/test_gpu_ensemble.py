@@ -27,6 +27,8 @@ def _cuda():
 
 
 def _maxrel(a, b):
+    if not (np.isfinite(a).all() and np.isfinite(b).all()):
+        return float("inf")  # a non-finite value is never a match
     out = 0.0
     for v in range(a.shape[1]):
         scale = np.abs(b[:, v]).max() + 1e-300
@@ -35,26 +37,32 @@ def _maxrel(a, b):
     return out
 
 
-def _cfg(precision="fp64", **kw):
+# The bound speed of the ensemble workload; with the default Einfeldt estimate
+# some of these strongly diverging Riemann problems turn non-finite (in the
+# oracle as on the GPU), see test_non_finite_instance_stops_alone.
+BOUNDSPEED = "cmaxleftright"
+
+
+def _cfg(precision="fp64", boundspeed=BOUNDSPEED, **kw):
     from amrvac_b200 import make_cfg
     return make_cfg(physics="hd", ndim=2, gamma=GAMMA, courantpar=0.8, typeboundary=["cont"] * 4,
-                    precision=precision, **kw)
+                    precision=precision, typeboundspeed=boundspeed, **kw)
 
 
-def _ensemble(specs, precision="fp64", **kw):
+def _ensemble(specs, precision="fp64", boundspeed=BOUNDSPEED):
     from amrvac_b200 import Ensemble
-    ens = Ensemble(_cfg(precision, **kw), [R.instance(s) for s in specs])
+    ens = Ensemble(_cfg(precision, boundspeed), [R.instance(s) for s in specs])
     for i, s in enumerate(specs):
         ens.upload(i, R.initial_blocks(s, GAMMA))
     return ens
 
 
-def _oracle_run(oracle_lib, spec, nsteps=None, **kw):
+def _oracle_run(oracle_lib, spec, nsteps=None, boundspeed=BOUNDSPEED):
     """The instance run by the oracle: nsteps steps, or to time_max."""
     O = oracle_lib
     nd = spec["ndim"]
     c = O.make_cfg(physics="hd", ndim=nd, gamma=GAMMA, flux_scheme=spec["flux_scheme"], limiter=spec["limiter"],
-                   courantpar=0.8, **kw)
+                   courantpar=0.8, typeboundspeed=boundspeed)
     g = O.Grid(c, list(spec["shape"]), [0.0] * nd, [1.0] * nd, ["cont"] * (2 * nd))
     blocks = R.initial_blocks(spec, GAMMA)
     for ib in range(g.nblocks):
@@ -207,3 +215,26 @@ def test_autotune_keeps_state():
     assert not done.any() and not steps.any() and not t.any()
     for i in range(len(specs)):
         assert np.array_equal(ens.download(i), before[i])
+
+
+def test_non_finite_instance_stops_alone(oracle_lib):
+    """An instance whose state turns non-finite (the oracle's does too) stops
+    with the NaN status; the others of the batch are unaffected."""
+    _cuda()
+    specs = R.ensemble_specs(512)
+    crash = dict(specs[20], time_max=0.02)
+    others = [dict(s, time_max=0.02) for s in R.ensemble_specs(4, seed=31, n1=(32, 96), n2=(32, 48))]
+    batch = [others[0], crash] + others[1:]
+    ens = _ensemble(batch, boundspeed="Einfeldt")
+    ens.run(max_steps=100000, chunk=4)
+    t, dt, steps, done = ens.state()
+    flags, per = ens.status()
+    assert done.all()
+    assert per[1] & 2 and steps[1] <= 2 and t[1] < 0.02
+    assert flags & 2
+    for i in (0, 2, 3, 4):
+        s = batch[i]
+        assert per[i] == 0 and abs(t[i] - 0.02) <= 1e-14
+        ref, _, nref = _oracle_run(oracle_lib, s, boundspeed="Einfeldt")
+        assert steps[i] == nref
+        assert _maxrel(P.interior(ens.download(i), s["ndim"]), P.interior(ref, s["ndim"])) <= 1e-9

@@ -80,6 +80,8 @@ def _setup(oracle_lib, name, n=32, bc=None, seed=P.SEED):
 
 def _maxrel(a, b):
     """max over cells of |a-b| / (|b| + 1e-3*max|b_v|) per variable."""
+    if not (np.isfinite(a).all() and np.isfinite(b).all()):
+        return float("inf")  # a non-finite value is never a match
     out = 0.0
     for v in range(a.shape[1]):
         scale = np.abs(b[:, v]).max() + 1e-300
