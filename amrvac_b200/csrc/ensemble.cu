@@ -96,9 +96,112 @@ __device__ __forceinline__ uint32_t ens_face(TF *wLp, TF *wRp, const PhysParams 
   return face_from_states<TF, false, ND, false, ND, SOLVER, 0>(wLp, wRp, P, TF(0), F);
 }
 
-// One RK stage on one tile.
+// Stage kernel organisation: 288 threads.  Threads 0..255 own the cells of
+// the tile (ci = t % 16, row cj = t / 16) and compute the x-face and the
+// y-face on the low side of their cell; the ninth warp computes the 16 x-faces
+// of the high side (lanes 0..15) and the 16 y-faces of the top (lanes 16..31),
+// so every thread handles at most two faces.  The shared tile is double
+// buffered and the row table triple buffered, so one tile costs two barriers:
+//   stage cells + halos (+ row table of the next tile, by the ninth warp)
+//   | barrier | all faces of both directions | barrier | accumulate + store.
+constexpr int ENS_THREADS = 288;
+
+// Shared tile of one buffer, in TF elements, for up to 4 variables.
+template <class TF>
+struct EnsTile {
+  static constexpr int NWM = 4;
+  static constexpr int TOTAL = NWM * (BN * BN + BN * 4 + 4 * BN + 2 * (BN + 1) * BN);
+};
+
+template <class TF, int NW>
+struct EnsView {
+  TF *ring, *hx, *hy, *fbx, *fby;  // [v][j][i], [v][j][c], [v][r][i], [v][j][17], [v][17][i]
+  __device__ __forceinline__ explicit EnsView(TF *s) {
+    ring = s;
+    hx = ring + NW * BN * BN;
+    hy = hx + NW * BN * 4;
+    fbx = hy + NW * 4 * BN;
+    fby = fbx + NW * (BN + 1) * BN;
+  }
+  // element offset of variable 0 at (i, j) in [-2, 17] x [0, 15] or [0, 15] x [-2, 17],
+  // and the stride between variables
+  __device__ __forceinline__ void addr(int i, int j, int &base, int &stride) const {
+    const bool ii = (unsigned)i < (unsigned)BN;
+    const bool jj = (unsigned)j < (unsigned)BN;
+    if (ii && jj) { base = j * BN + i; stride = BN * BN; }
+    else if (jj) { base = NW * BN * BN + j * 4 + halo_slot(i); stride = BN * 4; }
+    else { base = NW * BN * BN + NW * BN * 4 + halo_slot(j) * BN + i; stride = 4 * BN; }
+  }
+};
+
+// Row table entry of one row of a tile (2-D tile: the block, all rows alike).
+__device__ __forceinline__ void ens_fill_row(const EnsArgs &A, int tile, bool two_d, int row, EnsRow &R) {
+  const int b = A.tiles[tile * ENS_ROWS + (two_d ? 0 : row)];
+  int in = b >= 0 ? A.inst[two_d ? 1 : 0][b] : -1;
+  if (in >= 0 && A.done[in]) in = -1;
+  R.blk = b;
+  R.inst = in;
+  if (in >= 0) {
+    R.solver = A.solver[in];
+    R.limiter = A.limiter[in];
+    const double qdt = A.dtfactor * A.dt[in];
+    for (int d = 0; d < (two_d ? 2 : 1); ++d) {
+      const double dx = A.dx[in * 2 + d];
+      R.sc[d] = -qdt / dx;
+      const double r = A.sa[0].P.cada3_radius * dx;
+      R.rd[d] = 1.0 / (r * r);
+      R.dxinv[d] = 1.0 / dx;
+    }
+  }
+}
+
+// One face of direction D (run-time, so one copy of the face code serves
+// both directions and all call sites) at face coordinates (fi, fj): limited
+// reconstruction from the staged primitives, Riemann flux, store to fb.
 template <class TF, int ND>
-__device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, int tile, TF *smem, EnsRow *rows) {
+__device__ __forceinline__ uint32_t ens_face_at(const TF *s, const EnsView<TF, ND + 2> &tv, const EnsRow &Rf,
+                                                const PhysParams &P, int D, int fi, int fj) {
+  constexpr int NW = ND + 2;
+  constexpr int FB = (BN + 1) * BN;
+  constexpr bool FP64 = sizeof(TF) == 8;
+  const TF rd = TF(D == 0 ? Rf.rd[0] : Rf.rd[ND - 1]);
+  const int lim = Rf.limiter;
+  TF wLp[NW], wRp[NW];
+  int base[4], strd[4];
+#pragma unroll
+  for (int o = 0; o < 4; ++o) tv.addr(D == 0 ? fi + o - 2 : fi, D == 0 ? fj : fj + o - 2, base[o], strd[o]);
+#pragma unroll
+  for (int v = 0; v < NW; ++v) {
+    const int ov = orig_index_rt<false, ND>(v, D);
+    TF q[4];
+#pragma unroll
+    for (int o = 0; o < 4; ++o) q[o] = s[base[o] + ov * strd[o]];
+    const TF d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
+    wLp[v] = q[1] + TF(0.5) * limited_slope<TF, true, 0>(lim, d1, d0, rd);
+    wRp[v] = q[2] - TF(0.5) * limited_slope<TF, false, 0>(lim, d2, d1, rd);
+  }
+  TF Fr[NW];
+  uint32_t st;
+  if (Rf.solver == SOLVER_HLLC) st = ens_face<TF, ND, SOLVER_HLLC>(wLp, wRp, P, Fr);
+  else if (Rf.solver == SOLVER_HLL) st = ens_face<TF, ND, SOLVER_HLL>(wLp, wRp, P, Fr);
+  else st = ens_face<TF, ND, SOLVER_TVDLF>(wLp, wRp, P, Fr);
+  TF *fb = D == 0 ? tv.fbx : tv.fby;
+  const int f = D == 0 ? fj * (BN + 1) + fi : fj * BN + fi;
+  const double sc = D == 0 ? Rf.sc[0] : Rf.sc[ND - 1];
+#pragma unroll
+  for (int v = 0; v < NW; ++v) {
+    const int ov = orig_index_rt<false, ND>(v, D);
+    if constexpr (FP64) fb[ov * FB + f] = sc * Fr[v];
+    else fb[ov * FB + f] = Fr[v];
+  }
+  return st;
+}
+
+// One RK stage on one tile; `cur` holds this tile's rows, `nxt` receives the
+// rows of tile `next` (if < nt).
+template <class TF, int ND>
+__device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, TF *s, const EnsRow *cur, EnsRow *nxt,
+                                                   int next, int nt, int n2) {
   using V = Vars<false, ND, false>;
   constexpr int NW = V::NW;
   constexpr int FB = (BN + 1) * BN;
@@ -106,44 +209,44 @@ __device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, int tile, T
   const StageArgs &S = A.sa[ND - 1];
   const PhysParams &P = S.P;
   const int t = threadIdx.x;
-  const int ci = t & (BN - 1), cj = t >> 4;
+  const bool cell_thread = t < BN * BN;
+  const int ci = t & (BN - 1), cj = (t >> 4) & (BN - 1);
+  const int lane = t - BN * BN;  // ninth warp: 0..31
   uint32_t st = 0;
-  if (!ens_rows<ND>(A, tile, false, rows)) {
-    __syncthreads();
-    return 0;
+  EnsView<TF, NW> tv(s);
+  const EnsRow &R = cur[ND == 2 ? 0 : cj];
+  const bool active = cell_thread && R.inst >= 0;
+  const int cjj = ND == 2 ? cj : 0;
+  // ---- stage: cells, halos, RK combination; the ninth warp fetches the next tile's rows
+  if (!cell_thread) {
+    if (lane < ENS_ROWS && next < nt) ens_fill_row(A, next, next < n2, lane, nxt[lane]);
   }
-  TileView<TF, NW, 2> tv(smem);
-  const EnsRow &R = rows[ND == 2 ? 0 : cj];
-  const bool active = R.inst >= 0;
-  const int cjj = ND == 2 ? cj : 0;  // y index inside the block
-  // ---- stage the cells of the tile as primitives
   if (active) {
     double w[NW];
     st |= load_prim<false, ND, false, ND>(S, R.blk, ci, cjj, 0, w);
 #pragma unroll
-    for (int v = 0; v < NW; ++v) tv.center(0, v, ci, cj) = TF(w[v]);
+    for (int v = 0; v < NW; ++v) tv.ring[v * BN * BN + cj * BN + ci] = TF(w[v]);
   }
-  // ---- halo strips: x (both kinds of tile), y (2-D tiles)
   if (t < (ND == 2 ? 128 : 64)) {
-    const int h = t;
-    int i, j, row, stride;
+    int i, j, row;
     TF *dst;
-    if (h < 64) {
-      j = h >> 2;
-      const int c = h & 3;
+    int stride;
+    if (t < 64) {
+      j = t >> 2;
+      const int c = t & 3;
       i = c < 2 ? c - 2 : c + BN - 2;
       dst = tv.hx + j * 4 + c;
       stride = BN * 4;
       row = ND == 2 ? 0 : j;
     } else {
-      const int r = (h - 64) >> 4;
-      i = (h - 64) & (BN - 1);
+      const int r = (t - 64) >> 4;
+      i = (t - 64) & (BN - 1);
       j = r < 2 ? r - 2 : r + BN - 2;
       dst = tv.hy + r * BN + i;
       stride = 4 * BN;
       row = 0;
     }
-    const EnsRow &H = rows[row];
+    const EnsRow &H = cur[row];
     if (H.inst >= 0) {
       double w[NW];
       st |= load_prim<false, ND, false, ND>(S, H.blk, i, ND == 2 ? j : 0, 0, w);
@@ -151,7 +254,6 @@ __device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, int tile, T
       for (int v = 0; v < NW; ++v) dst[v * stride] = TF(w[v]);
     }
   }
-  // ---- RK combination wnew0 = a*base + b*in (src/mod_advance.t:254-266)
   double acc[NW];
   if (active) {
 #pragma unroll
@@ -162,59 +264,43 @@ __device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, int tile, T
     }
   }
   __syncthreads();
-  // ---- face phases
-#pragma unroll 1
-  for (int D = 0; D < ND; ++D) {
-#pragma unroll 1
-    for (int f = t; f < FB; f += STAGE_THREADS) {
-      int fi, fj;
-      if (D == 0) { fj = f / (BN + 1); fi = f - fj * (BN + 1); }
-      else { fj = f >> 4; fi = f & (BN - 1); }
-      const EnsRow &Rf = rows[ND == 2 ? 0 : fj];
-      if (Rf.inst < 0) continue;
-      const TF rd = TF(Rf.rd[D]);
-      const int lim = Rf.limiter;
-      TF wLp[NW], wRp[NW];
-      int base[4], strd[4];
-#pragma unroll
-      for (int o = 0; o < 4; ++o)
-        tv.addr(0, D == 0 ? fi + o - 2 : fi, D == 0 ? fj : fj + o - 2, base[o], strd[o]);
-#pragma unroll
-      for (int v = 0; v < NW; ++v) {
-        const int ov = orig_index_rt<false, ND>(v, D);
-        TF q[4];
-#pragma unroll
-        for (int o = 0; o < 4; ++o) q[o] = smem[base[o] + ov * strd[o]];
-        const TF d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
-        wLp[v] = q[1] + TF(0.5) * limited_slope<TF, true, 0>(lim, d1, d0, rd);
-        wRp[v] = q[2] - TF(0.5) * limited_slope<TF, false, 0>(lim, d2, d1, rd);
-      }
-      TF Fr[NW];
-      if (Rf.solver == SOLVER_HLLC) st |= ens_face<TF, ND, SOLVER_HLLC>(wLp, wRp, P, Fr);
-      else if (Rf.solver == SOLVER_HLL) st |= ens_face<TF, ND, SOLVER_HLL>(wLp, wRp, P, Fr);
-      else st |= ens_face<TF, ND, SOLVER_TVDLF>(wLp, wRp, P, Fr);
-      const double sc = Rf.sc[D];
-#pragma unroll
-      for (int v = 0; v < NW; ++v) {
-        const int ov = orig_index_rt<false, ND>(v, D);
-        if constexpr (FP64) tv.fb[ov * FB + f] = sc * Fr[v];
-        else tv.fb[ov * FB + f] = Fr[v];
+  // ---- faces of both directions: up to two per thread, one call site
+  {
+    int nf = 0, fd0 = 0, fi0 = 0, fj0 = 0, fi1 = 0, fj1 = 0;
+    const EnsRow *rf = &R;
+    if (active) {
+      nf = ND;  // x-face (ci, cj) and, in 2-D, y-face (ci, cj)
+      fi0 = ci; fj0 = cj; fi1 = ci; fj1 = cj;
+    } else if (!cell_thread) {
+      if (lane < BN) {
+        rf = &cur[ND == 2 ? 0 : lane];
+        nf = rf->inst >= 0 ? 1 : 0;
+        fi0 = BN; fj0 = lane;
+      } else if (ND == 2) {
+        rf = &cur[0];
+        nf = rf->inst >= 0 ? 1 : 0;
+        fd0 = 1; fi0 = lane - BN; fj0 = BN;
       }
     }
-    __syncthreads();
-    if (active) {
-      const double sc = FP64 ? 1.0 : R.sc[D];
+#pragma unroll 1
+    for (int q = 0; q < nf; ++q)
+      st |= ens_face_at<TF, ND>(s, tv, *rf, P, q == 0 ? fd0 : 1, q == 0 ? fi0 : fi1, q == 0 ? fj0 : fj1);
+  }
+  __syncthreads();
+  // ---- flux divergence in direction order, small values, store
+  if (active) {
+#pragma unroll
+    for (int D = 0; D < ND; ++D) {
+      const TF *fb = D == 0 ? tv.fbx : tv.fby;
       const int f = D == 0 ? cj * (BN + 1) + ci : cj * BN + ci;
       const int step = D == 0 ? 1 : BN;
+      const double sc = FP64 ? 1.0 : R.sc[D];
 #pragma unroll
       for (int v = 0; v < NW; ++v) {
-        if constexpr (FP64) acc[v] = acc[v] + tv.fb[v * FB + f + step] - tv.fb[v * FB + f];
-        else acc[v] = acc[v] + sc * double(tv.fb[v * FB + f + step]) - sc * double(tv.fb[v * FB + f]);
+        if constexpr (FP64) acc[v] = acc[v] + fb[v * FB + f + step] - fb[v * FB + f];
+        else acc[v] = acc[v] + sc * double(fb[v * FB + f + step]) - sc * double(fb[v * FB + f]);
       }
     }
-    __syncthreads();
-  }
-  if (active) {
     if (P.fix_small_values) {
       if (small_values<double, false, ND, false>(acc, false, P) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
     }
@@ -229,17 +315,27 @@ __device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, int tile, T
 }
 
 template <class TF>
-__global__ void __launch_bounds__(STAGE_THREADS, 2) ens_stage_kernel(const EnsArgs A) {
+__global__ void __launch_bounds__(ENS_THREADS, 2) ens_stage_kernel(const EnsArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TF *smem = reinterpret_cast<TF *>(smem_raw);
-  __shared__ EnsRow rows[ENS_ROWS];
+  TF *sm = reinterpret_cast<TF *>(smem_raw);
+  __shared__ EnsRow rows[3][ENS_ROWS];
   const int n2 = A.ntiles[0], nt = A.ntiles[1];
+  int tile = blockIdx.x;
+  if (tile >= nt) return;
+  const int t = threadIdx.x;
+  if (t >= BN * BN && t < BN * BN + ENS_ROWS) ens_fill_row(A, tile, tile < n2, t - BN * BN, rows[0][t - BN * BN]);
+  __syncthreads();
   uint32_t st = 0;
 #pragma unroll 1
-  for (int tile = blockIdx.x; tile < nt; tile += gridDim.x) {
-    if (tile < n2) st |= ens_stage_tile<TF, 2>(A, tile, smem, rows);
-    else st |= ens_stage_tile<TF, 1>(A, tile, smem, rows);
-    __syncthreads();  // the next tile rewrites rows[] and the shared tile
+  for (int k = 0; tile < nt; ++k, tile += gridDim.x) {
+    // buffers of tile k: shared tile k % 2 and row table k % 3 (a thread still
+    // accumulating tile k-1 reads only buffers that this iteration leaves alone)
+    TF *s = sm + (k & 1) * EnsTile<TF>::TOTAL;
+    const EnsRow *cur = rows[k % 3];
+    EnsRow *nxt = rows[(k + 1) % 3];
+    const int next = tile + gridDim.x;
+    if (tile < n2) st |= ens_stage_tile<TF, 2>(A, s, cur, nxt, next, nt, n2);
+    else st |= ens_stage_tile<TF, 1>(A, s, cur, nxt, next, nt, n2);
   }
   if (st) atomicOr(A.sa[0].status, st);
 }
@@ -401,7 +497,7 @@ int ecuda(cudaError_t e, const char *where) {
   } while (0)
 
 size_t ens_smem(bool mixed) {
-  return mixed ? Tile<float, 4, 2>::BYTES : Tile<double, 4, 2>::BYTES;
+  return mixed ? 2 * sizeof(float) * EnsTile<float>::TOTAL : 2 * sizeof(double) * EnsTile<double>::TOTAL;
 }
 
 EnsArgs ens_args(amrvac_ens *e, int reg_ct, int reg_new, int reg_base, double a, double b, double dtfactor) {
@@ -452,8 +548,8 @@ EnsTime ens_time(amrvac_ens *e) {
 
 int ens_launch_stage(amrvac_ens *e, int reg_ct, int reg_new, int reg_base, double a, double b, double dtf) {
   const EnsArgs A = ens_args(e, reg_ct, reg_new, reg_base, a, b, dtf);
-  if (e->mixed) ens_stage_kernel<float><<<e->grid, STAGE_THREADS, ens_smem(true), e->stream>>>(A);
-  else ens_stage_kernel<double><<<e->grid, STAGE_THREADS, ens_smem(false), e->stream>>>(A);
+  if (e->mixed) ens_stage_kernel<float><<<e->grid, ENS_THREADS, ens_smem(true), e->stream>>>(A);
+  else ens_stage_kernel<double><<<e->grid, ENS_THREADS, ens_smem(false), e->stream>>>(A);
   ECK(cudaGetLastError());
   ++e->launches;
   return 0;
@@ -765,8 +861,8 @@ int amrvac_ens_create(const amrvac_cfg *cfg, int ninst, const amrvac_ens_instanc
   else ce = cudaFuncSetAttribute(ens_stage_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ens_smem(false));
   if (ce) return fail_free(ce, "cudaFuncSetAttribute");
   int per_sm = 1, dev = 0, nsm = 148;
-  if (e->mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_stage_kernel<float>, STAGE_THREADS, ens_smem(true));
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_stage_kernel<double>, STAGE_THREADS, ens_smem(false));
+  if (e->mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_stage_kernel<float>, ENS_THREADS, ens_smem(true));
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_stage_kernel<double>, ENS_THREADS, ens_smem(false));
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   e->wave = std::max(1, per_sm) * nsm;
