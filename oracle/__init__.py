@@ -92,6 +92,8 @@ def lib():
         L.orc_count_flops_stage.argtypes = [cp, dp, dp, d, dp, d]
         L.orc_count_flops_getdt.restype = d
         L.orc_count_flops_getdt.argtypes = [cp, dp, dp]
+        L.orc_dual_run.restype = ctypes.c_int
+        L.orc_dual_run.argtypes = [cp, ip, dp, dp, ip, dp, dp, d, ctypes.c_int, dp, dp, ctypes.c_int, dp, dp, dp]
         _lib = L
     return _lib
 
@@ -264,3 +266,27 @@ def compare_logs(a: np.ndarray, b: np.ndarray, rtol=1.0e-5, atol=1.0e-8) -> bool
     if a.shape != b.shape:
         return False
     return bool(np.all(np.abs(a - b) <= atol + 0.5 * rtol * (np.abs(a) + np.abs(b))))
+
+
+def dual_run(c: OrcCfg, domain_nx, xprobmin, xprobmax, bc, w0, dw0, dgamma, dts, mask, nthreads=0,
+             want_final=False):
+    """Forward-mode reference gradient (orc_dual_run): loss = sum(mask * rho^2)
+    after len(dts) SSP-RK3 steps with the frozen dt sequence, and its
+    derivative along (dw0, dgamma).  w0, dw0: conserved block arrays
+    (nblocks, nw, nz, ny, nx); mask: (nblocks, nz, ny, nx)."""
+    nd = c.ndim
+    dn = np.array(list(domain_nx) + [1] * (3 - nd), np.int32)
+    xmn = np.array(list(xprobmin) + [0.0] * (3 - nd), np.float64)
+    xmx = np.array(list(xprobmax) + [1.0] * (3 - nd), np.float64)
+    bca = np.array([BC[b] if isinstance(b, str) else b for b in bc] + [0] * (6 - len(bc)), np.int32)
+    w0 = np.ascontiguousarray(w0, np.float64)
+    dw = None if dw0 is None else np.ascontiguousarray(dw0, np.float64)
+    dts = np.ascontiguousarray(dts, np.float64)
+    mask = np.ascontiguousarray(mask, np.float64)
+    loss = ctypes.c_double()
+    dloss = ctypes.c_double()
+    wf = np.empty_like(w0) if want_final else None
+    st = lib().orc_dual_run(ctypes.byref(c), _ip(dn), _dp(xmn), _dp(xmx), _ip(bca), _dp(w0),
+                            _dp(dw) if dw is not None else None, float(dgamma), len(dts), _dp(dts), _dp(mask),
+                            nthreads, ctypes.byref(loss), ctypes.byref(dloss), _dp(wf) if wf is not None else None)
+    return (loss.value, dloss.value, st) + ((wf,) if want_final else ())

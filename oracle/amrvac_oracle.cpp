@@ -8,7 +8,8 @@
 //
 // All routines are templates on the scalar type R: R=double is the oracle,
 // R=Counted counts +,-,*,/,sqrt,exp (FMA never occurs here) to give the
-// algorithmic flop count per zone update.
+// algorithmic flop count per zone update, and R=Dual carries one directional
+// derivative (forward mode) for the reference gradient of the adjoint.
 
 #include "amrvac_oracle.h"
 
@@ -53,6 +54,43 @@ inline double rsqrt_(double x) { return std::sqrt(x); }
 inline Counted rsqrt_(Counted x) { ++g_ops; return Counted(std::sqrt(x.v)); }
 inline double rexp_(double x) { return std::exp(x); }
 inline Counted rexp_(Counted x) { ++g_ops; return Counted(std::exp(x.v)); }
+// Forward-mode dual number: value and one directional derivative.  Branches
+// (limiters, upwind choices, max/min) follow the value, so the derivative is
+// that of the discrete scheme along the branch the value takes.
+struct Dual {
+  double v, d;
+  Dual() : v(0), d(0) {}
+  Dual(double x) : v(x), d(0) {}
+  Dual(double x, double dx) : v(x), d(dx) {}
+};
+inline Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
+inline Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
+inline Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+inline Dual operator/(Dual a, Dual b) {
+  const double q = a.v / b.v;
+  return Dual(q, (a.d - q * b.d) / b.v);
+}
+inline Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
+inline Dual &operator+=(Dual &a, Dual b) { a = a + b; return a; }
+inline Dual &operator-=(Dual &a, Dual b) { a = a - b; return a; }
+inline Dual &operator*=(Dual &a, Dual b) { a = a * b; return a; }
+inline bool operator<(Dual a, Dual b) { return a.v < b.v; }
+inline bool operator>(Dual a, Dual b) { return a.v > b.v; }
+inline bool operator<=(Dual a, Dual b) { return a.v <= b.v; }
+inline bool operator>=(Dual a, Dual b) { return a.v >= b.v; }
+inline bool operator==(Dual a, Dual b) { return a.v == b.v; }
+inline bool operator!=(Dual a, Dual b) { return a.v != b.v; }
+inline double val(Dual x) { return x.v; }
+inline Dual rsqrt_(Dual x) {
+  const double r = std::sqrt(x.v);
+  return Dual(r, x.d / (2.0 * r));
+}
+inline Dual rexp_(Dual x) {
+  const double e = std::exp(x.v);
+  return Dual(e, e * x.d);
+}
+inline Dual rabs(Dual x) { return x.v < 0.0 ? -x : x; }
+
 template <class R> inline R rabs(R x) { return R(std::fabs(val(x))); }
 template <class R> inline R rmax(R a, R b) { return (b > a) ? b : a; }
 template <class R> inline R rmin(R a, R b) { return (b < a) ? b : a; }
@@ -167,6 +205,20 @@ inline State make_state(const orc_cfg &c) {
   return s;
 }
 
+// gamma, gamma-1 and 1/(gamma-1) as scalars of type R.  double and Counted
+// use the values precomputed in State (no counted operation, bit-identical
+// to using them directly); Dual carries d(gamma) = g_dual_dgamma so that the
+// forward-mode run differentiates with respect to gamma as well.
+static double g_dual_dgamma = 0.0;
+template <class R> inline R gam_(const State &s) { return R(s.c.gamma); }
+template <class R> inline R gam1_(const State &s) { return R(s.gamma_1); }
+template <class R> inline R igam1_(const State &s) { return R(s.inv_gamma_1); }
+template <> inline Dual gam_<Dual>(const State &s) { return Dual(s.c.gamma, g_dual_dgamma); }
+template <> inline Dual gam1_<Dual>(const State &s) { return Dual(s.gamma_1, g_dual_dgamma); }
+template <> inline Dual igam1_<Dual>(const State &s) {
+  return Dual(s.inv_gamma_1, -s.inv_gamma_1 * s.inv_gamma_1 * g_dual_dgamma);
+}
+
 // Accessor for one cell's variables inside an Arr.
 #define W(a, v) a(i, j, k, v)
 
@@ -181,9 +233,9 @@ template <class R> void to_conserved(const State &s, const Box &b, Arr<R> &w) {
     if (x.mhd) {
       R b2 = W(w, x.mag[0]) * W(w, x.mag[0]);
       for (int c = 1; c < x.ndir; ++c) b2 = b2 + W(w, x.mag[c]) * W(w, x.mag[c]);
-      W(w, x.e) = W(w, x.e) * s.inv_gamma_1 + half * (v2 * W(w, x.rho) + b2);
+      W(w, x.e) = W(w, x.e) * igam1_<R>(s) + half * (v2 * W(w, x.rho) + b2);
     } else {
-      W(w, x.e) = W(w, x.e) * s.inv_gamma_1 + half * v2 * W(w, x.rho);
+      W(w, x.e) = W(w, x.e) * igam1_<R>(s) + half * v2 * W(w, x.rho);
     }
     for (int c = 0; c < x.ndir; ++c) W(w, x.mom[c]) = W(w, x.rho) * W(w, x.mom[c]);
   });
@@ -205,9 +257,9 @@ template <class R> int to_primitive(const State &s, const Box &b, Arr<R> &w) {
     if (x.mhd) {
       R b2 = W(w, x.mag[0]) * W(w, x.mag[0]);
       for (int c = 1; c < x.ndir; ++c) b2 = b2 + W(w, x.mag[c]) * W(w, x.mag[c]);
-      W(w, x.e) = R(s.gamma_1) * (W(w, x.e) - half * (W(w, x.rho) * v2 + b2));
+      W(w, x.e) = gam1_<R>(s) * (W(w, x.e) - half * (W(w, x.rho) * v2 + b2));
     } else {
-      W(w, x.e) = R(s.c.gamma - 1.0) * (W(w, x.e) - half * W(w, x.rho) * v2);
+      W(w, x.e) = gam1_<R>(s) * (W(w, x.e) - half * W(w, x.rho) * v2);
     }
   });
   return st;
@@ -232,7 +284,7 @@ template <class R> int handle_small_values(const State &s, bool primitive, Arr<R
       for (int q = 1; q < x.ndir; ++q) b2 = b2 + W(w, x.mag[q]) * W(w, x.mag[q]);
       fe = W(w, x.e) - half * (m2 / W(w, x.rho) + b2) < R(s.small_e);
     } else {
-      R tmp = R(c.gamma - 1.0) * (W(w, x.e) - half * m2 / W(w, x.rho));
+      R tmp = gam1_<R>(s) * (W(w, x.e) - half * m2 / W(w, x.rho));
       fe = tmp < R(c.small_pressure);
     }
     if (!frho && !fe) return;
@@ -306,7 +358,7 @@ template <class R>
 R csound_prim(const State &s, const Arr<R> &w, int i, int j, int k, int idim) {
   const Ix &x = s.x;
   R inv_rho = R(1.0) / W(w, x.rho);
-  R cs = R(s.c.gamma) * W(w, x.e) * inv_rho;
+  R cs = gam_<R>(s) * W(w, x.e) * inv_rho;
   R b2 = W(w, x.mag[0]) * W(w, x.mag[0]);
   for (int c = 1; c < x.ndir; ++c) b2 = b2 + W(w, x.mag[c]) * W(w, x.mag[c]);
   R cfast2 = b2 * inv_rho + cs;
@@ -323,13 +375,13 @@ R hd_csound2_cons(const State &s, const Arr<R> &w, int i, int j, int k, int &st)
   R m2 = W(w, x.mom[0]) * W(w, x.mom[0]);
   for (int c = 1; c < x.ndir; ++c) m2 = m2 + W(w, x.mom[c]) * W(w, x.mom[c]);
   R ke = R(0.5) * m2 / W(w, x.rho);
-  R pth = R(s.c.gamma - 1.0) * (W(w, x.e) - ke);
+  R pth = gam1_<R>(s) * (W(w, x.e) - ke);
   if (s.c.fix_small_values) {
     if (pth < R(s.c.small_pressure)) pth = R(s.c.small_pressure);
   } else if (s.c.check_small_values) {
     if (pth < R(s.c.small_pressure)) st |= ORC_ST_SMALL_VALUE;
   }
-  return R(s.c.gamma) * pth / W(w, x.rho);
+  return gam_<R>(s) * pth / W(w, x.rho);
 }
 
 // hd_get_cbounds (src/hd/mod_hd_phys.t:891-1001),
@@ -340,7 +392,6 @@ int get_cbounds(const State &s, const Arr<R> &wLC, const Arr<R> &wRC, const Arr<
   const Ix &x = s.x;
   const int mn = x.mom[idim];
   int st = 0;
-  const double gam = s.c.gamma;
   Arr<R> wmean;
   if (s.c.boundspeed == ORC_BS_CMAXMEAN) wmean = Arr<R>(s.g, x.nw);
   forbox(b, [&](int i, int j, int k) {
@@ -361,8 +412,8 @@ int get_cbounds(const State &s, const Arr<R> &wLC, const Arr<R> &wRC, const Arr<
           dmean = rsqrt_((tmp1 * (csL * csL) + tmp2 * (csR * csR)) * tmp3 +
                          half * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
         } else {
-          csL = R(gam) * W(wLp, x.e) / W(wLp, x.rho);
-          csR = R(gam) * W(wRp, x.e) / W(wRp, x.rho);
+          csL = gam_<R>(s) * W(wLp, x.e) / W(wLp, x.rho);
+          csR = gam_<R>(s) * W(wRp, x.e) / W(wRp, x.rho);
           dmean = (tmp1 * csL + tmp2 * csR) * tmp3 + R(0.5) * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv);
           dmean = rsqrt_(dmean);
         }
@@ -404,8 +455,8 @@ int get_cbounds(const State &s, const Arr<R> &wLC, const Arr<R> &wRC, const Arr<
           csR = csound_prim(s, wRp, i, j, k, idim);
           csL = rmax(csL, csR);
         } else {
-          csL = R(gam) * W(wLp, x.e) / W(wLp, x.rho);
-          csR = R(gam) * W(wRp, x.e) / W(wRp, x.rho);
+          csL = gam_<R>(s) * W(wLp, x.e) / W(wLp, x.rho);
+          csR = gam_<R>(s) * W(wRp, x.e) / W(wRp, x.rho);
           csL = rmax(rsqrt_(csL), rsqrt_(csR));
         }
         if (cmin) {
@@ -1005,7 +1056,7 @@ int getdt_block(const State &s, const Arr<R> &w, const double *dx, double *dtnew
       R cm;
       if (x.mhd) {
         R inv_rho = R(1.0) / W(wprim, x.rho);
-        R cs = R(c.gamma) * W(wprim, x.e) * inv_rho;
+        R cs = gam_<R>(s) * W(wprim, x.e) * inv_rho;
         R b2 = W(wprim, x.mag[0]) * W(wprim, x.mag[0]);
         for (int q = 1; q < x.ndir; ++q) b2 = b2 + W(wprim, x.mag[q]) * W(wprim, x.mag[q]);
         R cfast2 = b2 * inv_rho + cs;
@@ -1015,7 +1066,7 @@ int getdt_block(const State &s, const Arr<R> &w, const double *dx, double *dtnew
         cm = rsqrt_(R(half) * (cfast2 + rsqrt_(av)));
         cm = rabs(W(wprim, mn)) + cm;
       } else {
-        cm = rabs(W(wprim, mn)) + rsqrt_(R(c.gamma) * W(wprim, x.e) / W(wprim, x.rho));
+        cm = rabs(W(wprim, mn)) + rsqrt_(gam_<R>(s) * W(wprim, x.e) / W(wprim, x.rho));
       }
       cmax[g.idx(i, j, k)] = cm;
     });
@@ -1292,7 +1343,9 @@ void orc_srl_maps(int nghost, int block_nx, int *s_min, int *s_max, int *r_min, 
   }
 }
 
-static void getbc_reg(Grid &G, std::vector<double> &reg) {
+extern "C++" {
+template <class R>
+static void getbc_reg(const Grid &G, std::vector<R> &reg) {
   const State &s = G.s;
   const Geo &g = s.g;
   const int ndim = s.c.ndim, nw = s.x.nw;
@@ -1320,7 +1373,7 @@ static void getbc_reg(Grid &G, std::vector<double> &reg) {
             S.lo[d] = sminA[d][dd[d] + 1]; S.hi[d] = smaxA[d][dd[d] + 1];
             Rb.lo[d] = rminA[d][-dd[d] + 1]; Rb.hi[d] = rmaxA[d][-dd[d] + 1];
           }
-          double *src = &reg[G.bsize * ib], *dst = &reg[G.bsize * nb];
+          R *src = &reg[G.bsize * ib], *dst = &reg[G.bsize * nb];
           for (int iw = 0; iw < nw; ++iw)
             for (int k = 0; k <= S.hi[2] - S.lo[2]; ++k)
               for (int j = 0; j <= S.hi[1] - S.lo[1]; ++j)
@@ -1333,7 +1386,7 @@ static void getbc_reg(Grid &G, std::vector<double> &reg) {
   // with bc_phys cont/symm/asymm (src/mod_boundary_conditions.t:12-265)
   const int ng = s.c.nghost;
   for (int ib = 0; ib < G.nblocks; ++ib) {
-    double *w = &reg[G.bsize * ib];
+    R *w = &reg[G.bsize * ib];
     auto nbt = [&](int di, int dj, int dk) { return G.nbr[(size_t)ib * 27 + dir_index(di, dj, dk)] < 0; };
     for (int idims = 0; idims < ndim; ++idims) {
       int kmin[3] = {0, 0, 0}, kmax[3] = {0, 0, 0};
@@ -1367,7 +1420,7 @@ static void getbc_reg(Grid &G, std::vector<double> &reg) {
               // mirror: ghost ixOmin+m <- ixOmin-1-m (max side), ixOmax-m <- ixOmax+1+m (min side)
               int src = iside == 1 ? 2 * O.lo[idims] - 1 - c[idims] : 2 * O.hi[idims] + 1 - c[idims];
               q = p + (src - c[idims]) * o;
-              w[p + g.cells * (size_t)iw] = sgn * w[q + g.cells * (size_t)iw];
+              w[p + g.cells * (size_t)iw] = R(sgn) * w[q + g.cells * (size_t)iw];
             }
           });
         }
@@ -1375,6 +1428,7 @@ static void getbc_reg(Grid &G, std::vector<double> &reg) {
     }
   }
 }
+}  // extern "C++"
 
 void orc_grid_getbc(orc_grid *g) { getbc_reg(*g, g->reg[0]); }
 
@@ -1611,6 +1665,86 @@ double orc_count_flops_getdt(const orc_cfg *cfg, const double *w, const double *
   double cells = 1;
   for (int d = 0; d < cfg->ndim; ++d) cells *= cfg->block_nx[d];
   return double(g_ops) / cells;
+}
+
+
+// ---------------------------------------------------------------- forward mode
+// Reference gradient for the discrete adjoint: the run w0 -> nsteps SSP-RK3
+// steps (src/mod_advance.t:249-267, getbc after every stage) with a frozen
+// dt sequence, in dual numbers seeded with the direction (dw0, dgamma), and
+// the loss sum over interior cells of mask * rho^2.  Returns the loss and its
+// directional derivative; w_final (optional) receives the final values.
+// Not reentrant (the gamma seed is a process-wide static).
+int orc_dual_run(const orc_cfg *cfg, const int *domain_nx, const double *xprobmin, const double *xprobmax,
+                 const int *bc, const double *w0, const double *dw0, double dgamma, int nsteps,
+                 const double *dts, const double *mask, int nthreads, double *loss, double *dloss,
+                 double *w_final) {
+  orc_grid *g = orc_grid_create(cfg, domain_nx, xprobmin, xprobmax, bc);
+  const size_t n = g->bsize * g->nblocks;
+  std::vector<Dual> reg[3];
+  for (int r = 0; r < 3; ++r) reg[r].assign(n, Dual(0.0));
+  for (size_t p = 0; p < n; ++p) reg[0][p] = Dual(w0[p], dw0 ? dw0[p] : 0.0);
+  g_dual_dgamma = dgamma;
+  const State &s = g->s;
+  const size_t bs = g->bsize;
+  double b11, b22, b33, a21, a31;
+  if (s.c.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
+  else { b11 = 1.0; b22 = 1.0 / 4.0; b33 = 2.0 / 3.0; a21 = 3.0 / 4.0; a31 = 1.0 / 3.0; }
+  const double a22 = 1.0 - a21, a33 = 1.0 - a31;
+  auto advect = [&](int ra, int rb, double qdt, double dtfactor) {
+    int st = 0;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic) reduction(| : st)
+#endif
+    for (int ib = 0; ib < g->nblocks; ++ib) {
+      Arr<Dual> a(s.g, s.x.nw), b(s.g, s.x.nw);
+      std::copy(reg[ra].begin() + bs * ib, reg[ra].begin() + bs * (ib + 1), a.d.begin());
+      std::copy(reg[rb].begin() + bs * ib, reg[rb].begin() + bs * (ib + 1), b.d.begin());
+      st |= finite_volume(s, a, b, qdt, dtfactor, g->dx, 0.0);
+      std::copy(b.d.begin(), b.d.end(), reg[rb].begin() + bs * ib);
+    }
+    getbc_reg(*g, reg[rb]);
+    return st;
+  };
+  auto combine = [&](int dst, double a, int ra, double b, int rb) {
+    for (size_t p = 0; p < n; ++p) reg[dst][p] = Dual(a) * reg[ra][p] + Dual(b) * reg[rb][p];
+  };
+  int st = 0;
+  getbc_reg(*g, reg[0]);
+  for (int it = 0; it < nsteps; ++it) {
+    const double dt = dts[it];
+    reg[1] = reg[0];
+    st |= advect(0, 1, b11 * dt, b11);
+    combine(2, a21, 0, a22, 1);
+    st |= advect(1, 2, b22 * dt, b22);
+    combine(0, a31, 0, a33, 2);
+    st |= advect(2, 0, b33 * dt, b33);
+  }
+  Dual L(0.0);
+  const Geo &geo = s.g;
+  const Ix &x = s.x;
+  for (int ib = 0; ib < g->nblocks; ++ib) {
+    Arr<Dual> a(geo, x.nw);
+    std::copy(reg[0].begin() + bs * ib, reg[0].begin() + bs * (ib + 1), a.d.begin());
+    Box ixM;
+    for (int d = 0; d < 3; ++d) {
+      ixM.lo[d] = d < s.c.ndim ? s.c.nghost : 0;
+      ixM.hi[d] = d < s.c.ndim ? s.c.nghost + s.c.block_nx[d] - 1 : 0;
+    }
+    const double *mb = mask + bs / x.nw * ib;
+    forbox(ixM, [&](int i, int j, int k) {
+      const double m = mb[geo.idx(i, j, k)];
+      if (m != 0.0) L = L + Dual(m) * (W(a, x.rho) * W(a, x.rho));
+    });
+  }
+  if (w_final)
+    for (size_t p = 0; p < n; ++p) w_final[p] = reg[0][p].v;
+  *loss = L.v;
+  *dloss = L.d;
+  g_dual_dgamma = 0.0;
+  orc_grid_destroy(g);
+  return st;
 }
 
 }  // extern "C"

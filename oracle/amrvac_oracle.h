@@ -157,6 +157,17 @@ double orc_count_flops_stage(const orc_cfg *cfg, const double *wct,
 double orc_count_flops_getdt(const orc_cfg *cfg, const double *w,
                              const double *dx);
 
+/* Forward-mode (dual-number) reference gradient: from the conserved block
+ * arrays w0 (ghosted, nblocks x bsize) run nsteps SSP-RK3 steps with the dt
+ * sequence dts (frozen), seeded with the direction (dw0, dgamma); loss = sum
+ * over interior cells of mask * rho^2 (mask: nblocks x cells of a block,
+ * ghosted layout).  Returns status; loss and its directional derivative in
+ * *loss / *dloss; w_final (optional) the final conserved arrays. */
+int orc_dual_run(const orc_cfg *cfg, const int *domain_nx, const double *xprobmin,
+                 const double *xprobmax, const int *bc, const double *w0, const double *dw0,
+                 double dgamma, int nsteps, const double *dts, const double *mask, int nthreads,
+                 double *loss, double *dloss, double *w_final);
+
 #ifdef __cplusplus
 }
 #endif
