@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/amrvac_gpu.h"
+#include "adjoint.cuh"
 #include "aux.cuh"
 #include "kernels.cuh"
 
@@ -82,6 +83,9 @@ struct amrvac_ctx {
   int64_t graph_nodes = 0;
   int zchunk = 0;          // 0: persistent plane ranges; 16/8/4: one z-chunk per CTA
   int wave_ctas = 1;       // resident stage CTAs on the device (one wave)
+  std::vector<double> h_dx;            // [nblocks][3] cell sizes (host copy)
+  double *d_adj[3] = {nullptr, nullptr, nullptr};  // adjoint work registers (lazily)
+  bool adj_prepared = false;
 };
 
 namespace {
@@ -367,6 +371,7 @@ int amrvac_gpu_destroy(amrvac_ctx *c) {
   cudaFree(c->d_red);
   cudaFree(c->d_status);
   cudaFree(c->d_block_status);
+  for (int r = 0; r < 3; ++r) cudaFree(c->d_adj[r]);
   cudaFree(c->d_stage);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -439,6 +444,8 @@ int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const in
   CK(cudaMemcpyAsync(c->d_dx, dxb.data(), sizeof(double) * dxb.size(), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * nblocks, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  c->h_dx = dxb;
+  for (int r = 0; r < 3; ++r) { cudaFree(c->d_adj[r]); c->d_adj[r] = nullptr; }
   return 0;
 }
 
@@ -840,6 +847,90 @@ int amrvac_gpu_get_cbounds_points(amrvac_ctx *c, int n, const double *wlc, const
   if (!c) return fail(AMRVAC_E_ARG, "null context");
   if (idim < 1 || idim > c->cfg.ndir) return fail(AMRVAC_E_ARG, "idim out of range");
   return run_points(c, n, idim, wlc, wrc, wlp, wrp, cmax, 1, cmin, 0.0, 2);
+}
+
+
+// ---------------------------------------------------------------- adjoint
+int amrvac_gpu_step_dt(amrvac_ctx *c, double dt) {
+  if (int r = check_ctx(c, true)) return r;
+  if (!(dt > 0.0)) return fail(AMRVAC_E_ARG, "dt must be positive");
+  CK(launch_set_scalar(c->d_scal + 0, dt, c->stream));
+  ++c->launches;
+  return launch_rk(c);
+}
+
+int amrvac_gpu_register_copy(amrvac_ctx *c, int reg, double *dev, int to_register) {
+  if (int r = check_ctx(c, true)) return r;
+  if (reg < 0 || reg > 2 || !dev) return fail(AMRVAC_E_ARG, "bad register copy");
+  const size_t bytes = sizeof(double) * c->per_block * c->nw * c->nblocks;
+  CK(cudaMemcpyAsync(to_register ? c->pool[reg] : dev, to_register ? dev : c->pool[reg], bytes,
+                     cudaMemcpyDeviceToDevice, c->stream));
+  return 0;
+}
+
+int amrvac_gpu_adjoint_step(amrvac_ctx *c, double *lam, double dt, double *gamma_part) {
+  if (int r = check_ctx(c, true)) return r;
+  const amrvac_cfg &k = c->cfg;
+  if (!lam || !gamma_part || !(dt > 0.0)) return fail(AMRVAC_E_ARG, "bad adjoint arguments");
+  if (k.physics != 0 || k.ndim != 2 || k.flux_scheme != AMRVAC_FS_HLL || k.typeboundspeed != AMRVAC_BS_EINFELDT ||
+      (k.limiter != AMRVAC_LIM_MINMOD && k.limiter != AMRVAC_LIM_VANLEER) || k.fix_small_values || k.precision != 0)
+    return fail(AMRVAC_E_UNSUPPORTED,
+                "adjoint: 2-D hd, hll, minmod or vanleer, Einfeldt, FP64, no fix_small_values");
+  if (k.time_stepper != AMRVAC_TS_THREESTEP && k.time_stepper != AMRVAC_TS_TWOSTEP)
+    return fail(AMRVAC_E_UNSUPPORTED, "adjoint: threestep or twostep");
+  for (int sd = 0; sd < 4; ++sd)
+    if (c->bc.kind[sd] == BCK_MIRROR) return fail(AMRVAC_E_UNSUPPORTED, "adjoint: periodic or cont boundaries");
+  for (int b = 1; b < c->nblocks; ++b)
+    for (int d = 0; d < 2; ++d)
+      if (c->h_dx[(size_t)b * 3 + d] != c->h_dx[d]) return fail(AMRVAC_E_UNSUPPORTED, "adjoint: uniform dx");
+  if (!c->adj_prepared) {
+    CK(adjoint_prepare());
+    c->adj_prepared = true;
+  }
+  const size_t bytes = sizeof(double) * c->per_block * c->nw * c->nblocks;
+  for (int r = 0; r < 3; ++r)
+    if (!c->d_adj[r]) CK(cudaMalloc(&c->d_adj[r], bytes));
+  double *S1 = c->d_adj[0], *S2 = c->d_adj[1], *S3 = c->d_adj[2];
+  auto args = [&](int reg_w, const double *lam_new, double *out, const double *acc, double *base, int binit,
+                  double a, double b, double dtf) {
+    AdjArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.sa = stage_args(c, reg_w, reg_w, reg_w, 0.0, 1.0, 1.0);
+    A.lam = lam_new;
+    A.lam_out = out;
+    A.acc_in = acc;
+    A.base = base;
+    A.base_init = binit;
+    A.a = a;
+    A.b = b;
+    for (int d = 0; d < 2; ++d) A.s[d] = dtf * dt / c->h_dx[d];
+    A.gamma_part = gamma_part;
+    return A;
+  };
+  CK(launch_set_scalar(c->d_scal + 0, dt, c->stream));
+  ++c->launches;
+  if (k.time_stepper == AMRVAC_TS_TWOSTEP) {
+    // forward U1 = U0 + dt L(U0); U2 = (U0 + U1 + dt L(U1)) / 2
+    if (int r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0)) return r;
+    CK(launch_adjoint_stage(args(1, lam, S1, nullptr, S2, 1, 0.5, 0.5, 0.5), k.limiter, c->stream));
+    CK(launch_adjoint_stage(args(0, S1, lam, S2, nullptr, 0, 0.0, 1.0, 1.0), k.limiter, c->stream));
+    c->launches += 3;
+    return 0;
+  }
+  double b11, b22, b33, a21, a31;
+  if (k.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
+  else { b11 = 1.0; b22 = 1.0 / 4.0; b33 = 2.0 / 3.0; a21 = 3.0 / 4.0; a31 = 1.0 / 3.0; }
+  // recompute the stage inputs U1 (register 1) and U2 (register 2) from U^n (register 0)
+  if (int r = launch_stage(c, 0, 1, 0, 0.0, 1.0, b11)) return r;
+  if (int r = launch_stage(c, 1, 2, 0, a21, 1.0 - a21, b22)) return r;
+  // stage 3: U3 = a31 U0 + (1-a31) U2 + b33 dt L(U2)
+  CK(launch_adjoint_stage(args(2, lam, S1, nullptr, S2, 1, a31, 1.0 - a31, b33), k.limiter, c->stream));
+  // stage 2: U2 = a21 U0 + (1-a21) U1 + b22 dt L(U1)
+  CK(launch_adjoint_stage(args(1, S1, S3, nullptr, S2, 0, a21, 1.0 - a21, b22), k.limiter, c->stream));
+  // stage 1: U1 = U0 + b11 dt L(U0); dL/dU0 = base sum + stage-1 transpose
+  CK(launch_adjoint_stage(args(0, S3, lam, S2, nullptr, 0, 0.0, 1.0, b11), k.limiter, c->stream));
+  c->launches += 3;
+  return 0;
 }
 
 }  // extern "C"

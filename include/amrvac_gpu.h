@@ -229,6 +229,22 @@ int amrvac_gpu_riemann_points(amrvac_ctx *ctx, int n, const double *wlp, const d
 int amrvac_gpu_getdt_noalloc(const amrvac_cfg *cfg, const double *w_dev, int nblocks, const double *dx,
                              void *stream, double *dt, double *cmax_global);
 
+/* ---- Discrete adjoint (no counterpart in the reference) -------------------
+ * One step with a given dt (the configured RK stages, no setdt): the forward
+ * map of the adjoint, whose dt sequence is frozen. */
+int amrvac_gpu_step_dt(amrvac_ctx *ctx, double dt);
+/* Copy a whole register to (to_register = 0) or from (1) the caller's device
+ * buffer dev (register layout [block][var][y][x], 16^ndim per block). */
+int amrvac_gpu_register_copy(amrvac_ctx *ctx, int reg, double *dev, int to_register);
+/* Adjoint of one step U^n -> U^{n+1} at frozen dt, with U^n in register 0:
+ * lam (device, register layout) holds dL/dU^{n+1} on entry and dL/dU^n on
+ * return; gamma_part (device, [nblocks]) accumulates dL/dgamma of the step
+ * per block (sum it for the total).  Recomputes the stage inputs in
+ * registers 1 and 2.  2-D hydrodynamics, HLL with minmod or vanleer,
+ * Einfeldt bounds, FP64, periodic or cont boundaries, uniform dx, threestep
+ * or twostep.  Asynchronous on the context stream. */
+int amrvac_gpu_adjoint_step(amrvac_ctx *ctx, double *lam, double dt, double *gamma_part);
+
 /* ---- Batched ensembles (no counterpart in the reference) ------------------
  * Many independent hydrodynamics runs advanced together: 1-D and 2-D
  * instances of uneven sizes, each a uniform level-1 grid of 16^d blocks with
