@@ -93,21 +93,28 @@ class FrozenDtSolver:
         gpart = torch.zeros(self.ctx.nblocks, dtype=torch.float64, device=lam.device)
         N = len(dts)
         starts = sorted(ckpt)
+        nst = 3 if self.cfg.time_stepper == _lib.TIME_STEPPER["threestep"] else 2
+        h = self.ctx.h
+        seg = None
         for s0 in reversed(starts):
             s1 = min(s0 + checkpoint_every, N)
-            # recompute U^{s0..s1-1} from the checkpoint
-            states = [ckpt[s0]]
+            if seg is None:  # stage inputs of one segment: [step][stage] (reused)
+                seg = torch.empty((checkpoint_every, nst) + self.shape, dtype=torch.float64, device=lam.device)
+            # recompute the segment from its checkpoint, keeping every stage input:
+            # U^n before the step, U1 and U2 left in registers 1 and 2 by it
             self._load(ckpt[s0])
-            for n in range(s0, s1 - 1):
-                _lib.check(self.L.amrvac_gpu_step_dt(self.ctx.h, float(dts[n])), "step_dt")
-                u = torch.empty(self.shape, dtype=torch.float64, device=lam.device)
-                self._store(u)
-                states.append(u)
+            for n in range(s0, s1):
+                q = n - s0
+                _lib.check(self.L.amrvac_gpu_register_copy(h, 0, _ptr(seg[q, 0]), 0), "register_copy")
+                _lib.check(self.L.amrvac_gpu_step_dt(h, float(dts[n])), "step_dt")
+                for st in range(1, nst):
+                    _lib.check(self.L.amrvac_gpu_register_copy(h, st, _ptr(seg[q, st]), 0), "register_copy")
             for n in range(s1 - 1, s0 - 1, -1):
-                self._load(states[n - s0])
-                _lib.check(self.L.amrvac_gpu_adjoint_step(self.ctx.h, _ptr(lam), float(dts[n]), _ptr(gpart)),
-                           "adjoint_step")
-            self.ctx.synchronize()
+                q = n - s0
+                u2 = _ptr(seg[q, 2]) if nst == 3 else None
+                _lib.check(self.L.amrvac_gpu_adjoint_step_states(h, _ptr(seg[q, 0]), _ptr(seg[q, 1]), u2, _ptr(lam),
+                                                                 float(dts[n]), _ptr(gpart)), "adjoint_step_states")
+        self.ctx.synchronize()
         return lam, gpart.sum()
 
 
@@ -123,9 +130,12 @@ class _Solve:
 
             class Solve(torch.autograd.Function):
                 @staticmethod
-                def forward(ctx, U0, gamma, dts, grid, checkpoint_every, cfg_kw):
+                def forward(ctx, U0, gamma, dts, grid, checkpoint_every, cfg_kw, grad_on):
                     solver = FrozenDtSolver(*grid, float(gamma), **cfg_kw)
                     UN, ckpt = solver.forward(U0.detach(), dts, checkpoint_every)
+                    if not (grad_on and any(ctx.needs_input_grad[:2])):
+                        solver.close()  # no backward will come: release the context now
+                        return UN
                     ctx.solver = solver
                     ctx.ckpt = ckpt
                     ctx.dts = dts
@@ -137,7 +147,7 @@ class _Solve:
                     lam0, gg = ctx.solver.backward(gUN.detach(), ctx.dts, ctx.ckpt, ctx.k)
                     ctx.solver.close()
                     ctx.ckpt = None
-                    return lam0, gg.reshape(()), None, None, None, None
+                    return lam0, gg.reshape(()), None, None, None, None, None
 
             cls.fn = Solve
         return cls.fn
@@ -146,8 +156,10 @@ class _Solve:
 def solve(U0, gamma, dts, domain_nx, xprobmin, xprobmax, checkpoint_every=20, **cfg_kw):
     """U_N from U0 after len(dts) steps at the frozen dts; differentiable in U0
     and gamma (a 0-d float64 tensor)."""
+    import torch
     grid = (tuple(domain_nx), tuple(xprobmin), tuple(xprobmax))
-    return _Solve.get().apply(U0, gamma, np.asarray(dts, np.float64), grid, int(checkpoint_every), cfg_kw)
+    return _Solve.get().apply(U0, gamma, np.asarray(dts, np.float64), grid, int(checkpoint_every), cfg_kw,
+                              torch.is_grad_enabled())
 
 
 def domain_to_blocks(u, bn=16):

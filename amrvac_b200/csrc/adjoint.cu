@@ -32,6 +32,9 @@ namespace amrvac {
 namespace {
 
 constexpr int ADJ_THREADS = 320;
+#ifndef AMRVAC_ADJ_MINB
+#define AMRVAC_ADJ_MINB 2
+#endif
 constexpr int WP = 22;            // primitive tile edge: 16 + 2*3
 constexpr int LMW = 20;           // lambda tile edge: 16 + 2*2
 constexpr int NF = 19;            // faces -1..17 per row and direction
@@ -189,7 +192,7 @@ __device__ __forceinline__ double face_vjp(const double *wp, int D, int fi, int 
 }
 
 template <int LIM>
-__global__ void __launch_bounds__(ADJ_THREADS, 1) adj_stage_kernel(const AdjArgs A) {
+__global__ void __launch_bounds__(ADJ_THREADS, AMRVAC_ADJ_MINB) adj_stage_kernel(const AdjArgs A) {
   extern __shared__ __align__(16) double adj_sm[];
   double *wp = adj_sm;
   double *lm = wp + SM_WP;

@@ -868,7 +868,22 @@ int amrvac_gpu_register_copy(amrvac_ctx *c, int reg, double *dev, int to_registe
   return 0;
 }
 
+static int adjoint_step_impl(amrvac_ctx *c, const double *u0, const double *u1, const double *u2, double *lam,
+                             double dt, double *gamma_part);
+
 int amrvac_gpu_adjoint_step(amrvac_ctx *c, double *lam, double dt, double *gamma_part) {
+  return adjoint_step_impl(c, nullptr, nullptr, nullptr, lam, dt, gamma_part);
+}
+
+int amrvac_gpu_adjoint_step_states(amrvac_ctx *c, const double *u0, const double *u1, const double *u2, double *lam,
+                                   double dt, double *gamma_part) {
+  if (!u0 || !u1 || (!u2 && c && c->cfg.time_stepper == AMRVAC_TS_THREESTEP))
+    return fail(AMRVAC_E_ARG, "adjoint_step_states: null stage state");
+  return adjoint_step_impl(c, u0, u1, u2, lam, dt, gamma_part);
+}
+
+static int adjoint_step_impl(amrvac_ctx *c, const double *u0, const double *u1, const double *u2, double *lam,
+                             double dt, double *gamma_part) {
   if (int r = check_ctx(c, true)) return r;
   const amrvac_cfg &k = c->cfg;
   if (!lam || !gamma_part || !(dt > 0.0)) return fail(AMRVAC_E_ARG, "bad adjoint arguments");
@@ -891,11 +906,14 @@ int amrvac_gpu_adjoint_step(amrvac_ctx *c, double *lam, double dt, double *gamma
   for (int r = 0; r < 3; ++r)
     if (!c->d_adj[r]) CK(cudaMalloc(&c->d_adj[r], bytes));
   double *S1 = c->d_adj[0], *S2 = c->d_adj[1], *S3 = c->d_adj[2];
+  // stage inputs: the caller's buffers, or registers 0..2 recomputed below
+  const double *W[3] = {u0 ? u0 : c->pool[0], u1 ? u1 : c->pool[1], u2 ? u2 : c->pool[2]};
   auto args = [&](int reg_w, const double *lam_new, double *out, const double *acc, double *base, int binit,
                   double a, double b, double dtf) {
     AdjArgs A;
     std::memset(&A, 0, sizeof(A));
     A.sa = stage_args(c, reg_w, reg_w, reg_w, 0.0, 1.0, 1.0);
+    A.sa.uin = W[reg_w];
     A.lam = lam_new;
     A.lam_out = out;
     A.acc_in = acc;
@@ -911,7 +929,8 @@ int amrvac_gpu_adjoint_step(amrvac_ctx *c, double *lam, double dt, double *gamma
   ++c->launches;
   if (k.time_stepper == AMRVAC_TS_TWOSTEP) {
     // forward U1 = U0 + dt L(U0); U2 = (U0 + U1 + dt L(U1)) / 2
-    if (int r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0)) return r;
+    if (!u0)
+      if (int r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0)) return r;
     CK(launch_adjoint_stage(args(1, lam, S1, nullptr, S2, 1, 0.5, 0.5, 0.5), k.limiter, c->stream));
     CK(launch_adjoint_stage(args(0, S1, lam, S2, nullptr, 0, 0.0, 1.0, 1.0), k.limiter, c->stream));
     c->launches += 3;
@@ -921,8 +940,10 @@ int amrvac_gpu_adjoint_step(amrvac_ctx *c, double *lam, double dt, double *gamma
   if (k.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
   else { b11 = 1.0; b22 = 1.0 / 4.0; b33 = 2.0 / 3.0; a21 = 3.0 / 4.0; a31 = 1.0 / 3.0; }
   // recompute the stage inputs U1 (register 1) and U2 (register 2) from U^n (register 0)
-  if (int r = launch_stage(c, 0, 1, 0, 0.0, 1.0, b11)) return r;
-  if (int r = launch_stage(c, 1, 2, 0, a21, 1.0 - a21, b22)) return r;
+  if (!u0) {
+    if (int r = launch_stage(c, 0, 1, 0, 0.0, 1.0, b11)) return r;
+    if (int r = launch_stage(c, 1, 2, 0, a21, 1.0 - a21, b22)) return r;
+  }
   // stage 3: U3 = a31 U0 + (1-a31) U2 + b33 dt L(U2)
   CK(launch_adjoint_stage(args(2, lam, S1, nullptr, S2, 1, a31, 1.0 - a31, b33), k.limiter, c->stream));
   // stage 2: U2 = a21 U0 + (1-a21) U1 + b22 dt L(U1)

@@ -45,6 +45,12 @@ WORKLOADS = {
                         "256 2-D of 32^2-512^2 in 16^2 blocks), HLL/HLLC x minmod/vanleer per instance, SSP-RK3 "
                         "to t=0.2 with per-instance CFL dt (0.8), cont boundaries, one persistent launch per stage",
                    physics="hd", ensemble=512),
+    "blast512adj": dict(desc="Adjoint of the 2D Euler blast wave: 512^2 as 32x32 blocks of 16^2, gamma=1.4, "
+                             "rho = 1 + 0.1 G (Gaussian random field, correlation length 0.05), p = 0.1 with "
+                             "p = 10 for r < 0.1, v = 0, cont boundaries; HLL, minmod, SSP-RK3, 200 steps at the "
+                             "CFL (0.8) dt sequence of the forward run; loss = sum rho^2 on 0.25 < r < 0.35; "
+                             "gradient w.r.t. the initial rho field and gamma, checkpoint every 20 steps",
+                        physics="hd", adjoint=dict(n=512, steps=200, every=20)),
 }
 
 # Signal-speed estimate of the ensemble workload (typeboundspeed).  With the
@@ -225,6 +231,24 @@ def run_reference(args, ws, rank):
         def sample_fn():  # a few seconds of whole instances per step
             v, _, smp = _ens_cpu_sample(specs, init, budget_s=3.0)
             return v, smp
+    elif "adjoint" in WORKLOADS[args.workload]:
+        from tests import _blast as B
+        import oracle as O
+        O.build()
+        n = WORKLOADS[args.workload]["adjoint"]["n"]
+        c = O.make_cfg(physics="hd", ndim=2, gamma=B.GAMMA, flux_scheme="hll", limiter="minmod", courantpar=0.8)
+        w0 = B.to_cons_blocks(B.blast_prim(n))
+
+        def sample_fn():  # the oracle's forward run of the blast, 10 steps (the reference has no adjoint)
+            g = O.Grid(c, [n, n], [0.0, 0.0], [1.0, 1.0], ["cont"] * 4)
+            for ib in range(g.nblocks):
+                g.set_block(ib, w0[ib])
+            g.getbc()
+            t0 = time.perf_counter()
+            for _ in range(10):
+                dt, _ = g.getdt()
+                g.advance(dt, 0.0, nthreads)
+            return n * n * 10 / (time.perf_counter() - t0), f"10 SSP-RK3 steps of the {n}^2 blast (forward only)"
     else:
         def sample_fn():
             return cpu_baseline_sample(args.workload, nthreads, 1)
@@ -426,6 +450,155 @@ def run_ensemble(args, ws, rank, local):
         }))
 
 
+def run_adjoint(args, ws, rank, local):
+    """Adjoint workload: a step is one gradient evaluation (forward run of all
+    steps + the checkpointed adjoint sweep)."""
+    import torch
+    from tests import _blast as B
+    from amrvac_b200.adjoint import FrozenDtSolver, blocks_to_domain, domain_to_blocks, solve
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    w = WORKLOADS[args.workload]
+    n, nsteps, every = w["adjoint"]["n"], w["adjoint"]["steps"], w["adjoint"]["every"]
+    dev = "cuda"
+    prim = B.blast_prim(n)
+    rho0 = torch.tensor(prim[0, 0], dtype=torch.float64, device=dev)
+    p0 = torch.tensor(prim[3, 0], dtype=torch.float64, device=dev)
+    mask = torch.tensor(B.loss_mask(n), dtype=torch.float64, device=dev)
+    grid = ((n, n), (0.0, 0.0), (1.0, 1.0))
+    kw = dict(limiter="minmod", typeboundary=["cont"] * 4)
+    G = lambda x: torch.tensor(x, dtype=torch.float64, device=dev)  # noqa: E731
+
+    def U0_of(r, g):
+        z = torch.zeros_like(r)
+        return domain_to_blocks(torch.stack([r, z, z, p0 / (g - 1.0)]))
+
+    solver = FrozenDtSolver(*grid, B.GAMMA, **kw)
+    dts = solver.cfl_dts(U0_of(rho0, G(B.GAMMA)), nsteps)
+
+    def loss(r, g):
+        UN = solve(U0_of(r, g), g, dts, *grid, checkpoint_every=every, **kw)
+        rho = blocks_to_domain(UN, n, n)[0]
+        return (mask * rho * rho).sum()
+
+    # ---- timing: forward sweep and adjoint sweep, CUDA events on the library stream
+    s = torch.cuda.ExternalStream(solver.ctx.stream_ptr())
+    U0 = U0_of(rho0, G(B.GAMMA)).contiguous()
+    lamN = torch.zeros(solver.shape, dtype=torch.float64, device=dev)
+    lamN[:, 0] = 1.0
+    for _ in range(args.warmup):
+        UN, ck = solver.forward(U0, dts, every)
+        solver.backward(lamN, dts, ck, every)
+    fwd, bwd = [], []
+    l0 = solver.ctx.launch_count()
+    clk = ClockSampler(local)
+    clk.__enter__()
+    for _ in range(args.steps):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record(s)
+        UN, ck = solver.forward(U0, dts, every)
+        e1.record(s)
+        solver.backward(lamN, dts, ck, every)
+        e2.record(s)
+        e2.synchronize()
+        fwd.append(e0.elapsed_time(e1))
+        bwd.append(e1.elapsed_time(e2))
+    clk.__exit__()
+    launches = solver.ctx.launch_count() - l0
+    tf, tb = float(np.mean(fwd)), float(np.mean(bwd))
+    cells = n * n
+    # ---- the gradient through the autograd API, and its checks
+    r = rho0.clone().requires_grad_(True)
+    g = G(B.GAMMA).requires_grad_(True)
+    L = loss(r, g)
+    L.backward()
+    grad_r, grad_g = r.grad.detach(), float(g.grad)
+    rng = np.random.default_rng(B.SEED)
+    fd_err = {1e-7: [], 1e-8: []}
+    with torch.no_grad():
+        for _ in range(args.grad_checks):
+            d = G(rng.standard_normal((n, n)))
+            ad = float((grad_r * d).sum())
+            for eps in fd_err:
+                fd = (float(loss(rho0 + eps * d, G(B.GAMMA))) - float(loss(rho0 - eps * d, G(B.GAMMA)))) / (2 * eps)
+                fd_err[eps].append(abs(fd - ad) / max(abs(ad), 1e-300))
+        epg = 1e-7
+        fdg = (float(loss(rho0, G(B.GAMMA + epg))) - float(loss(rho0, G(B.GAMMA - epg)))) / (2 * epg)
+    # ---- e2e: pinned host rho0 in, gradient out, through the autograd API
+    pin = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    pin.copy_(torch.from_numpy(prim[0, 0]))
+    gout = torch.empty((n, n), dtype=torch.float64).pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    r2 = pin.to(dev, non_blocking=True).requires_grad_(True)
+    g2 = G(B.GAMMA).requires_grad_(True)
+    loss(r2, g2).backward()
+    gout.copy_(r2.grad, non_blocking=True)
+    gg2 = g2.grad.to("cpu")
+    e1.record()
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    # ---- dual-number oracle reference on the host cores (one density direction and gamma)
+    dual = None
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracle as O
+        O.build()
+        c = O.make_cfg(physics="hd", ndim=2, gamma=B.GAMMA, flux_scheme="hll", limiter="minmod", courantpar=0.8)
+        w0 = B.to_cons_blocks(prim)
+        mb = B.mask_blocks(n)
+        drho = np.random.default_rng(5).standard_normal((n, n))
+        nth = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        Lr, dr, _ = O.dual_run(c, [n, n], [0.0, 0.0], [1.0, 1.0], ["cont"] * 4, w0,
+                               B.cons_direction(prim, drho, 0.0), 0.0, dts, mb, nth)
+        t_dual = time.perf_counter() - t0
+        _, dgr, _ = O.dual_run(c, [n, n], [0.0, 0.0], [1.0, 1.0], ["cont"] * 4, w0,
+                               B.cons_direction(prim, np.zeros((n, n)), 1.0), 1.0, dts, mb, nth)
+        ad = float((grad_r.cpu().numpy() * drho).sum())
+        dual = {"loss_rel_diff": abs(float(L.detach()) - Lr) / abs(Lr),
+                "rho_direction_rel_err": abs(ad - dr) / abs(dr), "gamma_rel_err": abs(grad_g - dgr) / abs(dgr),
+                "dual_run_s": t_dual, "cores": nth,
+                "zone_updates_per_s_dual_cpu": cells * nsteps / t_dual}
+    solver.close()
+    peaks, peak_kind = _measured_peaks()
+    if rank == 0:
+        zu = cells * nsteps
+        print(json.dumps({
+            "metric": METRIC, "value": zu / ((tf + tb) * 1e-3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tf + tb, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["desc"], "step": "one gradient: forward run of 200 steps + adjoint sweep",
+                       "cells": cells, "blocks": solver.ctx.nblocks, "time_steps": nsteps,
+                       "checkpoint_every": every, "l2": "no flush: 3 registers + checkpoints (%.0f MB) > 126 MB L2"
+                       % ((3 + nsteps / every) * cells * 4 * 8 / 1e6)},
+            "adjoint": {"forward_ms": tf, "backward_ms": tb, "adjoint_cost_vs_forward": tb / tf,
+                        "forward_zone_updates_per_s": zu / (tf * 1e-3),
+                        "what": "backward = segment recomputation from checkpoints + per step two recomputed "
+                                "stages + three adjoint stages",
+                        "loss": float(L.detach()), "dL_dgamma": grad_g,
+                        "fd_check": {"directions": args.grad_checks,
+                                     "rel_err_by_eps": {str(e): {"median": float(np.median(v)), "max": float(np.max(v))}
+                                                        for e, v in fd_err.items() if v},
+                                     "gamma_eps": 1e-7, "gamma_rel_err": abs(fdg - grad_g) / abs(grad_g),
+                                     "note": "central differences of the FP64 forward at frozen dt: a larger step "
+                                             "crosses limiter kinks, a smaller one meets the roundoff of a loss of "
+                                             "~5e4; the exact check is dual_oracle_check"},
+                        "dual_oracle_check": dual},
+            "roofline": None,
+            "e2e": {"value": zu / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": float(pin.nbytes),
+                    "d2h_bytes_per_step": float(gout.nbytes + 8),
+                    "what": "torch autograd through the C-ABI: rho0 from pinned host, forward, loss, backward, "
+                            "dL/drho0 and dL/dgamma to host"},
+            "cpu_baseline": None if dual is None else {
+                "value": dual["zone_updates_per_s_dual_cpu"], "unit": UNIT, "cores": dual["cores"], "kind": "port",
+                "sample": "one forward-mode (dual-number) run of the oracle over all 200 steps"},
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+        }))
+
+
 def run_ours(args, ws, rank, local):
     import torch
     if not torch.cuda.is_available():
@@ -569,6 +742,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ot128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grad-checks", type=int, default=64,
+                    help="adjoint workload: seeded directions of the central-difference check")
     ap.add_argument("--it-max", type=int, default=None,
                     help="ensemble workloads: stop every instance after this many steps (the reference's it_max)")
     args = ap.parse_args()
@@ -579,6 +754,8 @@ def main():
             run_reference(args, ws, rank)
         elif "ensemble" in WORKLOADS[args.workload]:
             run_ensemble(args, ws, rank, local)
+        elif "adjoint" in WORKLOADS[args.workload]:
+            run_adjoint(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

@@ -244,6 +244,12 @@ int amrvac_gpu_register_copy(amrvac_ctx *ctx, int reg, double *dev, int to_regis
  * Einfeldt bounds, FP64, periodic or cont boundaries, uniform dx, threestep
  * or twostep.  Asynchronous on the context stream. */
 int amrvac_gpu_adjoint_step(amrvac_ctx *ctx, double *lam, double dt, double *gamma_part);
+/* The same with the step's stage inputs supplied by the caller (device,
+ * register layout): u0 = U^n, u1 and u2 the inputs of stages 2 and 3 (the
+ * contents of registers 1 and 2 after amrvac_gpu_step_dt from U^n; u2 unused
+ * for twostep).  No stage is recomputed and the registers are not touched. */
+int amrvac_gpu_adjoint_step_states(amrvac_ctx *ctx, const double *u0, const double *u1, const double *u2,
+                                   double *lam, double dt, double *gamma_part);
 
 /* ---- Batched ensembles (no counterpart in the reference) ------------------
  * Many independent hydrodynamics runs advanced together: 1-D and 2-D

@@ -159,3 +159,37 @@ def test_checkpoint_interval_does_not_change_the_gradient():
         grads.append((r.grad.clone(), float(g.grad)))
     for gr, gg in grads[1:]:
         assert torch.equal(gr, grads[0][0]) and gg == grads[0][1]
+
+
+def test_recomputing_and_supplied_stage_states_agree():
+    """amrvac_gpu_adjoint_step (recomputes the stages) and
+    amrvac_gpu_adjoint_step_states (caller's stage inputs): bit-identical."""
+    _cuda()
+    import ctypes
+    import torch
+    from amrvac_b200 import _lib
+    from amrvac_b200.adjoint import FrozenDtSolver, domain_to_blocks
+    from tests import _problems as P
+    n = 32
+    cons = P.prim_to_cons(P.random_smooth("hd", 2, 2, n, seed=4), "hd", 2, B.GAMMA)[:, 0]
+    U0 = domain_to_blocks(torch.tensor(cons, dtype=torch.float64, device="cuda")).contiguous()
+    s = FrozenDtSolver((n, n), (0.0, 0.0), (1.0, 1.0), B.GAMMA, limiter="vanleer", typeboundary=["cont"] * 4)
+    dt = float(s.cfl_dts(U0, 1)[0])
+    lam0 = torch.tensor(np.random.default_rng(2).standard_normal(s.shape), dtype=torch.float64, device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    la, ga = lam0.clone(), torch.zeros(s.ctx.nblocks, dtype=torch.float64, device="cuda")
+    s._load(U0)
+    _lib.check(s.L.amrvac_gpu_adjoint_step(s.ctx.h, p(la), dt, p(ga)), "adjoint_step")
+    s.ctx.synchronize()
+    st = [torch.empty(s.shape, dtype=torch.float64, device="cuda") for _ in range(3)]
+    s._load(U0)
+    s._store(st[0], 0)
+    _lib.check(s.L.amrvac_gpu_step_dt(s.ctx.h, dt), "step_dt")
+    s._store(st[1], 1)
+    s._store(st[2], 2)
+    lb, gb = lam0.clone(), torch.zeros(s.ctx.nblocks, dtype=torch.float64, device="cuda")
+    _lib.check(s.L.amrvac_gpu_adjoint_step_states(s.ctx.h, p(st[0]), p(st[1]), p(st[2]), p(lb), dt, p(gb)),
+               "adjoint_step_states")
+    s.ctx.synchronize()
+    s.close()
+    assert torch.equal(la, lb) and torch.equal(ga, gb)
