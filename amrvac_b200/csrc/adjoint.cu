@@ -1,5 +1,5 @@
-// Discrete adjoint of the fused finite-volume stage: 2-D hydrodynamics, HLL
-// Riemann solver (src/mod_finite_volume.t:381-437), minmod or vanleer
+// Discrete adjoint of the fused finite-volume stage: 2-D hydrodynamics, HLL or
+// HLLC Riemann solver (src/mod_finite_volume.t:381-504), minmod or vanleer
 // reconstruction (src/limiter/mod_limiter.t:173-209, reconstruct_LR
 // 1110-1228), Einfeldt signal speeds (src/hd/mod_hd_phys.t:911-932), for a
 // frozen time step.  There is no adjoint in the reference; this is the exact
@@ -7,7 +7,8 @@
 //
 // Per face the forward values are replayed from the staged primitives with
 // the forward's own device functions (so the limiter and upwind branches are
-// the forward's), then the derivatives run backwards: HLL -> Einfeldt bounds
+// the forward's), then the derivatives run backwards: HLL or HLLC (the
+// forward's region, patchf) -> Einfeldt bounds
 // -> physical fluxes -> primitive-to-conserved of the face states ->
 // reconstruction -> the four stencil cells.  Ties of max/min follow the
 // branch the forward value takes (vanleer's max(a*b, 0) takes the product
@@ -71,12 +72,150 @@ __device__ __forceinline__ void slope_partials(double a, double b, double &da, d
   }
 }
 
+// Reverse of the HLL flux (src/mod_finite_volume.t:381-437) for one face.
+__device__ __forceinline__ void hll_reverse(const double *cL, const double *cR, const double *fL, const double *fR,
+                                            double cmin, double cmax, const double *mu, double *fLb, double *fRb,
+                                            double *cLb, double *cRb, double &cmaxb, double &cminb,
+                                            bool ieee_div) {
+  if (cmin >= 0.0) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) fLb[v] = mu[v];
+    return;
+  }
+  if (cmax <= 0.0) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) fRb[v] = mu[v];
+    return;
+  }
+  const double iD = 1.0 / (cmax - cmin);
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const double dW = cR[v] - cL[v];
+    const double N = cmax * fL[v] - cmin * fR[v] + cmin * cmax * dW;
+    const double F = ieee_div ? N / (cmax - cmin) : div_(N, cmax - cmin);
+    fLb[v] = mu[v] * cmax * iD;
+    fRb[v] = -mu[v] * cmin * iD;
+    cRb[v] = mu[v] * cmin * cmax * iD;
+    cLb[v] = -cRb[v];
+    cmaxb += mu[v] * (fL[v] + cmin * dW - F) * iD;
+    cminb += mu[v] * (-fR[v] + cmax * dW + F) * iD;
+  }
+}
+
+// Reverse of the HD HLLC flux (get_Riemann_flux_hllc, src/mod_finite_volume.t:
+// 439-504, with hd_get_lCD / hd_get_wCD, src/hd/mod_hd_hllc.t:56-257): the
+// region (patchf) of the forward, then the star state of the upwind side.
+// Rotated variables: 0 rho, 1 normal momentum, 2 tangential momentum, 3 e.
+__device__ __forceinline__ void hllc_reverse(const double *cL, const double *cR, const double *fL, const double *fR,
+                                             double cmin, double cmax, const double *mu, double *fLb, double *fRb,
+                                             double *cLb, double *cRb, double &cmaxb, double &cminb) {
+  if (cmin >= 0.0 || cmax <= 0.0) {
+    hll_reverse(cL, cR, fL, fR, cmin, cmax, mu, fLb, fRb, cLb, cRb, cmaxb, cminb, true);
+    return;
+  }
+  const double Dn = cmax - cmin;
+  double whll[2];
+#pragma unroll
+  for (int v = 0; v < 2; ++v) whll[v] = (cmax * cR[v] - cmin * cL[v] + fL[v] - fR[v]) / Dn;
+  double lam = whll[1] / whll[0];
+  int patchf = 1;
+  bool cond = true;
+  if (cmin < 0.0 && lam > 0.0 && lam < cmax) patchf = -1;
+  else if (cmax > 0.0 && lam < 0.0 && lam > cmin) patchf = 1;
+  else if (lam >= cmax || lam <= cmin) { lam = 0.0; patchf = 3; cond = false; }
+  if (cond && lam == 0.0) patchf = (-cmin >= cmax) ? 1 : -1;
+  if (patchf == 3) {  // the HLL flux Fhll (plain division, as the forward)
+    hll_reverse(cL, cR, fL, fR, cmin, cmax, mu, fLb, fRb, cLb, cRb, cmaxb, cminb, true);
+    return;
+  }
+  const bool right = patchf == 1;
+  const double *wS = right ? cR : cL, *fS = right ? fR : fL;
+  double *wSb = right ? cRb : cLb, *fSb = right ? fRb : fLb;
+  const double cs = right ? cmax : cmin;
+  const double vS = wS[1] / wS[0];
+  const double csmls = 1.0 / (cs - lam);
+  double wCD[4];
+  wCD[0] = wS[0] * (cs - vS) * csmls;
+  wCD[2] = (cs * wS[2] - fS[2]) * csmls;
+  wCD[1] = wCD[0] * lam;
+  const double pCD = wS[0] * (cs - vS) * (lam - vS) + fS[1] - wS[1] * vS;
+  const double numE = cs * wS[3] - fS[3] + lam * pCD;
+  wCD[3] = numE * csmls;
+  // F = fS + cs (wCD - wS)
+  double csb = 0.0, lamb = 0.0, csmlsb = 0.0, vSb = 0.0, wCDb[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    fSb[v] += mu[v];
+    wCDb[v] = cs * mu[v];
+    wSb[v] -= cs * mu[v];
+    csb += mu[v] * (wCD[v] - wS[v]);
+  }
+  // wCD_e = (cs e - f_e + lam pCD) csmls
+  {
+    const double nb = wCDb[3] * csmls;
+    csmlsb += wCDb[3] * numE;
+    csb += nb * wS[3];
+    wSb[3] += nb * cs;
+    fSb[3] -= nb;
+    lamb += nb * pCD;
+    const double pb = nb * lam;
+    // pCD = rho (cs - v)(lam - v) + f_mn - mn v
+    wSb[0] += pb * (cs - vS) * (lam - vS);
+    csb += pb * wS[0] * (lam - vS);
+    lamb += pb * wS[0] * (cs - vS);
+    vSb += pb * (-wS[0] * (lam - vS) - wS[0] * (cs - vS) - wS[1]);
+    fSb[1] += pb;
+    wSb[1] -= pb * vS;
+  }
+  // wCD_mn = wCD_rho lam
+  wCDb[0] += wCDb[1] * lam;
+  lamb += wCDb[1] * wCD[0];
+  // wCD_mt = (cs mt - f_mt) csmls
+  {
+    const double nb = wCDb[2] * csmls;
+    csmlsb += wCDb[2] * (cs * wS[2] - fS[2]);
+    csb += nb * wS[2];
+    wSb[2] += nb * cs;
+    fSb[2] -= nb;
+  }
+  // wCD_rho = rho (cs - v) csmls
+  wSb[0] += wCDb[0] * (cs - vS) * csmls;
+  csb += wCDb[0] * wS[0] * csmls;
+  vSb -= wCDb[0] * wS[0] * csmls;
+  csmlsb += wCDb[0] * wS[0] * (cs - vS);
+  // csmls = 1 / (cs - lam)
+  {
+    const double d = -csmlsb * csmls * csmls;
+    csb += d;
+    lamb -= d;
+  }
+  // vS = mn / rho
+  wSb[1] += vSb / wS[0];
+  wSb[0] -= vSb * vS / wS[0];
+  // lam = whll_mn / whll_rho; whll_v = (cmax wR - cmin wL + fL - fR) / Dn
+  double whllb[2];
+  whllb[1] = lamb / whll[0];
+  whllb[0] = -lamb * lam / whll[0];
+#pragma unroll
+  for (int v = 0; v < 2; ++v) {
+    const double b = whllb[v] / Dn;
+    cRb[v] += b * cmax;
+    cLb[v] -= b * cmin;
+    fLb[v] += b;
+    fRb[v] -= b;
+    cmaxb += whllb[v] * (cR[v] - whll[v]) / Dn;
+    cminb += whllb[v] * (whll[v] - cL[v]) / Dn;
+  }
+  if (right) cmaxb += csb;
+  else cminb += csb;
+}
+
 // Vector-Jacobian product of one face flux.  wp: staged primitives; D: face
 // direction; fi: face index along D (-1..17, face fi lies between cells fi-1
 // and fi); row: the other coordinate; mu: dL/dF in rotated variable order
 // (1 = normal, 2 = tangential velocity).  Adds dL/d(primitive) of the four
 // stencil cells fi-2..fi+1 to gq (rotated order); returns dL/dgamma.
-template <int LIM>
+template <int LIM, int SOLVER>
 __device__ __forceinline__ double face_vjp(const double *wp, int D, int fi, int row, const double *mu,
                                            const PhysParams &P, double (&gq)[4][4]) {
   auto at = [&](int o, int ov) -> double {
@@ -108,30 +247,12 @@ __device__ __forceinline__ double face_vjp(const double *wp, int D, int fi, int 
   const double csL = g * L[3] / L[0], csR = g * R[3] / R[0];
   const double dm = sqrt((t1 * csL + t2 * csR) * t3 + 0.5 * t1 * t2 * (t3 * t3) * (dv * dv));
   const double cmin = um - dm, cmax = um + dm;
-  // ---- reverse: HLL
+  // ---- reverse: Riemann solver
   double fLb[4] = {0.0, 0.0, 0.0, 0.0}, fRb[4] = {0.0, 0.0, 0.0, 0.0};
   double cLb[4] = {0.0, 0.0, 0.0, 0.0}, cRb[4] = {0.0, 0.0, 0.0, 0.0};
   double cmaxb = 0.0, cminb = 0.0;
-  if (cmin >= 0.0) {
-#pragma unroll
-    for (int v = 0; v < 4; ++v) fLb[v] = mu[v];
-  } else if (cmax <= 0.0) {
-#pragma unroll
-    for (int v = 0; v < 4; ++v) fRb[v] = mu[v];
-  } else {
-    const double iD = 1.0 / (cmax - cmin);
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const double dW = cR[v] - cL[v];
-      const double F = div_(cmax * fL[v] - cmin * fR[v] + cmin * cmax * dW, cmax - cmin);
-      fLb[v] = mu[v] * cmax * iD;
-      fRb[v] = -mu[v] * cmin * iD;
-      cRb[v] = mu[v] * cmin * cmax * iD;
-      cLb[v] = -cRb[v];
-      cmaxb += mu[v] * (fL[v] + cmin * dW - F) * iD;
-      cminb += mu[v] * (-fR[v] + cmax * dW + F) * iD;
-    }
-  }
+  if constexpr (SOLVER == SOLVER_HLLC) hllc_reverse(cL, cR, fL, fR, cmin, cmax, mu, fLb, fRb, cLb, cRb, cmaxb, cminb);
+  else hll_reverse(cL, cR, fL, fR, cmin, cmax, mu, fLb, fRb, cLb, cRb, cmaxb, cminb, false);
   double Lb[4] = {0.0, 0.0, 0.0, 0.0}, Rb[4] = {0.0, 0.0, 0.0, 0.0}, gb = 0.0;
   // Einfeldt reverse
   {
@@ -191,7 +312,7 @@ __device__ __forceinline__ double face_vjp(const double *wp, int D, int fi, int 
   return gb;
 }
 
-template <int LIM>
+template <int LIM, int SOLVER>
 __global__ void __launch_bounds__(ADJ_THREADS, AMRVAC_ADJ_MINB) adj_stage_kernel(const AdjArgs A) {
   extern __shared__ __align__(16) double adj_sm[];
   double *wp = adj_sm;
@@ -263,7 +384,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, AMRVAC_ADJ_MINB) adj_stage_kernel
           mu[v] = A.s[D] * (lm[ov * (LMW * LMW) + (yr + 2) * LMW + (xr + 2)] -
                             lm[ov * (LMW * LMW) + (yl + 2) * LMW + (xl + 2)]);
         }
-        const double gface = face_vjp<LIM>(wp, D, fi, row, mu, P, gq);
+        const double gface = face_vjp<LIM, SOLVER>(wp, D, fi, row, mu, P, gq);
         // faces next to a block edge are computed by two or three blocks: the
         // gamma term counts once, in the block of the cell right of the face
         // (and face 16 at a physical high side)
@@ -332,19 +453,33 @@ __global__ void __launch_bounds__(ADJ_THREADS, AMRVAC_ADJ_MINB) adj_stage_kernel
 
 }  // namespace
 
+template <int LIM, int SOLVER>
+static cudaError_t prep_one() {
+  return cudaFuncSetAttribute(adj_stage_kernel<LIM, SOLVER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)ADJ_SMEM);
+}
+
 cudaError_t adjoint_prepare() {
-  cudaError_t e = cudaFuncSetAttribute(adj_stage_kernel<LIM_MINMOD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)ADJ_SMEM);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(adj_stage_kernel<LIM_VANLEER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)ADJ_SMEM);
+  cudaError_t e = prep_one<LIM_MINMOD, SOLVER_HLL>();
+  if (e == cudaSuccess) e = prep_one<LIM_VANLEER, SOLVER_HLL>();
+  if (e == cudaSuccess) e = prep_one<LIM_MINMOD, SOLVER_HLLC>();
+  if (e == cudaSuccess) e = prep_one<LIM_VANLEER, SOLVER_HLLC>();
   return e;
 }
 
-cudaError_t launch_adjoint_stage(const AdjArgs &A, int limiter, cudaStream_t s) {
-  if (limiter == LIM_MINMOD) adj_stage_kernel<LIM_MINMOD><<<A.sa.nblocks, ADJ_THREADS, ADJ_SMEM, s>>>(A);
-  else if (limiter == LIM_VANLEER) adj_stage_kernel<LIM_VANLEER><<<A.sa.nblocks, ADJ_THREADS, ADJ_SMEM, s>>>(A);
-  else return cudaErrorInvalidValue;
+cudaError_t launch_adjoint_stage(const AdjArgs &A, int limiter, int solver, cudaStream_t s) {
+  const int nb = A.sa.nblocks;
+  if (solver == SOLVER_HLL) {
+    if (limiter == LIM_MINMOD) adj_stage_kernel<LIM_MINMOD, SOLVER_HLL><<<nb, ADJ_THREADS, ADJ_SMEM, s>>>(A);
+    else if (limiter == LIM_VANLEER) adj_stage_kernel<LIM_VANLEER, SOLVER_HLL><<<nb, ADJ_THREADS, ADJ_SMEM, s>>>(A);
+    else return cudaErrorInvalidValue;
+  } else if (solver == SOLVER_HLLC) {
+    if (limiter == LIM_MINMOD) adj_stage_kernel<LIM_MINMOD, SOLVER_HLLC><<<nb, ADJ_THREADS, ADJ_SMEM, s>>>(A);
+    else if (limiter == LIM_VANLEER) adj_stage_kernel<LIM_VANLEER, SOLVER_HLLC><<<nb, ADJ_THREADS, ADJ_SMEM, s>>>(A);
+    else return cudaErrorInvalidValue;
+  } else {
+    return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 

@@ -27,8 +27,9 @@ struct AdjArgs {
   double *gamma_part;      // [nblocks]
 };
 
-// 2-D hydrodynamics, HLL, limiter minmod (1) or vanleer (5), Einfeldt bounds.
-cudaError_t launch_adjoint_stage(const AdjArgs &A, int limiter, cudaStream_t s);
+// 2-D hydrodynamics, solver HLL (2) or HLLC (3), limiter minmod (1) or
+// vanleer (5), Einfeldt bounds.
+cudaError_t launch_adjoint_stage(const AdjArgs &A, int limiter, int solver, cudaStream_t s);
 cudaError_t adjoint_prepare();
 // *p = v on the stream (a device scalar without a host round trip)
 cudaError_t launch_set_scalar(double *p, double v, cudaStream_t s);

@@ -887,10 +887,11 @@ static int adjoint_step_impl(amrvac_ctx *c, const double *u0, const double *u1, 
   if (int r = check_ctx(c, true)) return r;
   const amrvac_cfg &k = c->cfg;
   if (!lam || !gamma_part || !(dt > 0.0)) return fail(AMRVAC_E_ARG, "bad adjoint arguments");
-  if (k.physics != 0 || k.ndim != 2 || k.flux_scheme != AMRVAC_FS_HLL || k.typeboundspeed != AMRVAC_BS_EINFELDT ||
-      (k.limiter != AMRVAC_LIM_MINMOD && k.limiter != AMRVAC_LIM_VANLEER) || k.fix_small_values || k.precision != 0)
+  if (k.physics != 0 || k.ndim != 2 || (k.flux_scheme != AMRVAC_FS_HLL && k.flux_scheme != AMRVAC_FS_HLLC) ||
+      k.typeboundspeed != AMRVAC_BS_EINFELDT || (k.limiter != AMRVAC_LIM_MINMOD && k.limiter != AMRVAC_LIM_VANLEER) ||
+      k.fix_small_values || k.precision != 0)
     return fail(AMRVAC_E_UNSUPPORTED,
-                "adjoint: 2-D hd, hll, minmod or vanleer, Einfeldt, FP64, no fix_small_values");
+                "adjoint: 2-D hd, hll or hllc, minmod or vanleer, Einfeldt, FP64, no fix_small_values");
   if (k.time_stepper != AMRVAC_TS_THREESTEP && k.time_stepper != AMRVAC_TS_TWOSTEP)
     return fail(AMRVAC_E_UNSUPPORTED, "adjoint: threestep or twostep");
   for (int sd = 0; sd < 4; ++sd)
@@ -931,8 +932,8 @@ static int adjoint_step_impl(amrvac_ctx *c, const double *u0, const double *u1, 
     // forward U1 = U0 + dt L(U0); U2 = (U0 + U1 + dt L(U1)) / 2
     if (!u0)
       if (int r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0)) return r;
-    CK(launch_adjoint_stage(args(1, lam, S1, nullptr, S2, 1, 0.5, 0.5, 0.5), k.limiter, c->stream));
-    CK(launch_adjoint_stage(args(0, S1, lam, S2, nullptr, 0, 0.0, 1.0, 1.0), k.limiter, c->stream));
+    CK(launch_adjoint_stage(args(1, lam, S1, nullptr, S2, 1, 0.5, 0.5, 0.5), k.limiter, k.flux_scheme, c->stream));
+    CK(launch_adjoint_stage(args(0, S1, lam, S2, nullptr, 0, 0.0, 1.0, 1.0), k.limiter, k.flux_scheme, c->stream));
     c->launches += 3;
     return 0;
   }
@@ -945,11 +946,11 @@ static int adjoint_step_impl(amrvac_ctx *c, const double *u0, const double *u1, 
     if (int r = launch_stage(c, 1, 2, 0, a21, 1.0 - a21, b22)) return r;
   }
   // stage 3: U3 = a31 U0 + (1-a31) U2 + b33 dt L(U2)
-  CK(launch_adjoint_stage(args(2, lam, S1, nullptr, S2, 1, a31, 1.0 - a31, b33), k.limiter, c->stream));
+  CK(launch_adjoint_stage(args(2, lam, S1, nullptr, S2, 1, a31, 1.0 - a31, b33), k.limiter, k.flux_scheme, c->stream));
   // stage 2: U2 = a21 U0 + (1-a21) U1 + b22 dt L(U1)
-  CK(launch_adjoint_stage(args(1, S1, S3, nullptr, S2, 0, a21, 1.0 - a21, b22), k.limiter, c->stream));
+  CK(launch_adjoint_stage(args(1, S1, S3, nullptr, S2, 0, a21, 1.0 - a21, b22), k.limiter, k.flux_scheme, c->stream));
   // stage 1: U1 = U0 + b11 dt L(U0); dL/dU0 = base sum + stage-1 transpose
-  CK(launch_adjoint_stage(args(0, S3, lam, S2, nullptr, 0, 0.0, 1.0, b11), k.limiter, c->stream));
+  CK(launch_adjoint_stage(args(0, S3, lam, S2, nullptr, 0, 0.0, 1.0, b11), k.limiter, k.flux_scheme, c->stream));
   c->launches += 3;
   return 0;
 }

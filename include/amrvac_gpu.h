@@ -240,7 +240,7 @@ int amrvac_gpu_register_copy(amrvac_ctx *ctx, int reg, double *dev, int to_regis
  * lam (device, register layout) holds dL/dU^{n+1} on entry and dL/dU^n on
  * return; gamma_part (device, [nblocks]) accumulates dL/dgamma of the step
  * per block (sum it for the total).  Recomputes the stage inputs in
- * registers 1 and 2.  2-D hydrodynamics, HLL with minmod or vanleer,
+ * registers 1 and 2.  2-D hydrodynamics, HLL or HLLC with minmod or vanleer,
  * Einfeldt bounds, FP64, periodic or cont boundaries, uniform dx, threestep
  * or twostep.  Asynchronous on the context stream. */
 int amrvac_gpu_adjoint_step(amrvac_ctx *ctx, double *lam, double dt, double *gamma_part);

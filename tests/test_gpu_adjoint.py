@@ -30,7 +30,7 @@ def _setup(n, lim):
     return prim, rho0, p0, mask
 
 
-def _loss_fn(n, lim, dts, p0, mask, k=20):
+def _loss_fn(n, lim, dts, p0, mask, k=20, fs="hll"):
     import torch
     from amrvac_b200.adjoint import blocks_to_domain, domain_to_blocks, solve
 
@@ -38,16 +38,17 @@ def _loss_fn(n, lim, dts, p0, mask, k=20):
         z = torch.zeros_like(rho0)
         U0 = domain_to_blocks(torch.stack([rho0, z, z, p0 / (gamma - 1.0)]))
         UN = solve(U0, gamma, dts, (n, n), (0.0, 0.0), (1.0, 1.0), checkpoint_every=k, limiter=lim,
-                   typeboundary=["cont"] * 4)
+                   flux_scheme=fs, typeboundary=["cont"] * 4)
         rho = blocks_to_domain(UN, n, n)[0]
         return (mask * rho * rho).sum()
     return f
 
 
-def _dts(n, rho0, p0, nsteps, lim):
+def _dts(n, rho0, p0, nsteps, lim, fs="hll"):
     import torch
     from amrvac_b200.adjoint import FrozenDtSolver, domain_to_blocks
-    s = FrozenDtSolver((n, n), (0.0, 0.0), (1.0, 1.0), B.GAMMA, limiter=lim, typeboundary=["cont"] * 4)
+    s = FrozenDtSolver((n, n), (0.0, 0.0), (1.0, 1.0), B.GAMMA, limiter=lim, flux_scheme=fs,
+                       typeboundary=["cont"] * 4)
     z = torch.zeros_like(rho0)
     U0 = domain_to_blocks(torch.stack([rho0, z, z, p0 / (B.GAMMA - 1.0)]))
     dts = s.cfl_dts(U0, nsteps)
@@ -55,22 +56,25 @@ def _dts(n, rho0, p0, nsteps, lim):
     return dts
 
 
-@pytest.mark.parametrize("lim", ["minmod", "vanleer"])
-def test_gradient_matches_dual_number_reference(oracle_lib, lim):
+SCHEMES = [("hll", "minmod"), ("hll", "vanleer"), ("hllc", "minmod"), ("hllc", "vanleer")]
+
+
+@pytest.mark.parametrize("fs,lim", SCHEMES)
+def test_gradient_matches_dual_number_reference(oracle_lib, fs, lim):
     _cuda()
     import torch
     O = oracle_lib
     n, nsteps = 32, 20
     prim, rho0, p0, mask = _setup(n, lim)
-    dts = _dts(n, rho0, p0, nsteps, lim)
-    f = _loss_fn(n, lim, dts, p0, mask)
+    dts = _dts(n, rho0, p0, nsteps, lim, fs)
+    f = _loss_fn(n, lim, dts, p0, mask, fs=fs)
     r = rho0.clone().requires_grad_(True)
     g = torch.tensor(B.GAMMA, dtype=torch.float64, device="cuda", requires_grad=True)
     L = f(r, g)
     L.backward()
     grad_rho = r.grad.cpu().numpy()
     grad_gamma = float(g.grad)
-    c = O.make_cfg(physics="hd", ndim=2, gamma=B.GAMMA, flux_scheme="hll", limiter=lim, courantpar=0.8)
+    c = O.make_cfg(physics="hd", ndim=2, gamma=B.GAMMA, flux_scheme=fs, limiter=lim, courantpar=0.8)
     w0 = B.to_cons_blocks(prim)
     mb = B.mask_blocks(n)
     drho = np.random.default_rng(5).standard_normal((n, n))
@@ -116,8 +120,8 @@ def test_gradient_matches_central_differences():
     assert abs(fdg - float(g.grad)) <= 2e-5 * abs(float(g.grad)), (fdg, float(g.grad))
 
 
-@pytest.mark.parametrize("lim", ["minmod", "vanleer"])
-def test_adjoint_step_is_the_transpose_of_the_step(lim):
+@pytest.mark.parametrize("fs,lim", SCHEMES)
+def test_adjoint_step_is_the_transpose_of_the_step(fs, lim):
     """<lam, J dU> == <J^T lam, dU> for one SSP-RK3 step (J by central
     differences), on a smooth state with flow everywhere: no limiter slope
     sits exactly at a kink (the blast's v = 0, uniform-pressure regions do)."""
@@ -128,7 +132,8 @@ def test_adjoint_step_is_the_transpose_of_the_step(lim):
     n = 32
     cons = P.prim_to_cons(P.random_smooth("hd", 2, 2, n, seed=3), "hd", 2, B.GAMMA)[:, 0]
     U0 = domain_to_blocks(torch.tensor(cons, dtype=torch.float64, device="cuda")).contiguous()
-    s = FrozenDtSolver((n, n), (0.0, 0.0), (1.0, 1.0), B.GAMMA, limiter=lim, typeboundary=["cont"] * 4)
+    s = FrozenDtSolver((n, n), (0.0, 0.0), (1.0, 1.0), B.GAMMA, limiter=lim, flux_scheme=fs,
+                       typeboundary=["cont"] * 4)
     dt = float(s.cfl_dts(U0, 1)[0])
     rng = np.random.default_rng(23)
     lam = torch.tensor(rng.standard_normal(s.shape), dtype=torch.float64, device="cuda")
