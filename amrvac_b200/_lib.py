@@ -102,6 +102,7 @@ SIGNATURES = [
     ("amrvac_gpu_get_cbounds_points", _i, [_vp, _i, _dp, _dp, _dp, _dp, _i, _dp, _dp]),
     ("amrvac_gpu_riemann_points", _i, [_vp, _i, _dp, _dp, _i, _d, _dp]),
     ("amrvac_gpu_srl_maps", _i, [_i, _i, _ip, _ip, _ip, _ip]),
+    ("amrvac_gpu_lohner", _i, [_vp, _i, _dp, _ip, _i, _dp, _dp, _dp, _ip, _ip, _dp]),
     ("amrvac_gpu_step_dt", _i, [_vp, _d]),
     ("amrvac_gpu_register_copy", _i, [_vp, _i, _vp, _i]),
     ("amrvac_gpu_adjoint_step", _i, [_vp, _vp, _d, _vp]),

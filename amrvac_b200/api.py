@@ -156,6 +156,23 @@ class Context:
         _lib.check(self.L.amrvac_gpu_register_ptr(self.h, REG.get(reg, reg), ctypes.byref(p)), "register_ptr")
         return ctypes.cast(p, ctypes.c_void_p).value
 
+    def lohner(self, weight, logflag=None, refine_max_level=2, refine_threshold=0.1, derefine_ratio=0.125,
+               amr_wavefilter=1e-2, block_level=None, reg="ps"):
+        """Löhner estimator on all blocks: (flags, errmax) with flags 1 refine | 2 coarsen."""
+        nl = refine_max_level
+        per = lambda x: np.ascontiguousarray(np.broadcast_to(np.asarray(x, np.float64), (nl,)))  # noqa: E731
+        w = np.ascontiguousarray(weight, np.float64)
+        lf = None if logflag is None else np.ascontiguousarray(logflag, np.int32)
+        lv = None if block_level is None else np.ascontiguousarray(block_level, np.int32)
+        flags = np.zeros(self.nblocks, np.int32)
+        errmax = np.zeros(self.nblocks, np.float64)
+        ip = ctypes.POINTER(ctypes.c_int)
+        _lib.check(self.L.amrvac_gpu_lohner(self.h, REG.get(reg, reg), _dp(w), lf.ctypes.data_as(ip) if lf is not None
+                                            else None, nl, _dp(per(refine_threshold)), _dp(per(derefine_ratio)),
+                                            _dp(per(amr_wavefilter)), lv.ctypes.data_as(ip) if lv is not None else None,
+                                            flags.ctypes.data_as(ip), _dp(errmax)), "lohner")
+        return flags, errmax
+
     def launch_count(self) -> int:
         return int(self.L.amrvac_gpu_launch_count(self.h))
 

@@ -11,6 +11,7 @@
 
 #include "../../include/amrvac_gpu.h"
 #include "adjoint.cuh"
+#include "amr.cuh"
 #include "aux.cuh"
 #include "kernels.cuh"
 
@@ -85,6 +86,8 @@ struct amrvac_ctx {
   int wave_ctas = 1;       // resident stage CTAs on the device (one wave)
   std::vector<double> h_dx;            // [nblocks][3] cell sizes (host copy)
   double *d_adj[3] = {nullptr, nullptr, nullptr};  // adjoint work registers (lazily)
+  int *d_amr_int = nullptr;            // [2][nblocks] levels, flags (Löhner, lazily)
+  double *d_amr_err = nullptr;         // [nblocks] largest error per block
   bool adj_prepared = false;
 };
 
@@ -372,6 +375,8 @@ int amrvac_gpu_destroy(amrvac_ctx *c) {
   cudaFree(c->d_status);
   cudaFree(c->d_block_status);
   for (int r = 0; r < 3; ++r) cudaFree(c->d_adj[r]);
+  cudaFree(c->d_amr_int);
+  cudaFree(c->d_amr_err);
   cudaFree(c->d_stage);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -446,6 +451,8 @@ int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const in
   CK(cudaStreamSynchronize(c->stream));
   c->h_dx = dxb;
   for (int r = 0; r < 3; ++r) { cudaFree(c->d_adj[r]); c->d_adj[r] = nullptr; }
+  cudaFree(c->d_amr_int); c->d_amr_int = nullptr;
+  cudaFree(c->d_amr_err); c->d_amr_err = nullptr;
   return 0;
 }
 
@@ -952,6 +959,51 @@ static int adjoint_step_impl(amrvac_ctx *c, const double *u0, const double *u1, 
   // stage 1: U1 = U0 + b11 dt L(U0); dL/dU0 = base sum + stage-1 transpose
   CK(launch_adjoint_stage(args(0, S3, lam, S2, nullptr, 0, 0.0, 1.0, b11), k.limiter, k.flux_scheme, c->stream));
   c->launches += 3;
+  return 0;
+}
+
+
+// ---------------------------------------------------------------- AMR decisions
+int amrvac_gpu_lohner(amrvac_ctx *c, int reg, const double *weight, const int *logflag, int refine_max_level,
+                      const double *refine_threshold, const double *derefine_ratio, const double *amr_wavefilter,
+                      const int *block_level, int *flags, double *errmax) {
+  if (int r = check_ctx(c, true)) return r;
+  if (reg < 0 || reg > 2 || !weight || !flags || !refine_threshold || !derefine_ratio || !amr_wavefilter)
+    return fail(AMRVAC_E_ARG, "lohner: bad arguments");
+  if (refine_max_level < 1 || refine_max_level > AMR_MAX_LEVELS)
+    return fail(AMRVAC_E_ARG, "lohner: refine_max_level out of range");
+  if (c->cfg.ndim < 2) return fail(AMRVAC_E_UNSUPPORTED, "lohner: ndim 2 or 3");
+  LohnerArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.sa = stage_args(c, reg, reg, reg, 0.0, 1.0, 1.0);
+  A.nw = c->nw;
+  for (int v = 0; v < c->nw; ++v) {
+    A.weight[v] = weight[v];
+    if (logflag && logflag[v]) A.logflag |= 1u << v;
+  }
+  for (int l = 0; l < refine_max_level; ++l) {
+    A.threshold[l] = refine_threshold[l];
+    A.derefine[l] = derefine_ratio[l];
+    A.wavefilter[l] = amr_wavefilter[l];
+  }
+  A.refine_max_level = refine_max_level;
+  std::vector<int> lev(c->nblocks, 1);
+  if (block_level)
+    for (int b = 0; b < c->nblocks; ++b) {
+      if (block_level[b] < 1 || block_level[b] > refine_max_level) return fail(AMRVAC_E_ARG, "lohner: bad level");
+      lev[b] = block_level[b];
+    }
+  if (!c->d_amr_int) CK(cudaMalloc(&c->d_amr_int, sizeof(int) * 2 * c->nblocks));
+  if (!c->d_amr_err) CK(cudaMalloc(&c->d_amr_err, sizeof(double) * c->nblocks));
+  CK(cudaMemcpyAsync(c->d_amr_int, lev.data(), sizeof(int) * c->nblocks, cudaMemcpyHostToDevice, c->stream));
+  A.level = c->d_amr_int;
+  A.flags = c->d_amr_int + c->nblocks;
+  A.errmax = c->d_amr_err;
+  CK(launch_lohner(A, c->cfg.ndim, c->stream));
+  ++c->launches;
+  CK(cudaMemcpyAsync(flags, A.flags, sizeof(int) * c->nblocks, cudaMemcpyDeviceToHost, c->stream));
+  if (errmax) CK(cudaMemcpyAsync(errmax, c->d_amr_err, sizeof(double) * c->nblocks, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
 

@@ -229,6 +229,22 @@ int amrvac_gpu_riemann_points(amrvac_ctx *ctx, int n, const double *wlp, const d
 int amrvac_gpu_getdt_noalloc(const amrvac_cfg *cfg, const double *w_dev, int nblocks, const double *dx,
                              void *stream, double *dt, double *cmax_global);
 
+/* ---- AMR decisions --------------------------------------------------------
+ * Löhner error estimator (lohner_grid, src/amr/mod_errest.t:63-200,
+ * refine_criterion 3) on register reg, all blocks: flags[b] = 1 if the block
+ * should refine (some cell has error >= refine_threshold(level) and level <
+ * refine_max_level), 2 if it may coarsen (every cell has error <=
+ * derefine_ratio(level) * refine_threshold(level) and level > 1).  weight and
+ * logflag: w_refine_weight and logflag per conserved variable ([nw]; logflag
+ * may be NULL); refine_threshold, derefine_ratio, amr_wavefilter: per level
+ * ([refine_max_level]); block_level: 1-based level per block (NULL = all 1);
+ * errmax (may be NULL): the largest error of each block.  Host arrays;
+ * synchronous.  Ghost values are those of getbc (same-level neighbours and
+ * physical boundaries). */
+int amrvac_gpu_lohner(amrvac_ctx *ctx, int reg, const double *weight, const int *logflag, int refine_max_level,
+                      const double *refine_threshold, const double *derefine_ratio, const double *amr_wavefilter,
+                      const int *block_level, int *flags, double *errmax);
+
 /* ---- Discrete adjoint (no counterpart in the reference) -------------------
  * One step with a given dt (the configured RK stages, no setdt): the forward
  * map of the adjoint, whose dt sequence is frozen. */

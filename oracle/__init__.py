@@ -92,6 +92,8 @@ def lib():
         L.orc_count_flops_stage.argtypes = [cp, dp, dp, d, dp, d]
         L.orc_count_flops_getdt.restype = d
         L.orc_count_flops_getdt.argtypes = [cp, dp, dp]
+        L.orc_lohner_block.restype = None
+        L.orc_lohner_block.argtypes = [cp, dp, dp, ip, d, d, d, ctypes.c_int, ctypes.c_int, dp, ip, ip]
         L.orc_dual_run.restype = ctypes.c_int
         L.orc_dual_run.argtypes = [cp, ip, dp, dp, ip, dp, dp, d, ctypes.c_int, dp, dp, ctypes.c_int, dp, dp, dp]
         _lib = L
@@ -290,3 +292,20 @@ def dual_run(c: OrcCfg, domain_nx, xprobmin, xprobmax, bc, w0, dw0, dgamma, dts,
                             _dp(dw) if dw is not None else None, float(dgamma), len(dts), _dp(dts), _dp(mask),
                             nthreads, ctypes.byref(loss), ctypes.byref(dloss), _dp(wf) if wf is not None else None)
     return (loss.value, dloss.value, st) + ((wf,) if want_final else ())
+
+
+def lohner_block(c: OrcCfg, w, weight, logflag, wavefilter=1e-2, threshold=0.1, derefine=0.125, level=1,
+                 refine_max_level=2):
+    """Löhner error of one ghosted block: (error over the interior, refine, coarsen)."""
+    w = np.ascontiguousarray(w, np.float64)
+    wt = np.ascontiguousarray(weight, np.float64)
+    lf = np.ascontiguousarray(logflag, np.int32)
+    n = 1
+    for d in range(c.ndim):
+        n *= c.block_nx[d]
+    err = np.zeros(n)
+    r = ctypes.c_int()
+    co = ctypes.c_int()
+    lib().orc_lohner_block(ctypes.byref(c), _dp(w), _dp(wt), _ip(lf), wavefilter, threshold, derefine, level,
+                           refine_max_level, _dp(err), ctypes.byref(r), ctypes.byref(co))
+    return err, bool(r.value), bool(co.value)

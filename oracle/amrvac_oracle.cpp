@@ -1747,4 +1747,92 @@ int orc_dual_run(const orc_cfg *cfg, const int *domain_nx, const double *xprobmi
   return st;
 }
 
+
+// ---------------------------------------------------------------- Löhner estimator
+// lohner_grid (src/amr/mod_errest.t:63-200), refine_criterion 3, without B0
+// and user variables: on one ghosted block (>= 2 ghost layers filled).
+// error[interior cells] (optional), *refine / *coarsen as the reference sets
+// refine(igrid) / coarsen(igrid).
+void orc_lohner_block(const orc_cfg *cfg, const double *wblk, const double *weight, const int *logflag,
+                      double wavefilter, double threshold, double derefine, int level, int refine_max_level,
+                      double *error_out, int *refine, int *coarsen) {
+  State s = make_state(*cfg);
+  const Geo &g = s.g;
+  const int nw = s.x.nw, ndim = s.c.ndim;
+  Arr<double> w = wrap_in(g, nw, wblk);
+  const double epsilon = 1.0e-6;
+  Box ixM, ix;
+  for (int d = 0; d < 3; ++d) {
+    ixM.lo[d] = d < ndim ? s.c.nghost : 0;
+    ixM.hi[d] = d < ndim ? s.c.nghost + s.c.block_nx[d] - 1 : 0;
+    ix.lo[d] = d < ndim ? ixM.lo[d] - 1 : 0;
+    ix.hi[d] = d < ndim ? ixM.hi[d] + 1 : 0;
+  }
+  Arr<double> error(g, 1), numer(g, 1), denom(g, 1), tmp(g, 1), tmp2(g, 1);
+  forbox(ixM, [&](int i, int j, int k) { error(i, j, k, 0) = 0.0; });
+  auto val = [&](int iw, int i, int j, int k) {
+    const double v = w(i, j, k, iw);
+    return logflag[iw] ? std::log10(v) : v;
+  };
+  for (int iw = 0; iw < nw; ++iw) {
+    if (weight[iw] == 0.0) continue;
+    forbox(ixM, [&](int i, int j, int k) { numer(i, j, k, 0) = 0.0; denom(i, j, k, 0) = 0.0; });
+    for (int d = 0; d < ndim; ++d) {
+      int e[3] = {0, 0, 0};
+      e[d] = 1;
+      forbox(ix, [&](int i, int j, int k) {
+        tmp(i, j, k, 0) = val(iw, i + e[0], j + e[1], k + e[2]) - val(iw, i - e[0], j - e[1], k - e[2]);
+      });
+      for (int d2 = 0; d2 < ndim; ++d2) {
+        int f[3] = {0, 0, 0};
+        f[d2] = 1;
+        forbox(ixM, [&](int i, int j, int k) {
+          const double q = tmp(i + f[0], j + f[1], k + f[2], 0) - tmp(i - f[0], j - f[1], k - f[2], 0);
+          numer(i, j, k, 0) = numer(i, j, k, 0) + q * q;
+        });
+      }
+    }
+    for (int d = 0; d < ndim; ++d) {
+      int e[3] = {0, 0, 0};
+      e[d] = 1;
+      // tmp = |w| over the block; tmp2 on the extended box; then tmp on ixM
+      Box all;
+      for (int q = 0; q < 3; ++q) { all.lo[q] = 0; all.hi[q] = g.n[q] - 1; }
+      forbox(all, [&](int i, int j, int k) { tmp(i, j, k, 0) = std::fabs(val(iw, i, j, k)); });
+      forbox(ix, [&](int i, int j, int k) {
+        tmp2(i, j, k, 0) = tmp(i + e[0], j + e[1], k + e[2], 0) + tmp(i - e[0], j - e[1], k - e[2], 0);
+      });
+      forbox(ixM, [&](int i, int j, int k) {
+        const double c = val(iw, i, j, k);
+        tmp(i, j, k, 0) = std::fabs(val(iw, i + 2 * e[0], j + 2 * e[1], k + 2 * e[2]) - c) +
+                          std::fabs(c - val(iw, i - 2 * e[0], j - 2 * e[1], k - 2 * e[2]));
+      });
+      for (int d2 = 0; d2 < ndim; ++d2) {
+        int f[3] = {0, 0, 0};
+        f[d2] = 1;
+        forbox(ixM, [&](int i, int j, int k) {
+          const double q = tmp(i, j, k, 0) + wavefilter * (tmp2(i + f[0], j + f[1], k + f[2], 0) +
+                                                           tmp2(i - f[0], j - f[1], k - f[2], 0));
+          denom(i, j, k, 0) = denom(i, j, k, 0) + q * q;
+        });
+      }
+    }
+    forbox(ixM, [&](int i, int j, int k) {
+      error(i, j, k, 0) = error(i, j, k, 0) +
+                          weight[iw] * std::sqrt(numer(i, j, k, 0) / std::max(denom(i, j, k, 0), epsilon));
+    });
+  }
+  bool any_ref = false, all_coa = true;
+  size_t q = 0;
+  forbox(ixM, [&](int i, int j, int k) {
+    const double e = error(i, j, k, 0);
+    if (error_out) error_out[q++] = e;
+    if (e >= threshold) any_ref = true;
+    else if (!(e <= derefine * threshold)) all_coa = false;
+    if (e >= threshold) all_coa = false;
+  });
+  *refine = any_ref && level < refine_max_level;
+  *coarsen = all_coa && level > 1;
+}
+
 }  // extern "C"

@@ -168,6 +168,13 @@ int orc_dual_run(const orc_cfg *cfg, const int *domain_nx, const double *xprobmi
                  double dgamma, int nsteps, const double *dts, const double *mask, int nthreads,
                  double *loss, double *dloss, double *w_final);
 
+/* Löhner error estimator (lohner_grid, src/amr/mod_errest.t:63-200) of one
+ * ghosted block: error over the interior (x fastest, optional) and the
+ * reference's refine / coarsen decision for the block. */
+void orc_lohner_block(const orc_cfg *cfg, const double *w, const double *weight, const int *logflag,
+                      double wavefilter, double threshold, double derefine, int level, int refine_max_level,
+                      double *error, int *refine, int *coarsen);
+
 #ifdef __cplusplus
 }
 #endif
