@@ -92,6 +92,18 @@ def lib():
         L.orc_count_flops_stage.argtypes = [cp, dp, dp, d, dp, d]
         L.orc_count_flops_getdt.restype = d
         L.orc_count_flops_getdt.argtypes = [cp, dp, dp]
+        vp = ctypes.c_void_p
+        L.orc_amr_create.restype = vp
+        L.orc_amr_create.argtypes = [cp, ip, dp, dp, ctypes.c_int, ip]
+        L.orc_amr_destroy.argtypes = [vp]
+        L.orc_amr_neighbors.argtypes = [vp, ip, ip, ip]
+        L.orc_amr_set_block.argtypes = [vp, ctypes.c_int, dp]
+        L.orc_amr_get_block.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
+        L.orc_amr_getbc.argtypes = [vp]
+        L.orc_amr_getdt.argtypes = [vp, dp, dp]
+        L.orc_amr_advect1.argtypes = [vp, ctypes.c_int, ctypes.c_int, d, d, d, ctypes.c_int]
+        L.orc_amr_combine_reg.argtypes = [vp, ctypes.c_int, d, ctypes.c_int, d, ctypes.c_int]
+        L.orc_amr_advance.argtypes = [vp, d, d, ctypes.c_int]
         L.orc_lohner_block.restype = None
         L.orc_lohner_block.argtypes = [cp, dp, dp, ip, d, d, d, ctypes.c_int, ctypes.c_int, dp, ip, ip]
         L.orc_dual_run.restype = ctypes.c_int
@@ -309,3 +321,57 @@ def lohner_block(c: OrcCfg, w, weight, logflag, wavefilter=1e-2, threshold=0.1, 
     lib().orc_lohner_block(ctypes.byref(c), _dp(w), _dp(wt), _ip(lf), wavefilter, threshold, derefine, level,
                            refine_max_level, _dp(err), ctypes.byref(r), ctypes.byref(co))
     return err, bool(r.value), bool(co.value)
+
+
+class AmrGrid:
+    """Static multi-level grid of the oracle: leaves [(level, ig0, ig1, ig2)],
+    periodic boundaries, the reference's multi-level getbc and flux fix."""
+
+    def __init__(self, c: OrcCfg, nbase, xprobmin, xprobmax, leaves):
+        self.c = c
+        nd = c.ndim
+        nb = np.array(list(nbase) + [1] * (3 - nd), np.int32)
+        xmn = np.array(list(xprobmin) + [0.0] * (3 - nd), np.float64)
+        xmx = np.array(list(xprobmax) + [1.0] * (3 - nd), np.float64)
+        lv = np.ascontiguousarray(np.array([list(t) + [0] * (4 - len(t)) for t in leaves], np.int32).reshape(-1))
+        self.h = lib().orc_amr_create(ctypes.byref(c), _ip(nb), _dp(xmn), _dp(xmx), len(leaves), _ip(lv))
+        self.nblocks = len(leaves)
+        self.shape = block_shape(c)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_amr_destroy(self.h)
+            self.h = None
+
+    def neighbors(self):
+        t = np.zeros(27 * self.nblocks, np.int32)
+        i = np.zeros(27 * self.nblocks, np.int32)
+        ch = np.zeros(27 * 8 * self.nblocks, np.int32)
+        lib().orc_amr_neighbors(self.h, _ip(t), _ip(i), _ip(ch))
+        return t.reshape(-1, 27), i.reshape(-1, 27), ch.reshape(-1, 27, 8)
+
+    def set_block(self, b, w):
+        lib().orc_amr_set_block(self.h, b, _dp(np.ascontiguousarray(w, np.float64)))
+
+    def get_block(self, b, reg=0):
+        w = np.zeros(self.shape, np.float64)
+        lib().orc_amr_get_block(self.h, reg, b, _dp(w))
+        return w
+
+    def getbc(self):
+        lib().orc_amr_getbc(self.h)
+
+    def getdt(self):
+        dt = ctypes.c_double()
+        cm = ctypes.c_double()
+        lib().orc_amr_getdt(self.h, ctypes.byref(dt), ctypes.byref(cm))
+        return dt.value, cm.value
+
+    def advect1(self, ra, rb, qdt, dtfactor=1.0, cmax_global=0.0, nthreads=0):
+        return lib().orc_amr_advect1(self.h, ra, rb, qdt, dtfactor, cmax_global, nthreads)
+
+    def combine_reg(self, dst, ca, ra, cb, rb):
+        lib().orc_amr_combine_reg(self.h, dst, ca, ra, cb, rb)
+
+    def advance(self, dt, cmax_global=0.0, nthreads=0):
+        return lib().orc_amr_advance(self.h, dt, cmax_global, nthreads)

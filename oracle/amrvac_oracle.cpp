@@ -17,6 +17,8 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <array>
+#include <map>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -963,7 +965,7 @@ void add_source_linde(const State &s, double qdt, const Box &ixO, const Arr<R> &
 // finite_volume (src/mod_finite_volume.t:116-339), slab_uniform, no local dt.
 template <class R>
 int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, double dtfactor,
-                  const double *dxs, double cmax_global) {
+                  const double *dxs, double cmax_global, std::vector<Arr<R>> *keep_fc = nullptr) {
   const Ix &x = s.x;
   const orc_cfg &c = s.c;
   const Geo &g = s.g;
@@ -1032,6 +1034,7 @@ int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, d
     else if (c.divb == ORC_DIVB_LINDE) add_source_linde(s, qsrc, ixO, wCT, wnew, dxs);
   }
   (void)dtfactor;
+  if (keep_fc) *keep_fc = std::move(fC);  // scaled face fluxes -qdt/dx F, for store_flux
   return st;
 }
 
@@ -1833,6 +1836,511 @@ void orc_lohner_block(const orc_cfg *cfg, const double *wblk, const double *weig
   });
   *refine = any_ref && level < refine_max_level;
   *coarsen = all_coa && level > 1;
+}
+
+
+// ---------------------------------------------------------------- AMR grid
+// A static hierarchy of leaf blocks (2:1 balanced), restating the reference's
+// multi-level getbc (src/mod_ghostcells_update.t:350-578: coarsen_grid into
+// psc, bc_fill_srl, bc_fill_restrict, bc_fill_prolong, gc_prolong /
+// bc_prolong / interpolation_linear, with the index maps of init_bc 116-305,
+// nghostcells 2, interpolation order 2, conserved-variable restriction and
+// prolongation) and the flux correction (store_flux / fix_conserve,
+// src/mod_fix_conserve.t:465-648) applied after every stage, as advect1 does
+// (src/mod_advance.t:611-666).  Physical boundaries: periodic only.
+}  // extern "C"
+
+namespace orc {
+
+enum { NT_BOUNDARY = 0, NT_COARSE = 1, NT_SIBLING = 2, NT_FINE = 3 };
+
+struct AmrGrid {
+  State s;      // block state (block_nx 16)
+  State sc;     // coarse representation (block_nx 8)
+  int ndim, nb;
+  int nbase[3];
+  double xmin[3], xmax[3];
+  std::vector<int> level, ig;                 // ig[3*b]
+  std::vector<int> ntype, nid;                // [b*27]
+  std::vector<int> child;                     // [(b*27+q)*8 + cbits]
+  std::vector<double> reg[3];                 // ghosted blocks
+  std::vector<double> psc;                    // [b] coarse representation
+  std::vector<std::vector<double>> pflux;     // [b*6 + 2*d + side]
+  size_t bsize, csize;
+  double dx(int b, int d) const { return (xmax[d] - xmin[d]) / (nbase[d] * 16.0 * double(1 << (level[b] - 1))); }
+  double bxmin(int b, int d) const { return xmin[d] + ig[3 * b + d] * 16.0 * dx(b, d); }
+};
+
+inline int q27(const int *dd) { return (dd[0] + 1) + 3 * ((dd[1] + 1) + 3 * (dd[2] + 1)); }
+
+// Index maps of init_bc (1-based, nghostcells 2, block 16, coarse 8).
+struct AmrMaps {
+  int srlS[3][2], srlR[3][2];   // by i+1: ixS_srl / ixR_srl
+  int rS[3][2], rR[4][2];       // ixS_r by i+1, ixR_r by n_inc 0..3
+  int pS[4][2], pR[4][2];       // ixS_p, ixR_p by inc / n_inc 0..3
+};
+
+inline AmrMaps amr_maps() {
+  const int ng = 2, nx = 16, nxCo = 8, ixMmin = ng + 1, ixMmax = ng + nx, ixGmax = nx + 2 * ng;
+  const int ixCoMmin = ng + 1, ixCoMmax = ng + nxCo;
+  const int ngCo = (ng + 1) / 2, io = 2;
+  AmrMaps m;
+  const int srlS[3][2] = {{ixMmin, ixMmin - 1 + ng}, {ixMmin, ixMmax}, {ixMmax + 1 - ng, ixMmax}};
+  const int srlR[3][2] = {{1, ng}, {ixMmin, ixMmax}, {ixMmax + 1, ixGmax}};
+  const int rS[3][2] = {{ixCoMmin, ixCoMmin - 1 + ng}, {ixCoMmin, ixCoMmax}, {ixCoMmax + 1 - ng, ixCoMmax}};
+  const int rR[4][2] = {{1, ng}, {ixMmin, ixMmin - 1 + nxCo}, {ixMmin + nxCo, ixMmax}, {ixMmax + 1, ixGmax}};
+  const int pS[4][2] = {{ixMmin - (io - 1), ixMmin - 1 + ngCo + (io - 1)},
+                        {ixMmin - (io - 1), ixMmin - 1 + nxCo + ngCo + (io - 1)},
+                        {ixMmin + nxCo - ngCo - (io - 1), ixMmax + (io - 1)},
+                        {ixMmax + 1 - ngCo - (io - 1), ixMmax + (io - 1)}};
+  const int pR[4][2] = {{ixCoMmin - ngCo - (io - 1), ng + (io - 1)},
+                        {ixCoMmin - (io - 1), ixCoMmax + ngCo + (io - 1)},
+                        {ixCoMmin - ngCo - (io - 1), ixCoMmax + (io - 1)},
+                        {ixCoMmax + 1 - (io - 1), ixCoMmax + ngCo + (io - 1)}};
+  std::memcpy(m.srlS, srlS, sizeof(srlS)); std::memcpy(m.srlR, srlR, sizeof(srlR));
+  std::memcpy(m.rS, rS, sizeof(rS)); std::memcpy(m.rR, rR, sizeof(rR));
+  std::memcpy(m.pS, pS, sizeof(pS)); std::memcpy(m.pR, pR, sizeof(pR));
+  return m;
+}
+
+// copy a 1-based box of block-geometry ga array a into geometry gb array b
+inline void copy_box(const Geo &ga, const double *a, const int lo_a[3], const Geo &gb, double *b, const int lo_b[3],
+                     const int ext[3], int nw) {
+  for (int iw = 0; iw < nw; ++iw)
+    for (int k = 0; k < ext[2]; ++k)
+      for (int j = 0; j < ext[1]; ++j)
+        for (int i = 0; i < ext[0]; ++i)
+          b[gb.idx(lo_b[0] - 1 + i, lo_b[1] - 1 + j, lo_b[2] - 1 + k) + gb.cells * (size_t)iw] =
+              a[ga.idx(lo_a[0] - 1 + i, lo_a[1] - 1 + j, lo_a[2] - 1 + k) + ga.cells * (size_t)iw];
+}
+
+void amr_getbc(AmrGrid &G, std::vector<double> &reg) {
+  const int nd = G.ndim, nw = G.s.x.nw;
+  const Geo &g = G.s.g, &gc = G.sc.g;
+  const AmrMaps M = amr_maps();
+  auto has = [&](int b, int t) {
+    for (int q = 0; q < 27; ++q) if (q != 13 && G.ntype[b * 27 + q] == t) return true;
+    return false;
+  };
+  auto dir_of = [&](int q, int *dd) { dd[0] = q % 3 - 1; dd[1] = (q / 3) % 3 - 1; dd[2] = q / 9 - 1; };
+  auto valid_q = [&](int q) {
+    int dd[3];
+    dir_of(q, dd);
+    if (q == 13) return false;
+    for (int d = nd; d < 3; ++d) if (dd[d]) return false;
+    return true;
+  };
+  // coarsen_grid of blocks with a coarser neighbour: psc interior
+  for (int b = 0; b < G.nb; ++b) {
+    if (!has(b, NT_COARSE)) continue;
+    const double *w = &reg[G.bsize * b];
+    double *wc = &G.psc[G.csize * b];
+    const double cofi = 1.0 / double(1 << nd);
+    for (int iw = 0; iw < nw; ++iw)
+      for (int kc = 0; kc < (nd > 2 ? 8 : 1); ++kc)
+        for (int jc = 0; jc < (nd > 1 ? 8 : 1); ++jc)
+          for (int icc = 0; icc < 8; ++icc) {
+            const int i0 = 2 + 2 * icc, j0 = nd > 1 ? 2 + 2 * jc : 0, k0 = nd > 2 ? 2 + 2 * kc : 0;
+            double sum = 0.0;
+            bool first = true;
+            for (int kk = 0; kk < (nd > 2 ? 2 : 1); ++kk)
+              for (int jj = 0; jj < (nd > 1 ? 2 : 1); ++jj)
+                for (int ii = 0; ii < 2; ++ii) {
+                  const double v = w[g.idx(i0 + ii, j0 + jj, k0 + kk) + g.cells * (size_t)iw];
+                  sum = first ? v : sum + v;
+                  first = false;
+                }
+            wc[gc.idx(2 + icc, nd > 1 ? 2 + jc : 0, nd > 2 ? 2 + kc : 0) + gc.cells * (size_t)iw] = sum * cofi;
+          }
+  }
+  // same-level copies (bc_fill_srl) and restriction into coarser neighbours (bc_fill_restrict)
+  for (int b = 0; b < G.nb; ++b)
+    for (int q = 0; q < 27; ++q) {
+      if (!valid_q(q)) continue;
+      int dd[3];
+      dir_of(q, dd);
+      const int t = G.ntype[b * 27 + q];
+      if (t == NT_SIBLING) {
+        const int nbk = G.nid[b * 27 + q];
+        int lo_s[3], lo_r[3], ext[3];
+        for (int d = 0; d < 3; ++d) {
+          if (d < nd) {
+            lo_s[d] = M.srlS[dd[d] + 1][0];
+            lo_r[d] = M.srlR[-dd[d] + 1][0];
+            ext[d] = M.srlS[dd[d] + 1][1] - M.srlS[dd[d] + 1][0] + 1;
+          } else { lo_s[d] = lo_r[d] = 1; ext[d] = 1; }
+        }
+        copy_box(g, &reg[G.bsize * b], lo_s, g, &reg[G.bsize * nbk], lo_r, ext, nw);
+      } else if (t == NT_COARSE) {
+        int ic[3] = {1, 1, 1};
+        bool ok = true;
+        for (int d = 0; d < nd; ++d) {
+          ic[d] = 1 + (G.ig[3 * b + d] % 2);
+          if (!(dd[d] == 0 || dd[d] == 2 * ic[d] - 3)) ok = false;
+        }
+        if (!ok) continue;
+        const int nbk = G.nid[b * 27 + q];
+        int lo_s[3], lo_r[3], ext[3];
+        for (int d = 0; d < 3; ++d) {
+          if (d < nd) {
+            const int ninc = -2 * dd[d] + ic[d];
+            lo_s[d] = M.rS[dd[d] + 1][0];
+            lo_r[d] = M.rR[ninc][0];
+            ext[d] = M.rS[dd[d] + 1][1] - M.rS[dd[d] + 1][0] + 1;
+          } else { lo_s[d] = lo_r[d] = 1; ext[d] = 1; }
+        }
+        copy_box(gc, &G.psc[G.csize * b], lo_s, g, &reg[G.bsize * nbk], lo_r, ext, nw);
+      }
+    }
+  // coarse values into the finer neighbours' psc (bc_fill_prolong)
+  for (int b = 0; b < G.nb; ++b)
+    for (int q = 0; q < 27; ++q) {
+      if (!valid_q(q) || G.ntype[b * 27 + q] != NT_FINE) continue;
+      int dd[3];
+      dir_of(q, dd);
+      int icr[3][2];
+      for (int d = 0; d < 3; ++d) {
+        if (d < nd) { icr[d][0] = 1 + (1 - dd[d]) / 2; icr[d][1] = 2 - (1 + dd[d]) / 2; }
+        else { icr[d][0] = icr[d][1] = 1; }
+      }
+      for (int c2 = icr[2][0]; c2 <= icr[2][1]; ++c2)
+        for (int c1 = icr[1][0]; c1 <= icr[1][1]; ++c1)
+          for (int c0 = icr[0][0]; c0 <= icr[0][1]; ++c0) {
+            const int ic[3] = {c0, c1, c2};
+            const int cbits = (c0 - 1) + 2 * (nd > 1 ? c1 - 1 : 0) + 4 * (nd > 2 ? c2 - 1 : 0);
+            const int chd = G.child[(b * 27 + q) * 8 + cbits];
+            int lo_s[3], lo_r[3], ext[3];
+            for (int d = 0; d < 3; ++d) {
+              if (d < nd) {
+                const int inc = 2 * dd[d] + ic[d], ninc = ic[d] - dd[d];
+                lo_s[d] = M.pS[inc][0];
+                lo_r[d] = M.pR[ninc][0];
+                ext[d] = M.pS[inc][1] - M.pS[inc][0] + 1;
+              } else { lo_s[d] = lo_r[d] = 1; ext[d] = 1; }
+            }
+            copy_box(g, &reg[G.bsize * b], lo_s, gc, &G.psc[G.csize * chd], lo_r, ext, nw);
+          }
+    }
+  // prolongation of ghost cells from coarser neighbours (gc_prolong -> bc_prolong -> interpolation_linear)
+  for (int b = 0; b < G.nb; ++b)
+    for (int q = 0; q < 27; ++q) {
+      if (!valid_q(q) || G.ntype[b * 27 + q] != NT_COARSE) continue;
+      int dd[3];
+      dir_of(q, dd);
+      int lo[3] = {1, 1, 1}, hi[3] = {1, 1, 1};
+      double dxF[3] = {1, 1, 1}, dxC[3] = {1, 1, 1}, invC[3] = {1, 1, 1}, xFmin[3] = {0, 0, 0}, xCmin[3] = {0, 0, 0};
+      for (int d = 0; d < nd; ++d) {
+        lo[d] = M.srlR[dd[d] + 1][0];
+        hi[d] = M.srlR[dd[d] + 1][1];
+        dxF[d] = G.dx(b, d);
+        dxC[d] = 2.0 * dxF[d];
+        invC[d] = 1.0 / dxC[d];
+        xFmin[d] = G.bxmin(b, d) - 2.0 * dxF[d];
+        xCmin[d] = G.bxmin(b, d) - 2.0 * dxC[d];
+      }
+      const double *wc = &G.psc[G.csize * b];
+      double *w = &reg[G.bsize * b];
+      for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+          for (int i = lo[0]; i <= hi[0]; ++i) {
+            const int ixF[3] = {i, j, k};
+            int ixC[3] = {1, 1, 1};
+            double eta[3] = {0, 0, 0};
+            for (int d = 0; d < nd; ++d) {
+              const double xF = xFmin[d] + (double(ixF[d]) - 0.5) * dxF[d];
+              ixC[d] = int((xF - xCmin[d]) * invC[d]) + 1;
+              const double xC = xCmin[d] + (double(ixC[d]) - 0.5) * dxC[d];
+              eta[d] = (xF - xC) * invC[d];
+            }
+            for (int iw = 0; iw < nw; ++iw) {
+              auto C = [&](int a, int bb, int cc) {
+                return wc[gc.idx(a - 1, nd > 1 ? bb - 1 : 0, nd > 2 ? cc - 1 : 0) + gc.cells * (size_t)iw];
+              };
+              const double c0 = C(ixC[0], ixC[1], ixC[2]);
+              double slope[3] = {0, 0, 0};
+              for (int d = 0; d < nd; ++d) {
+                int h[3] = {ixC[0], ixC[1], ixC[2]}, jx[3] = {ixC[0], ixC[1], ixC[2]};
+                h[d] -= 1;
+                jx[d] += 1;
+                const double slopeL = c0 - C(h[0], h[1], h[2]);
+                const double slopeR = C(jx[0], jx[1], jx[2]) - c0;
+                const double slopeC = 0.5 * (slopeR + slopeL);
+                const double signC = std::copysign(1.0, slopeC);
+                slope[d] = signC * std::max(0.0, std::min(std::min(std::fabs(slopeC), signC * slopeL), signC * slopeR));
+              }
+              // psc(ixCo) + (slope_1 eta_1) + (slope_2 eta_2) + ..., left to right
+              double v = c0;
+              for (int d = 0; d < nd; ++d) v = v + slope[d] * eta[d];
+              w[g.idx(ixF[0] - 1, nd > 1 ? ixF[1] - 1 : 0, nd > 2 ? ixF[2] - 1 : 0) + g.cells * (size_t)iw] = v;
+            }
+          }
+    }
+}
+
+// store_flux (src/mod_fix_conserve.t:597-648) for one block from its scaled face fluxes.
+void amr_store_flux(AmrGrid &G, int b, const std::vector<Arr<double>> &fC) {
+  const int nd = G.ndim, nw = G.s.x.nw;
+  for (int d = 0; d < nd; ++d)
+    for (int side = 0; side < 2; ++side) {
+      int dd[3] = {0, 0, 0};
+      dd[d] = side ? 1 : -1;
+      const int t = G.ntype[b * 27 + q27(dd)];
+      std::vector<double> &pf = G.pflux[b * 6 + 2 * d + side];
+      const int t1 = (d + 1) % 3 < nd ? (d + 1) % 3 : -1, t2 = (d + 2) % 3 < nd ? (d + 2) % 3 : -1;
+      // tangential dimensions in increasing order
+      int ta = -1, tb = -1;
+      for (int e = 0; e < nd; ++e) if (e != d) { if (ta < 0) ta = e; else tb = e; }
+      (void)t1; (void)t2;
+      const int iface = side ? 17 : 1;  // 0-based face index: right face of cell iface
+      if (t == NT_FINE) {
+        const int n1 = ta >= 0 ? 16 : 1, n2 = tb >= 0 ? 16 : 1;
+        pf.assign((size_t)nw * n1 * n2, 0.0);
+        for (int iw = 0; iw < nw; ++iw)
+          for (int b2 = 0; b2 < n2; ++b2)
+            for (int a1 = 0; a1 < n1; ++a1) {
+              int c[3] = {0, 0, 0};
+              c[d] = iface;
+              if (ta >= 0) c[ta] = 2 + a1;
+              if (tb >= 0) c[tb] = 2 + b2;
+              const double f = fC[d](c[0], c[1], c[2], iw);
+              pf[((size_t)iw * n2 + b2) * n1 + a1] = side ? f : -f;
+            }
+      } else if (t == NT_COARSE) {
+        const int n1 = ta >= 0 ? 8 : 1, n2 = tb >= 0 ? 8 : 1;
+        pf.assign((size_t)nw * n1 * n2, 0.0);
+        for (int iw = 0; iw < nw; ++iw)
+          for (int b2 = 0; b2 < n2; ++b2)
+            for (int a1 = 0; a1 < n1; ++a1) {
+              double sum = 0.0;
+              bool first = true;
+              for (int y = 0; y < (tb >= 0 ? 2 : 1); ++y)
+                for (int x = 0; x < (ta >= 0 ? 2 : 1); ++x) {
+                  int c[3] = {0, 0, 0};
+                  c[d] = iface;
+                  if (ta >= 0) c[ta] = 2 + 2 * a1 + x;
+                  if (tb >= 0) c[tb] = 2 + 2 * b2 + y;
+                  const double f = fC[d](c[0], c[1], c[2], iw);
+                  sum = first ? f : sum + f;
+                  first = false;
+                }
+              pf[((size_t)iw * n2 + b2) * n1 + a1] = side ? -sum : sum;
+            }
+      } else {
+        pf.clear();
+      }
+    }
+}
+
+// fix_conserve (src/mod_fix_conserve.t:465-595) on one register.
+void amr_fix_conserve(AmrGrid &G, std::vector<double> &reg) {
+  const int nd = G.ndim, nw = G.s.x.nw;
+  const Geo &g = G.s.g;
+  const double cofi = 1.0 / double(1 << nd);
+  for (int b = 0; b < G.nb; ++b)
+    for (int d = 0; d < nd; ++d)
+      for (int side = 0; side < 2; ++side) {
+        int dd[3] = {0, 0, 0};
+        dd[d] = side ? 1 : -1;
+        const int q = q27(dd);
+        if (G.ntype[b * 27 + q] != NT_FINE) continue;
+        int ta = -1, tb = -1;
+        for (int e = 0; e < nd; ++e) if (e != d) { if (ta < 0) ta = e; else tb = e; }
+        const int ix = side ? 17 : 2;  // 0-based boundary cell
+        double *w = &reg[G.bsize * b];
+        const std::vector<double> &pc = G.pflux[b * 6 + 2 * d + side];
+        const int n1 = ta >= 0 ? 16 : 1, n2 = tb >= 0 ? 16 : 1;
+        for (int iw = 0; iw < nw; ++iw)
+          for (int b2 = 0; b2 < n2; ++b2)
+            for (int a1 = 0; a1 < n1; ++a1) {
+              int c[3] = {0, 0, 0};
+              c[d] = ix;
+              if (ta >= 0) c[ta] = 2 + a1;
+              if (tb >= 0) c[tb] = 2 + b2;
+              double &v = w[g.idx(c[0], c[1], c[2]) + g.cells * (size_t)iw];
+              v = v - pc[((size_t)iw * n2 + b2) * n1 + a1];
+            }
+        // children adjacent across the face
+        for (int c2 = 1; c2 <= (tb >= 0 ? 2 : 1); ++c2)
+          for (int c1 = 1; c1 <= (ta >= 0 ? 2 : 1); ++c1) {
+            int ic[3] = {1, 1, 1};
+            ic[d] = side ? 1 : 2;
+            if (ta >= 0) ic[ta] = c1;
+            if (tb >= 0) ic[tb] = c2;
+            const int cbits = (ic[0] - 1) + 2 * (nd > 1 ? ic[1] - 1 : 0) + 4 * (nd > 2 ? ic[2] - 1 : 0);
+            const int chd = G.child[(b * 27 + q) * 8 + cbits];
+            const std::vector<double> &pf = G.pflux[chd * 6 + 2 * d + (1 - side)];
+            const int m1 = ta >= 0 ? 8 : 1, m2 = tb >= 0 ? 8 : 1;
+            for (int iw = 0; iw < nw; ++iw)
+              for (int b2 = 0; b2 < m2; ++b2)
+                for (int a1 = 0; a1 < m1; ++a1) {
+                  int c[3] = {0, 0, 0};
+                  c[d] = ix;
+                  if (ta >= 0) c[ta] = 2 + (c1 - 1) * 8 + a1;
+                  if (tb >= 0) c[tb] = 2 + (c2 - 1) * 8 + b2;
+                  double &v = w[g.idx(c[0], c[1], c[2]) + g.cells * (size_t)iw];
+                  v = v + pf[((size_t)iw * m2 + b2) * m1 + a1] * cofi;
+                }
+          }
+      }
+}
+
+int amr_advect1(AmrGrid &G, int ra, int rb, double qdt, double dtfactor, double cmax_global, int nthreads) {
+  int st = 0;
+  const size_t bs = G.bsize;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic) reduction(| : st)
+#endif
+  for (int b = 0; b < G.nb; ++b) {
+    Arr<double> a = wrap_in(G.s.g, G.s.x.nw, &G.reg[ra][bs * b]);
+    Arr<double> w = wrap_in(G.s.g, G.s.x.nw, &G.reg[rb][bs * b]);
+    double dxb[3];
+    for (int d = 0; d < 3; ++d) dxb[d] = d < G.ndim ? G.dx(b, d) : 1.0;
+    std::vector<Arr<double>> fc;
+    st |= finite_volume(G.s, a, w, qdt, dtfactor, dxb, cmax_global, &fc);
+    std::memcpy(&G.reg[rb][bs * b], w.d.data(), sizeof(double) * bs);
+    amr_store_flux(G, b, fc);
+  }
+  amr_fix_conserve(G, G.reg[rb]);
+  amr_getbc(G, G.reg[rb]);
+  return st;
+}
+
+}  // namespace orc
+
+extern "C" {
+
+orc_amr *orc_amr_create(const orc_cfg *cfg, const int *nbase, const double *xprobmin, const double *xprobmax,
+                        int nleaf, const int *leaf /* [nleaf][4]: level, ig0, ig1, ig2 */) {
+  AmrGrid *G = new AmrGrid();
+  G->s = make_state(*cfg);
+  orc_cfg c8 = *cfg;
+  for (int d = 0; d < 3; ++d) c8.block_nx[d] = d < cfg->ndim ? 8 : 1;
+  G->sc = make_state(c8);
+  G->ndim = cfg->ndim;
+  G->nb = nleaf;
+  for (int d = 0; d < 3; ++d) {
+    G->nbase[d] = d < cfg->ndim ? nbase[d] : 1;
+    G->xmin[d] = d < cfg->ndim ? xprobmin[d] : 0.0;
+    G->xmax[d] = d < cfg->ndim ? xprobmax[d] : 1.0;
+  }
+  G->level.resize(nleaf);
+  G->ig.resize(3 * (size_t)nleaf);
+  std::map<std::array<int, 4>, int> key;
+  for (int b = 0; b < nleaf; ++b) {
+    G->level[b] = leaf[4 * b];
+    for (int d = 0; d < 3; ++d) G->ig[3 * b + d] = d < cfg->ndim ? leaf[4 * b + 1 + d] : 0;
+    key[{G->level[b], G->ig[3 * b], G->ig[3 * b + 1], G->ig[3 * b + 2]}] = b;
+  }
+  auto find = [&](int l, const int *jg) -> int {
+    auto it = key.find({l, jg[0], jg[1], jg[2]});
+    return it == key.end() ? -1 : it->second;
+  };
+  G->ntype.assign(27 * (size_t)nleaf, NT_BOUNDARY);
+  G->nid.assign(27 * (size_t)nleaf, -1);
+  G->child.assign(27 * 8 * (size_t)nleaf, -1);
+  const int nd = cfg->ndim;
+  for (int b = 0; b < nleaf; ++b) {
+    const int l = G->level[b];
+    for (int q = 0; q < 27; ++q) {
+      int dd[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
+      bool ok = true;
+      int jg[3] = {0, 0, 0};
+      for (int d = 0; d < 3; ++d) {
+        if (d >= nd) { if (dd[d]) ok = false; continue; }
+        const int nl = G->nbase[d] << (l - 1);
+        jg[d] = ((G->ig[3 * b + d] + dd[d]) % nl + nl) % nl;  // periodic
+      }
+      if (!ok) continue;
+      if (q == 13) { G->ntype[b * 27 + q] = NT_SIBLING; G->nid[b * 27 + q] = b; continue; }
+      int s2 = find(l, jg);
+      if (s2 >= 0) { G->ntype[b * 27 + q] = NT_SIBLING; G->nid[b * 27 + q] = s2; continue; }
+      int pg[3] = {jg[0] / 2, nd > 1 ? jg[1] / 2 : 0, nd > 2 ? jg[2] / 2 : 0};
+      int cb = l > 1 ? find(l - 1, pg) : -1;
+      if (cb >= 0) { G->ntype[b * 27 + q] = NT_COARSE; G->nid[b * 27 + q] = cb; continue; }
+      G->ntype[b * 27 + q] = NT_FINE;
+      for (int cbits = 0; cbits < 8; ++cbits) {
+        int cg[3] = {2 * jg[0] + (cbits & 1), nd > 1 ? 2 * jg[1] + ((cbits >> 1) & 1) : 0,
+                     nd > 2 ? 2 * jg[2] + ((cbits >> 2) & 1) : 0};
+        if ((nd < 2 && (cbits & 2)) || (nd < 3 && (cbits & 4))) continue;
+        G->child[(b * 27 + q) * 8 + cbits] = find(l + 1, cg);
+      }
+    }
+  }
+  G->bsize = G->s.g.cells * (size_t)G->s.x.nw;
+  G->csize = G->sc.g.cells * (size_t)G->s.x.nw;
+  for (int r = 0; r < 3; ++r) G->reg[r].assign(G->bsize * nleaf, 0.0);
+  G->psc.assign(G->csize * nleaf, 0.0);
+  G->pflux.assign(6 * (size_t)nleaf, {});
+  return reinterpret_cast<orc_amr *>(G);
+}
+
+void orc_amr_destroy(orc_amr *a) { delete reinterpret_cast<AmrGrid *>(a); }
+
+int orc_amr_neighbors(const orc_amr *a, int *ntype, int *nid, int *child) {
+  const AmrGrid *G = reinterpret_cast<const AmrGrid *>(a);
+  std::memcpy(ntype, G->ntype.data(), sizeof(int) * G->ntype.size());
+  std::memcpy(nid, G->nid.data(), sizeof(int) * G->nid.size());
+  if (child) std::memcpy(child, G->child.data(), sizeof(int) * G->child.size());
+  return G->nb;
+}
+
+void orc_amr_set_block(orc_amr *a, int b, const double *w) {
+  AmrGrid *G = reinterpret_cast<AmrGrid *>(a);
+  std::memcpy(&G->reg[0][G->bsize * b], w, sizeof(double) * G->bsize);
+}
+
+void orc_amr_get_block(const orc_amr *a, int reg, int b, double *w) {
+  const AmrGrid *G = reinterpret_cast<const AmrGrid *>(a);
+  std::memcpy(w, &G->reg[reg][G->bsize * b], sizeof(double) * G->bsize);
+}
+
+void orc_amr_getbc(orc_amr *a) {
+  AmrGrid *G = reinterpret_cast<AmrGrid *>(a);
+  amr_getbc(*G, G->reg[0]);
+}
+
+int orc_amr_getdt(orc_amr *a, double *dt, double *cmax_global) {
+  AmrGrid *G = reinterpret_cast<AmrGrid *>(a);
+  double dtmin = bigdouble, cmx = 0.0;
+  int st = 0;
+  for (int b = 0; b < G->nb; ++b) {
+    Arr<double> w = wrap_in(G->s.g, G->s.x.nw, &G->reg[0][G->bsize * b]);
+    double dxb[3];
+    for (int d = 0; d < 3; ++d) dxb[d] = d < G->ndim ? G->dx(b, d) : 1.0;
+    double dtn;
+    st |= getdt_block(G->s, w, dxb, &dtn, &cmx);
+    dtmin = std::min(dtmin, dtn);
+  }
+  *dt = dtmin;
+  *cmax_global = cmx;
+  return st;
+}
+
+// One stage reg_a -> reg_b (reg_b holds the RK base combination on entry),
+// flux correction and multi-level getbc on reg_b.
+int orc_amr_advect1(orc_amr *a, int ra, int rb, double qdt, double dtfactor, double cmax_global, int nthreads) {
+  return amr_advect1(*reinterpret_cast<AmrGrid *>(a), ra, rb, qdt, dtfactor, cmax_global, nthreads);
+}
+
+void orc_amr_combine_reg(orc_amr *a, int dst, double ca, int ra, double cb, int rb) {
+  AmrGrid *G = reinterpret_cast<AmrGrid *>(a);
+  for (size_t p = 0; p < G->reg[dst].size(); ++p) G->reg[dst][p] = ca * G->reg[ra][p] + cb * G->reg[rb][p];
+}
+
+int orc_amr_advance(orc_amr *a, double dt, double cmax_global, int nthreads) {
+  AmrGrid *G = reinterpret_cast<AmrGrid *>(a);
+  double b11, b22, b33, a21, a31;
+  if (G->s.c.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
+  else { b11 = 1.0; b22 = 1.0 / 4.0; b33 = 2.0 / 3.0; a21 = 3.0 / 4.0; a31 = 1.0 / 3.0; }
+  int st = 0;
+  G->reg[1] = G->reg[0];
+  st |= amr_advect1(*G, 0, 1, b11 * dt, b11, cmax_global, nthreads);
+  orc_amr_combine_reg(a, 2, a21, 0, 1.0 - a21, 1);
+  st |= amr_advect1(*G, 1, 2, b22 * dt, b22, cmax_global, nthreads);
+  orc_amr_combine_reg(a, 0, a31, 0, 1.0 - a31, 2);
+  st |= amr_advect1(*G, 2, 0, b33 * dt, b33, cmax_global, nthreads);
+  return st;
 }
 
 }  // extern "C"

@@ -175,6 +175,25 @@ void orc_lohner_block(const orc_cfg *cfg, const double *w, const double *weight,
                       double wavefilter, double threshold, double derefine, int level, int refine_max_level,
                       double *error, int *refine, int *coarsen);
 
+/* --- multi-level (AMR) grid: a static 2:1-balanced hierarchy of leaves --- */
+typedef struct orc_amr orc_amr;
+/* leaf[4*b] = level (1-based), leaf[4*b+1..3] = block index at that level
+ * (0-based); nbase: level-1 blocks per direction; periodic boundaries. */
+orc_amr *orc_amr_create(const orc_cfg *cfg, const int *nbase, const double *xprobmin,
+                        const double *xprobmax, int nleaf, const int *leaf);
+void orc_amr_destroy(orc_amr *a);
+/* ntype[b*27+q]: 0 boundary, 1 coarse, 2 sibling, 3 fine; nid: the sibling or
+ * coarse block; child[(b*27+q)*8 + cbits]: fine neighbours by child position. */
+int orc_amr_neighbors(const orc_amr *a, int *ntype, int *nid, int *child);
+void orc_amr_set_block(orc_amr *a, int b, const double *w);
+void orc_amr_get_block(const orc_amr *a, int reg, int b, double *w);
+void orc_amr_getbc(orc_amr *a);
+int orc_amr_getdt(orc_amr *a, double *dt, double *cmax_global);
+int orc_amr_advect1(orc_amr *a, int reg_a, int reg_b, double qdt, double dtfactor, double cmax_global,
+                    int nthreads);
+void orc_amr_combine_reg(orc_amr *a, int dst, double ca, int ra, double cb, int rb);
+int orc_amr_advance(orc_amr *a, double dt, double cmax_global, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

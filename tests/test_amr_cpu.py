@@ -1,0 +1,139 @@
+"""The oracle's multi-level grid (restated multi-level getbc and flux fix).
+
+* Linear conserved fields: every ghost cell of every block away from the
+  periodic wrap equals the field at its centre after getbc — same-level
+  copies, restriction (averages of fine cells) and prolongation (psc with
+  monotonized-central slopes) are all exact for linear data.
+* The flux correction makes the multi-level update conservative: totals of
+  every conserved variable stay constant to rounding on a periodic domain.
+* A hierarchy refined everywhere is the uniform finer grid, bit for bit.
+"""
+import numpy as np
+import pytest
+
+from tests import _amr as A
+
+
+def _cfg(O, nd, **kw):
+    base = dict(physics="hd", ndim=nd, gamma=1.4, flux_scheme="hllc", limiter="vanleer", courantpar=0.8)
+    base.update(kw)
+    return O.make_cfg(**base)
+
+
+def _nbase(nd):
+    return [8] * nd if nd == 2 else [4] * nd
+
+
+def _leaves(nd, levels=3):
+    def ref(c, lv):
+        r = np.linalg.norm(c - 0.5)
+        return r < (0.3 if lv == 1 else 0.15)
+    return A.build_leaves(nd, _nbase(nd), levels, ref)
+
+
+def _lin(nd):
+    def f(X, Y, Z):
+        out = np.zeros((nd + 2,) + X.shape)
+        out[0] = 1.0 + 0.1 * X + 0.2 * Y + (0.05 * Z if nd > 2 else 0)
+        out[1] = 0.1 + 0.05 * X - 0.02 * Y
+        out[2] = -0.1 * Y + 0.03 * X
+        if nd > 2:
+            out[3] = 0.02 * Z - 0.01 * X
+        out[nd + 1] = 3.0 + 0.2 * X - 0.1 * Y + (0.04 * Z if nd > 2 else 0)
+        return out
+    return f
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_ghost_cells_exact_for_linear_data(oracle_lib, nd):
+    O = oracle_lib
+    leaves = _leaves(nd, levels=3 if nd == 2 else 2)
+    assert len({l[0] for l in leaves}) == (3 if nd == 2 else 2)
+    c = _cfg(O, nd)
+    nb = _nbase(nd)
+    g = O.AmrGrid(c, nb, [0.0] * nd, [1.0] * nd, leaves)
+    blocks = A.fill_blocks(leaves, nd, nb, _lin(nd), "hd", nd, 1.4, conserved=True)
+    for b in range(len(leaves)):
+        g.set_block(b, blocks[b])
+    # scramble the ghost cells so that only getbc can make them right
+    for b in range(len(leaves)):
+        w = blocks[b].copy()
+        sl = (slice(None),) + tuple(slice(2, 18) if d < nd else slice(None) for d in (2, 1, 0))
+        z = np.full_like(w, -7.0)
+        z[sl] = w[sl]
+        g.set_block(b, z)
+    g.getbc()
+    checked = 0
+    for b, leaf in enumerate(leaves):
+        lv, ig = leaf[0], leaf[1:]
+        n = nb[0] << (lv - 1)
+        if any(i == 0 or i == n - 1 for i in ig):
+            continue  # the periodic wrap breaks a linear field
+        got = g.get_block(b)
+        assert np.allclose(got, blocks[b], rtol=0, atol=1e-13), (leaf, np.abs(got - blocks[b]).max())
+        checked += 1
+    assert checked > 0
+
+
+def _periodic(nd):
+    def f(X, Y, Z):
+        out = np.zeros((nd + 2,) + X.shape)
+        s = np.sin(2 * np.pi * X) * np.cos(2 * np.pi * Y) * (np.cos(2 * np.pi * Z) if nd > 2 else 1)
+        out[0] = 1.0 + 0.3 * s
+        out[1] = 0.5 + 0.2 * np.cos(2 * np.pi * Y)
+        out[2] = -0.3 + 0.2 * np.sin(2 * np.pi * X)
+        if nd > 2:
+            out[3] = 0.1 * np.sin(2 * np.pi * Y)
+        out[nd + 1] = 1.0 + 0.2 * s
+        return out
+    return f
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_flux_fix_conserves(oracle_lib, nd):
+    O = oracle_lib
+    leaves = _leaves(nd, levels=3 if nd == 2 else 2)
+    c = _cfg(O, nd)
+    nb = _nbase(nd)
+    g = O.AmrGrid(c, nb, [0.0] * nd, [1.0] * nd, leaves)
+    blocks = A.fill_blocks(leaves, nd, nb, _periodic(nd), "hd", nd, 1.4)
+    for b in range(len(leaves)):
+        g.set_block(b, blocks[b])
+    g.getbc()
+    sl = (slice(None),) + tuple(slice(2, 18) if d < nd else slice(None) for d in (2, 1, 0))
+
+    def totals():
+        return sum(g.get_block(b)[sl].reshape(nd + 2, -1).sum(axis=1) * A.block_volume(l, nd, nb)
+                   for b, l in enumerate(leaves))
+    t0 = totals()
+    for _ in range(4 if nd == 2 else 2):
+        dt, _ = g.getdt()
+        g.advance(dt)
+    t1 = totals()
+    assert np.all(np.abs(t1 - t0) <= 1e-13 * np.abs(t0).max()), (t0, t1)
+
+
+def test_refined_everywhere_is_the_uniform_grid(oracle_lib):
+    O = oracle_lib
+    nd = 2
+    leaves = A.build_leaves(nd, [2, 2], 2, lambda c, lv: True)
+    assert all(l[0] == 2 for l in leaves) and len(leaves) == 16
+    c = _cfg(O, nd)
+    g = O.AmrGrid(c, [2, 2], [0.0, 0.0], [1.0, 1.0], leaves)
+    blocks = A.fill_blocks(leaves, nd, [2, 2], _periodic(nd), "hd", nd, 1.4)
+    u = O.Grid(c, [64, 64], [0.0, 0.0], [1.0, 1.0], ["periodic"] * 4)
+    order = {}
+    for b, l in enumerate(leaves):
+        g.set_block(b, blocks[b])
+        order[b] = l[1] + 4 * l[2]
+        u.set_block(order[b], blocks[b])
+    g.getbc()
+    u.getbc()
+    for _ in range(3):
+        dt, _ = u.getdt()
+        dta, _ = g.getdt()
+        assert dt == dta
+        g.advance(dt)
+        u.advance(dt)
+    for b in range(len(leaves)):
+        assert np.array_equal(g.get_block(b), u.get_block(order[b]))
