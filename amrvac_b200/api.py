@@ -70,6 +70,25 @@ class Context:
             self.h, d.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(a), _dp(b)), "set_uniform_grid")
         self.nblocks = self.L.amrvac_gpu_nblocks(self.h)
 
+    def set_amr_grid(self, leaves, nbase, xprobmin, xprobmax):
+        """Static multi-level grid: leaves [(level, ig0, ig1[, ig2])] of a 2:1
+        balanced tree over nbase root blocks per direction (periodic)."""
+        nd = self.cfg.ndim
+        lv = np.zeros((len(leaves), 4), np.int32)
+        for b, t in enumerate(leaves):
+            lv[b, :len(t)] = t
+        nb = np.ascontiguousarray(list(nbase)[:nd] + [1] * (3 - nd), dtype=np.int32)
+        a = np.ascontiguousarray(list(xprobmin)[:nd] + [0.0] * (3 - nd), dtype=np.float64)
+        b = np.ascontiguousarray(list(xprobmax)[:nd] + [1.0] * (3 - nd), dtype=np.float64)
+        ip = ctypes.POINTER(ctypes.c_int)
+        _lib.check(self.L.amrvac_gpu_set_amr_grid(self.h, len(leaves), lv.ctypes.data_as(ip), nb.ctypes.data_as(ip),
+                                                  _dp(a), _dp(b)), "set_amr_grid")
+        self.nblocks = self.L.amrvac_gpu_nblocks(self.h)
+
+    @property
+    def amr_slots(self):
+        return self.L.amrvac_gpu_amr_slots(self.h)
+
     def set_blocks(self, dx, neighbor):
         dx = np.ascontiguousarray(dx, dtype=np.float64)
         nb = np.ascontiguousarray(neighbor, dtype=np.int32)
@@ -80,7 +99,11 @@ class Context:
 
     def upload(self, w: np.ndarray, reg="ps", first=0):
         w = np.ascontiguousarray(w, dtype=np.float64)
+        if w.ndim != 1 + len(self.block_shape) or tuple(w.shape[1:]) != tuple(self.block_shape):
+            raise ValueError(f"upload: blocks of shape {tuple(self.block_shape)} expected, got {w.shape[1:]}")
         n = w.shape[0]
+        if first < 0 or first + n > self.nblocks:
+            raise ValueError(f"upload: blocks {first}..{first + n - 1} outside 0..{self.nblocks - 1}")
         _lib.check(self.L.amrvac_gpu_upload(self.h, REG.get(reg, reg), first, n, _dp(w)), "upload")
 
     def download(self, reg="ps", first=0, n=None) -> np.ndarray:

@@ -25,4 +25,35 @@ struct LohnerArgs {
 
 cudaError_t launch_lohner(const LohnerArgs &A, int ndim, cudaStream_t s);
 
+// Static multi-level grid (level jumps between leaf blocks, 2:1 balanced,
+// periodic domain).  Neighbour kinds per block and direction.
+enum : int { AMR_BOUNDARY = 0, AMR_COARSE = 1, AMR_SIBLING = 2, AMR_FINE = 3 };
+
+struct AmrGhostArgs {
+  const double *u;          // the register whose ghosts are needed
+  double *gbuf;             // [slot][var][gz][gy][gx]
+  int nw;
+  const int *iblocks;       // [nslots] block of each slot
+  const int *ntype;         // [nblocks*27]
+  const int *level;         // [nblocks] 1-based
+  const int *ig;            // [nblocks*3] block index at its level
+  const double *bxmin;      // [nblocks*3] lower corner
+  const double *dxb;        // [nblocks*3] cell size
+  const int *owner;         // per level: leaf id, -2 refined, -1 covered by a coarser leaf
+  int owner_off[AMR_MAX_LEVELS + 2];
+  int nlev[AMR_MAX_LEVELS + 2][3];  // blocks per direction per level
+  int maxlevel;
+  uint32_t *status;
+};
+
+struct AmrFixArgs {
+  double *w;                // the stage's output register
+  const double *pflux;      // [slot][2*ndim][var][16*16]
+  int nw;
+  const int *iblocks, *gslot, *ntype, *child;  // child[(b*27+q)*8 + cbits]
+};
+
+cudaError_t launch_amr_ghosts(const AmrGhostArgs &A, int nslots, int ndim, cudaStream_t s);
+cudaError_t launch_amr_fix(const AmrFixArgs &A, int nslots, int ndim, cudaStream_t s);
+
 }  // namespace amrvac

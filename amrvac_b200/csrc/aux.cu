@@ -36,7 +36,7 @@ __global__ void unpack_kernel(const double *__restrict__ src, double *__restrict
 // (src/mod_boundary_conditions.t:12-265, applied per dimension).
 __global__ void pack_kernel(const double *__restrict__ pool, double *__restrict__ dst, int first, int n,
                             int nw, int ndim, int ng, const int *__restrict__ nbr, SrlMaps maps,
-                            BcSpec bc) {
+                            BcSpec bc, const double *__restrict__ gbuf) {
   const int gx = BN + 2 * ng, gy = ndim >= 2 ? BN + 2 * ng : 1, gz = ndim >= 3 ? BN + 2 * ng : 1;
   const size_t per_block_g = (size_t)gx * gy * gz;
   const size_t per_block = (size_t)BN * (ndim >= 2 ? BN : 1) * (ndim >= 3 ? BN : 1);
@@ -60,7 +60,7 @@ __global__ void pack_kernel(const double *__restrict__ pool, double *__restrict_
       int fd[3] = {0, 0, 0};
       fd[d] = q;
       const int nf = nbr[b * 27 + (fd[0] + 1) + 3 * (fd[1] + 1) + 9 * (fd[2] + 1)];
-      if (nf < 0) {
+      if (nf == -1) {
         const int side = q < 0 ? 0 : 1;
         if (bc.kind[2 * d + side] == 1) {  // cont
           g[d] = q < 0 ? ng : ng + BN - 1;
@@ -75,6 +75,15 @@ __global__ void pack_kernel(const double *__restrict__ pool, double *__restrict_
     int src = b;
     if (dir[0] | dir[1] | dir[2]) {
       src = nbr[b * 27 + (dir[0] + 1) + 3 * (dir[1] + 1) + 9 * (dir[2] + 1)];
+      if (src <= -2 && gbuf && ng == 2) {  // level jump: the block's ghost buffer (2 layers)
+        const int G = BN + 4, gy2 = ndim >= 2 ? G : 1, gz2 = ndim >= 3 ? G : 1;
+        const size_t gcell = e - (size_t)lb * per_block_g;
+        const size_t gofs = ((size_t)(ndim >= 3 ? g[2] : 0) * gy2 + (ndim >= 2 ? g[1] : 0)) * G + g[0];
+        for (int v = 0; v < nw; ++v)
+          dst[((size_t)lb * nw + v) * per_block_g + gcell] =
+              gbuf[((size_t)(-2 - src) * nw + v) * (size_t)(G * gy2 * gz2) + gofs];
+        continue;
+      }
       if (src < 0) {  // inconsistent neighbour table: never read out of bounds
         for (int v = 0; v < nw; ++v) dst[((size_t)lb * nw + v) * per_block_g + (e - (size_t)lb * per_block_g)] = 0.0;
         continue;
@@ -180,8 +189,8 @@ cudaError_t launch_unpack(const double *src, double *pool, int first, int n, int
   return cudaGetLastError();
 }
 cudaError_t launch_pack(const double *pool, double *dst, int first, int n, int nw, int ndim, int ng,
-                        const int *nbr, const SrlMaps &maps, const BcSpec &bc, cudaStream_t s) {
-  pack_kernel<<<592, 256, 0, s>>>(pool, dst, first, n, nw, ndim, ng, nbr, maps, bc);
+                        const int *nbr, const SrlMaps &maps, const BcSpec &bc, const double *gbuf, cudaStream_t s) {
+  pack_kernel<<<592, 256, 0, s>>>(pool, dst, first, n, nw, ndim, ng, nbr, maps, bc, gbuf);
   return cudaGetLastError();
 }
 cudaError_t launch_setdt_finalize(unsigned long long *red, double *scal, uint32_t *status, cudaStream_t s) {

@@ -25,7 +25,7 @@ cudaError_t measure_fp64_peak(double *tflops);
 cudaError_t launch_unpack(const double *src, double *pool, int first, int n, int nw, int ndim, int ng,
                           cudaStream_t s);
 cudaError_t launch_pack(const double *pool, double *dst, int first, int n, int nw, int ndim, int ng,
-                        const int *nbr, const SrlMaps &maps, const BcSpec &bc, cudaStream_t s);
+                        const int *nbr, const SrlMaps &maps, const BcSpec &bc, const double *gbuf, cudaStream_t s);
 cudaError_t launch_setdt_finalize(unsigned long long *red, double *scal, uint32_t *status, cudaStream_t s);
 cudaError_t launch_advance_time(double *scal, cudaStream_t s);
 cudaError_t launch_restore_blocks(const double *wct, double *wnew, const uint32_t *block_status, int nblocks,

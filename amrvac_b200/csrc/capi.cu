@@ -89,6 +89,27 @@ struct amrvac_ctx {
   int *d_amr_int = nullptr;            // [2][nblocks] levels, flags (Löhner, lazily)
   double *d_amr_err = nullptr;         // [nblocks] largest error per block
   bool adj_prepared = false;
+  struct AmrDev *amr = nullptr;        // multi-level grid (amrvac_gpu_set_amr_grid)
+};
+
+// Device copy of a static multi-level grid: neighbour kinds, per-level owner
+// maps, ghost buffers of the blocks next to a level jump and their boundary
+// face fluxes.
+struct AmrDev {
+  int nslots = 0;
+  int *d_int = nullptr;       // iblocks, gslot, face, ntype, level, ig, child, owner
+  double *d_bxmin = nullptr;  // [nblocks*3]
+  double *gbuf = nullptr;     // [slot][var][20^d]
+  double *pflux = nullptr;    // [slot][2*ndim][var][256]
+  AmrGhostArgs G;
+  AmrFixArgs F;
+  int *d_face = nullptr, *d_gslot = nullptr;
+  ~AmrDev() {
+    cudaFree(d_int);
+    cudaFree(d_bxmin);
+    cudaFree(gbuf);
+    cudaFree(pflux);
+  }
 };
 
 namespace {
@@ -122,10 +143,28 @@ StageArgs stage_args(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, doubl
   A.status = c->d_status;
   A.block_status = c->d_block_status;
   A.P = c->P;
+  if (c->amr) {
+    A.gbuf = c->amr->gbuf;
+    A.pflux = c->amr->pflux;
+    A.gslot = c->amr->d_gslot;
+    A.amr_face = c->amr->d_face;
+  }
   return A;
 }
 
+// Ghost values of the level-jump directions of register reg (restriction and
+// prolongation) into the ghost buffers.
+int launch_amr_ghost_pass(amrvac_ctx *c, int reg) {
+  AmrGhostArgs G = c->amr->G;
+  G.u = c->pool[reg];
+  CK(launch_amr_ghosts(G, c->amr->nslots, c->cfg.ndim, c->stream));
+  ++c->launches;
+  return 0;
+}
+
 int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a, double b, double dtfactor) {
+  if (c->amr)
+    if (int r = launch_amr_ghost_pass(c, reg_ct)) return r;
   StageArgs A = stage_args(c, reg_ct, reg_new, reg_base, a, b, dtfactor);
   const long planes = (long)c->nblocks * (c->cfg.ndim == 3 ? 16 : 1);
   int nctas;
@@ -138,6 +177,12 @@ int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a,
   if (c->P.fix_small_values && c->P.small_values_method == 0) {
     CK(launch_restore_blocks(c->pool[reg_ct], c->pool[reg_new], c->d_block_status, c->nblocks,
                              c->per_block * c->nw, c->stream));
+    ++c->launches;
+  }
+  if (c->amr) {  // fix_conserve on the stage's output
+    AmrFixArgs F = c->amr->F;
+    F.w = c->pool[reg_new];
+    CK(launch_amr_fix(F, c->amr->nslots, c->cfg.ndim, c->stream));
     ++c->launches;
   }
   return 0;
@@ -378,12 +423,21 @@ int amrvac_gpu_destroy(amrvac_ctx *c) {
   cudaFree(c->d_amr_int);
   cudaFree(c->d_amr_err);
   cudaFree(c->d_stage);
+  delete c->amr;
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
 }
 
+static int set_blocks_impl(amrvac_ctx *c, int nblocks, const double *dx, const int *neighbor, bool level_jumps);
+
 int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const int *neighbor) {
+  return set_blocks_impl(c, nblocks, dx, neighbor, false);
+}
+
+// neighbor entries: block id, -1 physical boundary, and (multi-level grids,
+// internal) <= -2 for a level jump whose ghost cells come from the ghost pass.
+static int set_blocks_impl(amrvac_ctx *c, int nblocks, const double *dx, const int *neighbor, bool level_jumps) {
   if (int r = check_ctx(c, false)) return r;
   if (nblocks <= 0 || !dx || !neighbor) return fail(AMRVAC_E_ARG, "bad block description");
   const int nd = c->cfg.ndim;
@@ -395,7 +449,7 @@ int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const in
     for (int q = 0; q < ndir3; ++q) {
       const int di = q % 3 - 1, dj = nd >= 2 ? (q / 3) % 3 - 1 : 0, dk = nd >= 3 ? q / 9 - 1 : 0;
       const int v = neighbor[(size_t)b * ndir3 + q];
-      if (v >= nblocks || v < -1) return fail(AMRVAC_E_ARG, "neighbor id out of range");
+      if (v >= nblocks || (v < -1 && !level_jumps)) return fail(AMRVAC_E_ARG, "neighbor id out of range");
       nbr[(size_t)b * 27 + (di + 1) + 3 * (dj + 1) + 9 * (dk + 1)] = v;
     }
     nbr[(size_t)b * 27 + 13] = b;
@@ -412,7 +466,7 @@ int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const in
         int o[3] = {0, 0, 0};
         o[d] = s ? 1 : -1;
         const int v = nbr[(size_t)b * 27 + (o[0] + 1) + 3 * (o[1] + 1) + 9 * (o[2] + 1)];
-        if (v < 0 && c->bc.kind[2 * d + s] == BCK_PERIODIC)
+        if (v == -1 && c->bc.kind[2 * d + s] == BCK_PERIODIC)
           return fail(AMRVAC_E_ARG, "physical boundary on a side declared periodic");
       }
   // every direction whose face components all lead to siblings must exist
@@ -428,7 +482,7 @@ int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const in
         f[d] = o[d];
         if (nbr[(size_t)b * 27 + (f[0] + 1) + 3 * (f[1] + 1) + 9 * (f[2] + 1)] < 0) inner = false;
       }
-      if (any && inner && nbr[(size_t)b * 27 + q] < 0)
+      if (any && inner && nbr[(size_t)b * 27 + q] == -1)
         return fail(AMRVAC_E_ARG, "missing edge/corner neighbour between two sibling faces");
     }
   cudaStreamSynchronize(c->stream);
@@ -453,6 +507,7 @@ int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const in
   for (int r = 0; r < 3; ++r) { cudaFree(c->d_adj[r]); c->d_adj[r] = nullptr; }
   cudaFree(c->d_amr_int); c->d_amr_int = nullptr;
   cudaFree(c->d_amr_err); c->d_amr_err = nullptr;
+  delete c->amr; c->amr = nullptr;
   return 0;
 }
 
@@ -494,6 +549,224 @@ int amrvac_gpu_set_uniform_grid(amrvac_ctx *c, const int *domain_nx, const doubl
   }
   return amrvac_gpu_set_blocks(c, total, dx.data(), nbr.data());
 }
+
+// A static multi-level grid: leaf blocks (level, ig) of a 2:1 balanced tree
+// over a periodic domain of nbase root blocks per direction (the reference's
+// forest, src/amr/mod_forest.t, with the neighbour kinds of
+// src/amr/mod_amr_neighbors.t: sibling, coarser, finer).  Same-level ghost
+// cells are read through the neighbour table as on a uniform grid; the ghost
+// cells of every level-jump direction are written by the ghost pass before
+// each stage, and every stage ends with fix_conserve.
+int amrvac_gpu_set_amr_grid(amrvac_ctx *c, int nleaf, const int *leaf, const int *nbase, const double *xprobmin,
+                            const double *xprobmax) {
+  if (int r = check_ctx(c, false)) return r;
+  const int nd = c->cfg.ndim;
+  if (nleaf <= 0 || !leaf || !nbase || !xprobmin || !xprobmax) return fail(AMRVAC_E_ARG, "set_amr_grid: bad arguments");
+  if (nd < 2) return fail(AMRVAC_E_UNSUPPORTED, "set_amr_grid: ndim 2 or 3");
+  if (c->cfg.nghostcells != 2) return fail(AMRVAC_E_UNSUPPORTED, "set_amr_grid: nghostcells 2");
+  for (int s = 0; s < 2 * nd; ++s)
+    if (c->bc.kind[s] != BCK_PERIODIC) return fail(AMRVAC_E_UNSUPPORTED, "set_amr_grid: periodic boundaries only");
+  int maxlev = 1;
+  for (int b = 0; b < nleaf; ++b) {
+    const int L = leaf[4 * b];
+    if (L < 1 || L > AMR_MAX_LEVELS) return fail(AMRVAC_E_ARG, "set_amr_grid: level out of range");
+    maxlev = std::max(maxlev, L);
+  }
+  // dense owner maps per level: leaf id, -2 refined, -1 covered by a coarser
+  // leaf, -3 not covered
+  AmrGhostArgs G;
+  std::memset(&G, 0, sizeof(G));
+  size_t total = 0;
+  for (int L = 1; L <= maxlev; ++L) {
+    size_t n = 1;
+    for (int d = 0; d < 3; ++d) {
+      G.nlev[L][d] = d < nd ? (nbase[d] << (L - 1)) : 1;
+      if (d < nd && nbase[d] <= 0) return fail(AMRVAC_E_ARG, "set_amr_grid: nbase must be positive");
+      n *= (size_t)G.nlev[L][d];
+    }
+    G.owner_off[L] = (int)total;
+    total += n;
+    if (total > ((size_t)1 << 26)) return fail(AMRVAC_E_UNSUPPORTED, "set_amr_grid: hierarchy too deep for the owner maps");
+  }
+  std::vector<int> owner(total, -3);
+  auto at = [&](int L, const int *jg) -> int & {
+    return owner[(size_t)G.owner_off[L] + jg[0] + (size_t)G.nlev[L][0] * (jg[1] + (size_t)G.nlev[L][1] * jg[2])];
+  };
+  std::vector<int> lev(nleaf), ig(3 * (size_t)nleaf, 0);
+  for (int b = 0; b < nleaf; ++b) {
+    const int L = leaf[4 * b];
+    lev[b] = L;
+    int g[3] = {0, 0, 0};
+    for (int d = 0; d < nd; ++d) {
+      g[d] = leaf[4 * b + 1 + d];
+      if (g[d] < 0 || g[d] >= G.nlev[L][d]) return fail(AMRVAC_E_ARG, "set_amr_grid: block index out of range");
+      ig[3 * b + d] = g[d];
+    }
+    if (at(L, g) != -3) return fail(AMRVAC_E_ARG, "set_amr_grid: overlapping leaves");
+    at(L, g) = b;
+    for (int L2 = L - 1; L2 >= 1; --L2) {  // ancestors are refined
+      int a[3] = {0, 0, 0};
+      for (int d = 0; d < nd; ++d) a[d] = g[d] >> (L - L2);
+      int &o = at(L2, a);
+      if (o >= 0 || o == -1) return fail(AMRVAC_E_ARG, "set_amr_grid: overlapping leaves");
+      o = -2;
+    }
+  }
+  for (int b = 0; b < nleaf; ++b)  // descendants are covered
+    for (int L2 = lev[b] + 1; L2 <= maxlev; ++L2) {
+      const int f = 1 << (L2 - lev[b]);
+      const int fy = nd >= 2 ? f : 1, fz = nd >= 3 ? f : 1;
+      for (int z = 0; z < fz; ++z)
+        for (int y = 0; y < fy; ++y)
+          for (int x = 0; x < f; ++x) {
+            const int g[3] = {ig[3 * b] * f + x, nd >= 2 ? ig[3 * b + 1] * f + y : 0, nd >= 3 ? ig[3 * b + 2] * f + z : 0};
+            int &o = at(L2, g);
+            if (o != -3) return fail(AMRVAC_E_ARG, "set_amr_grid: overlapping leaves");
+            o = -1;
+          }
+    }
+  for (int L = 1; L <= maxlev; ++L)  // every region is covered
+    for (int z = 0; z < G.nlev[L][2]; ++z)
+      for (int y = 0; y < G.nlev[L][1]; ++y)
+        for (int x = 0; x < G.nlev[L][0]; ++x) {
+          const int g[3] = {x, y, z};
+          const int o = at(L, g);
+          if (o == -3) {
+            const int p[3] = {x / 2, y / 2, z / 2};
+            if (L == 1 || at(L - 1, p) == -2) return fail(AMRVAC_E_ARG, "set_amr_grid: leaves do not cover the domain");
+          }
+          if (o == -2 && L == maxlev) return fail(AMRVAC_E_ARG, "set_amr_grid: inconsistent tree");
+        }
+  // neighbour kinds, the neighbour table and the children across each face
+  const int nb = nleaf;
+  std::vector<int> ntype(27 * (size_t)nb, AMR_BOUNDARY), child(27 * 8 * (size_t)nb, -1);
+  std::vector<int> gslot(nb, -1), face(nb, 0), iblocks;
+  int ndir3 = 1;
+  for (int d = 0; d < nd; ++d) ndir3 *= 3;
+  std::vector<int> nbr((size_t)nb * ndir3, -1);
+  std::vector<double> dx((size_t)nb * nd), bxmin(3 * (size_t)nb, 0.0), dxb3(3 * (size_t)nb, 1.0);
+  for (int b = 0; b < nb; ++b) {
+    const int L = lev[b];
+    for (int q = 0; q < 27; ++q) {
+      const int dd[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
+      bool ok = true;
+      int jg[3] = {0, 0, 0};
+      for (int d = 0; d < 3; ++d) {
+        if (d >= nd) { if (dd[d]) ok = false; continue; }
+        const int nl = G.nlev[L][d];
+        jg[d] = ((ig[3 * b + d] + dd[d]) % nl + nl) % nl;
+      }
+      if (!ok) continue;
+      if (q == 13) { ntype[b * 27 + q] = AMR_SIBLING; continue; }
+      const int o = at(L, jg);
+      if (o >= 0) {
+        ntype[b * 27 + q] = AMR_SIBLING;
+      } else if (o == -1) {
+        const int p[3] = {jg[0] / 2, jg[1] / 2, jg[2] / 2};
+        if (L == 1 || at(L - 1, p) < 0) return fail(AMRVAC_E_ARG, "set_amr_grid: tree not 2:1 balanced");
+        ntype[b * 27 + q] = AMR_COARSE;
+      } else {
+        ntype[b * 27 + q] = AMR_FINE;
+        for (int cb = 0; cb < (1 << nd); ++cb) {
+          const int cc[3] = {cb & 1, (cb >> 1) & 1, (cb >> 2) & 1};
+          bool adjacent = true;
+          for (int d = 0; d < nd; ++d)
+            if ((dd[d] == 1 && cc[d] != 0) || (dd[d] == -1 && cc[d] != 1)) adjacent = false;
+          const int g2[3] = {2 * jg[0] + cc[0], nd >= 2 ? 2 * jg[1] + cc[1] : 0, nd >= 3 ? 2 * jg[2] + cc[2] : 0};
+          const int o2 = at(L + 1, g2);
+          if (adjacent && o2 < 0) return fail(AMRVAC_E_ARG, "set_amr_grid: tree not 2:1 balanced");
+          child[(b * 27 + q) * 8 + cb] = o2 >= 0 ? o2 : -1;
+        }
+      }
+    }
+    bool jump = false;
+    for (int q = 0; q < 27; ++q) jump |= ntype[b * 27 + q] == AMR_COARSE || ntype[b * 27 + q] == AMR_FINE;
+    if (jump) {
+      gslot[b] = (int)iblocks.size();
+      iblocks.push_back(b);
+    }
+    for (int d = 0; d < nd; ++d)
+      for (int s = 0; s < 2; ++s) {
+        int o[3] = {0, 0, 0};
+        o[d] = s ? 1 : -1;
+        const int t = ntype[b * 27 + (o[0] + 1) + 3 * (o[1] + 1) + 9 * (o[2] + 1)];
+        if (t == AMR_COARSE || t == AMR_FINE) face[b] |= 1 << (2 * d + s);
+      }
+    for (int d = 0; d < nd; ++d) {
+      // cell size and corner as the reference's block geometry computes them
+      const double h = (xprobmax[d] - xprobmin[d]) / (nbase[d] * 16.0 * double(1 << (L - 1)));
+      dx[(size_t)b * nd + d] = h;
+      dxb3[3 * (size_t)b + d] = h;
+      bxmin[3 * (size_t)b + d] = xprobmin[d] + ig[3 * b + d] * 16.0 * h;
+    }
+  }
+  for (int b = 0; b < nb; ++b)
+    for (int q = 0; q < ndir3; ++q) {
+      const int dd[3] = {q % 3 - 1, nd >= 2 ? (q / 3) % 3 - 1 : 0, nd >= 3 ? q / 9 - 1 : 0};
+      const int q27 = (dd[0] + 1) + 3 * (dd[1] + 1) + 9 * (dd[2] + 1);
+      const int t = ntype[b * 27 + q27];
+      if (t == AMR_SIBLING) {
+        int jg[3] = {0, 0, 0};
+        for (int d = 0; d < nd; ++d) {
+          const int nl = G.nlev[lev[b]][d];
+          jg[d] = ((ig[3 * b + d] + dd[d]) % nl + nl) % nl;
+        }
+        nbr[(size_t)b * ndir3 + q] = q27 == 13 ? b : at(lev[b], jg);
+      } else {
+        nbr[(size_t)b * ndir3 + q] = -2 - gslot[b];
+      }
+    }
+  if (int r = set_blocks_impl(c, nb, dx.data(), nbr.data(), true)) return r;
+  // device copies
+  AmrDev *A = new AmrDev();
+  c->amr = A;
+  A->nslots = (int)iblocks.size();
+  const size_t ns = std::max<size_t>(1, iblocks.size());
+  std::vector<int> ints;
+  auto put = [&](const std::vector<int> &v) {
+    const size_t off = ints.size();
+    ints.insert(ints.end(), v.begin(), v.end());
+    return off;
+  };
+  const size_t o_ib = put(iblocks), o_gs = put(gslot), o_fc = put(face), o_nt = put(ntype), o_lv = put(lev),
+               o_ig = put(ig), o_ch = put(child), o_ow = put(owner);
+  CK(cudaMalloc(&A->d_int, sizeof(int) * ints.size()));
+  CK(cudaMemcpyAsync(A->d_int, ints.data(), sizeof(int) * ints.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMalloc(&A->d_bxmin, sizeof(double) * bxmin.size()));
+  CK(cudaMemcpyAsync(A->d_bxmin, bxmin.data(), sizeof(double) * bxmin.size(), cudaMemcpyHostToDevice, c->stream));
+  size_t gcells = 1;
+  for (int d = 0; d < nd; ++d) gcells *= 20;
+  CK(cudaMalloc(&A->gbuf, sizeof(double) * ns * c->nw * gcells));
+  CK(cudaMemsetAsync(A->gbuf, 0, sizeof(double) * ns * c->nw * gcells, c->stream));
+  CK(cudaMalloc(&A->pflux, sizeof(double) * ns * 2 * nd * c->nw * 256));
+  CK(cudaMemsetAsync(A->pflux, 0, sizeof(double) * ns * 2 * nd * c->nw * 256, c->stream));
+  A->d_gslot = A->d_int + o_gs;
+  A->d_face = A->d_int + o_fc;
+  G.u = nullptr;
+  G.gbuf = A->gbuf;
+  G.nw = c->nw;
+  G.iblocks = A->d_int + o_ib;
+  G.ntype = A->d_int + o_nt;
+  G.level = A->d_int + o_lv;
+  G.ig = A->d_int + o_ig;
+  G.bxmin = A->d_bxmin;
+  G.dxb = c->d_dx;
+  G.owner = A->d_int + o_ow;
+  G.maxlevel = maxlev;
+  G.status = c->d_status;
+  A->G = G;
+  std::memset(&A->F, 0, sizeof(A->F));
+  A->F.pflux = A->pflux;
+  A->F.nw = c->nw;
+  A->F.iblocks = G.iblocks;
+  A->F.gslot = A->d_gslot;
+  A->F.ntype = G.ntype;
+  A->F.child = A->d_int + o_ch;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int amrvac_gpu_amr_slots(const amrvac_ctx *c) { return c && c->amr ? c->amr->nslots : 0; }
 
 int amrvac_gpu_nblocks(const amrvac_ctx *c) { return c ? c->nblocks : AMRVAC_E_ARG; }
 
@@ -541,8 +814,10 @@ int amrvac_gpu_download(amrvac_ctx *c, int reg, int first, int n, double *w) {
   for (int b0 = 0; b0 < n; b0 += chunk) {
     const int m = std::min(chunk, n - b0);
     if (int r = ensure_stage(c, gpb * m)) return r;
+    if (c->amr && b0 == 0)
+      if (int r = launch_amr_ghost_pass(c, reg)) return r;
     CK(launch_pack(c->pool[reg], c->d_stage, first + b0, m, c->nw, c->cfg.ndim, c->cfg.nghostcells, c->d_nbr,
-                   c->maps, c->bc, c->stream));
+                   c->maps, c->bc, c->amr ? c->amr->gbuf : nullptr, c->stream));
     ++c->launches;
     CK(cudaMemcpyAsync(w + (size_t)b0 * gpb, c->d_stage, sizeof(double) * gpb * m, cudaMemcpyDeviceToHost,
                        c->stream));
@@ -894,6 +1169,7 @@ static int adjoint_step_impl(amrvac_ctx *c, const double *u0, const double *u1, 
   if (int r = check_ctx(c, true)) return r;
   const amrvac_cfg &k = c->cfg;
   if (!lam || !gamma_part || !(dt > 0.0)) return fail(AMRVAC_E_ARG, "bad adjoint arguments");
+  if (c->amr) return fail(AMRVAC_E_UNSUPPORTED, "adjoint: single-level grids only");
   if (k.physics != 0 || k.ndim != 2 || (k.flux_scheme != AMRVAC_FS_HLL && k.flux_scheme != AMRVAC_FS_HLLC) ||
       k.typeboundspeed != AMRVAC_BS_EINFELDT || (k.limiter != AMRVAC_LIM_MINMOD && k.limiter != AMRVAC_LIM_VANLEER) ||
       k.fix_small_values || k.precision != 0)
@@ -975,6 +1251,8 @@ int amrvac_gpu_lohner(amrvac_ctx *c, int reg, const double *weight, const int *l
   if (c->cfg.ndim < 2) return fail(AMRVAC_E_UNSUPPORTED, "lohner: ndim 2 or 3");
   LohnerArgs A;
   std::memset(&A, 0, sizeof(A));
+  if (c->amr)
+    if (int r = launch_amr_ghost_pass(c, reg)) return r;
   A.sa = stage_args(c, reg, reg, reg, 0.0, 1.0, 1.0);
   A.nw = c->nw;
   for (int v = 0; v < c->nw; ++v) {

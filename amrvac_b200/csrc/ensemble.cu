@@ -931,7 +931,7 @@ int amrvac_ens_download(amrvac_ens *e, int inst, double *w) {
   const size_t doubles = g * nw * e->nblk[inst];
   if (int r = ens_ensure_stage(e, doubles)) return r;
   ECK(launch_pack(e->pool[p][0], e->d_stage, e->first[inst], e->nblk[inst], nw, ndim, e->cfg.nghostcells,
-                  e->d_nbr[p], e->maps, e->bc, e->stream));
+                  e->d_nbr[p], e->maps, e->bc, nullptr, e->stream));
   ++e->launches;
   ECK(cudaMemcpyAsync(w, e->d_stage, sizeof(double) * doubles, cudaMemcpyDeviceToHost, e->stream));
   ECK(cudaStreamSynchronize(e->stream));

@@ -66,6 +66,15 @@ struct StageArgs {
   uint32_t *status;         // global status word (atomicOr)
   uint32_t *block_status;   // [nblocks] per-block status (crash restore)
   PhysParams P;
+  // Multi-level grids (all null on a single level).  A neighbour entry
+  // <= -2 means "the ghost cells of this direction are in the block's ghost
+  // buffer gbuf[-2 - entry]" (restricted or prolonged values, written by the
+  // AMR ghost pass); amr_face[b] bit 2d+side marks a level jump across that
+  // face, whose boundary face fluxes are stored in pflux[gslot[b]].
+  const double *gbuf;       // [slot][var][gz][gy][gx], ghosted (2 layers)
+  double *pflux;            // [slot][2*ndim][var][16*16] scaled face fluxes
+  const int *gslot;         // [nblocks] slot or -1
+  const int *amr_face;      // [nblocks] bitmask
 };
 
 __device__ __forceinline__ int dir_index(int di, int dj, int dk) {
@@ -88,7 +97,7 @@ __device__ __forceinline__ int resolve_cell(const StageArgs &A, int b, int &i, i
     int fd[3] = {0, 0, 0};
     fd[d] = side ? 1 : -1;
     const int nf = A.nbr[b * 27 + dir_index(fd[0], fd[1], fd[2])];
-    if (nf < 0) {
+    if (nf == -1) {
       const int kind = A.bc_kind[2 * d + side];
       if (kind == BCK_CONT) {
         c[d] = side ? BN - 1 : 0;
@@ -106,6 +115,8 @@ __device__ __forceinline__ int resolve_cell(const StageArgs &A, int b, int &i, i
     if (blk >= 0) {
 #pragma unroll
       for (int d = 0; d < NDIM; ++d) c[d] -= dir[d] * BN;
+    } else if (blk <= -2 && A.gbuf) {
+      // level jump: the value is in this block's ghost buffer at c
     } else {  // inconsistent neighbour table: stay in bounds and flag it
       blk = b;
 #pragma unroll
@@ -124,6 +135,17 @@ __device__ __forceinline__ size_t cell_offset(int blk, int nw, int v, int i, int
   return (((size_t)blk * nw + v) * NZ + k) * (size_t)(NY * BN) + (size_t)j * BN + i;
 }
 
+// Offset of cell (i, j, k) (block-local, up to 2 outside) in a ghosted
+// buffer of 2 ghost layers: [slot][var][gz][gy][gx].
+template <int NDIM>
+__device__ __forceinline__ size_t ghost_offset(int slot, int nw, int v, int i, int j, int k) {
+  constexpr int G = BN + 4;
+  constexpr int GY = NDIM >= 2 ? G : 1;
+  constexpr int GZ = NDIM >= 3 ? G : 1;
+  const int gj = NDIM >= 2 ? j + 2 : 0, gk = NDIM >= 3 ? k + 2 : 0;
+  return (((size_t)slot * nw + v) * GZ + gk) * (size_t)(GY * G) + (size_t)gj * G + (i + 2);
+}
+
 // Load the conserved state of a (possibly out-of-block) cell and return it
 // as primitives.  Returns a status bit if the small-value check fires.
 template <bool MHD, int NDIR, bool GLM, int NDIM>
@@ -132,10 +154,15 @@ __device__ __forceinline__ uint32_t load_prim(const StageArgs &A, int b, int i, 
   using V = Vars<MHD, NDIR, GLM>;
   uint32_t flip;
   const int blk = resolve_cell<NDIM>(A, b, i, j, k, flip);
+  if (blk >= 0) {
 #pragma unroll
-  for (int v = 0; v < V::NW; ++v) {
-    double x = __ldg(A.uin + cell_offset<NDIM>(blk, V::NW, v, i, j, k));
-    w[v] = ((flip >> v) & 1u) ? -x : x;
+    for (int v = 0; v < V::NW; ++v) {
+      double x = __ldg(A.uin + cell_offset<NDIM>(blk, V::NW, v, i, j, k));
+      w[v] = ((flip >> v) & 1u) ? -x : x;
+    }
+  } else {  // level jump: this block's ghost buffer
+#pragma unroll
+    for (int v = 0; v < V::NW; ++v) w[v] = __ldg(A.gbuf + ghost_offset<NDIM>(-2 - blk, V::NW, v, i, j, k));
   }
   uint32_t st = 0;
   if (A.P.fix_small_values) {
@@ -311,6 +338,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
   const int k1 = (int)(k0 + ((gend - g) < (PL - k0) ? (gend - g) : (PL - k0)));
   g += k1 - k0;
   uint32_t stb = 0;  // status of this block's update
+  const int amr_mask = A.amr_face ? A.amr_face[b] : 0;
   double dx[3], dxinv[3], rdel[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -426,6 +454,19 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
           const int ov = orig_index_rt<MHD, NDIR>(v, D);
           if constexpr (FP64) tv.fb[ov * FB + f] = sc * Fr[v];
           else tv.fb[ov * FB + f] = Fr[v];
+        }
+        // level jump across this block face: keep the boundary face flux
+        // (store_flux, src/mod_fix_conserve.t:597-648) for the flux fix
+        if (amr_mask) {
+          const int pos = D == 0 ? fi : (D == 1 ? fj : k + 1);
+          const int side = pos == 0 ? 0 : (pos == BN ? 1 : -1);
+          if (side >= 0 && ((amr_mask >> (2 * D + side)) & 1)) {
+            const int ta = D == 0 ? fj : fi, tb = D == 2 ? fj : k;
+            double *pf = A.pflux + ((size_t)A.gslot[b] * (2 * NDIM) + 2 * D + side) * NW * (BN * BN);
+#pragma unroll
+            for (int v = 0; v < NW; ++v)
+              pf[orig_index_rt<MHD, NDIR>(v, D) * (BN * BN) + ta + BN * (NDIM == 3 ? tb : 0)] = sc * double(Fr[v]);
+          }
         }
       }
       __syncthreads();

@@ -137,6 +137,21 @@ int amrvac_gpu_set_blocks(amrvac_ctx *ctx, int nblocks, const double *dx, const 
 int amrvac_gpu_set_uniform_grid(amrvac_ctx *ctx, const int *domain_nx, const double *xprobmin,
                                 const double *xprobmax);
 int amrvac_gpu_nblocks(const amrvac_ctx *ctx);
+/* Static multi-level grid (replaces the forest and neighbour search of
+ * src/amr/mod_forest.t and src/amr/mod_amr_neighbors.t for a fixed tree):
+ * leaf[4*b] = level (1-based), ig0, ig1, ig2 (block index at that level);
+ * nbase root blocks per direction over [xprobmin, xprobmax]; periodic
+ * boundaries, ndim 2 or 3, nghostcells 2, 2:1 balanced across faces, edges
+ * and corners.  Blocks are numbered in the order given.  Afterwards every
+ * stage fills the level-jump ghost cells as the reference's multi-level getbc
+ * does (restriction, and prolongation by interpolation_linear,
+ * src/mod_ghostcells_update.t:350-578, 1381-1525) and applies the flux fix
+ * (store_flux / fix_conserve, src/mod_fix_conserve.t:465-648); download
+ * returns those ghost cells too.  Replaces any previous block set. */
+int amrvac_gpu_set_amr_grid(amrvac_ctx *ctx, int nleaf, const int *leaf, const int *nbase, const double *xprobmin,
+                            const double *xprobmax);
+/* Blocks next to a level jump (0 on a single-level grid). */
+int amrvac_gpu_amr_slots(const amrvac_ctx *ctx);
 
 /* Copy n blocks starting at `first` between host Fortran arrays and register
  * reg (0 = ps, 1 = ps1, 2 = ps2).  Upload reads interior cells only; download

@@ -1,0 +1,174 @@
+"""Multi-level grids on the GPU against the oracle's AmrGrid.
+
+* Ghost cells: after the device ghost pass (restriction and
+  interpolation_linear prolongation at level jumps, same-level copies
+  elsewhere) every ghost cell of every block matches the oracle's
+  multi-level getbc to 1e-13 relative.
+* Steps: full SSPRK steps with the flux fix after every stage match the
+  oracle's advance (setdt, advect1 per stage, fix_conserve, getbc) to 1e-12
+  relative, and conserve every total to rounding on the periodic domain.
+* Hierarchies that break 2:1 balance, overlap or leave holes are refused.
+"""
+import numpy as np
+import pytest
+
+from tests import _amr as A
+
+pytestmark = pytest.mark.gpu
+
+
+def _cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _nbase(nd):
+    return [8] * nd if nd == 2 else [4] * nd
+
+
+def _leaves(nd, levels):
+    def ref(c, lv):
+        r = np.linalg.norm(c - 0.45)
+        return r < (0.3 if lv == 1 else 0.15)
+    return A.build_leaves(nd, _nbase(nd), levels, ref)
+
+
+def _field(nd, physics, glm=False):
+    def f(X, Y, Z):
+        nw = (nd + 2) if physics == "hd" else (2 * nd + 2 + int(glm))
+        out = np.zeros((nw,) + X.shape)
+        s = np.sin(2 * np.pi * X) * np.cos(2 * np.pi * Y) * (np.cos(2 * np.pi * Z) if nd > 2 else 1)
+        blob = np.exp(-((X - 0.45) ** 2 + (Y - 0.45) ** 2 + ((Z - 0.45) ** 2 if nd > 2 else 0)) / 0.01)
+        out[0] = 1.0 + 0.3 * s + 2.0 * blob
+        out[1] = 0.5 + 0.2 * np.cos(2 * np.pi * Y)
+        out[2] = -0.3 + 0.2 * np.sin(2 * np.pi * X)
+        if nd > 2:
+            out[3] = 0.1 * np.sin(2 * np.pi * Y)
+        out[nd + 1] = 1.0 + 0.2 * s + 3.0 * blob
+        if physics == "mhd":
+            out[nd + 2] = 0.3 + 0.1 * np.cos(2 * np.pi * Y)
+            out[nd + 3] = 0.2 + 0.1 * np.sin(2 * np.pi * X)
+            if nd > 2:
+                out[nd + 4] = 0.1
+            if glm:
+                out[2 * nd + 2] = 0.01 * np.sin(2 * np.pi * (X + Y))
+        return out
+    return f
+
+
+CASES = [
+    ("hd2_hllc_vanleer", 2, 3, dict(physics="hd", flux_scheme="hllc", limiter="vanleer")),
+    ("hd2_hll_minmod_ssprk32", 2, 3, dict(physics="hd", flux_scheme="hll", limiter="minmod", ssprk_order=2)),
+    ("hd2_tvdlf_koren", 2, 2, dict(physics="hd", flux_scheme="tvdlf", limiter="koren")),
+    ("mhd2_hlld_linde", 2, 2, dict(physics="mhd", flux_scheme="hlld", limiter="vanleer", typedivbfix="linde")),
+    ("mhd2_hll_glm", 2, 2, dict(physics="mhd", flux_scheme="hll", limiter="minmod", typedivbfix="glm")),
+    ("hd3_hllc", 3, 2, dict(physics="hd", flux_scheme="hllc", limiter="vanleer")),
+]
+
+
+def _setup(O, nd, levels, kw):
+    from amrvac_b200 import Context, make_cfg
+    leaves = _leaves(nd, levels)
+    nb = _nbase(nd)
+    physics = kw["physics"]
+    base = dict(ndim=nd, gamma=5.0 / 3.0 if physics == "mhd" else 1.4, courantpar=0.6)
+    base.update(kw)
+    gk = dict(base)
+    ok = dict(base)
+    if "typedivbfix" in ok:
+        ok["divb"] = ok.pop("typedivbfix")
+    ocfg = O.make_cfg(**ok)
+    gcfg = make_cfg(typeboundary=["periodic"] * (2 * nd), **gk)
+    og = O.AmrGrid(ocfg, nb, [0.0] * nd, [1.0] * nd, leaves)
+    ndir = nd
+    blocks = A.fill_blocks(leaves, nd, nb, _field(nd, physics, kw.get("typedivbfix") == "glm"), physics, ndir,
+                           base["gamma"])
+    for b in range(len(leaves)):
+        og.set_block(b, blocks[b])
+    og.getbc()
+    ctx = Context(gcfg)
+    ctx.set_amr_grid(leaves, nb, [0.0] * nd, [1.0] * nd)
+    ctx.upload(blocks)
+    return leaves, nb, og, ctx
+
+
+def _maxrel(a, b):
+    if not (np.isfinite(a).all() and np.isfinite(b).all()):
+        return np.inf
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("name,nd,levels,kw", CASES, ids=[c[0] for c in CASES])
+def test_amr_ghosts_and_steps(oracle_lib, name, nd, levels, kw):
+    _cuda()
+    O = oracle_lib
+    leaves, nb, og, ctx = _setup(O, nd, levels, kw)
+    assert len({l[0] for l in leaves}) == levels
+    assert ctx.amr_slots > 0
+    # ghost cells of the initial state
+    got = ctx.download()
+    for b in range(len(leaves)):
+        ref = og.get_block(b)
+        assert _maxrel(got[b], ref) <= 1e-13, (name, "ghosts", leaves[b], _maxrel(got[b], ref))
+    sl = (slice(None),) + tuple(slice(2, 18) if d < nd else slice(None) for d in (2, 1, 0))
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    nsteps = 3 if nd == 2 else 2
+    for n in range(nsteps):
+        dt_o, cm_o = og.getdt()
+        ctx.step()
+        dt_g, cm_g, _ = ctx.get_time()
+        assert abs(dt_g - dt_o) <= 1e-13 * dt_o, (name, n, dt_g, dt_o)
+        og.advance(dt_o, cm_o)
+        got = ctx.download()
+        for b in range(len(leaves)):
+            ref = og.get_block(b)
+            assert _maxrel(got[b][sl], ref[sl]) <= 1e-12, (name, n, leaves[b], _maxrel(got[b][sl], ref[sl]))
+    assert ctx.status() == 0
+    ctx.close()
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_amr_conserves(oracle_lib, nd):
+    _cuda()
+    O = oracle_lib
+    leaves, nb, og, ctx = _setup(O, nd, 3 if nd == 2 else 2,
+                                 dict(physics="hd", flux_scheme="hllc", limiter="vanleer"))
+    sl = (slice(None),) + tuple(slice(2, 18) if d < nd else slice(None) for d in (2, 1, 0))
+    vol = np.array([A.block_volume(l, nd, nb) for l in leaves])
+
+    def totals(blocks):
+        return np.einsum("bv,b->v", blocks[sl[:1] + (slice(None),) + sl[1:]].reshape(len(leaves), nd + 2, -1).sum(-1),
+                         vol)
+    t0 = totals(ctx.download())
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.run(10 if nd == 2 else 4)
+    t1 = totals(ctx.download())
+    assert np.all(np.abs(t1 - t0) <= 1e-13 * np.abs(t0).max()), (t0, t1)
+    ctx.close()
+
+
+def test_amr_refuses_bad_trees():
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    cfg = make_cfg(physics="hd", ndim=2, typeboundary=["periodic"] * 4)
+    ctx = Context(cfg)
+    nb = [2, 2]
+    base = [(1, i, j) for j in range(2) for i in range(2)]
+    # a hole
+    with pytest.raises(RuntimeError):
+        ctx.set_amr_grid(base[:3], nb, [0, 0], [1, 1])
+    # an overlap
+    with pytest.raises(RuntimeError):
+        ctx.set_amr_grid(base + [(2, 0, 0)], nb, [0, 0], [1, 1])
+    # level 1 next to level 3 (not 2:1 balanced)
+    fine = [(2, 2 + i, 2 + j) for j in range(2) for i in range(2) if (i, j) != (0, 0)]
+    fine += [(3, 4 + i, 4 + j) for j in range(2) for i in range(2)]
+    with pytest.raises(RuntimeError):
+        ctx.set_amr_grid(base[:3] + fine, nb, [0, 0], [1, 1])
+    # a good tree is accepted, and a uniform grid afterwards drops it
+    ctx.set_amr_grid(base[:3] + [(2, 2 + i, 2 + j) for j in range(2) for i in range(2)], nb, [0, 0], [1, 1])
+    assert ctx.nblocks == 7 and ctx.amr_slots > 0
+    ctx.set_uniform_grid([32, 32], [0, 0], [1, 1])
+    assert ctx.amr_slots == 0
+    ctx.close()
