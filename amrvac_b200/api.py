@@ -89,6 +89,12 @@ class Context:
     def amr_slots(self):
         return self.L.amrvac_gpu_amr_slots(self.h)
 
+    def amr_kernel_ms(self, reps=10):
+        """(ghost pass ms, flux fix ms) per launch; the fix changes register ps2."""
+        g, f = ctypes.c_double(), ctypes.c_double()
+        _lib.check(self.L.amrvac_gpu_amr_kernel_ms(self.h, reps, ctypes.byref(g), ctypes.byref(f)), "amr_kernel_ms")
+        return g.value, f.value
+
     def set_blocks(self, dx, neighbor):
         dx = np.ascontiguousarray(dx, dtype=np.float64)
         nb = np.ascontiguousarray(neighbor, dtype=np.int32)

@@ -35,7 +35,9 @@ __global__ void __launch_bounds__(256) lohner_kernel(const LohnerArgs A) {
     int ii = x, jj = y, kk = z;
     uint32_t flip;
     const int blk = resolve_cell<NDIM>(S, b, ii, jj, kk, flip);
-    double v = S.uin[cell_offset<NDIM>(blk, nw, iw, ii, jj, kk)];
+    // a level jump (blk <= -2) reads the ghost buffer the ghost pass filled
+    double v = blk >= 0 ? S.uin[cell_offset<NDIM>(blk, nw, iw, ii, jj, kk)]
+                        : S.gbuf[ghost_offset<NDIM>(-2 - blk, nw, iw, ii, jj, kk)];
     if ((flip >> iw) & 1u) v = -v;
     return ((A.logflag >> iw) & 1u) ? log10(v) : v;
   };
@@ -125,7 +127,8 @@ __device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int
 #pragma unroll
   for (int d = 0; d < NDIM; ++d) {
     const int n = A.nlev[L][d] * BN;
-    const int p = ((P[d] % n) + n) % n;  // periodic domain
+    int p = P[d];  // within 4 cells of the block, n >= 16: one periodic wrap
+    p = p < 0 ? p + n : (p >= n ? p - n : p);
     jg[d] = p >> 4;
     loc[d] = p & (BN - 1);
   }
@@ -141,15 +144,20 @@ __device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int
     }
     const int o2 = A.owner[A.owner_off[L + 1] + jf[0] + A.nlev[L + 1][0] * (jf[1] + A.nlev[L + 1][1] * jf[2])];
     if (o2 >= 0) {
-      double sum = 0.0;
-      bool first = true;
-      for (int kk = 0; kk < (NDIM > 2 ? 2 : 1); ++kk)
-        for (int jj = 0; jj < (NDIM > 1 ? 2 : 1); ++jj)
-          for (int ii = 0; ii < 2; ++ii) {
-            const double x = A.u[cell_offset<NDIM>(o2, A.nw, v, f[0] + ii, f[1] + jj, f[2] + kk)];
-            sum = first ? x : sum + x;
-            first = false;
-          }
+      const double *w = A.u + cell_offset<NDIM>(o2, A.nw, v, f[0], f[1], f[2]);
+      constexpr int SY = BN, SZ = BN * BN;
+      double sum = w[0];  // x fastest, left to right
+      sum = sum + w[1];
+      if constexpr (NDIM > 1) {
+        sum = sum + w[SY];
+        sum = sum + w[SY + 1];
+      }
+      if constexpr (NDIM > 2) {
+        sum = sum + w[SZ];
+        sum = sum + w[SZ + 1];
+        sum = sum + w[SZ + SY];
+        sum = sum + w[SZ + SY + 1];
+      }
       return sum * (1.0 / double(1 << NDIM));
     }
   }
@@ -157,107 +165,146 @@ __device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int
   return 0.0;
 }
 
+// One CTA per (block next to a level jump, variable).  The ghost cells of the
+// level-jump directions are enumerated region by region (a face region is
+// 2 x 16 x 16 cells, an edge 2 x 2 x 16, a corner 2 x 2 x 2), so no thread
+// walks the interior; the coarse representation psc is built first, only
+// where some prolongation stencil reads it.
 template <int NDIM>
 __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
-  extern __shared__ double psc[];  // 12^NDIM coarse representation of one variable
-  constexpr int G = BN + 4, GY = NDIM >= 2 ? G : 1, GZ = NDIM >= 3 ? G : 1;
+  extern __shared__ double psc[];  // 12^NDIM coarse representation of variable blockIdx.y
   constexpr int C = BN / 2 + 4, CY = NDIM >= 2 ? C : 1, CZ = NDIM >= 3 ? C : 1;
+  __shared__ int s_off[28];        // prefix sums of the jump regions' cell counts
+  __shared__ int s_q[27], s_kind[27];
+  __shared__ int s_nreg;
+  __shared__ uint32_t s_coarse;    // bit q: direction q has a coarser neighbour
   const int slot = blockIdx.x;
+  const int v = blockIdx.y;
   const int b = A.iblocks[slot];
   const int t = threadIdx.x;
   const int L = A.level[b];
-  const int *nt = A.ntype + b * 27;
-  bool has_coarse = false;
-  for (int q = 0; q < 27; ++q) has_coarse |= nt[q] == AMR_COARSE;
-  int igb[3] = {0, 0, 0};
-  double dxF[3] = {1, 1, 1}, dxC[3] = {1, 1, 1}, invC[3] = {1, 1, 1}, xFmin[3] = {0, 0, 0}, xCmin[3] = {0, 0, 0};
-#pragma unroll
-  for (int d = 0; d < NDIM; ++d) {
-    igb[d] = A.ig[3 * b + d];
-    dxF[d] = A.dxb[3 * b + d];
-    dxC[d] = 2.0 * dxF[d];
-    invC[d] = 1.0 / dxC[d];
-    xFmin[d] = A.bxmin[3 * b + d] - 2.0 * dxF[d];
-    xCmin[d] = A.bxmin[3 * b + d] - 2.0 * dxC[d];
+  if (t == 0) {
+    const int *nt = A.ntype + b * 27;
+    int n = 0, m = 0;
+    uint32_t cm = 0;
+    for (int q = 0; q < 27; ++q) {
+      const int kind = nt[q];
+      if (q == 13 || (kind != AMR_COARSE && kind != AMR_FINE)) continue;
+      const int dd[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
+      int cells = 1;
+      for (int d = 0; d < NDIM; ++d) cells *= dd[d] ? 2 : BN;
+      if (kind == AMR_COARSE) cm |= 1u << q;
+      s_q[m] = q;
+      s_kind[m] = kind;
+      s_off[m] = n;
+      n += cells;
+      ++m;
+    }
+    s_off[m] = n;
+    s_nreg = m;
+    s_coarse = cm;
   }
-  for (int v = 0; v < A.nw; ++v) {
-    if (has_coarse) {
-      for (int p = t; p < C * CY * CZ; p += blockDim.x) {
-        const int pc[3] = {p % C, (p / C) % CY, p / (C * CY)};
-        // only the cells some prolongation stencil reads: the centre of a
-        // ghost cell of a coarser-neighbour direction (coarse index 1 for
-        // the low ghosts, 2..9 beside the block, 10 for the high ghosts) or
-        // one of its axial neighbours
-        bool needed = false;
-        for (int m = 0; m <= 2 * NDIM && !needed; ++m) {
-          int cc[3] = {pc[0], pc[1], pc[2]};
-          if (m > 0) cc[(m - 1) >> 1] += (m & 1) ? 1 : -1;
-          int dd[3] = {0, 0, 0};
-          bool ok = true;
+  __syncthreads();
+  const int nreg = s_nreg;
+  const uint32_t cmask = s_coarse;
+  int igb[3] = {0, 0, 0};
 #pragma unroll
-          for (int d = 0; d < NDIM; ++d) {
-            if (cc[d] < 1 || cc[d] > BN / 2 + 2) ok = false;
-            dd[d] = cc[d] == 1 ? -1 : (cc[d] == BN / 2 + 2 ? 1 : 0);
-          }
-          needed = ok && (dd[0] | dd[1] | dd[2]) && nt[dir_index(dd[0], dd[1], dd[2])] == AMR_COARSE;
+  for (int d = 0; d < NDIM; ++d) igb[d] = A.ig[3 * b + d];
+  if (cmask) {
+    for (int p = t; p < C * CY * CZ; p += blockDim.x) {
+      const int pc[3] = {p % C, NDIM >= 2 ? (p / C) % CY : 0, NDIM >= 3 ? p / (C * CY) : 0};
+      // read by the stencils (centre +- 1 per direction) of the ghost cells
+      // of a coarser-neighbour direction: coarse index 1 for the low ghosts,
+      // 2..9 beside the block, 10 for the high ghosts
+      // (bit q of kDirBits[d][k + 1]: component d of direction q is k)
+      constexpr uint32_t kDirBits[3][3] = {{0x1249249u, 0x2492492u, 0x4924924u},
+                                           {0x01c0e07u, 0x0e07038u, 0x70381c0u},
+                                           {0x00001ffu, 0x003fe00u, 0x7fc0000u}};
+      uint32_t m = cmask;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        uint32_t md = 0;
+        if (d < NDIM) {
+          if (pc[d] <= 2) md |= kDirBits[d][0];
+          if (pc[d] >= 1 && pc[d] <= BN / 2 + 2) md |= kDirBits[d][1];
+          if (pc[d] >= BN / 2 + 1) md |= kDirBits[d][2];
+        } else {
+          md = kDirBits[d][1];
         }
-        if (!needed) continue;
-        int P[3] = {0, 0, 0};
-#pragma unroll
-        for (int d = 0; d < NDIM; ++d) P[d] = igb[d] * (BN / 2) + pc[d] - 2;
-        psc[p] = coarse_value<NDIM>(A, L - 1, P[0], P[1], P[2], v);
+        m &= md;
       }
+      if (!m) continue;
+      int P[3] = {0, 0, 0};
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) P[d] = igb[d] * (BN / 2) + pc[d] - 2;
+      psc[p] = coarse_value<NDIM>(A, L - 1, P[0], P[1], P[2], v);
     }
     __syncthreads();
-    for (int g = t; g < G * GY * GZ; g += blockDim.x) {
-      const int gc[3] = {g % G, (g / G) % GY, g / (G * GY)};
-      int dir[3] = {0, 0, 0};
-      bool inside = true;
+  }
+  double dxF[3] = {1, 1, 1}, dxC[3] = {1, 1, 1}, invC[3] = {1, 1, 1}, xFmin[3] = {0, 0, 0}, xCmin[3] = {0, 0, 0};
+  if (cmask) {
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+      dxF[d] = A.dxb[3 * b + d];
+      dxC[d] = 2.0 * dxF[d];
+      invC[d] = 1.0 / dxC[d];
+      xFmin[d] = A.bxmin[3 * b + d] - 2.0 * dxF[d];
+      xCmin[d] = A.bxmin[3 * b + d] - 2.0 * dxC[d];
+    }
+  }
+  const int total = s_off[nreg];
+  for (int e = t; e < total; e += blockDim.x) {
+    int lo = 0, hi = nreg - 1;  // region r with s_off[r] <= e < s_off[r+1]
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (s_off[mid] <= e) lo = mid;
+      else hi = mid - 1;
+    }
+    const int q = s_q[lo], kind = s_kind[lo];
+    const int dd[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
+    int li = e - s_off[lo];
+    int gc[3] = {0, 0, 0};  // ghosted index 0..19
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+      const int ext = dd[d] ? 2 : BN;
+      const int l = li & (ext - 1);
+      li = dd[d] ? li >> 1 : li >> 4;
+      gc[d] = dd[d] < 0 ? l : (dd[d] > 0 ? BN + 2 + l : 2 + l);
+    }
+    double val;
+    if (kind == AMR_COARSE) {  // prolongation (interpolation_linear)
+      int pc[3] = {0, 0, 0};
+      double eta[3] = {0, 0, 0};
 #pragma unroll
       for (int d = 0; d < NDIM; ++d) {
-        dir[d] = gc[d] < 2 ? -1 : (gc[d] >= BN + 2 ? 1 : 0);
-        inside = inside && dir[d] == 0;
+        const double xF = xFmin[d] + (double(gc[d] + 1) - 0.5) * dxF[d];
+        const int ixC = int((xF - xCmin[d]) * invC[d]) + 1;
+        const double xC = xCmin[d] + (double(ixC) - 0.5) * dxC[d];
+        eta[d] = (xF - xC) * invC[d];
+        pc[d] = ixC - 1;
       }
-      if (inside) continue;
-      const int kind = nt[dir_index(dir[0], dir[1], dir[2])];
-      double val;
-      if (kind == AMR_COARSE) {  // prolongation (interpolation_linear)
-        int pc[3] = {0, 0, 0};
-        double eta[3] = {0, 0, 0};
+      auto at = [&](int a, int bb, int cc) { return psc[a + C * (bb + CY * cc)]; };
+      const double c0 = at(pc[0], pc[1], pc[2]);
+      val = c0;
+      double slope[3] = {0, 0, 0};
 #pragma unroll
-        for (int d = 0; d < NDIM; ++d) {
-          const double xF = xFmin[d] + (double(gc[d] + 1) - 0.5) * dxF[d];
-          const int ixC = int((xF - xCmin[d]) * invC[d]) + 1;
-          const double xC = xCmin[d] + (double(ixC) - 0.5) * dxC[d];
-          eta[d] = (xF - xC) * invC[d];
-          pc[d] = ixC - 1;
-        }
-        auto at = [&](int a, int bb, int cc) { return psc[a + C * (bb + CY * cc)]; };
-        const double c0 = at(pc[0], pc[1], pc[2]);
-        val = c0;
-        double slope[3] = {0, 0, 0};
-#pragma unroll
-        for (int d = 0; d < NDIM; ++d) {
-          const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
-          const double sL = c0 - at(pc[0] - e0, pc[1] - e1, pc[2] - e2);
-          const double sR = at(pc[0] + e0, pc[1] + e1, pc[2] + e2) - c0;
-          const double sC = 0.5 * (sR + sL);
-          const double sg = copysign(1.0, sC);
-          slope[d] = sg * fmax(0.0, fmin(fmin(fabs(sC), sg * sL), sg * sR));
-        }
-#pragma unroll
-        for (int d = 0; d < NDIM; ++d) val = val + slope[d] * eta[d];
-      } else if (kind == AMR_FINE) {  // restriction
-        int P[3] = {0, 0, 0};
-#pragma unroll
-        for (int d = 0; d < NDIM; ++d) P[d] = igb[d] * BN + gc[d] - 2;
-        val = coarse_value<NDIM>(A, L, P[0], P[1], P[2], v);
-      } else {
-        continue;
+      for (int d = 0; d < NDIM; ++d) {
+        const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+        const double sL = c0 - at(pc[0] - e0, pc[1] - e1, pc[2] - e2);
+        const double sR = at(pc[0] + e0, pc[1] + e1, pc[2] + e2) - c0;
+        const double sC = 0.5 * (sR + sL);
+        const double sg = copysign(1.0, sC);
+        slope[d] = sg * fmax(0.0, fmin(fmin(fabs(sC), sg * sL), sg * sR));
       }
-      A.gbuf[ghost_offset<NDIM>(slot, A.nw, v, gc[0] - 2, gc[1] - 2, gc[2] - 2)] = val;
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) val = val + slope[d] * eta[d];
+    } else {  // restriction
+      int P[3] = {0, 0, 0};
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) P[d] = igb[d] * BN + gc[d] - 2;
+      val = coarse_value<NDIM>(A, L, P[0], P[1], P[2], v);
     }
-    __syncthreads();
+    A.gbuf[ghost_offset<NDIM>(slot, A.nw, v, gc[0] - 2, gc[1] - 2, gc[2] - 2)] = val;
   }
 }
 
@@ -317,8 +364,9 @@ __global__ void __launch_bounds__(256) amr_fix_kernel(const AmrFixArgs A) {
 
 cudaError_t launch_amr_ghosts(const AmrGhostArgs &A, int nslots, int ndim, cudaStream_t s) {
   if (nslots <= 0) return cudaSuccess;
-  if (ndim == 2) amr_ghost_kernel<2><<<nslots, 256, sizeof(double) * 12 * 12, s>>>(A);
-  else amr_ghost_kernel<3><<<nslots, 256, sizeof(double) * 12 * 12 * 12, s>>>(A);
+  const dim3 grid(nslots, A.nw);
+  if (ndim == 2) amr_ghost_kernel<2><<<grid, 256, sizeof(double) * 12 * 12, s>>>(A);
+  else amr_ghost_kernel<3><<<grid, 256, sizeof(double) * 12 * 12 * 12, s>>>(A);
   return cudaGetLastError();
 }
 

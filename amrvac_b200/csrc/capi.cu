@@ -768,6 +768,36 @@ int amrvac_gpu_set_amr_grid(amrvac_ctx *c, int nleaf, const int *leaf, const int
 
 int amrvac_gpu_amr_slots(const amrvac_ctx *c) { return c && c->amr ? c->amr->nslots : 0; }
 
+// Average device time of the level-jump ghost pass (on register 0) and of the
+// flux fix (on register 2, whose contents it changes) over reps launches.
+int amrvac_gpu_amr_kernel_ms(amrvac_ctx *c, int reps, double *ghost_ms, double *fix_ms) {
+  if (int r = check_ctx(c, true)) return r;
+  if (!c->amr) return fail(AMRVAC_E_STATE, "amr_kernel_ms: no multi-level grid");
+  if (reps <= 0 || !ghost_ms || !fix_ms) return fail(AMRVAC_E_ARG, "amr_kernel_ms: bad arguments");
+  cudaEvent_t e[3];
+  for (auto &x : e) CK(cudaEventCreate(&x));
+  AmrFixArgs F = c->amr->F;
+  F.w = c->pool[2];
+  if (int r = launch_amr_ghost_pass(c, 0)) return r;  // warm
+  CK(cudaEventRecord(e[0], c->stream));
+  for (int i = 0; i < reps; ++i)
+    if (int r = launch_amr_ghost_pass(c, 0)) return r;
+  CK(cudaEventRecord(e[1], c->stream));
+  for (int i = 0; i < reps; ++i) {
+    CK(launch_amr_fix(F, c->amr->nslots, c->cfg.ndim, c->stream));
+    ++c->launches;
+  }
+  CK(cudaEventRecord(e[2], c->stream));
+  CK(cudaEventSynchronize(e[2]));
+  float a, b;
+  CK(cudaEventElapsedTime(&a, e[0], e[1]));
+  CK(cudaEventElapsedTime(&b, e[1], e[2]));
+  for (auto &x : e) cudaEventDestroy(x);
+  *ghost_ms = a / reps;
+  *fix_ms = b / reps;
+  return 0;
+}
+
 int amrvac_gpu_nblocks(const amrvac_ctx *c) { return c ? c->nblocks : AMRVAC_E_ARG; }
 
 static int ensure_stage(amrvac_ctx *c, size_t doubles) {

@@ -293,6 +293,42 @@ __device__ __forceinline__ int orig_index_rt(int v, int D) {
 // float (mixed form: reconstruction, wave speeds, fluxes and Riemann solver in
 // FP32; conserved state, pressure recovery, RK algebra, flux-divergence
 // accumulation, sources and the small-value fix of wnew in FP64).
+// Mixed form, cold path: a face whose FP32 flux came out non-finite (FP32
+// round-off in a near-degenerate star state of a strong jump, e.g. the HLLD
+// denominator rho (S - u)(S - S_M) - Bn^2) is recomputed in FP64 from the
+// same staged primitives: reconstruction and Riemann flux as the FP64 kernel
+// does them.  It runs in a fix-up pass after the face phase, only when some
+// face of the phase failed, and out of line, so the hot face loop keeps its
+// registers; the flux comes back by value (rotated order, like the FP32 one).
+template <int NW>
+struct FaceFlux64 {
+  double F[NW];
+  uint32_t st;
+};
+
+template <class TF, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS>
+__device__ __noinline__ FaceFlux64<Vars<MHD, NDIR, GLM>::NW> face_retry_fp64(
+    const TF *smem, int D, int b0, int b1, int b2, int b3, int s0, int s1, int s2, int s3, double rd, double cg,
+    const PhysParams P) {
+  using V = Vars<MHD, NDIR, GLM>;
+  constexpr int NW = V::NW;
+  const int base[4] = {b0, b1, b2, b3}, strd[4] = {s0, s1, s2, s3};
+  double wLp[NW], wRp[NW];
+#pragma unroll
+  for (int v = 0; v < NW; ++v) {
+    const int ov = orig_index_rt<MHD, NDIR>(v, D);
+    double q[4];
+#pragma unroll
+    for (int o = 0; o < 4; ++o) q[o] = double(smem[base[o] + ov * strd[o]]);
+    const double d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
+    wLp[v] = q[1] + 0.5 * limited_slope<double, true, LIM>(P.limiter, d1, d0, rd);
+    wRp[v] = q[2] - 0.5 * limited_slope<double, false, LIM>(P.limiter, d2, d1, rd);
+  }
+  FaceFlux64<NW> r;
+  r.st = face_from_states<double, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, cg, r.F);
+  return r;
+}
+
 template <class TF, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS>
 __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_MINB : AMRVAC_STAGE_MINB_MIXED)
     fv_stage_kernel(const StageArgs A) {
@@ -331,6 +367,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
   const int ci = t & (BN - 1), cj = t >> 4;  // cell role for t < 256
   const bool cell_thread = t < BN * BN;
   const bool need_corners = MHD && !GLM && P.divb == DIVB_LINDE;
+  __shared__ int s_retry;  // mixed form: some face of this phase needs the FP64 retry
+  if (t == 0) s_retry = 0;
 #pragma unroll 1
   while (g < gend) {
   const int b = (int)(g / PL);
@@ -416,15 +454,11 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
     for (int D = dlo; D < NDIM; ++D) {
       const int nface = D < 2 ? FB : BN * BN;
 #pragma unroll 1
-      for (int f = t; f < nface; f += STAGE_THREADS) {
-        int fi, fj;
+      // face coordinates and the shared-memory offsets of the 4 stencil
+      // cells (variable 0) with the per-variable strides
+      auto face_at = [&](int f, int &fi, int &fj, int *base, int *strd) {
         if (D == 0) { fj = f / (BN + 1); fi = f - fj * (BN + 1); }
         else { fj = f >> 4; fi = f & (BN - 1); }
-        const TF rd = TF(D == 0 ? rdel[0] : (D == 1 ? rdel[1] : rdel[2]));
-        TF wLp[NW], wRp[NW];
-        // shared-memory offsets of the 4 stencil cells (variable 0) and the
-        // per-variable strides, computed once per face
-        int base[4], strd[4];
 #pragma unroll
         for (int o = 0; o < 4; ++o) {
           if (D == 2) {
@@ -434,6 +468,26 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
             tv.addr(slot, D == 0 ? fi + o - 2 : fi, D == 0 ? fj : fj + o - 2, base[o], strd[o]);
           }
         }
+      };
+      // level jump across this block face: keep the boundary face flux
+      // (store_flux, src/mod_fix_conserve.t:597-648) for the flux fix
+      auto capture = [&](int fi, int fj, const TF *Fr, double sc) {
+        const int pos = D == 0 ? fi : (D == 1 ? fj : k + 1);
+        const int side = pos == 0 ? 0 : (pos == BN ? 1 : -1);
+        if (side >= 0 && ((amr_mask >> (2 * D + side)) & 1)) {
+          const int ta = D == 0 ? fj : fi, tb = D == 2 ? fj : k;
+          double *pf = A.pflux + ((size_t)A.gslot[b] * (2 * NDIM) + 2 * D + side) * NW * (BN * BN);
+#pragma unroll
+          for (int v = 0; v < NW; ++v)
+            pf[orig_index_rt<MHD, NDIR>(v, D) * (BN * BN) + ta + BN * (NDIM == 3 ? tb : 0)] = sc * double(Fr[v]);
+        }
+      };
+      for (int f = t; f < nface; f += STAGE_THREADS) {
+        int fi, fj;
+        const TF rd = TF(D == 0 ? rdel[0] : (D == 1 ? rdel[1] : rdel[2]));
+        TF wLp[NW], wRp[NW];
+        int base[4], strd[4];
+        face_at(f, fi, fj, base, strd);
 #pragma unroll
         for (int v = 0; v < NW; ++v) {
           const int ov = orig_index_rt<MHD, NDIR>(v, D);
@@ -446,6 +500,12 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
         }
         TF Fr[NW];
         stb |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, TF(cg), Fr);
+        if constexpr (!FP64) {
+          bool finite = true;
+#pragma unroll
+          for (int v = 0; v < NW; ++v) finite = finite && isfinite(Fr[v]);
+          if (!finite) s_retry = 1;
+        }
         // FP64: the scaled flux fC = -qdt/dx * f as in the reference; mixed:
         // the FP32 flux, scaled in FP64 by the accumulating cell thread
         const double sc = D == 0 ? dxinv[0] : (D == 1 ? dxinv[1] : dxinv[2]);
@@ -455,21 +515,33 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
           if constexpr (FP64) tv.fb[ov * FB + f] = sc * Fr[v];
           else tv.fb[ov * FB + f] = Fr[v];
         }
-        // level jump across this block face: keep the boundary face flux
-        // (store_flux, src/mod_fix_conserve.t:597-648) for the flux fix
-        if (amr_mask) {
-          const int pos = D == 0 ? fi : (D == 1 ? fj : k + 1);
-          const int side = pos == 0 ? 0 : (pos == BN ? 1 : -1);
-          if (side >= 0 && ((amr_mask >> (2 * D + side)) & 1)) {
-            const int ta = D == 0 ? fj : fi, tb = D == 2 ? fj : k;
-            double *pf = A.pflux + ((size_t)A.gslot[b] * (2 * NDIM) + 2 * D + side) * NW * (BN * BN);
-#pragma unroll
-            for (int v = 0; v < NW; ++v)
-              pf[orig_index_rt<MHD, NDIR>(v, D) * (BN * BN) + ta + BN * (NDIM == 3 ? tb : 0)] = sc * double(Fr[v]);
-          }
-        }
+        if (amr_mask) capture(fi, fj, Fr, sc);
       }
       __syncthreads();
+      if constexpr (!FP64) {
+        if (s_retry) {  // fix-up pass: the faces whose FP32 flux is not finite, in FP64
+          const double sc = D == 0 ? dxinv[0] : (D == 1 ? dxinv[1] : dxinv[2]);
+          for (int f = t; f < nface; f += STAGE_THREADS) {
+            bool finite = true;
+            for (int v = 0; v < NW; ++v) finite = finite && isfinite(tv.fb[v * FB + f]);
+            if (finite) continue;
+            int fi, fj, base[4], strd[4];
+            face_at(f, fi, fj, base, strd);
+            const FaceFlux64<NW> r = face_retry_fp64<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>(
+                smem, D, base[0], base[1], base[2], base[3], strd[0], strd[1], strd[2], strd[3],
+                D == 0 ? rdel[0] : (D == 1 ? rdel[1] : rdel[2]), cg, P);
+            stb |= r.st;
+            TF Fr[NW];
+            for (int v = 0; v < NW; ++v) {
+              Fr[v] = TF(r.F[v]);
+              tv.fb[orig_index_rt<MHD, NDIR>(v, D) * FB + f] = Fr[v];
+            }
+            if (amr_mask) capture(fi, fj, Fr, sc);
+          }
+          __syncthreads();
+          if (t == 0) s_retry = 0;
+        }
+      }
       if (cell_thread) {
         const double sc = FP64 ? 1.0 : (D == 0 ? dxinv[0] : (D == 1 ? dxinv[1] : dxinv[2]));
         if (D == 0) {

@@ -2,7 +2,7 @@
 """Benchmark of the B200 finite-volume block update (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ot128|ot256|kh256]
+                    [--workload ot128|ot256|kh256|ens512|blast512adj|amrblast3d]
 
 A step is one full SSP-RK3 time step of the whole grid: setdt (CFL reduction
 on the device), three fused finite-volume stages, time update.  The default
@@ -51,6 +51,14 @@ WORKLOADS = {
                              "CFL (0.8) dt sequence of the forward run; loss = sum rho^2 on 0.25 < r < 0.35; "
                              "gradient w.r.t. the initial rho field and gamma, checkpoint every 20 steps",
                         physics="hd", adjoint=dict(n=512, steps=200, every=20)),
+    "amrblast3d": dict(desc="3D ideal MHD blast on a Löhner-refined hierarchy: [-0.5,0.5]^3, base 64^3 (4^3 root "
+                            "blocks of 16^3), refine_max_level 4 (effective 512^3); initial tree by settree on the "
+                            "initial state (Löhner, w_refine_weight 0.5 rho + 0.5 e, refine_threshold 0.1, "
+                            "derefine_ratio 1/8, amr_wavefilter 1e-2), kept fixed over the timed steps; gamma 5/3, "
+                            "rho 1, p 0.1 with p 100 for r < 0.1, B = (1,1,0)/sqrt 2, v = 0, psi = 0; HLLD, "
+                            "vanleer, GLM, SSP-RK3, CFL 0.8, periodic; every leaf block in one stage launch, "
+                            "level-jump ghost pass and flux fix per stage",
+                       physics="mhd", amr=dict(nbase=4, levels=4)),
 }
 
 # Signal-speed estimate of the ensemble workload (typeboundspeed).  With the
@@ -249,6 +257,13 @@ def run_reference(args, ws, rank):
                 dt, _ = g.getdt()
                 g.advance(dt, 0.0, nthreads)
             return n * n * 10 / (time.perf_counter() - t0), f"10 SSP-RK3 steps of the {n}^2 blast (forward only)"
+    elif "amr" in WORKLOADS[args.workload]:
+        tree, blocks = _amr_tree_oracle(WORKLOADS[args.workload])
+
+        def sample_fn():  # one multi-level step of the whole hierarchy
+            v, _ = _amr_cpu_sample(tree, blocks, nthreads, 1)
+            return v, (f"1 SSP-RK3 step of the whole {len(tree.leaves)}-block hierarchy "
+                       f"(levels {tree.counts()}), oracle multi-level advance")
     else:
         def sample_fn():
             return cpu_baseline_sample(args.workload, nthreads, 1)
@@ -599,6 +614,226 @@ def run_adjoint(args, ws, rank, local):
         }))
 
 
+# ---------------------------------------------------------------- multi-level blast (3-D MHD)
+AMR_X = ([-0.5] * 3, [0.5] * 3)
+
+
+def _amr_cfg_kwargs():
+    return dict(physics="mhd", ndim=3, ndir=3, flux_scheme="hlld", limiter="vanleer", typedivbfix="glm",
+                courantpar=0.8, gamma=5.0 / 3.0)
+
+
+def _amr_blast_prim(X, Y, Z):
+    r = np.sqrt(X * X + Y * Y + Z * Z)
+    out = np.zeros((9,) + X.shape)
+    out[0] = 1.0
+    out[4] = np.where(r < 0.1, 100.0, 0.1)
+    out[5] = out[6] = 1.0 / np.sqrt(2.0)
+    return out
+
+
+def _amr_init(tree):
+    from tests import _amr as A
+    return A.fill_blocks(tree.leaves, 3, tree.nbase, _amr_blast_prim, "mhd", 3, 5.0 / 3.0, *AMR_X)
+
+
+AMR_WEIGHT = [0.5, 0.0, 0.0, 0.0, 0.5, 0.0, 0.0, 0.0, 0.0]  # rho and e
+
+
+def _amr_tree_gpu(w):
+    """settree with the device's Löhner estimator."""
+    from amrvac_b200 import Context, make_cfg
+    from amrvac_b200.amr import Tree, initial_hierarchy, lohner_flags
+    a = w["amr"]
+    ctx = Context(make_cfg(typeboundary=["periodic"] * 6, **_amr_cfg_kwargs()))
+
+    def err(tree, blocks):
+        r, c, _ = lohner_flags(ctx, tree, blocks, *AMR_X, AMR_WEIGHT)
+        return r, c
+    tree, blocks = initial_hierarchy(Tree(3, [a["nbase"]] * 3, a["levels"]), _amr_init, err)
+    ctx.close()
+    return tree, blocks
+
+
+def _amr_tree_oracle(w):
+    """settree with the oracle's lohner_grid (CPU)."""
+    import oracle as O
+    from amrvac_b200.amr import Tree, initial_hierarchy
+    a = w["amr"]
+    c = _amr_oracle_cfg()
+    wt = np.array(AMR_WEIGHT)
+    lf = np.zeros(9, np.int32)
+
+    def err(tree, blocks):
+        g = O.AmrGrid(c, tree.nbase, *AMR_X, tree.leaves)
+        for b in range(len(tree.leaves)):
+            g.set_block(b, blocks[b])
+        g.getbc()
+        ref, coa = [], []
+        for b, t in enumerate(tree.leaves):
+            _, rr, cc = O.lohner_block(c, g.get_block(b), wt, lf, 1.0e-2, 0.1, 0.125, t[0], tree.max_level)
+            ref.append(bool(rr))
+            coa.append(bool(cc))
+        return ref, coa
+    return initial_hierarchy(Tree(3, [a["nbase"]] * 3, a["levels"]), _amr_init, err)
+
+
+def _amr_oracle_cfg():
+    import oracle as O
+    return O.make_cfg(physics="mhd", ndim=3, ndir=3, flux_scheme="hlld", limiter="vanleer", divb="glm",
+                      courantpar=0.8, gamma=5.0 / 3.0)
+
+
+def _amr_cpu_sample(tree, blocks, nthreads, steps=1):
+    """The oracle's multi-level step (advect1 per stage, flux fix, getbc) on
+    the whole hierarchy."""
+    import oracle as O
+    g = O.AmrGrid(_amr_oracle_cfg(), tree.nbase, *AMR_X, tree.leaves)
+    for b in range(len(tree.leaves)):
+        g.set_block(b, blocks[b])
+    g.getbc()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt, cm = g.getdt()
+        g.advance(dt, cm, nthreads)
+    el = time.perf_counter() - t0
+    return tree.cells() * steps / el, g
+
+
+def run_amr(args, ws, rank, local):
+    import torch
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    from amrvac_b200 import Context, make_cfg
+    wl = args.workload
+    w = WORKLOADS[wl]
+    t_build = time.perf_counter()
+    tree, blocks = _amr_tree_gpu(w)
+    t_build = time.perf_counter() - t_build
+    cells = tree.cells()
+    cfg = make_cfg(typeboundary=["periodic"] * 6, **_amr_cfg_kwargs())
+    ctx = Context(cfg)
+    ctx.set_amr_grid(tree.leaves, tree.nbase, *AMR_X)
+    ctx.upload(blocks)
+    nw = ctx.nw
+    zchunk, tune_ms = ctx.autotune(reps=3, cache=False)
+    ctx.upload(blocks)
+    # FP64 parity of the first step against the oracle on the same hierarchy
+    parity = None
+    if rank == 0 and not args.no_cpu_baseline:
+        nthreads = os.cpu_count() or 1
+        v_cpu, g = _amr_cpu_sample(tree, blocks, nthreads, 1)
+        ctx.set_time(0.0, 1.0e99, 0.0)
+        ctx.step()
+        got = ctx.download()
+        worst = 0.0
+        for b in range(len(tree.leaves)):
+            ref = g.get_block(b)[:, 2:18, 2:18, 2:18]
+            d = np.abs(got[b][:, 2:18, 2:18, 2:18] - ref).max() / max(np.abs(ref).max(), 1e-300)
+            worst = max(worst, float(d))
+        parity = {"steps": 1, "max_rel_diff_vs_oracle": worst, "tolerance": 1e-12, "ok": worst <= 1e-12}
+        ctx.upload(blocks)
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.run_timed(max(args.warmup, 3))
+    if ctx.status():
+        raise SystemExit(f"bench.py: runtime status {ctx.status()} during warm-up")
+    _barrier(ws)
+    torch.cuda.synchronize()
+    l0 = ctx.launch_count()
+    with ClockSampler(local) as clk:
+        total_ms, stage_ms, getdt_ms = ctx.run_timed(args.steps)
+    torch.cuda.synchronize()
+    _barrier(ws)
+    launches = ctx.launch_count() - l0
+    st = ctx.status()
+    state64 = ctx.download()
+    ghost_ms, fix_ms = ctx.amr_kernel_ms(10)
+    tmax = _allmax(total_ms, ws)
+    value = ws * cells * args.steps / (tmax * 1e-3)
+    nstage = 3 * args.steps
+    stage_kernel_s = (stage_ms / nstage - ghost_ms - fix_ms) * 1e-3
+    peaks, peak_kind = _measured_peaks()
+    bytes_per_cell = (2 + 3 + 3) / 3.0 * 8 * nw
+    achieved_gbs = bytes_per_cell * cells / stage_kernel_s / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved_gbs / peaks["hbm_gbs"], "peak_source": peak_kind, "traffic": None,
+                "kernel": "fv_stage_kernel", "algorithmic_bytes_per_cell": bytes_per_cell,
+                "avg_launch_ms": stage_kernel_s * 1e3, "launches": nstage,
+                "amr_overhead_ms_per_stage": {"ghost_pass": ghost_ms, "flux_fix": fix_ms}}
+    # e2e through the public API from pinned host blocks
+    e2e = None
+    try:
+        pinned = torch.empty(blocks.shape, dtype=torch.float64).pin_memory()
+        host = pinned.numpy()
+        host[...] = blocks
+        s = torch.cuda.ExternalStream(ctx.stream_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(s)
+        ctx.upload(host)
+        ctx.set_time(0.0, 1.0e99, 0.0)
+        for _ in range(args.steps):
+            ctx.step()
+            ctx.get_time()
+            ctx.status()
+        ctx.L.amrvac_gpu_download(ctx.h, 0, 0, ctx.nblocks, host.ctypes.data_as(
+            __import__("ctypes").POINTER(__import__("ctypes").c_double)))
+        e1.record(s)
+        e1.synchronize()
+        e2e_ms = _allmax(e0.elapsed_time(e1), ws)
+        e2e = {"value": ws * cells * args.steps / (e2e_ms * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": (blocks.nbytes + 32 * args.steps) / args.steps,
+               "d2h_bytes_per_step": (blocks.nbytes + 28 * args.steps) / args.steps,
+               "what": "C-ABI from pinned host block arrays: upload, K steps with a host round trip each, "
+                       "download with ghost cells (level-jump ghosts included); transfers amortised over K"}
+    except Exception as ex:
+        e2e = {"value": None, "unit": UNIT, "error": str(ex)}
+    mixed = None
+    try:
+        cm = Context(make_cfg(precision="mixed", typeboundary=["periodic"] * 6, **_amr_cfg_kwargs()))
+        cm.set_amr_grid(tree.leaves, tree.nbase, *AMR_X)
+        cm.upload(blocks)
+        zm, _ = cm.autotune(reps=3, cache=False)
+        cm.upload(blocks)
+        cm.set_time(0.0, 1.0e99, 0.0)
+        cm.run_timed(max(args.warmup, 3))
+        _barrier(ws)
+        mt, ms_stage, _ = cm.run_timed(args.steps)
+        mt = _allmax(mt, ws)
+        ref = state64[:, :, 2:18, 2:18, 2:18]
+        got = cm.download()[:, :, 2:18, 2:18, 2:18]
+        l1 = [float(np.abs(got[:, v] - ref[:, v]).sum() / max(np.abs(ref[:, v]).sum(), 1e-300))
+              for v in range(ref.shape[1])]
+        mixed = {"value": ws * cells * args.steps / (mt * 1e-3), "unit": UNIT, "ms_per_step": mt / args.steps,
+                 "speedup_vs_fp64": total_ms / mt, "zchunk": zm, "l1_rel_err_vs_fp64_per_var": l1,
+                 "status": cm.status()}
+        cm.close()
+    except Exception as ex:
+        mixed = {"error": str(ex)}
+    cpu = None
+    if parity is not None:
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": "1 SSP-RK3 step of the whole hierarchy (oracle multi-level advance)"}
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tmax / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w["desc"], "cells": cells, "blocks": ctx.nblocks, "nw": nw,
+                       "blocks_per_level": tree.counts(), "blocks_next_to_a_level_jump": ctx.amr_slots,
+                       "tree_build_s": t_build, "zchunk": zchunk, "autotuned_stage_ms": tune_ms,
+                       "parallelism": "replicas" if ws > 1 else "single GPU",
+                       "l2": "no flush: working set %.0f MB (3 registers) > 126 MB L2" % (3 * cells * nw * 8 / 1e6),
+                       "stage_weighted_cell_updates_per_s": 3 * value},
+            "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "mixed": mixed,
+            "gpu_launches": launches, "clocks": clk.summary(), "status": st,
+            "kernel_ms": {"stage_total_incl_amr": stage_ms, "getdt_total": getdt_ms, "step_total": total_ms},
+        }
+        print(json.dumps(out))
+    ctx.close()
+
+
 def run_ours(args, ws, rank, local):
     import torch
     if not torch.cuda.is_available():
@@ -756,6 +991,8 @@ def main():
             run_ensemble(args, ws, rank, local)
         elif "adjoint" in WORKLOADS[args.workload]:
             run_adjoint(args, ws, rank, local)
+        elif "amr" in WORKLOADS[args.workload]:
+            run_amr(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

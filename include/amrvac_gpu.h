@@ -152,6 +152,9 @@ int amrvac_gpu_set_amr_grid(amrvac_ctx *ctx, int nleaf, const int *leaf, const i
                             const double *xprobmax);
 /* Blocks next to a level jump (0 on a single-level grid). */
 int amrvac_gpu_amr_slots(const amrvac_ctx *ctx);
+/* Average device time of the level-jump ghost pass (register 0) and of the
+ * flux fix (applied to register 2, which it changes) over reps launches. */
+int amrvac_gpu_amr_kernel_ms(amrvac_ctx *ctx, int reps, double *ghost_ms, double *fix_ms);
 
 /* Copy n blocks starting at `first` between host Fortran arrays and register
  * reg (0 = ps, 1 = ps1, 2 = ps2).  Upload reads interior cells only; download

@@ -172,3 +172,50 @@ def test_amr_refuses_bad_trees():
     ctx.set_uniform_grid([32, 32], [0, 0], [1, 1])
     assert ctx.amr_slots == 0
     ctx.close()
+
+
+def test_settree_with_device_lohner_matches_oracle(oracle_lib):
+    """The initial hierarchy built with the device's Löhner estimator (ghost
+    cells across level jumps from the device ghost pass) is the one the
+    oracle's lohner_grid builds, level by level."""
+    _cuda()
+    O = oracle_lib
+    from amrvac_b200 import Context, make_cfg
+    from amrvac_b200.amr import Tree, initial_hierarchy, lohner_flags
+    nd, nb, levels = 2, [4, 4], 4
+    xmin, xmax = [-0.5, -0.5], [0.5, 0.5]
+
+    def prim(X, Y, Z):
+        r = np.sqrt(X * X + Y * Y)
+        out = np.zeros((4,) + X.shape)
+        out[0] = 1.0 + 0.5 * (r < 0.2)
+        out[3] = np.where(r < 0.1, 10.0, 0.1)
+        return out
+
+    def init(tree):
+        return A.fill_blocks(tree.leaves, nd, nb, prim, "hd", nd, 1.4, xmin, xmax)
+
+    weight = np.array([0.5, 0.0, 0.0, 0.5])
+    ctx = Context(make_cfg(physics="hd", ndim=2, gamma=1.4, typeboundary=["periodic"] * 4))
+
+    def err_gpu(tree, blocks):
+        r, c, _ = lohner_flags(ctx, tree, blocks, xmin, xmax, weight)
+        return r, c
+
+    ocfg = O.make_cfg(physics="hd", ndim=2, gamma=1.4)
+
+    def err_oracle(tree, blocks):
+        g = O.AmrGrid(ocfg, nb, xmin, xmax, tree.leaves)
+        for b in range(len(tree.leaves)):
+            g.set_block(b, blocks[b])
+        g.getbc()
+        out = [O.lohner_block(ocfg, g.get_block(b), weight, np.zeros(4, np.int32), 1e-2, 0.1, 0.125, t[0], levels)
+               for b, t in enumerate(tree.leaves)]
+        return [bool(o[1]) for o in out], [bool(o[2]) for o in out]
+
+    tg, bg = initial_hierarchy(Tree(nd, nb, levels), init, err_gpu)
+    to, bo = initial_hierarchy(Tree(nd, nb, levels), init, err_oracle)
+    assert tg.leaves == to.leaves
+    assert max(tg.level_of()) == levels and tg.balanced()
+    assert np.array_equal(bg, bo)
+    ctx.close()
