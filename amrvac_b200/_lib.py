@@ -79,6 +79,7 @@ SIGNATURES = [
     ("amrvac_gpu_nblocks", _i, [_vp]),
     ("amrvac_gpu_set_amr_grid", _i, [_vp, _i, _ip, _ip, _dp, _dp]),
     ("amrvac_gpu_amr_slots", _i, [_vp]),
+    ("amrvac_gpu_amr_regrid", _i, [_vp, _i, _ip, _ip]),
     ("amrvac_gpu_amr_kernel_ms", _i, [_vp, _i, _dp, _dp]),
     ("amrvac_gpu_upload", _i, [_vp, _i, _i, _i, _dp]),
     ("amrvac_gpu_download", _i, [_vp, _i, _i, _i, _dp]),

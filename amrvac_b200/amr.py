@@ -240,3 +240,37 @@ def lohner_flags(ctx, tree, blocks, xprobmin, xprobmax, weight, logflag=None, re
                                block_level=tree.level_of())
     flags = np.asarray(flags)
     return (flags & 1).astype(bool), (flags & 2).astype(bool), errmax
+
+
+def ops(origin):
+    """The op table of amrvac_gpu_amr_regrid from Tree.regrid's origin list."""
+    out = np.zeros((len(origin), 9), np.int32)
+    for b, o in enumerate(origin):
+        if o[0] == "same":
+            out[b, :2] = (0, o[1])
+        elif o[0] == "child":
+            out[b, :3] = (1, o[1], o[2])
+        else:
+            out[b, 0] = 2
+            out[b, 1:1 + len(o[1])] = o[1]
+    return out
+
+
+def regrid(ctx, tree, weight, logflag=None, refine_threshold=0.1, derefine_ratio=0.125, amr_wavefilter=1.0e-2):
+    """resettree on the resident state: errest with the device Löhner
+    estimator (register ps, the current leaves), the tree decision on the
+    host (Tree.regrid), the state remap on the device.  Returns the new tree
+    (the same object if nothing changes)."""
+    L = tree.max_level
+
+    def per_level(x):
+        return [float(x)] * L if np.isscalar(x) else list(x)
+    flags, _ = ctx.lohner(weight, logflag, refine_max_level=L, refine_threshold=per_level(refine_threshold),
+                          derefine_ratio=per_level(derefine_ratio), amr_wavefilter=per_level(amr_wavefilter),
+                          block_level=tree.level_of())
+    flags = np.asarray(flags)
+    nt, origin = tree.regrid((flags & 1).astype(bool), (flags & 2).astype(bool))
+    if nt.leaves == tree.leaves:
+        return tree
+    ctx.amr_regrid(nt.leaves, ops(origin))
+    return nt

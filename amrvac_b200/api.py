@@ -85,6 +85,18 @@ class Context:
                                                   _dp(a), _dp(b)), "set_amr_grid")
         self.nblocks = self.L.amrvac_gpu_nblocks(self.h)
 
+    def amr_regrid(self, leaves, ops):
+        """Regrid in place: new leaves and per new leaf the op row (9 ints)
+        saying how its state comes from the old tree (amrvac_b200.amr.ops)."""
+        lv = np.zeros((len(leaves), 4), np.int32)
+        for b, t in enumerate(leaves):
+            lv[b, :len(t)] = t
+        op = np.ascontiguousarray(ops, dtype=np.int32).reshape(len(leaves), 9)
+        ip = ctypes.POINTER(ctypes.c_int)
+        _lib.check(self.L.amrvac_gpu_amr_regrid(self.h, len(leaves), lv.ctypes.data_as(ip), op.ctypes.data_as(ip)),
+                   "amr_regrid")
+        self.nblocks = self.L.amrvac_gpu_nblocks(self.h)
+
     @property
     def amr_slots(self):
         return self.L.amrvac_gpu_amr_slots(self.h)

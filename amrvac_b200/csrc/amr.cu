@@ -362,6 +362,84 @@ __global__ void __launch_bounds__(256) amr_fix_kernel(const AmrFixArgs A) {
     }
 }
 
+// Regrid (amr_coarsen_refine, src/amr/mod_coarsen_refine.t:20-182): one CTA
+// per new leaf.  A refined child takes prolong_2nd (src/amr/mod_refine.t:
+// 81-167): per coarse cell of its footprint in the parent, monotonized-central
+// slopes from the parent's neighbours (across the parent's faces through the
+// old tree's gather, i.e. its getbc ghost values), then
+// w = wCo + (slope_1 eta_1) + (slope_2 eta_2) [+ (slope_3 eta_3)], left to
+// right, eta = 0.5 (i - ixFi - 0.5) = -1/4 or +1/4.  A coarsened parent takes
+// coarsen_grid of its children (src/amr/mod_coarsen.t:12-79): the average of
+// 2^d fine cells, x fastest.
+template <int NDIM>
+__global__ void __launch_bounds__(256) amr_remap_kernel(const AmrRemapArgs A) {
+  constexpr int NY = NDIM >= 2 ? BN : 1, NZ = NDIM >= 3 ? BN : 1, NC = BN * NY * NZ;
+  const int nb = blockIdx.x;
+  const int *op = A.op + 9 * nb;
+  const int kind = op[0];
+  const StageArgs &S = A.old;
+  for (int e = threadIdx.x; e < A.nw * NC; e += blockDim.x) {
+    const int v = e / NC, cell = e - v * NC;
+    const int i = cell & (BN - 1), j = NDIM >= 2 ? (cell >> 4) & (BN - 1) : 0, k = NDIM >= 3 ? cell >> 8 : 0;
+    double val;
+    if (kind == 0) {
+      val = S.uin[cell_offset<NDIM>(op[1], A.nw, v, i, j, k)];
+    } else if (kind == 1) {
+      const int p = op[1], cb = op[2];
+      const int co[3] = {(BN / 2) * (cb & 1) + (i >> 1), NDIM >= 2 ? (BN / 2) * ((cb >> 1) & 1) + (j >> 1) : 0,
+                         NDIM >= 3 ? (BN / 2) * ((cb >> 2) & 1) + (k >> 1) : 0};
+      auto wco = [&](int di, int dj, int dk) -> double {
+        int ii = co[0] + di, jj = co[1] + dj, kk = co[2] + dk;
+        uint32_t flip;
+        const int blk = resolve_cell<NDIM>(S, p, ii, jj, kk, flip);
+        const double x = blk >= 0 ? S.uin[cell_offset<NDIM>(blk, A.nw, v, ii, jj, kk)]
+                                  : S.gbuf[ghost_offset<NDIM>(-2 - blk, A.nw, v, ii, jj, kk)];
+        return ((flip >> v) & 1u) ? -x : x;
+      };
+      const double c0 = wco(0, 0, 0);
+      double slope[3] = {0, 0, 0};
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) {
+        const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+        const double sL = c0 - wco(-e0, -e1, -e2);
+        const double sR = wco(e0, e1, e2) - c0;
+        const double sC = 0.5 * (sR + sL);
+        const double sg = copysign(1.0, sC);
+        slope[d] = sg * fmax(0.0, fmin(fmin(fabs(sC), sg * sL), sg * sR));
+      }
+      const int f[3] = {i & 1, j & 1, k & 1};
+      val = c0;
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) val = val + slope[d] * (0.5 * (double(f[d]) - 0.5));
+    } else {
+      const int cbit = (i >> 3) | (NDIM >= 2 ? ((j >> 3) << 1) : 0) | (NDIM >= 3 ? ((k >> 3) << 2) : 0);
+      const double *w = S.uin + cell_offset<NDIM>(op[1 + cbit], A.nw, v, 2 * (i & 7), NDIM >= 2 ? 2 * (j & 7) : 0,
+                                                  NDIM >= 3 ? 2 * (k & 7) : 0);
+      double sum = w[0];
+      sum = sum + w[1];
+      if constexpr (NDIM > 1) {
+        sum = sum + w[BN];
+        sum = sum + w[BN + 1];
+      }
+      if constexpr (NDIM > 2) {
+        sum = sum + w[BN * BN];
+        sum = sum + w[BN * BN + 1];
+        sum = sum + w[BN * BN + BN];
+        sum = sum + w[BN * BN + BN + 1];
+      }
+      val = sum * (1.0 / double(1 << NDIM));
+    }
+    A.unew[cell_offset<NDIM>(nb, A.nw, v, i, j, k)] = val;
+  }
+}
+
+cudaError_t launch_amr_remap(const AmrRemapArgs &A, int nnew, int ndim, cudaStream_t s) {
+  if (nnew <= 0) return cudaSuccess;
+  if (ndim == 2) amr_remap_kernel<2><<<nnew, 256, 0, s>>>(A);
+  else amr_remap_kernel<3><<<nnew, 256, 0, s>>>(A);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_amr_ghosts(const AmrGhostArgs &A, int nslots, int ndim, cudaStream_t s) {
   if (nslots <= 0) return cudaSuccess;
   const dim3 grid(nslots, A.nw);

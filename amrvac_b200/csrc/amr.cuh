@@ -53,7 +53,19 @@ struct AmrFixArgs {
   const int *iblocks, *gslot, *ntype, *child;  // child[(b*27+q)*8 + cbits]
 };
 
+// Regrid: the state of the new tree's leaves from the old tree's register 0.
+// op[9*b]: 0 copy of old leaf op[1]; 1 child op[2] (bits x, y, z) of old
+// leaf op[1], by prolong_2nd; 2 parent of the old leaves op[1..2^d] (child
+// bits order), by coarsen_grid.
+struct AmrRemapArgs {
+  StageArgs old;        // the old tree: uin = old register 0, nbr, gbuf (ghost pass done)
+  const int *op;        // [nnew][9]
+  double *unew;         // the new register 0
+  int nw;
+};
+
 cudaError_t launch_amr_ghosts(const AmrGhostArgs &A, int nslots, int ndim, cudaStream_t s);
+cudaError_t launch_amr_remap(const AmrRemapArgs &A, int nnew, int ndim, cudaStream_t s);
 cudaError_t launch_amr_fix(const AmrFixArgs &A, int nslots, int ndim, cudaStream_t s);
 
 }  // namespace amrvac

@@ -104,6 +104,9 @@ struct AmrDev {
   AmrGhostArgs G;
   AmrFixArgs F;
   int *d_face = nullptr, *d_gslot = nullptr;
+  std::vector<int> h_leaf;    // [nblocks][4] level, ig0, ig1, ig2 (regrid checks)
+  int nbase[3] = {1, 1, 1};
+  double xmin[3] = {0, 0, 0}, xmax[3] = {1, 1, 1};
   ~AmrDev() {
     cudaFree(d_int);
     cudaFree(d_bxmin);
@@ -429,7 +432,8 @@ int amrvac_gpu_destroy(amrvac_ctx *c) {
   return 0;
 }
 
-static int set_blocks_impl(amrvac_ctx *c, int nblocks, const double *dx, const int *neighbor, bool level_jumps);
+static int set_blocks_impl(amrvac_ctx *c, int nblocks, const double *dx, const int *neighbor, bool level_jumps,
+                           double *adopt_reg0 = nullptr);
 
 int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const int *neighbor) {
   return set_blocks_impl(c, nblocks, dx, neighbor, false);
@@ -437,7 +441,11 @@ int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const in
 
 // neighbor entries: block id, -1 physical boundary, and (multi-level grids,
 // internal) <= -2 for a level jump whose ghost cells come from the ghost pass.
-static int set_blocks_impl(amrvac_ctx *c, int nblocks, const double *dx, const int *neighbor, bool level_jumps) {
+// adopt_reg0: a device buffer of nblocks blocks that becomes register 0 (the
+// state after a regrid) instead of a zeroed one; it is the caller's to free
+// unless c->pool[0] == adopt_reg0 afterwards.
+static int set_blocks_impl(amrvac_ctx *c, int nblocks, const double *dx, const int *neighbor, bool level_jumps,
+                           double *adopt_reg0) {
   if (int r = check_ctx(c, false)) return r;
   if (nblocks <= 0 || !dx || !neighbor) return fail(AMRVAC_E_ARG, "bad block description");
   const int nd = c->cfg.ndim;
@@ -493,6 +501,10 @@ static int set_blocks_impl(amrvac_ctx *c, int nblocks, const double *dx, const i
   c->nblocks = nblocks;
   const size_t bytes = sizeof(double) * c->per_block * c->nw * nblocks;
   for (int r = 0; r < 3; ++r) {
+    if (r == 0 && adopt_reg0) {
+      c->pool[0] = adopt_reg0;
+      continue;
+    }
     CK(cudaMalloc(&c->pool[r], bytes));
     CK(cudaMemsetAsync(c->pool[r], 0, bytes, c->stream));
   }
@@ -557,8 +569,34 @@ int amrvac_gpu_set_uniform_grid(amrvac_ctx *c, const int *domain_nx, const doubl
 // cells are read through the neighbour table as on a uniform grid; the ghost
 // cells of every level-jump direction are written by the ghost pass before
 // each stage, and every stage ends with fix_conserve.
+static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *nbase, const double *xprobmin,
+                         const double *xprobmax, const int *ops);
+
 int amrvac_gpu_set_amr_grid(amrvac_ctx *c, int nleaf, const int *leaf, const int *nbase, const double *xprobmin,
                             const double *xprobmax) {
+  return amr_grid_impl(c, nleaf, leaf, nbase, xprobmin, xprobmax, nullptr);
+}
+
+// Regrid in place (amr_coarsen_refine): the new leaves and, per new leaf, how
+// its state comes from the old tree's register 0 (see AmrRemapArgs).  The
+// domain and root blocks stay those of the current grid; registers 1 and 2
+// are scratch afterwards.
+int amrvac_gpu_amr_regrid(amrvac_ctx *c, int nleaf, const int *leaf, const int *op) {
+  if (int r = check_ctx(c, true)) return r;
+  if (!c->amr) return fail(AMRVAC_E_STATE, "amr_regrid: no multi-level grid (amrvac_gpu_set_amr_grid)");
+  if (!op) return fail(AMRVAC_E_ARG, "amr_regrid: null op table");
+  int nbase[3];
+  double xmin[3], xmax[3];
+  for (int d = 0; d < 3; ++d) {
+    nbase[d] = c->amr->nbase[d];
+    xmin[d] = c->amr->xmin[d];
+    xmax[d] = c->amr->xmax[d];
+  }
+  return amr_grid_impl(c, nleaf, leaf, nbase, xmin, xmax, op);
+}
+
+static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *nbase, const double *xprobmin,
+                         const double *xprobmax, const int *ops) {
   if (int r = check_ctx(c, false)) return r;
   const int nd = c->cfg.ndim;
   if (nleaf <= 0 || !leaf || !nbase || !xprobmin || !xprobmax) return fail(AMRVAC_E_ARG, "set_amr_grid: bad arguments");
@@ -716,10 +754,82 @@ int amrvac_gpu_set_amr_grid(amrvac_ctx *c, int nleaf, const int *leaf, const int
         nbr[(size_t)b * ndir3 + q] = -2 - gslot[b];
       }
     }
-  if (int r = set_blocks_impl(c, nb, dx.data(), nbr.data(), true)) return r;
+  // regrid: build the new register 0 from the old tree before it goes away
+  double *newreg = nullptr;
+  if (ops) {
+    const int nold = c->nblocks, nch = 1 << nd;
+    const std::vector<int> &old_leaf = c->amr->h_leaf;
+    auto same_block = [&](int ob, int L, const int *g) {
+      if (old_leaf[4 * ob] != L) return false;
+      for (int d = 0; d < nd; ++d)
+        if (old_leaf[4 * ob + 1 + d] != g[d]) return false;
+      return true;
+    };
+    for (int b = 0; b < nb; ++b) {
+      const int *o = ops + 9 * (size_t)b;
+      const int L = lev[b];
+      const int *g = &ig[3 * b];
+      bool ok = true;
+      if (o[0] == 0) {
+        ok = o[1] >= 0 && o[1] < nold && same_block(o[1], L, g);
+      } else if (o[0] == 1) {
+        int pg[3] = {0, 0, 0}, cb = 0;
+        for (int d = 0; d < nd; ++d) {
+          pg[d] = g[d] >> 1;
+          cb |= (g[d] & 1) << d;
+        }
+        ok = o[1] >= 0 && o[1] < nold && o[2] == cb && L > 1 && same_block(o[1], L - 1, pg);
+      } else if (o[0] == 2) {
+        for (int q = 0; q < nch && ok; ++q) {
+          int cg[3] = {0, 0, 0};
+          for (int d = 0; d < nd; ++d) cg[d] = 2 * g[d] + ((q >> d) & 1);
+          ok = o[1 + q] >= 0 && o[1 + q] < nold && same_block(o[1 + q], L + 1, cg);
+        }
+      } else {
+        ok = false;
+      }
+      if (!ok) return fail(AMRVAC_E_ARG, "amr_regrid: op " + std::to_string(b) + " does not match the old and new trees");
+    }
+    if (int r = launch_amr_ghost_pass(c, 0)) return r;  // the old tree's level-jump ghosts
+    int *d_op = nullptr;
+    cudaError_t e = cudaMalloc(&newreg, sizeof(double) * c->per_block * c->nw * nb);
+    if (e == cudaSuccess) e = cudaMalloc(&d_op, sizeof(int) * 9 * (size_t)nb);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_op, ops, sizeof(int) * 9 * (size_t)nb, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+      AmrRemapArgs R;
+      std::memset(&R, 0, sizeof(R));
+      R.old = stage_args(c, 0, 0, 0, 0.0, 1.0, 1.0);
+      R.op = d_op;
+      R.unew = newreg;
+      R.nw = c->nw;
+      e = launch_amr_remap(R, nb, nd, c->stream);
+      ++c->launches;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_op);
+    if (e != cudaSuccess) {
+      cudaFree(newreg);
+      return cuda_fail(e, "amr_regrid");
+    }
+  }
+  if (int r = set_blocks_impl(c, nb, dx.data(), nbr.data(), true, newreg)) {
+    if (newreg && c->pool[0] != newreg) cudaFree(newreg);
+    return r;
+  }
   // device copies
   AmrDev *A = new AmrDev();
   c->amr = A;
+  A->h_leaf.assign(4 * (size_t)nb, 0);
+  for (int b = 0; b < nb; ++b) {
+    A->h_leaf[4 * b] = lev[b];
+    for (int d = 0; d < nd; ++d) A->h_leaf[4 * b + 1 + d] = ig[3 * b + d];
+  }
+  for (int d = 0; d < 3; ++d) {
+    A->nbase[d] = d < nd ? nbase[d] : 1;
+    A->xmin[d] = d < nd ? xprobmin[d] : 0.0;
+    A->xmax[d] = d < nd ? xprobmax[d] : 1.0;
+  }
   A->nslots = (int)iblocks.size();
   const size_t ns = std::max<size_t>(1, iblocks.size());
   std::vector<int> ints;

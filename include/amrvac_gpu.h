@@ -150,6 +150,16 @@ int amrvac_gpu_nblocks(const amrvac_ctx *ctx);
  * returns those ghost cells too.  Replaces any previous block set. */
 int amrvac_gpu_set_amr_grid(amrvac_ctx *ctx, int nleaf, const int *leaf, const int *nbase, const double *xprobmin,
                             const double *xprobmax);
+/* Regrid in place (replaces amr_coarsen_refine, src/amr/mod_coarsen_refine.t:
+ * 20-182, for a tree the host has decided): the new leaves as for
+ * amrvac_gpu_set_amr_grid (same domain and root blocks), and per new leaf
+ * op[9*b]: {0, old} copy of an old leaf; {1, old parent, child bits} a child
+ * of a refined old leaf, by prolong_2nd (src/amr/mod_refine.t:81-167) from
+ * the parent and its getbc ghost values; {2, old children in child-bit
+ * order} a coarsened parent, by coarsen_grid (src/amr/mod_coarsen.t:12-79).
+ * Ops that do not match the old and new trees are refused.  Register 0
+ * carries the state over; registers 1 and 2 are scratch afterwards. */
+int amrvac_gpu_amr_regrid(amrvac_ctx *ctx, int nleaf, const int *leaf, const int *op);
 /* Blocks next to a level jump (0 on a single-level grid). */
 int amrvac_gpu_amr_slots(const amrvac_ctx *ctx);
 /* Average device time of the level-jump ghost pass (register 0) and of the

@@ -104,6 +104,8 @@ def lib():
         L.orc_amr_advect1.argtypes = [vp, ctypes.c_int, ctypes.c_int, d, d, d, ctypes.c_int]
         L.orc_amr_combine_reg.argtypes = [vp, ctypes.c_int, d, ctypes.c_int, d, ctypes.c_int]
         L.orc_amr_advance.argtypes = [vp, d, d, ctypes.c_int]
+        L.orc_amr_remap.restype = vp
+        L.orc_amr_remap.argtypes = [vp, ctypes.c_int, ip, ip]
         L.orc_lohner_block.restype = None
         L.orc_lohner_block.argtypes = [cp, dp, dp, ip, d, d, d, ctypes.c_int, ctypes.c_int, dp, ip, ip]
         L.orc_dual_run.restype = ctypes.c_int
@@ -375,3 +377,16 @@ class AmrGrid:
 
     def advance(self, dt, cmax_global=0.0, nthreads=0):
         return lib().orc_amr_advance(self.h, dt, cmax_global, nthreads)
+
+    def remap(self, leaves, ops):
+        """The regridded grid (amr_coarsen_refine): new leaves, and per new
+        leaf the op row of amrvac_b200.amr.ops; getbc is run on it."""
+        lv = np.ascontiguousarray(np.array([list(t) + [0] * (4 - len(t)) for t in leaves], np.int32).reshape(-1))
+        op = np.ascontiguousarray(np.asarray(ops, np.int32).reshape(-1))
+        new = AmrGrid.__new__(AmrGrid)
+        new.c = self.c
+        new.h = lib().orc_amr_remap(self.h, len(leaves), _ip(lv), _ip(op))
+        new.nblocks = len(leaves)
+        new.shape = self.shape
+        lib().orc_amr_getbc(new.h)
+        return new

@@ -2343,4 +2343,69 @@ int orc_amr_advance(orc_amr *a, double dt, double cmax_global, int nthreads) {
   return st;
 }
 
+// prolong_2nd (src/amr/mod_refine.t:81-167) for a child of a refined block
+// and coarsen_grid (src/amr/mod_coarsen.t:12-79) for a coarsened parent, on
+// the old grid's ghosted register 0.
+orc_amr *orc_amr_remap(const orc_amr *old, int nleaf, const int *leaf, const int *op) {
+  const AmrGrid *O = reinterpret_cast<const AmrGrid *>(old);
+  orc_amr *res = orc_amr_create(&O->s.c, O->nbase, O->xmin, O->xmax, nleaf, leaf);
+  AmrGrid *N = reinterpret_cast<AmrGrid *>(res);
+  const Geo &g = O->s.g;
+  const int nd = O->ndim, nw = O->s.x.nw;
+  const double cofi = 1.0 / double(1 << nd);
+  for (int b = 0; b < nleaf; ++b) {
+    const int *o = op + 9 * (size_t)b;
+    double *wn = &N->reg[0][N->bsize * b];
+    if (o[0] == 0) {
+      std::memcpy(wn, &O->reg[0][O->bsize * o[1]], sizeof(double) * O->bsize);
+      continue;
+    }
+    for (int iw = 0; iw < nw; ++iw)
+      for (int k = 0; k < (nd > 2 ? 16 : 1); ++k)
+        for (int j = 0; j < (nd > 1 ? 16 : 1); ++j)
+          for (int i = 0; i < 16; ++i) {
+            const int F[3] = {i, j, k};
+            double val;
+            if (o[0] == 1) {
+              const double *wc = &O->reg[0][O->bsize * o[1]];
+              int co[3] = {0, 0, 0};  // 0-based ghosted index of the coarse cell
+              for (int d = 0; d < nd; ++d) co[d] = 2 + 8 * ((o[2] >> d) & 1) + (F[d] >> 1);
+              auto wco = [&](int a, int bb, int cc) { return wc[g.idx(a, bb, cc) + g.cells * (size_t)iw]; };
+              const double c0 = wco(co[0], co[1], co[2]);
+              double slope[3] = {0, 0, 0};
+              for (int d = 0; d < nd; ++d) {
+                int h[3] = {co[0], co[1], co[2]}, jx[3] = {co[0], co[1], co[2]};
+                h[d] -= 1;
+                jx[d] += 1;
+                const double slopeL = c0 - wco(h[0], h[1], h[2]);
+                const double slopeR = wco(jx[0], jx[1], jx[2]) - c0;
+                const double slopeC = 0.5 * (slopeR + slopeL);
+                const double signC = std::copysign(1.0, slopeC);
+                slope[d] = signC * std::max(0.0, std::min(std::min(std::fabs(slopeC), signC * slopeL), signC * slopeR));
+              }
+              val = c0;
+              for (int d = 0; d < nd; ++d) val = val + slope[d] * (0.5 * (double(F[d] & 1) - 0.5));
+            } else {
+              int cb = 0;
+              for (int d = 0; d < nd; ++d) cb |= (F[d] >> 3) << d;
+              const double *wf = &O->reg[0][O->bsize * o[1 + cb]];
+              double sum = 0.0;
+              bool first = true;
+              for (int kk = 0; kk < (nd > 2 ? 2 : 1); ++kk)
+                for (int jj = 0; jj < (nd > 1 ? 2 : 1); ++jj)
+                  for (int ii = 0; ii < 2; ++ii) {
+                    const int fi = 2 + 2 * (F[0] & 7) + ii, fj = nd > 1 ? 2 + 2 * (F[1] & 7) + jj : 0,
+                              fk = nd > 2 ? 2 + 2 * (F[2] & 7) + kk : 0;
+                    const double x = wf[g.idx(fi, fj, fk) + g.cells * (size_t)iw];
+                    sum = first ? x : sum + x;
+                    first = false;
+                  }
+              val = sum * cofi;
+            }
+            wn[g.idx(2 + i, nd > 1 ? 2 + j : 0, nd > 2 ? 2 + k : 0) + g.cells * (size_t)iw] = val;
+          }
+  }
+  return res;
+}
+
 }  // extern "C"

@@ -193,6 +193,11 @@ int orc_amr_advect1(orc_amr *a, int reg_a, int reg_b, double qdt, double dtfacto
                     int nthreads);
 void orc_amr_combine_reg(orc_amr *a, int dst, double ca, int ra, double cb, int rb);
 int orc_amr_advance(orc_amr *a, double dt, double cmax_global, int nthreads);
+/* Regrid (amr_coarsen_refine): a new grid whose register 0 comes from the old
+ * grid's register 0 (after getbc) by op[9*b]: {0, old} copy, {1, old parent,
+ * child bits} prolong_2nd, {2, old children in child-bit order} coarsen_grid.
+ * The caller runs getbc on the new grid. */
+orc_amr *orc_amr_remap(const orc_amr *old, int nleaf, const int *leaf, const int *op);
 
 #ifdef __cplusplus
 }

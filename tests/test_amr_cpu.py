@@ -137,3 +137,47 @@ def test_refined_everywhere_is_the_uniform_grid(oracle_lib):
         u.advance(dt)
     for b in range(len(leaves)):
         assert np.array_equal(g.get_block(b), u.get_block(order[b]))
+
+
+def test_regrid_remap_is_exact_and_conservative(oracle_lib):
+    """prolong_2nd is exact for linear data, coarsen_grid conserves every
+    total, and refining then coarsening a block gives it back (to rounding)."""
+    from amrvac_b200.amr import Tree, ops
+    O = oracle_lib
+    nd, nb = 2, [4, 4]
+    c = _cfg(O, nd)
+    T = Tree(nd, nb, 3)
+    T, _ = T.regrid([t[1:3] in ((1, 1), (3, 3)) for t in T.leaves])
+    blocks = A.fill_blocks(T.leaves, nd, nb, _lin(nd), "hd", nd, 1.4, conserved=True)
+    g = O.AmrGrid(c, nb, [0.0] * nd, [1.0] * nd, T.leaves)
+    for b in range(len(T.leaves)):
+        g.set_block(b, blocks[b])
+    g.getbc()
+    sl = (slice(None), 0, slice(2, 18), slice(2, 18))
+
+    def totals(grid, tree):
+        return sum(grid.get_block(b)[sl].reshape(nd + 2, -1).sum(axis=1) * A.block_volume(l, nd, nb)
+                   for b, l in enumerate(tree.leaves))
+    t0 = totals(g, T)
+    # refine one level-2 block away from the wrap (proper nesting refines the
+    # level-1 leaves next to it as well), coarsen the children of root (3, 3)
+    ref = [t == (2, 3, 3, 0) for t in T.leaves]
+    coa = [t[0] == 2 and t[1] in (6, 7) and t[2] in (6, 7) for t in T.leaves]
+    T2, origin = T.regrid(ref, coa)
+    kinds = {o[0] for o in origin}
+    assert kinds == {"same", "child", "parent"}
+    g2 = g.remap(T2.leaves, ops(origin))
+    exact = A.fill_blocks(T2.leaves, nd, nb, _lin(nd), "hd", nd, 1.4, conserved=True)
+    for b, o in enumerate(origin):
+        if o[0] == "child":
+            got = g2.get_block(b)[sl]
+            assert np.allclose(got, exact[b][sl], rtol=0, atol=1e-14), np.abs(got - exact[b][sl]).max()
+    t1 = totals(g2, T2)
+    assert np.all(np.abs(t1 - t0) <= 1e-14 * np.abs(t0).max()), (t0, t1)
+    # refine then coarsen back: the parent's interior returns
+    assert (2, 3, 3, 0) not in T2.set and (1, 3, 3, 0) in T2.set
+    T3, o3 = T2.regrid([False] * len(T2.leaves), [t[0] == 3 for t in T2.leaves])
+    g3 = g2.remap(T3.leaves, ops(o3))
+    b3 = T3.leaves.index((2, 3, 3, 0))
+    b0 = T.leaves.index((2, 3, 3, 0))
+    assert np.allclose(g3.get_block(b3)[sl], g.get_block(b0)[sl], rtol=1e-15, atol=0)

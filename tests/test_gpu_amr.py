@@ -219,3 +219,92 @@ def test_settree_with_device_lohner_matches_oracle(oracle_lib):
     assert max(tg.level_of()) == levels and tg.balanced()
     assert np.array_equal(bg, bo)
     ctx.close()
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_regrid_every_step_matches_oracle(oracle_lib, nd):
+    """The reference's time loop with ditregrid = 1: advance, errest (Löhner),
+    amr_coarsen_refine (refined children by prolong_2nd, coarsened parents by
+    coarsen_grid), getbc.  Device (Löhner + remap kernels, tree decided on the
+    host) against the oracle (lohner_grid per block, orc_amr_remap): identical
+    flags and trees, states to 1e-12 after every step and regrid."""
+    _cuda()
+    O = oracle_lib
+    from amrvac_b200 import Context, make_cfg
+    from amrvac_b200.amr import Tree, ops, regrid
+    nb = [4] * nd if nd == 2 else [2] * nd
+    levels = 3
+    xmin, xmax = [-0.5] * nd, [0.5] * nd
+
+    def prim(X, Y, Z):
+        r = np.sqrt(X * X + Y * Y + (Z * Z if nd > 2 else 0))
+        out = np.zeros((nd + 2,) + X.shape)
+        out[0] = 1.0
+        out[1] = 0.3
+        out[nd + 1] = np.where(r < 0.1, 10.0, 0.1)
+        return out
+
+    def init(tree):
+        return A.fill_blocks(tree.leaves, nd, nb, prim, "hd", nd, 1.4, xmin, xmax)
+
+    # vanleer's regulariser is absolute, 2 max(ab, 0) / (a + b + 1e-12): where
+    # both differences are negative and near 1e-12 (the leading edge of the
+    # 3-D blast) it amplifies rounding differences ~1e5 times — the oracle
+    # against itself with 2e-16 input noise differs by 1.4e-11 after one step
+    # there, by 9e-16 with minmod — so the 3-D case uses minmod
+    kw = dict(physics="hd", ndim=nd, gamma=1.4, flux_scheme="hllc", limiter="vanleer" if nd == 2 else "minmod",
+              courantpar=0.6)
+    ctx = Context(make_cfg(typeboundary=["periodic"] * (2 * nd), **kw))
+    weight = np.zeros(nd + 2)
+    weight[0] = weight[nd + 1] = 0.5
+
+    # start from a tree the estimator disagrees with: a refined corner in the
+    # uniform region (it coarsens) and the blast on level 1 (it refines, one
+    # level per regrid)
+    tree = Tree(nd, nb, levels)
+    tree, _ = tree.regrid([all(i == 0 for i in t[1:1 + nd]) for t in tree.leaves])
+    blocks = init(tree)
+    ctx.set_amr_grid(tree.leaves, tree.nbase[:nd], xmin, xmax)
+    ctx.upload(blocks)
+    ocfg = O.make_cfg(**kw)
+    g = O.AmrGrid(ocfg, nb, xmin, xmax, tree.leaves)
+    for b in range(len(tree.leaves)):
+        g.set_block(b, blocks[b])
+    g.getbc()
+    sl = (slice(None),) + tuple(slice(2, 18) if d < nd else slice(None) for d in (2, 1, 0))
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    changes = 0
+    kinds = set()
+    for n in range(4 if nd == 2 else 3):
+        dt_o, cm_o = g.getdt()
+        ctx.step()
+        assert abs(ctx.get_time()[0] - dt_o) <= 1e-13 * dt_o
+        g.advance(dt_o, cm_o)
+        # the oracle's errest on its own state
+        oflags = [O.lohner_block(ocfg, g.get_block(b), weight, np.zeros(nd + 2, np.int32), 1e-2, 0.1, 0.125,
+                                 t[0], levels)[1:] for b, t in enumerate(tree.leaves)]
+        new = regrid(ctx, tree, weight)
+        to, origin = tree.regrid([bool(f[0]) for f in oflags], [bool(f[1]) for f in oflags])
+        assert new.leaves == to.leaves, n
+        if new is not tree:
+            changes += 1
+            kinds |= {o[0] for o in origin}
+            g = g.remap(to.leaves, ops(origin))
+        tree = new
+        got = ctx.download()
+        for b in range(len(tree.leaves)):
+            ref = g.get_block(b)
+            assert _maxrel(got[b][sl], ref[sl]) <= 1e-12, (n, tree.leaves[b], _maxrel(got[b][sl], ref[sl]))
+            assert _maxrel(got[b], ref) <= 1e-12, (n, "ghosts", tree.leaves[b])
+    assert changes >= 2 and max(tree.level_of()) == levels
+    assert "child" in kinds
+    if nd == 2:  # the refined corner was uniform: it coarsened
+        assert "parent" in kinds and (1, 0, 0, 0) in tree.set
+    assert ctx.status() == 0
+    # a wrong op table is refused and leaves the grid as it was
+    before = ctx.download()
+    bad = ops([("same", 0)] * len(tree.leaves))
+    with pytest.raises(RuntimeError):
+        ctx.amr_regrid(tree.leaves, bad)
+    assert np.array_equal(ctx.download(), before)
+    ctx.close()
