@@ -257,10 +257,21 @@ def ops(origin):
 
 
 def regrid(ctx, tree, weight, logflag=None, refine_threshold=0.1, derefine_ratio=0.125, amr_wavefilter=1.0e-2):
-    """resettree on the resident state: errest with the device Löhner
-    estimator (register ps, the current leaves), the tree decision on the
-    host (Tree.regrid), the state remap on the device.  Returns the new tree
-    (the same object if nothing changes)."""
+    """resettree on the resident state in one library call
+    (amrvac_gpu_amr_resettree: device Löhner on register ps, the C++ tree
+    decision, the device remap).  Returns the new Tree (the same object if
+    nothing changed)."""
+    changed = ctx.amr_resettree(weight, logflag, refine_max_level=tree.max_level, refine_threshold=refine_threshold,
+                                derefine_ratio=derefine_ratio, amr_wavefilter=amr_wavefilter)
+    if not changed:
+        return tree
+    return Tree(tree.nd, tree.nbase[:tree.nd], tree.max_level, ctx.amr_leaves())
+
+
+def regrid_python(ctx, tree, weight, logflag=None, refine_threshold=0.1, derefine_ratio=0.125,
+                  amr_wavefilter=1.0e-2):
+    """The same resettree with the tree decision made here (Tree.regrid) and
+    the remap through amrvac_gpu_amr_regrid."""
     L = tree.max_level
 
     def per_level(x):
@@ -274,3 +285,26 @@ def regrid(ctx, tree, weight, logflag=None, refine_threshold=0.1, derefine_ratio
         return tree
     ctx.amr_regrid(nt.leaves, ops(origin))
     return nt
+
+
+def plan_native(tree, refine, coarsen):
+    """Tree.regrid's decision computed by the library (amrvac_amr_plan, C++,
+    host only): (new leaves, op table)."""
+    import ctypes
+    from . import _lib
+    L = _lib.load()
+    nd = tree.nd
+    lv = np.ascontiguousarray(np.array(tree.leaves, np.int32).reshape(-1))
+    nb = np.ascontiguousarray(tree.nbase[:nd], np.int32)
+    r = np.ascontiguousarray(np.asarray(refine, np.uint8))
+    c = np.ascontiguousarray(np.asarray(coarsen, np.uint8))
+    cap = len(tree.leaves) << nd
+    out_l = np.zeros(4 * cap, np.int32)
+    out_o = np.zeros(9 * cap, np.int32)
+    n = ctypes.c_int(0)
+    ip, up = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_ubyte)
+    _lib.check(L.amrvac_amr_plan(nd, nb.ctypes.data_as(ip), tree.max_level, len(tree.leaves), lv.ctypes.data_as(ip),
+                                 r.ctypes.data_as(up), c.ctypes.data_as(up), cap, ctypes.byref(n),
+                                 out_l.ctypes.data_as(ip), out_o.ctypes.data_as(ip)), "amrvac_amr_plan")
+    k = n.value
+    return [tuple(int(x) for x in out_l[4 * b:4 * b + 4]) for b in range(k)], out_o[:9 * k].reshape(k, 9)

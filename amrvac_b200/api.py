@@ -97,6 +97,31 @@ class Context:
                    "amr_regrid")
         self.nblocks = self.L.amrvac_gpu_nblocks(self.h)
 
+    def amr_resettree(self, weight, logflag=None, refine_max_level=2, refine_threshold=0.1, derefine_ratio=0.125,
+                      amr_wavefilter=1e-2):
+        """resettree on the resident state (Löhner, tree decision, remap) in
+        one library call; returns True if the tree changed."""
+        nl = refine_max_level
+        per = lambda x: np.ascontiguousarray(np.broadcast_to(np.asarray(x, np.float64), (nl,)))  # noqa: E731
+        w = np.ascontiguousarray(weight, np.float64)
+        lf = None if logflag is None else np.ascontiguousarray(logflag, np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        ch = ctypes.c_int(0)
+        _lib.check(self.L.amrvac_gpu_amr_resettree(self.h, _dp(w), lf.ctypes.data_as(ip) if lf is not None else None,
+                                                   nl, _dp(per(refine_threshold)), _dp(per(derefine_ratio)),
+                                                   _dp(per(amr_wavefilter)), ctypes.byref(ch)), "amr_resettree")
+        self.nblocks = self.L.amrvac_gpu_nblocks(self.h)
+        return bool(ch.value)
+
+    def amr_leaves(self):
+        """The current leaves as (level, ig0, ig1, ig2) tuples in block order."""
+        n = self.L.amrvac_gpu_amr_leaves(self.h, None)
+        if n < 0:
+            raise RuntimeError("amr_leaves: no multi-level grid")
+        out = np.zeros((n, 4), np.int32)
+        self.L.amrvac_gpu_amr_leaves(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        return [tuple(int(x) for x in r) for r in out]
+
     @property
     def amr_slots(self):
         return self.L.amrvac_gpu_amr_slots(self.h)

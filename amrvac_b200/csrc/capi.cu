@@ -90,7 +90,27 @@ struct amrvac_ctx {
   double *d_amr_err = nullptr;         // [nblocks] largest error per block
   bool adj_prepared = false;
   struct AmrDev *amr = nullptr;        // multi-level grid (amrvac_gpu_set_amr_grid)
+  // Capacities (in blocks or elements) of the buffers that a new block set or
+  // a regrid reuses while they are large enough (grown by 25 % otherwise).
+  size_t pool_cap = 0, nbr_cap = 0, amr_int_cap = 0;
+  double *amr_gbuf = nullptr, *amr_pflux = nullptr, *amr_bxmin = nullptr;
+  int *amr_ints = nullptr;
+  size_t amr_gbuf_cap = 0, amr_pflux_cap = 0, amr_bxmin_cap = 0, amr_ints_cap = 0;
 };
+
+// Grow-only device buffer: reallocates (without keeping the contents) only
+// when need exceeds the capacity, then with 25 % headroom.
+template <class T>
+static cudaError_t ensure_capacity(T **p, size_t *cap, size_t need) {
+  if (*p && need <= *cap) return cudaSuccess;
+  cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  const size_t n = need + need / 4 + 1;
+  const cudaError_t e = cudaMalloc(p, sizeof(T) * n);
+  if (e == cudaSuccess) *cap = n;
+  return e;
+}
 
 // Device copy of a static multi-level grid: neighbour kinds, per-level owner
 // maps, ghost buffers of the blocks next to a level jump and their boundary
@@ -107,12 +127,7 @@ struct AmrDev {
   std::vector<int> h_leaf;    // [nblocks][4] level, ig0, ig1, ig2 (regrid checks)
   int nbase[3] = {1, 1, 1};
   double xmin[3] = {0, 0, 0}, xmax[3] = {1, 1, 1};
-  ~AmrDev() {
-    cudaFree(d_int);
-    cudaFree(d_bxmin);
-    cudaFree(gbuf);
-    cudaFree(pflux);
-  }
+  // the device buffers belong to the context (amr_* fields), reused across regrids
 };
 
 namespace {
@@ -427,6 +442,10 @@ int amrvac_gpu_destroy(amrvac_ctx *c) {
   cudaFree(c->d_amr_err);
   cudaFree(c->d_stage);
   delete c->amr;
+  cudaFree(c->amr_gbuf);
+  cudaFree(c->amr_pflux);
+  cudaFree(c->amr_bxmin);
+  cudaFree(c->amr_ints);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -494,31 +513,47 @@ static int set_blocks_impl(amrvac_ctx *c, int nblocks, const double *dx, const i
         return fail(AMRVAC_E_ARG, "missing edge/corner neighbour between two sibling faces");
     }
   cudaStreamSynchronize(c->stream);
-  for (int r = 0; r < 3; ++r) { cudaFree(c->pool[r]); c->pool[r] = nullptr; }
-  cudaFree(c->d_nbr); cudaFree(c->d_dx); cudaFree(c->d_block_status);
-  c->d_nbr = nullptr; c->d_dx = nullptr; c->d_block_status = nullptr;
   if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
-  c->nblocks = nblocks;
   const size_t bytes = sizeof(double) * c->per_block * c->nw * nblocks;
-  for (int r = 0; r < 3; ++r) {
-    if (r == 0 && adopt_reg0) {
-      c->pool[0] = adopt_reg0;
-      continue;
+  if (adopt_reg0 && adopt_reg0 == c->pool[1]) {
+    // regrid into the scratch register: swap it in, nothing is allocated
+    std::swap(c->pool[0], c->pool[1]);
+  } else if (adopt_reg0) {
+    // regrid into a new, larger buffer: the other registers follow its size
+    const size_t cap = (size_t)nblocks + nblocks / 4 + 1;
+    for (int r = 0; r < 3; ++r) { cudaFree(c->pool[r]); c->pool[r] = nullptr; }
+    c->pool_cap = 0;
+    c->pool[0] = adopt_reg0;
+    for (int r = 1; r < 3; ++r) CK(cudaMalloc(&c->pool[r], sizeof(double) * c->per_block * c->nw * cap));
+    c->pool_cap = cap;
+  } else {
+    if ((size_t)nblocks > c->pool_cap || !c->pool[0]) {
+      for (int r = 0; r < 3; ++r) { cudaFree(c->pool[r]); c->pool[r] = nullptr; }
+      c->pool_cap = 0;
+      const size_t cap = (size_t)nblocks + nblocks / 4 + 1;
+      for (int r = 0; r < 3; ++r) CK(cudaMalloc(&c->pool[r], sizeof(double) * c->per_block * c->nw * cap));
+      c->pool_cap = cap;
     }
-    CK(cudaMalloc(&c->pool[r], bytes));
-    CK(cudaMemsetAsync(c->pool[r], 0, bytes, c->stream));
+    for (int r = 0; r < 3; ++r) CK(cudaMemsetAsync(c->pool[r], 0, bytes, c->stream));
   }
-  CK(cudaMalloc(&c->d_nbr, sizeof(int) * nbr.size()));
-  CK(cudaMalloc(&c->d_dx, sizeof(double) * dxb.size()));
-  CK(cudaMalloc(&c->d_block_status, sizeof(uint32_t) * nblocks));
+  c->nblocks = nblocks;
+  if ((size_t)nblocks > c->nbr_cap || !c->d_nbr) {
+    cudaFree(c->d_nbr); cudaFree(c->d_dx); cudaFree(c->d_block_status);
+    c->d_nbr = nullptr; c->d_dx = nullptr; c->d_block_status = nullptr;
+    c->nbr_cap = 0;
+    const size_t cap = (size_t)nblocks + nblocks / 4 + 1;
+    CK(cudaMalloc(&c->d_nbr, sizeof(int) * 27 * cap));
+    CK(cudaMalloc(&c->d_dx, sizeof(double) * 3 * cap));
+    CK(cudaMalloc(&c->d_block_status, sizeof(uint32_t) * cap));
+    c->nbr_cap = cap;
+  }
   CK(cudaMemcpyAsync(c->d_nbr, nbr.data(), sizeof(int) * nbr.size(), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_dx, dxb.data(), sizeof(double) * dxb.size(), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * nblocks, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->h_dx = dxb;
   for (int r = 0; r < 3; ++r) { cudaFree(c->d_adj[r]); c->d_adj[r] = nullptr; }
-  cudaFree(c->d_amr_int); c->d_amr_int = nullptr;
-  cudaFree(c->d_amr_err); c->d_amr_err = nullptr;
+  c->adj_prepared = false;
   delete c->amr; c->amr = nullptr;
   return 0;
 }
@@ -792,7 +827,9 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
     }
     if (int r = launch_amr_ghost_pass(c, 0)) return r;  // the old tree's level-jump ghosts
     int *d_op = nullptr;
-    cudaError_t e = cudaMalloc(&newreg, sizeof(double) * c->per_block * c->nw * nb);
+    cudaError_t e = cudaSuccess;
+    if ((size_t)nb <= c->pool_cap) newreg = c->pool[1];  // scratch register: swapped in afterwards
+    else e = cudaMalloc(&newreg, sizeof(double) * c->per_block * c->nw * ((size_t)nb + nb / 4 + 1));
     if (e == cudaSuccess) e = cudaMalloc(&d_op, sizeof(int) * 9 * (size_t)nb);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(d_op, ops, sizeof(int) * 9 * (size_t)nb, cudaMemcpyHostToDevice, c->stream);
@@ -809,12 +846,12 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFree(d_op);
     if (e != cudaSuccess) {
-      cudaFree(newreg);
+      if (newreg != c->pool[1]) cudaFree(newreg);
       return cuda_fail(e, "amr_regrid");
     }
   }
   if (int r = set_blocks_impl(c, nb, dx.data(), nbr.data(), true, newreg)) {
-    if (newreg && c->pool[0] != newreg) cudaFree(newreg);
+    if (newreg && c->pool[0] != newreg && c->pool[1] != newreg) cudaFree(newreg);
     return r;
   }
   // device copies
@@ -840,16 +877,20 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
   };
   const size_t o_ib = put(iblocks), o_gs = put(gslot), o_fc = put(face), o_nt = put(ntype), o_lv = put(lev),
                o_ig = put(ig), o_ch = put(child), o_ow = put(owner);
-  CK(cudaMalloc(&A->d_int, sizeof(int) * ints.size()));
+  CK(ensure_capacity(&c->amr_ints, &c->amr_ints_cap, ints.size()));
+  A->d_int = c->amr_ints;
   CK(cudaMemcpyAsync(A->d_int, ints.data(), sizeof(int) * ints.size(), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMalloc(&A->d_bxmin, sizeof(double) * bxmin.size()));
+  CK(ensure_capacity(&c->amr_bxmin, &c->amr_bxmin_cap, bxmin.size()));
+  A->d_bxmin = c->amr_bxmin;
   CK(cudaMemcpyAsync(A->d_bxmin, bxmin.data(), sizeof(double) * bxmin.size(), cudaMemcpyHostToDevice, c->stream));
   size_t gcells = 1;
   for (int d = 0; d < nd; ++d) gcells *= 20;
-  CK(cudaMalloc(&A->gbuf, sizeof(double) * ns * c->nw * gcells));
-  CK(cudaMemsetAsync(A->gbuf, 0, sizeof(double) * ns * c->nw * gcells, c->stream));
-  CK(cudaMalloc(&A->pflux, sizeof(double) * ns * 2 * nd * c->nw * 256));
-  CK(cudaMemsetAsync(A->pflux, 0, sizeof(double) * ns * 2 * nd * c->nw * 256, c->stream));
+  // every ghost cell a kernel reads is written by the ghost pass first, and
+  // every face flux the fix reads by the stage before it: no clearing needed
+  CK(ensure_capacity(&c->amr_gbuf, &c->amr_gbuf_cap, ns * c->nw * gcells));
+  A->gbuf = c->amr_gbuf;
+  CK(ensure_capacity(&c->amr_pflux, &c->amr_pflux_cap, ns * 2 * nd * c->nw * 256));
+  A->pflux = c->amr_pflux;
   A->d_gslot = A->d_int + o_gs;
   A->d_face = A->d_int + o_fc;
   G.u = nullptr;
@@ -877,6 +918,45 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
 }
 
 int amrvac_gpu_amr_slots(const amrvac_ctx *c) { return c && c->amr ? c->amr->nslots : 0; }
+
+int amrvac_gpu_amr_leaves(const amrvac_ctx *c, int *leaf) {
+  if (!c || !c->amr) return AMRVAC_E_STATE;
+  if (leaf) std::memcpy(leaf, c->amr->h_leaf.data(), sizeof(int) * c->amr->h_leaf.size());
+  return (int)(c->amr->h_leaf.size() / 4);
+}
+
+// resettree (src/amr/mod_amr_grid.t:45-73): errest with the Löhner estimator
+// on register 0, the tree decision of amr_coarsen_refine (amrvac_amr_plan, on
+// the host), and the device remap; *changed = 0 when the tree stays.
+int amrvac_gpu_amr_resettree(amrvac_ctx *c, const double *weight, const int *logflag, int refine_max_level,
+                             const double *refine_threshold, const double *derefine_ratio,
+                             const double *amr_wavefilter, int *changed) {
+  if (int r = check_ctx(c, true)) return r;
+  if (!c->amr) return fail(AMRVAC_E_STATE, "amr_resettree: no multi-level grid (amrvac_gpu_set_amr_grid)");
+  const int nb = c->nblocks, nd = c->cfg.ndim;
+  std::vector<int> lev(nb), flags(nb);
+  for (int b = 0; b < nb; ++b) lev[b] = c->amr->h_leaf[4 * b];
+  if (int r = amrvac_gpu_lohner(c, 0, weight, logflag, refine_max_level, refine_threshold, derefine_ratio,
+                                amr_wavefilter, lev.data(), flags.data(), nullptr))
+    return r;
+  std::vector<unsigned char> ref(nb), coa(nb);
+  for (int b = 0; b < nb; ++b) {
+    ref[b] = (flags[b] & 1) != 0;
+    coa[b] = (flags[b] & 2) != 0;
+  }
+  const std::vector<int> old_leaf = c->amr->h_leaf;
+  const int cap = nb * (1 << nd);
+  std::vector<int> leaf_new(4 * (size_t)cap), op(9 * (size_t)cap);
+  int nnew = 0;
+  if (int r = amrvac_amr_plan(nd, c->amr->nbase, refine_max_level, nb, old_leaf.data(), ref.data(), coa.data(), cap,
+                              &nnew, leaf_new.data(), op.data()))
+    return fail(r, "amr_resettree: tree decision failed");
+  leaf_new.resize(4 * (size_t)nnew);
+  const bool same = nnew == nb && leaf_new == old_leaf;
+  if (changed) *changed = same ? 0 : 1;
+  if (same) return 0;
+  return amrvac_gpu_amr_regrid(c, nnew, leaf_new.data(), op.data());
+}
 
 // Average device time of the level-jump ghost pass (on register 0) and of the
 // flux fix (on register 2, whose contents it changes) over reps launches.
@@ -1411,8 +1491,17 @@ int amrvac_gpu_lohner(amrvac_ctx *c, int reg, const double *weight, const int *l
       if (block_level[b] < 1 || block_level[b] > refine_max_level) return fail(AMRVAC_E_ARG, "lohner: bad level");
       lev[b] = block_level[b];
     }
-  if (!c->d_amr_int) CK(cudaMalloc(&c->d_amr_int, sizeof(int) * 2 * c->nblocks));
-  if (!c->d_amr_err) CK(cudaMalloc(&c->d_amr_err, sizeof(double) * c->nblocks));
+  if ((size_t)c->nblocks > c->amr_int_cap || !c->d_amr_int) {
+    cudaFree(c->d_amr_int);
+    cudaFree(c->d_amr_err);
+    c->d_amr_int = nullptr;
+    c->d_amr_err = nullptr;
+    c->amr_int_cap = 0;
+    const size_t cap = (size_t)c->nblocks + c->nblocks / 4 + 1;
+    CK(cudaMalloc(&c->d_amr_int, sizeof(int) * 2 * cap));
+    CK(cudaMalloc(&c->d_amr_err, sizeof(double) * cap));
+    c->amr_int_cap = cap;
+  }
   CK(cudaMemcpyAsync(c->d_amr_int, lev.data(), sizeof(int) * c->nblocks, cudaMemcpyHostToDevice, c->stream));
   A.level = c->d_amr_int;
   A.flags = c->d_amr_int + c->nblocks;

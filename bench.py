@@ -789,6 +789,39 @@ def run_amr(args, ws, rank, local):
                        "download with ghost cells (level-jump ghosts included); transfers amortised over K"}
     except Exception as ex:
         e2e = {"value": None, "unit": UNIT, "error": str(ex)}
+    # the reference's time loop with ditregrid = 1: advance, then resettree
+    # (device Löhner, C++ tree decision, device remap) after every step
+    regrid_run = None
+    try:
+        ctx.set_amr_grid(tree.leaves, tree.nbase, *AMR_X)
+        ctx.upload(blocks)
+        ctx.set_time(0.0, 1.0e99, 0.0)
+        rkw = dict(refine_max_level=w["amr"]["levels"], refine_threshold=0.1, derefine_ratio=0.125,
+                   amr_wavefilter=1.0e-2)
+        for _ in range(2):
+            ctx.step()
+            ctx.amr_resettree(AMR_WEIGHT, **rkw)
+        s = torch.cuda.ExternalStream(ctx.stream_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        cells_done, changes, nmin, nmax = 0, 0, ctx.nblocks, ctx.nblocks
+        e0.record(s)
+        for _ in range(args.steps):
+            cells_done += ctx.nblocks * 16 ** 3
+            ctx.step()
+            changes += ctx.amr_resettree(AMR_WEIGHT, **rkw)
+            nmin, nmax = min(nmin, ctx.nblocks), max(nmax, ctx.nblocks)
+        e1.record(s)
+        e1.synchronize()
+        rg_ms = _allmax(e0.elapsed_time(e1), ws)
+        regrid_run = {"value": ws * cells_done / (rg_ms * 1e-3), "unit": UNIT, "ms_per_step": rg_ms / args.steps,
+                      "static_ms_per_step": tmax / args.steps, "regrids_that_changed_the_tree": changes,
+                      "blocks_min_max": [nmin, nmax], "status": ctx.status(),
+                      "what": "K steps each followed by amrvac_gpu_amr_resettree (Löhner on the device, tree "
+                              "decision in C++ on the host, remap kernel); CUDA events on the library stream, "
+                              "host work included"}
+    except Exception as ex:
+        regrid_run = {"error": str(ex)}
     mixed = None
     try:
         cm = Context(make_cfg(precision="mixed", typeboundary=["periodic"] * 6, **_amr_cfg_kwargs()))
@@ -827,6 +860,7 @@ def run_amr(args, ws, rank, local):
                        "l2": "no flush: working set %.0f MB (3 registers) > 126 MB L2" % (3 * cells * nw * 8 / 1e6),
                        "stage_weighted_cell_updates_per_s": 3 * value},
             "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "mixed": mixed,
+            "regrid_every_step": regrid_run,
             "gpu_launches": launches, "clocks": clk.summary(), "status": st,
             "kernel_ms": {"stage_total_incl_amr": stage_ms, "getdt_total": getdt_ms, "step_total": total_ms},
         }

@@ -160,6 +160,25 @@ int amrvac_gpu_set_amr_grid(amrvac_ctx *ctx, int nleaf, const int *leaf, const i
  * Ops that do not match the old and new trees are refused.  Register 0
  * carries the state over; registers 1 and 2 are scratch afterwards. */
 int amrvac_gpu_amr_regrid(amrvac_ctx *ctx, int nleaf, const int *leaf, const int *op);
+/* resettree (src/amr/mod_amr_grid.t:45-73): errest with the Löhner
+ * estimator on register 0 (arguments as for amrvac_gpu_lohner, levels taken
+ * from the current tree), the tree decision below, and amrvac_gpu_amr_regrid.
+ * *changed (may be NULL) = 1 when the tree changed. */
+int amrvac_gpu_amr_resettree(amrvac_ctx *ctx, const double *weight, const int *logflag, int refine_max_level,
+                             const double *refine_threshold, const double *derefine_ratio,
+                             const double *amr_wavefilter, int *changed);
+/* The current leaves, 4 ints each (level, ig0, ig1, ig2) in block order, if
+ * leaf is not NULL; returns their number (AMRVAC_E_STATE without a grid). */
+int amrvac_gpu_amr_leaves(const amrvac_ctx *ctx, int *leaf);
+/* The tree decision of amr_coarsen_refine with proper_nesting
+ * (src/amr/mod_coarsen_refine.t:20-319), host only: from the leaves and the
+ * per-leaf refine / coarsen flags, the new leaves (sorted by level, ig0, ig1,
+ * ig2) and their ops for amrvac_gpu_amr_regrid.  cap = capacity of leaf_new
+ * (4 ints per leaf) and op (9 ints per leaf) in leaves; *nnew is set even
+ * when it exceeds cap (then AMRVAC_E_ARG). */
+int amrvac_amr_plan(int ndim, const int *nbase, int max_level, int nleaf, const int *leaf,
+                    const unsigned char *refine, const unsigned char *coarsen, int cap, int *nnew, int *leaf_new,
+                    int *op);
 /* Blocks next to a level jump (0 on a single-level grid). */
 int amrvac_gpu_amr_slots(const amrvac_ctx *ctx);
 /* Average device time of the level-jump ghost pass (register 0) and of the

@@ -103,3 +103,21 @@ def test_initial_hierarchy_reaches_the_finest_level():
     T, blocks = initial_hierarchy(Tree(2, [4, 4], 4), init, err)
     assert max(T.level_of()) == 4 and T.balanced()
     assert blocks.shape[0] == len(T.leaves)
+
+
+@pytest.mark.parametrize("nd,nbase", [(2, [4, 4]), (3, [2, 2, 2]), (2, [3, 2])])
+def test_native_plan_matches_python(nd, nbase):
+    """The library's C++ tree decision (amrvac_amr_plan) equals Tree.regrid:
+    same leaves in the same order, same ops, over random regrid sequences."""
+    from amrvac_b200.amr import ops, plan_native
+    rng = np.random.default_rng(7 + nd)
+    T = Tree(nd, nbase, 4)
+    for it in range(10):
+        ref = rng.random(len(T.leaves)) < 0.2
+        coa = rng.random(len(T.leaves)) < 0.5
+        nt, origin = T.regrid(ref, coa)
+        leaves, op = plan_native(T, ref, coa)
+        assert leaves == nt.leaves, it
+        assert np.array_equal(op, ops(origin)), it
+        T = nt
+    assert max(T.level_of()) >= 3

@@ -20,7 +20,7 @@ def test_library_exports_every_declared_symbol(lib):
     """Every function declared in include/amrvac_gpu.h is exported by the .so."""
     with open(os.path.join(ROOT, "include", "amrvac_gpu.h")) as f:
         text = f.read()
-    names = set(re.findall(r"\b(amrvac_(?:gpu|ens)_\w+)\s*\(", text))
+    names = set(re.findall(r"\b(amrvac_(?:gpu|ens|amr)_\w+)\s*\(", text))
     assert len(names) >= 40
     for n in sorted(names):
         assert hasattr(lib, n), n
