@@ -608,8 +608,12 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
                 acc[V::M0 + c] = acc[V::M0 + c] - qsrc * double(tv.at(slot, V::B0 + c, ci, cj)) * divb;
             }
           } else if (P.divb == DIVB_LINDE) {
-            if constexpr (NDIM == 2) {
-              // add_source_linde (src/mhd/mod_mhd_phys.t:5599-5665), uniform grid
+            // the reference leaves out the cell layer next to a level-jump
+            // face "for AMR stability" (src/mhd/mod_mhd_phys.t:5616-5642)
+            const bool jump_layer = amr_mask && (((amr_mask & 1) && ci == 0) || ((amr_mask & 2) && ci == BN - 1) ||
+                                                 ((amr_mask & 4) && cj == 0) || ((amr_mask & 8) && cj == BN - 1));
+            if constexpr (NDIM == 2) if (!jump_layer) {
+              // add_source_linde (src/mhd/mod_mhd_phys.t:5599-5665)
               auto divb_at = [&](int i, int j) -> double {
                 double d = 0.5 * (double(tv.at(slot, V::B0, i + 1, j)) - double(tv.at(slot, V::B0, i - 1, j))) * (1.0 / dx[0]);
                 d = d + 0.5 * (double(tv.at(slot, V::B0 + 1, i, j + 1)) - double(tv.at(slot, V::B0 + 1, i, j - 1))) * (1.0 / dx[1]);

@@ -932,10 +932,12 @@ void add_source_glm(const State &s, double qdt, const Box &ixI, const Box &ixO, 
   (void)ixI;
 }
 
-// add_source_linde (src/mhd/mod_mhd_phys.t:5599-5665), uniform grid (no level jumps).
+// add_source_linde (src/mhd/mod_mhd_phys.t:5599-5665).  jump_faces bit
+// 2d+side marks a face with a coarser or finer neighbour: the source skips the
+// cell layer next to it ("for AMR stability", 5616-5642).
 template <class R>
 void add_source_linde(const State &s, double qdt, const Box &ixO, const Arr<R> &wCT, Arr<R> &w,
-                      const double *dxlevel) {
+                      const double *dxlevel, int jump_faces = 0) {
   const Ix &x = s.x;
   const orc_cfg &c = s.c;
   Box ixp = ixO;
@@ -948,9 +950,14 @@ void add_source_linde(const State &s, double qdt, const Box &ixO, const Arr<R> &
     for (int d = 1; d < c.ndim; ++d) acc = acc + R(1.0) / (R(dxlevel[d]) * R(dxlevel[d]));
     inv2 = acc;
   }
+  Box ixq = ixO;
+  for (int d = 0; d < c.ndim; ++d) {
+    if ((jump_faces >> (2 * d)) & 1) ixq.lo[d] += 1;
+    if ((jump_faces >> (2 * d + 1)) & 1) ixq.hi[d] -= 1;
+  }
   for (int d = 0; d < c.ndim; ++d) {
     const int o = s.g.off(d);
-    forbox(ixO, [&](int i, int j, int k) {
+    forbox(ixq, [&](int i, int j, int k) {
       const int p = s.g.idx(i, j, k);
       R gq = (divb[p + o] - divb[p - o]) * R(half);
       gq = gq / R(dxlevel[d]);
@@ -965,7 +972,8 @@ void add_source_linde(const State &s, double qdt, const Box &ixO, const Arr<R> &
 // finite_volume (src/mod_finite_volume.t:116-339), slab_uniform, no local dt.
 template <class R>
 int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, double dtfactor,
-                  const double *dxs, double cmax_global, std::vector<Arr<R>> *keep_fc = nullptr) {
+                  const double *dxs, double cmax_global, std::vector<Arr<R>> *keep_fc = nullptr,
+                  int jump_faces = 0) {
   const Ix &x = s.x;
   const orc_cfg &c = s.c;
   const Geo &g = s.g;
@@ -1031,7 +1039,7 @@ int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, d
   if (x.mhd && ndim > 1) {
     double qsrc = qdt * double(ndim) / double(ndim);
     if (c.divb == ORC_DIVB_GLM) add_source_glm(s, qsrc, ixI, ixO, wCT, wnew, dxs, cmax_global);
-    else if (c.divb == ORC_DIVB_LINDE) add_source_linde(s, qsrc, ixO, wCT, wnew, dxs);
+    else if (c.divb == ORC_DIVB_LINDE) add_source_linde(s, qsrc, ixO, wCT, wnew, dxs, jump_faces);
   }
   (void)dtfactor;
   if (keep_fc) *keep_fc = std::move(fC);  // scaled face fluxes -qdt/dx F, for store_flux
@@ -2197,7 +2205,15 @@ int amr_advect1(AmrGrid &G, int ra, int rb, double qdt, double dtfactor, double 
     double dxb[3];
     for (int d = 0; d < 3; ++d) dxb[d] = d < G.ndim ? G.dx(b, d) : 1.0;
     std::vector<Arr<double>> fc;
-    st |= finite_volume(G.s, a, w, qdt, dtfactor, dxb, cmax_global, &fc);
+    int jumps = 0;  // faces with a coarser or finer neighbour
+    for (int d = 0; d < G.ndim; ++d)
+      for (int side = 0; side < 2; ++side) {
+        int dd[3] = {0, 0, 0};
+        dd[d] = side ? 1 : -1;
+        const int t = G.ntype[b * 27 + q27(dd)];
+        if (t == NT_COARSE || t == NT_FINE) jumps |= 1 << (2 * d + side);
+      }
+    st |= finite_volume(G.s, a, w, qdt, dtfactor, dxb, cmax_global, &fc, jumps);
     std::memcpy(&G.reg[rb][bs * b], w.d.data(), sizeof(double) * bs);
     amr_store_flux(G, b, fc);
   }

@@ -50,3 +50,89 @@ def test_field_loop_golden_log_gpu(oracle_lib, name, kw, nw):
     ib = 1 + nw + 2
     rel = np.abs(rows[:, ib] - gold[:, ib]) / np.abs(gold[:, ib])
     assert rel.max() < 1e-5
+
+
+# ---------------------------------------------------------------- multi-level
+# Orszag-Tang 2-D (tests/mhd/Orszag_Tang_2D, reference): 64^2 level-1 cells in
+# 16^2 blocks on [0,1]^2, periodic, refine_max_level 3, Löhner on rho and e
+# (w_refine_weight 0.5 each, refine_threshold 0.4), the initial tree by
+# settree on the initial condition and a resettree after every step
+# (ditregrid = 1), log every 1e-3 to t = 0.1.
+
+
+def _ot2d_prim(nw):
+    rho0, p0, b0 = 25.0 / 36.0 / np.pi, 5.0 / 12.0 / np.pi, 1.0 / np.sqrt(4.0 * np.pi)
+
+    def f(X, Y, Z):
+        out = np.zeros((nw,) + X.shape)
+        out[0] = rho0
+        out[1] = -np.sin(2.0 * np.pi * Y)
+        out[2] = np.sin(2.0 * np.pi * X)
+        out[3] = p0
+        out[4] = -b0 * np.sin(2.0 * np.pi * Y)
+        out[5] = b0 * np.sin(4.0 * np.pi * X)
+        return out
+    return f
+
+
+def _amr_log_row(blocks, leaves, nbase, t, nw):
+    """printlog_regression_test: volume averages of w and w**2 over the leaves."""
+    s1, s2, vol = np.zeros(nw), np.zeros(nw), 0.0
+    for b, lf in enumerate(leaves):
+        dv = (1.0 / (nbase[0] * 16 * (1 << (lf[0] - 1)))) * (1.0 / (nbase[1] * 16 * (1 << (lf[0] - 1))))
+        w = blocks[b][:nw, 0, 2:18, 2:18].reshape(nw, -1)
+        s1 += w.sum(axis=1) * dv
+        s2 += (w * w).sum(axis=1) * dv
+        vol += 256 * dv
+    return np.concatenate([[t], s1 / vol, s2 / vol])
+
+
+def _run_ot2d_amr(kw, nw, time_max=0.1, dtsave=1.0e-3):
+    from tests import _amr as A
+    from amrvac_b200 import Context, make_cfg
+    from amrvac_b200.amr import Tree, initial_hierarchy, lohner_flags
+    nb, xmin, xmax = [4, 4], [0.0, 0.0], [1.0, 1.0]
+    cfg = make_cfg(physics="mhd", ndim=2, ndir=2, typeboundary=["periodic"] * 4, **kw)
+    ctx = Context(cfg)
+    weight = np.zeros(nw)
+    weight[0] = weight[3] = 0.5
+    lkw = dict(refine_threshold=0.4, derefine_ratio=0.125, amr_wavefilter=1.0e-2)
+
+    def init(tree):
+        return A.fill_blocks(tree.leaves, 2, nb, _ot2d_prim(nw), "mhd", 2, 5.0 / 3.0, xmin, xmax)
+
+    def err(tree, blocks):
+        r, c, _ = lohner_flags(ctx, tree, blocks, xmin, xmax, weight, **lkw)
+        return r, c
+    tree, blocks = initial_hierarchy(Tree(2, nb, 3), init, err)
+    ctx.set_amr_grid(tree.leaves, nb, xmin, xmax)
+    ctx.upload(blocks)
+    ctx.set_time(0.0, time_max, dtsave)
+    rows = []
+    tsavelast = 0.0
+    for _ in range(100000):
+        ctx.step()
+        ctx.amr_resettree(weight, refine_max_level=3, **lkw)
+        dt, cg, t = ctx.get_time()
+        if t >= tsavelast + dtsave - 1e-12:
+            tsavelast = t
+            rows.append(_amr_log_row(ctx.download(), ctx.amr_leaves(), nb, t, nw))
+        if t >= time_max - 1e-10:
+            break
+    assert ctx.status() == 0
+    ctx.close()
+    return np.array(rows)
+
+
+@pytest.mark.parametrize("name,kw,nw", [
+    ("hlld", dict(flux_scheme="hlld", limiter="cada3", typedivbfix="glm", courantpar=0.9), 7),
+    ("hll", dict(flux_scheme="hll", limiter="cada3", typedivbfix="linde", typeboundspeed="cmaxmean",
+                 courantpar=0.9), 6),
+])
+def test_orszag_tang_2d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
+    rows = _run_ot2d_amr(kw, nw)
+    gold = oracle_lib.read_log(os.path.join(GOLD, f"ot_2d_3step_{name}_cada.log"))
+    assert rows.shape == gold.shape, (rows.shape, gold.shape)
+    bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
+    assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
+        np.argwhere(bad)[:10].tolist(), rows[bad][:10].tolist(), gold[bad][:10].tolist())
