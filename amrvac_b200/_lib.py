@@ -50,6 +50,7 @@ class AmrvacCfg(ctypes.Structure):
         ("typeboundary", (ctypes.c_int * MAX_NW) * 6),
         ("zchunk", ctypes.c_int),
         ("precision", ctypes.c_int),
+        ("slowsteps", ctypes.c_int),
     ]
 
 

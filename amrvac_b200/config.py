@@ -106,7 +106,7 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
              typecourant="maxsum", cada3_radius=0.1, tvdlfeps=1.0, fix_small_values=False,
              check_small_values=True, small_values_method="error", small_density=0.0,
              small_pressure=0.0, time_stepper="threestep", ssprk_order=3, dtmin=1.0e-10,
-             typeboundary=None, zchunk=0, precision="fp64") -> _lib.AmrvacCfg:
+             typeboundary=None, zchunk=0, precision="fp64", slowsteps=-1) -> _lib.AmrvacCfg:
     """Build an ``amrvac_cfg`` from reference-style parameter names.
 
     typeboundary: list of 2*ndim entries (min1, max1, min2, ...), each a name
@@ -144,6 +144,7 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
     c.dtmin = dtmin
     c.zchunk = zchunk
     c.precision = _lib.PRECISION[precision]
+    c.slowsteps = int(slowsteps)
     nw = L.amrvac_gpu_nw(c)
     tb = typeboundary or ["periodic"] * (2 * ndim)
     for s in range(6):
@@ -193,6 +194,7 @@ def config_from_par(paths) -> RunConfig:
         typeboundspeed=meth.get("typeboundspeed", "Einfeldt"),
         courantpar=float(param.get("courantpar", 0.8)),
         typecourant=param.get("typecourant", "maxsum"),
+        slowsteps=int(param.get("slowsteps", -1)),
         cada3_radius=float(meth.get("cada3_radius", 0.1)),
         tvdlfeps=float(meth.get("tvdlfeps", 1.0)),
         fix_small_values=bool(meth.get("fix_small_values", False)),

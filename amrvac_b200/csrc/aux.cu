@@ -107,9 +107,10 @@ __global__ void pack_kernel(const double *__restrict__ pool, double *__restrict_
 
 // ---------------------------------------------------------------- setdt tail
 // After getdt_kernel: dt = courantpar / max (src/mod_dt.t:233-235), the
-// dtmin check (55-60), final_dt_reduction (69-79) and the output-interval cap
-// (88-99).  scal: [0]=dt [1]=cmax_global [2]=global_time [3]=time_max
-// [4]=dtsave [5]=dtmin [6]=courantpar [7]=final_exit flag.
+// dtmin check (55-60), the slowsteps ramp (64-67), final_dt_reduction (69-79)
+// and the output-interval cap (88-99).  scal: [0]=dt [1]=cmax_global
+// [2]=global_time [3]=time_max [4]=dtsave [5]=dtmin [6]=courantpar
+// [7]=final_exit flag [8]=slowsteps [9]=steps since set_time (it - it_init).
 __global__ void setdt_finalize_kernel(unsigned long long *red, double *scal, uint32_t *status) {
   const double smalldouble = 1.0e-12, bigdouble = 1.0e99;
   const double x = __longlong_as_double((long long)red[0]);
@@ -119,6 +120,10 @@ __global__ void setdt_finalize_kernel(unsigned long long *red, double *scal, uin
   double dt = bigdouble;
   if (x > smalldouble) dt = fmin(dt, scal[6] / x);
   if (dt < scal[5]) atomicOr(status, ST_DT_TOO_SMALL);
+  if (scal[8] > scal[9] + 1.0) {
+    const double q = 1.0 - (scal[9] + 1.0) / scal[8];
+    dt = dt * (1.0 - q * q);
+  }
   const double t = scal[2], tmax = scal[3], dtsave = scal[4];
   if (tmax - t <= scal[5]) scal[7] = 1.0;
   dt = fmin(dt, tmax - t);
@@ -133,7 +138,10 @@ __global__ void setdt_finalize_kernel(unsigned long long *red, double *scal, uin
   scal[1] = cm;
 }
 
-__global__ void advance_time_kernel(double *scal) { scal[2] = scal[2] + scal[0]; }
+__global__ void advance_time_kernel(double *scal) {
+  scal[2] = scal[2] + scal[0];
+  scal[9] = scal[9] + 1.0;
+}
 
 __global__ void restore_blocks_kernel(const double *__restrict__ wct, double *__restrict__ wnew,
                                       const uint32_t *__restrict__ block_status, size_t per_block) {

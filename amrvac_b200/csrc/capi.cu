@@ -291,6 +291,7 @@ void amrvac_gpu_default_cfg(amrvac_cfg *c) {
   c->dtmin = 1.0e-10;
   c->zchunk = 0;
   c->precision = 0;
+  c->slowsteps = -1;
 }
 
 int amrvac_gpu_nw(const amrvac_cfg *cfg) { return cfg ? nw_of(cfg) : AMRVAC_E_ARG; }
@@ -411,8 +412,9 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
     delete c;
     return cuda_fail(e, "cudaStreamCreate");
   }
-  // scalars: dt, cmax_global, time, time_max, dtsave, dtmin, courantpar, final flag
-  const double sc[8] = {0.0, 0.0, 0.0, 1.0e99, 0.0, k.dtmin, k.courantpar, 0.0};
+  // scalars: dt, cmax_global, time, time_max, dtsave, dtmin, courantpar, final
+  // flag, slowsteps, steps since set_time
+  const double sc[10] = {0.0, 0.0, 0.0, 1.0e99, 0.0, k.dtmin, k.courantpar, 0.0, double(k.slowsteps), 0.0};
   if ((e = cudaMalloc(&c->d_scal, sizeof(sc))) != cudaSuccess ||
       (e = cudaMemcpy(c->d_scal, sc, sizeof(sc), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (e = cudaMalloc(&c->d_red, 2 * sizeof(unsigned long long))) != cudaSuccess ||
@@ -1092,6 +1094,7 @@ int amrvac_gpu_set_time(amrvac_ctx *c, double t, double time_max, double dtsave)
   CK(cudaMemcpyAsync(c->d_scal + 2, v, sizeof(v), cudaMemcpyHostToDevice, c->stream));
   const double z = 0.0;
   CK(cudaMemcpyAsync(c->d_scal + 7, &z, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_scal + 9, &z, sizeof(double), cudaMemcpyHostToDevice, c->stream));  // it_init = it
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }

@@ -115,6 +115,10 @@ typedef struct amrvac_cfg {
   int precision;            /* 0 = plain FP64; 1 = mixed: FP32 reconstruction, wave
                                speeds, fluxes, Riemann solver; FP64 conserved state,
                                pressure recovery, accumulation, sources, small values */
+  int slowsteps;            /* setdt ramp (src/mod_dt.t:64-67): during the first
+                               slowsteps steps after amrvac_gpu_set_time, dt is
+                               scaled by 1 - (1 - n/slowsteps)^2 (n = 1, 2, ...);
+                               <= 0: off (default -1) */
 } amrvac_cfg;
 
 typedef struct amrvac_ctx amrvac_ctx;

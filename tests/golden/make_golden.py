@@ -7,8 +7,9 @@ Run once in a checkout that has the reference repository next to it:
 The logs are the reference's own correct_output fixtures: the only
 uniform-grid (refine_max_level=1) regression tests on the HLL/HLLD path,
 tests/mhd/field_loop_2.5D/correct_output/fl_2d_3step_{hlld,hll}_cada.log, and
-the periodic multi-level Orszag-Tang 2-D tests on the same schemes,
-tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_3step_{hlld,hll}_cada.log.
+the periodic multi-level tests on the same schemes,
+tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_3step_{hlld,hll}_cada.log and
+tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_3step_hll_cada.log.
 They are copied verbatim so the parity tests can run where the reference
 repository is absent.
 """
@@ -22,6 +23,7 @@ LOGS = [
     # multi-level (refine_max_level = 3, Löhner, regrid every step), periodic
     "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_3step_hlld_cada.log",
     "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_3step_hll_cada.log",
+    "tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_3step_hll_cada.log",
 ]
 
 

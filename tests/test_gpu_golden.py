@@ -87,24 +87,25 @@ def _amr_log_row(blocks, leaves, nbase, t, nw):
     return np.concatenate([[t], s1 / vol, s2 / vol])
 
 
-def _run_ot2d_amr(kw, nw, time_max=0.1, dtsave=1.0e-3):
+def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsave=1.0e-3, levels=3):
+    """The reference's time loop on a periodic 2-D multi-level grid: settree,
+    then setdt + advance + resettree every step, a log row at every dtsave."""
     from tests import _amr as A
     from amrvac_b200 import Context, make_cfg
     from amrvac_b200.amr import Tree, initial_hierarchy, lohner_flags
-    nb, xmin, xmax = [4, 4], [0.0, 0.0], [1.0, 1.0]
-    cfg = make_cfg(physics="mhd", ndim=2, ndir=2, typeboundary=["periodic"] * 4, **kw)
+    nw = len(weight)
+    xmin, xmax = [0.0, 0.0], [1.0, 1.0]
+    cfg = make_cfg(physics=physics, ndim=2, ndir=2, typeboundary=["periodic"] * 4, **kw)
     ctx = Context(cfg)
-    weight = np.zeros(nw)
-    weight[0] = weight[3] = 0.5
-    lkw = dict(refine_threshold=0.4, derefine_ratio=0.125, amr_wavefilter=1.0e-2)
+    lkw = dict(refine_threshold=threshold, derefine_ratio=0.125, amr_wavefilter=1.0e-2)
 
     def init(tree):
-        return A.fill_blocks(tree.leaves, 2, nb, _ot2d_prim(nw), "mhd", 2, 5.0 / 3.0, xmin, xmax)
+        return A.fill_blocks(tree.leaves, 2, nb, prim_fn, physics, 2, cfg.gamma, xmin, xmax)
 
     def err(tree, blocks):
         r, c, _ = lohner_flags(ctx, tree, blocks, xmin, xmax, weight, **lkw)
         return r, c
-    tree, blocks = initial_hierarchy(Tree(2, nb, 3), init, err)
+    tree, blocks = initial_hierarchy(Tree(2, nb, levels), init, err)
     ctx.set_amr_grid(tree.leaves, nb, xmin, xmax)
     ctx.upload(blocks)
     ctx.set_time(0.0, time_max, dtsave)
@@ -112,7 +113,7 @@ def _run_ot2d_amr(kw, nw, time_max=0.1, dtsave=1.0e-3):
     tsavelast = 0.0
     for _ in range(100000):
         ctx.step()
-        ctx.amr_resettree(weight, refine_max_level=3, **lkw)
+        ctx.amr_resettree(weight, refine_max_level=levels, **lkw)
         dt, cg, t = ctx.get_time()
         if t >= tsavelast + dtsave - 1e-12:
             tsavelast = t
@@ -130,8 +131,43 @@ def _run_ot2d_amr(kw, nw, time_max=0.1, dtsave=1.0e-3):
                  courantpar=0.9), 6),
 ])
 def test_orszag_tang_2d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
-    rows = _run_ot2d_amr(kw, nw)
+    weight = np.zeros(nw)
+    weight[0] = weight[3] = 0.5  # w_refine_weight(1) = w_refine_weight(4) = 0.5
+    rows = _run_amr_golden("mhd", [4, 4], _ot2d_prim(nw), weight, 0.4, kw, time_max=0.1)
     gold = oracle_lib.read_log(os.path.join(GOLD, f"ot_2d_3step_{name}_cada.log"))
+    assert rows.shape == gold.shape, (rows.shape, gold.shape)
+    bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
+    assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
+        np.argwhere(bad)[:10].tolist(), rows[bad][:10].tolist(), gold[bad][:10].tolist())
+
+
+# Kelvin-Helmholtz 2-D (tests/hd/Kelvin_Helmholtz_2D, reference, iprob 1):
+# 32^2 level-1 cells in 16^2 blocks, periodic, refine_max_level 3 with the
+# default estimator settings (w_refine_weight(1) = 1, refine_threshold 0.1),
+# slowsteps 10; scheme 3step_hll_cada (HLL, cada3, cmaxmean, CFL 0.9).
+
+
+def _kh2d_prim(X, Y, Z):
+    rhodens, rholight, kx, pint, dlin, sigma, vextra = 10.0, 1.0, 4.0 * np.pi, 2.5, 0.025, 0.00125, 0.0
+    out = np.zeros((4,) + X.shape)
+    out[0] = np.where((Y < 0.25) | (Y > 0.75), rholight, rhodens)
+    out[3] = pint
+    vx = np.zeros_like(X)
+    vx = np.where((Y <= 0.25 - dlin) | (Y >= 0.75 + dlin), vextra - 0.5, vx)
+    vx = np.where((Y >= 0.25 + dlin) & (Y <= 0.75 - dlin), vextra + 0.5, vx)
+    low = (Y > 0.25 - dlin) & (Y < 0.25 + dlin)
+    vx = np.where(low, (Y - (0.25 - dlin)) * ((vextra + 0.5) - (vextra - 0.5)) / (2.0 * dlin) + (vextra - 0.5), vx)
+    high = (Y > 0.75 - dlin) & (Y < 0.75 + dlin)
+    vx = np.where(high, (Y - (0.75 - dlin)) * ((vextra - 0.5) - (vextra + 0.5)) / (2.0 * dlin) + (vextra + 0.5), vx)
+    out[1] = vx
+    out[2] = 0.01 * np.sin(kx * X) * (np.exp(-0.5 * (Y - 0.25) ** 2 / sigma) + np.exp(-0.5 * (Y - 0.75) ** 2 / sigma))
+    return out
+
+
+def test_kelvin_helmholtz_2d_amr_golden_log_gpu(oracle_lib):
+    kw = dict(flux_scheme="hll", limiter="cada3", typeboundspeed="cmaxmean", courantpar=0.9, slowsteps=10)
+    rows = _run_amr_golden("hd", [2, 2], _kh2d_prim, np.array([1.0, 0.0, 0.0, 0.0]), 0.1, kw, time_max=0.05)
+    gold = oracle_lib.read_log(os.path.join(GOLD, "kh_2d_3step_hll_cada.log"))
     assert rows.shape == gold.shape, (rows.shape, gold.shape)
     bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
     assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
