@@ -106,7 +106,8 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
              typecourant="maxsum", cada3_radius=0.1, tvdlfeps=1.0, fix_small_values=False,
              check_small_values=True, small_values_method="error", small_density=0.0,
              small_pressure=0.0, time_stepper="threestep", ssprk_order=3, dtmin=1.0e-10,
-             typeboundary=None, zchunk=0, precision="fp64", slowsteps=-1) -> _lib.AmrvacCfg:
+             typeboundary=None, zchunk=0, precision="fp64", slowsteps=-1,
+             time_integrator="default") -> _lib.AmrvacCfg:
     """Build an ``amrvac_cfg`` from reference-style parameter names.
 
     typeboundary: list of 2*ndim entries (min1, max1, min2, ...), each a name
@@ -145,6 +146,7 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
     c.zchunk = zchunk
     c.precision = _lib.PRECISION[precision]
     c.slowsteps = int(slowsteps)
+    c.time_integrator = _lib.TIME_INTEGRATOR[time_integrator]
     nw = L.amrvac_gpu_nw(c)
     tb = typeboundary or ["periodic"] * (2 * ndim)
     for s in range(6):
@@ -186,6 +188,8 @@ def config_from_par(paths) -> RunConfig:
         raise ValueError(f"time_integrator {integ} not supported")
     if ts == "threestep" and integ not in (None, "ssprk3"):
         raise ValueError(f"time_integrator {integ} not supported")
+    if ts == "fourstep" and integ not in (None, "ssprk4", "rk4"):
+        raise ValueError(f"time_integrator {integ} not supported")
     cfg_kw = dict(
         physics=physics, ndim=ndim,
         gamma=plist.get(f"{physics}_gamma", None),
@@ -204,6 +208,7 @@ def config_from_par(paths) -> RunConfig:
         small_pressure=float(meth.get("small_pressure", 0.0)),
         time_stepper=ts,
         ssprk_order=int(meth.get("ssprk_order", 3)),
+        time_integrator=integ or "default",
     )
     if physics == "mhd":
         cfg_kw.update(typedivbfix=plist.get("typedivbfix", "linde"),

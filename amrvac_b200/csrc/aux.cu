@@ -201,6 +201,22 @@ cudaError_t launch_pack(const double *pool, double *dst, int first, int n, int n
   pack_kernel<<<592, 256, 0, s>>>(pool, dst, first, n, nw, ndim, ng, nbr, maps, bc, gbuf);
   return cudaGetLastError();
 }
+// rk4 combination (src/mod_advance.t:497-502): ps = (1/3)(-ps + ps1 + 2 ps2 + ps3),
+// summed left to right.
+__global__ void rk4_combine_kernel(double *__restrict__ u0, const double *__restrict__ u1,
+                                   const double *__restrict__ u2, const double *__restrict__ u3, size_t n) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const double s = ((-u0[e] + u1[e]) + 2.0 * u2[e]) + u3[e];
+    u0[e] = (1.0 / 3.0) * s;
+  }
+}
+
+cudaError_t launch_rk4_combine(double *u0, const double *u1, const double *u2, const double *u3, size_t n,
+                               cudaStream_t s) {
+  rk4_combine_kernel<<<4 * 148, 256, 0, s>>>(u0, u1, u2, u3, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_setdt_finalize(unsigned long long *red, double *scal, uint32_t *status, cudaStream_t s) {
   setdt_finalize_kernel<<<1, 1, 0, s>>>(red, scal, status);
   return cudaGetLastError();

@@ -70,7 +70,8 @@ struct amrvac_ctx {
   cudaStream_t stream = nullptr;
   int nblocks = 0;
   size_t per_block = 0;  // doubles per block per variable
-  double *pool[3] = {nullptr, nullptr, nullptr};
+  double *pool[4] = {nullptr, nullptr, nullptr, nullptr};  // ps, ps1, ps2 (+ ps3 for rk4)
+  int nreg = 3;                          // registers allocated
   int *d_nbr = nullptr;
   double *d_dx = nullptr;
   double *d_scal = nullptr;              // see setdt_finalize_kernel
@@ -219,6 +220,48 @@ int launch_getdt(amrvac_ctx *c, int reg) {
   return 0;
 }
 
+// fourstep (src/mod_advance.t:454-512), coefficients src/io/mod_input_output.t:
+// 1036-1067.  ssprk4 in registers 0..2: ps1 = ps + b11 dt L(ps); ps2 = a21 ps
+// + a22 ps1 + b22 dt L(ps1); ps1 = a31 ps + a33 ps2 + b33 dt L(ps2); ps = a41
+// ps + a44 ps1 + b44 dt L(ps1).  rk4 with register 3: ps1 = ps + dt/2 L(ps),
+// ps2 = ps + dt/2 L(ps1), ps3 = ps + dt L(ps2), ps = (1/3)(-ps + ps1 + 2 ps2 +
+// ps3), ps = ps + dt/6 L(ps3).  ev (optional) receives an event after every
+// stage.
+int launch_fourstep(amrvac_ctx *c, cudaEvent_t *ev) {
+  const amrvac_cfg &k = c->cfg;
+  int r = 0;
+  auto mark = [&](int i) { if (ev) cudaEventRecord(ev[i], c->stream); };
+  if (k.time_integrator == AMRVAC_TI_RK4) {
+    if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 0.5))) return r;
+    mark(0);
+    if ((r = launch_stage(c, 1, 2, 0, 1.0, 0.0, 0.5))) return r;
+    mark(1);
+    if ((r = launch_stage(c, 2, 3, 0, 1.0, 0.0, 1.0))) return r;
+    CK(launch_rk4_combine(c->pool[0], c->pool[1], c->pool[2], c->pool[3], c->per_block * c->nw * c->nblocks,
+                          c->stream));
+    ++c->launches;
+    mark(2);
+    r = launch_stage(c, 3, 0, 0, 1.0, 0.0, 1.0 / 6.0);
+    mark(3);
+    return r;
+  }
+  double b11, b22, b33, b44, a21, a31, a41;
+  if (k.ssprk_order == 2) {
+    b11 = 1.0 / 3.0; b22 = 1.0 / 3.0; b33 = 1.0 / 3.0; b44 = 1.0 / 4.0; a21 = 0.0; a31 = 0.0; a41 = 1.0 / 4.0;
+  } else {
+    b11 = 1.0 / 2.0; b22 = 1.0 / 2.0; b33 = 1.0 / 6.0; b44 = 1.0 / 2.0; a21 = 0.0; a31 = 2.0 / 3.0; a41 = 0.0;
+  }
+  if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, b11))) return r;
+  mark(0);
+  if ((r = launch_stage(c, 1, 2, 0, a21, 1.0 - a21, b22))) return r;
+  mark(1);
+  if ((r = launch_stage(c, 2, 1, 0, a31, 1.0 - a31, b33))) return r;
+  mark(2);
+  r = launch_stage(c, 1, 0, 0, a41, 1.0 - a41, b44);
+  mark(3);
+  return r;
+}
+
 // The configured RK stages (src/mod_advance.t:56-567) on registers 0..2.
 int launch_rk(amrvac_ctx *c) {
   const amrvac_cfg &k = c->cfg;
@@ -230,6 +273,8 @@ int launch_rk(amrvac_ctx *c) {
   } else if (k.time_stepper == AMRVAC_TS_TWOSTEP) {
     if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0))) return r;
     r = launch_stage(c, 1, 0, 0, 0.5, 0.5, 0.5);
+  } else if (k.time_stepper == AMRVAC_TS_FOURSTEP) {
+    r = launch_fourstep(c, nullptr);
   } else {
     double b11, b22, b33, a21, a31;
     if (k.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
@@ -292,6 +337,7 @@ void amrvac_gpu_default_cfg(amrvac_cfg *c) {
   c->zchunk = 0;
   c->precision = 0;
   c->slowsteps = -1;
+  c->time_integrator = AMRVAC_TI_DEFAULT;
 }
 
 int amrvac_gpu_nw(const amrvac_cfg *cfg) { return cfg ? nw_of(cfg) : AMRVAC_E_ARG; }
@@ -315,7 +361,13 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   if (k.limiter < 1 || k.limiter > 9) return fail(AMRVAC_E_UNSUPPORTED, "limiter not supported");
   if (k.typeboundspeed < 1 || k.typeboundspeed > 3) return fail(AMRVAC_E_ARG, "bad typeboundspeed");
   if (k.type_courant < 1 || k.type_courant > 3) return fail(AMRVAC_E_ARG, "bad type_courant");
-  if (k.time_stepper < 1 || k.time_stepper > 3) return fail(AMRVAC_E_UNSUPPORTED, "time_stepper not supported");
+  if (k.time_stepper < 1 || k.time_stepper > 4) return fail(AMRVAC_E_UNSUPPORTED, "time_stepper not supported");
+  if (k.time_integrator != AMRVAC_TI_DEFAULT &&
+      !(k.time_stepper == AMRVAC_TS_FOURSTEP && k.time_integrator == AMRVAC_TI_RK4))
+    return fail(AMRVAC_E_UNSUPPORTED, "time_integrator not supported for this time_stepper");
+  if ((k.time_stepper == AMRVAC_TS_THREESTEP || k.time_stepper == AMRVAC_TS_FOURSTEP) && k.ssprk_order != 2 &&
+      k.ssprk_order != 3)
+    return fail(AMRVAC_E_ARG, "ssprk_order must be 2 or 3");
   if (k.physics == 0 && k.ndir != k.ndim) return fail(AMRVAC_E_UNSUPPORTED, "hd requires ndir == ndim");
   if (k.physics == 1) {
     if (k.flux_scheme == AMRVAC_FS_HLLC) return fail(AMRVAC_E_UNSUPPORTED, "mhd hllc not supported");
@@ -330,6 +382,7 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   if (nw > AMRVAC_MAX_NW) return fail(AMRVAC_E_UNSUPPORTED, "too many variables");
   amrvac_ctx *c = new amrvac_ctx();
   c->cfg = k;
+  c->nreg = (k.time_stepper == AMRVAC_TS_FOURSTEP && k.time_integrator == AMRVAC_TI_RK4) ? 4 : 3;
   c->nw = nw;
   KernelKey key{k.physics == 1, k.ndim, k.ndir, k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM,
                 k.flux_scheme, k.limiter, k.typeboundspeed, k.precision == 1};
@@ -432,7 +485,7 @@ int amrvac_gpu_destroy(amrvac_ctx *c) {
   if (!c) return AMRVAC_E_ARG;
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->graph) cudaGraphExecDestroy(c->graph);
-  for (int r = 0; r < 3; ++r) cudaFree(c->pool[r]);
+  for (int r = 0; r < 4; ++r) cudaFree(c->pool[r]);
   cudaFree(c->d_nbr);
   cudaFree(c->d_dx);
   cudaFree(c->d_scal);
@@ -523,20 +576,20 @@ static int set_blocks_impl(amrvac_ctx *c, int nblocks, const double *dx, const i
   } else if (adopt_reg0) {
     // regrid into a new, larger buffer: the other registers follow its size
     const size_t cap = (size_t)nblocks + nblocks / 4 + 1;
-    for (int r = 0; r < 3; ++r) { cudaFree(c->pool[r]); c->pool[r] = nullptr; }
+    for (int r = 0; r < 4; ++r) { cudaFree(c->pool[r]); c->pool[r] = nullptr; }
     c->pool_cap = 0;
     c->pool[0] = adopt_reg0;
-    for (int r = 1; r < 3; ++r) CK(cudaMalloc(&c->pool[r], sizeof(double) * c->per_block * c->nw * cap));
+    for (int r = 1; r < c->nreg; ++r) CK(cudaMalloc(&c->pool[r], sizeof(double) * c->per_block * c->nw * cap));
     c->pool_cap = cap;
   } else {
     if ((size_t)nblocks > c->pool_cap || !c->pool[0]) {
-      for (int r = 0; r < 3; ++r) { cudaFree(c->pool[r]); c->pool[r] = nullptr; }
+      for (int r = 0; r < 4; ++r) { cudaFree(c->pool[r]); c->pool[r] = nullptr; }
       c->pool_cap = 0;
       const size_t cap = (size_t)nblocks + nblocks / 4 + 1;
-      for (int r = 0; r < 3; ++r) CK(cudaMalloc(&c->pool[r], sizeof(double) * c->per_block * c->nw * cap));
+      for (int r = 0; r < c->nreg; ++r) CK(cudaMalloc(&c->pool[r], sizeof(double) * c->per_block * c->nw * cap));
       c->pool_cap = cap;
     }
-    for (int r = 0; r < 3; ++r) CK(cudaMemsetAsync(c->pool[r], 0, bytes, c->stream));
+    for (int r = 0; r < c->nreg; ++r) CK(cudaMemsetAsync(c->pool[r], 0, bytes, c->stream));
   }
   c->nblocks = nblocks;
   if ((size_t)nblocks > c->nbr_cap || !c->d_nbr) {
@@ -1156,6 +1209,9 @@ int amrvac_gpu_run_timed(amrvac_ctx *c, int nsteps, double *total_ms, double *st
       CK(cudaEventRecord(ev[q++], c->stream));
       if (!r) r = launch_stage(c, 1, 0, 0, 0.5, 0.5, 0.5);
       CK(cudaEventRecord(ev[q++], c->stream));
+    } else if (k.time_stepper == AMRVAC_TS_FOURSTEP) {
+      r = launch_fourstep(c, &ev[q]);
+      q += 4;
     } else {
       double b11, b22, b33, a21, a31;
       if (k.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }

@@ -79,6 +79,9 @@ extern "C" {
 #define AMRVAC_TS_ONESTEP   1   /* Forward_Euler */
 #define AMRVAC_TS_TWOSTEP   2   /* ssprk2 (Heun) */
 #define AMRVAC_TS_THREESTEP 3   /* ssprk3, ssprk_order 3 or 2 */
+#define AMRVAC_TS_FOURSTEP  4   /* ssprk4 (ssprk_order 3: SSPRK(4,3), 2: SSP(4,2)) or rk4 */
+#define AMRVAC_TI_DEFAULT   0   /* time_integrator: the stepper's default (fourstep: ssprk4) */
+#define AMRVAC_TI_RK4       1   /* fourstep: the classical RK(4,4) */
 
 #define AMRVAC_MAX_NW 16
 
@@ -119,6 +122,7 @@ typedef struct amrvac_cfg {
                                slowsteps steps after amrvac_gpu_set_time, dt is
                                scaled by 1 - (1 - n/slowsteps)^2 (n = 1, 2, ...);
                                <= 0: off (default -1) */
+  int time_integrator;      /* AMRVAC_TI_* (src/mod_advance.t:454-512) */
 } amrvac_cfg;
 
 typedef struct amrvac_ctx amrvac_ctx;

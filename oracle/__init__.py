@@ -37,6 +37,7 @@ class OrcCfg(ctypes.Structure):
         ("check_small_values", ctypes.c_int), ("small_values_method", ctypes.c_int),
         ("small_density", ctypes.c_double), ("small_pressure", ctypes.c_double),
         ("divbdiff", ctypes.c_double), ("ssprk_order", ctypes.c_int),
+        ("time_stepper", ctypes.c_int), ("time_integrator", ctypes.c_int),
     ]
 
 
@@ -129,7 +130,7 @@ def make_cfg(*, ndim=2, ndir=None, physics="hd", block_nx=16, nghost=2, gamma=No
              glm_alpha=0.5, glm_extended=True, courantpar=0.8, type_courant=1,
              cada3_radius=0.1, tvdlfeps=1.0, fix_small_values=False, check_small_values=True,
              small_values_method="error", small_density=0.0, small_pressure=0.0,
-             divbdiff=0.8, ssprk_order=3) -> OrcCfg:
+             divbdiff=0.8, ssprk_order=3, time_stepper="threestep", time_integrator="default") -> OrcCfg:
     c = OrcCfg()
     c.ndim = ndim
     c.ndir = ndim if ndir is None else ndir
@@ -156,6 +157,8 @@ def make_cfg(*, ndim=2, ndir=None, physics="hd", block_nx=16, nghost=2, gamma=No
     c.small_pressure = small_pressure
     c.divbdiff = divbdiff
     c.ssprk_order = ssprk_order
+    c.time_stepper = {"threestep": 3, "fourstep": 4}[time_stepper]
+    c.time_integrator = {"default": 0, "ssprk4": 0, "rk4": 1}[time_integrator]
     lib().orc_cfg_finalize(ctypes.byref(c))
     return c
 

@@ -1130,7 +1130,7 @@ struct Grid {
   double dx[3], xmin[3], xmax[3];
   int bc[6];
   std::vector<int> nbr;  // [ib][27] neighbour block or -1 (physical boundary)
-  std::vector<double> reg[3];
+  std::vector<double> reg[4];
   size_t bsize;
 };
 
@@ -1148,6 +1148,7 @@ int orc_cfg_finalize(orc_cfg *cfg) {
   Ix x = make_ix(*cfg);
   cfg->nw = x.nw;
   if (cfg->ssprk_order == 0) cfg->ssprk_order = 3;
+  if (cfg->time_stepper == 0) cfg->time_stepper = 3;
   return x.nw;
 }
 
@@ -1288,7 +1289,7 @@ orc_grid *orc_grid_create(const orc_cfg *cfg, const int *domain_nx, const double
   }
   for (int q = 0; q < 6; ++q) g->bc[q] = q < 2 * cfg->ndim ? bc[q] : ORC_BC_PERIODIC;
   g->bsize = g->s.g.cells * (size_t)g->s.x.nw;
-  for (int r = 0; r < 3; ++r) g->reg[r].assign(g->bsize * g->nblocks, 0.0);
+  for (int r = 0; r < 4; ++r) g->reg[r].assign(g->bsize * g->nblocks, 0.0);
   g->nbr.assign((size_t)g->nblocks * 27, -1);
   for (int ib = 0; ib < g->nblocks; ++ib) {
     int ig[3] = {ib % g->nb[0], (ib / g->nb[0]) % g->nb[1], ib / (g->nb[0] * g->nb[1])};
@@ -1484,9 +1485,57 @@ void orc_grid_combine_reg(orc_grid *g, int dst, double a, int ra, double b, int 
   for (size_t p = 0; p < D.size(); ++p) D[p] = a * A[p] + b * B[p];
 }
 
+extern "C++" {
+// fourstep (src/mod_advance.t:454-512), coefficients
+// src/io/mod_input_output.t:1036-1067, on registers 0..3 through the grid's
+// advect1 (stage plus getbc), copy and two-term combination.
+template <class Adv, class Copy, class Comb, class Comb4>
+int fourstep(const orc_cfg &c, double dt, Adv advect1, Copy copy, Comb combine, Comb4 rk4_combine) {
+  int st = 0;
+  copy(1, 0);  // advect: ps1 = ps before the stepper
+  if (c.time_integrator == 1) {  // rk4
+    copy(2, 0);
+    copy(3, 0);
+    st |= advect1(0, 1, 0.5 * dt, 0.5);
+    st |= advect1(1, 2, 0.5 * dt, 0.5);
+    st |= advect1(2, 3, 1.0 * dt, 1.0);
+    rk4_combine();
+    st |= advect1(3, 0, (1.0 / 6.0) * dt, 1.0 / 6.0);
+    return st;
+  }
+  double b11, b22, b33, b44, a21, a31, a41;
+  if (c.ssprk_order == 2) {
+    b11 = 1.0 / 3.0; b22 = 1.0 / 3.0; b33 = 1.0 / 3.0; b44 = 1.0 / 4.0; a21 = 0.0; a31 = 0.0; a41 = 1.0 / 4.0;
+  } else {
+    b11 = 1.0 / 2.0; b22 = 1.0 / 2.0; b33 = 1.0 / 6.0; b44 = 1.0 / 2.0; a21 = 0.0; a31 = 2.0 / 3.0; a41 = 0.0;
+  }
+  st |= advect1(0, 1, b11 * dt, b11);
+  combine(2, a21, 0, 1.0 - a21, 1);
+  st |= advect1(1, 2, b22 * dt, b22);
+  combine(1, a31, 0, 1.0 - a31, 2);
+  st |= advect1(2, 1, b33 * dt, b33);
+  combine(0, a41, 0, 1.0 - a41, 1);
+  st |= advect1(1, 0, b44 * dt, b44);
+  return st;
+}
+
+// ps = (1/3)(-ps + ps1 + 2 ps2 + ps3) over whole (ghosted) registers
+inline void rk4_combine_regs(std::vector<double> *reg) {
+  for (size_t p = 0; p < reg[0].size(); ++p)
+    reg[0][p] = (1.0 / 3.0) * (((-reg[0][p] + reg[1][p]) + 2.0 * reg[2][p]) + reg[3][p]);
+}
+}  // extern "C++"
+
 // advect threestep/ssprk3 (src/mod_advance.t:56-73, 249-267), coefficients
-// src/io/mod_input_output.t:941-964.
+// src/io/mod_input_output.t:941-964; fourstep as above.
 int orc_grid_advance(orc_grid *g, double dt, double cmax_global, int nthreads) {
+  if (g->s.c.time_stepper == 4)
+    return fourstep(
+        g->s.c, dt,
+        [&](int ra, int rb, double qdt, double f) { return orc_grid_advect1(g, ra, rb, qdt, f, cmax_global, nthreads); },
+        [&](int d, int s2) { orc_grid_copy_reg(g, d, s2); },
+        [&](int d, double a, int ra, double b, int rb) { orc_grid_combine_reg(g, d, a, ra, b, rb); },
+        [&]() { rk4_combine_regs(g->reg); });
   double b11, b22, b33, a21, a31;
   if (g->s.c.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
   else { b11 = 1.0; b22 = 1.0 / 4.0; b33 = 2.0 / 3.0; a21 = 3.0 / 4.0; a31 = 1.0 / 3.0; }
@@ -1871,7 +1920,7 @@ struct AmrGrid {
   std::vector<int> level, ig;                 // ig[3*b]
   std::vector<int> ntype, nid;                // [b*27]
   std::vector<int> child;                     // [(b*27+q)*8 + cbits]
-  std::vector<double> reg[3];                 // ghosted blocks
+  std::vector<double> reg[4];                 // ghosted blocks
   std::vector<double> psc;                    // [b] coarse representation
   std::vector<std::vector<double>> pflux;     // [b*6 + 2*d + side]
   size_t bsize, csize;
@@ -2285,7 +2334,7 @@ orc_amr *orc_amr_create(const orc_cfg *cfg, const int *nbase, const double *xpro
   }
   G->bsize = G->s.g.cells * (size_t)G->s.x.nw;
   G->csize = G->sc.g.cells * (size_t)G->s.x.nw;
-  for (int r = 0; r < 3; ++r) G->reg[r].assign(G->bsize * nleaf, 0.0);
+  for (int r = 0; r < 4; ++r) G->reg[r].assign(G->bsize * nleaf, 0.0);
   G->psc.assign(G->csize * nleaf, 0.0);
   G->pflux.assign(6 * (size_t)nleaf, {});
   return reinterpret_cast<orc_amr *>(G);
@@ -2346,6 +2395,13 @@ void orc_amr_combine_reg(orc_amr *a, int dst, double ca, int ra, double cb, int 
 
 int orc_amr_advance(orc_amr *a, double dt, double cmax_global, int nthreads) {
   AmrGrid *G = reinterpret_cast<AmrGrid *>(a);
+  if (G->s.c.time_stepper == 4)
+    return fourstep(
+        G->s.c, dt,
+        [&](int ra, int rb, double qdt, double f) { return amr_advect1(*G, ra, rb, qdt, f, cmax_global, nthreads); },
+        [&](int d, int s2) { G->reg[d] = G->reg[s2]; },
+        [&](int d, double x, int ra, double y, int rb) { orc_amr_combine_reg(a, d, x, ra, y, rb); },
+        [&]() { rk4_combine_regs(G->reg); });
   double b11, b22, b33, a21, a31;
   if (G->s.c.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
   else { b11 = 1.0; b22 = 1.0 / 4.0; b33 = 2.0 / 3.0; a21 = 3.0 / 4.0; a31 = 1.0 / 3.0; }

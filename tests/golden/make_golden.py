@@ -9,7 +9,9 @@ uniform-grid (refine_max_level=1) regression tests on the HLL/HLLD path,
 tests/mhd/field_loop_2.5D/correct_output/fl_2d_3step_{hlld,hll}_cada.log, and
 the periodic multi-level tests on the same schemes,
 tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_3step_{hlld,hll}_cada.log and
-tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_3step_hll_cada.log.
+tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_3step_hll_cada.log, and the
+fourstep variants (rk4 with HLL and woodward, ssprk4 with HLLC and koren)
+ot_2d_4step_hll_mc.log, kh_2d_4step_hll_mc.log, kh_2d_4step_hllc_ko.log.
 They are copied verbatim so the parity tests can run where the reference
 repository is absent.
 """
@@ -24,6 +26,9 @@ LOGS = [
     "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_3step_hlld_cada.log",
     "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_3step_hll_cada.log",
     "tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_3step_hll_cada.log",
+    "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_4step_hll_mc.log",
+    "tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_4step_hll_mc.log",
+    "tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_4step_hllc_ko.log",
 ]
 
 

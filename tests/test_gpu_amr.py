@@ -64,6 +64,11 @@ CASES = [
     ("mhd2_hlld_linde", 2, 2, dict(physics="mhd", flux_scheme="hlld", limiter="vanleer", typedivbfix="linde")),
     ("mhd2_hll_glm", 2, 2, dict(physics="mhd", flux_scheme="hll", limiter="minmod", typedivbfix="glm")),
     ("hd3_hllc", 3, 2, dict(physics="hd", flux_scheme="hllc", limiter="vanleer")),
+    ("hd2_hllc_koren_ssprk43", 2, 3, dict(physics="hd", flux_scheme="hllc", limiter="koren", time_stepper="fourstep")),
+    ("hd2_hll_woodward_ssp42", 2, 2, dict(physics="hd", flux_scheme="hll", limiter="woodward", time_stepper="fourstep",
+                                          ssprk_order=2)),
+    ("mhd2_hll_woodward_rk4", 2, 3, dict(physics="mhd", flux_scheme="hll", limiter="woodward", typedivbfix="linde",
+                                         time_stepper="fourstep", time_integrator="rk4")),
 ]
 
 

@@ -126,15 +126,17 @@ def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsav
 
 
 @pytest.mark.parametrize("name,kw,nw", [
-    ("hlld", dict(flux_scheme="hlld", limiter="cada3", typedivbfix="glm", courantpar=0.9), 7),
-    ("hll", dict(flux_scheme="hll", limiter="cada3", typedivbfix="linde", typeboundspeed="cmaxmean",
-                 courantpar=0.9), 6),
+    ("3step_hlld_cada", dict(flux_scheme="hlld", limiter="cada3", typedivbfix="glm", courantpar=0.9), 7),
+    ("3step_hll_cada", dict(flux_scheme="hll", limiter="cada3", typedivbfix="linde", typeboundspeed="cmaxmean",
+                            courantpar=0.9), 6),
+    ("4step_hll_mc", dict(flux_scheme="hll", limiter="woodward", typedivbfix="linde", typeboundspeed="cmaxmean",
+                          courantpar=0.9, time_stepper="fourstep", time_integrator="rk4"), 6),
 ])
 def test_orszag_tang_2d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
     weight = np.zeros(nw)
     weight[0] = weight[3] = 0.5  # w_refine_weight(1) = w_refine_weight(4) = 0.5
     rows = _run_amr_golden("mhd", [4, 4], _ot2d_prim(nw), weight, 0.4, kw, time_max=0.1)
-    gold = oracle_lib.read_log(os.path.join(GOLD, f"ot_2d_3step_{name}_cada.log"))
+    gold = oracle_lib.read_log(os.path.join(GOLD, f"ot_2d_{name}.log"))
     assert rows.shape == gold.shape, (rows.shape, gold.shape)
     bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
     assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
@@ -144,7 +146,9 @@ def test_orszag_tang_2d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
 # Kelvin-Helmholtz 2-D (tests/hd/Kelvin_Helmholtz_2D, reference, iprob 1):
 # 32^2 level-1 cells in 16^2 blocks, periodic, refine_max_level 3 with the
 # default estimator settings (w_refine_weight(1) = 1, refine_threshold 0.1),
-# slowsteps 10; scheme 3step_hll_cada (HLL, cada3, cmaxmean, CFL 0.9).
+# slowsteps 10; schemes 3step_hll_cada (SSP-RK3, HLL, cada3), 4step_hll_mc
+# (RK4, HLL, woodward) and 4step_hllc_ko (SSPRK(4,3), HLLC, koren), all with
+# cmaxmean and CFL 0.9.
 
 
 def _kh2d_prim(X, Y, Z):
@@ -164,10 +168,16 @@ def _kh2d_prim(X, Y, Z):
     return out
 
 
-def test_kelvin_helmholtz_2d_amr_golden_log_gpu(oracle_lib):
-    kw = dict(flux_scheme="hll", limiter="cada3", typeboundspeed="cmaxmean", courantpar=0.9, slowsteps=10)
+@pytest.mark.parametrize("name,kw", [
+    ("3step_hll_cada", dict(flux_scheme="hll", limiter="cada3", typeboundspeed="cmaxmean")),
+    ("4step_hll_mc", dict(flux_scheme="hll", limiter="woodward", typeboundspeed="cmaxmean", time_stepper="fourstep",
+                          time_integrator="rk4")),
+    ("4step_hllc_ko", dict(flux_scheme="hllc", limiter="koren", typeboundspeed="cmaxmean", time_stepper="fourstep")),
+])
+def test_kelvin_helmholtz_2d_amr_golden_log_gpu(oracle_lib, name, kw):
+    kw = dict(kw, courantpar=0.9, slowsteps=10)
     rows = _run_amr_golden("hd", [2, 2], _kh2d_prim, np.array([1.0, 0.0, 0.0, 0.0]), 0.1, kw, time_max=0.05)
-    gold = oracle_lib.read_log(os.path.join(GOLD, "kh_2d_3step_hll_cada.log"))
+    gold = oracle_lib.read_log(os.path.join(GOLD, f"kh_2d_{name}.log"))
     assert rows.shape == gold.shape, (rows.shape, gold.shape)
     bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
     assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
