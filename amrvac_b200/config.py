@@ -184,7 +184,7 @@ def config_from_par(paths) -> RunConfig:
             tb.append(v if isinstance(v, list) else [v])
     ts = _first(meth.get("time_stepper", "twostep"))
     integ = _first(meth.get("time_integrator", None))
-    if ts == "twostep" and integ not in (None, "ssprk2"):
+    if ts == "twostep" and integ not in (None, "ssprk2", "Predictor_Corrector"):
         raise ValueError(f"time_integrator {integ} not supported")
     if ts == "threestep" and integ not in (None, "ssprk3"):
         raise ValueError(f"time_integrator {integ} not supported")

@@ -181,7 +181,10 @@ int launch_amr_ghost_pass(amrvac_ctx *c, int reg) {
   return 0;
 }
 
-int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a, double b, double dtfactor) {
+// fix: apply fix_conserve after the stage on a multi-level grid (the
+// reference's predictor step skips it: fix_conserve_at_step = .false.).
+int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a, double b, double dtfactor,
+                 bool fix = true) {
   if (c->amr)
     if (int r = launch_amr_ghost_pass(c, reg_ct)) return r;
   StageArgs A = stage_args(c, reg_ct, reg_new, reg_base, a, b, dtfactor);
@@ -198,7 +201,7 @@ int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a,
                              c->per_block * c->nw, c->stream));
     ++c->launches;
   }
-  if (c->amr) {  // fix_conserve on the stage's output
+  if (c->amr && fix) {  // fix_conserve on the stage's output
     AmrFixArgs F = c->amr->F;
     F.w = c->pool[reg_new];
     CK(launch_amr_fix(F, c->amr->nslots, c->cfg.ndim, c->stream));
@@ -271,8 +274,13 @@ int launch_rk(amrvac_ctx *c) {
                        cudaMemcpyDeviceToDevice, c->stream));
     r = launch_stage(c, 1, 0, 0, 0.0, 1.0, 1.0);
   } else if (k.time_stepper == AMRVAC_TS_TWOSTEP) {
-    if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0))) return r;
-    r = launch_stage(c, 1, 0, 0, 0.5, 0.5, 0.5);
+    if (k.time_integrator == AMRVAC_TI_SSPRK2) {
+      if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0))) return r;
+      r = launch_stage(c, 1, 0, 0, 0.5, 0.5, 0.5);
+    } else {  // Predictor_Corrector (src/mod_advance.t:104-111)
+      if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 0.5, false))) return r;
+      r = launch_stage(c, 1, 0, 0, 1.0, 0.0, 1.0);
+    }
   } else if (k.time_stepper == AMRVAC_TS_FOURSTEP) {
     r = launch_fourstep(c, nullptr);
   } else {
@@ -363,8 +371,12 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   if (k.type_courant < 1 || k.type_courant > 3) return fail(AMRVAC_E_ARG, "bad type_courant");
   if (k.time_stepper < 1 || k.time_stepper > 4) return fail(AMRVAC_E_UNSUPPORTED, "time_stepper not supported");
   if (k.time_integrator != AMRVAC_TI_DEFAULT &&
-      !(k.time_stepper == AMRVAC_TS_FOURSTEP && k.time_integrator == AMRVAC_TI_RK4))
+      !(k.time_stepper == AMRVAC_TS_FOURSTEP && k.time_integrator == AMRVAC_TI_RK4) &&
+      !(k.time_stepper == AMRVAC_TS_TWOSTEP && k.time_integrator == AMRVAC_TI_SSPRK2))
     return fail(AMRVAC_E_UNSUPPORTED, "time_integrator not supported for this time_stepper");
+  if (k.time_stepper == AMRVAC_TS_TWOSTEP && k.time_integrator == AMRVAC_TI_DEFAULT && k.flux_scheme == AMRVAC_FS_TVDLF)
+    return fail(AMRVAC_E_UNSUPPORTED,
+                "twostep Predictor_Corrector with tvdlf needs the Hancock predictor (not built); use ssprk2");
   if ((k.time_stepper == AMRVAC_TS_THREESTEP || k.time_stepper == AMRVAC_TS_FOURSTEP) && k.ssprk_order != 2 &&
       k.ssprk_order != 3)
     return fail(AMRVAC_E_ARG, "ssprk_order must be 2 or 3");
@@ -1205,9 +1217,10 @@ int amrvac_gpu_run_timed(amrvac_ctx *c, int nsteps, double *total_ms, double *st
       r = launch_stage(c, 1, 0, 0, 0.0, 1.0, 1.0);
       CK(cudaEventRecord(ev[q++], c->stream));
     } else if (k.time_stepper == AMRVAC_TS_TWOSTEP) {
-      r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);
+      const bool pc = k.time_integrator != AMRVAC_TI_SSPRK2;
+      r = pc ? launch_stage(c, 0, 1, 0, 0.0, 1.0, 0.5, false) : launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);
       CK(cudaEventRecord(ev[q++], c->stream));
-      if (!r) r = launch_stage(c, 1, 0, 0, 0.5, 0.5, 0.5);
+      if (!r) r = pc ? launch_stage(c, 1, 0, 0, 1.0, 0.0, 1.0) : launch_stage(c, 1, 0, 0, 0.5, 0.5, 0.5);
       CK(cudaEventRecord(ev[q++], c->stream));
     } else if (k.time_stepper == AMRVAC_TS_FOURSTEP) {
       r = launch_fourstep(c, &ev[q]);
@@ -1454,8 +1467,9 @@ static int adjoint_step_impl(amrvac_ctx *c, const double *u0, const double *u1, 
       k.fix_small_values || k.precision != 0)
     return fail(AMRVAC_E_UNSUPPORTED,
                 "adjoint: 2-D hd, hll or hllc, minmod or vanleer, Einfeldt, FP64, no fix_small_values");
-  if (k.time_stepper != AMRVAC_TS_THREESTEP && k.time_stepper != AMRVAC_TS_TWOSTEP)
-    return fail(AMRVAC_E_UNSUPPORTED, "adjoint: threestep or twostep");
+  if (k.time_stepper != AMRVAC_TS_THREESTEP &&
+      !(k.time_stepper == AMRVAC_TS_TWOSTEP && k.time_integrator == AMRVAC_TI_SSPRK2))
+    return fail(AMRVAC_E_UNSUPPORTED, "adjoint: threestep or twostep with time_integrator ssprk2");
   for (int sd = 0; sd < 4; ++sd)
     if (c->bc.kind[sd] == BCK_MIRROR) return fail(AMRVAC_E_UNSUPPORTED, "adjoint: periodic or cont boundaries");
   for (int b = 1; b < c->nblocks; ++b)

@@ -687,6 +687,8 @@ int amrvac_ens_create(const amrvac_cfg *cfg, int ninst, const amrvac_ens_instanc
   if (k.type_courant != AMRVAC_COURANT_MAXSUM) return efail(AMRVAC_E_UNSUPPORTED, "ensembles use typecourant maxsum");
   if (k.typeboundspeed < 1 || k.typeboundspeed > 3) return efail(AMRVAC_E_ARG, "bad typeboundspeed");
   if (k.time_stepper < 1 || k.time_stepper > 3) return efail(AMRVAC_E_UNSUPPORTED, "time_stepper not supported");
+  if (k.time_stepper == AMRVAC_TS_TWOSTEP && k.time_integrator != AMRVAC_TI_SSPRK2)
+    return efail(AMRVAC_E_UNSUPPORTED, "ensembles: twostep with time_integrator ssprk2 only");
   if (k.precision != 0 && k.precision != 1) return efail(AMRVAC_E_ARG, "precision must be 0 or 1");
   for (int s = 0; s < 4; ++s)
     for (int v = 0; v < 4; ++v) {

@@ -77,11 +77,13 @@ extern "C" {
 #define AMRVAC_BC_ASYMM    3
 /* time_stepper / time_integrator (src/mod_advance.t:56-567) */
 #define AMRVAC_TS_ONESTEP   1   /* Forward_Euler */
-#define AMRVAC_TS_TWOSTEP   2   /* ssprk2 (Heun) */
+#define AMRVAC_TS_TWOSTEP   2   /* Predictor_Corrector (default) or ssprk2 (Heun) */
 #define AMRVAC_TS_THREESTEP 3   /* ssprk3, ssprk_order 3 or 2 */
 #define AMRVAC_TS_FOURSTEP  4   /* ssprk4 (ssprk_order 3: SSPRK(4,3), 2: SSP(4,2)) or rk4 */
-#define AMRVAC_TI_DEFAULT   0   /* time_integrator: the stepper's default (fourstep: ssprk4) */
+#define AMRVAC_TI_DEFAULT   0   /* time_integrator: the stepper's default (twostep:
+                                   Predictor_Corrector, threestep: ssprk3, fourstep: ssprk4) */
 #define AMRVAC_TI_RK4       1   /* fourstep: the classical RK(4,4) */
+#define AMRVAC_TI_SSPRK2    2   /* twostep: ssprk2 (Heun) */
 
 #define AMRVAC_MAX_NW 16
 

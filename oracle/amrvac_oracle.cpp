@@ -1519,6 +1519,24 @@ int fourstep(const orc_cfg &c, double dt, Adv advect1, Copy copy, Comb combine, 
   return st;
 }
 
+// twostep (src/mod_advance.t:102-133): Predictor_Corrector — predictor
+// ps1 = ps + dt/2 L(ps) with the same scheme (typepred1 for hll, hllc,
+// hlld) and no flux fix, corrector ps = ps + dt L(ps1) — or ssprk2.
+template <class Adv, class Copy, class Comb>
+int twostep(const orc_cfg &c, double dt, Adv advect1, Copy copy, Comb combine) {
+  int st = 0;
+  copy(1, 0);
+  if (c.time_integrator == 2) {
+    st |= advect1(0, 1, dt, 1.0, true);
+    combine(0, 0.5, 0, 0.5, 1);
+    st |= advect1(1, 0, 0.5 * dt, 0.5, true);
+    return st;
+  }
+  st |= advect1(0, 1, 0.5 * dt, 0.5, false);
+  st |= advect1(1, 0, dt, 1.0, true);
+  return st;
+}
+
 // ps = (1/3)(-ps + ps1 + 2 ps2 + ps3) over whole (ghosted) registers
 inline void rk4_combine_regs(std::vector<double> *reg) {
   for (size_t p = 0; p < reg[0].size(); ++p)
@@ -1529,6 +1547,12 @@ inline void rk4_combine_regs(std::vector<double> *reg) {
 // advect threestep/ssprk3 (src/mod_advance.t:56-73, 249-267), coefficients
 // src/io/mod_input_output.t:941-964; fourstep as above.
 int orc_grid_advance(orc_grid *g, double dt, double cmax_global, int nthreads) {
+  if (g->s.c.time_stepper == 2)
+    return twostep(
+        g->s.c, dt,
+        [&](int ra, int rb, double qdt, double f, bool) { return orc_grid_advect1(g, ra, rb, qdt, f, cmax_global, nthreads); },
+        [&](int d, int s2) { orc_grid_copy_reg(g, d, s2); },
+        [&](int d, double a, int ra, double b, int rb) { orc_grid_combine_reg(g, d, a, ra, b, rb); });
   if (g->s.c.time_stepper == 4)
     return fourstep(
         g->s.c, dt,
@@ -2241,7 +2265,8 @@ void amr_fix_conserve(AmrGrid &G, std::vector<double> &reg) {
       }
 }
 
-int amr_advect1(AmrGrid &G, int ra, int rb, double qdt, double dtfactor, double cmax_global, int nthreads) {
+int amr_advect1(AmrGrid &G, int ra, int rb, double qdt, double dtfactor, double cmax_global, int nthreads,
+                bool fix = true) {
   int st = 0;
   const size_t bs = G.bsize;
 #ifdef _OPENMP
@@ -2266,7 +2291,7 @@ int amr_advect1(AmrGrid &G, int ra, int rb, double qdt, double dtfactor, double 
     std::memcpy(&G.reg[rb][bs * b], w.d.data(), sizeof(double) * bs);
     amr_store_flux(G, b, fc);
   }
-  amr_fix_conserve(G, G.reg[rb]);
+  if (fix) amr_fix_conserve(G, G.reg[rb]);
   amr_getbc(G, G.reg[rb]);
   return st;
 }
@@ -2395,6 +2420,14 @@ void orc_amr_combine_reg(orc_amr *a, int dst, double ca, int ra, double cb, int 
 
 int orc_amr_advance(orc_amr *a, double dt, double cmax_global, int nthreads) {
   AmrGrid *G = reinterpret_cast<AmrGrid *>(a);
+  if (G->s.c.time_stepper == 2)
+    return twostep(
+        G->s.c, dt,
+        [&](int ra, int rb, double qdt, double f, bool fix) {
+          return amr_advect1(*G, ra, rb, qdt, f, cmax_global, nthreads, fix);
+        },
+        [&](int d, int s2) { G->reg[d] = G->reg[s2]; },
+        [&](int d, double x, int ra, double y, int rb) { orc_amr_combine_reg(a, d, x, ra, y, rb); });
   if (G->s.c.time_stepper == 4)
     return fourstep(
         G->s.c, dt,

@@ -61,8 +61,8 @@ typedef struct {
   double small_density, small_pressure;
   double divbdiff;
   int ssprk_order;        /* 3 (Gottlieb-Shu) or 2 */
-  int time_stepper;       /* 3 threestep (0 means 3), 4 fourstep */
-  int time_integrator;    /* fourstep: 0 ssprk4, 1 rk4 */
+  int time_stepper;       /* 2 twostep, 3 threestep (0 means 3), 4 fourstep */
+  int time_integrator;    /* twostep: 0 Predictor_Corrector, 2 ssprk2; fourstep: 0 ssprk4, 1 rk4 */
 } orc_cfg;
 
 /* Number of flux variables implied by cfg (sets cfg->nw too). */

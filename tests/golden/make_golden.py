@@ -11,7 +11,8 @@ the periodic multi-level tests on the same schemes,
 tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_3step_{hlld,hll}_cada.log and
 tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_3step_hll_cada.log, and the
 fourstep variants (rk4 with HLL and woodward, ssprk4 with HLLC and koren)
-ot_2d_4step_hll_mc.log, kh_2d_4step_hll_mc.log, kh_2d_4step_hllc_ko.log.
+ot_2d_4step_hll_mc.log, kh_2d_4step_hll_mc.log, kh_2d_4step_hllc_ko.log and
+(RK4, TVDLF, cada3) ot_2d_rk4_tvdlf_cada.log, kh_2d_rk4_tvdlf_cada.log.
 They are copied verbatim so the parity tests can run where the reference
 repository is absent.
 """
@@ -29,6 +30,8 @@ LOGS = [
     "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_4step_hll_mc.log",
     "tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_4step_hll_mc.log",
     "tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_4step_hllc_ko.log",
+    "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_rk4_tvdlf_cada.log",
+    "tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_rk4_tvdlf_cada.log",
 ]
 
 

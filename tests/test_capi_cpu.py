@@ -128,3 +128,20 @@ def test_config_from_par(tmp_path):
     assert rc.physics == "hd" and rc.domain_nx == [256, 256]
     assert rc.cfg.flux_scheme == 3 and rc.cfg.limiter == 5 and rc.cfg.gamma == 1.4
     assert rc.cfg.time_stepper == 3 and rc.xprobmin == [0.0, -0.5]
+
+
+def test_time_integrators_are_checked():
+    """twostep is Predictor_Corrector by default (the reference's default) or
+    ssprk2 on request; TVDLF's Hancock predictor is not built, so that pair
+    is refused at creation (which needs no device: the check comes first)."""
+    from amrvac_b200 import _lib, make_cfg
+    lib = _lib.load()
+    import ctypes
+    h = ctypes.c_void_p()
+    bad = make_cfg(physics="hd", ndim=2, flux_scheme="tvdlf", time_stepper="twostep")
+    assert lib.amrvac_gpu_create(ctypes.byref(bad), ctypes.byref(h)) == _lib.E_UNSUPPORTED
+    bad = make_cfg(physics="hd", ndim=2, flux_scheme="hll", time_stepper="threestep", time_integrator="rk4")
+    assert lib.amrvac_gpu_create(ctypes.byref(bad), ctypes.byref(h)) == _lib.E_UNSUPPORTED
+    ok = make_cfg(physics="hd", ndim=2, flux_scheme="hll", time_stepper="twostep")
+    assert ok.time_stepper == 2 and ok.time_integrator == 0
+    assert make_cfg(physics="hd", ndim=2, time_stepper="twostep", time_integrator="ssprk2").time_integrator == 2

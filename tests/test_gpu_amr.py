@@ -69,6 +69,9 @@ CASES = [
                                           ssprk_order=2)),
     ("mhd2_hll_woodward_rk4", 2, 3, dict(physics="mhd", flux_scheme="hll", limiter="woodward", typedivbfix="linde",
                                          time_stepper="fourstep", time_integrator="rk4")),
+    ("hd2_hllc_minmod_pc", 2, 3, dict(physics="hd", flux_scheme="hllc", limiter="minmod", time_stepper="twostep")),
+    ("mhd2_hlld_glm_ssprk2", 2, 2, dict(physics="mhd", flux_scheme="hlld", limiter="vanleer", typedivbfix="glm",
+                                        time_stepper="twostep", time_integrator="ssprk2")),
 ]
 
 

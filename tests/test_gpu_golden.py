@@ -131,6 +131,8 @@ def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsav
                             courantpar=0.9), 6),
     ("4step_hll_mc", dict(flux_scheme="hll", limiter="woodward", typedivbfix="linde", typeboundspeed="cmaxmean",
                           courantpar=0.9, time_stepper="fourstep", time_integrator="rk4"), 6),
+    ("rk4_tvdlf_cada", dict(flux_scheme="tvdlf", limiter="cada3", typedivbfix="linde", typeboundspeed="cmaxmean",
+                            courantpar=0.9, time_stepper="fourstep", time_integrator="rk4"), 6),
 ])
 def test_orszag_tang_2d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
     weight = np.zeros(nw)
@@ -173,6 +175,8 @@ def _kh2d_prim(X, Y, Z):
     ("4step_hll_mc", dict(flux_scheme="hll", limiter="woodward", typeboundspeed="cmaxmean", time_stepper="fourstep",
                           time_integrator="rk4")),
     ("4step_hllc_ko", dict(flux_scheme="hllc", limiter="koren", typeboundspeed="cmaxmean", time_stepper="fourstep")),
+    ("rk4_tvdlf_cada", dict(flux_scheme="tvdlf", limiter="cada3", typeboundspeed="cmaxmean", time_stepper="fourstep",
+                            time_integrator="rk4")),
 ])
 def test_kelvin_helmholtz_2d_amr_golden_log_gpu(oracle_lib, name, kw):
     kw = dict(kw, courantpar=0.9, slowsteps=10)
