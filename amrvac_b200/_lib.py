@@ -86,7 +86,7 @@ SIGNATURES = [
     ("amrvac_gpu_amr_regrid", _i, [_vp, _i, _ip, _ip]),
     ("amrvac_gpu_amr_resettree", _i, [_vp, _dp, _ip, _i, _dp, _dp, _dp, _ip]),
     ("amrvac_gpu_amr_leaves", _i, [_vp, _ip]),
-    ("amrvac_amr_plan", _i, [_i, _ip, _i, _i, _ip, _P(ctypes.c_ubyte), _P(ctypes.c_ubyte), _i, _ip, _ip, _ip]),
+    ("amrvac_amr_plan", _i, [_i, _ip, _ip, _i, _i, _ip, _P(ctypes.c_ubyte), _P(ctypes.c_ubyte), _i, _ip, _ip, _ip]),
     ("amrvac_gpu_amr_kernel_ms", _i, [_vp, _i, _dp, _dp]),
     ("amrvac_gpu_upload", _i, [_vp, _i, _i, _i, _dp]),
     ("amrvac_gpu_download", _i, [_vp, _i, _i, _i, _dp]),

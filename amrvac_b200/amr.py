@@ -32,10 +32,11 @@ import numpy as np
 
 
 class Tree:
-    def __init__(self, ndim, nbase, max_level, leaves=None):
+    def __init__(self, ndim, nbase, max_level, leaves=None, periodic=None):
         self.nd = int(ndim)
         self.nbase = [int(n) for n in list(nbase)[:self.nd]] + [1] * (3 - self.nd)
         self.max_level = int(max_level)
+        self.periodic = [True] * self.nd if periodic is None else [bool(p) for p in periodic][:self.nd]
         if leaves is None:
             leaves = [(1,) + ig for ig in itertools.product(*[range(n) for n in self.nbase[:self.nd]])]
         self.leaves = [self._key(t) for t in leaves]
@@ -55,7 +56,18 @@ class Tree:
                 self.refined.add((L2,) + tuple(i >> (L - L2) for i in ig))
 
     def _wrap(self, L, ig):
-        return tuple(ig[d] % (self.nbase[d] << (L - 1)) if d < self.nd else 0 for d in range(3))
+        """ig inside the domain (wrapped across periodic sides), or None
+        across a physical boundary."""
+        out = []
+        for d in range(3):
+            if d >= self.nd:
+                out.append(0)
+                continue
+            n = self.nbase[d] << (L - 1)
+            if not (0 <= ig[d] < n) and not self.periodic[d]:
+                return None
+            out.append(ig[d] % n)
+        return tuple(out)
 
     def _dirs(self):
         return [dd + (0,) * (3 - self.nd) for dd in itertools.product((-1, 0, 1), repeat=self.nd) if any(dd)]
@@ -91,9 +103,9 @@ class Tree:
                 for inp in itertools.product(*rng):
                     if not any(inp):
                         continue
-                    p = (L - 1,) + self._wrap(L - 1, tuple(pg[d] + inp[d] for d in range(3)))
-                    if p in self.set:
-                        ref.add(p)
+                    w = self._wrap(L - 1, tuple(pg[d] + inp[d] for d in range(3)))
+                    if w is not None and (L - 1,) + w in self.set:
+                        ref.add((L - 1,) + w)
         coa -= ref
         # proper_nesting, coarsening part: whole sibling groups whose outer
         # neighbours neither refine nor are refined further (unless those
@@ -118,7 +130,10 @@ class Tree:
                 for i in itertools.product(*rng):
                     if not any(i):
                         continue
-                    nb = (t[0],) + self._wrap(t[0], tuple(ig[d] + i[d] for d in range(3)))
+                    w = self._wrap(t[0], tuple(ig[d] + i[d] for d in range(3)))
+                    if w is None:  # a physical boundary: no neighbour
+                        continue
+                    nb = (t[0],) + w
                     if nb in self.set:
                         if nb in ref:
                             ok = False
@@ -152,7 +167,7 @@ class Tree:
             else:
                 new.append(t)
                 origin[t] = ("same", pos[t])
-        T = Tree(self.nd, self.nbase, self.max_level, new)
+        T = Tree(self.nd, self.nbase, self.max_level, new, self.periodic)
         return T, [origin[t] for t in T.leaves]
 
     def balanced(self):
@@ -162,6 +177,8 @@ class Tree:
             L, ig = t[0], t[1:]
             for dd in self._dirs():
                 g = self._wrap(L, tuple(ig[d] + dd[d] for d in range(3)))
+                if g is None:
+                    continue
                 # the leaf covering g at level L, or a refined region
                 if (L,) + g in self.set or (L,) + g in self.refined:
                     if (L,) + g in self.refined:
@@ -265,7 +282,7 @@ def regrid(ctx, tree, weight, logflag=None, refine_threshold=0.1, derefine_ratio
                                 derefine_ratio=derefine_ratio, amr_wavefilter=amr_wavefilter)
     if not changed:
         return tree
-    return Tree(tree.nd, tree.nbase[:tree.nd], tree.max_level, ctx.amr_leaves())
+    return Tree(tree.nd, tree.nbase[:tree.nd], tree.max_level, ctx.amr_leaves(), tree.periodic)
 
 
 def regrid_python(ctx, tree, weight, logflag=None, refine_threshold=0.1, derefine_ratio=0.125,
@@ -303,7 +320,9 @@ def plan_native(tree, refine, coarsen):
     out_o = np.zeros(9 * cap, np.int32)
     n = ctypes.c_int(0)
     ip, up = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_ubyte)
-    _lib.check(L.amrvac_amr_plan(nd, nb.ctypes.data_as(ip), tree.max_level, len(tree.leaves), lv.ctypes.data_as(ip),
+    per = np.ascontiguousarray([1 if p else 0 for p in tree.periodic], np.int32)
+    _lib.check(L.amrvac_amr_plan(nd, nb.ctypes.data_as(ip), per.ctypes.data_as(ip), tree.max_level,
+                                 len(tree.leaves), lv.ctypes.data_as(ip),
                                  r.ctypes.data_as(up), c.ctypes.data_as(up), cap, ctypes.byref(n),
                                  out_l.ctypes.data_as(ip), out_o.ctypes.data_as(ip)), "amrvac_amr_plan")
     k = n.value

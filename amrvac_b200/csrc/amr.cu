@@ -124,16 +124,31 @@ template <int NDIM>
 __device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int P2, int v) {
   const int P[3] = {P0, P1, P2};
   int jg[3] = {0, 0, 0}, loc[3] = {0, 0, 0};
+  uint32_t flip = 0;
 #pragma unroll
   for (int d = 0; d < NDIM; ++d) {
     const int n = A.nlev[L][d] * BN;
-    int p = P[d];  // within 4 cells of the block, n >= 16: one periodic wrap
-    p = p < 0 ? p + n : (p >= n ? p - n : p);
+    int p = P[d];  // within 4 cells of the block and n >= 16: one wrap or mirror
+    if (p < 0 || p >= n) {
+      // across the domain boundary: the boundary rule at this level, as the
+      // coarse neighbour's own physical ghost cells hold it (bc_phys)
+      const int side = p < 0 ? 0 : 1;
+      const int kind = A.bc_kind[2 * d + side];
+      if (kind == BCK_PERIODIC) {
+        p = side ? p - n : p + n;
+      } else if (kind == BCK_CONT) {
+        p = side ? n - 1 : 0;
+      } else {
+        p = side ? 2 * n - 1 - p : -1 - p;
+        flip ^= A.bc_flip[2 * d + side];
+      }
+    }
     jg[d] = p >> 4;
     loc[d] = p & (BN - 1);
   }
+  const double sg = ((flip >> v) & 1u) ? -1.0 : 1.0;
   const int o = A.owner[A.owner_off[L] + jg[0] + A.nlev[L][0] * (jg[1] + A.nlev[L][1] * jg[2])];
-  if (o >= 0) return A.u[cell_offset<NDIM>(o, A.nw, v, loc[0], loc[1], loc[2])];
+  if (o >= 0) return sg * A.u[cell_offset<NDIM>(o, A.nw, v, loc[0], loc[1], loc[2])];
   if (o == -2 && L < A.maxlevel) {
     int jf[3] = {0, 0, 0}, f[3] = {0, 0, 0};
 #pragma unroll
@@ -158,7 +173,7 @@ __device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int
         sum = sum + w[SZ + SY];
         sum = sum + w[SZ + SY + 1];
       }
-      return sum * (1.0 / double(1 << NDIM));
+      return sg * (sum * (1.0 / double(1 << NDIM)));
     }
   }
   atomicOr(A.status, ST_BOUNDS);  // hierarchy not 2:1 balanced here

@@ -43,6 +43,8 @@ struct AmrGhostArgs {
   int owner_off[AMR_MAX_LEVELS + 2];
   int nlev[AMR_MAX_LEVELS + 2][3];  // blocks per direction per level
   int maxlevel;
+  int bc_kind[6];           // BCK_* per side (periodic sides wrap)
+  uint32_t bc_flip[6];      // per side, bit v: variable v changes sign (asymm)
   uint32_t *status;
 };
 

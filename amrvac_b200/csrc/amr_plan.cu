@@ -6,7 +6,8 @@
 //      leaves above level 1;
 //   2. proper nesting, levels from fine to coarse: a leaf of level L flagged
 //      for refinement flags the leaves of level L-1 next to its parent on the
-//      parent's sides it touches (directions ic-2..ic-1 per dimension);
+//      parent's sides it touches (directions ic-2..ic-1 per dimension; none
+//      across a physical boundary);
 //   3. refinement wins over coarsening;
 //   4. sibling groups, finer levels first: a group coarsens only when all
 //      2^d siblings are flagged leaves and no neighbour across the siblings'
@@ -41,12 +42,16 @@ inline int d_or0(int nd, int d, const int *t) { return d < nd ? t[1 + d] : 0; }
 struct Plan {
   int nd, max_level;
   int nbase[3];
+  bool periodic[3];
   std::unordered_map<uint64_t, int> pos;     // leaf -> old index
   std::unordered_set<uint64_t> refined;      // non-leaf ancestors
   std::vector<Leaf> leaves;
 
+  // index i of level L in dimension d inside the domain, or -1 across a
+  // physical (non-periodic) boundary
   int wrap(int L, int d, int i) const {
     const int n = nbase[d] << (L - 1);
+    if ((i < 0 || i >= n) && !periodic[d]) return -1;
     return ((i % n) + n) % n;
   }
   bool is_leaf(const Leaf &t) const { return pos.count(key(t)) != 0; }
@@ -54,15 +59,18 @@ struct Plan {
 
 }  // namespace
 
-extern "C" int amrvac_amr_plan(int ndim, const int *nbase, int max_level, int nleaf, const int *leaf,
-                               const unsigned char *refine, const unsigned char *coarsen, int cap, int *nnew,
-                               int *leaf_new, int *op) {
+extern "C" int amrvac_amr_plan(int ndim, const int *nbase, const int *periodic, int max_level, int nleaf,
+                               const int *leaf, const unsigned char *refine, const unsigned char *coarsen, int cap,
+                               int *nnew, int *leaf_new, int *op) {
   if (ndim < 1 || ndim > 3 || !nbase || max_level < 1 || max_level > 20 || nleaf <= 0 || !leaf || !nnew)
     return AMRVAC_E_ARG;
   Plan P;
   P.nd = ndim;
   P.max_level = max_level;
-  for (int d = 0; d < 3; ++d) P.nbase[d] = d < ndim ? nbase[d] : 1;
+  for (int d = 0; d < 3; ++d) {
+    P.nbase[d] = d < ndim ? nbase[d] : 1;
+    P.periodic[d] = d >= ndim || !periodic || periodic[d];
+  }
   P.leaves.resize(nleaf);
   for (int b = 0; b < nleaf; ++b) {
     Leaf t = {leaf[4 * b], d_or0(ndim, 0, leaf + 4 * b), d_or0(ndim, 1, leaf + 4 * b), d_or0(ndim, 2, leaf + 4 * b)};
@@ -102,8 +110,12 @@ extern "C" int amrvac_amr_plan(int ndim, const int *nbase, int max_level, int nl
             if (!a && !bb && !c) continue;
             const int inp[3] = {c, bb, a};
             Leaf p = {L - 1, 0, 0, 0};
-            for (int d = 0; d < nd; ++d) p[1 + d] = P.wrap(L - 1, d, (t[1 + d] >> 1) + inp[d]);
-            if (P.is_leaf(p)) ref.insert(key(p));
+            bool inside = true;
+            for (int d = 0; d < nd; ++d) {
+              p[1 + d] = P.wrap(L - 1, d, (t[1 + d] >> 1) + inp[d]);
+              inside = inside && p[1 + d] >= 0;
+            }
+            if (inside && P.is_leaf(p)) ref.insert(key(p));
           }
     }
   }
@@ -147,7 +159,12 @@ extern "C" int amrvac_amr_plan(int ndim, const int *nbase, int max_level, int nl
             if (!a && !bb && !c) continue;
             const int inc[3] = {c, bb, a};
             Leaf nb = {t[0], 0, 0, 0};
-            for (int d = 0; d < nd; ++d) nb[1 + d] = P.wrap(t[0], d, t[1 + d] + inc[d]);
+            bool inside = true;
+            for (int d = 0; d < nd; ++d) {
+              nb[1 + d] = P.wrap(t[0], d, t[1 + d] + inc[d]);
+              inside = inside && nb[1 + d] >= 0;
+            }
+            if (!inside) continue;  // a physical boundary: no neighbour
             if (P.is_leaf(nb)) {
               if (ref.count(key(nb))) ok = false;
             } else if (P.refined.count(key(nb))) {

@@ -79,9 +79,10 @@ __global__ void pack_kernel(const double *__restrict__ pool, double *__restrict_
         const int G = BN + 4, gy2 = ndim >= 2 ? G : 1, gz2 = ndim >= 3 ? G : 1;
         const size_t gcell = e - (size_t)lb * per_block_g;
         const size_t gofs = ((size_t)(ndim >= 3 ? g[2] : 0) * gy2 + (ndim >= 2 ? g[1] : 0)) * G + g[0];
-        for (int v = 0; v < nw; ++v)
-          dst[((size_t)lb * nw + v) * per_block_g + gcell] =
-              gbuf[((size_t)(-2 - src) * nw + v) * (size_t)(G * gy2 * gz2) + gofs];
+        for (int v = 0; v < nw; ++v) {
+          const double x = gbuf[((size_t)(-2 - src) * nw + v) * (size_t)(G * gy2 * gz2) + gofs];
+          dst[((size_t)lb * nw + v) * per_block_g + gcell] = ((flip >> v) & 1u) ? -x : x;
+        }
         continue;
       }
       if (src < 0) {  // inconsistent neighbour table: never read out of bounds

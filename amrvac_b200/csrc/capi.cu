@@ -704,8 +704,12 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
   if (nleaf <= 0 || !leaf || !nbase || !xprobmin || !xprobmax) return fail(AMRVAC_E_ARG, "set_amr_grid: bad arguments");
   if (nd < 2) return fail(AMRVAC_E_UNSUPPORTED, "set_amr_grid: ndim 2 or 3");
   if (c->cfg.nghostcells != 2) return fail(AMRVAC_E_UNSUPPORTED, "set_amr_grid: nghostcells 2");
-  for (int s = 0; s < 2 * nd; ++s)
-    if (c->bc.kind[s] != BCK_PERIODIC) return fail(AMRVAC_E_UNSUPPORTED, "set_amr_grid: periodic boundaries only");
+  bool periodic[3] = {true, true, true};
+  for (int d = 0; d < nd; ++d) {
+    const bool p0 = c->bc.kind[2 * d] == BCK_PERIODIC, p1 = c->bc.kind[2 * d + 1] == BCK_PERIODIC;
+    if (p0 != p1) return fail(AMRVAC_E_ARG, "set_amr_grid: a dimension is periodic on one side only");
+    periodic[d] = p0;
+  }
   int maxlev = 1;
   for (int b = 0; b < nleaf; ++b) {
     const int L = leaf[4 * b];
@@ -794,7 +798,9 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
       for (int d = 0; d < 3; ++d) {
         if (d >= nd) { if (dd[d]) ok = false; continue; }
         const int nl = G.nlev[L][d];
-        jg[d] = ((ig[3 * b + d] + dd[d]) % nl + nl) % nl;
+        const int j = ig[3 * b + d] + dd[d];
+        if ((j < 0 || j >= nl) && !periodic[d]) ok = false;  // a physical boundary
+        jg[d] = (j % nl + nl) % nl;
       }
       if (!ok) continue;
       if (q == 13) { ntype[b * 27 + q] = AMR_SIBLING; continue; }
@@ -845,7 +851,9 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
       const int dd[3] = {q % 3 - 1, nd >= 2 ? (q / 3) % 3 - 1 : 0, nd >= 3 ? q / 9 - 1 : 0};
       const int q27 = (dd[0] + 1) + 3 * (dd[1] + 1) + 9 * (dd[2] + 1);
       const int t = ntype[b * 27 + q27];
-      if (t == AMR_SIBLING) {
+      if (t == AMR_BOUNDARY) {
+        nbr[(size_t)b * ndir3 + q] = -1;
+      } else if (t == AMR_SIBLING) {
         int jg[3] = {0, 0, 0};
         for (int d = 0; d < nd; ++d) {
           const int nl = G.nlev[lev[b]][d];
@@ -971,6 +979,10 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
   G.dxb = c->d_dx;
   G.owner = A->d_int + o_ow;
   G.maxlevel = maxlev;
+  for (int q = 0; q < 6; ++q) {
+    G.bc_kind[q] = c->bc.kind[q];
+    G.bc_flip[q] = c->bc.flip[q];
+  }
   G.status = c->d_status;
   A->G = G;
   std::memset(&A->F, 0, sizeof(A->F));
@@ -1015,7 +1027,9 @@ int amrvac_gpu_amr_resettree(amrvac_ctx *c, const double *weight, const int *log
   const int cap = nb * (1 << nd);
   std::vector<int> leaf_new(4 * (size_t)cap), op(9 * (size_t)cap);
   int nnew = 0;
-  if (int r = amrvac_amr_plan(nd, c->amr->nbase, refine_max_level, nb, old_leaf.data(), ref.data(), coa.data(), cap,
+  int periodic[3] = {1, 1, 1};
+  for (int d = 0; d < nd; ++d) periodic[d] = c->bc.kind[2 * d] == BCK_PERIODIC;
+  if (int r = amrvac_amr_plan(nd, c->amr->nbase, periodic, refine_max_level, nb, old_leaf.data(), ref.data(), coa.data(), cap,
                               &nnew, leaf_new.data(), op.data()))
     return fail(r, "amr_resettree: tree decision failed");
   leaf_new.resize(4 * (size_t)nnew);

@@ -162,7 +162,10 @@ __device__ __forceinline__ uint32_t load_prim(const StageArgs &A, int b, int i, 
     }
   } else {  // level jump: this block's ghost buffer
 #pragma unroll
-    for (int v = 0; v < V::NW; ++v) w[v] = __ldg(A.gbuf + ghost_offset<NDIM>(-2 - blk, V::NW, v, i, j, k));
+    for (int v = 0; v < V::NW; ++v) {
+      const double x = __ldg(A.gbuf + ghost_offset<NDIM>(-2 - blk, V::NW, v, i, j, k));
+      w[v] = ((flip >> v) & 1u) ? -x : x;
+    }
   }
   uint32_t st = 0;
   if (A.P.fix_small_values) {

@@ -150,8 +150,9 @@ int amrvac_gpu_nblocks(const amrvac_ctx *ctx);
 /* Static multi-level grid (replaces the forest and neighbour search of
  * src/amr/mod_forest.t and src/amr/mod_amr_neighbors.t for a fixed tree):
  * leaf[4*b] = level (1-based), ig0, ig1, ig2 (block index at that level);
- * nbase root blocks per direction over [xprobmin, xprobmax]; periodic
- * boundaries, ndim 2 or 3, nghostcells 2, 2:1 balanced across faces, edges
+ * nbase root blocks per direction over [xprobmin, xprobmax]; the boundary
+ * kinds of cfg->typeboundary (a dimension periodic on both sides or
+ * neither), ndim 2 or 3, nghostcells 2, 2:1 balanced across faces, edges
  * and corners.  Blocks are numbered in the order given.  Afterwards every
  * stage fills the level-jump ghost cells as the reference's multi-level getbc
  * does (restriction, and prolongation by interpolation_linear,
@@ -181,14 +182,15 @@ int amrvac_gpu_amr_resettree(amrvac_ctx *ctx, const double *weight, const int *l
  * leaf is not NULL; returns their number (AMRVAC_E_STATE without a grid). */
 int amrvac_gpu_amr_leaves(const amrvac_ctx *ctx, int *leaf);
 /* The tree decision of amr_coarsen_refine with proper_nesting
- * (src/amr/mod_coarsen_refine.t:20-319), host only: from the leaves and the
+ * (src/amr/mod_coarsen_refine.t:20-319), host only: from the leaves (on a
+ * domain periodic in the dimensions flagged in periodic) and the
  * per-leaf refine / coarsen flags, the new leaves (sorted by level, ig0, ig1,
  * ig2) and their ops for amrvac_gpu_amr_regrid.  cap = capacity of leaf_new
  * (4 ints per leaf) and op (9 ints per leaf) in leaves; *nnew is set even
  * when it exceeds cap (then AMRVAC_E_ARG). */
-int amrvac_amr_plan(int ndim, const int *nbase, int max_level, int nleaf, const int *leaf,
-                    const unsigned char *refine, const unsigned char *coarsen, int cap, int *nnew, int *leaf_new,
-                    int *op);
+int amrvac_amr_plan(int ndim, const int *nbase, const int *periodic /* [ndim], NULL: all periodic */,
+                    int max_level, int nleaf, const int *leaf, const unsigned char *refine,
+                    const unsigned char *coarsen, int cap, int *nnew, int *leaf_new, int *op);
 /* Blocks next to a level jump (0 on a single-level grid). */
 int amrvac_gpu_amr_slots(const amrvac_ctx *ctx);
 /* Average device time of the level-jump ghost pass (register 0) and of the

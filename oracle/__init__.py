@@ -95,7 +95,7 @@ def lib():
         L.orc_count_flops_getdt.argtypes = [cp, dp, dp]
         vp = ctypes.c_void_p
         L.orc_amr_create.restype = vp
-        L.orc_amr_create.argtypes = [cp, ip, dp, dp, ctypes.c_int, ip]
+        L.orc_amr_create.argtypes = [cp, ip, dp, dp, ctypes.c_int, ip, ip]
         L.orc_amr_destroy.argtypes = [vp]
         L.orc_amr_neighbors.argtypes = [vp, ip, ip, ip]
         L.orc_amr_set_block.argtypes = [vp, ctypes.c_int, dp]
@@ -332,14 +332,17 @@ class AmrGrid:
     """Static multi-level grid of the oracle: leaves [(level, ig0, ig1, ig2)],
     periodic boundaries, the reference's multi-level getbc and flux fix."""
 
-    def __init__(self, c: OrcCfg, nbase, xprobmin, xprobmax, leaves):
+    def __init__(self, c: OrcCfg, nbase, xprobmin, xprobmax, leaves, bc=None):
         self.c = c
         nd = c.ndim
         nb = np.array(list(nbase) + [1] * (3 - nd), np.int32)
         xmn = np.array(list(xprobmin) + [0.0] * (3 - nd), np.float64)
         xmx = np.array(list(xprobmax) + [1.0] * (3 - nd), np.float64)
         lv = np.ascontiguousarray(np.array([list(t) + [0] * (4 - len(t)) for t in leaves], np.int32).reshape(-1))
-        self.h = lib().orc_amr_create(ctypes.byref(c), _ip(nb), _dp(xmn), _dp(xmx), len(leaves), _ip(lv))
+        bc = ["periodic"] * (2 * nd) if bc is None else list(bc)
+        self.bca = np.array([BC[b] if isinstance(b, str) else b for b in bc] + [0] * (6 - len(bc)), np.int32)
+        self.h = lib().orc_amr_create(ctypes.byref(c), _ip(nb), _dp(xmn), _dp(xmx), len(leaves), _ip(lv),
+                                      _ip(self.bca))
         self.nblocks = len(leaves)
         self.shape = block_shape(c)
 
@@ -388,6 +391,7 @@ class AmrGrid:
         op = np.ascontiguousarray(np.asarray(ops, np.int32).reshape(-1))
         new = AmrGrid.__new__(AmrGrid)
         new.c = self.c
+        new.bca = self.bca
         new.h = lib().orc_amr_remap(self.h, len(leaves), _ip(lv), _ip(op))
         new.nblocks = len(leaves)
         new.shape = self.shape

@@ -1356,6 +1356,9 @@ void orc_srl_maps(int nghost, int block_nx, int *s_min, int *s_max, int *r_min, 
 }
 
 extern "C++" {
+template <class R, class NBT>
+static void bc_phys_block(const State &s, const int *bcs, R *w, NBT nbt);
+
 template <class R>
 static void getbc_reg(const Grid &G, std::vector<R> &reg) {
   const State &s = G.s;
@@ -1394,12 +1397,21 @@ static void getbc_reg(const Grid &G, std::vector<R> &reg) {
                       src[g.idx(S.lo[0] + i, S.lo[1] + j, S.lo[2] + k) + g.cells * (size_t)iw];
         }
   }
-  // physical boundaries: fill_boundary_after_gc (src/mod_ghostcells_update.t:580-615)
-  // with bc_phys cont/symm/asymm (src/mod_boundary_conditions.t:12-265)
+  for (int ib = 0; ib < G.nblocks; ++ib)
+    bc_phys_block(s, G.bc, &reg[G.bsize * ib],
+                  [&](int di, int dj, int dk) { return G.nbr[(size_t)ib * 27 + dir_index(di, dj, dk)] < 0; });
+}
+
+// physical boundaries of one ghosted block: fill_boundary_after_gc
+// (src/mod_ghostcells_update.t:580-615) with bc_phys cont/symm/asymm
+// (src/mod_boundary_conditions.t:12-265); nbt(dir) is true for a direction
+// that leaves the domain.
+template <class R, class NBT>
+static void bc_phys_block(const State &s, const int *bcs, R *w, NBT nbt) {
+  const Geo &g = s.g;
+  const int ndim = s.c.ndim, nw = s.x.nw;
   const int ng = s.c.nghost;
-  for (int ib = 0; ib < G.nblocks; ++ib) {
-    R *w = &reg[G.bsize * ib];
-    auto nbt = [&](int di, int dj, int dk) { return G.nbr[(size_t)ib * 27 + dir_index(di, dj, dk)] < 0; };
+  {
     for (int idims = 0; idims < ndim; ++idims) {
       int kmin[3] = {0, 0, 0}, kmax[3] = {0, 0, 0};
       if (ndim >= 2) { kmin[1] = (idims < 1 && nbt(0, -1, 0)) ? 1 : 0; kmax[1] = (idims < 1 && nbt(0, 1, 0)) ? 1 : 0; }
@@ -1412,7 +1424,7 @@ static void getbc_reg(const Grid &G, std::vector<R> &reg) {
         int dd[3] = {0, 0, 0};
         dd[idims] = iside == 0 ? -1 : 1;
         if (!nbt(dd[0], dd[1], dd[2])) continue;
-        int type = G.bc[2 * idims + iside];
+        int type = bcs[2 * idims + iside];
         Box O = B;
         if (iside == 1) O.lo[idims] = B.hi[idims] + 1 - ng;
         else O.hi[idims] = B.lo[idims] - 1 + ng;
@@ -1941,6 +1953,7 @@ struct AmrGrid {
   int ndim, nb;
   int nbase[3];
   double xmin[3], xmax[3];
+  int bc[6];                                  // ORC_BC_* per side
   std::vector<int> level, ig;                 // ig[3*b]
   std::vector<int> ntype, nid;                // [b*27]
   std::vector<int> child;                     // [(b*27+q)*8 + cbits]
@@ -2073,6 +2086,16 @@ void amr_getbc(AmrGrid &G, std::vector<double> &reg) {
         copy_box(gc, &G.psc[G.csize * b], lo_s, g, &reg[G.bsize * nbk], lo_r, ext, nw);
       }
     }
+  // physical boundaries of every block before the coarse values are sent:
+  // the coarse neighbours' ghost cells across the domain boundary are then
+  // those of the current data (the reference leaves whatever the register
+  // held from its previous fill there)
+  auto phys_all = [&]() {
+    for (int b = 0; b < G.nb; ++b)
+      bc_phys_block(G.s, G.bc, &reg[G.bsize * b],
+                    [&](int di, int dj, int dk) { return G.ntype[b * 27 + dir_index(di, dj, dk)] == NT_BOUNDARY; });
+  };
+  phys_all();
   // coarse values into the finer neighbours' psc (bc_fill_prolong)
   for (int b = 0; b < G.nb; ++b)
     for (int q = 0; q < 27; ++q) {
@@ -2156,6 +2179,7 @@ void amr_getbc(AmrGrid &G, std::vector<double> &reg) {
             }
           }
     }
+  phys_all();  // fill_boundary_after_gc
 }
 
 // store_flux (src/mod_fix_conserve.t:597-648) for one block from its scaled face fluxes.
@@ -2301,8 +2325,9 @@ int amr_advect1(AmrGrid &G, int ra, int rb, double qdt, double dtfactor, double 
 extern "C" {
 
 orc_amr *orc_amr_create(const orc_cfg *cfg, const int *nbase, const double *xprobmin, const double *xprobmax,
-                        int nleaf, const int *leaf /* [nleaf][4]: level, ig0, ig1, ig2 */) {
+                        int nleaf, const int *leaf /* [nleaf][4]: level, ig0, ig1, ig2 */, const int *bc) {
   AmrGrid *G = new AmrGrid();
+  for (int q = 0; q < 6; ++q) G->bc[q] = (bc && q < 2 * cfg->ndim) ? bc[q] : ORC_BC_PERIODIC;
   G->s = make_state(*cfg);
   orc_cfg c8 = *cfg;
   for (int d = 0; d < 3; ++d) c8.block_nx[d] = d < cfg->ndim ? 8 : 1;
@@ -2336,12 +2361,15 @@ orc_amr *orc_amr_create(const orc_cfg *cfg, const int *nbase, const double *xpro
       int dd[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
       bool ok = true;
       int jg[3] = {0, 0, 0};
+      bool outside = false;
       for (int d = 0; d < 3; ++d) {
         if (d >= nd) { if (dd[d]) ok = false; continue; }
         const int nl = G->nbase[d] << (l - 1);
-        jg[d] = ((G->ig[3 * b + d] + dd[d]) % nl + nl) % nl;  // periodic
+        const int j = G->ig[3 * b + d] + dd[d];
+        if ((j < 0 || j >= nl) && G->bc[2 * d + (j < 0 ? 0 : 1)] != ORC_BC_PERIODIC) outside = true;
+        jg[d] = (j % nl + nl) % nl;
       }
-      if (!ok) continue;
+      if (!ok || outside) continue;  // outside: a physical boundary
       if (q == 13) { G->ntype[b * 27 + q] = NT_SIBLING; G->nid[b * 27 + q] = b; continue; }
       int s2 = find(l, jg);
       if (s2 >= 0) { G->ntype[b * 27 + q] = NT_SIBLING; G->nid[b * 27 + q] = s2; continue; }
@@ -2453,7 +2481,7 @@ int orc_amr_advance(orc_amr *a, double dt, double cmax_global, int nthreads) {
 // the old grid's ghosted register 0.
 orc_amr *orc_amr_remap(const orc_amr *old, int nleaf, const int *leaf, const int *op) {
   const AmrGrid *O = reinterpret_cast<const AmrGrid *>(old);
-  orc_amr *res = orc_amr_create(&O->s.c, O->nbase, O->xmin, O->xmax, nleaf, leaf);
+  orc_amr *res = orc_amr_create(&O->s.c, O->nbase, O->xmin, O->xmax, nleaf, leaf, O->bc);
   AmrGrid *N = reinterpret_cast<AmrGrid *>(res);
   const Geo &g = O->s.g;
   const int nd = O->ndim, nw = O->s.x.nw;

@@ -180,9 +180,11 @@ void orc_lohner_block(const orc_cfg *cfg, const double *w, const double *weight,
 /* --- multi-level (AMR) grid: a static 2:1-balanced hierarchy of leaves --- */
 typedef struct orc_amr orc_amr;
 /* leaf[4*b] = level (1-based), leaf[4*b+1..3] = block index at that level
- * (0-based); nbase: level-1 blocks per direction; periodic boundaries. */
+ * (0-based); nbase: level-1 blocks per direction; bc per side (one kind for
+ * all variables), physical ghosts filled with current data. */
 orc_amr *orc_amr_create(const orc_cfg *cfg, const int *nbase, const double *xprobmin,
-                        const double *xprobmax, int nleaf, const int *leaf);
+                        const double *xprobmax, int nleaf, const int *leaf,
+                        const int *bc /* [6] ORC_BC_* per side, NULL: periodic */);
 void orc_amr_destroy(orc_amr *a);
 /* ntype[b*27+q]: 0 boundary, 1 coarse, 2 sibling, 3 fine; nid: the sibling or
  * coarse block; child[(b*27+q)*8 + cbits]: fine neighbours by child position. */

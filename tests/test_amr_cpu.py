@@ -181,3 +181,34 @@ def test_regrid_remap_is_exact_and_conservative(oracle_lib):
     b3 = T3.leaves.index((2, 3, 3, 0))
     b0 = T.leaves.index((2, 3, 3, 0))
     assert np.allclose(g3.get_block(b3)[sl], g.get_block(b0)[sl], rtol=1e-15, atol=0)
+
+
+@pytest.mark.parametrize("bc", ["cont", "symm"])
+def test_refined_everywhere_with_physical_boundaries_is_the_uniform_grid(oracle_lib, bc):
+    """Physical boundaries on a multi-level grid (fill_boundary_after_gc per
+    block): a tree refined everywhere reproduces the uniform finer grid with
+    the same boundaries, bit for bit."""
+    O = oracle_lib
+    nd = 2
+    leaves = A.build_leaves(nd, [2, 2], 2, lambda c, lv: True)
+    c = _cfg(O, nd)
+    bcs = [bc] * 4
+    g = O.AmrGrid(c, [2, 2], [0.0, 0.0], [1.0, 1.0], leaves, bc=bcs)
+    blocks = A.fill_blocks(leaves, nd, [2, 2], _periodic(nd), "hd", nd, 1.4)
+    u = O.Grid(c, [64, 64], [0.0, 0.0], [1.0, 1.0], bcs)
+    order = {}
+    for b, l in enumerate(leaves):
+        g.set_block(b, blocks[b])
+        order[b] = l[1] + 4 * l[2]
+        u.set_block(order[b], blocks[b])
+    g.getbc()
+    u.getbc()
+    for b in range(len(leaves)):
+        assert np.array_equal(g.get_block(b), u.get_block(order[b]))
+    for _ in range(3):
+        dt, _ = u.getdt()
+        assert g.getdt()[0] == dt
+        g.advance(dt)
+        u.advance(dt)
+    for b in range(len(leaves)):
+        assert np.array_equal(g.get_block(b), u.get_block(order[b]))

@@ -105,13 +105,15 @@ def test_initial_hierarchy_reaches_the_finest_level():
     assert blocks.shape[0] == len(T.leaves)
 
 
-@pytest.mark.parametrize("nd,nbase", [(2, [4, 4]), (3, [2, 2, 2]), (2, [3, 2])])
-def test_native_plan_matches_python(nd, nbase):
+@pytest.mark.parametrize("nd,nbase,periodic", [(2, [4, 4], None), (3, [2, 2, 2], None), (2, [3, 2], None),
+                                                (2, [4, 4], [False, False]), (3, [2, 2, 2], [True, False, False])])
+def test_native_plan_matches_python(nd, nbase, periodic):
     """The library's C++ tree decision (amrvac_amr_plan) equals Tree.regrid:
-    same leaves in the same order, same ops, over random regrid sequences."""
+    same leaves in the same order, same ops, over random regrid sequences,
+    on periodic domains and with physical boundaries."""
     from amrvac_b200.amr import ops, plan_native
-    rng = np.random.default_rng(7 + nd)
-    T = Tree(nd, nbase, 4)
+    rng = np.random.default_rng(7 + nd + (0 if periodic is None else 3))
+    T = Tree(nd, nbase, 4, periodic=periodic)
     for it in range(10):
         ref = rng.random(len(T.leaves)) < 0.2
         coa = rng.random(len(T.leaves)) < 0.5

@@ -72,23 +72,30 @@ CASES = [
     ("hd2_hllc_minmod_pc", 2, 3, dict(physics="hd", flux_scheme="hllc", limiter="minmod", time_stepper="twostep")),
     ("mhd2_hlld_glm_ssprk2", 2, 2, dict(physics="mhd", flux_scheme="hlld", limiter="vanleer", typedivbfix="glm",
                                         time_stepper="twostep", time_integrator="ssprk2")),
+    ("hd2_hllc_cont", 2, 3, dict(physics="hd", flux_scheme="hllc", limiter="vanleer", bc=["cont"] * 4)),
+    ("hd2_hll_symm_x_periodic_y", 2, 3, dict(physics="hd", flux_scheme="hll", limiter="minmod",
+                                             bc=["symm", "symm", "periodic", "periodic"])),
+    ("mhd2_hlld_cont", 2, 2, dict(physics="mhd", flux_scheme="hlld", limiter="cada3", typedivbfix="glm",
+                                  bc=["cont"] * 4)),
+    ("hd3_hllc_cont", 3, 2, dict(physics="hd", flux_scheme="hllc", limiter="vanleer", bc=["cont"] * 6)),
 ]
 
 
 def _setup(O, nd, levels, kw):
     from amrvac_b200 import Context, make_cfg
-    leaves = _leaves(nd, levels)
+    leaves = _bleaves(nd, levels) if "bc" in kw else _leaves(nd, levels)
     nb = _nbase(nd)
     physics = kw["physics"]
     base = dict(ndim=nd, gamma=5.0 / 3.0 if physics == "mhd" else 1.4, courantpar=0.6)
     base.update(kw)
+    bc = base.pop("bc", ["periodic"] * (2 * nd))
     gk = dict(base)
     ok = dict(base)
     if "typedivbfix" in ok:
         ok["divb"] = ok.pop("typedivbfix")
     ocfg = O.make_cfg(**ok)
-    gcfg = make_cfg(typeboundary=["periodic"] * (2 * nd), **gk)
-    og = O.AmrGrid(ocfg, nb, [0.0] * nd, [1.0] * nd, leaves)
+    gcfg = make_cfg(typeboundary=bc, **gk)
+    og = O.AmrGrid(ocfg, nb, [0.0] * nd, [1.0] * nd, leaves, bc=bc)
     ndir = nd
     blocks = A.fill_blocks(leaves, nd, nb, _field(nd, physics, kw.get("typedivbfix") == "glm"), physics, ndir,
                            base["gamma"])
@@ -99,6 +106,14 @@ def _setup(O, nd, levels, kw):
     ctx.set_amr_grid(leaves, nb, [0.0] * nd, [1.0] * nd)
     ctx.upload(blocks)
     return leaves, nb, og, ctx
+
+
+def _bleaves(nd, levels):
+    """A hierarchy whose finest blocks touch the domain boundary (refined
+    around a point near x = 0)."""
+    def ref(c, lv):
+        return np.linalg.norm(c - np.array([0.05] + [0.5] * (nd - 1))) < (0.3 if lv == 1 else 0.15)
+    return A.build_leaves(nd, _nbase(nd), levels, ref)
 
 
 def _maxrel(a, b):

@@ -87,15 +87,17 @@ def _amr_log_row(blocks, leaves, nbase, t, nw):
     return np.concatenate([[t], s1 / vol, s2 / vol])
 
 
-def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsave=1.0e-3, levels=3):
-    """The reference's time loop on a periodic 2-D multi-level grid: settree,
-    then setdt + advance + resettree every step, a log row at every dtsave."""
+def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsave=1.0e-3, levels=3, xmax=1.0,
+                    bc="periodic"):
+    """The reference's time loop on a 2-D multi-level grid over [0, xmax]^2:
+    settree, then setdt + advance + resettree every step, a log row at every
+    dtsave."""
     from tests import _amr as A
     from amrvac_b200 import Context, make_cfg
     from amrvac_b200.amr import Tree, initial_hierarchy, lohner_flags
     nw = len(weight)
-    xmin, xmax = [0.0, 0.0], [1.0, 1.0]
-    cfg = make_cfg(physics=physics, ndim=2, ndir=2, typeboundary=["periodic"] * 4, **kw)
+    xmin, xmax = [0.0, 0.0], [xmax, xmax]
+    cfg = make_cfg(physics=physics, ndim=2, ndir=2, typeboundary=[bc] * 4, **kw)
     ctx = Context(cfg)
     lkw = dict(refine_threshold=threshold, derefine_ratio=0.125, amr_wavefilter=1.0e-2)
 
@@ -105,7 +107,7 @@ def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsav
     def err(tree, blocks):
         r, c, _ = lohner_flags(ctx, tree, blocks, xmin, xmax, weight, **lkw)
         return r, c
-    tree, blocks = initial_hierarchy(Tree(2, nb, levels), init, err)
+    tree, blocks = initial_hierarchy(Tree(2, nb, levels, periodic=[bc == "periodic"] * 2), init, err)
     ctx.set_amr_grid(tree.leaves, nb, xmin, xmax)
     ctx.upload(blocks)
     ctx.set_time(0.0, time_max, dtsave)
@@ -182,6 +184,38 @@ def test_kelvin_helmholtz_2d_amr_golden_log_gpu(oracle_lib, name, kw):
     kw = dict(kw, courantpar=0.9, slowsteps=10)
     rows = _run_amr_golden("hd", [2, 2], _kh2d_prim, np.array([1.0, 0.0, 0.0, 0.0]), 0.1, kw, time_max=0.05)
     gold = oracle_lib.read_log(os.path.join(GOLD, f"kh_2d_{name}.log"))
+    assert rows.shape == gold.shape, (rows.shape, gold.shape)
+    bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
+    assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
+        np.argwhere(bad)[:10].tolist(), rows[bad][:10].tolist(), gold[bad][:10].tolist())
+
+
+# Blast wave 2-D (tests/hd/blast_wave_Cartesian_2D, reference): [0,2]^2,
+# 32^2 level-1 cells in 16^2 blocks, cont boundaries, refine_max_level 3 with
+# w_refine_weight(1) = w_refine_weight(4) = 0.5, p = 100 for r < 0.2 around
+# the centre, rho = 1, p = 1, v = 0; log every 1e-3 to t = 0.05.
+
+
+def _bw2d_prim(X, Y, Z):
+    out = np.zeros((4,) + X.shape)
+    out[0] = 1.0
+    out[3] = np.where((X - 1.0) ** 2 + (Y - 1.0) ** 2 < 0.2 ** 2, 100.0, 1.0)
+    return out
+
+
+@pytest.mark.parametrize("name,kw", [
+    ("3step_hll_cada", dict(flux_scheme="hll", limiter="cada3", typeboundspeed="cmaxmean")),
+    ("4step_hll_mc", dict(flux_scheme="hll", limiter="woodward", typeboundspeed="cmaxmean", time_stepper="fourstep",
+                          time_integrator="rk4")),
+    ("4step_hllc_ko", dict(flux_scheme="hllc", limiter="koren", typeboundspeed="cmaxmean", time_stepper="fourstep")),
+    ("rk4_tvdlf_cada", dict(flux_scheme="tvdlf", limiter="cada3", typeboundspeed="cmaxmean", time_stepper="fourstep",
+                            time_integrator="rk4")),
+])
+def test_blast_wave_2d_amr_golden_log_gpu(oracle_lib, name, kw):
+    kw = dict(kw, courantpar=0.9)
+    weight = np.array([0.5, 0.0, 0.0, 0.5])
+    rows = _run_amr_golden("hd", [2, 2], _bw2d_prim, weight, 0.1, kw, time_max=0.05, xmax=2.0, bc="cont")
+    gold = oracle_lib.read_log(os.path.join(GOLD, f"bw_2d_{name}.log"))
     assert rows.shape == gold.shape, (rows.shape, gold.shape)
     bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
     assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
