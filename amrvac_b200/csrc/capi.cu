@@ -133,6 +133,14 @@ struct AmrDev {
 
 namespace {
 
+// twostep Predictor_Corrector predicts with the MUSCL-Hancock scheme when the
+// flux scheme is tvdlf (typepred1 = fs_hancock, src/io/mod_input_output.t:
+// 787-797); the other schemes predict with their own finite_volume.
+bool uses_hancock(const amrvac_cfg &k) {
+  return k.time_stepper == AMRVAC_TS_TWOSTEP && k.time_integrator == AMRVAC_TI_DEFAULT &&
+         k.flux_scheme == AMRVAC_FS_TVDLF;
+}
+
 int check_ctx(amrvac_ctx *c, bool need_blocks) {
   if (!c) return fail(AMRVAC_E_ARG, "null context");
   if (need_blocks && c->nblocks == 0) return fail(AMRVAC_E_STATE, "no blocks set (amrvac_gpu_set_blocks)");
@@ -183,8 +191,11 @@ int launch_amr_ghost_pass(amrvac_ctx *c, int reg) {
 
 // fix: apply fix_conserve after the stage on a multi-level grid (the
 // reference's predictor step skips it: fix_conserve_at_step = .false.).
+// hancock: the MUSCL-Hancock predictor instead of finite_volume (no flux fix,
+// no block restore on a small-value crash).
 int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a, double b, double dtfactor,
-                 bool fix = true) {
+                 bool fix = true, bool hancock = false) {
+  if (hancock && !c->ks.hancock) return fail(AMRVAC_E_UNSUPPORTED, "no Hancock predictor for this configuration");
   if (c->amr)
     if (int r = launch_amr_ghost_pass(c, reg_ct)) return r;
   StageArgs A = stage_args(c, reg_ct, reg_new, reg_base, a, b, dtfactor);
@@ -192,11 +203,12 @@ int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a,
   int nctas;
   if (c->zchunk > 0) nctas = c->cfg.ndim == 3 ? c->nblocks * (16 / c->zchunk) : c->nblocks;
   else nctas = (int)std::min<long>(planes, c->wave_ctas);
-  if (c->P.fix_small_values && c->P.small_values_method == 0)
-    CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * c->nblocks, c->stream));
-  CK(c->ks.stage(A, nctas, c->stream));
+  const bool restore = !hancock && c->P.fix_small_values && c->P.small_values_method == 0;
+  if (restore) CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * c->nblocks, c->stream));
+  CK(hancock ? c->ks.hancock(A, nctas, c->stream) : c->ks.stage(A, nctas, c->stream));
   ++c->launches;
-  if (c->P.fix_small_values && c->P.small_values_method == 0) {
+  if (hancock) return 0;
+  if (restore) {
     CK(launch_restore_blocks(c->pool[reg_ct], c->pool[reg_new], c->d_block_status, c->nblocks,
                              c->per_block * c->nw, c->stream));
     ++c->launches;
@@ -277,8 +289,8 @@ int launch_rk(amrvac_ctx *c) {
     if (k.time_integrator == AMRVAC_TI_SSPRK2) {
       if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0))) return r;
       r = launch_stage(c, 1, 0, 0, 0.5, 0.5, 0.5);
-    } else {  // Predictor_Corrector (src/mod_advance.t:104-111)
-      if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 0.5, false))) return r;
+    } else {  // Predictor_Corrector (src/mod_advance.t:104-111), typepred1
+      if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 0.5, false, uses_hancock(k)))) return r;
       r = launch_stage(c, 1, 0, 0, 1.0, 0.0, 1.0);
     }
   } else if (k.time_stepper == AMRVAC_TS_FOURSTEP) {
@@ -374,9 +386,8 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
       !(k.time_stepper == AMRVAC_TS_FOURSTEP && k.time_integrator == AMRVAC_TI_RK4) &&
       !(k.time_stepper == AMRVAC_TS_TWOSTEP && k.time_integrator == AMRVAC_TI_SSPRK2))
     return fail(AMRVAC_E_UNSUPPORTED, "time_integrator not supported for this time_stepper");
-  if (k.time_stepper == AMRVAC_TS_TWOSTEP && k.time_integrator == AMRVAC_TI_DEFAULT && k.flux_scheme == AMRVAC_FS_TVDLF)
-    return fail(AMRVAC_E_UNSUPPORTED,
-                "twostep Predictor_Corrector with tvdlf needs the Hancock predictor (not built); use ssprk2");
+  if (uses_hancock(k) && k.precision == 1)
+    return fail(AMRVAC_E_UNSUPPORTED, "the Hancock predictor (twostep with tvdlf) is FP64 only");
   if ((k.time_stepper == AMRVAC_TS_THREESTEP || k.time_stepper == AMRVAC_TS_FOURSTEP) && k.ssprk_order != 2 &&
       k.ssprk_order != 3)
     return fail(AMRVAC_E_ARG, "ssprk_order must be 2 or 3");
@@ -1232,7 +1243,7 @@ int amrvac_gpu_run_timed(amrvac_ctx *c, int nsteps, double *total_ms, double *st
       CK(cudaEventRecord(ev[q++], c->stream));
     } else if (k.time_stepper == AMRVAC_TS_TWOSTEP) {
       const bool pc = k.time_integrator != AMRVAC_TI_SSPRK2;
-      r = pc ? launch_stage(c, 0, 1, 0, 0.0, 1.0, 0.5, false) : launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);
+      r = pc ? launch_stage(c, 0, 1, 0, 0.0, 1.0, 0.5, false, uses_hancock(k)) : launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);
       CK(cudaEventRecord(ev[q++], c->stream));
       if (!r) r = pc ? launch_stage(c, 1, 0, 0, 1.0, 0.0, 1.0) : launch_stage(c, 1, 0, 0, 0.5, 0.5, 0.5);
       CK(cudaEventRecord(ev[q++], c->stream));

@@ -169,6 +169,8 @@ struct KernelSet {
   cudaError_t (*prepare)() = nullptr;
   int (*ctas_per_sm)() = nullptr;
   cudaError_t (*stage)(const StageArgs &, int nctas, cudaStream_t) = nullptr;
+  // MUSCL-Hancock predictor of twostep Predictor_Corrector (tvdlf sets only)
+  cudaError_t (*hancock)(const StageArgs &, int nctas, cudaStream_t) = nullptr;
   cudaError_t (*getdt)(const GetdtArgs &, cudaStream_t) = nullptr;
   cudaError_t (*riemann_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
   cudaError_t (*flux_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
@@ -180,13 +182,29 @@ template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM = 0, int B
 struct Launch {
   using V = Vars<MHD, NDIR, GLM>;
   static constexpr size_t SMEM = Tile<TF, V::NW, NDIM>::BYTES;
+  // typepred1 = fs_hancock for tvdlf (src/io/mod_input_output.t:787-797)
+  static constexpr bool HAS_HANCOCK = SOLVER == SOLVER_TVDLF && sizeof(TF) == 8;
   static cudaError_t prepare() {
-    return cudaFuncSetAttribute(fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    cudaError_t e = cudaFuncSetAttribute(fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    if constexpr (HAS_HANCOCK) {
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER_HANCOCK, LIM, BS>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    }
+    return e;
   }
   static cudaError_t stage(const StageArgs &A, int nctas, cudaStream_t s) {
     fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
     return cudaGetLastError();
+  }
+  static cudaError_t hancock(const StageArgs &A, int nctas, cudaStream_t s) {
+    if constexpr (HAS_HANCOCK) {
+      fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER_HANCOCK, LIM, BS><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
   }
   static int ctas_per_sm() {
     int n = 0;
@@ -237,6 +255,7 @@ struct Launch {
     k.prepare = &prepare;
     k.ctas_per_sm = &ctas_per_sm;
     k.stage = &stage;
+    if (HAS_HANCOCK) k.hancock = &hancock;
     k.getdt = &getdt;
     k.riemann_points = &riemann_points;
     k.flux_points = &flux_points;

@@ -332,6 +332,52 @@ __device__ __noinline__ FaceFlux64<Vars<MHD, NDIR, GLM>::NW> face_retry_fp64(
   return r;
 }
 
+// MUSCL-Hancock predictor, one direction D (hancock, src/mod_finite_volume.t:
+// 56-101; reconstruct_LR default branch 1171-1222): from the primitives of
+// cells c-1, c, c+1 along D (shared-memory offsets base[o], strides strd[o]),
+// the cell's limited edge states — right edge wprim + ldw/2 (the left state of
+// the face above), left edge wprim - rdw/2 (the right state of the face
+// below) — the primitive small-value check on both, their conserved forms and
+// physical fluxes, and wnew += -qdt/dx (f(right edge) - f(left edge)).  No
+// Riemann solver and no GLM state modification.  D is a template parameter
+// so the accumulator index stays compile-time (registers, no local memory).
+template <bool MHD, int NDIR, bool GLM, int LIM, int D>
+__device__ __forceinline__ uint32_t hancock_dir(const double *smem, const int *base, const int *strd, double rd,
+                                                double sc, double cg, const PhysParams &P, double *acc) {
+  using V = Vars<MHD, NDIR, GLM>;
+  constexpr int NW = V::NW;
+  double wl[NW], wr[NW];
+#pragma unroll
+  for (int v = 0; v < NW; ++v) {
+    const int ov = orig_index<MHD, NDIR, D>(v);
+    const double q0 = smem[base[0] + ov * strd[0]], q1 = smem[base[1] + ov * strd[1]],
+                 q2 = smem[base[2] + ov * strd[2]];
+    const double dm = q1 - q0, dp = q2 - q1;
+    wr[v] = q1 + 0.5 * limited_slope<double, true, LIM>(P.limiter, dp, dm, rd);
+    wl[v] = q1 - 0.5 * limited_slope<double, false, LIM>(P.limiter, dp, dm, rd);
+  }
+  uint32_t st = 0;
+  if (P.fix_small_values) {
+    const bool fr = small_values<double, MHD, NDIR, GLM>(wr, true, P);
+    const bool fl = small_values<double, MHD, NDIR, GLM>(wl, true, P);
+    if ((fr || fl) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
+  }
+  double cl[NW], cr[NW];
+#pragma unroll
+  for (int v = 0; v < NW; ++v) { cl[v] = wl[v]; cr[v] = wr[v]; }
+  to_conserved<double, MHD, NDIR, GLM>(cl, P);
+  to_conserved<double, MHD, NDIR, GLM>(cr, P);
+  double fl[NW], fr[NW];
+  phys_flux<double, MHD, NDIR, GLM, 0>(cl, wl, cg, fl);
+  phys_flux<double, MHD, NDIR, GLM, 0>(cr, wr, cg, fr);
+#pragma unroll
+  for (int v = 0; v < NW; ++v) {
+    const int ov = orig_index<MHD, NDIR, D>(v);
+    acc[ov] = acc[ov] + sc * (fr[v] - fl[v]);
+  }
+  return st;
+}
+
 template <class TF, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS>
 __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_MINB : AMRVAC_STAGE_MINB_MIXED)
     fv_stage_kernel(const StageArgs A) {
@@ -450,6 +496,28 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
       }
     }
     __syncthreads();
+    if constexpr (SOLVER == SOLVER_HANCOCK) {
+      // ---- Hancock predictor: each cell thread, all directions, from the
+      // staged primitives (cells c-1, c, c+1; z from ring slots k-1..k+1)
+      static_assert(sizeof(TF) == 8, "the Hancock predictor is FP64 only");
+      if (update && cell_thread) {
+        int base[3], strd[3];
+#pragma unroll
+        for (int o = 0; o < 3; ++o) tv.addr(slot, ci + o - 1, cj, base[o], strd[o]);
+        stb |= hancock_dir<MHD, NDIR, GLM, LIM, 0>(smem, base, strd, rdel[0], dxinv[0], cg, P, acc);
+#pragma unroll
+        for (int o = 0; o < 3; ++o) tv.addr(slot, ci, cj + o - 1, base[o], strd[o]);
+        stb |= hancock_dir<MHD, NDIR, GLM, LIM, 1>(smem, base, strd, rdel[1], dxinv[1], cg, P, acc);
+        if constexpr (NDIM == 3) {
+#pragma unroll
+          for (int o = 0; o < 3; ++o) {
+            base[o] = ((k + o - 1) & 3) * NW * (BN * BN) + cj * BN + ci;
+            strd[o] = BN * BN;
+          }
+          stb |= hancock_dir<MHD, NDIR, GLM, LIM, 2>(smem, base, strd, rdel[2], dxinv[2], cg, P, acc);
+        }
+      }
+    } else {
     // ---- face phases x, y (plane k) and z (face k+1/2 of every column); one
     // copy of the face code serves all three through the state rotation.
     const int dlo = update ? 0 : (NDIM == 3 && k == k0 - 1 ? 2 : NDIM);
@@ -572,9 +640,11 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
       }
       __syncthreads();
     }
+    }  // face phases
     if (update && cell_thread) {
-      // ---- small values on wnew (src/mod_finite_volume.t:326-333)
-      if (P.fix_small_values) {
+      // ---- small values on wnew (src/mod_finite_volume.t:326-333; the
+      // Hancock predictor checks after the sources instead)
+      if (SOLVER != SOLVER_HANCOCK && P.fix_small_values) {
         if (small_values<double, MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) stb |= ST_SMALL_VALUE;
       }
       // ---- unsplit divB sources (addsource2 -> mhd_add_source)
@@ -640,6 +710,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
           }
         }
       }
+      // ---- 'exit hancock' small-value check (src/mod_finite_volume.t:106-109)
+      if (SOLVER == SOLVER_HANCOCK && P.fix_small_values) {
+        if (small_values<double, MHD, NDIR, GLM>(acc, false, P) && P.small_values_method != 1) stb |= ST_SMALL_VALUE;
+      }
       if (!isfinite(acc[V::RHO]) || !isfinite(acc[V::E])) stb |= ST_NAN;
 #pragma unroll
       for (int v = 0; v < NW; ++v) A.uout[cell_offset<NDIM>(b, NW, v, ci, cj, k)] = acc[v];
@@ -649,7 +723,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
     __syncthreads();
   }
   // the reference restores the whole block to wCT on a small-value crash
-  if (stb & ST_SMALL_VALUE) atomicOr(A.block_status + b, ST_SMALL_VALUE);
+  // (finite_volume; hancock does not)
+  if (SOLVER != SOLVER_HANCOCK && (stb & ST_SMALL_VALUE)) atomicOr(A.block_status + b, ST_SMALL_VALUE);
   st |= stb;
   }  // while (g < gend)
   if (st) atomicOr(A.status, st);

@@ -1046,6 +1046,52 @@ int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, d
   return st;
 }
 
+// hancock (src/mod_finite_volume.t:19-113), slab_uniform, no local dt: the
+// MUSCL-Hancock predictor of twostep Predictor_Corrector for tvdlf.  Per
+// direction the cell's edge states (wLp on ixO: right edge; wRp on hxO = ixO -
+// e_d: the left edge of the cell above), their physical fluxes and
+// wnew(ixO) += -qdt/dx (fLC(ixO) - fRC(hxO)); then the divB sources and the
+// small-value check on wnew (no restore to wCT).
+template <class R>
+int hancock(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, const double *dxs,
+            double cmax_global, int jump_faces = 0) {
+  const Ix &x = s.x;
+  const orc_cfg &c = s.c;
+  const Geo &g = s.g;
+  const int nw = x.nw, ndim = c.ndim;
+  Box ixI = g.ixG(), ixO = g.ixM();
+  int st = 0;
+  Arr<R> wprim = wCT;
+  st |= to_primitive(s, ixI, wprim);
+  Arr<R> wLp(g, nw), wRp(g, nw), wLC(g, nw), wRC(g, nw), fLC(g, nw), fRC(g, nw);
+  for (int idims = 0; idims < ndim; ++idims) {
+    const int o = g.off(idims);
+    const Box hxO = shift(ixO, idims, -1);
+    for (int iw = 0; iw < nw; ++iw)
+      forbox(ixO, [&](int i, int j, int k) {
+        const size_t p = g.idx(i, j, k) + g.cells * (size_t)iw;
+        wRp.d[p - o] = wprim.d[p];
+        wLp.d[p] = wprim.d[p];
+      });
+    st |= reconstruct_LR(s, ixO, hxO, idims, wprim, wLC, wRC, wLp, wRp, dxs[idims]);
+    get_flux(s, wRC, wRp, hxO, idims, cmax_global, fRC);
+    get_flux(s, wLC, wLp, ixO, idims, cmax_global, fLC);
+    const R dxinv = -R(qdt) / R(dxs[idims]);
+    for (int iw = 0; iw < nw; ++iw)
+      forbox(ixO, [&](int i, int j, int k) {
+        const size_t p = g.idx(i, j, k) + g.cells * (size_t)iw;
+        wnew.d[p] = wnew.d[p] + dxinv * (fLC.d[p] - fRC.d[p - o]);
+      });
+  }
+  if (x.mhd && ndim > 1) {
+    double qsrc = qdt * double(ndim) / double(ndim);
+    if (c.divb == ORC_DIVB_GLM) add_source_glm(s, qsrc, ixI, ixO, wCT, wnew, dxs, cmax_global);
+    else if (c.divb == ORC_DIVB_LINDE) add_source_linde(s, qsrc, ixO, wCT, wnew, dxs, jump_faces);
+  }
+  if (c.fix_small_values) st |= handle_small_values(s, false, wnew, ixO);
+  return st;
+}
+
 // getdt_courant (src/mod_dt.t:160-287) with hd_get_cmax (src/hd/mod_hd_phys.t:787-811)
 // and mhd_get_cmax_origin (src/mhd/mod_mhd_phys.t:2482-2550).
 template <class R>
@@ -1471,9 +1517,12 @@ int orc_grid_getdt(orc_grid *g, double *dt, double *cmax_global) {
   return st;
 }
 
-int orc_grid_advect1(orc_grid *g, int ra, int rb, double qdt, double dtfactor, double cmax_global,
-                     int nthreads) {
+// predictor: the twostep Predictor_Corrector predictor, advect1 with
+// typepred1 (hancock for tvdlf, src/io/mod_input_output.t:787-797).
+static int grid_advect1(orc_grid *g, int ra, int rb, double qdt, double dtfactor, double cmax_global, int nthreads,
+                        bool predictor) {
   const size_t bs = g->bsize;
+  const bool hk = predictor && g->s.c.flux_scheme == ORC_FS_TVDLF;
   int st = 0;
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -1482,11 +1531,17 @@ int orc_grid_advect1(orc_grid *g, int ra, int rb, double qdt, double dtfactor, d
   for (int ib = 0; ib < g->nblocks; ++ib) {
     Arr<double> a = wrap_in(g->s.g, g->s.x.nw, &g->reg[ra][bs * ib]);
     Arr<double> b = wrap_in(g->s.g, g->s.x.nw, &g->reg[rb][bs * ib]);
-    st |= finite_volume(g->s, a, b, qdt, dtfactor, g->dx, cmax_global);
+    if (hk) st |= hancock(g->s, a, b, qdt, g->dx, cmax_global);
+    else st |= finite_volume(g->s, a, b, qdt, dtfactor, g->dx, cmax_global);
     std::memcpy(&g->reg[rb][bs * ib], b.d.data(), sizeof(double) * bs);
   }
   getbc_reg(*g, g->reg[rb]);
   return st;
+}
+
+int orc_grid_advect1(orc_grid *g, int ra, int rb, double qdt, double dtfactor, double cmax_global,
+                     int nthreads) {
+  return grid_advect1(g, ra, rb, qdt, dtfactor, cmax_global, nthreads, false);
 }
 
 void orc_grid_copy_reg(orc_grid *g, int dst, int src) { g->reg[dst] = g->reg[src]; }
@@ -1532,8 +1587,9 @@ int fourstep(const orc_cfg &c, double dt, Adv advect1, Copy copy, Comb combine, 
 }
 
 // twostep (src/mod_advance.t:102-133): Predictor_Corrector — predictor
-// ps1 = ps + dt/2 L(ps) with the same scheme (typepred1 for hll, hllc,
-// hlld) and no flux fix, corrector ps = ps + dt L(ps1) — or ssprk2.
+// ps1 = ps + dt/2 L(ps) with typepred1 (the same scheme for hll, hllc, hlld;
+// hancock for tvdlf) and no flux fix, corrector ps = ps + dt L(ps1) — or
+// ssprk2.  advect1's last argument is false for the predictor only.
 template <class Adv, class Copy, class Comb>
 int twostep(const orc_cfg &c, double dt, Adv advect1, Copy copy, Comb combine) {
   int st = 0;
@@ -1562,7 +1618,9 @@ int orc_grid_advance(orc_grid *g, double dt, double cmax_global, int nthreads) {
   if (g->s.c.time_stepper == 2)
     return twostep(
         g->s.c, dt,
-        [&](int ra, int rb, double qdt, double f, bool) { return orc_grid_advect1(g, ra, rb, qdt, f, cmax_global, nthreads); },
+        [&](int ra, int rb, double qdt, double f, bool corr) {
+          return grid_advect1(g, ra, rb, qdt, f, cmax_global, nthreads, !corr);
+        },
         [&](int d, int s2) { orc_grid_copy_reg(g, d, s2); },
         [&](int d, double a, int ra, double b, int rb) { orc_grid_combine_reg(g, d, a, ra, b, rb); });
   if (g->s.c.time_stepper == 4)
@@ -2289,8 +2347,11 @@ void amr_fix_conserve(AmrGrid &G, std::vector<double> &reg) {
       }
 }
 
+// fix == false: the Predictor_Corrector predictor (no flux fix; hancock for
+// tvdlf, which stores no fluxes).
 int amr_advect1(AmrGrid &G, int ra, int rb, double qdt, double dtfactor, double cmax_global, int nthreads,
                 bool fix = true) {
+  const bool hk = !fix && G.s.c.flux_scheme == ORC_FS_TVDLF;
   int st = 0;
   const size_t bs = G.bsize;
 #ifdef _OPENMP
@@ -2311,6 +2372,11 @@ int amr_advect1(AmrGrid &G, int ra, int rb, double qdt, double dtfactor, double 
         const int t = G.ntype[b * 27 + q27(dd)];
         if (t == NT_COARSE || t == NT_FINE) jumps |= 1 << (2 * d + side);
       }
+    if (hk) {
+      st |= hancock(G.s, a, w, qdt, dxb, cmax_global, jumps);
+      std::memcpy(&G.reg[rb][bs * b], w.d.data(), sizeof(double) * bs);
+      continue;
+    }
     st |= finite_volume(G.s, a, w, qdt, dtfactor, dxb, cmax_global, &fc, jumps);
     std::memcpy(&G.reg[rb][bs * b], w.d.data(), sizeof(double) * bs);
     amr_store_flux(G, b, fc);

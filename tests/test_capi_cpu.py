@@ -132,13 +132,14 @@ def test_config_from_par(tmp_path):
 
 def test_time_integrators_are_checked():
     """twostep is Predictor_Corrector by default (the reference's default) or
-    ssprk2 on request; TVDLF's Hancock predictor is not built, so that pair
-    is refused at creation (which needs no device: the check comes first)."""
+    ssprk2 on request; TVDLF's Hancock predictor is FP64 only, so the mixed
+    form of that pair is refused at creation (which needs no device: the
+    check comes first)."""
     from amrvac_b200 import _lib, make_cfg
     lib = _lib.load()
     import ctypes
     h = ctypes.c_void_p()
-    bad = make_cfg(physics="hd", ndim=2, flux_scheme="tvdlf", time_stepper="twostep")
+    bad = make_cfg(physics="hd", ndim=2, flux_scheme="tvdlf", time_stepper="twostep", precision="mixed")
     assert lib.amrvac_gpu_create(ctypes.byref(bad), ctypes.byref(h)) == _lib.E_UNSUPPORTED
     bad = make_cfg(physics="hd", ndim=2, flux_scheme="hll", time_stepper="threestep", time_integrator="rk4")
     assert lib.amrvac_gpu_create(ctypes.byref(bad), ctypes.byref(h)) == _lib.E_UNSUPPORTED

@@ -72,6 +72,12 @@ CASES = [
     ("hd2_hllc_minmod_pc", 2, 3, dict(physics="hd", flux_scheme="hllc", limiter="minmod", time_stepper="twostep")),
     ("mhd2_hlld_glm_ssprk2", 2, 2, dict(physics="mhd", flux_scheme="hlld", limiter="vanleer", typedivbfix="glm",
                                         time_stepper="twostep", time_integrator="ssprk2")),
+    ("hd2_tvdlf_vanleer_hancock", 2, 3, dict(physics="hd", flux_scheme="tvdlf", limiter="vanleer",
+                                             time_stepper="twostep")),
+    ("mhd2_tvdlf_mcbeta_linde_hancock", 2, 2, dict(physics="mhd", flux_scheme="tvdlf", limiter="mcbeta",
+                                                   typedivbfix="linde", time_stepper="twostep")),
+    ("hd3_tvdlf_minmod_hancock_cont", 3, 2, dict(physics="hd", flux_scheme="tvdlf", limiter="minmod",
+                                                 time_stepper="twostep", bc=["cont"] * 6)),
     ("hd2_hllc_cont", 2, 3, dict(physics="hd", flux_scheme="hllc", limiter="vanleer", bc=["cont"] * 4)),
     ("hd2_hll_symm_x_periodic_y", 2, 3, dict(physics="hd", flux_scheme="hll", limiter="minmod",
                                              bc=["symm", "symm", "periodic", "periodic"])),

@@ -135,6 +135,8 @@ def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsav
                           courantpar=0.9, time_stepper="fourstep", time_integrator="rk4"), 6),
     ("rk4_tvdlf_cada", dict(flux_scheme="tvdlf", limiter="cada3", typedivbfix="linde", typeboundspeed="cmaxmean",
                             courantpar=0.9, time_stepper="fourstep", time_integrator="rk4"), 6),
+    ("2step_tvdlf_mm", dict(flux_scheme="tvdlf", limiter="minmod", typedivbfix="linde", typeboundspeed="cmaxmean",
+                            courantpar=0.9, time_stepper="twostep"), 6),
 ])
 def test_orszag_tang_2d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
     weight = np.zeros(nw)
@@ -210,6 +212,7 @@ def _bw2d_prim(X, Y, Z):
     ("4step_hllc_ko", dict(flux_scheme="hllc", limiter="koren", typeboundspeed="cmaxmean", time_stepper="fourstep")),
     ("rk4_tvdlf_cada", dict(flux_scheme="tvdlf", limiter="cada3", typeboundspeed="cmaxmean", time_stepper="fourstep",
                             time_integrator="rk4")),
+    ("2step_tvdlf_mm", dict(flux_scheme="tvdlf", limiter="minmod", typeboundspeed="cmaxmean", time_stepper="twostep")),
 ])
 def test_blast_wave_2d_amr_golden_log_gpu(oracle_lib, name, kw):
     kw = dict(kw, courantpar=0.9)

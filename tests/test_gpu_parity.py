@@ -43,6 +43,17 @@ CASES = {
                                     typedivbfix="linde"),
     "mhd25_hlld_cada_glm_lr": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hlld", limiter="cada",
                                    typedivbfix="glm", typeboundspeed="cmaxleftright", mhd_glm_extended=False),
+    # twostep Predictor_Corrector with tvdlf: the MUSCL-Hancock predictor
+    "hd2_tvdlf_vanleer_hancock": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="tvdlf", limiter="vanleer",
+                                      time_stepper="twostep"),
+    "hd3_tvdlf_koren_hancock": dict(physics="hd", ndim=3, gamma=1.4, flux_scheme="tvdlf", limiter="koren",
+                                    time_stepper="twostep"),
+    "mhd25_tvdlf_cada3_glm_hancock": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="tvdlf", limiter="cada3",
+                                          typedivbfix="glm", time_stepper="twostep"),
+    "mhd2_tvdlf_woodward_linde_hancock": dict(physics="mhd", ndim=2, flux_scheme="tvdlf", limiter="woodward",
+                                              typedivbfix="linde", time_stepper="twostep"),
+    "mhd3_tvdlf_minmod_glm_hancock": dict(physics="mhd", ndim=3, flux_scheme="tvdlf", limiter="minmod",
+                                          typedivbfix="glm", time_stepper="twostep"),
 }
 
 
@@ -135,7 +146,8 @@ def test_stage_matches_oracle(oracle_lib, name):
 
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_full_step_matches_oracle(oracle_lib, name):
-    """setdt + all SSP-RK3 stages on the device vs the oracle's advance."""
+    """setdt + all stages of the configured time stepper (SSP-RK3, or twostep
+    with the Hancock predictor) on the device vs the oracle's advance."""
     _cuda()
     O, ocfg, og, ctx = _setup(oracle_lib, name)
     dt_ref, cg_ref = og.getdt()
