@@ -393,7 +393,6 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
     return fail(AMRVAC_E_ARG, "ssprk_order must be 2 or 3");
   if (k.physics == 0 && k.ndir != k.ndim) return fail(AMRVAC_E_UNSUPPORTED, "hd requires ndir == ndim");
   if (k.physics == 1) {
-    if (k.flux_scheme == AMRVAC_FS_HLLC) return fail(AMRVAC_E_UNSUPPORTED, "mhd hllc not supported");
     if (k.typedivbfix != AMRVAC_DIVB_NONE && k.typedivbfix != AMRVAC_DIVB_GLM && k.typedivbfix != AMRVAC_DIVB_LINDE)
       return fail(AMRVAC_E_UNSUPPORTED, "typedivbfix must be none, glm or linde");
     if (k.ndim == 3 && k.typedivbfix == AMRVAC_DIVB_LINDE)

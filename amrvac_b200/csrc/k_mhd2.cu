@@ -36,6 +36,10 @@ bool lookup_mhd2(const KernelKey &k, KernelSet *out) {
   AMRVAC_M2(3, true, SOLVER_TVDLF)
   AMRVAC_M2(3, true, SOLVER_HLL)
   AMRVAC_M2(3, true, SOLVER_HLLD)
+  AMRVAC_M2(2, false, SOLVER_HLLC)
+  AMRVAC_M2(2, true, SOLVER_HLLC)
+  AMRVAC_M2(3, false, SOLVER_HLLC)
+  AMRVAC_M2(3, true, SOLVER_HLLC)
 #undef AMRVAC_M2
   return false;
 }

@@ -30,6 +30,8 @@ bool lookup_mhd3(const KernelKey &k, KernelSet *out) {
   AMRVAC_M3(true, SOLVER_TVDLF)
   AMRVAC_M3(true, SOLVER_HLL)
   AMRVAC_M3(true, SOLVER_HLLD)
+  AMRVAC_M3(false, SOLVER_HLLC)
+  AMRVAC_M3(true, SOLVER_HLLC)
 #undef AMRVAC_M3
   return false;
 }

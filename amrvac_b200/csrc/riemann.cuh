@@ -115,6 +115,88 @@ __device__ __forceinline__ void riemann_hllc_hd(const T *wLC, const T *wRC, cons
   for (int v = 0; v < NW; ++v) F[v] = fSub[v] + cspeed * (wCD[v] - wSub[v]);
 }
 
+// get_Riemann_flux_hllc (mod_finite_volume.t:439-504) + mhd_get_lCD /
+// mhd_get_wCD (src/mhd/mod_mhd_hllc.t:56-241), no hllcd diffusion,
+// flathllc=.false.  The star state keeps the HLL magnetic field; its flux
+// has zero normal-B (and psi) entries, which the flux_type rules then
+// replace by the diffusive tvdlf form without GLM, and keep with GLM (the
+// reference's HLLC takes no flux_special branch).
+template <class T, int NDIR, bool GLM, int NDIM, int D>
+__device__ __forceinline__ void riemann_hllc_mhd(const T *wLC, const T *wRC, const T *fL, const T *fR, T cmax,
+                                                 T cmin, T tvdlfeps, T *F) {
+  using V = Vars<true, NDIR, GLM>;
+  using FT = FluxTypes<true, NDIM, GLM>;
+  constexpr int NW = V::NW, MN = V::M0 + D, BNI = V::B0 + D;
+  int patchf = 1;
+  if (cmin >= T(0.0)) patchf = -2;
+  else if (cmax <= T(0.0)) patchf = 2;
+  T whll[NW], Fhll[NW], fCD[NW];
+  T lambdaCD = T(0.0);
+  if (patchf == 1) {
+#pragma unroll
+    for (int v = 0; v < NW; ++v) {
+      Fhll[v] = (cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v])) / (cmax - cmin);
+      whll[v] = (cmax * wRC[v] - cmin * wLC[v] + fL[v] - fR[v]) / (cmax - cmin);
+    }
+    lambdaCD = whll[MN] / whll[V::RHO];
+    bool cond = true;
+    if (cmin < T(0.0) && lambdaCD > T(0.0) && lambdaCD < cmax) {
+      patchf = -1;
+    } else if (cmax > T(0.0) && lambdaCD < T(0.0) && lambdaCD > cmin) {
+      patchf = 1;
+    } else if (lambdaCD >= cmax || lambdaCD <= cmin) {
+      lambdaCD = T(0.0);
+      patchf = 3;
+      cond = false;
+    }
+    if (cond && lambdaCD == T(0.0)) patchf = (-cmin >= cmax) ? 1 : -1;
+  }
+  if (patchf == 1 || patchf == -1) {
+    const bool right = (patchf == 1);
+    const T *wSub = right ? wRC : wLC;
+    const T *fSub = right ? fR : fL;
+    const T cspeed = right ? cmax : cmin;
+    const T vSub = wSub[MN] / wSub[V::RHO];
+    const T den = cspeed - lambdaCD;
+    T wCD[NW];
+    wCD[V::RHO] = wSub[V::RHO] * (cspeed - vSub) / den;
+#pragma unroll
+    for (int c = 0; c < NDIR; ++c) wCD[V::B0 + c] = whll[V::B0 + c];
+#pragma unroll
+    for (int c = 0; c < NDIR; ++c) {
+      if (c != D) wCD[V::M0 + c] = (cspeed * wSub[V::M0 + c] - fSub[V::M0 + c] - wCD[BNI] * wCD[V::B0 + c]) / den;
+      else wCD[V::M0 + c] = wCD[V::RHO] * lambdaCD;
+    }
+    // V.B of the HLL state (summed in the order the components arrive)
+    T vdb = whll[V::M0] * whll[V::B0];
+#pragma unroll
+    for (int c = 1; c < NDIR; ++c) vdb = vdb + whll[V::M0 + c] * whll[V::B0 + c];
+    vdb = vdb / whll[V::RHO];
+    const T pCD = wSub[V::RHO] * (cspeed - vSub) * (lambdaCD - vSub) + fSub[MN] - wSub[MN] * vSub +
+                  wCD[BNI] * wCD[BNI];
+    wCD[V::E] = (cspeed * wSub[V::E] - fSub[V::E] + lambdaCD * pCD - vdb * wCD[BNI]) / den;
+#pragma unroll
+    for (int v = 0; v < NW; ++v) {
+      if (v == BNI || (GLM && v == V::PSI)) fCD[v] = T(0.0);
+      else fCD[v] = fSub[v] + cspeed * (wCD[v] - wSub[v]);
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < NW; ++v) {
+    if (FT::bn_tvdlf && v == BNI) {
+      F[v] = -(tvdlfeps * T(0.5) * fmax(cmax, fabs(cmin))) * (wRC[v] - wLC[v]);
+    } else if (patchf == -2) {
+      F[v] = fL[v];
+    } else if (patchf == 2) {
+      F[v] = fR[v];
+    } else if (patchf == 3) {
+      F[v] = Fhll[v];
+    } else {
+      F[v] = fCD[v];
+    }
+  }
+}
+
 // get_Riemann_flux_hlld (mod_finite_volume.t:507-729), no B0 / equilibrium split.
 template <class T, int NDIR, bool GLM, int NDIM, int D>
 __device__ __forceinline__ void riemann_hlld(const T *wLC, const T *wRC, const T *wLp,

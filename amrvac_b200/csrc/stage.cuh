@@ -220,8 +220,8 @@ __device__ __forceinline__ uint32_t face_from_states(T *wLp, T *wRp, const PhysP
     if constexpr (SOLVER == SOLVER_HLL) {
       riemann_hll<T, MHD, NDIR, GLM, NDIM, D>(wLC, wRC, fL, fR, cmax, cmin, T(P.tvdlfeps), F);
     } else if constexpr (SOLVER == SOLVER_HLLC) {
-      static_assert(!MHD, "HLLC is implemented for HD only");
-      riemann_hllc_hd<T, NDIR, D>(wLC, wRC, fL, fR, cmax, cmin, F);
+      if constexpr (MHD) riemann_hllc_mhd<T, NDIR, GLM, NDIM, D>(wLC, wRC, fL, fR, cmax, cmin, T(P.tvdlfeps), F);
+      else riemann_hllc_hd<T, NDIR, D>(wLC, wRC, fL, fR, cmax, cmin, F);
     } else {
       static_assert(MHD, "HLLD needs MHD");
       riemann_hlld<T, NDIR, GLM, NDIM, D>(wLC, wRC, wLp, wRp, fL, fR, cmax, cmin, F);

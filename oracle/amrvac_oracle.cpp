@@ -680,7 +680,8 @@ void riemann_tvdlf(const State &s, const Box &b, int idims, const Arr<R> &wLC, c
 }
 
 // get_Riemann_flux_hllc (src/mod_finite_volume.t:439-504) with hd_get_lCD and
-// hd_get_wCD (src/hd/mod_hd_hllc.t:56-257).  HD only.
+// hd_get_wCD (src/hd/mod_hd_hllc.t:56-257), or mhd_get_lCD and mhd_get_wCD
+// (src/mhd/mod_mhd_hllc.t:56-241) for MHD.
 template <class R>
 void riemann_hllc(const State &s, const Box &b, int idims, const Arr<R> &wLC, const Arr<R> &wRC,
                   Arr<R> &fLC, const Arr<R> &fRC, const Arr<R> &cmaxC, const Arr<R> &cminC,
@@ -692,7 +693,7 @@ void riemann_hllc(const State &s, const Box &b, int idims, const Arr<R> &wLC, co
     int patchf = 1;
     if (cmin >= R(zero)) patchf = -2;
     else if (cmax <= R(zero)) patchf = 2;
-    R whll[8], Fhll[8], fCD[8];
+    R whll[16], Fhll[16], fCD[16];
     R lambdaCD(0.0);
     if (patchf == 1) {
       for (int iw = 0; iw < nw; ++iw) {
@@ -713,6 +714,31 @@ void riemann_hllc(const State &s, const Box &b, int idims, const Arr<R> &wLC, co
       const Arr<R> *wSub, *fSub;
       if (patchf == 1) { cspeed = cmax; vSub = W(wRC, mn) / W(wRC, x.rho); wSub = &wRC; fSub = &fRC; }
       else { cspeed = cmin; vSub = W(wLC, mn) / W(wLC, x.rho); wSub = &wLC; fSub = &fLC; }
+      if (x.mhd) {
+        // mhd_get_wCD: the star state keeps the HLL magnetic field (Li 2005)
+        const R den = cspeed - lambdaCD;
+        const int bn = x.mag[idims];
+        R wCD[16];
+        wCD[x.rho] = (*wSub)(i, j, k, x.rho) * (cspeed - vSub) / den;
+        for (int c = 0; c < x.ndir; ++c) wCD[x.mag[c]] = whll[x.mag[c]];
+        for (int c = 0; c < x.ndir; ++c) {
+          if (c != idims)
+            wCD[x.mom[c]] = (cspeed * (*wSub)(i, j, k, x.mom[c]) - (*fSub)(i, j, k, x.mom[c]) -
+                             wCD[bn] * wCD[x.mag[c]]) / den;
+          else
+            wCD[x.mom[c]] = wCD[x.rho] * lambdaCD;
+        }
+        R vdb = whll[x.mom[0]] * whll[x.mag[0]];
+        for (int c = 1; c < x.ndir; ++c) vdb = vdb + whll[x.mom[c]] * whll[x.mag[c]];
+        vdb = vdb / whll[x.rho];
+        R pCD = (*wSub)(i, j, k, x.rho) * (cspeed - vSub) * (lambdaCD - vSub) + (*fSub)(i, j, k, mn) -
+                (*wSub)(i, j, k, mn) * vSub + wCD[bn] * wCD[bn];
+        wCD[x.e] = (cspeed * (*wSub)(i, j, k, x.e) - (*fSub)(i, j, k, x.e) + lambdaCD * pCD - vdb * wCD[bn]) / den;
+        for (int iw = 0; iw < nw; ++iw) {
+          if (iw == bn || (x.glm && iw == x.psi)) fCD[iw] = R(zero);
+          else fCD[iw] = (*fSub)(i, j, k, iw) + cspeed * (wCD[iw] - (*wSub)(i, j, k, iw));
+        }
+      } else {
       R csmls = R(one) / (cspeed - lambdaCD);
       R wCD[8];
       wCD[x.rho] = (*wSub)(i, j, k, x.rho) * (cspeed - vSub) * csmls;
@@ -727,10 +753,13 @@ void riemann_hllc(const State &s, const Box &b, int idims, const Arr<R> &wLC, co
       wCD[x.e] = (cspeed * (*wSub)(i, j, k, x.e) - (*fSub)(i, j, k, x.e) + lambdaCD * pCD) * csmls;
       for (int iw = 0; iw < nw; ++iw)
         fCD[iw] = (*fSub)(i, j, k, iw) + cspeed * (wCD[iw] - (*wSub)(i, j, k, iw));
+      }
     }
     for (int iw = 0; iw < nw; ++iw) {
       R out = W(fLC, iw);
-      if (patchf == -2) out = W(fLC, iw);
+      if (flux_type(s.c, x, idims, iw) == FT_TVDLF)
+        out = -(R(s.c.tvdlfeps) * R(half) * rmax(cmax, rabs(cmin))) * (W(wRC, iw) - W(wLC, iw));
+      else if (patchf == -2) out = W(fLC, iw);
       else if (patchf == 1 || patchf == -1) out = fCD[iw];
       else if (patchf == 2) out = W(fRC, iw);
       else if (patchf == 3) out = Fhll[iw];

@@ -14,7 +14,8 @@ fourstep variants (rk4 with HLL and woodward, ssprk4 with HLLC and koren)
 ot_2d_4step_hll_mc.log, kh_2d_4step_hll_mc.log, kh_2d_4step_hllc_ko.log and
 (RK4, TVDLF, cada3) ot_2d_rk4_tvdlf_cada.log, kh_2d_rk4_tvdlf_cada.log, and
 the twostep Predictor_Corrector variant (MUSCL-Hancock predictor, TVDLF,
-minmod) ot_2d_2step_tvdlf_mm.log; and the 2-D blast wave with cont
+minmod) ot_2d_2step_tvdlf_mm.log, and MHD HLLC (SSPRK(4,3), koren, Linde)
+ot_2d_4step_hllc_ko.log; and the 2-D blast wave with cont
 boundaries, tests/hd/blast_wave_Cartesian_2D/correct_output/
 bw_2d_{3step_hll_cada,4step_hll_mc,4step_hllc_ko,rk4_tvdlf_cada,
 2step_tvdlf_mm}.log.
@@ -38,6 +39,7 @@ LOGS = [
     "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_rk4_tvdlf_cada.log",
     "tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_rk4_tvdlf_cada.log",
     "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_2step_tvdlf_mm.log",
+    "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_4step_hllc_ko.log",
     # multi-level with cont boundaries
     "tests/hd/blast_wave_Cartesian_2D/correct_output/bw_2d_3step_hll_cada.log",
     "tests/hd/blast_wave_Cartesian_2D/correct_output/bw_2d_4step_hll_mc.log",

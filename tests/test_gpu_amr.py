@@ -78,6 +78,10 @@ CASES = [
                                                    typedivbfix="linde", time_stepper="twostep")),
     ("hd3_tvdlf_minmod_hancock_cont", 3, 2, dict(physics="hd", flux_scheme="tvdlf", limiter="minmod",
                                                  time_stepper="twostep", bc=["cont"] * 6)),
+    ("mhd2_hllc_koren_linde_ssprk43", 2, 3, dict(physics="mhd", flux_scheme="hllc", limiter="koren",
+                                                 typedivbfix="linde", time_stepper="fourstep")),
+    ("mhd2_hllc_vanleer_glm_cont", 2, 2, dict(physics="mhd", flux_scheme="hllc", limiter="vanleer",
+                                              typedivbfix="glm", bc=["cont"] * 4)),
     ("hd2_hllc_cont", 2, 3, dict(physics="hd", flux_scheme="hllc", limiter="vanleer", bc=["cont"] * 4)),
     ("hd2_hll_symm_x_periodic_y", 2, 3, dict(physics="hd", flux_scheme="hll", limiter="minmod",
                                              bc=["symm", "symm", "periodic", "periodic"])),

@@ -43,6 +43,12 @@ CASES = {
                                     typedivbfix="linde"),
     "mhd25_hlld_cada_glm_lr": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hlld", limiter="cada",
                                    typedivbfix="glm", typeboundspeed="cmaxleftright", mhd_glm_extended=False),
+    # MHD HLLC (mhd_get_lCD / mhd_get_wCD)
+    "mhd2_hllc_koren_linde": dict(physics="mhd", ndim=2, flux_scheme="hllc", limiter="koren", typedivbfix="linde"),
+    "mhd25_hllc_vanleer_glm_cmaxmean": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hllc", limiter="vanleer",
+                                            typedivbfix="glm", typeboundspeed="cmaxmean"),
+    "mhd3_hllc_minmod_glm": dict(physics="mhd", ndim=3, flux_scheme="hllc", limiter="minmod", typedivbfix="glm"),
+    "mhd3_hllc_cada3_none": dict(physics="mhd", ndim=3, flux_scheme="hllc", limiter="cada3", typedivbfix="none"),
     # twostep Predictor_Corrector with tvdlf: the MUSCL-Hancock predictor
     "hd2_tvdlf_vanleer_hancock": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="tvdlf", limiter="vanleer",
                                       time_stepper="twostep"),
