@@ -107,11 +107,12 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
              check_small_values=True, small_values_method="error", small_density=0.0,
              small_pressure=0.0, time_stepper="threestep", ssprk_order=3, dtmin=1.0e-10,
              typeboundary=None, zchunk=0, precision="fp64", slowsteps=-1,
-             time_integrator="default") -> _lib.AmrvacCfg:
+             time_integrator="default", nghostcells=None) -> _lib.AmrvacCfg:
     """Build an ``amrvac_cfg`` from reference-style parameter names.
 
     typeboundary: list of 2*ndim entries (min1, max1, min2, ...), each a name
-    applied to all variables or a list of per-variable names.
+    applied to all variables or a list of per-variable names.  nghostcells
+    defaults to 3 for mp5 (which needs them) and 2 otherwise.
     """
     L = _lib.load()
     c = _lib.AmrvacCfg()
@@ -124,6 +125,7 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
     c.gamma = (5.0 / 3.0) if gamma is None else float(gamma)
     c.flux_scheme = _lib.FS[flux_scheme]
     c.limiter = _lib.LIMITER[limiter]
+    c.nghostcells = int(nghostcells) if nghostcells is not None else (3 if limiter == "mp5" else 2)
     c.typeboundspeed = _lib.BOUNDSPEED[typeboundspeed]
     if typedivbfix is None:
         typedivbfix = "linde" if physics == "mhd" else "none"
@@ -209,6 +211,7 @@ def config_from_par(paths) -> RunConfig:
         time_stepper=ts,
         ssprk_order=int(meth.get("ssprk_order", 3)),
         time_integrator=integ or "default",
+        nghostcells=int(mesh["nghostcells"]) if "nghostcells" in mesh else None,
     )
     if physics == "mhd":
         cfg_kw.update(typedivbfix=plist.get("typedivbfix", "linde"),

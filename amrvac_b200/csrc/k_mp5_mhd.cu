@@ -1,0 +1,25 @@
+// Stage kernels with MP5 reconstruction (three-cell halo) for MHD: 2-D with
+// two or three vector components, 3-D; GLM or not; HLL and HLLD.
+#include "kernels.cuh"
+
+namespace amrvac {
+
+bool lookup_mp5_mhd(const KernelKey &k, KernelSet *out) {
+  if (!k.mhd || k.mixed || k.limiter != LIM_MP5) return false;
+#define AMRVAC_MP5_M(ND, NDIR, GLM, S)                                      \
+  if (k.ndim == ND && k.ndir == NDIR && k.glm == GLM && k.solver == S) {    \
+    *out = Launch<true, NDIR, GLM, ND, S, LIM_MP5>::set();                  \
+    return true;                                                            \
+  }
+  AMRVAC_MP5_M(2, 2, false, SOLVER_HLL)
+  AMRVAC_MP5_M(2, 2, false, SOLVER_HLLD)
+  AMRVAC_MP5_M(2, 3, true, SOLVER_HLL)
+  AMRVAC_MP5_M(2, 3, true, SOLVER_HLLD)
+  AMRVAC_MP5_M(3, 3, false, SOLVER_HLLD)
+  AMRVAC_MP5_M(3, 3, true, SOLVER_HLL)
+  AMRVAC_MP5_M(3, 3, true, SOLVER_HLLD)
+#undef AMRVAC_MP5_M
+  return false;
+}
+
+}  // namespace amrvac

@@ -181,7 +181,7 @@ struct KernelSet {
 template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM = 0, int BS = 0, class TF = double>
 struct Launch {
   using V = Vars<MHD, NDIR, GLM>;
-  static constexpr size_t SMEM = Tile<TF, V::NW, NDIM>::BYTES;
+  static constexpr size_t SMEM = Tile<TF, V::NW, NDIM, HaloW<LIM>::value>::BYTES;
   // typepred1 = fs_hancock for tvdlf (src/io/mod_input_output.t:787-797)
   static constexpr bool HAS_HANCOCK = SOLVER == SOLVER_TVDLF && sizeof(TF) == 8;
   static cudaError_t prepare() {
@@ -277,6 +277,8 @@ struct KernelKey {
 };
 
 bool lookup_hd(const KernelKey &k, KernelSet *out);
+bool lookup_mp5_hd(const KernelKey &k, KernelSet *out);
+bool lookup_mp5_mhd(const KernelKey &k, KernelSet *out);
 bool lookup_mhd2(const KernelKey &k, KernelSet *out);
 bool lookup_mhd3(const KernelKey &k, KernelSet *out);
 

@@ -82,7 +82,7 @@ __device__ __forceinline__ int dir_index(int di, int dj, int dk) {
 }
 
 // Resolve a cell of block b given local coordinates that may lie up to two
-// cells outside the block: physical sides first (clamp for cont, mirror for
+// (three with MP5) cells outside the block: physical sides first (clamp for cont, mirror for
 // symm/asymm), then the remaining offset through the neighbour table.
 template <int NDIM>
 __device__ __forceinline__ int resolve_cell(const StageArgs &A, int b, int &i, int &j, int &k,
@@ -179,12 +179,13 @@ __device__ __forceinline__ uint32_t load_prim(const StageArgs &A, int b, int i, 
 // fix, to_conserved, GLM modify_wLR, physical fluxes, cbounds, Riemann solver
 // (src/mod_finite_volume.t:1217-1222, 200-245).  wLp/wRp are modified.
 template <class T, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int BS>
-__device__ __forceinline__ uint32_t face_from_states(T *wLp, T *wRp, const PhysParams &P, T cg, T *F) {
+__device__ __forceinline__ uint32_t face_from_states(T *wLp, T *wRp, const PhysParams &P, T cg, T *F,
+                                                     bool small_check = true) {
   constexpr int D = 0;  // states arrive rotated: the face normal is component 0
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
   uint32_t st = 0;
-  if (P.fix_small_values) {
+  if (small_check && P.fix_small_values) {
     bool fl = small_values<T, MHD, NDIR, GLM>(wLp, true, P);
     bool fr = small_values<T, MHD, NDIR, GLM>(wRp, true, P);
     if ((fl || fr) && P.small_values_method != 1) st |= ST_SMALL_VALUE;
@@ -230,53 +231,102 @@ __device__ __forceinline__ uint32_t face_from_states(T *wLp, T *wRp, const PhysP
   return st;
 }
 
-// Shared-memory tile (sizes in doubles).
-template <class TF, int NW, int NDIM>
+// MP5 reconstruction (MP5limiter, src/limiter/mod_mp5.t:16-201: Suresh &
+// Huynh 1997 in the convention of Mignone et al. 2010), minmod and median as
+// mod_mp5.t:404-432.  mp5_side(w(i-2), w(i-1), w(i), w(i+1), w(i+2)) is the
+// left state at face i+1/2; the right state is the same formula on the data
+// mirrored about the face, mp5_side(w(i+3), w(i+2), w(i+1), w(i), w(i-1)),
+// which reproduces the reference's right-side expressions term for term.
+__device__ __forceinline__ double mp5_minmod(double a, double b) {
+  return (copysign(1.0, a) + copysign(1.0, b)) / 2.0 * fmin(fabs(a), fabs(b));
+}
+__device__ __forceinline__ double mp5_median(double a, double b, double c) {
+  const double t1 = b - a, t2 = c - a;
+  return a + (copysign(1.0, t1) + copysign(1.0, t2)) / 2.0 * fmin(fabs(t1), fabs(t2));
+}
+__device__ __forceinline__ double mp5_side(double wmm, double wm, double w0, double wp, double wpp) {
+  const double f = (1.0 / 60.0) * ((((2.0 * wmm - 13.0 * wm) + 47.0 * w0) + 27.0 * wp) - 3.0 * wpp);
+  const double b = 4.0 * (w0 - wm);  // alpha = 4
+  const double fmp = w0 + mp5_minmod(wp - w0, b);
+  const double ful = w0 + b;
+  const double dm = (w0 - 2.0 * wm) + wmm;   // d at i-1
+  const double d0 = (wp - 2.0 * w0) + wm;    // d at i
+  const double dp = (wpp - 2.0 * wp) + w0;   // d at i+1
+  const double dm4_0 = mp5_minmod(mp5_minmod(4.0 * d0 - dp, 4.0 * dp - d0), mp5_minmod(d0, dp));
+  const double dm4_m = mp5_minmod(mp5_minmod(4.0 * dm - d0, 4.0 * d0 - dm), mp5_minmod(dm, d0));
+  const double fmd = (w0 + wp) / 2.0 - dm4_0 / 2.0;
+  const double flc = 0.5 * (3.0 * w0 - wm) + (4.0 / 3.0) * dm4_m;
+  const double fmin_ = fmax(fmin(fmin(w0, wp), fmd), fmin(fmin(w0, ful), flc));
+  const double fmax_ = fmin(fmax(fmax(w0, wp), fmd), fmax(fmax(w0, ful), flc));
+  if ((f - w0) * (f - fmp) <= 0.0) return f;
+  return mp5_median(fmin_, f, fmax_);
+}
+
+// Halo width of the staged tile: two cells for the slope limiters, three for
+// MP5 (its face stencil spans cells i-2 .. i+3).
+template <int LIM>
+struct HaloW {
+  static constexpr int value = LIM == LIM_MP5 ? 3 : 2;
+};
+
+// Shared-memory tile (sizes in doubles), halo width HW.
+template <class TF, int NW, int NDIM, int HW = 2>
 struct Tile {
-  static constexpr int NSLOT = NDIM == 3 ? 4 : 1;
+  static constexpr int H2 = 2 * HW;
+  static constexpr int NSLOT = NDIM == 3 ? H2 : 1;      // z ring: planes k-HW+1 .. k+HW
   static constexpr int PLANE = BN * BN;
   static constexpr int RING = NSLOT * NW * PLANE;        // [slot][v][j][i]
-  static constexpr int HX = NW * BN * 4;                 // [v][j][c] c: i=-2,-1,16,17
-  static constexpr int HY = NW * 4 * BN;                 // [v][r][i] r: j=-2,-1,16,17
-  static constexpr int HC = NW * 16;                     // [v][r][c] corners
+  static constexpr int HX = NW * BN * H2;                // [v][j][c] c: i=-HW..-1, BN..BN+HW-1
+  static constexpr int HY = NW * H2 * BN;                // [v][r][i] r: j likewise
+  static constexpr int HC = NW * H2 * H2;                // [v][r][c] corners
   static constexpr int FB = NW * (BN + 1) * BN;          // [v][face]
   static constexpr int TOTAL = RING + HX + HY + HC + FB;
   static constexpr size_t BYTES = sizeof(TF) * TOTAL;
 };
 
 __device__ __forceinline__ int halo_slot(int c) { return c < 0 ? c + 2 : c - (BN - 2); }
+template <int HW>
+__device__ __forceinline__ int halo_slot_w(int c) { return c < 0 ? c + HW : c - (BN - HW); }
 
-template <class TF, int NW, int NDIM>
+// Ring slot of z-plane k (k >= -2 HW).
+template <int HW>
+__device__ __forceinline__ int ring_slot(int k) {
+  if constexpr (HW == 2) return k & 3;
+  else return (k + 4 * HW) % (2 * HW);
+}
+
+template <class TF, int NW, int NDIM, int HW = 2>
 struct TileView {
+  static constexpr int H2 = 2 * HW;
   TF *ring, *hx, *hy, *hc, *fb;
   __device__ TileView(TF *s) {
-    using T = Tile<TF, NW, NDIM>;
+    using T = Tile<TF, NW, NDIM, HW>;
     ring = s;
     hx = ring + T::RING;
     hy = hx + T::HX;
     hc = hy + T::HY;
     fb = hc + T::HC;
   }
-  // primitive v at in-plane (i, j) in [-2, 17]^2 of the plane held in `slot`
+  // primitive v at in-plane (i, j) in [-HW, BN+HW-1]^2 of the plane held in `slot`
   __device__ __forceinline__ TF at(int slot, int v, int i, int j) const {
     const bool ii = (unsigned)i < (unsigned)BN, jj = (unsigned)j < (unsigned)BN;
     if (ii && jj) return ring[(slot * NW + v) * (BN * BN) + j * BN + i];
-    if (jj) return hx[(v * BN + j) * 4 + halo_slot(i)];
-    if (ii) return hy[(v * 4 + halo_slot(j)) * BN + i];
-    return hc[(v * 4 + halo_slot(j)) * 4 + halo_slot(i)];
+    if (jj) return hx[(v * BN + j) * H2 + halo_slot_w<HW>(i)];
+    if (ii) return hy[(v * H2 + halo_slot_w<HW>(j)) * BN + i];
+    return hc[(v * H2 + halo_slot_w<HW>(j)) * H2 + halo_slot_w<HW>(i)];
   }
   // Offset (in doubles from the tile start) of variable 0 at in-plane (i, j)
   // of the plane in `slot`, and the stride between variables there; branch-free.
   __device__ __forceinline__ void addr(int slot, int i, int j, int &base, int &stride) const {
-    using T = Tile<TF, NW, NDIM>;
+    using T = Tile<TF, NW, NDIM, HW>;
     const bool ii = (unsigned)i < (unsigned)BN, jj = (unsigned)j < (unsigned)BN;
-    const int hi = halo_slot(i), hj = halo_slot(j);
+    const int hi = halo_slot_w<HW>(i), hj = halo_slot_w<HW>(j);
     const int oc = slot * NW * (BN * BN) + j * BN + i;
-    const int ox = T::RING + j * 4 + hi;
+    const int ox = T::RING + j * H2 + hi;
     const int oy = T::RING + T::HX + hj * BN + i;
-    const int oz = T::RING + T::HX + T::HY + hj * 4 + hi;
+    const int oz = T::RING + T::HX + T::HY + hj * H2 + hi;
     base = ii ? (jj ? oc : oy) : (jj ? ox : oz);
-    stride = ii ? (jj ? BN * BN : 4 * BN) : (jj ? 4 * BN : 16);
+    stride = ii ? (jj ? BN * BN : H2 * BN) : (jj ? H2 * BN : H2 * H2);
   }
   __device__ __forceinline__ TF &center(int slot, int v, int i, int j) {
     return ring[(slot * NW + v) * (BN * BN) + j * BN + i];
@@ -378,16 +428,22 @@ __device__ __forceinline__ uint32_t hancock_dir(const double *smem, const int *b
   return st;
 }
 
+// MP5 (three-cell halo) takes one CTA per SM: its 6-plane ring fills most of
+// the shared memory of the 3-D MHD tile, and the registers it frees avoid
+// spills in the 6-cell face stencil.
 template <class TF, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS>
-__global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_MINB : AMRVAC_STAGE_MINB_MIXED)
+__global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (LIM == LIM_MP5 ? 1 : AMRVAC_STAGE_MINB)
+                                                                 : AMRVAC_STAGE_MINB_MIXED)
     fv_stage_kernel(const StageArgs A) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
   constexpr int FB = (BN + 1) * BN;  // face-buffer stride per variable
   constexpr bool FP64 = sizeof(TF) == 8;
+  constexpr int HW = HaloW<LIM>::value;  // halo width: 2, or 3 for MP5
+  constexpr int H2 = 2 * HW;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TF *smem = reinterpret_cast<TF *>(smem_raw);
-  TileView<TF, NW, NDIM> tv(smem);
+  TileView<TF, NW, NDIM, HW> tv(smem);
   const int t = threadIdx.x;
   // Work: global z-planes g = block*PL + k (PL = 16 in 3-D, 1 in 2-D).
   // zchunk > 0: one z-chunk of one block per CTA.  zchunk == 0: persistent
@@ -438,47 +494,48 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
 #pragma unroll
   for (int v = 0; v < (NDIM == 3 ? NW : 1); ++v) fz_prev[v] = 0.0;
 
-  // 3-D: iteration k stages plane k+2; iterations k0-4 .. k0-1 only stage the
-  // planes k0-2 .. k0+1 (and, at k0-1, compute the z-face k0-1/2);
+  // 3-D: iteration k stages plane k+HW; iterations k0-2HW .. k0-1 only stage
+  // the planes k0-HW .. k0+HW-1 (and, at k0-1, compute the z-face k0-1/2);
   // iterations k0 .. k1-1 update plane k.
-  const int kstart = NDIM == 3 ? k0 - 4 : 0;
+  const int kstart = NDIM == 3 ? k0 - 2 * HW : 0;
 #pragma unroll 1
   for (int k = kstart; k < k1; ++k) {
     const bool update = k >= k0;
-    const int slot = NDIM == 3 ? (k & 3) : 0;
-    // ---- stage plane k+2 (3-D) / the block (2-D) as primitives
+    const int slot = NDIM == 3 ? ring_slot<HW>(k) : 0;
+    // ---- stage plane k+HW (3-D) / the block (2-D) as primitives
     if (cell_thread) {
       double w[NW];
-      const int kk = NDIM == 3 ? k + 2 : 0;
+      const int kk = NDIM == 3 ? k + HW : 0;
       stb |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, ci, cj, kk, w);
-      const int s2 = NDIM == 3 ? (kk & 3) : 0;
+      const int s2 = NDIM == 3 ? ring_slot<HW>(kk) : 0;
 #pragma unroll
       for (int v = 0; v < NW; ++v) tv.center(s2, v, ci, cj) = TF(w[v]);
     }
     // ---- x/y halo strips (and corners for Linde) of plane k
-    const int nhalo = update ? (need_corners ? 144 : 128) : 0;
+    constexpr int NHX = BN * H2, NHY = H2 * BN, NHC = H2 * H2;
+    const int nhalo = update ? (need_corners ? NHX + NHY + NHC : NHX + NHY) : 0;
     if (t < nhalo) {
       const int h = t;
       int i, j, stride;
       TF *dst;
-      if (h < 64) {
-        j = h >> 2;
-        const int c = h & 3;
-        i = c < 2 ? c - 2 : c + BN - 2;
-        dst = tv.hx + j * 4 + c;
-        stride = BN * 4;
-      } else if (h < 128) {
-        const int r = (h - 64) >> 4;
-        i = (h - 64) & (BN - 1);
-        j = r < 2 ? r - 2 : r + BN - 2;
+      if (h < NHX) {
+        j = h / H2;
+        const int c = h - j * H2;
+        i = c < HW ? c - HW : c + BN - HW;
+        dst = tv.hx + j * H2 + c;
+        stride = BN * H2;
+      } else if (h < NHX + NHY) {
+        const int r = (h - NHX) / BN;
+        i = (h - NHX) - r * BN;
+        j = r < HW ? r - HW : r + BN - HW;
         dst = tv.hy + r * BN + i;
-        stride = 4 * BN;
+        stride = H2 * BN;
       } else {
-        const int r = (h - 128) >> 2, c = (h - 128) & 3;
-        i = c < 2 ? c - 2 : c + BN - 2;
-        j = r < 2 ? r - 2 : r + BN - 2;
-        dst = tv.hc + r * 4 + c;
-        stride = 16;
+        const int r = (h - NHX - NHY) / H2, c = (h - NHX - NHY) - r * H2;
+        i = c < HW ? c - HW : c + BN - HW;
+        j = r < HW ? r - HW : r + BN - HW;
+        dst = tv.hc + r * H2 + c;
+        stride = H2 * H2;
       }
       double w[NW];
       stb |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, i, j, k, w);
@@ -511,7 +568,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
         if constexpr (NDIM == 3) {
 #pragma unroll
           for (int o = 0; o < 3; ++o) {
-            base[o] = ((k + o - 1) & 3) * NW * (BN * BN) + cj * BN + ci;
+            base[o] = ring_slot<HW>(k + o - 1) * NW * (BN * BN) + cj * BN + ci;
             strd[o] = BN * BN;
           }
           stb |= hancock_dir<MHD, NDIR, GLM, LIM, 2>(smem, base, strd, rdel[2], dxinv[2], cg, P, acc);
@@ -525,18 +582,18 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
     for (int D = dlo; D < NDIM; ++D) {
       const int nface = D < 2 ? FB : BN * BN;
 #pragma unroll 1
-      // face coordinates and the shared-memory offsets of the 4 stencil
+      // face coordinates and the shared-memory offsets of the 2 HW stencil
       // cells (variable 0) with the per-variable strides
       auto face_at = [&](int f, int &fi, int &fj, int *base, int *strd) {
         if (D == 0) { fj = f / (BN + 1); fi = f - fj * (BN + 1); }
         else { fj = f >> 4; fi = f & (BN - 1); }
 #pragma unroll
-        for (int o = 0; o < 4; ++o) {
+        for (int o = 0; o < H2; ++o) {
           if (D == 2) {
-            base[o] = ((k + o - 1) & 3) * NW * (BN * BN) + f;
+            base[o] = ring_slot<HW>(k + o - HW + 1) * NW * (BN * BN) + f;
             strd[o] = BN * BN;
           } else {
-            tv.addr(slot, D == 0 ? fi + o - 2 : fi, D == 0 ? fj : fj + o - 2, base[o], strd[o]);
+            tv.addr(slot, D == 0 ? fi + o - HW : fi, D == 0 ? fj : fj + o - HW, base[o], strd[o]);
           }
         }
       };
@@ -557,20 +614,48 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
         int fi, fj;
         const TF rd = TF(D == 0 ? rdel[0] : (D == 1 ? rdel[1] : rdel[2]));
         TF wLp[NW], wRp[NW];
-        int base[4], strd[4];
+        int base[H2], strd[H2];
         face_at(f, fi, fj, base, strd);
+        if constexpr (LIM == LIM_MP5) {
+          static_assert(FP64, "MP5 is FP64 only");
+          // MP5limiter, then fix_limiter1 (src/limiter/mod_weno.t:135-163):
+          // a variable keeps the flat states w(i), w(i+1) where phys_check_w
+          // flags it (rho < small_density, p < small_pressure) in either
+          // reconstructed state
 #pragma unroll
-        for (int v = 0; v < NW; ++v) {
-          const int ov = orig_index_rt<MHD, NDIR>(v, D);
-          TF q[4];
+          for (int v = 0; v < NW; ++v) {
+            const int ov = orig_index_rt<MHD, NDIR>(v, D);
+            double q[6];
 #pragma unroll
-          for (int o = 0; o < 4; ++o) q[o] = smem[base[o] + ov * strd[o]];
-          const TF d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
-          wLp[v] = q[1] + TF(0.5) * limited_slope<TF, true, LIM>(P.limiter, d1, d0, rd);
-          wRp[v] = q[2] - TF(0.5) * limited_slope<TF, false, LIM>(P.limiter, d2, d1, rd);
+            for (int o = 0; o < 6; ++o) q[o] = smem[base[o] + ov * strd[o]];
+            wLp[v] = mp5_side(q[0], q[1], q[2], q[3], q[4]);
+            wRp[v] = mp5_side(q[5], q[4], q[3], q[2], q[1]);
+          }
+          // density and energy are not rotated: variable index = tile index
+          if (wLp[V::RHO] < P.small_density || wRp[V::RHO] < P.small_density) {
+            wLp[V::RHO] = smem[base[2] + V::RHO * strd[2]];
+            wRp[V::RHO] = smem[base[3] + V::RHO * strd[3]];
+          }
+          if (wLp[V::E] < P.small_pressure || wRp[V::E] < P.small_pressure) {
+            wLp[V::E] = smem[base[2] + V::E * strd[2]];
+            wRp[V::E] = smem[base[3] + V::E * strd[3]];
+          }
+        } else {
+#pragma unroll
+          for (int v = 0; v < NW; ++v) {
+            const int ov = orig_index_rt<MHD, NDIR>(v, D);
+            TF q[4];
+#pragma unroll
+            for (int o = 0; o < 4; ++o) q[o] = smem[base[o] + ov * strd[o]];
+            const TF d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
+            wLp[v] = q[1] + TF(0.5) * limited_slope<TF, true, LIM>(P.limiter, d1, d0, rd);
+            wRp[v] = q[2] - TF(0.5) * limited_slope<TF, false, LIM>(P.limiter, d2, d1, rd);
+          }
         }
         TF Fr[NW];
-        stb |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, TF(cg), Fr);
+        // the MP5 branch of reconstruct_LR has no small-value fix of the states
+        stb |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, TF(cg), Fr,
+                                                                       LIM != LIM_MP5);
         if constexpr (!FP64) {
           bool finite = true;
 #pragma unroll
@@ -596,7 +681,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
             bool finite = true;
             for (int v = 0; v < NW; ++v) finite = finite && isfinite(tv.fb[v * FB + f]);
             if (finite) continue;
-            int fi, fj, base[4], strd[4];
+            int fi, fj, base[H2], strd[H2];
             face_at(f, fi, fj, base, strd);
             const FaceFlux64<NW> r = face_retry_fp64<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>(
                 smem, D, base[0], base[1], base[2], base[3], strd[0], strd[1], strd[2], strd[3],
@@ -665,7 +750,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? AMRVAC_STAGE_
               auto nbv = [&](int d, int s, int v) -> double {  // wCT at cell +/- e_d
                 if (d == 0) return double(tv.at(slot, v, ci + s, cj));
                 if (d == 1) return double(tv.at(slot, v, ci, cj + s));
-                return double(tv.ring[((((k + s) & 3)) * NW + v) * (BN * BN) + cj * BN + ci]);
+                return double(tv.ring[(ring_slot<HW>(k + s) * NW + v) * (BN * BN) + cj * BN + ci]);
               };
 #pragma unroll
               for (int d = 0; d < NDIM; ++d) {

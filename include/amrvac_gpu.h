@@ -58,6 +58,7 @@ extern "C" {
 #define AMRVAC_LIM_KOREN    7
 #define AMRVAC_LIM_CADA     8
 #define AMRVAC_LIM_CADA3    9
+#define AMRVAC_LIM_MP5      13  /* fifth order, uniform grids, nghostcells >= 3 */
 /* typeboundspeed: src/io/mod_input_output.t:1632-1641 */
 #define AMRVAC_BS_EINFELDT      1
 #define AMRVAC_BS_CMAXMEAN      2

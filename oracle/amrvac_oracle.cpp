@@ -574,13 +574,71 @@ void dwlimiter2(const State &s, const Arr<R> &dwC, const Box &ixC, int idims, do
   });
 }
 
+// MP5limiter (src/limiter/mod_mp5.t:16-201) with its minmod and median
+// (404-432), one variable of one face: the left state at face i+1/2 from
+// w(i-2) .. w(i+2); the right state is the same expression on the data
+// mirrored about the face (w(i+3) .. w(i-1)), term for term the reference's
+// right-side formulas.
+template <class R> R mp5_minmod(R a, R b) {
+  return (rsign(one, a) + rsign(one, b)) / R(2.0) * rmin(rabs(a), rabs(b));
+}
+template <class R> R mp5_median(R a, R b, R c) {
+  R t1 = b - a, t2 = c - a;
+  return a + (rsign(one, t1) + rsign(one, t2)) / R(2.0) * rmin(rabs(t1), rabs(t2));
+}
+template <class R> R mp5_side(R wmm, R wm, R w0, R wp, R wpp) {
+  R f = R(1.0 / 60.0) * ((((R(2.0) * wmm - R(13.0) * wm) + R(47.0) * w0) + R(27.0) * wp) - R(3.0) * wpp);
+  R b = R(4.0) * (w0 - wm);
+  R fmp = w0 + mp5_minmod(wp - w0, b);
+  R ful = w0 + b;
+  R dm = (w0 - R(2.0) * wm) + wmm, d0 = (wp - R(2.0) * w0) + wm, dp = (wpp - R(2.0) * wp) + w0;
+  R dm4_0 = mp5_minmod(mp5_minmod(R(4.0) * d0 - dp, R(4.0) * dp - d0), mp5_minmod(d0, dp));
+  R dm4_m = mp5_minmod(mp5_minmod(R(4.0) * dm - d0, R(4.0) * d0 - dm), mp5_minmod(dm, d0));
+  R fmd = (w0 + wp) / R(2.0) - dm4_0 / R(2.0);
+  R flc = R(half) * (R(3.0) * w0 - wm) + R(4.0 / 3.0) * dm4_m;
+  R fmn = rmax(rmin(rmin(w0, wp), fmd), rmin(rmin(w0, ful), flc));
+  R fmx = rmin(rmax(rmax(w0, wp), fmd), rmax(rmax(w0, ful), flc));
+  if ((f - w0) * (f - fmp) <= R(0.0)) return f;
+  return mp5_median(fmn, f, fmx);
+}
+
 // reconstruct_LR default (limiter) branch (src/mod_finite_volume.t:1110-1228)
+// and its MP5 branch (1131-1132: MP5limiter with fix_limiter1,
+// src/limiter/mod_weno.t:135-163; no small-value fix of the states)
 template <class R>
 int reconstruct_LR(const State &s, const Box &ixL, const Box &ixR, int idims, const Arr<R> &w,
                    Arr<R> &wLC, Arr<R> &wRC, Arr<R> &wLp, Arr<R> &wRp, double dxdim) {
   const Ix &x = s.x;
   const Geo &g = s.g;
   const int o = g.off(idims);
+  if (s.c.limiter == ORC_LIM_MP5) {
+    // faces iL = ixL (ixR == ixL here: finite_volume's ixCR)
+    forbox(ixL, [&](int i, int j, int k) {
+      const size_t p = g.idx(i, j, k);
+      R wl[16], wr[16];
+      for (int iw = 0; iw < x.nw; ++iw) {
+        const R *q = &w.d[p + g.cells * (size_t)iw];
+        wl[iw] = mp5_side(q[-2 * o], q[-o], q[0], q[o], q[2 * o]);
+        wr[iw] = mp5_side(q[3 * o], q[2 * o], q[o], q[0], q[-o]);
+      }
+      // fix_limiter1: phys_check_w flags (primitive) on both states
+      const bool frho = wl[x.rho] < R(s.c.small_density) || wr[x.rho] < R(s.c.small_density);
+      const bool fe = wl[x.e] < R(s.c.small_pressure) || wr[x.e] < R(s.c.small_pressure);
+      for (int iw = 0; iw < x.nw; ++iw) {
+        if ((iw == x.rho && frho) || (iw == x.e && fe)) continue;
+        wLp.d[p + g.cells * (size_t)iw] = wl[iw];
+        wRp.d[p + g.cells * (size_t)iw] = wr[iw];
+      }
+    });
+    for (int iw = 0; iw < x.nw; ++iw) {
+      forbox(ixL, [&](int i, int j, int k) { wLC(i, j, k, iw) = wLp(i, j, k, iw); });
+      forbox(ixR, [&](int i, int j, int k) { wRC(i, j, k, iw) = wRp(i, j, k, iw); });
+    }
+    to_conserved(s, ixL, wLC);
+    to_conserved(s, ixR, wRC);
+    (void)dxdim;
+    return 0;
+  }
   Box jxR = shift(ixR, idims, 1);
   Box ixC;
   for (int d = 0; d < 3; ++d) { ixC.hi[d] = jxR.hi[d]; ixC.lo[d] = ixL.lo[d]; }

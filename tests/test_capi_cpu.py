@@ -145,3 +145,17 @@ def test_time_integrators_are_checked():
     ok = make_cfg(physics="hd", ndim=2, flux_scheme="hll", time_stepper="twostep")
     assert ok.time_stepper == 2 and ok.time_integrator == 0
     assert make_cfg(physics="hd", ndim=2, time_stepper="twostep", time_integrator="ssprk2").time_integrator == 2
+
+
+def test_mp5_needs_three_ghost_cells_and_fp64(lib):
+    """MP5 (limiter 13) is taken with nghostcells >= 3 (make_cfg's default for
+    it) in FP64; two ghost cells or the mixed form are refused before any
+    device call."""
+    from amrvac_b200 import make_cfg, _lib
+    h = ctypes.c_void_p()
+    assert make_cfg(physics="hd", ndim=2, limiter="mp5").nghostcells == 3
+    assert make_cfg(physics="hd", ndim=2).nghostcells == 2
+    bad = make_cfg(physics="hd", ndim=2, flux_scheme="hll", limiter="mp5", nghostcells=2)
+    assert lib.amrvac_gpu_create(ctypes.byref(bad), ctypes.byref(h)) == _lib.E_ARG
+    bad = make_cfg(physics="hd", ndim=2, flux_scheme="hll", limiter="mp5", precision="mixed")
+    assert lib.amrvac_gpu_create(ctypes.byref(bad), ctypes.byref(h)) == _lib.E_UNSUPPORTED
