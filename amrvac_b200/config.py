@@ -112,7 +112,8 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
 
     typeboundary: list of 2*ndim entries (min1, max1, min2, ...), each a name
     applied to all variables or a list of per-variable names.  nghostcells
-    defaults to 3 for mp5 (which needs them) and 2 otherwise.
+    defaults to 3 for the fifth-order reconstructions (mp5, weno5, wenoz5,
+    wenozp5: they need them) and 2 otherwise.
     """
     L = _lib.load()
     c = _lib.AmrvacCfg()
@@ -125,7 +126,8 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
     c.gamma = (5.0 / 3.0) if gamma is None else float(gamma)
     c.flux_scheme = _lib.FS[flux_scheme]
     c.limiter = _lib.LIMITER[limiter]
-    c.nghostcells = int(nghostcells) if nghostcells is not None else (3 if limiter == "mp5" else 2)
+    five = limiter in ("mp5", "weno5", "wenoz5", "wenozp5")
+    c.nghostcells = int(nghostcells) if nghostcells is not None else (3 if five else 2)
     c.typeboundspeed = _lib.BOUNDSPEED[typeboundspeed]
     if typedivbfix is None:
         typedivbfix = "linde" if physics == "mhd" else "none"

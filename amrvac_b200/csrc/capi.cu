@@ -378,12 +378,11 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
     if (k.block_nx[d] != 16) return fail(AMRVAC_E_UNSUPPORTED, "block_nx must be 16");
   if (k.nghostcells < 2) return fail(AMRVAC_E_UNSUPPORTED, "nghostcells must be >= 2");
   if (k.physics != 0 && k.physics != 1) return fail(AMRVAC_E_ARG, "physics must be 0 (hd) or 1 (mhd)");
-  if ((k.limiter < 1 || k.limiter > 9) && k.limiter != AMRVAC_LIM_MP5)
-    return fail(AMRVAC_E_UNSUPPORTED, "limiter not supported");
-  if (k.limiter == AMRVAC_LIM_MP5 && k.nghostcells < 3)
-    return fail(AMRVAC_E_ARG, "mp5 needs nghostcells >= 3");
-  if (k.limiter == AMRVAC_LIM_MP5 && k.precision == 1)
-    return fail(AMRVAC_E_UNSUPPORTED, "mp5 is FP64 only");
+  const bool fifth = k.limiter == AMRVAC_LIM_MP5 || k.limiter == AMRVAC_LIM_WENO5 ||
+                     k.limiter == AMRVAC_LIM_WENOZ5 || k.limiter == AMRVAC_LIM_WENOZP5;
+  if ((k.limiter < 1 || k.limiter > 9) && !fifth) return fail(AMRVAC_E_UNSUPPORTED, "limiter not supported");
+  if (fifth && k.nghostcells < 3) return fail(AMRVAC_E_ARG, "mp5 / weno5 need nghostcells >= 3");
+  if (fifth && k.precision == 1) return fail(AMRVAC_E_UNSUPPORTED, "mp5 / weno5 are FP64 only");
   if (k.typeboundspeed < 1 || k.typeboundspeed > 3) return fail(AMRVAC_E_ARG, "bad typeboundspeed");
   if (k.type_courant < 1 || k.type_courant > 3) return fail(AMRVAC_E_ARG, "bad type_courant");
   if (k.time_stepper < 1 || k.time_stepper > 4) return fail(AMRVAC_E_UNSUPPORTED, "time_stepper not supported");
@@ -414,10 +413,10 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   KernelKey key{k.physics == 1, k.ndim, k.ndir, k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM,
                 k.flux_scheme, k.limiter, k.typeboundspeed, k.precision == 1};
   if (k.precision != 0 && k.precision != 1) return fail(AMRVAC_E_ARG, "precision must be 0 (fp64) or 1 (mixed)");
-  if (std::getenv("AMRVAC_GENERIC_KERNELS") && k.limiter != AMRVAC_LIM_MP5) { key.limiter = 0; key.boundspeed = 0; }
-  bool found = k.limiter == AMRVAC_LIM_MP5
-                   ? (lookup_mp5_hd(key, &c->ks) || lookup_mp5_mhd(key, &c->ks))
-                   : (lookup_hd(key, &c->ks) || lookup_mhd2(key, &c->ks) || lookup_mhd3(key, &c->ks));
+  if (std::getenv("AMRVAC_GENERIC_KERNELS") && !fifth) { key.limiter = 0; key.boundspeed = 0; }
+  if (fifth && k.limiter != AMRVAC_LIM_MP5) key.limiter = LIM_WENO5;  // one kernel family, variant at run time
+  bool found = fifth ? (lookup_mp5_hd(key, &c->ks) || lookup_mp5_mhd(key, &c->ks))
+                     : (lookup_hd(key, &c->ks) || lookup_mhd2(key, &c->ks) || lookup_mhd3(key, &c->ks));
   if (!found) {
     delete c;
     return fail(AMRVAC_E_UNSUPPORTED, key.mixed ? "no mixed-precision kernel for this scheme"

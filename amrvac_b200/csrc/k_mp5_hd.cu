@@ -1,15 +1,20 @@
-// Stage kernels with MP5 reconstruction (three-cell halo) for hydrodynamics,
-// 2-D and 3-D, HLL and HLLC.
+// Stage kernels with the fifth-order reconstructions (three-cell halo) for
+// hydrodynamics, 2-D and 3-D, HLL and HLLC: MP5, and the WENO5 family (one
+// kernel, variant at run time).
 #include "kernels.cuh"
 
 namespace amrvac {
 
 bool lookup_mp5_hd(const KernelKey &k, KernelSet *out) {
-  if (k.mhd || k.mixed || k.limiter != LIM_MP5 || k.ndir != k.ndim) return false;
-#define AMRVAC_MP5_HD(ND, S)                                          \
-  if (k.ndim == ND && k.solver == S) {                                \
-    *out = Launch<false, ND, false, ND, S, LIM_MP5>::set();           \
-    return true;                                                      \
+  if (k.mhd || k.mixed || k.ndir != k.ndim) return false;
+#define AMRVAC_MP5_HD(ND, S)                                                              \
+  if (k.ndim == ND && k.solver == S && k.limiter == LIM_MP5) {                            \
+    *out = Launch<false, ND, false, ND, S, LIM_MP5>::set();                               \
+    return true;                                                                          \
+  }                                                                                       \
+  if (k.ndim == ND && k.solver == S && k.limiter == LIM_WENO5) {                          \
+    *out = Launch<false, ND, false, ND, S, LIM_WENO5>::set();                             \
+    return true;                                                                          \
   }
   AMRVAC_MP5_HD(2, SOLVER_HLL)
   AMRVAC_MP5_HD(2, SOLVER_HLLC)

@@ -262,11 +262,52 @@ __device__ __forceinline__ double mp5_side(double wmm, double wm, double w0, dou
   return mp5_median(fmin_, f, fmax_);
 }
 
+// WENO5 family (WENO5limiter, src/limiter/mod_weno.t:254-377; var 1 WENO-JS,
+// 2 WENO-Z, 3 WENO-Z+ with lambda = dx^(2/3)): the left state at face i+1/2
+// from w(i-2) .. w(i+2); the right state is the same expression on the
+// mirrored data, as for MP5.  Constants as the reference writes them.
+__device__ __forceinline__ double weno5_side(double wmm, double wm, double w0, double wp, double wpp, int var,
+                                             double lambda) {
+  constexpr double eps = 1.0e-18;  // weno_eps_machine
+  constexpr double b1 = 1.0833333333333333, b2 = 0.25;
+  constexpr double d1 = 1.0 / 10.0, d2 = 3.0 / 5.0, d3 = 3.0 / 10.0;
+  const double f1 = (1.0 / 3.0) * wmm + (-7.0 / 6.0) * wm + (11.0 / 6.0) * w0;
+  const double f2 = (-1.0 / 6.0) * wm + (5.0 / 6.0) * w0 + (1.0 / 3.0) * wp;
+  const double f3 = (1.0 / 3.0) * w0 + (5.0 / 6.0) * wp + (-1.0 / 6.0) * wpp;
+  const double s1 = wmm + w0 - 2.0 * wm, t1 = wmm - 4.0 * wm + 3.0 * w0;
+  const double s2 = wm + wp - 2.0 * w0, t2 = wm - wp;
+  const double s3 = w0 + wpp - 2.0 * wp, t3 = 3.0 * w0 - 4.0 * wp + wpp;
+  const double be1 = b1 * (s1 * s1) + b2 * (t1 * t1);
+  const double be2 = b1 * (s2 * s2) + b2 * (t2 * t2);
+  const double be3 = b1 * (s3 * s3) + b2 * (t3 * t3);
+  double a1, a2, a3;
+  if (var == 1) {
+    a1 = d1 / ((be1 + eps) * (be1 + eps));
+    a2 = d2 / ((be2 + eps) * (be2 + eps));
+    a3 = d3 / ((be3 + eps) * (be3 + eps));
+  } else if (var == 2) {
+    const double tau = fabs(be1 - be3);
+    const double r1 = tau / (be1 + eps), r2 = tau / (be2 + eps), r3 = tau / (be3 + eps);
+    a1 = d1 * (1.0 + r1 * r1);
+    a2 = d2 * (1.0 + r2 * r2);
+    a3 = d3 * (1.0 + r3 * r3);
+  } else {
+    const double tau = fabs(be1 - be3);
+    const double r1 = (tau + eps) / (be1 + eps), r2 = (tau + eps) / (be2 + eps), r3 = (tau + eps) / (be3 + eps);
+    a1 = d1 * (1.0 + r1 * r1 + lambda / r1);
+    a2 = d2 * (1.0 + r2 * r2 + lambda / r2);
+    a3 = d3 * (1.0 + r3 * r3 + lambda / r3);
+  }
+  const double asum = ((0.0 + a1) + a2) + a3;
+  return ((0.0 + f1 * a1 / asum) + f2 * a2 / asum) + f3 * a3 / asum;
+}
+
 // Halo width of the staged tile: two cells for the slope limiters, three for
-// MP5 (its face stencil spans cells i-2 .. i+3).
+// the fifth-order reconstructions (face stencil i-2 .. i+3).  LIM_WENO5 as a
+// template argument stands for the whole WENO5 family (variant at run time).
 template <int LIM>
 struct HaloW {
-  static constexpr int value = LIM == LIM_MP5 ? 3 : 2;
+  static constexpr int value = (LIM == LIM_MP5 || LIM == LIM_WENO5) ? 3 : 2;
 };
 
 // Shared-memory tile (sizes in doubles), halo width HW.
@@ -432,7 +473,7 @@ __device__ __forceinline__ uint32_t hancock_dir(const double *smem, const int *b
 // the shared memory of the 3-D MHD tile, and the registers it frees avoid
 // spills in the 6-cell face stencil.
 template <class TF, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS>
-__global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (LIM == LIM_MP5 ? 1 : AMRVAC_STAGE_MINB)
+__global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::value == 3 ? 1 : AMRVAC_STAGE_MINB)
                                                                  : AMRVAC_STAGE_MINB_MIXED)
     fv_stage_kernel(const StageArgs A) {
   using V = Vars<MHD, NDIR, GLM>;
@@ -483,12 +524,14 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (LIM == LIM_M
   uint32_t stb = 0;  // status of this block's update
   const int amr_mask = A.amr_face ? A.amr_face[b] : 0;
   double dx[3], dxinv[3], rdel[3];
+  [[maybe_unused]] double wlam[3];  // WENO-Z+: dx^(2/3) per direction
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     dx[d] = d < NDIM ? A.dxb[b * 3 + d] : 1.0;
     dxinv[d] = -qdt / dx[d];
     const double r = P.cada3_radius * dx[d];
     rdel[d] = 1.0 / (r * r);
+    if constexpr (LIM == LIM_WENO5) wlam[d] = pow(dx[d], 2.0 / 3.0);
   }
   double fz_prev[NDIM == 3 ? NW : 1];
 #pragma unroll
@@ -640,6 +683,31 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (LIM == LIM_M
             wLp[V::E] = smem[base[2] + V::E * strd[2]];
             wRp[V::E] = smem[base[3] + V::E * strd[3]];
           }
+        } else if constexpr (LIM == LIM_WENO5) {
+          static_assert(FP64, "WENO5 is FP64 only");
+          // WENO5limiter, then fix_limiter (src/limiter/mod_weno.t:100-133): a
+          // flagged density or pressure in either state makes every variable
+          // of the face take the flat states w(i), w(i+1)
+          const int var = P.limiter == LIM_WENO5 ? 1 : (P.limiter == LIM_WENOZ5 ? 2 : 3);
+          const double lam = D == 0 ? wlam[0] : (D == 1 ? wlam[1] : wlam[2]);
+#pragma unroll
+          for (int v = 0; v < NW; ++v) {
+            const int ov = orig_index_rt<MHD, NDIR>(v, D);
+            double q[6];
+#pragma unroll
+            for (int o = 0; o < 6; ++o) q[o] = smem[base[o] + ov * strd[o]];
+            wLp[v] = weno5_side(q[0], q[1], q[2], q[3], q[4], var, lam);
+            wRp[v] = weno5_side(q[5], q[4], q[3], q[2], q[1], var, lam);
+          }
+          if (wLp[V::RHO] < P.small_density || wRp[V::RHO] < P.small_density || wLp[V::E] < P.small_pressure ||
+              wRp[V::E] < P.small_pressure) {
+#pragma unroll
+            for (int v = 0; v < NW; ++v) {
+              const int ov = orig_index_rt<MHD, NDIR>(v, D);
+              wLp[v] = smem[base[2] + ov * strd[2]];
+              wRp[v] = smem[base[3] + ov * strd[3]];
+            }
+          }
         } else {
 #pragma unroll
           for (int v = 0; v < NW; ++v) {
@@ -653,9 +721,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (LIM == LIM_M
           }
         }
         TF Fr[NW];
-        // the MP5 branch of reconstruct_LR has no small-value fix of the states
+        // the MP5 / WENO branches of reconstruct_LR have no small-value fix of
+        // the states
         stb |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, TF(cg), Fr,
-                                                                       LIM != LIM_MP5);
+                                                                       HW == 2);
         if constexpr (!FP64) {
           bool finite = true;
 #pragma unroll

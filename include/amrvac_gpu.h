@@ -59,6 +59,9 @@ extern "C" {
 #define AMRVAC_LIM_CADA     8
 #define AMRVAC_LIM_CADA3    9
 #define AMRVAC_LIM_MP5      13  /* fifth order, uniform grids, nghostcells >= 3 */
+#define AMRVAC_LIM_WENO5    16  /* WENO-JS, likewise */
+#define AMRVAC_LIM_WENOZ5   18  /* WENO-Z, likewise */
+#define AMRVAC_LIM_WENOZP5  20  /* WENO-Z+, likewise */
 /* typeboundspeed: src/io/mod_input_output.t:1632-1641 */
 #define AMRVAC_BS_EINFELDT      1
 #define AMRVAC_BS_CMAXMEAN      2

@@ -602,6 +602,42 @@ template <class R> R mp5_side(R wmm, R wm, R w0, R wp, R wpp) {
   return mp5_median(fmn, f, fmx);
 }
 
+// WENO5limiter (src/limiter/mod_weno.t:254-377), one variable of one face;
+// var 1 WENO-JS, 2 WENO-Z, 3 WENO-Z+ (lambda = dx^(2/3)).  Left state from
+// w(i-2) .. w(i+2); the right state is the same expression on the mirrored
+// data, term for term the reference's right-side formulas.
+template <class R> R weno5_side(R wmm, R wm, R w0, R wp, R wpp, int var, R lambda) {
+  const double eps = 1.0e-18;  // weno_eps_machine
+  const double b1 = 1.0833333333333333, b2 = 0.25;
+  const double d[3] = {1.0 / 10.0, 3.0 / 5.0, 3.0 / 10.0};
+  R f[3], be[3], a[3];
+  f[0] = R(1.0 / 3.0) * wmm + R(-7.0 / 6.0) * wm + R(11.0 / 6.0) * w0;
+  f[1] = R(-1.0 / 6.0) * wm + R(5.0 / 6.0) * w0 + R(1.0 / 3.0) * wp;
+  f[2] = R(1.0 / 3.0) * w0 + R(5.0 / 6.0) * wp + R(-1.0 / 6.0) * wpp;
+  R s1 = wmm + w0 - R(2.0) * wm, t1 = wmm - R(4.0) * wm + R(3.0) * w0;
+  R s2 = wm + wp - R(2.0) * w0, t2 = wm - wp;
+  R s3 = w0 + wpp - R(2.0) * wp, t3 = R(3.0) * w0 - R(4.0) * wp + wpp;
+  be[0] = R(b1) * (s1 * s1) + R(b2) * (t1 * t1);
+  be[1] = R(b1) * (s2 * s2) + R(b2) * (t2 * t2);
+  be[2] = R(b1) * (s3 * s3) + R(b2) * (t3 * t3);
+  const R tau = rabs(be[0] - be[2]);
+  for (int i = 0; i < 3; ++i) {
+    if (var == 1) {
+      a[i] = R(d[i]) / ((be[i] + R(eps)) * (be[i] + R(eps)));
+    } else if (var == 2) {
+      R r = tau / (be[i] + R(eps));
+      a[i] = R(d[i]) * (R(1.0) + r * r);
+    } else {
+      R r = (tau + R(eps)) / (be[i] + R(eps));
+      a[i] = R(d[i]) * (R(1.0) + r * r + lambda / r);
+    }
+  }
+  R asum = ((R(0.0) + a[0]) + a[1]) + a[2];
+  R out(0.0);
+  for (int i = 0; i < 3; ++i) out = out + f[i] * a[i] / asum;
+  return out;
+}
+
 // reconstruct_LR default (limiter) branch (src/mod_finite_volume.t:1110-1228)
 // and its MP5 branch (1131-1132: MP5limiter with fix_limiter1,
 // src/limiter/mod_weno.t:135-163; no small-value fix of the states)
@@ -611,6 +647,35 @@ int reconstruct_LR(const State &s, const Box &ixL, const Box &ixR, int idims, co
   const Ix &x = s.x;
   const Geo &g = s.g;
   const int o = g.off(idims);
+  if (s.c.limiter == ORC_LIM_WENO5 || s.c.limiter == ORC_LIM_WENOZ5 || s.c.limiter == ORC_LIM_WENOZP5) {
+    // WENO5limiter then fix_limiter (src/limiter/mod_weno.t:100-133): any
+    // flagged density or pressure keeps every variable of the face flat
+    const int var = s.c.limiter == ORC_LIM_WENO5 ? 1 : (s.c.limiter == ORC_LIM_WENOZ5 ? 2 : 3);
+    const R lambda = R(std::pow(dxdim, 2.0 / 3.0));
+    forbox(ixL, [&](int i, int j, int k) {
+      const size_t p = g.idx(i, j, k);
+      R wl[16], wr[16];
+      for (int iw = 0; iw < x.nw; ++iw) {
+        const R *q = &w.d[p + g.cells * (size_t)iw];
+        wl[iw] = weno5_side(q[-2 * o], q[-o], q[0], q[o], q[2 * o], var, lambda);
+        wr[iw] = weno5_side(q[3 * o], q[2 * o], q[o], q[0], q[-o], var, lambda);
+      }
+      const bool flag = wl[x.rho] < R(s.c.small_density) || wr[x.rho] < R(s.c.small_density) ||
+                        wl[x.e] < R(s.c.small_pressure) || wr[x.e] < R(s.c.small_pressure);
+      if (flag) return;
+      for (int iw = 0; iw < x.nw; ++iw) {
+        wLp.d[p + g.cells * (size_t)iw] = wl[iw];
+        wRp.d[p + g.cells * (size_t)iw] = wr[iw];
+      }
+    });
+    for (int iw = 0; iw < x.nw; ++iw) {
+      forbox(ixL, [&](int i, int j, int k) { wLC(i, j, k, iw) = wLp(i, j, k, iw); });
+      forbox(ixR, [&](int i, int j, int k) { wRC(i, j, k, iw) = wRp(i, j, k, iw); });
+    }
+    to_conserved(s, ixL, wLC);
+    to_conserved(s, ixR, wRC);
+    return 0;
+  }
   if (s.c.limiter == ORC_LIM_MP5) {
     // faces iL = ixL (ixR == ixL here: finite_volume's ixCR)
     forbox(ixL, [&](int i, int j, int k) {

@@ -155,6 +155,7 @@ def test_mp5_needs_three_ghost_cells_and_fp64(lib):
     h = ctypes.c_void_p()
     assert make_cfg(physics="hd", ndim=2, limiter="mp5").nghostcells == 3
     assert make_cfg(physics="hd", ndim=2).nghostcells == 2
+    assert make_cfg(physics="hd", ndim=2, limiter="wenozp5").nghostcells == 3
     bad = make_cfg(physics="hd", ndim=2, flux_scheme="hll", limiter="mp5", nghostcells=2)
     assert lib.amrvac_gpu_create(ctypes.byref(bad), ctypes.byref(h)) == _lib.E_ARG
     bad = make_cfg(physics="hd", ndim=2, flux_scheme="hll", limiter="mp5", precision="mixed")

@@ -1,4 +1,5 @@
-"""MP5 reconstruction (three ghost cells) on the GPU against the oracle.
+"""Fifth-order reconstructions (three ghost cells) on the GPU against the
+oracle: MP5 and the WENO5 family.
 
 The stage kernel stages a three-cell halo (a six-plane z ring in 3-D) and
 reconstructs each face from six cells with MP5limiter's formulas, then
@@ -27,6 +28,15 @@ CASES = {
     "mhd3_hlld_mp5_glm": dict(physics="mhd", ndim=3, flux_scheme="hlld", typedivbfix="glm"),
     "mhd3_hll_mp5_glm_pc": dict(physics="mhd", ndim=3, flux_scheme="hll", typedivbfix="glm",
                                 time_stepper="twostep"),
+    # the WENO5 family (WENO5limiter: JS, Z, Z+)
+    "hd2_hllc_weno5": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hllc", limiter="weno5"),
+    "hd2_hll_wenozp5_cont": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll", limiter="wenozp5",
+                                 bc=["cont"] * 4),
+    "hd3_hll_wenoz5": dict(physics="hd", ndim=3, gamma=1.4, flux_scheme="hll", limiter="wenoz5"),
+    "mhd2_hll_weno5_linde": dict(physics="mhd", ndim=2, flux_scheme="hll", limiter="weno5", typedivbfix="linde"),
+    "mhd25_hlld_wenozp5_glm": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hlld", limiter="wenozp5",
+                                   typedivbfix="glm"),
+    "mhd3_hlld_wenoz5_glm": dict(physics="mhd", ndim=3, flux_scheme="hlld", limiter="wenoz5", typedivbfix="glm"),
 }
 
 
@@ -41,14 +51,15 @@ def _setup(oracle_lib, name, n=32):
     O = oracle_lib
     kw = dict(CASES[name])
     bc = kw.pop("bc", None)
+    limiter = kw.pop("limiter", "mp5")
     ndim = kw["ndim"]
     ndir = kw.get("ndir", ndim)
     bc = bc or ["periodic"] * (2 * ndim)
-    gcfg = make_cfg(typeboundary=bc, limiter="mp5", **kw)
+    gcfg = make_cfg(typeboundary=bc, limiter=limiter, **kw)
     assert gcfg.nghostcells == 3
     ok = dict(kw)
     div = ok.pop("typedivbfix", "none")
-    ocfg = O.make_cfg(divb=div, limiter="mp5", nghost=3, **ok)
+    ocfg = O.make_cfg(divb=div, limiter=limiter, nghost=3, **ok)
     glm = kw.get("typedivbfix") == "glm"
     prim = P.random_smooth(kw["physics"], ndim, ndir, n, seed=P.SEED, glm=glm)
     cons = P.prim_to_cons(prim, kw["physics"], ndir, ocfg.gamma)
@@ -136,11 +147,11 @@ def test_mp5_conserves_on_periodic_domain(oracle_lib):
     assert np.all(np.abs(after - before) <= 1e-13 * scale)
 
 
-def _device_l1_error(n, tend=0.1):
+def _device_l1_error(n, limiter="mp5", tend=0.1):
     """The oracle-side accuracy pin (tests/test_oracle_mp5_cpu.py) on the
     device: a smooth density wave advected at v = (1, 0)."""
     from amrvac_b200 import Context, make_cfg
-    cfg = make_cfg(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll", limiter="mp5", courantpar=0.1)
+    cfg = make_cfg(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll", limiter=limiter, courantpar=0.1)
     x = (np.arange(n) + 0.5) / n
     X, _ = np.meshgrid(x, x, indexing="xy")
     k, h = 2.0 * np.pi, 1.0 / n
@@ -165,7 +176,8 @@ def _device_l1_error(n, tend=0.1):
     return float(np.abs(got[:, 0] - ex[:, 0]).mean())
 
 
-def test_mp5_fifth_order_on_smooth_wave():
+@pytest.mark.parametrize("limiter", ["mp5", "weno5", "wenoz5", "wenozp5"])
+def test_fifth_order_on_smooth_wave(limiter):
     _cuda()
-    e32, e64 = _device_l1_error(32), _device_l1_error(64)
+    e32, e64 = _device_l1_error(32, limiter), _device_l1_error(64, limiter)
     assert 24.0 < e32 / e64 < 40.0, (e32, e64)

@@ -1,4 +1,4 @@
-"""Known-answer accuracy pin of the oracle's MP5 restatement.
+"""Known-answer accuracy pin of the oracle's MP5 and WENO5 restatements.
 
 A density wave rho = 1 + 0.2 sin(2 pi x) advected at v = (1, 0) with
 constant pressure is an exact solution of the Euler equations (translation);
@@ -6,7 +6,9 @@ starting from exact cell averages, a fifth-order reconstruction (MP5limiter,
 src/limiter/mod_mp5.t:16-201: the (2, -13, 47, 27, -3)/60 interpolant with
 its monotonicity limits inactive on smooth data) must cut the L1 error of the
 cell averages by about 2^5 per doubling of the resolution when the time
-error is small (CFL 0.1).  Slope limiters stay near second order.
+error is small (CFL 0.1); so must the WENO5 family (WENO5limiter,
+src/limiter/mod_weno.t:254-377: WENO-JS, WENO-Z, WENO-Z+).  Slope limiters
+stay near second order.
 """
 import numpy as np
 import pytest
@@ -44,7 +46,9 @@ def _l1_error(O, n, limiter, nghost, cfl=0.1, tend=0.1):
     return float(np.abs(got[:, 0] - ex[:, 0]).mean())
 
 
-@pytest.mark.parametrize("limiter,nghost,lo,hi", [("mp5", 3, 24.0, 40.0), ("minmod", 2, 2.5, 4.5)])
+@pytest.mark.parametrize("limiter,nghost,lo,hi", [("mp5", 3, 24.0, 40.0), ("weno5", 3, 24.0, 40.0),
+                                                   ("wenoz5", 3, 24.0, 40.0), ("wenozp5", 3, 24.0, 40.0),
+                                                   ("minmod", 2, 2.5, 4.5)])
 def test_convergence_order_on_smooth_wave(oracle_lib, limiter, nghost, lo, hi):
     e32 = _l1_error(oracle_lib, 32, limiter, nghost)
     e64 = _l1_error(oracle_lib, 64, limiter, nghost)
