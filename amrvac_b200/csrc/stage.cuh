@@ -321,7 +321,8 @@ struct Tile {
   static constexpr int HY = NW * H2 * BN;                // [v][r][i] r: j likewise
   static constexpr int HC = NW * H2 * H2;                // [v][r][c] corners
   static constexpr int FB = NW * (BN + 1) * BN;          // [v][face]
-  static constexpr int TOTAL = RING + HX + HY + HC + FB;
+  static constexpr int YX = NW * BN;                     // [v][i] y-faces of the top row (j = BN)
+  static constexpr int TOTAL = RING + HX + HY + HC + FB + YX;
   static constexpr size_t BYTES = sizeof(TF) * TOTAL;
 };
 
@@ -339,7 +340,7 @@ __device__ __forceinline__ int ring_slot(int k) {
 template <class TF, int NW, int NDIM, int HW = 2>
 struct TileView {
   static constexpr int H2 = 2 * HW;
-  TF *ring, *hx, *hy, *hc, *fb;
+  TF *ring, *hx, *hy, *hc, *fb, *yx;
   __device__ TileView(TF *s) {
     using T = Tile<TF, NW, NDIM, HW>;
     ring = s;
@@ -347,6 +348,7 @@ struct TileView {
     hy = hx + T::HX;
     hc = hy + T::HY;
     fb = hc + T::HC;
+    yx = fb + T::FB;
   }
   // primitive v at in-plane (i, j) in [-HW, BN+HW-1]^2 of the plane held in `slot`
   __device__ __forceinline__ TF at(int slot, int v, int i, int j) const {
@@ -620,45 +622,59 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
     } else {
     // ---- face phases x, y (plane k) and z (face k+1/2 of every column); one
     // copy of the face code serves all three through the state rotation.
+    // The x phase also computes the 16 y-faces of the top row (j = BN) into
+    // tv.yx: 272 x-faces + 16 = 288 faces make its second round one full warp,
+    // and the y phase one round of 256 (instead of two rounds of 256 + 16).
     const int dlo = update ? 0 : (NDIM == 3 && k == k0 - 1 ? 2 : NDIM);
 #pragma unroll 1
     for (int D = dlo; D < NDIM; ++D) {
-      const int nface = D < 2 ? FB : BN * BN;
-#pragma unroll 1
+      const int nface = D == 0 ? FB + BN : BN * BN;
+      // direction FD and index fl (in that direction's face layout) of face f
+      // of this phase
+      auto face_dir = [&](int f, int &FD, int &fl) {
+        if (D == 0 && f >= FB) { FD = 1; fl = BN * BN + (f - FB); }
+        else { FD = D; fl = f; }
+      };
+      // where the flux of variable ov of face f lives
+      auto flux_ref = [&](int f, int FD, int fl, int ov) -> TF & {
+        return FD == D ? tv.fb[ov * FB + f] : tv.yx[ov * BN + (fl - BN * BN)];
+      };
       // face coordinates and the shared-memory offsets of the 2 HW stencil
       // cells (variable 0) with the per-variable strides
-      auto face_at = [&](int f, int &fi, int &fj, int *base, int *strd) {
-        if (D == 0) { fj = f / (BN + 1); fi = f - fj * (BN + 1); }
-        else { fj = f >> 4; fi = f & (BN - 1); }
+      auto face_at = [&](int FD, int fl, int &fi, int &fj, int *base, int *strd) {
+        if (FD == 0) { fj = fl / (BN + 1); fi = fl - fj * (BN + 1); }
+        else { fj = fl >> 4; fi = fl & (BN - 1); }
 #pragma unroll
         for (int o = 0; o < H2; ++o) {
-          if (D == 2) {
-            base[o] = ring_slot<HW>(k + o - HW + 1) * NW * (BN * BN) + f;
+          if (FD == 2) {
+            base[o] = ring_slot<HW>(k + o - HW + 1) * NW * (BN * BN) + fl;
             strd[o] = BN * BN;
           } else {
-            tv.addr(slot, D == 0 ? fi + o - HW : fi, D == 0 ? fj : fj + o - HW, base[o], strd[o]);
+            tv.addr(slot, FD == 0 ? fi + o - HW : fi, FD == 0 ? fj : fj + o - HW, base[o], strd[o]);
           }
         }
       };
       // level jump across this block face: keep the boundary face flux
       // (store_flux, src/mod_fix_conserve.t:597-648) for the flux fix
-      auto capture = [&](int fi, int fj, const TF *Fr, double sc) {
-        const int pos = D == 0 ? fi : (D == 1 ? fj : k + 1);
+      auto capture = [&](int FD, int fi, int fj, const TF *Fr, double sc) {
+        const int pos = FD == 0 ? fi : (FD == 1 ? fj : k + 1);
         const int side = pos == 0 ? 0 : (pos == BN ? 1 : -1);
-        if (side >= 0 && ((amr_mask >> (2 * D + side)) & 1)) {
-          const int ta = D == 0 ? fj : fi, tb = D == 2 ? fj : k;
-          double *pf = A.pflux + ((size_t)A.gslot[b] * (2 * NDIM) + 2 * D + side) * NW * (BN * BN);
+        if (side >= 0 && ((amr_mask >> (2 * FD + side)) & 1)) {
+          const int ta = FD == 0 ? fj : fi, tb = FD == 2 ? fj : k;
+          double *pf = A.pflux + ((size_t)A.gslot[b] * (2 * NDIM) + 2 * FD + side) * NW * (BN * BN);
 #pragma unroll
           for (int v = 0; v < NW; ++v)
-            pf[orig_index_rt<MHD, NDIR>(v, D) * (BN * BN) + ta + BN * (NDIM == 3 ? tb : 0)] = sc * double(Fr[v]);
+            pf[orig_index_rt<MHD, NDIR>(v, FD) * (BN * BN) + ta + BN * (NDIM == 3 ? tb : 0)] = sc * double(Fr[v]);
         }
       };
+#pragma unroll 1
       for (int f = t; f < nface; f += STAGE_THREADS) {
-        int fi, fj;
-        const TF rd = TF(D == 0 ? rdel[0] : (D == 1 ? rdel[1] : rdel[2]));
+        int fi, fj, FD, fl;
+        face_dir(f, FD, fl);
+        const TF rd = TF(FD == 0 ? rdel[0] : (FD == 1 ? rdel[1] : rdel[2]));
         TF wLp[NW], wRp[NW];
         int base[H2], strd[H2];
-        face_at(f, fi, fj, base, strd);
+        face_at(FD, fl, fi, fj, base, strd);
         if constexpr (LIM == LIM_MP5) {
           static_assert(FP64, "MP5 is FP64 only");
           // MP5limiter, then fix_limiter1 (src/limiter/mod_weno.t:135-163):
@@ -667,7 +683,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
           // reconstructed state
 #pragma unroll
           for (int v = 0; v < NW; ++v) {
-            const int ov = orig_index_rt<MHD, NDIR>(v, D);
+            const int ov = orig_index_rt<MHD, NDIR>(v, FD);
             double q[6];
 #pragma unroll
             for (int o = 0; o < 6; ++o) q[o] = smem[base[o] + ov * strd[o]];
@@ -689,10 +705,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
           // flagged density or pressure in either state makes every variable
           // of the face take the flat states w(i), w(i+1)
           const int var = P.limiter == LIM_WENO5 ? 1 : (P.limiter == LIM_WENOZ5 ? 2 : 3);
-          const double lam = D == 0 ? wlam[0] : (D == 1 ? wlam[1] : wlam[2]);
+          const double lam = FD == 0 ? wlam[0] : (FD == 1 ? wlam[1] : wlam[2]);
 #pragma unroll
           for (int v = 0; v < NW; ++v) {
-            const int ov = orig_index_rt<MHD, NDIR>(v, D);
+            const int ov = orig_index_rt<MHD, NDIR>(v, FD);
             double q[6];
 #pragma unroll
             for (int o = 0; o < 6; ++o) q[o] = smem[base[o] + ov * strd[o]];
@@ -703,7 +719,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
               wRp[V::E] < P.small_pressure) {
 #pragma unroll
             for (int v = 0; v < NW; ++v) {
-              const int ov = orig_index_rt<MHD, NDIR>(v, D);
+              const int ov = orig_index_rt<MHD, NDIR>(v, FD);
               wLp[v] = smem[base[2] + ov * strd[2]];
               wRp[v] = smem[base[3] + ov * strd[3]];
             }
@@ -711,7 +727,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
         } else {
 #pragma unroll
           for (int v = 0; v < NW; ++v) {
-            const int ov = orig_index_rt<MHD, NDIR>(v, D);
+            const int ov = orig_index_rt<MHD, NDIR>(v, FD);
             TF q[4];
 #pragma unroll
             for (int o = 0; o < 4; ++o) q[o] = smem[base[o] + ov * strd[o]];
@@ -733,35 +749,37 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
         }
         // FP64: the scaled flux fC = -qdt/dx * f as in the reference; mixed:
         // the FP32 flux, scaled in FP64 by the accumulating cell thread
-        const double sc = D == 0 ? dxinv[0] : (D == 1 ? dxinv[1] : dxinv[2]);
+        const double sc = FD == 0 ? dxinv[0] : (FD == 1 ? dxinv[1] : dxinv[2]);
 #pragma unroll
         for (int v = 0; v < NW; ++v) {
-          const int ov = orig_index_rt<MHD, NDIR>(v, D);
-          if constexpr (FP64) tv.fb[ov * FB + f] = sc * Fr[v];
-          else tv.fb[ov * FB + f] = Fr[v];
+          const int ov = orig_index_rt<MHD, NDIR>(v, FD);
+          if constexpr (FP64) flux_ref(f, FD, fl, ov) = sc * Fr[v];
+          else flux_ref(f, FD, fl, ov) = Fr[v];
         }
-        if (amr_mask) capture(fi, fj, Fr, sc);
+        if (amr_mask) capture(FD, fi, fj, Fr, sc);
       }
       __syncthreads();
       if constexpr (!FP64) {
         if (s_retry) {  // fix-up pass: the faces whose FP32 flux is not finite, in FP64
-          const double sc = D == 0 ? dxinv[0] : (D == 1 ? dxinv[1] : dxinv[2]);
           for (int f = t; f < nface; f += STAGE_THREADS) {
+            int FD, fl;
+            face_dir(f, FD, fl);
             bool finite = true;
-            for (int v = 0; v < NW; ++v) finite = finite && isfinite(tv.fb[v * FB + f]);
+            for (int v = 0; v < NW; ++v) finite = finite && isfinite(flux_ref(f, FD, fl, v));
             if (finite) continue;
+            const double sc = FD == 0 ? dxinv[0] : (FD == 1 ? dxinv[1] : dxinv[2]);
             int fi, fj, base[H2], strd[H2];
-            face_at(f, fi, fj, base, strd);
+            face_at(FD, fl, fi, fj, base, strd);
             const FaceFlux64<NW> r = face_retry_fp64<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>(
-                smem, D, base[0], base[1], base[2], base[3], strd[0], strd[1], strd[2], strd[3],
-                D == 0 ? rdel[0] : (D == 1 ? rdel[1] : rdel[2]), cg, P);
+                smem, FD, base[0], base[1], base[2], base[3], strd[0], strd[1], strd[2], strd[3],
+                FD == 0 ? rdel[0] : (FD == 1 ? rdel[1] : rdel[2]), cg, P);
             stb |= r.st;
             TF Fr[NW];
             for (int v = 0; v < NW; ++v) {
               Fr[v] = TF(r.F[v]);
-              tv.fb[orig_index_rt<MHD, NDIR>(v, D) * FB + f] = Fr[v];
+              flux_ref(f, FD, fl, orig_index_rt<MHD, NDIR>(v, FD)) = Fr[v];
             }
-            if (amr_mask) capture(fi, fj, Fr, sc);
+            if (amr_mask) capture(FD, fi, fj, Fr, sc);
           }
           __syncthreads();
           if (t == 0) s_retry = 0;
@@ -780,8 +798,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
           const int f = cj * BN + ci;
 #pragma unroll
           for (int v = 0; v < NW; ++v) {
-            if constexpr (FP64) acc[v] = acc[v] + tv.fb[v * FB + f + BN] - tv.fb[v * FB + f];
-            else acc[v] = acc[v] + sc * double(tv.fb[v * FB + f + BN]) - sc * double(tv.fb[v * FB + f]);
+            // the face above the top row was computed in the x phase
+            const TF up = cj == BN - 1 ? tv.yx[v * BN + ci] : tv.fb[v * FB + f + BN];
+            if constexpr (FP64) acc[v] = acc[v] + up - tv.fb[v * FB + f];
+            else acc[v] = acc[v] + sc * double(up) - sc * double(tv.fb[v * FB + f]);
           }
         } else if constexpr (NDIM == 3) {
 #pragma unroll
