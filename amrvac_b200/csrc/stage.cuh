@@ -814,7 +814,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
           }
         }
       }
-      __syncthreads();
+      // the next phase overwrites the face buffer; after the last phase the
+      // barrier at the end of the plane orders the reads against the next
+      // plane's writes
+      if (D < NDIM - 1) __syncthreads();
     }
     }  // face phases
     if (update && cell_thread) {
