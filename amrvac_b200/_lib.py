@@ -27,8 +27,8 @@ BOUNDSPEED = {"Einfeldt": 1, "cmaxmean": 2, "cmaxleftright": 3}
 DIVB = {"none": 0, "glm": 1, "linde": 4}
 COURANT = {"maxsum": 1, "summax": 2, "minimum": 3}
 BC = {"periodic": 0, "cont": 1, "symm": 2, "asymm": 3}
-TIME_STEPPER = {"onestep": 1, "twostep": 2, "threestep": 3, "fourstep": 4}
-TIME_INTEGRATOR = {"default": 0, "Predictor_Corrector": 0, "ssprk4": 0, "ssprk3": 0, "Forward_Euler": 0, "rk4": 1,
+TIME_STEPPER = {"onestep": 1, "twostep": 2, "threestep": 3, "fourstep": 4, "fivestep": 5}
+TIME_INTEGRATOR = {"default": 0, "Predictor_Corrector": 0, "ssprk5": 0, "ssprk4": 0, "ssprk3": 0, "Forward_Euler": 0, "rk4": 1,
                    "ssprk2": 2}
 PRECISION = {"fp64": 0, "mixed": 1}
 

@@ -194,6 +194,8 @@ def config_from_par(paths) -> RunConfig:
         raise ValueError(f"time_integrator {integ} not supported")
     if ts == "fourstep" and integ not in (None, "ssprk4", "rk4"):
         raise ValueError(f"time_integrator {integ} not supported")
+    if ts == "fivestep" and integ not in (None, "ssprk5"):
+        raise ValueError(f"time_integrator {integ} not supported")
     cfg_kw = dict(
         physics=physics, ndim=ndim,
         gamma=plist.get(f"{physics}_gamma", None),

@@ -218,6 +218,32 @@ cudaError_t launch_rk4_combine(double *u0, const double *u1, const double *u2, c
   return cudaGetLastError();
 }
 
+// fivestep ssprk5 combinations (src/mod_advance.t:534-550): ps3 = a53 ps2 +
+// a54 ps1, and ps = ps3 + a55 ps2 + r (ps2 - (a41 ps + a44 ps1)) with
+// r = beta54 / beta44, each in the reference's order of operations.
+__global__ void ssprk5_ps3_kernel(double *__restrict__ u3, const double *__restrict__ u2,
+                                  const double *__restrict__ u1, double a53, double a54, size_t n) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    u3[e] = a53 * u2[e] + a54 * u1[e];
+}
+__global__ void ssprk5_final_kernel(double *__restrict__ u0, const double *__restrict__ u1,
+                                    const double *__restrict__ u2, const double *__restrict__ u3, double a55,
+                                    double r, double a41, double a44, size_t n) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    u0[e] = (u3[e] + a55 * u2[e]) + r * (u2[e] - (a41 * u0[e] + a44 * u1[e]));
+}
+
+cudaError_t launch_ssprk5_ps3(double *u3, const double *u2, const double *u1, double a53, double a54, size_t n,
+                              cudaStream_t s) {
+  ssprk5_ps3_kernel<<<4 * 148, 256, 0, s>>>(u3, u2, u1, a53, a54, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_ssprk5_final(double *u0, const double *u1, const double *u2, const double *u3, double a55,
+                                double r, double a41, double a44, size_t n, cudaStream_t s) {
+  ssprk5_final_kernel<<<4 * 148, 256, 0, s>>>(u0, u1, u2, u3, a55, r, a41, a44, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_setdt_finalize(unsigned long long *red, double *scal, uint32_t *status, cudaStream_t s) {
   setdt_finalize_kernel<<<1, 1, 0, s>>>(red, scal, status);
   return cudaGetLastError();

@@ -28,6 +28,10 @@ cudaError_t launch_pack(const double *pool, double *dst, int first, int n, int n
                         const int *nbr, const SrlMaps &maps, const BcSpec &bc, const double *gbuf, cudaStream_t s);
 cudaError_t launch_setdt_finalize(unsigned long long *red, double *scal, uint32_t *status, cudaStream_t s);
 cudaError_t launch_advance_time(double *scal, cudaStream_t s);
+cudaError_t launch_ssprk5_ps3(double *u3, const double *u2, const double *u1, double a53, double a54, size_t n,
+                              cudaStream_t s);
+cudaError_t launch_ssprk5_final(double *u0, const double *u1, const double *u2, const double *u3, double a55,
+                                double r, double a41, double a44, size_t n, cudaStream_t s);
 cudaError_t launch_rk4_combine(double *u0, const double *u1, const double *u2, const double *u3, size_t n,
                                cudaStream_t s);
 cudaError_t launch_restore_blocks(const double *wct, double *wnew, const uint32_t *block_status, int nblocks,

@@ -277,6 +277,62 @@ int launch_fourstep(amrvac_ctx *c, cudaEvent_t *ev) {
   return r;
 }
 
+// fivestep ssprk5 (src/mod_advance.t:513-557), coefficients
+// src/io/mod_input_output.t:1079-1140 (ssprk_order 3: Gottlieb 2005; 2:
+// Spiteri-Ruuth), on registers 0..3:
+//   ps1 = ps + b11 dt L(ps)
+//   ps2 = a21 ps + a22 ps1 + b22 dt L(ps1)
+//   ps1 = a31 ps + a33 ps2 + b33 dt L(ps2)
+//   ps3 = a53 ps2 + a54 ps1;  ps2 = a41 ps + a44 ps1 + b44 dt L(ps1)
+//   ps = ps3 + a55 ps2 + (b54/b44)(ps2 - (a41 ps + a44 ps1));  ps += b55 dt L(ps2)
+struct Ssprk5 {
+  double b11, b22, b33, b44, b54, b55, a21, a31, a41, a53, a54, a22, a33, a44, a55;
+};
+Ssprk5 ssprk5_coefficients(int order) {
+  Ssprk5 k;
+  if (order == 2) {
+    k.b11 = 0.39175222700392; k.b22 = 0.36841059262959; k.b33 = 0.25189177424738; k.b44 = 0.54497475021237;
+    k.a21 = 0.44437049406734; k.a31 = 0.62010185138540; k.a41 = 0.17807995410773; k.a53 = 0.51723167208978;
+    k.a22 = 1.0 - k.a21; k.a33 = 1.0 - k.a31; k.a44 = 1.0 - k.a41;
+    const double rka51 = 0.00683325884039, rka54 = 0.12759831133288, rkb54 = 0.08460416338212;
+    k.b54 = rkb54 - k.b44 * rka51 / k.a41;
+    k.a54 = rka54 - k.a44 * rka51 / k.a41;
+    k.a55 = 1.0 - k.a53 - k.a54;
+    const double c2 = k.b11, c3 = k.a22 * c2 + k.b22, c4 = k.a33 * c3 + k.b33, c5 = k.a44 * c4 + k.b44;
+    k.b55 = 1.0 - k.b54 - k.a53 * c3 - k.a54 * c4 - k.a55 * c5;
+  } else {
+    k.b11 = 0.391752226571890; k.b22 = 0.368410593050371; k.b33 = 0.251891774271694;
+    k.b44 = 0.544974750228521; k.b54 = 0.063692468666290; k.b55 = 0.226007483236906;
+    k.a21 = 0.444370493651235; k.a31 = 0.620101851488403; k.a41 = 0.178079954393132;
+    k.a53 = 0.517231671970585; k.a54 = 0.096059710526147;
+    k.a22 = 1.0 - k.a21; k.a33 = 1.0 - k.a31; k.a44 = 1.0 - k.a41; k.a55 = 1.0 - k.a53 - k.a54;
+  }
+  return k;
+}
+
+int launch_fivestep(amrvac_ctx *c, cudaEvent_t *ev) {
+  const Ssprk5 K = ssprk5_coefficients(c->cfg.ssprk_order);
+  const size_t n = c->per_block * c->nw * c->nblocks;
+  int r = 0;
+  auto mark = [&](int i) { if (ev) cudaEventRecord(ev[i], c->stream); };
+  if ((r = launch_stage(c, 0, 1, 0, 0.0, 1.0, K.b11))) return r;
+  mark(0);
+  if ((r = launch_stage(c, 1, 2, 0, K.a21, K.a22, K.b22))) return r;
+  mark(1);
+  if ((r = launch_stage(c, 2, 1, 0, K.a31, K.a33, K.b33))) return r;
+  mark(2);
+  CK(launch_ssprk5_ps3(c->pool[3], c->pool[2], c->pool[1], K.a53, K.a54, n, c->stream));
+  ++c->launches;
+  if ((r = launch_stage(c, 1, 2, 0, K.a41, K.a44, K.b44))) return r;
+  CK(launch_ssprk5_final(c->pool[0], c->pool[1], c->pool[2], c->pool[3], K.a55, K.b54 / K.b44, K.a41, K.a44, n,
+                         c->stream));
+  ++c->launches;
+  mark(3);
+  r = launch_stage(c, 2, 0, 0, 1.0, 0.0, K.b55);
+  mark(4);
+  return r;
+}
+
 // The configured RK stages (src/mod_advance.t:56-567) on registers 0..2.
 int launch_rk(amrvac_ctx *c) {
   const amrvac_cfg &k = c->cfg;
@@ -295,6 +351,8 @@ int launch_rk(amrvac_ctx *c) {
     }
   } else if (k.time_stepper == AMRVAC_TS_FOURSTEP) {
     r = launch_fourstep(c, nullptr);
+  } else if (k.time_stepper == AMRVAC_TS_FIVESTEP) {
+    r = launch_fivestep(c, nullptr);
   } else {
     double b11, b22, b33, a21, a31;
     if (k.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
@@ -385,15 +443,15 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   if (fifth && k.precision == 1) return fail(AMRVAC_E_UNSUPPORTED, "mp5 / weno5 are FP64 only");
   if (k.typeboundspeed < 1 || k.typeboundspeed > 3) return fail(AMRVAC_E_ARG, "bad typeboundspeed");
   if (k.type_courant < 1 || k.type_courant > 3) return fail(AMRVAC_E_ARG, "bad type_courant");
-  if (k.time_stepper < 1 || k.time_stepper > 4) return fail(AMRVAC_E_UNSUPPORTED, "time_stepper not supported");
+  if (k.time_stepper < 1 || k.time_stepper > 5) return fail(AMRVAC_E_UNSUPPORTED, "time_stepper not supported");
   if (k.time_integrator != AMRVAC_TI_DEFAULT &&
       !(k.time_stepper == AMRVAC_TS_FOURSTEP && k.time_integrator == AMRVAC_TI_RK4) &&
       !(k.time_stepper == AMRVAC_TS_TWOSTEP && k.time_integrator == AMRVAC_TI_SSPRK2))
     return fail(AMRVAC_E_UNSUPPORTED, "time_integrator not supported for this time_stepper");
   if (uses_hancock(k) && k.precision == 1)
     return fail(AMRVAC_E_UNSUPPORTED, "the Hancock predictor (twostep with tvdlf) is FP64 only");
-  if ((k.time_stepper == AMRVAC_TS_THREESTEP || k.time_stepper == AMRVAC_TS_FOURSTEP) && k.ssprk_order != 2 &&
-      k.ssprk_order != 3)
+  if ((k.time_stepper == AMRVAC_TS_THREESTEP || k.time_stepper == AMRVAC_TS_FOURSTEP ||
+       k.time_stepper == AMRVAC_TS_FIVESTEP) && k.ssprk_order != 2 && k.ssprk_order != 3)
     return fail(AMRVAC_E_ARG, "ssprk_order must be 2 or 3");
   if (k.physics == 0 && k.ndir != k.ndim) return fail(AMRVAC_E_UNSUPPORTED, "hd requires ndir == ndim");
   if (k.physics == 1) {
@@ -408,7 +466,8 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   if (nw > AMRVAC_MAX_NW) return fail(AMRVAC_E_UNSUPPORTED, "too many variables");
   amrvac_ctx *c = new amrvac_ctx();
   c->cfg = k;
-  c->nreg = (k.time_stepper == AMRVAC_TS_FOURSTEP && k.time_integrator == AMRVAC_TI_RK4) ? 4 : 3;
+  c->nreg = ((k.time_stepper == AMRVAC_TS_FOURSTEP && k.time_integrator == AMRVAC_TI_RK4) ||
+             k.time_stepper == AMRVAC_TS_FIVESTEP) ? 4 : 3;
   c->nw = nw;
   KernelKey key{k.physics == 1, k.ndim, k.ndir, k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM,
                 k.flux_scheme, k.limiter, k.typeboundspeed, k.precision == 1};
@@ -1255,6 +1314,9 @@ int amrvac_gpu_run_timed(amrvac_ctx *c, int nsteps, double *total_ms, double *st
     } else if (k.time_stepper == AMRVAC_TS_FOURSTEP) {
       r = launch_fourstep(c, &ev[q]);
       q += 4;
+    } else if (k.time_stepper == AMRVAC_TS_FIVESTEP) {
+      r = launch_fivestep(c, &ev[q]);
+      q += 5;
     } else {
       double b11, b22, b33, a21, a31;
       if (k.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }

@@ -84,6 +84,7 @@ extern "C" {
 #define AMRVAC_TS_TWOSTEP   2   /* Predictor_Corrector (default) or ssprk2 (Heun) */
 #define AMRVAC_TS_THREESTEP 3   /* ssprk3, ssprk_order 3 or 2 */
 #define AMRVAC_TS_FOURSTEP  4   /* ssprk4 (ssprk_order 3: SSPRK(4,3), 2: SSP(4,2)) or rk4 */
+#define AMRVAC_TS_FIVESTEP  5   /* ssprk5: SSPRK(5,4) (ssprk_order 3: Gottlieb 2005, 2: Spiteri-Ruuth) */
 #define AMRVAC_TI_DEFAULT   0   /* time_integrator: the stepper's default (twostep:
                                    Predictor_Corrector, threestep: ssprk3, fourstep: ssprk4) */
 #define AMRVAC_TI_RK4       1   /* fourstep: the classical RK(4,4) */

@@ -157,7 +157,7 @@ def make_cfg(*, ndim=2, ndir=None, physics="hd", block_nx=16, nghost=2, gamma=No
     c.small_pressure = small_pressure
     c.divbdiff = divbdiff
     c.ssprk_order = ssprk_order
-    c.time_stepper = {"twostep": 2, "threestep": 3, "fourstep": 4}[time_stepper]
+    c.time_stepper = {"twostep": 2, "threestep": 3, "fourstep": 4, "fivestep": 5}[time_stepper]
     c.time_integrator = {"default": 0, "Predictor_Corrector": 0, "ssprk4": 0, "rk4": 1, "ssprk2": 2}[time_integrator]
     lib().orc_cfg_finalize(ctypes.byref(c))
     return c

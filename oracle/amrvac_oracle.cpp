@@ -1738,6 +1738,47 @@ int fourstep(const orc_cfg &c, double dt, Adv advect1, Copy copy, Comb combine, 
   return st;
 }
 
+// fivestep ssprk5 (src/mod_advance.t:513-557), coefficients
+// src/io/mod_input_output.t:1079-1140 (ssprk_order 3: Gottlieb 2005, the
+// default; 2: Spiteri-Ruuth), over whole (ghosted) registers 0..3.
+template <class Adv, class Copy, class Comb>
+int fivestep(const orc_cfg &c, double dt, Adv advect1, Copy copy, Comb combine, std::vector<double> *reg) {
+  double b11, b22, b33, b44, b54, b55, a21, a31, a41, a53, a54, a22, a33, a44, a55;
+  if (c.ssprk_order == 2) {
+    b11 = 0.39175222700392; b22 = 0.36841059262959; b33 = 0.25189177424738; b44 = 0.54497475021237;
+    a21 = 0.44437049406734; a31 = 0.62010185138540; a41 = 0.17807995410773; a53 = 0.51723167208978;
+    a22 = 1.0 - a21; a33 = 1.0 - a31; a44 = 1.0 - a41;
+    const double rka51 = 0.00683325884039, rka54 = 0.12759831133288, rkb54 = 0.08460416338212;
+    b54 = rkb54 - b44 * rka51 / a41;
+    a54 = rka54 - a44 * rka51 / a41;
+    a55 = 1.0 - a53 - a54;
+    const double c2 = b11, c3 = a22 * c2 + b22, c4 = a33 * c3 + b33, c5 = a44 * c4 + b44;
+    b55 = 1.0 - b54 - a53 * c3 - a54 * c4 - a55 * c5;
+  } else {
+    b11 = 0.391752226571890; b22 = 0.368410593050371; b33 = 0.251891774271694; b44 = 0.544974750228521;
+    b54 = 0.063692468666290; b55 = 0.226007483236906; a21 = 0.444370493651235; a31 = 0.620101851488403;
+    a41 = 0.178079954393132; a53 = 0.517231671970585; a54 = 0.096059710526147;
+    a22 = 1.0 - a21; a33 = 1.0 - a31; a44 = 1.0 - a41; a55 = 1.0 - a53 - a54;
+  }
+  int st = 0;
+  copy(1, 0);  // advect: ps1 = ps before the stepper
+  copy(2, 0);  // (sizes registers 2 and 3)
+  copy(3, 0);
+  st |= advect1(0, 1, b11 * dt, b11);
+  combine(2, a21, 0, a22, 1);
+  st |= advect1(1, 2, b22 * dt, b22);
+  combine(1, a31, 0, a33, 2);
+  st |= advect1(2, 1, b33 * dt, b33);
+  combine(3, a53, 2, a54, 1);
+  combine(2, a41, 0, a44, 1);
+  st |= advect1(1, 2, b44 * dt, b44);
+  const double r = b54 / b44;
+  for (size_t p = 0; p < reg[0].size(); ++p)
+    reg[0][p] = (reg[3][p] + a55 * reg[2][p]) + r * (reg[2][p] - (a41 * reg[0][p] + a44 * reg[1][p]));
+  st |= advect1(2, 0, b55 * dt, b55);
+  return st;
+}
+
 // twostep (src/mod_advance.t:102-133): Predictor_Corrector — predictor
 // ps1 = ps + dt/2 L(ps) with typepred1 (the same scheme for hll, hllc, hlld;
 // hancock for tvdlf) and no flux fix, corrector ps = ps + dt L(ps1) — or
@@ -1775,6 +1816,12 @@ int orc_grid_advance(orc_grid *g, double dt, double cmax_global, int nthreads) {
         },
         [&](int d, int s2) { orc_grid_copy_reg(g, d, s2); },
         [&](int d, double a, int ra, double b, int rb) { orc_grid_combine_reg(g, d, a, ra, b, rb); });
+  if (g->s.c.time_stepper == 5)
+    return fivestep(
+        g->s.c, dt,
+        [&](int ra, int rb, double qdt, double f) { return orc_grid_advect1(g, ra, rb, qdt, f, cmax_global, nthreads); },
+        [&](int d, int s2) { orc_grid_copy_reg(g, d, s2); },
+        [&](int d, double a, int ra, double b, int rb) { orc_grid_combine_reg(g, d, a, ra, b, rb); }, g->reg);
   if (g->s.c.time_stepper == 4)
     return fourstep(
         g->s.c, dt,
@@ -2674,6 +2721,12 @@ int orc_amr_advance(orc_amr *a, double dt, double cmax_global, int nthreads) {
         },
         [&](int d, int s2) { G->reg[d] = G->reg[s2]; },
         [&](int d, double x, int ra, double y, int rb) { orc_amr_combine_reg(a, d, x, ra, y, rb); });
+  if (G->s.c.time_stepper == 5)
+    return fivestep(
+        G->s.c, dt,
+        [&](int ra, int rb, double qdt, double f) { return amr_advect1(*G, ra, rb, qdt, f, cmax_global, nthreads); },
+        [&](int d, int s2) { G->reg[d] = G->reg[s2]; },
+        [&](int d, double x, int ra, double y, int rb) { orc_amr_combine_reg(a, d, x, ra, y, rb); }, G->reg);
   if (G->s.c.time_stepper == 4)
     return fourstep(
         G->s.c, dt,

@@ -145,6 +145,9 @@ def test_time_integrators_are_checked():
     ok = make_cfg(physics="hd", ndim=2, flux_scheme="hll", time_stepper="twostep")
     assert ok.time_stepper == 2 and ok.time_integrator == 0
     assert make_cfg(physics="hd", ndim=2, time_stepper="twostep", time_integrator="ssprk2").time_integrator == 2
+    assert make_cfg(physics="hd", ndim=2, time_stepper="fivestep").time_stepper == 5
+    bad = make_cfg(physics="hd", ndim=2, flux_scheme="hll", time_stepper="fivestep", ssprk_order=4)
+    assert lib.amrvac_gpu_create(ctypes.byref(bad), ctypes.byref(h)) == _lib.E_ARG
 
 
 def test_mp5_needs_three_ghost_cells_and_fp64(lib):

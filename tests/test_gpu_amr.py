@@ -82,6 +82,9 @@ CASES = [
                                                  typedivbfix="linde", time_stepper="fourstep")),
     ("mhd2_hllc_vanleer_glm_cont", 2, 2, dict(physics="mhd", flux_scheme="hllc", limiter="vanleer",
                                               typedivbfix="glm", bc=["cont"] * 4)),
+    ("hd2_hll_koren_ssprk54", 2, 3, dict(physics="hd", flux_scheme="hll", limiter="koren", time_stepper="fivestep")),
+    ("mhd2_hlld_vanleer_linde_ssprk54", 2, 2, dict(physics="mhd", flux_scheme="hlld", limiter="vanleer",
+                                                   typedivbfix="linde", time_stepper="fivestep")),
     ("hd2_hllc_cont", 2, 3, dict(physics="hd", flux_scheme="hllc", limiter="vanleer", bc=["cont"] * 4)),
     ("hd2_hll_symm_x_periodic_y", 2, 3, dict(physics="hd", flux_scheme="hll", limiter="minmod",
                                              bc=["symm", "symm", "periodic", "periodic"])),

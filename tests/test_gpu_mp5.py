@@ -28,6 +28,7 @@ CASES = {
     "mhd3_hlld_mp5_glm": dict(physics="mhd", ndim=3, flux_scheme="hlld", typedivbfix="glm"),
     "mhd3_hll_mp5_glm_pc": dict(physics="mhd", ndim=3, flux_scheme="hll", typedivbfix="glm",
                                 time_stepper="twostep"),
+    "hd2_hll_mp5_ssprk54": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll", time_stepper="fivestep"),
     # the WENO5 family (WENO5limiter: JS, Z, Z+)
     "hd2_hllc_weno5": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hllc", limiter="weno5"),
     "hd2_hll_wenozp5_cont": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll", limiter="wenozp5",

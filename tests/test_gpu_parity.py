@@ -43,6 +43,11 @@ CASES = {
                                     typedivbfix="linde"),
     "mhd25_hlld_cada_glm_lr": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hlld", limiter="cada",
                                    typedivbfix="glm", typeboundspeed="cmaxleftright", mhd_glm_extended=False),
+    # fivestep ssprk5 (SSPRK(5,4); ssprk_order 3 and 2 coefficient sets)
+    "hd2_hllc_vanleer_ssprk54": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hllc", limiter="vanleer",
+                                     time_stepper="fivestep"),
+    "mhd3_hlld_cada3_glm_ssprk54_sr": dict(physics="mhd", ndim=3, flux_scheme="hlld", limiter="cada3",
+                                           typedivbfix="glm", time_stepper="fivestep", ssprk_order=2),
     # MHD HLLC (mhd_get_lCD / mhd_get_wCD)
     "mhd2_hllc_koren_linde": dict(physics="mhd", ndim=2, flux_scheme="hllc", limiter="koren", typedivbfix="linde"),
     "mhd25_hllc_vanleer_glm_cmaxmean": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hllc", limiter="vanleer",
