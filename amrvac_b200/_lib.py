@@ -19,7 +19,7 @@ MAX_NW = 16
 E_ARG, E_UNSUPPORTED, E_CUDA, E_STATE = -1, -2, -3, -4
 ST_SMALL_VALUE, ST_NAN, ST_DT_TOO_SMALL = 1, 2, 4
 
-FS = {"tvdlf": 1, "hll": 2, "hllc": 3, "hlld": 4}
+FS = {"tvdlf": 1, "hll": 2, "hllc": 3, "hlld": 4, "tvdmu": 5}
 LIMITER = {"minmod": 1, "woodward": 2, "mcbeta": 3, "superbee": 4, "vanleer": 5,
            "albada": 6, "koren": 7, "cada": 8, "cada3": 9, "mp5": 13,
            "weno5": 16, "wenoz5": 18, "wenozp5": 20}
@@ -55,6 +55,7 @@ class AmrvacCfg(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("slowsteps", ctypes.c_int),
         ("time_integrator", ctypes.c_int),
+        ("dimsplit", ctypes.c_int),
     ]
 
 

@@ -107,7 +107,8 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
              check_small_values=True, small_values_method="error", small_density=0.0,
              small_pressure=0.0, time_stepper="threestep", ssprk_order=3, dtmin=1.0e-10,
              typeboundary=None, zchunk=0, precision="fp64", slowsteps=-1,
-             time_integrator="default", nghostcells=None) -> _lib.AmrvacCfg:
+             time_integrator="default", nghostcells=None, dimsplit=False,
+             typedimsplit="xyyx") -> _lib.AmrvacCfg:
     """Build an ``amrvac_cfg`` from reference-style parameter names.
 
     typeboundary: list of 2*ndim entries (min1, max1, min2, ...), each a name
@@ -151,6 +152,7 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
     c.precision = _lib.PRECISION[precision]
     c.slowsteps = int(slowsteps)
     c.time_integrator = _lib.TIME_INTEGRATOR[time_integrator]
+    c.dimsplit = 0 if not dimsplit else (2 if typedimsplit == "xy" else 1)
     nw = L.amrvac_gpu_nw(c)
     tb = typeboundary or ["periodic"] * (2 * ndim)
     for s in range(6):
@@ -216,6 +218,8 @@ def config_from_par(paths) -> RunConfig:
         ssprk_order=int(meth.get("ssprk_order", 3)),
         time_integrator=integ or "default",
         nghostcells=int(mesh["nghostcells"]) if "nghostcells" in mesh else None,
+        dimsplit=bool(meth.get("dimsplit", False)),
+        typedimsplit=meth.get("typedimsplit", "xyyx"),
     )
     if physics == "mhd":
         cfg_kw.update(typedivbfix=plist.get("typedivbfix", "linde"),

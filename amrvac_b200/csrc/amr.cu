@@ -333,8 +333,10 @@ __global__ void __launch_bounds__(256) amr_fix_kernel(const AmrFixArgs A) {
   const int b = A.iblocks[slot];
   const int t = threadIdx.x;
   const double cofi = 1.0 / double(1 << NDIM);
+  const int dsel = sweep_dir(A.sweep, A.split_xy, A.scal, NDIM);
   for (int d = 0; d < NDIM; ++d)
     for (int side = 0; side < 2; ++side) {
+      if (dsel >= 0 && d != dsel) continue;
       int dd[3] = {0, 0, 0};
       dd[d] = side ? 1 : -1;
       const int q = dir_index(dd[0], dd[1], dd[2]);

@@ -53,6 +53,10 @@ struct AmrFixArgs {
   const double *pflux;      // [slot][2*ndim][var][16*16]
   int nw;
   const int *iblocks, *gslot, *ntype, *child;  // child[(b*27+q)*8 + cbits]
+  // dimensional splitting: only the sweep's direction (fix_conserve with
+  // idim^LIM = idim, idim); sweep < 0: all directions
+  int sweep, split_xy;
+  const double *scal;
 };
 
 // Regrid: the state of the new tree's leaves from the old tree's register 0.

@@ -84,6 +84,7 @@ struct amrvac_ctx {
   int64_t launches = 0;
   int64_t graph_nodes = 0;
   int zchunk = 0;          // 0: persistent plane ranges; 16/8/4: one z-chunk per CTA
+  int sweep = -1;          // dimensional splitting: the current sweep of the step (-1: unsplit)
   int wave_ctas = 1;       // resident stage CTAs on the device (one wave)
   std::vector<double> h_dx;            // [nblocks][3] cell sizes (host copy)
   double *d_adj[3] = {nullptr, nullptr, nullptr};  // adjoint work registers (lazily)
@@ -138,7 +139,7 @@ namespace {
 // 787-797); the other schemes predict with their own finite_volume.
 bool uses_hancock(const amrvac_cfg &k) {
   return k.time_stepper == AMRVAC_TS_TWOSTEP && k.time_integrator == AMRVAC_TI_DEFAULT &&
-         k.flux_scheme == AMRVAC_FS_TVDLF;
+         (k.flux_scheme == AMRVAC_FS_TVDLF || k.flux_scheme == AMRVAC_FS_TVDMU);
 }
 
 int check_ctx(amrvac_ctx *c, bool need_blocks) {
@@ -170,6 +171,8 @@ StageArgs stage_args(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, doubl
   A.status = c->d_status;
   A.block_status = c->d_block_status;
   A.P = c->P;
+  A.sweep = c->sweep;
+  A.split_xy = c->cfg.dimsplit == 2;
   if (c->amr) {
     A.gbuf = c->amr->gbuf;
     A.pflux = c->amr->pflux;
@@ -216,6 +219,8 @@ int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a,
   if (c->amr && fix) {  // fix_conserve on the stage's output
     AmrFixArgs F = c->amr->F;
     F.w = c->pool[reg_new];
+    F.sweep = c->sweep;
+    F.split_xy = c->cfg.dimsplit == 2;
     CK(launch_amr_fix(F, c->amr->nslots, c->cfg.ndim, c->stream));
     ++c->launches;
   }
@@ -370,7 +375,16 @@ int launch_step(amrvac_ctx *c) {
   if ((r = launch_getdt(c, 0))) return r;
   CK(launch_setdt_finalize(c->d_red, c->d_scal, c->d_status, c->stream));
   ++c->launches;
-  if ((r = launch_rk(c))) return r;
+  if (c->cfg.dimsplit) {  // one full stepper per direction (src/mod_advance.t:23-45)
+    for (int s = 0; s < c->cfg.ndim && !r; ++s) {
+      c->sweep = s;
+      r = launch_rk(c);
+    }
+    c->sweep = -1;
+    if (r) return r;
+  } else if ((r = launch_rk(c))) {
+    return r;
+  }
   CK(launch_advance_time(c->d_scal, c->stream));
   ++c->launches;
   return 0;
@@ -462,6 +476,14 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   } else if (k.flux_scheme == AMRVAC_FS_HLLD) {
     return fail(AMRVAC_E_UNSUPPORTED, "hlld needs mhd");
   }
+  if (k.flux_scheme < AMRVAC_FS_TVDLF || k.flux_scheme > AMRVAC_FS_TVDMU)
+    return fail(AMRVAC_E_ARG, "unknown flux_scheme");
+  if (k.dimsplit < 0 || k.dimsplit > 2) return fail(AMRVAC_E_ARG, "dimsplit must be 0, 1 (xyyx) or 2 (xy)");
+  // The reference's unsplit TVD-MUSCL limits every direction with the states
+  // reconstructed for the last one (finite_volume's flux and update loops are
+  // separate); its tests run TVD-MUSCL dimensionally split only.
+  if (k.flux_scheme == AMRVAC_FS_TVDMU && (k.physics != 0 || !k.dimsplit || k.precision == 1))
+    return fail(AMRVAC_E_UNSUPPORTED, "tvdmu: hd, dimsplit, FP64");
   const int nw = nw_of(cfg);
   if (nw > AMRVAC_MAX_NW) return fail(AMRVAC_E_UNSUPPORTED, "too many variables");
   amrvac_ctx *c = new amrvac_ctx();
@@ -1067,6 +1089,8 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
   A->F.gslot = A->d_gslot;
   A->F.ntype = G.ntype;
   A->F.child = A->d_int + o_ch;
+  A->F.sweep = -1;
+  A->F.scal = c->d_scal;
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
@@ -1284,6 +1308,7 @@ int amrvac_gpu_run(amrvac_ctx *c, int nsteps) {
 
 int amrvac_gpu_run_timed(amrvac_ctx *c, int nsteps, double *total_ms, double *stage_ms, double *getdt_ms) {
   if (int r = check_ctx(c, true)) return r;
+  if (c->cfg.dimsplit) return fail(AMRVAC_E_UNSUPPORTED, "run_timed: dimsplit (use amrvac_gpu_step / run)");
   if (nsteps <= 0) return fail(AMRVAC_E_ARG, "nsteps must be positive");
   const int nst = c->cfg.time_stepper;  // stages per step
   const int per = 3 + nst;              // events per step

@@ -26,6 +26,8 @@ bool lookup_hd(const KernelKey &k, KernelSet *out) {
     return true;                                                \
   }
   AMRVAC_HD(2, SOLVER_TVDLF)
+  AMRVAC_HD(2, SOLVER_TVDMU)
+  AMRVAC_HD(3, SOLVER_TVDMU)
   AMRVAC_HD(2, SOLVER_HLL)
   AMRVAC_HD(2, SOLVER_HLLC)
   AMRVAC_HD(3, SOLVER_TVDLF)

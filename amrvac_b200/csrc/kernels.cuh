@@ -182,8 +182,8 @@ template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM = 0, int B
 struct Launch {
   using V = Vars<MHD, NDIR, GLM>;
   static constexpr size_t SMEM = Tile<TF, V::NW, NDIM, HaloW<LIM>::value>::BYTES;
-  // typepred1 = fs_hancock for tvdlf (src/io/mod_input_output.t:787-797)
-  static constexpr bool HAS_HANCOCK = SOLVER == SOLVER_TVDLF && sizeof(TF) == 8;
+  // typepred1 = fs_hancock for tvdlf and tvdmu (src/io/mod_input_output.t:787-797)
+  static constexpr bool HAS_HANCOCK = (SOLVER == SOLVER_TVDLF || SOLVER == SOLVER_TVDMU) && sizeof(TF) == 8;
   static cudaError_t prepare() {
     cudaError_t e = cudaFuncSetAttribute(fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);

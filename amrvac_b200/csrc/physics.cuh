@@ -18,7 +18,8 @@ enum : int { LIM_MINMOD = 1, LIM_WOODWARD = 2, LIM_MCBETA = 3, LIM_SUPERBEE = 4,
              LIM_VANLEER = 5, LIM_ALBADA = 6, LIM_KOREN = 7, LIM_CADA = 8, LIM_CADA3 = 9,
              LIM_MP5 = 13, LIM_WENO5 = 16, LIM_WENOZ5 = 18, LIM_WENOZP5 = 20 };
 enum : int { BS_EINFELDT = 1, BS_CMAXMEAN = 2, BS_CMAXLEFTRIGHT = 3 };
-enum : int { SOLVER_TVDLF = 1, SOLVER_HLL = 2, SOLVER_HLLC = 3, SOLVER_HLLD = 4, SOLVER_HANCOCK = 8 };
+enum : int { SOLVER_TVDLF = 1, SOLVER_HLL = 2, SOLVER_HLLC = 3, SOLVER_HLLD = 4, SOLVER_TVDMU = 5,
+             SOLVER_HANCOCK = 8 };
 enum : int { DIVB_NONE = 0, DIVB_GLM = 1, DIVB_LINDE = 4 };
 // Runtime status bits (atomicOr into the context's status word).
 enum : uint32_t { ST_SMALL_VALUE = 1u, ST_NAN = 2u, ST_DT_TOO_SMALL = 4u, ST_BOUNDS = 8u };

@@ -197,6 +197,71 @@ __device__ __forceinline__ void riemann_hllc_mhd(const T *wLC, const T *wRC, con
   }
 }
 
+// TVD-MUSCL (fs_tvdmu) for hydrodynamics: the central flux of
+// get_Riemann_flux_tvdmu (src/mod_finite_volume.t:342-346) with the
+// characteristic limiter tvdlimit2 (src/mod_tvd.t:38-112) folded into the
+// face flux — the Roe average hd_average, the wave speeds and jumps of
+// geteigenjump2 and the right eigenvectors of rtimes2
+// (src/hd/mod_hd_roe.t:58-296), entropy fix 'nul', getphi's tvdmu branch
+// phi = |a qdt/dx| jump.  tvdlimit2 adds 0.5 R phi to the scaled flux
+// -qdt/dx F; here F - 0.5 sum R |a| jump is returned for the same scaling.
+// Rotated states: the face normal is component 0, the shear waves follow in
+// the tangential components' order.
+template <class T, int NDIR>
+__device__ __forceinline__ void riemann_tvdmu_hd(const T *wLC, const T *wRC, const T *fL, const T *fR,
+                                                 const PhysParams &P, T *F) {
+  using V = Vars<false, NDIR, false>;
+  constexpr int NW = V::NW;
+#pragma unroll
+  for (int v = 0; v < NW; ++v) F[v] = T(0.5) * (fL[v] + fR[v]);
+  // hd_average
+  const T qL = sqrt(wLC[V::RHO]), qR = sqrt(wRC[V::RHO]);
+  const T rho = qL * qR;
+  const T r = qL / qR;
+  T vel[NDIR];
+#pragma unroll
+  for (int c = 0; c < NDIR; ++c)
+    vel[c] = (wLC[V::M0 + c] / wLC[V::RHO] * r + wRC[V::M0 + c] / wRC[V::RHO]) / (T(1.0) + r);
+  auto pth = [&](const T *w) {  // hd_get_pthermal
+    T m2 = w[V::M0] * w[V::M0];
+#pragma unroll
+    for (int c = 1; c < NDIR; ++c) m2 = m2 + w[V::M0 + c] * w[V::M0 + c];
+    T p = T(P.gamma - 1.0) * (w[V::E] - T(0.5) * m2 / w[V::RHO]);
+    if (P.fix_small_values && p < T(P.small_pressure)) p = T(P.small_pressure);
+    return p;
+  };
+  const T pL = pth(wLC), pR = pth(wRC);
+  const T hL = (pL + wLC[V::E]) / wLC[V::RHO];
+  const T hR = (pR + wRC[V::E]) / wRC[V::RHO];
+  const T H = (hL * r + hR) / (T(1.0) + r);
+  // geteigenjump2, il = 1 part
+  T v2 = vel[0] * vel[0];
+#pragma unroll
+  for (int c = 1; c < NDIR; ++c) v2 = v2 + vel[c] * vel[c];
+  const T kin = T(0.5) * v2;
+  T c2 = T(P.gamma - 1.0) * (H - kin);
+  c2 = fmax(T(P.gamma) * T(1.0e-12) / rho, c2);  // smalldouble
+  const T dpperc2 = (pR - pL) / c2;
+  const T cs = sqrt(c2);
+  const T dvperc = (wRC[V::M0] / wRC[V::RHO] - wLC[V::M0] / wLC[V::RHO]) / cs;
+  const T u = vel[0];
+  // sound waves (right, left) and the entropy wave: R columns
+  const T aR = fabs(u + cs) * (T(0.5) * (dpperc2 + rho * dvperc));
+  const T aL = fabs(u - cs) * (T(0.5) * (dpperc2 - rho * dvperc));
+  const T aE = fabs(u) * ((-dpperc2 + wRC[V::RHO]) - wLC[V::RHO]);
+  F[V::RHO] = F[V::RHO] - (T(0.5) * aR + T(0.5) * aL + T(0.5) * aE);
+  F[V::E] = F[V::E] - (T(0.5) * (aR * (H + u * cs)) + T(0.5) * (aL * (H - u * cs)) + T(0.5) * (aE * kin));
+  F[V::M0] = F[V::M0] - (T(0.5) * (aR * (u + cs)) + T(0.5) * (aL * (u - cs)) + T(0.5) * (aE * u));
+#pragma unroll
+  for (int c = 1; c < NDIR; ++c) {
+    // shear wave of component c: a = u, jump = rho (vR_c - vL_c)
+    const T aS = fabs(u) * (rho * (wRC[V::M0 + c] / wRC[V::RHO] - wLC[V::M0 + c] / wLC[V::RHO]));
+    F[V::E] = F[V::E] - T(0.5) * (aS * vel[c]);
+    F[V::M0 + c] = F[V::M0 + c] - (T(0.5) * (aR * vel[c]) + T(0.5) * (aL * vel[c]) + T(0.5) * (aE * vel[c]) +
+                                   T(0.5) * aS);
+  }
+}
+
 // get_Riemann_flux_hlld (mod_finite_volume.t:507-729), no B0 / equilibrium split.
 template <class T, int NDIR, bool GLM, int NDIM, int D>
 __device__ __forceinline__ void riemann_hlld(const T *wLC, const T *wRC, const T *wLp,

@@ -75,7 +75,21 @@ struct StageArgs {
   double *pflux;            // [slot][2*ndim][var][16*16] scaled face fluxes
   const int *gslot;         // [nblocks] slot or -1
   const int *amr_face;      // [nblocks] bitmask
+  // Dimensional splitting: sweep < 0 advances all directions; otherwise the
+  // stage is the sweep-th of the step's one-direction sweeps (see sweep_dir).
+  int sweep;
+  int split_xy;             // 1: typedimsplit 'xy' (same order every step)
 };
+
+// Direction of a dimensionally split sweep (src/mod_advance.t:23-45):
+// increasing order on even steps (and always with typedimsplit 'xy'),
+// decreasing on odd steps ('xyyx'); the step count is the device scalar
+// scal[9] (steps since set_time).  -1: unsplit.
+__device__ __forceinline__ int sweep_dir(int sweep, int split_xy, const double *scal, int ndim) {
+  if (sweep < 0) return -1;
+  const long it = (long)scal[9];
+  return (split_xy || (it & 1L) == 0) ? sweep : ndim - 1 - sweep;
+}
 
 __device__ __forceinline__ int dir_index(int di, int dj, int dk) {
   return (di + 1) + 3 * (dj + 1) + 9 * (dk + 1);
@@ -213,7 +227,11 @@ __device__ __forceinline__ uint32_t face_from_states(T *wLp, T *wRp, const PhysP
   phys_flux<T, MHD, NDIR, GLM, D>(wLC, wLp, cg, fL);
   phys_flux<T, MHD, NDIR, GLM, D>(wRC, wRp, cg, fR);
   T cmax, cmin = T(0.0);
-  if constexpr (SOLVER == SOLVER_TVDLF) {
+  if constexpr (SOLVER == SOLVER_TVDMU) {
+    static_assert(!MHD, "TVD-MUSCL is implemented for HD only");
+    (void)cmax;
+    riemann_tvdmu_hd<T, NDIR>(wLC, wRC, fL, fR, P, F);
+  } else if constexpr (SOLVER == SOLVER_TVDLF) {
     st |= cbounds<T, MHD, NDIR, GLM, D, false, BS>(wLC, wRC, wLp, wRp, P, cmax, cmin);
     riemann_tvdlf<T, NW>(wLC, wRC, fL, fR, cmax, T(P.tvdlfeps), F);
   } else {
@@ -510,6 +528,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
   const PhysParams &P = A.P;
   const double dt = *A.dt_dev;
   const double qdt = A.dtfactor * dt;
+  const int dsel = sweep_dir(A.sweep, A.split_xy, A.dt_dev, NDIM);  // -1: all directions
   const double cg = GLM ? *A.cmax_dev : 0.0;
   uint32_t st = 0;
   const int ci = t & (BN - 1), cj = t >> 4;  // cell role for t < 256
@@ -604,13 +623,17 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
       static_assert(sizeof(TF) == 8, "the Hancock predictor is FP64 only");
       if (update && cell_thread) {
         int base[3], strd[3];
+        if (dsel < 0 || dsel == 0) {
 #pragma unroll
-        for (int o = 0; o < 3; ++o) tv.addr(slot, ci + o - 1, cj, base[o], strd[o]);
-        stb |= hancock_dir<MHD, NDIR, GLM, LIM, 0>(smem, base, strd, rdel[0], dxinv[0], cg, P, acc);
+          for (int o = 0; o < 3; ++o) tv.addr(slot, ci + o - 1, cj, base[o], strd[o]);
+          stb |= hancock_dir<MHD, NDIR, GLM, LIM, 0>(smem, base, strd, rdel[0], dxinv[0], cg, P, acc);
+        }
+        if (dsel < 0 || dsel == 1) {
 #pragma unroll
-        for (int o = 0; o < 3; ++o) tv.addr(slot, ci, cj + o - 1, base[o], strd[o]);
-        stb |= hancock_dir<MHD, NDIR, GLM, LIM, 1>(smem, base, strd, rdel[1], dxinv[1], cg, P, acc);
-        if constexpr (NDIM == 3) {
+          for (int o = 0; o < 3; ++o) tv.addr(slot, ci, cj + o - 1, base[o], strd[o]);
+          stb |= hancock_dir<MHD, NDIR, GLM, LIM, 1>(smem, base, strd, rdel[1], dxinv[1], cg, P, acc);
+        }
+        if (NDIM == 3 && (dsel < 0 || dsel == 2)) {
 #pragma unroll
           for (int o = 0; o < 3; ++o) {
             base[o] = ring_slot<HW>(k + o - 1) * NW * (BN * BN) + cj * BN + ci;
@@ -625,11 +648,13 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
     // The x phase also computes the 16 y-faces of the top row (j = BN) into
     // tv.yx: 272 x-faces + 16 = 288 faces make its second round one full warp,
     // and the y phase one round of 256 (instead of two rounds of 256 + 16).
-    // (With 272 or more threads a phase of 272 faces is one round already.)
-    constexpr bool MERGE_YX = STAGE_THREADS < FB;
+    // (With 272 or more threads a phase of 272 faces is one round already;
+    // a split sweep has one phase only.)
+    const bool MERGE_YX = STAGE_THREADS < FB && dsel < 0;
     const int dlo = update ? 0 : (NDIM == 3 && k == k0 - 1 ? 2 : NDIM);
 #pragma unroll 1
     for (int D = dlo; D < NDIM; ++D) {
+      if (dsel >= 0 && D != dsel) continue;  // not this sweep's direction (uniform)
       const int nface = D == 0 ? (MERGE_YX ? FB + BN : FB) : (D == 1 && !MERGE_YX ? FB : BN * BN);
       // direction FD and index fl (in that direction's face layout) of face f
       // of this phase
@@ -829,7 +854,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
       // ---- unsplit divB sources (addsource2 -> mhd_add_source)
       if constexpr (MHD) {
         if (NDIM > 1) {
-          const double qsrc = qdt * double(NDIM) / double(NDIM);
+          // addsource2 with qdt (idimmax - idimmin + 1) / ndim
+          const double qsrc = qdt * double(dsel < 0 ? NDIM : 1) / double(NDIM);
           if constexpr (GLM) {
             // add_source_glm (src/mhd/mod_mhd_phys.t:5472-5531)
             double mindx = dx[0];

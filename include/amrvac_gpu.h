@@ -48,6 +48,7 @@ extern "C" {
 #define AMRVAC_FS_HLL   2
 #define AMRVAC_FS_HLLC  3
 #define AMRVAC_FS_HLLD  4
+#define AMRVAC_FS_TVDMU 5  /* TVD-MUSCL (HD; with dimsplit, as the reference runs it) */
 /* limiter ids: src/limiter/mod_limiter.t:14-24 */
 #define AMRVAC_LIM_MINMOD   1
 #define AMRVAC_LIM_WOODWARD 2
@@ -130,6 +131,9 @@ typedef struct amrvac_cfg {
                                scaled by 1 - (1 - n/slowsteps)^2 (n = 1, 2, ...);
                                <= 0: off (default -1) */
   int time_integrator;      /* AMRVAC_TI_* (src/mod_advance.t:454-512) */
+  int dimsplit;             /* 0 unsplit (default); 1 dimensionally split with
+                               typedimsplit 'xyyx' (the order reverses on odd
+                               steps), 2 'xy' (src/mod_advance.t:23-45) */
 } amrvac_cfg;
 
 typedef struct amrvac_ctx amrvac_ctx;

@@ -16,7 +16,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 
-FS = {"tvdlf": 1, "hll": 2, "hllc": 3, "hlld": 4}
+FS = {"tvdlf": 1, "hll": 2, "hllc": 3, "hlld": 4, "tvdmu": 5}
 LIMITER = {"minmod": 1, "woodward": 2, "mcbeta": 3, "superbee": 4, "vanleer": 5,
            "albada": 6, "koren": 7, "cada": 8, "cada3": 9, "mp5": 13, "weno5": 16, "wenoz5": 18, "wenozp5": 20}
 BOUNDSPEED = {"Einfeldt": 1, "cmaxmean": 2, "cmaxleftright": 3}
@@ -38,6 +38,7 @@ class OrcCfg(ctypes.Structure):
         ("small_density", ctypes.c_double), ("small_pressure", ctypes.c_double),
         ("divbdiff", ctypes.c_double), ("ssprk_order", ctypes.c_int),
         ("time_stepper", ctypes.c_int), ("time_integrator", ctypes.c_int),
+        ("dimsplit", ctypes.c_int),
     ]
 
 
@@ -130,7 +131,8 @@ def make_cfg(*, ndim=2, ndir=None, physics="hd", block_nx=16, nghost=2, gamma=No
              glm_alpha=0.5, glm_extended=True, courantpar=0.8, type_courant=1,
              cada3_radius=0.1, tvdlfeps=1.0, fix_small_values=False, check_small_values=True,
              small_values_method="error", small_density=0.0, small_pressure=0.0,
-             divbdiff=0.8, ssprk_order=3, time_stepper="threestep", time_integrator="default") -> OrcCfg:
+             divbdiff=0.8, ssprk_order=3, time_stepper="threestep", time_integrator="default",
+             dimsplit=False, typedimsplit="xyyx") -> OrcCfg:
     c = OrcCfg()
     c.ndim = ndim
     c.ndir = ndim if ndir is None else ndir
@@ -159,6 +161,7 @@ def make_cfg(*, ndim=2, ndir=None, physics="hd", block_nx=16, nghost=2, gamma=No
     c.ssprk_order = ssprk_order
     c.time_stepper = {"twostep": 2, "threestep": 3, "fourstep": 4, "fivestep": 5}[time_stepper]
     c.time_integrator = {"default": 0, "Predictor_Corrector": 0, "ssprk4": 0, "rk4": 1, "ssprk2": 2}[time_integrator]
+    c.dimsplit = 0 if not dimsplit else (2 if typedimsplit == "xy" else 1)
     lib().orc_cfg_finalize(ctypes.byref(c))
     return c
 

@@ -193,6 +193,9 @@ struct State {
   Geo g;
   Ix x;
   double gamma_1, inv_gamma_1, small_e;
+  // the directions advect1 advances (idim^LIM; a dimensionally split sweep
+  // sets one), 0-based
+  int idlo = 0, idhi = 0;
 };
 
 inline State make_state(const orc_cfg &c) {
@@ -202,6 +205,8 @@ inline State make_state(const orc_cfg &c) {
   s.x = make_ix(c);
   s.gamma_1 = c.gamma - 1.0;
   s.inv_gamma_1 = 1.0 / s.gamma_1;
+  s.idlo = 0;
+  s.idhi = c.ndim - 1;
   // hd_check_params (src/hd/mod_hd_phys.t:541) / mhd_check_params (1213-1214)
   s.small_e = c.physics == 1 ? c.small_pressure * s.inv_gamma_1 : c.small_pressure / (c.gamma - 1.0);
   return s;
@@ -1121,6 +1126,112 @@ void add_source_linde(const State &s, double qdt, const Box &ixO, const Arr<R> &
   (void)qdt;
 }
 
+// tvdlimit2 (src/mod_tvd.t:38-112) for fs_tvdmu with hydrodynamics: the Roe
+// average hd_average, the waves of geteigenjump2 and the right eigenvectors
+// of rtimes2 (src/hd/mod_hd_roe.t:58-296), typeentropy 'nul', getphi's
+// tvdmu branch phi = |a qdt/dx| jump; each characteristic adds
+// rphi = R phi / 2 to the scaled face flux and rphi(i) - rphi(i-1) to wnew.
+template <class R>
+void tvdlimit2_hd(const State &s, double qdt, const Box &ixO, int idims, const Arr<R> &wL, const Arr<R> &wR,
+                  Arr<R> &wnew, Arr<R> &fC, const double *dxs) {
+  const Ix &x = s.x;
+  const Geo &g = s.g;
+  const int nw = x.nw, ndir = x.ndir, o = g.off(idims);
+  const double gam = s.c.gamma;
+  Box ixC = ixO;
+  ixC.lo[idims] -= 1;
+  Arr<R> wroe(g, nw), csound(g, 1), dpperc2(g, 1), dvperc(g, 1), a(g, 1), jump(g, 1), phi(g, 1), rphi(g, 1);
+  auto pth = [&](const Arr<R> &w, int i, int j, int k) {  // hd_get_pthermal
+    R m2 = W(w, x.mom[0]) * W(w, x.mom[0]);
+    for (int c = 1; c < ndir; ++c) m2 = m2 + W(w, x.mom[c]) * W(w, x.mom[c]);
+    R p = R(gam - 1.0) * (W(w, x.e) - R(0.5) * m2 / W(w, x.rho));
+    if (s.c.fix_small_values && p < R(s.c.small_pressure)) p = R(s.c.small_pressure);
+    return p;
+  };
+  // hd_average
+  forbox(ixC, [&](int i, int j, int k) {
+    R w1 = rsqrt_(W(wL, x.rho)), w2 = rsqrt_(W(wR, x.rho));
+    W(wroe, x.rho) = w1 * w2;
+    w1 = w1 / w2;
+    for (int c = 0; c < ndir; ++c)
+      W(wroe, x.mom[c]) = (W(wL, x.mom[c]) / W(wL, x.rho) * w1 + W(wR, x.mom[c]) / W(wR, x.rho)) / (R(one) + w1);
+    W(wroe, x.e) = (pth(wL, i, j, k) + W(wL, x.e)) / W(wL, x.rho);
+    R t2 = (pth(wR, i, j, k) + W(wR, x.e)) / W(wR, x.rho);
+    W(wroe, x.e) = (W(wroe, x.e) * w1 + t2) / (R(one) + w1);
+  });
+  const double dxinv = qdt / dxs[idims];
+  const int soundR = 0, soundL = 1, entrop = 2;  // il - 1; shear waves from 3
+  for (int il = 0; il < nw; ++il) {
+    // geteigenjump2
+    forbox(ixC, [&](int i, int j, int k) {
+      const int p = g.idx(i, j, k);
+      if (il == 0) {
+        R v2 = W(wroe, x.mom[0]) * W(wroe, x.mom[0]);
+        for (int c = 1; c < ndir; ++c) v2 = v2 + W(wroe, x.mom[c]) * W(wroe, x.mom[c]);
+        R kin = R(0.5) * v2;
+        R c2 = R(gam - 1.0) * (W(wroe, x.e) - kin);
+        c2 = rmax(R(gam * 1.0e-12) / W(wroe, x.rho), c2);  // smalldouble
+        dpperc2.d[p] = (pth(wR, i, j, k) - pth(wL, i, j, k)) / c2;
+        csound.d[p] = rsqrt_(c2);
+        dvperc.d[p] = (W(wR, x.mom[idims]) / W(wR, x.rho) - W(wL, x.mom[idims]) / W(wL, x.rho)) / csound.d[p];
+      }
+      const R u = W(wroe, x.mom[idims]);
+      if (il == soundR) {
+        a.d[p] = u + csound.d[p];
+        jump.d[p] = R(half) * (dpperc2.d[p] + W(wroe, x.rho) * dvperc.d[p]);
+      } else if (il == soundL) {
+        a.d[p] = u - csound.d[p];
+        jump.d[p] = R(half) * (dpperc2.d[p] - W(wroe, x.rho) * dvperc.d[p]);
+      } else if (il == entrop) {
+        a.d[p] = u;
+        jump.d[p] = -dpperc2.d[p] + W(wR, x.rho) - W(wL, x.rho);
+      } else {
+        int idir = il - 3;
+        if (idir >= idims) idir += 1;
+        a.d[p] = u;
+        jump.d[p] = W(wroe, x.rho) * (W(wR, x.mom[idir]) / W(wR, x.rho) - W(wL, x.mom[idir]) / W(wL, x.rho));
+      }
+      phi.d[p] = rabs(a.d[p] * R(dxinv)) * jump.d[p];  // getphi, tvdmu, typeentropy 'nul'
+    });
+    const bool shear = il > entrop;
+    int sdir = idims;
+    if (shear) { sdir = il - 3; if (sdir >= idims) sdir += 1; }
+    for (int iw = 0; iw < nw; ++iw) {
+      // rtimes2
+      forbox(ixC, [&](int i, int j, int k) {
+        const int p = g.idx(i, j, k);
+        const R q = phi.d[p];
+        R rq;
+        if (iw == x.rho) {
+          rq = shear ? R(zero) : q;
+        } else if (iw == x.e) {
+          if (il == soundR) rq = q * (W(wroe, x.e) + W(wroe, x.mom[idims]) * csound.d[p]);
+          else if (il == soundL) rq = q * (W(wroe, x.e) - W(wroe, x.mom[idims]) * csound.d[p]);
+          else if (il == entrop) {
+            R v2 = W(wroe, x.mom[0]) * W(wroe, x.mom[0]);
+            for (int c = 1; c < ndir; ++c) v2 = v2 + W(wroe, x.mom[c]) * W(wroe, x.mom[c]);
+            rq = q * R(0.5) * v2;
+          } else rq = q * W(wroe, x.mom[sdir]);
+        } else if (iw == x.mom[idims]) {
+          if (il == soundR) rq = q * (W(wroe, x.mom[idims]) + csound.d[p]);
+          else if (il == soundL) rq = q * (W(wroe, x.mom[idims]) - csound.d[p]);
+          else if (il == entrop) rq = q * W(wroe, x.mom[idims]);
+          else rq = R(zero);
+        } else {
+          if (shear) rq = (iw == x.mom[sdir]) ? q : R(zero);
+          else rq = q * W(wroe, iw);
+        }
+        rphi.d[p] = rq * R(half);
+        W(fC, iw) = W(fC, iw) + rphi.d[p];
+      });
+      forbox(ixO, [&](int i, int j, int k) {
+        const int p = g.idx(i, j, k);
+        W(wnew, iw) = W(wnew, iw) + rphi.d[p] - rphi.d[p - o];
+      });
+    }
+  }
+}
+
 // finite_volume (src/mod_finite_volume.t:116-339), slab_uniform, no local dt.
 template <class R>
 int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, double dtfactor,
@@ -1138,7 +1249,7 @@ int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, d
   Arr<R> cmaxC(g, 1), cminC(g, 1);
   std::vector<Arr<R>> fC;
   for (int d = 0; d < ndim; ++d) fC.emplace_back(g, nw);
-  for (int idims = 0; idims < ndim; ++idims) {
+  for (int idims = s.idlo; idims <= s.idhi; ++idims) {
     const int o = g.off(idims);
     Box kxC = ixI;
     kxC.hi[idims] -= 1;
@@ -1156,7 +1267,11 @@ int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, d
     if (x.glm) modify_wLR(s, ixCR, wLC, wRC, wLp, wRp, idims, cmax_global);
     get_flux(s, wLC, wLp, ixC, idims, cmax_global, fLC);
     get_flux(s, wRC, wRp, ixC, idims, cmax_global, fRC);
-    if (c.flux_scheme == ORC_FS_TVDLF) {
+    if (c.flux_scheme == ORC_FS_TVDMU) {
+      // get_Riemann_flux_tvdmu (src/mod_finite_volume.t:342-346)
+      for (int iw = 0; iw < nw; ++iw)
+        forbox(ixC, [&](int i, int j, int k) { W(fC[idims], iw) = R(half) * (W(fLC, iw) + W(fRC, iw)); });
+    } else if (c.flux_scheme == ORC_FS_TVDLF) {
       st |= get_cbounds(s, wLC, wRC, wLp, wRp, ixC, idims, cmaxC, (Arr<R> *)nullptr);
       riemann_tvdlf(s, ixC, idims, wLC, wRC, fLC, fRC, cmaxC, fC[idims]);
     } else {
@@ -1169,7 +1284,7 @@ int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, d
     }
   }
   // conservative update (src/mod_finite_volume.t:269-284)
-  for (int idims = 0; idims < ndim; ++idims) {
+  for (int idims = s.idlo; idims <= s.idhi; ++idims) {
     const int o = g.off(idims);
     R dxinv = -R(qdt) / R(dxs[idims]);
     Box hb = ixO;
@@ -1181,6 +1296,9 @@ int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, d
         wnew.d[p] = wnew.d[p] + fC[idims].d[p] - fC[idims].d[p - o];
       });
     }
+    // the MUSCL scheme's characteristic limiter, with the states of the
+    // last direction reconstructed (one direction per dimensionally split sweep)
+    if (c.flux_scheme == ORC_FS_TVDMU) tvdlimit2_hd(s, qdt, ixO, idims, wLC, wRC, wnew, fC[idims], dxs);
   }
   if (c.fix_small_values) {
     int s2 = handle_small_values(s, false, wnew, ixO);
@@ -1189,7 +1307,7 @@ int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, d
   }
   // addsource2 -> mhd_add_source divB part (src/mod_source.t:130-160)
   if (x.mhd && ndim > 1) {
-    double qsrc = qdt * double(ndim) / double(ndim);
+    double qsrc = qdt * double(s.idhi - s.idlo + 1) / double(ndim);
     if (c.divb == ORC_DIVB_GLM) add_source_glm(s, qsrc, ixI, ixO, wCT, wnew, dxs, cmax_global);
     else if (c.divb == ORC_DIVB_LINDE) add_source_linde(s, qsrc, ixO, wCT, wnew, dxs, jump_faces);
   }
@@ -1216,7 +1334,7 @@ int hancock(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, const d
   Arr<R> wprim = wCT;
   st |= to_primitive(s, ixI, wprim);
   Arr<R> wLp(g, nw), wRp(g, nw), wLC(g, nw), wRC(g, nw), fLC(g, nw), fRC(g, nw);
-  for (int idims = 0; idims < ndim; ++idims) {
+  for (int idims = s.idlo; idims <= s.idhi; ++idims) {
     const int o = g.off(idims);
     const Box hxO = shift(ixO, idims, -1);
     for (int iw = 0; iw < nw; ++iw)
@@ -1236,7 +1354,7 @@ int hancock(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, const d
       });
   }
   if (x.mhd && ndim > 1) {
-    double qsrc = qdt * double(ndim) / double(ndim);
+    double qsrc = qdt * double(s.idhi - s.idlo + 1) / double(ndim);
     if (c.divb == ORC_DIVB_GLM) add_source_glm(s, qsrc, ixI, ixO, wCT, wnew, dxs, cmax_global);
     else if (c.divb == ORC_DIVB_LINDE) add_source_linde(s, qsrc, ixO, wCT, wnew, dxs, jump_faces);
   }
@@ -1330,6 +1448,7 @@ struct Grid {
   std::vector<int> nbr;  // [ib][27] neighbour block or -1 (physical boundary)
   std::vector<double> reg[4];
   size_t bsize;
+  long it = 0;  // steps advanced (the parity of a split step's sweep order)
 };
 
 inline int dir_index(int di, int dj, int dk) { return (di + 1) + 3 * ((dj + 1) + 3 * (dk + 1)); }
@@ -1670,11 +1789,11 @@ int orc_grid_getdt(orc_grid *g, double *dt, double *cmax_global) {
 }
 
 // predictor: the twostep Predictor_Corrector predictor, advect1 with
-// typepred1 (hancock for tvdlf, src/io/mod_input_output.t:787-797).
+// typepred1 (hancock for tvdlf and tvdmu, src/io/mod_input_output.t:787-797).
 static int grid_advect1(orc_grid *g, int ra, int rb, double qdt, double dtfactor, double cmax_global, int nthreads,
                         bool predictor) {
   const size_t bs = g->bsize;
-  const bool hk = predictor && g->s.c.flux_scheme == ORC_FS_TVDLF;
+  const bool hk = predictor && (g->s.c.flux_scheme == ORC_FS_TVDLF || g->s.c.flux_scheme == ORC_FS_TVDMU);
   int st = 0;
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -1807,7 +1926,7 @@ inline void rk4_combine_regs(std::vector<double> *reg) {
 
 // advect threestep/ssprk3 (src/mod_advance.t:56-73, 249-267), coefficients
 // src/io/mod_input_output.t:941-964; fourstep as above.
-int orc_grid_advance(orc_grid *g, double dt, double cmax_global, int nthreads) {
+static int grid_advance_stepper(orc_grid *g, double dt, double cmax_global, int nthreads) {
   if (g->s.c.time_stepper == 2)
     return twostep(
         g->s.c, dt,
@@ -2205,6 +2324,7 @@ namespace orc {
 enum { NT_BOUNDARY = 0, NT_COARSE = 1, NT_SIBLING = 2, NT_FINE = 3 };
 
 struct AmrGrid {
+  long it = 0;  // steps advanced (the parity of a split step's sweep order)
   State s;      // block state (block_nx 16)
   State sc;     // coarse representation (block_nx 8)
   int ndim, nb;
@@ -2499,7 +2619,7 @@ void amr_fix_conserve(AmrGrid &G, std::vector<double> &reg) {
   const Geo &g = G.s.g;
   const double cofi = 1.0 / double(1 << nd);
   for (int b = 0; b < G.nb; ++b)
-    for (int d = 0; d < nd; ++d)
+    for (int d = G.s.idlo; d <= G.s.idhi; ++d)  // idim^LIM
       for (int side = 0; side < 2; ++side) {
         int dd[3] = {0, 0, 0};
         dd[d] = side ? 1 : -1;
@@ -2550,7 +2670,7 @@ void amr_fix_conserve(AmrGrid &G, std::vector<double> &reg) {
 // tvdlf, which stores no fluxes).
 int amr_advect1(AmrGrid &G, int ra, int rb, double qdt, double dtfactor, double cmax_global, int nthreads,
                 bool fix = true) {
-  const bool hk = !fix && G.s.c.flux_scheme == ORC_FS_TVDLF;
+  const bool hk = !fix && (G.s.c.flux_scheme == ORC_FS_TVDLF || G.s.c.flux_scheme == ORC_FS_TVDMU);
   int st = 0;
   const size_t bs = G.bsize;
 #ifdef _OPENMP
@@ -2711,7 +2831,7 @@ void orc_amr_combine_reg(orc_amr *a, int dst, double ca, int ra, double cb, int 
   for (size_t p = 0; p < G->reg[dst].size(); ++p) G->reg[dst][p] = ca * G->reg[ra][p] + cb * G->reg[rb][p];
 }
 
-int orc_amr_advance(orc_amr *a, double dt, double cmax_global, int nthreads) {
+static int amr_advance_stepper(orc_amr *a, double dt, double cmax_global, int nthreads) {
   AmrGrid *G = reinterpret_cast<AmrGrid *>(a);
   if (G->s.c.time_stepper == 2)
     return twostep(
@@ -2745,6 +2865,40 @@ int orc_amr_advance(orc_amr *a, double dt, double cmax_global, int nthreads) {
   orc_amr_combine_reg(a, 0, a31, 0, 1.0 - a31, 2);
   st |= amr_advect1(*G, 2, 0, b33 * dt, b33, cmax_global, nthreads);
   return st;
+}
+
+// advect with dimsplit (src/mod_advance.t:23-45): one full stepper per
+// direction, increasing order on even steps (always with typedimsplit 'xy'),
+// decreasing on odd steps ('xyyx').
+extern "C++" {
+template <class G, class Stepper>
+static int split_advance(G &grid, State &s, Stepper stepper) {
+  int st = 0;
+  if (!s.c.dimsplit) {
+    st = stepper();
+  } else {
+    const int nd = s.c.ndim;
+    const bool fwd = s.c.dimsplit == 2 || (grid.it % 2) == 0;
+    for (int q = 0; q < nd; ++q) {
+      const int d = fwd ? q : nd - 1 - q;
+      s.idlo = s.idhi = d;
+      st |= stepper();
+    }
+    s.idlo = 0;
+    s.idhi = nd - 1;
+  }
+  ++grid.it;
+  return st;
+}
+}  // extern "C++"
+
+int orc_grid_advance(orc_grid *g, double dt, double cmax_global, int nthreads) {
+  return split_advance(*g, g->s, [&]() { return grid_advance_stepper(g, dt, cmax_global, nthreads); });
+}
+
+int orc_amr_advance(orc_amr *a, double dt, double cmax_global, int nthreads) {
+  AmrGrid *G = reinterpret_cast<AmrGrid *>(a);
+  return split_advance(*G, G->s, [&]() { return amr_advance_stepper(a, dt, cmax_global, nthreads); });
 }
 
 // prolong_2nd (src/amr/mod_refine.t:81-167) for a child of a refined block

@@ -22,7 +22,7 @@ extern "C" {
 
 /* Flux scheme ids: values of the reference's fs_* parameters are not used;
  * these are this oracle's own (the names follow mod_finite_volume.t). */
-enum { ORC_FS_TVDLF = 1, ORC_FS_HLL = 2, ORC_FS_HLLC = 3, ORC_FS_HLLD = 4 };
+enum { ORC_FS_TVDLF = 1, ORC_FS_HLL = 2, ORC_FS_HLLC = 3, ORC_FS_HLLD = 4, ORC_FS_TVDMU = 5 };
 /* Limiter ids follow src/limiter/mod_limiter.t:14-24. */
 enum { ORC_LIM_MINMOD = 1, ORC_LIM_WOODWARD = 2, ORC_LIM_MCBETA = 3,
        ORC_LIM_SUPERBEE = 4, ORC_LIM_VANLEER = 5, ORC_LIM_ALBADA = 6,
@@ -64,6 +64,7 @@ typedef struct {
   int ssprk_order;        /* 3 (Gottlieb-Shu) or 2 */
   int time_stepper;       /* 2 twostep, 3 threestep (0 means 3), 4 fourstep */
   int time_integrator;    /* twostep: 0 Predictor_Corrector, 2 ssprk2; fourstep: 0 ssprk4, 1 rk4 */
+  int dimsplit;           /* 0 unsplit, 1 'xyyx', 2 'xy' */
 } orc_cfg;
 
 /* Number of flux variables implied by cfg (sets cfg->nw too). */

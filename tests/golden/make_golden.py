@@ -18,7 +18,8 @@ minmod) ot_2d_2step_tvdlf_mm.log, and MHD HLLC (SSPRK(4,3), koren, Linde)
 ot_2d_4step_hllc_ko.log; and the 2-D blast wave with cont
 boundaries, tests/hd/blast_wave_Cartesian_2D/correct_output/
 bw_2d_{3step_hll_cada,4step_hll_mc,4step_hllc_ko,rk4_tvdlf_cada,
-2step_tvdlf_mm}.log.
+2step_tvdlf_mm,2step_tvdmu_al}.log (the last with TVD-MUSCL, dimensionally
+split).
 They are copied verbatim so the parity tests can run where the reference
 repository is absent.
 """
@@ -46,6 +47,7 @@ LOGS = [
     "tests/hd/blast_wave_Cartesian_2D/correct_output/bw_2d_4step_hllc_ko.log",
     "tests/hd/blast_wave_Cartesian_2D/correct_output/bw_2d_rk4_tvdlf_cada.log",
     "tests/hd/blast_wave_Cartesian_2D/correct_output/bw_2d_2step_tvdlf_mm.log",
+    "tests/hd/blast_wave_Cartesian_2D/correct_output/bw_2d_2step_tvdmu_al.log",
 ]
 
 

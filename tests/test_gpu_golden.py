@@ -215,6 +215,8 @@ def _bw2d_prim(X, Y, Z):
     ("rk4_tvdlf_cada", dict(flux_scheme="tvdlf", limiter="cada3", typeboundspeed="cmaxmean", time_stepper="fourstep",
                             time_integrator="rk4")),
     ("2step_tvdlf_mm", dict(flux_scheme="tvdlf", limiter="minmod", typeboundspeed="cmaxmean", time_stepper="twostep")),
+    ("2step_tvdmu_al", dict(flux_scheme="tvdmu", limiter="albada", typeboundspeed="cmaxmean", time_stepper="twostep",
+                            dimsplit=True)),
 ])
 def test_blast_wave_2d_amr_golden_log_gpu(oracle_lib, name, kw):
     kw = dict(kw, courantpar=0.9)
