@@ -452,7 +452,11 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   if (k.physics != 0 && k.physics != 1) return fail(AMRVAC_E_ARG, "physics must be 0 (hd) or 1 (mhd)");
   const bool fifth = k.limiter == AMRVAC_LIM_MP5 || k.limiter == AMRVAC_LIM_WENO5 ||
                      k.limiter == AMRVAC_LIM_WENOZ5 || k.limiter == AMRVAC_LIM_WENOZP5;
-  if ((k.limiter < 1 || k.limiter > 9) && !fifth) return fail(AMRVAC_E_UNSUPPORTED, "limiter not supported");
+  // reconstructions outside reconstruct_LR's slope-limiter branch (their own kernels)
+  const bool special = fifth || k.limiter == AMRVAC_LIM_VENK || k.limiter == AMRVAC_LIM_WENO3 ||
+                       k.limiter == AMRVAC_LIM_WENOYC3;
+  if ((k.limiter < 1 || k.limiter > 9) && !special) return fail(AMRVAC_E_UNSUPPORTED, "limiter not supported");
+  if (special && k.precision == 1) return fail(AMRVAC_E_UNSUPPORTED, "this limiter is FP64 only");
   if (fifth && k.nghostcells < 3) return fail(AMRVAC_E_ARG, "mp5 / weno5 need nghostcells >= 3");
   if (fifth && k.precision == 1) return fail(AMRVAC_E_UNSUPPORTED, "mp5 / weno5 are FP64 only");
   if (k.typeboundspeed < 1 || k.typeboundspeed > 3) return fail(AMRVAC_E_ARG, "bad typeboundspeed");
@@ -494,10 +498,12 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   KernelKey key{k.physics == 1, k.ndim, k.ndir, k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM,
                 k.flux_scheme, k.limiter, k.typeboundspeed, k.precision == 1};
   if (k.precision != 0 && k.precision != 1) return fail(AMRVAC_E_ARG, "precision must be 0 (fp64) or 1 (mixed)");
-  if (std::getenv("AMRVAC_GENERIC_KERNELS") && !fifth) { key.limiter = 0; key.boundspeed = 0; }
-  if (fifth && k.limiter != AMRVAC_LIM_MP5) key.limiter = LIM_WENO5;  // one kernel family, variant at run time
-  bool found = fifth ? (lookup_mp5_hd(key, &c->ks) || lookup_mp5_mhd(key, &c->ks))
-                     : (lookup_hd(key, &c->ks) || lookup_mhd2(key, &c->ks) || lookup_mhd3(key, &c->ks));
+  if (std::getenv("AMRVAC_GENERIC_KERNELS") && !special) { key.limiter = 0; key.boundspeed = 0; }
+  // one kernel per family, the variant read at run time
+  if (fifth && k.limiter != AMRVAC_LIM_MP5) key.limiter = LIM_WENO5;
+  if (k.limiter == AMRVAC_LIM_WENOYC3) key.limiter = LIM_WENO3;
+  bool found = special ? (lookup_mp5_hd(key, &c->ks) || lookup_mp5_mhd(key, &c->ks))
+                       : (lookup_hd(key, &c->ks) || lookup_mhd2(key, &c->ks) || lookup_mhd3(key, &c->ks));
   if (!found) {
     delete c;
     return fail(AMRVAC_E_UNSUPPORTED, key.mixed ? "no mixed-precision kernel for this scheme"

@@ -1,6 +1,7 @@
 // Stage kernels with the fifth-order reconstructions (three-cell halo) for
 // hydrodynamics, 2-D and 3-D, HLL and HLLC: MP5, and the WENO5 family (one
-// kernel, variant at run time).
+// kernel, variant at run time); and, on the two-cell halo, the WENO3 family
+// and the Venkatakrishnan limiter.
 #include "kernels.cuh"
 
 namespace amrvac {
@@ -14,6 +15,14 @@ bool lookup_mp5_hd(const KernelKey &k, KernelSet *out) {
   }                                                                                       \
   if (k.ndim == ND && k.solver == S && k.limiter == LIM_WENO5) {                          \
     *out = Launch<false, ND, false, ND, S, LIM_WENO5>::set();                             \
+    return true;                                                                          \
+  }                                                                                       \
+  if (k.ndim == ND && k.solver == S && k.limiter == LIM_WENO3) {                          \
+    *out = Launch<false, ND, false, ND, S, LIM_WENO3>::set();                             \
+    return true;                                                                          \
+  }                                                                                       \
+  if (k.ndim == ND && k.solver == S && k.limiter == LIM_VENK) {                           \
+    *out = Launch<false, ND, false, ND, S, LIM_VENK>::set();                              \
     return true;                                                                          \
   }
   AMRVAC_MP5_HD(2, SOLVER_HLL)

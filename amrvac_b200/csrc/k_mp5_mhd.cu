@@ -1,6 +1,6 @@
 // Stage kernels with the fifth-order reconstructions (three-cell halo) for
 // MHD: 2-D with two or three vector components, 3-D; GLM or not; HLL and
-// HLLD; MP5 and the WENO5 family.
+// HLLD; MP5, the WENO5 and WENO3 families and the Venkatakrishnan limiter.
 #include "kernels.cuh"
 
 namespace amrvac {
@@ -14,6 +14,14 @@ bool lookup_mp5_mhd(const KernelKey &k, KernelSet *out) {
   }                                                                                             \
   if (k.ndim == ND && k.ndir == NDIR && k.glm == GLM && k.solver == S && k.limiter == LIM_WENO5) { \
     *out = Launch<true, NDIR, GLM, ND, S, LIM_WENO5>::set();                                    \
+    return true;                                                                                \
+  }                                                                                             \
+  if (k.ndim == ND && k.ndir == NDIR && k.glm == GLM && k.solver == S && k.limiter == LIM_WENO3) { \
+    *out = Launch<true, NDIR, GLM, ND, S, LIM_WENO3>::set();                                    \
+    return true;                                                                                \
+  }                                                                                             \
+  if (k.ndim == ND && k.ndir == NDIR && k.glm == GLM && k.solver == S && k.limiter == LIM_VENK) { \
+    *out = Launch<true, NDIR, GLM, ND, S, LIM_VENK>::set();                                     \
     return true;                                                                                \
   }
   AMRVAC_MP5_M(2, 2, false, SOLVER_HLL)

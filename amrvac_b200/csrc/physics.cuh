@@ -16,7 +16,8 @@ namespace amrvac {
 // Limiter ids as in src/limiter/mod_limiter.t:14-24.
 enum : int { LIM_MINMOD = 1, LIM_WOODWARD = 2, LIM_MCBETA = 3, LIM_SUPERBEE = 4,
              LIM_VANLEER = 5, LIM_ALBADA = 6, LIM_KOREN = 7, LIM_CADA = 8, LIM_CADA3 = 9,
-             LIM_MP5 = 13, LIM_WENO5 = 16, LIM_WENOZ5 = 18, LIM_WENOZP5 = 20 };
+             LIM_VENK = 11, LIM_MP5 = 13, LIM_WENO3 = 14, LIM_WENOYC3 = 15, LIM_WENO5 = 16,
+             LIM_WENOZ5 = 18, LIM_WENOZP5 = 20 };
 enum : int { BS_EINFELDT = 1, BS_CMAXMEAN = 2, BS_CMAXLEFTRIGHT = 3 };
 enum : int { SOLVER_TVDLF = 1, SOLVER_HLL = 2, SOLVER_HLLC = 3, SOLVER_HLLD = 4, SOLVER_TVDMU = 5,
              SOLVER_HANCOCK = 8 };

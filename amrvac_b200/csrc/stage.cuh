@@ -320,6 +320,50 @@ __device__ __forceinline__ double weno5_side(double wmm, double wm, double w0, d
   return ((0.0 + f1 * a1 / asum) + f2 * a2 / asum) + f3 * a3 / asum;
 }
 
+// WENO3 family (WENO3limiter, src/limiter/mod_weno.t:165-252; var 1 WENO3,
+// 2 WENO-YC3 with dx^2 in the weights): the left state at face i+1/2 from
+// w(i-1), w(i), w(i+1); the right state on the mirrored data w(i+2), w(i+1),
+// w(i) (the smoothness indicators are squares, so the mirror is exact).
+__device__ __forceinline__ double weno3_side(double wm, double w0, double wp, int var, double dx2) {
+  constexpr double eps = 1.0e-18;  // weno_eps_machine
+  const double f1 = (-1.0 / 2.0) * wm + (3.0 / 2.0) * w0;
+  const double f2 = (1.0 / 2.0) * w0 + (1.0 / 2.0) * wp;
+  const double d1 = w0 - wm, d2 = wp - w0;
+  const double be1 = d1 * d1, be2 = d2 * d2;
+  double a1, a2;
+  if (var == 1) {
+    a1 = (1.0 / 3.0) / ((be1 + eps) * (be1 + eps));
+    a2 = (2.0 / 3.0) / ((be2 + eps) * (be2 + eps));
+  } else {
+    const double tau = fabs(be2 - be1);
+    a1 = (1.0 / 3.0) * (1.0 + tau / (be1 + dx2));
+    a2 = (2.0 / 3.0) * (1.0 + tau / (be2 + dx2));
+  }
+  const double asum = (0.0 + a1) + a2;
+  return (0.0 + f1 * a1 / asum) + f2 * a2 / asum;
+}
+
+// Venkatakrishnan's limiter function phi of one cell from w(i-1), w(i),
+// w(i+1) (venklimiter, src/limiter/mod_venk.t:6-106; k = 0.3, omega = 1e-12,
+// eps2 = (k dx)^3).
+__device__ __forceinline__ double venk_phi(double wm, double w0, double wp, double eps2) {
+  constexpr double omega = 1.0e-12;
+  const double wmax = fmax(fmax(wm, w0), wp), wmin = fmin(fmin(wm, w0), wp);
+  const double westp = w0 + (wp - wm) * 0.25, westm = w0 - (wp - wm) * 0.25;
+  auto ratio = [&](double dp, double dmr) {
+    const double dm = copysign(fabs(dmr) + omega, dmr);
+    const double p1 = (dp * dp + eps2) + 2.0 * dp * dm;
+    const double p2 = ((dp * dp + 2.0 * (dm * dm)) + dp * dm) + eps2;
+    return p1 / p2;
+  };
+  double phip = 1.0, phim = 1.0;
+  if (westp > w0) phip = ratio(wmax - w0, westp - w0);
+  else if (westp < w0) phip = ratio(wmin - w0, westp - w0);
+  if (westm < w0) phim = ratio(-(wmax - w0), westm - w0);
+  else if (westm > w0) phim = ratio(-(wmin - w0), westm - w0);
+  return fmin(phim, phip);
+}
+
 // Halo width of the staged tile: two cells for the slope limiters, three for
 // the fifth-order reconstructions (face stencil i-2 .. i+3).  LIM_WENO5 as a
 // template argument stands for the whole WENO5 family (variant at run time).
@@ -751,6 +795,45 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
               wRp[v] = smem[base[3] + ov * strd[3]];
             }
           }
+        } else if constexpr (LIM == LIM_WENO3) {
+          static_assert(FP64, "WENO3 is FP64 only");
+          // WENO3limiter then fix_limiter (all variables flat where density or
+          // pressure is flagged in either state)
+          const int var = P.limiter == LIM_WENO3 ? 1 : 2;
+          const double dxd = FD == 0 ? dx[0] : (FD == 1 ? dx[1] : dx[2]);
+          const double dx2 = dxd * dxd;
+#pragma unroll
+          for (int v = 0; v < NW; ++v) {
+            const int ov = orig_index_rt<MHD, NDIR>(v, FD);
+            double q[4];
+#pragma unroll
+            for (int o = 0; o < 4; ++o) q[o] = smem[base[o] + ov * strd[o]];
+            wLp[v] = weno3_side(q[0], q[1], q[2], var, dx2);
+            wRp[v] = weno3_side(q[3], q[2], q[1], var, dx2);
+          }
+          if (wLp[V::RHO] < P.small_density || wRp[V::RHO] < P.small_density || wLp[V::E] < P.small_pressure ||
+              wRp[V::E] < P.small_pressure) {
+#pragma unroll
+            for (int v = 0; v < NW; ++v) {
+              const int ov = orig_index_rt<MHD, NDIR>(v, FD);
+              wLp[v] = smem[base[1] + ov * strd[1]];
+              wRp[v] = smem[base[2] + ov * strd[2]];
+            }
+          }
+        } else if constexpr (LIM == LIM_VENK) {
+          static_assert(FP64, "the Venkatakrishnan limiter is FP64 only");
+          const double dxd = FD == 0 ? dx[0] : (FD == 1 ? dx[1] : dx[2]);
+          const double kd = 0.3 * dxd;
+          const double eps2 = kd * kd * kd;
+#pragma unroll
+          for (int v = 0; v < NW; ++v) {
+            const int ov = orig_index_rt<MHD, NDIR>(v, FD);
+            double q[4];
+#pragma unroll
+            for (int o = 0; o < 4; ++o) q[o] = smem[base[o] + ov * strd[o]];
+            wLp[v] = q[1] + 0.25 * (q[2] - q[0]) * venk_phi(q[0], q[1], q[2], eps2);
+            wRp[v] = q[2] - 0.25 * (q[3] - q[1]) * venk_phi(q[1], q[2], q[3], eps2);
+          }
         } else {
 #pragma unroll
           for (int v = 0; v < NW; ++v) {
@@ -767,7 +850,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
         // the MP5 / WENO branches of reconstruct_LR have no small-value fix of
         // the states
         stb |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, TF(cg), Fr,
-                                                                       HW == 2);
+                                                                       HW == 2 && LIM != LIM_WENO3);
         if constexpr (!FP64) {
           bool finite = true;
 #pragma unroll

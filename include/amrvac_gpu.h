@@ -59,7 +59,10 @@ extern "C" {
 #define AMRVAC_LIM_KOREN    7
 #define AMRVAC_LIM_CADA     8
 #define AMRVAC_LIM_CADA3    9
+#define AMRVAC_LIM_VENK     11  /* Venkatakrishnan */
 #define AMRVAC_LIM_MP5      13  /* fifth order, uniform grids, nghostcells >= 3 */
+#define AMRVAC_LIM_WENO3    14  /* third-order WENO */
+#define AMRVAC_LIM_WENOYC3  15  /* third-order WENO-YC */
 #define AMRVAC_LIM_WENO5    16  /* WENO-JS, likewise */
 #define AMRVAC_LIM_WENOZ5   18  /* WENO-Z, likewise */
 #define AMRVAC_LIM_WENOZP5  20  /* WENO-Z+, likewise */

@@ -643,6 +643,46 @@ template <class R> R weno5_side(R wmm, R wm, R w0, R wp, R wpp, int var, R lambd
   return out;
 }
 
+// WENO3limiter (src/limiter/mod_weno.t:165-252), one variable of one face;
+// var 1 WENO3, 2 WENO-YC3.  Left state from w(i-1), w(i), w(i+1); the right
+// state on the mirrored data w(i+2), w(i+1), w(i).
+template <class R> R weno3_side(R wm, R w0, R wp, int var, double dx2) {
+  const double eps = 1.0e-18;
+  R f1 = R(-1.0 / 2.0) * wm + R(3.0 / 2.0) * w0;
+  R f2 = R(1.0 / 2.0) * w0 + R(1.0 / 2.0) * wp;
+  R be1 = (w0 - wm) * (w0 - wm), be2 = (wp - w0) * (wp - w0);
+  R a1, a2;
+  if (var == 1) {
+    a1 = R(1.0 / 3.0) / ((be1 + R(eps)) * (be1 + R(eps)));
+    a2 = R(2.0 / 3.0) / ((be2 + R(eps)) * (be2 + R(eps)));
+  } else {
+    R tau = rabs(be2 - be1);
+    a1 = R(1.0 / 3.0) * (R(1.0) + tau / (be1 + R(dx2)));
+    a2 = R(2.0 / 3.0) * (R(1.0) + tau / (be2 + R(dx2)));
+  }
+  R asum = (R(0.0) + a1) + a2;
+  return (R(0.0) + f1 * a1 / asum) + f2 * a2 / asum;
+}
+
+// venklimiter (src/limiter/mod_venk.t:6-106): phi of one cell.
+template <class R> R venk_phi(R wm, R w0, R wp, R eps2) {
+  const double omega = 1.0e-12;
+  R wmax = rmax(rmax(wm, w0), wp), wmin = rmin(rmin(wm, w0), wp);
+  R westp = w0 + (wp - wm) * R(0.25), westm = w0 - (wp - wm) * R(0.25);
+  auto ratio = [&](R dp, R dmr) {
+    R dm = rsign(val(rabs(dmr)) + omega, dmr);
+    R p1 = (dp * dp + eps2) + R(2.0) * dp * dm;
+    R p2 = dp * dp + R(2.0) * (dm * dm) + dp * dm + eps2;
+    return p1 / p2;
+  };
+  R phip(1.0), phim(1.0);
+  if (westp > w0) phip = ratio(wmax - w0, westp - w0);
+  else if (westp < w0) phip = ratio(wmin - w0, westp - w0);
+  if (westm < w0) phim = ratio(-(wmax - w0), westm - w0);
+  else if (westm > w0) phim = ratio(-(wmin - w0), westm - w0);
+  return rmin(phim, phip);
+}
+
 // reconstruct_LR default (limiter) branch (src/mod_finite_volume.t:1110-1228)
 // and its MP5 branch (1131-1132: MP5limiter with fix_limiter1,
 // src/limiter/mod_weno.t:135-163; no small-value fix of the states)
@@ -652,6 +692,59 @@ int reconstruct_LR(const State &s, const Box &ixL, const Box &ixR, int idims, co
   const Ix &x = s.x;
   const Geo &g = s.g;
   const int o = g.off(idims);
+  if (s.c.limiter == ORC_LIM_VENK) {
+    // venklimiter, then the small-value fix of both states (1157-1162)
+    const R kd = R(0.3) * R(dxdim);
+    const R eps2 = kd * kd * kd;
+    for (int iw = 0; iw < x.nw; ++iw)
+      forbox(ixL, [&](int i, int j, int k) {
+        const size_t p = g.idx(i, j, k) + g.cells * (size_t)iw;
+        const R *q = &w.d[p];
+        wLp.d[p] = q[0] + R(0.25) * (q[o] - q[-o]) * venk_phi(q[-o], q[0], q[o], eps2);
+        wRp.d[p] = q[o] - R(0.25) * (q[2 * o] - q[0]) * venk_phi(q[0], q[o], q[2 * o], eps2);
+      });
+    int st = 0;
+    if (s.c.fix_small_values) {
+      st |= handle_small_values(s, true, wLp, ixL);
+      st |= handle_small_values(s, true, wRp, ixR);
+    }
+    for (int iw = 0; iw < x.nw; ++iw) {
+      forbox(ixL, [&](int i, int j, int k) { wLC(i, j, k, iw) = wLp(i, j, k, iw); });
+      forbox(ixR, [&](int i, int j, int k) { wRC(i, j, k, iw) = wRp(i, j, k, iw); });
+    }
+    to_conserved(s, ixL, wLC);
+    to_conserved(s, ixR, wRC);
+    return st;
+  }
+  if (s.c.limiter == ORC_LIM_WENO3 || s.c.limiter == ORC_LIM_WENOYC3) {
+    // WENO3limiter then fix_limiter (any flagged density or pressure: every
+    // variable of the face flat)
+    const int var = s.c.limiter == ORC_LIM_WENO3 ? 1 : 2;
+    const double dx2 = dxdim * dxdim;
+    forbox(ixL, [&](int i, int j, int k) {
+      const size_t p = g.idx(i, j, k);
+      R wl[16], wr[16];
+      for (int iw = 0; iw < x.nw; ++iw) {
+        const R *q = &w.d[p + g.cells * (size_t)iw];
+        wl[iw] = weno3_side(q[-o], q[0], q[o], var, dx2);
+        wr[iw] = weno3_side(q[2 * o], q[o], q[0], var, dx2);
+      }
+      const bool flag = wl[x.rho] < R(s.c.small_density) || wr[x.rho] < R(s.c.small_density) ||
+                        wl[x.e] < R(s.c.small_pressure) || wr[x.e] < R(s.c.small_pressure);
+      if (flag) return;
+      for (int iw = 0; iw < x.nw; ++iw) {
+        wLp.d[p + g.cells * (size_t)iw] = wl[iw];
+        wRp.d[p + g.cells * (size_t)iw] = wr[iw];
+      }
+    });
+    for (int iw = 0; iw < x.nw; ++iw) {
+      forbox(ixL, [&](int i, int j, int k) { wLC(i, j, k, iw) = wLp(i, j, k, iw); });
+      forbox(ixR, [&](int i, int j, int k) { wRC(i, j, k, iw) = wRp(i, j, k, iw); });
+    }
+    to_conserved(s, ixL, wLC);
+    to_conserved(s, ixR, wRC);
+    return 0;
+  }
   if (s.c.limiter == ORC_LIM_WENO5 || s.c.limiter == ORC_LIM_WENOZ5 || s.c.limiter == ORC_LIM_WENOZP5) {
     // WENO5limiter then fix_limiter (src/limiter/mod_weno.t:100-133): any
     // flagged density or pressure keeps every variable of the face flat

@@ -54,6 +54,12 @@ CASES = {
                                             typedivbfix="glm", typeboundspeed="cmaxmean"),
     "mhd3_hllc_minmod_glm": dict(physics="mhd", ndim=3, flux_scheme="hllc", limiter="minmod", typedivbfix="glm"),
     "mhd3_hllc_cada3_none": dict(physics="mhd", ndim=3, flux_scheme="hllc", limiter="cada3", typedivbfix="none"),
+    # WENO3 family and the Venkatakrishnan limiter (two ghost cells)
+    "hd2_hllc_weno3": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hllc", limiter="weno3"),
+    "mhd25_hlld_wenoyc3_glm": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hlld", limiter="wenoyc3",
+                                   typedivbfix="glm"),
+    "hd3_hll_venk": dict(physics="hd", ndim=3, gamma=1.4, flux_scheme="hll", limiter="venk"),
+    "mhd2_hll_venk_linde": dict(physics="mhd", ndim=2, flux_scheme="hll", limiter="venk", typedivbfix="linde"),
     # twostep Predictor_Corrector with tvdlf: the MUSCL-Hancock predictor
     "hd2_tvdlf_vanleer_hancock": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="tvdlf", limiter="vanleer",
                                       time_stepper="twostep"),

@@ -7,8 +7,10 @@ src/limiter/mod_mp5.t:16-201: the (2, -13, 47, 27, -3)/60 interpolant with
 its monotonicity limits inactive on smooth data) must cut the L1 error of the
 cell averages by about 2^5 per doubling of the resolution when the time
 error is small (CFL 0.1); so must the WENO5 family (WENO5limiter,
-src/limiter/mod_weno.t:254-377: WENO-JS, WENO-Z, WENO-Z+).  Slope limiters
-stay near second order.
+src/limiter/mod_weno.t:254-377: WENO-JS, WENO-Z, WENO-Z+).  WENO-YC3
+(WENO3limiter var 2, mod_weno.t:165-252) is third order (2^3); the
+Venkatakrishnan limiter (src/limiter/mod_venk.t) and the slope limiters stay
+near second order.
 """
 import numpy as np
 import pytest
@@ -48,6 +50,7 @@ def _l1_error(O, n, limiter, nghost, cfl=0.1, tend=0.1, time_stepper="threestep"
 
 @pytest.mark.parametrize("limiter,nghost,lo,hi", [("mp5", 3, 24.0, 40.0), ("weno5", 3, 24.0, 40.0),
                                                    ("wenoz5", 3, 24.0, 40.0), ("wenozp5", 3, 24.0, 40.0),
+                                                   ("wenoyc3", 2, 6.5, 9.5), ("venk", 2, 3.8, 5.8),
                                                    ("minmod", 2, 2.5, 4.5)])
 def test_convergence_order_on_smooth_wave(oracle_lib, limiter, nghost, lo, hi):
     e32 = _l1_error(oracle_lib, 32, limiter, nghost)
