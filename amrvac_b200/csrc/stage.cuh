@@ -6,7 +6,7 @@
 //     reconstruction (reconstruct_LR 1110-1228), GLM modify_wLR, physical
 //     fluxes, signal-speed bounds, Riemann flux, conservative update;
 //   the SSP-RK stage combination (src/mod_advance.t:249-267);
-//   the unsplit divB sources (add_source_glm / add_source_linde,
+//   the divB sources (add_source_glm / add_source_linde,
 //     src/mhd/mod_mhd_phys.t:5472-5531, 5599-5665);
 //   the same-resolution ghost fill (bc_fill_srl, src/mod_ghostcells_update.t:
 //     812-852) and cont/symm/asymm physical boundaries, done as a gather from
@@ -15,12 +15,17 @@
 // Layout in HBM: pool[block][var][z][y][x], interior cells only, 16^d per
 // block and variable (2 KB rows of 16 doubles).  No ghost cells are stored.
 //
-// CTA organisation (3-D): 288 threads march over the z-planes of the tile.
-// Shared memory holds a ring of 4 primitive planes (k-1..k+2, 16x16 each),
-// the x/y halo strips of plane k, and one buffer of scaled face fluxes.
-// Per plane: x-faces (17x16 = 272, one per thread), per-cell accumulation,
-// y-faces (16x17), accumulation, then each cell thread computes its own
-// z-face k+1/2 and keeps the k-1/2 flux in registers.
+// CTA organisation (3-D): 256 threads march over the z-planes of the tile.
+// Shared memory holds a ring of 2 HW primitive planes (HW = 2 halo cells,
+// 3 for the fifth-order reconstructions; planes k-HW+1 .. k+HW, 16x16 each),
+// the x/y halo strips of plane k, one buffer of scaled face fluxes and a
+// 16-face side buffer.  Per plane: the 17x16 x-faces together with the 16
+// y-faces of the top row (288 faces: a second round of one warp), per-cell
+// accumulation, the remaining 16x16 y-faces, accumulation, then each cell
+// thread computes its own z-face k+1/2 and keeps the k-1/2 flux in
+// registers.  Variants of the same kernel: the MUSCL-Hancock predictor
+// (per-cell edge fluxes, no Riemann solver) and dimensionally split sweeps
+// (one direction per launch).
 #pragma once
 
 #include <cuda_runtime.h>
