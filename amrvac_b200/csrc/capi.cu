@@ -486,8 +486,9 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   // The reference's unsplit TVD-MUSCL limits every direction with the states
   // reconstructed for the last one (finite_volume's flux and update loops are
   // separate); its tests run TVD-MUSCL dimensionally split only.
-  if (k.flux_scheme == AMRVAC_FS_TVDMU && (k.physics != 0 || !k.dimsplit || k.precision == 1))
-    return fail(AMRVAC_E_UNSUPPORTED, "tvdmu: hd, dimsplit, FP64");
+  if (k.flux_scheme == AMRVAC_FS_TVDMU &&
+      (!k.dimsplit || k.precision == 1 || (k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM)))
+    return fail(AMRVAC_E_UNSUPPORTED, "tvdmu: dimsplit, FP64, no GLM");
   const int nw = nw_of(cfg);
   if (nw > AMRVAC_MAX_NW) return fail(AMRVAC_E_UNSUPPORTED, "too many variables");
   amrvac_ctx *c = new amrvac_ctx();

@@ -27,6 +27,8 @@ bool lookup_mhd2(const KernelKey &k, KernelSet *out) {
   AMRVAC_M2(2, false, SOLVER_TVDLF)
   AMRVAC_M2(2, false, SOLVER_HLL)
   AMRVAC_M2(2, false, SOLVER_HLLD)
+  AMRVAC_M2(2, false, SOLVER_TVDMU)
+  AMRVAC_M2(3, false, SOLVER_TVDMU)
   AMRVAC_M2(2, true, SOLVER_TVDLF)
   AMRVAC_M2(2, true, SOLVER_HLL)
   AMRVAC_M2(2, true, SOLVER_HLLD)

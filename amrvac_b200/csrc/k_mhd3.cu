@@ -27,6 +27,7 @@ bool lookup_mhd3(const KernelKey &k, KernelSet *out) {
   AMRVAC_M3(false, SOLVER_TVDLF)
   AMRVAC_M3(false, SOLVER_HLL)
   AMRVAC_M3(false, SOLVER_HLLD)
+  AMRVAC_M3(false, SOLVER_TVDMU)
   AMRVAC_M3(true, SOLVER_TVDLF)
   AMRVAC_M3(true, SOLVER_HLL)
   AMRVAC_M3(true, SOLVER_HLLD)

@@ -262,6 +262,167 @@ __device__ __forceinline__ void riemann_tvdmu_hd(const T *wLC, const T *wRC, con
   }
 }
 
+// TVD-MUSCL for MHD (no GLM): the central flux with tvdlimit2's
+// characteristic limiter folded in, the Roe system of src/mhd/mod_mhd_roe.t
+// (average2 61-146 with arithmetic averages, geteigenjump2 160-342,
+// rtimes2 355-506; divbwave on, typeentropy 'nul').  The waves are taken in
+// the reference's order il = 1..nwflux: Alfven R/L, fast R/L, slow R/L, then
+// (ndir 3 only: nwflux = 8) the divB and entropy waves — with ndir 2
+// (nwflux = 6) the limiter loop never reaches those two.  Rotated states:
+// idim = component 0, idir = 1, jdir = 2 (ndir 3) or 0 (ndir 2, where the
+// reference's jdir = idir + 1 - ndir (idir / ndir) wraps to idim).
+template <class T, int NDIR>
+__device__ __forceinline__ void riemann_tvdmu_mhd(const T *wLC, const T *wRC, const T *fL, const T *fR,
+                                                  const PhysParams &P, T *F) {
+  using V = Vars<true, NDIR, false>;
+  constexpr int NW = V::NW, RHO = V::RHO, E = V::E, M = V::M0, B = V::B0;
+  constexpr int ID = 1, JD = NDIR == 3 ? 2 : 0;
+  constexpr T smalld = T(1.0e-12);
+#pragma unroll
+  for (int v = 0; v < NW; ++v) F[v] = T(0.5) * (fL[v] + fR[v]);
+  const T g = T(P.gamma);
+  auto pth = [&](const T *w) {  // mhd_get_pthermal_origin
+    T m2 = w[M] * w[M], b2 = w[B] * w[B];
+#pragma unroll
+    for (int c = 1; c < NDIR; ++c) { m2 = m2 + w[M + c] * w[M + c]; b2 = b2 + w[B + c] * w[B + c]; }
+    T p = T(P.gamma - 1.0) * (w[E] - T(0.5) * (m2 / w[RHO] + b2));
+    if (P.fix_small_values && p < T(P.small_pressure)) p = T(P.small_pressure);
+    return p;
+  };
+  // average2
+  T rho = T(0.5) * (wLC[RHO] + wRC[RHO]);
+  T v[NDIR], b[NDIR], dv[NDIR], db[NDIR];
+#pragma unroll
+  for (int c = 0; c < NDIR; ++c) {
+    v[c] = T(0.5) * (wLC[M + c] / wLC[RHO] + wRC[M + c] / wRC[RHO]);
+    b[c] = T(0.5) * (wLC[B + c] + wRC[B + c]);
+    dv[c] = wRC[M + c] / wRC[RHO] - wLC[M + c] / wLC[RHO];
+    db[c] = wRC[B + c] - wLC[B + c];
+  }
+  const T pL = pth(wLC), pR = pth(wRC);
+  const T pav = T(0.5) * (pL + pR);
+  const T dp = pR - pL;
+  const T rhodv = wRC[M] - wLC[M] - v[0] * (wRC[RHO] - wLC[RHO]);
+  const T cs2 = g * pav / rho;
+  T bb = b[0] * b[0];
+#pragma unroll
+  for (int c = 1; c < NDIR; ++c) bb = bb + b[c] * b[c];
+  T cf = bb / rho + cs2;
+  T cl = T(0.5) * (cf - sqrt(cf * cf - T(4.0) * cs2 * (b[0] * b[0]) / rho));
+  cf = cf - cl;
+  T af = (cs2 - cl) / (cf - cl);
+  af = fmin(T(1.0), fmax(af, T(0.0)));
+  const T as = sqrt(T(1.0) - af);
+  af = sqrt(af);
+  cf = sqrt(cf);
+  cl = sqrt(cl);
+  rho = sqrt(rho);
+  if (fabs(b[0]) < smalld) b[0] = smalld;
+  if constexpr (NDIR == 2) {
+    b[ID] = b[ID] >= T(0.0) ? T(1.0) : T(-1.0);
+  } else {
+    const T tmp = sqrt(b[1] * b[1] + b[2] * b[2]);
+    if (tmp > smalld) { b[1] = b[1] / tmp; b[2] = b[2] / tmp; }
+    else { b[1] = sqrt(T(0.5)); b[2] = sqrt(T(0.5)); }
+  }
+  const T u = v[0];
+  const T sgn = copysign(T(1.0), b[0]);
+  const T sqcs2 = sqrt(cs2);
+  T v2 = v[0] * v[0];
+#pragma unroll
+  for (int c = 1; c < NDIR; ++c) v2 = v2 + v[c] * v[c];
+  const T v2a2 = T(0.5) * v2 + (T(2.0) - g) / (g - T(1.0)) * cs2;
+  // Alfven waves
+  const T bdvA = ((b[JD] * dv[ID] - b[ID] * dv[JD]) * T(0.5)) * (rho * rho);
+  const T bdbA = ((b[JD] * db[ID] - b[ID] * db[JD]) * T(0.5)) * copysign(rho, b[0]);
+  const T bvA = b[JD] * v[ID] - b[ID] * v[JD];
+  // fast and slow waves
+  T bdvF = b[ID] * dv[ID], bdbF = b[ID] * db[ID], bvF = b[ID] * v[ID];
+  if constexpr (NDIR == 3) {
+    bdvF = bdvF + b[JD] * dv[JD];
+    bdbF = bdbF + b[JD] * db[JD];
+    bvF = bvF + b[JD] * v[JD];
+  }
+  bdvF = bdvF * copysign(rho * rho, b[0]);
+  bdbF = (bdbF * sqcs2) * rho;
+  bvF = bvF * sgn;
+  const T h = T(0.5) / cs2;
+  T D[NW];
+#pragma unroll
+  for (int w = 0; w < NW; ++w) D[w] = T(0.0);
+  // il = alfvR, alfvL, fastR, fastL, slowR, slowL (then divB, entropy for ndir 3)
+#pragma unroll
+  for (int il = 0; il < (NDIR == 3 ? 8 : 6); ++il) {
+    T a, jump;
+    switch (il) {
+      case 0: a = u + fabs(b[0]) / rho; jump = bdvA - bdbA; break;
+      case 1: a = u - fabs(b[0]) / rho; jump = -bdvA - bdbA; break;
+      case 2: a = u + cf; jump = h * (af * (cf * rhodv + dp) + as * (-cl * bdvF + bdbF)); break;
+      case 3: a = u - cf; jump = h * (af * (-cf * rhodv + dp) + as * (cl * bdvF + bdbF)); break;
+      case 4: a = u + cl; jump = h * (as * (cl * rhodv + dp) + af * (cf * bdvF - bdbF)); break;
+      case 5: a = u - cl; jump = h * (as * (-cl * rhodv + dp) + af * (-cf * bdvF - bdbF)); break;
+      case 6: a = u; jump = db[0]; break;
+      default: a = u; jump = (wRC[RHO] - wLC[RHO]) - dp / cs2; break;
+    }
+    const T q = fabs(a) * jump;
+    const bool fast = il == 2 || il == 3, slow = il == 4 || il == 5, alf = il < 2;
+    const T pm = (il == 2 || il == 4) ? T(1.0) : T(-1.0);  // R / L of fast and slow
+    // rtimes2 rows
+    T r_rho, r_e, r_mn, r_bn;
+    if (fast) {
+      r_rho = q * af;
+      r_e = q * (-pm * as * cl * bvF + af * (v2a2 + cf * (cf + pm * u)));
+      r_mn = (q * af) * (u + pm * cf);
+    } else if (slow) {
+      r_rho = q * as;
+      r_e = q * (pm * af * cf * bvF + as * (v2a2 + cl * (cl + pm * u)));
+      r_mn = (q * as) * (u + pm * cl);
+    } else if (alf) {
+      r_rho = T(0.0);
+      r_e = il == 0 ? q * bvA : -q * bvA;
+      r_mn = T(0.0);
+    } else if (il == 6) {
+      r_rho = T(0.0);
+      r_e = q * b[0];
+      r_mn = T(0.0);
+    } else {
+      r_rho = q;
+      r_e = q * T(0.5) * v2;
+      r_mn = q * u;
+    }
+    r_bn = il == 6 ? q : T(0.0);
+    D[RHO] = D[RHO] + T(0.5) * r_rho;
+    D[E] = D[E] + T(0.5) * r_e;
+    D[M] = D[M] + T(0.5) * r_mn;
+    D[B] = D[B] + T(0.5) * r_bn;
+#pragma unroll
+    for (int t = 1; t < NDIR; ++t) {
+      T r_m, r_b;
+      if (fast) {
+        r_m = q * (af * v[t] - pm * as * cl * b[t] * sgn);
+        r_b = ((q * as) * sqcs2) * b[t] / rho;
+      } else if (slow) {
+        r_m = q * (as * v[t] + pm * af * cf * b[t] * sgn);
+        r_b = -((q * af) * sqcs2) * b[t] / rho;
+      } else if (alf) {
+        const T s = il == 0 ? T(1.0) : T(-1.0);
+        r_m = t == ID ? s * q * b[JD] : -s * q * b[ID];
+        r_b = t == ID ? -q * b[JD] / copysign(rho, b[0]) : q * b[ID] / copysign(rho, b[0]);
+      } else if (il == 6) {
+        r_m = T(0.0);
+        r_b = T(0.0);
+      } else {
+        r_m = q * v[t];
+        r_b = T(0.0);
+      }
+      D[M + t] = D[M + t] + T(0.5) * r_m;
+      D[B + t] = D[B + t] + T(0.5) * r_b;
+    }
+  }
+#pragma unroll
+  for (int w = 0; w < NW; ++w) F[w] = F[w] - D[w];
+}
+
 // get_Riemann_flux_hlld (mod_finite_volume.t:507-729), no B0 / equilibrium split.
 template <class T, int NDIR, bool GLM, int NDIM, int D>
 __device__ __forceinline__ void riemann_hlld(const T *wLC, const T *wRC, const T *wLp,

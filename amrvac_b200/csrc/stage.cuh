@@ -233,9 +233,13 @@ __device__ __forceinline__ uint32_t face_from_states(T *wLp, T *wRp, const PhysP
   phys_flux<T, MHD, NDIR, GLM, D>(wRC, wRp, cg, fR);
   T cmax, cmin = T(0.0);
   if constexpr (SOLVER == SOLVER_TVDMU) {
-    static_assert(!MHD, "TVD-MUSCL is implemented for HD only");
     (void)cmax;
-    riemann_tvdmu_hd<T, NDIR>(wLC, wRC, fL, fR, P, F);
+    if constexpr (MHD) {
+      static_assert(!GLM, "TVD-MUSCL with GLM is not built");
+      riemann_tvdmu_mhd<T, NDIR>(wLC, wRC, fL, fR, P, F);
+    } else {
+      riemann_tvdmu_hd<T, NDIR>(wLC, wRC, fL, fR, P, F);
+    }
   } else if constexpr (SOLVER == SOLVER_TVDLF) {
     st |= cbounds<T, MHD, NDIR, GLM, D, false, BS>(wLC, wRC, wLp, wRp, P, cmax, cmin);
     riemann_tvdlf<T, NW>(wLC, wRC, fL, fR, cmax, T(P.tvdlfeps), F);

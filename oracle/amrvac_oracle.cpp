@@ -1325,6 +1325,197 @@ void tvdlimit2_hd(const State &s, double qdt, const Box &ixO, int idims, const A
   }
 }
 
+// tvdlimit2 for MHD without GLM (src/mod_tvd.t:38-112) with the Roe system
+// of src/mhd/mod_mhd_roe.t: average2 (61-146), geteigenjump2 (160-342),
+// rtimes2 (355-506); divbwave on, typeentropy 'nul'; characteristic fields
+// il = 1..nwflux with alfvRW 1, alfvLW 2, fastRW 3, fastLW 4, slowRW 5,
+// slowLW 6, diverW 7, entroW 8 (ndir 2: nwflux 6, the last two never
+// enter).  idir = idim+1-ndir*(idim/ndir), jdir likewise from idir (1-based).
+template <class R>
+void tvdlimit2_mhd(const State &s, double qdt, const Box &ixO, int idims, const Arr<R> &wL, const Arr<R> &wR,
+                   Arr<R> &wnew, Arr<R> &fC, const double *dxs) {
+  const Ix &x = s.x;
+  const Geo &g = s.g;
+  const int nw = x.nw, ndir = x.ndir, o = g.off(idims);
+  const double gam = s.c.gamma;
+  const double smalld = 1.0e-12;
+  // 1-based direction rule of the reference, back to 0-based
+  const int idim1 = idims + 1;
+  const int idir1 = idim1 + 1 - ndir * (idim1 / ndir), jdir1 = idir1 + 1 - ndir * (idir1 / ndir);
+  const int idir = idir1 - 1, jdir = jdir1 - 1;
+  Box ixC = ixO;
+  ixC.lo[idims] -= 1;
+  struct Roe { R rho, v[3], b[3], cs2, cf, cl, af, as, dp, rhodv, bdv, bdb, bv, v2a2; };
+  std::vector<Roe> roe(g.cells);
+  auto pth = [&](const Arr<R> &w, int i, int j, int k) {
+    R m2 = W(w, x.mom[0]) * W(w, x.mom[0]), b2 = W(w, x.mag[0]) * W(w, x.mag[0]);
+    for (int c = 1; c < ndir; ++c) {
+      m2 = m2 + W(w, x.mom[c]) * W(w, x.mom[c]);
+      b2 = b2 + W(w, x.mag[c]) * W(w, x.mag[c]);
+    }
+    R p = R(gam - 1.0) * (W(w, x.e) - R(half) * (m2 / W(w, x.rho) + b2));
+    if (s.c.fix_small_values && p < R(s.c.small_pressure)) p = R(s.c.small_pressure);
+    return p;
+  };
+  forbox(ixC, [&](int i, int j, int k) {  // average2
+    Roe &r = roe[g.idx(i, j, k)];
+    r.rho = R(half) * (W(wL, x.rho) + W(wR, x.rho));
+    for (int c = 0; c < ndir; ++c) {
+      r.v[c] = R(half) * (W(wL, x.mom[c]) / W(wL, x.rho) + W(wR, x.mom[c]) / W(wR, x.rho));
+      r.b[c] = R(half) * (W(wL, x.mag[c]) + W(wR, x.mag[c]));
+    }
+    const R pL = pth(wL, i, j, k), pR = pth(wR, i, j, k);
+    const R pav = R(half) * (pL + pR);
+    r.dp = pR - pL;
+    r.rhodv = W(wR, x.mom[idims]) - W(wL, x.mom[idims]) - r.v[idims] * (W(wR, x.rho) - W(wL, x.rho));
+    r.cs2 = R(gam) * pav / r.rho;
+    R bb = r.b[0] * r.b[0];
+    for (int c = 1; c < ndir; ++c) bb = bb + r.b[c] * r.b[c];
+    r.cf = bb / r.rho + r.cs2;
+    r.cl = R(half) * (r.cf - rsqrt_(r.cf * r.cf - R(4.0) * r.cs2 * (r.b[idims] * r.b[idims]) / r.rho));
+    r.cf = r.cf - r.cl;
+    r.af = (r.cs2 - r.cl) / (r.cf - r.cl);
+    r.af = rmin(R(one), rmax(r.af, R(zero)));
+    r.as = rsqrt_(R(one) - r.af);
+    r.af = rsqrt_(r.af);
+    r.cf = rsqrt_(r.cf);
+    r.cl = rsqrt_(r.cl);
+    r.rho = rsqrt_(r.rho);
+    if (rabs(r.b[idims]) < R(smalld)) r.b[idims] = R(smalld);
+    if (ndir == 2) {
+      r.b[idir] = r.b[idir] >= R(zero) ? R(one) : R(-1.0);
+    } else {
+      R t = rsqrt_(r.b[idir] * r.b[idir] + r.b[jdir] * r.b[jdir]);
+      if (t > R(smalld)) { r.b[idir] = r.b[idir] / t; r.b[jdir] = r.b[jdir] / t; }
+      else { r.b[idir] = rsqrt_(R(half)); r.b[jdir] = rsqrt_(R(half)); }
+    }
+  });
+  const double dxinv = qdt / dxs[idims];
+  Arr<R> phi(g, 1), rphi(g, 1);
+  auto dvel = [&](int i, int j, int k, int c) {
+    return W(wR, x.mom[c]) / W(wR, x.rho) - W(wL, x.mom[c]) / W(wL, x.rho);
+  };
+  auto dmag = [&](int i, int j, int k, int c) { return W(wR, x.mag[c]) - W(wL, x.mag[c]); };
+  for (int il = 1; il <= nw; ++il) {
+    if (il > 8) break;
+    // geteigenjump2
+    forbox(ixC, [&](int i, int j, int k) {
+      Roe &r = roe[g.idx(i, j, k)];
+      if (il == 3) {  // fastRW_
+        r.bdv = r.b[idir] * dvel(i, j, k, idir);
+        if (ndir == 3) r.bdv = r.bdv + r.b[jdir] * dvel(i, j, k, jdir);
+        r.bdv = r.bdv * rsign(val(r.rho * r.rho), r.b[idims]);
+        r.bdb = r.b[idir] * dmag(i, j, k, idir);
+        if (ndir == 3) r.bdb = r.bdb + r.b[jdir] * dmag(i, j, k, jdir);
+        r.bdb = r.bdb * rsqrt_(r.cs2) * r.rho;
+      }
+      if (il == 1) {  // alfvRW_
+        r.bdv = r.b[jdir] * dvel(i, j, k, idir) - r.b[idir] * dvel(i, j, k, jdir);
+        r.bdb = r.b[jdir] * dmag(i, j, k, idir) - r.b[idir] * dmag(i, j, k, jdir);
+        r.bdv = r.bdv * R(half) * (r.rho * r.rho);
+        r.bdb = r.bdb * R(half) * rsign(val(r.rho), r.b[idims]);
+      }
+      const R u = r.v[idims], h = R(half) / r.cs2;
+      R a, jump;
+      switch (il) {
+        case 3: a = u + r.cf; jump = h * (r.af * (r.cf * r.rhodv + r.dp) + r.as * (-r.cl * r.bdv + r.bdb)); break;
+        case 4: a = u - r.cf; jump = h * (r.af * (-r.cf * r.rhodv + r.dp) + r.as * (r.cl * r.bdv + r.bdb)); break;
+        case 5: a = u + r.cl; jump = h * (r.as * (r.cl * r.rhodv + r.dp) + r.af * (r.cf * r.bdv - r.bdb)); break;
+        case 6: a = u - r.cl; jump = h * (r.as * (-r.cl * r.rhodv + r.dp) + r.af * (-r.cf * r.bdv - r.bdb)); break;
+        case 8: a = u; jump = W(wR, x.rho) - W(wL, x.rho) - r.dp / r.cs2; break;
+        case 7: a = u; jump = dmag(i, j, k, idims); break;
+        case 1: a = u + rabs(r.b[idims]) / r.rho; jump = r.bdv - r.bdb; break;
+        default: a = u - rabs(r.b[idims]) / r.rho; jump = -r.bdv - r.bdb; break;
+      }
+      phi.d[g.idx(i, j, k)] = rabs(a * R(dxinv)) * jump;
+    });
+    for (int iw = 0; iw < nw; ++iw) {
+      forbox(ixC, [&](int i, int j, int k) {  // rtimes2
+        Roe &r = roe[g.idx(i, j, k)];
+        const R q = phi.d[g.idx(i, j, k)];
+        const R u = r.v[idims];
+        R rq(0.0);
+        if (iw == x.rho) {
+          if (il == 3 || il == 4) rq = q * r.af;
+          else if (il == 5 || il == 6) rq = q * r.as;
+          else if (il == 8) rq = q;
+        } else if (iw == x.e) {
+          if (il == 3) {
+            R v2 = r.v[0] * r.v[0];
+            for (int c = 1; c < ndir; ++c) v2 = v2 + r.v[c] * r.v[c];
+            r.v2a2 = R(half) * v2 + R((2.0 - gam) / (gam - 1.0)) * r.cs2;
+            r.bv = r.b[idir] * r.v[idir];
+            if (ndir == 3) r.bv = r.bv + r.b[jdir] * r.v[jdir];
+            r.bv = r.bv * rsign(one, r.b[idims]);
+          } else if (il == 1) {
+            r.bv = r.b[jdir] * r.v[idir] - r.b[idir] * r.v[jdir];
+          }
+          switch (il) {
+            case 3: rq = q * (-r.as * r.cl * r.bv + r.af * (r.v2a2 + r.cf * (r.cf + u))); break;
+            case 4: rq = q * (r.as * r.cl * r.bv + r.af * (r.v2a2 + r.cf * (r.cf - u))); break;
+            case 5: rq = q * (r.af * r.cf * r.bv + r.as * (r.v2a2 + r.cl * (r.cl + u))); break;
+            case 6: rq = q * (-r.af * r.cf * r.bv + r.as * (r.v2a2 + r.cl * (r.cl - u))); break;
+            case 8: {
+              R v2 = r.v[0] * r.v[0];
+              for (int c = 1; c < ndir; ++c) v2 = v2 + r.v[c] * r.v[c];
+              rq = q * R(half) * v2;
+              break;
+            }
+            case 7: rq = q * r.b[idims]; break;
+            case 1: rq = q * r.bv; break;
+            default: rq = -q * r.bv; break;
+          }
+        } else if (iw >= x.mom[0] && iw < x.mom[0] + ndir) {
+          const int c = iw - x.mom[0];
+          if (c == idims) {
+            switch (il) {
+              case 3: rq = q * r.af * (r.v[c] + r.cf); break;
+              case 4: rq = q * r.af * (r.v[c] - r.cf); break;
+              case 5: rq = q * r.as * (r.v[c] + r.cl); break;
+              case 6: rq = q * r.as * (r.v[c] - r.cl); break;
+              case 8: rq = q * r.v[c]; break;
+              default: break;
+            }
+          } else {
+            const R sg = rsign(one, r.b[idims]);
+            switch (il) {
+              case 3: rq = q * (r.af * r.v[c] - r.as * r.cl * r.b[c] * sg); break;
+              case 4: rq = q * (r.af * r.v[c] + r.as * r.cl * r.b[c] * sg); break;
+              case 5: rq = q * (r.as * r.v[c] + r.af * r.cf * r.b[c] * sg); break;
+              case 6: rq = q * (r.as * r.v[c] - r.af * r.cf * r.b[c] * sg); break;
+              case 8: rq = q * r.v[c]; break;
+              case 7: break;
+              case 1: rq = c == idir ? q * r.b[jdir] : -q * r.b[idir]; break;
+              default: rq = c == idir ? -q * r.b[jdir] : q * r.b[idir]; break;
+            }
+          }
+        } else {  // magnetic field
+          const int c = iw - x.mag[0];
+          if (c == idims) {
+            if (il == 7) rq = q;
+          } else {
+            switch (il) {
+              case 3: case 4: rq = q * r.as * rsqrt_(r.cs2) * r.b[c] / r.rho; break;
+              case 5: case 6: rq = -q * r.af * rsqrt_(r.cs2) * r.b[c] / r.rho; break;
+              case 1: case 2:
+                rq = c == idir ? -q * r.b[jdir] / rsign(val(r.rho), r.b[idims])
+                               : q * r.b[idir] / rsign(val(r.rho), r.b[idims]);
+                break;
+              default: break;
+            }
+          }
+        }
+        rphi.d[g.idx(i, j, k)] = rq * R(half);
+        W(fC, iw) = W(fC, iw) + rphi.d[g.idx(i, j, k)];
+      });
+      forbox(ixO, [&](int i, int j, int k) {
+        const int p = g.idx(i, j, k);
+        W(wnew, iw) = W(wnew, iw) + rphi.d[p] - rphi.d[p - o];
+      });
+    }
+  }
+}
+
 // finite_volume (src/mod_finite_volume.t:116-339), slab_uniform, no local dt.
 template <class R>
 int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, double dtfactor,
@@ -1391,7 +1582,10 @@ int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, d
     }
     // the MUSCL scheme's characteristic limiter, with the states of the
     // last direction reconstructed (one direction per dimensionally split sweep)
-    if (c.flux_scheme == ORC_FS_TVDMU) tvdlimit2_hd(s, qdt, ixO, idims, wLC, wRC, wnew, fC[idims], dxs);
+    if (c.flux_scheme == ORC_FS_TVDMU) {
+      if (x.mhd) tvdlimit2_mhd(s, qdt, ixO, idims, wLC, wRC, wnew, fC[idims], dxs);
+      else tvdlimit2_hd(s, qdt, ixO, idims, wLC, wRC, wnew, fC[idims], dxs);
+    }
   }
   if (c.fix_small_values) {
     int s2 = handle_small_values(s, false, wnew, ixO);

@@ -15,7 +15,8 @@ ot_2d_4step_hll_mc.log, kh_2d_4step_hll_mc.log, kh_2d_4step_hllc_ko.log and
 (RK4, TVDLF, cada3) ot_2d_rk4_tvdlf_cada.log, kh_2d_rk4_tvdlf_cada.log, and
 the twostep Predictor_Corrector variant (MUSCL-Hancock predictor, TVDLF,
 minmod) ot_2d_2step_tvdlf_mm.log, and MHD HLLC (SSPRK(4,3), koren, Linde)
-ot_2d_4step_hllc_ko.log; and the 2-D blast wave with cont
+ot_2d_4step_hllc_ko.log, and MHD TVD-MUSCL (dimensionally split, albada)
+ot_2d_2step_tvdmu_al.log; and the 2-D blast wave with cont
 boundaries, tests/hd/blast_wave_Cartesian_2D/correct_output/
 bw_2d_{3step_hll_cada,4step_hll_mc,4step_hllc_ko,rk4_tvdlf_cada,
 2step_tvdlf_mm,2step_tvdmu_al}.log (the last with TVD-MUSCL, dimensionally
@@ -41,6 +42,7 @@ LOGS = [
     "tests/hd/Kelvin_Helmholtz_2D/correct_output/kh_2d_rk4_tvdlf_cada.log",
     "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_2step_tvdlf_mm.log",
     "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_4step_hllc_ko.log",
+    "tests/mhd/Orszag_Tang_2D/correct_output/ot_2d_2step_tvdmu_al.log",
     # multi-level with cont boundaries
     "tests/hd/blast_wave_Cartesian_2D/correct_output/bw_2d_3step_hll_cada.log",
     "tests/hd/blast_wave_Cartesian_2D/correct_output/bw_2d_4step_hll_mc.log",

@@ -139,6 +139,8 @@ def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsav
                             courantpar=0.9, time_stepper="twostep"), 6),
     ("4step_hllc_ko", dict(flux_scheme="hllc", limiter="koren", typedivbfix="linde", typeboundspeed="cmaxmean",
                            courantpar=0.9, time_stepper="fourstep"), 6),
+    ("2step_tvdmu_al", dict(flux_scheme="tvdmu", limiter="albada", typedivbfix="linde", typeboundspeed="cmaxmean",
+                            courantpar=0.9, time_stepper="twostep", dimsplit=True), 6),
 ])
 def test_orszag_tang_2d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
     weight = np.zeros(nw)

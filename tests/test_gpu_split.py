@@ -18,6 +18,14 @@ from tests import _amr as A
 pytestmark = pytest.mark.gpu
 
 RTOL = 1e-12
+# MHD TVD-MUSCL is ill-conditioned in the Roe normalisation of its fast and
+# slow eigenvectors (cslow = (cf - sqrt(cf^2 - 4 cs^2 bn^2 / rho)) / 2 and
+# the weights af, as where the two speeds approach each other): the oracle
+# alone turns a 1-ulp relative perturbation of its input into 3.5e-11 after
+# three split steps of the 2-D case (MHD HLL: 8e-14, HD TVD-MUSCL: 7e-14), so
+# the FMA-contraction differences between device and oracle get the bar of
+# that self-noise rather than 1e-12.
+RTOL_MHD_TVDMU = 1e-10
 
 CASES = {
     "hd2_hll_minmod_xyyx": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll", limiter="minmod"),
@@ -34,6 +42,13 @@ CASES = {
     "hd3_tvdmu_minmod_pc": dict(physics="hd", ndim=3, gamma=1.4, flux_scheme="tvdmu", limiter="minmod",
                                 time_stepper="twostep"),
     "hd2_tvdmu_woodward_ssprk3": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="tvdmu", limiter="woodward"),
+    # MHD TVD-MUSCL (the Roe system of src/mhd/mod_mhd_roe.t)
+    "mhd2_tvdmu_albada_linde_pc": dict(physics="mhd", ndim=2, flux_scheme="tvdmu", limiter="albada",
+                                       typedivbfix="linde", time_stepper="twostep", typeboundspeed="cmaxmean"),
+    "mhd25_tvdmu_minmod_none": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="tvdmu", limiter="minmod",
+                                    typedivbfix="none", time_stepper="twostep"),
+    "mhd3_tvdmu_vanleer_none": dict(physics="mhd", ndim=3, flux_scheme="tvdmu", limiter="vanleer",
+                                    typedivbfix="none"),
 }
 
 
@@ -92,7 +107,8 @@ def test_split_steps_match_oracle(oracle_lib, name):
     got = P.interior(ctx.download("ps"), ndim)
     ref = P.interior(np.array([og.get_block(ib) for ib in range(og.nblocks)]), ndim)
     err = _maxrel(got, ref)
-    assert err <= RTOL, f"{name}: max rel err {err:.3e}"
+    tol = RTOL_MHD_TVDMU if (kw["physics"] == "mhd" and kw["flux_scheme"] == "tvdmu") else RTOL
+    assert err <= tol, f"{name}: max rel err {err:.3e}"
     assert ctx.status() == 0
 
 
@@ -124,6 +140,8 @@ AMR_CASES = [
     ("hd2_hllc_vanleer_split", dict(physics="hd", flux_scheme="hllc", limiter="vanleer"), ["periodic"] * 4),
     ("mhd2_hlld_linde_split", dict(physics="mhd", flux_scheme="hlld", limiter="minmod", typedivbfix="linde"),
      ["periodic"] * 4),
+    ("mhd2_tvdmu_albada_linde_pc", dict(physics="mhd", flux_scheme="tvdmu", limiter="albada", typedivbfix="linde",
+                                        time_stepper="twostep"), ["periodic"] * 4),
 ]
 
 
@@ -163,5 +181,6 @@ def test_split_amr_steps_match_oracle(oracle_lib, name, kw, bc):
         og.advance(dt, cg)
         got = ctx.download()
         worst = max(_maxrel(got[b][sl][None], og.get_block(b)[sl][None]) for b in range(len(leaves)))
-        assert worst <= RTOL, (name, n, worst)
+        tol = RTOL_MHD_TVDMU if (physics == "mhd" and kw["flux_scheme"] == "tvdmu") else RTOL
+        assert worst <= tol, (name, n, worst)
     assert ctx.status() == 0
