@@ -78,8 +78,11 @@ ALG_FLOPS = {
     "kh256": dict(stage=416.7, getdt=21.0),
 }
 # Per-launch DRAM traffic of the stage kernel from one ncu capture, bytes per
-# interior cell (profiles/fv_stage_*.md); None until captured.
-NCU_TRAFFIC_PER_CELL = {"ot128": None, "ot256": None, "kh256": None}
+# interior cell (profiles/fv_stage_*.md); None until captured.  ot128: the
+# FP64 kernel's stage-1 launch (ps -> ps1; algorithmic 2 * 8 * nw = 144 B per
+# cell), dram__bytes_read.sum + dram__bytes_write.sum = 180.65 MB + 127.96 MB
+# over 128^3 cells.
+NCU_TRAFFIC_PER_CELL = {"ot128": (180.652032e6 + 127.964928e6) / 128 ** 3, "ot256": None, "kh256": None}
 
 
 def _cfg_kwargs(wl: str):
@@ -915,6 +918,8 @@ def run_ours(args, ws, rank, local):
     roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved_gbs / peaks["hbm_gbs"], "peak_source": peak_kind,
                 "traffic": None if traffic is None else traffic * cells,
+                "traffic_note": None if traffic is None else
+                "ncu dram read+write of a stage-1 launch (algorithmic 2*8*nw B/cell for that launch)",
                 "kernel": "fv_stage_kernel", "algorithmic_bytes_per_cell": bytes_per_cell,
                 "avg_launch_ms": stage_avg_s * 1e3, "launches": nstage}
     fp64_peak = fp64_peak_tflops()
