@@ -108,7 +108,7 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
              small_pressure=0.0, time_stepper="threestep", ssprk_order=3, dtmin=1.0e-10,
              typeboundary=None, zchunk=0, precision="fp64", slowsteps=-1,
              time_integrator="default", nghostcells=None, dimsplit=False,
-             typedimsplit="xyyx") -> _lib.AmrvacCfg:
+             typedimsplit="xyyx", schmid_rad=(1.0, 1.0, 1.0)) -> _lib.AmrvacCfg:
     """Build an ``amrvac_cfg`` from reference-style parameter names.
 
     typeboundary: list of 2*ndim entries (min1, max1, min2, ...), each a name
@@ -153,6 +153,8 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
     c.slowsteps = int(slowsteps)
     c.time_integrator = _lib.TIME_INTEGRATOR[time_integrator]
     c.dimsplit = 0 if not dimsplit else (2 if typedimsplit == "xy" else 1)
+    for d in range(3):
+        c.schmid_rad[d] = float(schmid_rad[d])
     nw = L.amrvac_gpu_nw(c)
     tb = typeboundary or ["periodic"] * (2 * ndim)
     for s in range(6):
@@ -219,6 +221,7 @@ def config_from_par(paths) -> RunConfig:
         time_integrator=integ or "default",
         nghostcells=int(mesh["nghostcells"]) if "nghostcells" in mesh else None,
         dimsplit=bool(meth.get("dimsplit", False)),
+        schmid_rad=tuple(float(meth.get(f"schmid_rad{d + 1}", 1.0)) for d in range(3)),
         typedimsplit=meth.get("typedimsplit", "xyyx"),
     )
     if physics == "mhd":

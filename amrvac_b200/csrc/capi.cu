@@ -419,6 +419,7 @@ void amrvac_gpu_default_cfg(amrvac_cfg *c) {
   c->courantpar = 0.8;
   c->type_courant = AMRVAC_COURANT_MAXSUM;
   c->cada3_radius = 0.1;
+  c->schmid_rad[0] = c->schmid_rad[1] = c->schmid_rad[2] = 1.0;
   c->tvdlfeps = 1.0;
   c->fix_small_values = 0;
   c->check_small_values = 1;
@@ -455,7 +456,7 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   // reconstructions outside reconstruct_LR's slope-limiter branch (their own kernels)
   const bool special = fifth || k.limiter == AMRVAC_LIM_VENK || k.limiter == AMRVAC_LIM_WENO3 ||
                        k.limiter == AMRVAC_LIM_WENOYC3;
-  if ((k.limiter < 1 || k.limiter > 9) && !special) return fail(AMRVAC_E_UNSUPPORTED, "limiter not supported");
+  if ((k.limiter < 1 || k.limiter > 10) && !special) return fail(AMRVAC_E_UNSUPPORTED, "limiter not supported");
   if (special && k.precision == 1) return fail(AMRVAC_E_UNSUPPORTED, "this limiter is FP64 only");
   if (fifth && k.nghostcells < 3) return fail(AMRVAC_E_ARG, "mp5 / weno5 need nghostcells >= 3");
   if (fifth && k.precision == 1) return fail(AMRVAC_E_UNSUPPORTED, "mp5 / weno5 are FP64 only");
@@ -520,6 +521,7 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   P.small_e = k.physics == 1 ? k.small_pressure * P.inv_gamma_1 : k.small_pressure / (k.gamma - 1.0);
   P.tvdlfeps = k.tvdlfeps;
   P.cada3_radius = k.cada3_radius;
+  for (int d = 0; d < 3; ++d) P.schmid_rad[d] = k.schmid_rad[d];
   P.glm_alpha = k.mhd_glm_alpha;
   P.divbdiff = k.divbdiff;
   P.courantpar = k.courantpar;

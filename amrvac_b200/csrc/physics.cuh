@@ -16,7 +16,7 @@ namespace amrvac {
 // Limiter ids as in src/limiter/mod_limiter.t:14-24.
 enum : int { LIM_MINMOD = 1, LIM_WOODWARD = 2, LIM_MCBETA = 3, LIM_SUPERBEE = 4,
              LIM_VANLEER = 5, LIM_ALBADA = 6, LIM_KOREN = 7, LIM_CADA = 8, LIM_CADA3 = 9,
-             LIM_VENK = 11, LIM_MP5 = 13, LIM_WENO3 = 14, LIM_WENOYC3 = 15, LIM_WENO5 = 16,
+             LIM_SCHMID = 10, LIM_VENK = 11, LIM_MP5 = 13, LIM_WENO3 = 14, LIM_WENOYC3 = 15, LIM_WENO5 = 16,
              LIM_WENOZ5 = 18, LIM_WENOZP5 = 20 };
 enum : int { BS_EINFELDT = 1, BS_CMAXMEAN = 2, BS_CMAXLEFTRIGHT = 3 };
 enum : int { SOLVER_TVDLF = 1, SOLVER_HLL = 2, SOLVER_HLLC = 3, SOLVER_HLLD = 4, SOLVER_TVDMU = 5,
@@ -30,6 +30,7 @@ struct PhysParams {
   double gamma, gamma_1, inv_gamma_1;
   double small_density, small_pressure, small_e;
   double tvdlfeps, cada3_radius, glm_alpha, divbdiff, courantpar;
+  double schmid_rad[3];
   int limiter, boundspeed, divb, glm_extended;
   int fix_small_values, check_small_values, small_values_method;
 };
@@ -317,6 +318,18 @@ __device__ __forceinline__ T slope_impl(int lim, T a, T b, T rdelinv) {
       const T t = LEFT ? div_(b, a + fsign(eps, a)) : div_(a, b + fsign(eps, b));
       const T A = (T(2.0) + t) * third;
       const T lim2 = fmax(T(0.0), fmin(A, fmax(-(cadalfa * t), fmin(fmin(cadbeta * t, A), cadgamma))));
+      const T t2 = (tmpeta - T(1.0)) * invcadepsilon;
+      const T blend = T(0.5) * ((T(1.0) - t2) * A + (T(1.0) + t2) * lim2);
+      const T phi = tmpeta <= T(1.0) - cadepsilon ? A : (tmpeta >= T(1.0) + cadepsilon ? lim2 : blend);
+      return phi * (LEFT ? a : b);
+    }
+    case LIM_SCHMID: {
+      // dwlimiter2 limiter_schmid (src/limiter/mod_limiter.t:291-333), the
+      // schmid2 form: rdelinv carries (a2max + cadepsilon) dx^2 here
+      const T tmpeta = sqrt(T(0.4) * (a * a + b * b)) / rdelinv;
+      const T t = LEFT ? div_(b, a + fsign(eps, a)) : div_(a, b + fsign(eps, b));
+      const T A = (T(2.0) + t) * third;
+      const T lim2 = fmax(T(0.0), fmin(A, fmax(-t, fmin(fmin(cadbeta * t, A), T(1.5)))));
       const T t2 = (tmpeta - T(1.0)) * invcadepsilon;
       const T blend = T(0.5) * ((T(1.0) - t2) * A + (T(1.0) + t2) * lim2);
       const T phi = tmpeta <= T(1.0) - cadepsilon ? A : (tmpeta >= T(1.0) + cadepsilon ? lim2 : blend);

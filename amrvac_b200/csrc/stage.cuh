@@ -604,7 +604,9 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
     dx[d] = d < NDIM ? A.dxb[b * 3 + d] : 1.0;
     dxinv[d] = -qdt / dx[d];
     const double r = P.cada3_radius * dx[d];
-    rdel[d] = 1.0 / (r * r);
+    // cada3: 1 / (cada3_radius dx)^2; schmid: (schmid_rad + cadepsilon) dx^2
+    rdel[d] = (LIM == LIM_SCHMID || (LIM == 0 && P.limiter == LIM_SCHMID))
+                  ? (P.schmid_rad[d] + 1.0e-14) * (dx[d] * dx[d]) : 1.0 / (r * r);
     if constexpr (LIM == LIM_WENO5) wlam[d] = pow(dx[d], 2.0 / 3.0);
   }
   double fz_prev[NDIM == 3 ? NW : 1];

@@ -59,6 +59,7 @@ extern "C" {
 #define AMRVAC_LIM_KOREN    7
 #define AMRVAC_LIM_CADA     8
 #define AMRVAC_LIM_CADA3    9
+#define AMRVAC_LIM_SCHMID   10  /* schmid2 (a2max = schmid_rad per direction) */
 #define AMRVAC_LIM_VENK     11  /* Venkatakrishnan */
 #define AMRVAC_LIM_MP5      13  /* fifth order, uniform grids, nghostcells >= 3 */
 #define AMRVAC_LIM_WENO3    14  /* third-order WENO */
@@ -137,6 +138,7 @@ typedef struct amrvac_cfg {
   int dimsplit;             /* 0 unsplit (default); 1 dimensionally split with
                                typedimsplit 'xyyx' (the order reverses on odd
                                steps), 2 'xy' (src/mod_advance.t:23-45) */
+  double schmid_rad[3];     /* schmid limiter radii per direction (default 1) */
 } amrvac_cfg;
 
 typedef struct amrvac_ctx amrvac_ctx;

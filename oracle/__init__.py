@@ -18,7 +18,7 @@ _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 
 FS = {"tvdlf": 1, "hll": 2, "hllc": 3, "hlld": 4, "tvdmu": 5}
 LIMITER = {"minmod": 1, "woodward": 2, "mcbeta": 3, "superbee": 4, "vanleer": 5,
-           "albada": 6, "koren": 7, "cada": 8, "cada3": 9, "venk": 11, "mp5": 13, "weno3": 14, "wenoyc3": 15, "weno5": 16, "wenoz5": 18, "wenozp5": 20}
+           "albada": 6, "koren": 7, "cada": 8, "cada3": 9, "schmid2": 10, "venk": 11, "mp5": 13, "weno3": 14, "wenoyc3": 15, "weno5": 16, "wenoz5": 18, "wenozp5": 20}
 BOUNDSPEED = {"Einfeldt": 1, "cmaxmean": 2, "cmaxleftright": 3}
 DIVB = {"none": 0, "glm": 1, "linde": 4}
 BC = {"periodic": 0, "cont": 1, "symm": 2, "asymm": 3}
@@ -39,6 +39,7 @@ class OrcCfg(ctypes.Structure):
         ("divbdiff", ctypes.c_double), ("ssprk_order", ctypes.c_int),
         ("time_stepper", ctypes.c_int), ("time_integrator", ctypes.c_int),
         ("dimsplit", ctypes.c_int),
+        ("schmid_rad", ctypes.c_double * 3),
     ]
 
 
@@ -132,7 +133,7 @@ def make_cfg(*, ndim=2, ndir=None, physics="hd", block_nx=16, nghost=2, gamma=No
              cada3_radius=0.1, tvdlfeps=1.0, fix_small_values=False, check_small_values=True,
              small_values_method="error", small_density=0.0, small_pressure=0.0,
              divbdiff=0.8, ssprk_order=3, time_stepper="threestep", time_integrator="default",
-             dimsplit=False, typedimsplit="xyyx") -> OrcCfg:
+             dimsplit=False, typedimsplit="xyyx", schmid_rad=(1.0, 1.0, 1.0)) -> OrcCfg:
     c = OrcCfg()
     c.ndim = ndim
     c.ndir = ndim if ndir is None else ndir
@@ -162,6 +163,8 @@ def make_cfg(*, ndim=2, ndir=None, physics="hd", block_nx=16, nghost=2, gamma=No
     c.time_stepper = {"twostep": 2, "threestep": 3, "fourstep": 4, "fivestep": 5}[time_stepper]
     c.time_integrator = {"default": 0, "Predictor_Corrector": 0, "ssprk4": 0, "rk4": 1, "ssprk2": 2}[time_integrator]
     c.dimsplit = 0 if not dimsplit else (2 if typedimsplit == "xy" else 1)
+    for d in range(3):
+        c.schmid_rad[d] = float(schmid_rad[d])
     lib().orc_cfg_finalize(ctypes.byref(c))
     return c
 

@@ -553,6 +553,21 @@ void dwlimiter2(const State &s, const Arr<R> &dwC, const Box &ixC, int idims, do
         r = rmax(R(zero), rmin(t2, rmax(-(R(cadalfa) * t), rmin(rmin(R(cadbeta) * t, t2), R(cadgamma))))) * bb;
         break;
       }
+      case ORC_LIM_SCHMID: {  // schmid2: a2max = schmid_rad(idims) (src/limiter/mod_limiter.t:291-333)
+        R tmpeta = rsqrt_(R(0.4) * (a * a + bb * bb)) /
+                   ((R(s.c.schmid_rad[idims]) + R(cadepsilon)) * (R(dxlevel) * R(dxlevel)));
+        auto phi = [&](R t) {
+          R A = (R(two) + t) * R(third);
+          R B = rmax(R(zero), rmin(A, rmax(-t, rmin(rmin(R(cadbeta) * t, A), R(1.5)))));
+          if (tmpeta <= R(one - cadepsilon)) return A;
+          if (tmpeta >= R(one + cadepsilon)) return B;
+          R t2 = (tmpeta - R(one)) * R(invcadepsilon);
+          return R(half) * ((R(one) - t2) * A + (R(one) + t2) * B);
+        };
+        l = phi(bb / (a + rsign(eps, a))) * a;
+        r = phi(a / (bb + rsign(eps, bb))) * bb;
+        break;
+      }
       default: {  // cada3
         R tmpeta = (a * a + bb * bb) * rdelinv;
         auto phi = [&](R t) {

@@ -26,7 +26,7 @@ enum { ORC_FS_TVDLF = 1, ORC_FS_HLL = 2, ORC_FS_HLLC = 3, ORC_FS_HLLD = 4, ORC_F
 /* Limiter ids follow src/limiter/mod_limiter.t:14-24. */
 enum { ORC_LIM_MINMOD = 1, ORC_LIM_WOODWARD = 2, ORC_LIM_MCBETA = 3,
        ORC_LIM_SUPERBEE = 4, ORC_LIM_VANLEER = 5, ORC_LIM_ALBADA = 6,
-       ORC_LIM_KOREN = 7, ORC_LIM_CADA = 8, ORC_LIM_CADA3 = 9, ORC_LIM_VENK = 11, ORC_LIM_MP5 = 13,
+       ORC_LIM_KOREN = 7, ORC_LIM_CADA = 8, ORC_LIM_CADA3 = 9, ORC_LIM_SCHMID = 10, ORC_LIM_VENK = 11, ORC_LIM_MP5 = 13,
        ORC_LIM_WENO3 = 14, ORC_LIM_WENOYC3 = 15,
        ORC_LIM_WENO5 = 16, ORC_LIM_WENOZ5 = 18, ORC_LIM_WENOZP5 = 20 };
 /* boundspeed ids follow src/io/mod_input_output.t:1632-1641. */
@@ -66,6 +66,7 @@ typedef struct {
   int time_stepper;       /* 2 twostep, 3 threestep (0 means 3), 4 fourstep */
   int time_integrator;    /* twostep: 0 Predictor_Corrector, 2 ssprk2; fourstep: 0 ssprk4, 1 rk4 */
   int dimsplit;           /* 0 unsplit, 1 'xyyx', 2 'xy' */
+  double schmid_rad[3];   /* schmid2 limiter radii per direction */
 } orc_cfg;
 
 /* Number of flux variables implied by cfg (sets cfg->nw too). */

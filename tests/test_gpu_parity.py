@@ -54,6 +54,13 @@ CASES = {
                                             typedivbfix="glm", typeboundspeed="cmaxmean"),
     "mhd3_hllc_minmod_glm": dict(physics="mhd", ndim=3, flux_scheme="hllc", limiter="minmod", typedivbfix="glm"),
     "mhd3_hllc_cada3_none": dict(physics="mhd", ndim=3, flux_scheme="hllc", limiter="cada3", typedivbfix="none"),
+    # the schmid2 slope limiter (per-direction schmid_rad; radii near the
+    # median of sqrt(0.4 (a^2 + b^2)) / dx^2 on this data, so both of its
+    # branches occur)
+    "hd2_hll_schmid2": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll", limiter="schmid2",
+                            schmid_rad=(42.0, 50.0, 1.0)),
+    "mhd3_hlld_schmid2_glm": dict(physics="mhd", ndim=3, flux_scheme="hlld", limiter="schmid2", typedivbfix="glm",
+                                  schmid_rad=(63.0, 10.0, 200.0)),
     # WENO3 family and the Venkatakrishnan limiter (two ghost cells)
     "hd2_hllc_weno3": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hllc", limiter="weno3"),
     "mhd25_hlld_wenoyc3_glm": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hlld", limiter="wenoyc3",
