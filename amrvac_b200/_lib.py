@@ -97,6 +97,7 @@ SIGNATURES = [
     ("amrvac_gpu_getdt", _i, [_vp, _i, _dp, _dp]),
     ("amrvac_gpu_getdt_noalloc", _i, [_cfgp, _vp, _i, _dp, _vp, _dp, _dp]),
     ("amrvac_gpu_advect1", _i, [_vp, _i, _i, _i, _d, _d, _d, _d]),
+    ("amrvac_gpu_advect1_dim", _i, [_vp, _i, _i, _i, _d, _d, _d, _d, _i]),
     ("amrvac_gpu_set_cmax_global", _i, [_vp, _d]),
     ("amrvac_gpu_set_time", _i, [_vp, _d, _d, _d]),
     ("amrvac_gpu_step", _i, [_vp]),

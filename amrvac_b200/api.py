@@ -166,7 +166,13 @@ class Context:
     def set_cmax_global(self, cmax_global: float):
         _lib.check(self.L.amrvac_gpu_set_cmax_global(self.h, cmax_global), "set_cmax_global")
 
-    def advect1(self, reg_ct, reg_new, dtfactor, dt, reg_base="ps", a_base=0.0, b_in=1.0):
+    def advect1(self, reg_ct, reg_new, dtfactor, dt, reg_base="ps", a_base=0.0, b_in=1.0, idim=0):
+        """One stage; idim 1..ndim restricts it to that direction (a
+        dimensionally split sweep), 0 advances all directions."""
+        if idim:
+            return _lib.check(self.L.amrvac_gpu_advect1_dim(self.h, REG.get(reg_ct, reg_ct), REG.get(reg_new, reg_new),
+                                                            REG.get(reg_base, reg_base), a_base, b_in, dtfactor, dt,
+                                                            idim), "advect1_dim")
         return _lib.check(self.L.amrvac_gpu_advect1(self.h, REG.get(reg_ct, reg_ct), REG.get(reg_new, reg_new),
                                                     REG.get(reg_base, reg_base), a_base, b_in, dtfactor, dt),
                           "advect1")

@@ -85,6 +85,7 @@ struct amrvac_ctx {
   int64_t graph_nodes = 0;
   int zchunk = 0;          // 0: persistent plane ranges; 16/8/4: one z-chunk per CTA
   int sweep = -1;          // dimensional splitting: the current sweep of the step (-1: unsplit)
+  bool fixed_dir = false;  // sweep is a direction (amrvac_gpu_advect1_dim), not a sweep index
   int wave_ctas = 1;       // resident stage CTAs on the device (one wave)
   std::vector<double> h_dx;            // [nblocks][3] cell sizes (host copy)
   double *d_adj[3] = {nullptr, nullptr, nullptr};  // adjoint work registers (lazily)
@@ -172,7 +173,7 @@ StageArgs stage_args(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, doubl
   A.block_status = c->d_block_status;
   A.P = c->P;
   A.sweep = c->sweep;
-  A.split_xy = c->cfg.dimsplit == 2;
+  A.split_xy = c->fixed_dir || c->cfg.dimsplit == 2;
   if (c->amr) {
     A.gbuf = c->amr->gbuf;
     A.pflux = c->amr->pflux;
@@ -220,7 +221,7 @@ int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a,
     AmrFixArgs F = c->amr->F;
     F.w = c->pool[reg_new];
     F.sweep = c->sweep;
-    F.split_xy = c->cfg.dimsplit == 2;
+    F.split_xy = c->fixed_dir || c->cfg.dimsplit == 2;
     CK(launch_amr_fix(F, c->amr->nslots, c->cfg.ndim, c->stream));
     ++c->launches;
   }
@@ -1272,6 +1273,18 @@ int amrvac_gpu_advect1(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, dou
   CK(cudaMemcpyAsync(c->d_scal + 0, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   int r = launch_stage(c, reg_ct, reg_new, reg_base, a_base, b_in, dtfactor);
   CK(cudaStreamSynchronize(c->stream));
+  return r;
+}
+
+int amrvac_gpu_advect1_dim(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a_base, double b_in,
+                           double dtfactor, double dt, int idim) {
+  if (int r = check_ctx(c, true)) return r;
+  if (idim < 0 || idim > c->cfg.ndim) return fail(AMRVAC_E_ARG, "idim must be 0 (all) or 1..ndim");
+  c->sweep = idim - 1;
+  c->fixed_dir = idim > 0;
+  const int r = amrvac_gpu_advect1(c, reg_ct, reg_new, reg_base, a_base, b_in, dtfactor, dt);
+  c->sweep = -1;
+  c->fixed_dir = false;
   return r;
 }
 

@@ -227,6 +227,12 @@ int amrvac_gpu_getdt(amrvac_ctx *ctx, int reg, double *dt, double *cmax_global);
  * Uses cmax_global from the last getdt / set_cmax_global.  Asynchronous. */
 int amrvac_gpu_advect1(amrvac_ctx *ctx, int reg_ct, int reg_new, int reg_base, double a_base,
                        double b_in, double dtfactor, double dt);
+/* The same stage restricted to direction idim (1..ndim; 0: all), as advect1
+ * with idim^LIM = idim, idim in a dimensionally split step
+ * (src/mod_advance.t:23-45, 611-666): that direction's fluxes, its flux fix
+ * on multi-level grids, and the divB sources with qdt / ndim.  Synchronous. */
+int amrvac_gpu_advect1_dim(amrvac_ctx *ctx, int reg_ct, int reg_new, int reg_base, double a_base,
+                           double b_in, double dtfactor, double dt, int idim);
 int amrvac_gpu_set_cmax_global(amrvac_ctx *ctx, double cmax_global);
 
 /* Time control for amrvac_gpu_step: current time, time_max (final_dt_reduction)

@@ -184,3 +184,32 @@ def test_split_amr_steps_match_oracle(oracle_lib, name, kw, bc):
         tol = RTOL_MHD_TVDMU if (physics == "mhd" and kw["flux_scheme"] == "tvdmu") else RTOL
         assert worst <= tol, (name, n, worst)
     assert ctx.status() == 0
+
+
+def test_advect1_dim_reproduces_a_split_step(oracle_lib):
+    """The C ABI's one-direction stage (amrvac_gpu_advect1_dim): a split
+    onestep step equals the x stage then the y stage through the ABI, bit for
+    bit (same kernels, same dt)."""
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    n = 32
+    prim = P.random_smooth("mhd", 2, 2, n, seed=P.SEED)
+    blocks = P.to_blocks(P.prim_to_cons(prim, "mhd", 2, 5.0 / 3.0), 2)
+    kw = dict(physics="mhd", ndim=2, flux_scheme="hlld", limiter="vanleer", typedivbfix="linde",
+              time_stepper="onestep", dimsplit=True)
+    a = Context(make_cfg(**kw))
+    a.set_uniform_grid([n, n], [0.0, 0.0], [1.0, 1.0])
+    a.upload(blocks)
+    _, cg, _ = a.getdt("ps")
+    a.set_time(0.0, 1.0e99, 0.0)
+    a.step()
+    dt = a.get_time()[0]
+    b = Context(make_cfg(**kw))
+    b.set_uniform_grid([n, n], [0.0, 0.0], [1.0, 1.0])
+    b.upload(blocks)
+    b.set_cmax_global(cg)
+    b.advect1("ps", "ps1", 1.0, dt, idim=1)
+    b.advect1("ps1", "ps", 1.0, dt, reg_base="ps1", idim=2)
+    assert np.array_equal(a.download("ps"), b.download("ps"))
+    a.close()
+    b.close()
