@@ -163,3 +163,50 @@ def test_mp5_needs_three_ghost_cells_and_fp64(lib):
     assert lib.amrvac_gpu_create(ctypes.byref(bad), ctypes.byref(h)) == _lib.E_ARG
     bad = make_cfg(physics="hd", ndim=2, flux_scheme="hll", limiter="mp5", precision="mixed")
     assert lib.amrvac_gpu_create(ctypes.byref(bad), ctypes.byref(h)) == _lib.E_UNSUPPORTED
+
+
+def test_config_from_par_reads_the_method_options(tmp_path):
+    """methodlist options of the reconstructions, steppers and splitting:
+    twostep TVD-MUSCL dimensionally split; fivestep with MP5 (three ghost
+    cells by default, as the reference sets them); schmid2 radii."""
+    from amrvac_b200 import config_from_par
+    from amrvac_b200 import _lib
+    common = """
+ &meshlist
+        domain_nx1 = 64
+        domain_nx2 = 64
+ /
+ &paramlist
+        courantpar = 0.9
+ /
+"""
+    p = tmp_path / "a.par"
+    p.write_text(""" &methodlist
+        time_stepper = 'twostep'
+        flux_scheme = 20*'tvdmu'
+        limiter = 20*'albada'
+        dimsplit = .true.
+        typeboundspeed = 'cmaxmean'
+ /
+""" + common)
+    c = config_from_par([str(p)]).cfg
+    assert (c.time_stepper, c.flux_scheme, c.limiter, c.dimsplit) == (2, _lib.FS["tvdmu"], 6, 1)
+    assert c.typeboundspeed == 2 and c.nghostcells == 2
+    p.write_text(""" &methodlist
+        time_stepper = 'fivestep'
+        flux_scheme = 20*'hll'
+        limiter = 20*'mp5'
+        dimsplit = .true.
+        typedimsplit = 'xy'
+ /
+""" + common)
+    c = config_from_par([str(p)]).cfg
+    assert (c.time_stepper, c.limiter, c.nghostcells, c.dimsplit) == (5, 13, 3, 2)
+    p.write_text(""" &methodlist
+        limiter = 20*'schmid2'
+        schmid_rad1 = 2.5d0
+        schmid_rad2 = 0.5d0
+ /
+""" + common)
+    c = config_from_par([str(p)]).cfg
+    assert c.limiter == 10 and list(c.schmid_rad) == [2.5, 0.5, 1.0]
