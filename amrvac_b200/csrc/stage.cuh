@@ -705,16 +705,16 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
     // and the y phase one round of 256 (instead of two rounds of 256 + 16).
     // (With 272 or more threads a phase of 272 faces is one round already;
     // a split sweep has one phase only.)
-    const bool MERGE_YX = STAGE_THREADS < FB && dsel < 0;
+    const bool merge_yx = STAGE_THREADS < FB && dsel < 0;
     const int dlo = update ? 0 : (NDIM == 3 && k == k0 - 1 ? 2 : NDIM);
 #pragma unroll 1
     for (int D = dlo; D < NDIM; ++D) {
       if (dsel >= 0 && D != dsel) continue;  // not this sweep's direction (uniform)
-      const int nface = D == 0 ? (MERGE_YX ? FB + BN : FB) : (D == 1 && !MERGE_YX ? FB : BN * BN);
+      const int nface = D == 0 ? (merge_yx ? FB + BN : FB) : (D == 1 && !merge_yx ? FB : BN * BN);
       // direction FD and index fl (in that direction's face layout) of face f
       // of this phase
       auto face_dir = [&](int f, int &FD, int &fl) {
-        if (MERGE_YX && D == 0 && f >= FB) { FD = 1; fl = BN * BN + (f - FB); }
+        if (merge_yx && D == 0 && f >= FB) { FD = 1; fl = BN * BN + (f - FB); }
         else { FD = D; fl = f; }
       };
       // where the flux of variable ov of face f lives
@@ -920,7 +920,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
 #pragma unroll
           for (int v = 0; v < NW; ++v) {
             // the face above the top row was computed in the x phase
-            const TF up = (MERGE_YX && cj == BN - 1) ? tv.yx[v * BN + ci] : tv.fb[v * FB + f + BN];
+            const TF up = (merge_yx && cj == BN - 1) ? tv.yx[v * BN + ci] : tv.fb[v * FB + f + BN];
             if constexpr (FP64) acc[v] = acc[v] + up - tv.fb[v * FB + f];
             else acc[v] = acc[v] + sc * double(up) - sc * double(tv.fb[v * FB + f]);
           }
