@@ -211,6 +211,11 @@ int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a,
   if (restore) CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * c->nblocks, c->stream));
   CK(hancock ? c->ks.hancock(A, nctas, c->stream) : c->ks.stage(A, nctas, c->stream));
   ++c->launches;
+  if (c->cfg.ndim == 3 && c->cfg.physics == 1 && c->cfg.typedivbfix == AMRVAC_DIVB_LINDE) {
+    if (!c->ks.linde3d) return fail(AMRVAC_E_UNSUPPORTED, "no 3-D Linde kernel for this configuration");
+    CK(c->ks.linde3d(A, c->stream));  // addsource2 of finite_volume / hancock
+    ++c->launches;
+  }
   if (hancock) return 0;
   if (restore) {
     CK(launch_restore_blocks(c->pool[reg_ct], c->pool[reg_new], c->d_block_status, c->nblocks,
@@ -477,8 +482,6 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   if (k.physics == 1) {
     if (k.typedivbfix != AMRVAC_DIVB_NONE && k.typedivbfix != AMRVAC_DIVB_GLM && k.typedivbfix != AMRVAC_DIVB_LINDE)
       return fail(AMRVAC_E_UNSUPPORTED, "typedivbfix must be none, glm or linde");
-    if (k.ndim == 3 && k.typedivbfix == AMRVAC_DIVB_LINDE)
-      return fail(AMRVAC_E_UNSUPPORTED, "3-D Linde divB source not supported (use glm)");
   } else if (k.flux_scheme == AMRVAC_FS_HLLD) {
     return fail(AMRVAC_E_UNSUPPORTED, "hlld needs mhd");
   }

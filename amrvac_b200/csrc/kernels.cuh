@@ -164,6 +164,65 @@ __global__ void cbounds_points_kernel(const PointArgs A) {
   if (A.out2) A.out2[p] = cmin;
 }
 
+// ---------------------------------------------------------------- Linde, 3-D
+// add_source_linde (src/mhd/mod_mhd_phys.t:5599-5665) for 3-D blocks, run
+// after the stage kernel on its output: w(B_d) += g_d, w(e) += wCT(B_d) g_d
+// with g_d = divbdiff / sum_d(1/dx_d^2) * d(divB)/dx_d (central), divB of wCT
+// (central, get_divb with mhd_divb_nth = 1), leaving out the cell layers next
+// to level-jump faces; then the small-value check of mhd_add_source.  Its
+// stencil (divB at the six neighbours: B two cells out and across the z
+// planes' halos) is gathered here through the stage's neighbour resolution
+// (and the level-jump ghost buffers); one CTA per z-plane of a block.
+template <int NDIR>
+__global__ void __launch_bounds__(256) linde3d_kernel(const StageArgs A) {
+  using V = Vars<true, NDIR, false>;
+  constexpr int NW = V::NW;
+  const int b = blockIdx.x / BN, k = blockIdx.x - (blockIdx.x / BN) * BN;
+  const int i = threadIdx.x & (BN - 1), j = threadIdx.x >> 4;
+  if (b >= A.nblocks) return;
+  const int m = A.amr_face ? A.amr_face[b] : 0;
+  if (m && (((m & 1) && i == 0) || ((m & 2) && i == BN - 1) || ((m & 4) && j == 0) || ((m & 8) && j == BN - 1) ||
+            ((m & 16) && k == 0) || ((m & 32) && k == BN - 1)))
+    return;
+  double dx[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) dx[d] = A.dxb[b * 3 + d];
+  auto bct = [&](int ii, int jj, int kk, int c) -> double {  // wCT's B_c, up to two cells outside
+    uint32_t flip;
+    const int blk = resolve_cell<3>(A, b, ii, jj, kk, flip);
+    const int v = V::B0 + c;
+    const double x = blk >= 0 ? __ldg(A.uin + cell_offset<3>(blk, NW, v, ii, jj, kk))
+                              : __ldg(A.gbuf + ghost_offset<3>(-2 - blk, NW, v, ii, jj, kk));
+    return ((flip >> v) & 1u) ? -x : x;
+  };
+  auto divb = [&](int ii, int jj, int kk) {
+    double d = 0.5 * (bct(ii + 1, jj, kk, 0) - bct(ii - 1, jj, kk, 0)) * (1.0 / dx[0]);
+    d = d + 0.5 * (bct(ii, jj + 1, kk, 1) - bct(ii, jj - 1, kk, 1)) * (1.0 / dx[1]);
+    d = d + 0.5 * (bct(ii, jj, kk + 1, 2) - bct(ii, jj, kk - 1, 2)) * (1.0 / dx[2]);
+    return d;
+  };
+  const double inv2 = (1.0 / (dx[0] * dx[0]) + 1.0 / (dx[1] * dx[1])) + 1.0 / (dx[2] * dx[2]);
+  double w[NW];
+#pragma unroll
+  for (int v = 0; v < NW; ++v) w[v] = A.uout[cell_offset<3>(b, NW, v, i, j, k)];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double dp = d == 0 ? divb(i + 1, j, k) : (d == 1 ? divb(i, j + 1, k) : divb(i, j, k + 1));
+    const double dm = d == 0 ? divb(i - 1, j, k) : (d == 1 ? divb(i, j - 1, k) : divb(i, j, k - 1));
+    double g = (dp - dm) * 0.5;
+    g = g / dx[d];
+    g = g * A.P.divbdiff / inv2;
+    w[V::B0 + d] = w[V::B0 + d] + g;
+    w[V::E] = w[V::E] + __ldg(A.uin + cell_offset<3>(b, NW, V::B0 + d, i, j, k)) * g;
+  }
+  if (A.P.fix_small_values) {
+    if (small_values<double, true, NDIR, false>(w, false, A.P) && A.P.small_values_method != 1)
+      atomicOr(A.status, ST_SMALL_VALUE);
+  }
+#pragma unroll
+  for (int v = 0; v < NW; ++v) A.uout[cell_offset<3>(b, NW, v, i, j, k)] = w[v];
+}
+
 // ---------------------------------------------------------------- dispatch
 struct KernelSet {
   cudaError_t (*prepare)() = nullptr;
@@ -171,6 +230,8 @@ struct KernelSet {
   cudaError_t (*stage)(const StageArgs &, int nctas, cudaStream_t) = nullptr;
   // MUSCL-Hancock predictor of twostep Predictor_Corrector (tvdlf sets only)
   cudaError_t (*hancock)(const StageArgs &, int nctas, cudaStream_t) = nullptr;
+  // the 3-D Linde divB source after a stage (3-D MHD sets without GLM)
+  cudaError_t (*linde3d)(const StageArgs &, cudaStream_t) = nullptr;
   cudaError_t (*getdt)(const GetdtArgs &, cudaStream_t) = nullptr;
   cudaError_t (*riemann_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
   cudaError_t (*flux_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
@@ -197,6 +258,14 @@ struct Launch {
   static cudaError_t stage(const StageArgs &A, int nctas, cudaStream_t s) {
     fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
     return cudaGetLastError();
+  }
+  static cudaError_t linde3d(const StageArgs &A, cudaStream_t s) {
+    if constexpr (MHD && NDIM == 3 && !GLM) {
+      linde3d_kernel<NDIR><<<A.nblocks * BN, 256, 0, s>>>(A);
+      return cudaGetLastError();
+    } else {
+      return cudaErrorNotSupported;
+    }
   }
   static cudaError_t hancock(const StageArgs &A, int nctas, cudaStream_t s) {
     if constexpr (HAS_HANCOCK) {
@@ -256,6 +325,7 @@ struct Launch {
     k.ctas_per_sm = &ctas_per_sm;
     k.stage = &stage;
     if (HAS_HANCOCK) k.hancock = &hancock;
+    if (MHD && NDIM == 3 && !GLM) k.linde3d = &linde3d;
     k.getdt = &getdt;
     k.riemann_points = &riemann_points;
     k.flux_points = &flux_points;

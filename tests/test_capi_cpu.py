@@ -58,7 +58,7 @@ def test_unsupported_configurations_are_refused_without_gpu(lib):
     """Config errors come back as negative codes before any CUDA call."""
     from amrvac_b200 import make_cfg, _lib
     h = ctypes.c_void_p()
-    bad = [make_cfg(physics="mhd", ndim=3, typedivbfix="linde", flux_scheme="hll"),
+    bad = [make_cfg(physics="mhd", ndim=3, typedivbfix="glm", flux_scheme="tvdmu", dimsplit=True),
            make_cfg(physics="hd", ndim=2, flux_scheme="hlld")]
     c = make_cfg(physics="hd", ndim=2)
     c.block_nx[0] = 8

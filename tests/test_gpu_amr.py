@@ -90,6 +90,9 @@ CASES = [
                                              bc=["symm", "symm", "periodic", "periodic"])),
     ("mhd2_hlld_cont", 2, 2, dict(physics="mhd", flux_scheme="hlld", limiter="cada3", typedivbfix="glm",
                                   bc=["cont"] * 4)),
+    ("mhd3_hll_minmod_linde", 3, 2, dict(physics="mhd", flux_scheme="hll", limiter="minmod", typedivbfix="linde")),
+    ("mhd3_hlld_vanleer_linde_cont", 3, 2, dict(physics="mhd", flux_scheme="hlld", limiter="vanleer",
+                                                typedivbfix="linde", bc=["cont"] * 6)),
     ("hd3_hllc_cont", 3, 2, dict(physics="hd", flux_scheme="hllc", limiter="vanleer", bc=["cont"] * 6)),
 ]
 

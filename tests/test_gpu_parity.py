@@ -54,6 +54,10 @@ CASES = {
                                             typedivbfix="glm", typeboundspeed="cmaxmean"),
     "mhd3_hllc_minmod_glm": dict(physics="mhd", ndim=3, flux_scheme="hllc", limiter="minmod", typedivbfix="glm"),
     "mhd3_hllc_cada3_none": dict(physics="mhd", ndim=3, flux_scheme="hllc", limiter="cada3", typedivbfix="none"),
+    # the Linde divB source in 3-D (the reference's default typedivbfix)
+    "mhd3_hll_cada3_linde": dict(physics="mhd", ndim=3, flux_scheme="hll", limiter="cada3", typedivbfix="linde"),
+    "mhd3_hlld_vanleer_linde": dict(physics="mhd", ndim=3, flux_scheme="hlld", limiter="vanleer",
+                                    typedivbfix="linde"),
     # the schmid2 slope limiter (per-direction schmid_rad; radii near the
     # median of sqrt(0.4 (a^2 + b^2)) / dx^2 on this data, so both of its
     # branches occur)
