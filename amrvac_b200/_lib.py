@@ -21,7 +21,7 @@ ST_SMALL_VALUE, ST_NAN, ST_DT_TOO_SMALL = 1, 2, 4
 
 FS = {"tvdlf": 1, "hll": 2, "hllc": 3, "hlld": 4, "tvdmu": 5}
 LIMITER = {"minmod": 1, "woodward": 2, "mcbeta": 3, "superbee": 4, "vanleer": 5,
-           "albada": 6, "koren": 7, "cada": 8, "cada3": 9, "schmid2": 10, "venk": 11, "mp5": 13,
+           "albada": 6, "koren": 7, "cada": 8, "cada3": 9, "schmid1": 10, "schmid2": 10, "venk": 11, "mp5": 13,
            "weno3": 14, "wenoyc3": 15,
            "weno5": 16, "wenoz5": 18, "wenozp5": 20}
 BOUNDSPEED = {"Einfeldt": 1, "cmaxmean": 2, "cmaxleftright": 3}
@@ -58,6 +58,7 @@ class AmrvacCfg(ctypes.Structure):
         ("time_integrator", ctypes.c_int),
         ("dimsplit", ctypes.c_int),
         ("schmid_rad", ctypes.c_double * 3),
+        ("schmid_global", ctypes.c_int),
     ]
 
 

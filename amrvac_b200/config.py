@@ -155,6 +155,7 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
     c.dimsplit = 0 if not dimsplit else (2 if typedimsplit == "xy" else 1)
     for d in range(3):
         c.schmid_rad[d] = float(schmid_rad[d])
+    c.schmid_global = int(limiter == "schmid1")
     nw = L.amrvac_gpu_nw(c)
     tb = typeboundary or ["periodic"] * (2 * ndim)
     for s in range(6):

@@ -243,6 +243,14 @@ int launch_getdt(amrvac_ctx *c, int reg) {
   G.P = c->P;
   CK(c->ks.getdt(G, c->stream));
   ++c->launches;
+  if (c->cfg.schmid_global) {  // a2max_global for schmid1 (getdt_courant + MPI_ALLREDUCE max)
+    if (c->amr)
+      if (int r = launch_amr_ghost_pass(c, reg)) return r;
+    CK(cudaMemsetAsync(c->d_scal + 10, 0, 3 * sizeof(double), c->stream));
+    StageArgs A = stage_args(c, reg, reg, reg, 0.0, 1.0, 1.0);
+    CK(c->ks.a2max(A, c->d_scal + 10, c->stream));
+    ++c->launches;
+  }
   return 0;
 }
 
@@ -526,6 +534,7 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   P.tvdlfeps = k.tvdlfeps;
   P.cada3_radius = k.cada3_radius;
   for (int d = 0; d < 3; ++d) P.schmid_rad[d] = k.schmid_rad[d];
+  P.schmid_global = k.schmid_global;
   P.glm_alpha = k.mhd_glm_alpha;
   P.divbdiff = k.divbdiff;
   P.courantpar = k.courantpar;
@@ -588,8 +597,9 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
     return cuda_fail(e, "cudaStreamCreate");
   }
   // scalars: dt, cmax_global, time, time_max, dtsave, dtmin, courantpar, final
-  // flag, slowsteps, steps since set_time
-  const double sc[10] = {0.0, 0.0, 0.0, 1.0e99, 0.0, k.dtmin, k.courantpar, 0.0, double(k.slowsteps), 0.0};
+  // flag, slowsteps, steps since set_time, a2max_global(1:3) (schmid1)
+  const double sc[13] = {0.0, 0.0, 0.0, 1.0e99, 0.0, k.dtmin, k.courantpar, 0.0, double(k.slowsteps), 0.0,
+                         0.0, 0.0, 0.0};
   if ((e = cudaMalloc(&c->d_scal, sizeof(sc))) != cudaSuccess ||
       (e = cudaMemcpy(c->d_scal, sc, sizeof(sc), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (e = cudaMalloc(&c->d_red, 2 * sizeof(unsigned long long))) != cudaSuccess ||

@@ -722,6 +722,8 @@ int amrvac_ens_create(const amrvac_cfg *cfg, int ninst, const amrvac_ens_instanc
   P.small_e = k.small_pressure / (k.gamma - 1.0);
   P.tvdlfeps = k.tvdlfeps;
   P.cada3_radius = k.cada3_radius;
+  for (int d = 0; d < 3; ++d) P.schmid_rad[d] = 1.0;  // the ensemble takes no schmid limiter
+  P.schmid_global = 0;
   P.courantpar = k.courantpar;
   P.limiter = 0;
   P.boundspeed = k.typeboundspeed;

@@ -164,6 +164,51 @@ __global__ void cbounds_points_kernel(const PointArgs A) {
   if (A.out2) A.out2[p] = cmin;
 }
 
+// ---------------------------------------------------------------- a2max
+// phys_get_a2max (hd_get_a2max src/hd/mod_hd_phys.t:813-833; MHD the same,
+// src/mhd/mod_mhd_phys.t:2678-2698) reduced as getdt_courant and setdt do
+// for schmid1 (src/mod_dt.t:193-197, 130): per block and direction d the
+// maximum over its cells and conserved variables of
+// |-w(i+2) + 16 w(i+1) - 30 w(i) + 16 w(i-1) - w(i-2)|, / 12 / dx_d^2, then
+// the maximum over blocks into out[d].  One CTA per z-plane of a block.
+template <int NW, int NDIM>
+__global__ void __launch_bounds__(256) a2max_kernel(const StageArgs A, double *out) {
+  constexpr int PL = NDIM == 3 ? BN : 1;
+  const int b = blockIdx.x / PL, k = blockIdx.x - (blockIdx.x / PL) * PL;
+  const int i = threadIdx.x & (BN - 1), j = threadIdx.x >> 4;
+  auto w = [&](int ii, int jj, int kk, int v) {
+    uint32_t flip;
+    const int blk = resolve_cell<NDIM>(A, b, ii, jj, kk, flip);
+    const double x = blk >= 0 ? __ldg(A.uin + cell_offset<NDIM>(blk, NW, v, ii, jj, kk))
+                              : __ldg(A.gbuf + ghost_offset<NDIM>(-2 - blk, NW, v, ii, jj, kk));
+    return ((flip >> v) & 1u) ? -x : x;
+  };
+  __shared__ double red[8];
+#pragma unroll 1
+  for (int d = 0; d < NDIM; ++d) {
+    const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+    double m = 0.0;
+#pragma unroll
+    for (int v = 0; v < NW; ++v) {
+      const double a = fabs(((((-w(i + 2 * e0, j + 2 * e1, k + 2 * e2, v) + 16.0 * w(i + e0, j + e1, k + e2, v)) -
+                               30.0 * w(i, j, k, v)) +
+                              16.0 * w(i - e0, j - e1, k - e2, v)) -
+                             w(i - 2 * e0, j - 2 * e1, k - 2 * e2, v)));
+      m = fmax(m, a);
+    }
+    m = warp_max(m);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double mm = red[0];
+      for (int q = 1; q < 8; ++q) mm = fmax(mm, red[q]);
+      const double dx = A.dxb[b * 3 + d];
+      atomic_max_pos(reinterpret_cast<unsigned long long *>(out + d), mm / 12.0 / (dx * dx));
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------- Linde, 3-D
 // add_source_linde (src/mhd/mod_mhd_phys.t:5599-5665) for 3-D blocks, run
 // after the stage kernel on its output: w(B_d) += g_d, w(e) += wCT(B_d) g_d
@@ -232,6 +277,8 @@ struct KernelSet {
   cudaError_t (*hancock)(const StageArgs &, int nctas, cudaStream_t) = nullptr;
   // the 3-D Linde divB source after a stage (3-D MHD sets without GLM)
   cudaError_t (*linde3d)(const StageArgs &, cudaStream_t) = nullptr;
+  // a2max_global of schmid1 (every set)
+  cudaError_t (*a2max)(const StageArgs &, double *out, cudaStream_t) = nullptr;
   cudaError_t (*getdt)(const GetdtArgs &, cudaStream_t) = nullptr;
   cudaError_t (*riemann_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
   cudaError_t (*flux_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
@@ -257,6 +304,10 @@ struct Launch {
   }
   static cudaError_t stage(const StageArgs &A, int nctas, cudaStream_t s) {
     fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
+    return cudaGetLastError();
+  }
+  static cudaError_t a2max(const StageArgs &A, double *out, cudaStream_t s) {
+    a2max_kernel<V::NW, NDIM><<<A.nblocks * (NDIM == 3 ? BN : 1), 256, 0, s>>>(A, out);
     return cudaGetLastError();
   }
   static cudaError_t linde3d(const StageArgs &A, cudaStream_t s) {
@@ -326,6 +377,7 @@ struct Launch {
     k.stage = &stage;
     if (HAS_HANCOCK) k.hancock = &hancock;
     if (MHD && NDIM == 3 && !GLM) k.linde3d = &linde3d;
+    k.a2max = &a2max;
     k.getdt = &getdt;
     k.riemann_points = &riemann_points;
     k.flux_points = &flux_points;

@@ -31,7 +31,7 @@ struct PhysParams {
   double small_density, small_pressure, small_e;
   double tvdlfeps, cada3_radius, glm_alpha, divbdiff, courantpar;
   double schmid_rad[3];
-  int limiter, boundspeed, divb, glm_extended;
+  int limiter, boundspeed, divb, glm_extended, schmid_global;
   int fix_small_values, check_small_values, small_values_method;
 };
 

@@ -604,9 +604,11 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
     dx[d] = d < NDIM ? A.dxb[b * 3 + d] : 1.0;
     dxinv[d] = -qdt / dx[d];
     const double r = P.cada3_radius * dx[d];
-    // cada3: 1 / (cada3_radius dx)^2; schmid: (schmid_rad + cadepsilon) dx^2
+    // cada3: 1 / (cada3_radius dx)^2; schmid: (a2max + cadepsilon) dx^2 with
+    // a2max = schmid_rad (schmid2) or a2max_global of this step (schmid1)
+    const double a2m = P.schmid_global ? A.dt_dev[10 + d] : P.schmid_rad[d];
     rdel[d] = (LIM == LIM_SCHMID || (LIM == 0 && P.limiter == LIM_SCHMID))
-                  ? (P.schmid_rad[d] + 1.0e-14) * (dx[d] * dx[d]) : 1.0 / (r * r);
+                  ? (a2m + 1.0e-14) * (dx[d] * dx[d]) : 1.0 / (r * r);
     if constexpr (LIM == LIM_WENO5) wlam[d] = pow(dx[d], 2.0 / 3.0);
   }
   double fz_prev[NDIM == 3 ? NW : 1];

@@ -59,7 +59,7 @@ extern "C" {
 #define AMRVAC_LIM_KOREN    7
 #define AMRVAC_LIM_CADA     8
 #define AMRVAC_LIM_CADA3    9
-#define AMRVAC_LIM_SCHMID   10  /* schmid2 (a2max = schmid_rad per direction) */
+#define AMRVAC_LIM_SCHMID   10  /* schmid2 (a2max = schmid_rad), schmid1 with schmid_global */
 #define AMRVAC_LIM_VENK     11  /* Venkatakrishnan */
 #define AMRVAC_LIM_MP5      13  /* fifth order, uniform grids, nghostcells >= 3 */
 #define AMRVAC_LIM_WENO3    14  /* third-order WENO */
@@ -139,6 +139,8 @@ typedef struct amrvac_cfg {
                                typedimsplit 'xyyx' (the order reverses on odd
                                steps), 2 'xy' (src/mod_advance.t:23-45) */
   double schmid_rad[3];     /* schmid limiter radii per direction (default 1) */
+  int schmid_global;        /* 1: schmid1, a2max from the domain every setdt
+                               (need_global_a2max) instead of schmid_rad */
 } amrvac_cfg;
 
 typedef struct amrvac_ctx amrvac_ctx;

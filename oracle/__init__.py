@@ -18,7 +18,7 @@ _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 
 FS = {"tvdlf": 1, "hll": 2, "hllc": 3, "hlld": 4, "tvdmu": 5}
 LIMITER = {"minmod": 1, "woodward": 2, "mcbeta": 3, "superbee": 4, "vanleer": 5,
-           "albada": 6, "koren": 7, "cada": 8, "cada3": 9, "schmid2": 10, "venk": 11, "mp5": 13, "weno3": 14, "wenoyc3": 15, "weno5": 16, "wenoz5": 18, "wenozp5": 20}
+           "albada": 6, "koren": 7, "cada": 8, "cada3": 9, "schmid1": 10, "schmid2": 10, "venk": 11, "mp5": 13, "weno3": 14, "wenoyc3": 15, "weno5": 16, "wenoz5": 18, "wenozp5": 20}
 BOUNDSPEED = {"Einfeldt": 1, "cmaxmean": 2, "cmaxleftright": 3}
 DIVB = {"none": 0, "glm": 1, "linde": 4}
 BC = {"periodic": 0, "cont": 1, "symm": 2, "asymm": 3}
@@ -40,6 +40,7 @@ class OrcCfg(ctypes.Structure):
         ("time_stepper", ctypes.c_int), ("time_integrator", ctypes.c_int),
         ("dimsplit", ctypes.c_int),
         ("schmid_rad", ctypes.c_double * 3),
+        ("schmid_global", ctypes.c_int),
     ]
 
 
@@ -165,6 +166,7 @@ def make_cfg(*, ndim=2, ndir=None, physics="hd", block_nx=16, nghost=2, gamma=No
     c.dimsplit = 0 if not dimsplit else (2 if typedimsplit == "xy" else 1)
     for d in range(3):
         c.schmid_rad[d] = float(schmid_rad[d])
+    c.schmid_global = int(limiter == "schmid1")
     lib().orc_cfg_finalize(ctypes.byref(c))
     return c
 

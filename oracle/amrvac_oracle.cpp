@@ -2075,16 +2075,39 @@ static void bc_phys_block(const State &s, const int *bcs, R *w, NBT nbt) {
 
 void orc_grid_getbc(orc_grid *g) { getbc_reg(*g, g->reg[0]); }
 
+// phys_get_a2max (src/hd/mod_hd_phys.t:813-833, src/mhd/mod_mhd_phys.t:
+// 2678-2698) of one ghosted block, maxed into a2m (getdt_courant,
+// src/mod_dt.t:193-197): |-w(i+2) + 16 w(i+1) - 30 w(i) + 16 w(i-1) - w(i-2)|
+// over the interior and every conserved variable, / 12 / dx^2.
+static void a2max_block(const State &s, const Arr<double> &w, const double *dx, double *a2m) {
+  const Box O = s.g.ixM();
+  for (int d = 0; d < s.c.ndim; ++d) {
+    const int o = s.g.off(d);
+    double m = 0.0;
+    for (int iw = 0; iw < s.x.nw; ++iw)
+      forbox(O, [&](int i, int j, int k) {
+        const double *q = &w.d[s.g.idx(i, j, k) + s.g.cells * (size_t)iw];
+        m = std::max(m, std::fabs((((-q[2 * o] + 16.0 * q[o]) - 30.0 * q[0]) + 16.0 * q[-o]) - q[-2 * o]));
+      });
+    a2m[d] = std::max(a2m[d], m / 12.0 / (dx[d] * dx[d]));
+  }
+}
+
 int orc_grid_getdt(orc_grid *g, double *dt, double *cmax_global) {
   const size_t bs = g->bsize;
   double dtmin = bigdouble, cmx = 0.0;
+  double a2m[3] = {0.0, 0.0, 0.0};
   int st = 0;
   for (int ib = 0; ib < g->nblocks; ++ib) {
     Arr<double> a = wrap_in(g->s.g, g->s.x.nw, &g->reg[0][bs * ib]);
     double dtn;
     st |= getdt_block(g->s, a, g->dx, &dtn, &cmx);
     dtmin = std::min(dtmin, dtn);
+    if (g->s.c.schmid_global) a2max_block(g->s, a, g->dx, a2m);
   }
+  // schmid1: the limiter's a2max is a2max_global of this setdt
+  if (g->s.c.schmid_global)
+    for (int d = 0; d < 3; ++d) g->s.c.schmid_rad[d] = a2m[d];
   *dt = dtmin;
   *cmax_global = cmx;
   return st;
@@ -3108,6 +3131,7 @@ void orc_amr_getbc(orc_amr *a) {
 int orc_amr_getdt(orc_amr *a, double *dt, double *cmax_global) {
   AmrGrid *G = reinterpret_cast<AmrGrid *>(a);
   double dtmin = bigdouble, cmx = 0.0;
+  double a2m[3] = {0.0, 0.0, 0.0};
   int st = 0;
   for (int b = 0; b < G->nb; ++b) {
     Arr<double> w = wrap_in(G->s.g, G->s.x.nw, &G->reg[0][G->bsize * b]);
@@ -3116,7 +3140,10 @@ int orc_amr_getdt(orc_amr *a, double *dt, double *cmax_global) {
     double dtn;
     st |= getdt_block(G->s, w, dxb, &dtn, &cmx);
     dtmin = std::min(dtmin, dtn);
+    if (G->s.c.schmid_global) a2max_block(G->s, w, dxb, a2m);
   }
+  if (G->s.c.schmid_global)
+    for (int d = 0; d < 3; ++d) G->s.c.schmid_rad[d] = a2m[d];
   *dt = dtmin;
   *cmax_global = cmx;
   return st;

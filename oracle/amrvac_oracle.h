@@ -67,6 +67,7 @@ typedef struct {
   int time_integrator;    /* twostep: 0 Predictor_Corrector, 2 ssprk2; fourstep: 0 ssprk4, 1 rk4 */
   int dimsplit;           /* 0 unsplit, 1 'xyyx', 2 'xy' */
   double schmid_rad[3];   /* schmid2 limiter radii per direction */
+  int schmid_global;      /* schmid1: a2max_global from every getdt instead */
 } orc_cfg;
 
 /* Number of flux variables implied by cfg (sets cfg->nw too). */

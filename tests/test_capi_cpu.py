@@ -209,4 +209,6 @@ def test_config_from_par_reads_the_method_options(tmp_path):
  /
 """ + common)
     c = config_from_par([str(p)]).cfg
-    assert c.limiter == 10 and list(c.schmid_rad) == [2.5, 0.5, 1.0]
+    assert c.limiter == 10 and list(c.schmid_rad) == [2.5, 0.5, 1.0] and c.schmid_global == 0
+    from amrvac_b200 import make_cfg
+    assert make_cfg(limiter="schmid1").schmid_global == 1
