@@ -594,8 +594,8 @@ def run_adjoint(args, ws, rank, local):
                        % ((3 + nsteps / every) * cells * 4 * 8 / 1e6)},
             "adjoint": {"forward_ms": tf, "backward_ms": tb, "adjoint_cost_vs_forward": tb / tf,
                         "forward_zone_updates_per_s": zu / (tf * 1e-3),
-                        "what": "backward = segment recomputation from checkpoints + per step two recomputed "
-                                "stages + three adjoint stages",
+                        "what": "backward = segment recomputation from checkpoints keeping every stage "
+                                "input + three adjoint stages per step",
                         "loss": float(L.detach()), "dL_dgamma": grad_g,
                         "fd_check": {"directions": args.grad_checks,
                                      "rel_err_by_eps": {str(e): {"median": float(np.median(v)), "max": float(np.max(v))}
