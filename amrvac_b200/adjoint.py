@@ -71,19 +71,46 @@ class FrozenDtSolver:
             out.append(self.ctx.get_time()[0])
         return np.array(out)
 
+    def _nstages(self):
+        return 3 if self.cfg.time_stepper == _lib.TIME_STEPPER["threestep"] else 2
+
+    def _step_keeping(self, seg_q, dt):
+        """One step that leaves its stage inputs in seg_q[0..nst-1]: U^n
+        before the step, U1 and U2 left in registers 1 and 2 by it."""
+        h = self.ctx.h
+        _lib.check(self.L.amrvac_gpu_register_copy(h, 0, _ptr(seg_q[0]), 0), "register_copy")
+        _lib.check(self.L.amrvac_gpu_step_dt(h, float(dt)), "step_dt")
+        for st in range(1, seg_q.shape[0]):
+            _lib.check(self.L.amrvac_gpu_register_copy(h, st, _ptr(seg_q[st]), 0), "register_copy")
+
     def forward(self, U0, dts, checkpoint_every=20):
+        """U_N and the checkpoints {step: U^step}.  The last segment, the
+        first one the backward walks, also keeps every stage input
+        (ckpt["last"] = (first step, [step][stage] states)), so the backward
+        recomputes only the segments before it."""
         torch = self.torch
         U0 = U0.contiguous()
         self._load(U0)
         ckpt = {0: U0.clone()}
+        N = len(dts)
+        s_last = ((N - 1) // checkpoint_every) * checkpoint_every if N else 0
+        seg = None
         for n, dt in enumerate(dts):
             if n > 0 and n % checkpoint_every == 0:
                 c = torch.empty(self.shape, dtype=torch.float64, device=U0.device)
                 self._store(c)
                 ckpt[n] = c
-            _lib.check(self.L.amrvac_gpu_step_dt(self.ctx.h, float(dt)), "step_dt")
+            if n >= s_last:
+                if seg is None:
+                    seg = torch.empty((checkpoint_every, self._nstages()) + self.shape, dtype=torch.float64,
+                                      device=U0.device)
+                self._step_keeping(seg[n - s_last], dt)
+            else:
+                _lib.check(self.L.amrvac_gpu_step_dt(self.ctx.h, float(dt)), "step_dt")
         UN = torch.empty(self.shape, dtype=torch.float64, device=U0.device)
         self._store(UN)
+        if seg is not None:
+            ckpt["last"] = (s_last, seg)
         return UN, ckpt
 
     def backward(self, lamN, dts, ckpt, checkpoint_every=20):
@@ -92,23 +119,23 @@ class FrozenDtSolver:
         lam = lamN.contiguous().clone()
         gpart = torch.zeros(self.ctx.nblocks, dtype=torch.float64, device=lam.device)
         N = len(dts)
-        starts = sorted(ckpt)
-        nst = 3 if self.cfg.time_stepper == _lib.TIME_STEPPER["threestep"] else 2
+        starts = sorted(k for k in ckpt if isinstance(k, int))
+        nst = self._nstages()
         h = self.ctx.h
+        kept = ckpt.get("last")
         seg = None
         for s0 in reversed(starts):
             s1 = min(s0 + checkpoint_every, N)
-            if seg is None:  # stage inputs of one segment: [step][stage] (reused)
-                seg = torch.empty((checkpoint_every, nst) + self.shape, dtype=torch.float64, device=lam.device)
-            # recompute the segment from its checkpoint, keeping every stage input:
-            # U^n before the step, U1 and U2 left in registers 1 and 2 by it
-            self._load(ckpt[s0])
-            for n in range(s0, s1):
-                q = n - s0
-                _lib.check(self.L.amrvac_gpu_register_copy(h, 0, _ptr(seg[q, 0]), 0), "register_copy")
-                _lib.check(self.L.amrvac_gpu_step_dt(h, float(dts[n])), "step_dt")
-                for st in range(1, nst):
-                    _lib.check(self.L.amrvac_gpu_register_copy(h, st, _ptr(seg[q, st]), 0), "register_copy")
+            if kept is not None and kept[0] == s0 and kept[1].shape[0] == checkpoint_every:
+                seg = kept[1]  # the forward kept this segment's stage inputs
+            else:
+                if seg is None or (kept is not None and seg is kept[1]):
+                    # stage inputs of one segment: [step][stage] (reused)
+                    seg = torch.empty((checkpoint_every, nst) + self.shape, dtype=torch.float64, device=lam.device)
+                # recompute the segment from its checkpoint, keeping every stage input
+                self._load(ckpt[s0])
+                for n in range(s0, s1):
+                    self._step_keeping(seg[n - s0], dts[n])
             for n in range(s1 - 1, s0 - 1, -1):
                 q = n - s0
                 u2 = _ptr(seg[q, 2]) if nst == 3 else None
