@@ -118,6 +118,7 @@ SIGNATURES = [
     ("amrvac_gpu_get_flux_points", _i, [_vp, _i, _dp, _dp, _i, _d, _dp]),
     ("amrvac_gpu_get_cbounds_points", _i, [_vp, _i, _dp, _dp, _dp, _dp, _i, _dp, _dp]),
     ("amrvac_gpu_riemann_points", _i, [_vp, _i, _dp, _dp, _i, _d, _dp]),
+    ("amrvac_gpu_div_points", _i, [_i, _dp, _dp, _dp, _dp, _dp]),
     ("amrvac_gpu_srl_maps", _i, [_i, _i, _ip, _ip, _ip, _ip]),
     ("amrvac_gpu_lohner", _i, [_vp, _i, _dp, _ip, _i, _dp, _dp, _dp, _ip, _ip, _dp]),
     ("amrvac_gpu_step_dt", _i, [_vp, _d]),

@@ -192,6 +192,22 @@ cudaError_t measure_fp64_peak(double *tflops) {
   return cudaGetLastError();
 }
 
+// The FP64 reciprocal and quotient of the stage kernels (rcp_, div_ in
+// physics.cuh) and the hardware seed they start from, point by point.
+__global__ void div_points_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
+                                  double *__restrict__ q, double *__restrict__ r, double *__restrict__ seed) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    q[i] = div_(x[i], y[i]);
+    r[i] = rcp_(y[i]);
+    seed[i] = rcp_seed(y[i]);
+  }
+}
+cudaError_t launch_div_points(int n, const double *x, const double *y, double *q, double *r, double *seed,
+                              cudaStream_t s) {
+  div_points_kernel<<<148 * 4, 256, 0, s>>>(n, x, y, q, r, seed);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_unpack(const double *src, double *pool, int first, int n, int nw, int ndim, int ng,
                           cudaStream_t s) {
   unpack_kernel<<<592, 256, 0, s>>>(src, pool, first, n, nw, ndim, ng);

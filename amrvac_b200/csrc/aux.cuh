@@ -22,6 +22,9 @@ struct BcSpec {
 };
 
 cudaError_t measure_fp64_peak(double *tflops);
+// rcp_ / div_ / rcp_seed of the stage kernels on n device points (test entry).
+cudaError_t launch_div_points(int n, const double *x, const double *y, double *q, double *r, double *seed,
+                              cudaStream_t s);
 cudaError_t launch_unpack(const double *src, double *pool, int first, int n, int nw, int ndim, int ng,
                           cudaStream_t s);
 cudaError_t launch_pack(const double *pool, double *dst, int first, int n, int nw, int ndim, int ng,

@@ -1575,6 +1575,22 @@ int amrvac_gpu_get_cbounds_points(amrvac_ctx *c, int n, const double *wlc, const
   return run_points(c, n, idim, wlc, wrc, wlp, wrp, cmax, 1, cmin, 0.0, 2);
 }
 
+int amrvac_gpu_div_points(int n, const double *x, const double *y, double *q, double *r, double *seed) {
+  if (n <= 0 || !x || !y || !q || !r || !seed) return fail(AMRVAC_E_ARG, "div_points: bad arguments");
+  const size_t b = sizeof(double) * (size_t)n;
+  double *d = nullptr;
+  CK(cudaMalloc(&d, 5 * b));
+  cudaError_t e = cudaMemcpy(d, x, b, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + n, y, b, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = launch_div_points(n, d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n, d + 4 * (size_t)n, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(q, d + 2 * (size_t)n, b, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(r, d + 3 * (size_t)n, b, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(seed, d + 4 * (size_t)n, b, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "div_points");
+  return 0;
+}
+
 
 // ---------------------------------------------------------------- adjoint
 int amrvac_gpu_step_dt(amrvac_ctx *c, double dt) {

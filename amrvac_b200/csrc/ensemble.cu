@@ -177,8 +177,10 @@ __device__ __forceinline__ uint32_t ens_face_at(const TF *s, const EnsView<TF, N
 #pragma unroll
     for (int o = 0; o < 4; ++o) q[o] = s[base[o] + ov * strd[o]];
     const TF d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
-    wLp[v] = q[1] + TF(0.5) * limited_slope<TF, true, 0>(lim, d1, d0, rd);
-    wRp[v] = q[2] - TF(0.5) * limited_slope<TF, false, 0>(lim, d2, d1, rd);
+    TF ldw, rdw;
+    face_slopes<TF, 0>(lim, d0, d1, d2, rd, ldw, rdw);
+    wLp[v] = q[1] + TF(0.5) * ldw;
+    wRp[v] = q[2] - TF(0.5) * rdw;
   }
   TF Fr[NW];
   uint32_t st;

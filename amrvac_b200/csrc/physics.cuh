@@ -55,24 +55,48 @@ __device__ __forceinline__ float div_(float x, float y) { return x / y; }
 #ifndef AMRVAC_IEEE_DIV
 #define AMRVAC_NR_DIV 1
 #endif
+// Correctly rounded IEEE division, out of line: the cold path of rcp_/div_.
+static __device__ __noinline__ double div_ieee(double x, double y) { return x / y; }
+// The hardware's approximate double-precision reciprocal (PTX
+// rcp.approx.ftz.f64): the seed of the Newton-Raphson reciprocal below.
+__device__ __forceinline__ double rcp_seed(double y) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(y));
+  return r;
+}
 #ifdef AMRVAC_NR_DIV
-// Reciprocal and quotient by Newton-Raphson iteration from a single-precision
-// seed (Markstein, "IA-64 and Elementary Functions", 2000, ch. 8): each step
-// r <- r + r(1 - y r) squares the relative error (2^-23 -> 2^-46 -> 2^-92); the
-// quotient gets one residual correction q <- q + r(x - y q).  Branch-free;
-// valid for |y| within the single-precision normal range (the path's
-// denominators are densities, wave speeds and limiter slopes >= 2^-26).
+// Reciprocal and quotient by Newton-Raphson iteration (Markstein, "IA-64 and
+// Elementary Functions", 2000, ch. 8) from the hardware's approximate
+// double-precision reciprocal (PTX rcp.approx.ftz.f64, about 20 correct bits
+// over the whole double exponent range).  Each step r <- r + r(1 - y r)
+// squares the relative error (2^-20 -> 2^-40 -> 2^-80); the quotient takes
+// one step and then the residual correction q <- q + r(x - y q), which
+// leaves an error of order 2^-80 before the final rounding.
+// Guard (integer operations on the high word): y zero, subnormal, infinite,
+// NaN or with |y| >= 2^1021 (1/y at or near the subnormal range), and a
+// quotient that came out non-finite, take the correctly rounded division
+// instead, so that every input gives IEEE's special values.
+__device__ __forceinline__ bool nr_range(double y) {
+  const unsigned e = ((unsigned)__double2hiint(y) >> 20) & 0x7ffu;  // biased exponent
+  return e - 1u < 2043u;  // 2^-1022 <= |y| < 2^1021
+}
+__device__ __forceinline__ bool finite_hi(double q) {
+  return ((unsigned)__double2hiint(q) & 0x7ff00000u) != 0x7ff00000u;
+}
 __device__ __forceinline__ double rcp_(double y) {
-  double r = (double)__frcp_rn(__double2float_rn(y));
-  double e = fma(-y, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-y, r, 1.0);
-  return fma(r, e, r);
+  double r = rcp_seed(y);
+  r = fma(r, fma(-y, r, 1.0), r);
+  r = fma(r, fma(-y, r, 1.0), r);
+  if (!nr_range(y)) r = div_ieee(1.0, y);
+  return r;
 }
 __device__ __forceinline__ double div_(double x, double y) {
-  const double r = rcp_(y);
-  const double q = x * r;
-  return fma(fma(-y, q, x), r, q);
+  double r = rcp_seed(y);
+  r = fma(r, fma(-y, r, 1.0), r);
+  const double q0 = x * r;
+  double q = fma(fma(-y, q0, x), r, q0);
+  if (!(nr_range(y) && finite_hi(q))) q = div_ieee(x, y);
+  return q;
 }
 #else
 __device__ __forceinline__ double rcp_(double y) { return 1.0 / y; }
@@ -369,6 +393,60 @@ __device__ __forceinline__ T slope_impl(int lim, T a, T b, T rdelinv) {
 template <class T, bool LEFT, int LIM>
 __device__ __forceinline__ T limited_slope(int lim_rt, T a, T b, T rdelinv) {
   return slope_impl<T, LEFT>(LIM ? LIM : lim_rt, a, b, rdelinv);
+}
+
+// phi of the cada3 / schmid limiters (dwlimiter2, src/limiter/mod_limiter.t:
+// 253-290, 291-333) from the slope ratio t and tmpeta: the asymptotic third-
+// order form below 1 - cadepsilon, the limited form above 1 + cadepsilon,
+// their blend in between.  alfa / gam: 0.5 / 1.6 (cada3), 1 / 1.5 (schmid).
+// The blend is formed only inside its 2e-14 wide band.
+template <class T>
+__device__ __forceinline__ T cada_blend_phi(T t, T tmpeta, T alfa, T gam) {
+  constexpr T cadbeta = T(2.0), cadepsilon = T(1.0e-14), invcadepsilon = T(1.0e14);
+  constexpr T third = T(1.0) / T(3.0);
+  const T A = (T(2.0) + t) * third;
+  const T lim2 = fmax(T(0.0), fmin(A, fmax(-(alfa * t), fmin(fmin(cadbeta * t, A), gam))));
+  const bool low = tmpeta <= T(1.0) - cadepsilon;
+  T phi = low ? A : lim2;
+  if (!low && !(tmpeta >= T(1.0) + cadepsilon)) {
+    const T t2 = (tmpeta - T(1.0)) * invcadepsilon;
+    phi = T(0.5) * ((T(1.0) - t2) * A + (T(1.0) + t2) * lim2);
+  }
+  return phi;
+}
+
+// Both limited slopes of one face i+1/2 and one variable from the centred
+// differences d0 = w(i)-w(i-1), d1 = w(i+1)-w(i), d2 = w(i+2)-w(i+1):
+// ldw of cell i (dwlimiter2 with a = d1, b = d0) and rdw of cell i+1
+// (a = d2, b = d1).  The cada family divides both ratios by the same
+// d1 + sign(eps, d1), so one reciprocal serves the face; the other limiters
+// take slope_impl as it is.
+template <class T, int LIM>
+__device__ __forceinline__ void face_slopes(int lim_rt, T d0, T d1, T d2, T rdelinv, T &ldw, T &rdw) {
+  constexpr T eps = T(1.4901161193847656e-08);  // sqrt(epsilon(1d0)) = 2**-26
+  const int lim = LIM ? LIM : lim_rt;
+  if (lim == LIM_CADA3 || lim == LIM_CADA || lim == LIM_SCHMID) {
+    const T rinv = rcp_(d1 + fsign(eps, d1));
+    const T tl = d0 * rinv, tr = d2 * rinv;
+    T pl, pr;
+    if (lim == LIM_CADA3) {
+      pl = cada_blend_phi<T>(tl, (d1 * d1 + d0 * d0) * rdelinv, T(0.5), T(1.6));
+      pr = cada_blend_phi<T>(tr, (d2 * d2 + d1 * d1) * rdelinv, T(0.5), T(1.6));
+    } else if (lim == LIM_SCHMID) {  // rdelinv carries (a2max + cadepsilon) dx^2
+      pl = cada_blend_phi<T>(tl, sqrt(T(0.4) * (d1 * d1 + d0 * d0)) / rdelinv, T(1.0), T(1.5));
+      pr = cada_blend_phi<T>(tr, sqrt(T(0.4) * (d2 * d2 + d1 * d1)) / rdelinv, T(1.0), T(1.5));
+    } else {  // cada
+      constexpr T third = T(1.0) / T(3.0);
+      const T al = (T(2.0) + tl) * third, ar = (T(2.0) + tr) * third;
+      pl = fmax(T(0.0), fmin(al, fmax(-(T(0.5) * tl), fmin(fmin(T(2.0) * tl, al), T(1.6)))));
+      pr = fmax(T(0.0), fmin(ar, fmax(-(T(0.5) * tr), fmin(fmin(T(2.0) * tr, ar), T(1.6)))));
+    }
+    ldw = pl * d1;  // phi * a (left), phi * b (right): both d1
+    rdw = pr * d1;
+  } else {
+    ldw = slope_impl<T, true>(lim, d1, d0, rdelinv);
+    rdw = slope_impl<T, false>(lim, d2, d1, rdelinv);
+  }
 }
 
 // Index in the reference variable order of entry v of a state whose vector

@@ -451,8 +451,10 @@ __device__ __forceinline__ void riemann_hlld(const T *wLC, const T *wRC, const T
   T w1R[NW], w1L[NW], w2R[NW], w2L[NW];
   w1R[m1] = sm; w1L[m1] = sm; w2R[m1] = sm; w2L[m1] = sm;
   w1R[b1] = Bx; w1L[b1] = Bx;
-  w1R[RHO] = div_(suR, sR - sm);
-  w1L[RHO] = div_(suL, sL - sm);
+  // one reciprocal of s - s_M per side serves the star density and energy
+  const T isR = rcp_(sR - sm), isL = rcp_(sL - sm);
+  w1R[RHO] = suR * isR;
+  w1L[RHO] = suL * isL;
   T r1R = suR * (sR - sm) - Bx * Bx;
   if (r1R != T(0.0)) r1R = rcp_(r1R);
   T r1L = suL * (sL - sm) - Bx * Bx;
@@ -480,8 +482,8 @@ __device__ __forceinline__ void riemann_hlld(const T *wLC, const T *wRC, const T
       v1bR = v1bR + w1R[M0 + c] * w1R[B0 + c];
       v1bL = v1bL + w1L[M0 + c] * w1L[B0 + c];
     }
-    w1R[E] = div_((sR - vR) * wRC[E] - ptR * vR + pts * sm + Bx * (vbR - v1bR), sR - sm);
-    w1L[E] = div_((sL - vL) * wLC[E] - ptL * vL + pts * sm + Bx * (vbL - v1bL), sL - sm);
+    w1R[E] = ((sR - vR) * wRC[E] - ptR * vR + pts * sm + Bx * (vbR - v1bR)) * isR;
+    w1L[E] = ((sL - vL) * wLC[E] - ptL * vL + pts * sm + Bx * (vbL - v1bL)) * isL;
   }
   w2R[RHO] = w1R[RHO]; w2L[RHO] = w1L[RHO];
   w2R[b1] = Bx; w2L[b1] = Bx;

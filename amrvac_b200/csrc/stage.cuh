@@ -488,8 +488,10 @@ __device__ __noinline__ FaceFlux64<Vars<MHD, NDIR, GLM>::NW> face_retry_fp64(
 #pragma unroll
     for (int o = 0; o < 4; ++o) q[o] = double(smem[base[o] + ov * strd[o]]);
     const double d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
-    wLp[v] = q[1] + 0.5 * limited_slope<double, true, LIM>(P.limiter, d1, d0, rd);
-    wRp[v] = q[2] - 0.5 * limited_slope<double, false, LIM>(P.limiter, d2, d1, rd);
+    double ldw, rdw;
+    face_slopes<double, LIM>(P.limiter, d0, d1, d2, rd, ldw, rdw);
+    wLp[v] = q[1] + 0.5 * ldw;
+    wRp[v] = q[2] - 0.5 * rdw;
   }
   FaceFlux64<NW> r;
   r.st = face_from_states<double, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, cg, r.F);
@@ -855,8 +857,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
 #pragma unroll
             for (int o = 0; o < 4; ++o) q[o] = smem[base[o] + ov * strd[o]];
             const TF d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
-            wLp[v] = q[1] + TF(0.5) * limited_slope<TF, true, LIM>(P.limiter, d1, d0, rd);
-            wRp[v] = q[2] - TF(0.5) * limited_slope<TF, false, LIM>(P.limiter, d2, d1, rd);
+            TF ldw, rdw;
+            face_slopes<TF, LIM>(P.limiter, d0, d1, d2, rd, ldw, rdw);
+            wLp[v] = q[1] + TF(0.5) * ldw;
+            wRp[v] = q[2] - TF(0.5) * rdw;
           }
         }
         TF Fr[NW];

@@ -289,6 +289,12 @@ int amrvac_gpu_get_cbounds_points(amrvac_ctx *ctx, int n, const double *wlc, con
                                   double *cmin);
 int amrvac_gpu_riemann_points(amrvac_ctx *ctx, int n, const double *wlp, const double *wrp, int idim,
                               double cmax_global, double *f);
+/* The FP64 reciprocal and quotient every stage kernel uses in place of the
+ * reference's divisions, on n host points: q = x/y, r = 1/y (Newton-Raphson
+ * from the hardware seed, with IEEE division outside its range), and the
+ * seed itself.  No counterpart in the reference (its divisions are IEEE);
+ * used to test the device arithmetic against IEEE division. */
+int amrvac_gpu_div_points(int n, const double *x, const double *y, double *q, double *r, double *seed);
 
 /* CFL reduction without any device allocation (no counterpart in the
  * reference).  For callers that must not call cudaMalloc/cudaFree: host codes

@@ -26,11 +26,12 @@ def _count(O, physics, ndim, ndir, bn, **kw):
 @pytest.mark.parametrize("wl,args,sizes", [
     ("ot128", ("mhd", 3, 3), (32, 64)),
     ("kh256", ("hd", 2, 2), (128, 256)),
+    ("amrblast3d", ("mhd", 3, 3), (32, 64)),
 ])
 def test_alg_flops_constants(oracle_lib, wl, args, sizes):
     import bench
-    kw = dict(flux_scheme="hlld", limiter="cada3", divb="glm") if args[0] == "mhd" else \
-        dict(flux_scheme="hllc", limiter="vanleer", gamma=1.4)
+    kw = dict(flux_scheme="hlld", limiter="vanleer" if wl == "amrblast3d" else "cada3", divb="glm") \
+        if args[0] == "mhd" else dict(flux_scheme="hllc", limiter="vanleer", gamma=1.4)
     a = _count(oracle_lib, *args, sizes[0], **kw)
     b = _count(oracle_lib, *args, sizes[1], **kw)
     stage = 2 * b[0] - a[0]

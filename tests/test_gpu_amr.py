@@ -12,6 +12,8 @@
 import numpy as np
 import pytest
 
+from tests._parity import percell_err
+
 from tests import _amr as A
 
 pytestmark = pytest.mark.gpu
@@ -133,9 +135,16 @@ def _bleaves(nd, levels):
 
 
 def _maxrel(a, b):
-    if not (np.isfinite(a).all() and np.isfinite(b).all()):
-        return np.inf
-    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    """Per-cell parity measure (tests/_parity.py) over a stack of blocks
+    (block, var, ...): relative error for cells >= 1e-3 of the variable's
+    maximum over the whole hierarchy, absolute at that scale below it."""
+    return percell_err(a, b, var_axis=1)
+
+
+def _worst_block(got, refs):
+    """The per-block error of the worst block, for the failure message."""
+    errs = [percell_err(got[b][None], refs[b][None]) for b in range(len(refs))]
+    return int(np.argmax(errs)), float(max(errs))
 
 
 @pytest.mark.parametrize("name,nd,levels,kw", CASES, ids=[c[0] for c in CASES])
@@ -147,9 +156,8 @@ def test_amr_ghosts_and_steps(oracle_lib, name, nd, levels, kw):
     assert ctx.amr_slots > 0
     # ghost cells of the initial state
     got = ctx.download()
-    for b in range(len(leaves)):
-        ref = og.get_block(b)
-        assert _maxrel(got[b], ref) <= 1e-13, (name, "ghosts", leaves[b], _maxrel(got[b], ref))
+    ref = np.array([og.get_block(b) for b in range(len(leaves))])
+    assert _maxrel(got, ref) <= 1e-13, (name, "ghosts", _maxrel(got, ref), _worst_block(got, ref))
     sl = (slice(None),) + tuple(slice(2, 18) if d < nd else slice(None) for d in (2, 1, 0))
     ctx.set_time(0.0, 1.0e99, 0.0)
     nsteps = 3 if nd == 2 else 2
@@ -159,10 +167,9 @@ def test_amr_ghosts_and_steps(oracle_lib, name, nd, levels, kw):
         dt_g, cm_g, _ = ctx.get_time()
         assert abs(dt_g - dt_o) <= 1e-13 * dt_o, (name, n, dt_g, dt_o)
         og.advance(dt_o, cm_o)
-        got = ctx.download()
-        for b in range(len(leaves)):
-            ref = og.get_block(b)
-            assert _maxrel(got[b][sl], ref[sl]) <= 1e-12, (name, n, leaves[b], _maxrel(got[b][sl], ref[sl]))
+        got = ctx.download()[(slice(None),) + sl]
+        ref = np.array([og.get_block(b)[sl] for b in range(len(leaves))])
+        assert _maxrel(got, ref) <= 1e-12, (name, n, _maxrel(got, ref), _worst_block(got, ref))
     assert ctx.status() == 0
     ctx.close()
 
@@ -331,10 +338,10 @@ def test_regrid_every_step_matches_oracle(oracle_lib, nd):
             g = g.remap(to.leaves, ops(origin))
         tree = new
         got = ctx.download()
-        for b in range(len(tree.leaves)):
-            ref = g.get_block(b)
-            assert _maxrel(got[b][sl], ref[sl]) <= 1e-12, (n, tree.leaves[b], _maxrel(got[b][sl], ref[sl]))
-            assert _maxrel(got[b], ref) <= 1e-12, (n, "ghosts", tree.leaves[b])
+        ref = np.array([g.get_block(b) for b in range(len(tree.leaves))])
+        gi, ri = got[(slice(None),) + sl], ref[(slice(None),) + sl]
+        assert _maxrel(gi, ri) <= 1e-12, (n, _maxrel(gi, ri), _worst_block(gi, ri))
+        assert _maxrel(got, ref) <= 1e-12, (n, "ghosts", _maxrel(got, ref), _worst_block(got, ref))
     assert changes >= 2 and max(tree.level_of()) == levels
     assert "child" in kinds
     if nd == 2:  # the refined corner was uniform: it coarsened

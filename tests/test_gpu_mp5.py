@@ -10,6 +10,8 @@ fill bit-exact (now three layers), one stage and full steps <= 1e-12.
 import numpy as np
 import pytest
 
+from tests._parity import percell_err
+
 from tests import _problems as P
 
 pytestmark = pytest.mark.gpu
@@ -77,13 +79,9 @@ def _setup(oracle_lib, name, n=32):
 
 
 def _maxrel(a, b):
-    if not (np.isfinite(a).all() and np.isfinite(b).all()):
-        return float("inf")
-    out = 0.0
-    for v in range(a.shape[1]):
-        scale = np.abs(b[:, v]).max() + 1e-300
-        out = max(out, float((np.abs(a[:, v] - b[:, v]) / (np.abs(b[:, v]) + 1e-3 * scale)).max()))
-    return out
+    """Per-cell parity measure (tests/_parity.py): relative error for cells
+    >= 1e-3 of the variable's maximum, absolute at that scale below it."""
+    return percell_err(a, b, var_axis=1)
 
 
 @pytest.mark.parametrize("name", sorted(CASES))

@@ -9,6 +9,8 @@ import ctypes
 import numpy as np
 import pytest
 
+from tests._parity import percell_err
+
 from tests import _problems as P
 
 pytestmark = pytest.mark.gpu
@@ -118,15 +120,9 @@ def _setup(oracle_lib, name, n=32, bc=None, seed=P.SEED):
 
 
 def _maxrel(a, b):
-    """max over cells of |a-b| / (|b| + 1e-3*max|b_v|) per variable."""
-    if not (np.isfinite(a).all() and np.isfinite(b).all()):
-        return float("inf")  # a non-finite value is never a match
-    out = 0.0
-    for v in range(a.shape[1]):
-        scale = np.abs(b[:, v]).max() + 1e-300
-        r = np.abs(a[:, v] - b[:, v]) / (np.abs(b[:, v]) + 1e-3 * scale)
-        out = max(out, float(r.max()))
-    return out
+    """Per-cell parity measure (tests/_parity.py): relative error for cells
+    >= 1e-3 of the variable's maximum, absolute at that scale below it."""
+    return percell_err(a, b, var_axis=1)
 
 
 @pytest.mark.parametrize("name", sorted(CASES))

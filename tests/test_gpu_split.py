@@ -12,6 +12,8 @@ the path's 1e-12 per cell.
 import numpy as np
 import pytest
 
+from tests._parity import percell_err
+
 from tests import _problems as P
 from tests import _amr as A
 
@@ -59,13 +61,9 @@ def _cuda():
 
 
 def _maxrel(a, b):
-    if not (np.isfinite(a).all() and np.isfinite(b).all()):
-        return float("inf")
-    out = 0.0
-    for v in range(a.shape[1]):
-        scale = np.abs(b[:, v]).max() + 1e-300
-        out = max(out, float((np.abs(a[:, v] - b[:, v]) / (np.abs(b[:, v]) + 1e-3 * scale)).max()))
-    return out
+    """Per-cell parity measure (tests/_parity.py): relative error for cells
+    >= 1e-3 of the variable's maximum, absolute at that scale below it."""
+    return percell_err(a, b, var_axis=1)
 
 
 def _cfgs(O, name, bc):
