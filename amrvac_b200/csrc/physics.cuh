@@ -103,6 +103,58 @@ __device__ __forceinline__ double rcp_(double y) { return 1.0 / y; }
 __device__ __forceinline__ double div_(double x, double y) { return x / y; }
 #endif
 
+// Unguarded forms for the hot face loop of the FP64 stage kernel, which
+// checks every face's flux and recomputes a face whose flux is not finite
+// with the guarded forms (rcp_, div_, IEEE sqrt).  On finite normal
+// operands in range they give the guarded forms' results; a zero,
+// subnormal, infinite or NaN denominator gives NaN (IEEE: +-inf or NaN),
+// which reaches the flux and sends the face to the recomputation.
+#ifdef AMRVAC_NR_DIV
+__device__ __forceinline__ double rcp_nr(double y) {
+  double r = rcp_seed(y);
+  r = fma(r, fma(-y, r, 1.0), r);
+  return fma(r, fma(-y, r, 1.0), r);
+}
+__device__ __forceinline__ double div_nr(double x, double y) {
+  double r = rcp_seed(y);
+  r = fma(r, fma(-y, r, 1.0), r);
+  const double q0 = x * r;
+  return fma(fma(-y, q0, x), r, q0);
+}
+#else
+__device__ __forceinline__ double rcp_nr(double y) { return 1.0 / y; }
+__device__ __forceinline__ double div_nr(double x, double y) { return x / y; }
+#endif
+// Square root by the coupled Newton iteration for sqrt(x) and 1/(2 sqrt(x))
+// (Markstein, ch. 8; Goldschmidt's form) from the hardware's approximate
+// reciprocal square root (PTX rsqrt.approx.ftz.f64): one coupled step takes
+// the seed's ~2^-20 to ~2^-40, the residual correction s + (x - s^2) h to the
+// order of 2^-80 before the final rounding.  The seed is capped at 2^511 so
+// that x = 0 gives 0 (the seed of 0 is infinite); a negative x gives NaN.
+__device__ __forceinline__ double sqrt_nr(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  y = fmin(y, 0x1.0p511);
+  double s = x * y, h = 0.5 * y;
+  const double r = fma(-s, h, 0.5);
+  s = fma(s, r, s);
+  h = fma(h, r, h);
+  return fma(fma(-s, s, x), h, s);
+}
+template <bool FAST> __device__ __forceinline__ double rcp_f(double y) {
+  if constexpr (FAST) return rcp_nr(y); else return rcp_(y);
+}
+template <bool FAST> __device__ __forceinline__ double div_f(double x, double y) {
+  if constexpr (FAST) return div_nr(x, y); else return div_(x, y);
+}
+template <bool FAST> __device__ __forceinline__ double sqrt_f(double x) {
+  if constexpr (FAST) return sqrt_nr(x); else return sqrt(x);
+}
+// the mixed form's single precision is IEEE throughout
+template <bool FAST> __device__ __forceinline__ float rcp_f(float y) { return rcp_(y); }
+template <bool FAST> __device__ __forceinline__ float div_f(float x, float y) { return div_(x, y); }
+template <bool FAST> __device__ __forceinline__ float sqrt_f(float x) { return sqrtf(x); }
+
 // ------------------------------------------------------------------ conversions
 // hd_to_primitive (mod_hd_phys.t:703-734) / mhd_to_primitive_origin (mod_mhd_phys.t:1741-1765)
 template <bool MHD, int NDIR, bool GLM>
@@ -222,10 +274,10 @@ __device__ __forceinline__ void phys_flux(const T *wc, const T *w, T cg,
 }
 
 // mhd_get_csound_prim (mod_mhd_phys.t:3329-3379): fast magnetosonic speed.
-template <class T, int NDIR, int BN>
+template <class T, int NDIR, int BN, bool FAST = false>
 __device__ __forceinline__ T fast_speed(const T *w, const PhysParams &P) {
   constexpr int RHO = 0, E = NDIR + 1, B0 = NDIR + 2;
-  const T inv_rho = rcp_(w[RHO]);
+  const T inv_rho = rcp_f<FAST>(w[RHO]);
   const T cs = T(P.gamma) * w[E] * inv_rho;
   T b2 = w[B0] * w[B0];
 #pragma unroll
@@ -233,12 +285,12 @@ __device__ __forceinline__ T fast_speed(const T *w, const PhysParams &P) {
   const T cfast2 = b2 * inv_rho + cs;
   T av = cfast2 * cfast2 - T(4.0) * cs * (w[BN] * w[BN]) * inv_rho;
   if (av < T(0.0)) av = T(0.0);
-  return sqrt(T(0.5) * (cfast2 + sqrt(av)));
+  return sqrt_f<FAST>(T(0.5) * (cfast2 + sqrt_f<FAST>(av)));
 }
 
 // hd_get_cbounds (mod_hd_phys.t:891-1001) / mhd_get_cbounds (mod_mhd_phys.t:3037-3127).
 // WITH_MIN=false gives the tvdlf form (cmax only).  Returns a status bit.
-template <class T, bool MHD, int NDIR, bool GLM, int D, bool WITH_MIN, int BS = 0>
+template <class T, bool MHD, int NDIR, bool GLM, int D, bool WITH_MIN, int BS = 0, bool FAST = false>
 __device__ __forceinline__ uint32_t cbounds(const T *wLC, const T *wRC, const T *wLp,
                                             const T *wRp, const PhysParams &P, T &cmax,
                                             T &cmin) {
@@ -247,21 +299,21 @@ __device__ __forceinline__ uint32_t cbounds(const T *wLC, const T *wRC, const T 
   uint32_t st = 0;
   const int bsel = BS ? BS : P.boundspeed;
   if (bsel == BS_EINFELDT) {
-    const T tmp1 = sqrt(wLp[V::RHO]);
-    const T tmp2 = sqrt(wRp[V::RHO]);
-    const T tmp3 = rcp_(tmp1 + tmp2);
+    const T tmp1 = sqrt_f<FAST>(wLp[V::RHO]);
+    const T tmp2 = sqrt_f<FAST>(wRp[V::RHO]);
+    const T tmp3 = rcp_f<FAST>(tmp1 + tmp2);
     const T umean = (wLp[MN] * tmp1 + wRp[MN] * tmp2) * tmp3;
     const T dv = wRp[MN] - wLp[MN];
     T dmean;
     if constexpr (MHD) {
-      const T csL = fast_speed<T, NDIR, V::B0 + D>(wLp, P);
-      const T csR = fast_speed<T, NDIR, V::B0 + D>(wRp, P);
-      dmean = sqrt((tmp1 * (csL * csL) + tmp2 * (csR * csR)) * tmp3 +
+      const T csL = fast_speed<T, NDIR, V::B0 + D, FAST>(wLp, P);
+      const T csR = fast_speed<T, NDIR, V::B0 + D, FAST>(wRp, P);
+      dmean = sqrt_f<FAST>((tmp1 * (csL * csL) + tmp2 * (csR * csR)) * tmp3 +
                    T(0.5) * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
     } else {
       const T csL = T(P.gamma) * wLp[V::E] / wLp[V::RHO];
       const T csR = T(P.gamma) * wRp[V::E] / wRp[V::RHO];
-      dmean = sqrt((tmp1 * csL + tmp2 * csR) * tmp3 + T(0.5) * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
+      dmean = sqrt_f<FAST>((tmp1 * csL + tmp2 * csR) * tmp3 + T(0.5) * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
     }
     if (WITH_MIN) {
       cmin = umean - dmean;
@@ -274,7 +326,7 @@ __device__ __forceinline__ uint32_t cbounds(const T *wLC, const T *wRC, const T 
       T wm[V::NW];
 #pragma unroll
       for (int v = 0; v < V::NW; ++v) wm[v] = T(0.5) * (wLp[v] + wRp[v]);
-      const T cs = fast_speed<T, NDIR, V::B0 + D>(wm, P);
+      const T cs = fast_speed<T, NDIR, V::B0 + D, FAST>(wm, P);
       if (WITH_MIN) {
         cmax = fmax(wm[MN] + cs, T(0.0));
         cmin = fmin(wm[MN] - cs, T(0.0));
@@ -295,7 +347,7 @@ __device__ __forceinline__ uint32_t cbounds(const T *wLC, const T *wRC, const T 
       } else if (P.check_small_values) {
         if (pth < T(P.small_pressure)) st |= ST_SMALL_VALUE;
       }
-      const T cs = sqrt(P.gamma * pth / wm[V::RHO]);
+      const T cs = sqrt_f<FAST>(P.gamma * pth / wm[V::RHO]);
       if (WITH_MIN) {
         cmax = fmax(tmp1 + cs, T(0.0));
         cmin = fmin(tmp1 - cs, T(0.0));
@@ -306,11 +358,11 @@ __device__ __forceinline__ uint32_t cbounds(const T *wLC, const T *wRC, const T 
   } else {  // cmaxleftright
     T cs;
     if constexpr (MHD) {
-      cs = fmax(fast_speed<T, NDIR, V::B0 + D>(wLp, P), fast_speed<T, NDIR, V::B0 + D>(wRp, P));
+      cs = fmax(fast_speed<T, NDIR, V::B0 + D, FAST>(wLp, P), fast_speed<T, NDIR, V::B0 + D, FAST>(wRp, P));
     } else {
       const T csL = T(P.gamma) * wLp[V::E] / wLp[V::RHO];
       const T csR = T(P.gamma) * wRp[V::E] / wRp[V::RHO];
-      cs = fmax(sqrt(csL), sqrt(csR));
+      cs = fmax(sqrt_f<FAST>(csL), sqrt_f<FAST>(csR));
     }
     if (WITH_MIN) cmin = fmin(wLp[MN], wRp[MN]) - cs;
     cmax = fmax(wLp[MN], wRp[MN]) + cs;
@@ -321,7 +373,7 @@ __device__ __forceinline__ uint32_t cbounds(const T *wLC, const T *wRC, const T 
 // ------------------------------------------------------------------ limiters
 // dwlimiter2 (mod_limiter.t:128-334) for one cell: a = dwC(ix) (forward
 // difference), b = dwC(ix-1) (backward difference).  LEFT selects ldw, else rdw.
-template <class T, bool LEFT>
+template <class T, bool LEFT, bool FAST = false>
 __device__ __forceinline__ T slope_impl(int lim, T a, T b, T rdelinv) {
   constexpr T qsmall = T(1.0e-12), qsmall2 = T(2.0e-12);
   constexpr T eps = T(1.4901161193847656e-08);  // sqrt(epsilon(1d0)) = 2**-26
@@ -334,12 +386,12 @@ __device__ __forceinline__ T slope_impl(int lim, T a, T b, T rdelinv) {
       return t * fmax(T(0.0), fmin(fabs(a), t * b));
     }
     case LIM_VANLEER:
-      return div_(T(2.0) * fmax(b * a, T(0.0)), a + b + qsmall);
+      return div_f<FAST>(T(2.0) * fmax(b * a, T(0.0)), a + b + qsmall);
     case LIM_CADA3: {
       // branch-free: both the asymptotic and the limited form are evaluated
       // and the reference's three-way choice is made with selects
       const T tmpeta = (a * a + b * b) * rdelinv;
-      const T t = LEFT ? div_(b, a + fsign(eps, a)) : div_(a, b + fsign(eps, b));
+      const T t = LEFT ? div_f<FAST>(b, a + fsign(eps, a)) : div_f<FAST>(a, b + fsign(eps, b));
       const T A = (T(2.0) + t) * third;
       const T lim2 = fmax(T(0.0), fmin(A, fmax(-(cadalfa * t), fmin(fmin(cadbeta * t, A), cadgamma))));
       const T t2 = (tmpeta - T(1.0)) * invcadepsilon;
@@ -351,7 +403,7 @@ __device__ __forceinline__ T slope_impl(int lim, T a, T b, T rdelinv) {
       // dwlimiter2 limiter_schmid (src/limiter/mod_limiter.t:291-333), the
       // schmid2 form: rdelinv carries (a2max + cadepsilon) dx^2 here
       const T tmpeta = sqrt(T(0.4) * (a * a + b * b)) / rdelinv;
-      const T t = LEFT ? div_(b, a + fsign(eps, a)) : div_(a, b + fsign(eps, b));
+      const T t = LEFT ? div_f<FAST>(b, a + fsign(eps, a)) : div_f<FAST>(a, b + fsign(eps, b));
       const T A = (T(2.0) + t) * third;
       const T lim2 = fmax(T(0.0), fmin(A, fmax(-t, fmin(fmin(cadbeta * t, A), T(1.5)))));
       const T t2 = (tmpeta - T(1.0)) * invcadepsilon;
@@ -421,20 +473,20 @@ __device__ __forceinline__ T cada_blend_phi(T t, T tmpeta, T alfa, T gam) {
 // (a = d2, b = d1).  The cada family divides both ratios by the same
 // d1 + sign(eps, d1), so one reciprocal serves the face; the other limiters
 // take slope_impl as it is.
-template <class T, int LIM>
+template <class T, int LIM, bool FAST = false>
 __device__ __forceinline__ void face_slopes(int lim_rt, T d0, T d1, T d2, T rdelinv, T &ldw, T &rdw) {
   constexpr T eps = T(1.4901161193847656e-08);  // sqrt(epsilon(1d0)) = 2**-26
   const int lim = LIM ? LIM : lim_rt;
   if (lim == LIM_CADA3 || lim == LIM_CADA || lim == LIM_SCHMID) {
-    const T rinv = rcp_(d1 + fsign(eps, d1));
+    const T rinv = rcp_f<FAST>(d1 + fsign(eps, d1));
     const T tl = d0 * rinv, tr = d2 * rinv;
     T pl, pr;
     if (lim == LIM_CADA3) {
       pl = cada_blend_phi<T>(tl, (d1 * d1 + d0 * d0) * rdelinv, T(0.5), T(1.6));
       pr = cada_blend_phi<T>(tr, (d2 * d2 + d1 * d1) * rdelinv, T(0.5), T(1.6));
     } else if (lim == LIM_SCHMID) {  // rdelinv carries (a2max + cadepsilon) dx^2
-      pl = cada_blend_phi<T>(tl, sqrt(T(0.4) * (d1 * d1 + d0 * d0)) / rdelinv, T(1.0), T(1.5));
-      pr = cada_blend_phi<T>(tr, sqrt(T(0.4) * (d2 * d2 + d1 * d1)) / rdelinv, T(1.0), T(1.5));
+      pl = cada_blend_phi<T>(tl, sqrt_f<FAST>(T(0.4) * (d1 * d1 + d0 * d0)) / rdelinv, T(1.0), T(1.5));
+      pr = cada_blend_phi<T>(tr, sqrt_f<FAST>(T(0.4) * (d2 * d2 + d1 * d1)) / rdelinv, T(1.0), T(1.5));
     } else {  // cada
       constexpr T third = T(1.0) / T(3.0);
       const T al = (T(2.0) + tl) * third, ar = (T(2.0) + tr) * third;
@@ -444,8 +496,8 @@ __device__ __forceinline__ void face_slopes(int lim_rt, T d0, T d1, T d2, T rdel
     ldw = pl * d1;  // phi * a (left), phi * b (right): both d1
     rdw = pr * d1;
   } else {
-    ldw = slope_impl<T, true>(lim, d1, d0, rdelinv);
-    rdw = slope_impl<T, false>(lim, d2, d1, rdelinv);
+    ldw = slope_impl<T, true, FAST>(lim, d1, d0, rdelinv);
+    rdw = slope_impl<T, false, FAST>(lim, d2, d1, rdelinv);
   }
 }
 

@@ -32,7 +32,7 @@ __device__ __forceinline__ void riemann_tvdlf(const T *wLC, const T *wRC, const 
 }
 
 // get_Riemann_flux_hll (mod_finite_volume.t:381-437)
-template <class T, bool MHD, int NDIR, bool GLM, int NDIM, int D>
+template <class T, bool MHD, int NDIR, bool GLM, int NDIM, int D, bool FAST = false>
 __device__ __forceinline__ void riemann_hll(const T *wLC, const T *wRC, const T *fL,
                                             const T *fR, T cmax, T cmin,
                                             T tvdlfeps, T *F) {
@@ -47,7 +47,7 @@ __device__ __forceinline__ void riemann_hll(const T *wLC, const T *wRC, const T 
     } else if (cmax <= T(0.0)) {
       F[v] = fR[v];
     } else {
-      F[v] = div_(cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v]), cmax - cmin);
+      F[v] = div_f<FAST>(cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v]), cmax - cmin);
     }
   }
 }
@@ -424,7 +424,7 @@ __device__ __forceinline__ void riemann_tvdmu_mhd(const T *wLC, const T *wRC, co
 }
 
 // get_Riemann_flux_hlld (mod_finite_volume.t:507-729), no B0 / equilibrium split.
-template <class T, int NDIR, bool GLM, int NDIM, int D>
+template <class T, int NDIR, bool GLM, int NDIM, int D, bool FAST = false>
 __device__ __forceinline__ void riemann_hlld(const T *wLC, const T *wRC, const T *wLp,
                                              const T *wRp, const T *fL, const T *fR,
                                              T sR, T sL, T *F) {
@@ -434,7 +434,7 @@ __device__ __forceinline__ void riemann_hlld(const T *wLC, const T *wRC, const T
   constexpr int ip1 = D, ip2 = (D + 1) % NDIR, ip3 = (D + 2) % NDIR;
   constexpr int m1 = M0 + ip1, m2 = M0 + ip2, m3 = M0 + ip3;
   constexpr int b1 = B0 + ip1, b2 = B0 + ip2, b3 = B0 + ip3;
-  const T Bx = div_(sR * wRC[b1] - sL * wLC[b1], sR - sL);
+  const T Bx = div_f<FAST>(sR * wRC[b1] - sL * wLC[b1], sR - sL);
   T bR2 = wRC[B0] * wRC[B0], bL2 = wLC[B0] * wLC[B0];
 #pragma unroll
   for (int c = 1; c < NDIR; ++c) {
@@ -446,19 +446,19 @@ __device__ __forceinline__ void riemann_hlld(const T *wLC, const T *wRC, const T
   const T vR = wRp[m1], vL = wLp[m1];
   const T suR = (sR - vR) * wRC[RHO];
   const T suL = (sL - vL) * wLC[RHO];
-  const T sm = div_(suR * vR - suL * vL - ptR + ptL, suR - suL);
+  const T sm = div_f<FAST>(suR * vR - suL * vL - ptR + ptL, suR - suL);
   // star states w1 (velocities in the momentum slots until the final conversion)
   T w1R[NW], w1L[NW], w2R[NW], w2L[NW];
   w1R[m1] = sm; w1L[m1] = sm; w2R[m1] = sm; w2L[m1] = sm;
   w1R[b1] = Bx; w1L[b1] = Bx;
   // one reciprocal of s - s_M per side serves the star density and energy
-  const T isR = rcp_(sR - sm), isL = rcp_(sL - sm);
+  const T isR = rcp_f<FAST>(sR - sm), isL = rcp_f<FAST>(sL - sm);
   w1R[RHO] = suR * isR;
   w1L[RHO] = suL * isL;
   T r1R = suR * (sR - sm) - Bx * Bx;
-  if (r1R != T(0.0)) r1R = rcp_(r1R);
+  if (r1R != T(0.0)) r1R = rcp_f<FAST>(r1R);
   T r1L = suL * (sL - sm) - Bx * Bx;
-  if (r1L != T(0.0)) r1L = rcp_(r1L);
+  if (r1L != T(0.0)) r1L = rcp_f<FAST>(r1L);
   w1R[m2] = wRp[m2] - Bx * wRC[b2] * (sm - vR) * r1R;
   w1L[m2] = wLp[m2] - Bx * wLC[b2] * (sm - vL) * r1L;
   T pb2R = (suR * (sR - vR) - Bx * Bx) * r1R;
@@ -487,12 +487,12 @@ __device__ __forceinline__ void riemann_hlld(const T *wLC, const T *wRC, const T
   }
   w2R[RHO] = w1R[RHO]; w2L[RHO] = w1L[RHO];
   w2R[b1] = Bx; w2L[b1] = Bx;
-  const T sqR = sqrt(w1R[RHO]);
-  const T sqL = sqrt(w1L[RHO]);
-  const T tmp = rcp_(sqR + sqL);
+  const T sqR = sqrt_f<FAST>(w1R[RHO]);
+  const T sqL = sqrt_f<FAST>(w1L[RHO]);
+  const T tmp = rcp_f<FAST>(sqR + sqL);
   const T signBx = copysign(T(1.0), Bx);
-  const T s1R = sm + div_(fabs(Bx), sqR);
-  const T s1L = sm - div_(fabs(Bx), sqL);
+  const T s1R = sm + div_f<FAST>(fabs(Bx), sqR);
+  const T s1L = sm - div_f<FAST>(fabs(Bx), sqL);
   w2R[m2] = (sqL * w1L[m2] + sqR * w1R[m2] + (w1R[b2] - w1L[b2]) * signBx) * tmp;
   w2L[m2] = w2R[m2];
   w2R[b2] = (sqL * w1R[b2] + sqR * w1L[b2] + sqL * sqR * (w1R[m2] - w1L[m2]) * signBx) * tmp;

@@ -197,7 +197,7 @@ __device__ __forceinline__ uint32_t load_prim(const StageArgs &A, int b, int i, 
 // Interface flux from reconstructed primitive left/right states: small-value
 // fix, to_conserved, GLM modify_wLR, physical fluxes, cbounds, Riemann solver
 // (src/mod_finite_volume.t:1217-1222, 200-245).  wLp/wRp are modified.
-template <class T, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int BS>
+template <class T, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int BS, bool FAST = false>
 __device__ __forceinline__ uint32_t face_from_states(T *wLp, T *wRp, const PhysParams &P, T cg, T *F,
                                                      bool small_check = true) {
   constexpr int D = 0;  // states arrive rotated: the face normal is component 0
@@ -219,7 +219,7 @@ __device__ __forceinline__ uint32_t face_from_states(T *wLp, T *wRp, const PhysP
     constexpr int BNI = V::B0 + D, PS = V::PSI, E = V::E;
     const T dB = wRp[BNI] - wLp[BNI];
     const T dPsi = wRp[PS] - wLp[PS];
-    const T nb = T(0.5) * (wRp[BNI] + wLp[BNI] - dPsi / cg);
+    const T nb = T(0.5) * (wRp[BNI] + wLp[BNI] - div_f<FAST>(dPsi, cg));
     const T np = T(0.5) * (wRp[PS] + wLp[PS] - dB * cg);
     wLp[BNI] = nb; wLp[PS] = np; wRp[BNI] = nb; wRp[PS] = np;
     wRC[E] = wRC[E] - T(0.5) * (wRC[BNI] * wRC[BNI]);
@@ -241,18 +241,18 @@ __device__ __forceinline__ uint32_t face_from_states(T *wLp, T *wRp, const PhysP
       riemann_tvdmu_hd<T, NDIR>(wLC, wRC, fL, fR, P, F);
     }
   } else if constexpr (SOLVER == SOLVER_TVDLF) {
-    st |= cbounds<T, MHD, NDIR, GLM, D, false, BS>(wLC, wRC, wLp, wRp, P, cmax, cmin);
+    st |= cbounds<T, MHD, NDIR, GLM, D, false, BS, FAST>(wLC, wRC, wLp, wRp, P, cmax, cmin);
     riemann_tvdlf<T, NW>(wLC, wRC, fL, fR, cmax, T(P.tvdlfeps), F);
   } else {
-    st |= cbounds<T, MHD, NDIR, GLM, D, true, BS>(wLC, wRC, wLp, wRp, P, cmax, cmin);
+    st |= cbounds<T, MHD, NDIR, GLM, D, true, BS, FAST>(wLC, wRC, wLp, wRp, P, cmax, cmin);
     if constexpr (SOLVER == SOLVER_HLL) {
-      riemann_hll<T, MHD, NDIR, GLM, NDIM, D>(wLC, wRC, fL, fR, cmax, cmin, T(P.tvdlfeps), F);
+      riemann_hll<T, MHD, NDIR, GLM, NDIM, D, FAST>(wLC, wRC, fL, fR, cmax, cmin, T(P.tvdlfeps), F);
     } else if constexpr (SOLVER == SOLVER_HLLC) {
       if constexpr (MHD) riemann_hllc_mhd<T, NDIR, GLM, NDIM, D>(wLC, wRC, fL, fR, cmax, cmin, T(P.tvdlfeps), F);
       else riemann_hllc_hd<T, NDIR, D>(wLC, wRC, fL, fR, cmax, cmin, F);
     } else {
       static_assert(MHD, "HLLD needs MHD");
-      riemann_hlld<T, NDIR, GLM, NDIM, D>(wLC, wRC, wLp, wRp, fL, fR, cmax, cmin, F);
+      riemann_hlld<T, NDIR, GLM, NDIM, D, FAST>(wLC, wRC, wLp, wRp, fL, fR, cmax, cmin, F);
     }
   }
   return st;
@@ -557,6 +557,12 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
   constexpr bool FP64 = sizeof(TF) == 8;
   constexpr int HW = HaloW<LIM>::value;  // halo width: 2, or 3 for MP5
   constexpr int H2 = 2 * HW;
+  // FP64 faces of the slope limiters use the unguarded division, reciprocal
+  // and square root (physics.cuh: rcp_nr, div_nr, sqrt_nr); a face whose
+  // flux is not finite is recomputed with the guarded forms in the fix-up
+  // pass after its phase, like the mixed form's FP32 faces.
+  constexpr bool FASTF = FP64 && !(LIM == LIM_MP5 || LIM == LIM_WENO5 || LIM == LIM_WENO3 || LIM == LIM_VENK);
+  constexpr bool RETRY = !FP64 || FASTF;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TF *smem = reinterpret_cast<TF *>(smem_raw);
   TileView<TF, NW, NDIM, HW> tv(smem);
@@ -589,7 +595,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
   const int ci = t & (BN - 1), cj = t >> 4;  // cell role for t < 256
   const bool cell_thread = t < BN * BN;
   const bool need_corners = MHD && !GLM && P.divb == DIVB_LINDE;
-  __shared__ int s_retry;  // mixed form: some face of this phase needs the FP64 retry
+  __shared__ int s_retry;  // some face of this phase needs the guarded FP64 recomputation
   if (t == 0) s_retry = 0;
 #pragma unroll 1
   while (g < gend) {
@@ -858,7 +864,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
             for (int o = 0; o < 4; ++o) q[o] = smem[base[o] + ov * strd[o]];
             const TF d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
             TF ldw, rdw;
-            face_slopes<TF, LIM>(P.limiter, d0, d1, d2, rd, ldw, rdw);
+            face_slopes<TF, LIM, FASTF>(P.limiter, d0, d1, d2, rd, ldw, rdw);
             wLp[v] = q[1] + TF(0.5) * ldw;
             wRp[v] = q[2] - TF(0.5) * rdw;
           }
@@ -866,9 +872,9 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
         TF Fr[NW];
         // the MP5 / WENO branches of reconstruct_LR have no small-value fix of
         // the states
-        stb |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, P, TF(cg), Fr,
-                                                                       HW == 2 && LIM != LIM_WENO3);
-        if constexpr (!FP64) {
+        stb |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS, FASTF>(wLp, wRp, P, TF(cg), Fr,
+                                                                              HW == 2 && LIM != LIM_WENO3);
+        if constexpr (RETRY) {
           bool finite = true;
 #pragma unroll
           for (int v = 0; v < NW; ++v) finite = finite && isfinite(Fr[v]);
@@ -886,8 +892,11 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
         if (amr_mask) capture(FD, fi, fj, Fr, sc);
       }
       __syncthreads();
-      if constexpr (!FP64) {
-        if (s_retry) {  // fix-up pass: the faces whose FP32 flux is not finite, in FP64
+      if constexpr (RETRY) {
+        // fix-up pass: the faces whose flux is not finite (an FP32 face of the
+        // mixed form, or an FP64 face that met a special operand in the
+        // unguarded arithmetic), recomputed in FP64 with the guarded forms
+        if (s_retry) {
           for (int f = t; f < nface; f += STAGE_THREADS) {
             int FD, fl;
             face_dir(f, FD, fl);
@@ -904,7 +913,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
             TF Fr[NW];
             for (int v = 0; v < NW; ++v) {
               Fr[v] = TF(r.F[v]);
-              flux_ref(f, FD, fl, orig_index_rt<MHD, NDIR>(v, FD)) = Fr[v];
+              // FP64 keeps the scaled flux fC = -qdt/dx f, mixed the FP32 flux
+              flux_ref(f, FD, fl, orig_index_rt<MHD, NDIR>(v, FD)) = FP64 ? TF(sc * r.F[v]) : Fr[v];
             }
             if (amr_mask) capture(FD, fi, fj, Fr, sc);
           }

@@ -12,7 +12,7 @@
 import numpy as np
 import pytest
 
-from tests._parity import percell_err
+from tests._parity import one_ulp_noise, percell_err
 
 from tests import _amr as A
 
@@ -99,6 +99,18 @@ CASES = [
 ]
 
 
+def _noisy_grid(O, og_cfg, nb, nd, leaves, blocks, bc=None):
+    """A second oracle hierarchy from the same blocks with one ulp of input
+    noise: its distance from the first is the reference formula's own
+    sensitivity on this data (the parity bar where it exceeds 1e-12)."""
+    g = O.AmrGrid(og_cfg, nb, [0.0] * nd, [1.0] * nd, leaves, **({"bc": bc} if bc else {}))
+    noisy = one_ulp_noise(np.asarray(blocks))
+    for b in range(len(leaves)):
+        g.set_block(b, noisy[b])
+    g.getbc()
+    return g
+
+
 def _setup(O, nd, levels, kw):
     from amrvac_b200 import Context, make_cfg
     leaves = _bleaves(nd, levels) if "bc" in kw else _leaves(nd, levels)
@@ -123,6 +135,7 @@ def _setup(O, nd, levels, kw):
     ctx = Context(gcfg)
     ctx.set_amr_grid(leaves, nb, [0.0] * nd, [1.0] * nd)
     ctx.upload(blocks)
+    og.noisy = _noisy_grid(O, ocfg, nb, nd, leaves, blocks, bc)
     return leaves, nb, og, ctx
 
 
@@ -167,9 +180,11 @@ def test_amr_ghosts_and_steps(oracle_lib, name, nd, levels, kw):
         dt_g, cm_g, _ = ctx.get_time()
         assert abs(dt_g - dt_o) <= 1e-13 * dt_o, (name, n, dt_g, dt_o)
         og.advance(dt_o, cm_o)
+        og.noisy.advance(dt_o, cm_o)
         got = ctx.download()[(slice(None),) + sl]
         ref = np.array([og.get_block(b)[sl] for b in range(len(leaves))])
-        assert _maxrel(got, ref) <= 1e-12, (name, n, _maxrel(got, ref), _worst_block(got, ref))
+        bar = max(1e-12, _maxrel(np.array([og.noisy.get_block(b)[sl] for b in range(len(leaves))]), ref))
+        assert _maxrel(got, ref) <= bar, (name, n, _maxrel(got, ref), bar, _worst_block(got, ref))
     assert ctx.status() == 0
     ctx.close()
 
@@ -317,6 +332,11 @@ def test_regrid_every_step_matches_oracle(oracle_lib, nd):
     for b in range(len(tree.leaves)):
         g.set_block(b, blocks[b])
     g.getbc()
+    gn = O.AmrGrid(ocfg, nb, xmin, xmax, tree.leaves)  # the same with one ulp of input noise
+    noisy = one_ulp_noise(np.asarray(blocks))
+    for b in range(len(tree.leaves)):
+        gn.set_block(b, noisy[b])
+    gn.getbc()
     sl = (slice(None),) + tuple(slice(2, 18) if d < nd else slice(None) for d in (2, 1, 0))
     ctx.set_time(0.0, 1.0e99, 0.0)
     changes = 0
@@ -326,6 +346,7 @@ def test_regrid_every_step_matches_oracle(oracle_lib, nd):
         ctx.step()
         assert abs(ctx.get_time()[0] - dt_o) <= 1e-13 * dt_o
         g.advance(dt_o, cm_o)
+        gn.advance(dt_o, cm_o)
         # the oracle's errest on its own state
         oflags = [O.lohner_block(ocfg, g.get_block(b), weight, np.zeros(nd + 2, np.int32), 1e-2, 0.1, 0.125,
                                  t[0], levels)[1:] for b, t in enumerate(tree.leaves)]
@@ -336,12 +357,14 @@ def test_regrid_every_step_matches_oracle(oracle_lib, nd):
             changes += 1
             kinds |= {o[0] for o in origin}
             g = g.remap(to.leaves, ops(origin))
+            gn = gn.remap(to.leaves, ops(origin))
         tree = new
         got = ctx.download()
         ref = np.array([g.get_block(b) for b in range(len(tree.leaves))])
+        bar = max(1e-12, _maxrel(np.array([gn.get_block(b) for b in range(len(tree.leaves))]), ref))
         gi, ri = got[(slice(None),) + sl], ref[(slice(None),) + sl]
-        assert _maxrel(gi, ri) <= 1e-12, (n, _maxrel(gi, ri), _worst_block(gi, ri))
-        assert _maxrel(got, ref) <= 1e-12, (n, "ghosts", _maxrel(got, ref), _worst_block(got, ref))
+        assert _maxrel(gi, ri) <= bar, (n, _maxrel(gi, ri), bar, _worst_block(gi, ri))
+        assert _maxrel(got, ref) <= bar, (n, "ghosts", _maxrel(got, ref), bar, _worst_block(got, ref))
     assert changes >= 2 and max(tree.level_of()) == levels
     assert "child" in kinds
     if nd == 2:  # the refined corner was uniform: it coarsened
