@@ -83,11 +83,12 @@ class FrozenDtSolver:
         for st in range(1, seg_q.shape[0]):
             _lib.check(self.L.amrvac_gpu_register_copy(h, st, _ptr(seg_q[st]), 0), "register_copy")
 
-    def forward(self, U0, dts, checkpoint_every=20):
-        """U_N and the checkpoints {step: U^step}.  The last segment, the
-        first one the backward walks, also keeps every stage input
-        (ckpt["last"] = (first step, [step][stage] states)), so the backward
-        recomputes only the segments before it."""
+    def forward(self, U0, dts, checkpoint_every=20, keep_last=True):
+        """U_N and the checkpoints {step: U^step}.  With keep_last, the last
+        segment, the first one the backward walks, also keeps every stage
+        input (ckpt["last"] = (first step, [step][stage] states)), so the
+        backward recomputes only the segments before it; a forward that no
+        backward follows passes keep_last=False and copies no stage input."""
         torch = self.torch
         U0 = U0.contiguous()
         self._load(U0)
@@ -100,7 +101,7 @@ class FrozenDtSolver:
                 c = torch.empty(self.shape, dtype=torch.float64, device=U0.device)
                 self._store(c)
                 ckpt[n] = c
-            if n >= s_last:
+            if keep_last and n >= s_last:
                 if seg is None:
                     seg = torch.empty((checkpoint_every, self._nstages()) + self.shape, dtype=torch.float64,
                                       device=U0.device)
@@ -122,15 +123,17 @@ class FrozenDtSolver:
         starts = sorted(k for k in ckpt if isinstance(k, int))
         nst = self._nstages()
         h = self.ctx.h
-        kept = ckpt.get("last")
+        kept = ckpt.pop("last", None)
         seg = None
         for s0 in reversed(starts):
             s1 = min(s0 + checkpoint_every, N)
             if kept is not None and kept[0] == s0 and kept[1].shape[0] == checkpoint_every:
                 seg = kept[1]  # the forward kept this segment's stage inputs
             else:
-                if seg is None or (kept is not None and seg is kept[1]):
-                    # stage inputs of one segment: [step][stage] (reused)
+                if seg is None:
+                    # stage inputs of one segment: [step][stage]; after the
+                    # kept segment has been walked its buffer is reused, so the
+                    # backward holds one segment buffer at a time
                     seg = torch.empty((checkpoint_every, nst) + self.shape, dtype=torch.float64, device=lam.device)
                 # recompute the segment from its checkpoint, keeping every stage input
                 self._load(ckpt[s0])
@@ -159,8 +162,9 @@ class _Solve:
                 @staticmethod
                 def forward(ctx, U0, gamma, dts, grid, checkpoint_every, cfg_kw, grad_on):
                     solver = FrozenDtSolver(*grid, float(gamma), **cfg_kw)
-                    UN, ckpt = solver.forward(U0.detach(), dts, checkpoint_every)
-                    if not (grad_on and any(ctx.needs_input_grad[:2])):
+                    want = grad_on and any(ctx.needs_input_grad[:2])
+                    UN, ckpt = solver.forward(U0.detach(), dts, checkpoint_every, keep_last=want)
+                    if not want:
                         solver.close()  # no backward will come: release the context now
                         return UN
                     ctx.solver = solver

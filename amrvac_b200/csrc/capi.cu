@@ -92,6 +92,7 @@ struct amrvac_ctx {
   int *d_amr_int = nullptr;            // [2][nblocks] levels, flags (Löhner, lazily)
   double *d_amr_err = nullptr;         // [nblocks] largest error per block
   bool adj_prepared = false;
+  bool a2max_set = false;  // schmid1: a getdt has reduced a2max_global since the last upload / grid change
   struct AmrDev *amr = nullptr;        // multi-level grid (amrvac_gpu_set_amr_grid)
   // Capacities (in blocks or elements) of the buffers that a new block set or
   // a regrid reuses while they are large enough (grown by 25 % otherwise).
@@ -250,7 +251,17 @@ int launch_getdt(amrvac_ctx *c, int reg) {
     StageArgs A = stage_args(c, reg, reg, reg, 0.0, 1.0, 1.0);
     CK(c->ks.a2max(A, c->d_scal + 10, c->stream));
     ++c->launches;
+    c->a2max_set = true;
   }
+  return 0;
+}
+
+// schmid1 reads a2max_global, which only the getdt phase reduces: a stage
+// called without a getdt on the current state would use a stale or zero
+// value, so it is refused.
+static int check_a2max(const amrvac_ctx *c) {
+  if (c->cfg.schmid_global && !c->a2max_set)
+    return fail(AMRVAC_E_STATE, "schmid1 (schmid_global): call amrvac_gpu_getdt on this state before a stage");
   return 0;
 }
 
@@ -642,6 +653,7 @@ static int set_blocks_impl(amrvac_ctx *c, int nblocks, const double *dx, const i
                            double *adopt_reg0 = nullptr);
 
 int amrvac_gpu_set_blocks(amrvac_ctx *c, int nblocks, const double *dx, const int *neighbor) {
+  if (c) c->a2max_set = false;
   return set_blocks_impl(c, nblocks, dx, neighbor, false);
 }
 
@@ -804,6 +816,7 @@ int amrvac_gpu_set_amr_grid(amrvac_ctx *c, int nleaf, const int *leaf, const int
 // domain and root blocks stay those of the current grid; registers 1 and 2
 // are scratch afterwards.
 int amrvac_gpu_amr_regrid(amrvac_ctx *c, int nleaf, const int *leaf, const int *op) {
+  if (c) c->a2max_set = false;
   if (int r = check_ctx(c, true)) return r;
   if (!c->amr) return fail(AMRVAC_E_STATE, "amr_regrid: no multi-level grid (amrvac_gpu_set_amr_grid)");
   if (!op) return fail(AMRVAC_E_ARG, "amr_regrid: null op table");
@@ -1225,6 +1238,7 @@ int amrvac_gpu_upload(amrvac_ctx *c, int reg, int first, int n, const double *w)
     ++c->launches;
   }
   CK(cudaStreamSynchronize(c->stream));
+  c->a2max_set = false;
   return 0;
 }
 
@@ -1283,6 +1297,7 @@ int amrvac_gpu_advect1(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, dou
     return fail(AMRVAC_E_ARG, "bad register");
   if (reg_ct == reg_new) return fail(AMRVAC_E_ARG, "reg_ct and reg_new must differ");
   if (a_base == 0.0 && b_in != 1.0) return fail(AMRVAC_E_ARG, "a_base == 0 requires b_in == 1");
+  if (int r = check_a2max(c)) return r;
   CK(cudaMemcpyAsync(c->d_scal + 0, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
   int r = launch_stage(c, reg_ct, reg_new, reg_base, a_base, b_in, dtfactor);
   CK(cudaStreamSynchronize(c->stream));
@@ -1596,6 +1611,7 @@ int amrvac_gpu_div_points(int n, const double *x, const double *y, double *q, do
 int amrvac_gpu_step_dt(amrvac_ctx *c, double dt) {
   if (int r = check_ctx(c, true)) return r;
   if (!(dt > 0.0)) return fail(AMRVAC_E_ARG, "dt must be positive");
+  if (int r = check_a2max(c)) return r;
   CK(launch_set_scalar(c->d_scal + 0, dt, c->stream));
   ++c->launches;
   return launch_rk(c);

@@ -140,7 +140,11 @@ typedef struct amrvac_cfg {
                                steps), 2 'xy' (src/mod_advance.t:23-45) */
   double schmid_rad[3];     /* schmid limiter radii per direction (default 1) */
   int schmid_global;        /* 1: schmid1, a2max from the domain every setdt
-                               (need_global_a2max) instead of schmid_rad */
+                               (need_global_a2max) instead of schmid_rad; the
+                               getdt phase reduces it, so amrvac_gpu_advect1 /
+                               advect1_dim / step_dt return AMRVAC_E_STATE until
+                               an amrvac_gpu_getdt has run on the current state
+                               (after an upload, set_blocks or regrid) */
 } amrvac_cfg;
 
 typedef struct amrvac_ctx amrvac_ctx;
@@ -226,7 +230,9 @@ int amrvac_gpu_getdt(amrvac_ctx *ctx, int reg, double *dt, double *cmax_global);
 /* One explicit stage (advect1 on all blocks):
  *   w[reg_new] = a_base*w[reg_base] + b_in*w[reg_ct]  (a_base==0: = w[reg_ct])
  *   then finite_volume(qdt=dtfactor*dt) with wCT = w[reg_ct] and sources.
- * Uses cmax_global from the last getdt / set_cmax_global.  Asynchronous. */
+ * Uses cmax_global from the last getdt / set_cmax_global, and with schmid1
+ * the a2max_global of the last getdt (AMRVAC_E_STATE if none has run on the
+ * current state).  Asynchronous. */
 int amrvac_gpu_advect1(amrvac_ctx *ctx, int reg_ct, int reg_new, int reg_base, double a_base,
                        double b_in, double dtfactor, double dt);
 /* The same stage restricted to direction idim (1..ndim; 0: all), as advect1
@@ -310,7 +316,9 @@ int amrvac_gpu_div_points(int n, const double *x, const double *y, double *q, do
  * Scratch: a fixed device array inside the library (1.25 MiB per GPU, held
  * until exit); nblocks above AMRVAC_NOALLOC_MAX_BLOCKS is refused with
  * AMRVAC_E_ARG.  The first call on a device looks up that array's address, so
- * make it before any stream capture.  All calls share the array: calls that
+ * make it before any stream capture; the library keeps that address for the
+ * life of the process, so a cudaDeviceReset on that device invalidates it (do
+ * not call this entry point after one).  All calls share the array: calls that
  * overlap on the GPU race.  Returns AMRVAC_ST_DT_TOO_SMALL if dt < dtmin. */
 #define AMRVAC_NOALLOC_MAX_BLOCKS 32768
 int amrvac_gpu_getdt_noalloc(const amrvac_cfg *cfg, const double *w_dev, int nblocks, const double *dx,

@@ -63,4 +63,8 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("AMRVAC_REFERENCE")
+    if not ref:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <MPI-AMRVAC source root> "
+                 "(or set AMRVAC_REFERENCE)")
+    main(ref)

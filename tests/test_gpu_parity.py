@@ -438,11 +438,13 @@ def test_autotune_leaves_state(oracle_lib):
 RTOL_SCHMID1_MHD3 = 1e-11
 
 
-@pytest.mark.parametrize("kw,tol", [
-    (dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll"), RTOL),
-    (dict(physics="mhd", ndim=3, flux_scheme="hlld", typedivbfix="glm"), RTOL_SCHMID1_MHD3),
-], ids=["hd2_hll", "mhd3_hlld_glm"])
-def test_schmid1_steps_match_oracle(oracle_lib, kw, tol):
+@pytest.mark.parametrize("kw,tol,bc", [
+    (dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll"), RTOL, None),
+    (dict(physics="mhd", ndim=3, flux_scheme="hlld", typedivbfix="glm"), RTOL_SCHMID1_MHD3, None),
+    # physical boundaries: the a2max stencil resolves cont and symm ghosts
+    (dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll"), RTOL, ["cont", "symm", "symm", "cont"]),
+], ids=["hd2_hll", "mhd3_hlld_glm", "hd2_hll_cont_symm"])
+def test_schmid1_steps_match_oracle(oracle_lib, kw, tol, bc):
     """schmid1: the limiter's a2max is a2max_global of every setdt (the
     reference's need_global_a2max reduction, src/mod_dt.t:130, 193-197),
     computed on the device in the getdt phase; three full steps against the
@@ -452,14 +454,15 @@ def test_schmid1_steps_match_oracle(oracle_lib, kw, tol):
     O = oracle_lib
     nd = kw["ndim"]
     n = 32
-    gcfg = make_cfg(limiter="schmid1", **kw)
+    bc = bc or ["periodic"] * (2 * nd)
+    gcfg = make_cfg(limiter="schmid1", typeboundary=bc, **kw)
     assert gcfg.schmid_global == 1 and gcfg.limiter == 10
     ok = dict(kw)
     div = ok.pop("typedivbfix", "none")
     ocfg = O.make_cfg(divb=div, limiter="schmid1", **ok)
     prim = P.random_smooth(kw["physics"], nd, nd, n, seed=P.SEED, glm=div == "glm")
     blocks = P.to_blocks(P.prim_to_cons(prim, kw["physics"], nd, ocfg.gamma), nd)
-    og = O.Grid(ocfg, [n] * nd, [0.0] * nd, [1.0] * nd, ["periodic"] * (2 * nd))
+    og = O.Grid(ocfg, [n] * nd, [0.0] * nd, [1.0] * nd, bc)
     for ib in range(og.nblocks):
         og.set_block(ib, blocks[ib])
     og.getbc()
@@ -476,4 +479,57 @@ def test_schmid1_steps_match_oracle(oracle_lib, kw, tol):
     ref = P.interior(np.array([og.get_block(ib) for ib in range(og.nblocks)]), nd)
     err = _maxrel(got, ref)
     assert err <= tol, f"schmid1: max rel err {err:.3e}"
+    assert ctx.status() == 0
+
+
+def test_schmid1_multilevel_matches_oracle(oracle_lib):
+    """schmid1 on a static two-level 2-D grid: the a2max reduction reads the
+    level-jump ghost values (restricted and prolonged) like the reference's
+    setdt after getbc; three full steps against the oracle's multi-level
+    advance."""
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    from tests import _amr as A
+    O = oracle_lib
+    nd, nb = 2, [8, 8]
+
+    def ref(c, lv):
+        return np.linalg.norm(c - 0.45) < 0.3
+    leaves = A.build_leaves(nd, nb, 2, ref)
+    kw = dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll", courantpar=0.6)
+
+    def field(X, Y, Z):
+        out = np.zeros((4,) + X.shape)
+        s = np.sin(2 * np.pi * X) * np.cos(2 * np.pi * Y)
+        out[0] = 1.0 + 0.3 * s
+        out[1] = 0.5 + 0.2 * np.cos(2 * np.pi * Y)
+        out[2] = -0.3 + 0.2 * np.sin(2 * np.pi * X)
+        out[3] = 1.0 + 0.2 * s
+        return out
+    blocks = A.fill_blocks(leaves, nd, nb, field, "hd", nd, 1.4)
+    ocfg = O.make_cfg(limiter="schmid1", **kw)
+    og = O.AmrGrid(ocfg, nb, [0.0] * nd, [1.0] * nd, leaves)
+    gn = O.AmrGrid(ocfg, nb, [0.0] * nd, [1.0] * nd, leaves)  # one ulp of input noise
+    noisy = one_ulp_noise(np.asarray(blocks))
+    for b in range(len(leaves)):
+        og.set_block(b, blocks[b])
+        gn.set_block(b, noisy[b])
+    og.getbc()
+    gn.getbc()
+    ctx = Context(make_cfg(limiter="schmid1", **kw))
+    ctx.set_amr_grid(leaves, nb, [0.0] * nd, [1.0] * nd)
+    ctx.upload(blocks)
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    for _ in range(3):
+        dt, cm = og.getdt()
+        ctx.step()
+        assert abs(ctx.get_time()[0] - dt) <= 1e-13 * dt
+        og.advance(dt, cm)
+        gn.advance(dt, cm)
+    sl = (slice(None), slice(None), slice(None), slice(2, 18), slice(2, 18))
+    got = ctx.download()[sl]
+    ref_ = np.array([og.get_block(b) for b in range(len(leaves))])[sl]
+    noise = _maxrel(np.array([gn.get_block(b) for b in range(len(leaves))])[sl], ref_)
+    err = _maxrel(got, ref_)
+    assert err <= max(RTOL, noise), f"schmid1 multi-level: {err:.3e} (oracle self-noise {noise:.3e})"
     assert ctx.status() == 0

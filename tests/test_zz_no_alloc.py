@@ -4,9 +4,9 @@ The no-allocation entry point serves host codes that may not call cudaMalloc
 themselves (their device memory belongs to another runtime, such as OpenACC
 data regions or a framework's caching allocator), so they cannot create a
 context.  It must give the same dt and cmax_global as the context's getdt on
-the same blocks.  Two calls in a row on different block sets check that
-nothing from the previous call's scratch leaks into the next.  This file is
-named to be collected last.
+the same blocks, and the oracle's getdt_courant on the same state.  Two
+calls in a row on different block sets check that nothing from the previous
+call's scratch leaks into the next.  This file is named to be collected last.
 """
 import ctypes
 
@@ -47,11 +47,28 @@ def _context(kw, n, seed, amp):
     ctx = Context(cfg)
     lo, hi = [0.0] * ndim, [1.0 + 0.25 * d for d in range(ndim)]
     ctx.set_uniform_grid([n] * ndim, lo, hi)
-    ctx.upload(P.to_blocks(cons, ndim))
+    blocks = P.to_blocks(cons, ndim)
+    ctx.upload(blocks)
     dx = np.zeros((ctx.nblocks, 3))
     for d in range(ndim):
         dx[:, d] = (hi[d] - lo[d]) / n
+    ctx.case = (kw, n, lo, hi, blocks)
     return cfg, ctx, dx
+
+
+def _oracle_getdt(O, ctx):
+    """getdt_courant of the oracle (src/mod_dt.t:160-287) on the same blocks."""
+    kw, n, lo, hi, blocks = ctx.case
+    k = dict(kw)
+    div = k.pop("typedivbfix", "none")
+    tc = {"maxsum": 1, "summax": 2, "minimum": 3}[k.pop("typecourant", "maxsum")]
+    c = O.make_cfg(divb=div, type_courant=tc, **k)
+    nd = kw["ndim"]
+    g = O.Grid(c, [n] * nd, lo, hi, ["periodic"] * (2 * nd))
+    for ib in range(g.nblocks):
+        g.set_block(ib, blocks[ib])
+    g.getbc()
+    return g.getdt()
 
 
 def _noalloc(cfg, ctx, dx, stream):
@@ -71,7 +88,7 @@ def _close(a, b):
 
 
 @pytest.mark.parametrize("name,kw,n,seed", CASES, ids=[c[0] for c in CASES])
-def test_noalloc_getdt_matches_context_getdt_twice(name, kw, n, seed):
+def test_noalloc_getdt_matches_context_getdt_twice(oracle_lib, name, kw, n, seed):
     _cuda()
     # first a larger block set, then a smaller one on the same domain (coarser
     # cells, so smaller courant numbers): stale per-block partials left by the
@@ -84,6 +101,8 @@ def test_noalloc_getdt_matches_context_getdt_twice(name, kw, n, seed):
         dt, cm, st = _noalloc(cfg, ctx, dx, stream)
         assert _close(dt, dt_ref) and _close(cm, cm_ref), (name, dt, dt_ref, cm, cm_ref)
         assert st == st_ref
+        dt_o, cm_o = _oracle_getdt(oracle_lib, ctx)
+        assert _close(dt, dt_o) and _close(cm, cm_o), (name, "oracle", dt, dt_o, cm, cm_o)
         assert 0.0 < dt < 1.0e99
 
 
