@@ -194,11 +194,13 @@ class Tree:
         return True
 
 
-def coarsen_average(children, ndim, ng=2, bn=16):
+def coarsen_average(children, ndim, ng=2, bn=None):
     """Parent block (ghosted, ghost cells zero) from its 2^d children
     (ghosted), child bits x fastest: the average of every 2^d fine cells
-    (coarsen_grid on conserved variables), summed x fastest."""
+    (coarsen_grid on conserved variables), summed x fastest.  bn: cells per
+    block edge (default: from the children's shape)."""
     nw = children[0].shape[0]
+    bn = children[0].shape[-1] - 2 * ng if bn is None else bn
     g = [bn + 2 * ng if d < ndim else 1 for d in range(3)]
     out = np.zeros((nw, g[2], g[1], g[0]))
     h = bn // 2

@@ -41,7 +41,8 @@ class Context:
         self.h = h
         self.nblocks = 0
         ng = cfg.nghostcells
-        self.ghosted = tuple([16 + 2 * ng if d < cfg.ndim else 1 for d in (2, 1, 0)])
+        self.bn = int(cfg.block_nx[0])  # cells per block edge
+        self.ghosted = tuple([self.bn + 2 * ng if d < cfg.ndim else 1 for d in (2, 1, 0)])
         self.block_shape = (self.nw,) + self.ghosted
 
     def close(self):

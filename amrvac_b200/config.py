@@ -108,13 +108,14 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
              small_pressure=0.0, time_stepper="threestep", ssprk_order=3, dtmin=1.0e-10,
              typeboundary=None, zchunk=0, precision="fp64", slowsteps=-1,
              time_integrator="default", nghostcells=None, dimsplit=False,
-             typedimsplit="xyyx", schmid_rad=(1.0, 1.0, 1.0)) -> _lib.AmrvacCfg:
+             typedimsplit="xyyx", schmid_rad=(1.0, 1.0, 1.0), block_nx=16) -> _lib.AmrvacCfg:
     """Build an ``amrvac_cfg`` from reference-style parameter names.
 
     typeboundary: list of 2*ndim entries (min1, max1, min2, ...), each a name
     applied to all variables or a list of per-variable names.  nghostcells
     defaults to 3 for the fifth-order reconstructions (mp5, weno5, wenoz5,
-    wenozp5: they need them) and 2 otherwise.
+    wenozp5: they need them) and 2 otherwise.  block_nx: cells per block
+    edge, the same in every direction (the library runs 8, 10, 12, 16, 32).
     """
     L = _lib.load()
     c = _lib.AmrvacCfg()
@@ -123,7 +124,7 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
     c.ndir = ndim if ndir is None else ndir
     c.physics = 1 if physics == "mhd" else 0
     for d in range(3):
-        c.block_nx[d] = 16
+        c.block_nx[d] = int(block_nx)
     c.gamma = (5.0 / 3.0) if gamma is None else float(gamma)
     c.flux_scheme = _lib.FS[flux_scheme]
     c.limiter = _lib.LIMITER[limiter]
@@ -182,10 +183,12 @@ def config_from_par(paths) -> RunConfig:
     plist = nl.get("mhd_list" if physics == "mhd" else "hd_list", {})
     ndim = 1 + sum(1 for k in ("domain_nx2", "domain_nx3") if k in mesh)
     domain_nx = [int(mesh.get(f"domain_nx{d + 1}", 32)) for d in range(ndim)]
-    for d in range(ndim):
-        bnx = int(mesh.get(f"block_nx{d + 1}", 16))
-        if bnx != 16:
-            raise ValueError("block_nx must be 16 for the B200 path")
+    # block_nx1..3 (default 16, src/io/mod_input_output.t:301); the library
+    # needs the same edge in every direction
+    bnxs = [int(mesh.get(f"block_nx{d + 1}", 16)) for d in range(ndim)]
+    if len(set(bnxs)) != 1:
+        raise ValueError("block_nx must be the same in every direction for the B200 path")
+    bnx = bnxs[0]
     tb = []
     for d in range(ndim):
         for side in ("min", "max"):
@@ -224,6 +227,7 @@ def config_from_par(paths) -> RunConfig:
         dimsplit=bool(meth.get("dimsplit", False)),
         schmid_rad=tuple(float(meth.get(f"schmid_rad{d + 1}", 1.0)) for d in range(3)),
         typedimsplit=meth.get("typedimsplit", "xyyx"),
+        block_nx=bnx,
     )
     if physics == "mhd":
         cfg_kw.update(typedivbfix=plist.get("typedivbfix", "linde"),

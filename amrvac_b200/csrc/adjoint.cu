@@ -39,7 +39,7 @@ constexpr int ADJ_THREADS = 320;
 constexpr int WP = 22;            // primitive tile edge: 16 + 2*3
 constexpr int LMW = 20;           // lambda tile edge: 16 + 2*2
 constexpr int NF = 19;            // faces -1..17 per row and direction
-constexpr int NFACE = NF * BN;    // 304
+constexpr int NFACE = NF * BN16;    // 304
 constexpr int SM_WP = 4 * WP * WP;
 constexpr int SM_LM = 4 * LMW * LMW;
 constexpr int SM_G = 16 * NFACE;  // [slot][var][face]
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, AMRVAC_ADJ_MINB) adj_stage_kernel
     } else {
       const int q = p - 22 * 16, r = q >> 4;
       y = r < 3 ? r - 3 : r + 13;
-      x = q & (BN - 1);
+      x = q & (BN16 - 1);
     }
     double w[4];
     load_prim<false, 2, false, 2>(S, b, x, y, 0, w);
@@ -350,10 +350,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, AMRVAC_ADJ_MINB) adj_stage_kernel
     } else {
       const int q = p - 20 * 16, r = q >> 4;
       y = r < 2 ? r - 2 : r + 14;
-      x = q & (BN - 1);
+      x = q & (BN16 - 1);
     }
-    const bool phys = (x < 0 && phys_lo[0]) || (x >= BN && phys_hi[0]) || (y < 0 && phys_lo[1]) ||
-                      (y >= BN && phys_hi[1]);
+    const bool phys = (x < 0 && phys_lo[0]) || (x >= BN16 && phys_hi[0]) || (y < 0 && phys_lo[1]) ||
+                      (y >= BN16 && phys_hi[1]);
     double l[4] = {0.0, 0.0, 0.0, 0.0};
     if (!phys) {
       int i = x, j = y, k = 0;
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, AMRVAC_ADJ_MINB) adj_stage_kernel
   for (int D = 0; D < 2; ++D) {
     if (t < NFACE) {
       const int row = t / NF, fi = t - row * NF - 1;
-      const bool valid = !((fi == -1 && phys_lo[D]) || (fi == BN + 1 && phys_hi[D]));
+      const bool valid = !((fi == -1 && phys_lo[D]) || (fi == BN16 + 1 && phys_hi[D]));
       double gq[4][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
       if (valid) {
         double mu[4];
@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, AMRVAC_ADJ_MINB) adj_stage_kernel
         // faces next to a block edge are computed by two or three blocks: the
         // gamma term counts once, in the block of the cell right of the face
         // (and face 16 at a physical high side)
-        if ((fi >= 0 && fi < BN) || (fi == BN && phys_hi[D])) gg += gface;
+        if ((fi >= 0 && fi < BN16) || (fi == BN16 && phys_hi[D])) gg += gface;
       }
 #pragma unroll
       for (int o = 0; o < 4; ++o)
@@ -396,8 +396,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, AMRVAC_ADJ_MINB) adj_stage_kernel
         for (int v = 0; v < 4; ++v) G[(o * 4 + orig_index_rt<false, 2>(v, D)) * NFACE + t] = gq[o][v];
     }
     __syncthreads();
-    if (t < BN * BN) {
-      const int ci = t & (BN - 1), cj = t >> 4;
+    if (t < BN16 * BN16) {
+      const int ci = t & (BN16 - 1), cj = t >> 4;
       const int c = D == 0 ? ci : cj, row = D == 0 ? cj : ci;
       const int base = row * NF;  // face f is entry base + f + 1
 #pragma unroll
@@ -408,15 +408,15 @@ __global__ void __launch_bounds__(ADJ_THREADS, AMRVAC_ADJ_MINB) adj_stage_kernel
         double sum = g0[base + c + 3] + g1[base + c + 2] + g2[base + c + 1] + g3[base + c];
         if (c == 0 && phys_lo[D])       // ghosts -2, -1 copy cell 0
           sum += g0[base + 1] + g1[base + 1] + g0[base + 2];
-        if (c == BN - 1 && phys_hi[D])  // ghosts 16, 17 copy cell 15
-          sum += g2[base + BN + 1] + g3[base + BN + 1] + g3[base + BN];
+        if (c == BN16 - 1 && phys_hi[D])  // ghosts 16, 17 copy cell 15
+          sum += g2[base + BN16 + 1] + g3[base + BN16 + 1] + g3[base + BN16];
         gp[v] += sum;
       }
     }
     __syncthreads();
   }
-  if (t < BN * BN) {
-    const int ci = t & (BN - 1), cj = t >> 4;
+  if (t < BN16 * BN16) {
+    const int ci = t & (BN16 - 1), cj = t >> 4;
     double w[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) w[v] = S.uin[cell_offset<2>(b, 4, v, ci, cj, 0)];

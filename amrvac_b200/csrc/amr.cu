@@ -26,26 +26,26 @@ template <int NDIM>
 __global__ void __launch_bounds__(256) lohner_kernel(const LohnerArgs A) {
   const int b = blockIdx.x;
   const int t = threadIdx.x;
-  const int i = t & (BN - 1), j = NDIM >= 2 ? t >> 4 : 0;
   const StageArgs &S = A.sa;
+  const int bn = S.bn;
   const int nw = A.nw;
   const int lev = A.level[b];
   const double wf = A.wavefilter[lev - 1], thr = A.threshold[lev - 1], der = A.derefine[lev - 1];
   auto wv = [&](int iw, int x, int y, int z) -> double {
     int ii = x, jj = y, kk = z;
     uint32_t flip;
-    const int blk = resolve_cell<NDIM>(S, b, ii, jj, kk, flip);
+    const int blk = resolve_cell<NDIM>(S, b, ii, jj, kk, flip, bn);
     // a level jump (blk <= -2) reads the ghost buffer the ghost pass filled
-    double v = blk >= 0 ? S.uin[cell_offset<NDIM>(blk, nw, iw, ii, jj, kk)]
-                        : S.gbuf[ghost_offset<NDIM>(-2 - blk, nw, iw, ii, jj, kk)];
+    double v = blk >= 0 ? S.uin[cell_offset<NDIM>(blk, nw, iw, ii, jj, kk, bn)]
+                        : S.gbuf[ghost_offset<NDIM>(-2 - blk, nw, iw, ii, jj, kk, bn)];
     if ((flip >> iw) & 1u) v = -v;
     return ((A.logflag >> iw) & 1u) ? log10(v) : v;
   };
   bool any_ref = false, all_coa = true;
   double emax = 0.0;
-  const bool active = t < (NDIM >= 2 ? BN * BN : BN);
-  const int nz = NDIM == 3 ? BN : 1;
-  for (int k = 0; k < nz && active; ++k) {
+  const int ncell = bn * (NDIM >= 2 ? bn : 1) * (NDIM == 3 ? bn : 1);
+  for (int cell = t; cell < ncell; cell += 256) {  // the block's cells, x fastest
+    const int i = cell % bn, j = NDIM >= 2 ? (cell / bn) % bn : 0, k = NDIM == 3 ? cell / (bn * bn) : 0;
     double err = 0.0;
     for (int iw = 0; iw < nw; ++iw) {
       const double wt = A.weight[iw];
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(256) lohner_kernel(const LohnerArgs A) {
   // block reduction
   __shared__ double red[8];
   const int r_any = __syncthreads_or(any_ref);
-  const int r_all = __syncthreads_and(active ? all_coa : true);
+  const int r_all = __syncthreads_and(all_coa);
   double m = emax;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -125,10 +125,11 @@ __device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int
   const int P[3] = {P0, P1, P2};
   int jg[3] = {0, 0, 0}, loc[3] = {0, 0, 0};
   uint32_t flip = 0;
+  const int bn = A.bn, half = bn / 2;
 #pragma unroll
   for (int d = 0; d < NDIM; ++d) {
-    const int n = A.nlev[L][d] * BN;
-    int p = P[d];  // within 4 cells of the block and n >= 16: one wrap or mirror
+    const int n = A.nlev[L][d] * bn;
+    int p = P[d];  // within 4 cells of the block and n >= 4: one wrap or mirror
     if (p < 0 || p >= n) {
       // across the domain boundary: the boundary rule at this level, as the
       // coarse neighbour's own physical ghost cells hold it (bc_phys)
@@ -143,24 +144,24 @@ __device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int
         flip ^= A.bc_flip[2 * d + side];
       }
     }
-    jg[d] = p >> 4;
-    loc[d] = p & (BN - 1);
+    jg[d] = p / bn;
+    loc[d] = p - jg[d] * bn;
   }
   const double sg = ((flip >> v) & 1u) ? -1.0 : 1.0;
   const int o = A.owner[A.owner_off[L] + jg[0] + A.nlev[L][0] * (jg[1] + A.nlev[L][1] * jg[2])];
-  if (o >= 0) return sg * A.u[cell_offset<NDIM>(o, A.nw, v, loc[0], loc[1], loc[2])];
+  if (o >= 0) return sg * A.u[cell_offset<NDIM>(o, A.nw, v, loc[0], loc[1], loc[2], bn)];
   if (o == -2 && L < A.maxlevel) {
     int jf[3] = {0, 0, 0}, f[3] = {0, 0, 0};
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) {
-      const int c = loc[d] >> 3;
+      const int c = loc[d] >= half;
       jf[d] = 2 * jg[d] + c;
-      f[d] = 2 * (loc[d] - 8 * c);
+      f[d] = 2 * (loc[d] - half * c);
     }
     const int o2 = A.owner[A.owner_off[L + 1] + jf[0] + A.nlev[L + 1][0] * (jf[1] + A.nlev[L + 1][1] * jf[2])];
     if (o2 >= 0) {
-      const double *w = A.u + cell_offset<NDIM>(o2, A.nw, v, f[0], f[1], f[2]);
-      constexpr int SY = BN, SZ = BN * BN;
+      const double *w = A.u + cell_offset<NDIM>(o2, A.nw, v, f[0], f[1], f[2], bn);
+      const int SY = bn, SZ = bn * bn;
       double sum = w[0];  // x fastest, left to right
       sum = sum + w[1];
       if constexpr (NDIM > 1) {
@@ -187,8 +188,9 @@ __device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int
 // where some prolongation stencil reads it.
 template <int NDIM>
 __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
-  extern __shared__ double psc[];  // 12^NDIM coarse representation of variable blockIdx.y
-  constexpr int C = BN / 2 + 4, CY = NDIM >= 2 ? C : 1, CZ = NDIM >= 3 ? C : 1;
+  extern __shared__ double psc[];  // (bn/2+4)^NDIM coarse representation of variable blockIdx.y
+  const int bn = A.bn;
+  const int C = bn / 2 + 4, CY = NDIM >= 2 ? C : 1, CZ = NDIM >= 3 ? C : 1;
   __shared__ int s_off[28];        // prefix sums of the jump regions' cell counts
   __shared__ int s_q[27], s_kind[27];
   __shared__ int s_nreg;
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
       if (q == 13 || (kind != AMR_COARSE && kind != AMR_FINE)) continue;
       const int dd[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
       int cells = 1;
-      for (int d = 0; d < NDIM; ++d) cells *= dd[d] ? 2 : BN;
+      for (int d = 0; d < NDIM; ++d) cells *= dd[d] ? 2 : bn;
       if (kind == AMR_COARSE) cm |= 1u << q;
       s_q[m] = q;
       s_kind[m] = kind;
@@ -230,7 +232,7 @@ __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
       const int pc[3] = {p % C, NDIM >= 2 ? (p / C) % CY : 0, NDIM >= 3 ? p / (C * CY) : 0};
       // read by the stencils (centre +- 1 per direction) of the ghost cells
       // of a coarser-neighbour direction: coarse index 1 for the low ghosts,
-      // 2..9 beside the block, 10 for the high ghosts
+      // 2..bn/2+1 beside the block, bn/2+2 for the high ghosts
       // (bit q of kDirBits[d][k + 1]: component d of direction q is k)
       constexpr uint32_t kDirBits[3][3] = {{0x1249249u, 0x2492492u, 0x4924924u},
                                            {0x01c0e07u, 0x0e07038u, 0x70381c0u},
@@ -241,8 +243,8 @@ __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
         uint32_t md = 0;
         if (d < NDIM) {
           if (pc[d] <= 2) md |= kDirBits[d][0];
-          if (pc[d] >= 1 && pc[d] <= BN / 2 + 2) md |= kDirBits[d][1];
-          if (pc[d] >= BN / 2 + 1) md |= kDirBits[d][2];
+          if (pc[d] >= 1 && pc[d] <= bn / 2 + 2) md |= kDirBits[d][1];
+          if (pc[d] >= bn / 2 + 1) md |= kDirBits[d][2];
         } else {
           md = kDirBits[d][1];
         }
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
       if (!m) continue;
       int P[3] = {0, 0, 0};
 #pragma unroll
-      for (int d = 0; d < NDIM; ++d) P[d] = igb[d] * (BN / 2) + pc[d] - 2;
+      for (int d = 0; d < NDIM; ++d) P[d] = igb[d] * (bn / 2) + pc[d] - 2;
       psc[p] = coarse_value<NDIM>(A, L - 1, P[0], P[1], P[2], v);
     }
     __syncthreads();
@@ -278,13 +280,13 @@ __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
     const int q = s_q[lo], kind = s_kind[lo];
     const int dd[3] = {q % 3 - 1, (q / 3) % 3 - 1, q / 9 - 1};
     int li = e - s_off[lo];
-    int gc[3] = {0, 0, 0};  // ghosted index 0..19
+    int gc[3] = {0, 0, 0};  // ghosted index 0..bn+3
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) {
-      const int ext = dd[d] ? 2 : BN;
-      const int l = li & (ext - 1);
-      li = dd[d] ? li >> 1 : li >> 4;
-      gc[d] = dd[d] < 0 ? l : (dd[d] > 0 ? BN + 2 + l : 2 + l);
+      const int ext = dd[d] ? 2 : bn;
+      const int l = li % ext;
+      li /= ext;
+      gc[d] = dd[d] < 0 ? l : (dd[d] > 0 ? bn + 2 + l : 2 + l);
     }
     double val;
     if (kind == AMR_COARSE) {  // prolongation (interpolation_linear)
@@ -316,10 +318,10 @@ __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
     } else {  // restriction
       int P[3] = {0, 0, 0};
 #pragma unroll
-      for (int d = 0; d < NDIM; ++d) P[d] = igb[d] * BN + gc[d] - 2;
+      for (int d = 0; d < NDIM; ++d) P[d] = igb[d] * bn + gc[d] - 2;
       val = coarse_value<NDIM>(A, L, P[0], P[1], P[2], v);
     }
-    A.gbuf[ghost_offset<NDIM>(slot, A.nw, v, gc[0] - 2, gc[1] - 2, gc[2] - 2)] = val;
+    A.gbuf[ghost_offset<NDIM>(slot, A.nw, v, gc[0] - 2, gc[1] - 2, gc[2] - 2, bn)] = val;
   }
 }
 
@@ -334,6 +336,7 @@ __global__ void __launch_bounds__(256) amr_fix_kernel(const AmrFixArgs A) {
   const int t = threadIdx.x;
   const double cofi = 1.0 / double(1 << NDIM);
   const int dsel = sweep_dir(A.sweep, A.split_xy, A.scal, NDIM);
+  const int BN = A.bn;
   for (int d = 0; d < NDIM; ++d)
     for (int side = 0; side < 2; ++side) {
       if (dsel >= 0 && d != dsel) continue;
@@ -371,7 +374,7 @@ __global__ void __launch_bounds__(256) amr_fix_kernel(const AmrFixArgs A) {
             first = false;
           }
         const double pf = side ? sum : -sum;  // the fine block's side 1 - side
-        double &w = A.w[cell_offset<NDIM>(b, A.nw, v, c[0], c[1], c[2])];
+        double &w = A.w[cell_offset<NDIM>(b, A.nw, v, c[0], c[1], c[2], BN)];
         w = w - pc;
         w = w + pf * cofi;
       }
@@ -390,17 +393,18 @@ __global__ void __launch_bounds__(256) amr_fix_kernel(const AmrFixArgs A) {
 // 2^d fine cells, x fastest.
 template <int NDIM>
 __global__ void __launch_bounds__(256) amr_remap_kernel(const AmrRemapArgs A) {
-  constexpr int NY = NDIM >= 2 ? BN : 1, NZ = NDIM >= 3 ? BN : 1, NC = BN * NY * NZ;
+  const StageArgs &S = A.old;
+  const int BN = S.bn, half = BN / 2;
+  const int NY = NDIM >= 2 ? BN : 1, NZ = NDIM >= 3 ? BN : 1, NC = BN * NY * NZ;
   const int nb = blockIdx.x;
   const int *op = A.op + 9 * nb;
   const int kind = op[0];
-  const StageArgs &S = A.old;
   for (int e = threadIdx.x; e < A.nw * NC; e += blockDim.x) {
     const int v = e / NC, cell = e - v * NC;
-    const int i = cell & (BN - 1), j = NDIM >= 2 ? (cell >> 4) & (BN - 1) : 0, k = NDIM >= 3 ? cell >> 8 : 0;
+    const int i = cell % BN, j = NDIM >= 2 ? (cell / BN) % BN : 0, k = NDIM >= 3 ? cell / (BN * BN) : 0;
     double val;
     if (kind == 0) {
-      val = S.uin[cell_offset<NDIM>(op[1], A.nw, v, i, j, k)];
+      val = S.uin[cell_offset<NDIM>(op[1], A.nw, v, i, j, k, BN)];
     } else if (kind == 1) {
       const int p = op[1], cb = op[2];
       const int co[3] = {(BN / 2) * (cb & 1) + (i >> 1), NDIM >= 2 ? (BN / 2) * ((cb >> 1) & 1) + (j >> 1) : 0,
@@ -408,9 +412,9 @@ __global__ void __launch_bounds__(256) amr_remap_kernel(const AmrRemapArgs A) {
       auto wco = [&](int di, int dj, int dk) -> double {
         int ii = co[0] + di, jj = co[1] + dj, kk = co[2] + dk;
         uint32_t flip;
-        const int blk = resolve_cell<NDIM>(S, p, ii, jj, kk, flip);
-        const double x = blk >= 0 ? S.uin[cell_offset<NDIM>(blk, A.nw, v, ii, jj, kk)]
-                                  : S.gbuf[ghost_offset<NDIM>(-2 - blk, A.nw, v, ii, jj, kk)];
+        const int blk = resolve_cell<NDIM>(S, p, ii, jj, kk, flip, BN);
+        const double x = blk >= 0 ? S.uin[cell_offset<NDIM>(blk, A.nw, v, ii, jj, kk, BN)]
+                                  : S.gbuf[ghost_offset<NDIM>(-2 - blk, A.nw, v, ii, jj, kk, BN)];
         return ((flip >> v) & 1u) ? -x : x;
       };
       const double c0 = wco(0, 0, 0);
@@ -429,9 +433,11 @@ __global__ void __launch_bounds__(256) amr_remap_kernel(const AmrRemapArgs A) {
 #pragma unroll
       for (int d = 0; d < NDIM; ++d) val = val + slope[d] * (0.5 * (double(f[d]) - 0.5));
     } else {
-      const int cbit = (i >> 3) | (NDIM >= 2 ? ((j >> 3) << 1) : 0) | (NDIM >= 3 ? ((k >> 3) << 2) : 0);
-      const double *w = S.uin + cell_offset<NDIM>(op[1 + cbit], A.nw, v, 2 * (i & 7), NDIM >= 2 ? 2 * (j & 7) : 0,
-                                                  NDIM >= 3 ? 2 * (k & 7) : 0);
+      const int ci = i >= half, cj = j >= half, ck = k >= half;
+      const int cbit = ci | (NDIM >= 2 ? cj << 1 : 0) | (NDIM >= 3 ? ck << 2 : 0);
+      const double *w = S.uin + cell_offset<NDIM>(op[1 + cbit], A.nw, v, 2 * (i - half * ci),
+                                                  NDIM >= 2 ? 2 * (j - half * cj) : 0,
+                                                  NDIM >= 3 ? 2 * (k - half * ck) : 0, BN);
       double sum = w[0];
       sum = sum + w[1];
       if constexpr (NDIM > 1) {
@@ -446,7 +452,7 @@ __global__ void __launch_bounds__(256) amr_remap_kernel(const AmrRemapArgs A) {
       }
       val = sum * (1.0 / double(1 << NDIM));
     }
-    A.unew[cell_offset<NDIM>(nb, A.nw, v, i, j, k)] = val;
+    A.unew[cell_offset<NDIM>(nb, A.nw, v, i, j, k, BN)] = val;
   }
 }
 
@@ -460,8 +466,9 @@ cudaError_t launch_amr_remap(const AmrRemapArgs &A, int nnew, int ndim, cudaStre
 cudaError_t launch_amr_ghosts(const AmrGhostArgs &A, int nslots, int ndim, cudaStream_t s) {
   if (nslots <= 0) return cudaSuccess;
   const dim3 grid(nslots, A.nw);
-  if (ndim == 2) amr_ghost_kernel<2><<<grid, 256, sizeof(double) * 12 * 12, s>>>(A);
-  else amr_ghost_kernel<3><<<grid, 256, sizeof(double) * 12 * 12 * 12, s>>>(A);
+  const size_t c = (size_t)A.bn / 2 + 4;  // psc edge
+  if (ndim == 2) amr_ghost_kernel<2><<<grid, 256, sizeof(double) * c * c, s>>>(A);
+  else amr_ghost_kernel<3><<<grid, 256, sizeof(double) * c * c * c, s>>>(A);
   return cudaGetLastError();
 }
 

@@ -43,6 +43,7 @@ struct AmrGhostArgs {
   int owner_off[AMR_MAX_LEVELS + 2];
   int nlev[AMR_MAX_LEVELS + 2][3];  // blocks per direction per level
   int maxlevel;
+  int bn;                   // block edge
   int bc_kind[6];           // BCK_* per side (periodic sides wrap)
   uint32_t bc_flip[6];      // per side, bit v: variable v changes sign (asymm)
   uint32_t *status;
@@ -50,8 +51,9 @@ struct AmrGhostArgs {
 
 struct AmrFixArgs {
   double *w;                // the stage's output register
-  const double *pflux;      // [slot][2*ndim][var][16*16]
+  const double *pflux;      // [slot][2*ndim][var][bn*bn]
   int nw;
+  int bn;                   // block edge
   const int *iblocks, *gslot, *ntype, *child;  // child[(b*27+q)*8 + cbits]
   // dimensional splitting: only the sweep's direction (fix_conserve with
   // idim^LIM = idim, idim); sweep < 0: all directions
@@ -71,6 +73,7 @@ struct AmrRemapArgs {
 };
 
 cudaError_t launch_amr_ghosts(const AmrGhostArgs &A, int nslots, int ndim, cudaStream_t s);
+// (the remap and Löhner kernels read the block edge from their StageArgs)
 cudaError_t launch_amr_remap(const AmrRemapArgs &A, int nnew, int ndim, cudaStream_t s);
 cudaError_t launch_amr_fix(const AmrFixArgs &A, int nslots, int ndim, cudaStream_t s);
 

@@ -10,7 +10,7 @@ namespace amrvac {
 // ---------------------------------------------------------------- upload
 // Fortran w(ixG^S,1:nw) blocks (ghosts included) -> pool interior.
 __global__ void unpack_kernel(const double *__restrict__ src, double *__restrict__ pool, int first,
-                              int n, int nw, int ndim, int ng) {
+                              int n, int nw, int ndim, int ng, int BN) {
   const int nx = BN, ny = ndim >= 2 ? BN : 1, nz = ndim >= 3 ? BN : 1;
   const int gx = BN + 2 * ng, gy = ndim >= 2 ? BN + 2 * ng : 1, gz = ndim >= 3 ? BN + 2 * ng : 1;
   const size_t per_block = (size_t)nx * ny * nz;
@@ -35,7 +35,7 @@ __global__ void unpack_kernel(const double *__restrict__ src, double *__restrict
 // 150-162, 812-852) and physical cont/symm/asymm boundaries
 // (src/mod_boundary_conditions.t:12-265, applied per dimension).
 __global__ void pack_kernel(const double *__restrict__ pool, double *__restrict__ dst, int first, int n,
-                            int nw, int ndim, int ng, const int *__restrict__ nbr, SrlMaps maps,
+                            int nw, int ndim, int ng, int BN, const int *__restrict__ nbr, SrlMaps maps,
                             BcSpec bc, const double *__restrict__ gbuf) {
   const int gx = BN + 2 * ng, gy = ndim >= 2 ? BN + 2 * ng : 1, gz = ndim >= 3 ? BN + 2 * ng : 1;
   const size_t per_block_g = (size_t)gx * gy * gz;
@@ -208,14 +208,14 @@ cudaError_t launch_div_points(int n, const double *x, const double *y, double *q
   return cudaGetLastError();
 }
 
-cudaError_t launch_unpack(const double *src, double *pool, int first, int n, int nw, int ndim, int ng,
+cudaError_t launch_unpack(const double *src, double *pool, int first, int n, int nw, int ndim, int ng, int bn,
                           cudaStream_t s) {
-  unpack_kernel<<<592, 256, 0, s>>>(src, pool, first, n, nw, ndim, ng);
+  unpack_kernel<<<592, 256, 0, s>>>(src, pool, first, n, nw, ndim, ng, bn);
   return cudaGetLastError();
 }
-cudaError_t launch_pack(const double *pool, double *dst, int first, int n, int nw, int ndim, int ng,
+cudaError_t launch_pack(const double *pool, double *dst, int first, int n, int nw, int ndim, int ng, int bn,
                         const int *nbr, const SrlMaps &maps, const BcSpec &bc, const double *gbuf, cudaStream_t s) {
-  pack_kernel<<<592, 256, 0, s>>>(pool, dst, first, n, nw, ndim, ng, nbr, maps, bc, gbuf);
+  pack_kernel<<<592, 256, 0, s>>>(pool, dst, first, n, nw, ndim, ng, bn, nbr, maps, bc, gbuf);
   return cudaGetLastError();
 }
 // rk4 combination (src/mod_advance.t:497-502): ps = (1/3)(-ps + ps1 + 2 ps2 + ps3),

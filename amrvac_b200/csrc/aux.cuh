@@ -25,9 +25,9 @@ cudaError_t measure_fp64_peak(double *tflops);
 // rcp_ / div_ / rcp_seed of the stage kernels on n device points (test entry).
 cudaError_t launch_div_points(int n, const double *x, const double *y, double *q, double *r, double *seed,
                               cudaStream_t s);
-cudaError_t launch_unpack(const double *src, double *pool, int first, int n, int nw, int ndim, int ng,
+cudaError_t launch_unpack(const double *src, double *pool, int first, int n, int nw, int ndim, int ng, int bn,
                           cudaStream_t s);
-cudaError_t launch_pack(const double *pool, double *dst, int first, int n, int nw, int ndim, int ng,
+cudaError_t launch_pack(const double *pool, double *dst, int first, int n, int nw, int ndim, int ng, int bn,
                         const int *nbr, const SrlMaps &maps, const BcSpec &bc, const double *gbuf, cudaStream_t s);
 cudaError_t launch_setdt_finalize(unsigned long long *red, double *scal, uint32_t *status, cudaStream_t s);
 cudaError_t launch_advance_time(double *scal, cudaStream_t s);

@@ -69,7 +69,8 @@ struct amrvac_ctx {
   SrlMaps maps;
   cudaStream_t stream = nullptr;
   int nblocks = 0;
-  size_t per_block = 0;  // doubles per block per variable
+  int bn = 16;           // block edge (block_nx)
+  size_t per_block = 0;  // doubles per block per variable (bn^ndim)
   double *pool[4] = {nullptr, nullptr, nullptr, nullptr};  // ps, ps1, ps2 (+ ps3 for rk4)
   int nreg = 3;                          // registers allocated
   int *d_nbr = nullptr;
@@ -123,8 +124,8 @@ struct AmrDev {
   int nslots = 0;
   int *d_int = nullptr;       // iblocks, gslot, face, ntype, level, ig, child, owner
   double *d_bxmin = nullptr;  // [nblocks*3]
-  double *gbuf = nullptr;     // [slot][var][20^d]
-  double *pflux = nullptr;    // [slot][2*ndim][var][256]
+  double *gbuf = nullptr;     // [slot][var][(bn+4)^d]
+  double *pflux = nullptr;    // [slot][2*ndim][var][bn*bn]
   AmrGhostArgs G;
   AmrFixArgs F;
   int *d_face = nullptr, *d_gslot = nullptr;
@@ -175,6 +176,7 @@ StageArgs stage_args(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, doubl
   A.P = c->P;
   A.sweep = c->sweep;
   A.split_xy = c->fixed_dir || c->cfg.dimsplit == 2;
+  A.bn = c->bn;
   if (c->amr) {
     A.gbuf = c->amr->gbuf;
     A.pflux = c->amr->pflux;
@@ -204,9 +206,11 @@ int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a,
   if (c->amr)
     if (int r = launch_amr_ghost_pass(c, reg_ct)) return r;
   StageArgs A = stage_args(c, reg_ct, reg_new, reg_base, a, b, dtfactor);
-  const long planes = (long)c->nblocks * (c->cfg.ndim == 3 ? 16 : 1);
+  // tile-planes: tiles per block plane x z-planes (3-D)
+  const int bn = c->bn, ntile = (bn / tile_edge(bn)) * (bn / tile_edge(bn));
+  const long planes = (long)c->nblocks * ntile * (c->cfg.ndim == 3 ? bn : 1);
   int nctas;
-  if (c->zchunk > 0) nctas = c->cfg.ndim == 3 ? c->nblocks * (16 / c->zchunk) : c->nblocks;
+  if (c->zchunk > 0) nctas = c->nblocks * ntile * (c->cfg.ndim == 3 ? bn / c->zchunk : 1);
   else nctas = (int)std::min<long>(planes, c->wave_ctas);
   const bool restore = !hancock && c->P.fix_small_values && c->P.small_values_method == 0;
   if (restore) CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * c->nblocks, c->stream));
@@ -234,11 +238,16 @@ int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a,
   return 0;
 }
 
+// Work distribution of the 3-D stage kernel: 0 (persistent plane ranges) or
+// z-chunks of zchunk planes, zchunk >= 2 dividing the block edge.
+static bool valid_zchunk(int bn, int zchunk) { return zchunk == 0 || (zchunk >= 2 && bn % zchunk == 0); }
+
 int launch_getdt(amrvac_ctx *c, int reg) {
   GetdtArgs G;
   G.u = c->pool[reg];
   G.dxb = c->d_dx;
   G.nblocks = c->nblocks;
+  G.bn = c->bn;
   G.type_courant = c->cfg.type_courant;
   G.red = c->d_red;
   G.P = c->P;
@@ -472,8 +481,11 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   const amrvac_cfg &k = *cfg;
   if (k.ndim < 2 || k.ndim > 3) return fail(AMRVAC_E_UNSUPPORTED, "ndim must be 2 or 3");
   if (k.ndir < k.ndim || k.ndir > 3) return fail(AMRVAC_E_UNSUPPORTED, "ndir must be in [ndim, 3]");
+  const int bn = k.block_nx[0];
   for (int d = 0; d < k.ndim; ++d)
-    if (k.block_nx[d] != 16) return fail(AMRVAC_E_UNSUPPORTED, "block_nx must be 16");
+    if (k.block_nx[d] != bn) return fail(AMRVAC_E_UNSUPPORTED, "block_nx must be the same in every direction");
+  if (!block_edge_built(bn))
+    return fail(AMRVAC_E_UNSUPPORTED, "block_nx must be 8, 10, 12, 16 or 32 (the block edges this library is built for)");
   if (k.nghostcells < 2) return fail(AMRVAC_E_UNSUPPORTED, "nghostcells must be >= 2");
   if (k.physics != 0 && k.physics != 1) return fail(AMRVAC_E_ARG, "physics must be 0 (hd) or 1 (mhd)");
   const bool fifth = k.limiter == AMRVAC_LIM_MP5 || k.limiter == AMRVAC_LIM_WENO5 ||
@@ -483,6 +495,8 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
                        k.limiter == AMRVAC_LIM_WENOYC3;
   if ((k.limiter < 1 || k.limiter > 10) && !special) return fail(AMRVAC_E_UNSUPPORTED, "limiter not supported");
   if (special && k.precision == 1) return fail(AMRVAC_E_UNSUPPORTED, "this limiter is FP64 only");
+  if (bn != 16 && (special || k.precision == 1 || k.flux_scheme == AMRVAC_FS_TVDMU))
+    return fail(AMRVAC_E_UNSUPPORTED, "block_nx other than 16: FP64 with the slope limiters, no tvdmu");
   if (fifth && k.nghostcells < 3) return fail(AMRVAC_E_ARG, "mp5 / weno5 need nghostcells >= 3");
   if (fifth && k.precision == 1) return fail(AMRVAC_E_UNSUPPORTED, "mp5 / weno5 are FP64 only");
   if (k.typeboundspeed < 1 || k.typeboundspeed > 3) return fail(AMRVAC_E_ARG, "bad typeboundspeed");
@@ -520,15 +534,24 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   c->nreg = ((k.time_stepper == AMRVAC_TS_FOURSTEP && k.time_integrator == AMRVAC_TI_RK4) ||
              k.time_stepper == AMRVAC_TS_FIVESTEP) ? 4 : 3;
   c->nw = nw;
+  c->bn = bn;
   KernelKey key{k.physics == 1, k.ndim, k.ndir, k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM,
-                k.flux_scheme, k.limiter, k.typeboundspeed, k.precision == 1};
+                k.flux_scheme, k.limiter, k.typeboundspeed, k.precision == 1, bn};
   if (k.precision != 0 && k.precision != 1) return fail(AMRVAC_E_ARG, "precision must be 0 (fp64) or 1 (mixed)");
   if (std::getenv("AMRVAC_GENERIC_KERNELS") && !special) { key.limiter = 0; key.boundspeed = 0; }
   // one kernel per family, the variant read at run time
   if (fifth && k.limiter != AMRVAC_LIM_MP5) key.limiter = LIM_WENO5;
   if (k.limiter == AMRVAC_LIM_WENOYC3) key.limiter = LIM_WENO3;
-  bool found = special ? (lookup_mp5_hd(key, &c->ks) || lookup_mp5_mhd(key, &c->ks))
-                       : (lookup_hd(key, &c->ks) || lookup_mhd2(key, &c->ks) || lookup_mhd3(key, &c->ks));
+  bool found;
+  if (bn != 16) {
+    key.limiter = 0;  // run-time limiter and bound speed
+    key.boundspeed = 0;
+    found = lookup_bn8(key, &c->ks) || lookup_bn10(key, &c->ks) || lookup_bn12(key, &c->ks) ||
+            lookup_bn32(key, &c->ks);
+  } else {
+    found = special ? (lookup_mp5_hd(key, &c->ks) || lookup_mp5_mhd(key, &c->ks))
+                    : (lookup_hd(key, &c->ks) || lookup_mhd2(key, &c->ks) || lookup_mhd3(key, &c->ks));
+  }
   if (!found) {
     delete c;
     return fail(AMRVAC_E_UNSUPPORTED, key.mixed ? "no mixed-precision kernel for this scheme"
@@ -584,7 +607,7 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   }
   for (int d = 0; d < 3; ++d) {
     if (d < k.ndim) {
-      srl_maps_1d(k.nghostcells, 16, c->maps.smin[d], c->maps.smax[d], c->maps.rmin[d], c->maps.rmax[d]);
+      srl_maps_1d(k.nghostcells, bn, c->maps.smin[d], c->maps.smax[d], c->maps.rmin[d], c->maps.rmax[d]);
     } else {
       for (int q = 0; q < 3; ++q) c->maps.smin[d][q] = c->maps.smax[d][q] = c->maps.rmin[d][q] = c->maps.rmax[d][q] = 0;
     }
@@ -593,7 +616,7 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
     delete c;
     return cuda_fail(e0, "cudaFuncSetAttribute");
   }
-  c->zchunk = (k.zchunk == 8 || k.zchunk == 4 || k.zchunk == 16) ? k.zchunk : 0;
+  c->zchunk = valid_zchunk(bn, k.zchunk) ? k.zchunk : 0;
   {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
@@ -601,7 +624,7 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
     c->wave_ctas = nsm * c->ks.ctas_per_sm();
   }
   c->per_block = 1;
-  for (int d = 0; d < k.ndim; ++d) c->per_block *= 16;
+  for (int d = 0; d < k.ndim; ++d) c->per_block *= bn;
   cudaError_t e;
   if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
     delete c;
@@ -766,8 +789,8 @@ int amrvac_gpu_set_uniform_grid(amrvac_ctx *c, const int *domain_nx, const doubl
   double h[3] = {1, 1, 1};
   int total = 1;
   for (int d = 0; d < nd; ++d) {
-    if (domain_nx[d] <= 0 || domain_nx[d] % 16) return fail(AMRVAC_E_ARG, "domain_nx must be a multiple of block_nx");
-    nb[d] = domain_nx[d] / 16;
+    if (domain_nx[d] <= 0 || domain_nx[d] % c->bn) return fail(AMRVAC_E_ARG, "domain_nx must be a multiple of block_nx");
+    nb[d] = domain_nx[d] / c->bn;
     h[d] = (xprobmax[d] - xprobmin[d]) / double(domain_nx[d]);
     total *= nb[d];
   }
@@ -973,10 +996,10 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
       }
     for (int d = 0; d < nd; ++d) {
       // cell size and corner as the reference's block geometry computes them
-      const double h = (xprobmax[d] - xprobmin[d]) / (nbase[d] * 16.0 * double(1 << (L - 1)));
+      const double h = (xprobmax[d] - xprobmin[d]) / (nbase[d] * double(c->bn) * double(1 << (L - 1)));
       dx[(size_t)b * nd + d] = h;
       dxb3[3 * (size_t)b + d] = h;
-      bxmin[3 * (size_t)b + d] = xprobmin[d] + ig[3 * b + d] * 16.0 * h;
+      bxmin[3 * (size_t)b + d] = xprobmin[d] + ig[3 * b + d] * double(c->bn) * h;
     }
   }
   for (int b = 0; b < nb; ++b)
@@ -1092,12 +1115,12 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
   A->d_bxmin = c->amr_bxmin;
   CK(cudaMemcpyAsync(A->d_bxmin, bxmin.data(), sizeof(double) * bxmin.size(), cudaMemcpyHostToDevice, c->stream));
   size_t gcells = 1;
-  for (int d = 0; d < nd; ++d) gcells *= 20;
+  for (int d = 0; d < nd; ++d) gcells *= (size_t)c->bn + 4;
   // every ghost cell a kernel reads is written by the ghost pass first, and
   // every face flux the fix reads by the stage before it: no clearing needed
   CK(ensure_capacity(&c->amr_gbuf, &c->amr_gbuf_cap, ns * c->nw * gcells));
   A->gbuf = c->amr_gbuf;
-  CK(ensure_capacity(&c->amr_pflux, &c->amr_pflux_cap, ns * 2 * nd * c->nw * 256));
+  CK(ensure_capacity(&c->amr_pflux, &c->amr_pflux_cap, ns * 2 * nd * c->nw * (size_t)c->bn * c->bn));
   A->pflux = c->amr_pflux;
   A->d_gslot = A->d_int + o_gs;
   A->d_face = A->d_int + o_fc;
@@ -1112,6 +1135,7 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
   G.dxb = c->d_dx;
   G.owner = A->d_int + o_ow;
   G.maxlevel = maxlev;
+  G.bn = c->bn;
   for (int q = 0; q < 6; ++q) {
     G.bc_kind[q] = c->bc.kind[q];
     G.bc_flip[q] = c->bc.flip[q];
@@ -1121,6 +1145,7 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
   std::memset(&A->F, 0, sizeof(A->F));
   A->F.pflux = A->pflux;
   A->F.nw = c->nw;
+  A->F.bn = c->bn;
   A->F.iblocks = G.iblocks;
   A->F.gslot = A->d_gslot;
   A->F.ntype = G.ntype;
@@ -1219,7 +1244,7 @@ static int ensure_stage(amrvac_ctx *c, size_t doubles) {
 
 static size_t ghosted_per_block(const amrvac_ctx *c) {
   size_t g = 1;
-  for (int d = 0; d < c->cfg.ndim; ++d) g *= (size_t)(16 + 2 * c->cfg.nghostcells);
+  for (int d = 0; d < c->cfg.ndim; ++d) g *= (size_t)(c->bn + 2 * c->cfg.nghostcells);
   return g * c->nw;
 }
 
@@ -1234,7 +1259,8 @@ int amrvac_gpu_upload(amrvac_ctx *c, int reg, int first, int n, const double *w)
     if (int r = ensure_stage(c, gpb * m)) return r;
     CK(cudaMemcpyAsync(c->d_stage, w + (size_t)b0 * gpb, sizeof(double) * gpb * m, cudaMemcpyHostToDevice,
                        c->stream));
-    CK(launch_unpack(c->d_stage, c->pool[reg], first + b0, m, c->nw, c->cfg.ndim, c->cfg.nghostcells, c->stream));
+    CK(launch_unpack(c->d_stage, c->pool[reg], first + b0, m, c->nw, c->cfg.ndim, c->cfg.nghostcells, c->bn,
+                     c->stream));
     ++c->launches;
   }
   CK(cudaStreamSynchronize(c->stream));
@@ -1253,7 +1279,7 @@ int amrvac_gpu_download(amrvac_ctx *c, int reg, int first, int n, double *w) {
     if (int r = ensure_stage(c, gpb * m)) return r;
     if (c->amr && b0 == 0)
       if (int r = launch_amr_ghost_pass(c, reg)) return r;
-    CK(launch_pack(c->pool[reg], c->d_stage, first + b0, m, c->nw, c->cfg.ndim, c->cfg.nghostcells, c->d_nbr,
+    CK(launch_pack(c->pool[reg], c->d_stage, first + b0, m, c->nw, c->cfg.ndim, c->cfg.nghostcells, c->bn, c->d_nbr,
                    c->maps, c->bc, c->amr ? c->amr->gbuf : nullptr, c->stream));
     ++c->launches;
     CK(cudaMemcpyAsync(w + (size_t)b0 * gpb, c->d_stage, sizeof(double) * gpb * m, cudaMemcpyDeviceToHost,
@@ -1436,8 +1462,8 @@ int amrvac_gpu_run_timed(amrvac_ctx *c, int nsteps, double *total_ms, double *st
 
 int amrvac_gpu_set_zchunk(amrvac_ctx *c, int zchunk) {
   if (int r = check_ctx(c, false)) return r;
-  if (zchunk != 16 && zchunk != 8 && zchunk != 4 && zchunk != 0)
-    return fail(AMRVAC_E_ARG, "zchunk must be 0 (persistent plane ranges), 16, 8 or 4");
+  if (!valid_zchunk(c->bn, zchunk))
+    return fail(AMRVAC_E_ARG, "zchunk must be 0 (persistent plane ranges) or a divisor >= 2 of block_nx");
   if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
   c->zchunk = zchunk;
   return 0;
@@ -1446,8 +1472,13 @@ int amrvac_gpu_set_zchunk(amrvac_ctx *c, int zchunk) {
 int amrvac_gpu_autotune(amrvac_ctx *c, int reps, int *best_zchunk, double *best_ms) {
   if (int r = check_ctx(c, true)) return r;
   if (reps <= 0) reps = 3;
-  const int ncand = c->cfg.ndim == 3 ? 4 : 2;
-  const int cand[4] = {0, 16, 8, 4};
+  // persistent, then z-chunks of the whole block, a half and a quarter of it
+  const int bn = c->bn;
+  int cand[4] = {0, bn, 0, 0}, ncand = 2;
+  if (c->cfg.ndim == 3) {
+    if (valid_zchunk(bn, bn / 2) && bn % 2 == 0) cand[ncand++] = bn / 2;
+    if (bn % 4 == 0 && valid_zchunk(bn, bn / 4)) cand[ncand++] = bn / 4;
+  }
   // dt and cmax_global of the current state (GLM needs cmax_global > 0)
   if (int r = launch_getdt(c, 0)) return r;
   CK(launch_setdt_finalize(c->d_red, c->d_scal, c->d_status, c->stream));

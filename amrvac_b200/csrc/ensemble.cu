@@ -110,7 +110,7 @@ constexpr int ENS_THREADS = 288;
 template <class TF>
 struct EnsTile {
   static constexpr int NWM = 4;
-  static constexpr int TOTAL = NWM * (BN * BN + BN * 4 + 4 * BN + 2 * (BN + 1) * BN);
+  static constexpr int TOTAL = NWM * (BN16 * BN16 + BN16 * 4 + 4 * BN16 + 2 * (BN16 + 1) * BN16);
 };
 
 template <class TF, int NW>
@@ -118,19 +118,19 @@ struct EnsView {
   TF *ring, *hx, *hy, *fbx, *fby;  // [v][j][i], [v][j][c], [v][r][i], [v][j][17], [v][17][i]
   __device__ __forceinline__ explicit EnsView(TF *s) {
     ring = s;
-    hx = ring + NW * BN * BN;
-    hy = hx + NW * BN * 4;
-    fbx = hy + NW * 4 * BN;
-    fby = fbx + NW * (BN + 1) * BN;
+    hx = ring + NW * BN16 * BN16;
+    hy = hx + NW * BN16 * 4;
+    fbx = hy + NW * 4 * BN16;
+    fby = fbx + NW * (BN16 + 1) * BN16;
   }
   // element offset of variable 0 at (i, j) in [-2, 17] x [0, 15] or [0, 15] x [-2, 17],
   // and the stride between variables
   __device__ __forceinline__ void addr(int i, int j, int &base, int &stride) const {
-    const bool ii = (unsigned)i < (unsigned)BN;
-    const bool jj = (unsigned)j < (unsigned)BN;
-    if (ii && jj) { base = j * BN + i; stride = BN * BN; }
-    else if (jj) { base = NW * BN * BN + j * 4 + halo_slot(i); stride = BN * 4; }
-    else { base = NW * BN * BN + NW * BN * 4 + halo_slot(j) * BN + i; stride = 4 * BN; }
+    const bool ii = (unsigned)i < (unsigned)BN16;
+    const bool jj = (unsigned)j < (unsigned)BN16;
+    if (ii && jj) { base = j * BN16 + i; stride = BN16 * BN16; }
+    else if (jj) { base = NW * BN16 * BN16 + j * 4 + halo_slot_w<2>(i); stride = BN16 * 4; }
+    else { base = NW * BN16 * BN16 + NW * BN16 * 4 + halo_slot_w<2>(j) * BN16 + i; stride = 4 * BN16; }
   }
 };
 
@@ -162,7 +162,7 @@ template <class TF, int ND>
 __device__ __forceinline__ uint32_t ens_face_at(const TF *s, const EnsView<TF, ND + 2> &tv, const EnsRow &Rf,
                                                 const PhysParams &P, int D, int fi, int fj) {
   constexpr int NW = ND + 2;
-  constexpr int FB = (BN + 1) * BN;
+  constexpr int FB = (BN16 + 1) * BN16;
   constexpr bool FP64 = sizeof(TF) == 8;
   const TF rd = TF(D == 0 ? Rf.rd[0] : Rf.rd[ND - 1]);
   const int lim = Rf.limiter;
@@ -188,7 +188,7 @@ __device__ __forceinline__ uint32_t ens_face_at(const TF *s, const EnsView<TF, N
   else if (Rf.solver == SOLVER_HLL) st = ens_face<TF, ND, SOLVER_HLL>(wLp, wRp, P, Fr);
   else st = ens_face<TF, ND, SOLVER_TVDLF>(wLp, wRp, P, Fr);
   TF *fb = D == 0 ? tv.fbx : tv.fby;
-  const int f = D == 0 ? fj * (BN + 1) + fi : fj * BN + fi;
+  const int f = D == 0 ? fj * (BN16 + 1) + fi : fj * BN16 + fi;
   const double sc = D == 0 ? Rf.sc[0] : Rf.sc[ND - 1];
 #pragma unroll
   for (int v = 0; v < NW; ++v) {
@@ -206,14 +206,14 @@ __device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, TF *s, cons
                                                    int next, int nt, int n2) {
   using V = Vars<false, ND, false>;
   constexpr int NW = V::NW;
-  constexpr int FB = (BN + 1) * BN;
+  constexpr int FB = (BN16 + 1) * BN16;
   constexpr bool FP64 = sizeof(TF) == 8;
   const StageArgs &S = A.sa[ND - 1];
   const PhysParams &P = S.P;
   const int t = threadIdx.x;
-  const bool cell_thread = t < BN * BN;
-  const int ci = t & (BN - 1), cj = (t >> 4) & (BN - 1);
-  const int lane = t - BN * BN;  // ninth warp: 0..31
+  const bool cell_thread = t < BN16 * BN16;
+  const int ci = t & (BN16 - 1), cj = (t >> 4) & (BN16 - 1);
+  const int lane = t - BN16 * BN16;  // ninth warp: 0..31
   uint32_t st = 0;
   EnsView<TF, NW> tv(s);
   const EnsRow &R = cur[ND == 2 ? 0 : cj];
@@ -227,7 +227,7 @@ __device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, TF *s, cons
     double w[NW];
     st |= load_prim<false, ND, false, ND>(S, R.blk, ci, cjj, 0, w);
 #pragma unroll
-    for (int v = 0; v < NW; ++v) tv.ring[v * BN * BN + cj * BN + ci] = TF(w[v]);
+    for (int v = 0; v < NW; ++v) tv.ring[v * BN16 * BN16 + cj * BN16 + ci] = TF(w[v]);
   }
   if (t < (ND == 2 ? 128 : 64)) {
     int i, j, row;
@@ -236,16 +236,16 @@ __device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, TF *s, cons
     if (t < 64) {
       j = t >> 2;
       const int c = t & 3;
-      i = c < 2 ? c - 2 : c + BN - 2;
+      i = c < 2 ? c - 2 : c + BN16 - 2;
       dst = tv.hx + j * 4 + c;
-      stride = BN * 4;
+      stride = BN16 * 4;
       row = ND == 2 ? 0 : j;
     } else {
       const int r = (t - 64) >> 4;
-      i = (t - 64) & (BN - 1);
-      j = r < 2 ? r - 2 : r + BN - 2;
-      dst = tv.hy + r * BN + i;
-      stride = 4 * BN;
+      i = (t - 64) & (BN16 - 1);
+      j = r < 2 ? r - 2 : r + BN16 - 2;
+      dst = tv.hy + r * BN16 + i;
+      stride = 4 * BN16;
       row = 0;
     }
     const EnsRow &H = cur[row];
@@ -274,14 +274,14 @@ __device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, TF *s, cons
       nf = ND;  // x-face (ci, cj) and, in 2-D, y-face (ci, cj)
       fi0 = ci; fj0 = cj; fi1 = ci; fj1 = cj;
     } else if (!cell_thread) {
-      if (lane < BN) {
+      if (lane < BN16) {
         rf = &cur[ND == 2 ? 0 : lane];
         nf = rf->inst >= 0 ? 1 : 0;
-        fi0 = BN; fj0 = lane;
+        fi0 = BN16; fj0 = lane;
       } else if (ND == 2) {
         rf = &cur[0];
         nf = rf->inst >= 0 ? 1 : 0;
-        fd0 = 1; fi0 = lane - BN; fj0 = BN;
+        fd0 = 1; fi0 = lane - BN16; fj0 = BN16;
       }
     }
 #pragma unroll 1
@@ -294,8 +294,8 @@ __device__ __forceinline__ uint32_t ens_stage_tile(const EnsArgs &A, TF *s, cons
 #pragma unroll
     for (int D = 0; D < ND; ++D) {
       const TF *fb = D == 0 ? tv.fbx : tv.fby;
-      const int f = D == 0 ? cj * (BN + 1) + ci : cj * BN + ci;
-      const int step = D == 0 ? 1 : BN;
+      const int f = D == 0 ? cj * (BN16 + 1) + ci : cj * BN16 + ci;
+      const int step = D == 0 ? 1 : BN16;
       const double sc = FP64 ? 1.0 : R.sc[D];
 #pragma unroll
       for (int v = 0; v < NW; ++v) {
@@ -325,7 +325,7 @@ __device__ __forceinline__ void ens_stage_body(const EnsArgs &A) {
   int tile = blockIdx.x;
   if (tile >= nt) return;
   const int t = threadIdx.x;
-  if (t >= BN * BN && t < BN * BN + ENS_ROWS) ens_fill_row(A, tile, tile < n2, t - BN * BN, rows[0][t - BN * BN]);
+  if (t >= BN16 * BN16 && t < BN16 * BN16 + ENS_ROWS) ens_fill_row(A, tile, tile < n2, t - BN16 * BN16, rows[0][t - BN16 * BN16]);
   __syncthreads();
   uint32_t st = 0;
 #pragma unroll 1
@@ -356,7 +356,7 @@ __device__ __forceinline__ void ens_getdt_tile(const EnsArgs &A, int tile, EnsRo
   constexpr int NW = V::NW;
   const StageArgs &S = A.sa[ND - 1];
   const int t = threadIdx.x;
-  const int ci = t & (BN - 1), cj = t >> 4;
+  const int ci = t & (BN16 - 1), cj = t >> 4;
   if (!ens_rows<ND>(A, tile, true, rows)) {
     __syncthreads();
     return;
@@ -922,7 +922,7 @@ int amrvac_ens_upload(amrvac_ens *e, int inst, const double *w) {
   const size_t doubles = g * nw * e->nblk[inst];
   if (int r = ens_ensure_stage(e, doubles)) return r;
   ECK(cudaMemcpyAsync(e->d_stage, w, sizeof(double) * doubles, cudaMemcpyHostToDevice, e->stream));
-  ECK(launch_unpack(e->d_stage, e->pool[p][0], e->first[inst], e->nblk[inst], nw, ndim, e->cfg.nghostcells,
+  ECK(launch_unpack(e->d_stage, e->pool[p][0], e->first[inst], e->nblk[inst], nw, ndim, e->cfg.nghostcells, BN16,
                     e->stream));
   ++e->launches;
   ECK(cudaStreamSynchronize(e->stream));
@@ -936,7 +936,7 @@ int amrvac_ens_download(amrvac_ens *e, int inst, double *w) {
   const size_t g = (size_t)(16 + 2 * e->cfg.nghostcells) * (p ? 16 + 2 * e->cfg.nghostcells : 1);
   const size_t doubles = g * nw * e->nblk[inst];
   if (int r = ens_ensure_stage(e, doubles)) return r;
-  ECK(launch_pack(e->pool[p][0], e->d_stage, e->first[inst], e->nblk[inst], nw, ndim, e->cfg.nghostcells,
+  ECK(launch_pack(e->pool[p][0], e->d_stage, e->first[inst], e->nblk[inst], nw, ndim, e->cfg.nghostcells, BN16,
                   e->d_nbr[p], e->maps, e->bc, nullptr, e->stream));
   ++e->launches;
   ECK(cudaMemcpyAsync(w, e->d_stage, sizeof(double) * doubles, cudaMemcpyDeviceToHost, e->stream));

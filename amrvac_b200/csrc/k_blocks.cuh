@@ -1,0 +1,53 @@
+// Stage / getdt / point kernels for block edges other than 16 (block_nx 8,
+// 10, 12, 32: the reference's own 3-D blast and Kelvin-Helmholtz and 2-D
+// Riemann tests run 8^3, 10^3 and 12^2 blocks).  FP64, the slope limiters
+// and bound speeds at run time (LIM = 0, BS = 0), every solver but
+// TVD-MUSCL.  Each block edge is instantiated in its own translation unit
+// (k_bn*.cu) so that they compile in parallel.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace amrvac {
+
+template <int BN>
+bool lookup_bn(const KernelKey &k, KernelSet *out) {
+  if (k.bn != BN || k.mixed || k.solver == SOLVER_TVDMU) return false;
+  if (!k.mhd) {
+    if (k.ndir != k.ndim) return false;
+#define AMRVAC_BHD(ND, S)                                              \
+    if (k.ndim == ND && k.solver == S) {                                 \
+      *out = Launch<false, ND, false, ND, S, 0, 0, double, BN>::set();   \
+      return true;                                                       \
+    }
+    AMRVAC_BHD(2, SOLVER_TVDLF)
+    AMRVAC_BHD(2, SOLVER_HLL)
+    AMRVAC_BHD(2, SOLVER_HLLC)
+    AMRVAC_BHD(3, SOLVER_TVDLF)
+    AMRVAC_BHD(3, SOLVER_HLL)
+    AMRVAC_BHD(3, SOLVER_HLLC)
+#undef AMRVAC_BHD
+    return false;
+  }
+#define AMRVAC_BM(ND, NDIR, GLM, S)                                      \
+  if (k.ndim == ND && k.ndir == NDIR && k.glm == GLM && k.solver == S) { \
+    *out = Launch<true, NDIR, GLM, ND, S, 0, 0, double, BN>::set();       \
+    return true;                                                          \
+  }
+#define AMRVAC_BM4(ND, NDIR, GLM)            \
+  AMRVAC_BM(ND, NDIR, GLM, SOLVER_TVDLF)     \
+  AMRVAC_BM(ND, NDIR, GLM, SOLVER_HLL)       \
+  AMRVAC_BM(ND, NDIR, GLM, SOLVER_HLLC)      \
+  AMRVAC_BM(ND, NDIR, GLM, SOLVER_HLLD)
+  AMRVAC_BM4(2, 2, false)
+  AMRVAC_BM4(2, 2, true)
+  AMRVAC_BM4(2, 3, false)
+  AMRVAC_BM4(2, 3, true)
+  AMRVAC_BM4(3, 3, false)
+  AMRVAC_BM4(3, 3, true)
+#undef AMRVAC_BM4
+#undef AMRVAC_BM
+  return false;
+}
+
+}  // namespace amrvac

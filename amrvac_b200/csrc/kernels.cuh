@@ -15,6 +15,7 @@ struct GetdtArgs {
   const double *u;
   const double *dxb;
   int nblocks;
+  int bn;  // block edge
   int type_courant;
   unsigned long long *red;
   PhysParams P;
@@ -35,18 +36,20 @@ template <bool MHD, int NDIR, bool GLM, int NDIM>
 __global__ void __launch_bounds__(256) getdt_kernel(const GetdtArgs A) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
-  constexpr int NZ = NDIM == 3 ? BN : 1;
+  const int bn = A.bn;
+  const int ncell = bn * (NDIM >= 2 ? bn : 1) * (NDIM == 3 ? bn : 1);
   const int b = blockIdx.x;
   const int t = threadIdx.x;
-  const int i = t & (BN - 1), j = t >> 4;
   double dxinv[3];
 #pragma unroll
   for (int d = 0; d < NDIM; ++d) dxinv[d] = 1.0 / A.dxb[b * 3 + d];
   double mtot = 0.0, mcm = 0.0, mdim[3] = {0.0, 0.0, 0.0};
-  for (int k = 0; k < NZ; ++k) {
+  // the block's cells, x fastest (coalesced), 256 at a time
+  for (int c = t; c < ncell; c += 256) {
+    const int i = c % bn, j = NDIM >= 2 ? (c / bn) % bn : 0, k = NDIM == 3 ? c / (bn * bn) : 0;
     double w[NW];
 #pragma unroll
-    for (int v = 0; v < NW; ++v) w[v] = __ldg(A.u + cell_offset<NDIM>(b, NW, v, i, j, k));
+    for (int v = 0; v < NW; ++v) w[v] = __ldg(A.u + cell_offset<NDIM>(b, NW, v, i, j, k, bn));
     to_primitive<MHD, NDIR, GLM>(w, A.P);
     double tot = 0.0;
 #pragma unroll
@@ -171,16 +174,15 @@ __global__ void cbounds_points_kernel(const PointArgs A) {
 // maximum over its cells and conserved variables of
 // |-w(i+2) + 16 w(i+1) - 30 w(i) + 16 w(i-1) - w(i-2)|, / 12 / dx_d^2, then
 // the maximum over blocks into out[d].  One CTA per z-plane of a block.
-template <int NW, int NDIM>
+template <int NW, int NDIM, int BN = BN16>
 __global__ void __launch_bounds__(256) a2max_kernel(const StageArgs A, double *out) {
   constexpr int PL = NDIM == 3 ? BN : 1;
   const int b = blockIdx.x / PL, k = blockIdx.x - (blockIdx.x / PL) * PL;
-  const int i = threadIdx.x & (BN - 1), j = threadIdx.x >> 4;
   auto w = [&](int ii, int jj, int kk, int v) {
     uint32_t flip;
-    const int blk = resolve_cell<NDIM>(A, b, ii, jj, kk, flip);
-    const double x = blk >= 0 ? __ldg(A.uin + cell_offset<NDIM>(blk, NW, v, ii, jj, kk))
-                              : __ldg(A.gbuf + ghost_offset<NDIM>(-2 - blk, NW, v, ii, jj, kk));
+    const int blk = resolve_cell<NDIM>(A, b, ii, jj, kk, flip, BN);
+    const double x = blk >= 0 ? __ldg(A.uin + cell_offset<NDIM>(blk, NW, v, ii, jj, kk, BN))
+                              : __ldg(A.gbuf + ghost_offset<NDIM>(-2 - blk, NW, v, ii, jj, kk, BN));
     return ((flip >> v) & 1u) ? -x : x;
   };
   __shared__ double red[8];
@@ -188,13 +190,16 @@ __global__ void __launch_bounds__(256) a2max_kernel(const StageArgs A, double *o
   for (int d = 0; d < NDIM; ++d) {
     const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
     double m = 0.0;
+    for (int c = threadIdx.x; c < BN * BN; c += 256) {  // the cells of the plane
+      const int i = c % BN, j = c / BN;
 #pragma unroll
-    for (int v = 0; v < NW; ++v) {
-      const double a = fabs(((((-w(i + 2 * e0, j + 2 * e1, k + 2 * e2, v) + 16.0 * w(i + e0, j + e1, k + e2, v)) -
-                               30.0 * w(i, j, k, v)) +
-                              16.0 * w(i - e0, j - e1, k - e2, v)) -
-                             w(i - 2 * e0, j - 2 * e1, k - 2 * e2, v)));
-      m = fmax(m, a);
+      for (int v = 0; v < NW; ++v) {
+        const double a = fabs(((((-w(i + 2 * e0, j + 2 * e1, k + 2 * e2, v) + 16.0 * w(i + e0, j + e1, k + e2, v)) -
+                                 30.0 * w(i, j, k, v)) +
+                                16.0 * w(i - e0, j - e1, k - e2, v)) -
+                               w(i - 2 * e0, j - 2 * e1, k - 2 * e2, v)));
+        m = fmax(m, a);
+      }
     }
     m = warp_max(m);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
@@ -218,26 +223,27 @@ __global__ void __launch_bounds__(256) a2max_kernel(const StageArgs A, double *o
 // stencil (divB at the six neighbours: B two cells out and across the z
 // planes' halos) is gathered here through the stage's neighbour resolution
 // (and the level-jump ghost buffers); one CTA per z-plane of a block.
-template <int NDIR>
+template <int NDIR, int BN = BN16>
 __global__ void __launch_bounds__(256) linde3d_kernel(const StageArgs A) {
   using V = Vars<true, NDIR, false>;
   constexpr int NW = V::NW;
   const int b = blockIdx.x / BN, k = blockIdx.x - (blockIdx.x / BN) * BN;
-  const int i = threadIdx.x & (BN - 1), j = threadIdx.x >> 4;
   if (b >= A.nblocks) return;
   const int m = A.amr_face ? A.amr_face[b] : 0;
+  for (int c = threadIdx.x; c < BN * BN; c += 256) {  // the cells of the plane
+  const int i = c % BN, j = c / BN;
   if (m && (((m & 1) && i == 0) || ((m & 2) && i == BN - 1) || ((m & 4) && j == 0) || ((m & 8) && j == BN - 1) ||
             ((m & 16) && k == 0) || ((m & 32) && k == BN - 1)))
-    return;
+    continue;
   double dx[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) dx[d] = A.dxb[b * 3 + d];
   auto bct = [&](int ii, int jj, int kk, int c) -> double {  // wCT's B_c, up to two cells outside
     uint32_t flip;
-    const int blk = resolve_cell<3>(A, b, ii, jj, kk, flip);
+    const int blk = resolve_cell<3>(A, b, ii, jj, kk, flip, BN);
     const int v = V::B0 + c;
-    const double x = blk >= 0 ? __ldg(A.uin + cell_offset<3>(blk, NW, v, ii, jj, kk))
-                              : __ldg(A.gbuf + ghost_offset<3>(-2 - blk, NW, v, ii, jj, kk));
+    const double x = blk >= 0 ? __ldg(A.uin + cell_offset<3>(blk, NW, v, ii, jj, kk, BN))
+                              : __ldg(A.gbuf + ghost_offset<3>(-2 - blk, NW, v, ii, jj, kk, BN));
     return ((flip >> v) & 1u) ? -x : x;
   };
   auto divb = [&](int ii, int jj, int kk) {
@@ -249,7 +255,7 @@ __global__ void __launch_bounds__(256) linde3d_kernel(const StageArgs A) {
   const double inv2 = (1.0 / (dx[0] * dx[0]) + 1.0 / (dx[1] * dx[1])) + 1.0 / (dx[2] * dx[2]);
   double w[NW];
 #pragma unroll
-  for (int v = 0; v < NW; ++v) w[v] = A.uout[cell_offset<3>(b, NW, v, i, j, k)];
+  for (int v = 0; v < NW; ++v) w[v] = A.uout[cell_offset<3>(b, NW, v, i, j, k, BN)];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const double dp = d == 0 ? divb(i + 1, j, k) : (d == 1 ? divb(i, j + 1, k) : divb(i, j, k + 1));
@@ -258,14 +264,15 @@ __global__ void __launch_bounds__(256) linde3d_kernel(const StageArgs A) {
     g = g / dx[d];
     g = g * A.P.divbdiff / inv2;
     w[V::B0 + d] = w[V::B0 + d] + g;
-    w[V::E] = w[V::E] + __ldg(A.uin + cell_offset<3>(b, NW, V::B0 + d, i, j, k)) * g;
+    w[V::E] = w[V::E] + __ldg(A.uin + cell_offset<3>(b, NW, V::B0 + d, i, j, k, BN)) * g;
   }
   if (A.P.fix_small_values) {
     if (small_values<double, true, NDIR, false>(w, false, A.P) && A.P.small_values_method != 1)
       atomicOr(A.status, ST_SMALL_VALUE);
   }
 #pragma unroll
-  for (int v = 0; v < NW; ++v) A.uout[cell_offset<3>(b, NW, v, i, j, k)] = w[v];
+  for (int v = 0; v < NW; ++v) A.uout[cell_offset<3>(b, NW, v, i, j, k, BN)] = w[v];
+  }  // cells of the plane
 }
 
 // ---------------------------------------------------------------- dispatch
@@ -284,35 +291,38 @@ struct KernelSet {
   cudaError_t (*flux_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
   cudaError_t (*cbounds_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
   size_t stage_smem = 0;
+  int bn = BN16;  // the block edge the stage kernels were built for
 };
 
-template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM = 0, int BS = 0, class TF = double>
+template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM = 0, int BS = 0, class TF = double,
+          int BN = BN16>
 struct Launch {
   using V = Vars<MHD, NDIR, GLM>;
-  static constexpr size_t SMEM = Tile<TF, V::NW, NDIM, HaloW<LIM>::value>::BYTES;
+  static constexpr int THREADS = StageOcc<TF, LIM, BN>::THREADS;
+  static constexpr size_t SMEM = Tile<TF, V::NW, NDIM, HaloW<LIM>::value, tile_edge(BN)>::BYTES;
   // typepred1 = fs_hancock for tvdlf and tvdmu (src/io/mod_input_output.t:787-797)
   static constexpr bool HAS_HANCOCK = (SOLVER == SOLVER_TVDLF || SOLVER == SOLVER_TVDMU) && sizeof(TF) == 8;
   static cudaError_t prepare() {
-    cudaError_t e = cudaFuncSetAttribute(fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>,
+    cudaError_t e = cudaFuncSetAttribute(fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, BN>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
     if constexpr (HAS_HANCOCK) {
       if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER_HANCOCK, LIM, BS>,
+        e = cudaFuncSetAttribute(fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER_HANCOCK, LIM, BS, BN>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
     }
     return e;
   }
   static cudaError_t stage(const StageArgs &A, int nctas, cudaStream_t s) {
-    fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
+    fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, BN><<<nctas, THREADS, SMEM, s>>>(A);
     return cudaGetLastError();
   }
   static cudaError_t a2max(const StageArgs &A, double *out, cudaStream_t s) {
-    a2max_kernel<V::NW, NDIM><<<A.nblocks * (NDIM == 3 ? BN : 1), 256, 0, s>>>(A, out);
+    a2max_kernel<V::NW, NDIM, BN><<<A.nblocks * (NDIM == 3 ? BN : 1), 256, 0, s>>>(A, out);
     return cudaGetLastError();
   }
   static cudaError_t linde3d(const StageArgs &A, cudaStream_t s) {
     if constexpr (MHD && NDIM == 3 && !GLM) {
-      linde3d_kernel<NDIR><<<A.nblocks * BN, 256, 0, s>>>(A);
+      linde3d_kernel<NDIR, BN><<<A.nblocks * BN, 256, 0, s>>>(A);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;
@@ -320,7 +330,7 @@ struct Launch {
   }
   static cudaError_t hancock(const StageArgs &A, int nctas, cudaStream_t s) {
     if constexpr (HAS_HANCOCK) {
-      fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER_HANCOCK, LIM, BS><<<nctas, STAGE_THREADS, SMEM, s>>>(A);
+      fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER_HANCOCK, LIM, BS, BN><<<nctas, THREADS, SMEM, s>>>(A);
       return cudaGetLastError();
     } else {
       return cudaErrorNotSupported;
@@ -328,8 +338,8 @@ struct Launch {
   }
   static int ctas_per_sm() {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>,
-                                                      STAGE_THREADS, SMEM) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, BN>, THREADS, SMEM) != cudaSuccess)
       return 1;
     return n > 0 ? n : 1;
   }
@@ -383,6 +393,7 @@ struct Launch {
     k.flux_points = &flux_points;
     k.cbounds_points = &cbounds_points;
     k.stage_smem = SMEM;
+    k.bn = BN;
     return k;
   }
 };
@@ -396,9 +407,15 @@ struct KernelKey {
   int limiter;     // used to pick a compile-time specialised stage kernel
   int boundspeed;
   bool mixed;      // FP32 face arithmetic (mixed form)
+  int bn;          // block edge (block_nx)
 };
 
 bool lookup_hd(const KernelKey &k, KernelSet *out);
+// block edges other than 16 (k_blocks.cuh, one unit per edge)
+bool lookup_bn8(const KernelKey &k, KernelSet *out);
+bool lookup_bn10(const KernelKey &k, KernelSet *out);
+bool lookup_bn12(const KernelKey &k, KernelSet *out);
+bool lookup_bn32(const KernelKey &k, KernelSet *out);
 bool lookup_mp5_hd(const KernelKey &k, KernelSet *out);
 bool lookup_mp5_mhd(const KernelKey &k, KernelSet *out);
 bool lookup_mhd2(const KernelKey &k, KernelSet *out);

@@ -69,24 +69,24 @@ int scratch_for_current_device(double **out) {
 // block writes its (courant, cmax) pair to its own scratch slot instead of
 // folding it into global atomics.
 template <bool MHD, int NDIR, bool GLM, int NDIM>
-__global__ void __launch_bounds__(256) getdt_blocks_kernel(const double *__restrict__ u, int type_courant,
+__global__ void __launch_bounds__(256) getdt_blocks_kernel(const double *__restrict__ u, int bn, int type_courant,
                                                            PhysParams P, double *__restrict__ scratch) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
-  constexpr int NZ = NDIM == 3 ? BN : 1;
+  const int ncell = bn * (NDIM >= 2 ? bn : 1) * (NDIM == 3 ? bn : 1);
   const int b = blockIdx.x;
   const int t = threadIdx.x;
-  const int i = t & (BN - 1), j = t >> 4;
   const double *dx = scratch + OFF_DX + (size_t)b * 3;
   double dxinv[3] = {0.0, 0.0, 0.0};
 #pragma unroll
   for (int d = 0; d < NDIM; ++d) dxinv[d] = 1.0 / dx[d];
   // per thread: max of the cell sums, of cmax, and of cmax_d/dx_d per direction
   double msum = 0.0, mcm = 0.0, mdir[3] = {0.0, 0.0, 0.0};
-  for (int k = 0; k < NZ; ++k) {
+  for (int c = t; c < ncell; c += 256) {  // the block's cells, x fastest
+    const int i = c % bn, j = NDIM >= 2 ? (c / bn) % bn : 0, k = NDIM == 3 ? c / (bn * bn) : 0;
     double w[NW];
 #pragma unroll
-    for (int v = 0; v < NW; ++v) w[v] = __ldg(u + cell_offset<NDIM>(b, NW, v, i, j, k));
+    for (int v = 0; v < NW; ++v) w[v] = __ldg(u + cell_offset<NDIM>(b, NW, v, i, j, k, bn));
     to_primitive<MHD, NDIR, GLM>(w, P);
     double sum = 0.0;
 #pragma unroll
@@ -158,13 +158,13 @@ __global__ void __launch_bounds__(256) getdt_combine_kernel(int nblocks, double 
 }
 
 template <bool MHD, int NDIR, bool GLM, int NDIM>
-cudaError_t launch_blocks(const double *u, int nblocks, int type_courant, const PhysParams &P, double *scratch,
-                          cudaStream_t s) {
-  getdt_blocks_kernel<MHD, NDIR, GLM, NDIM><<<nblocks, 256, 0, s>>>(u, type_courant, P, scratch);
+cudaError_t launch_blocks(const double *u, int nblocks, int bn, int type_courant, const PhysParams &P,
+                          double *scratch, cudaStream_t s) {
+  getdt_blocks_kernel<MHD, NDIR, GLM, NDIM><<<nblocks, 256, 0, s>>>(u, bn, type_courant, P, scratch);
   return cudaGetLastError();
 }
 
-using BlocksFn = cudaError_t (*)(const double *, int, int, const PhysParams &, double *, cudaStream_t);
+using BlocksFn = cudaError_t (*)(const double *, int, int, int, const PhysParams &, double *, cudaStream_t);
 
 BlocksFn pick(const amrvac_cfg &k, bool glm) {
   if (k.physics == 0) {
@@ -191,8 +191,11 @@ extern "C" int amrvac_gpu_getdt_noalloc(const amrvac_cfg *cfg, const double *w_d
   const amrvac_cfg &k = *cfg;
   if (k.physics != 0 && k.physics != 1) return record_error(AMRVAC_E_ARG, "getdt_noalloc: physics must be 0 or 1");
   if (k.type_courant < 1 || k.type_courant > 3) return record_error(AMRVAC_E_ARG, "getdt_noalloc: bad type_courant");
+  const int bn = k.block_nx[0];
   for (int d = 0; d < k.ndim && d < 3; ++d)
-    if (k.block_nx[d] != 16) return record_error(AMRVAC_E_UNSUPPORTED, "getdt_noalloc: block_nx must be 16");
+    if (k.block_nx[d] != bn || bn < 4 || bn % 2 || bn > 1024)
+      return record_error(AMRVAC_E_UNSUPPORTED,
+                          "getdt_noalloc: block_nx must be even, >= 4 and the same in every direction");
   const bool glm = k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM;
   BlocksFn fn = pick(k, glm);
   if (!fn) return record_error(AMRVAC_E_UNSUPPORTED, "getdt_noalloc: unsupported physics/ndim/ndir");
@@ -208,7 +211,7 @@ extern "C" int amrvac_gpu_getdt_noalloc(const amrvac_cfg *cfg, const double *w_d
   double res[2] = {0.0, 0.0};
   cudaError_t e = cudaMemcpyAsync(scratch + OFF_DX, dx, sizeof(double) * 3 * (size_t)nblocks,
                                   cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = fn(w_dev, nblocks, k.type_courant, P, scratch, s);
+  if (e == cudaSuccess) e = fn(w_dev, nblocks, bn, k.type_courant, P, scratch, s);
   if (e == cudaSuccess) {
     getdt_combine_kernel<<<1, 256, 0, s>>>(nblocks, scratch);
     e = cudaGetLastError();

@@ -35,7 +35,28 @@
 
 namespace amrvac {
 
-constexpr int BN = 16;               // cells per block edge
+// Block edge (block_nx, the same in every direction).  The reference allows
+// any even block_nx >= 4 (src/io/mod_input_output.t:1494-1503); the library
+// runs the sizes of BLOCK_SIZES.  Helpers that address blocks take the edge
+// as an argument (a constant in the stage kernel, so it folds there).
+constexpr int BN16 = 16;
+// The stage kernel advances a tile of TB x TB cells of a block's z-plane per
+// CTA: the whole plane up to block_nx 16, else the largest divisor of
+// block_nx that is at most 16 (32 -> four 16 x 16 tiles per plane).
+__host__ __device__ constexpr int tile_edge(int bn) {
+  if (bn <= 16) return bn;
+  for (int t = 16; t > 1; --t)
+    if (bn % t == 0) return t;
+  return 1;
+}
+// The block edges the library's kernels are built for.
+__host__ __device__ constexpr bool block_edge_built(int bn) {
+  return bn == 8 || bn == 10 || bn == 12 || bn == 16 || bn == 32;
+}
+// threads of a stage CTA: one per cell of the tile, rounded up to whole warps
+__host__ __device__ constexpr int stage_threads(int bn) {
+  return (tile_edge(bn) * tile_edge(bn) + 31) / 32 * 32;
+}
 #ifndef AMRVAC_STAGE_THREADS
 #define AMRVAC_STAGE_THREADS 256
 #endif
@@ -84,6 +105,7 @@ struct StageArgs {
   // stage is the sweep-th of the step's one-direction sweeps (see sweep_dir).
   int sweep;
   int split_xy;             // 1: typedimsplit 'xy' (same order every step)
+  int bn;                   // block edge, for the kernels that take it at run time
 };
 
 // Direction of a dimensionally split sweep (src/mod_advance.t:23-45):
@@ -100,12 +122,13 @@ __device__ __forceinline__ int dir_index(int di, int dj, int dk) {
   return (di + 1) + 3 * (dj + 1) + 9 * (dk + 1);
 }
 
-// Resolve a cell of block b given local coordinates that may lie up to two
-// (three with MP5) cells outside the block: physical sides first (clamp for cont, mirror for
-// symm/asymm), then the remaining offset through the neighbour table.
+// Resolve a cell of block b (edge bn) given local coordinates that may lie
+// up to two (three with MP5) cells outside the block: physical sides first
+// (clamp for cont, mirror for symm/asymm), then the remaining offset through
+// the neighbour table.
 template <int NDIM>
 __device__ __forceinline__ int resolve_cell(const StageArgs &A, int b, int &i, int &j, int &k,
-                                            uint32_t &flip) {
+                                            uint32_t &flip, int BN = BN16) {
   int c[3] = {i, j, k};
   int dir[3] = {0, 0, 0};
   flip = 0;
@@ -148,41 +171,41 @@ __device__ __forceinline__ int resolve_cell(const StageArgs &A, int b, int &i, i
 }
 
 template <int NDIM>
-__device__ __forceinline__ size_t cell_offset(int blk, int nw, int v, int i, int j, int k) {
-  constexpr int NY = NDIM >= 2 ? BN : 1;
-  constexpr int NZ = NDIM >= 3 ? BN : 1;
+__device__ __forceinline__ size_t cell_offset(int blk, int nw, int v, int i, int j, int k, int BN = BN16) {
+  const int NY = NDIM >= 2 ? BN : 1;
+  const int NZ = NDIM >= 3 ? BN : 1;
   return (((size_t)blk * nw + v) * NZ + k) * (size_t)(NY * BN) + (size_t)j * BN + i;
 }
 
 // Offset of cell (i, j, k) (block-local, up to 2 outside) in a ghosted
 // buffer of 2 ghost layers: [slot][var][gz][gy][gx].
 template <int NDIM>
-__device__ __forceinline__ size_t ghost_offset(int slot, int nw, int v, int i, int j, int k) {
-  constexpr int G = BN + 4;
-  constexpr int GY = NDIM >= 2 ? G : 1;
-  constexpr int GZ = NDIM >= 3 ? G : 1;
+__device__ __forceinline__ size_t ghost_offset(int slot, int nw, int v, int i, int j, int k, int BN = BN16) {
+  const int G = BN + 4;
+  const int GY = NDIM >= 2 ? G : 1;
+  const int GZ = NDIM >= 3 ? G : 1;
   const int gj = NDIM >= 2 ? j + 2 : 0, gk = NDIM >= 3 ? k + 2 : 0;
   return (((size_t)slot * nw + v) * GZ + gk) * (size_t)(GY * G) + (size_t)gj * G + (i + 2);
 }
 
 // Load the conserved state of a (possibly out-of-block) cell and return it
 // as primitives.  Returns a status bit if the small-value check fires.
-template <bool MHD, int NDIR, bool GLM, int NDIM>
+template <bool MHD, int NDIR, bool GLM, int NDIM, int BN = BN16>
 __device__ __forceinline__ uint32_t load_prim(const StageArgs &A, int b, int i, int j, int k,
                                               double *w) {
   using V = Vars<MHD, NDIR, GLM>;
   uint32_t flip;
-  const int blk = resolve_cell<NDIM>(A, b, i, j, k, flip);
+  const int blk = resolve_cell<NDIM>(A, b, i, j, k, flip, BN);
   if (blk >= 0) {
 #pragma unroll
     for (int v = 0; v < V::NW; ++v) {
-      double x = __ldg(A.uin + cell_offset<NDIM>(blk, V::NW, v, i, j, k));
+      double x = __ldg(A.uin + cell_offset<NDIM>(blk, V::NW, v, i, j, k, BN));
       w[v] = ((flip >> v) & 1u) ? -x : x;
     }
   } else {  // level jump: this block's ghost buffer
 #pragma unroll
     for (int v = 0; v < V::NW; ++v) {
-      const double x = __ldg(A.gbuf + ghost_offset<NDIM>(-2 - blk, V::NW, v, i, j, k));
+      const double x = __ldg(A.gbuf + ghost_offset<NDIM>(-2 - blk, V::NW, v, i, j, k, BN));
       w[v] = ((flip >> v) & 1u) ? -x : x;
     }
   }
@@ -381,8 +404,8 @@ struct HaloW {
   static constexpr int value = (LIM == LIM_MP5 || LIM == LIM_WENO5) ? 3 : 2;
 };
 
-// Shared-memory tile (sizes in doubles), halo width HW.
-template <class TF, int NW, int NDIM, int HW = 2>
+// Shared-memory tile of BN x BN cells (sizes in doubles), halo width HW.
+template <class TF, int NW, int NDIM, int HW = 2, int BN = BN16>
 struct Tile {
   static constexpr int H2 = 2 * HW;
   static constexpr int NSLOT = NDIM == 3 ? H2 : 1;      // z ring: planes k-HW+1 .. k+HW
@@ -397,8 +420,7 @@ struct Tile {
   static constexpr size_t BYTES = sizeof(TF) * TOTAL;
 };
 
-__device__ __forceinline__ int halo_slot(int c) { return c < 0 ? c + 2 : c - (BN - 2); }
-template <int HW>
+template <int HW, int BN = BN16>
 __device__ __forceinline__ int halo_slot_w(int c) { return c < 0 ? c + HW : c - (BN - HW); }
 
 // Ring slot of z-plane k (k >= -2 HW).
@@ -408,12 +430,12 @@ __device__ __forceinline__ int ring_slot(int k) {
   else return (k + 4 * HW) % (2 * HW);
 }
 
-template <class TF, int NW, int NDIM, int HW = 2>
+template <class TF, int NW, int NDIM, int HW = 2, int BN = BN16>
 struct TileView {
   static constexpr int H2 = 2 * HW;
   TF *ring, *hx, *hy, *hc, *fb, *yx;
   __device__ TileView(TF *s) {
-    using T = Tile<TF, NW, NDIM, HW>;
+    using T = Tile<TF, NW, NDIM, HW, BN>;
     ring = s;
     hx = ring + T::RING;
     hy = hx + T::HX;
@@ -425,16 +447,16 @@ struct TileView {
   __device__ __forceinline__ TF at(int slot, int v, int i, int j) const {
     const bool ii = (unsigned)i < (unsigned)BN, jj = (unsigned)j < (unsigned)BN;
     if (ii && jj) return ring[(slot * NW + v) * (BN * BN) + j * BN + i];
-    if (jj) return hx[(v * BN + j) * H2 + halo_slot_w<HW>(i)];
-    if (ii) return hy[(v * H2 + halo_slot_w<HW>(j)) * BN + i];
-    return hc[(v * H2 + halo_slot_w<HW>(j)) * H2 + halo_slot_w<HW>(i)];
+    if (jj) return hx[(v * BN + j) * H2 + halo_slot_w<HW, BN>(i)];
+    if (ii) return hy[(v * H2 + halo_slot_w<HW, BN>(j)) * BN + i];
+    return hc[(v * H2 + halo_slot_w<HW, BN>(j)) * H2 + halo_slot_w<HW, BN>(i)];
   }
   // Offset (in doubles from the tile start) of variable 0 at in-plane (i, j)
   // of the plane in `slot`, and the stride between variables there; branch-free.
   __device__ __forceinline__ void addr(int slot, int i, int j, int &base, int &stride) const {
-    using T = Tile<TF, NW, NDIM, HW>;
+    using T = Tile<TF, NW, NDIM, HW, BN>;
     const bool ii = (unsigned)i < (unsigned)BN, jj = (unsigned)j < (unsigned)BN;
-    const int hi = halo_slot_w<HW>(i), hj = halo_slot_w<HW>(j);
+    const int hi = halo_slot_w<HW, BN>(i), hj = halo_slot_w<HW, BN>(j);
     const int oc = slot * NW * (BN * BN) + j * BN + i;
     const int ox = T::RING + j * H2 + hi;
     const int oy = T::RING + T::HX + hj * BN + i;
@@ -547,13 +569,29 @@ __device__ __forceinline__ uint32_t hancock_dir(const double *smem, const int *b
 // MP5 (three-cell halo) takes one CTA per SM: its 6-plane ring fills most of
 // the shared memory of the 3-D MHD tile, and the registers it frees avoid
 // spills in the 6-cell face stencil.
-template <class TF, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS>
-__global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::value == 3 ? 1 : AMRVAC_STAGE_MINB)
-                                                                 : AMRVAC_STAGE_MINB_MIXED)
+// CTAs per SM the stage kernel is built for: two of 256 threads (FP64; one
+// with the fifth-order halo), three in the mixed form; smaller tiles keep the
+// same threads per SM.
+template <class TF, int LIM, int BN>
+struct StageOcc {
+  static constexpr int THREADS = BN == BN16 ? STAGE_THREADS : stage_threads(BN);
+  static constexpr int BASE = sizeof(TF) == 8 ? (HaloW<LIM>::value == 3 ? 1 : AMRVAC_STAGE_MINB)
+                                              : AMRVAC_STAGE_MINB_MIXED;
+  static constexpr int MINB = BASE * 256 / THREADS < 1 ? 1 : (BASE * 256 / THREADS > 16 ? 16 : BASE * 256 / THREADS);
+};
+
+template <class TF, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS, int BN = BN16>
+__global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, LIM, BN>::MINB)
     fv_stage_kernel(const StageArgs A) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
-  constexpr int FB = (BN + 1) * BN;  // face-buffer stride per variable
+  // block edge BN; this CTA's tile is TB x TB cells of a z-plane (x/y), at
+  // (ti0, tj0) in the block; TBY = TB in 2-D and 3-D
+  constexpr int TB = tile_edge(BN);
+  constexpr int NTX = BN / TB;                       // tiles per plane row
+  constexpr int NT = NDIM >= 2 ? NTX * NTX : NTX;    // tiles per plane
+  constexpr int THREADS = StageOcc<TF, LIM, BN>::THREADS;
+  constexpr int FB = (TB + 1) * TB;  // face-buffer stride per variable
   constexpr bool FP64 = sizeof(TF) == 8;
   constexpr int HW = HaloW<LIM>::value;  // halo width: 2, or 3 for MP5
   constexpr int H2 = 2 * HW;
@@ -565,23 +603,23 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
   constexpr bool RETRY = !FP64 || FASTF;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TF *smem = reinterpret_cast<TF *>(smem_raw);
-  TileView<TF, NW, NDIM, HW> tv(smem);
+  TileView<TF, NW, NDIM, HW, TB> tv(smem);
   const int t = threadIdx.x;
-  // Work: global z-planes g = block*PL + k (PL = 16 in 3-D, 1 in 2-D).
-  // zchunk > 0: one z-chunk of one block per CTA.  zchunk == 0: persistent
-  // plane ranges — the grid is one wave of CTAs, each marching a contiguous
-  // range of planes across block boundaries and re-staging halo planes only
-  // where a new block starts.
+  // Work: global tile-planes g = (block*NT + tile)*PL + k (PL = BN in 3-D,
+  // 1 in 2-D).  zchunk > 0: one z-chunk of one tile column per CTA.
+  // zchunk == 0: persistent plane ranges — the grid is one wave of CTAs,
+  // each marching a contiguous range of tile-planes across block boundaries
+  // and re-staging halo planes only where a new tile column starts.
   constexpr int PL = NDIM == 3 ? BN : 1;
   long g, gend;
   if (A.zchunk > 0) {
     const int nchunk = NDIM == 3 ? BN / A.zchunk : 1;
-    const int b0 = blockIdx.x / nchunk;
-    if (b0 >= A.nblocks) return;
-    g = (long)b0 * PL + (NDIM == 3 ? (blockIdx.x - b0 * nchunk) * A.zchunk : 0);
+    const int c0 = blockIdx.x / nchunk;  // tile column: block*NT + tile
+    if (c0 >= A.nblocks * NT) return;
+    g = (long)c0 * PL + (NDIM == 3 ? (blockIdx.x - c0 * nchunk) * A.zchunk : 0);
     gend = g + (NDIM == 3 ? A.zchunk : 1);
   } else {
-    const long total = (long)A.nblocks * PL;
+    const long total = (long)A.nblocks * NT * PL;
     g = (long)blockIdx.x * total / gridDim.x;
     gend = (long)(blockIdx.x + 1) * total / gridDim.x;
   }
@@ -592,15 +630,19 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
   const int dsel = sweep_dir(A.sweep, A.split_xy, A.dt_dev, NDIM);  // -1: all directions
   const double cg = GLM ? *A.cmax_dev : 0.0;
   uint32_t st = 0;
-  const int ci = t & (BN - 1), cj = t >> 4;  // cell role for t < 256
-  const bool cell_thread = t < BN * BN;
+  const int ci = t % TB, cj = t / TB;  // cell role (tile-relative) for t < TB*TB
+  const bool cell_thread = t < TB * TB;
   const bool need_corners = MHD && !GLM && P.divb == DIVB_LINDE;
   __shared__ int s_retry;  // some face of this phase needs the guarded FP64 recomputation
   if (t == 0) s_retry = 0;
 #pragma unroll 1
   while (g < gend) {
-  const int b = (int)(g / PL);
-  const int k0 = (int)(g - (long)b * PL);
+  const int col = (int)(g / PL);  // tile column: block*NT + tile
+  const int b = col / NT;
+  const int ti0 = NT == 1 ? 0 : ((col - b * NT) % NTX) * TB;   // tile origin in the block
+  const int tj0 = NT == 1 ? 0 : ((col - b * NT) / NTX) * TB;
+  const int bi = ti0 + ci, bj = NDIM >= 2 ? tj0 + cj : 0;      // the cell role's cell in the block
+  const int k0 = (int)(g - (long)col * PL);
   const int k1 = (int)(k0 + ((gend - g) < (PL - k0) ? (gend - g) : (PL - k0)));
   g += k1 - k0;
   uint32_t stb = 0;  // status of this block's update
@@ -635,39 +677,40 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
     if (cell_thread) {
       double w[NW];
       const int kk = NDIM == 3 ? k + HW : 0;
-      stb |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, ci, cj, kk, w);
+      stb |= load_prim<MHD, NDIR, GLM, NDIM, BN>(A, b, bi, bj, kk, w);
       const int s2 = NDIM == 3 ? ring_slot<HW>(kk) : 0;
 #pragma unroll
       for (int v = 0; v < NW; ++v) tv.center(s2, v, ci, cj) = TF(w[v]);
     }
     // ---- x/y halo strips (and corners for Linde) of plane k
-    constexpr int NHX = BN * H2, NHY = H2 * BN, NHC = H2 * H2;
+    constexpr int NHX = TB * H2, NHY = H2 * TB, NHC = H2 * H2;
     const int nhalo = update ? (need_corners ? NHX + NHY + NHC : NHX + NHY) : 0;
-    if (t < nhalo) {
-      const int h = t;
+    // (small tiles have fewer threads than halo cells: a thread may take two)
+#pragma unroll 1
+    for (int h = t; h < nhalo; h += THREADS) {
       int i, j, stride;
       TF *dst;
       if (h < NHX) {
         j = h / H2;
         const int c = h - j * H2;
-        i = c < HW ? c - HW : c + BN - HW;
+        i = c < HW ? c - HW : c + TB - HW;
         dst = tv.hx + j * H2 + c;
-        stride = BN * H2;
+        stride = TB * H2;
       } else if (h < NHX + NHY) {
-        const int r = (h - NHX) / BN;
-        i = (h - NHX) - r * BN;
-        j = r < HW ? r - HW : r + BN - HW;
-        dst = tv.hy + r * BN + i;
-        stride = H2 * BN;
+        const int r = (h - NHX) / TB;
+        i = (h - NHX) - r * TB;
+        j = r < HW ? r - HW : r + TB - HW;
+        dst = tv.hy + r * TB + i;
+        stride = H2 * TB;
       } else {
         const int r = (h - NHX - NHY) / H2, c = (h - NHX - NHY) - r * H2;
-        i = c < HW ? c - HW : c + BN - HW;
-        j = r < HW ? r - HW : r + BN - HW;
+        i = c < HW ? c - HW : c + TB - HW;
+        j = r < HW ? r - HW : r + TB - HW;
         dst = tv.hc + r * H2 + c;
         stride = H2 * H2;
       }
       double w[NW];
-      stb |= load_prim<MHD, NDIR, GLM, NDIM>(A, b, i, j, k, w);
+      stb |= load_prim<MHD, NDIR, GLM, NDIM, BN>(A, b, i + ti0, j + tj0, k, w);
 #pragma unroll
       for (int v = 0; v < NW; ++v) dst[v * stride] = TF(w[v]);
     }
@@ -676,7 +719,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
     if (update && cell_thread) {
 #pragma unroll
       for (int v = 0; v < NW; ++v) {
-        const size_t o = cell_offset<NDIM>(b, NW, v, ci, cj, k);
+        const size_t o = cell_offset<NDIM>(b, NW, v, bi, bj, k, BN);
         const double win = A.uin[o];
         acc[v] = (A.a_base == 0.0) ? win : A.a_base * A.ubase[o] + A.b_in * win;
       }
@@ -701,8 +744,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
         if (NDIM == 3 && (dsel < 0 || dsel == 2)) {
 #pragma unroll
           for (int o = 0; o < 3; ++o) {
-            base[o] = ring_slot<HW>(k + o - 1) * NW * (BN * BN) + cj * BN + ci;
-            strd[o] = BN * BN;
+            base[o] = ring_slot<HW>(k + o - 1) * NW * (TB * TB) + cj * TB + ci;
+            strd[o] = TB * TB;
           }
           stb |= hancock_dir<MHD, NDIR, GLM, LIM, 2>(smem, base, strd, rdel[2], dxinv[2], cg, P, acc);
         }
@@ -715,32 +758,32 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
     // and the y phase one round of 256 (instead of two rounds of 256 + 16).
     // (With 272 or more threads a phase of 272 faces is one round already;
     // a split sweep has one phase only.)
-    const bool merge_yx = STAGE_THREADS < FB && dsel < 0;
+    const bool merge_yx = THREADS < FB && dsel < 0;
     const int dlo = update ? 0 : (NDIM == 3 && k == k0 - 1 ? 2 : NDIM);
 #pragma unroll 1
     for (int D = dlo; D < NDIM; ++D) {
       if (dsel >= 0 && D != dsel) continue;  // not this sweep's direction (uniform)
-      const int nface = D == 0 ? (merge_yx ? FB + BN : FB) : (D == 1 && !merge_yx ? FB : BN * BN);
+      const int nface = D == 0 ? (merge_yx ? FB + TB : FB) : (D == 1 && !merge_yx ? FB : TB * TB);
       // direction FD and index fl (in that direction's face layout) of face f
       // of this phase
       auto face_dir = [&](int f, int &FD, int &fl) {
-        if (merge_yx && D == 0 && f >= FB) { FD = 1; fl = BN * BN + (f - FB); }
+        if (merge_yx && D == 0 && f >= FB) { FD = 1; fl = TB * TB + (f - FB); }
         else { FD = D; fl = f; }
       };
       // where the flux of variable ov of face f lives
       auto flux_ref = [&](int f, int FD, int fl, int ov) -> TF & {
-        return FD == D ? tv.fb[ov * FB + f] : tv.yx[ov * BN + (fl - BN * BN)];
+        return FD == D ? tv.fb[ov * FB + f] : tv.yx[ov * TB + (fl - TB * TB)];
       };
       // face coordinates and the shared-memory offsets of the 2 HW stencil
       // cells (variable 0) with the per-variable strides
       auto face_at = [&](int FD, int fl, int &fi, int &fj, int *base, int *strd) {
-        if (FD == 0) { fj = fl / (BN + 1); fi = fl - fj * (BN + 1); }
-        else { fj = fl >> 4; fi = fl & (BN - 1); }
+        if (FD == 0) { fj = fl / (TB + 1); fi = fl - fj * (TB + 1); }
+        else { fj = fl / TB; fi = fl - fj * TB; }
 #pragma unroll
         for (int o = 0; o < H2; ++o) {
           if (FD == 2) {
-            base[o] = ring_slot<HW>(k + o - HW + 1) * NW * (BN * BN) + fl;
-            strd[o] = BN * BN;
+            base[o] = ring_slot<HW>(k + o - HW + 1) * NW * (TB * TB) + fl;
+            strd[o] = TB * TB;
           } else {
             tv.addr(slot, FD == 0 ? fi + o - HW : fi, FD == 0 ? fj : fj + o - HW, base[o], strd[o]);
           }
@@ -749,10 +792,10 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
       // level jump across this block face: keep the boundary face flux
       // (store_flux, src/mod_fix_conserve.t:597-648) for the flux fix
       auto capture = [&](int FD, int fi, int fj, const TF *Fr, double sc) {
-        const int pos = FD == 0 ? fi : (FD == 1 ? fj : k + 1);
+        const int pos = FD == 0 ? fi + ti0 : (FD == 1 ? fj + tj0 : k + 1);  // face position in the block
         const int side = pos == 0 ? 0 : (pos == BN ? 1 : -1);
         if (side >= 0 && ((amr_mask >> (2 * FD + side)) & 1)) {
-          const int ta = FD == 0 ? fj : fi, tb = FD == 2 ? fj : k;
+          const int ta = FD == 0 ? fj + tj0 : fi + ti0, tb = FD == 2 ? fj + tj0 : k;
           double *pf = A.pflux + ((size_t)A.gslot[b] * (2 * NDIM) + 2 * FD + side) * NW * (BN * BN);
 #pragma unroll
           for (int v = 0; v < NW; ++v)
@@ -760,7 +803,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
         }
       };
 #pragma unroll 1
-      for (int f = t; f < nface; f += STAGE_THREADS) {
+      for (int f = t; f < nface; f += THREADS) {
         int fi, fj, FD, fl;
         face_dir(f, FD, fl);
         const TF rd = TF(FD == 0 ? rdel[0] : (FD == 1 ? rdel[1] : rdel[2]));
@@ -897,7 +940,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
         // mixed form, or an FP64 face that met a special operand in the
         // unguarded arithmetic), recomputed in FP64 with the guarded forms
         if (s_retry) {
-          for (int f = t; f < nface; f += STAGE_THREADS) {
+          for (int f = t; f < nface; f += THREADS) {
             int FD, fl;
             face_dir(f, FD, fl);
             bool finite = true;
@@ -925,18 +968,18 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
       if (cell_thread) {
         const double sc = FP64 ? 1.0 : (D == 0 ? dxinv[0] : (D == 1 ? dxinv[1] : dxinv[2]));
         if (D == 0) {
-          const int f = cj * (BN + 1) + ci;
+          const int f = cj * (TB + 1) + ci;
 #pragma unroll
           for (int v = 0; v < NW; ++v) {
             if constexpr (FP64) acc[v] = acc[v] + tv.fb[v * FB + f + 1] - tv.fb[v * FB + f];
             else acc[v] = acc[v] + sc * double(tv.fb[v * FB + f + 1]) - sc * double(tv.fb[v * FB + f]);
           }
         } else if (D == 1) {
-          const int f = cj * BN + ci;
+          const int f = cj * TB + ci;
 #pragma unroll
           for (int v = 0; v < NW; ++v) {
             // the face above the top row was computed in the x phase
-            const TF up = (merge_yx && cj == BN - 1) ? tv.yx[v * BN + ci] : tv.fb[v * FB + f + BN];
+            const TF up = (merge_yx && cj == TB - 1) ? tv.yx[v * TB + ci] : tv.fb[v * FB + f + TB];
             if constexpr (FP64) acc[v] = acc[v] + up - tv.fb[v * FB + f];
             else acc[v] = acc[v] + sc * double(up) - sc * double(tv.fb[v * FB + f]);
           }
@@ -972,7 +1015,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
 #pragma unroll
             for (int d = 1; d < NDIM; ++d) mindx = fmin(mindx, dx[d]);
             if (P.glm_alpha < 0.0) {
-              acc[V::PSI] = fabs(P.glm_alpha) * A.uin[cell_offset<NDIM>(b, NW, V::PSI, ci, cj, k)];
+              acc[V::PSI] = fabs(P.glm_alpha) * A.uin[cell_offset<NDIM>(b, NW, V::PSI, bi, bj, k, BN)];
             } else {
               acc[V::PSI] = exp(-(qsrc * cg * P.glm_alpha) / mindx) * acc[V::PSI];
             }
@@ -980,7 +1023,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
               auto nbv = [&](int d, int s, int v) -> double {  // wCT at cell +/- e_d
                 if (d == 0) return double(tv.at(slot, v, ci + s, cj));
                 if (d == 1) return double(tv.at(slot, v, ci, cj + s));
-                return double(tv.ring[(ring_slot<HW>(k + s) * NW + v) * (BN * BN) + cj * BN + ci]);
+                return double(tv.ring[(ring_slot<HW>(k + s) * NW + v) * (TB * TB) + cj * TB + ci]);
               };
 #pragma unroll
               for (int d = 0; d < NDIM; ++d) {
@@ -998,8 +1041,8 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
           } else if (P.divb == DIVB_LINDE) {
             // the reference leaves out the cell layer next to a level-jump
             // face "for AMR stability" (src/mhd/mod_mhd_phys.t:5616-5642)
-            const bool jump_layer = amr_mask && (((amr_mask & 1) && ci == 0) || ((amr_mask & 2) && ci == BN - 1) ||
-                                                 ((amr_mask & 4) && cj == 0) || ((amr_mask & 8) && cj == BN - 1));
+            const bool jump_layer = amr_mask && (((amr_mask & 1) && bi == 0) || ((amr_mask & 2) && bi == BN - 1) ||
+                                                 ((amr_mask & 4) && bj == 0) || ((amr_mask & 8) && bj == BN - 1));
             if constexpr (NDIM == 2) if (!jump_layer) {
               // add_source_linde (src/mhd/mod_mhd_phys.t:5599-5665)
               auto divb_at = [&](int i, int j) -> double {
@@ -1031,7 +1074,7 @@ __global__ void __launch_bounds__(STAGE_THREADS, sizeof(TF) == 8 ? (HaloW<LIM>::
       }
       if (!isfinite(acc[V::RHO]) || !isfinite(acc[V::E])) stb |= ST_NAN;
 #pragma unroll
-      for (int v = 0; v < NW; ++v) A.uout[cell_offset<NDIM>(b, NW, v, ci, cj, k)] = acc[v];
+      for (int v = 0; v < NW; ++v) A.uout[cell_offset<NDIM>(b, NW, v, bi, bj, k, BN)] = acc[v];
     }
     // the next iteration (or the next block) overwrites ring slot (k-1)&3
     // and the halo strips, which the sources above read

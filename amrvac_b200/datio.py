@@ -90,16 +90,18 @@ def forest_flags(leaves, nd, nbase):
 
 
 def write_snapshot(path, leaves, blocks, *, ndim, ndir, physics, gamma, xprobmin, xprobmax, nbase, time=0.0,
-                   it=0, periodic=None, geometry=None, snapshotnext=0, slicenext=0, collapsenext=0, nghost=2):
+                   it=0, periodic=None, geometry=None, snapshotnext=0, slicenext=0, collapsenext=0, nghost=2,
+                   block_nx=16):
     """leaves: (level, ig0, ig1, ig2) per block (0-based ig); blocks: ghosted
     block arrays (nblocks, nw, nz, ny, nx) as Context.download returns them,
-    or interior arrays (nblocks, nw, nz', ny', nx') with 16 cells per
+    or interior arrays (nblocks, nw, nz', ny', nx') with block_nx cells per
     dimension."""
     nd = ndim
+    bnx = int(block_nx)
     blocks = np.asarray(blocks, np.float64)
     nw = blocks.shape[1]
     sl = (slice(None), slice(None)) + tuple(
-        slice(nghost, nghost + 16) if (d < nd and blocks.shape[4 - d] == 16 + 2 * nghost) else slice(None)
+        slice(nghost, nghost + bnx) if (d < nd and blocks.shape[4 - d] == bnx + 2 * nghost) else slice(None)
         for d in (2, 1, 0))
     inner = blocks[sl]
     order = leaf_order(leaves, nd, nbase)
@@ -122,8 +124,8 @@ def write_snapshot(path, leaves, blocks, *, ndim, ndir, physics, gamma, xprobmin
         f64(time)
         f64(*[float(x) for x in xprobmin[:nd]])
         f64(*[float(x) for x in xprobmax[:nd]])
-        i32(*[int(n) * 16 for n in nbase[:nd]])
-        i32(*([16] * nd))
+        i32(*[int(n) * bnx for n in nbase[:nd]])
+        i32(*([bnx] * nd))
         i32(*[1 if p else 0 for p in periodic])
         head.extend(_pad(geometry))
         i32(0)  # staggered
@@ -143,7 +145,7 @@ def write_snapshot(path, leaves, blocks, *, ndim, ndir, physics, gamma, xprobmin
     tree.extend(struct.pack("<" + "i" * (nleafs * nd), *[leaves[b][1 + d] + 1 for b in order for d in range(nd)]))
     offset_offsets = offset_tree + len(tree)
     offset_blocks = offset_offsets + 8 * nleafs
-    rec = 4 * 2 * nd + 8 * nw * 16 ** nd
+    rec = 4 * 2 * nd + 8 * nw * bnx ** nd
     offsets = [offset_blocks + q * rec for q in range(nleafs)]
     with open(path, "wb") as f:
         f.write(header(offset_tree, offset_blocks))
@@ -227,14 +229,15 @@ def save(ctx, path, *, nbase, xprobmin, xprobmax, leaves=None, it=0, time=None, 
         time = ctx.get_time()[2]
     write_snapshot(path, leaves, ctx.download(), ndim=cfg.ndim, ndir=cfg.ndir,
                    physics="mhd" if cfg.physics == 1 else "hd", gamma=cfg.gamma, xprobmin=xprobmin,
-                   xprobmax=xprobmax, nbase=nbase, it=it, time=time, **kw)
+                   xprobmax=xprobmax, nbase=nbase, it=it, time=time, block_nx=ctx.bn, **kw)
 
 
 def ghosted(blocks, nd, nghost=2):
     """Interior blocks as ghosted arrays (zero ghosts) for Context.upload."""
     nb, nw = blocks.shape[:2]
-    g = [16 + 2 * nghost if d < nd else 1 for d in range(3)]
+    bnx = blocks.shape[-1]
+    g = [bnx + 2 * nghost if d < nd else 1 for d in range(3)]
     out = np.zeros((nb, nw, g[2], g[1], g[0]))
-    sl = (slice(None), slice(None)) + tuple(slice(nghost, nghost + 16) if d < nd else slice(None) for d in (2, 1, 0))
+    sl = (slice(None), slice(None)) + tuple(slice(nghost, nghost + bnx) if d < nd else slice(None) for d in (2, 1, 0))
     out[sl] = blocks
     return out

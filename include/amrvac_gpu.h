@@ -308,8 +308,9 @@ int amrvac_gpu_div_points(int n, const double *x, const double *y, double *q, do
  * data regions, a framework's caching allocator) and so cannot create an
  * amrvac_ctx.  Computes what amrvac_gpu_getdt computes — dt from courantpar
  * and cmax_global — over nblocks blocks that the caller holds on the current
- * device in the register layout w_dev[block][var][z][y][x] (16^ndim cells,
- * interior only), with dx the host array [nblocks][3].  Uses only
+ * device in the register layout w_dev[block][var][z][y][x] (block_nx^ndim
+ * cells, interior only; block_nx even, >= 4, the same in every direction),
+ * with dx the host array [nblocks][3].  Uses only
  * cfg->physics, ndim, ndir, block_nx, gamma, typedivbfix, courantpar,
  * type_courant and dtmin.  Runs on `stream` (a cudaStream_t; NULL = the
  * default stream) and synchronises it.

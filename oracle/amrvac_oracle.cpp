@@ -2650,9 +2650,10 @@ enum { NT_BOUNDARY = 0, NT_COARSE = 1, NT_SIBLING = 2, NT_FINE = 3 };
 
 struct AmrGrid {
   long it = 0;  // steps advanced (the parity of a split step's sweep order)
-  State s;      // block state (block_nx 16)
-  State sc;     // coarse representation (block_nx 8)
+  State s;      // block state (block_nx bn)
+  State sc;     // coarse representation (block_nx bn/2)
   int ndim, nb;
+  int bn = 16;  // block edge (block_nx, the same in every direction)
   int nbase[3];
   double xmin[3], xmax[3];
   int bc[6];                                  // ORC_BC_* per side
@@ -2663,21 +2664,21 @@ struct AmrGrid {
   std::vector<double> psc;                    // [b] coarse representation
   std::vector<std::vector<double>> pflux;     // [b*6 + 2*d + side]
   size_t bsize, csize;
-  double dx(int b, int d) const { return (xmax[d] - xmin[d]) / (nbase[d] * 16.0 * double(1 << (level[b] - 1))); }
-  double bxmin(int b, int d) const { return xmin[d] + ig[3 * b + d] * 16.0 * dx(b, d); }
+  double dx(int b, int d) const { return (xmax[d] - xmin[d]) / (nbase[d] * double(bn) * double(1 << (level[b] - 1))); }
+  double bxmin(int b, int d) const { return xmin[d] + ig[3 * b + d] * double(bn) * dx(b, d); }
 };
 
 inline int q27(const int *dd) { return (dd[0] + 1) + 3 * ((dd[1] + 1) + 3 * (dd[2] + 1)); }
 
-// Index maps of init_bc (1-based, nghostcells 2, block 16, coarse 8).
+// Index maps of init_bc (1-based, nghostcells 2, block bn, coarse bn/2).
 struct AmrMaps {
   int srlS[3][2], srlR[3][2];   // by i+1: ixS_srl / ixR_srl
   int rS[3][2], rR[4][2];       // ixS_r by i+1, ixR_r by n_inc 0..3
   int pS[4][2], pR[4][2];       // ixS_p, ixR_p by inc / n_inc 0..3
 };
 
-inline AmrMaps amr_maps() {
-  const int ng = 2, nx = 16, nxCo = 8, ixMmin = ng + 1, ixMmax = ng + nx, ixGmax = nx + 2 * ng;
+inline AmrMaps amr_maps(int bn) {
+  const int ng = 2, nx = bn, nxCo = bn / 2, ixMmin = ng + 1, ixMmax = ng + nx, ixGmax = nx + 2 * ng;
   const int ixCoMmin = ng + 1, ixCoMmax = ng + nxCo;
   const int ngCo = (ng + 1) / 2, io = 2;
   AmrMaps m;
@@ -2713,7 +2714,7 @@ inline void copy_box(const Geo &ga, const double *a, const int lo_a[3], const Ge
 void amr_getbc(AmrGrid &G, std::vector<double> &reg) {
   const int nd = G.ndim, nw = G.s.x.nw;
   const Geo &g = G.s.g, &gc = G.sc.g;
-  const AmrMaps M = amr_maps();
+  const AmrMaps M = amr_maps(G.bn);
   auto has = [&](int b, int t) {
     for (int q = 0; q < 27; ++q) if (q != 13 && G.ntype[b * 27 + q] == t) return true;
     return false;
@@ -2732,10 +2733,11 @@ void amr_getbc(AmrGrid &G, std::vector<double> &reg) {
     const double *w = &reg[G.bsize * b];
     double *wc = &G.psc[G.csize * b];
     const double cofi = 1.0 / double(1 << nd);
+    const int half = G.bn / 2;
     for (int iw = 0; iw < nw; ++iw)
-      for (int kc = 0; kc < (nd > 2 ? 8 : 1); ++kc)
-        for (int jc = 0; jc < (nd > 1 ? 8 : 1); ++jc)
-          for (int icc = 0; icc < 8; ++icc) {
+      for (int kc = 0; kc < (nd > 2 ? half : 1); ++kc)
+        for (int jc = 0; jc < (nd > 1 ? half : 1); ++jc)
+          for (int icc = 0; icc < half; ++icc) {
             const int i0 = 2 + 2 * icc, j0 = nd > 1 ? 2 + 2 * jc : 0, k0 = nd > 2 ? 2 + 2 * kc : 0;
             double sum = 0.0;
             bool first = true;
@@ -2898,9 +2900,9 @@ void amr_store_flux(AmrGrid &G, int b, const std::vector<Arr<double>> &fC) {
       int ta = -1, tb = -1;
       for (int e = 0; e < nd; ++e) if (e != d) { if (ta < 0) ta = e; else tb = e; }
       (void)t1; (void)t2;
-      const int iface = side ? 17 : 1;  // 0-based face index: right face of cell iface
+      const int iface = side ? G.bn + 1 : 1;  // 0-based face index: right face of cell iface
       if (t == NT_FINE) {
-        const int n1 = ta >= 0 ? 16 : 1, n2 = tb >= 0 ? 16 : 1;
+        const int n1 = ta >= 0 ? G.bn : 1, n2 = tb >= 0 ? G.bn : 1;
         pf.assign((size_t)nw * n1 * n2, 0.0);
         for (int iw = 0; iw < nw; ++iw)
           for (int b2 = 0; b2 < n2; ++b2)
@@ -2913,7 +2915,7 @@ void amr_store_flux(AmrGrid &G, int b, const std::vector<Arr<double>> &fC) {
               pf[((size_t)iw * n2 + b2) * n1 + a1] = side ? f : -f;
             }
       } else if (t == NT_COARSE) {
-        const int n1 = ta >= 0 ? 8 : 1, n2 = tb >= 0 ? 8 : 1;
+        const int n1 = ta >= 0 ? G.bn / 2 : 1, n2 = tb >= 0 ? G.bn / 2 : 1;
         pf.assign((size_t)nw * n1 * n2, 0.0);
         for (int iw = 0; iw < nw; ++iw)
           for (int b2 = 0; b2 < n2; ++b2)
@@ -2952,10 +2954,10 @@ void amr_fix_conserve(AmrGrid &G, std::vector<double> &reg) {
         if (G.ntype[b * 27 + q] != NT_FINE) continue;
         int ta = -1, tb = -1;
         for (int e = 0; e < nd; ++e) if (e != d) { if (ta < 0) ta = e; else tb = e; }
-        const int ix = side ? 17 : 2;  // 0-based boundary cell
+        const int ix = side ? G.bn + 1 : 2;  // 0-based boundary cell
         double *w = &reg[G.bsize * b];
         const std::vector<double> &pc = G.pflux[b * 6 + 2 * d + side];
-        const int n1 = ta >= 0 ? 16 : 1, n2 = tb >= 0 ? 16 : 1;
+        const int n1 = ta >= 0 ? G.bn : 1, n2 = tb >= 0 ? G.bn : 1;
         for (int iw = 0; iw < nw; ++iw)
           for (int b2 = 0; b2 < n2; ++b2)
             for (int a1 = 0; a1 < n1; ++a1) {
@@ -2976,14 +2978,15 @@ void amr_fix_conserve(AmrGrid &G, std::vector<double> &reg) {
             const int cbits = (ic[0] - 1) + 2 * (nd > 1 ? ic[1] - 1 : 0) + 4 * (nd > 2 ? ic[2] - 1 : 0);
             const int chd = G.child[(b * 27 + q) * 8 + cbits];
             const std::vector<double> &pf = G.pflux[chd * 6 + 2 * d + (1 - side)];
-            const int m1 = ta >= 0 ? 8 : 1, m2 = tb >= 0 ? 8 : 1;
+            const int half = G.bn / 2;
+            const int m1 = ta >= 0 ? half : 1, m2 = tb >= 0 ? half : 1;
             for (int iw = 0; iw < nw; ++iw)
               for (int b2 = 0; b2 < m2; ++b2)
                 for (int a1 = 0; a1 < m1; ++a1) {
                   int c[3] = {0, 0, 0};
                   c[d] = ix;
-                  if (ta >= 0) c[ta] = 2 + (c1 - 1) * 8 + a1;
-                  if (tb >= 0) c[tb] = 2 + (c2 - 1) * 8 + b2;
+                  if (ta >= 0) c[ta] = 2 + (c1 - 1) * half + a1;
+                  if (tb >= 0) c[tb] = 2 + (c2 - 1) * half + b2;
                   double &v = w[g.idx(c[0], c[1], c[2]) + g.cells * (size_t)iw];
                   v = v + pf[((size_t)iw * m2 + b2) * m1 + a1] * cofi;
                 }
@@ -3039,8 +3042,9 @@ orc_amr *orc_amr_create(const orc_cfg *cfg, const int *nbase, const double *xpro
   AmrGrid *G = new AmrGrid();
   for (int q = 0; q < 6; ++q) G->bc[q] = (bc && q < 2 * cfg->ndim) ? bc[q] : ORC_BC_PERIODIC;
   G->s = make_state(*cfg);
+  G->bn = cfg->block_nx[0];
   orc_cfg c8 = *cfg;
-  for (int d = 0; d < 3; ++d) c8.block_nx[d] = d < cfg->ndim ? 8 : 1;
+  for (int d = 0; d < 3; ++d) c8.block_nx[d] = d < cfg->ndim ? G->bn / 2 : 1;
   G->sc = make_state(c8);
   G->ndim = cfg->ndim;
   G->nb = nleaf;
@@ -3247,16 +3251,17 @@ orc_amr *orc_amr_remap(const orc_amr *old, int nleaf, const int *leaf, const int
       std::memcpy(wn, &O->reg[0][O->bsize * o[1]], sizeof(double) * O->bsize);
       continue;
     }
+    const int bn = O->bn, half = bn / 2;
     for (int iw = 0; iw < nw; ++iw)
-      for (int k = 0; k < (nd > 2 ? 16 : 1); ++k)
-        for (int j = 0; j < (nd > 1 ? 16 : 1); ++j)
-          for (int i = 0; i < 16; ++i) {
+      for (int k = 0; k < (nd > 2 ? bn : 1); ++k)
+        for (int j = 0; j < (nd > 1 ? bn : 1); ++j)
+          for (int i = 0; i < bn; ++i) {
             const int F[3] = {i, j, k};
             double val;
             if (o[0] == 1) {
               const double *wc = &O->reg[0][O->bsize * o[1]];
               int co[3] = {0, 0, 0};  // 0-based ghosted index of the coarse cell
-              for (int d = 0; d < nd; ++d) co[d] = 2 + 8 * ((o[2] >> d) & 1) + (F[d] >> 1);
+              for (int d = 0; d < nd; ++d) co[d] = 2 + half * ((o[2] >> d) & 1) + (F[d] >> 1);
               auto wco = [&](int a, int bb, int cc) { return wc[g.idx(a, bb, cc) + g.cells * (size_t)iw]; };
               const double c0 = wco(co[0], co[1], co[2]);
               double slope[3] = {0, 0, 0};
@@ -3274,15 +3279,15 @@ orc_amr *orc_amr_remap(const orc_amr *old, int nleaf, const int *leaf, const int
               for (int d = 0; d < nd; ++d) val = val + slope[d] * (0.5 * (double(F[d] & 1) - 0.5));
             } else {
               int cb = 0;
-              for (int d = 0; d < nd; ++d) cb |= (F[d] >> 3) << d;
+              for (int d = 0; d < nd; ++d) cb |= (F[d] >= half ? 1 : 0) << d;
               const double *wf = &O->reg[0][O->bsize * o[1 + cb]];
               double sum = 0.0;
               bool first = true;
               for (int kk = 0; kk < (nd > 2 ? 2 : 1); ++kk)
                 for (int jj = 0; jj < (nd > 1 ? 2 : 1); ++jj)
                   for (int ii = 0; ii < 2; ++ii) {
-                    const int fi = 2 + 2 * (F[0] & 7) + ii, fj = nd > 1 ? 2 + 2 * (F[1] & 7) + jj : 0,
-                              fk = nd > 2 ? 2 + 2 * (F[2] & 7) + kk : 0;
+                    const int fi = 2 + 2 * (F[0] % half) + ii, fj = nd > 1 ? 2 + 2 * (F[1] % half) + jj : 0,
+                              fk = nd > 2 ? 2 + 2 * (F[2] % half) + kk : 0;
                     const double x = wf[g.idx(fi, fj, fk) + g.cells * (size_t)iw];
                     sum = first ? x : sum + x;
                     first = false;

@@ -50,6 +50,14 @@ LOGS = [
     "tests/hd/blast_wave_Cartesian_2D/correct_output/bw_2d_rk4_tvdlf_cada.log",
     "tests/hd/blast_wave_Cartesian_2D/correct_output/bw_2d_2step_tvdlf_mm.log",
     "tests/hd/blast_wave_Cartesian_2D/correct_output/bw_2d_2step_tvdmu_al.log",
+    # 3-D multi-level with 8^3 blocks (block_nx 8), cont boundaries
+    "tests/mhd/blast_wave_Cartesian_3D/correct_output/bw_3d_3step_hlld_cada.log",
+    "tests/mhd/blast_wave_Cartesian_3D/correct_output/bw_3d_3step_hll_cada.log",
+    "tests/mhd/blast_wave_Cartesian_3D/correct_output/bw_3d_3step_hll_ko.log",
+    "tests/mhd/blast_wave_Cartesian_3D/correct_output/bw_3d_4step_hll_mc.log",
+    "tests/mhd/blast_wave_Cartesian_3D/correct_output/bw_3d_4step_hllc_ko.log",
+    "tests/mhd/blast_wave_Cartesian_3D/correct_output/bw_3d_rk4_tvdlf_cada.log",
+    "tests/mhd/blast_wave_Cartesian_3D/correct_output/bw_3d_2step_tvdlf_mm.log",
 ]
 
 

@@ -7,6 +7,9 @@
 * The flux correction makes the multi-level update conservative: totals of
   every conserved variable stay constant to rounding on a periodic domain.
 * A hierarchy refined everywhere is the uniform finer grid, bit for bit.
+
+Each holds for blocks of 16 and of 8 cells per edge (block_nx; the
+reference's 3-D blast test runs 8^3 blocks).
 """
 import numpy as np
 import pytest
@@ -16,6 +19,7 @@ from tests import _amr as A
 
 def _cfg(O, nd, **kw):
     base = dict(physics="hd", ndim=nd, gamma=1.4, flux_scheme="hllc", limiter="vanleer", courantpar=0.8)
+    # (block_nx passes through **kw)
     base.update(kw)
     return O.make_cfg(**base)
 
@@ -45,20 +49,21 @@ def _lin(nd):
 
 
 @pytest.mark.parametrize("nd", [2, 3])
-def test_ghost_cells_exact_for_linear_data(oracle_lib, nd):
+@pytest.mark.parametrize("bn", [16, 8])
+def test_ghost_cells_exact_for_linear_data(oracle_lib, nd, bn):
     O = oracle_lib
     leaves = _leaves(nd, levels=3 if nd == 2 else 2)
     assert len({l[0] for l in leaves}) == (3 if nd == 2 else 2)
-    c = _cfg(O, nd)
+    c = _cfg(O, nd, block_nx=bn)
     nb = _nbase(nd)
     g = O.AmrGrid(c, nb, [0.0] * nd, [1.0] * nd, leaves)
-    blocks = A.fill_blocks(leaves, nd, nb, _lin(nd), "hd", nd, 1.4, conserved=True)
+    blocks = A.fill_blocks(leaves, nd, nb, _lin(nd), "hd", nd, 1.4, conserved=True, bn=bn)
     for b in range(len(leaves)):
         g.set_block(b, blocks[b])
     # scramble the ghost cells so that only getbc can make them right
     for b in range(len(leaves)):
         w = blocks[b].copy()
-        sl = (slice(None),) + tuple(slice(2, 18) if d < nd else slice(None) for d in (2, 1, 0))
+        sl = (slice(None),) + tuple(slice(2, 2 + bn) if d < nd else slice(None) for d in (2, 1, 0))
         z = np.full_like(w, -7.0)
         z[sl] = w[sl]
         g.set_block(b, z)
@@ -90,20 +95,21 @@ def _periodic(nd):
 
 
 @pytest.mark.parametrize("nd", [2, 3])
-def test_flux_fix_conserves(oracle_lib, nd):
+@pytest.mark.parametrize("bn", [16, 8])
+def test_flux_fix_conserves(oracle_lib, nd, bn):
     O = oracle_lib
     leaves = _leaves(nd, levels=3 if nd == 2 else 2)
-    c = _cfg(O, nd)
+    c = _cfg(O, nd, block_nx=bn)
     nb = _nbase(nd)
     g = O.AmrGrid(c, nb, [0.0] * nd, [1.0] * nd, leaves)
-    blocks = A.fill_blocks(leaves, nd, nb, _periodic(nd), "hd", nd, 1.4)
+    blocks = A.fill_blocks(leaves, nd, nb, _periodic(nd), "hd", nd, 1.4, bn=bn)
     for b in range(len(leaves)):
         g.set_block(b, blocks[b])
     g.getbc()
-    sl = (slice(None),) + tuple(slice(2, 18) if d < nd else slice(None) for d in (2, 1, 0))
+    sl = (slice(None),) + tuple(slice(2, 2 + bn) if d < nd else slice(None) for d in (2, 1, 0))
 
     def totals():
-        return sum(g.get_block(b)[sl].reshape(nd + 2, -1).sum(axis=1) * A.block_volume(l, nd, nb)
+        return sum(g.get_block(b)[sl].reshape(nd + 2, -1).sum(axis=1) * A.block_volume(l, nd, nb, bn=bn)
                    for b, l in enumerate(leaves))
     t0 = totals()
     for _ in range(4 if nd == 2 else 2):
@@ -113,15 +119,16 @@ def test_flux_fix_conserves(oracle_lib, nd):
     assert np.all(np.abs(t1 - t0) <= 1e-13 * np.abs(t0).max()), (t0, t1)
 
 
-def test_refined_everywhere_is_the_uniform_grid(oracle_lib):
+@pytest.mark.parametrize("bn", [16, 8])
+def test_refined_everywhere_is_the_uniform_grid(oracle_lib, bn):
     O = oracle_lib
     nd = 2
     leaves = A.build_leaves(nd, [2, 2], 2, lambda c, lv: True)
     assert all(l[0] == 2 for l in leaves) and len(leaves) == 16
-    c = _cfg(O, nd)
+    c = _cfg(O, nd, block_nx=bn)
     g = O.AmrGrid(c, [2, 2], [0.0, 0.0], [1.0, 1.0], leaves)
-    blocks = A.fill_blocks(leaves, nd, [2, 2], _periodic(nd), "hd", nd, 1.4)
-    u = O.Grid(c, [64, 64], [0.0, 0.0], [1.0, 1.0], ["periodic"] * 4)
+    blocks = A.fill_blocks(leaves, nd, [2, 2], _periodic(nd), "hd", nd, 1.4, bn=bn)
+    u = O.Grid(c, [4 * bn, 4 * bn], [0.0, 0.0], [1.0, 1.0], ["periodic"] * 4)
     order = {}
     for b, l in enumerate(leaves):
         g.set_block(b, blocks[b])

@@ -61,11 +61,48 @@ def test_unsupported_configurations_are_refused_without_gpu(lib):
     bad = [make_cfg(physics="mhd", ndim=3, typedivbfix="glm", flux_scheme="tvdmu", dimsplit=True),
            make_cfg(physics="hd", ndim=2, flux_scheme="hlld")]
     c = make_cfg(physics="hd", ndim=2)
-    c.block_nx[0] = 8
+    c.block_nx[0] = 8  # block_nx must be the same in every direction
     bad.append(c)
+    # block edges the library has no kernels for, and what only block_nx 16 runs
+    bad += [make_cfg(physics="hd", ndim=2, block_nx=14), make_cfg(physics="hd", ndim=3, block_nx=6),
+            make_cfg(physics="hd", ndim=2, block_nx=8, precision="mixed"),
+            make_cfg(physics="hd", ndim=2, block_nx=12, limiter="mp5"),
+            make_cfg(physics="mhd", ndim=2, block_nx=10, flux_scheme="tvdmu", dimsplit=True, typedivbfix="none")]
     for cfg in bad:
         r = lib.amrvac_gpu_create(ctypes.byref(cfg), ctypes.byref(h))
         assert r == _lib.E_UNSUPPORTED, lib.amrvac_gpu_last_error()
+
+
+def test_block_nx_from_par_file(tmp_path):
+    """block_nx1..3 of &meshlist reach the configuration (the reference's own
+    3-D blast test runs 8^3 blocks); unequal edges are refused."""
+    from amrvac_b200.config import config_from_par
+
+    def config_from_par_text(text):
+        f = tmp_path / "t.par"
+        f.write_text(text)
+        return config_from_par([str(f)])
+    base = """
+ &methodlist
+        time_stepper = 'threestep'
+        flux_scheme = 20*'hll'
+        limiter = 20*'koren'
+ /
+ &meshlist
+        domain_nx1=16
+        domain_nx2=16
+        domain_nx3=16
+        block_nx1=8
+        block_nx2=8
+        block_nx3=%d
+ /
+ &mhd_list
+ /
+"""
+    rc = config_from_par_text(base % 8)
+    assert list(rc.cfg.block_nx) == [8, 8, 8]
+    with pytest.raises(ValueError):
+        config_from_par_text(base % 16)
 
 
 def test_par_namelist_parser():

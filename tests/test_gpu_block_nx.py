@@ -1,0 +1,217 @@
+"""block_nx other than 16 on the GPU against the oracle.
+
+The reference accepts any even block_nx >= 4 (src/io/mod_input_output.t:
+1494-1503); its own regression tests run 8^3 (3-D MHD blast), 10^3 (3-D
+Kelvin-Helmholtz) and 12^2 (2-D Riemann) blocks.  The library runs block
+edges 8, 10, 12, 16 and 32: a stage CTA takes the whole block plane up to 16
+cells per edge and 16 x 16 tiles of a 32-cell plane.  Checked here, per block
+edge, on uniform and multi-level grids: the ghost fill of the download bit
+for bit, one stage and one full step cell by cell (tests/_parity.py; the bar
+is 1e-12, or the oracle's own response to one ulp of input noise where that
+is larger), and the level-jump ghost cells and steps of a two-level grid.
+"""
+import numpy as np
+import pytest
+
+from tests import _amr as A
+from tests import _problems as P
+from tests._parity import one_ulp_noise, percell_err
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+CASES = {
+    "hd2_hllc_vanleer": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hllc", limiter="vanleer"),
+    "hd3_hll_minmod_cont": dict(physics="hd", ndim=3, gamma=1.4, flux_scheme="hll", limiter="minmod",
+                                bc="cont"),
+    "mhd3_hlld_cada3_glm": dict(physics="mhd", ndim=3, flux_scheme="hlld", limiter="cada3", typedivbfix="glm"),
+    "mhd25_hll_cada3_linde_cmaxmean": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hll", limiter="cada3",
+                                           typedivbfix="linde", typeboundspeed="cmaxmean"),
+    "mhd3_hllc_koren_linde": dict(physics="mhd", ndim=3, flux_scheme="hllc", limiter="koren", typedivbfix="linde"),
+    "hd2_tvdlf_koren_hancock": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="tvdlf", limiter="koren",
+                                    time_stepper="twostep"),
+}
+BLOCK_NX = [8, 10, 12, 32]
+
+
+def _cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _maxrel(a, b):
+    return percell_err(a, b, var_axis=1)
+
+
+def _grids(O, name, bn, noisy=False):
+    """(oracle grid, blocks, kwargs) on a domain of two blocks per direction."""
+    kw = dict(CASES[name])
+    bc = kw.pop("bc", "periodic")
+    ndim = kw["ndim"]
+    ndir = kw.get("ndir", ndim)
+    n = 2 * bn
+    ok = dict(kw)
+    ok["divb"] = ok.pop("typedivbfix", "none")
+    ocfg = O.make_cfg(block_nx=bn, **ok)
+    prim = P.random_smooth(kw["physics"], ndim, ndir, n, glm=ok["divb"] == "glm")
+    blocks = P.to_blocks(P.prim_to_cons(prim, kw["physics"], ndir, ocfg.gamma), ndim, bn=bn)
+    if noisy:
+        blocks = one_ulp_noise(blocks)
+    og = O.Grid(ocfg, [n] * ndim, [0.0] * ndim, [1.0] * ndim, [bc] * (2 * ndim))
+    for ib in range(og.nblocks):
+        og.set_block(ib, blocks[ib])
+    og.getbc()
+    return og, blocks, kw, bc, ocfg
+
+
+def _setup(O, name, bn):
+    from amrvac_b200 import Context, make_cfg
+    og, blocks, kw, bc, ocfg = _grids(O, name, bn)
+    nd = kw["ndim"]
+    ctx = Context(make_cfg(block_nx=bn, typeboundary=[bc] * (2 * nd), **kw))
+    ctx.set_uniform_grid([2 * bn] * nd, [0.0] * nd, [1.0] * nd)
+    assert ctx.nblocks == og.nblocks == 2 ** nd
+    ctx.upload(blocks)
+    return og, ctx, ocfg
+
+
+def _interior(blocks, nd, bn):
+    return blocks[(slice(None), slice(None)) + tuple(slice(2, 2 + bn) if d < nd else slice(None) for d in (2, 1, 0))]
+
+
+@pytest.mark.parametrize("bn", BLOCK_NX)
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_ghost_fill_bit_exact(oracle_lib, name, bn):
+    _cuda()
+    og, ctx, _ = _setup(oracle_lib, name, bn)
+    ref = np.array([og.get_block(ib) for ib in range(og.nblocks)])
+    assert np.array_equal(ctx.download(), ref)
+
+
+@pytest.mark.parametrize("bn", BLOCK_NX)
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_full_step_matches_oracle(oracle_lib, name, bn):
+    """setdt and all stages of the time stepper on blocks of bn cells."""
+    _cuda()
+    O = oracle_lib
+    og, ctx, ocfg = _setup(O, name, bn)
+    nd = ocfg.ndim
+    dt_ref, cg_ref = og.getdt()
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.step()
+    dt, cg, _ = ctx.get_time()
+    assert abs(dt - dt_ref) <= 1e-13 * dt_ref and abs(cg - cg_ref) <= 1e-13 * cg_ref
+    og.advance(dt_ref, cg_ref)
+    gn = _grids(O, name, bn, noisy=True)[0]
+    gn.advance(dt_ref, cg_ref)
+    got = _interior(ctx.download(), nd, bn)
+    ref = _interior(np.array([og.get_block(ib) for ib in range(og.nblocks)]), nd, bn)
+    noise = _maxrel(_interior(np.array([gn.get_block(ib) for ib in range(gn.nblocks)]), nd, bn), ref)
+    err = _maxrel(got, ref)
+    assert err <= max(RTOL, noise), f"{name} block_nx {bn}: {err:.3e} (oracle self-noise {noise:.3e})"
+    assert ctx.status() == 0
+
+
+@pytest.mark.parametrize("bn", [8, 32])
+@pytest.mark.parametrize("name", ["mhd3_hlld_cada3_glm", "hd2_hllc_vanleer"])
+def test_stage_zchunks_match_oracle(oracle_lib, name, bn):
+    """One stage with every work distribution of the 3-D kernel (z-chunks
+    dividing the block edge, persistent plane ranges)."""
+    _cuda()
+    O = oracle_lib
+    og, ctx, ocfg = _setup(O, name, bn)
+    nd = ocfg.ndim
+    dt, cg = og.getdt()
+    dt *= 0.5
+    ref = []
+    for ib in range(og.nblocks):
+        w = og.get_block(ib)
+        wn = w.copy()
+        O.finite_volume(ocfg, w, wn, dt, og.dx(), cg)
+        ref.append(wn)
+    ref = _interior(np.array(ref), nd, bn)
+    ctx.set_cmax_global(cg)
+    for z in ([0, bn, bn // 2, bn // 4] if nd == 3 else [0, bn]):
+        ctx.set_zchunk(z)
+        assert ctx.advect1("ps", "ps1", 1.0, dt) == 0
+        err = _maxrel(_interior(ctx.download("ps1"), nd, bn), ref)
+        assert err <= RTOL, (name, bn, z, err)
+
+
+def _amr_field(nd, physics, glm):
+    def f(X, Y, Z):
+        nw = (nd + 2) if physics == "hd" else (2 * nd + 2 + int(glm))
+        out = np.zeros((nw,) + X.shape)
+        s = np.sin(2 * np.pi * X) * np.cos(2 * np.pi * Y) * (np.cos(2 * np.pi * Z) if nd > 2 else 1)
+        blob = np.exp(-((X - 0.45) ** 2 + (Y - 0.45) ** 2 + ((Z - 0.45) ** 2 if nd > 2 else 0)) / 0.01)
+        out[0] = 1.0 + 0.3 * s + 2.0 * blob
+        out[1] = 0.5 + 0.2 * np.cos(2 * np.pi * Y)
+        out[2] = -0.3 + 0.2 * np.sin(2 * np.pi * X)
+        if nd > 2:
+            out[3] = 0.1 * np.sin(2 * np.pi * Y)
+        out[nd + 1] = 1.0 + 0.2 * s + 3.0 * blob
+        if physics == "mhd":
+            out[nd + 2] = 0.3 + 0.1 * np.cos(2 * np.pi * Y)
+            out[nd + 3] = 0.2 + 0.1 * np.sin(2 * np.pi * X)
+            if nd > 2:
+                out[nd + 4] = 0.1
+            if glm:
+                out[2 * nd + 2] = 0.01 * np.sin(2 * np.pi * (X + Y))
+        return out
+    return f
+
+
+@pytest.mark.parametrize("case", [
+    ("hd2_hllc_vanleer", 2, dict(physics="hd", flux_scheme="hllc", limiter="vanleer")),
+    ("mhd3_hlld_cada3_glm", 3, dict(physics="mhd", flux_scheme="hlld", limiter="cada3", typedivbfix="glm")),
+    ("mhd3_hll_koren_linde", 3, dict(physics="mhd", flux_scheme="hll", limiter="koren", typedivbfix="linde")),
+], ids=lambda c: c[0])
+def test_two_level_grid_block_nx_8(oracle_lib, case):
+    """A static two-level grid of 8-cell blocks: level-jump ghost cells
+    (restriction, prolongation) and two full steps with the flux fix."""
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    O = oracle_lib
+    name, nd, kw = case
+    bn = 8
+    nb = [4] * nd
+
+    def ref_fn(c, lv):
+        return np.linalg.norm(c - 0.45) < 0.3
+    leaves = A.build_leaves(nd, nb, 2, ref_fn)
+    assert len({l[0] for l in leaves}) == 2
+    base = dict(ndim=nd, gamma=5.0 / 3.0 if kw["physics"] == "mhd" else 1.4, courantpar=0.6, **kw)
+    ok = dict(base)
+    ok["divb"] = ok.pop("typedivbfix", "none")
+    ocfg = O.make_cfg(block_nx=bn, **ok)
+    glm = ok["divb"] == "glm"
+    blocks = A.fill_blocks(leaves, nd, nb, _amr_field(nd, kw["physics"], glm), kw["physics"], nd, base["gamma"], bn=bn)
+    og = O.AmrGrid(ocfg, nb, [0.0] * nd, [1.0] * nd, leaves)
+    gn = O.AmrGrid(ocfg, nb, [0.0] * nd, [1.0] * nd, leaves)
+    noisy = one_ulp_noise(np.asarray(blocks))
+    for b in range(len(leaves)):
+        og.set_block(b, blocks[b])
+        gn.set_block(b, noisy[b])
+    og.getbc()
+    gn.getbc()
+    ctx = Context(make_cfg(block_nx=bn, **base))
+    ctx.set_amr_grid(leaves, nb, [0.0] * nd, [1.0] * nd)
+    ctx.upload(blocks)
+    assert ctx.amr_slots > 0
+    ref = np.array([og.get_block(b) for b in range(len(leaves))])
+    assert _maxrel(ctx.download(), ref) <= 1e-13
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    for n in range(2):
+        dt, cm = og.getdt()
+        ctx.step()
+        assert abs(ctx.get_time()[0] - dt) <= 1e-13 * dt
+        og.advance(dt, cm)
+        gn.advance(dt, cm)
+        got = _interior(ctx.download(), nd, bn)
+        ref = _interior(np.array([og.get_block(b) for b in range(len(leaves))]), nd, bn)
+        noise = _maxrel(_interior(np.array([gn.get_block(b) for b in range(len(leaves))]), nd, bn), ref)
+        err = _maxrel(got, ref)
+        assert err <= max(RTOL, noise), (name, n, err, noise)
+    assert ctx.status() == 0

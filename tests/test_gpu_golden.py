@@ -75,39 +75,43 @@ def _ot2d_prim(nw):
     return f
 
 
-def _amr_log_row(blocks, leaves, nbase, t, nw):
+def _amr_log_row(blocks, leaves, nbase, t, nw, nd=2, bn=16, xlen=1.0):
     """printlog_regression_test: volume averages of w and w**2 over the leaves."""
     s1, s2, vol = np.zeros(nw), np.zeros(nw), 0.0
+    sl = (slice(None, nw),) + tuple(slice(2, 2 + bn) if d < nd else slice(None) for d in (2, 1, 0))
     for b, lf in enumerate(leaves):
-        dv = (1.0 / (nbase[0] * 16 * (1 << (lf[0] - 1)))) * (1.0 / (nbase[1] * 16 * (1 << (lf[0] - 1))))
-        w = blocks[b][:nw, 0, 2:18, 2:18].reshape(nw, -1)
+        dv = 1.0
+        for d in range(nd):
+            dv *= xlen / (nbase[d] * bn * (1 << (lf[0] - 1)))
+        w = blocks[b][sl].reshape(nw, -1)
         s1 += w.sum(axis=1) * dv
         s2 += (w * w).sum(axis=1) * dv
-        vol += 256 * dv
+        vol += bn ** nd * dv
     return np.concatenate([[t], s1 / vol, s2 / vol])
 
 
 def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsave=1.0e-3, levels=3, xmax=1.0,
-                    bc="periodic"):
-    """The reference's time loop on a 2-D multi-level grid over [0, xmax]^2:
-    settree, then setdt + advance + resettree every step, a log row at every
-    dtsave."""
+                    bc="periodic", nd=2, bn=16):
+    """The reference's time loop on a multi-level grid over [0, xmax]^nd with
+    blocks of bn^nd cells: settree, then setdt + advance + resettree every
+    step, a log row at every dtsave."""
     from tests import _amr as A
     from amrvac_b200 import Context, make_cfg
     from amrvac_b200.amr import Tree, initial_hierarchy, lohner_flags
     nw = len(weight)
-    xmin, xmax = [0.0, 0.0], [xmax, xmax]
-    cfg = make_cfg(physics=physics, ndim=2, ndir=2, typeboundary=[bc] * 4, **kw)
+    xlen = xmax
+    xmin, xmax = [0.0] * nd, [xmax] * nd
+    cfg = make_cfg(physics=physics, ndim=nd, ndir=nd, typeboundary=[bc] * (2 * nd), block_nx=bn, **kw)
     ctx = Context(cfg)
     lkw = dict(refine_threshold=threshold, derefine_ratio=0.125, amr_wavefilter=1.0e-2)
 
     def init(tree):
-        return A.fill_blocks(tree.leaves, 2, nb, prim_fn, physics, 2, cfg.gamma, xmin, xmax)
+        return A.fill_blocks(tree.leaves, nd, nb, prim_fn, physics, nd, cfg.gamma, xmin, xmax, bn=bn)
 
     def err(tree, blocks):
         r, c, _ = lohner_flags(ctx, tree, blocks, xmin, xmax, weight, **lkw)
         return r, c
-    tree, blocks = initial_hierarchy(Tree(2, nb, levels, periodic=[bc == "periodic"] * 2), init, err)
+    tree, blocks = initial_hierarchy(Tree(nd, nb, levels, periodic=[bc == "periodic"] * nd), init, err)
     ctx.set_amr_grid(tree.leaves, nb, xmin, xmax)
     ctx.upload(blocks)
     ctx.set_time(0.0, time_max, dtsave)
@@ -119,7 +123,7 @@ def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsav
         dt, cg, t = ctx.get_time()
         if t >= tsavelast + dtsave - 1e-12:
             tsavelast = t
-            rows.append(_amr_log_row(ctx.download(), ctx.amr_leaves(), nb, t, nw))
+            rows.append(_amr_log_row(ctx.download(), ctx.amr_leaves(), nb, t, nw, nd, bn, xlen))
         if t >= time_max - 1e-10:
             break
     assert ctx.status() == 0
@@ -225,6 +229,51 @@ def test_blast_wave_2d_amr_golden_log_gpu(oracle_lib, name, kw):
     weight = np.array([0.5, 0.0, 0.0, 0.5])
     rows = _run_amr_golden("hd", [2, 2], _bw2d_prim, weight, 0.1, kw, time_max=0.05, xmax=2.0, bc="cont")
     gold = oracle_lib.read_log(os.path.join(GOLD, f"bw_2d_{name}.log"))
+    assert rows.shape == gold.shape, (rows.shape, gold.shape)
+    bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
+    assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
+        np.argwhere(bad)[:10].tolist(), rows[bad][:10].tolist(), gold[bad][:10].tolist())
+
+
+# Blast wave 3-D MHD (tests/mhd/blast_wave_Cartesian_3D, reference): [0,2]^3,
+# 16^3 level-1 cells in 8^3 blocks (block_nx 8), cont boundaries,
+# refine_max_level 3 with w_refine_weight(1) = w_refine_weight(5) = 0.5 and
+# refine_threshold 0.2, rho = 1, p = 1 with p = 100 for r < 0.2 around the
+# centre, v = 0, B = (1, 1, 1) (Busr = 1), psi = 0; small_density =
+# small_pressure = 1e-14 with fix_small_values; log every 1e-3 to t = 0.02.
+# The first golden logs of the 3-D path and of a block edge other than 16.
+
+
+def _bw3d_prim(nw):
+    def f(X, Y, Z):
+        out = np.zeros((nw,) + X.shape)
+        out[0] = 1.0
+        out[4] = np.where((X - 1.0) ** 2 + (Y - 1.0) ** 2 + (Z - 1.0) ** 2 < 0.2 ** 2, 100.0, 1.0)
+        out[5] = out[6] = out[7] = 1.0
+        return out
+    return f
+
+
+@pytest.mark.parametrize("name,kw,nw", [
+    ("3step_hlld_cada", dict(flux_scheme="hlld", limiter="cada3", typedivbfix="glm"), 9),
+    ("3step_hll_cada", dict(flux_scheme="hll", limiter="cada3", typedivbfix="linde", typeboundspeed="cmaxmean"), 8),
+    ("3step_hll_ko", dict(flux_scheme="hll", limiter="koren", typedivbfix="linde", typeboundspeed="cmaxmean"), 8),
+    ("4step_hll_mc", dict(flux_scheme="hll", limiter="woodward", typedivbfix="linde", typeboundspeed="cmaxmean",
+                          time_stepper="fourstep", time_integrator="rk4"), 8),
+    ("4step_hllc_ko", dict(flux_scheme="hllc", limiter="koren", typedivbfix="linde", typeboundspeed="cmaxmean",
+                           time_stepper="fourstep"), 8),
+    ("rk4_tvdlf_cada", dict(flux_scheme="tvdlf", limiter="cada3", typedivbfix="linde", typeboundspeed="cmaxmean",
+                            time_stepper="fourstep", time_integrator="rk4"), 8),
+    ("2step_tvdlf_mm", dict(flux_scheme="tvdlf", limiter="minmod", typedivbfix="linde", typeboundspeed="cmaxmean",
+                            time_stepper="twostep"), 8),
+])
+def test_blast_wave_3d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
+    kw = dict(kw, courantpar=0.9, fix_small_values=True, small_density=1.0e-14, small_pressure=1.0e-14)
+    weight = np.zeros(nw)
+    weight[0] = weight[4] = 0.5
+    rows = _run_amr_golden("mhd", [2, 2, 2], _bw3d_prim(nw), weight, 0.2, kw, time_max=0.02, xmax=2.0, bc="cont",
+                           nd=3, bn=8)
+    gold = oracle_lib.read_log(os.path.join(GOLD, f"bw_3d_{name}.log"))
     assert rows.shape == gold.shape, (rows.shape, gold.shape)
     bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
     assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
