@@ -150,10 +150,30 @@ template <bool FAST> __device__ __forceinline__ double div_f(double x, double y)
 template <bool FAST> __device__ __forceinline__ double sqrt_f(double x) {
   if constexpr (FAST) return sqrt_nr(x); else return sqrt(x);
 }
-// the mixed form's single precision is IEEE throughout
-template <bool FAST> __device__ __forceinline__ float rcp_f(float y) { return rcp_(y); }
-template <bool FAST> __device__ __forceinline__ float div_f(float x, float y) { return div_(x, y); }
-template <bool FAST> __device__ __forceinline__ float sqrt_f(float x) { return sqrtf(x); }
+// Single precision (the mixed form's faces): IEEE, or with FAST the hardware
+// approximations of PTX (rcp.approx.ftz.f32, sqrt.approx.ftz.f32, about one
+// unit in the last place of FP32; the quotient x * (1/y) adds a rounding).
+// The mixed form's faces are accurate to FP32 rounding either way; a face
+// whose flux is not finite is recomputed in FP64.
+__device__ __forceinline__ float rcp_approx(float y) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
+  return r;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+template <bool FAST> __device__ __forceinline__ float rcp_f(float y) {
+  if constexpr (FAST) return rcp_approx(y); else return rcp_(y);
+}
+template <bool FAST> __device__ __forceinline__ float div_f(float x, float y) {
+  if constexpr (FAST) return x * rcp_approx(y); else return div_(x, y);
+}
+template <bool FAST> __device__ __forceinline__ float sqrt_f(float x) {
+  if constexpr (FAST) return sqrt_approx(x); else return sqrtf(x);
+}
 
 // ------------------------------------------------------------------ conversions
 // hd_to_primitive (mod_hd_phys.t:703-734) / mhd_to_primitive_origin (mod_mhd_phys.t:1741-1765)
@@ -311,8 +331,8 @@ __device__ __forceinline__ uint32_t cbounds(const T *wLC, const T *wRC, const T 
       dmean = sqrt_f<FAST>((tmp1 * (csL * csL) + tmp2 * (csR * csR)) * tmp3 +
                    T(0.5) * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
     } else {
-      const T csL = T(P.gamma) * wLp[V::E] / wLp[V::RHO];
-      const T csR = T(P.gamma) * wRp[V::E] / wRp[V::RHO];
+      const T csL = div_f<FAST>(T(P.gamma) * wLp[V::E], wLp[V::RHO]);
+      const T csR = div_f<FAST>(T(P.gamma) * wRp[V::E], wRp[V::RHO]);
       dmean = sqrt_f<FAST>((tmp1 * csL + tmp2 * csR) * tmp3 + T(0.5) * tmp1 * tmp2 * (tmp3 * tmp3) * (dv * dv));
     }
     if (WITH_MIN) {
@@ -337,17 +357,17 @@ __device__ __forceinline__ uint32_t cbounds(const T *wLC, const T *wRC, const T 
       T wm[V::NW];
 #pragma unroll
       for (int v = 0; v < V::NW; ++v) wm[v] = T(0.5) * (wLC[v] + wRC[v]);
-      const T tmp1 = wm[MN] / wm[V::RHO];
+      const T tmp1 = div_f<FAST>(wm[MN], wm[V::RHO]);
       T m2 = wm[V::M0] * wm[V::M0];
 #pragma unroll
       for (int c = 1; c < NDIR; ++c) m2 = m2 + wm[V::M0 + c] * wm[V::M0 + c];
-      T pth = T(P.gamma_1) * (wm[V::E] - T(0.5) * m2 / wm[V::RHO]);
+      T pth = T(P.gamma_1) * (wm[V::E] - div_f<FAST>(T(0.5) * m2, wm[V::RHO]));
       if (P.fix_small_values) {
         if (pth < T(P.small_pressure)) pth = T(P.small_pressure);
       } else if (P.check_small_values) {
         if (pth < T(P.small_pressure)) st |= ST_SMALL_VALUE;
       }
-      const T cs = sqrt_f<FAST>(P.gamma * pth / wm[V::RHO]);
+      const T cs = sqrt_f<FAST>(div_f<FAST>(T(P.gamma) * pth, wm[V::RHO]));
       if (WITH_MIN) {
         cmax = fmax(tmp1 + cs, T(0.0));
         cmin = fmin(tmp1 - cs, T(0.0));
@@ -360,8 +380,8 @@ __device__ __forceinline__ uint32_t cbounds(const T *wLC, const T *wRC, const T 
     if constexpr (MHD) {
       cs = fmax(fast_speed<T, NDIR, V::B0 + D, FAST>(wLp, P), fast_speed<T, NDIR, V::B0 + D, FAST>(wRp, P));
     } else {
-      const T csL = T(P.gamma) * wLp[V::E] / wLp[V::RHO];
-      const T csR = T(P.gamma) * wRp[V::E] / wRp[V::RHO];
+      const T csL = div_f<FAST>(T(P.gamma) * wLp[V::E], wLp[V::RHO]);
+      const T csR = div_f<FAST>(T(P.gamma) * wRp[V::E], wRp[V::RHO]);
       cs = fmax(sqrt_f<FAST>(csL), sqrt_f<FAST>(csR));
     }
     if (WITH_MIN) cmin = fmin(wLp[MN], wRp[MN]) - cs;

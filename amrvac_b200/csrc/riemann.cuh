@@ -38,6 +38,7 @@ __device__ __forceinline__ void riemann_hll(const T *wLC, const T *wRC, const T 
                                             T tvdlfeps, T *F) {
   using V = Vars<MHD, NDIR, GLM>;
   using FT = FluxTypes<MHD, NDIM, GLM>;
+  const T rden = rcp_f<FAST>(cmax - cmin);  // one reciprocal for every variable
 #pragma unroll
   for (int v = 0; v < V::NW; ++v) {
     if (FT::bn_tvdlf && v == V::B0 + D) {
@@ -47,14 +48,14 @@ __device__ __forceinline__ void riemann_hll(const T *wLC, const T *wRC, const T 
     } else if (cmax <= T(0.0)) {
       F[v] = fR[v];
     } else {
-      F[v] = div_f<FAST>(cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v]), cmax - cmin);
+      F[v] = (cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v])) * rden;
     }
   }
 }
 
 // get_Riemann_flux_hllc (mod_finite_volume.t:439-504) + hd_get_lCD / hd_get_wCD
 // (mod_hd_hllc.t:56-257); HD only, no hllcd diffusion, flathllc=.false.
-template <class T, int NDIR, int D>
+template <class T, int NDIR, int D, bool FAST = false>
 __device__ __forceinline__ void riemann_hllc_hd(const T *wLC, const T *wRC, const T *fL,
                                                 const T *fR, T cmax, T cmin,
                                                 T *F) {
@@ -74,12 +75,13 @@ __device__ __forceinline__ void riemann_hllc_hd(const T *wLC, const T *wRC, cons
     return;
   }
   T whll[NW], Fhll[NW];
+  const T rden = rcp_f<FAST>(cmax - cmin);  // one reciprocal for every variable
 #pragma unroll
   for (int v = 0; v < NW; ++v) {
-    Fhll[v] = (cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v])) / (cmax - cmin);
-    whll[v] = (cmax * wRC[v] - cmin * wLC[v] + fL[v] - fR[v]) / (cmax - cmin);
+    Fhll[v] = (cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v])) * rden;
+    whll[v] = (cmax * wRC[v] - cmin * wLC[v] + fL[v] - fR[v]) * rden;
   }
-  T lambdaCD = whll[MN] / whll[V::RHO];
+  T lambdaCD = div_f<FAST>(whll[MN], whll[V::RHO]);
   bool cond = true;
   if (cmin < T(0.0) && lambdaCD > T(0.0) && lambdaCD < cmax) {
     patchf = -1;
@@ -100,8 +102,8 @@ __device__ __forceinline__ void riemann_hllc_hd(const T *wLC, const T *wRC, cons
   const T *wSub = right ? wRC : wLC;
   const T *fSub = right ? fR : fL;
   const T cspeed = right ? cmax : cmin;
-  const T vSub = wSub[MN] / wSub[V::RHO];
-  const T csmls = T(1.0) / (cspeed - lambdaCD);
+  const T vSub = div_f<FAST>(wSub[MN], wSub[V::RHO]);
+  const T csmls = rcp_f<FAST>(cspeed - lambdaCD);
   T wCD[NW];
   wCD[V::RHO] = wSub[V::RHO] * (cspeed - vSub) * csmls;
 #pragma unroll
@@ -121,7 +123,7 @@ __device__ __forceinline__ void riemann_hllc_hd(const T *wLC, const T *wRC, cons
 // has zero normal-B (and psi) entries, which the flux_type rules then
 // replace by the diffusive tvdlf form without GLM, and keep with GLM (the
 // reference's HLLC takes no flux_special branch).
-template <class T, int NDIR, bool GLM, int NDIM, int D>
+template <class T, int NDIR, bool GLM, int NDIM, int D, bool FAST = false>
 __device__ __forceinline__ void riemann_hllc_mhd(const T *wLC, const T *wRC, const T *fL, const T *fR, T cmax,
                                                  T cmin, T tvdlfeps, T *F) {
   using V = Vars<true, NDIR, GLM>;
@@ -133,12 +135,13 @@ __device__ __forceinline__ void riemann_hllc_mhd(const T *wLC, const T *wRC, con
   T whll[NW], Fhll[NW], fCD[NW];
   T lambdaCD = T(0.0);
   if (patchf == 1) {
+    const T rden = rcp_f<FAST>(cmax - cmin);  // one reciprocal for every variable
 #pragma unroll
     for (int v = 0; v < NW; ++v) {
-      Fhll[v] = (cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v])) / (cmax - cmin);
-      whll[v] = (cmax * wRC[v] - cmin * wLC[v] + fL[v] - fR[v]) / (cmax - cmin);
+      Fhll[v] = (cmax * fL[v] - cmin * fR[v] + cmin * cmax * (wRC[v] - wLC[v])) * rden;
+      whll[v] = (cmax * wRC[v] - cmin * wLC[v] + fL[v] - fR[v]) * rden;
     }
-    lambdaCD = whll[MN] / whll[V::RHO];
+    lambdaCD = div_f<FAST>(whll[MN], whll[V::RHO]);
     bool cond = true;
     if (cmin < T(0.0) && lambdaCD > T(0.0) && lambdaCD < cmax) {
       patchf = -1;
@@ -156,25 +159,25 @@ __device__ __forceinline__ void riemann_hllc_mhd(const T *wLC, const T *wRC, con
     const T *wSub = right ? wRC : wLC;
     const T *fSub = right ? fR : fL;
     const T cspeed = right ? cmax : cmin;
-    const T vSub = wSub[MN] / wSub[V::RHO];
-    const T den = cspeed - lambdaCD;
+    const T vSub = div_f<FAST>(wSub[MN], wSub[V::RHO]);
+    const T rden = rcp_f<FAST>(cspeed - lambdaCD);  // one reciprocal for the star state
     T wCD[NW];
-    wCD[V::RHO] = wSub[V::RHO] * (cspeed - vSub) / den;
+    wCD[V::RHO] = wSub[V::RHO] * (cspeed - vSub) * rden;
 #pragma unroll
     for (int c = 0; c < NDIR; ++c) wCD[V::B0 + c] = whll[V::B0 + c];
 #pragma unroll
     for (int c = 0; c < NDIR; ++c) {
-      if (c != D) wCD[V::M0 + c] = (cspeed * wSub[V::M0 + c] - fSub[V::M0 + c] - wCD[BNI] * wCD[V::B0 + c]) / den;
+      if (c != D) wCD[V::M0 + c] = (cspeed * wSub[V::M0 + c] - fSub[V::M0 + c] - wCD[BNI] * wCD[V::B0 + c]) * rden;
       else wCD[V::M0 + c] = wCD[V::RHO] * lambdaCD;
     }
     // V.B of the HLL state (summed in the order the components arrive)
     T vdb = whll[V::M0] * whll[V::B0];
 #pragma unroll
     for (int c = 1; c < NDIR; ++c) vdb = vdb + whll[V::M0 + c] * whll[V::B0 + c];
-    vdb = vdb / whll[V::RHO];
+    vdb = div_f<FAST>(vdb, whll[V::RHO]);
     const T pCD = wSub[V::RHO] * (cspeed - vSub) * (lambdaCD - vSub) + fSub[MN] - wSub[MN] * vSub +
                   wCD[BNI] * wCD[BNI];
-    wCD[V::E] = (cspeed * wSub[V::E] - fSub[V::E] + lambdaCD * pCD - vdb * wCD[BNI]) / den;
+    wCD[V::E] = (cspeed * wSub[V::E] - fSub[V::E] + lambdaCD * pCD - vdb * wCD[BNI]) * rden;
 #pragma unroll
     for (int v = 0; v < NW; ++v) {
       if (v == BNI || (GLM && v == V::PSI)) fCD[v] = T(0.0);

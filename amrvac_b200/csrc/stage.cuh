@@ -271,8 +271,8 @@ __device__ __forceinline__ uint32_t face_from_states(T *wLp, T *wRp, const PhysP
     if constexpr (SOLVER == SOLVER_HLL) {
       riemann_hll<T, MHD, NDIR, GLM, NDIM, D, FAST>(wLC, wRC, fL, fR, cmax, cmin, T(P.tvdlfeps), F);
     } else if constexpr (SOLVER == SOLVER_HLLC) {
-      if constexpr (MHD) riemann_hllc_mhd<T, NDIR, GLM, NDIM, D>(wLC, wRC, fL, fR, cmax, cmin, T(P.tvdlfeps), F);
-      else riemann_hllc_hd<T, NDIR, D>(wLC, wRC, fL, fR, cmax, cmin, F);
+      if constexpr (MHD) riemann_hllc_mhd<T, NDIR, GLM, NDIM, D, FAST>(wLC, wRC, fL, fR, cmax, cmin, T(P.tvdlfeps), F);
+      else riemann_hllc_hd<T, NDIR, D, FAST>(wLC, wRC, fL, fR, cmax, cmin, F);
     } else {
       static_assert(MHD, "HLLD needs MHD");
       riemann_hlld<T, NDIR, GLM, NDIM, D, FAST>(wLC, wRC, wLp, wRp, fL, fR, cmax, cmin, F);
@@ -595,11 +595,11 @@ __global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, L
   constexpr bool FP64 = sizeof(TF) == 8;
   constexpr int HW = HaloW<LIM>::value;  // halo width: 2, or 3 for MP5
   constexpr int H2 = 2 * HW;
-  // FP64 faces of the slope limiters use the unguarded division, reciprocal
-  // and square root (physics.cuh: rcp_nr, div_nr, sqrt_nr); a face whose
-  // flux is not finite is recomputed with the guarded forms in the fix-up
-  // pass after its phase, like the mixed form's FP32 faces.
-  constexpr bool FASTF = FP64 && !(LIM == LIM_MP5 || LIM == LIM_WENO5 || LIM == LIM_WENO3 || LIM == LIM_VENK);
+  // Faces of the slope limiters use the fast division, reciprocal and square
+  // root (physics.cuh: unguarded Newton in FP64, the hardware approximations
+  // in the mixed form's FP32); a face whose flux is not finite is recomputed
+  // in FP64 with the guarded forms in the fix-up pass after its phase.
+  constexpr bool FASTF = !(LIM == LIM_MP5 || LIM == LIM_WENO5 || LIM == LIM_WENO3 || LIM == LIM_VENK);
   constexpr bool RETRY = !FP64 || FASTF;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TF *smem = reinterpret_cast<TF *>(smem_raw);

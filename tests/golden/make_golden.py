@@ -58,6 +58,19 @@ LOGS = [
     "tests/mhd/blast_wave_Cartesian_3D/correct_output/bw_3d_4step_hllc_ko.log",
     "tests/mhd/blast_wave_Cartesian_3D/correct_output/bw_3d_rk4_tvdlf_cada.log",
     "tests/mhd/blast_wave_Cartesian_3D/correct_output/bw_3d_2step_tvdlf_mm.log",
+    # 2-D HD with 12^2 blocks (block_nx 12), cont boundaries
+    "tests/hd/Riemann_2D/correct_output/rm_2d_3step_hll_cada.log",
+    "tests/hd/Riemann_2D/correct_output/rm_2d_4step_hll_mc.log",
+    "tests/hd/Riemann_2D/correct_output/rm_2d_4step_hllc_ko.log",
+    "tests/hd/Riemann_2D/correct_output/rm_2d_rk4_tvdlf_cada.log",
+    "tests/hd/Riemann_2D/correct_output/rm_2d_2step_tvdlf_mm.log",
+    # 3-D MHD with 10^3 blocks (block_nx 10), periodic x, cont y and z
+    "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_3step_hll_cada.log",
+    "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_3step_hlld_cada.log",
+    "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_4step_hll_mc.log",
+    "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_4step_hllc_ko.log",
+    "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_rk4_tvdlf_cada.log",
+    "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_2step_tvdlf_mm.log",
 ]
 
 

@@ -76,13 +76,15 @@ def _ot2d_prim(nw):
 
 
 def _amr_log_row(blocks, leaves, nbase, t, nw, nd=2, bn=16, xlen=1.0):
-    """printlog_regression_test: volume averages of w and w**2 over the leaves."""
+    """printlog_regression_test: volume averages of w and w**2 over the leaves
+    (xlen: the domain length, one value or one per dimension)."""
     s1, s2, vol = np.zeros(nw), np.zeros(nw), 0.0
     sl = (slice(None, nw),) + tuple(slice(2, 2 + bn) if d < nd else slice(None) for d in (2, 1, 0))
+    xl = np.broadcast_to(np.asarray(xlen, float), (nd,))
     for b, lf in enumerate(leaves):
         dv = 1.0
         for d in range(nd):
-            dv *= xlen / (nbase[d] * bn * (1 << (lf[0] - 1)))
+            dv *= xl[d] / (nbase[d] * bn * (1 << (lf[0] - 1)))
         w = blocks[b][sl].reshape(nw, -1)
         s1 += w.sum(axis=1) * dv
         s2 += (w * w).sum(axis=1) * dv
@@ -91,17 +93,20 @@ def _amr_log_row(blocks, leaves, nbase, t, nw, nd=2, bn=16, xlen=1.0):
 
 
 def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsave=1.0e-3, levels=3, xmax=1.0,
-                    bc="periodic", nd=2, bn=16):
-    """The reference's time loop on a multi-level grid over [0, xmax]^nd with
-    blocks of bn^nd cells: settree, then setdt + advance + resettree every
-    step, a log row at every dtsave."""
+                    bc="periodic", nd=2, bn=16, xmin=0.0):
+    """The reference's time loop on a multi-level grid over [xmin, xmax]^nd
+    (one value or one per dimension) with blocks of bn^nd cells: settree,
+    then setdt + advance + resettree every step, a log row at every dtsave.
+    bc: one boundary for every side, or one per side (min1, max1, ...)."""
     from tests import _amr as A
     from amrvac_b200 import Context, make_cfg
     from amrvac_b200.amr import Tree, initial_hierarchy, lohner_flags
     nw = len(weight)
-    xlen = xmax
-    xmin, xmax = [0.0] * nd, [xmax] * nd
-    cfg = make_cfg(physics=physics, ndim=nd, ndir=nd, typeboundary=[bc] * (2 * nd), block_nx=bn, **kw)
+    xmin = list(np.broadcast_to(np.asarray(xmin, float), (nd,)))
+    xmax = list(np.broadcast_to(np.asarray(xmax, float), (nd,)))
+    xlen = [b - a for a, b in zip(xmin, xmax)]
+    bcs = [bc] * (2 * nd) if isinstance(bc, str) else list(bc)
+    cfg = make_cfg(physics=physics, ndim=nd, ndir=nd, typeboundary=bcs, block_nx=bn, **kw)
     ctx = Context(cfg)
     lkw = dict(refine_threshold=threshold, derefine_ratio=0.125, amr_wavefilter=1.0e-2)
 
@@ -111,7 +116,8 @@ def _run_amr_golden(physics, nb, prim_fn, weight, threshold, kw, time_max, dtsav
     def err(tree, blocks):
         r, c, _ = lohner_flags(ctx, tree, blocks, xmin, xmax, weight, **lkw)
         return r, c
-    tree, blocks = initial_hierarchy(Tree(nd, nb, levels, periodic=[bc == "periodic"] * nd), init, err)
+    tree, blocks = initial_hierarchy(Tree(nd, nb, levels, periodic=[bcs[2 * d] == "periodic" for d in range(nd)]),
+                                     init, err)
     ctx.set_amr_grid(tree.leaves, nb, xmin, xmax)
     ctx.upload(blocks)
     ctx.set_time(0.0, time_max, dtsave)
@@ -274,6 +280,99 @@ def test_blast_wave_3d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
     rows = _run_amr_golden("mhd", [2, 2, 2], _bw3d_prim(nw), weight, 0.2, kw, time_max=0.02, xmax=2.0, bc="cont",
                            nd=3, bn=8)
     gold = oracle_lib.read_log(os.path.join(GOLD, f"bw_3d_{name}.log"))
+    assert rows.shape == gold.shape, (rows.shape, gold.shape)
+    bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
+    assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
+        np.argwhere(bad)[:10].tolist(), rows[bad][:10].tolist(), gold[bad][:10].tolist())
+
+
+# Riemann problem 2-D (tests/hd/Riemann_2D, reference, rm_2d.par): [0,1]^2,
+# 24^2 level-1 cells in 12^2 blocks (block_nx 12), cont boundaries,
+# refine_max_level 3 with the default estimator settings (w_refine_weight(1)
+# = 1, refine_threshold 0.1), gamma 1.4, four quadrants about (0.5, 0.5);
+# log every 1e-2 to t = 0.5.  (Its TVD-MUSCL log needs block_nx 16.)
+
+
+def _rm2d_prim(X, Y, Z):
+    out = np.zeros((4,) + X.shape)
+    ul = (np.abs(X) < 0.5) & (Y > 0.5) & (Y < 1.0)
+    ur = (np.abs(X) > 0.5) & (X < 1.0) & (Y > 0.5) & (Y < 1.0)
+    ll = (np.abs(X) < 0.5) & (Y < 0.5)
+    lr = (np.abs(X) > 0.5) & (X < 1.0) & (Y < 0.5)
+    out[3] = np.where(ul | lr, 0.3, np.where(ur | ll, 1.5, 0.0))
+    out[0] = np.where(ul | lr, 0.5323, np.where(ur | ll, 1.5, 0.0))
+    out[1] = np.where(ul, 1.206, 0.0)
+    out[2] = np.where(lr, 1.206, 0.0)
+    return out
+
+
+@pytest.mark.parametrize("name,kw", [
+    ("3step_hll_cada", dict(flux_scheme="hll", limiter="cada3", typeboundspeed="cmaxmean")),
+    ("4step_hll_mc", dict(flux_scheme="hll", limiter="woodward", typeboundspeed="cmaxmean", time_stepper="fourstep",
+                          time_integrator="rk4")),
+    ("4step_hllc_ko", dict(flux_scheme="hllc", limiter="koren", typeboundspeed="cmaxmean", time_stepper="fourstep")),
+    ("rk4_tvdlf_cada", dict(flux_scheme="tvdlf", limiter="cada3", typeboundspeed="cmaxmean", time_stepper="fourstep",
+                            time_integrator="rk4")),
+    ("2step_tvdlf_mm", dict(flux_scheme="tvdlf", limiter="minmod", typeboundspeed="cmaxmean", time_stepper="twostep")),
+])
+def test_riemann_2d_amr_golden_log_gpu(oracle_lib, name, kw):
+    kw = dict(kw, courantpar=0.9, gamma=1.4, dtmin=1.0e-6)
+    rows = _run_amr_golden("hd", [2, 2], _rm2d_prim, np.array([1.0, 0.0, 0.0, 0.0]), 0.1, kw, time_max=0.5,
+                           dtsave=1.0e-2, bc="cont", bn=12)
+    gold = oracle_lib.read_log(os.path.join(GOLD, f"rm_2d_{name}.log"))
+    assert rows.shape == gold.shape, (rows.shape, gold.shape)
+    bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
+    assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
+        np.argwhere(bad)[:10].tolist(), rows[bad][:10].tolist(), gold[bad][:10].tolist())
+
+
+# Kelvin-Helmholtz 3-D MHD jet (tests/mhd/Kelvin_Helmholtz_3D, reference):
+# [0,1] x [-1,1]^2, 20 x 40 x 40 level-1 cells in 10^3 blocks (block_nx 10),
+# periodic in x, cont in y and z, refine_max_level 3 with w_refine_weight
+# 0.4 (rho) and 0.2 (m1, m2, m3), refine_threshold 0.2, slowsteps 10; rho = 1,
+# p = 1, B = (0.129, 0, 0), v_x = 0.645 tanh((r - 0.5)/0.05) with an m = 1
+# perturbation of 0.01 in v_y, v_z; log every 1e-3 to t = 0.01.  (Its
+# TVD-MUSCL log needs block_nx 16.)
+
+
+def _kh3d_prim(nw):
+    def f(X, Y, Z):
+        out = np.zeros((nw,) + X.shape)
+        r = np.sqrt(Y * Y + Z * Z)
+        phi = np.arctan2(Z, Y)
+        k1 = 2.0 * np.pi / 1.0
+        rjet, width, qv, b0, dv = 0.5, 0.05, 0.645, 0.129, 0.01
+        out[0] = 1.0
+        out[4] = 1.0
+        out[5] = b0
+        out[1] = qv * np.tanh((r - rjet) / width)
+        env = dv * np.exp(-((r - rjet) / (4.0 * width)) ** 2) * np.cos(phi) * np.sin(k1 * X)
+        out[2] = env * np.cos(phi)
+        out[3] = env * np.sin(phi)
+        return out
+    return f
+
+
+@pytest.mark.parametrize("name,kw,nw", [
+    ("3step_hll_cada", dict(flux_scheme="hll", limiter="cada3", typedivbfix="linde", typeboundspeed="cmaxmean"), 8),
+    ("3step_hlld_cada", dict(flux_scheme="hlld", limiter="cada3", typedivbfix="glm"), 9),
+    ("4step_hll_mc", dict(flux_scheme="hll", limiter="woodward", typedivbfix="linde", typeboundspeed="cmaxmean",
+                          time_stepper="fourstep", time_integrator="rk4"), 8),
+    ("4step_hllc_ko", dict(flux_scheme="hllc", limiter="koren", typedivbfix="linde", typeboundspeed="cmaxmean",
+                           time_stepper="fourstep"), 8),
+    ("rk4_tvdlf_cada", dict(flux_scheme="tvdlf", limiter="cada3", typedivbfix="linde", typeboundspeed="cmaxmean",
+                            time_stepper="fourstep", time_integrator="rk4"), 8),
+    ("2step_tvdlf_mm", dict(flux_scheme="tvdlf", limiter="minmod", typedivbfix="linde", typeboundspeed="cmaxmean",
+                            time_stepper="twostep"), 8),
+])
+def test_kelvin_helmholtz_3d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
+    kw = dict(kw, courantpar=0.9, slowsteps=10)
+    weight = np.zeros(nw)
+    weight[0], weight[1], weight[2], weight[3] = 0.4, 0.2, 0.2, 0.2
+    rows = _run_amr_golden("mhd", [2, 4, 4], _kh3d_prim(nw), weight, 0.2, kw, time_max=1.0e-2, nd=3, bn=10,
+                           xmin=[0.0, -1.0, -1.0], xmax=[1.0, 1.0, 1.0],
+                           bc=["periodic", "periodic", "cont", "cont", "cont", "cont"])
+    gold = oracle_lib.read_log(os.path.join(GOLD, f"kh_3D_{name}.log"))
     assert rows.shape == gold.shape, (rows.shape, gold.shape)
     bad = np.abs(rows - gold) > 1e-8 + 1e-5 * np.abs(gold)
     assert oracle_lib.compare_logs(rows, gold, rtol=1e-5, atol=1e-8), (
