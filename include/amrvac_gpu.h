@@ -42,6 +42,7 @@ extern "C" {
 #define AMRVAC_ST_SMALL_VALUE  1u   /* small density/pressure (the reference's crash) */
 #define AMRVAC_ST_NAN          2u
 #define AMRVAC_ST_DT_TOO_SMALL 4u   /* dt < dtmin (src/mod_dt.t:55-60) */
+#define AMRVAC_ST_BOUNDS       8u   /* inconsistent neighbour table (read clamped) */
 
 /* flux_scheme (src/mod_finite_volume.t method ids are private; names match) */
 #define AMRVAC_FS_TVDLF 1
