@@ -100,6 +100,11 @@ class RunConfig:
     physics: str = "hd"
 
 
+# small_values_method names in the order of amrvac_cfg.small_values_method
+# (src/mod_small_values.t:9; 'average' is not built)
+SMALL_VALUES_METHODS = ("error", "replace")
+
+
 def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf",
              limiter="minmod", typeboundspeed="Einfeldt", typedivbfix=None,
              mhd_glm_alpha=0.5, mhd_glm_extended=True, divbdiff=0.8, courantpar=0.8,
@@ -143,7 +148,10 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
     c.tvdlfeps = tvdlfeps
     c.fix_small_values = int(fix_small_values)
     c.check_small_values = int(check_small_values)
-    c.small_values_method = 1 if small_values_method == "replace" else 0
+    if small_values_method not in SMALL_VALUES_METHODS:
+        raise ValueError(f"small_values_method {small_values_method!r}: the library runs "
+                         f"{', '.join(SMALL_VALUES_METHODS)}")
+    c.small_values_method = SMALL_VALUES_METHODS.index(small_values_method)
     c.small_density = small_density
     c.small_pressure = small_pressure
     c.time_stepper = _lib.TIME_STEPPER[time_stepper]

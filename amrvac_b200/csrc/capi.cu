@@ -251,6 +251,7 @@ int launch_getdt(amrvac_ctx *c, int reg) {
   G.type_courant = c->cfg.type_courant;
   G.red = c->d_red;
   G.P = c->P;
+  G.status = c->d_status;
   CK(c->ks.getdt(G, c->stream));
   ++c->launches;
   if (c->cfg.schmid_global) {  // a2max_global for schmid1 (getdt_courant + MPI_ALLREDUCE max)
@@ -529,6 +530,9 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
     return fail(AMRVAC_E_UNSUPPORTED, "tvdmu: dimsplit, FP64, no GLM");
   const int nw = nw_of(cfg);
   if (nw > AMRVAC_MAX_NW) return fail(AMRVAC_E_UNSUPPORTED, "too many variables");
+  if (k.precision != 0 && k.precision != 1) return fail(AMRVAC_E_ARG, "precision must be 0 (fp64) or 1 (mixed)");
+  if (k.fix_small_values && k.small_values_method != 0 && k.small_values_method != 1)
+    return fail(AMRVAC_E_UNSUPPORTED, "small_values_method: error (0) and replace (1) are built");
   amrvac_ctx *c = new amrvac_ctx();
   c->cfg = k;
   c->nreg = ((k.time_stepper == AMRVAC_TS_FOURSTEP && k.time_integrator == AMRVAC_TI_RK4) ||
@@ -537,7 +541,6 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   c->bn = bn;
   KernelKey key{k.physics == 1, k.ndim, k.ndir, k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM,
                 k.flux_scheme, k.limiter, k.typeboundspeed, k.precision == 1, bn};
-  if (k.precision != 0 && k.precision != 1) return fail(AMRVAC_E_ARG, "precision must be 0 (fp64) or 1 (mixed)");
   if (std::getenv("AMRVAC_GENERIC_KERNELS") && !special) { key.limiter = 0; key.boundspeed = 0; }
   // one kernel per family, the variant read at run time
   if (fifth && k.limiter != AMRVAC_LIM_MP5) key.limiter = LIM_WENO5;

@@ -367,6 +367,11 @@ __device__ __forceinline__ void ens_getdt_tile(const EnsArgs &A, int tile, EnsRo
     double w[NW];
 #pragma unroll
     for (int v = 0; v < NW; ++v) w[v] = __ldg(S.uin + cell_offset<ND>(R.blk, NW, v, ci, ND == 2 ? cj : 0, 0));
+    // phys_to_primitive with its small-value fix (src/mod_dt.t:189-191)
+    if (S.P.fix_small_values) {
+      if (small_values<double, false, ND, false>(w, false, S.P) && S.P.small_values_method != 1)
+        atomicOr(A.inst_status + R.inst, ST_SMALL_VALUE);
+    }
     to_primitive<false, ND, false>(w, S.P);
 #pragma unroll
     for (int d = 0; d < ND; ++d) {

@@ -19,6 +19,7 @@ struct GetdtArgs {
   int type_courant;
   unsigned long long *red;
   PhysParams P;
+  uint32_t *status;  // the context's status word: the small-value check of getdt
 };
 
 __device__ __forceinline__ double warp_max(double v) {
@@ -50,6 +51,12 @@ __global__ void __launch_bounds__(256) getdt_kernel(const GetdtArgs A) {
     double w[NW];
 #pragma unroll
     for (int v = 0; v < NW; ++v) w[v] = __ldg(A.u + cell_offset<NDIM>(b, NW, v, i, j, k, bn));
+    // getdt_courant takes the primitives through phys_to_primitive, small-value
+    // fix included (src/mod_dt.t:189-191)
+    if (A.P.fix_small_values) {
+      if (small_values<double, MHD, NDIR, GLM>(w, false, A.P) && A.P.small_values_method != 1 && A.status)
+        atomicOr(A.status, ST_SMALL_VALUE);
+    }
     to_primitive<MHD, NDIR, GLM>(w, A.P);
     double tot = 0.0;
 #pragma unroll

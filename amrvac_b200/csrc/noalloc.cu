@@ -87,6 +87,8 @@ __global__ void __launch_bounds__(256) getdt_blocks_kernel(const double *__restr
     double w[NW];
 #pragma unroll
     for (int v = 0; v < NW; ++v) w[v] = __ldg(u + cell_offset<NDIM>(b, NW, v, i, j, k, bn));
+    // phys_to_primitive with its small-value fix (src/mod_dt.t:189-191)
+    if (P.fix_small_values) small_values<double, MHD, NDIR, GLM>(w, false, P);
     to_primitive<MHD, NDIR, GLM>(w, P);
     double sum = 0.0;
 #pragma unroll

@@ -520,6 +520,53 @@ __device__ __noinline__ FaceFlux64<Vars<MHD, NDIR, GLM>::NW> face_retry_fp64(
   return r;
 }
 
+// Mixed form's recomputation: the face's four stencil cells (R cell at
+// block-local (i, j, k), the others 2 and 1 below it and 1 above along D)
+// gathered from the FP64 state and converted exactly as the FP64 kernel
+// stages them (load_prim), then the guarded FP64 reconstruction, small-value
+// check and Riemann flux: a recomputed face carries the FP64 kernel's flux
+// and its FP64 small-value decisions.  The staged cells' own status bits
+// were raised when they were staged.
+template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS, int BN>
+__device__ __noinline__ FaceFlux64<Vars<MHD, NDIR, GLM>::NW> face_retry_state(const StageArgs *A, int b, int D, int i,
+                                                                             int j, int k, double rd, double cg) {
+  using V = Vars<MHD, NDIR, GLM>;
+  constexpr int NW = V::NW;
+  double q[4][NW];
+#pragma unroll
+  for (int o = 0; o < 4; ++o)
+    load_prim<MHD, NDIR, GLM, NDIM, BN>(*A, b, i + (D == 0 ? o - 2 : 0), j + (D == 1 ? o - 2 : 0),
+                                        k + (D == 2 ? o - 2 : 0), q[o]);
+  double wLp[NW], wRp[NW];
+#pragma unroll
+  for (int v = 0; v < NW; ++v) {
+    const int ov = orig_index_rt<MHD, NDIR>(v, D);
+    const double d0 = q[1][ov] - q[0][ov], d1 = q[2][ov] - q[1][ov], d2 = q[3][ov] - q[2][ov];
+    double ldw, rdw;
+    face_slopes<double, LIM>(A->P.limiter, d0, d1, d2, rd, ldw, rdw);
+    wLp[v] = q[1][ov] + 0.5 * ldw;
+    wRp[v] = q[2][ov] - 0.5 * rdw;
+  }
+  FaceFlux64<NW> r;
+  r.st = face_from_states<double, MHD, NDIR, GLM, NDIM, SOLVER, BS>(wLp, wRp, A->P, cg, r.F);
+  return r;
+}
+
+// The mixed form's small-value decisions are made in FP64: with
+// fix_small_values set, a face whose FP32 left or right state has a density
+// or pressure within 2^-14 of its stencil's largest magnitude of the floor
+// (or below it) is recomputed by face_retry_state.  The FP32 state differs
+// from the FP64 one by a few FP32 roundings of that magnitude (2^-21 at
+// most), so every face the FP64 check would flag is recomputed.
+template <bool MHD, int NDIR, bool GLM>
+__device__ __forceinline__ bool sv_near_floor(const float *wLp, const float *wRp, float srho, float sp,
+                                              const PhysParams &P) {
+  using V = Vars<MHD, NDIR, GLM>;
+  const float m = 0x1p-14f;
+  return wLp[V::RHO] < float(P.small_density) + m * srho || wRp[V::RHO] < float(P.small_density) + m * srho ||
+         wLp[V::E] < float(P.small_pressure) + m * sp || wRp[V::E] < float(P.small_pressure) + m * sp;
+}
+
 // MUSCL-Hancock predictor, one direction D (hancock, src/mod_finite_volume.t:
 // 56-101; reconstruct_LR default branch 1171-1222): from the primitives of
 // cells c-1, c, c+1 along D (shared-memory offsets base[o], strides strd[o]),
@@ -582,7 +629,7 @@ struct StageOcc {
 
 template <class TF, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS, int BN = BN16>
 __global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, LIM, BN>::MINB)
-    fv_stage_kernel(const StageArgs A) {
+    fv_stage_kernel(const __grid_constant__ StageArgs A) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
   // block edge BN; this CTA's tile is TB x TB cells of a z-plane (x/y), at
@@ -912,16 +959,33 @@ __global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, L
             wRp[v] = q[2] - TF(0.5) * rdw;
           }
         }
+        // mixed form with fix_small_values: a state near a floor goes to the
+        // FP64 recomputation (its flux is marked non-finite)
+        bool near = false;
+        if constexpr (!FP64 && HW == 2) {
+          if (P.fix_small_values) {
+            TF srho = TF(0), sp = TF(0);
+#pragma unroll
+            for (int o = 0; o < 4; ++o) {
+              srho = fmaxf(srho, fabsf(smem[base[o] + V::RHO * strd[o]]));
+              sp = fmaxf(sp, fabsf(smem[base[o] + V::E * strd[o]]));
+            }
+            near = sv_near_floor<MHD, NDIR, GLM>(wLp, wRp, srho, sp, P);
+          }
+        }
         TF Fr[NW];
         // the MP5 / WENO branches of reconstruct_LR have no small-value fix of
         // the states
         stb |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS, FASTF>(wLp, wRp, P, TF(cg), Fr,
-                                                                              HW == 2 && LIM != LIM_WENO3);
+                                                                              HW == 2 && LIM != LIM_WENO3 && !near);
         if constexpr (RETRY) {
-          bool finite = true;
+          bool finite = !near;
 #pragma unroll
           for (int v = 0; v < NW; ++v) finite = finite && isfinite(Fr[v]);
-          if (!finite) s_retry = 1;
+          if (!finite) {
+            s_retry = 1;
+            Fr[0] = TF(NAN);
+          }
         }
         // FP64: the scaled flux fC = -qdt/dx * f as in the reference; mixed:
         // the FP32 flux, scaled in FP64 by the accumulating cell thread
@@ -949,9 +1013,14 @@ __global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, L
             const double sc = FD == 0 ? dxinv[0] : (FD == 1 ? dxinv[1] : dxinv[2]);
             int fi, fj, base[H2], strd[H2];
             face_at(FD, fl, fi, fj, base, strd);
-            const FaceFlux64<NW> r = face_retry_fp64<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>(
-                smem, FD, base[0], base[1], base[2], base[3], strd[0], strd[1], strd[2], strd[3],
-                FD == 0 ? rdel[0] : (FD == 1 ? rdel[1] : rdel[2]), cg, P);
+            const double rdd = FD == 0 ? rdel[0] : (FD == 1 ? rdel[1] : rdel[2]);
+            FaceFlux64<NW> r;
+            if constexpr (FP64)
+              r = face_retry_fp64<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS>(
+                  smem, FD, base[0], base[1], base[2], base[3], strd[0], strd[1], strd[2], strd[3], rdd, cg, P);
+            else  // the R cell of the face, block-local
+              r = face_retry_state<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, BN>(
+                  &A, b, FD, ti0 + fi, tj0 + fj, FD == 2 ? k + 1 : k, rdd, cg);
             stb |= r.st;
             TF Fr[NW];
             for (int v = 0; v < NW; ++v) {

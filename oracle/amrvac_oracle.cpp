@@ -1166,9 +1166,11 @@ void divb_central(const State &s, const Arr<R> &w, const Box &ixO, const double 
 }
 
 // add_source_glm (src/mhd/mod_mhd_phys.t:5472-5531)
+// Both divB sources end with the small-value fix of the updated state
+// (src/mhd/mod_mhd_phys.t:5529, 5662); the status of that fix is returned.
 template <class R>
-void add_source_glm(const State &s, double qdt, const Box &ixI, const Box &ixO, const Arr<R> &wCT,
-                    Arr<R> &w, const double *dxlevel, double cmax_global) {
+int add_source_glm(const State &s, double qdt, const Box &ixI, const Box &ixO, const Arr<R> &wCT,
+                   Arr<R> &w, const double *dxlevel, double cmax_global) {
   const Ix &x = s.x;
   const orc_cfg &c = s.c;
   double mindx = dxlevel[0];
@@ -1195,14 +1197,15 @@ void add_source_glm(const State &s, double qdt, const Box &ixI, const Box &ixO, 
     }
   }
   (void)ixI;
+  return c.fix_small_values ? handle_small_values(s, false, w, ixO) : 0;
 }
 
 // add_source_linde (src/mhd/mod_mhd_phys.t:5599-5665).  jump_faces bit
 // 2d+side marks a face with a coarser or finer neighbour: the source skips the
 // cell layer next to it ("for AMR stability", 5616-5642).
 template <class R>
-void add_source_linde(const State &s, double qdt, const Box &ixO, const Arr<R> &wCT, Arr<R> &w,
-                      const double *dxlevel, int jump_faces = 0) {
+int add_source_linde(const State &s, double qdt, const Box &ixO, const Arr<R> &wCT, Arr<R> &w,
+                     const double *dxlevel, int jump_faces = 0) {
   const Ix &x = s.x;
   const orc_cfg &c = s.c;
   Box ixp = ixO;
@@ -1232,6 +1235,7 @@ void add_source_linde(const State &s, double qdt, const Box &ixO, const Arr<R> &
     });
   }
   (void)qdt;
+  return c.fix_small_values ? handle_small_values(s, false, w, ixO) : 0;
 }
 
 // tvdlimit2 (src/mod_tvd.t:38-112) for fs_tvdmu with hydrodynamics: the Roe
@@ -1610,8 +1614,8 @@ int finite_volume(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, d
   // addsource2 -> mhd_add_source divB part (src/mod_source.t:130-160)
   if (x.mhd && ndim > 1) {
     double qsrc = qdt * double(s.idhi - s.idlo + 1) / double(ndim);
-    if (c.divb == ORC_DIVB_GLM) add_source_glm(s, qsrc, ixI, ixO, wCT, wnew, dxs, cmax_global);
-    else if (c.divb == ORC_DIVB_LINDE) add_source_linde(s, qsrc, ixO, wCT, wnew, dxs, jump_faces);
+    if (c.divb == ORC_DIVB_GLM) st |= add_source_glm(s, qsrc, ixI, ixO, wCT, wnew, dxs, cmax_global);
+    else if (c.divb == ORC_DIVB_LINDE) st |= add_source_linde(s, qsrc, ixO, wCT, wnew, dxs, jump_faces);
   }
   (void)dtfactor;
   if (keep_fc) *keep_fc = std::move(fC);  // scaled face fluxes -qdt/dx F, for store_flux
@@ -1657,8 +1661,8 @@ int hancock(const State &s, const Arr<R> &wCT, Arr<R> &wnew, double qdt, const d
   }
   if (x.mhd && ndim > 1) {
     double qsrc = qdt * double(s.idhi - s.idlo + 1) / double(ndim);
-    if (c.divb == ORC_DIVB_GLM) add_source_glm(s, qsrc, ixI, ixO, wCT, wnew, dxs, cmax_global);
-    else if (c.divb == ORC_DIVB_LINDE) add_source_linde(s, qsrc, ixO, wCT, wnew, dxs, jump_faces);
+    if (c.divb == ORC_DIVB_GLM) st |= add_source_glm(s, qsrc, ixI, ixO, wCT, wnew, dxs, cmax_global);
+    else if (c.divb == ORC_DIVB_LINDE) st |= add_source_linde(s, qsrc, ixO, wCT, wnew, dxs, jump_faces);
   }
   if (c.fix_small_values) st |= handle_small_values(s, false, wnew, ixO);
   return st;

@@ -1,0 +1,151 @@
+"""fix_small_values on the GPU against the oracle, on fields with planted
+small densities and pressures.
+
+The reference fixes small values at three places of a stage: the conversion
+of the ghosted block to primitives (hd_to_primitive / mhd_to_primitive_origin
+calling phys_handle_small_values, src/hd/mod_hd_phys.t:703-734,
+src/mhd/mod_mhd_phys.t:1741-1765), the reconstructed left and right face
+states (src/mod_finite_volume.t:1212-1216) and the updated state on exit
+(src/mod_finite_volume.t:326-333); the sound speeds clamp the thermal
+pressure at small_pressure (src/hd/mod_hd_phys.t:1040-1045,
+src/mhd/mod_mhd_phys.t:3573).  Method 'replace' (src/hd/mod_hd_phys.t:
+1440-1466, src/mhd/mod_mhd_phys.t:2207-2225) sets density and pressure to
+their floors and zeroes the momentum where the density is small; it raises
+no error.  Each case plants a cell below small_density, one with negative
+pressure and one on a block edge, and compares setdt and a full step cell by
+cell (tests/_parity.py; bar 1e-12 or the oracle's own one-ulp noise).
+"""
+import numpy as np
+import pytest
+
+from tests import _problems as P
+from tests._parity import one_ulp_noise, percell_err
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+SMALL = dict(fix_small_values=True, small_values_method="replace", small_density=1e-8, small_pressure=1e-8)
+
+CASES = {
+    "hd2_hll_minmod": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="hll", limiter="minmod"),
+    "hd3_hllc_vanleer": dict(physics="hd", ndim=3, gamma=1.4, flux_scheme="hllc", limiter="vanleer"),
+    "hd2_tvdlf_koren_twostep": dict(physics="hd", ndim=2, gamma=1.4, flux_scheme="tvdlf", limiter="koren",
+                                    time_stepper="twostep"),
+    "mhd3_hlld_cada3_glm": dict(physics="mhd", ndim=3, flux_scheme="hlld", limiter="cada3", typedivbfix="glm"),
+    "mhd25_hll_vanleer_linde": dict(physics="mhd", ndim=2, ndir=3, flux_scheme="hll", limiter="vanleer",
+                                    typedivbfix="linde"),
+    "mhd2_hllc_minmod_none": dict(physics="mhd", ndim=2, flux_scheme="hllc", limiter="minmod", typedivbfix="none"),
+}
+
+
+def _cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _planted(physics, ndim, ndir, n, glm, gamma):
+    """Conserved field with three planted cells: density 1e-10 (below the
+    1e-8 floor, with pressure 1e-10), pressure -1e-3, and density 1e-10 on
+    the last cell row of the first block along y (x in 1-D)."""
+    prim = P.random_smooth(physics, ndim, ndir, n, glm=glm)
+    ip = ndir + 1
+    mid = tuple([n // 2 + 3] * ndim)[::-1]
+    other = tuple([5] * ndim)[::-1]
+    edge = tuple([7] * (ndim - 1) + [15])[::-1] if ndim > 1 else (15,)
+    pad = (0,) * (3 - ndim)
+    for cell, (rho, p) in ((mid, (1e-10, 1e-10)), (other, (None, -1e-3)), (edge, (1e-10, 1e-10))):
+        ix = pad + cell
+        if rho is not None:
+            prim[(0,) + ix] = rho
+        prim[(ip,) + ix] = p
+    return P.prim_to_cons(prim, physics, ndir, gamma)
+
+
+def _setup(O, name, noisy=False):
+    from amrvac_b200 import Context, make_cfg
+    kw = dict(CASES[name], **SMALL)
+    nd = kw["ndim"]
+    ndir = kw.get("ndir", nd)
+    ok = dict(kw)
+    ok["divb"] = ok.pop("typedivbfix", "none")
+    ocfg = O.make_cfg(**ok)
+    n = 32
+    cons = _planted(kw["physics"], nd, ndir, n, ok["divb"] == "glm", ocfg.gamma)
+    blocks = P.to_blocks(cons, nd)
+    if noisy:
+        blocks = one_ulp_noise(blocks)
+    og = O.Grid(ocfg, [n] * nd, [0.0] * nd, [1.0] * nd, ["periodic"] * (2 * nd))
+    for ib in range(og.nblocks):
+        og.set_block(ib, blocks[ib])
+    og.getbc()
+    ctx = None
+    if not noisy:
+        ctx = Context(make_cfg(**kw))
+        ctx.set_uniform_grid([n] * nd, [0.0] * nd, [1.0] * nd)
+        ctx.upload(blocks)
+    return og, ctx, nd
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_replace_step_matches_oracle(oracle_lib, name):
+    _cuda()
+    O = oracle_lib
+    og, ctx, nd = _setup(O, name)
+    dt_ref, cg_ref = og.getdt()
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.step()
+    dt, cg, _ = ctx.get_time()
+    assert abs(dt - dt_ref) <= 1e-13 * dt_ref and abs(cg - cg_ref) <= 1e-13 * cg_ref
+    st = og.advance(dt_ref, cg_ref)
+    gn = _setup(O, name, noisy=True)[0]
+    gn.getdt()
+    gn.advance(dt_ref, cg_ref)
+    got = P.interior(ctx.download(), nd)
+    ref = P.interior(np.array([og.get_block(ib) for ib in range(og.nblocks)]), nd)
+    noise = percell_err(P.interior(np.array([gn.get_block(ib) for ib in range(gn.nblocks)]), nd), ref)
+    err = percell_err(got, ref)
+    assert np.isfinite(got).all()
+    assert err <= max(RTOL, noise), f"{name}: {err:.3e} (oracle self-noise {noise:.3e})"
+    # 'replace' repairs and carries on: no error status on either side
+    assert ctx.status() == 0
+    assert not (st or 0) & 1
+
+
+def test_replace_floors_the_planted_cells(oracle_lib):
+    """The planted cells stay at or above the floors after the step: the
+    exit fix of the updated state ran (src/mod_finite_volume.t:326-333)."""
+    _cuda()
+    og, ctx, nd = _setup(oracle_lib, "hd2_hll_minmod")
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.step()
+    got = P.interior(ctx.download(), nd)
+    assert got[:, 0].min() >= 1e-8
+
+
+@pytest.mark.parametrize("name", ["hd2_hll_minmod", "hd3_hllc_vanleer", "mhd3_hlld_cada3_glm",
+                                  "mhd25_hll_vanleer_linde"])
+def test_mixed_form_takes_the_fp64_decisions(oracle_lib, name):
+    """Mixed form (FP32 faces) with 'replace': the faces whose states come
+    near a floor are recomputed from the FP64 state, so the replace
+    decisions are the FP64 kernel's and no cell moves by more than FP32
+    round-off against it (a different decision would move a cell by O(1):
+    the momentum is zeroed)."""
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    og, ctx, nd = _setup(oracle_lib, name)
+    kw = dict(CASES[name], **SMALL)
+    blocks = ctx.download()
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    ctx.step()
+    ref = P.interior(ctx.download(), nd)
+    mx = Context(make_cfg(precision="mixed", **kw))
+    mx.set_uniform_grid([32] * nd, [0.0] * nd, [1.0] * nd)
+    mx.upload(blocks)
+    mx.set_time(0.0, 1.0e99, 0.0)
+    mx.step()
+    got = P.interior(mx.download(), nd)
+    assert mx.status() == 0
+    scale = np.abs(ref).reshape(ref.shape[0], ref.shape[1], -1).max(axis=(0, 2))
+    dev = np.abs(got - ref).max(axis=(0, 2, 3, 4)) / scale
+    assert dev.max() <= 1e-4, dev
