@@ -108,6 +108,8 @@ SIGNATURES = [
     ("amrvac_gpu_fp64_peak", _i, [_dp]),
     ("amrvac_gpu_autotune", _i, [_vp, _i, _ip, _dp]),
     ("amrvac_gpu_set_zchunk", _i, [_vp, _i]),
+    ("amrvac_gpu_set_stage_variant", _i, [_vp, _i]),
+    ("amrvac_gpu_stage_variant", _i, [_vp, _ip, _ip, _ip, _ip, _ip]),
     ("amrvac_gpu_status", _i, [_vp, _P(_u32)]),
     ("amrvac_gpu_clear_status", _i, [_vp]),
     ("amrvac_gpu_synchronize", _i, [_vp]),

@@ -202,6 +202,18 @@ class Context:
     def set_zchunk(self, zchunk: int):
         _lib.check(self.L.amrvac_gpu_set_zchunk(self.h, zchunk), "set_zchunk")
 
+    def set_stage_variant(self, var: int):
+        """Select stage-kernel variant var (0: the scheme's default kernel)."""
+        _lib.check(self.L.amrvac_gpu_set_stage_variant(self.h, var), "set_stage_variant")
+
+    def stage_variant(self) -> dict:
+        """The current stage-kernel variant: its index, the number of
+        variants, threads per CTA, CTAs per SM, asynchronous staging."""
+        v = [ctypes.c_int() for _ in range(5)]
+        _lib.check(self.L.amrvac_gpu_stage_variant(self.h, *[ctypes.byref(x) for x in v]), "stage_variant")
+        return dict(variant=v[0].value, nvariants=v[1].value, threads=v[2].value, ctas_per_sm=v[3].value,
+                    async_staging=bool(v[4].value))
+
     def get_time(self):
         dt, cm, t = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         _lib.check(self.L.amrvac_gpu_get_time(self.h, ctypes.byref(dt), ctypes.byref(cm), ctypes.byref(t)),

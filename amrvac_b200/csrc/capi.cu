@@ -88,6 +88,8 @@ struct amrvac_ctx {
   int sweep = -1;          // dimensional splitting: the current sweep of the step (-1: unsplit)
   bool fixed_dir = false;  // sweep is a direction (amrvac_gpu_advect1_dim), not a sweep index
   int wave_ctas = 1;       // resident stage CTAs on the device (one wave)
+  int var = 0;             // stage-kernel variant (KernelSet::stage_v; chosen by the autotuner)
+  int wave_v[KernelSet::MAXVAR] = {1, 1, 1, 1};  // one wave of each variant
   std::vector<double> h_dx;            // [nblocks][3] cell sizes (host copy)
   double *d_adj[3] = {nullptr, nullptr, nullptr};  // adjoint work registers (lazily)
   int *d_amr_int = nullptr;            // [2][nblocks] levels, flags (Löhner, lazily)
@@ -211,10 +213,10 @@ int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a,
   const long planes = (long)c->nblocks * ntile * (c->cfg.ndim == 3 ? bn : 1);
   int nctas;
   if (c->zchunk > 0) nctas = c->nblocks * ntile * (c->cfg.ndim == 3 ? bn / c->zchunk : 1);
-  else nctas = (int)std::min<long>(planes, c->wave_ctas);
+  else nctas = (int)std::min<long>(planes, hancock ? c->wave_ctas : c->wave_v[c->var]);
   const bool restore = !hancock && c->P.fix_small_values && c->P.small_values_method == 0;
   if (restore) CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * c->nblocks, c->stream));
-  CK(hancock ? c->ks.hancock(A, nctas, c->stream) : c->ks.stage(A, nctas, c->stream));
+  CK(hancock ? c->ks.hancock(A, nctas, c->stream) : c->ks.stage_v[c->var](A, nctas, c->stream));
   ++c->launches;
   if (c->cfg.ndim == 3 && c->cfg.physics == 1 && c->cfg.typedivbfix == AMRVAC_DIVB_LINDE) {
     if (!c->ks.linde3d) return fail(AMRVAC_E_UNSUPPORTED, "no 3-D Linde kernel for this configuration");
@@ -560,6 +562,7 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
     return fail(AMRVAC_E_UNSUPPORTED, key.mixed ? "no mixed-precision kernel for this scheme"
                                                 : "no kernel for this physics/ndim/ndir/solver combination");
   }
+  if (bn == 16 && !special) add_stage_variants(key, &c->ks);
   cudaError_t e0;
   PhysParams &P = c->P;
   P.gamma = k.gamma;
@@ -619,12 +622,19 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
     delete c;
     return cuda_fail(e0, "cudaFuncSetAttribute");
   }
+  for (int v = 1; v < c->ks.nvar; ++v) {
+    if ((e0 = c->ks.prepare_v[v]()) != cudaSuccess) {
+      delete c;
+      return cuda_fail(e0, "cudaFuncSetAttribute");
+    }
+  }
   c->zchunk = valid_zchunk(bn, k.zchunk) ? k.zchunk : 0;
   {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     c->wave_ctas = nsm * c->ks.ctas_per_sm();
+    for (int v = 0; v < c->ks.nvar; ++v) c->wave_v[v] = nsm * c->ks.ctas_v[v]();
   }
   c->per_block = 1;
   for (int d = 0; d < k.ndim; ++d) c->per_block *= bn;
@@ -1472,6 +1482,24 @@ int amrvac_gpu_set_zchunk(amrvac_ctx *c, int zchunk) {
   return 0;
 }
 
+int amrvac_gpu_set_stage_variant(amrvac_ctx *c, int var) {
+  if (int r = check_ctx(c, false)) return r;
+  if (var < 0 || var >= c->ks.nvar) return fail(AMRVAC_E_ARG, "no such stage-kernel variant for this scheme");
+  if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+  c->var = var;
+  return 0;
+}
+
+int amrvac_gpu_stage_variant(amrvac_ctx *c, int *var, int *nvar, int *threads, int *ctas_per_sm, int *async) {
+  if (int r = check_ctx(c, false)) return r;
+  if (var) *var = c->var;
+  if (nvar) *nvar = c->ks.nvar;
+  if (threads) *threads = c->ks.var_threads[c->var];
+  if (ctas_per_sm) *ctas_per_sm = c->ks.var_minb[c->var];
+  if (async) *async = c->ks.var_async[c->var];
+  return 0;
+}
+
 int amrvac_gpu_autotune(amrvac_ctx *c, int reps, int *best_zchunk, double *best_ms) {
   if (int r = check_ctx(c, true)) return r;
   if (reps <= 0) reps = 3;
@@ -1489,24 +1517,29 @@ int amrvac_gpu_autotune(amrvac_ctx *c, int reps, int *best_zchunk, double *best_
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
-  int best = c->zchunk;
+  // every stage-kernel variant of the scheme with every work distribution
+  int best = c->zchunk, bvar = c->var;
   float bms = 1e30f;
-  for (int q = 0; q < ncand; ++q) {
-    c->zchunk = cand[q];
-    int r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);  // warm
-    CK(cudaEventRecord(a, c->stream));
-    for (int i = 0; i < reps && !r; ++i) r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);
-    CK(cudaEventRecord(b, c->stream));
-    CK(cudaEventSynchronize(b));
-    if (r) { cudaEventDestroy(a); cudaEventDestroy(b); return r; }
-    float ms;
-    CK(cudaEventElapsedTime(&ms, a, b));
-    ms /= reps;
-    if (ms < bms) { bms = ms; best = cand[q]; }
+  for (int v = 0; v < c->ks.nvar; ++v) {
+    c->var = v;
+    for (int q = 0; q < ncand; ++q) {
+      c->zchunk = cand[q];
+      int r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);  // warm
+      CK(cudaEventRecord(a, c->stream));
+      for (int i = 0; i < reps && !r; ++i) r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);
+      CK(cudaEventRecord(b, c->stream));
+      CK(cudaEventSynchronize(b));
+      if (r) { cudaEventDestroy(a); cudaEventDestroy(b); return r; }
+      float ms;
+      CK(cudaEventElapsedTime(&ms, a, b));
+      ms /= reps;
+      if (ms < bms) { bms = ms; best = cand[q]; bvar = v; }
+    }
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   c->zchunk = best;
+  c->var = bvar;
   if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
   if (best_zchunk) *best_zchunk = best;
   if (best_ms) *best_ms = bms;

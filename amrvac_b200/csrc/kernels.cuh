@@ -299,6 +299,47 @@ struct KernelSet {
   cudaError_t (*cbounds_points)(const PointArgs &, int idim, cudaStream_t) = nullptr;
   size_t stage_smem = 0;
   int bn = BN16;  // the block edge the stage kernels were built for
+  // Stage-kernel variants the autotuner times (variant 0 is `stage`): per
+  // variant the launch, its occupancy query, threads per CTA, the CTAs per
+  // SM its registers are capped for, and asynchronous plane staging.
+  static constexpr int MAXVAR = 4;
+  int nvar = 1;
+  cudaError_t (*stage_v[MAXVAR])(const StageArgs &, int nctas, cudaStream_t) = {};
+  int (*ctas_v[MAXVAR])() = {};
+  cudaError_t (*prepare_v[MAXVAR])() = {};
+  int var_threads[MAXVAR] = {}, var_minb[MAXVAR] = {}, var_async[MAXVAR] = {};
+};
+
+// One stage-kernel variant of a scheme (see stage_variant).
+template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS, class TF, int BN, int VAR>
+struct StageVar {
+  using V = Vars<MHD, NDIR, GLM>;
+  using O = StageOcc<TF, LIM, BN, VAR>;
+  static constexpr size_t SMEM = Tile<TF, V::NW, NDIM, HaloW<LIM>::value, tile_edge(BN)>::BYTES;
+  static cudaError_t prepare() {
+    return cudaFuncSetAttribute(fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, BN, VAR>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+  }
+  static cudaError_t stage(const StageArgs &A, int nctas, cudaStream_t s) {
+    fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, BN, VAR><<<nctas, O::THREADS, SMEM, s>>>(A);
+    return cudaGetLastError();
+  }
+  static int ctas_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, fv_stage_kernel<TF, MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, BN, VAR>, O::THREADS, SMEM) != cudaSuccess)
+      return 1;
+    return n > 0 ? n : 1;
+  }
+  static void add(KernelSet &k, int slot) {
+    k.stage_v[slot] = &stage;
+    k.ctas_v[slot] = &ctas_per_sm;
+    k.prepare_v[slot] = &prepare;
+    k.var_threads[slot] = O::THREADS;
+    k.var_minb[slot] = O::MINB;
+    k.var_async[slot] = O::ASYNC && sizeof(TF) == 8 && NDIM == 3 && tile_edge(BN) == BN && HaloW<LIM>::value == 2;
+    if (slot + 1 > k.nvar) k.nvar = slot + 1;
+  }
 };
 
 template <bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM = 0, int BS = 0, class TF = double,
@@ -401,6 +442,7 @@ struct Launch {
     k.cbounds_points = &cbounds_points;
     k.stage_smem = SMEM;
     k.bn = BN;
+    StageVar<MHD, NDIR, GLM, NDIM, SOLVER, LIM, BS, TF, BN, 0>::add(k, 0);
     return k;
   }
 };
@@ -418,6 +460,8 @@ struct KernelKey {
 };
 
 bool lookup_hd(const KernelKey &k, KernelSet *out);
+// The variants 1..3 of the benchmark schemes' stage kernels (k_tune.cu).
+bool add_stage_variants(const KernelKey &k, KernelSet *out);
 // block edges other than 16 (k_blocks.cuh, one unit per edge)
 bool lookup_bn8(const KernelKey &k, KernelSet *out);
 bool lookup_bn10(const KernelKey &k, KernelSet *out);

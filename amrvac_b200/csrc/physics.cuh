@@ -23,7 +23,7 @@ enum : int { SOLVER_TVDLF = 1, SOLVER_HLL = 2, SOLVER_HLLC = 3, SOLVER_HLLD = 4,
              SOLVER_HANCOCK = 8 };
 enum : int { DIVB_NONE = 0, DIVB_GLM = 1, DIVB_LINDE = 4 };
 // Runtime status bits (atomicOr into the context's status word).
-enum : uint32_t { ST_SMALL_VALUE = 1u, ST_NAN = 2u, ST_DT_TOO_SMALL = 4u, ST_BOUNDS = 8u };
+enum : uint32_t { ST_SMALL_VALUE = 1u, ST_NAN = 2u, ST_DT_TOO_SMALL = 4u, ST_BOUNDS = 8u, ST_TIMEOUT = 16u };
 
 // Physics constants shared by all kernels of one context.
 struct PhysParams {

@@ -619,16 +619,77 @@ __device__ __forceinline__ uint32_t hancock_dir(const double *smem, const int *b
 // CTAs per SM the stage kernel is built for: two of 256 threads (FP64; one
 // with the fifth-order halo), three in the mixed form; smaller tiles keep the
 // same threads per SM.
-template <class TF, int LIM, int BN>
+//
+// Variants (VAR > 0) are the alternatives the autotuner times for the
+// benchmark schemes: threads per CTA, the CTAs per SM the registers are
+// capped for, and the staging mode (asynchronous bulk copies of the next
+// conserved plane, FP64 only).  stage_variant(VAR, fp64) gives them.
+struct StageVariant {
+  int threads, minb;
+  bool async;
+};
+__host__ __device__ constexpr StageVariant stage_variant(int var, bool fp64) {
+  if (fp64) {
+    return var == 1 ? StageVariant{256, 2, true}
+                    : var == 2 ? StageVariant{288, 2, false} : StageVariant{256, 1, false};
+  }
+  return var == 1 ? StageVariant{256, 2, false} : var == 2 ? StageVariant{256, 4, false} : StageVariant{288, 3, false};
+}
+template <class TF, int LIM, int BN, int VAR = 0>
 struct StageOcc {
-  static constexpr int THREADS = BN == BN16 ? STAGE_THREADS : stage_threads(BN);
-  static constexpr int BASE = sizeof(TF) == 8 ? (HaloW<LIM>::value == 3 ? 1 : AMRVAC_STAGE_MINB)
-                                              : AMRVAC_STAGE_MINB_MIXED;
-  static constexpr int MINB = BASE * 256 / THREADS < 1 ? 1 : (BASE * 256 / THREADS > 16 ? 16 : BASE * 256 / THREADS);
+  static constexpr bool FP64 = sizeof(TF) == 8;
+  static constexpr int THREADS =
+      VAR > 0 ? stage_variant(VAR, FP64).threads : (BN == BN16 ? STAGE_THREADS : stage_threads(BN));
+  static constexpr int BASE = FP64 ? (HaloW<LIM>::value == 3 ? 1 : AMRVAC_STAGE_MINB) : AMRVAC_STAGE_MINB_MIXED;
+  static constexpr int MINB0 = BASE * 256 / THREADS < 1 ? 1 : (BASE * 256 / THREADS > 16 ? 16 : BASE * 256 / THREADS);
+  static constexpr int MINB = VAR > 0 ? stage_variant(VAR, FP64).minb : MINB0;
+  static constexpr bool ASYNC = VAR > 0 && stage_variant(VAR, FP64).async;
 };
 
-template <class TF, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS, int BN = BN16>
-__global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, LIM, BN>::MINB)
+// Asynchronous plane staging: one thread copies a block's conserved plane
+// (TB x TB doubles per variable, contiguous in HBM) into a ring slot with
+// bulk copies (cp.async.bulk, this GPU's own memory, no multicast) that
+// complete on an mbarrier; the waits are bounded (AMRVAC_ASYNC_SPINS polls)
+// and a wait that runs out raises ST_TIMEOUT.
+#ifndef AMRVAC_ASYNC_SPINS
+#define AMRVAC_ASYNC_SPINS (1 << 22)
+#endif
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t mbar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// n copies of `bytes` each, source stride sstride doubles, destination
+// stride dstride bytes; the arrival carries the expected byte count.
+__device__ __forceinline__ void plane_copy_async(uint32_t mbar, uint32_t dst, uint32_t dstride, const double *src,
+                                                 size_t sstride, int n, uint32_t bytes) {
+  // earlier generic-proxy reads of the slot before the asynchronous writes
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes * (uint32_t)n)
+               : "memory");
+  for (int v = 0; v < n; ++v)
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     dst + (uint32_t)v * dstride),
+                 "l"(src + (size_t)v * sstride), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (int i = 0; i < AMRVAC_ASYNC_SPINS; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <class TF, bool MHD, int NDIR, bool GLM, int NDIM, int SOLVER, int LIM, int BS, int BN = BN16, int VAR = 0>
+__global__ void __launch_bounds__(StageOcc<TF, LIM, BN, VAR>::THREADS, StageOcc<TF, LIM, BN, VAR>::MINB)
     fv_stage_kernel(const __grid_constant__ StageArgs A) {
   using V = Vars<MHD, NDIR, GLM>;
   constexpr int NW = V::NW;
@@ -637,7 +698,7 @@ __global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, L
   constexpr int TB = tile_edge(BN);
   constexpr int NTX = BN / TB;                       // tiles per plane row
   constexpr int NT = NDIM >= 2 ? NTX * NTX : NTX;    // tiles per plane
-  constexpr int THREADS = StageOcc<TF, LIM, BN>::THREADS;
+  constexpr int THREADS = StageOcc<TF, LIM, BN, VAR>::THREADS;
   constexpr int FB = (TB + 1) * TB;  // face-buffer stride per variable
   constexpr bool FP64 = sizeof(TF) == 8;
   constexpr int HW = HaloW<LIM>::value;  // halo width: 2, or 3 for MP5
@@ -682,6 +743,21 @@ __global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, L
   const bool need_corners = MHD && !GLM && P.divb == DIVB_LINDE;
   __shared__ int s_retry;  // some face of this phase needs the guarded FP64 recomputation
   if (t == 0) s_retry = 0;
+  // Asynchronous staging (variant; 3-D FP64, whole-plane tiles, slope
+  // limiters): the conserved plane k+2 that iteration k stages is a
+  // contiguous row of TB*TB doubles per variable, in this block or its
+  // same-level z neighbour.  One thread copies it into its ring slot at the
+  // start of the iteration; the cells convert it to primitives in place
+  // just before the z phase, the first phase that reads it, so the copy runs
+  // behind the x and y phases.  Planes behind a physical boundary or a level
+  // jump take the gather (load_prim).
+  constexpr bool ASYNC = StageOcc<TF, LIM, BN, VAR>::ASYNC && FP64 && NDIM == 3 && NT == 1 && HW == 2 &&
+                         SOLVER != SOLVER_HANCOCK;
+  __shared__ __align__(8) unsigned long long s_mbar;
+  uint32_t mphase = 0;
+  if constexpr (ASYNC) {
+    if (t == 0) mbar_init(smem_addr(&s_mbar));
+  }
 #pragma unroll 1
   while (g < gend) {
   const int col = (int)(g / PL);  // tile column: block*NT + tile
@@ -721,7 +797,23 @@ __global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, L
     const bool update = k >= k0;
     const int slot = NDIM == 3 ? ring_slot<HW>(k) : 0;
     // ---- stage plane k+HW (3-D) / the block (2-D) as primitives
-    if (cell_thread) {
+    bool pend = false;  // an asynchronous copy of plane k+HW is in flight (uniform)
+    if constexpr (ASYNC) {
+      const int kk = k + HW;
+      int src = b, sk = kk;
+      if (kk >= BN || kk < 0) {  // the z neighbour's plane, if it is a same-level block
+        src = A.nbr[b * 27 + dir_index(0, 0, kk >= BN ? 1 : -1)];
+        sk = kk >= BN ? kk - BN : kk + BN;
+      }
+      if (src >= 0 && src < A.nblocks) {
+        pend = true;
+        if (t == 0)
+          plane_copy_async(smem_addr(&s_mbar), smem_addr(&tv.center(ring_slot<HW>(kk), 0, 0, 0)),
+                           (uint32_t)(sizeof(double) * TB * TB), A.uin + cell_offset<3>(src, NW, 0, 0, 0, sk, BN),
+                           (size_t)BN * BN * BN, NW, (uint32_t)(sizeof(double) * TB * TB));
+      }
+    }
+    if (cell_thread && !pend) {
       double w[NW];
       const int kk = NDIM == 3 ? k + HW : 0;
       stb |= load_prim<MHD, NDIR, GLM, NDIM, BN>(A, b, bi, bj, kk, w);
@@ -729,6 +821,30 @@ __global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, L
 #pragma unroll
       for (int v = 0; v < NW; ++v) tv.center(s2, v, ci, cj) = TF(w[v]);
     }
+    // the asynchronous plane: wait for the copy (bounded) and convert each
+    // cell to primitives in place, with load_prim's small-value check
+    auto finish_async = [&]() {
+      if constexpr (ASYNC) {
+        if (!mbar_wait(smem_addr(&s_mbar), mphase)) {
+          stb |= ST_TIMEOUT;
+          mbar_wait(smem_addr(&s_mbar), mphase);  // a second bounded wait for the copy in flight
+        }
+        mphase ^= 1u;
+        if (cell_thread) {
+          const int s2 = ring_slot<HW>(k + HW);
+          double w[NW];
+#pragma unroll
+          for (int v = 0; v < NW; ++v) w[v] = double(tv.center(s2, v, ci, cj));
+          if (P.fix_small_values) {
+            if (small_values<double, MHD, NDIR, GLM>(w, false, P) && P.small_values_method != 1) stb |= ST_SMALL_VALUE;
+          }
+          to_primitive<MHD, NDIR, GLM>(w, P);
+#pragma unroll
+          for (int v = 0; v < NW; ++v) tv.center(s2, v, ci, cj) = TF(w[v]);
+        }
+      }
+      pend = false;
+    };
     // ---- x/y halo strips (and corners for Linde) of plane k
     constexpr int NHX = TB * H2, NHY = H2 * TB, NHC = H2 * H2;
     const int nhalo = update ? (need_corners ? NHX + NHY + NHC : NHX + NHY) : 0;
@@ -809,6 +925,10 @@ __global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, L
     const int dlo = update ? 0 : (NDIM == 3 && k == k0 - 1 ? 2 : NDIM);
 #pragma unroll 1
     for (int D = dlo; D < NDIM; ++D) {
+      if (pend && D == 2) {  // the z phase reads plane k+2 (k+HW)
+        finish_async();
+        __syncthreads();
+      }
       if (dsel >= 0 && D != dsel) continue;  // not this sweep's direction (uniform)
       const int nface = D == 0 ? (merge_yx ? FB + TB : FB) : (D == 1 && !merge_yx ? FB : TB * TB);
       // direction FD and index fl (in that direction's face layout) of face f
@@ -1061,11 +1181,16 @@ __global__ void __launch_bounds__(StageOcc<TF, LIM, BN>::THREADS, StageOcc<TF, L
           }
         }
       }
+      // plane k+2 ready for the z phase, ordered by the barrier below
+      if (pend && D == 1) finish_async();
       // the next phase overwrites the face buffer; after the last phase the
       // barrier at the end of the plane orders the reads against the next
       // plane's writes
       if (D < NDIM - 1) __syncthreads();
     }
+    // no z phase this iteration: the plane is needed by the next one (the
+    // barrier at the end of the iteration orders it)
+    if (pend) finish_async();
     }  // face phases
     if (update && cell_thread) {
       // ---- small values on wnew (src/mod_finite_volume.t:326-333; the

@@ -86,6 +86,16 @@ ALG_FLOPS = {
 NCU_TRAFFIC_PER_CELL = {"ot128": (180.652032e6 + 127.964928e6) / 128 ** 3, "ot256": None, "kh256": None}
 
 
+def _tile(ctx, zchunk):
+    """The autotuned launch shape of the stage kernel: work distribution and
+    kernel variant (threads per CTA, CTAs per SM, staging mode)."""
+    v = ctx.stage_variant()
+    return {"zchunk": zchunk, "distribution": "persistent plane ranges" if zchunk == 0 else f"z-chunks of {zchunk}",
+            "variant": v["variant"], "variants_timed": v["nvariants"], "threads": v["threads"],
+            "ctas_per_sm": v["ctas_per_sm"],
+            "staging": "asynchronous bulk copies" if v["async_staging"] else "gathered loads"}
+
+
 def _cfg_kwargs(wl: str):
     w = WORKLOADS[wl]
     if w["physics"] == "mhd":
@@ -944,7 +954,7 @@ def run_amr(args, ws, rank, local):
             "config": _config(wl),
             "run": {"cells": cells, "blocks": timed_blocks, "nw": nw,
                        "blocks_per_level": tree.counts(), "blocks_next_to_a_level_jump": timed_slots,
-                       "tree_build_s": t_build, "zchunk": zchunk, "autotuned_stage_ms": tune_ms,
+                       "tree_build_s": t_build, "tile": _tile(ctx, zchunk), "autotuned_stage_ms": tune_ms,
                        "parallelism": "replicas" if ws > 1 else "single GPU",
                        "l2": "no flush: working set %.0f MB (3 registers) > 126 MB L2" % (3 * cells * nw * 8 / 1e6),
                        "stage_weighted_cell_updates_per_s": 3 * value},
@@ -1107,7 +1117,7 @@ def run_ours(args, ws, rank, local):
         l1 = [float(np.abs(got[:, v] - ref[:, v]).sum() / max(np.abs(ref[:, v]).sum(), 1e-300))
               for v in range(ref.shape[1])]
         mixed = {"value": ws * cells * args.steps / (mt * 1e-3), "unit": UNIT, "ms_per_step": mt / args.steps,
-                 "speedup_vs_fp64": tmax / mt, "zchunk": zm, "stage_avg_ms": ms_stage / nstage,
+                 "speedup_vs_fp64": tmax / mt, "tile": _tile(cm, zm), "stage_avg_ms": ms_stage / nstage,
                  "l1_rel_err_vs_fp64_per_var": l1,
                  "l1_note": "L1 of the mixed state against the FP64 GPU state after the same warm-up + 2K steps "
                             "from the same initial state; the FP64 path itself is checked against the oracle "
@@ -1134,7 +1144,7 @@ def run_ours(args, ws, rank, local):
             "config": _config(wl),
             "execution": ("replicas, one per GPU" if ws > 1 else "single GPU") + "; the K timed steps are "
                          "replays of the captured step graph",
-            "tile": {"zchunk": zchunk, "threads": 256, "autotuned_stage_ms": tune_ms},
+            "tile": dict(_tile(ctx, zchunk), autotuned_stage_ms=tune_ms),
             "stage_weighted_cell_updates_per_s": 3 * value,
             "roofline": roofline, "roofline_other": other, "parity": parity, "cpu_baseline": cpu, "e2e": e2e,
             "mixed": mixed, "gpu_launches": launches, "clocks": clk.summary(), "status": st,

@@ -43,6 +43,7 @@ extern "C" {
 #define AMRVAC_ST_NAN          2u
 #define AMRVAC_ST_DT_TOO_SMALL 4u   /* dt < dtmin (src/mod_dt.t:55-60) */
 #define AMRVAC_ST_BOUNDS       8u   /* inconsistent neighbour table (read clamped) */
+#define AMRVAC_ST_TIMEOUT     16u   /* an asynchronous plane copy of the stage kernel did not complete in time */
 
 /* flux_scheme (src/mod_finite_volume.t method ids are private; names match) */
 #define AMRVAC_FS_TVDLF 1
@@ -260,14 +261,24 @@ int amrvac_gpu_run_timed(amrvac_ctx *ctx, int nsteps, double *total_ms, double *
 /* Measured FP64 FMA throughput of the current device (TFLOP/s, 2 flops per
  * FMA) from an in-register FMA-chain kernel; the FP64 roofline denominator. */
 int amrvac_gpu_fp64_peak(double *tflops);
-/* Work-distribution autotuner: times one stage (ps -> ps1, the state in ps is
- * left unchanged) for each candidate — 0: persistent CTAs (one wave), each
- * marching a contiguous range of z-planes across blocks; 16, 8, 4: one
- * z-chunk of that many planes per CTA (3-D only) — keeps the fastest for this
- * context and returns it.  Call after the state has been uploaded. */
+/* Autotuner (no counterpart in the reference, whose block loop has no launch
+ * shape): times one stage (ps -> ps1, the state in ps is left unchanged) for
+ * each stage-kernel variant of the scheme with each work distribution —
+ * 0: persistent CTAs (one wave), each marching a contiguous range of
+ * z-planes across blocks; block_nx, block_nx/2, block_nx/4: one z-chunk of
+ * that many planes per CTA (3-D only) — keeps the fastest pair for this
+ * context and returns the z-chunk (amrvac_gpu_stage_variant reports the
+ * variant).  Call after the state has been uploaded. */
 int amrvac_gpu_autotune(amrvac_ctx *ctx, int reps, int *best_zchunk, double *best_ms);
 /* Set the work distribution directly (0, 16, 8 or 4), e.g. from a cache. */
 int amrvac_gpu_set_zchunk(amrvac_ctx *ctx, int zchunk);
+/* Stage-kernel variants: 0 is the scheme's default kernel; the 3-D MHD
+ * HLLD + cada3 + Einfeldt + GLM scheme at block_nx 16 has three more —
+ * threads per CTA, the CTAs per SM the registers are capped for, and (FP64)
+ * asynchronous bulk-copy staging of the next conserved plane.  Select one
+ * (e.g. from a cache), or read the current one with its parameters. */
+int amrvac_gpu_set_stage_variant(amrvac_ctx *ctx, int var);
+int amrvac_gpu_stage_variant(amrvac_ctx *ctx, int *var, int *nvar, int *threads, int *ctas_per_sm, int *async);
 /* Read back the last step's dt, cmax_global and global_time (synchronises). */
 int amrvac_gpu_get_time(amrvac_ctx *ctx, double *dt, double *cmax_global, double *global_time);
 
