@@ -79,11 +79,11 @@ ALG_FLOPS = {
     "amrblast3d": dict(stage=1696.5, getdt=86.5),
 }
 # Per-launch DRAM traffic of the stage kernel from one ncu capture, bytes per
-# interior cell (profiles/fv_stage_*.md); None until captured.  ot128: the
-# FP64 kernel's stage-1 launch (ps -> ps1; algorithmic 2 * 8 * nw = 144 B per
-# cell), dram__bytes_read.sum + dram__bytes_write.sum = 180.65 MB + 127.96 MB
-# over 128^3 cells.
-NCU_TRAFFIC_PER_CELL = {"ot128": (180.652032e6 + 127.964928e6) / 128 ** 3, "ot256": None, "kh256": None}
+# interior cell; None until captured.  ot128: the FP64 kernel's stage-1
+# launch (variant 0, z-chunks of 8; ps -> ps1; algorithmic 2 * 8 * nw = 144 B
+# per cell), dram__bytes_read.sum + dram__bytes_write.sum = 181.38 MB +
+# 127.85 MB over 128^3 cells.
+NCU_TRAFFIC_PER_CELL = {"ot128": (181.381888e6 + 127.851776e6) / 128 ** 3, "ot256": None, "kh256": None}
 
 
 def _tile(ctx, zchunk):
