@@ -97,5 +97,20 @@ module mod_gpu_bridge
      integer(c_int) function amrvac_gpu_get_time(ctx, dt, cmax_global, global_time) bind(c)
        import; type(c_ptr), value :: ctx; real(c_double) :: dt, cmax_global, global_time
      end function
+     ! launch shape: time every stage-kernel variant and work distribution once
+     ! after the upload, or set a cached choice
+     integer(c_int) function amrvac_gpu_autotune(ctx, reps, best_zchunk, best_ms) bind(c)
+       import; type(c_ptr), value :: ctx; integer(c_int), value :: reps
+       integer(c_int) :: best_zchunk; real(c_double) :: best_ms
+     end function
+     integer(c_int) function amrvac_gpu_set_zchunk(ctx, zchunk) bind(c)
+       import; type(c_ptr), value :: ctx; integer(c_int), value :: zchunk
+     end function
+     integer(c_int) function amrvac_gpu_set_stage_variant(ctx, var) bind(c)
+       import; type(c_ptr), value :: ctx; integer(c_int), value :: var
+     end function
+     integer(c_int) function amrvac_gpu_stage_variant(ctx, var, nvar, threads, ctas_per_sm, async) bind(c)
+       import; type(c_ptr), value :: ctx; integer(c_int) :: var, nvar, threads, ctas_per_sm, async
+     end function
   end interface
 end module mod_gpu_bridge
