@@ -105,7 +105,7 @@ typedef struct amrvac_cfg {
   int ndim;                 /* 2 or 3 (1-D: see amrvac_gpu_create) */
   int ndir;                 /* vector components (2.5D: ndim=2, ndir=3) */
   int physics;              /* 0 = hd, 1 = mhd */
-  int block_nx[3];          /* block_nx^D; this build requires 16 */
+  int block_nx[3];          /* block_nx^D, the same in every direction: 8, 10, 12, 16 or 32 */
   int nghostcells;          /* ghost width of the host arrays (2) */
   double gamma;             /* hd_gamma / mhd_gamma */
   int flux_scheme;          /* AMRVAC_FS_* (one for all levels) */
@@ -157,7 +157,10 @@ void amrvac_gpu_default_cfg(amrvac_cfg *cfg);
 int amrvac_gpu_nw(const amrvac_cfg *cfg);
 
 /* Create a context on the current CUDA device.  Refuses unsupported options
- * (AMRVAC_E_UNSUPPORTED): block_nx != 16, 1-D, mhd hllc, 3-D Linde, ndir=1 mhd. */
+ * (AMRVAC_E_UNSUPPORTED), e.g.: 1-D, ndir < ndim, block_nx other than 8, 10,
+ * 12, 16, 32 (and, other than 16, the mixed form, MP5/WENO5 and tvdmu),
+ * small_values_method 'average' (the configuration has no geometry field:
+ * blocks are Cartesian); the text comes from amrvac_gpu_last_error(). */
 int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **ctx);
 int amrvac_gpu_destroy(amrvac_ctx *ctx);
 
