@@ -59,6 +59,7 @@ class AmrvacCfg(ctypes.Structure):
         ("dimsplit", ctypes.c_int),
         ("schmid_rad", ctypes.c_double * 3),
         ("schmid_global", ctypes.c_int),
+        ("small_values_daverage", ctypes.c_int),
     ]
 
 

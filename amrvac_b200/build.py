@@ -25,7 +25,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", 
          "--expt-relaxed-constexpr", "-I", INCLUDE]
 EXTRA = os.environ.get("AMRVAC_NVCC_EXTRA", "").split()
 UNITS = ["capi.cu", "aux.cu", "k_hd.cu", "k_mhd2.cu", "k_mhd3.cu", "noalloc.cu", "ensemble.cu", "adjoint.cu", "amr.cu", "amr_plan.cu", "k_mp5_hd.cu", "k_mp5_mhd.cu",
-         "k_bn8.cu", "k_bn10.cu", "k_bn12.cu", "k_bn32.cu", "k_tune.cu"]
+         "k_bn8.cu", "k_bn10.cu", "k_bn12.cu", "k_bn32.cu", "k_tune.cu", "smallavg.cu"]
 
 
 def _digest() -> str:

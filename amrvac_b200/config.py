@@ -101,8 +101,8 @@ class RunConfig:
 
 
 # small_values_method names in the order of amrvac_cfg.small_values_method
-# (src/mod_small_values.t:9; 'average' is not built)
-SMALL_VALUES_METHODS = ("error", "replace")
+# (src/mod_small_values.t:9)
+SMALL_VALUES_METHODS = ("error", "replace", "average")
 
 
 def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf",
@@ -113,7 +113,8 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
              small_pressure=0.0, time_stepper="threestep", ssprk_order=3, dtmin=1.0e-10,
              typeboundary=None, zchunk=0, precision="fp64", slowsteps=-1,
              time_integrator="default", nghostcells=None, dimsplit=False,
-             typedimsplit="xyyx", schmid_rad=(1.0, 1.0, 1.0), block_nx=16) -> _lib.AmrvacCfg:
+             typedimsplit="xyyx", schmid_rad=(1.0, 1.0, 1.0), block_nx=16,
+             small_values_daverage=1) -> _lib.AmrvacCfg:
     """Build an ``amrvac_cfg`` from reference-style parameter names.
 
     typeboundary: list of 2*ndim entries (min1, max1, min2, ...), each a name
@@ -165,6 +166,7 @@ def make_cfg(*, physics="hd", ndim=2, ndir=None, gamma=None, flux_scheme="tvdlf"
     for d in range(3):
         c.schmid_rad[d] = float(schmid_rad[d])
     c.schmid_global = int(limiter == "schmid1")
+    c.small_values_daverage = int(small_values_daverage)
     nw = L.amrvac_gpu_nw(c)
     tb = typeboundary or ["periodic"] * (2 * ndim)
     for s in range(6):
@@ -226,6 +228,7 @@ def config_from_par(paths) -> RunConfig:
         fix_small_values=bool(meth.get("fix_small_values", False)),
         check_small_values=bool(meth.get("check_small_values", True)),
         small_values_method=meth.get("small_values_method", "error"),
+        small_values_daverage=int(meth.get("small_values_daverage", 1)),
         small_density=float(meth.get("small_density", 0.0)),
         small_pressure=float(meth.get("small_pressure", 0.0)),
         time_stepper=ts,

@@ -89,6 +89,16 @@ struct amrvac_ctx {
   bool fixed_dir = false;  // sweep is a direction (amrvac_gpu_advect1_dim), not a sweep index
   int wave_ctas = 1;       // resident stage CTAs on the device (one wave)
   int var = 0;             // stage-kernel variant (KernelSet::stage_v; chosen by the autotuner)
+  // small_values_method 'average': whole-block recomputation of the flagged
+  // blocks (smallavg.cu), its scratch, and a pre-stage copy of a register
+  // the stage writes in place (the output's ghost values are the RK
+  // combination of the inputs' values from before the stage)
+  bool sv_on = false;
+  SvSet sv;
+  double *sv_scratch = nullptr;
+  size_t sv_per_cta = 0;
+  int sv_ctas = 0;
+  double *sv_snap = nullptr;
   int wave_v[KernelSet::MAXVAR] = {1, 1, 1, 1};  // one wave of each variant
   std::vector<double> h_dx;            // [nblocks][3] cell sizes (host copy)
   double *d_adj[3] = {nullptr, nullptr, nullptr};  // adjoint work registers (lazily)
@@ -215,9 +225,28 @@ int launch_stage(amrvac_ctx *c, int reg_ct, int reg_new, int reg_base, double a,
   if (c->zchunk > 0) nctas = c->nblocks * ntile * (c->cfg.ndim == 3 ? bn / c->zchunk : 1);
   else nctas = (int)std::min<long>(planes, hancock ? c->wave_ctas : c->wave_v[c->var]);
   const bool restore = !hancock && c->P.fix_small_values && c->P.small_values_method == 0;
-  if (restore) CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * c->nblocks, c->stream));
+  if (restore || c->sv_on) CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * c->nblocks, c->stream));
+  // 'average': a register the stage overwrites in place is copied first (the
+  // whole-block path reads its neighbours' values from before the stage)
+  const double *snap_base = nullptr, *snap_in = nullptr;
+  if (c->sv_on) {
+    const size_t bytes = sizeof(double) * c->per_block * c->nw * c->nblocks;
+    if (a != 0.0 && reg_base == reg_new) {
+      CK(cudaMemcpyAsync(c->sv_snap, c->pool[reg_base], bytes, cudaMemcpyDeviceToDevice, c->stream));
+      snap_base = c->sv_snap;
+    } else if (reg_ct == reg_new) {
+      CK(cudaMemcpyAsync(c->sv_snap, c->pool[reg_ct], bytes, cudaMemcpyDeviceToDevice, c->stream));
+      snap_in = c->sv_snap;
+    }
+    CK(c->sv.detect(A, c->pool[reg_ct], c->stream));
+    ++c->launches;
+  }
   CK(hancock ? c->ks.hancock(A, nctas, c->stream) : c->ks.stage_v[c->var](A, nctas, c->stream));
   ++c->launches;
+  if (c->sv_on) {
+    CK(c->sv.stage(A, snap_base, snap_in, SvScratch{c->sv_scratch, c->sv_per_cta}, c->sv_ctas, c->stream));
+    ++c->launches;
+  }
   if (c->cfg.ndim == 3 && c->cfg.physics == 1 && c->cfg.typedivbfix == AMRVAC_DIVB_LINDE) {
     if (!c->ks.linde3d) return fail(AMRVAC_E_UNSUPPORTED, "no 3-D Linde kernel for this configuration");
     CK(c->ks.linde3d(A, c->stream));  // addsource2 of finite_volume / hancock
@@ -254,8 +283,22 @@ int launch_getdt(amrvac_ctx *c, int reg) {
   G.red = c->d_red;
   G.P = c->P;
   G.status = c->d_status;
+  G.skip = nullptr;
+  StageArgs SA;
+  if (c->sv_on) {  // 'average': the blocks with a small value go through sv_getdt
+    SA = stage_args(c, reg, reg, reg, 0.0, 1.0, 1.0);
+    CK(cudaMemsetAsync(c->d_block_status, 0, sizeof(uint32_t) * c->nblocks, c->stream));
+    CK(c->sv.detect(SA, c->pool[reg], c->stream));
+    ++c->launches;
+    G.skip = c->d_block_status;
+  }
   CK(c->ks.getdt(G, c->stream));
   ++c->launches;
+  if (c->sv_on) {
+    CK(c->sv.getdt(SA, c->pool[reg], c->cfg.type_courant, c->d_red, SvScratch{c->sv_scratch, c->sv_per_cta},
+                   c->sv_ctas, c->stream));
+    ++c->launches;
+  }
   if (c->cfg.schmid_global) {  // a2max_global for schmid1 (getdt_courant + MPI_ALLREDUCE max)
     if (c->amr)
       if (int r = launch_amr_ghost_pass(c, reg)) return r;
@@ -461,6 +504,7 @@ void amrvac_gpu_default_cfg(amrvac_cfg *c) {
   c->fix_small_values = 0;
   c->check_small_values = 1;
   c->small_values_method = 0;
+  c->small_values_daverage = 1;
   c->time_stepper = AMRVAC_TS_THREESTEP;
   c->ssprk_order = 3;
   c->dtmin = 1.0e-10;
@@ -533,8 +577,21 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   const int nw = nw_of(cfg);
   if (nw > AMRVAC_MAX_NW) return fail(AMRVAC_E_UNSUPPORTED, "too many variables");
   if (k.precision != 0 && k.precision != 1) return fail(AMRVAC_E_ARG, "precision must be 0 (fp64) or 1 (mixed)");
-  if (k.fix_small_values && k.small_values_method != 0 && k.small_values_method != 1)
-    return fail(AMRVAC_E_UNSUPPORTED, "small_values_method: error (0) and replace (1) are built");
+  if (k.fix_small_values && (k.small_values_method < 0 || k.small_values_method > 2))
+    return fail(AMRVAC_E_UNSUPPORTED, "small_values_method: error (0), replace (1) or average (2)");
+  if (k.fix_small_values && k.small_values_method == 2) {
+    // the whole-block path of 'average' (smallavg.cu) covers FP64, unsplit
+    // finite_volume stages with the dwlimiter2 limiters and GLM or no divB
+    // source
+    if (k.precision != 0) return fail(AMRVAC_E_UNSUPPORTED, "small_values_method average: FP64 only");
+    if (k.dimsplit) return fail(AMRVAC_E_UNSUPPORTED, "small_values_method average: unsplit stages only");
+    if (k.limiter < 1 || k.limiter > 10 || k.limiter == AMRVAC_LIM_VENK)
+      return fail(AMRVAC_E_UNSUPPORTED, "small_values_method average: the dwlimiter2 limiters only");
+    if (k.physics == 1 && k.ndim > 1 && k.typedivbfix == AMRVAC_DIVB_LINDE)
+      return fail(AMRVAC_E_UNSUPPORTED, "small_values_method average: GLM or no divB source (not linde)");
+    if (uses_hancock(k)) return fail(AMRVAC_E_UNSUPPORTED, "small_values_method average: no Hancock predictor");
+    if (k.small_values_daverage < 0) return fail(AMRVAC_E_ARG, "small_values_daverage must be >= 0");
+  }
   amrvac_ctx *c = new amrvac_ctx();
   c->cfg = k;
   c->nreg = ((k.time_stepper == AMRVAC_TS_FOURSTEP && k.time_integrator == AMRVAC_TI_RK4) ||
@@ -563,6 +620,13 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
                                                 : "no kernel for this physics/ndim/ndir/solver combination");
   }
   if (bn == 16 && !special) add_stage_variants(key, &c->ks);
+  if (k.fix_small_values && k.small_values_method == 2) {
+    if (!lookup_sv(key, &c->sv)) {
+      delete c;
+      return fail(AMRVAC_E_UNSUPPORTED, "small_values_method average: no whole-block kernel for this scheme");
+    }
+    c->sv_on = true;
+  }
   cudaError_t e0;
   PhysParams &P = c->P;
   P.gamma = k.gamma;
@@ -585,6 +649,7 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   P.fix_small_values = k.fix_small_values;
   P.check_small_values = k.check_small_values;
   P.small_values_method = k.small_values_method;
+  P.small_values_daverage = k.small_values_daverage;
   // physical boundaries: per side all variables periodic, all cont, or all symm/asymm
   for (int s = 0; s < 6; ++s) {
     c->bc.kind[s] = 0;
@@ -656,6 +721,22 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
     amrvac_gpu_destroy(c);
     return cuda_fail(e, "context allocation");
   }
+  if (c->sv_on) {
+    // per CTA: five [nw][(bn+4)^ndim] arrays and two flag arrays; as many
+    // CTAs as fit in 256 MB, at most one per SM
+    size_t gc = 1;
+    for (int d = 0; d < k.ndim; ++d) gc *= (size_t)(bn + 4);
+    c->sv_per_cta = 5 * (size_t)nw * gc + (2 * gc + 7) / 8;
+    int nsm = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const size_t fit = ((size_t)256 << 20) / (sizeof(double) * c->sv_per_cta);
+    c->sv_ctas = (int)std::max<size_t>(1, std::min<size_t>(fit, (size_t)nsm));
+    if ((e = cudaMalloc(&c->sv_scratch, sizeof(double) * c->sv_per_cta * c->sv_ctas)) != cudaSuccess) {
+      amrvac_gpu_destroy(c);
+      return cuda_fail(e, "small-value scratch allocation");
+    }
+  }
   *out = c;
   return 0;
 }
@@ -675,6 +756,8 @@ int amrvac_gpu_destroy(amrvac_ctx *c) {
   cudaFree(c->d_amr_int);
   cudaFree(c->d_amr_err);
   cudaFree(c->d_stage);
+  cudaFree(c->sv_scratch);
+  cudaFree(c->sv_snap);
   delete c->amr;
   cudaFree(c->amr_gbuf);
   cudaFree(c->amr_pflux);
@@ -768,6 +851,11 @@ static int set_blocks_impl(amrvac_ctx *c, int nblocks, const double *dx, const i
       const size_t cap = (size_t)nblocks + nblocks / 4 + 1;
       for (int r = 0; r < c->nreg; ++r) CK(cudaMalloc(&c->pool[r], sizeof(double) * c->per_block * c->nw * cap));
       c->pool_cap = cap;
+      if (c->sv_on) {
+        cudaFree(c->sv_snap);
+        c->sv_snap = nullptr;
+        CK(cudaMalloc(&c->sv_snap, sizeof(double) * c->per_block * c->nw * cap));
+      }
     }
     for (int r = 0; r < c->nreg; ++r) CK(cudaMemsetAsync(c->pool[r], 0, bytes, c->stream));
   }
@@ -872,6 +960,7 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
   const int nd = c->cfg.ndim;
   if (nleaf <= 0 || !leaf || !nbase || !xprobmin || !xprobmax) return fail(AMRVAC_E_ARG, "set_amr_grid: bad arguments");
   if (nd < 2) return fail(AMRVAC_E_UNSUPPORTED, "set_amr_grid: ndim 2 or 3");
+  if (c->sv_on) return fail(AMRVAC_E_UNSUPPORTED, "set_amr_grid: not with small_values_method average");
   if (c->cfg.nghostcells != 2) return fail(AMRVAC_E_UNSUPPORTED, "set_amr_grid: nghostcells 2");
   bool periodic[3] = {true, true, true};
   for (int d = 0; d < nd; ++d) {
@@ -1713,6 +1802,7 @@ static int adjoint_step_impl(amrvac_ctx *c, const double *u0, const double *u1, 
   const amrvac_cfg &k = c->cfg;
   if (!lam || !gamma_part || !(dt > 0.0)) return fail(AMRVAC_E_ARG, "bad adjoint arguments");
   if (c->amr) return fail(AMRVAC_E_UNSUPPORTED, "adjoint: single-level grids only");
+  if (c->sv_on) return fail(AMRVAC_E_UNSUPPORTED, "adjoint: not with small_values_method average");
   if (k.physics != 0 || k.ndim != 2 || (k.flux_scheme != AMRVAC_FS_HLL && k.flux_scheme != AMRVAC_FS_HLLC) ||
       k.typeboundspeed != AMRVAC_BS_EINFELDT || (k.limiter != AMRVAC_LIM_MINMOD && k.limiter != AMRVAC_LIM_VANLEER) ||
       k.fix_small_values || k.precision != 0)

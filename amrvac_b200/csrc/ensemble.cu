@@ -697,6 +697,8 @@ int amrvac_ens_create(const amrvac_cfg *cfg, int ninst, const amrvac_ens_instanc
   if (k.time_stepper == AMRVAC_TS_TWOSTEP && k.time_integrator != AMRVAC_TI_SSPRK2)
     return efail(AMRVAC_E_UNSUPPORTED, "ensembles: twostep with time_integrator ssprk2 only");
   if (k.precision != 0 && k.precision != 1) return efail(AMRVAC_E_ARG, "precision must be 0 or 1");
+  if (k.fix_small_values && k.small_values_method == 2)
+    return efail(AMRVAC_E_UNSUPPORTED, "ensembles: small_values_method error or replace");
   for (int s = 0; s < 4; ++s)
     for (int v = 0; v < 4; ++v) {
       const int b = k.typeboundary[s][v];

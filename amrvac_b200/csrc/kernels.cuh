@@ -20,6 +20,7 @@ struct GetdtArgs {
   unsigned long long *red;
   PhysParams P;
   uint32_t *status;  // the context's status word: the small-value check of getdt
+  const uint32_t *skip;  // 'average': blocks flagged ST_SV_AVG are reduced by sv_getdt_kernel
 };
 
 __device__ __forceinline__ double warp_max(double v) {
@@ -41,6 +42,7 @@ __global__ void __launch_bounds__(256) getdt_kernel(const GetdtArgs A) {
   const int ncell = bn * (NDIM >= 2 ? bn : 1) * (NDIM == 3 ? bn : 1);
   const int b = blockIdx.x;
   const int t = threadIdx.x;
+  if (A.skip && (A.skip[b] & ST_SV_AVG)) return;
   double dxinv[3];
 #pragma unroll
   for (int d = 0; d < NDIM; ++d) dxinv[d] = 1.0 / A.dxb[b * 3 + d];
@@ -460,6 +462,21 @@ struct KernelKey {
 };
 
 bool lookup_hd(const KernelKey &k, KernelSet *out);
+// small_values_method 'average' (smallavg.cu): detection, whole-block stage
+// and getdt of the flagged blocks; scratch per CTA (SvScratch).
+struct SvScratch;
+struct SvSet {
+  cudaError_t (*detect)(const StageArgs &, const double *reg, cudaStream_t) = nullptr;
+  cudaError_t (*stage)(const StageArgs &, const double *snap_base, const double *snap_in, SvScratch, int nctas,
+                       cudaStream_t) = nullptr;
+  cudaError_t (*getdt)(const StageArgs &, const double *reg, int type_courant, unsigned long long *red, SvScratch,
+                       int nctas, cudaStream_t) = nullptr;
+};
+struct SvScratch {
+  double *base;
+  size_t per_cta;  // doubles per CTA
+};
+bool lookup_sv(const KernelKey &k, SvSet *out);
 // The variants 1..3 of the benchmark schemes' stage kernels (k_tune.cu).
 bool add_stage_variants(const KernelKey &k, KernelSet *out);
 // block edges other than 16 (k_blocks.cuh, one unit per edge)

@@ -198,6 +198,9 @@ extern "C" int amrvac_gpu_getdt_noalloc(const amrvac_cfg *cfg, const double *w_d
     if (k.block_nx[d] != bn || bn < 4 || bn % 2 || bn > 1024)
       return record_error(AMRVAC_E_UNSUPPORTED,
                           "getdt_noalloc: block_nx must be even, >= 4 and the same in every direction");
+  if (k.fix_small_values && k.small_values_method == 2)
+    return record_error(AMRVAC_E_UNSUPPORTED,
+                        "getdt_noalloc: small_values_method average needs the ghost cells of a context");
   const bool glm = k.physics == 1 && k.typedivbfix == AMRVAC_DIVB_GLM;
   BlocksFn fn = pick(k, glm);
   if (!fn) return record_error(AMRVAC_E_UNSUPPORTED, "getdt_noalloc: unsupported physics/ndim/ndir");

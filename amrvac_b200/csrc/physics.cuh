@@ -24,6 +24,9 @@ enum : int { SOLVER_TVDLF = 1, SOLVER_HLL = 2, SOLVER_HLLC = 3, SOLVER_HLLD = 4,
 enum : int { DIVB_NONE = 0, DIVB_GLM = 1, DIVB_LINDE = 4 };
 // Runtime status bits (atomicOr into the context's status word).
 enum : uint32_t { ST_SMALL_VALUE = 1u, ST_NAN = 2u, ST_DT_TOO_SMALL = 4u, ST_BOUNDS = 8u, ST_TIMEOUT = 16u };
+// Per-block only (block_status): small_values_method 'average' needs the
+// block's whole-block recomputation (smallavg.cu).
+enum : uint32_t { ST_SV_AVG = 32u };
 
 // Physics constants shared by all kernels of one context.
 struct PhysParams {
@@ -33,6 +36,7 @@ struct PhysParams {
   double schmid_rad[3];
   int limiter, boundspeed, divb, glm_extended, schmid_global;
   int fix_small_values, check_small_values, small_values_method;
+  int small_values_daverage;  // 'average': largest cube half-width
 };
 
 // Variable layout in the reference order: rho, m(1:ndir), e, [b(1:ndir), psi].

@@ -1275,8 +1275,18 @@ __global__ void __launch_bounds__(StageOcc<TF, LIM, BN, VAR>::THREADS, StageOcc<
     __syncthreads();
   }
   // the reference restores the whole block to wCT on a small-value crash
-  // (finite_volume; hancock does not)
-  if (SOLVER != SOLVER_HANCOCK && (stb & ST_SMALL_VALUE)) atomicOr(A.block_status + b, ST_SMALL_VALUE);
+  // (finite_volume; hancock does not).  With 'average' a small value sends
+  // the block to the whole-block recomputation instead (smallavg.cu), and a
+  // non-finite result goes to the block's status: the recomputation reports
+  // it only for the blocks it does not replace (another thread or CTA of
+  // the block may be the one that saw the small value).
+  if (P.small_values_method == 2) {
+    if (stb & (ST_SMALL_VALUE | ST_NAN))
+      atomicOr(A.block_status + b, ((stb & ST_SMALL_VALUE) ? ST_SV_AVG : 0u) | (stb & ST_NAN));
+    stb &= ~(ST_SMALL_VALUE | ST_NAN);
+  } else if (SOLVER != SOLVER_HANCOCK && (stb & ST_SMALL_VALUE)) {
+    atomicOr(A.block_status + b, ST_SMALL_VALUE);
+  }
   st |= stb;
   }  // while (g < gend)
   if (st) atomicOr(A.status, st);

@@ -121,7 +121,7 @@ typedef struct amrvac_cfg {
   double tvdlfeps;          /* 1.0 */
   int fix_small_values;     /* 0 */
   int check_small_values;   /* 1 */
-  int small_values_method;  /* 0 = error, 1 = replace */
+  int small_values_method;  /* 0 = error, 1 = replace, 2 = average */
   double small_density, small_pressure;
   int time_stepper;         /* AMRVAC_TS_* */
   int ssprk_order;          /* 3 */
@@ -147,6 +147,9 @@ typedef struct amrvac_cfg {
                                advect1_dim / step_dt return AMRVAC_E_STATE until
                                an amrvac_gpu_getdt has run on the current state
                                (after an upload, set_blocks or regrid) */
+  int small_values_daverage; /* small_values_daverage (src/mod_small_values.t:12):
+                               largest cube half-width of method 'average'
+                               (default 1) */
 } amrvac_cfg;
 
 typedef struct amrvac_ctx amrvac_ctx;

@@ -27,6 +27,7 @@ module mod_gpu_bridge
      integer(c_int)  :: zchunk, precision, slowsteps, time_integrator, dimsplit
      real(c_double)  :: schmid_rad(3)
      integer(c_int)  :: schmid_global
+     integer(c_int)  :: small_values_daverage
   end type
   interface
      subroutine amrvac_gpu_default_cfg(cfg) bind(c)

@@ -41,6 +41,7 @@ class OrcCfg(ctypes.Structure):
         ("dimsplit", ctypes.c_int),
         ("schmid_rad", ctypes.c_double * 3),
         ("schmid_global", ctypes.c_int),
+        ("small_values_daverage", ctypes.c_int),
     ]
 
 
@@ -134,7 +135,8 @@ def make_cfg(*, ndim=2, ndir=None, physics="hd", block_nx=16, nghost=2, gamma=No
              cada3_radius=0.1, tvdlfeps=1.0, fix_small_values=False, check_small_values=True,
              small_values_method="error", small_density=0.0, small_pressure=0.0,
              divbdiff=0.8, ssprk_order=3, time_stepper="threestep", time_integrator="default",
-             dimsplit=False, typedimsplit="xyyx", schmid_rad=(1.0, 1.0, 1.0)) -> OrcCfg:
+             dimsplit=False, typedimsplit="xyyx", schmid_rad=(1.0, 1.0, 1.0),
+             small_values_daverage=1) -> OrcCfg:
     c = OrcCfg()
     c.ndim = ndim
     c.ndir = ndim if ndir is None else ndir
@@ -156,7 +158,7 @@ def make_cfg(*, ndim=2, ndir=None, physics="hd", block_nx=16, nghost=2, gamma=No
     c.tvdlfeps = tvdlfeps
     c.fix_small_values = int(fix_small_values)
     c.check_small_values = int(check_small_values)
-    c.small_values_method = 1 if small_values_method == "replace" else 0
+    c.small_values_method = {"error": 0, "replace": 1, "average": 2}[small_values_method]
     c.small_density = small_density
     c.small_pressure = small_pressure
     c.divbdiff = divbdiff
@@ -167,6 +169,7 @@ def make_cfg(*, ndim=2, ndir=None, physics="hd", block_nx=16, nghost=2, gamma=No
     for d in range(3):
         c.schmid_rad[d] = float(schmid_rad[d])
     c.schmid_global = int(limiter == "schmid1")
+    c.small_values_daverage = int(small_values_daverage)
     lib().orc_cfg_finalize(ctypes.byref(c))
     return c
 

@@ -272,13 +272,114 @@ template <class R> int to_primitive(const State &s, const Box &b, Arr<R> &w) {
   return st;
 }
 
+// small_values_average (src/mod_small_values.t:89-144) of component iw over
+// ixO: a flagged value becomes the mean of the unflagged values of the
+// smallest cube of half-width 1 .. small_values_daverage around it (clipped
+// to the whole block array, ixI) that holds one, summed x fastest as
+// Fortran's sum(mask) does; with none, rho -> small_density and e ->
+// small_pressure.  flag: per cell of the array, false outside ixO.
+template <class R>
+void small_values_average(const State &s, Arr<R> &w, const Box &ixO, const std::vector<char> &flag, int iw) {
+  const Geo &g = s.g;
+  const Box ixI = g.ixG();
+  const int nd = s.c.ndim, dav = std::max(s.c.small_values_daverage, 1);
+  const size_t vo = g.cells * (size_t)iw;
+  forbox(ixO, [&](int i, int j, int k) {
+    if (!flag[g.idx(i, j, k)]) return;
+    const int ix[3] = {i, j, k};
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    bool ok = false;
+    for (int r = 1; r <= dav && !ok; ++r) {
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = d < nd ? std::max(ix[d] - r, ixI.lo[d]) : ix[d];
+        hi[d] = d < nd ? std::min(ix[d] + r, ixI.hi[d]) : ix[d];
+      }
+      for (int kk = lo[2]; kk <= hi[2] && !ok; ++kk)
+        for (int jj = lo[1]; jj <= hi[1] && !ok; ++jj)
+          for (int ii = lo[0]; ii <= hi[0] && !ok; ++ii) ok = !flag[g.idx(ii, jj, kk)];
+    }
+    if (ok) {
+      R sum(0.0);
+      int cnt = 0;
+      for (int kk = lo[2]; kk <= hi[2]; ++kk)
+        for (int jj = lo[1]; jj <= hi[1]; ++jj)
+          for (int ii = lo[0]; ii <= hi[0]; ++ii) {
+            const size_t p = g.idx(ii, jj, kk);
+            if (!flag[p]) { sum = sum + w.d[vo + p]; ++cnt; }
+          }
+      w.d[vo + g.idx(i, j, k)] = sum / R(double(cnt));
+    } else if (iw == s.x.e) {
+      w.d[vo + g.idx(i, j, k)] = R(s.c.small_pressure);
+    } else if (iw == s.x.rho) {
+      w.d[vo + g.idx(i, j, k)] = R(s.c.small_density);
+    }
+  });
+}
+
 // hd_check_w (src/hd/mod_hd_phys.t:648-674), mhd_check_w_origin (1452-1473),
-// handle_small_values replace/error (src/hd/mod_hd_phys.t:1420-1516,
-// src/mhd/mod_mhd_phys.t:2191-2253, src/mod_small_values.t:25-87).
+// handle_small_values replace/error/average (src/hd/mod_hd_phys.t:1420-1516,
+// src/mhd/mod_mhd_phys.t:2191-2253, src/mod_small_values.t:25-144).  The
+// array w spans the whole block (ixI); b is ixO.
 template <class R> int handle_small_values(const State &s, bool primitive, Arr<R> &w, const Box &b) {
   const Ix &x = s.x;
   const orc_cfg &c = s.c;
   int st = 0;
+  if (c.small_values_method == 2) {  // average: flags first, then the averages
+    const Geo &g = s.g;
+    std::vector<char> frho(g.cells, 0), fe(g.cells, 0);
+    bool any = false;
+    forbox(b, [&](int i, int j, int k) {
+      R m2 = W(w, x.mom[0]) * W(w, x.mom[0]);
+      for (int q = 1; q < x.ndir; ++q) m2 = m2 + W(w, x.mom[q]) * W(w, x.mom[q]);
+      bool fl_e;
+      if (primitive) {
+        fl_e = W(w, x.e) < R(c.small_pressure);
+      } else if (x.mhd) {
+        R b2 = W(w, x.mag[0]) * W(w, x.mag[0]);
+        for (int q = 1; q < x.ndir; ++q) b2 = b2 + W(w, x.mag[q]) * W(w, x.mag[q]);
+        fl_e = W(w, x.e) - half * (m2 / W(w, x.rho) + b2) < R(s.small_e);
+      } else {
+        fl_e = gam1_<R>(s) * (W(w, x.e) - half * m2 / W(w, x.rho)) < R(c.small_pressure);
+      }
+      const bool fl_r = W(w, x.rho) < R(c.small_density);
+      frho[g.idx(i, j, k)] = fl_r;
+      fe[g.idx(i, j, k)] = fl_e;
+      any = any || fl_r || fl_e;
+    });
+    if (!any) return 0;
+    const Box ixI = g.ixG();
+    auto m2_of = [&](int i, int j, int k) {
+      R m2 = W(w, x.mom[0]) * W(w, x.mom[0]);
+      for (int q = 1; q < x.ndir; ++q) m2 = m2 + W(w, x.mom[q]) * W(w, x.mom[q]);
+      return m2;
+    };
+    auto b2_of = [&](int i, int j, int k) {
+      R b2 = W(w, x.mag[0]) * W(w, x.mag[0]);
+      for (int q = 1; q < x.ndir; ++q) b2 = b2 + W(w, x.mag[q]) * W(w, x.mag[q]);
+      return b2;
+    };
+    small_values_average(s, w, b, frho, x.rho);
+    if (primitive) {
+      small_values_average(s, w, b, fe, x.e);
+    } else if (x.mhd) {  // internal energy, averaged, back (mod_mhd_phys.t:2227-2240)
+      forbox(ixI, [&](int i, int j, int k) {
+        W(w, x.e) = W(w, x.e) - half * (m2_of(i, j, k) / W(w, x.rho) + b2_of(i, j, k));
+      });
+      small_values_average(s, w, b, fe, x.e);
+      forbox(ixI, [&](int i, int j, int k) {
+        W(w, x.e) = W(w, x.e) + half * (m2_of(i, j, k) / W(w, x.rho) + b2_of(i, j, k));
+      });
+    } else {  // pressure, averaged, back (mod_hd_phys.t:1482-1489)
+      forbox(ixI, [&](int i, int j, int k) {
+        W(w, x.e) = gam1_<R>(s) * (W(w, x.e) - R(0.5) * m2_of(i, j, k) / W(w, x.rho));
+      });
+      small_values_average(s, w, b, fe, x.e);
+      forbox(ixI, [&](int i, int j, int k) {
+        W(w, x.e) = W(w, x.e) / gam1_<R>(s) + R(0.5) * m2_of(i, j, k) / W(w, x.rho);
+      });
+    }
+    return 0;
+  }
   forbox(b, [&](int i, int j, int k) {
     bool frho = W(w, x.rho) < R(c.small_density);
     bool fe;

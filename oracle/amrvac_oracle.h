@@ -59,7 +59,7 @@ typedef struct {
   double tvdlfeps;
   int fix_small_values;
   int check_small_values;
-  int small_values_method;/* 0 = error, 1 = replace */
+  int small_values_method;/* 0 = error, 1 = replace, 2 = average */
   double small_density, small_pressure;
   double divbdiff;
   int ssprk_order;        /* 3 (Gottlieb-Shu) or 2 */
@@ -68,6 +68,7 @@ typedef struct {
   int dimsplit;           /* 0 unsplit, 1 'xyyx', 2 'xy' */
   double schmid_rad[3];   /* schmid2 limiter radii per direction */
   int schmid_global;      /* schmid1: a2max_global from every getdt instead */
+  int small_values_daverage; /* cube half-width of the 'average' fix (0 means 1) */
 } orc_cfg;
 
 /* Number of flux variables implied by cfg (sets cfg->nw too). */

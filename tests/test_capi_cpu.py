@@ -68,15 +68,21 @@ def test_unsupported_configurations_are_refused_without_gpu(lib):
             make_cfg(physics="hd", ndim=2, block_nx=8, precision="mixed"),
             make_cfg(physics="hd", ndim=2, block_nx=12, limiter="mp5"),
             make_cfg(physics="mhd", ndim=2, block_nx=10, flux_scheme="tvdmu", dimsplit=True, typedivbfix="none")]
-    # small_values_method 'average' (2 in the C layout) is not built
+    # small_values_method: no method 3; 'average' outside its whole-block path
     c = make_cfg(physics="hd", ndim=2, fix_small_values=True)
-    c.small_values_method = 2
+    c.small_values_method = 3
     bad.append(c)
+    avg = dict(fix_small_values=True, small_values_method="average")
+    bad += [make_cfg(physics="hd", ndim=2, precision="mixed", flux_scheme="hllc", limiter="vanleer", **avg),
+            make_cfg(physics="mhd", ndim=2, typedivbfix="linde", flux_scheme="hll", **avg),
+            make_cfg(physics="hd", ndim=2, flux_scheme="tvdlf", time_stepper="twostep", **avg),
+            make_cfg(physics="hd", ndim=2, flux_scheme="hll", dimsplit=True, **avg),
+            make_cfg(physics="hd", ndim=2, flux_scheme="hll", limiter="venk", **avg)]
     for cfg in bad:
         r = lib.amrvac_gpu_create(ctypes.byref(cfg), ctypes.byref(h))
         assert r == _lib.E_UNSUPPORTED, lib.amrvac_gpu_last_error()
     with pytest.raises(ValueError):
-        make_cfg(physics="hd", ndim=2, fix_small_values=True, small_values_method="average")
+        make_cfg(physics="hd", ndim=2, fix_small_values=True, small_values_method="ignore")
 
 
 def test_block_nx_from_par_file(tmp_path):
