@@ -61,10 +61,10 @@ __device__ __forceinline__ void slope_partials(double a, double b, double &da, d
     }
   } else {  // vanleer: 2*max(b*a, 0) / (a + b + qsmall)
     if (b * a >= 0.0) {
-      const double den = a + b + 1.0e-12;
+      const double den = a + b + 1.0e-12, iden = rcp_(den);
       const double s = div_(2.0 * fmax(b * a, 0.0), den);
-      da = (2.0 * b - s) / den;
-      db = (2.0 * a - s) / den;
+      da = (2.0 * b - s) * iden;
+      db = (2.0 * a - s) * iden;
     } else {
       da = 0.0;
       db = 0.0;
@@ -75,8 +75,7 @@ __device__ __forceinline__ void slope_partials(double a, double b, double &da, d
 // Reverse of the HLL flux (src/mod_finite_volume.t:381-437) for one face.
 __device__ __forceinline__ void hll_reverse(const double *cL, const double *cR, const double *fL, const double *fR,
                                             double cmin, double cmax, const double *mu, double *fLb, double *fRb,
-                                            double *cLb, double *cRb, double &cmaxb, double &cminb,
-                                            bool ieee_div) {
+                                            double *cLb, double *cRb, double &cmaxb, double &cminb) {
   if (cmin >= 0.0) {
 #pragma unroll
     for (int v = 0; v < 4; ++v) fLb[v] = mu[v];
@@ -87,12 +86,12 @@ __device__ __forceinline__ void hll_reverse(const double *cL, const double *cR, 
     for (int v = 0; v < 4; ++v) fRb[v] = mu[v];
     return;
   }
-  const double iD = 1.0 / (cmax - cmin);
+  const double iD = rcp_(cmax - cmin);
 #pragma unroll
   for (int v = 0; v < 4; ++v) {
     const double dW = cR[v] - cL[v];
     const double N = cmax * fL[v] - cmin * fR[v] + cmin * cmax * dW;
-    const double F = ieee_div ? N / (cmax - cmin) : div_(N, cmax - cmin);
+    const double F = N * iD;  // the forward's flux to rounding: it enters derivatives only
     fLb[v] = mu[v] * cmax * iD;
     fRb[v] = -mu[v] * cmin * iD;
     cRb[v] = mu[v] * cmin * cmax * iD;
@@ -110,30 +109,32 @@ __device__ __forceinline__ void hllc_reverse(const double *cL, const double *cR,
                                              double cmin, double cmax, const double *mu, double *fLb, double *fRb,
                                              double *cLb, double *cRb, double &cmaxb, double &cminb) {
   if (cmin >= 0.0 || cmax <= 0.0) {
-    hll_reverse(cL, cR, fL, fR, cmin, cmax, mu, fLb, fRb, cLb, cRb, cmaxb, cminb, true);
+    hll_reverse(cL, cR, fL, fR, cmin, cmax, mu, fLb, fRb, cLb, cRb, cmaxb, cminb);
     return;
   }
-  const double Dn = cmax - cmin;
+  const double Dn = cmax - cmin, iDn = rcp_(Dn);
   double whll[2];
 #pragma unroll
-  for (int v = 0; v < 2; ++v) whll[v] = (cmax * cR[v] - cmin * cL[v] + fL[v] - fR[v]) / Dn;
-  double lam = whll[1] / whll[0];
+  for (int v = 0; v < 2; ++v) whll[v] = (cmax * cR[v] - cmin * cL[v] + fL[v] - fR[v]) * iDn;
+  const double iwh0 = rcp_(whll[0]);
+  double lam = whll[1] * iwh0;
   int patchf = 1;
   bool cond = true;
   if (cmin < 0.0 && lam > 0.0 && lam < cmax) patchf = -1;
   else if (cmax > 0.0 && lam < 0.0 && lam > cmin) patchf = 1;
   else if (lam >= cmax || lam <= cmin) { lam = 0.0; patchf = 3; cond = false; }
   if (cond && lam == 0.0) patchf = (-cmin >= cmax) ? 1 : -1;
-  if (patchf == 3) {  // the HLL flux Fhll (plain division, as the forward)
-    hll_reverse(cL, cR, fL, fR, cmin, cmax, mu, fLb, fRb, cLb, cRb, cmaxb, cminb, true);
+  if (patchf == 3) {  // the HLL flux Fhll
+    hll_reverse(cL, cR, fL, fR, cmin, cmax, mu, fLb, fRb, cLb, cRb, cmaxb, cminb);
     return;
   }
   const bool right = patchf == 1;
   const double *wS = right ? cR : cL, *fS = right ? fR : fL;
   double *wSb = right ? cRb : cLb, *fSb = right ? fRb : fLb;
   const double cs = right ? cmax : cmin;
-  const double vS = wS[1] / wS[0];
-  const double csmls = 1.0 / (cs - lam);
+  const double iw0 = rcp_(wS[0]);
+  const double vS = wS[1] * iw0;
+  const double csmls = rcp_(cs - lam);
   double wCD[4];
   wCD[0] = wS[0] * (cs - vS) * csmls;
   wCD[2] = (cs * wS[2] - fS[2]) * csmls;
@@ -190,21 +191,21 @@ __device__ __forceinline__ void hllc_reverse(const double *cL, const double *cR,
     lamb -= d;
   }
   // vS = mn / rho
-  wSb[1] += vSb / wS[0];
-  wSb[0] -= vSb * vS / wS[0];
+  wSb[1] += vSb * iw0;
+  wSb[0] -= vSb * vS * iw0;
   // lam = whll_mn / whll_rho; whll_v = (cmax wR - cmin wL + fL - fR) / Dn
   double whllb[2];
-  whllb[1] = lamb / whll[0];
-  whllb[0] = -lamb * lam / whll[0];
+  whllb[1] = lamb * iwh0;
+  whllb[0] = -lamb * lam * iwh0;
 #pragma unroll
   for (int v = 0; v < 2; ++v) {
-    const double b = whllb[v] / Dn;
+    const double b = whllb[v] * iDn;
     cRb[v] += b * cmax;
     cLb[v] -= b * cmin;
     fLb[v] += b;
     fRb[v] -= b;
-    cmaxb += whllb[v] * (cR[v] - whll[v]) / Dn;
-    cminb += whllb[v] * (whll[v] - cL[v]) / Dn;
+    cmaxb += b * (cR[v] - whll[v]);
+    cminb += b * (whll[v] - cL[v]);
   }
   if (right) cmaxb += csb;
   else cminb += csb;
@@ -244,7 +245,8 @@ __device__ __forceinline__ double face_vjp(const double *wp, int D, int fi, int 
   // Einfeldt bounds
   const double t1 = sqrt(L[0]), t2 = sqrt(R[0]), t3 = rcp_(t1 + t2);
   const double um = (L[1] * t1 + R[1] * t2) * t3, dv = R[1] - L[1];
-  const double csL = g * L[3] / L[0], csR = g * R[3] / R[0];
+  const double iL0 = rcp_(L[0]), iR0 = rcp_(R[0]);
+  const double csL = g * L[3] * iL0, csR = g * R[3] * iR0;
   const double dm = sqrt((t1 * csL + t2 * csR) * t3 + 0.5 * t1 * t2 * (t3 * t3) * (dv * dv));
   const double cmin = um - dm, cmax = um + dm;
   // ---- reverse: Riemann solver
@@ -252,12 +254,12 @@ __device__ __forceinline__ double face_vjp(const double *wp, int D, int fi, int 
   double cLb[4] = {0.0, 0.0, 0.0, 0.0}, cRb[4] = {0.0, 0.0, 0.0, 0.0};
   double cmaxb = 0.0, cminb = 0.0;
   if constexpr (SOLVER == SOLVER_HLLC) hllc_reverse(cL, cR, fL, fR, cmin, cmax, mu, fLb, fRb, cLb, cRb, cmaxb, cminb);
-  else hll_reverse(cL, cR, fL, fR, cmin, cmax, mu, fLb, fRb, cLb, cRb, cmaxb, cminb, false);
+  else hll_reverse(cL, cR, fL, fR, cmin, cmax, mu, fLb, fRb, cLb, cRb, cmaxb, cminb);
   double Lb[4] = {0.0, 0.0, 0.0, 0.0}, Rb[4] = {0.0, 0.0, 0.0, 0.0}, gb = 0.0;
   // Einfeldt reverse
   {
     const double umb = cmaxb + cminb, dmb = cmaxb - cminb;
-    const double Xb = 0.5 * dmb / dm;
+    const double Xb = 0.5 * dmb * rcp_(dm);
     const double dv2 = dv * dv, t33 = t3 * t3;
     double t1b = Xb * (csL * t3 + 0.5 * t2 * t33 * dv2) + umb * L[1] * t3;
     double t2b = Xb * (csR * t3 + 0.5 * t1 * t33 * dv2) + umb * R[1] * t3;
@@ -268,14 +270,14 @@ __device__ __forceinline__ double face_vjp(const double *wp, int D, int fi, int 
     Rb[1] += umb * t2 * t3 + dvb;
     t1b -= t3b * t33;
     t2b -= t3b * t33;
-    Lb[0] += 0.5 * t1b / t1;
-    Rb[0] += 0.5 * t2b / t2;
-    Lb[3] += csLb * g / L[0];
-    Lb[0] -= csLb * csL / L[0];
-    gb += csLb * L[3] / L[0];
-    Rb[3] += csRb * g / R[0];
-    Rb[0] -= csRb * csR / R[0];
-    gb += csRb * R[3] / R[0];
+    Lb[0] += 0.5 * t1b * rcp_(t1);
+    Rb[0] += 0.5 * t2b * rcp_(t2);
+    Lb[3] += csLb * g * iL0;
+    Lb[0] -= csLb * csL * iL0;
+    gb += csLb * L[3] * iL0;
+    Rb[3] += csRb * g * iR0;
+    Rb[0] -= csRb * csR * iR0;
+    gb += csRb * R[3] * iR0;
   }
   // physical flux and to_conserved reverse, per side
   auto side = [&](const double *W, const double *c, const double *fb, const double *cb, double *Wb) {
