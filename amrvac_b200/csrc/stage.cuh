@@ -1099,9 +1099,12 @@ __global__ void __launch_bounds__(StageOcc<TF, LIM, BN, VAR>::THREADS, StageOcc<
         stb |= face_from_states<TF, MHD, NDIR, GLM, NDIM, SOLVER, BS, FASTF>(wLp, wRp, P, TF(cg), Fr,
                                                                               HW == 2 && LIM != LIM_WENO3 && !near);
         if constexpr (RETRY) {
-          bool finite = !near;
+          // one test on the sum: an infinite or NaN flux component makes it
+          // non-finite (a finite sum that overflows only costs a retry)
+          TF fsum = Fr[0];
 #pragma unroll
-          for (int v = 0; v < NW; ++v) finite = finite && isfinite(Fr[v]);
+          for (int v = 1; v < NW; ++v) fsum = fsum + Fr[v];
+          const bool finite = !near && isfinite(fsum);
           if (!finite) {
             s_retry = 1;
             Fr[0] = TF(NAN);
