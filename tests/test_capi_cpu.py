@@ -117,6 +117,44 @@ def test_block_nx_from_par_file(tmp_path):
         config_from_par_text(base % 16)
 
 
+def test_small_values_from_par_file(tmp_path):
+    """fix_small_values, small_values_method and small_values_daverage of
+    &methodlist reach the configuration (src/mod_small_values.t:9-12)."""
+    from amrvac_b200.config import config_from_par
+    f = tmp_path / "sv.par"
+    f.write_text("""
+ &methodlist
+        time_stepper = 'threestep'
+        flux_scheme = 20*'hllc'
+        limiter = 20*'cada3'
+        fix_small_values = .true.
+        small_values_method = 'average'
+        small_values_daverage = 2
+        small_density = 1.d-6
+        small_pressure = 1.d-7
+ /
+ &meshlist
+        domain_nx1=32
+        domain_nx2=32
+ /
+ &hd_list
+ /
+""")
+    rc = config_from_par([str(f)])
+    c = rc.cfg
+    assert c.fix_small_values == 1 and c.small_values_method == 2 and c.small_values_daverage == 2
+    assert c.small_density == 1e-6 and c.small_pressure == 1e-7
+
+
+def test_stage_variant_entry_points_check_their_arguments(lib):
+    """The launch-shape entry points refuse a null context (no device
+    needed)."""
+    v = [ctypes.c_int() for _ in range(5)]
+    assert lib.amrvac_gpu_set_stage_variant(None, 0) < 0
+    assert lib.amrvac_gpu_stage_variant(None, *[ctypes.byref(x) for x in v]) < 0
+    assert lib.amrvac_gpu_set_zchunk(None, 0) < 0
+
+
 def test_par_namelist_parser():
     from amrvac_b200 import parse_namelists
     text = """
