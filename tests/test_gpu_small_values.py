@@ -248,3 +248,20 @@ def test_average_steps_match_oracle(oracle_lib, name):
         assert np.isfinite(got).all()
         assert err <= max(RTOL, noise), f"{name} step {step}: {err:.3e} (oracle self-noise {noise:.3e})"
     assert ctx.status() == 0
+
+
+def test_average_graph_replay_matches_direct_steps(oracle_lib):
+    """The captured step graph (amrvac_gpu_run) holds the detection, the
+    register copy and the whole-block recomputation: three replayed steps
+    give the directly launched steps bit for bit."""
+    _cuda()
+    O = oracle_lib
+    _, a, nd = _setup_avg(O, "mhd3_hlld_cada3_glm_dip")
+    _, b, _ = _setup_avg(O, "mhd3_hlld_cada3_glm_dip")
+    a.set_time(0.0, 1.0e99, 0.0)
+    b.set_time(0.0, 1.0e99, 0.0)
+    for _ in range(3):
+        a.step()
+    b.run(3)
+    assert np.array_equal(a.download(), b.download())
+    assert a.status() == 0 and b.status() == 0
