@@ -91,9 +91,12 @@ __device__ __forceinline__ bool ens_rows(const EnsArgs &A, int tile, bool for_ge
   return __syncthreads_or(act) != 0;
 }
 
+// The mixed form's FP32 faces use the hardware approximations (rcp.approx /
+// sqrt.approx, about one FP32 ulp) as the stage kernel's do; FP64 faces keep
+// the guarded division (this kernel has no recomputation pass).
 template <class TF, int ND, int SOLVER>
 __device__ __forceinline__ uint32_t ens_face(TF *wLp, TF *wRp, const PhysParams &P, TF *F) {
-  return face_from_states<TF, false, ND, false, ND, SOLVER, 0>(wLp, wRp, P, TF(0), F);
+  return face_from_states<TF, false, ND, false, ND, SOLVER, 0, sizeof(TF) == 4>(wLp, wRp, P, TF(0), F);
 }
 
 // Stage kernel organisation: 288 threads.  Threads 0..255 own the cells of
@@ -178,7 +181,7 @@ __device__ __forceinline__ uint32_t ens_face_at(const TF *s, const EnsView<TF, N
     for (int o = 0; o < 4; ++o) q[o] = s[base[o] + ov * strd[o]];
     const TF d0 = q[1] - q[0], d1 = q[2] - q[1], d2 = q[3] - q[2];
     TF ldw, rdw;
-    face_slopes<TF, 0>(lim, d0, d1, d2, rd, ldw, rdw);
+    face_slopes<TF, 0, sizeof(TF) == 4>(lim, d0, d1, d2, rd, ldw, rdw);
     wLp[v] = q[1] + TF(0.5) * ldw;
     wRp[v] = q[2] - TF(0.5) * rdw;
   }
