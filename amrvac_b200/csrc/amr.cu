@@ -186,10 +186,12 @@ __device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int
 // 2 x 16 x 16 cells, an edge 2 x 2 x 16, a corner 2 x 2 x 2), so no thread
 // walks the interior; the coarse representation psc is built first, only
 // where some prolongation stencil reads it.
-template <int NDIM>
+// BNC: the block edge as a constant (16, the default) so that the index
+// arithmetic folds, or 0 to read it from the arguments.
+template <int NDIM, int BNC = 0>
 __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
   extern __shared__ double psc[];  // (bn/2+4)^NDIM coarse representation of variable blockIdx.y
-  const int bn = A.bn;
+  const int bn = BNC ? BNC : A.bn;
   const int C = bn / 2 + 4, CY = NDIM >= 2 ? C : 1, CZ = NDIM >= 3 ? C : 1;
   __shared__ int s_off[28];        // prefix sums of the jump regions' cell counts
   __shared__ int s_q[27], s_kind[27];
@@ -467,8 +469,13 @@ cudaError_t launch_amr_ghosts(const AmrGhostArgs &A, int nslots, int ndim, cudaS
   if (nslots <= 0) return cudaSuccess;
   const dim3 grid(nslots, A.nw);
   const size_t c = (size_t)A.bn / 2 + 4;  // psc edge
-  if (ndim == 2) amr_ghost_kernel<2><<<grid, 256, sizeof(double) * c * c, s>>>(A);
-  else amr_ghost_kernel<3><<<grid, 256, sizeof(double) * c * c * c, s>>>(A);
+  if (A.bn == 16) {
+    if (ndim == 2) amr_ghost_kernel<2, 16><<<grid, 256, sizeof(double) * c * c, s>>>(A);
+    else amr_ghost_kernel<3, 16><<<grid, 256, sizeof(double) * c * c * c, s>>>(A);
+  } else {
+    if (ndim == 2) amr_ghost_kernel<2><<<grid, 256, sizeof(double) * c * c, s>>>(A);
+    else amr_ghost_kernel<3><<<grid, 256, sizeof(double) * c * c * c, s>>>(A);
+  }
   return cudaGetLastError();
 }
 

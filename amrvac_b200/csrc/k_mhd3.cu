@@ -10,13 +10,22 @@ bool lookup_mhd3(const KernelKey &k, KernelSet *out) {
       *out = Launch<true, 3, true, 3, SOLVER_HLLD, LIM_CADA3, BS_EINFELDT, float>::set();
       return true;
     }
+    if (k.glm && k.solver == SOLVER_HLLD && k.limiter == LIM_VANLEER && k.boundspeed == BS_EINFELDT) {
+      *out = Launch<true, 3, true, 3, SOLVER_HLLD, LIM_VANLEER, BS_EINFELDT, float>::set();
+      return true;
+    }
     if (k.glm && k.solver == SOLVER_HLLD) { *out = Launch<true, 3, true, 3, SOLVER_HLLD, 0, 0, float>::set(); return true; }
     if (k.glm && k.solver == SOLVER_HLL) { *out = Launch<true, 3, true, 3, SOLVER_HLL, 0, 0, float>::set(); return true; }
     return false;
   }
   // compile-time limiter / bound speed for the 3-D Orszag-Tang configuration
+  // and the 3-D blast on the multi-level grid
   if (k.glm && k.solver == SOLVER_HLLD && k.limiter == LIM_CADA3 && k.boundspeed == BS_EINFELDT) {
     *out = Launch<true, 3, true, 3, SOLVER_HLLD, LIM_CADA3, BS_EINFELDT>::set();
+    return true;
+  }
+  if (k.glm && k.solver == SOLVER_HLLD && k.limiter == LIM_VANLEER && k.boundspeed == BS_EINFELDT) {
+    *out = Launch<true, 3, true, 3, SOLVER_HLLD, LIM_VANLEER, BS_EINFELDT>::set();
     return true;
   }
 #define AMRVAC_M3(GLM, S)                                       \
