@@ -265,3 +265,49 @@ def test_average_graph_replay_matches_direct_steps(oracle_lib):
     b.run(3)
     assert np.array_equal(a.download(), b.download())
     assert a.status() == 0 and b.status() == 0
+
+
+@pytest.mark.parametrize("bn,bc", [(8, "cont"), (16, "symm")])
+def test_average_block_edges_and_physical_sides(oracle_lib, bn, bc):
+    """'average' on 8^3 blocks with 'cont' sides and on 16^3 blocks with
+    'symm' sides: the cubes of cells next to the domain boundary reach the
+    physical ghost cells, which the device gathers as the reference's
+    boundary fill leaves them; two full steps against the oracle."""
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    O = oracle_lib
+    kw = dict(physics="hd", ndim=3, gamma=1.4, flux_scheme="hllc", limiter="cada3", fix_small_values=True,
+              small_values_method="average", small_density=1e-3, small_pressure=1e-8)
+    n = 2 * bn
+    ocfg = O.make_cfg(block_nx=bn, **kw)
+
+    def grid(noisy):
+        cons = _dip("hd", 3, 3, n, False, ocfg.gamma, 1e-3)
+        blocks = P.to_blocks(cons, 3, bn=bn)
+        if noisy:
+            blocks = one_ulp_noise(blocks)
+        g = O.Grid(ocfg, [n] * 3, [0.0] * 3, [1.0] * 3, [bc] * 6)
+        for ib in range(g.nblocks):
+            g.set_block(ib, blocks[ib])
+        g.getbc()
+        return g, blocks
+    og, blocks = grid(False)
+    gn, _ = grid(True)
+    ctx = Context(make_cfg(block_nx=bn, typeboundary=[bc] * 6, **kw))
+    ctx.set_uniform_grid([n] * 3, [0.0] * 3, [1.0] * 3)
+    ctx.upload(blocks)
+    ctx.set_time(0.0, 1.0e99, 0.0)
+    for step in range(2):
+        dt_ref, cg_ref = og.getdt()
+        gn.getdt()
+        ctx.step()
+        dt = ctx.get_time()[0]
+        assert abs(dt - dt_ref) <= 1e-13 * dt_ref
+        og.advance(dt_ref, cg_ref)
+        gn.advance(dt_ref, cg_ref)
+        got = P.interior(ctx.download(), 3)
+        ref = P.interior(np.array([og.get_block(ib) for ib in range(og.nblocks)]), 3)
+        noise = percell_err(P.interior(np.array([gn.get_block(ib) for ib in range(gn.nblocks)]), 3), ref)
+        err = percell_err(got, ref)
+        assert err <= max(RTOL, noise), (bn, bc, step, err, noise)
+    assert ctx.status() == 0
