@@ -126,6 +126,7 @@ SIGNATURES = [
     ("amrvac_gpu_lohner", _i, [_vp, _i, _dp, _ip, _i, _dp, _dp, _dp, _ip, _ip, _dp]),
     ("amrvac_gpu_step_dt", _i, [_vp, _d]),
     ("amrvac_gpu_register_copy", _i, [_vp, _i, _vp, _i]),
+    ("amrvac_gpu_step_dt_states", _i, [_vp, _d, _vp, _vp, _vp, _vp]),
     ("amrvac_gpu_adjoint_step", _i, [_vp, _vp, _d, _vp]),
     ("amrvac_gpu_adjoint_step_states", _i, [_vp, _vp, _vp, _vp, _vp, _d, _vp]),
     ("amrvac_ens_create", _i, [_cfgp, _i, _P(AmrvacEnsInstance), _P(_vp)]),

@@ -1782,6 +1782,53 @@ int amrvac_gpu_register_copy(amrvac_ctx *c, int reg, double *dev, int to_registe
   return 0;
 }
 
+// One step at dt whose stage inputs and result live in the caller's buffers.
+// The stages are those of launch_rk (same kernels, coefficients and order),
+// with the registers pointed at the caller's buffers for the duration of the
+// call: stage 1 reads u0 and writes u1, stage 2 writes u2 (threestep), the
+// last stage writes unew (which may be u0: its base is read cell by cell).
+int amrvac_gpu_step_dt_states(amrvac_ctx *c, double dt, const double *u0, double *u1, double *u2, double *unew) {
+  if (int r = check_ctx(c, true)) return r;
+  const amrvac_cfg &k = c->cfg;
+  const bool three = k.time_stepper == AMRVAC_TS_THREESTEP;
+  if (!three && !(k.time_stepper == AMRVAC_TS_TWOSTEP && k.time_integrator == AMRVAC_TI_SSPRK2))
+    return fail(AMRVAC_E_UNSUPPORTED, "step_dt_states: threestep or twostep with time_integrator ssprk2");
+  if (c->amr || k.dimsplit || c->sv_on)
+    return fail(AMRVAC_E_UNSUPPORTED, "step_dt_states: single-level unsplit grids, no small_values average");
+  if (!(dt > 0.0)) return fail(AMRVAC_E_ARG, "dt must be positive");
+  if (!u0 || !u1 || (three && !u2)) return fail(AMRVAC_E_ARG, "step_dt_states: null stage buffer");
+  const double *last_in = three ? u2 : u1;
+  if (u1 == u0 || (three && (u2 == u0 || u2 == u1)) || (unew && (unew == last_in || (three && unew == u1))))
+    return fail(AMRVAC_E_ARG, "step_dt_states: a stage would read and write the same buffer");
+  if (int r = check_a2max(c)) return r;
+  CK(launch_set_scalar(c->d_scal + 0, dt, c->stream));
+  ++c->launches;
+  double *const saved[3] = {c->pool[0], c->pool[1], c->pool[2]};
+  c->pool[0] = const_cast<double *>(u0);  // read only: every stage takes it as input or base
+  c->pool[1] = u1;
+  int r;
+  if (!three) {
+    r = launch_stage(c, 0, 1, 0, 0.0, 1.0, 1.0);
+    if (!r && unew) {
+      c->pool[2] = unew;
+      r = launch_stage(c, 1, 2, 0, 0.5, 0.5, 0.5);
+    }
+  } else {
+    double b11, b22, b33, a21, a31;
+    if (k.ssprk_order == 2) { b11 = 0.5; b22 = 0.5; b33 = 1.0 / 3.0; a21 = 0.0; a31 = 1.0 / 3.0; }
+    else { b11 = 1.0; b22 = 1.0 / 4.0; b33 = 2.0 / 3.0; a21 = 3.0 / 4.0; a31 = 1.0 / 3.0; }
+    c->pool[2] = u2;
+    r = launch_stage(c, 0, 1, 0, 0.0, 1.0, b11);
+    if (!r) r = launch_stage(c, 1, 2, 0, a21, 1.0 - a21, b22);
+    if (!r && unew) {
+      c->pool[1] = unew;
+      r = launch_stage(c, 2, 1, 0, a31, 1.0 - a31, b33);
+    }
+  }
+  for (int i = 0; i < 3; ++i) c->pool[i] = saved[i];
+  return r;
+}
+
 static int adjoint_step_impl(amrvac_ctx *c, const double *u0, const double *u1, const double *u2, double *lam,
                              double dt, double *gamma_part);
 

@@ -366,6 +366,14 @@ int amrvac_gpu_step_dt(amrvac_ctx *ctx, double dt);
 /* Copy a whole register to (to_register = 0) or from (1) the caller's device
  * buffer dev (register layout [block][var][y][x], 16^ndim per block). */
 int amrvac_gpu_register_copy(amrvac_ctx *ctx, int reg, double *dev, int to_register);
+/* One step with a given dt whose stage inputs and result are the caller's
+ * device buffers (register layout), so that a checkpointed sweep keeps every
+ * stage input without copies: the stages of amrvac_gpu_step_dt read u0 = U^n
+ * and write u1, u2 (the inputs of stages 2 and 3; u2 unused for twostep) and
+ * unew = U^{n+1}, which may be u0; unew NULL skips the last stage.  threestep
+ * or twostep ssprk2, single-level unsplit grids; the registers are not
+ * touched.  Asynchronous on the context stream. */
+int amrvac_gpu_step_dt_states(amrvac_ctx *ctx, double dt, const double *u0, double *u1, double *u2, double *unew);
 /* Adjoint of one step U^n -> U^{n+1} at frozen dt, with U^n in register 0:
  * lam (device, register layout) holds dL/dU^{n+1} on entry and dL/dU^n on
  * return; gamma_part (device, [nblocks]) accumulates dL/dgamma of the step

@@ -155,6 +155,12 @@ def test_stage_variant_entry_points_check_their_arguments(lib):
     assert lib.amrvac_gpu_set_zchunk(None, 0) < 0
 
 
+def test_step_with_caller_stage_buffers_checks_its_arguments(lib):
+    """amrvac_gpu_step_dt_states refuses a null context before it touches a
+    buffer (no device needed)."""
+    assert lib.amrvac_gpu_step_dt_states(None, 1.0, None, None, None, None) < 0
+
+
 def test_par_namelist_parser():
     from amrvac_b200 import parse_namelists
     text = """

@@ -198,3 +198,52 @@ def test_recomputing_and_supplied_stage_states_agree():
     s.ctx.synchronize()
     s.close()
     assert torch.equal(la, lb) and torch.equal(ga, gb)
+
+
+@pytest.mark.parametrize("stepper", [dict(), dict(time_stepper="twostep", time_integrator="ssprk2")])
+def test_step_with_caller_stage_buffers_matches_the_registers(stepper):
+    """amrvac_gpu_step_dt_states writes the same stage inputs and U^{n+1} as
+    amrvac_gpu_step_dt leaves in the registers (bit-identical), also in place
+    (unew = u0); without unew it leaves u0 untouched; aliased stage buffers
+    are refused."""
+    _cuda()
+    import ctypes
+    import torch
+    from amrvac_b200 import _lib
+    from amrvac_b200.adjoint import FrozenDtSolver, domain_to_blocks
+    from tests import _problems as P
+    n = 32
+    cons = P.prim_to_cons(P.random_smooth("hd", 2, 2, n, seed=6), "hd", 2, B.GAMMA)[:, 0]
+    U0 = domain_to_blocks(torch.tensor(cons, dtype=torch.float64, device="cuda")).contiguous()
+    s = FrozenDtSolver((n, n), (0.0, 0.0), (1.0, 1.0), B.GAMMA, limiter="vanleer", typeboundary=["cont"] * 4,
+                       **stepper)
+    nst = s._nstages()
+    dt = float(s.cfl_dts(U0, 1)[0])
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    ref = [torch.empty(s.shape, dtype=torch.float64, device="cuda") for _ in range(3)]
+    s._load(U0)
+    _lib.check(s.L.amrvac_gpu_step_dt(s.ctx.h, dt), "step_dt")
+    for r in range(3):
+        s._store(ref[r], r)
+    got = [U0.clone()] + [torch.full(s.shape, np.nan, dtype=torch.float64, device="cuda") for _ in range(3)]
+    torch.cuda.synchronize()
+    u2 = p(got[2]) if nst == 3 else None
+    _lib.check(s.L.amrvac_gpu_step_dt_states(s.ctx.h, dt, p(got[0]), p(got[1]), u2, p(got[3])), "step_dt_states")
+    s.ctx.synchronize()
+    assert torch.equal(got[0], U0) and torch.equal(got[1], ref[1]) and torch.equal(got[3], ref[0])
+    if nst == 3:
+        assert torch.equal(got[2], ref[2])
+    # in place: U^{n+1} over u0; no last stage: u0 untouched
+    _lib.check(s.L.amrvac_gpu_step_dt_states(s.ctx.h, dt, p(got[0]), p(got[1]), u2, p(got[0])), "step_dt_states")
+    s.ctx.synchronize()
+    assert torch.equal(got[0], ref[0])
+    got[0].copy_(U0)
+    torch.cuda.synchronize()
+    _lib.check(s.L.amrvac_gpu_step_dt_states(s.ctx.h, dt, p(got[0]), p(got[1]), u2, None), "step_dt_states")
+    s.ctx.synchronize()
+    assert torch.equal(got[0], U0) and torch.equal(got[1], ref[1])
+    # a stage that would read and write one buffer
+    last = got[2] if nst == 3 else got[1]
+    assert s.L.amrvac_gpu_step_dt_states(s.ctx.h, dt, p(got[0]), p(got[0]), u2, None) == _lib.E_ARG
+    assert s.L.amrvac_gpu_step_dt_states(s.ctx.h, dt, p(got[0]), p(got[1]), u2, p(last)) == _lib.E_ARG
+    s.close()
