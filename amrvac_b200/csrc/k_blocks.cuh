@@ -1,9 +1,9 @@
 // Stage / getdt / point kernels for block edges other than 16 (block_nx 8,
 // 10, 12, 32: the reference's own 3-D blast and Kelvin-Helmholtz and 2-D
 // Riemann tests run 8^3, 10^3 and 12^2 blocks).  FP64, the slope limiters
-// and bound speeds at run time (LIM = 0, BS = 0), every solver but
-// TVD-MUSCL.  Each block edge is instantiated in its own translation unit
-// (k_bn*.cu) so that they compile in parallel.
+// and bound speeds at run time (LIM = 0, BS = 0), every solver (TVD-MUSCL
+// with its MUSCL-Hancock predictor).  Each block edge is instantiated in its
+// own translation unit (k_bn*.cu) so that they compile in parallel.
 #pragma once
 
 #include "kernels.cuh"
@@ -12,7 +12,7 @@ namespace amrvac {
 
 template <int BN>
 bool lookup_bn(const KernelKey &k, KernelSet *out) {
-  if (k.bn != BN || k.mixed || k.solver == SOLVER_TVDMU) return false;
+  if (k.bn != BN || k.mixed) return false;
   if (!k.mhd) {
     if (k.ndir != k.ndim) return false;
 #define AMRVAC_BHD(ND, S)                                              \
@@ -23,9 +23,11 @@ bool lookup_bn(const KernelKey &k, KernelSet *out) {
     AMRVAC_BHD(2, SOLVER_TVDLF)
     AMRVAC_BHD(2, SOLVER_HLL)
     AMRVAC_BHD(2, SOLVER_HLLC)
+    AMRVAC_BHD(2, SOLVER_TVDMU)
     AMRVAC_BHD(3, SOLVER_TVDLF)
     AMRVAC_BHD(3, SOLVER_HLL)
     AMRVAC_BHD(3, SOLVER_HLLC)
+    AMRVAC_BHD(3, SOLVER_TVDMU)
 #undef AMRVAC_BHD
     return false;
   }
@@ -45,6 +47,10 @@ bool lookup_bn(const KernelKey &k, KernelSet *out) {
   AMRVAC_BM4(2, 3, true)
   AMRVAC_BM4(3, 3, false)
   AMRVAC_BM4(3, 3, true)
+  // TVD-MUSCL without GLM, as at block edge 16
+  AMRVAC_BM(2, 2, false, SOLVER_TVDMU)
+  AMRVAC_BM(2, 3, false, SOLVER_TVDMU)
+  AMRVAC_BM(3, 3, false, SOLVER_TVDMU)
 #undef AMRVAC_BM4
 #undef AMRVAC_BM
   return false;

@@ -20,7 +20,9 @@ ot_2d_2step_tvdmu_al.log; and the 2-D blast wave with cont
 boundaries, tests/hd/blast_wave_Cartesian_2D/correct_output/
 bw_2d_{3step_hll_cada,4step_hll_mc,4step_hllc_ko,rk4_tvdlf_cada,
 2step_tvdlf_mm,2step_tvdmu_al}.log (the last with TVD-MUSCL, dimensionally
-split).
+split); the 3-D MHD blast wave (8^3 blocks), the 2-D Riemann problem (12^2
+blocks) and the 3-D MHD Kelvin-Helmholtz jet (10^3 blocks) in the schemes
+listed below.
 They are copied verbatim so the parity tests can run where the reference
 repository is absent.
 """
@@ -64,6 +66,7 @@ LOGS = [
     "tests/hd/Riemann_2D/correct_output/rm_2d_4step_hllc_ko.log",
     "tests/hd/Riemann_2D/correct_output/rm_2d_rk4_tvdlf_cada.log",
     "tests/hd/Riemann_2D/correct_output/rm_2d_2step_tvdlf_mm.log",
+    "tests/hd/Riemann_2D/correct_output/rm_2d_2step_tvdmu_al.log",
     # 3-D MHD with 10^3 blocks (block_nx 10), periodic x, cont y and z
     "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_3step_hll_cada.log",
     "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_3step_hlld_cada.log",
@@ -71,6 +74,7 @@ LOGS = [
     "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_4step_hllc_ko.log",
     "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_rk4_tvdlf_cada.log",
     "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_2step_tvdlf_mm.log",
+    "tests/mhd/Kelvin_Helmholtz_3D/correct_output/kh_3D_2step_tvdmu_al.log",
 ]
 
 

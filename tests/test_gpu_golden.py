@@ -290,7 +290,7 @@ def test_blast_wave_3d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
 # 24^2 level-1 cells in 12^2 blocks (block_nx 12), cont boundaries,
 # refine_max_level 3 with the default estimator settings (w_refine_weight(1)
 # = 1, refine_threshold 0.1), gamma 1.4, four quadrants about (0.5, 0.5);
-# log every 1e-2 to t = 0.5.  (Its TVD-MUSCL log needs block_nx 16.)
+# log every 1e-2 to t = 0.5.
 
 
 def _rm2d_prim(X, Y, Z):
@@ -314,6 +314,8 @@ def _rm2d_prim(X, Y, Z):
     ("rk4_tvdlf_cada", dict(flux_scheme="tvdlf", limiter="cada3", typeboundspeed="cmaxmean", time_stepper="fourstep",
                             time_integrator="rk4")),
     ("2step_tvdlf_mm", dict(flux_scheme="tvdlf", limiter="minmod", typeboundspeed="cmaxmean", time_stepper="twostep")),
+    ("2step_tvdmu_al", dict(flux_scheme="tvdmu", limiter="albada", typeboundspeed="cmaxmean", time_stepper="twostep",
+                            dimsplit=True)),
 ])
 def test_riemann_2d_amr_golden_log_gpu(oracle_lib, name, kw):
     kw = dict(kw, courantpar=0.9, gamma=1.4, dtmin=1.0e-6)
@@ -331,8 +333,7 @@ def test_riemann_2d_amr_golden_log_gpu(oracle_lib, name, kw):
 # periodic in x, cont in y and z, refine_max_level 3 with w_refine_weight
 # 0.4 (rho) and 0.2 (m1, m2, m3), refine_threshold 0.2, slowsteps 10; rho = 1,
 # p = 1, B = (0.129, 0, 0), v_x = 0.645 tanh((r - 0.5)/0.05) with an m = 1
-# perturbation of 0.01 in v_y, v_z; log every 1e-3 to t = 0.01.  (Its
-# TVD-MUSCL log needs block_nx 16.)
+# perturbation of 0.01 in v_y, v_z; log every 1e-3 to t = 0.01.
 
 
 def _kh3d_prim(nw):
@@ -364,6 +365,8 @@ def _kh3d_prim(nw):
                             time_stepper="fourstep", time_integrator="rk4"), 8),
     ("2step_tvdlf_mm", dict(flux_scheme="tvdlf", limiter="minmod", typedivbfix="linde", typeboundspeed="cmaxmean",
                             time_stepper="twostep"), 8),
+    ("2step_tvdmu_al", dict(flux_scheme="tvdmu", limiter="albada", typedivbfix="linde", typeboundspeed="cmaxmean",
+                            time_stepper="twostep", dimsplit=True), 8),
 ])
 def test_kelvin_helmholtz_3d_amr_golden_log_gpu(oracle_lib, name, kw, nw):
     kw = dict(kw, courantpar=0.9, slowsteps=10)
