@@ -142,6 +142,8 @@ SIGNATURES = [
     ("amrvac_ens_set_grid", _i, [_vp, _i]),
     ("amrvac_ens_grid", _i, [_vp, _ip, _ip]),
     ("amrvac_ens_autotune", _i, [_vp, _i, _ip, _dp]),
+    ("amrvac_ens_set_variant", _i, [_vp, _i]),
+    ("amrvac_ens_variant", _i, [_vp, _ip, _ip, _ip]),
     ("amrvac_ens_stream", _i, [_vp, _P(_vp)]),
     ("amrvac_ens_launch_count", _i64, [_vp]),
 ]

@@ -348,8 +348,19 @@ __device__ __forceinline__ void ens_stage_body(const EnsArgs &A) {
 // Occupancy: two CTAs of 288 threads per SM in FP64 (96 registers: 18 warps
 // put five on one SM sub-partition, whose 16 K registers then cap a thread at
 // 102), three in the mixed form (72 registers, measured 1.23x faster than two).
+// Each form has a second variant one CTA per SM denser, which the autotuner
+// times against the first: FP64 at three CTAs (72 registers, a few spilled),
+// mixed at four (56 registers).
 __global__ void __launch_bounds__(ENS_THREADS, 2) ens_stage_kernel_fp64(const EnsArgs A) { ens_stage_body<double>(A); }
+__global__ void __launch_bounds__(ENS_THREADS, 3) ens_stage_kernel_fp64_3(const EnsArgs A) { ens_stage_body<double>(A); }
 __global__ void __launch_bounds__(ENS_THREADS, 3) ens_stage_kernel_mixed(const EnsArgs A) { ens_stage_body<float>(A); }
+__global__ void __launch_bounds__(ENS_THREADS, 4) ens_stage_kernel_mixed_4(const EnsArgs A) { ens_stage_body<float>(A); }
+
+// the stage kernel of (precision, variant)
+static void (*ens_stage_fn(bool mixed, int var))(const EnsArgs) {
+  if (mixed) return var == 1 ? ens_stage_kernel_mixed_4 : ens_stage_kernel_mixed;
+  return var == 1 ? ens_stage_kernel_fp64_3 : ens_stage_kernel_fp64;
+}
 
 // getdt_courant (src/mod_dt.t:160-287), maxsum, per instance: the max over
 // the instance's cells of sum_d (|v_d| + c_s) / dx_d.
@@ -496,7 +507,10 @@ struct amrvac_ens {
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   int grid = 0;          // CTAs per stage / getdt launch
-  int wave = 1;          // resident stage CTAs
+  int wave = 1;          // resident stage CTAs of the current variant
+  int var = 0;           // stage-kernel variant: 1 is one CTA per SM denser than 0
+  int nvar = 2;
+  int wave_v[2] = {1, 1};
   int64_t launches = 0;
 };
 
@@ -564,8 +578,7 @@ EnsTime ens_time(amrvac_ens *e) {
 
 int ens_launch_stage(amrvac_ens *e, int reg_ct, int reg_new, int reg_base, double a, double b, double dtf) {
   const EnsArgs A = ens_args(e, reg_ct, reg_new, reg_base, a, b, dtf);
-  if (e->mixed) ens_stage_kernel_mixed<<<e->grid, ENS_THREADS, ens_smem(true), e->stream>>>(A);
-  else ens_stage_kernel_fp64<<<e->grid, ENS_THREADS, ens_smem(false), e->stream>>>(A);
+  ens_stage_fn(e->mixed, e->var)<<<e->grid, ENS_THREADS, ens_smem(e->mixed), e->stream>>>(A);
   ECK(cudaGetLastError());
   ++e->launches;
   return 0;
@@ -879,15 +892,20 @@ int amrvac_ens_create(const amrvac_cfg *cfg, int ninst, const amrvac_ens_instanc
     for (int r = 0; r < 3; ++r)
       if (e->pool[p][r] && (ce = cudaMemset(e->pool[p][r], 0, sizeof(double) * (p ? 4 * 256 : 3 * 16) * e->nb[p])))
         return fail_free(ce, "cudaMemset(pool)");
-  if (e->mixed) ce = cudaFuncSetAttribute(ens_stage_kernel_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ens_smem(true));
-  else ce = cudaFuncSetAttribute(ens_stage_kernel_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ens_smem(false));
-  if (ce) return fail_free(ce, "cudaFuncSetAttribute");
-  int per_sm = 1, dev = 0, nsm = 148;
-  if (e->mixed) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_stage_kernel_mixed, ENS_THREADS, ens_smem(true));
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_stage_kernel_fp64, ENS_THREADS, ens_smem(false));
+  int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  e->wave = std::max(1, per_sm) * nsm;
+  for (int v = 0; v < e->nvar; ++v) {
+    ce = cudaFuncSetAttribute(ens_stage_fn(e->mixed, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)ens_smem(e->mixed));
+    if (ce) return fail_free(ce, "cudaFuncSetAttribute");
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_stage_fn(e->mixed, v), ENS_THREADS,
+                                                  ens_smem(e->mixed));
+    e->wave_v[v] = std::max(1, per_sm) * nsm;
+  }
+  e->var = 0;
+  e->wave = e->wave_v[0];
   e->grid = e->wave;
   *out = e;
   if (int r = amrvac_ens_reset_time(e)) {
@@ -1043,8 +1061,30 @@ int amrvac_ens_grid(const amrvac_ens *e, int *ctas, int *wave) {
   return 0;
 }
 
+int amrvac_ens_set_variant(amrvac_ens *e, int var) {
+  if (int r = check_ens(e)) return r;
+  if (var < 0 || var >= e->nvar) return efail(AMRVAC_E_ARG, "no such stage-kernel variant");
+  if (var != e->var && e->graph) {
+    cudaGraphExecDestroy(e->graph);
+    e->graph = nullptr;
+  }
+  if (e->grid == e->wave) e->grid = e->wave_v[var];  // one resident wave stays one wave
+  e->var = var;
+  e->wave = e->wave_v[var];
+  return 0;
+}
+
+int amrvac_ens_variant(const amrvac_ens *e, int *var, int *nvar, int *ctas_per_sm) {
+  if (!e) return AMRVAC_E_ARG;
+  if (var) *var = e->var;
+  if (nvar) *nvar = e->nvar;
+  if (ctas_per_sm) *ctas_per_sm = (e->mixed ? 3 : 2) + e->var;  // the launch bounds of the variant
+  return 0;
+}
+
 // Times one forward-Euler-like stage (register 0 -> 1, the state in 0 is
-// untouched) for each candidate grid size and keeps the fastest.
+// untouched) for each stage-kernel variant and candidate grid size, and
+// keeps the fastest pair.
 int amrvac_ens_autotune(amrvac_ens *e, int reps, int *best_ctas, double *best_ms) {
   if (int r = check_ens(e)) return r;
   if (reps <= 0) reps = 5;
@@ -1057,33 +1097,44 @@ int amrvac_ens_autotune(amrvac_ens *e, int reps, int *best_ctas, double *best_ms
   ens_finalize_kernel<<<(e->ninst + 127) / 128, 128, 0, e->stream>>>(T);
   ECK(cudaGetLastError());
   ECK(cudaStreamSynchronize(e->stream));
-  const int cands[4] = {e->wave, 2 * e->wave, 4 * e->wave, e->wave / 2};
   cudaEvent_t a, b;
   ECK(cudaEventCreate(&a));
   ECK(cudaEventCreate(&b));
   double best = 1e30;
-  int bestg = e->wave;
-  const int saved = e->grid;
-  for (int c : cands) {
-    if (c <= 0) continue;
-    e->grid = c;
-    int r = ens_launch_stage(e, 0, 1, 0, 0.0, 1.0, 1.0);  // warm-up
-    if (r) { e->grid = saved; return r; }
-    ECK(cudaEventRecord(a, e->stream));
-    for (int q = 0; q < reps && !r; ++q) r = ens_launch_stage(e, 0, 1, 0, 0.0, 1.0, 1.0);
-    ECK(cudaEventRecord(b, e->stream));
-    ECK(cudaEventSynchronize(b));
-    if (r) { e->grid = saved; return r; }
-    float ms = 0;
-    ECK(cudaEventElapsedTime(&ms, a, b));
-    if (ms / reps < best) { best = ms / reps; bestg = c; }
+  int bestg = e->wave, bestv = e->var;
+  const int saved = e->grid, saved_var = e->var;
+  auto restore = [&]() {
+    e->var = saved_var;
+    e->wave = e->wave_v[saved_var];
+    e->grid = saved;
+  };
+  for (int v = 0; v < e->nvar; ++v) {
+    e->var = v;
+    e->wave = e->wave_v[v];
+    const int cands[4] = {e->wave, 2 * e->wave, 4 * e->wave, e->wave / 2};
+    for (int c : cands) {
+      if (c <= 0) continue;
+      e->grid = c;
+      int r = ens_launch_stage(e, 0, 1, 0, 0.0, 1.0, 1.0);  // warm-up
+      if (r) { restore(); return r; }
+      ECK(cudaEventRecord(a, e->stream));
+      for (int q = 0; q < reps && !r; ++q) r = ens_launch_stage(e, 0, 1, 0, 0.0, 1.0, 1.0);
+      ECK(cudaEventRecord(b, e->stream));
+      ECK(cudaEventSynchronize(b));
+      if (r) { restore(); return r; }
+      float ms = 0;
+      ECK(cudaEventElapsedTime(&ms, a, b));
+      if (ms / reps < best) { best = ms / reps; bestg = c; bestv = v; }
+    }
   }
+  restore();
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   // the probe must not change the instances' clocks: restore done flags and dt
   ECK(cudaMemcpyAsync(e->d_done, done_save.data(), sizeof(int) * e->ninst, cudaMemcpyHostToDevice, e->stream));
   ECK(cudaMemsetAsync(e->d_dt, 0, sizeof(double) * e->ninst, e->stream));
   ECK(cudaStreamSynchronize(e->stream));
+  if (int r = amrvac_ens_set_variant(e, bestv)) return r;
   if (int r = amrvac_ens_set_grid(e, bestg)) return r;
   if (best_ctas) *best_ctas = bestg;
   if (best_ms) *best_ms = best;

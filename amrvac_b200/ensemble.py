@@ -130,6 +130,16 @@ class Ensemble:
         _lib.check(self.L.amrvac_ens_grid(self.h, ctypes.byref(c), ctypes.byref(w)), "amrvac_ens_grid")
         return c.value, w.value
 
+    def set_variant(self, var: int):
+        _lib.check(self.L.amrvac_ens_set_variant(self.h, var), "amrvac_ens_set_variant")
+
+    def variant(self):
+        """{"variant", "nvariants", "ctas_per_sm"} of the stage kernel."""
+        v, n, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(self.L.amrvac_ens_variant(self.h, ctypes.byref(v), ctypes.byref(n), ctypes.byref(c)),
+                   "amrvac_ens_variant")
+        return {"variant": v.value, "nvariants": n.value, "ctas_per_sm": c.value}
+
     def autotune(self, reps: int = 5):
         c = ctypes.c_int()
         ms = ctypes.c_double()

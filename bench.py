@@ -467,6 +467,7 @@ def run_ensemble(args, ws, rank, local):
         ens = _ens_build(specs, prec)
         load(ens)
         grid, tune_ms = ens.autotune(reps=3)
+        tuned = ens.variant()
         for _ in range(args.warmup):  # partial runs: kernels, graph, first touch
             load(ens)
             ens.run(max_steps=min(64, args.it_max or 64), chunk=16)
@@ -488,7 +489,7 @@ def run_ensemble(args, ws, rank, local):
         finals[prec] = [ens.download(i) for i in range(len(specs))]
         ms = float(np.mean(ms_all))
         alg_bytes = float((cells * steps * 72.0 * nw).sum())  # 72*nw B per zone-update: 3 stages + getdt
-        out[prec] = dict(ms=ms, value=ws * zu / (ms * 1e-3), steps=steps, grid=grid, tune_ms=tune_ms,
+        out[prec] = dict(ms=ms, value=ws * zu / (ms * 1e-3), steps=steps, grid=grid, tune_ms=tune_ms, tuned=tuned,
                          launches=launches, chunk_steps=taken, status=flags,
                          hbm_gbs=alg_bytes / (ms * 1e-3) / 1e9, clocks=clk.summary() if clk else None)
         if prec == "fp64":
@@ -537,6 +538,7 @@ def run_ensemble(args, ws, rank, local):
                        "zone_updates_per_run": float((cells * f["steps"]).sum()),
                        "max_steps_of_an_instance": int(f["steps"].max()), "graph_chunk_steps": 16,
                        "grid_ctas": f["grid"], "autotuned_stage_ms": f["tune_ms"],
+                       "stage_variant": f["tuned"],
                        "parallelism": "replicas" if ws > 1 else "single GPU",
                        "l2": "no flush: working set %.0f MB (3 registers) > 126 MB L2" % (
                            3 * float((cells * nw).sum()) * 8 / 1e6)},
@@ -547,6 +549,7 @@ def run_ensemble(args, ws, rank, local):
             "cpu_baseline": cpu, "e2e": out["e2e"],
             "mixed": {"value": out["mixed"]["value"], "unit": UNIT, "ms_per_step": out["mixed"]["ms"],
                       "speedup_vs_fp64": f["ms"] / out["mixed"]["ms"], "grid_ctas": out["mixed"]["grid"],
+                      "stage_variant": out["mixed"]["tuned"],
                       "l1_rel_err_density_vs_fp64": {"max": max(l1), "median": float(np.median(l1))},
                       "status": out["mixed"]["status"]},
             "gpu_launches": int(f["launches"]), "clocks": f["clocks"], "status": f["status"],

@@ -435,8 +435,13 @@ int amrvac_ens_status(amrvac_ens *ens, uint32_t *flags, uint32_t *inst_flags);
 /* CTAs of each stage launch (0 = one resident wave), and the current value. */
 int amrvac_ens_set_grid(amrvac_ens *ens, int ctas);
 int amrvac_ens_grid(const amrvac_ens *ens, int *ctas, int *wave);
-/* Times one stage for candidate grid sizes on the current state (left
- * unchanged) and keeps the fastest. */
+/* Stage-kernel variant: 0 or 1, the second one CTA per SM denser (FP64: two
+ * CTAs per SM at 96 registers, or three at 72; mixed: three at 72, or four
+ * at 56).  Same arithmetic, bit-identical results. */
+int amrvac_ens_set_variant(amrvac_ens *ens, int var);
+int amrvac_ens_variant(const amrvac_ens *ens, int *var, int *nvar, int *ctas_per_sm);
+/* Times one stage for every variant and candidate grid size on the current
+ * state (left unchanged) and keeps the fastest pair. */
 int amrvac_ens_autotune(amrvac_ens *ens, int reps, int *best_ctas, double *best_ms);
 int amrvac_ens_stream(amrvac_ens *ens, void **stream);
 int64_t amrvac_ens_launch_count(const amrvac_ens *ens);
