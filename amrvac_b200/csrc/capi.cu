@@ -1797,9 +1797,12 @@ int amrvac_gpu_step_dt_states(amrvac_ctx *c, double dt, const double *u0, double
     return fail(AMRVAC_E_UNSUPPORTED, "step_dt_states: single-level unsplit grids, no small_values average");
   if (!(dt > 0.0)) return fail(AMRVAC_E_ARG, "dt must be positive");
   if (!u0 || !u1 || (three && !u2)) return fail(AMRVAC_E_ARG, "step_dt_states: null stage buffer");
-  const double *last_in = three ? u2 : u1;
-  if (u1 == u0 || (three && (u2 == u0 || u2 == u1)) || (unew && (unew == last_in || (three && unew == u1))))
-    return fail(AMRVAC_E_ARG, "step_dt_states: a stage would read and write the same buffer");
+  // distinct stage inputs; U^{n+1} may replace u0 only (a stage reads its
+  // input's neighbours, its base cell by cell)
+  if (u1 == u0 || (three && (u2 == u0 || u2 == u1)))
+    return fail(AMRVAC_E_ARG, "step_dt_states: u0, u1 and u2 must be distinct buffers");
+  if (unew && (unew == u1 || (three && unew == u2)))
+    return fail(AMRVAC_E_ARG, "step_dt_states: unew must be u0 or a buffer of its own");
   if (int r = check_a2max(c)) return r;
   CK(launch_set_scalar(c->d_scal + 0, dt, c->stream));
   ++c->launches;
