@@ -197,13 +197,16 @@ __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
   __shared__ int s_q[27], s_kind[27];
   __shared__ int s_nreg;
   __shared__ uint32_t s_coarse;    // bit q: direction q has a coarser neighbour
+  __shared__ int s_nt[27];         // the block's neighbour types, loaded by 27 threads at once
   const int slot = blockIdx.x;
   const int v = blockIdx.y;
   const int b = A.iblocks[slot];
   const int t = threadIdx.x;
   const int L = A.level[b];
+  if (t < 27) s_nt[t] = A.ntype[b * 27 + t];
+  __syncthreads();
   if (t == 0) {
-    const int *nt = A.ntype + b * 27;
+    const int *nt = s_nt;
     int n = 0, m = 0;
     uint32_t cm = 0;
     for (int q = 0; q < 27; ++q) {
