@@ -305,3 +305,16 @@ def test_config_from_par_reads_the_method_options(tmp_path):
     assert c.limiter == 10 and list(c.schmid_rad) == [2.5, 0.5, 1.0] and c.schmid_global == 0
     from amrvac_b200 import make_cfg
     assert make_cfg(limiter="schmid1").schmid_global == 1
+
+
+def test_product_fails_loudly_without_the_library(tmp_path):
+    """With the CUDA library absent there is no fallback: creating a context
+    raises ImportError naming the missing library (fresh process)."""
+    import subprocess
+    import sys
+    env = dict(os.environ, AMRVAC_GPU_LIB=str(tmp_path / "missing" / "libamrvac_gpu.so"))
+    code = ("from amrvac_b200 import Context, make_cfg\n"
+            "Context(make_cfg(physics='hd', ndim=2))\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode != 0
+    assert "ImportError" in r.stderr and "There is no CPU fallback" in r.stderr
