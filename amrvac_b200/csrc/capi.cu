@@ -580,10 +580,10 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
   if (k.fix_small_values && (k.small_values_method < 0 || k.small_values_method > 2))
     return fail(AMRVAC_E_UNSUPPORTED, "small_values_method: error (0), replace (1) or average (2)");
   if (k.fix_small_values && k.small_values_method == 2) {
-    // the whole-block path of 'average' (smallavg.cu) covers FP64, unsplit
+    // the whole-block path of 'average' (smallavg.cu) covers unsplit
     // finite_volume stages with the dwlimiter2 limiters and GLM or no divB
-    // source
-    if (k.precision != 0) return fail(AMRVAC_E_UNSUPPORTED, "small_values_method average: FP64 only");
+    // source; it recomputes a flagged block in FP64 in either form (the
+    // mixed form decides the face-state flags in FP64: sv_near_floor)
     if (k.dimsplit) return fail(AMRVAC_E_UNSUPPORTED, "small_values_method average: unsplit stages only");
     if (k.limiter < 1 || k.limiter > 10 || k.limiter == AMRVAC_LIM_VENK)
       return fail(AMRVAC_E_UNSUPPORTED, "small_values_method average: the dwlimiter2 limiters only");

@@ -73,8 +73,7 @@ def test_unsupported_configurations_are_refused_without_gpu(lib):
     c.small_values_method = 3
     bad.append(c)
     avg = dict(fix_small_values=True, small_values_method="average")
-    bad += [make_cfg(physics="hd", ndim=2, precision="mixed", flux_scheme="hllc", limiter="vanleer", **avg),
-            make_cfg(physics="mhd", ndim=2, typedivbfix="linde", flux_scheme="hll", **avg),
+    bad += [make_cfg(physics="mhd", ndim=2, typedivbfix="linde", flux_scheme="hll", **avg),
             make_cfg(physics="hd", ndim=2, flux_scheme="tvdlf", time_stepper="twostep", **avg),
             make_cfg(physics="hd", ndim=2, flux_scheme="hll", dimsplit=True, **avg),
             make_cfg(physics="hd", ndim=2, flux_scheme="hll", limiter="venk", **avg)]

@@ -311,3 +311,93 @@ def test_average_block_edges_and_physical_sides(oracle_lib, bn, bc):
         err = percell_err(got, ref)
         assert err <= max(RTOL, noise), (bn, bc, step, err, noise)
     assert ctx.status() == 0
+
+
+@pytest.mark.parametrize("name", ["hd2_hll_minmod", "hd2_hllc_cada3_dip", "mhd3_hlld_cada3_glm",
+                                  "mhd3_hlld_cada3_glm_dip"])
+def test_average_mixed_form_takes_the_fp64_decisions(oracle_lib, name):
+    """Mixed form (FP32 faces) with 'average': a face state near a floor is
+    recomputed in FP64, so the blocks the whole-block path recomputes (in
+    FP64) are the FP64 kernel's, and after two steps no cell is further from
+    the FP64 run than FP32 round-off (a missed average would leave a cell at
+    the floor or below it: an O(1) difference)."""
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    _, c64, nd = _setup_avg(oracle_lib, name)
+    kw = dict(AVG_CASES[name], fix_small_values=True, small_values_method="average", small_density=1e-8,
+              small_pressure=1e-8)
+    dip = kw.pop("dip", None)
+    if dip:
+        kw["small_density"] = dip
+    blocks = c64.download()
+    mx = Context(make_cfg(precision="mixed", **kw))
+    mx.set_uniform_grid([32] * nd, [0.0] * nd, [1.0] * nd)
+    mx.upload(blocks)
+    for c in (c64, mx):
+        c.set_time(0.0, 1.0e99, 0.0)
+        c.step()
+        c.step()
+    ref = P.interior(c64.download(), nd)
+    got = P.interior(mx.download(), nd)
+    assert c64.status() == 0 and mx.status() == 0
+    assert np.isfinite(got).all() and got[:, 0].min() >= kw["small_density"] * (1 - 1e-6)
+    scale = np.abs(ref).reshape(ref.shape[0], ref.shape[1], -1).max(axis=(0, 2))
+    dev = np.abs(got - ref).reshape(ref.shape[0], ref.shape[1], -1).max(axis=(0, 2)) / scale
+    assert dev.max() <= 1e-4, dev
+
+
+@pytest.mark.parametrize("name,presteps", [("hd2_hll_minmod", 0), ("hd2_hllc_cada3_dip", 1),
+                                           ("mhd3_hlld_cada3_glm_dip", 1)])
+def test_average_mixed_form_recomputes_the_fp64_blocks(oracle_lib, name, presteps):
+    """One stage from the same state (the planted field, or the dip after one
+    FP64 step, when cada3 first reconstructs face densities below the
+    floor): every block where a small-value fix fires — the oracle's
+    'average' and 'replace' stages differ there — is recomputed in FP64 by
+    the whole-block path in the mixed form too, so it is bit-identical to the
+    FP64 run's; the other blocks differ from it by FP32 round-off only."""
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    O = oracle_lib
+    og, c64, nd = _setup_avg(O, name)
+    kw = dict(AVG_CASES[name], fix_small_values=True, small_values_method="average", small_density=1e-8,
+              small_pressure=1e-8)
+    dip = kw.pop("dip", None)
+    if dip:
+        kw["small_density"] = dip
+    ok = dict(kw)
+    ok["divb"] = ok.pop("typedivbfix", "none")
+    rep = O.make_cfg(**dict(ok, small_values_method="replace"))
+    avg = O.make_cfg(**ok)
+    c64.set_time(0.0, 1.0e99, 0.0)
+    for _ in range(presteps):
+        c64.step()
+    state = c64.download()
+    for ib in range(og.nblocks):
+        og.set_block(ib, state[ib])
+    og.getbc()
+    dt, cg = og.getdt()
+    dt *= 0.5
+    fired = []
+    for ib in range(og.nblocks):
+        w = og.get_block(ib)
+        wa, wr = w.copy(), w.copy()
+        O.finite_volume(avg, w, wa, dt, og.dx(), cg)
+        O.finite_volume(rep, w, wr, dt, og.dx(), cg)
+        fired.append(not np.array_equal(wa, wr))
+    assert any(fired) and not all(fired), fired
+    mx = Context(make_cfg(precision="mixed", **kw))
+    mx.set_uniform_grid([32] * nd, [0.0] * nd, [1.0] * nd)
+    for c in (c64, mx):
+        c.upload(state)
+        c.set_cmax_global(cg)
+        assert c.advect1("ps", "ps1", 1.0, dt) == 0
+    ref = P.interior(c64.download("ps1"), nd)
+    got = P.interior(mx.download("ps1"), nd)
+    scale = np.abs(ref).reshape(ref.shape[0], ref.shape[1], -1).max(axis=(0, 2))
+    for ib, f in enumerate(fired):
+        if f:
+            assert np.array_equal(got[ib], ref[ib]), ib
+        else:
+            dev = np.abs(got[ib] - ref[ib]).reshape(ref.shape[1], -1).max(axis=1) / scale
+            assert dev.max() <= 1e-4, (ib, dev)
+    assert c64.status() == 0 and mx.status() == 0
