@@ -120,8 +120,18 @@ __global__ void __launch_bounds__(256) lohner_kernel(const LohnerArgs A) {
 // neighbours' cells, bc_fill_prolong) is coarse-level data around its
 // footprint, from which interpolation_linear (1381-1525) prolongs the fine
 // ghost cells with monotonized-central slopes.
+// Where a coarse value comes from: the cell itself (n = 1) or its 2^NDIM
+// children one level finer (n = 2^NDIM, averaged x fastest), as the address
+// of variable 0 (each variable bn^NDIM further); flip: bit v, variable v
+// changes sign across a mirror side.  w == nullptr: not found.
+struct CoarseSrc {
+  const double *w;
+  int n;
+  uint32_t flip;
+};
+
 template <int NDIM>
-__device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int P2, int v) {
+__device__ CoarseSrc coarse_source(const AmrGhostArgs &A, int L, int P0, int P1, int P2) {
   const int P[3] = {P0, P1, P2};
   int jg[3] = {0, 0, 0}, loc[3] = {0, 0, 0};
   uint32_t flip = 0;
@@ -147,9 +157,8 @@ __device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int
     jg[d] = p / bn;
     loc[d] = p - jg[d] * bn;
   }
-  const double sg = ((flip >> v) & 1u) ? -1.0 : 1.0;
   const int o = A.owner[A.owner_off[L] + jg[0] + A.nlev[L][0] * (jg[1] + A.nlev[L][1] * jg[2])];
-  if (o >= 0) return sg * A.u[cell_offset<NDIM>(o, A.nw, v, loc[0], loc[1], loc[2], bn)];
+  if (o >= 0) return CoarseSrc{A.u + cell_offset<NDIM>(o, A.nw, 0, loc[0], loc[1], loc[2], bn), 1, flip};
   if (o == -2 && L < A.maxlevel) {
     int jf[3] = {0, 0, 0}, f[3] = {0, 0, 0};
 #pragma unroll
@@ -159,47 +168,59 @@ __device__ double coarse_value(const AmrGhostArgs &A, int L, int P0, int P1, int
       f[d] = 2 * (loc[d] - half * c);
     }
     const int o2 = A.owner[A.owner_off[L + 1] + jf[0] + A.nlev[L + 1][0] * (jf[1] + A.nlev[L + 1][1] * jf[2])];
-    if (o2 >= 0) {
-      const double *w = A.u + cell_offset<NDIM>(o2, A.nw, v, f[0], f[1], f[2], bn);
-      const int SY = bn, SZ = bn * bn;
-      double sum = w[0];  // x fastest, left to right
-      sum = sum + w[1];
-      if constexpr (NDIM > 1) {
-        sum = sum + w[SY];
-        sum = sum + w[SY + 1];
-      }
-      if constexpr (NDIM > 2) {
-        sum = sum + w[SZ];
-        sum = sum + w[SZ + 1];
-        sum = sum + w[SZ + SY];
-        sum = sum + w[SZ + SY + 1];
-      }
-      return sg * (sum * (1.0 / double(1 << NDIM)));
-    }
+    if (o2 >= 0)
+      return CoarseSrc{A.u + cell_offset<NDIM>(o2, A.nw, 0, f[0], f[1], f[2], bn), 1 << NDIM, flip};
   }
   atomicOr(A.status, ST_BOUNDS);  // hierarchy not 2:1 balanced here
-  return 0.0;
+  return CoarseSrc{nullptr, 0, 0u};
 }
 
-// One CTA per (block next to a level jump, variable).  The ghost cells of the
-// level-jump directions are enumerated region by region (a face region is
-// 2 x 16 x 16 cells, an edge 2 x 2 x 16, a corner 2 x 2 x 2), so no thread
-// walks the interior; the coarse representation psc is built first, only
-// where some prolongation stencil reads it.
+// Variable v of a coarse value (coarse_source).
+template <int NDIM>
+__device__ __forceinline__ double coarse_read(const CoarseSrc &s, int v, int bn) {
+  if (!s.w) return 0.0;
+  const int SY = bn, SZ = bn * bn;
+  const double sg = ((s.flip >> v) & 1u) ? -1.0 : 1.0;
+  const double *w = s.w + (size_t)v * (NDIM == 3 ? bn * SZ : (NDIM == 2 ? SZ : bn));
+  if (s.n == 1) return sg * w[0];
+  double sum = w[0];  // x fastest, left to right
+  sum = sum + w[1];
+  if constexpr (NDIM > 1) {
+    sum = sum + w[SY];
+    sum = sum + w[SY + 1];
+  }
+  if constexpr (NDIM > 2) {
+    sum = sum + w[SZ];
+    sum = sum + w[SZ + 1];
+    sum = sum + w[SZ + SY];
+    sum = sum + w[SZ + SY + 1];
+  }
+  return sg * (sum * (1.0 / double(1 << NDIM)));
+}
+
+// One CTA per (block next to a level jump, group of AMR_GHOST_VG variables).
+// The ghost cells of the level-jump directions are enumerated region by
+// region (a face region is 2 x 16 x 16 cells, an edge 2 x 2 x 16, a corner
+// 2 x 2 x 2), so no thread walks the interior; the coarse representation psc
+// is built first, only where some prolongation stencil reads it.  A thread
+// locates a source cell once (coarse_source) and reads it for every variable
+// of the group: independent loads in flight together.
 // BNC: the block edge as a constant (16, the default) so that the index
 // arithmetic folds, or 0 to read it from the arguments.
 template <int NDIM, int BNC = 0>
 __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
-  extern __shared__ double psc[];  // (bn/2+4)^NDIM coarse representation of variable blockIdx.y
+  extern __shared__ double psc[];  // [var of the group][(bn/2+4)^NDIM] coarse representation
   const int bn = BNC ? BNC : A.bn;
   const int C = bn / 2 + 4, CY = NDIM >= 2 ? C : 1, CZ = NDIM >= 3 ? C : 1;
+  const int CC = C * CY * CZ;
   __shared__ int s_off[28];        // prefix sums of the jump regions' cell counts
   __shared__ int s_q[27], s_kind[27];
   __shared__ int s_nreg;
   __shared__ uint32_t s_coarse;    // bit q: direction q has a coarser neighbour
   __shared__ int s_nt[27];         // the block's neighbour types, loaded by 27 threads at once
   const int slot = blockIdx.x;
-  const int v = blockIdx.y;
+  const int v0 = blockIdx.y * AMR_GHOST_VG;
+  const int nv = min(AMR_GHOST_VG, A.nw - v0);
   const int b = A.iblocks[slot];
   const int t = threadIdx.x;
   const int L = A.level[b];
@@ -233,7 +254,7 @@ __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
 #pragma unroll
   for (int d = 0; d < NDIM; ++d) igb[d] = A.ig[3 * b + d];
   if (cmask) {
-    for (int p = t; p < C * CY * CZ; p += blockDim.x) {
+    for (int p = t; p < CC; p += blockDim.x) {
       const int pc[3] = {p % C, NDIM >= 2 ? (p / C) % CY : 0, NDIM >= 3 ? p / (C * CY) : 0};
       // read by the stencils (centre +- 1 per direction) of the ghost cells
       // of a coarser-neighbour direction: coarse index 1 for the low ghosts,
@@ -259,7 +280,14 @@ __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
       int P[3] = {0, 0, 0};
 #pragma unroll
       for (int d = 0; d < NDIM; ++d) P[d] = igb[d] * (bn / 2) + pc[d] - 2;
-      psc[p] = coarse_value<NDIM>(A, L - 1, P[0], P[1], P[2], v);
+      const CoarseSrc src = coarse_source<NDIM>(A, L - 1, P[0], P[1], P[2]);
+      double val[AMR_GHOST_VG];
+#pragma unroll
+      for (int vv = 0; vv < AMR_GHOST_VG; ++vv)
+        if (vv < nv) val[vv] = coarse_read<NDIM>(src, v0 + vv, bn);
+#pragma unroll
+      for (int vv = 0; vv < AMR_GHOST_VG; ++vv)
+        if (vv < nv) psc[vv * CC + p] = val[vv];
     }
     __syncthreads();
   }
@@ -293,7 +321,7 @@ __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
       li /= ext;
       gc[d] = dd[d] < 0 ? l : (dd[d] > 0 ? bn + 2 + l : 2 + l);
     }
-    double val;
+    double val[AMR_GHOST_VG];
     if (kind == AMR_COARSE) {  // prolongation (interpolation_linear)
       int pc[3] = {0, 0, 0};
       double eta[3] = {0, 0, 0};
@@ -305,28 +333,39 @@ __global__ void __launch_bounds__(256) amr_ghost_kernel(const AmrGhostArgs A) {
         eta[d] = (xF - xC) * invC[d];
         pc[d] = ixC - 1;
       }
-      auto at = [&](int a, int bb, int cc) { return psc[a + C * (bb + CY * cc)]; };
-      const double c0 = at(pc[0], pc[1], pc[2]);
-      val = c0;
-      double slope[3] = {0, 0, 0};
 #pragma unroll
-      for (int d = 0; d < NDIM; ++d) {
-        const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
-        const double sL = c0 - at(pc[0] - e0, pc[1] - e1, pc[2] - e2);
-        const double sR = at(pc[0] + e0, pc[1] + e1, pc[2] + e2) - c0;
-        const double sC = 0.5 * (sR + sL);
-        const double sg = copysign(1.0, sC);
-        slope[d] = sg * fmax(0.0, fmin(fmin(fabs(sC), sg * sL), sg * sR));
+      for (int vv = 0; vv < AMR_GHOST_VG; ++vv) {
+        if (vv >= nv) break;
+        const double *ps = psc + vv * CC;
+        auto at = [&](int a, int bb, int cc) { return ps[a + C * (bb + CY * cc)]; };
+        const double c0 = at(pc[0], pc[1], pc[2]);
+        double x = c0;
+        double slope[3] = {0, 0, 0};
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+          const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+          const double sL = c0 - at(pc[0] - e0, pc[1] - e1, pc[2] - e2);
+          const double sR = at(pc[0] + e0, pc[1] + e1, pc[2] + e2) - c0;
+          const double sC = 0.5 * (sR + sL);
+          const double sg = copysign(1.0, sC);
+          slope[d] = sg * fmax(0.0, fmin(fmin(fabs(sC), sg * sL), sg * sR));
+        }
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) x = x + slope[d] * eta[d];
+        val[vv] = x;
       }
-#pragma unroll
-      for (int d = 0; d < NDIM; ++d) val = val + slope[d] * eta[d];
     } else {  // restriction
       int P[3] = {0, 0, 0};
 #pragma unroll
       for (int d = 0; d < NDIM; ++d) P[d] = igb[d] * bn + gc[d] - 2;
-      val = coarse_value<NDIM>(A, L, P[0], P[1], P[2], v);
+      const CoarseSrc src = coarse_source<NDIM>(A, L, P[0], P[1], P[2]);
+#pragma unroll
+      for (int vv = 0; vv < AMR_GHOST_VG; ++vv)
+        if (vv < nv) val[vv] = coarse_read<NDIM>(src, v0 + vv, bn);
     }
-    A.gbuf[ghost_offset<NDIM>(slot, A.nw, v, gc[0] - 2, gc[1] - 2, gc[2] - 2, bn)] = val;
+#pragma unroll
+    for (int vv = 0; vv < AMR_GHOST_VG; ++vv)
+      if (vv < nv) A.gbuf[ghost_offset<NDIM>(slot, A.nw, v0 + vv, gc[0] - 2, gc[1] - 2, gc[2] - 2, bn)] = val[vv];
   }
 }
 
@@ -468,16 +507,29 @@ cudaError_t launch_amr_remap(const AmrRemapArgs &A, int nnew, int ndim, cudaStre
   return cudaGetLastError();
 }
 
+cudaError_t prepare_amr_ghosts(int ndim, int bn) {
+  const size_t c = (size_t)bn / 2 + 4;
+  const int sm2 = (int)(sizeof(double) * AMR_GHOST_VG * c * c), sm3 = (int)(sm2 * c);
+  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  if (bn == 16) {
+    if (ndim == 2) return cudaFuncSetAttribute(amr_ghost_kernel<2, 16>, attr, sm2);
+    return cudaFuncSetAttribute(amr_ghost_kernel<3, 16>, attr, sm3);
+  }
+  if (ndim == 2) return cudaFuncSetAttribute(amr_ghost_kernel<2>, attr, sm2);
+  return cudaFuncSetAttribute(amr_ghost_kernel<3>, attr, sm3);
+}
+
 cudaError_t launch_amr_ghosts(const AmrGhostArgs &A, int nslots, int ndim, cudaStream_t s) {
   if (nslots <= 0) return cudaSuccess;
-  const dim3 grid(nslots, A.nw);
+  const dim3 grid(nslots, (A.nw + AMR_GHOST_VG - 1) / AMR_GHOST_VG);
   const size_t c = (size_t)A.bn / 2 + 4;  // psc edge
+  const size_t sm2 = sizeof(double) * AMR_GHOST_VG * c * c, sm3 = sm2 * c;
   if (A.bn == 16) {
-    if (ndim == 2) amr_ghost_kernel<2, 16><<<grid, 256, sizeof(double) * c * c, s>>>(A);
-    else amr_ghost_kernel<3, 16><<<grid, 256, sizeof(double) * c * c * c, s>>>(A);
+    if (ndim == 2) amr_ghost_kernel<2, 16><<<grid, 256, sm2, s>>>(A);
+    else amr_ghost_kernel<3, 16><<<grid, 256, sm3, s>>>(A);
   } else {
-    if (ndim == 2) amr_ghost_kernel<2><<<grid, 256, sizeof(double) * c * c, s>>>(A);
-    else amr_ghost_kernel<3><<<grid, 256, sizeof(double) * c * c * c, s>>>(A);
+    if (ndim == 2) amr_ghost_kernel<2><<<grid, 256, sm2, s>>>(A);
+    else amr_ghost_kernel<3><<<grid, 256, sm3, s>>>(A);
   }
   return cudaGetLastError();
 }

@@ -72,7 +72,12 @@ struct AmrRemapArgs {
   int nw;
 };
 
+// Variables per CTA of the level-jump ghost pass.
+constexpr int AMR_GHOST_VG = 3;
 cudaError_t launch_amr_ghosts(const AmrGhostArgs &A, int nslots, int ndim, cudaStream_t s);
+// Opt the ghost-pass kernel of (ndim, block edge) into its shared memory
+// (AMR_GHOST_VG coarse representations); once per grid set-up.
+cudaError_t prepare_amr_ghosts(int ndim, int bn);
 // (the remap and Löhner kernels read the block edge from their StageArgs)
 cudaError_t launch_amr_remap(const AmrRemapArgs &A, int nnew, int ndim, cudaStream_t s);
 cudaError_t launch_amr_fix(const AmrFixArgs &A, int nslots, int ndim, cudaStream_t s);

@@ -1244,6 +1244,7 @@ static int amr_grid_impl(amrvac_ctx *c, int nleaf, const int *leaf, const int *n
   }
   G.status = c->d_status;
   A->G = G;
+  CK(prepare_amr_ghosts(nd, c->bn));
   std::memset(&A->F, 0, sizeof(A->F));
   A->F.pflux = A->pflux;
   A->F.nw = c->nw;
