@@ -47,12 +47,14 @@ __global__ void __launch_bounds__(256) getdt_kernel(const GetdtArgs A) {
 #pragma unroll
   for (int d = 0; d < NDIM; ++d) dxinv[d] = 1.0 / A.dxb[b * 3 + d];
   double mtot = 0.0, mcm = 0.0, mdim[3] = {0.0, 0.0, 0.0};
-  // the block's cells, x fastest (coalesced), 256 at a time
+  // the block's cells, x fastest (coalesced), 256 at a time; c is the
+  // cell's index within its block-variable row (cell_offset's layout)
+  const double *ub = A.u + (size_t)b * NW * ncell;
+#pragma unroll 2
   for (int c = t; c < ncell; c += 256) {
-    const int i = c % bn, j = NDIM >= 2 ? (c / bn) % bn : 0, k = NDIM == 3 ? c / (bn * bn) : 0;
     double w[NW];
 #pragma unroll
-    for (int v = 0; v < NW; ++v) w[v] = __ldg(A.u + cell_offset<NDIM>(b, NW, v, i, j, k, bn));
+    for (int v = 0; v < NW; ++v) w[v] = __ldg(ub + (size_t)v * ncell + c);
     // getdt_courant takes the primitives through phys_to_primitive, small-value
     // fix included (src/mod_dt.t:189-191)
     if (A.P.fix_small_values) {
