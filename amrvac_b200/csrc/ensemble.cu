@@ -348,19 +348,23 @@ __device__ __forceinline__ void ens_stage_body(const EnsArgs &A) {
 // Occupancy: two CTAs of 288 threads per SM in FP64 (96 registers: 18 warps
 // put five on one SM sub-partition, whose 16 K registers then cap a thread at
 // 102), three in the mixed form (72 registers, measured 1.23x faster than two).
-// Each form has a second variant one CTA per SM denser, which the autotuner
-// times against the first: FP64 at three CTAs (72 registers, a few spilled),
-// mixed at four (56 registers).
+// Denser variants, which the autotuner times against the first kernel of a
+// form: FP64 at three CTAs per SM (72 registers, a few spilled; four do not
+// fit its shared memory), mixed at four (56 registers) and five (40).
 __global__ void __launch_bounds__(ENS_THREADS, 2) ens_stage_kernel_fp64(const EnsArgs A) { ens_stage_body<double>(A); }
 __global__ void __launch_bounds__(ENS_THREADS, 3) ens_stage_kernel_fp64_3(const EnsArgs A) { ens_stage_body<double>(A); }
 __global__ void __launch_bounds__(ENS_THREADS, 3) ens_stage_kernel_mixed(const EnsArgs A) { ens_stage_body<float>(A); }
 __global__ void __launch_bounds__(ENS_THREADS, 4) ens_stage_kernel_mixed_4(const EnsArgs A) { ens_stage_body<float>(A); }
+__global__ void __launch_bounds__(ENS_THREADS, 5) ens_stage_kernel_mixed_5(const EnsArgs A) { ens_stage_body<float>(A); }
 
-// the stage kernel of (precision, variant)
+// the stage kernel of (precision, variant); variant v is capped for
+// ens_variant_ctas(mixed, v) CTAs per SM
 static void (*ens_stage_fn(bool mixed, int var))(const EnsArgs) {
-  if (mixed) return var == 1 ? ens_stage_kernel_mixed_4 : ens_stage_kernel_mixed;
+  if (mixed) return var == 2 ? ens_stage_kernel_mixed_5 : (var == 1 ? ens_stage_kernel_mixed_4 : ens_stage_kernel_mixed);
   return var == 1 ? ens_stage_kernel_fp64_3 : ens_stage_kernel_fp64;
 }
+static int ens_variants(bool mixed) { return mixed ? 3 : 2; }
+static int ens_variant_ctas(bool mixed, int var) { return (mixed ? 3 : 2) + var; }
 
 // getdt_courant (src/mod_dt.t:160-287), maxsum, per instance: the max over
 // the instance's cells of sum_d (|v_d| + c_s) / dx_d.
@@ -508,9 +512,9 @@ struct amrvac_ens {
   int graph_steps = 0;
   int grid = 0;          // CTAs per stage / getdt launch
   int wave = 1;          // resident stage CTAs of the current variant
-  int var = 0;           // stage-kernel variant: 1 is one CTA per SM denser than 0
+  int var = 0;           // stage-kernel variant: each one CTA per SM denser than the last
   int nvar = 2;
-  int wave_v[2] = {1, 1};
+  int wave_v[3] = {1, 1, 1};
   int64_t launches = 0;
 };
 
@@ -895,6 +899,7 @@ int amrvac_ens_create(const amrvac_cfg *cfg, int ninst, const amrvac_ens_instanc
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  e->nvar = ens_variants(e->mixed);
   for (int v = 0; v < e->nvar; ++v) {
     ce = cudaFuncSetAttribute(ens_stage_fn(e->mixed, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)ens_smem(e->mixed));
@@ -1078,7 +1083,7 @@ int amrvac_ens_variant(const amrvac_ens *e, int *var, int *nvar, int *ctas_per_s
   if (!e) return AMRVAC_E_ARG;
   if (var) *var = e->var;
   if (nvar) *nvar = e->nvar;
-  if (ctas_per_sm) *ctas_per_sm = (e->mixed ? 3 : 2) + e->var;  // the launch bounds of the variant
+  if (ctas_per_sm) *ctas_per_sm = ens_variant_ctas(e->mixed, e->var);  // the launch bounds of the variant
   return 0;
 }
 

@@ -219,27 +219,28 @@ def test_autotune_keeps_state():
         assert np.array_equal(ens.download(i), before[i])
 
 
-@pytest.mark.parametrize("precision,ctas", [("fp64", (2, 3)), ("mixed", (3, 4))])
+@pytest.mark.parametrize("precision,ctas", [("fp64", (2, 3)), ("mixed", (3, 4, 5))])
 def test_stage_variants_give_identical_runs(precision, ctas):
-    """The two stage-kernel variants of a form (one CTA per SM apart) run the
+    """The stage-kernel variants of a form (one CTA per SM apart) run the
     same arithmetic: a whole run is bit-identical."""
     _cuda()
     specs = R.ensemble_specs(12, seed=9, n1=(64, 512), n2=(32, 96), time_max=0.02)
     runs = []
-    for var in (0, 1):
+    for var in range(len(ctas)):
         ens = _ensemble(specs, precision=precision)
         info = ens.variant()
-        assert info["nvariants"] == 2 and info["variant"] == 0
+        assert info["nvariants"] == len(ctas) and info["variant"] == 0
         ens.set_variant(var)
-        assert ens.variant() == {"variant": var, "nvariants": 2, "ctas_per_sm": ctas[var]}
+        assert ens.variant() == {"variant": var, "nvariants": len(ctas), "ctas_per_sm": ctas[var]}
         ens.run(max_steps=100000, chunk=16)
         assert ens.status()[0] == 0
         runs.append(([ens.download(i) for i in range(len(specs))], ens.state()[2]))
-    for a, b in zip(runs[0][0], runs[1][0]):
-        assert np.array_equal(a, b)
-    assert np.array_equal(runs[0][1], runs[1][1])
+    for r in runs[1:]:
+        for a, b in zip(runs[0][0], r[0]):
+            assert np.array_equal(a, b)
+        assert np.array_equal(runs[0][1], r[1])
     with pytest.raises(Exception):
-        ens.set_variant(2)
+        ens.set_variant(len(ctas))
 
 
 def test_non_finite_instance_stops_alone(oracle_lib):
