@@ -107,6 +107,114 @@ __global__ void __launch_bounds__(256) lohner_kernel(const LohnerArgs A) {
   }
 }
 
+// The same estimator with each weighted variable's ghosted block (two
+// layers, the cells the stencil reaches) gathered once into shared memory —
+// the same gather, flips and log10 as lohner_kernel's wv — and the stencils
+// read from there; per-cell error sums in shared memory, variables in
+// ascending order as there.
+template <int NDIM>
+__global__ void __launch_bounds__(256) lohner_staged_kernel(const LohnerArgs A) {
+  extern __shared__ double lsm[];
+  const int b = blockIdx.x;
+  const int t = threadIdx.x;
+  const StageArgs &S = A.sa;
+  const int bn = S.bn;
+  const int nw = A.nw;
+  const int lev = A.level[b];
+  const double wf = A.wavefilter[lev - 1], thr = A.threshold[lev - 1], der = A.derefine[lev - 1];
+  const int G = bn + 4, GY = NDIM >= 2 ? G : 1, GZ = NDIM == 3 ? G : 1;
+  const int ng = G * GY * GZ;
+  const int ncell = bn * (NDIM >= 2 ? bn : 1) * (NDIM == 3 ? bn : 1);
+  double *sw = lsm, *serr = lsm + ng;
+  for (int cell = t; cell < ncell; cell += 256) serr[cell] = 0.0;
+  // staged value at block-local (x, y, z), each in -2 .. bn+1
+  auto at = [&](int x, int y, int z) -> double {
+    return sw[(x + 2) + G * ((NDIM >= 2 ? y + 2 : 0) + GY * (NDIM == 3 ? z + 2 : 0))];
+  };
+  for (int iw = 0; iw < nw; ++iw) {
+    const double wt = A.weight[iw];
+    if (wt == 0.0) continue;
+    __syncthreads();  // the previous variable's stencils are read
+    for (int p = t; p < ng; p += 256) {
+      const int x = p % G - 2, y = NDIM >= 2 ? (p / G) % GY - 2 : 0, z = NDIM == 3 ? p / (G * GY) - 2 : 0;
+      // reached by the stencil: +-2 along one axis, or +-1 along two
+      const int ox = x < 0 ? -x : (x >= bn ? x - bn + 1 : 0);
+      const int oy = y < 0 ? -y : (y >= bn ? y - bn + 1 : 0);
+      const int oz = z < 0 ? -z : (z >= bn ? z - bn + 1 : 0);
+      const int nout = (ox > 0) + (oy > 0) + (oz > 0);
+      if (nout > 2 || (nout == 2 && (ox > 1 || oy > 1 || oz > 1))) continue;
+      int ii = x, jj = y, kk = z;
+      uint32_t flip;
+      const int blk = resolve_cell<NDIM>(S, b, ii, jj, kk, flip, bn);
+      double v = blk >= 0 ? S.uin[cell_offset<NDIM>(blk, nw, iw, ii, jj, kk, bn)]
+                          : S.gbuf[ghost_offset<NDIM>(-2 - blk, nw, iw, ii, jj, kk, bn)];
+      if ((flip >> iw) & 1u) v = -v;
+      sw[p] = ((A.logflag >> iw) & 1u) ? log10(v) : v;
+    }
+    __syncthreads();
+    for (int cell = t; cell < ncell; cell += 256) {
+      const int i = cell % bn, j = NDIM >= 2 ? (cell / bn) % bn : 0, k = NDIM == 3 ? cell / (bn * bn) : 0;
+      double num = 0.0, den = 0.0;
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) {
+        const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+#pragma unroll
+        for (int d2 = 0; d2 < NDIM; ++d2) {
+          const int f0 = d2 == 0, f1 = d2 == 1, f2 = d2 == 2;
+          const double tp = at(i + f0 + e0, j + f1 + e1, k + f2 + e2) - at(i + f0 - e0, j + f1 - e1, k + f2 - e2);
+          const double tm = at(i - f0 + e0, j - f1 + e1, k - f2 + e2) - at(i - f0 - e0, j - f1 - e1, k - f2 - e2);
+          const double q = tp - tm;
+          num = num + q * q;
+        }
+      }
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) {
+        const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+        const double c = at(i, j, k);
+        const double ta = fabs(at(i + 2 * e0, j + 2 * e1, k + 2 * e2) - c) +
+                          fabs(c - at(i - 2 * e0, j - 2 * e1, k - 2 * e2));
+#pragma unroll
+        for (int d2 = 0; d2 < NDIM; ++d2) {
+          const int f0 = d2 == 0, f1 = d2 == 1, f2 = d2 == 2;
+          const double ap = fabs(at(i + f0 + e0, j + f1 + e1, k + f2 + e2)) +
+                            fabs(at(i + f0 - e0, j + f1 - e1, k + f2 - e2));
+          const double am = fabs(at(i - f0 + e0, j - f1 + e1, k - f2 + e2)) +
+                            fabs(at(i - f0 - e0, j - f1 - e1, k - f2 - e2));
+          const double q = ta + wf * (ap + am);
+          den = den + q * q;
+        }
+      }
+      serr[cell] = serr[cell] + wt * sqrt(num / fmax(den, 1.0e-6));
+    }
+  }
+  __syncthreads();
+  bool any_ref = false, all_coa = true;
+  double emax = 0.0;
+  for (int cell = t; cell < ncell; cell += 256) {
+    const double err = serr[cell];
+    if (err >= thr) { any_ref = true; all_coa = false; }
+    else if (!(err <= der * thr)) all_coa = false;
+    emax = fmax(emax, err);
+  }
+  __shared__ double red[8];
+  const int r_any = __syncthreads_or(any_ref);
+  const int r_all = __syncthreads_and(all_coa);
+  double m = emax;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((t & 31) == 0) red[t >> 5] = m;
+  __syncthreads();
+  if (t == 0) {
+    double mm = 0.0;
+    for (int q = 0; q < 8; ++q) mm = fmax(mm, red[q]);
+    int fl = 0;
+    if (r_any && lev < A.refine_max_level) fl |= 1;
+    if (r_all && lev > 1) fl |= 2;
+    A.flags[b] = fl;
+    A.errmax[b] = mm;
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- level jumps
@@ -541,10 +649,30 @@ cudaError_t launch_amr_fix(const AmrFixArgs &A, int nslots, int ndim, cudaStream
   return cudaGetLastError();
 }
 
+// Shared memory of lohner_staged_kernel: one ghosted block-variable (two
+// layers) and the per-cell error sums.
+static size_t lohner_smem(int ndim, int bn) {
+  const size_t g = (size_t)bn + 4;
+  const size_t ng = ndim == 3 ? g * g * g : g * g, nc = ndim == 3 ? (size_t)bn * bn * bn : (size_t)bn * bn;
+  return sizeof(double) * (ng + nc);
+}
+
 cudaError_t launch_lohner(const LohnerArgs &A, int ndim, cudaStream_t s) {
+  if (ndim != 2 && ndim != 3) return cudaErrorInvalidValue;
+  const size_t sm = lohner_smem(ndim, A.sa.bn);
+  if (sm <= 100 * 1024) {  // block edges up to 16 in 3-D, every edge in 2-D
+    const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (ndim == 2) {
+      if (cudaError_t e = cudaFuncSetAttribute(lohner_staged_kernel<2>, attr, (int)sm)) return e;
+      lohner_staged_kernel<2><<<A.sa.nblocks, 256, sm, s>>>(A);
+    } else {
+      if (cudaError_t e = cudaFuncSetAttribute(lohner_staged_kernel<3>, attr, (int)sm)) return e;
+      lohner_staged_kernel<3><<<A.sa.nblocks, 256, sm, s>>>(A);
+    }
+    return cudaGetLastError();
+  }
   if (ndim == 2) lohner_kernel<2><<<A.sa.nblocks, 256, 0, s>>>(A);
-  else if (ndim == 3) lohner_kernel<3><<<A.sa.nblocks, 256, 0, s>>>(A);
-  else return cudaErrorInvalidValue;
+  else lohner_kernel<3><<<A.sa.nblocks, 256, 0, s>>>(A);
   return cudaGetLastError();
 }
 
