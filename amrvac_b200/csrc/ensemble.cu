@@ -333,9 +333,12 @@ __device__ __forceinline__ void ens_stage_body(const EnsArgs &A) {
   uint32_t st = 0;
 #pragma unroll 1
   for (int k = 0; tile < nt; ++k, tile += gridDim.x) {
-    // buffers of tile k: shared tile k % 2 and row table k % 3 (a thread still
-    // accumulating tile k-1 reads only buffers that this iteration leaves alone)
-    TF *s = sm + (k & 1) * EnsTile<TF>::TOTAL;
+    // One shared tile serves every tile: the faces read the cells and halos
+    // before the second barrier, the next tile's staging writes them after
+    // it; the next tile's faces write the flux buffers only after its first
+    // barrier, which every thread reaches after accumulating this tile.  The
+    // row table is k % 3 (the ninth warp fills tile k+1's while tile k runs).
+    TF *s = sm;
     const EnsRow *cur = rows[k % 3];
     EnsRow *nxt = rows[(k + 1) % 3];
     const int next = tile + gridDim.x;
@@ -349,10 +352,11 @@ __device__ __forceinline__ void ens_stage_body(const EnsArgs &A) {
 // put five on one SM sub-partition, whose 16 K registers then cap a thread at
 // 102), three in the mixed form (72 registers, measured 1.23x faster than two).
 // Denser variants, which the autotuner times against the first kernel of a
-// form: FP64 at three CTAs per SM (72 registers, a few spilled; four do not
-// fit its shared memory), mixed at four (56 registers) and five (40).
+// form: FP64 at three CTAs per SM (72 registers, a few spilled) and four (56),
+// mixed at four (56 registers) and five (40).
 __global__ void __launch_bounds__(ENS_THREADS, 2) ens_stage_kernel_fp64(const EnsArgs A) { ens_stage_body<double>(A); }
 __global__ void __launch_bounds__(ENS_THREADS, 3) ens_stage_kernel_fp64_3(const EnsArgs A) { ens_stage_body<double>(A); }
+__global__ void __launch_bounds__(ENS_THREADS, 4) ens_stage_kernel_fp64_4(const EnsArgs A) { ens_stage_body<double>(A); }
 __global__ void __launch_bounds__(ENS_THREADS, 3) ens_stage_kernel_mixed(const EnsArgs A) { ens_stage_body<float>(A); }
 __global__ void __launch_bounds__(ENS_THREADS, 4) ens_stage_kernel_mixed_4(const EnsArgs A) { ens_stage_body<float>(A); }
 __global__ void __launch_bounds__(ENS_THREADS, 5) ens_stage_kernel_mixed_5(const EnsArgs A) { ens_stage_body<float>(A); }
@@ -361,9 +365,9 @@ __global__ void __launch_bounds__(ENS_THREADS, 5) ens_stage_kernel_mixed_5(const
 // ens_variant_ctas(mixed, v) CTAs per SM
 static void (*ens_stage_fn(bool mixed, int var))(const EnsArgs) {
   if (mixed) return var == 2 ? ens_stage_kernel_mixed_5 : (var == 1 ? ens_stage_kernel_mixed_4 : ens_stage_kernel_mixed);
-  return var == 1 ? ens_stage_kernel_fp64_3 : ens_stage_kernel_fp64;
+  return var == 2 ? ens_stage_kernel_fp64_4 : (var == 1 ? ens_stage_kernel_fp64_3 : ens_stage_kernel_fp64);
 }
-static int ens_variants(bool mixed) { return mixed ? 3 : 2; }
+static int ens_variants(bool) { return 3; }
 static int ens_variant_ctas(bool mixed, int var) { return (mixed ? 3 : 2) + var; }
 
 // getdt_courant (src/mod_dt.t:160-287), maxsum, per instance: the max over
@@ -531,7 +535,7 @@ int ecuda(cudaError_t e, const char *where) {
   } while (0)
 
 size_t ens_smem(bool mixed) {
-  return mixed ? 2 * sizeof(float) * EnsTile<float>::TOTAL : 2 * sizeof(double) * EnsTile<double>::TOTAL;
+  return mixed ? sizeof(float) * EnsTile<float>::TOTAL : sizeof(double) * EnsTile<double>::TOTAL;
 }
 
 EnsArgs ens_args(amrvac_ens *e, int reg_ct, int reg_new, int reg_base, double a, double b, double dtfactor) {

@@ -437,9 +437,10 @@ int amrvac_ens_status(amrvac_ens *ens, uint32_t *flags, uint32_t *inst_flags);
 /* CTAs of each stage launch (0 = one resident wave), and the current value. */
 int amrvac_ens_set_grid(amrvac_ens *ens, int ctas);
 int amrvac_ens_grid(const amrvac_ens *ens, int *ctas, int *wave);
-/* Stage-kernel variant, each one CTA per SM denser than the last (FP64: two
- * CTAs per SM at 96 registers, or three at 72; mixed: three at 72, four at
- * 56, or five at 40).  Same arithmetic, bit-identical results. */
+/* Stage-kernel variant 0, 1 or 2, each one CTA per SM denser than the last
+ * (FP64: two CTAs per SM at 96 registers, three at 72 or four at 56; mixed:
+ * three at 72, four at 56 or five at 40).  Same arithmetic, bit-identical
+ * results. */
 int amrvac_ens_set_variant(amrvac_ens *ens, int var);
 int amrvac_ens_variant(const amrvac_ens *ens, int *var, int *nvar, int *ctas_per_sm);
 /* Times one stage for every variant and candidate grid size on the current

@@ -219,7 +219,7 @@ def test_autotune_keeps_state():
         assert np.array_equal(ens.download(i), before[i])
 
 
-@pytest.mark.parametrize("precision,ctas", [("fp64", (2, 3)), ("mixed", (3, 4, 5))])
+@pytest.mark.parametrize("precision,ctas", [("fp64", (2, 3, 4)), ("mixed", (3, 4, 5))])
 def test_stage_variants_give_identical_runs(precision, ctas):
     """The stage-kernel variants of a form (one CTA per SM apart) run the
     same arithmetic: a whole run is bit-identical."""
