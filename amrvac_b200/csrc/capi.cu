@@ -1282,9 +1282,15 @@ int amrvac_gpu_amr_resettree(amrvac_ctx *c, const double *weight, const int *log
                                 amr_wavefilter, lev.data(), flags.data(), nullptr))
     return r;
   std::vector<unsigned char> ref(nb), coa(nb);
+  bool any = false;
   for (int b = 0; b < nb; ++b) {
     ref[b] = (flags[b] & 1) != 0;
     coa[b] = (flags[b] & 2) != 0;
+    any = any || ref[b] || coa[b];
+  }
+  if (!any) {  // nothing to refine or coarsen: the tree stays (it is 2:1 balanced)
+    if (changed) *changed = 0;
+    return 0;
   }
   const std::vector<int> old_leaf = c->amr->h_leaf;
   const int cap = nb * (1 << nd);
