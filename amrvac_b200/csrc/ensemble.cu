@@ -103,8 +103,8 @@ __device__ __forceinline__ uint32_t ens_face(TF *wLp, TF *wRp, const PhysParams 
 // the tile (ci = t % 16, row cj = t / 16) and compute the x-face and the
 // y-face on the low side of their cell; the ninth warp computes the 16 x-faces
 // of the high side (lanes 0..15) and the 16 y-faces of the top (lanes 16..31),
-// so every thread handles at most two faces.  The shared tile is double
-// buffered and the row table triple buffered, so one tile costs two barriers:
+// so every thread handles at most two faces.  One shared tile and a triple-
+// buffered row table, so one tile costs two barriers:
 //   stage cells + halos (+ row table of the next tile, by the ninth warp)
 //   | barrier | all faces of both directions | barrier | accumulate + store.
 constexpr int ENS_THREADS = 288;
