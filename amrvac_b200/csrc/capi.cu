@@ -542,8 +542,8 @@ int amrvac_gpu_create(const amrvac_cfg *cfg, amrvac_ctx **out) {
                        k.limiter == AMRVAC_LIM_WENOYC3;
   if ((k.limiter < 1 || k.limiter > 10) && !special) return fail(AMRVAC_E_UNSUPPORTED, "limiter not supported");
   if (special && k.precision == 1) return fail(AMRVAC_E_UNSUPPORTED, "this limiter is FP64 only");
-  if (bn != 16 && (special || k.precision == 1))
-    return fail(AMRVAC_E_UNSUPPORTED, "block_nx other than 16: FP64 with the slope limiters");
+  if (bn != 16 && special)
+    return fail(AMRVAC_E_UNSUPPORTED, "block_nx other than 16: the slope limiters only");
   if (fifth && k.nghostcells < 3) return fail(AMRVAC_E_ARG, "mp5 / weno5 need nghostcells >= 3");
   if (fifth && k.precision == 1) return fail(AMRVAC_E_UNSUPPORTED, "mp5 / weno5 are FP64 only");
   if (k.typeboundspeed < 1 || k.typeboundspeed > 3) return fail(AMRVAC_E_ARG, "bad typeboundspeed");

@@ -1,8 +1,9 @@
 // Stage / getdt / point kernels for block edges other than 16 (block_nx 8,
 // 10, 12, 32: the reference's own 3-D blast and Kelvin-Helmholtz and 2-D
-// Riemann tests run 8^3, 10^3 and 12^2 blocks).  FP64, the slope limiters
-// and bound speeds at run time (LIM = 0, BS = 0), every solver (TVD-MUSCL
-// with its MUSCL-Hancock predictor).  Each block edge is instantiated in its
+// Riemann tests run 8^3, 10^3 and 12^2 blocks).  The slope limiters and
+// bound speeds at run time (LIM = 0, BS = 0); FP64 with every solver
+// (TVD-MUSCL with its MUSCL-Hancock predictor), the mixed form with the
+// schemes it has at block edge 16.  Each block edge is instantiated in its
 // own translation unit (k_bn*.cu) so that they compile in parallel.
 #pragma once
 
@@ -12,7 +13,33 @@ namespace amrvac {
 
 template <int BN>
 bool lookup_bn(const KernelKey &k, KernelSet *out) {
-  if (k.bn != BN || k.mixed) return false;
+  if (k.bn != BN) return false;
+  if (k.mixed) {
+    if (!k.mhd) {
+      if (k.ndir != k.ndim) return false;
+      if (k.ndim == 2 && k.solver == SOLVER_HLLC) { *out = Launch<false, 2, false, 2, SOLVER_HLLC, 0, 0, float, BN>::set(); return true; }
+      if (k.ndim == 2 && k.solver == SOLVER_HLL) { *out = Launch<false, 2, false, 2, SOLVER_HLL, 0, 0, float, BN>::set(); return true; }
+      if (k.ndim == 3 && k.solver == SOLVER_HLLC) { *out = Launch<false, 3, false, 3, SOLVER_HLLC, 0, 0, float, BN>::set(); return true; }
+      return false;
+    }
+    if (k.ndim == 2 && k.ndir == 3 && k.glm && k.solver == SOLVER_HLLD) {
+      *out = Launch<true, 3, true, 2, SOLVER_HLLD, 0, 0, float, BN>::set();
+      return true;
+    }
+    if (k.ndim == 2 && k.ndir == 3 && !k.glm && k.solver == SOLVER_HLL) {
+      *out = Launch<true, 3, false, 2, SOLVER_HLL, 0, 0, float, BN>::set();
+      return true;
+    }
+    if (k.ndim == 3 && k.ndir == 3 && k.glm && k.solver == SOLVER_HLLD) {
+      *out = Launch<true, 3, true, 3, SOLVER_HLLD, 0, 0, float, BN>::set();
+      return true;
+    }
+    if (k.ndim == 3 && k.ndir == 3 && k.glm && k.solver == SOLVER_HLL) {
+      *out = Launch<true, 3, true, 3, SOLVER_HLL, 0, 0, float, BN>::set();
+      return true;
+    }
+    return false;
+  }
   if (!k.mhd) {
     if (k.ndir != k.ndim) return false;
 #define AMRVAC_BHD(ND, S)                                              \

@@ -161,7 +161,7 @@ int amrvac_gpu_nw(const amrvac_cfg *cfg);
 
 /* Create a context on the current CUDA device.  Refuses unsupported options
  * (AMRVAC_E_UNSUPPORTED), e.g.: 1-D, ndir < ndim, block_nx other than 8, 10,
- * 12, 16, 32 (and, other than 16, the mixed form and MP5/WENO5),
+ * 12, 16, 32 (and, other than 16, MP5/WENO5),
  * small_values_method 'average' with dimsplit, Linde, the MUSCL-Hancock
  * predictor or a limiter outside dwlimiter2; the text comes from
  * amrvac_gpu_last_error().  The configuration has no geometry field: blocks

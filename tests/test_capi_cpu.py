@@ -65,7 +65,7 @@ def test_unsupported_configurations_are_refused_without_gpu(lib):
     bad.append(c)
     # block edges the library has no kernels for, and what only block_nx 16 runs
     bad += [make_cfg(physics="hd", ndim=2, block_nx=14), make_cfg(physics="hd", ndim=3, block_nx=6),
-            make_cfg(physics="hd", ndim=2, block_nx=8, precision="mixed"),
+            make_cfg(physics="hd", ndim=2, block_nx=8, precision="mixed", flux_scheme="tvdlf"),
             make_cfg(physics="hd", ndim=2, block_nx=12, limiter="mp5"),
             make_cfg(physics="mhd", ndim=3, block_nx=10, flux_scheme="tvdmu", dimsplit=True, typedivbfix="glm")]
     # small_values_method: no method 3; 'average' outside its whole-block path
