@@ -377,3 +377,33 @@ def test_regrid_every_step_matches_oracle(oracle_lib, nd):
         ctx.amr_regrid(tree.leaves, bad)
     assert np.array_equal(ctx.download(), before)
     ctx.close()
+
+
+def test_resettree_without_flags_keeps_the_tree():
+    """A single-level tree with refine_max_level 1: no block can be flagged
+    (refinement needs a finer level, coarsening a coarser one), so
+    amrvac_gpu_amr_resettree keeps the tree and the state and reports no
+    change."""
+    _cuda()
+    from amrvac_b200 import Context, make_cfg
+    from amrvac_b200.amr import Tree
+    nd, nb = 2, [4, 4]
+    xmin, xmax = [-0.5] * nd, [0.5] * nd
+
+    def prim(X, Y, Z):
+        out = np.zeros((nd + 2,) + X.shape)
+        out[0] = 1.0 + 0.5 * np.exp(-(X * X + Y * Y) / 0.01)
+        out[nd + 1] = 1.0
+        return out
+    tree = Tree(nd, nb, 1)
+    blocks = A.fill_blocks(tree.leaves, nd, nb, prim, "hd", nd, 1.4, xmin, xmax)
+    ctx = Context(make_cfg(physics="hd", ndim=nd, gamma=1.4, flux_scheme="hll", limiter="minmod",
+                           typeboundary=["periodic"] * (2 * nd)))
+    ctx.set_amr_grid(tree.leaves, nb, xmin, xmax)
+    ctx.upload(blocks)
+    before = ctx.download()
+    weight = np.array([1.0, 0.0, 0.0, 0.0])
+    assert ctx.amr_resettree(weight, refine_max_level=1) is False
+    assert ctx.amr_leaves() == [tuple(t) + (0,) * (4 - len(t)) for t in tree.leaves]
+    assert np.array_equal(ctx.download(), before)
+    ctx.close()
