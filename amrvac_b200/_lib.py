@@ -107,6 +107,7 @@ SIGNATURES = [
     ("amrvac_gpu_get_time", _i, [_vp, _dp, _dp, _dp]),
     ("amrvac_gpu_run_timed", _i, [_vp, _i, _dp, _dp, _dp]),
     ("amrvac_gpu_fp64_peak", _i, [_dp]),
+    ("amrvac_gpu_wait_probe", _i, [_i, _P(_u32)]),
     ("amrvac_gpu_autotune", _i, [_vp, _i, _ip, _dp]),
     ("amrvac_gpu_set_zchunk", _i, [_vp, _i]),
     ("amrvac_gpu_set_stage_variant", _i, [_vp, _i]),

@@ -164,6 +164,29 @@ __global__ void fp64_fma_kernel(double *out, int iters, double a, double b) {
   if (s == 1.2345678) out[0] = s;  // keeps the chains live
 }
 
+// The stage kernel's bounded mbarrier wait on a phase that nothing completes
+// (no arrival, no copy): it gives up after `spins` polls and reports
+// ST_TIMEOUT; nothing is left in flight.
+__global__ void wait_probe_kernel(int spins, uint32_t *status) {
+  __shared__ __align__(8) unsigned long long bar;
+  const uint32_t m = smem_addr(&bar);
+  if (threadIdx.x == 0) mbar_init(m);
+  __syncthreads();
+  if (!mbar_wait(m, 0u, spins) && threadIdx.x == 0) atomicOr(status, ST_TIMEOUT);
+}
+
+cudaError_t run_wait_probe(int spins, uint32_t *flags) {
+  uint32_t *d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(uint32_t));
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemset(d, 0, sizeof(uint32_t))) == cudaSuccess) {
+    wait_probe_kernel<<<1, 32>>>(spins, d);
+    if ((e = cudaGetLastError()) == cudaSuccess) e = cudaMemcpy(flags, d, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  return e;
+}
+
 cudaError_t measure_fp64_peak(double *tflops) {
   int dev, nsm;
   cudaError_t e;

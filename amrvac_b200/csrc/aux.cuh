@@ -22,6 +22,7 @@ struct BcSpec {
 };
 
 cudaError_t measure_fp64_peak(double *tflops);
+cudaError_t run_wait_probe(int spins, uint32_t *flags);
 // rcp_ / div_ / rcp_seed of the stage kernels on n device points (test entry).
 cudaError_t launch_div_points(int n, const double *x, const double *y, double *q, double *r, double *seed,
                               cudaStream_t s);

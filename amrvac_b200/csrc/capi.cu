@@ -1642,6 +1642,12 @@ int amrvac_gpu_autotune(amrvac_ctx *c, int reps, int *best_zchunk, double *best_
   return 0;
 }
 
+int amrvac_gpu_wait_probe(int spins, uint32_t *flags) {
+  if (!flags || spins < 1 || spins > AMRVAC_ASYNC_SPINS) return fail(AMRVAC_E_ARG, "wait_probe: bad arguments");
+  if (cudaError_t e = run_wait_probe(spins, flags)) return cuda_fail(e, "wait_probe");
+  return 0;
+}
+
 int amrvac_gpu_fp64_peak(double *tflops) {
   if (!tflops) return fail(AMRVAC_E_ARG, "null pointer");
   CK(measure_fp64_peak(tflops));

@@ -675,8 +675,8 @@ __device__ __forceinline__ void plane_copy_async(uint32_t mbar, uint32_t dst, ui
                  "l"(src + (size_t)v * sstride), "r"(bytes), "r"(mbar)
                  : "memory");
 }
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (int i = 0; i < AMRVAC_ASYNC_SPINS; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, int spins = AMRVAC_ASYNC_SPINS) {
+  for (int i = 0; i < spins; ++i) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"

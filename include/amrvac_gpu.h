@@ -269,6 +269,13 @@ int amrvac_gpu_run_timed(amrvac_ctx *ctx, int nsteps, double *total_ms, double *
 /* Measured FP64 FMA throughput of the current device (TFLOP/s, 2 flops per
  * FMA) from an in-register FMA-chain kernel; the FP64 roofline denominator. */
 int amrvac_gpu_fp64_peak(double *tflops);
+/* Diagnostic of the bounded wait of the stage kernel's asynchronous plane
+ * staging (no counterpart in the reference): one CTA waits on an mbarrier
+ * phase that nothing completes, gives up after `spins` polls (1 ..
+ * 4194304) and sets AMRVAC_ST_TIMEOUT in *flags (host) — the path a stage
+ * takes when a bulk copy does not arrive; the device stays usable.
+ * Synchronous. */
+int amrvac_gpu_wait_probe(int spins, uint32_t *flags);
 /* Autotuner (no counterpart in the reference, whose block loop has no launch
  * shape): times one stage (ps -> ps1, the state in ps is left unchanged) for
  * each stage-kernel variant of the scheme with each work distribution —

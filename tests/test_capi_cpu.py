@@ -154,6 +154,15 @@ def test_stage_variant_entry_points_check_their_arguments(lib):
     assert lib.amrvac_gpu_set_zchunk(None, 0) < 0
 
 
+def test_wait_probe_checks_its_arguments(lib):
+    """The bounded-wait diagnostic refuses a null result and spin counts
+    outside 1 .. 4194304 before any device work."""
+    f = ctypes.c_uint32(0)
+    assert lib.amrvac_gpu_wait_probe(100, None) < 0
+    assert lib.amrvac_gpu_wait_probe(0, ctypes.byref(f)) < 0
+    assert lib.amrvac_gpu_wait_probe((1 << 22) + 1, ctypes.byref(f)) < 0
+
+
 def test_step_with_caller_stage_buffers_checks_its_arguments(lib):
     """amrvac_gpu_step_dt_states refuses a null context before it touches a
     buffer (no device needed)."""

@@ -128,3 +128,26 @@ def test_autotune_reports_the_chosen_variant(oracle_lib, tmp_path, monkeypatch):
     got = P.interior(ctx.download(), 3)
     ref = P.interior(np.array([og.get_block(ib) for ib in range(og.nblocks)]), 3)
     assert percell_err(got, ref) <= RTOL
+
+
+def test_bounded_wait_gives_up_with_timeout_status(oracle_lib):
+    """The asynchronous variant's mbarrier wait is bounded: a wait on a
+    phase that nothing completes gives up after its poll limit and reports
+    AMRVAC_ST_TIMEOUT (16) instead of hanging; the device stays usable — a
+    stage of the asynchronous variant right after still matches the oracle."""
+    _cuda()
+    import ctypes
+    from amrvac_b200 import _lib
+    L = _lib.load()
+    f = ctypes.c_uint32(0)
+    assert L.amrvac_gpu_wait_probe(1000, ctypes.byref(f)) == 0
+    assert f.value == 16
+    O = oracle_lib
+    og, ocfg, ctx = _setup(O, "periodic")
+    dt, cg, ref = _oracle_stage(O, og, ocfg)
+    ctx.set_cmax_global(cg)
+    ctx.set_stage_variant(1)
+    assert ctx.stage_variant()["async_staging"]
+    assert ctx.advect1("ps", "ps1", 1.0, dt) == 0
+    assert percell_err(P.interior(ctx.download("ps1"), 3), ref) <= RTOL
+    assert ctx.status() == 0
