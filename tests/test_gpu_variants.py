@@ -1,5 +1,5 @@
-"""Stage-kernel variants of the 3-D MHD HLLD + cada3 + GLM scheme against
-the oracle: threads per CTA, CTAs per SM, and asynchronous bulk-copy staging
+"""Stage-kernel variants of the 3-D MHD HLLD + GLM schemes (cada3, and
+vanleer on 'cont' sides) against the oracle: threads per CTA, CTAs per SM, and asynchronous bulk-copy staging
 of the next conserved plane (FP64).  Each variant runs one stage with every
 work distribution (persistent plane ranges, z-chunks of 16, 8 and 4 planes)
 on a 48^3 grid of 27 blocks — z neighbours inside the domain take the bulk
@@ -27,9 +27,10 @@ def _cuda():
         pytest.skip("no CUDA device")
 
 
-def _setup(O, bc, precision="fp64"):
+def _setup(O, bc, precision="fp64", lim="cada3"):
     from amrvac_b200 import Context, make_cfg
-    ok = dict(KW)
+    kw = dict(KW, limiter=lim)
+    ok = dict(kw)
     ok["divb"] = ok.pop("typedivbfix")
     ocfg = O.make_cfg(**ok)
     prim = P.random_smooth("mhd", 3, 3, N, glm=True)
@@ -38,7 +39,7 @@ def _setup(O, bc, precision="fp64"):
     for ib in range(og.nblocks):
         og.set_block(ib, blocks[ib])
     og.getbc()
-    ctx = Context(make_cfg(precision=precision, typeboundary=[bc] * 6, **KW))
+    ctx = Context(make_cfg(precision=precision, typeboundary=[bc] * 6, **kw))
     ctx.set_uniform_grid([N] * 3, [0.0] * 3, [1.0] * 3)
     ctx.upload(blocks)
     return og, ocfg, ctx
@@ -56,11 +57,11 @@ def _oracle_stage(O, og, ocfg):
     return dt, cg, P.interior(np.array(ref), 3)
 
 
-@pytest.mark.parametrize("bc", ["periodic", "cont"])
-def test_fp64_variants_match_oracle(oracle_lib, bc):
+@pytest.mark.parametrize("bc,lim", [("periodic", "cada3"), ("cont", "cada3"), ("cont", "vanleer")])
+def test_fp64_variants_match_oracle(oracle_lib, bc, lim):
     _cuda()
     O = oracle_lib
-    og, ocfg, ctx = _setup(O, bc)
+    og, ocfg, ctx = _setup(O, bc, lim=lim)
     dt, cg, ref = _oracle_stage(O, og, ocfg)
     ctx.set_cmax_global(cg)
     info = ctx.stage_variant()
